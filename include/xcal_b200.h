@@ -1,0 +1,287 @@
+/*
+ * xcal_b200.h -- C ABI of libxcal_b200.so, the sm_100a implementation of the
+ * XCALibre.jl finite-volume hot path (assembly -> CSR, Gauss gradients, face
+ * interpolation, CG/BiCGSTAB with Jacobi/DILU, SIMPLE/PISO corrections).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns
+ * an int32_t status (XCAL_OK == 0, negative on error; xcal_last_error() gives the
+ * message).  Indices in this ABI are 0-based; the Julia side subtracts 1.
+ *
+ * Each declaration names the reference function it replaces (paths are relative
+ * to the XCALibre.jl project root).
+ */
+#ifndef XCAL_B200_H
+#define XCAL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+    XCAL_OK = 0,
+    XCAL_ERR_INVALID = -1,        /* bad argument, mesh or config            */
+    XCAL_ERR_CUDA = -2,           /* CUDA runtime error                      */
+    XCAL_ERR_OOM = -3,            /* device allocation failed                */
+    XCAL_ERR_NOT_CONVERGED = -4,  /* outer loop ended without convergence   */
+    XCAL_ERR_DIVERGED = -5,       /* NaN/Inf seen in a residual             */
+    XCAL_ERR_TIMEOUT = -6,        /* a bounded device wait gave up          */
+    XCAL_ERR_UNSUPPORTED = -7     /* option outside the implemented path    */
+};
+
+/* ---- enumerations mirroring the reference's dispatch types ------------- */
+/* boundary conditions: src/Discretise/boundary_conditions/ *.jl           */
+enum {
+    XCAL_BC_DIRICHLET = 1,          /* dirichlet.jl                          */
+    XCAL_BC_DIRICHLET_FUNCTION = 2, /* dirichletFunction.jl (values per face)*/
+    XCAL_BC_WALL = 3,               /* wall.jl                               */
+    XCAL_BC_ZEROGRADIENT = 4,       /* zerogradient.jl                       */
+    XCAL_BC_EXTRAPOLATED = 5,       /* extrapolated.jl                       */
+    XCAL_BC_EMPTY = 6,              /* empty.jl                              */
+    XCAL_BC_SYMMETRY = 7,           /* symmetry.jl                           */
+    XCAL_BC_NEUMANN = 8,            /* neumann.jl (scalar fields)            */
+    XCAL_BC_PERIODIC = 9,           /* periodic.jl `Periodic` (shadow side)  */
+    XCAL_BC_PERIODIC_PARENT = 10    /* periodic.jl `PeriodicParent`          */
+};
+/* Time{T}: src/Discretise/Discretise_1_schemes.jl:12-45 */
+enum { XCAL_TIME_STEADY = 0, XCAL_TIME_EULER = 1 };
+/* Divergence{T}: src/Discretise/Discretise_1_schemes.jl:114-180 */
+enum { XCAL_DIV_LINEAR = 0, XCAL_DIV_UPWIND = 1, XCAL_DIV_LUST = 2 };
+/* Krylov solver: src/Solve/Solve_1_Krylov_solvers.jl:6-15 */
+enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
+/* preconditioner: src/Solve/Preconditioners/preconditioners_0_types.jl */
+enum { XCAL_PRECOND_NONE = 0, XCAL_PRECOND_JACOBI = 1, XCAL_PRECOND_DILU = 2 };
+/* turbulence: RANS{Laminar} / LES{Smagorinsky} */
+enum { XCAL_TURB_LAMINAR = 0, XCAL_TURB_SMAGORINSKY = 1 };
+/* arithmetic of the Krylov inner iterations */
+enum { XCAL_PREC_FP64 = 0, XCAL_PREC_MIXED = 1 };
+/* pressure-velocity algorithm: run! dispatch, src/Solvers/Solvers_3_solver_dispatch.jl:120,225 */
+enum { XCAL_ALGO_SIMPLE = 0, XCAL_ALGO_PISO = 1 };
+/* equations */
+enum { XCAL_EQN_U = 0, XCAL_EQN_P = 1 };
+
+/* field identifiers for xcal_case_get_field / xcal_case_set_field.
+ * Cell fields hold n_cells values per component, face fields n_faces; vector
+ * fields are stored component-major (all x, then all y, then all z), tensor
+ * fields in the order xx,xy,xz,yx,yy,yz,zx,zy,zz (res[i,j] = d u_i / d x_j). */
+enum {
+    XCAL_FIELD_U = 0,      /* VectorField U (3 x n_cells)                   */
+    XCAL_FIELD_P = 1,      /* ScalarField p                                 */
+    XCAL_FIELD_MDOTF = 2,  /* FaceScalarField mdotf                         */
+    XCAL_FIELD_NUEFF = 3,  /* FaceScalarField nueff                         */
+    XCAL_FIELD_GRADP = 4,  /* Grad{Gauss}(p).result (3 x n_cells)           */
+    XCAL_FIELD_GRADU = 5,  /* Grad{Gauss}(U).result (9 x n_cells)           */
+    XCAL_FIELD_RD = 6,     /* rD (n_cells)                                  */
+    XCAL_FIELD_HV = 7,     /* Hv (3 x n_cells)                              */
+    XCAL_FIELD_DIVHV = 8,  /* divHv (n_cells)                               */
+    XCAL_FIELD_NUT = 9,    /* nut (n_cells)                                 */
+    XCAL_FIELD_NUTF = 10,  /* nutf (n_faces)                                */
+    XCAL_FIELD_UF = 11,    /* Uf (3 x n_faces)                              */
+    XCAL_FIELD_PF = 12,    /* pf (n_faces)                                  */
+    XCAL_FIELD_RDF = 13,   /* rDf (n_faces)                                 */
+    XCAL_FIELD_DELTA = 14, /* LES filter (C*Delta)^2 (n_cells)              */
+    XCAL_FIELD_COUNT = 15
+};
+
+/* ---- mesh: the Mesh3 contract (src/Mesh/Mesh_0_types.jl:28-205) ---------
+ * Faces 0..n_bfaces-1 are boundary faces, patch-contiguous, with
+ * face_owner[f] == face_neigh[f]; faces n_bfaces..n_faces-1 are internal.
+ * cell_faces lists each cell's INTERNAL faces (owner before neighbour in
+ * increasing face order, src/FoamMesh/FoamMesh_2_connect.jl:24-69) with the
+ * normal sign (+1 owner, -1 neighbour) and the cell across the face.
+ * Vectors are interleaved xyz (3 doubles per face/cell).                    */
+typedef struct {
+    int32_t n_cells;
+    int32_t n_faces;
+    int32_t n_bfaces;
+    const int32_t* face_owner;        /* [n_faces]  ownerCells[1]            */
+    const int32_t* face_neigh;        /* [n_faces]  ownerCells[2]            */
+    const double* face_centre;        /* [3*n_faces]                         */
+    const double* face_normal;        /* [3*n_faces]                         */
+    const double* face_e;             /* [3*n_faces]                         */
+    const double* face_area;          /* [n_faces]                           */
+    const double* face_delta;         /* [n_faces]                           */
+    const double* face_weight;        /* [n_faces]                           */
+    const double* cell_centre;        /* [3*n_cells]                         */
+    const double* cell_volume;        /* [n_cells]                           */
+    const int32_t* cell_faces_offset; /* [n_cells+1] (faces_range)           */
+    const int32_t* cell_faces;        /* [2*n_ifaces]                        */
+    const int32_t* cell_nsign;        /* [2*n_ifaces]                        */
+    const int32_t* cell_neighbours;   /* [2*n_ifaces]                        */
+    const int32_t* boundary_cellsID;  /* [n_bfaces]                          */
+    int32_t n_patches;
+    const int32_t* patch_start;       /* [n_patches] first face id           */
+    const int32_t* patch_count;       /* [n_patches]                         */
+} xcal_mesh_desc;
+
+/* ---- boundary condition (one per patch per field) ----------------------
+ * Mirrors the functor structs in src/Discretise/boundary_conditions/
+ * after `assign` (src/Discretise/Discretise_4_assign_boundaries.jl:5).      */
+typedef struct {
+    int32_t type;               /* XCAL_BC_*                                 */
+    int32_t patch;              /* patch index into the mesh's patch list   */
+    double value[3];            /* scalar in value[0], vector in value[0..2]*/
+    /* DirichletFunction: values of f(face.centre, time, i) for the patch's
+     * faces, evaluated by the caller (components interleaved for vectors). */
+    const double* face_values;
+    /* Periodic / PeriodicParent (construct_periodic, periodic.jl:95-217)  */
+    const int32_t* face_map;    /* [patch_count] partner face ids           */
+    double distance[3];         /* LinearTransform.distance                 */
+    int32_t partner_patch;
+} xcal_bc;
+
+/* SolverSetup (src/Solve/Solve_1_api.jl:8-83) */
+typedef struct {
+    int32_t solver;             /* XCAL_SOLVER_*                             */
+    int32_t precond;            /* XCAL_PRECOND_*                            */
+    double convergence;
+    double relax;
+    double atol;
+    double rtol;
+    int32_t itmax;
+} xcal_solver_setup;
+
+/* Schemes (src/Solve/Solve_1_api.jl:205-211); gradient is always Gauss and
+ * the Laplacian always Linear on this path. */
+typedef struct {
+    int32_t time;               /* XCAL_TIME_*                               */
+    int32_t divergence;         /* XCAL_DIV_*                                */
+} xcal_schemes;
+
+/* Configuration + Physics (src/Simulate/Simulate_0_types.jl:32-74,
+ * src/ModelPhysics/0_type_definition.jl:196-229) reduced to what the hot
+ * path reads. */
+typedef struct {
+    int32_t algorithm;          /* XCAL_ALGO_SIMPLE / XCAL_ALGO_PISO         */
+    int32_t turbulence;         /* XCAL_TURB_*                               */
+    double nu;                  /* Fluid{Incompressible}(nu)                 */
+    double smagorinsky_C;       /* LES{Smagorinsky}(C)                       */
+    xcal_schemes U_schemes;
+    xcal_schemes p_schemes;
+    xcal_solver_setup U_solver;
+    xcal_solver_setup p_solver;
+    int32_t iterations;         /* Runtime.iterations                        */
+    double dt;                  /* Runtime.dt (time step; 1 for steady)      */
+    int32_t has_pref;           /* run!(...; pref) given                     */
+    double pref;
+    int32_t inner_loops;        /* PISO correctors (run!(...; inner_loops))  */
+    int32_t precision;          /* XCAL_PREC_*                               */
+    int32_t n_bc_U, n_bc_p, n_bc_nut;
+    const xcal_bc* bc_U;
+    const xcal_bc* bc_p;
+    const xcal_bc* bc_nut;
+} xcal_config;
+
+typedef struct xcal_ctx xcal_ctx;
+typedef struct xcal_mesh xcal_mesh;
+typedef struct xcal_case xcal_case;
+
+/* ---- context ------------------------------------------------------------ */
+/* Hardware(backend=B200Backend()) (src/Simulate/Simulate_0_types.jl:70-74) */
+int32_t xcal_ctx_create(int32_t device, xcal_ctx** out);
+int32_t xcal_ctx_destroy(xcal_ctx* ctx);
+/* message of the last error on this context (never NULL) */
+const char* xcal_last_error(const xcal_ctx* ctx);
+/* library version string */
+const char* xcal_version(void);
+
+/* ---- mesh ----------------------------------------------------------------*/
+/* adapt(backend, mesh) (docs/src/user_guide/1_preprocessing.md:88): copies
+ * the Mesh3 arrays to HBM as SoA and derives the CSR-slot maps that replace
+ * spindex searches (src/ModelFramework/ModelFramework_0_types.jl:246-258). */
+int32_t xcal_mesh_upload(xcal_ctx* ctx, const xcal_mesh_desc* desc, xcal_mesh** out);
+int32_t xcal_mesh_destroy(xcal_mesh* mesh);
+
+/* ---- case: equations, fields, solver state -------------------------------*/
+/* setup_incompressible_solvers (src/Solvers/Solvers_1_SIMPLE.jl:45-101):
+ * builds U_eqn (VectorEquation) and p_eqn (ScalarEquation), their CSR
+ * patterns (sparse_matrix_connectivity + periodic extend_matrix,
+ * ModelFramework_0_types.jl:223-243, periodic.jl:219-254), preconditioners
+ * and Krylov workspaces.  Fields start at zero (initialise! sets them). */
+int32_t xcal_case_create(xcal_ctx* ctx, const xcal_mesh* mesh,
+                         const xcal_config* cfg, xcal_case** out);
+int32_t xcal_case_destroy(xcal_case* cs);
+/* nnz of the equation's CSR (U or p) */
+int32_t xcal_case_nnz(const xcal_case* cs, int32_t eqn, int64_t* nnz);
+/* export the CSR pattern (0-based rowptr[n+1], colval[nnz]) */
+int32_t xcal_case_csr_pattern(const xcal_case* cs, int32_t eqn,
+                              int32_t* rowptr, int32_t* colval);
+/* export the current matrix values and right-hand side of an equation.
+ * eqn U: component 0..2 selects bx/by/bz, nzval is the A of the last
+ * component whose boundary conditions were applied; component -1 returns
+ * A0 (the assembled matrix before boundary conditions) with bx.  */
+int32_t xcal_case_get_system(const xcal_case* cs, int32_t eqn, int32_t component,
+                             double* nzval, double* b);
+/* initialise! (src/Fields/Fields_0_types.jl:381-401) and field transfer */
+int32_t xcal_case_set_field(xcal_case* cs, int32_t field, const double* host, int64_t count);
+int32_t xcal_case_get_field(const xcal_case* cs, int32_t field, double* host, int64_t count);
+/* replace DirichletFunction face values of BC `bc_index` of field
+ * (XCAL_EQN_U or XCAL_EQN_P) -- the host-evaluated f(centre, time, i) */
+int32_t xcal_case_set_bc_values(xcal_case* cs, int32_t eqn, int32_t bc_index,
+                                const double* values, int64_t count);
+
+/* ---- algorithms ------------------------------------------------------------*/
+/* SIMPLE outer iterations (src/Solvers/Solvers_1_SIMPLE.jl:103-263).  The
+ * first call runs the initial calculations (:150-156).  res_hist receives
+ * 4 residuals (Ux, Uy, Uz, p) per iteration; *converged is set when every
+ * residual fell below its SolverSetup.convergence (the loop then stops). */
+int32_t xcal_simple_iterate(xcal_case* cs, int32_t n_iter, double* res_hist,
+                            int32_t* n_done, int32_t* converged);
+/* PISO time steps (src/Solvers/Solvers_2_PISO.jl:40-211); res_hist as above,
+ * courant (may be NULL) receives max_courant_number! per step. */
+int32_t xcal_piso_step(xcal_case* cs, int32_t n_steps, double* res_hist,
+                       double* courant, int32_t* n_done);
+
+/* ---- fine-grained hooks (one reference function each) -------------------*/
+/* interpolate!(Uf,U) + correct_boundaries! + flux! + grad!(∇p) + update_nueff!
+ * (Solvers_1_SIMPLE.jl:150-156) */
+int32_t xcal_initial_calculations(xcal_case* cs);
+/* discretise! (src/Discretise/Discretise_2_generated_distretisation.jl:3,89) */
+int32_t xcal_discretise(xcal_case* cs, int32_t eqn);
+/* update_equation! + apply_boundary_conditions! (Discretise_5_apply_bcs.jl:5)
+ * for one component (U: 0..2; p: 0) */
+int32_t xcal_apply_boundary_conditions(xcal_case* cs, int32_t eqn, int32_t component);
+/* implicit_relaxation_diagdom! (src/Solve/Solve_1_api.jl:370-411) on U */
+int32_t xcal_implicit_relaxation_diagdom(xcal_case* cs, int32_t component);
+/* setReference! (src/Solve/Solve_1_api.jl:414-439) on p */
+int32_t xcal_set_reference(xcal_case* cs);
+/* update_preconditioner! (preconditioners_2_functions.jl:65-108) */
+int32_t xcal_update_preconditioner(xcal_case* cs, int32_t eqn);
+/* solve_system! (src/Solve/Solve_1_api.jl:268-307): Krylov solve warm-started
+ * from the field, copy back, then residual (:441-464). */
+int32_t xcal_solve_system(xcal_case* cs, int32_t eqn, int32_t component,
+                          double* residual, int32_t* iterations);
+/* solve_equation! (src/Solve/Solve_1_api.jl:214-266); res[3] for U, res[1] p */
+int32_t xcal_solve_equation(xcal_case* cs, int32_t eqn, double* res);
+/* inverse_diagonal! + interpolate!(rDf, rD) + correct_interpolation_periodic
+ * + remove_pressure_source! + H! (Solvers_1_SIMPLE.jl:170-174) */
+int32_t xcal_pressure_predictor(xcal_case* cs);
+/* interpolate!(Uf,Hv) + correct_boundaries! + flux! + div!
+ * (Solvers_1_SIMPLE.jl:177-185) */
+int32_t xcal_flux_divergence(xcal_case* cs);
+/* explicit_relaxation! (src/Solve/Solve_1_api.jl:317-335): p = prev + a(p-prev) */
+int32_t xcal_explicit_relaxation_p(xcal_case* cs, double alpha);
+/* grad!(∇p, pf, p, BCs.p) (src/Calculate/Calculate_0_gradient.jl:105-111) */
+int32_t xcal_grad_p(xcal_case* cs);
+/* correct_mass_flux! + correct_velocity! (Solvers_1_SIMPLE.jl:210-211) */
+int32_t xcal_correct(xcal_case* cs);
+/* turbulence! + update_nueff! (RANS_laminar.jl:73-79, LES_Smagorinsky.jl:105-132,
+ * Solvers_0_functions.jl:5-35) */
+int32_t xcal_turbulence(xcal_case* cs);
+/* max_courant_number! (Solvers_0_functions.jl:253-276) */
+int32_t xcal_max_courant(xcal_case* cs, double* courant);
+
+/* ---- timers --------------------------------------------------------------*/
+/* cumulative device time (ms) per phase since case creation:
+ * [0] assembly+BCs, [1] U Krylov, [2] p Krylov, [3] gradients/interp/flux,
+ * [4] residuals, [5] total iterate; returns the number of entries written */
+int32_t xcal_get_timings(const xcal_case* cs, double* ms, int32_t n);
+/* number of kernel launches issued by this case since creation */
+int32_t xcal_get_launch_count(const xcal_case* cs, int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XCAL_B200_H */

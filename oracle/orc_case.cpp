@@ -1,0 +1,1219 @@
+// orc_case.cpp -- oracle restatement of the SIMPLE/PISO hot path.
+//
+// TEST INFRASTRUCTURE ONLY (see orc_common.hpp).  Every function cites the
+// XCALibre.jl source it restates (paths relative to the project root).
+#include "orc_internal.hpp"
+
+#include <cstring>
+#include <stdexcept>
+
+namespace orc {
+
+// ---------------------------------------------------------------------------
+// CSR helpers
+// ---------------------------------------------------------------------------
+// spindex (src/ModelFramework/ModelFramework_0_types.jl:246-258), 0-based
+int CSR::find(int i, int j) const {
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k)
+        if (colval[k] == j) return k;
+    return -1;
+}
+
+// sparse_matrix_connectivity (ModelFramework_0_types.jl:223-243) + periodic
+// extend_matrix (periodic.jl:219-254) + sparsecsr (sorted rows, merged
+// duplicates, explicit zeros kept).
+static void build_pattern(const Mesh& m, const std::vector<BC>& bcs, CSR& A) {
+    int n = m.n_cells;
+    std::vector<std::vector<int>> rows(n);
+    for (int c = 0; c < n; ++c) {
+        rows[c].push_back(c);
+        for (int k = m.cf_off[c]; k < m.cf_off[c + 1]; ++k) rows[c].push_back(m.cell_neigh[k]);
+    }
+    for (const BC& bc : bcs) {
+        if (bc.type != XCAL_BC_PERIODIC_PARENT) continue;
+        for (int i = 0; i < bc.count; ++i) {
+            int f1 = bc.start + i, f2 = bc.face_map[i];
+            int c1 = m.owner[f1], c2 = m.owner[f2];
+            rows[c1].push_back(c2);
+            rows[c2].push_back(c1);
+        }
+    }
+    A.n = n;
+    A.rowptr.assign(n + 1, 0);
+    A.colval.clear();
+    for (int c = 0; c < n; ++c) {
+        std::sort(rows[c].begin(), rows[c].end());
+        rows[c].erase(std::unique(rows[c].begin(), rows[c].end()), rows[c].end());
+        for (int j : rows[c]) A.colval.push_back(j);
+        A.rowptr[c + 1] = (int)A.colval.size();
+    }
+    A.nzval.assign(A.colval.size(), 0.0);
+    A.diag.resize(n);
+    for (int c = 0; c < n; ++c) A.diag[c] = A.find(c, c);
+}
+
+static void spmv(const CSR& A, const std::vector<double>& x, std::vector<double>& y) {
+    // xmul! (src/Multithread/spmvm.jl:35-59): sequential per row from 0
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < A.n; ++i) {
+        double acc = 0.0;
+        for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) acc = acc + A.nzval[k] * x[A.colval[k]];
+        y[i] = acc;
+    }
+}
+
+static double cdot(const std::vector<double>& a, const std::vector<double>& b) {
+    const double* pa = a.data();
+    const double* pb = b.data();
+    return creduce((int64_t)a.size(), [&](int64_t i) { return pa[i] * pb[i]; });
+}
+
+// ---------------------------------------------------------------------------
+// case construction
+// ---------------------------------------------------------------------------
+static void copy_bcs(const Mesh& m, const xcal_bc* src, int n, std::vector<BC>& dst, int ncomp) {
+    dst.clear();
+    for (int b = 0; b < n; ++b) {
+        BC bc;
+        bc.type = src[b].type;
+        bc.patch = src[b].patch;
+        if (bc.patch < 0 || bc.patch >= (int)m.patch_start.size()) throw std::runtime_error("bad patch");
+        for (int c = 0; c < 3; ++c) bc.value[c] = src[b].value[c];
+        bc.start = m.patch_start[bc.patch];
+        bc.count = m.patch_count[bc.patch];
+        if (bc.type == XCAL_BC_DIRICHLET_FUNCTION) {
+            if (!src[b].face_values) throw std::runtime_error("DirichletFunction without values");
+            bc.face_values.assign(src[b].face_values, src[b].face_values + (size_t)ncomp * bc.count);
+        }
+        if (bc.type == XCAL_BC_PERIODIC || bc.type == XCAL_BC_PERIODIC_PARENT) {
+            if (!src[b].face_map) throw std::runtime_error("periodic without face_map");
+            bc.face_map.assign(src[b].face_map, src[b].face_map + bc.count);
+            bc.distance = {src[b].distance[0], src[b].distance[1], src[b].distance[2]};
+            bc.partner_patch = src[b].partner_patch;
+        }
+        dst.push_back(bc);
+    }
+}
+
+Case* case_create(const Mesh* m, const xcal_config* cfg) {
+    Case* C = new Case();
+    C->m = m;
+    C->cfg = *cfg;
+    C->nC = m->n_cells;
+    C->nF = m->n_faces;
+    C->nB = m->n_bfaces;
+    copy_bcs(*m, cfg->bc_U, cfg->n_bc_U, C->bcU, 3);
+    copy_bcs(*m, cfg->bc_p, cfg->n_bc_p, C->bcP, 1);
+    copy_bcs(*m, cfg->bc_nut, cfg->n_bc_nut, C->bcNut, 1);
+    C->cfg.bc_U = C->cfg.bc_p = C->cfg.bc_nut = nullptr;
+    int nC = C->nC, nF = C->nF;
+    for (int d = 0; d < 3; ++d) {
+        C->U[d].assign(nC, 0.0);
+        C->gradp[d].assign(nC, 0.0);
+        C->Hv[d].assign(nC, 0.0);
+        C->Uf[d].assign(nF, 0.0);
+        C->bU[d].assign(nC, 0.0);
+    }
+    for (int d = 0; d < 9; ++d) C->gradU[d].assign(nC, 0.0);
+    C->p.assign(nC, 0.0);
+    C->mdotf.assign(nF, 0.0);
+    C->nueff.assign(nF, 0.0);
+    C->rD.assign(nC, 0.0);
+    C->divHv.assign(nC, 0.0);
+    C->nut.assign(nC, 0.0);
+    C->nutf.assign(nF, 0.0);
+    C->pf.assign(nF, 0.0);
+    C->rDf.assign(nF, 1.0);  // initialise!(rDf, 1.0) (Solvers_1_SIMPLE.jl:61)
+    C->Delta.assign(nC, 0.0);
+    C->prev.assign(nC, 0.0);
+    C->cellsCourant.assign(nC, 0.0);
+    C->bp.assign(nC, 0.0);
+    build_pattern(*m, C->bcU, C->AU);
+    C->AU0 = C->AU;
+    build_pattern(*m, C->bcP, C->Ap);
+    C->PU.assign(nC, 0.0);
+    C->Pp.assign(nC, 0.0);
+    // LES{Smagorinsky} initialise (LES_Smagorinsky.jl:84-101, LES_functions.jl:1-55)
+    if (cfg->turbulence == XCAL_TURB_SMAGORINSKY) {
+        double distance = 1.0, power = 1.0 / 3.0;
+        for (const BC& bc : C->bcU)
+            if (bc.type == XCAL_BC_EMPTY) {
+                // 2D slab: distance between the Empty patches (delta_scaling, Mesh3)
+                V3 pmin{0, 0, 0}, pmax{0, 0, 0};
+                for (int f = 0; f < C->nB; ++f)
+                    for (int k = m->fn_off[f]; k < m->fn_off[f + 1]; ++k) {
+                        V3 c = m->points[m->face_nodes[k]];
+                        pmin = {std::min(pmin.x, c.x), std::min(pmin.y, c.y), std::min(pmin.z, c.z)};
+                        pmax = {std::max(pmax.x, c.x), std::max(pmax.y, c.y), std::max(pmax.z, c.z)};
+                    }
+                V3 n = m->fnormal[bc.start];
+                distance = std::fabs(dot(pmin, n)) + std::fabs(dot(pmax, n));
+                power = 0.5;
+                break;
+            }
+        for (int i = 0; i < nC; ++i) {
+            double d = std::pow(m->cvol[i] / distance, power);
+            double dc = d * cfg->smagorinsky_C;
+            C->Delta[i] = dc * dc;
+        }
+    }
+    return C;
+}
+
+// ---------------------------------------------------------------------------
+// discretisation
+// ---------------------------------------------------------------------------
+enum TermKind { T_TIME, T_DIV, T_LAP };
+struct Term {
+    TermKind kind;
+    double sign;
+    const std::vector<double>* flux;  // face flux (Div: mdotf, Lap: nueff/rDf)
+    int scheme;                       // time or divergence scheme
+};
+
+// terms of U_eqn: Time(U) + Divergence(mdotf,U) - Laplacian(nueff,U) == -Source(grad p)
+// (Solvers_1_SIMPLE.jl:68-74)
+static std::vector<Term> u_terms(Case& C) {
+    return {{T_TIME, 1.0, nullptr, C.cfg.U_schemes.time},
+            {T_DIV, 1.0, &C.mdotf, C.cfg.U_schemes.divergence},
+            {T_LAP, -1.0, &C.nueff, 0}};
+}
+// p_eqn: -Laplacian(rDf, p) == -Source(divHv) (Solvers_1_SIMPLE.jl:76-78)
+static std::vector<Term> p_terms(Case& C) { return {{T_LAP, -1.0, &C.rDf, 0}}; }
+
+// scheme! (src/Discretise/Discretise_1_schemes.jl)
+static void scheme(const Mesh& m, const Term& t, int fID, int ns, double& ac, double& an) {
+    if (t.kind == T_TIME) {  // :12-23, :26-34
+        ac = 0.0;
+        an = 0.0;
+        return;
+    }
+    double dns = (double)ns;
+    double flux = (*t.flux)[fID];
+    if (t.kind == T_LAP) {  // Laplacian{Linear} :68-110
+        V3 Sf = (dns * m.farea[fID]) * m.fnormal[fID];
+        V3 e = dns * m.fe[fID];
+        V3 Ef = (dot(Sf, Sf) / dot(Sf, e)) * e;
+        double Ef_mag = norm(Ef);
+        double ap = (t.sign * (flux * Ef_mag)) / m.fdelta[fID];
+        ac = -ap;
+        an = ap;
+        return;
+    }
+    double ap = t.sign * (flux * dns);
+    if (t.scheme == XCAL_DIV_LINEAR) {  // :114-134
+        double w = m.fweight[fID];
+        w = 0.5 + dns * (w - 0.5);
+        ac = ap * w;
+        an = ap * (1.0 - w);
+    } else if (t.scheme == XCAL_DIV_UPWIND) {  // :137-152
+        ac = jl_max(ap, 0.0);
+        an = -jl_max(-ap, 0.0);
+    } else {  // LUST :155-180
+        double w = m.fweight[fID];
+        if (ns < 0) w = 1.0 - w;
+        double acL = ap * w, anL = ap * (1.0 - w);
+        double acU = jl_max(ap, 0.0), anU = -jl_max(-ap, 0.0);
+        ac = 0.75 * acL + 0.25 * acU;
+        an = 0.75 * anL + 0.25 * anU;
+    }
+}
+
+// scheme_source! for Time{Euler} (:36-45); zero for every other term
+static void scheme_source(const Case& C, const Term& t, int c, double prev, double& ac, double& b) {
+    if (t.kind == T_TIME && t.scheme == XCAL_TIME_EULER) {
+        double vol_rdt = (1.0 * C.m->cvol[c]) / C.cfg.dt;
+        ac = vol_rdt;
+        b = prev * vol_rdt;
+    } else {
+        ac = 0.0;
+        b = 0.0;
+    }
+}
+
+// _discretise_vector_model! (Discretise_2_generated_distretisation.jl:39-87)
+static void discretise_U(Case& C) {
+    const Mesh& m = *C.m;
+    std::vector<Term> terms = u_terms(C);
+    CSR& A0 = C.AU0;
+    std::fill(A0.nzval.begin(), A0.nzval.end(), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < C.nC; ++i) {
+        double ac_sum = 0.0;
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            int fID = m.cell_faces[k], ns = m.cell_nsign[k], nID = m.cell_neigh[k];
+            int nIndex = A0.find(i, nID);
+            double AC = 0.0, AN = 0.0;
+            for (const Term& t : terms) {
+                double ac, an;
+                scheme(m, t, fID, ns, ac, an);
+                AC = AC + ac;
+                AN = AN + an;
+            }
+            ac_sum = ac_sum + AC;
+            A0.nzval[nIndex] = AN;
+        }
+        double AC = 0.0, BX = 0.0, BY = 0.0, BZ = 0.0;
+        for (const Term& t : terms) {
+            double ac, bx, by, bz;
+            scheme_source(C, t, i, C.U[0][i], ac, bx);
+            scheme_source(C, t, i, C.U[1][i], ac, by);
+            scheme_source(C, t, i, C.U[2][i], ac, bz);
+            AC = AC + ac;
+            BX = BX + bx;
+            BY = BY + by;
+            BZ = BZ + bz;
+        }
+        A0.nzval[A0.diag[i]] = ac_sum + AC;
+        // _sources!: -Source(grad p): Bx += sign*field.x*volume
+        double V = m.cvol[i];
+        double Bx = 0.0 + (-1.0 * C.gradp[0][i]) * V;
+        double By = 0.0 + (-1.0 * C.gradp[1][i]) * V;
+        double Bz = 0.0 + (-1.0 * C.gradp[2][i]) * V;
+        C.bU[0][i] = BX + Bx;
+        C.bU[1][i] = BY + By;
+        C.bU[2][i] = BZ + Bz;
+    }
+}
+
+// _discretise_scalar_model! (:125-167)
+static void discretise_p(Case& C) {
+    const Mesh& m = *C.m;
+    std::vector<Term> terms = p_terms(C);
+    CSR& A = C.Ap;
+    std::fill(A.nzval.begin(), A.nzval.end(), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < C.nC; ++i) {
+        double ac_sum = 0.0;
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            int fID = m.cell_faces[k], ns = m.cell_nsign[k], nID = m.cell_neigh[k];
+            int nIndex = A.find(i, nID);
+            double AC = 0.0, AN = 0.0;
+            for (const Term& t : terms) {
+                double ac, an;
+                scheme(m, t, fID, ns, ac, an);
+                AC = AC + ac;
+                AN = AN + an;
+            }
+            ac_sum = ac_sum + AC;
+            A.nzval[nIndex] = AN;
+        }
+        double AC = 0.0, B = 0.0;
+        for (const Term& t : terms) {
+            double ac, b;
+            scheme_source(C, t, i, 0.0, ac, b);
+            AC = AC + ac;
+            B = B + b;
+        }
+        A.nzval[A.diag[i]] = ac_sum + AC;
+        double b2 = 0.0 + (-1.0 * C.divHv[i]) * m.cvol[i];
+        C.bp[i] = b2 + B;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// boundary conditions (Discretise_5_apply_bcs.jl + boundary_conditions/*.jl)
+// ---------------------------------------------------------------------------
+static const BC* find_bc(const std::vector<BC>& bcs, int f) {
+    for (const BC& bc : bcs)
+        if (f >= bc.start && f < bc.start + bc.count) return &bc;
+    return nullptr;
+}
+
+struct BCCtx {
+    Case* C;
+    CSR* A;
+    bool vector;
+    int comp;                     // component (vector fields)
+    const std::vector<double>* phi;  // component values / scalar values
+};
+
+static double bc_value(const BC& bc, bool vector, int comp, int i) {
+    if (bc.type == XCAL_BC_DIRICHLET_FUNCTION) return vector ? bc.face_values[3 * i + comp] : bc.face_values[i];
+    return vector ? bc.value[comp] : bc.value[0];
+}
+
+// one BC functor call: returns (ap, bp); periodic parents also update A
+static void bc_functor(BCCtx& X, const BC& bc, const Term& t, int f, double& ap, double& bp) {
+    Case& C = *X.C;
+    const Mesh& m = *C.m;
+    int i = f - bc.start;
+    int cell = m.bcell[f];
+    ap = 0.0;
+    bp = 0.0;
+    if (t.kind == T_TIME) return;  // Discretise_3_boundary_conditions.jl:2-9
+    double flux = (*t.flux)[f];
+    switch (bc.type) {
+        case XCAL_BC_DIRICHLET:
+        case XCAL_BC_DIRICHLET_FUNCTION: {  // dirichlet.jl, dirichletFunction.jl
+            double val = bc_value(bc, X.vector, X.comp, i);
+            if (t.kind == T_LAP) {
+                double fl = (flux * m.farea[f]) / m.fdelta[f];
+                double a = t.sign * (-fl);
+                ap = a;
+                bp = a * val;
+            } else {
+                double fl = -flux;
+                double a = t.sign * fl;
+                ap = 0.0;
+                bp = a * val;
+            }
+            return;
+        }
+        case XCAL_BC_WALL: {  // wall.jl
+            if (t.kind == T_LAP) {
+                if (!X.vector) return;
+                double fl = (flux * m.farea[f]) / m.fdelta[f];
+                double a = t.sign * (-fl);
+                V3 n = m.fnormal[f];
+                V3 vb{bc.value[0], bc.value[1], bc.value[2]};
+                V3 vc{C.U[0][cell], C.U[1][cell], C.U[2][cell]};
+                V3 vc_n = dot(vc, n) * n;
+                V3 vb_n = dot(vb, n) * n;
+                V3 vb_p = vb - vb_n;
+                ap = a;
+                bp = a * (comp(vb_p, X.comp) + comp(vc_n, X.comp));
+            } else {
+                if (X.vector) return;
+                ap = t.sign * flux;
+            }
+            return;
+        }
+        case XCAL_BC_ZEROGRADIENT:  // zerogradient.jl
+            if (t.kind == T_DIV) ap = t.sign * flux;
+            return;
+        case XCAL_BC_EXTRAPOLATED:  // extrapolated.jl
+            if (t.kind == T_LAP) {
+                double fl = ((-flux) * m.farea[f]) / m.fdelta[f];
+                double a = t.sign * fl;
+                ap = a;
+                bp = a * (*X.phi)[cell];
+            } else {
+                ap = t.sign * flux;
+            }
+            return;
+        case XCAL_BC_EMPTY:
+        case XCAL_BC_PERIODIC:
+            return;
+        case XCAL_BC_SYMMETRY: {  // symmetry.jl
+            if (t.kind == T_LAP) {
+                if (!X.vector) return;
+                double fl = (flux * m.farea[f]) / m.fdelta[f];
+                double a = t.sign * (-fl);
+                V3 n = m.fnormal[f];
+                V3 vc{C.U[0][cell], C.U[1][cell], C.U[2][cell]};
+                V3 vn = dot(vc, n) * n;
+                V3 vp = vc - vn;
+                ap = a;
+                bp = a * comp(vp, X.comp);
+            } else {
+                double a = t.sign * flux;
+                if (!X.vector) {
+                    ap = a;
+                    return;
+                }
+                V3 n = m.fnormal[f];
+                V3 vc{C.U[0][cell], C.U[1][cell], C.U[2][cell]};
+                V3 vn = dot(vc, n) * n;
+                ap = a;
+                bp = a * comp(vn, X.comp);
+            }
+            return;
+        }
+        case XCAL_BC_NEUMANN: {  // neumann.jl (scalar)
+            if (t.kind == T_LAP) {
+                double fl = flux * m.farea[f];
+                ap = 0.0;
+                bp = fl * bc.value[0];
+            } else {
+                double a = t.sign * flux;
+                ap = a;
+                bp = ((-bc.value[0]) * a) * m.fdelta[f];
+            }
+            return;
+        }
+        case XCAL_BC_PERIODIC_PARENT: {  // periodic.jl:261-443
+            CSR& A = *X.A;
+            int pfID = bc.face_map[i];
+            int pcell = m.owner[pfID];
+            int NN = A.find(pcell, pcell), NP = A.find(pcell, cell), PN = A.find(cell, pcell);
+            if (t.kind == T_LAP) {
+                V3 C1 = m.ccentre[cell];
+                V3 C2 = m.ccentre[pcell] - bc.distance;
+                V3 d = C2 - C1;
+                double Delta = norm(d);
+                V3 Sf = m.farea[f] * m.fnormal[f];
+                V3 e = m.fe[f];
+                V3 Ef = (dot(Sf, Sf) / dot(Sf, e)) * e;
+                double Ef_mag = norm(Ef);
+                double gamma = ((-t.sign) * (flux * Ef_mag)) / Delta;
+                A.nzval[NN] = A.nzval[NN] + gamma;
+                A.nzval[NP] = A.nzval[NP] + (-gamma);
+                A.nzval[PN] = A.nzval[PN] + (-gamma);
+                ap = gamma;
+                return;
+            }
+            if (t.scheme == XCAL_DIV_UPWIND) {
+                double mdot = t.sign * flux;
+                double a = jl_max(mdot, 0.0), an = -jl_max(-mdot, 0.0);
+                A.nzval[NN] = A.nzval[NN] + (-an);
+                A.nzval[NP] = A.nzval[NP] + (-a);
+                A.nzval[PN] = A.nzval[PN] + an;
+                ap = a;
+                return;
+            }
+            V3 C1 = m.ccentre[cell];
+            V3 C2 = m.ccentre[pcell] - bc.distance;
+            V3 Cf = m.fcentre[f], n = m.fnormal[f];
+            V3 Pf = Cf - C1, PNv = C2 - C1;
+            double wn = dot(Pf, n) / dot(PNv, n);
+            double w = 1.0 - wn;
+            double ac, an;
+            if (t.scheme == XCAL_DIV_LINEAR) {
+                double a = t.sign * flux;
+                ac = a * w;
+                an = a * wn;
+            } else {  // LUST
+                double mdot = t.sign * flux;
+                double acL = mdot * w, anL = mdot * wn;
+                double acU = jl_max(mdot, 0.0), anU = -jl_max(-mdot, 0.0);
+                ac = 0.75 * acL + 0.25 * acU;
+                an = 0.75 * anL + 0.25 * anU;
+            }
+            A.nzval[NN] = A.nzval[NN] + (-an);
+            A.nzval[NP] = A.nzval[NP] + (-ac);
+            A.nzval[PN] = A.nzval[PN] + an;
+            ap = ac;
+            return;
+        }
+        default:
+            return;
+    }
+}
+
+// apply_boundary_conditions! in boundary-face order (the reference's atomics
+// are applied here in ascending face id order)
+static void apply_bcs(Case& C, bool vector, int comp) {
+    const Mesh& m = *C.m;
+    std::vector<Term> terms = vector ? u_terms(C) : p_terms(C);
+    CSR& A = vector ? C.AU : C.Ap;
+    std::vector<double>& b = vector ? C.bU[comp] : C.bp;
+    const std::vector<BC>& bcs = vector ? C.bcU : C.bcP;
+    BCCtx X{&C, &A, vector, comp, vector ? &C.U[comp] : &C.p};
+    for (int f = 0; f < C.nB; ++f) {
+        const BC* bc = find_bc(bcs, f);
+        if (!bc) continue;
+        int cell = m.bcell[f];
+        double AP = 0.0, BP = 0.0;
+        for (const Term& t : terms) {
+            double ap, bp;
+            bc_functor(X, *bc, t, f, ap, bp);
+            AP = AP + ap;
+            BP = BP + bp;
+        }
+        A.nzval[A.diag[cell]] = A.nzval[A.diag[cell]] + AP;
+        b[cell] = b[cell] + BP;
+    }
+}
+
+// update_equation! (:305-330) A <- A0
+static void update_equation(Case& C) { C.AU.nzval = C.AU0.nzval; }
+
+// implicit_relaxation_diagdom! (src/Solve/Solve_1_api.jl:388-411)
+static void relax_diagdom(Case& C, int comp) {
+    CSR& A = C.AU;
+    std::vector<double>& b = C.bU[comp];
+    const std::vector<double>& field = C.U[comp];
+    double alpha = C.cfg.U_solver.relax;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < A.n; ++i) {
+        int c = A.diag[i];
+        double sumv = 0.0;
+        for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) sumv = sumv + std::fabs(A.nzval[k]);
+        sumv = sumv - std::fabs(A.nzval[c]);
+        double D0 = A.nzval[c];
+        double D_max = jl_max(std::fabs(D0), sumv) / alpha;
+        A.nzval[c] = D_max;
+        b[i] = b[i] + (D_max - D0) * field[i];
+    }
+}
+
+// setReference! (Solve_1_api.jl:414-439), cellID = 1
+static void set_reference(Case& C) {
+    if (!C.cfg.has_pref) return;
+    CSR& A = C.Ap;
+    int c = A.diag[0];
+    C.bp[0] = A.nzval[c] * C.cfg.pref;
+    A.nzval[c] = A.nzval[c] + A.nzval[c];
+}
+
+// update_preconditioner! (preconditioners_2_functions.jl:65-108; DILU
+// preconditioners_1_DILU.jl:43-82)
+static void update_precond(const CSR& A, int type, std::vector<double>& P) {
+    if (type == XCAL_PRECOND_JACOBI) {
+        for (int i = 0; i < A.n; ++i) {
+            double d = std::fabs(A.nzval[A.diag[i]]);
+            P[i] = 1.0 / d;
+        }
+    } else if (type == XCAL_PRECOND_DILU) {
+        for (int i = 0; i < A.n; ++i) P[i] = A.nzval[A.diag[i]];
+        for (int i = 0; i < A.n; ++i) {
+            for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) {
+                int j = A.colval[k];
+                if (j > i) {
+                    int k2 = A.find(j, i);
+                    if (k2 >= 0) P[j] = P[j] - (A.nzval[k] * A.nzval[k2]) / P[i];
+                }
+            }
+        }
+    }
+}
+
+// forward/backward_substitution! (preconditioners_1_DILU.jl:84-120)
+static void dilu_ldiv(const CSR& A, const std::vector<double>& D, std::vector<double>& x,
+                      const std::vector<double>& b) {
+    int n = A.n;
+    for (int i = 0; i < n; ++i) {
+        double sum = 0.0;
+        for (int k = A.rowptr[i]; k < A.diag[i]; ++k) {
+            int j = A.colval[k];
+            sum = sum + (A.nzval[k] * x[j]) * (1.0 / D[j]);
+        }
+        x[i] = b[i] - sum;
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double sum = 0.0;
+        for (int k = A.diag[i] + 1; k < A.rowptr[i + 1]; ++k) sum = sum + A.nzval[k] * x[A.colval[k]];
+        x[i] = (x[i] - sum) / D[i];
+    }
+}
+
+static void apply_M(const CSR& A, int type, const std::vector<double>& P, std::vector<double>& out,
+                    const std::vector<double>& in) {
+    if (type == XCAL_PRECOND_JACOBI) {
+        for (int i = 0; i < A.n; ++i) out[i] = P[i] * in[i];
+    } else if (type == XCAL_PRECOND_DILU) {
+        dilu_ldiv(A, P, out, in);
+    } else {
+        out = in;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Krylov.jl 0.10 restatements (warm start x0 = field values)
+// ---------------------------------------------------------------------------
+// CG (Hestenes-Stiefel) as in Krylov.jl cg!: x0 = 0 plus warm-start shift
+static int krylov_cg(const CSR& A, const std::vector<double>& b, std::vector<double>& field, int ptype,
+                     const std::vector<double>& P, const xcal_solver_setup& S, Krylov& K) {
+    int n = A.n;
+    K.dx = field;
+    K.x.assign(n, 0.0);
+    K.r.assign(n, 0.0);
+    K.p.assign(n, 0.0);
+    K.q.assign(n, 0.0);
+    K.z.assign(n, 0.0);
+    spmv(A, K.dx, K.r);
+    for (int i = 0; i < n; ++i) K.r[i] = b[i] - K.r[i];
+    bool MisI = ptype == XCAL_PRECOND_NONE;
+    std::vector<double>& z = MisI ? K.r : K.z;
+    if (!MisI) apply_M(A, ptype, P, z, K.r);
+    K.p = z;
+    double gamma = cdot(K.r, z);
+    double rNorm = std::sqrt(gamma);
+    int iter = 0;
+    if (gamma == 0.0) {
+        for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + K.dx[i];
+        field = K.x;
+        K.niter = 0;
+        return 0;
+    }
+    int itmax = S.itmax == 0 ? 2 * n : S.itmax;
+    double pNorm2 = gamma;
+    double eps_ = S.atol + S.rtol * rNorm;
+    const double epsT = std::numeric_limits<double>::epsilon();
+    bool solved = rNorm <= eps_, tired = iter >= itmax, zero_curv = false;
+    while (!(solved || tired || zero_curv)) {
+        spmv(A, K.p, K.q);
+        double pAp = cdot(K.p, K.q);
+        if (pAp <= epsT * pNorm2) {
+            if (std::fabs(pAp) <= epsT * pNorm2) zero_curv = true;
+        }
+        if (zero_curv) continue;
+        double alpha = gamma / pAp;
+        for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + alpha * K.p[i];
+        for (int i = 0; i < n; ++i) K.r[i] = K.r[i] + (-alpha) * K.q[i];
+        if (!MisI) apply_M(A, ptype, P, z, K.r);
+        double gamma_next = cdot(K.r, z);
+        rNorm = std::sqrt(gamma_next);
+        bool mach = (rNorm + 1.0 <= 1.0);
+        solved = (rNorm <= eps_) || mach;
+        if (!solved) {
+            double beta = gamma_next / gamma;
+            pNorm2 = gamma_next + (beta * beta) * pNorm2;
+            gamma = gamma_next;
+            for (int i = 0; i < n; ++i) K.p[i] = z[i] + beta * K.p[i];
+        }
+        iter = iter + 1;
+        tired = iter >= itmax;
+    }
+    for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + K.dx[i];
+    field = K.x;
+    K.niter = iter;
+    return iter;
+}
+
+// BiCGSTAB (van der Vorst) as in Krylov.jl bicgstab! with left preconditioner
+// M, c = b (shadow residual), warm start.
+static int krylov_bicgstab(const CSR& A, const std::vector<double>& b, std::vector<double>& field, int ptype,
+                           const std::vector<double>& P, const xcal_solver_setup& S, Krylov& K) {
+    int n = A.n;
+    bool MisI = ptype == XCAL_PRECOND_NONE;
+    K.dx = field;
+    K.x.assign(n, 0.0);
+    K.s.assign(n, 0.0);
+    K.v.assign(n, 0.0);
+    K.r.assign(n, 0.0);
+    K.q.assign(n, 0.0);
+    K.t.assign(n, 0.0);
+    std::vector<double> r0(n);
+    spmv(A, K.dx, r0);
+    for (int i = 0; i < n; ++i) r0[i] = b[i] - r0[i];
+    if (!MisI)
+        apply_M(A, ptype, P, K.r, r0);
+    else
+        K.r = r0;
+    K.p = K.r;
+    const std::vector<double>& c = b;
+    double rNorm = std::sqrt(cdot(K.r, K.r));
+    int iter = 0;
+    if (rNorm == 0.0) {
+        for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + K.dx[i];
+        field = K.x;
+        K.niter = 0;
+        return 0;
+    }
+    int itmax = S.itmax == 0 ? 2 * n : S.itmax;
+    double eps_ = S.atol + S.rtol * rNorm;
+    double next_rho = cdot(c, K.r);
+    if (next_rho == 0.0) {
+        for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + K.dx[i];
+        field = K.x;
+        K.niter = 0;
+        return 0;
+    }
+    bool solved = rNorm <= eps_, tired = iter >= itmax, breakdown = false;
+    std::vector<double> d(n);
+    while (!(solved || tired || breakdown)) {
+        iter = iter + 1;
+        double rho = next_rho;
+        spmv(A, K.p, K.q);  // q = A y, y = p
+        if (!MisI)
+            apply_M(A, ptype, P, K.v, K.q);
+        else
+            K.v = K.q;
+        double alpha = rho / cdot(c, K.v);
+        for (int i = 0; i < n; ++i) K.s[i] = K.r[i] + (-alpha) * K.v[i];
+        for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + alpha * K.p[i];
+        spmv(A, K.s, d);  // d = A z, z = s
+        if (!MisI)
+            apply_M(A, ptype, P, K.t, d);
+        else
+            K.t = d;
+        std::vector<double>& tt = K.t;
+        double omega = cdot(tt, K.s) / cdot(tt, tt);
+        for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + omega * K.s[i];
+        for (int i = 0; i < n; ++i) K.r[i] = K.s[i] + (-omega) * tt[i];
+        next_rho = cdot(c, K.r);
+        double beta = (next_rho / rho) * (alpha / omega);
+        for (int i = 0; i < n; ++i) K.p[i] = K.r[i] + beta * (K.p[i] + (-omega) * K.v[i]);
+        rNorm = std::sqrt(cdot(K.r, K.r));
+        bool mach = (rNorm + 1.0 <= 1.0);
+        solved = (rNorm <= eps_) || mach;
+        tired = iter >= itmax;
+        breakdown = (alpha == 0.0) || std::isnan(alpha);
+    }
+    for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + K.dx[i];
+    field = K.x;
+    K.niter = iter;
+    return iter;
+}
+
+// residual (Solve_1_api.jl:441-464)
+static double residual(const CSR& A, const std::vector<double>& b, const std::vector<double>& x) {
+    std::vector<double> Fx(A.n);
+    spmv(A, x, Fx);
+    const double* pb = b.data();
+    const double* pf = Fx.data();
+    double sR = creduce(A.n, [&](int64_t i) {
+        double d = pb[i] - pf[i];
+        return d * d;
+    });
+    double normb = std::sqrt(creduce(A.n, [&](int64_t i) { return pb[i] * pb[i]; }));
+    double denom = normb > jl_eps(normb) ? normb : 1.0;
+    return std::sqrt(sR) / denom;
+}
+
+// solve_system! (Solve_1_api.jl:268-307)
+static double solve_system(Case& C, bool vector, int comp, int* iters) {
+    const xcal_solver_setup& S = vector ? C.cfg.U_solver : C.cfg.p_solver;
+    CSR& A = vector ? C.AU : C.Ap;
+    std::vector<double>& b = vector ? C.bU[comp] : C.bp;
+    std::vector<double>& field = vector ? C.U[comp] : C.p;
+    std::vector<double>& P = vector ? C.PU : C.Pp;
+    Krylov& K = vector ? C.kU : C.kp;
+    int it = S.solver == XCAL_SOLVER_CG ? krylov_cg(A, b, field, S.precond, P, S, K)
+                                        : krylov_bicgstab(A, b, field, S.precond, P, S, K);
+    if (iters) *iters = it;
+    return residual(A, b, field);
+}
+
+// ---------------------------------------------------------------------------
+// calculus: interpolation, boundaries, gradients, divergence, flux
+// ---------------------------------------------------------------------------
+// interpolate_Scalar! (Calculate_2_interpolation.jl:58-76)
+static void interpolate(const Mesh& m, const std::vector<double>& phi, std::vector<double>& phif) {
+#pragma omp parallel for schedule(static)
+    for (int f = 0; f < m.n_faces; ++f) {
+        double w = m.fweight[f];
+        double omw = 1.0 - w;
+        phif[f] = w * phi[m.owner[f]] + omw * phi[m.neigh[f]];
+    }
+}
+
+// boundary_interpolation! for every BC (1_boundary_interpolation.jl and the
+// *_interpolation.jl files); vector fields pass all three components
+static void correct_boundaries(Case& C, const std::vector<BC>& bcs, std::vector<double>* phif,
+                               const std::vector<double>* phi, bool vector) {
+    const Mesh& m = *C.m;
+    int ncomp = vector ? 3 : 1;
+    for (int f = 0; f < C.nB; ++f) {
+        const BC* bc = find_bc(bcs, f);
+        if (!bc) continue;
+        int i = f - bc->start;
+        int c = m.bcell[f];
+        switch (bc->type) {
+            case XCAL_BC_DIRICHLET:
+            case XCAL_BC_DIRICHLET_FUNCTION:
+                for (int d = 0; d < ncomp; ++d) phif[d][f] = bc_value(*bc, vector, d, i);
+                break;
+            case XCAL_BC_WALL:
+                if (vector)
+                    for (int d = 0; d < 3; ++d) phif[d][f] = bc->value[d];
+                else
+                    phif[0][f] = phi[0][c];
+                break;
+            case XCAL_BC_ZEROGRADIENT:
+            case XCAL_BC_EXTRAPOLATED:
+                for (int d = 0; d < ncomp; ++d) phif[d][f] = phi[d][c];
+                break;
+            case XCAL_BC_EMPTY:
+                for (int d = 0; d < ncomp; ++d) phif[d][f] = 0.0;
+                break;
+            case XCAL_BC_SYMMETRY:
+                if (!vector) {
+                    phif[0][f] = phi[0][c];
+                } else {
+                    V3 n = m.fnormal[f];
+                    V3 pc{phi[0][c], phi[1][c], phi[2][c]};
+                    V3 pn = dot(pc, n) * n;
+                    V3 r = pc - pn;
+                    phif[0][f] = r.x;
+                    phif[1][f] = r.y;
+                    phif[2][f] = r.z;
+                }
+                break;
+            case XCAL_BC_NEUMANN:
+                phif[0][f] = phi[0][c] + m.fdelta[f] * bc->value[0];
+                break;
+            case XCAL_BC_PERIODIC:
+                break;
+            case XCAL_BC_PERIODIC_PARENT: {
+                int pfID = bc->face_map[i];
+                int pc = m.owner[pfID];
+                int cID = m.owner[f];
+                V3 Pf = m.fcentre[f] - m.ccentre[cID];
+                V3 PN = (m.ccentre[pc] - bc->distance) - m.ccentre[cID];
+                V3 n = m.fnormal[f];
+                double wn = dot(Pf, n) / dot(PN, n);
+                double w = 1.0 - wn;
+                for (int d = 0; d < ncomp; ++d) {
+                    double v = w * phi[d][cID] + wn * phi[d][pc];
+                    phif[d][f] = v;
+                    phif[d][pfID] = v;
+                }
+                break;
+            }
+            default:
+                break;
+        }
+    }
+}
+
+// green_gauss! scalar -> vector (Calculate_1_green_gauss.jl:5-78)
+static void green_gauss(const Mesh& m, const std::vector<double>& phif, std::vector<double>* g) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < m.n_cells; ++i) {
+        V3 res{0, 0, 0};
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            int f = m.cell_faces[k];
+            V3 Sf = (m.farea[f] * m.fnormal[f]) * (double)m.cell_nsign[k];
+            res = res + phif[f] * Sf;
+        }
+        res = res / m.cvol[i];
+        g[0][i] = res.x;
+        g[1][i] = res.y;
+        g[2][i] = res.z;
+    }
+    for (int f = 0; f < m.n_bfaces; ++f) {
+        int c = m.owner[f];
+        V3 res = phif[f] * (m.farea[f] * m.fnormal[f]);
+        res = res / m.cvol[c];
+        g[0][c] = g[0][c] + res.x;
+        g[1][c] = g[1][c] + res.y;
+        g[2][c] = g[2][c] + res.z;
+    }
+}
+
+// green_gauss! vector -> tensor (Calculate_1_green_gauss.jl:82-173)
+static void green_gauss_tensor(const Mesh& m, const std::vector<double>* psif, std::vector<double>* g) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < m.n_cells; ++i) {
+        double res[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            int f = m.cell_faces[k];
+            V3 Sf = (m.farea[f] * m.fnormal[f]) * (double)m.cell_nsign[k];
+            double u[3] = {psif[0][f], psif[1][f], psif[2][f]};
+            double s[3] = {Sf.x, Sf.y, Sf.z};
+            for (int a = 0; a < 3; ++a)
+                for (int bb = 0; bb < 3; ++bb) res[3 * a + bb] = res[3 * a + bb] + u[a] * s[bb];
+        }
+        for (int q = 0; q < 9; ++q) g[q][i] = res[q] / m.cvol[i];
+    }
+    for (int f = 0; f < m.n_bfaces; ++f) {
+        int c = m.owner[f];
+        V3 Sf = m.farea[f] * m.fnormal[f];
+        double u[3] = {psif[0][f], psif[1][f], psif[2][f]};
+        double s[3] = {Sf.x, Sf.y, Sf.z};
+        for (int a = 0; a < 3; ++a)
+            for (int bb = 0; bb < 3; ++bb) {
+                double r = (u[a] * s[bb]) / m.cvol[c];
+                g[3 * a + bb][c] = g[3 * a + bb][c] + r;
+            }
+    }
+}
+
+// div! of a face scalar (Calculate_0_divergence.jl:99-170)
+static void divergence(const Mesh& m, const std::vector<double>& psif, std::vector<double>& out) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < m.n_cells; ++i) {
+        double red = 0.0;
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k)
+            red = red + psif[m.cell_faces[k]] * (double)m.cell_nsign[k];
+        out[i] = red / m.cvol[i];
+    }
+    for (int f = 0; f < m.n_bfaces; ++f) {
+        int c = m.owner[f];
+        out[c] = out[c] + psif[f] / m.cvol[c];
+    }
+}
+
+// flux! (Solvers_0_functions.jl:41-62)
+static void flux(const Mesh& m, const std::vector<double>* Uf, std::vector<double>& mdot) {
+#pragma omp parallel for schedule(static)
+    for (int f = 0; f < m.n_faces; ++f) {
+        V3 Sf = m.farea[f] * m.fnormal[f];
+        V3 u{Uf[0][f], Uf[1][f], Uf[2][f]};
+        mdot[f] = dot(u, Sf);
+    }
+}
+
+// correct_interpolation_periodic (Solvers_1_SIMPLE.jl:427-470)
+static void correct_interp_periodic(Case& C, std::vector<double>& phif, const std::vector<double>& phi) {
+    const Mesh& m = *C.m;
+    for (const BC& bc : C.bcU) {
+        if (bc.type != XCAL_BC_PERIODIC_PARENT) continue;
+        for (int i = 0; i < bc.count; ++i) {
+            int f = bc.start + i, pf = bc.face_map[i];
+            int c = m.owner[f], pc = m.owner[pf];
+            double w = m.fdelta[pf] / (m.fdelta[f] + m.fdelta[pf]);
+            double omw = 1.0 - w;
+            double v = w * phi[c] + omw * phi[pc];
+            phif[f] = v;
+            phif[pf] = v;
+        }
+    }
+}
+
+// grad!(grad p) (Calculate_0_gradient.jl:105-111)
+static void grad_p(Case& C) {
+    interpolate(*C.m, C.p, C.pf);
+    correct_boundaries(C, C.bcP, &C.pf, &C.p, false);
+    green_gauss(*C.m, C.pf, C.gradp);
+}
+
+// grad!(grad U) (Calculate_0_gradient.jl:113-119)
+static void grad_U(Case& C) {
+    for (int d = 0; d < 3; ++d) interpolate(*C.m, C.U[d], C.Uf[d]);
+    correct_boundaries(C, C.bcU, C.Uf, C.U, true);
+    green_gauss_tensor(*C.m, C.Uf, C.gradU);
+}
+
+// update_nueff! (Solvers_0_functions.jl:5-35)
+static void update_nueff(Case& C) {
+    for (int f = 0; f < C.nF; ++f)
+        C.nueff[f] = C.cfg.turbulence == XCAL_TURB_LAMINAR ? C.cfg.nu : C.cfg.nu + C.nutf[f];
+}
+
+// ---------------------------------------------------------------------------
+// SIMPLE / PISO building blocks
+// ---------------------------------------------------------------------------
+void initial_calculations(Case& C) {  // Solvers_1_SIMPLE.jl:150-156
+    for (int d = 0; d < 3; ++d) interpolate(*C.m, C.U[d], C.Uf[d]);
+    correct_boundaries(C, C.bcU, C.Uf, C.U, true);
+    flux(*C.m, C.Uf, C.mdotf);
+    grad_p(C);
+    update_nueff(C);
+    C.initialised = true;
+}
+
+void solve_equation_U(Case& C, double res[3], int iters[3]) {  // Solve_1_api.jl:233-266
+    discretise_U(C);
+    for (int d = 0; d < 3; ++d) {
+        update_equation(C);
+        apply_bcs(C, true, d);
+        relax_diagdom(C, d);
+        if (d == 0) update_precond(C.AU, C.cfg.U_solver.precond, C.PU);
+        res[d] = solve_system(C, true, d, iters ? &iters[d] : nullptr);
+    }
+}
+
+double solve_equation_p(Case& C, int* iters) {  // Solve_1_api.jl:214-231
+    discretise_p(C);
+    apply_bcs(C, false, 0);
+    set_reference(C);
+    update_precond(C.Ap, C.cfg.p_solver.precond, C.Pp);
+    return solve_system(C, false, 0, iters);
+}
+
+void pressure_predictor(Case& C, bool with_H) {  // Solvers_1_SIMPLE.jl:170-174
+    const Mesh& m = *C.m;
+    CSR& A = C.AU;
+    for (int i = 0; i < C.nC; ++i) C.rD[i] = m.cvol[i] / A.nzval[A.diag[i]];
+    interpolate(m, C.rD, C.rDf);
+    correct_interp_periodic(C, C.rDf, C.rD);
+    // remove_pressure_source! (Solvers_0_functions.jl:156-181), source sign -1
+    for (int i = 0; i < C.nC; ++i) {
+        double V = m.cvol[i];
+        for (int d = 0; d < 3; ++d) {
+            double calc = (-1.0 * C.gradp[d][i]) * V;
+            C.bU[d][i] = C.bU[d][i] - calc;
+        }
+    }
+    if (with_H) {
+        extern void H(Case & C);
+        H(C);
+    }
+}
+
+// H! (Solvers_0_functions.jl:184-249)
+void H(Case& C) {
+    CSR& A = C.AU;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < C.nC; ++i) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) {
+            int j = A.colval[k];
+            double val = A.nzval[k];
+            sx = sx + val * C.U[0][j];
+            sy = sy + val * C.U[1][j];
+            sz = sz + val * C.U[2][j];
+        }
+        double D = A.nzval[A.diag[i]];
+        sx = sx - D * C.U[0][i];
+        sy = sy - D * C.U[1][i];
+        sz = sz - D * C.U[2][i];
+        double rD = 1.0 / D;
+        C.Hv[0][i] = (C.bU[0][i] - sx) * rD;
+        C.Hv[1][i] = (C.bU[1][i] - sy) * rD;
+        C.Hv[2][i] = (C.bU[2][i] - sz) * rD;
+    }
+}
+
+void flux_divergence(Case& C) {  // Solvers_1_SIMPLE.jl:177-185
+    for (int d = 0; d < 3; ++d) interpolate(*C.m, C.Hv[d], C.Uf[d]);
+    correct_boundaries(C, C.bcU, C.Uf, C.Hv, true);
+    flux(*C.m, C.Uf, C.mdotf);
+    divergence(*C.m, C.mdotf, C.divHv);
+}
+
+void explicit_relaxation_p(Case& C, double alpha) {  // Solve_1_api.jl:317-335
+    for (int i = 0; i < C.nC; ++i) C.p[i] = C.prev[i] + alpha * (C.p[i] - C.prev[i]);
+}
+
+// correct_mass_flux! (Solvers_1_SIMPLE.jl:340-557) + correct_velocity!
+void correct(Case& C) {
+    const Mesh& m = *C.m;
+    CSR& A = C.Ap;
+    for (int f = C.nB; f < C.nF; ++f) {
+        int c1 = m.owner[f], c2 = m.neigh[f];
+        double aN = A.nzval[A.find(c1, c2)];
+        C.mdotf[f] = C.mdotf[f] + aN * (C.p[c2] - C.p[c1]);
+    }
+    for (const BC& bc : C.bcP) {
+        if (bc.type != XCAL_BC_PERIODIC_PARENT) continue;
+        for (int i = 0; i < bc.count; ++i) {
+            int f = bc.start + i, pf = bc.face_map[i];
+            int c1 = m.owner[f], c2 = m.owner[pf];
+            double aN = A.nzval[A.find(c1, c2)];
+            double corr = aN * (C.p[c2] - C.p[c1]);
+            C.mdotf[f] = C.mdotf[f] + corr;
+            C.mdotf[pf] = -C.mdotf[f];
+        }
+    }
+    for (int f = 0; f < C.nB; ++f) {
+        const BC* bc = find_bc(C.bcP, f);
+        if (!bc) continue;
+        int c = m.bcell[f];
+        if (bc->type == XCAL_BC_DIRICHLET || bc->type == XCAL_BC_DIRICHLET_FUNCTION) {
+            double fl = (C.rDf[f] * m.farea[f]) / m.fdelta[f];
+            double ap = -1.0 * (-fl);
+            double val = bc_value(*bc, false, 0, f - bc->start);
+            C.mdotf[f] = C.mdotf[f] + ap * (C.p[c] - val);
+        } else if (bc->type == XCAL_BC_NEUMANN) {
+            C.mdotf[f] = C.mdotf[f] - (C.rDf[f] * m.farea[f]) * bc->value[0];
+        }
+    }
+    // correct_velocity! (Solvers_0_functions.jl:126-151)
+    for (int i = 0; i < C.nC; ++i) {
+        double r = C.rD[i];
+        for (int d = 0; d < 3; ++d) C.U[d][i] = C.Hv[d][i] - C.gradp[d][i] * r;
+    }
+}
+
+void turbulence(Case& C) {
+    grad_U(C);  // RANS_laminar.jl:73-79, LES_Smagorinsky.jl:117
+    if (C.cfg.turbulence == XCAL_TURB_SMAGORINSKY) {
+        // LES_Smagorinsky.jl:122-131
+        for (int i = 0; i < C.nC; ++i) {
+            double G[3][3];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) G[a][b] = C.gradU[3 * a + b][i];
+            double S[3][3];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) S[a][b] = 0.5 * (G[a][b] + G[b][a]);
+            // (2.0*S) . S over column-major linear index
+            double acc = 0.0;
+            bool first = true;
+            for (int b = 0; b < 3; ++b)
+                for (int a = 0; a < 3; ++a) {
+                    double pr = (2.0 * S[a][b]) * S[a][b];
+                    acc = first ? pr : acc + pr;
+                    first = false;
+                }
+            double magS = std::sqrt(acc);
+            C.nut[i] = C.Delta[i] * magS;
+        }
+        interpolate(*C.m, C.nut, C.nutf);
+        correct_boundaries(C, C.bcNut, &C.nutf, &C.nut, false);
+    }
+    update_nueff(C);
+}
+
+double max_courant(Case& C) {  // Solvers_0_functions.jl:253-276
+    double mx = -std::numeric_limits<double>::infinity();
+    for (int i = 0; i < C.nC; ++i) {
+        V3 u{C.U[0][i], C.U[1][i], C.U[2][i]};
+        double umag = norm(u);
+        double V = C.m->cvol[i];
+        double dx = std::pow(V, 1.0 / 3.0);
+        double co = (umag * C.cfg.dt) / dx;
+        C.cellsCourant[i] = co;
+        mx = (i == 0) ? co : jl_max(mx, co);
+    }
+    return mx;
+}
+
+// one SIMPLE iteration (Solvers_1_SIMPLE.jl:164-240); returns converged
+bool simple_iteration(Case& C, double* res4) {
+    if (!C.initialised) initial_calculations(C);
+    C.iteration += 1;
+    double r3[3];
+    solve_equation_U(C, r3, nullptr);
+    pressure_predictor(C, true);
+    flux_divergence(C);
+    C.prev = C.p;
+    double rp = solve_equation_p(C, nullptr);
+    explicit_relaxation_p(C, C.cfg.p_solver.relax);
+    grad_p(C);
+    correct(C);
+    turbulence(C);
+    res4[0] = r3[0];
+    res4[1] = r3[1];
+    res4[2] = r3[2];
+    res4[3] = rp;
+    bool turb_conv = C.cfg.turbulence == XCAL_TURB_LAMINAR;
+    return r3[0] <= C.cfg.U_solver.convergence && r3[1] <= C.cfg.U_solver.convergence &&
+           r3[2] <= C.cfg.U_solver.convergence && rp <= C.cfg.p_solver.convergence && turb_conv;
+}
+
+// one PISO time step (Solvers_2_PISO.jl:108-187); returns the Courant number
+double piso_step(Case& C, double* res4) {
+    if (!C.initialised) initial_calculations(C);
+    C.iteration += 1;
+    C.time = C.time + C.cfg.dt;
+    double r3[3];
+    solve_equation_U(C, r3, nullptr);
+    pressure_predictor(C, false);
+    double rp = 0.0;
+    int inner = C.cfg.inner_loops;
+    for (int it = 1; it <= inner; ++it) {
+        H(C);
+        flux_divergence(C);
+        C.prev = C.p;
+        rp = solve_equation_p(C, nullptr);
+        explicit_relaxation_p(C, it == inner ? 1.0 : C.cfg.p_solver.relax);
+        grad_p(C);
+        correct(C);
+    }
+    turbulence(C);
+    double co = max_courant(C);
+    res4[0] = r3[0];
+    res4[1] = r3[1];
+    res4[2] = r3[2];
+    res4[3] = rp;
+    return co;
+}
+
+// expose the internal steps to the C API
+void o_discretise(Case& C, int eqn) {
+    if (eqn == XCAL_EQN_U)
+        discretise_U(C);
+    else
+        discretise_p(C);
+}
+void o_apply_bcs(Case& C, int eqn, int comp) {
+    if (eqn == XCAL_EQN_U) {
+        update_equation(C);
+        apply_bcs(C, true, comp);
+    } else {
+        apply_bcs(C, false, 0);
+    }
+}
+void o_relax(Case& C, int comp) { relax_diagdom(C, comp); }
+void o_set_reference(Case& C) { set_reference(C); }
+void o_update_precond(Case& C, int eqn) {
+    if (eqn == XCAL_EQN_U)
+        update_precond(C.AU, C.cfg.U_solver.precond, C.PU);
+    else
+        update_precond(C.Ap, C.cfg.p_solver.precond, C.Pp);
+}
+double o_solve_system(Case& C, int eqn, int comp, int* iters) {
+    return solve_system(C, eqn == XCAL_EQN_U, comp, iters);
+}
+void o_grad_p(Case& C) { grad_p(C); }
+void o_dilu(const CSR& A, std::vector<double>& D) { update_precond(A, XCAL_PRECOND_DILU, D); }
+void o_dilu_ldiv(const CSR& A, const std::vector<double>& D, std::vector<double>& x, const std::vector<double>& b) {
+    dilu_ldiv(A, D, x, b);
+}
+
+}  // namespace orc

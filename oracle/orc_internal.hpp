@@ -1,0 +1,84 @@
+// orc_internal.hpp -- data structures of the CPU oracle (test infrastructure).
+#pragma once
+#include "orc_common.hpp"
+#include "../include/xcal_b200.h"
+
+#include <string>
+#include <vector>
+
+namespace orc {
+
+// Mesh3 contract (src/Mesh/Mesh_0_types.jl), SoA, 0-based.
+struct Mesh {
+    int n_cells = 0, n_faces = 0, n_bfaces = 0, n_ifaces = 0;
+    std::vector<V3> points;
+    std::vector<int> owner, neigh;  // ownerCells[1], ownerCells[2]
+    std::vector<V3> fcentre, fnormal, fe;
+    std::vector<double> farea, fdelta, fweight;
+    std::vector<int> fn_off, face_nodes;
+    std::vector<V3> ccentre;
+    std::vector<double> cvol;
+    std::vector<int> cf_off, cell_faces, cell_nsign, cell_neigh;
+    std::vector<int> cn_off, cell_nodes;
+    std::vector<int> bcell;  // boundary_cellsID
+    std::vector<int> patch_start, patch_count;
+};
+
+Mesh* build_foam_mesh(int n_points, const double* points, int n_faces, const int* face_off,
+                      const int* face_nodes, const int* owner, int n_ifaces, const int* neighbour,
+                      int n_patches, const int* patch_nfaces);
+Mesh* mesh_from_desc(const xcal_mesh_desc* d);
+int construct_periodic(const Mesh* m, int patch1, int patch2, double tol, int* map1, int* map2,
+                       double* distance);
+
+// compressed sparse row matrix (SparseMatricesCSR semantics: sorted columns,
+// duplicates merged)
+struct CSR {
+    int n = 0;
+    std::vector<int> rowptr, colval;
+    std::vector<double> nzval;
+    std::vector<int> diag;  // diagonal_indices!
+    int find(int i, int j) const;  // spindex (0-based, -1 when absent)
+};
+
+struct BC {
+    int type = 0;
+    int patch = 0;
+    double value[3] = {0, 0, 0};
+    std::vector<double> face_values;  // DirichletFunction
+    std::vector<int> face_map;        // periodic
+    V3 distance{0, 0, 0};
+    int partner_patch = -1;
+    int start = 0, count = 0;  // IDs_range
+};
+
+struct Krylov {
+    // workspace vectors
+    std::vector<double> x, r, p, q, z, v, s, t, dx, c;
+    int niter = 0;
+};
+
+struct Case {
+    const Mesh* m = nullptr;
+    xcal_config cfg{};
+    std::vector<BC> bcU, bcP, bcNut;
+    int nC = 0, nF = 0, nB = 0;
+
+    // fields
+    std::vector<double> U[3], p, mdotf, nueff, gradp[3], gradU[9], rD, Hv[3], divHv, nut, nutf, Uf[3], pf,
+        rDf, Delta, prev, cellsCourant;
+    // equations
+    CSR AU, AU0, Ap;
+    std::vector<double> bU[3], bp;
+    // preconditioners
+    std::vector<double> PU, Pp;  // Jacobi storage (1/|A_ii|) or DILU D
+    Krylov kU, kp;
+    double time = 0.0;
+    bool initialised = false;
+    int iteration = 0;
+    std::string err;
+};
+
+Case* case_create(const Mesh* m, const xcal_config* cfg);
+
+}  // namespace orc

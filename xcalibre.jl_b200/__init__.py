@@ -1,0 +1,17 @@
+"""xcalibre.jl_b200 -- sm_100a implementation of XCALibre.jl's finite-volume
+hot path behind a C ABI (libxcal_b200.so), with a host-side mirror of the
+reference's user API for that path.
+
+The directory name contains a dot, so load it with ``importlib`` (see
+``__graft_entry__.load_package``); it is registered as ``xcalibre_b200``.
+"""
+from . import _abi, cases
+from .api import (B200Backend, Bicgstab, Case, Cg, Configuration, Context, DeviceMesh, DILU, Dirichlet,
+                  DirichletFunction, Empty, Energy, Euler, Extrapolated, Fluid, Gauss, Hardware, Incompressible,
+                  Isothermal, Jacobi, LES, LUST, Laminar, Linear, Neumann, Physics, RANS, Runtime, Schemes,
+                  Smagorinsky, SolverSetup, Steady, SteadyState, Symmetry, Transient, Upwind, Wall, Zerogradient,
+                  assign, build_config, construct_periodic, initialise_, launch_count, run_)
+from .foam import Mesh3, build_mesh3
+from .meshgen import PolyMesh, box_polymesh, cavity_polymesh, channel_polymesh, periodic_box_polymesh
+
+__all__ = [n for n in dir() if not n.startswith("_")] + ["_abi"]

@@ -1,0 +1,638 @@
+"""Host-side mirror of XCALibre.jl's user API for the SIMPLE/PISO hot path.
+
+The names, keyword arguments and semantics follow the reference:
+
+  Physics / Fluid{Incompressible} / RANS{Laminar} / LES{Smagorinsky}
+      src/ModelPhysics/0_type_definition.jl:196-229, 2_fluid_models.jl:49-71
+  Dirichlet, DirichletFunction, Wall, Zerogradient, Extrapolated, Empty,
+  Symmetry, Neumann, construct_periodic, assign
+      src/Discretise/boundary_conditions/*.jl, Discretise_4_assign_boundaries.jl:5
+  Schemes, SolverSetup, Runtime        src/Solve/Solve_1_api.jl:8-211
+  Hardware, Configuration              src/Simulate/Simulate_0_types.jl:32-74
+  run! -> run_(model, config; pref, ncorrectors, inner_loops)
+      src/Solvers/Solvers_3_solver_dispatch.jl:120,225
+
+Everything below the API goes through libxcal_b200.so (``Engine`` classes);
+Python only marshals arrays.  ``B200Backend`` is the backend type that
+selects this implementation (the reference's ``CUDABackend()`` slot).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Callable
+
+import numpy as np
+
+from . import _abi
+from ._lib import check, lib
+from .foam import Mesh3
+
+EPS64 = float(np.finfo(np.float64).eps)
+
+# ---------------------------------------------------------------------------
+# schemes, solvers, preconditioners (marker types)
+# ---------------------------------------------------------------------------
+
+
+class SteadyState: ...
+
+
+class Euler: ...
+
+
+class Linear: ...
+
+
+class Upwind: ...
+
+
+class LUST: ...
+
+
+class Gauss: ...
+
+
+class Cg: ...
+
+
+class Bicgstab: ...
+
+
+class Jacobi: ...
+
+
+class DILU: ...
+
+
+class Steady: ...
+
+
+class Transient: ...
+
+
+class Laminar: ...
+
+
+class Smagorinsky: ...
+
+
+class Incompressible: ...
+
+
+class Isothermal: ...
+
+
+def _inst(x):
+    return x() if isinstance(x, type) else x
+
+
+@dataclass
+class Schemes:
+    time: type = SteadyState
+    divergence: type = Linear
+    laplacian: type = Linear
+    gradient: type = Gauss
+    limiter: object = None
+
+
+@dataclass
+class SolverSetup:
+    solver: object
+    preconditioner: object
+    convergence: float
+    relax: float
+    float_type: str = "Float64"
+    smoother: object = None
+    limit: object = None
+    itmax: int = 1000
+    atol: float | None = None
+    rtol: float = 0.1
+
+    def __post_init__(self):
+        if self.atol is None:
+            self.atol = EPS64 ** 0.9  # (eps(float_type))^0.9 (Solve_1_api.jl:70)
+        if self.smoother is not None:
+            raise NotImplementedError("smoothers are outside the implemented path")
+
+
+@dataclass
+class Runtime:
+    iterations: int
+    write_interval: int
+    time_step: float
+    adaptive: object = None
+
+
+@dataclass
+class B200Backend:
+    """Backend selecting libxcal_b200 (one GPU).  ``precision`` is "fp64"
+    (plain path) or "mixed" (FP32 Krylov inner iterations)."""
+    device: int = 0
+    precision: str = "fp64"
+
+
+@dataclass
+class Hardware:
+    backend: object
+    workgroup: int = 32
+
+
+@dataclass
+class Configuration:
+    solvers: dict
+    schemes: dict
+    runtime: Runtime
+    hardware: Hardware
+    boundaries: dict
+    postprocess: object = None
+
+
+# ---------------------------------------------------------------------------
+# physics
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class Fluid:
+    kind: type
+    nu: float
+    rho: float = 1.0
+
+
+@dataclass
+class RANS:
+    model: type = Laminar
+
+
+@dataclass
+class LES:
+    model: type = Smagorinsky
+    C: float = 0.15
+
+
+@dataclass
+class Energy:
+    kind: type = Isothermal
+
+
+@dataclass
+class Momentum:
+    U: np.ndarray
+    p: np.ndarray
+
+
+class Physics:
+    def __init__(self, time, fluid: Fluid, turbulence, energy, domain: Mesh3):
+        self.time = _inst(time)
+        self.fluid = fluid
+        self.turbulence = turbulence
+        self.energy = energy
+        self.domain = domain
+        n = domain.n_cells
+        self.momentum = Momentum(U=np.zeros((3, n)), p=np.zeros(n))
+        self.nut = np.zeros(n)
+
+
+def initialise_(field: np.ndarray, value) -> None:
+    """initialise! (src/Fields/Fields_0_types.jl:381-401)."""
+    if field.ndim == 2:
+        v = np.asarray(value, dtype=np.float64)
+        if v.shape != (3,):
+            raise ValueError("Vectors should have 3 components")
+        field[:] = v[:, None]
+    else:
+        field[:] = float(value)
+
+
+# ---------------------------------------------------------------------------
+# boundary conditions
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class BC:
+    kind: int
+    name: str
+    value: object = 0.0
+    func: Callable | None = None
+    face_map: np.ndarray | None = None
+    distance: np.ndarray | None = None
+    partner: str | None = None
+
+
+def Dirichlet(name, value):
+    return BC(_abi.BC_DIRICHLET, name, value)
+
+
+def DirichletFunction(name, f):
+    """``f(coords, time, index)`` returns a 3-vector (vector fields) or a
+    number (scalar fields); it is evaluated on the host for every face."""
+    return BC(_abi.BC_DIRICHLET_FUNCTION, name, 0.0, func=f)
+
+
+def Wall(name, value=0.0):
+    return BC(_abi.BC_WALL, name, value)
+
+
+def Zerogradient(name):
+    return BC(_abi.BC_ZEROGRADIENT, name)
+
+
+def Extrapolated(name):
+    return BC(_abi.BC_EXTRAPOLATED, name)
+
+
+def Empty(name):
+    return BC(_abi.BC_EMPTY, name)
+
+
+def Symmetry(name):
+    return BC(_abi.BC_SYMMETRY, name)
+
+
+def Neumann(name, value):
+    return BC(_abi.BC_NEUMANN, name, value)
+
+
+def _pairwise_sum(a: np.ndarray) -> np.ndarray:
+    """Julia's `sum` over a vector (pairwise blocks of 1024, sequential leaves)."""
+    def rec(lo, hi):
+        if lo == hi:
+            return a[lo].copy()
+        if hi - lo < 1024:
+            v = a[lo] + a[lo + 1]
+            for i in range(lo + 2, hi + 1):
+                v = v + a[i]
+            return v
+        mid = lo + ((hi - lo) >> 1)
+        return rec(lo, mid) + rec(mid + 1, hi)
+    return rec(0, a.shape[0] - 1)
+
+
+def construct_periodic(mesh: Mesh3, backend, patch1: str, patch2: str, tol: float = 1e-7):
+    """construct_periodic (src/Discretise/boundary_conditions/periodic.jl:95-217):
+    match the faces of two conformal patches by translated centroids."""
+    r1, r2 = mesh.patch_range(patch1), mesh.patch_range(patch2)
+    if len(r1) != len(r2):
+        raise ValueError(f"Periodic mismatch: Patch {patch1} has {len(r1)} faces, but {patch2} has {len(r2)}")
+    c1 = mesh.face_centre[r1.start:r1.stop]
+    c2 = mesh.face_centre[r2.start:r2.stop]
+    nf = len(r1)
+    tr = _pairwise_sum(c2) / float(nf) - _pairwise_sum(c1) / float(nf)
+    targets = c1 + tr
+    # lexicographic extremes (minimum/maximum over SVectors)
+    order = np.lexsort((targets[:, 2], targets[:, 1], targets[:, 0]))
+    ext = targets[order[-1]] - targets[order[0]]
+    axis = int(np.argmax(ext))
+    p1 = np.argsort(targets[:, axis], kind="stable")
+    p2 = np.argsort(c2[:, axis], kind="stable")
+    ts, ss = targets[p1], c2[p2]
+    map1 = np.zeros(nf, dtype=np.int32)
+    map2 = np.zeros(nf, dtype=np.int32)
+    start = 0
+    sv = ss[:, axis]
+    for i in range(nf):
+        t = ts[i]
+        tv = t[axis]
+        while start < nf and sv[start] < tv - tol:
+            start += 1
+        stop = start
+        while stop < nf and sv[stop] - tv <= tol:
+            stop += 1
+        if stop == start:
+            raise ValueError(f"Periodic mismatch at Face {i}: no match found closer than tolerance {tol}")
+        d = ss[start:stop] - t
+        dist = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+        j = int(np.argmin(dist))
+        if not dist[j] < tol:
+            raise ValueError(f"Periodic mismatch at Face {i}: no match found closer than tolerance {tol}")
+        l1, l2 = p1[i], p2[start + j]
+        map1[l1] = r2.start + l2
+        map2[l2] = r1.start + l1
+    parent = BC(_abi.BC_PERIODIC_PARENT, patch1, 0.0, face_map=map1, distance=tr, partner=patch2)
+    shadow = BC(_abi.BC_PERIODIC, patch2, 0.0, face_map=map2, distance=tr, partner=patch1)
+    return parent, shadow
+
+
+def assign(region: Mesh3, **fields) -> dict:
+    """assign (src/Discretise/Discretise_4_assign_boundaries.jl:5-18)."""
+    out = {}
+    nb = len(region.patch_names)
+    for name, bcs in fields.items():
+        bcs = list(bcs)
+        for bc in bcs:
+            region.patch_index(bc.name)  # raises for unknown names
+        if len(bcs) != nb:
+            raise ValueError(f"Inconsistent number of boundaries assigned to field {name}")
+        out[name] = bcs
+    return out
+
+
+# ---------------------------------------------------------------------------
+# engine: handles of the C ABI
+# ---------------------------------------------------------------------------
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        code = lib().xcal_ctx_create(device, C.byref(h))
+        if code != 0:
+            raise RuntimeError(f"xcal_ctx_create failed ({code}); is a CUDA device visible?")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().xcal_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceMesh:
+    def __init__(self, ctx: Context, mesh: Mesh3):
+        self.ctx, self.mesh = ctx, mesh
+        desc, keep = _abi.mesh_desc(mesh)
+        h = C.c_void_p()
+        check(lib().xcal_mesh_upload(ctx.h, C.byref(desc), C.byref(h)), ctx.h)
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().xcal_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _bc_array(mesh: Mesh3, bcs, ncomp: int, keep: list):
+    arr = (_abi.BCDesc * max(1, len(bcs)))()
+    for k, bc in enumerate(bcs):
+        d = arr[k]
+        d.type = bc.kind
+        d.patch = mesh.patch_index(bc.name)
+        v = np.zeros(3)
+        if bc.kind not in (_abi.BC_DIRICHLET_FUNCTION, _abi.BC_PERIODIC, _abi.BC_PERIODIC_PARENT):
+            val = np.asarray(bc.value, dtype=np.float64).ravel()
+            v[: val.size] = val[:3]
+        for c in range(3):
+            d.value[c] = v[c]
+        if bc.kind == _abi.BC_DIRICHLET_FUNCTION:
+            vals = dirichlet_function_values(mesh, bc, ncomp, 0.0)
+            keep.append(vals)
+            d.face_values = _abi.ptr(vals, C.c_double)
+        if bc.face_map is not None:
+            fm = np.ascontiguousarray(bc.face_map, dtype=np.int32)
+            keep.append(fm)
+            d.face_map = _abi.ptr(fm, C.c_int32)
+            for c in range(3):
+                d.distance[c] = float(bc.distance[c])
+            d.partner_patch = mesh.patch_index(bc.partner)
+    return arr
+
+
+def dirichlet_function_values(mesh: Mesh3, bc: BC, ncomp: int, time) -> np.ndarray:
+    """Evaluate f(face.centre, time, i) for every face of the patch (i is the
+    1-based local face index, as in dirichletFunction.jl)."""
+    r = mesh.patch_range(bc.name)
+    vals = np.zeros((len(r), ncomp))
+    for i, f in enumerate(r):
+        v = bc.func(mesh.face_centre[f], time, i + 1)
+        vals[i] = np.asarray(v, dtype=np.float64).ravel()[:ncomp]
+    return np.ascontiguousarray(vals.ravel())
+
+
+_SCHEME_TIME = {SteadyState: _abi.TIME_STEADY, Euler: _abi.TIME_EULER}
+_SCHEME_DIV = {Linear: _abi.DIV_LINEAR, Upwind: _abi.DIV_UPWIND, LUST: _abi.DIV_LUST}
+
+
+def _kind(x):
+    return x if isinstance(x, type) else type(x)
+
+
+def _solver_desc(s: SolverSetup) -> _abi.SolverSetupDesc:
+    solver = {Cg: _abi.SOLVER_CG, Bicgstab: _abi.SOLVER_BICGSTAB}[_kind(s.solver)]
+    pre = {Jacobi: _abi.PRECOND_JACOBI, DILU: _abi.PRECOND_DILU, type(None): _abi.PRECOND_NONE}[_kind(s.preconditioner)]
+    return _abi.SolverSetupDesc(solver=solver, precond=pre, convergence=float(s.convergence),
+                                relax=float(s.relax), atol=float(s.atol), rtol=float(s.rtol), itmax=int(s.itmax))
+
+
+def build_config(model: Physics, config: Configuration, pref=None, inner_loops=None):
+    """Translate the Python API objects into an xcal_config (keep the second
+    return value alive while the config is in use)."""
+    mesh = model.domain
+    keep: list = []
+    transient = isinstance(model.time, Transient)
+    turb = model.turbulence
+    les = isinstance(turb, LES)
+    bnd = config.boundaries
+    bU = _bc_array(mesh, bnd["U"], 3, keep)
+    bP = _bc_array(mesh, bnd["p"], 1, keep)
+    nut_bcs = bnd.get("nut", []) if les else []
+    bN = _bc_array(mesh, nut_bcs, 1, keep)
+    keep += [bU, bP, bN]
+    sU, sP = config.schemes["U"], config.schemes["p"]
+    backend = config.hardware.backend
+    prec = _abi.PREC_MIXED if getattr(backend, "precision", "fp64") == "mixed" else _abi.PREC_FP64
+    if inner_loops is None:
+        inner_loops = 2 if transient else 0
+    cfg = _abi.ConfigDesc(
+        algorithm=_abi.ALGO_PISO if transient else _abi.ALGO_SIMPLE,
+        turbulence=_abi.TURB_SMAGORINSKY if les else _abi.TURB_LAMINAR,
+        nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if les else 0.0,
+        U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)]),
+        p_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sP.time)], divergence=_SCHEME_DIV[_kind(sP.divergence)]),
+        U_solver=_solver_desc(config.solvers["U"]), p_solver=_solver_desc(config.solvers["p"]),
+        iterations=int(config.runtime.iterations), dt=float(config.runtime.time_step),
+        has_pref=0 if pref is None else 1, pref=0.0 if pref is None else float(pref),
+        inner_loops=int(inner_loops), precision=prec,
+        n_bc_U=len(bnd["U"]), n_bc_p=len(bnd["p"]), n_bc_nut=len(nut_bcs),
+        bc_U=C.cast(bU, C.POINTER(_abi.BCDesc)), bc_p=C.cast(bP, C.POINTER(_abi.BCDesc)),
+        bc_nut=C.cast(bN, C.POINTER(_abi.BCDesc)))
+    return cfg, keep
+
+
+class Case:
+    """A solver case on the GPU (xcal_case)."""
+
+    def __init__(self, dmesh: DeviceMesh, cfg: _abi.ConfigDesc):
+        self.dmesh, self.ctx = dmesh, dmesh.ctx
+        self.mesh = dmesh.mesh
+        h = C.c_void_p()
+        check(lib().xcal_case_create(self.ctx.h, dmesh.h, C.byref(cfg), C.byref(h)), self.ctx.h)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().xcal_case_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, code):
+        check(code, self.ctx.h)
+
+    def _size(self, field):
+        nc, kind = _abi.FIELD_SHAPE[field]
+        per = self.mesh.n_cells if kind == "cell" else self.mesh.n_faces
+        return nc, per
+
+    def set_field(self, field: int, values) -> None:
+        nc, per = self._size(field)
+        a = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(nc * per))
+        self._chk(lib().xcal_case_set_field(self.h, field, _abi.ptr(a, C.c_double), a.size))
+
+    def get_field(self, field: int) -> np.ndarray:
+        nc, per = self._size(field)
+        a = np.empty(nc * per)
+        self._chk(lib().xcal_case_get_field(self.h, field, _abi.ptr(a, C.c_double), a.size))
+        return a.reshape(nc, per) if nc > 1 else a
+
+    def nnz(self, eqn: int) -> int:
+        n = C.c_int64()
+        self._chk(lib().xcal_case_nnz(self.h, eqn, C.byref(n)))
+        return n.value
+
+    def pattern(self, eqn: int):
+        nnz = self.nnz(eqn)
+        rp = np.empty(self.mesh.n_cells + 1, dtype=np.int32)
+        cv = np.empty(nnz, dtype=np.int32)
+        self._chk(lib().xcal_case_csr_pattern(self.h, eqn, _abi.ptr(rp, C.c_int32), _abi.ptr(cv, C.c_int32)))
+        return rp, cv
+
+    def system(self, eqn: int, component: int = 0):
+        nz = np.empty(self.nnz(eqn))
+        b = np.empty(self.mesh.n_cells)
+        self._chk(lib().xcal_case_get_system(self.h, eqn, component, _abi.ptr(nz, C.c_double),
+                                             _abi.ptr(b, C.c_double)))
+        return nz, b
+
+    def simple_iterate(self, n: int):
+        res = np.zeros((max(n, 1), 4))
+        done, conv = C.c_int32(), C.c_int32()
+        self._chk(lib().xcal_simple_iterate(self.h, n, _abi.ptr(res, C.c_double), C.byref(done), C.byref(conv)))
+        return res[: done.value], bool(conv.value)
+
+    def piso_step(self, n: int):
+        res = np.zeros((max(n, 1), 4))
+        co = np.zeros(max(n, 1))
+        done = C.c_int32()
+        self._chk(lib().xcal_piso_step(self.h, n, _abi.ptr(res, C.c_double), _abi.ptr(co, C.c_double),
+                                       C.byref(done)))
+        return res[: done.value], co[: done.value]
+
+    # fine-grained hooks
+    def initial_calculations(self):
+        self._chk(lib().xcal_initial_calculations(self.h))
+
+    def discretise(self, eqn):
+        self._chk(lib().xcal_discretise(self.h, eqn))
+
+    def apply_boundary_conditions(self, eqn, comp=0):
+        self._chk(lib().xcal_apply_boundary_conditions(self.h, eqn, comp))
+
+    def implicit_relaxation_diagdom(self, comp):
+        self._chk(lib().xcal_implicit_relaxation_diagdom(self.h, comp))
+
+    def set_reference(self):
+        self._chk(lib().xcal_set_reference(self.h))
+
+    def update_preconditioner(self, eqn):
+        self._chk(lib().xcal_update_preconditioner(self.h, eqn))
+
+    def solve_system(self, eqn, comp=0):
+        r, it = C.c_double(), C.c_int32()
+        self._chk(lib().xcal_solve_system(self.h, eqn, comp, C.byref(r), C.byref(it)))
+        return r.value, it.value
+
+    def solve_equation(self, eqn):
+        res = np.zeros(3)
+        self._chk(lib().xcal_solve_equation(self.h, eqn, _abi.ptr(res, C.c_double)))
+        return res if eqn == _abi.EQN_U else res[0]
+
+    def pressure_predictor(self):
+        self._chk(lib().xcal_pressure_predictor(self.h))
+
+    def flux_divergence(self):
+        self._chk(lib().xcal_flux_divergence(self.h))
+
+    def explicit_relaxation_p(self, alpha):
+        self._chk(lib().xcal_explicit_relaxation_p(self.h, float(alpha)))
+
+    def grad_p(self):
+        self._chk(lib().xcal_grad_p(self.h))
+
+    def correct(self):
+        self._chk(lib().xcal_correct(self.h))
+
+    def turbulence(self):
+        self._chk(lib().xcal_turbulence(self.h))
+
+    def max_courant(self):
+        c = C.c_double()
+        self._chk(lib().xcal_max_courant(self.h, C.byref(c)))
+        return c.value
+
+    def timings(self):
+        ms = np.zeros(6)
+        lib().xcal_get_timings(self.h, _abi.ptr(ms, C.c_double), 6)
+        return ms
+
+
+def launch_count() -> int:
+    n = C.c_int64()
+    lib().xcal_get_launch_count(None, C.byref(n))
+    return n.value
+
+
+# ---------------------------------------------------------------------------
+# run!
+# ---------------------------------------------------------------------------
+_CTX_CACHE: dict = {}
+
+
+def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0, inner_loops=None):
+    """run! (Solvers_3_solver_dispatch.jl:120,225): SIMPLE for Steady, PISO
+    for Transient.  Returns the residual histories (Ux, Uy, Uz, p) and writes
+    the final fields back into ``model.momentum``."""
+    if ncorrectors != 0:
+        raise NotImplementedError("non-orthogonal correctors are outside the implemented path")
+    backend = config.hardware.backend
+    if not isinstance(backend, B200Backend):
+        raise TypeError("Hardware.backend must be B200Backend() for this implementation")
+    dev = backend.device
+    if dev not in _CTX_CACHE:
+        _CTX_CACHE[dev] = Context(dev)
+    ctx = _CTX_CACHE[dev]
+    cfg, keep = build_config(model, config, pref, inner_loops)
+    dmesh = DeviceMesh(ctx, model.domain)
+    case = Case(dmesh, cfg)
+    try:
+        case.set_field(_abi.FIELD_U, model.momentum.U)
+        case.set_field(_abi.FIELD_P, model.momentum.p)
+        n = config.runtime.iterations
+        if isinstance(model.time, Transient):
+            res, _ = case.piso_step(n)
+        else:
+            res, _ = case.simple_iterate(n)
+        model.momentum.U[:] = case.get_field(_abi.FIELD_U)
+        model.momentum.p[:] = case.get_field(_abi.FIELD_P)
+        if isinstance(model.turbulence, LES):
+            model.nut[:] = case.get_field(_abi.FIELD_NUT)
+    finally:
+        case.close()
+        dmesh.close()
+    return {"Ux": res[:, 0], "Uy": res[:, 1], "Uz": res[:, 2], "p": res[:, 3]}

@@ -1,0 +1,102 @@
+"""The benchmark workloads, written with the reference-style API.
+
+* cavity_case        -- 2D lid-driven cavity (80x80x1, Re = 100), SIMPLE,
+                        Upwind, CG+Jacobi (p), BiCGSTAB+DILU (U), relax 0.7/0.3
+                        (after examples/2D_cavity.jl:30-83 with the stated solvers)
+* channel_case       -- 3D steady laminar channel 4x1x1, parabolic inlet
+                        (peak 1 m/s), zeroGradient outlet, no-slip walls,
+                        nu = 1e-3, LUST, SIMPLE
+* periodic_les_case  -- periodic cube, PISO + Smagorinsky (Cs = 0.17),
+                        Euler, Linear divergence, nu = 1e-4
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import api as A
+from .foam import Mesh3
+
+
+def _solvers(U_pre=A.DILU, p_pre=A.Jacobi, relax_U=0.7, relax_p=0.3, conv=1e-7, rtol_U=0.1, rtol_p=0.1):
+    return {
+        "U": A.SolverSetup(solver=A.Bicgstab(), preconditioner=U_pre(), convergence=conv, relax=relax_U,
+                           rtol=rtol_U),
+        "p": A.SolverSetup(solver=A.Cg(), preconditioner=p_pre(), convergence=conv, relax=relax_p, rtol=rtol_p),
+    }
+
+
+def cavity_case(mesh: Mesh3, iterations: int = 1000, precision: str = "fp64", device: int = 0):
+    nu = 0.01  # Re = 100 on the unit square with lid speed 1
+    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=nu), turbulence=A.RANS(A.Laminar),
+                      energy=A.Energy(A.Isothermal), domain=mesh)
+    BCs = A.assign(
+        region=mesh,
+        U=[A.Wall("lid", [1.0, 0.0, 0.0]), A.Wall("walls", [0.0, 0.0, 0.0]), A.Empty("frontAndBack")],
+        p=[A.Wall("lid"), A.Wall("walls"), A.Empty("frontAndBack")],
+    )
+    schemes = {"U": A.Schemes(divergence=A.Upwind), "p": A.Schemes()}
+    config = A.Configuration(solvers=_solvers(), schemes=schemes,
+                             runtime=A.Runtime(iterations=iterations, write_interval=-1, time_step=1.0),
+                             hardware=A.Hardware(backend=A.B200Backend(device=device, precision=precision)),
+                             boundaries=BCs)
+    A.initialise_(model.momentum.U, [0.0, 0.0, 0.0])
+    A.initialise_(model.momentum.p, 0.0)
+    return model, config
+
+
+def parabolic_inlet(coords, time, index):
+    """U_x = 16 y(1-y) z(1-z): peak 1 m/s at the centre of the unit section."""
+    y, z = coords[1], coords[2]
+    return [16.0 * y * (1.0 - y) * z * (1.0 - z), 0.0, 0.0]
+
+
+def channel_case(mesh: Mesh3, iterations: int = 500, precision: str = "fp64", device: int = 0,
+                 convergence: float = 1e-6):
+    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=1e-3), turbulence=A.RANS(A.Laminar),
+                      energy=A.Energy(A.Isothermal), domain=mesh)
+    BCs = A.assign(
+        region=mesh,
+        U=[A.DirichletFunction("inlet", parabolic_inlet), A.Zerogradient("outlet"), A.Wall("walls", [0.0, 0.0, 0.0])],
+        p=[A.Zerogradient("inlet"), A.Dirichlet("outlet", 0.0), A.Wall("walls")],
+    )
+    schemes = {"U": A.Schemes(divergence=A.LUST), "p": A.Schemes()}
+    config = A.Configuration(solvers=_solvers(conv=convergence), schemes=schemes,
+                             runtime=A.Runtime(iterations=iterations, write_interval=-1, time_step=1.0),
+                             hardware=A.Hardware(backend=A.B200Backend(device=device, precision=precision)),
+                             boundaries=BCs)
+    A.initialise_(model.momentum.U, [0.0, 0.0, 0.0])
+    A.initialise_(model.momentum.p, 0.0)
+    return model, config
+
+
+def taylor_green(mesh: Mesh3, rms: float = 1.0) -> np.ndarray:
+    """Divergence-free periodic field on [0, 2pi]^3 (deterministic)."""
+    x, y, z = mesh.cell_centre[:, 0], mesh.cell_centre[:, 1], mesh.cell_centre[:, 2]
+    U = np.stack([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z), np.zeros_like(x)])
+    cur = np.sqrt(np.mean(np.sum(U * U, axis=0)))
+    return U * (rms / cur)
+
+
+def periodic_les_case(mesh: Mesh3, steps: int = 200, dt: float | None = None, precision: str = "fp64",
+                      device: int = 0, U0: np.ndarray | None = None):
+    pairs = [A.construct_periodic(mesh, None, a, b) for a, b in (("xmin", "xmax"), ("ymin", "ymax"), ("zmin", "zmax"))]
+    per = [bc for pair in pairs for bc in pair]
+    model = A.Physics(time=A.Transient(), fluid=A.Fluid(A.Incompressible, nu=1e-4), turbulence=A.LES(A.Smagorinsky, C=0.17),
+                      energy=A.Energy(A.Isothermal), domain=mesh)
+    BCs = A.assign(region=mesh, U=per, p=per, nut=per)
+    schemes = {"U": A.Schemes(time=A.Euler, divergence=A.Linear), "p": A.Schemes(time=A.Euler)}
+    if U0 is None:
+        U0 = taylor_green(mesh)
+    if dt is None:
+        # dt from CFL = 0.5 with the Courant definition of max_courant_number!
+        umag = np.sqrt(np.sum(U0 * U0, axis=0))
+        dx = np.power(mesh.cell_volume, 1.0 / 3.0)
+        dt = 0.5 * float(np.min(dx / np.maximum(umag, 1e-30)))
+    solvers = _solvers(relax_U=1.0, relax_p=1.0, rtol_U=0.1, rtol_p=0.01)
+    config = A.Configuration(solvers=solvers, schemes=schemes,
+                             runtime=A.Runtime(iterations=steps, write_interval=-1, time_step=dt),
+                             hardware=A.Hardware(backend=A.B200Backend(device=device, precision=precision)),
+                             boundaries=BCs)
+    model.momentum.U[:] = U0
+    A.initialise_(model.momentum.p, 0.0)
+    return model, config

@@ -1,0 +1,286 @@
+// capi.cu -- extern "C" entry points of libxcal_b200.so (include/xcal_b200.h).
+// Every call catches library errors and turns them into a status code plus a
+// message retrievable with xcal_last_error; nothing aborts the process.
+#include <exception>
+#include <new>
+
+#include "case.hpp"
+
+namespace xcal {
+DevMesh* upload_mesh(const xcal_mesh_desc* d, cudaStream_t s);
+std::atomic<long long> g_launch_count{0};
+}
+using namespace xcal;
+
+static int set_error(xcal_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return code;
+}
+
+#define XCAL_GUARD(ctx, ...)                                                  \
+    try {                                                                     \
+        __VA_ARGS__;                                                          \
+        return XCAL_OK;                                                       \
+    } catch (const ::xcal::Error& e) {                                        \
+        return set_error(ctx, e.code, e.msg);                                 \
+    } catch (const std::bad_alloc&) {                                         \
+        return set_error(ctx, XCAL_ERR_OOM, "host allocation failed");        \
+    } catch (const std::exception& e) {                                       \
+        return set_error(ctx, XCAL_ERR_INVALID, e.what());                    \
+    }
+
+static xcal_ctx* case_ctx(const xcal_case* cs) { return cs && cs->c ? cs->c->ctx : nullptr; }
+
+static int select_device(xcal_ctx* ctx) {
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return set_error(ctx, XCAL_ERR_CUDA, cudaGetErrorString(e));
+    return XCAL_OK;
+}
+
+extern "C" {
+
+const char* xcal_version(void) { return "xcal_b200 0.1 (sm_100a, FP64 hot path)"; }
+
+int32_t xcal_ctx_create(int32_t device, xcal_ctx** out) {
+    if (!out) return XCAL_ERR_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return XCAL_ERR_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return XCAL_ERR_CUDA;
+    cudaFree(nullptr);  // create the context now
+    xcal_ctx* c = new (std::nothrow) xcal_ctx();
+    if (!c) return XCAL_ERR_OOM;
+    c->device = device;
+    *out = c;
+    return XCAL_OK;
+}
+
+int32_t xcal_ctx_destroy(xcal_ctx* ctx) {
+    delete ctx;
+    return XCAL_OK;
+}
+
+const char* xcal_last_error(const xcal_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+int32_t xcal_mesh_upload(xcal_ctx* ctx, const xcal_mesh_desc* desc, xcal_mesh** out) {
+    if (!ctx || !out) return XCAL_ERR_INVALID;
+    *out = nullptr;
+    if (int e = select_device(ctx)) return e;
+    XCAL_GUARD(ctx, {
+        std::unique_ptr<DevMesh> m(upload_mesh(desc, 0));
+        xcal_mesh* h = new xcal_mesh();
+        h->ctx = ctx;
+        h->m = std::move(m);
+        *out = h;
+    })
+}
+
+int32_t xcal_mesh_destroy(xcal_mesh* mesh) {
+    delete mesh;
+    return XCAL_OK;
+}
+
+int32_t xcal_case_create(xcal_ctx* ctx, const xcal_mesh* mesh, const xcal_config* cfg, xcal_case** out) {
+    if (!ctx || !mesh || !cfg || !out) return XCAL_ERR_INVALID;
+    *out = nullptr;
+    if (int e = select_device(ctx)) return e;
+    XCAL_GUARD(ctx, {
+        std::unique_ptr<Case> c(new Case(ctx, mesh->m.get(), cfg));
+        xcal_case* h = new xcal_case();
+        h->c = std::move(c);
+        *out = h;
+    })
+}
+
+int32_t xcal_case_destroy(xcal_case* cs) {
+    delete cs;
+    return XCAL_OK;
+}
+
+int32_t xcal_case_nnz(const xcal_case* cs, int32_t eqn, int64_t* nnz) {
+    if (!cs || !nnz || (eqn != XCAL_EQN_U && eqn != XCAL_EQN_P)) return XCAL_ERR_INVALID;
+    *nnz = eqn == XCAL_EQN_U ? cs->c->U.nnz : cs->c->P.nnz;
+    return XCAL_OK;
+}
+
+int32_t xcal_case_csr_pattern(const xcal_case* cs, int32_t eqn, int32_t* rowptr, int32_t* colval) {
+    if (!cs || !rowptr || !colval || (eqn != XCAL_EQN_U && eqn != XCAL_EQN_P)) return XCAL_ERR_INVALID;
+    const Equation& E = eqn == XCAL_EQN_U ? cs->c->U : cs->c->P;
+    std::memcpy(rowptr, E.rowptr.data(), E.rowptr.size() * sizeof(int32_t));
+    std::memcpy(colval, E.colval.data(), E.colval.size() * sizeof(int32_t));
+    return XCAL_OK;
+}
+
+int32_t xcal_case_get_system(const xcal_case* cs, int32_t eqn, int32_t component, double* nzval, double* b) {
+    if (!cs || (eqn != XCAL_EQN_U && eqn != XCAL_EQN_P)) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    XCAL_GUARD(c->ctx, {
+        const Equation& E = eqn == XCAL_EQN_U ? c->U : c->P;
+        if (eqn == XCAL_EQN_U && (component < -1 || component > 2)) fail(XCAL_ERR_INVALID, "component");
+        c->sync();
+        if (nzval) {
+            XCAL_CUDA(cudaMemcpy(nzval, E.nz.p, E.nnz * sizeof(double), cudaMemcpyDeviceToHost));
+            if (eqn == XCAL_EQN_U && component < 0) {
+                std::vector<double> d0(E.n);
+                XCAL_CUDA(cudaMemcpy(d0.data(), E.diag0.p, E.n * sizeof(double), cudaMemcpyDeviceToHost));
+                for (int i = 0; i < E.n; ++i) nzval[E.diag[i]] = d0[i];
+            }
+        }
+        if (b) {
+            int bc = eqn == XCAL_EQN_U ? (component < 0 ? 0 : component) : 0;
+            XCAL_CUDA(cudaMemcpy(b, E.b[bc].p, E.n * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+    })
+}
+
+static int field_io(xcal_case* cs, int32_t field, double* host, int64_t count, bool set) {
+    if (!cs || !host || field < 0 || field >= XCAL_FIELD_COUNT) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    XCAL_GUARD(c->ctx, {
+        int ncomp = field == XCAL_FIELD_U || field == XCAL_FIELD_GRADP || field == XCAL_FIELD_HV ||
+                            field == XCAL_FIELD_UF
+                        ? 3
+                        : (field == XCAL_FIELD_GRADU ? 9 : 1);
+        long per = 0;
+        c->field_comp(field, 0, per);
+        if (count != (int64_t)ncomp * per) fail(XCAL_ERR_INVALID, "field size mismatch");
+        c->sync();
+        for (int d = 0; d < ncomp; ++d) {
+            long n = 0;
+            double* p = c->field_comp(field, d, n);
+            if (set)
+                XCAL_CUDA(cudaMemcpy(p, host + (size_t)d * per, per * sizeof(double), cudaMemcpyHostToDevice));
+            else
+                XCAL_CUDA(cudaMemcpy(host + (size_t)d * per, p, per * sizeof(double), cudaMemcpyDeviceToHost));
+        }
+    })
+}
+
+int32_t xcal_case_set_field(xcal_case* cs, int32_t field, const double* host, int64_t count) {
+    return field_io(cs, field, const_cast<double*>(host), count, true);
+}
+
+int32_t xcal_case_get_field(const xcal_case* cs, int32_t field, double* host, int64_t count) {
+    return field_io(const_cast<xcal_case*>(cs), field, host, count, false);
+}
+
+int32_t xcal_case_set_bc_values(xcal_case* cs, int32_t eqn, int32_t bc_index, const double* values, int64_t count) {
+    if (!cs || !values) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    XCAL_GUARD(c->ctx, {
+        BCTable& T = eqn == XCAL_EQN_U ? c->bcU : c->bcP;
+        int ncomp = eqn == XCAL_EQN_U ? 3 : 1;
+        if (bc_index < 0 || bc_index >= (int)T.src.size()) fail(XCAL_ERR_INVALID, "bc_index");
+        const xcal_bc& bc = T.src[bc_index];
+        if (bc.type != XCAL_BC_DIRICHLET_FUNCTION) fail(XCAL_ERR_INVALID, "BC is not a DirichletFunction");
+        int start = c->mesh->patch_start[bc.patch], n = c->mesh->patch_count[bc.patch];
+        if (count != (int64_t)ncomp * n) fail(XCAL_ERR_INVALID, "value count mismatch");
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < ncomp; ++d) T.val[3 * (size_t)(start + i) + d] = values[(size_t)ncomp * i + d];
+        c->sync();
+        XCAL_CUDA(cudaMemcpy(T.d_val.p, T.val.data(), T.val.size() * sizeof(double), cudaMemcpyHostToDevice));
+    })
+}
+
+int32_t xcal_simple_iterate(xcal_case* cs, int32_t n_iter, double* res_hist, int32_t* n_done, int32_t* converged) {
+    if (!cs || n_iter < 0) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    if (n_done) *n_done = 0;
+    if (converged) *converged = 0;
+    XCAL_GUARD(c->ctx, {
+        for (int k = 0; k < n_iter; ++k) {
+            double r[4];
+            bool conv = c->simple_iteration(r);
+            if (res_hist)
+                for (int q = 0; q < 4; ++q) res_hist[4 * k + q] = r[q];
+            if (n_done) *n_done = k + 1;
+            if (conv) {
+                if (converged) *converged = 1;
+                break;
+            }
+        }
+    })
+}
+
+int32_t xcal_piso_step(xcal_case* cs, int32_t n_steps, double* res_hist, double* courant, int32_t* n_done) {
+    if (!cs || n_steps < 0) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    if (n_done) *n_done = 0;
+    XCAL_GUARD(c->ctx, {
+        for (int k = 0; k < n_steps; ++k) {
+            double r[4];
+            double co = c->piso_step(r);
+            if (res_hist)
+                for (int q = 0; q < 4; ++q) res_hist[4 * k + q] = r[q];
+            if (courant) courant[k] = co;
+            if (n_done) *n_done = k + 1;
+        }
+    })
+}
+
+#define XCAL_STEP(name, ...)                            \
+    int32_t name {                                      \
+        if (!cs) return XCAL_ERR_INVALID;               \
+        Case* c = cs->c.get();                          \
+        XCAL_GUARD(c->ctx, { __VA_ARGS__; c->sync(); }) \
+    }
+
+XCAL_STEP(xcal_initial_calculations(xcal_case* cs), c->initial_calculations())
+XCAL_STEP(xcal_discretise(xcal_case* cs, int32_t eqn), c->discretise(eqn))
+XCAL_STEP(xcal_apply_boundary_conditions(xcal_case* cs, int32_t eqn, int32_t component),
+          c->apply_bcs(eqn, component))
+XCAL_STEP(xcal_implicit_relaxation_diagdom(xcal_case* cs, int32_t component), c->relax_U(component))
+XCAL_STEP(xcal_set_reference(xcal_case* cs), c->set_reference())
+XCAL_STEP(xcal_update_preconditioner(xcal_case* cs, int32_t eqn), c->update_precond(eqn))
+XCAL_STEP(xcal_pressure_predictor(xcal_case* cs), c->pressure_predictor(true))
+XCAL_STEP(xcal_flux_divergence(xcal_case* cs), {
+    c->flux_divergence();
+    XCAL_CUDA(cudaMemcpyAsync(c->prev.p, c->p.p, c->mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+})
+XCAL_STEP(xcal_explicit_relaxation_p(xcal_case* cs, double alpha), c->explicit_relaxation_p(alpha))
+XCAL_STEP(xcal_grad_p(xcal_case* cs), c->grad_p())
+XCAL_STEP(xcal_correct(xcal_case* cs), c->correct())
+XCAL_STEP(xcal_turbulence(xcal_case* cs), c->turbulence())
+
+int32_t xcal_solve_system(xcal_case* cs, int32_t eqn, int32_t component, double* residual, int32_t* iterations) {
+    if (!cs) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    XCAL_GUARD(c->ctx, {
+        int it = 0;
+        double r = c->solve_system(eqn, eqn == XCAL_EQN_U ? component : 0, &it);
+        if (residual) *residual = r;
+        if (iterations) *iterations = it;
+    })
+}
+
+int32_t xcal_solve_equation(xcal_case* cs, int32_t eqn, double* res) {
+    if (!cs || !res) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    XCAL_GUARD(c->ctx, {
+        if (eqn == XCAL_EQN_U)
+            c->solve_equation_U(res);
+        else
+            res[0] = c->solve_equation_p();
+    })
+}
+
+int32_t xcal_max_courant(xcal_case* cs, double* courant) {
+    if (!cs || !courant) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    XCAL_GUARD(c->ctx, { *courant = c->max_courant(); })
+}
+
+int32_t xcal_get_timings(const xcal_case* cs, double* ms, int32_t n) {
+    if (!cs || !ms) return XCAL_ERR_INVALID;
+    int k = n < 6 ? n : 6;
+    for (int i = 0; i < k; ++i) ms[i] = cs->c->ms[i];
+    return k;
+}
+
+int32_t xcal_get_launch_count(const xcal_case* cs, int64_t* count) {
+    if (!cs || !count) return XCAL_ERR_INVALID;
+    *count = g_launch_count.load();
+    return XCAL_OK;
+}
+
+}  // extern "C"

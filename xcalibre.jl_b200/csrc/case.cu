@@ -1,0 +1,832 @@
+// case.cu -- host orchestration of the hot path (mesh upload, equation
+// patterns, BC tables, SIMPLE/PISO steps).  Host floating-point code is
+// compiled without contraction so precomputed geometry matches the reference
+// formulas bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "case.hpp"
+#include "kernels.hpp"
+
+namespace xcal {
+
+// ---------------------------------------------------------------------------
+// views
+// ---------------------------------------------------------------------------
+MeshView DevMesh::view() const {
+    MeshView v;
+    v.nC = nC;
+    v.nF = nF;
+    v.nB = nB;
+    v.owner = d_owner.p;
+    v.neigh = d_neigh.p;
+    v.area = d_area.p;
+    v.delta = d_delta.p;
+    v.weight = d_weight.p;
+    v.Sx = d_Sx.p;
+    v.Sy = d_Sy.p;
+    v.Sz = d_Sz.p;
+    v.nx = d_nx.p;
+    v.ny = d_ny.p;
+    v.nz = d_nz.p;
+    v.Efmag = d_Ef.p;
+    v.vol = d_vol.p;
+    v.cf_off = d_cf_off.p;
+    v.cf_face = d_cf_face.p;
+    v.cf_nb = d_cf_nb.p;
+    v.cf_sign = d_cf_sign.p;
+    v.bf_off = d_bf_off.p;
+    v.bf_face = d_bf_face.p;
+    v.bcell = d_bcell.p;
+    v.bcells = d_bcells.p;
+    v.n_bcells = (int)bcells.size();
+    return v;
+}
+
+CSRView Equation::view() const {
+    CSRView v;
+    v.n = n;
+    v.rowptr = d_rowptr.p;
+    v.colval = d_colval.p;
+    v.diag = d_diag.p;
+    v.trans = d_trans.p;
+    v.cf_slot = d_cf_slot.p;
+    v.fslot = d_fslot.p;
+    return v;
+}
+
+int Equation::find(int i, int j) const {
+    auto b = colval.begin() + rowptr[i], e = colval.begin() + rowptr[i + 1];
+    auto it = std::lower_bound(b, e, j);
+    return (it != e && *it == j) ? (int)(it - colval.begin()) : -1;
+}
+
+BCView BCTable::view() const {
+    BCView v;
+    v.type = d_type.p;
+    v.val = d_val.p;
+    v.peer_face = d_peer_face.p;
+    v.peer_cell = d_peer_cell.p;
+    v.pw = d_pw.p;
+    v.pwn = d_pwn.p;
+    v.pEf = d_pEf.p;
+    v.pDelta = d_pDelta.p;
+    v.pwdelta = d_pwdelta.p;
+    v.pNN = d_pNN.p;
+    v.pNP = d_pNP.p;
+    v.pPN = d_pPN.p;
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// mesh upload
+// ---------------------------------------------------------------------------
+DevMesh* upload_mesh(const xcal_mesh_desc* d, cudaStream_t s) {
+    if (!d || d->n_cells <= 0 || d->n_faces <= 0 || d->n_bfaces < 0 || d->n_bfaces > d->n_faces)
+        fail(XCAL_ERR_INVALID, "mesh: invalid sizes");
+    if (!d->face_owner || !d->face_neigh || !d->face_normal || !d->face_area || !d->face_delta ||
+        !d->face_weight || !d->face_e || !d->cell_volume || !d->cell_faces_offset || !d->cell_faces ||
+        !d->cell_nsign || !d->cell_neighbours || !d->boundary_cellsID || !d->cell_centre || !d->face_centre)
+        fail(XCAL_ERR_INVALID, "mesh: missing array");
+    auto m = std::make_unique<DevMesh>();
+    int nC = m->nC = d->n_cells, nF = m->nF = d->n_faces, nB = m->nB = d->n_bfaces;
+    int nI = m->nI = nF - nB;
+    m->owner.assign(d->face_owner, d->face_owner + nF);
+    m->neigh.assign(d->face_neigh, d->face_neigh + nF);
+    m->cf_off.assign(d->cell_faces_offset, d->cell_faces_offset + nC + 1);
+    if (m->cf_off[0] != 0 || m->cf_off[nC] != 2 * nI) fail(XCAL_ERR_INVALID, "mesh: cell_faces_offset mismatch");
+    for (int c = 0; c < nC; ++c)
+        if (m->cf_off[c + 1] < m->cf_off[c]) fail(XCAL_ERR_INVALID, "mesh: decreasing cell_faces_offset");
+    int nk = 2 * nI;
+    m->cf_face.assign(d->cell_faces, d->cell_faces + nk);
+    m->cf_nb.assign(d->cell_neighbours, d->cell_neighbours + nk);
+    m->cf_sign.resize(nk);
+    for (int k = 0; k < nk; ++k) {
+        int sgn = d->cell_nsign[k];
+        if ((sgn != 1 && sgn != -1) || m->cf_face[k] < nB || m->cf_face[k] >= nF || m->cf_nb[k] < 0 ||
+            m->cf_nb[k] >= nC)
+            fail(XCAL_ERR_INVALID, "mesh: invalid cell_faces entry");
+        m->cf_sign[k] = (signed char)sgn;
+    }
+    for (int f = 0; f < nF; ++f)
+        if (m->owner[f] < 0 || m->owner[f] >= nC || m->neigh[f] < 0 || m->neigh[f] >= nC)
+            fail(XCAL_ERR_INVALID, "mesh: face cell index out of range");
+    m->bcell.assign(d->boundary_cellsID, d->boundary_cellsID + nB);
+    m->patch_start.assign(d->patch_start, d->patch_start + d->n_patches);
+    m->patch_count.assign(d->patch_count, d->patch_count + d->n_patches);
+    // cell -> boundary faces (ascending face id)
+    std::vector<int> cnt(nC, 0);
+    for (int f = 0; f < nB; ++f) {
+        if (m->bcell[f] < 0 || m->bcell[f] >= nC) fail(XCAL_ERR_INVALID, "mesh: boundary_cellsID out of range");
+        cnt[m->bcell[f]]++;
+    }
+    m->bf_off.assign(nC + 1, 0);
+    for (int c = 0; c < nC; ++c) m->bf_off[c + 1] = m->bf_off[c] + cnt[c];
+    m->bf_face.resize(nB);
+    {
+        std::vector<int> cur(m->bf_off.begin(), m->bf_off.end() - 1);
+        for (int f = 0; f < nB; ++f) m->bf_face[cur[m->bcell[f]]++] = f;
+    }
+    for (int c = 0; c < nC; ++c)
+        if (cnt[c]) m->bcells.push_back(c);
+    // geometry
+    m->vol.assign(d->cell_volume, d->cell_volume + nC);
+    m->area.assign(d->face_area, d->face_area + nF);
+    m->delta.assign(d->face_delta, d->face_delta + nF);
+    std::vector<double> Sx(nF), Sy(nF), Sz(nF), Ef(nF);
+    m->nxh.resize(nF);
+    m->nyh.resize(nF);
+    m->nzh.resize(nF);
+    m->ex.resize(nF);
+    m->ey.resize(nF);
+    m->ez.resize(nF);
+    m->fcx.resize(nF);
+    m->fcy.resize(nF);
+    m->fcz.resize(nF);
+    for (int f = 0; f < nF; ++f) {
+        double a = d->face_area[f];
+        double nx = d->face_normal[3 * f], ny = d->face_normal[3 * f + 1], nz = d->face_normal[3 * f + 2];
+        double ex = d->face_e[3 * f], ey = d->face_e[3 * f + 1], ez = d->face_e[3 * f + 2];
+        m->nxh[f] = nx;
+        m->nyh[f] = ny;
+        m->nzh[f] = nz;
+        m->ex[f] = ex;
+        m->ey[f] = ey;
+        m->ez[f] = ez;
+        m->fcx[f] = d->face_centre[3 * f];
+        m->fcy[f] = d->face_centre[3 * f + 1];
+        m->fcz[f] = d->face_centre[3 * f + 2];
+        // Sf = area*normal (flux!, green_gauss!)
+        double sx = a * nx, sy = a * ny, sz = a * nz;
+        Sx[f] = sx;
+        Sy[f] = sy;
+        Sz[f] = sz;
+        // |E_f| with Sf = (ns*area)*normal and e' = ns*e; independent of the
+        // sign ns (Discretise_1_schemes.jl:77-93)
+        double ss = sx * sx + sy * sy + sz * sz;
+        double se = sx * ex + sy * ey + sz * ez;
+        double r = ss / se;
+        double efx = r * ex, efy = r * ey, efz = r * ez;
+        Ef[f] = std::sqrt(efx * efx + efy * efy + efz * efz);
+    }
+    m->ccx.resize(nC);
+    m->ccy.resize(nC);
+    m->ccz.resize(nC);
+    for (int c = 0; c < nC; ++c) {
+        m->ccx[c] = d->cell_centre[3 * c];
+        m->ccy[c] = d->cell_centre[3 * c + 1];
+        m->ccz[c] = d->cell_centre[3 * c + 2];
+    }
+    // device copies
+    m->d_owner.upload(m->owner, s);
+    m->d_neigh.upload(m->neigh, s);
+    m->d_cf_off.upload(m->cf_off, s);
+    m->d_cf_face.upload(m->cf_face, s);
+    m->d_cf_nb.upload(m->cf_nb, s);
+    m->d_cf_sign.upload(m->cf_sign, s);
+    m->d_bf_off.upload(m->bf_off, s);
+    m->d_bf_face.upload(m->bf_face, s);
+    m->d_bcell.upload(m->bcell, s);
+    m->d_bcells.upload(m->bcells, s);
+    m->d_area.upload(m->area, s);
+    m->d_delta.upload(m->delta, s);
+    m->d_weight.upload(d->face_weight, nF, s);
+    m->d_Sx.upload(Sx, s);
+    m->d_Sy.upload(Sy, s);
+    m->d_Sz.upload(Sz, s);
+    m->d_nx.upload(m->nxh, s);
+    m->d_ny.upload(m->nyh, s);
+    m->d_nz.upload(m->nzh, s);
+    m->d_Ef.upload(Ef, s);
+    m->d_vol.upload(m->vol, s);
+    XCAL_CUDA(cudaStreamSynchronize(s));
+    return m.release();
+}
+
+// ---------------------------------------------------------------------------
+// equation pattern (sparse_matrix_connectivity + extend_matrix + sparsecsr)
+// ---------------------------------------------------------------------------
+static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal_bc>& bcs, int nvec,
+                           bool need_dilu, cudaStream_t s) {
+    int n = E.n = m.nC;
+    std::vector<std::vector<int>> extra(n);
+    for (const xcal_bc& bc : bcs) {
+        if (bc.type != XCAL_BC_PERIODIC_PARENT) continue;
+        E.has_periodic = true;
+        int start = m.patch_start[bc.patch], count = m.patch_count[bc.patch];
+        for (int i = 0; i < count; ++i) {
+            int f1 = start + i, f2 = bc.face_map[i];
+            int c1 = m.owner[f1], c2 = m.owner[f2];
+            extra[c1].push_back(c2);
+            extra[c2].push_back(c1);
+        }
+    }
+    E.rowptr.assign(n + 1, 0);
+    E.colval.clear();
+    E.colval.reserve((size_t)n + m.cf_face.size());
+    std::vector<int> row;
+    for (int c = 0; c < n; ++c) {
+        row.clear();
+        row.push_back(c);
+        for (int k = m.cf_off[c]; k < m.cf_off[c + 1]; ++k) row.push_back(m.cf_nb[k]);
+        for (int j : extra[c]) row.push_back(j);
+        std::sort(row.begin(), row.end());
+        row.erase(std::unique(row.begin(), row.end()), row.end());
+        E.colval.insert(E.colval.end(), row.begin(), row.end());
+        E.rowptr[c + 1] = (int)E.colval.size();
+    }
+    E.nnz = (long)E.colval.size();
+    E.diag.resize(n);
+    for (int c = 0; c < n; ++c) E.diag[c] = E.find(c, c);
+    std::vector<int> trans(E.nnz), cf_slot(m.cf_face.size()), fslot(m.nI);
+    for (int i = 0; i < n; ++i)
+        for (int e = E.rowptr[i]; e < E.rowptr[i + 1]; ++e) trans[e] = E.find(E.colval[e], i);
+    for (int c = 0; c < n; ++c)
+        for (int k = m.cf_off[c]; k < m.cf_off[c + 1]; ++k) cf_slot[k] = E.find(c, m.cf_nb[k]);
+    for (int f = m.nB; f < m.nF; ++f) fslot[f - m.nB] = E.find(m.owner[f], m.neigh[f]);
+    E.d_rowptr.upload(E.rowptr, s);
+    E.d_colval.upload(E.colval, s);
+    E.d_diag.upload(E.diag, s);
+    E.d_trans.upload(trans, s);
+    E.d_cf_slot.upload(cf_slot, s);
+    E.d_fslot.upload(fslot, s);
+    E.nz.alloc(E.nnz);
+    E.nz.zero(s);
+    if (E.has_periodic) {
+        E.nz0.alloc(E.nnz);
+        E.nz0.zero(s);
+    }
+    E.diag0.alloc(n);
+    E.diag0.zero(s);
+    E.P.alloc(n);
+    E.P.zero(s);
+    for (int d = 0; d < nvec; ++d) {
+        E.b[d].alloc(n);
+        E.b[d].zero(s);
+    }
+    if (need_dilu) {
+        // dependency levels of the lower (ascending) and upper (descending)
+        // triangular sweeps in the ORIGINAL numbering
+        std::vector<int> lvl(n, 0);
+        int maxl = 0;
+        for (int i = 0; i < n; ++i) {
+            int l = 0;
+            for (int e = E.rowptr[i]; e < E.diag[i]; ++e) l = std::max(l, lvl[E.colval[e]] + 1);
+            lvl[i] = l;
+            maxl = std::max(maxl, l);
+        }
+        std::vector<int> rows(n);
+        E.lower_off.assign(maxl + 2, 0);
+        for (int i = 0; i < n; ++i) E.lower_off[lvl[i] + 1]++;
+        for (int l = 0; l <= maxl; ++l) E.lower_off[l + 1] += E.lower_off[l];
+        {
+            std::vector<int> cur(E.lower_off.begin(), E.lower_off.end() - 1);
+            for (int i = 0; i < n; ++i) rows[cur[lvl[i]]++] = i;
+        }
+        E.d_lower_rows.upload(rows, s);
+        std::fill(lvl.begin(), lvl.end(), 0);
+        maxl = 0;
+        for (int i = n - 1; i >= 0; --i) {
+            int l = 0;
+            for (int e = E.diag[i] + 1; e < E.rowptr[i + 1]; ++e) l = std::max(l, lvl[E.colval[e]] + 1);
+            lvl[i] = l;
+            maxl = std::max(maxl, l);
+        }
+        E.upper_off.assign(maxl + 2, 0);
+        for (int i = 0; i < n; ++i) E.upper_off[lvl[i] + 1]++;
+        for (int l = 0; l <= maxl; ++l) E.upper_off[l + 1] += E.upper_off[l];
+        {
+            std::vector<int> cur(E.upper_off.begin(), E.upper_off.end() - 1);
+            for (int i = 0; i < n; ++i) rows[cur[lvl[i]]++] = i;
+        }
+        E.d_upper_rows.upload(rows, s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// BC tables
+// ---------------------------------------------------------------------------
+static void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int nbc, int ncomp, const Equation* E,
+                           cudaStream_t s) {
+    int nB = m.nB;
+    T.src.assign(bcs, bcs + nbc);
+    T.type.assign(nB, 0);
+    T.val.assign(3 * (size_t)nB, 0.0);
+    std::vector<int> peer_face(nB, -1), peer_cell(nB, -1), pNN(nB, -1), pNP(nB, -1), pPN(nB, -1);
+    std::vector<double> pw(nB, 0.0), pwn(nB, 0.0), pEf(nB, 0.0), pDelta(nB, 0.0), pwdelta(nB, 0.0);
+    int np = (int)m.patch_start.size();
+    for (int b = 0; b < nbc; ++b) {
+        const xcal_bc& bc = bcs[b];
+        if (bc.patch < 0 || bc.patch >= np) fail(XCAL_ERR_INVALID, "bc: patch index out of range");
+        if (bc.type < XCAL_BC_DIRICHLET || bc.type > XCAL_BC_PERIODIC_PARENT)
+            fail(XCAL_ERR_INVALID, "bc: unknown type");
+        if (ncomp == 3 && bc.type == XCAL_BC_NEUMANN)
+            fail(XCAL_ERR_UNSUPPORTED, "Neumann boundary condition for vector fields is not implemented");
+        int start = m.patch_start[bc.patch], count = m.patch_count[bc.patch];
+        for (int i = 0; i < count; ++i) {
+            int f = start + i;
+            if (T.type[f] != 0) continue;  // first BC listed for a face wins
+            T.type[f] = (signed char)bc.type;
+            for (int c = 0; c < 3; ++c) {
+                double v = bc.value[c];
+                if (bc.type == XCAL_BC_DIRICHLET_FUNCTION) {
+                    if (!bc.face_values) fail(XCAL_ERR_INVALID, "DirichletFunction without face values");
+                    v = c < ncomp ? bc.face_values[(size_t)ncomp * i + c] : 0.0;
+                }
+                T.val[3 * (size_t)f + c] = v;
+            }
+            if (bc.type == XCAL_BC_PERIODIC || bc.type == XCAL_BC_PERIODIC_PARENT) {
+                if (!bc.face_map) fail(XCAL_ERR_INVALID, "periodic BC without face_map");
+                int pf = bc.face_map[i];
+                if (pf < 0 || pf >= nB) fail(XCAL_ERR_INVALID, "periodic face_map out of range");
+                T.has_periodic = true;
+                peer_face[f] = pf;
+                int c1 = m.owner[f], c2 = m.owner[pf];
+                peer_cell[f] = c2;
+                if (bc.type == XCAL_BC_PERIODIC_PARENT) {
+                    double dx = bc.distance[0], dy = bc.distance[1], dz = bc.distance[2];
+                    // periodic.jl:282-296, 336-346; periodic_interpolation.jl:58-66
+                    double C1x = m.ccx[c1], C1y = m.ccy[c1], C1z = m.ccz[c1];
+                    double C2x = m.ccx[c2] - dx, C2y = m.ccy[c2] - dy, C2z = m.ccz[c2] - dz;
+                    double Pfx = m.fcx[f] - C1x, Pfy = m.fcy[f] - C1y, Pfz = m.fcz[f] - C1z;
+                    double PNx = C2x - C1x, PNy = C2y - C1y, PNz = C2z - C1z;
+                    double nx = m.nxh[f], ny = m.nyh[f], nz = m.nzh[f];
+                    double wn = (Pfx * nx + Pfy * ny + Pfz * nz) / (PNx * nx + PNy * ny + PNz * nz);
+                    pwn[f] = wn;
+                    pw[f] = 1.0 - wn;
+                    pDelta[f] = std::sqrt(PNx * PNx + PNy * PNy + PNz * PNz);
+                    double a = m.area[f];
+                    double sx = a * nx, sy = a * ny, sz = a * nz;
+                    double ss = sx * sx + sy * sy + sz * sz;
+                    double se = sx * m.ex[f] + sy * m.ey[f] + sz * m.ez[f];
+                    double r = ss / se;
+                    double efx = r * m.ex[f], efy = r * m.ey[f], efz = r * m.ez[f];
+                    pEf[f] = std::sqrt(efx * efx + efy * efy + efz * efz);
+                    pwdelta[f] = m.delta[pf] / (m.delta[f] + m.delta[pf]);  // Solvers_1_SIMPLE.jl:463
+                    if (E) {
+                        pNN[f] = E->find(c2, c2);
+                        pNP[f] = E->find(c2, c1);
+                        pPN[f] = E->find(c1, c2);
+                    }
+                }
+            }
+        }
+    }
+    T.d_type.upload(T.type, s);
+    T.d_val.upload(T.val, s);
+    T.d_peer_face.upload(peer_face, s);
+    T.d_peer_cell.upload(peer_cell, s);
+    T.d_pw.upload(pw, s);
+    T.d_pwn.upload(pwn, s);
+    T.d_pEf.upload(pEf, s);
+    T.d_pDelta.upload(pDelta, s);
+    T.d_pwdelta.upload(pwdelta, s);
+    T.d_pNN.upload(pNN, s);
+    T.d_pNP.upload(pNP, s);
+    T.d_pPN.upload(pPN, s);
+}
+
+// ---------------------------------------------------------------------------
+// case
+// ---------------------------------------------------------------------------
+Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(m), cfg(*cf) {
+    if (cfg.U_solver.relax <= 0.0 || cfg.p_solver.relax <= 0.0) fail(XCAL_ERR_INVALID, "relax must be > 0");
+    if (cfg.algorithm == XCAL_ALGO_PISO && cfg.dt <= 0.0) fail(XCAL_ERR_INVALID, "PISO needs dt > 0");
+    if (cfg.precision != XCAL_PREC_FP64 && cfg.precision != XCAL_PREC_MIXED)
+        fail(XCAL_ERR_INVALID, "unknown precision mode");
+    for (auto* ss : {&cfg.U_solver, &cfg.p_solver}) {
+        if (ss->solver != XCAL_SOLVER_CG && ss->solver != XCAL_SOLVER_BICGSTAB)
+            fail(XCAL_ERR_UNSUPPORTED, "solver must be Cg or Bicgstab");
+        if (ss->precond < XCAL_PRECOND_NONE || ss->precond > XCAL_PRECOND_DILU)
+            fail(XCAL_ERR_UNSUPPORTED, "unknown preconditioner");
+    }
+    XCAL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    for (auto& e : ev) XCAL_CUDA(cudaEventCreate(&e));
+    XCAL_CUDA(cudaMallocHost(&h_S, 2 * sizeof(KScalars)));
+    XCAL_CUDA(cudaMallocHost(&h_res, 8 * sizeof(double)));
+    int nC = m->nC, nF = m->nF;
+    std::vector<xcal_bc> bU(cfg.bc_U, cfg.bc_U + cfg.n_bc_U), bP(cfg.bc_p, cfg.bc_p + cfg.n_bc_p);
+    build_equation(U, *m, bU, 3, cfg.U_solver.precond == XCAL_PRECOND_DILU, stream);
+    build_equation(P, *m, bP, 1, cfg.p_solver.precond == XCAL_PRECOND_DILU, stream);
+    if (U.has_periodic) fail(XCAL_ERR_UNSUPPORTED, "periodic boundaries on U are not enabled in this build");
+    build_bc_table(bcU, *m, cfg.bc_U, cfg.n_bc_U, 3, &U, stream);
+    build_bc_table(bcP, *m, cfg.bc_p, cfg.n_bc_p, 1, &P, stream);
+    build_bc_table(bcNut, *m, cfg.bc_nut, cfg.n_bc_nut, 1, nullptr, stream);
+    cfg.bc_U = cfg.bc_p = cfg.bc_nut = nullptr;  // not retained
+    for (int d = 0; d < 3; ++d) {
+        Uc[d].alloc(nC);
+        gradp[d].alloc(nC);
+        Hv[d].alloc(nC);
+        Uf[d].alloc(nF);
+    }
+    for (int d = 0; d < 9; ++d) gradU[d].alloc(nC);
+    for (DBuf<double>* b : {&p, &rD, &divHv, &nut, &Delta, &prev, &courant, &dx13}) b->alloc(nC);
+    for (DBuf<double>* b : {&mdot, &nueff, &nutf, &pf, &rDf}) b->alloc(nF);
+    for (int d = 0; d < 3; ++d) {
+        Uc[d].zero(stream);
+        gradp[d].zero(stream);
+        Hv[d].zero(stream);
+        Uf[d].zero(stream);
+    }
+    for (int d = 0; d < 9; ++d) gradU[d].zero(stream);
+    for (DBuf<double>* b : {&p, &rD, &divHv, &nut, &Delta, &prev, &courant, &mdot, &nueff, &nutf, &pf})
+        b->zero(stream);
+    launch_fill(stream, rDf.p, 1.0, nF);  // initialise!(rDf, 1.0) (Solvers_1_SIMPLE.jl:61)
+    // Krylov workspace
+    int T = (nC + 2047) / 2048;
+    for (DBuf<double>* b : {&ws.x, &ws.dx, &ws.r, &ws.z, &ws.p, &ws.q, &ws.v, &ws.s, &ws.t}) {
+        b->alloc(nC);
+        b->zero(stream);
+    }
+    ws.part0.alloc(T);
+    ws.part1.alloc(T);
+    ws.S.alloc(2);
+    ws.S.zero(stream);
+    resbuf.alloc(8);
+    resbuf.zero(stream);
+    cmax.alloc(T);
+    // host-side per-cell constants: V^(1/3) (Courant) and the LES filter
+    std::vector<double> h(nC);
+    for (int i = 0; i < nC; ++i) h[i] = std::pow(m->vol[i], 1.0 / 3.0);
+    XCAL_CUDA(cudaMemcpyAsync(dx13.p, h.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (cfg.turbulence == XCAL_TURB_SMAGORINSKY) {
+        // LES_Smagorinsky.jl:84-101 + LES_functions.jl:1-55 (delta! with delta_scaling)
+        double distance = 1.0, power = 1.0 / 3.0;
+        for (const xcal_bc& bc : bcU.src)
+            if (bc.type == XCAL_BC_EMPTY) {
+                double pmin[3] = {0, 0, 0}, pmax[3] = {0, 0, 0};
+                for (int f = 0; f < m->nB; ++f) {
+                    double c3[3] = {m->fcx[f], m->fcy[f], m->fcz[f]};
+                    for (int k = 0; k < 3; ++k) {
+                        pmin[k] = std::min(pmin[k], c3[k]);
+                        pmax[k] = std::max(pmax[k], c3[k]);
+                    }
+                }
+                int f0 = m->patch_start[bc.patch];
+                double n3[3] = {m->nxh[f0], m->nyh[f0], m->nzh[f0]};
+                double d1 = std::fabs(pmin[0] * n3[0] + pmin[1] * n3[1] + pmin[2] * n3[2]);
+                double d2 = std::fabs(pmax[0] * n3[0] + pmax[1] * n3[1] + pmax[2] * n3[2]);
+                distance = d1 + d2;
+                power = 0.5;
+                break;
+            }
+        for (int i = 0; i < nC; ++i) {
+            double dd = std::pow(m->vol[i] / distance, power);
+            double dc = dd * cfg.smagorinsky_C;
+            h[i] = dc * dc;
+        }
+        XCAL_CUDA(cudaMemcpyAsync(Delta.p, h.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream));
+    }
+    XCAL_CUDA(cudaStreamSynchronize(stream));
+}
+
+Case::~Case() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (h_S) cudaFreeHost(h_S);
+    if (h_res) cudaFreeHost(h_res);
+    if (stream && own_stream) cudaStreamDestroy(stream);
+}
+
+void Case::sync() { XCAL_CUDA(cudaStreamSynchronize(stream)); }
+
+double* Case::field_comp(int field, int comp, long& count) {
+    count = mesh->nC;
+    switch (field) {
+        case XCAL_FIELD_U: return Uc[comp].p;
+        case XCAL_FIELD_P: return p.p;
+        case XCAL_FIELD_MDOTF: count = mesh->nF; return mdot.p;
+        case XCAL_FIELD_NUEFF: count = mesh->nF; return nueff.p;
+        case XCAL_FIELD_GRADP: return gradp[comp].p;
+        case XCAL_FIELD_GRADU: return gradU[comp].p;
+        case XCAL_FIELD_RD: return rD.p;
+        case XCAL_FIELD_HV: return Hv[comp].p;
+        case XCAL_FIELD_DIVHV: return divHv.p;
+        case XCAL_FIELD_NUT: return nut.p;
+        case XCAL_FIELD_NUTF: count = mesh->nF; return nutf.p;
+        case XCAL_FIELD_UF: count = mesh->nF; return Uf[comp].p;
+        case XCAL_FIELD_PF: count = mesh->nF; return pf.p;
+        case XCAL_FIELD_RDF: count = mesh->nF; return rDf.p;
+        case XCAL_FIELD_DELTA: return Delta.p;
+        default: return nullptr;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// steps
+// ---------------------------------------------------------------------------
+void Case::initial_calculations() {  // Solvers_1_SIMPLE.jl:150-156
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    double* Ufp[3] = {Uf[0].p, Uf[1].p, Uf[2].p};
+    launch_interp_U(stream, mv(), bcU.view(), Ucp, Ufp, mdot.p);
+    grad_p();
+    if (cfg.turbulence == XCAL_TURB_LAMINAR)
+        launch_fill(stream, nueff.p, cfg.nu, mesh->nF);
+    else
+        launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
+    initialised = true;
+}
+
+void Case::discretise(int eqn) {
+    if (eqn == XCAL_EQN_U) {
+        const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+        const double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
+        double* bp[3] = {U.b[0].p, U.b[1].p, U.b[2].p};
+        launch_assemble_U(stream, mv(), U.view(), mdot.p, nueff.p, Ucp, gp, U.nz.p, U.diag0.p, bp,
+                          cfg.U_schemes.time, cfg.U_schemes.divergence, cfg.dt);
+    } else {
+        launch_assemble_p(stream, mv(), P.view(), rDf.p, divHv.p, P.nz.p, P.b[0].p);
+    }
+}
+
+// update_equation! + apply_boundary_conditions! (+ relaxation for U, fused)
+void Case::apply_bcs(int eqn, int comp) {
+    if (eqn == XCAL_EQN_U) {
+        const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+        launch_bc_relax_U(stream, mv(), U.view(), bcU.view(), comp, cfg.U_schemes.divergence, U.nz.p, U.diag0.p,
+                          U.b[comp].p, mdot.p, nueff.p, Ucp, cfg.U_solver.relax, BCR_DIAG0 | BCR_BC);
+    } else {
+        launch_bc_p(stream, mv(), P.view(), bcP.view(), P.nz.p, P.b[0].p, rDf.p, p.p);
+    }
+}
+
+void Case::relax_U(int comp) {
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    launch_bc_relax_U(stream, mv(), U.view(), bcU.view(), comp, cfg.U_schemes.divergence, U.nz.p, U.diag0.p,
+                      U.b[comp].p, mdot.p, nueff.p, Ucp, cfg.U_solver.relax, BCR_RELAX);
+}
+
+void Case::bc_relax_U(int comp) {
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    launch_bc_relax_U(stream, mv(), U.view(), bcU.view(), comp, cfg.U_schemes.divergence, U.nz.p, U.diag0.p,
+                      U.b[comp].p, mdot.p, nueff.p, Ucp, cfg.U_solver.relax, BCR_DIAG0 | BCR_BC | BCR_RELAX);
+}
+
+void Case::set_reference() {
+    if (cfg.has_pref) launch_set_reference(stream, P.view(), P.nz.p, P.b[0].p, cfg.pref);
+}
+
+void Case::update_precond(int eqn) {
+    Equation& E = eqn == XCAL_EQN_U ? U : P;
+    int pt = eqn == XCAL_EQN_U ? cfg.U_solver.precond : cfg.p_solver.precond;
+    if (pt == XCAL_PRECOND_JACOBI) {
+        kr_jacobi_update(stream, E.view(), E.nz.p, E.P.p);
+    } else if (pt == XCAL_PRECOND_DILU) {
+        for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
+            kr_dilu_D(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], E.view(),
+                      E.nz.p, E.P.p);
+    }
+}
+
+void Case::dilu_ldiv(Equation& E, const double* b, double* out, const KScalars* S) {
+    CSRView A = E.view();
+    for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
+        kr_dilu_fwd(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], A, E.nz.p,
+                    E.P.p, b, out, S);
+    for (size_t l = 0; l + 1 < E.upper_off.size(); ++l)
+        kr_dilu_bwd(stream, E.d_upper_rows.p + E.upper_off[l], E.upper_off[l + 1] - E.upper_off[l], A, E.nz.p,
+                    E.P.p, out, S);
+}
+
+void Case::apply_M(Equation& E, int ptype, const double* in, double* out, const KScalars* S) {
+    if (ptype == XCAL_PRECOND_JACOBI)
+        kr_jacobi_apply(stream, E.n, E.P.p, in, out, S);
+    else if (ptype == XCAL_PRECOND_DILU)
+        dilu_ldiv(E, in, out, S);
+    else
+        kr_copy(stream, E.n, in, out, S);
+}
+
+// solve_system! (Solve_1_api.jl:268-307)
+double Case::solve_system(int eqn, int comp, int* iters) {
+    bool isU = eqn == XCAL_EQN_U;
+    Equation& E = isU ? U : P;
+    const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
+    double* field = isU ? Uc[comp].p : p.p;
+    const double* b = isU ? U.b[comp].p : P.b[0].p;
+    KScalars* S = ws.S.p + (isU ? 0 : 1);
+    KScalars* hS = h_S + (isU ? 0 : 1);
+    int n = E.n;
+    CSRView A = E.view();
+    const double* nz = E.nz.p;
+    std::memset(hS, 0, sizeof(KScalars));
+    hS->atol = SS.atol;
+    hS->rtol = SS.rtol;
+    hS->itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
+    XCAL_CUDA(cudaMemcpyAsync(S, hS, sizeof(KScalars), cudaMemcpyHostToDevice, stream));
+    int pt = SS.precond;
+    double *x = ws.x.p, *dx = ws.dx.p, *r = ws.r.p, *z = ws.z.p, *pp = ws.p.p, *q = ws.q.p, *v = ws.v.p,
+           *s = ws.s.p, *t = ws.t.p;
+    if (SS.solver == XCAL_SOLVER_CG) {
+        kr_init_resid(stream, A, nz, b, field, dx, x, r);
+        double* zz = pt == XCAL_PRECOND_NONE ? r : z;
+        if (pt != XCAL_PRECOND_NONE) apply_M(E, pt, r, zz, nullptr);
+        kr_cg_start(stream, n, r, zz, pp, S, ws.part0.p);
+        int chunk = 4;
+        long launched = 0;
+        for (;;) {
+            if ((launched += chunk) > (long)hS->itmax + 64 + 32)
+                fail(XCAL_ERR_TIMEOUT, "CG did not report completion within itmax iterations");
+            for (int c = 0; c < chunk; ++c) {
+                kr_cg_spmv(stream, A, nz, pp, q, S, ws.part0.p);
+                if (pt == XCAL_PRECOND_JACOBI) {
+                    kr_cg_update(stream, n, x, pp, r, q, zz, E.P.p, 1, S, ws.part0.p);
+                } else {
+                    kr_cg_update(stream, n, x, pp, r, q, zz, E.P.p, 0, S, ws.part0.p);
+                    if (pt == XCAL_PRECOND_DILU) dilu_ldiv(E, r, zz, S);
+                    kr_cg_rz(stream, n, r, zz, S, ws.part0.p);
+                }
+                kr_cg_p(stream, n, zz, pp, S);
+            }
+            XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
+            sync();
+            if (hS->done) break;
+            if (chunk < 32) chunk *= 2;
+        }
+    } else {
+        kr_init_resid(stream, A, nz, b, field, dx, x, q);  // r0 in q
+        apply_M(E, pt, q, r, nullptr);
+        kr_bicg_start(stream, n, b, r, pp, S, ws.part0.p, ws.part1.p);
+        int chunk = 1;
+        long launched = 0;
+        for (;;) {
+            if ((launched += chunk) > (long)hS->itmax + 16 + 8)
+                fail(XCAL_ERR_TIMEOUT, "BiCGSTAB did not report completion within itmax iterations");
+            for (int c = 0; c < chunk; ++c) {
+                kr_spmv(stream, A, nz, pp, q, S);
+                apply_M(E, pt, q, v, S);
+                kr_bicg_alpha(stream, n, b, v, S, ws.part0.p);
+                kr_bicg_s(stream, n, r, v, pp, s, x, S);
+                kr_spmv(stream, A, nz, s, q, S);
+                apply_M(E, pt, q, t, S);
+                kr_bicg_omega(stream, n, t, s, S, ws.part0.p, ws.part1.p);
+                kr_bicg_xr(stream, n, x, s, t, r, b, S, ws.part0.p, ws.part1.p);
+                kr_bicg_p(stream, n, r, v, pp, S);
+            }
+            XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
+            sync();
+            if (hS->done) break;
+            if (chunk < 8) chunk *= 2;
+        }
+    }
+    kr_finish(stream, n, x, dx, field);
+    if (iters) *iters = hS->iter;
+    // residual (Solve_1_api.jl:441-464)
+    kr_residual(stream, A, nz, field, b, S, ws.part0.p, ws.part1.p, resbuf.p);
+    XCAL_CUDA(cudaMemcpyAsync(h_res, resbuf.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    sync();
+    return h_res[0];
+}
+
+void Case::solve_equation_U(double res[3]) {  // Solve_1_api.jl:233-266
+    discretise(XCAL_EQN_U);
+    for (int d = 0; d < 3; ++d) {
+        bc_relax_U(d);
+        if (d == 0) update_precond(XCAL_EQN_U);
+        res[d] = solve_system(XCAL_EQN_U, d, &last_iters[d]);
+    }
+}
+
+double Case::solve_equation_p() {  // Solve_1_api.jl:214-231
+    discretise(XCAL_EQN_P);
+    apply_bcs(XCAL_EQN_P, 0);
+    set_reference();
+    update_precond(XCAL_EQN_P);
+    return solve_system(XCAL_EQN_P, 0, &last_iters[3]);
+}
+
+void Case::pressure_predictor(bool with_H) {  // Solvers_1_SIMPLE.jl:170-174
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    const double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
+    double* bp[3] = {U.b[0].p, U.b[1].p, U.b[2].p};
+    double* Hp[3] = {Hv[0].p, Hv[1].p, Hv[2].p};
+    launch_rD_remove_H(stream, mv(), U.view(), U.nz.p, Ucp, gp, bp, rD.p, Hp, with_H ? 1 : 0);
+    launch_interp_rD(stream, mv(), bcU.view(), rD.p, rDf.p);
+}
+
+void Case::H() {
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    const double* bp[3] = {U.b[0].p, U.b[1].p, U.b[2].p};
+    double* Hp[3] = {Hv[0].p, Hv[1].p, Hv[2].p};
+    launch_H(stream, mv(), U.view(), U.nz.p, Ucp, bp, Hp);
+}
+
+void Case::flux_divergence() {  // Solvers_1_SIMPLE.jl:177-185
+    const double* Hp[3] = {Hv[0].p, Hv[1].p, Hv[2].p};
+    double* Ufp[3] = {Uf[0].p, Uf[1].p, Uf[2].p};
+    launch_interp_U(stream, mv(), bcU.view(), Hp, Ufp, mdot.p);
+    launch_div(stream, mv(), mdot.p, divHv.p);
+}
+
+void Case::explicit_relaxation_p(double a) { launch_relax_explicit(stream, mesh->nC, p.p, prev.p, a); }
+
+void Case::grad_p() {  // Calculate_0_gradient.jl:105-111
+    launch_interp_scalar(stream, mv(), bcP.view(), p.p, pf.p, nullptr, 0.0);
+    double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
+    launch_green_gauss(stream, mv(), pf.p, gp);
+}
+
+void Case::correct() {  // Solvers_1_SIMPLE.jl:210-211
+    launch_correct_mdot(stream, mv(), P.view(), bcP.view(), P.nz.p, p.p, rDf.p, mdot.p);
+    double* Hp[3] = {Hv[0].p, Hv[1].p, Hv[2].p};
+    const double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
+    double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    launch_correct_U(stream, mesh->nC, Hp, gp, rD.p, Ucp);
+}
+
+void Case::turbulence() {
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    double* Ufp[3] = {Uf[0].p, Uf[1].p, Uf[2].p};
+    launch_interp_U(stream, mv(), bcU.view(), Ucp, Ufp, nullptr);
+    double* g[9];
+    for (int q = 0; q < 9; ++q) g[q] = gradU[q].p;
+    bool les = cfg.turbulence == XCAL_TURB_SMAGORINSKY;
+    launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, les ? nut.p : nullptr);
+    if (les)
+        launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
+    else
+        launch_fill(stream, nueff.p, cfg.nu, mesh->nF);
+}
+
+double Case::max_courant() {
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    launch_courant(stream, mesh->nC, Ucp, dx13.p, cfg.dt, courant.p);
+    std::vector<double> h(mesh->nC);
+    XCAL_CUDA(cudaMemcpyAsync(h.data(), courant.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    sync();
+    double mx = h[0];
+    for (int i = 1; i < mesh->nC; ++i) {
+        double y = h[i];
+        bool take_y = (y > mx) || (std::signbit(y) < std::signbit(mx));
+        mx = take_y ? (std::isnan(mx) ? mx : y) : (std::isnan(y) ? y : mx);
+    }
+    return mx;
+}
+
+bool Case::simple_iteration(double res[4]) {  // Solvers_1_SIMPLE.jl:164-240
+    if (!initialised) initial_calculations();
+    iteration += 1;
+    XCAL_CUDA(cudaEventRecord(ev[0], stream));
+    double r3[3];
+    solve_equation_U(r3);
+    XCAL_CUDA(cudaEventRecord(ev[1], stream));
+    pressure_predictor(true);
+    flux_divergence();
+    XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    XCAL_CUDA(cudaEventRecord(ev[2], stream));
+    double rp = solve_equation_p();
+    XCAL_CUDA(cudaEventRecord(ev[3], stream));
+    explicit_relaxation_p(cfg.p_solver.relax);
+    grad_p();
+    correct();
+    turbulence();
+    XCAL_CUDA(cudaEventRecord(ev[4], stream));
+    sync();
+    float a = 0, b = 0, c = 0, d = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[1], ev[2]);
+    cudaEventElapsedTime(&c, ev[2], ev[3]);
+    cudaEventElapsedTime(&d, ev[3], ev[4]);
+    ms[1] += a;
+    ms[3] += b + d;
+    ms[2] += c;
+    ms[5] += a + b + c + d;
+    res[0] = r3[0];
+    res[1] = r3[1];
+    res[2] = r3[2];
+    res[3] = rp;
+    for (int k = 0; k < 4; ++k)
+        if (std::isnan(res[k]) || std::isinf(res[k])) fail(XCAL_ERR_DIVERGED, "residual is NaN/Inf");
+    bool turb_conv = cfg.turbulence == XCAL_TURB_LAMINAR;
+    return r3[0] <= cfg.U_solver.convergence && r3[1] <= cfg.U_solver.convergence &&
+           r3[2] <= cfg.U_solver.convergence && rp <= cfg.p_solver.convergence && turb_conv;
+}
+
+double Case::piso_step(double res[4]) {  // Solvers_2_PISO.jl:108-187
+    if (!initialised) initial_calculations();
+    iteration += 1;
+    time = time + cfg.dt;
+    double r3[3];
+    solve_equation_U(r3);
+    pressure_predictor(false);
+    double rp = 0.0;
+    for (int it = 1; it <= cfg.inner_loops; ++it) {
+        H();
+        flux_divergence();
+        XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        rp = solve_equation_p();
+        explicit_relaxation_p(it == cfg.inner_loops ? 1.0 : cfg.p_solver.relax);
+        grad_p();
+        correct();
+    }
+    turbulence();
+    double co = max_courant();
+    res[0] = r3[0];
+    res[1] = r3[1];
+    res[2] = r3[2];
+    res[3] = rp;
+    return co;
+}
+
+}  // namespace xcal

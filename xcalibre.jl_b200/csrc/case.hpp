@@ -1,0 +1,124 @@
+// case.hpp -- host objects behind the C ABI handles.
+#pragma once
+#include <memory>
+
+#include "xcal_internal.hpp"
+
+struct xcal_ctx {
+    int device = 0;
+    std::string last_error;
+};
+
+namespace xcal {
+
+// Mesh3 in HBM plus host copies needed to derive per-equation structures
+struct DevMesh {
+    int nC = 0, nF = 0, nB = 0, nI = 0;
+    // host copies (0-based)
+    std::vector<int> owner, neigh, cf_off, cf_face, cf_nb, bcell, bf_off, bf_face, bcells, patch_start, patch_count;
+    std::vector<signed char> cf_sign;
+    std::vector<double> vol, area, delta, ccx, ccy, ccz, fcx, fcy, fcz, nxh, nyh, nzh, ex, ey, ez;
+    // device
+    DBuf<int> d_owner, d_neigh, d_cf_off, d_cf_face, d_cf_nb, d_bf_off, d_bf_face, d_bcell, d_bcells;
+    DBuf<signed char> d_cf_sign;
+    DBuf<double> d_area, d_delta, d_weight, d_Sx, d_Sy, d_Sz, d_nx, d_ny, d_nz, d_Ef, d_vol;
+    MeshView view() const;
+};
+
+struct Equation {
+    int n = 0;
+    long nnz = 0;
+    std::vector<int> rowptr, colval, diag;  // host pattern
+    DBuf<int> d_rowptr, d_colval, d_diag, d_trans, d_cf_slot, d_fslot;
+    DBuf<double> nz, nz0, diag0, P;
+    DBuf<double> b[3];
+    // DILU level schedules (rows grouped by dependency level)
+    DBuf<int> d_lower_rows, d_upper_rows;
+    std::vector<int> lower_off, upper_off;
+    bool has_periodic = false;
+    CSRView view() const;
+    int find(int i, int j) const;  // slot or -1
+};
+
+struct BCTable {
+    std::vector<xcal_bc> src;  // as given (pointers not retained)
+    std::vector<signed char> type;
+    std::vector<double> val;
+    DBuf<signed char> d_type;
+    DBuf<double> d_val, d_pw, d_pwn, d_pEf, d_pDelta, d_pwdelta;
+    DBuf<int> d_peer_face, d_peer_cell, d_pNN, d_pNP, d_pPN;
+    bool has_periodic = false;
+    BCView view() const;
+};
+
+struct KrylovWS {
+    DBuf<double> x, dx, r, z, p, q, v, s, t, part0, part1;
+    DBuf<KScalars> S;  // [2]: U, p
+};
+
+struct Case {
+    xcal_ctx* ctx = nullptr;
+    const DevMesh* mesh = nullptr;
+    xcal_config cfg{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = true;
+    BCTable bcU, bcP, bcNut;
+    Equation U, P;
+    KrylovWS ws;
+    // fields
+    DBuf<double> Uc[3], p, mdot, nueff, gradp[3], gradU[9], rD, Hv[3], divHv, nut, nutf, Uf[3], pf, rDf, Delta, prev,
+        courant, dx13, resbuf, cmax;
+    bool initialised = false;
+    int iteration = 0;
+    double time = 0.0;
+    int last_iters[4] = {0, 0, 0, 0};
+    // timing
+    double ms[6] = {0, 0, 0, 0, 0, 0};
+    long long launches = 0;
+    cudaEvent_t ev[8];
+    KScalars* h_S = nullptr;  // pinned host mirror (2 entries)
+    double* h_res = nullptr;  // pinned
+
+    Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cfg);
+    ~Case();
+
+    // steps (each mirrors a reference function)
+    void initial_calculations();
+    void discretise(int eqn);
+    void apply_bcs(int eqn, int comp);
+    void relax_U(int comp);
+    void bc_relax_U(int comp);
+    void set_reference();
+    void update_precond(int eqn);
+    double solve_system(int eqn, int comp, int* iters);
+    void solve_equation_U(double res[3]);
+    double solve_equation_p();
+    void pressure_predictor(bool with_H);
+    void H();
+    void flux_divergence();
+    void explicit_relaxation_p(double a);
+    void grad_p();
+    void correct();
+    void turbulence();
+    double max_courant();
+    bool simple_iteration(double res[4]);
+    double piso_step(double res[4]);
+
+    // helpers
+    MeshView mv() const { return mesh->view(); }
+    double* field_comp(int field, int comp, long& count);
+    void sync();
+    void dilu_ldiv(Equation& E, const double* b, double* out, const KScalars* S);
+    void apply_M(Equation& E, int ptype, const double* in, double* out, const KScalars* S);
+};
+
+}  // namespace xcal
+
+struct xcal_mesh {
+    xcal_ctx* ctx = nullptr;
+    std::unique_ptr<xcal::DevMesh> m;
+};
+
+struct xcal_case {
+    std::unique_ptr<xcal::Case> c;
+};

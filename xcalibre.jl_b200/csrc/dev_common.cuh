@@ -1,0 +1,79 @@
+// dev_common.cuh -- device helpers shared by the kernels.
+//
+// Arithmetic contract (matches the reference's Julia code, which never fuses
+// a*b+c): the library is compiled with --fmad=false, every expression below
+// is written in the operation order of the cited Julia source, and all
+// reductions use the fixed "canonical tile" tree so results are
+// deterministic and independent of scheduling.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "xcal_internal.hpp"
+
+namespace xcal {
+
+// canonical reduction geometry: a tile is RED_THREADS threads x RED_ITEMS rows;
+// thread t of tile b owns rows b*RED_TILE + k*RED_THREADS + t, k < RED_ITEMS
+constexpr int RED_THREADS = 256;
+constexpr int RED_ITEMS = 8;
+constexpr int RED_TILE = RED_THREADS * RED_ITEMS;
+
+__device__ __forceinline__ int tile_row(int k) { return blockIdx.x * RED_TILE + k * RED_THREADS + threadIdx.x; }
+
+// Julia's max(x, y) for floats (NaN propagating, -0.0 < 0.0)
+__device__ __forceinline__ double jl_max(double x, double y) {
+    bool take_y = (y > x) || (signbit(y) < signbit(x));
+    return take_y ? (isnan(x) ? x : y) : (isnan(y) ? y : x);
+}
+
+// Julia's eps(x)
+__device__ __forceinline__ double jl_eps(double x) {
+    x = fabs(x);
+    return nextafter(x, __longlong_as_double(0x7ff0000000000000ULL)) - x;
+}
+
+// Block tree of the canonical reduction: xor butterfly (16..1) inside each
+// warp, then butterfly (4,2,1) over the 8 warp sums.  Result valid in thread 0.
+__device__ __forceinline__ double block_tree(double v, double* smem8) {
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();  // smem8 may still be read by a previous tree
+    if (lane == 0) smem8[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (warp == 0) {
+        double w = lane < (RED_THREADS / 32) ? smem8[lane] : 0.0;
+#pragma unroll
+        for (int off = (RED_THREADS / 64); off >= 1; off >>= 1) w = w + __shfl_xor_sync(0xffffffffu, w, off);
+        r = w;
+    }
+    return r;
+}
+
+// Final pass over tile partials (executed by one block): thread t sums
+// partials t, t+RED_THREADS, ... sequentially, then the block tree.
+__device__ __forceinline__ double reduce_partials(const double* part, int T, double* smem8) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < T; i += RED_THREADS) s = s + __ldcg(part + i);
+    return block_tree(s, smem8);
+}
+
+// Last-block election: every block publishes its partial(s) before calling;
+// returns true in all threads of the block that arrives last (the counter is
+// reset by it).  No block waits, so there is no spin.
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int ticket = atomicAdd(counter, 1u);
+        is_last = (ticket == gridDim.x - 1);
+        if (is_last) *counter = 0u;
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+}  // namespace xcal

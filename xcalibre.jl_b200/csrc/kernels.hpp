@@ -1,0 +1,78 @@
+// kernels.hpp -- host-side launchers of the device kernels.
+#pragma once
+#include "xcal_internal.hpp"
+
+namespace xcal {
+
+// flags of launch_bc_relax_U: start from the assembled diagonal, apply the
+// boundary conditions, apply the implicit relaxation
+enum { BCR_DIAG0 = 1, BCR_BC = 2, BCR_RELAX = 4 };
+
+// finite-volume kernels (kernels_fv.cu)
+void launch_assemble_U(cudaStream_t s, const MeshView& m, const CSRView& A, const double* mdot, const double* nueff,
+                       const double* const U[3], const double* const g[3], double* nz, double* diag0,
+                       double* const b[3], int time_scheme, int div_scheme, double dt);
+void launch_assemble_p(cudaStream_t s, const MeshView& m, const CSRView& A, const double* rDf, const double* divHv,
+                       double* nz, double* b);
+void launch_bc_relax_U(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, int comp,
+                       int div_scheme, double* nz, const double* diag0, double* b, const double* mdot,
+                       const double* nueff, const double* const U[3], double alpha, int flags);
+void launch_bc_p(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz, double* b,
+                 const double* rDf, const double* p);
+void launch_set_reference(cudaStream_t s, const CSRView& A, double* nz, double* b, double pref);
+void launch_interp_U(cudaStream_t s, const MeshView& m, const BCView& bc, const double* const U[3],
+                     double* const Uf[3], double* mdot);
+void launch_interp_scalar(cudaStream_t s, const MeshView& m, const BCView& bc, const double* phi, double* phif,
+                          double* nueff, double nu);
+void launch_interp_rD(cudaStream_t s, const MeshView& m, const BCView& bcU, const double* rD, double* rDf);
+void launch_fill(cudaStream_t s, double* a, double v, long n);
+void launch_green_gauss(cudaStream_t s, const MeshView& m, const double* phif, double* const g[3]);
+void launch_green_gauss_tensor(cudaStream_t s, const MeshView& m, double* const Uf[3], double* const g[9],
+                               const double* Delta, double* nut);
+void launch_div(cudaStream_t s, const MeshView& m, const double* psif, double* out);
+void launch_rD_remove_H(cudaStream_t s, const MeshView& m, const CSRView& A, const double* nz,
+                        const double* const U[3], const double* const g[3], double* const b[3], double* rD,
+                        double* const H[3], int do_H);
+void launch_H(cudaStream_t s, const MeshView& m, const CSRView& A, const double* nz, const double* const U[3],
+              const double* const b[3], double* const H[3]);
+void launch_correct_mdot(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bcp, const double* nz,
+                         const double* p, const double* rDf, double* mdot);
+void launch_correct_U(cudaStream_t s, int n, double* const H[3], const double* const g[3], const double* rD,
+                      double* const U[3]);
+void launch_relax_explicit(cudaStream_t s, int n, double* phi, const double* phi0, double alpha);
+void launch_courant(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* co);
+
+// Krylov kernels (kernels_krylov.cu)
+void kr_init_resid(cudaStream_t s, const CSRView& A, const double* nz, const double* b, const double* field,
+                   double* dx, double* x, double* r);
+void kr_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* x, double* y, const KScalars* S);
+void kr_jacobi_apply(cudaStream_t s, int n, const double* P, const double* r, double* z, const KScalars* S);
+void kr_copy(cudaStream_t s, int n, const double* a, double* b, const KScalars* S);
+void kr_cg_start(cudaStream_t s, int n, const double* r, const double* z, double* p, KScalars* S, double* part);
+void kr_cg_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* p, double* q, KScalars* S,
+                double* part);
+void kr_cg_update(cudaStream_t s, int n, double* x, const double* p, double* r, const double* q, double* z,
+                  const double* P, int jacobi_fused, KScalars* S, double* part);
+void kr_cg_rz(cudaStream_t s, int n, const double* r, const double* z, KScalars* S, double* part);
+void kr_cg_p(cudaStream_t s, int n, const double* z, double* p, const KScalars* S);
+void kr_finish(cudaStream_t s, int n, const double* x, const double* dx, double* field);
+void kr_bicg_start(cudaStream_t s, int n, const double* c, const double* r, double* p, KScalars* S, double* part0,
+                   double* part1);
+void kr_bicg_alpha(cudaStream_t s, int n, const double* c, const double* v, KScalars* S, double* part);
+void kr_bicg_s(cudaStream_t s, int n, const double* r, const double* v, const double* p, double* sv, double* x,
+               const KScalars* S);
+void kr_bicg_omega(cudaStream_t s, int n, const double* t, const double* sv, KScalars* S, double* part0,
+                   double* part1);
+void kr_bicg_xr(cudaStream_t s, int n, double* x, const double* sv, const double* t, double* r, const double* c,
+                KScalars* S, double* part0, double* part1);
+void kr_bicg_p(cudaStream_t s, int n, const double* r, const double* v, double* p, const KScalars* S);
+void kr_jacobi_update(cudaStream_t s, const CSRView& A, const double* nz, double* P);
+void kr_dilu_D(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, double* D);
+void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, const double* D,
+                 const double* b, double* y, const KScalars* S);
+void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, const double* D,
+                 double* x, const KScalars* S);
+void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
+                 double* part0, double* part1, double* out);
+
+}  // namespace xcal

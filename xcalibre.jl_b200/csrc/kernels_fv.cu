@@ -1,0 +1,775 @@
+// kernels_fv.cu -- finite-volume kernels of the SIMPLE/PISO path (FP64).
+//
+// Each kernel restates one reference kernel; the operation order inside every
+// expression is the Julia source's (cited per kernel).  Gathers replace the
+// reference's Atomix scatters: boundary contributions to a cell are applied by
+// the thread owning the cell, in ascending boundary-face order.
+#include "dev_common.cuh"
+#include "kernels.hpp"
+
+namespace xcal {
+
+constexpr int TPB = 256;
+static inline int nblk(long n) { return (int)((n + TPB - 1) / TPB); }
+
+// ---------------------------------------------------------------------------
+// boundary-condition functors (src/Discretise/boundary_conditions/*.jl)
+// ---------------------------------------------------------------------------
+// value of a Dirichlet-like BC at boundary face f, component c
+__device__ __forceinline__ double bc_val(const BCView& bc, int f, int c) { return bc.val[3 * f + c]; }
+
+// U equation: terms Time + Divergence(mdotf,U) - Laplacian(nueff,U); returns
+// (AP, BP) summed over the terms in order (apply!, Discretise_5_apply_bcs.jl:158-183)
+__device__ void bc_U(const MeshView& m, const BCView& bc, int f, int cell, int comp, int div_scheme,
+                     const double* mdot, const double* nueff, const double* Ux, const double* Uy,
+                     const double* Uz, double& AP, double& BP) {
+    int type = bc.type[f];
+    double ap_d = 0.0, bp_d = 0.0, ap_l = 0.0, bp_l = 0.0;
+    switch (type) {
+        case XCAL_BC_DIRICHLET:
+        case XCAL_BC_DIRICHLET_FUNCTION: {  // dirichlet.jl:46-75
+            double val = bc_val(bc, f, comp);
+            double fl = -mdot[f];
+            double a = 1.0 * fl;
+            ap_d = 0.0;
+            bp_d = a * val;
+            double fll = (nueff[f] * m.area[f]) / m.delta[f];
+            double al = -1.0 * (-fll);
+            ap_l = al;
+            bp_l = al * val;
+            break;
+        }
+        case XCAL_BC_WALL: {  // wall.jl:26-42
+            double fll = (nueff[f] * m.area[f]) / m.delta[f];
+            double al = -1.0 * (-fll);
+            double nx = m.nx[f], ny = m.ny[f], nz = m.nz[f];
+            double vbx = bc_val(bc, f, 0), vby = bc_val(bc, f, 1), vbz = bc_val(bc, f, 2);
+            double vcx = Ux[cell], vcy = Uy[cell], vcz = Uz[cell];
+            double dc = vcx * nx + vcy * ny + vcz * nz;
+            double db = vbx * nx + vby * ny + vbz * nz;
+            double vcn = comp == 0 ? dc * nx : (comp == 1 ? dc * ny : dc * nz);
+            double vbn = comp == 0 ? db * nx : (comp == 1 ? db * ny : db * nz);
+            double vb = comp == 0 ? vbx : (comp == 1 ? vby : vbz);
+            double vbp = vb - vbn;
+            ap_l = al;
+            bp_l = al * (vbp + vcn);
+            break;
+        }
+        case XCAL_BC_ZEROGRADIENT:  // zerogradient.jl:40-46
+            ap_d = 1.0 * mdot[f];
+            break;
+        case XCAL_BC_EXTRAPOLATED: {  // extrapolated.jl:21-41
+            ap_d = 1.0 * mdot[f];
+            double fll = ((-nueff[f]) * m.area[f]) / m.delta[f];
+            double al = -1.0 * fll;
+            const double* U = comp == 0 ? Ux : (comp == 1 ? Uy : Uz);
+            ap_l = al;
+            bp_l = al * U[cell];
+            break;
+        }
+        case XCAL_BC_SYMMETRY: {  // symmetry.jl:23-41, 103-117
+            double nx = m.nx[f], ny = m.ny[f], nz = m.nz[f];
+            double vcx = Ux[cell], vcy = Uy[cell], vcz = Uz[cell];
+            double dc = vcx * nx + vcy * ny + vcz * nz;
+            double vn = comp == 0 ? dc * nx : (comp == 1 ? dc * ny : dc * nz);
+            double vc = comp == 0 ? vcx : (comp == 1 ? vcy : vcz);
+            double a = 1.0 * mdot[f];
+            ap_d = a;
+            bp_d = a * vn;
+            double fll = (nueff[f] * m.area[f]) / m.delta[f];
+            double al = -1.0 * (-fll);
+            ap_l = al;
+            bp_l = al * (vc - vn);
+            break;
+        }
+        default:  // Empty, Periodic (shadow), none
+            break;
+    }
+    double ap = 0.0, bp = 0.0;
+    ap = ap + 0.0;  // Time term (Discretise_3_boundary_conditions.jl:2-9)
+    bp = bp + 0.0;
+    ap = ap + ap_d;
+    bp = bp + bp_d;
+    ap = ap + ap_l;
+    bp = bp + bp_l;
+    AP = ap;
+    BP = bp;
+}
+
+// p equation: single term -Laplacian(rDf, p)
+__device__ void bc_p(const MeshView& m, const BCView& bc, int f, int cell, const double* rDf, const double* p,
+                     double& AP, double& BP) {
+    int type = bc.type[f];
+    double a = 0.0, b = 0.0;
+    switch (type) {
+        case XCAL_BC_DIRICHLET:
+        case XCAL_BC_DIRICHLET_FUNCTION: {  // dirichlet.jl:19-25
+            double fl = (rDf[f] * m.area[f]) / m.delta[f];
+            a = -1.0 * (-fl);
+            b = a * bc_val(bc, f, 0);
+            break;
+        }
+        case XCAL_BC_EXTRAPOLATED: {  // extrapolated.jl:21-33
+            double fl = ((-rDf[f]) * m.area[f]) / m.delta[f];
+            a = -1.0 * fl;
+            b = a * p[cell];
+            break;
+        }
+        case XCAL_BC_NEUMANN: {  // neumann.jl:23-30
+            double fl = rDf[f] * m.area[f];
+            a = 0.0;
+            b = fl * bc_val(bc, f, 0);
+            break;
+        }
+        default:  // Wall, Zerogradient, Empty, Symmetry, Periodic: (0, 0)
+            break;
+    }
+    AP = 0.0 + a;
+    BP = 0.0 + b;
+}
+
+// ---------------------------------------------------------------------------
+// assembly: _discretise_vector_model! / _discretise_scalar_model!
+// (Discretise_2_generated_distretisation.jl:39-87, 125-167)
+// ---------------------------------------------------------------------------
+__global__ void k_assemble_U(MeshView m, CSRView A, const double* __restrict__ mdot,
+                             const double* __restrict__ nueff, const double* __restrict__ Ux,
+                             const double* __restrict__ Uy, const double* __restrict__ Uz,
+                             const double* __restrict__ gx, const double* __restrict__ gy,
+                             const double* __restrict__ gz, double* nz, double* diag0, double* bx, double* by,
+                             double* bz, int time_scheme, int div_scheme, double dt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    double ac_sum = 0.0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        int f = m.cf_face[k];
+        int ns = m.cf_sign[k];
+        double dns = (double)ns;
+        double AC = 0.0, AN = 0.0;
+        AC = AC + 0.0;  // Time{...} scheme! (Discretise_1_schemes.jl:12-34)
+        AN = AN + 0.0;
+        // Divergence (Discretise_1_schemes.jl:114-180)
+        double ap = 1.0 * (mdot[f] * dns);
+        double ac, an;
+        if (div_scheme == XCAL_DIV_LINEAR) {
+            double w = m.weight[f];
+            w = 0.5 + dns * (w - 0.5);
+            ac = ap * w;
+            an = ap * (1.0 - w);
+        } else if (div_scheme == XCAL_DIV_UPWIND) {
+            ac = jl_max(ap, 0.0);
+            an = -jl_max(-ap, 0.0);
+        } else {
+            double w = m.weight[f];
+            if (ns < 0) w = 1.0 - w;
+            double acL = ap * w, anL = ap * (1.0 - w);
+            double acU = jl_max(ap, 0.0), anU = -jl_max(-ap, 0.0);
+            ac = 0.75 * acL + 0.25 * acU;
+            an = 0.75 * anL + 0.25 * anU;
+        }
+        AC = AC + ac;
+        AN = AN + an;
+        // Laplacian{Linear}, sign -1 (Discretise_1_schemes.jl:68-110)
+        double apl = (-1.0 * (nueff[f] * m.Efmag[f])) / m.delta[f];
+        AC = AC + (-apl);
+        AN = AN + apl;
+        ac_sum = ac_sum + AC;
+        nz[A.cf_slot[k]] = AN;
+    }
+    double V = m.vol[i];
+    double acs = 0.0, bxs = 0.0, bys = 0.0, bzs = 0.0;  // _scheme_source!
+    if (time_scheme == XCAL_TIME_EULER) {
+        double vol_rdt = (1.0 * V) / dt;  // Discretise_1_schemes.jl:36-45
+        acs = acs + vol_rdt;
+        bxs = bxs + Ux[i] * vol_rdt;
+        bys = bys + Uy[i] * vol_rdt;
+        bzs = bzs + Uz[i] * vol_rdt;
+    } else {
+        acs = acs + 0.0;
+        bxs = bxs + 0.0;
+        bys = bys + 0.0;
+        bzs = bzs + 0.0;
+    }
+    acs = acs + 0.0;  // Divergence, Laplacian scheme_source!
+    bxs = bxs + 0.0;
+    bys = bys + 0.0;
+    bzs = bzs + 0.0;
+    acs = acs + 0.0;
+    bxs = bxs + 0.0;
+    bys = bys + 0.0;
+    bzs = bzs + 0.0;
+    double d = ac_sum + acs;
+    nz[A.diag[i]] = d;
+    diag0[i] = d;
+    // _sources!: -Source(grad p)
+    double Bx = 0.0 + (-1.0 * gx[i]) * V;
+    double By = 0.0 + (-1.0 * gy[i]) * V;
+    double Bz = 0.0 + (-1.0 * gz[i]) * V;
+    bx[i] = bxs + Bx;
+    by[i] = bys + By;
+    bz[i] = bzs + Bz;
+}
+
+__global__ void k_assemble_p(MeshView m, CSRView A, const double* __restrict__ rDf,
+                             const double* __restrict__ divHv, double* nz, double* b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    double ac_sum = 0.0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        int f = m.cf_face[k];
+        double ap = (-1.0 * (rDf[f] * m.Efmag[f])) / m.delta[f];
+        double AC = 0.0 + (-ap);
+        double AN = 0.0 + ap;
+        ac_sum = ac_sum + AC;
+        nz[A.cf_slot[k]] = AN;
+    }
+    double acs = 0.0 + 0.0, bs = 0.0 + 0.0;
+    nz[A.diag[i]] = ac_sum + acs;
+    double b2 = 0.0 + (-1.0 * divHv[i]) * m.vol[i];
+    b[i] = b2 + bs;
+}
+
+// ---------------------------------------------------------------------------
+// boundary conditions + implicit relaxation (U), per row
+// apply_boundary_conditions! (Discretise_5_apply_bcs.jl:84-123) then
+// implicit_relaxation_diagdom! (Solve_1_api.jl:388-411)
+// ---------------------------------------------------------------------------
+__global__ void k_bc_relax_U(MeshView m, CSRView A, BCView bc, int comp, int div_scheme, double* nz,
+                             const double* __restrict__ diag0, double* b, const double* __restrict__ mdot,
+                             const double* __restrict__ nueff, const double* __restrict__ Ux,
+                             const double* __restrict__ Uy, const double* __restrict__ Uz, double alpha,
+                             int flags) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    int ds = A.diag[i];
+    double d = (flags & BCR_DIAG0) ? diag0[i] : nz[ds];
+    double bi = b[i];
+    if (flags & BCR_BC) {
+        for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
+            int f = m.bf_face[k];
+            double AP, BP;
+            bc_U(m, bc, f, i, comp, div_scheme, mdot, nueff, Ux, Uy, Uz, AP, BP);
+            d = d + AP;
+            bi = bi + BP;
+        }
+    }
+    if (!(flags & BCR_RELAX)) {
+        nz[ds] = d;
+        b[i] = bi;
+        return;
+    }
+    double sumv = 0.0;
+    for (int e = A.rowptr[i]; e < A.rowptr[i + 1]; ++e) sumv = sumv + fabs(e == ds ? d : nz[e]);
+    sumv = sumv - fabs(d);
+    double D0 = d;
+    double Dmax = jl_max(fabs(D0), sumv) / alpha;
+    nz[ds] = Dmax;
+    const double* U = comp == 0 ? Ux : (comp == 1 ? Uy : Uz);
+    b[i] = bi + (Dmax - D0) * U[i];
+}
+
+// boundary conditions of the p equation (cells owning boundary faces)
+__global__ void k_bc_p(MeshView m, CSRView A, BCView bc, double* nz, double* b, const double* __restrict__ rDf,
+                       const double* __restrict__ p) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m.n_bcells) return;
+    int i = m.bcells[t];
+    int ds = A.diag[i];
+    double d = nz[ds];
+    double bi = b[i];
+    for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
+        int f = m.bf_face[k];
+        double AP, BP;
+        bc_p(m, bc, f, i, rDf, p, AP, BP);
+        d = d + AP;
+        bi = bi + BP;
+    }
+    nz[ds] = d;
+    b[i] = bi;
+}
+
+// setReference! (Solve_1_api.jl:431-439)
+__global__ void k_set_reference(CSRView A, double* nz, double* b, double pref) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int c = A.diag[0];
+        b[0] = nz[c] * pref;
+        nz[c] = nz[c] + nz[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// face interpolation + boundary values (+ flux)
+// interpolate_Vector! (Calculate_2_interpolation.jl:374-397), correct_boundaries!
+// (1_boundary_interpolation.jl), flux! (Solvers_0_functions.jl:51-62)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void periodic_interp3(const MeshView& m, const BCView& bc, int pf, const double* ux,
+                                                 const double* uy, const double* uz, double& fx, double& fy,
+                                                 double& fz) {
+    // value written by the parent face pf (periodic_interpolation.jl:45-73)
+    int c = m.owner[pf], pc = bc.peer_cell[pf];
+    double w = bc.pw[pf], wn = bc.pwn[pf];
+    fx = w * ux[c] + wn * ux[pc];
+    fy = w * uy[c] + wn * uy[pc];
+    fz = w * uz[c] + wn * uz[pc];
+}
+
+__global__ void k_interp_U(MeshView m, BCView bc, const double* __restrict__ ux, const double* __restrict__ uy,
+                           const double* __restrict__ uz, double* fx, double* fy, double* fz, double* mdot) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nF) return;
+    int o = m.owner[f], n = m.neigh[f];
+    double w = m.weight[f];
+    double omw = 1.0 - w;
+    double vx = w * ux[o] + omw * ux[n];
+    double vy = w * uy[o] + omw * uy[n];
+    double vz = w * uz[o] + omw * uz[n];
+    if (f < m.nB) {
+        switch (bc.type[f]) {
+            case XCAL_BC_DIRICHLET:
+            case XCAL_BC_DIRICHLET_FUNCTION:
+            case XCAL_BC_WALL:
+                vx = bc_val(bc, f, 0);
+                vy = bc_val(bc, f, 1);
+                vz = bc_val(bc, f, 2);
+                break;
+            case XCAL_BC_ZEROGRADIENT:
+            case XCAL_BC_EXTRAPOLATED:
+                vx = ux[o];
+                vy = uy[o];
+                vz = uz[o];
+                break;
+            case XCAL_BC_EMPTY:
+                vx = 0.0;
+                vy = 0.0;
+                vz = 0.0;
+                break;
+            case XCAL_BC_SYMMETRY: {
+                double nx = m.nx[f], ny = m.ny[f], nz = m.nz[f];
+                double px = ux[o], py = uy[o], pz = uz[o];
+                double dd = px * nx + py * ny + pz * nz;
+                vx = px - dd * nx;
+                vy = py - dd * ny;
+                vz = pz - dd * nz;
+                break;
+            }
+            case XCAL_BC_PERIODIC_PARENT:
+                periodic_interp3(m, bc, f, ux, uy, uz, vx, vy, vz);
+                break;
+            case XCAL_BC_PERIODIC:
+                periodic_interp3(m, bc, bc.peer_face[f], ux, uy, uz, vx, vy, vz);
+                break;
+            default:
+                break;
+        }
+    }
+    if (fx) {
+        fx[f] = vx;
+        fy[f] = vy;
+        fz[f] = vz;
+    }
+    if (mdot) mdot[f] = vx * m.Sx[f] + vy * m.Sy[f] + vz * m.Sz[f];
+}
+
+// scalar interpolation with the boundary values of a scalar field
+// (p: Calculate_0_gradient.jl:105-111; nut: LES_Smagorinsky.jl:129-130)
+__global__ void k_interp_scalar(MeshView m, BCView bc, const double* __restrict__ phi, double* phif,
+                                double* nueff_out, double nu) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nF) return;
+    int o = m.owner[f], n = m.neigh[f];
+    double w = m.weight[f];
+    double omw = 1.0 - w;
+    double v = w * phi[o] + omw * phi[n];
+    if (f < m.nB) {
+        switch (bc.type[f]) {
+            case XCAL_BC_DIRICHLET:
+            case XCAL_BC_DIRICHLET_FUNCTION:
+                v = bc_val(bc, f, 0);
+                break;
+            case XCAL_BC_WALL:
+            case XCAL_BC_ZEROGRADIENT:
+            case XCAL_BC_EXTRAPOLATED:
+            case XCAL_BC_SYMMETRY:
+                v = phi[o];
+                break;
+            case XCAL_BC_EMPTY:
+                v = 0.0;
+                break;
+            case XCAL_BC_NEUMANN:
+                v = phi[o] + m.delta[f] * bc_val(bc, f, 0);
+                break;
+            case XCAL_BC_PERIODIC_PARENT: {
+                int c = m.owner[f], pc = bc.peer_cell[f];
+                v = bc.pw[f] * phi[c] + bc.pwn[f] * phi[pc];
+                break;
+            }
+            case XCAL_BC_PERIODIC: {
+                int pf = bc.peer_face[f];
+                int c = m.owner[pf], pc = bc.peer_cell[pf];
+                v = bc.pw[pf] * phi[c] + bc.pwn[pf] * phi[pc];
+                break;
+            }
+            default:
+                break;
+        }
+    }
+    phif[f] = v;
+    if (nueff_out) nueff_out[f] = nu + v;  // update_nueff_turbulent! (Solvers_0_functions.jl:30-35)
+}
+
+// interpolate!(rDf, rD) + correct_interpolation_periodic (Solvers_1_SIMPLE.jl:427-470)
+__global__ void k_interp_rD(MeshView m, BCView bcU, const double* __restrict__ rD, double* rDf) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nF) return;
+    int o = m.owner[f], n = m.neigh[f];
+    double w = m.weight[f];
+    double omw = 1.0 - w;
+    double v = w * rD[o] + omw * rD[n];
+    if (f < m.nB) {
+        int pf = -1;
+        if (bcU.type[f] == XCAL_BC_PERIODIC_PARENT) pf = f;
+        if (bcU.type[f] == XCAL_BC_PERIODIC) pf = bcU.peer_face[f];
+        if (pf >= 0) {
+            double wp = bcU.pwdelta[pf];
+            double omwp = 1.0 - wp;
+            v = wp * rD[m.owner[pf]] + omwp * rD[bcU.peer_cell[pf]];
+        }
+    }
+    rDf[f] = v;
+}
+
+__global__ void k_fill(double* a, double v, long n) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Green-Gauss gradients (Calculate_1_green_gauss.jl:27-78, 106-173)
+// ---------------------------------------------------------------------------
+__global__ void k_green_gauss(MeshView m, const double* __restrict__ phif, double* gx, double* gy, double* gz) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    double rx = 0.0, ry = 0.0, rz = 0.0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        int f = m.cf_face[k];
+        double s = (double)m.cf_sign[k];
+        double v = phif[f];
+        rx = rx + v * (m.Sx[f] * s);
+        ry = ry + v * (m.Sy[f] * s);
+        rz = rz + v * (m.Sz[f] * s);
+    }
+    double V = m.vol[i];
+    rx = rx / V;
+    ry = ry / V;
+    rz = rz / V;
+    for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
+        int f = m.bf_face[k];
+        double v = phif[f];
+        rx = rx + (v * m.Sx[f]) / V;
+        ry = ry + (v * m.Sy[f]) / V;
+        rz = rz + (v * m.Sz[f]) / V;
+    }
+    gx[i] = rx;
+    gy[i] = ry;
+    gz[i] = rz;
+}
+
+// vector -> tensor; with Smagorinsky also nut = (C Delta)^2 sqrt(2 S:S)
+// (LES_Smagorinsky.jl:122-127)
+__global__ void k_green_gauss_tensor(MeshView m, const double* __restrict__ fx, const double* __restrict__ fy,
+                                     const double* __restrict__ fz, double* g0, double* g1, double* g2, double* g3,
+                                     double* g4, double* g5, double* g6, double* g7, double* g8,
+                                     const double* __restrict__ Delta, double* nut) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    double r[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) r[q] = 0.0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        int f = m.cf_face[k];
+        double s = (double)m.cf_sign[k];
+        double S[3] = {m.Sx[f] * s, m.Sy[f] * s, m.Sz[f] * s};
+        double u[3] = {fx[f], fy[f], fz[f]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) r[3 * a + b] = r[3 * a + b] + u[a] * S[b];
+    }
+    double V = m.vol[i];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) r[q] = r[q] / V;
+    for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
+        int f = m.bf_face[k];
+        double S[3] = {m.Sx[f], m.Sy[f], m.Sz[f]};
+        double u[3] = {fx[f], fy[f], fz[f]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) r[3 * a + b] = r[3 * a + b] + (u[a] * S[b]) / V;
+    }
+    g0[i] = r[0];
+    g1[i] = r[1];
+    g2[i] = r[2];
+    g3[i] = r[3];
+    g4[i] = r[4];
+    g5[i] = r[5];
+    g6[i] = r[6];
+    g7[i] = r[7];
+    g8[i] = r[8];
+    if (nut) {
+        // S = 0.5 (G + G'), (2S).S over the column-major linear index
+        double acc = 0.0;
+        bool first = true;
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                double s = 0.5 * (r[3 * a + b] + r[3 * b + a]);
+                double pr = (2.0 * s) * s;
+                acc = first ? pr : acc + pr;
+                first = false;
+            }
+        nut[i] = Delta[i] * sqrt(acc);
+    }
+}
+
+// div! of a face scalar (Calculate_0_divergence.jl:129-170)
+__global__ void k_div(MeshView m, const double* __restrict__ psif, double* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    double red = 0.0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) red = red + psif[m.cf_face[k]] * (double)m.cf_sign[k];
+    double V = m.vol[i];
+    double r = red / V;
+    for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) r = r + psif[m.bf_face[k]] / V;
+    out[i] = r;
+}
+
+// ---------------------------------------------------------------------------
+// pressure-velocity coupling (Solvers_0_functions.jl, Solvers_1_SIMPLE.jl)
+// ---------------------------------------------------------------------------
+// inverse_diagonal! (:108-120) + remove_pressure_source! (:170-181) + H! (:201-249)
+__global__ void k_rD_remove_H(MeshView m, CSRView A, const double* __restrict__ nz, const double* __restrict__ Ux,
+                              const double* __restrict__ Uy, const double* __restrict__ Uz,
+                              const double* __restrict__ gx, const double* __restrict__ gy,
+                              const double* __restrict__ gz, double* bx, double* by, double* bz, double* rD,
+                              double* Hx, double* Hy, double* Hz, int do_H) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    double V = m.vol[i];
+    double D = nz[A.diag[i]];
+    rD[i] = V / D;
+    double cx = (-1.0 * gx[i]) * V, cy = (-1.0 * gy[i]) * V, cz = (-1.0 * gz[i]) * V;
+    double bxi = bx[i] - cx, byi = by[i] - cy, bzi = bz[i] - cz;
+    bx[i] = bxi;
+    by[i] = byi;
+    bz[i] = bzi;
+    if (!do_H) return;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int e = A.rowptr[i]; e < A.rowptr[i + 1]; ++e) {
+        int j = A.colval[e];
+        double val = nz[e];
+        sx = sx + val * Ux[j];
+        sy = sy + val * Uy[j];
+        sz = sz + val * Uz[j];
+    }
+    sx = sx - D * Ux[i];
+    sy = sy - D * Uy[i];
+    sz = sz - D * Uz[i];
+    double r = 1.0 / D;
+    Hx[i] = (bxi - sx) * r;
+    Hy[i] = (byi - sy) * r;
+    Hz[i] = (bzi - sz) * r;
+}
+
+// H! alone (PISO correctors, Solvers_2_PISO.jl:122)
+__global__ void k_H(MeshView m, CSRView A, const double* __restrict__ nz, const double* __restrict__ Ux,
+                    const double* __restrict__ Uy, const double* __restrict__ Uz, const double* __restrict__ bx,
+                    const double* __restrict__ by, const double* __restrict__ bz, double* Hx, double* Hy,
+                    double* Hz) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int e = A.rowptr[i]; e < A.rowptr[i + 1]; ++e) {
+        int j = A.colval[e];
+        double val = nz[e];
+        sx = sx + val * Ux[j];
+        sy = sy + val * Uy[j];
+        sz = sz + val * Uz[j];
+    }
+    double D = nz[A.diag[i]];
+    sx = sx - D * Ux[i];
+    sy = sy - D * Uy[i];
+    sz = sz - D * Uz[i];
+    double r = 1.0 / D;
+    Hx[i] = (bx[i] - sx) * r;
+    Hy[i] = (by[i] - sy) * r;
+    Hz[i] = (bz[i] - sz) * r;
+}
+
+// correct_mass_flux! (Solvers_1_SIMPLE.jl:371-388), periodic (:403-425),
+// boundary (:474-557)
+__global__ void k_correct_mdot(MeshView m, CSRView A, BCView bcp, const double* __restrict__ nz,
+                               const double* __restrict__ p, const double* __restrict__ rDf, double* mdot) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nF) return;
+    if (f >= m.nB) {
+        int o = m.owner[f], n = m.neigh[f];
+        double aN = nz[A.fslot[f - m.nB]];
+        mdot[f] = mdot[f] + aN * (p[n] - p[o]);
+        return;
+    }
+    int c = m.bcell[f];
+    switch (bcp.type[f]) {
+        case XCAL_BC_DIRICHLET:
+        case XCAL_BC_DIRICHLET_FUNCTION: {
+            double fl = (rDf[f] * m.area[f]) / m.delta[f];
+            double ap = -1.0 * (-fl);
+            mdot[f] = mdot[f] + ap * (p[c] - bc_val(bcp, f, 0));
+            break;
+        }
+        case XCAL_BC_NEUMANN:
+            mdot[f] = mdot[f] - (rDf[f] * m.area[f]) * bc_val(bcp, f, 0);
+            break;
+        case XCAL_BC_PERIODIC_PARENT: {
+            int pf = bcp.peer_face[f];
+            int c2 = bcp.peer_cell[f];
+            double aN = nz[bcp.pPN[f]];
+            double corr = aN * (p[c2] - p[c]);
+            double v = mdot[f] + corr;
+            mdot[f] = v;
+            mdot[pf] = -v;
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+// correct_velocity! (Solvers_0_functions.jl:136-151)
+__global__ void k_correct_U(int n, const double* __restrict__ Hx, const double* __restrict__ Hy,
+                            const double* __restrict__ Hz, const double* __restrict__ gx,
+                            const double* __restrict__ gy, const double* __restrict__ gz,
+                            const double* __restrict__ rD, double* Ux, double* Uy, double* Uz) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double r = rD[i];
+    Ux[i] = Hx[i] - gx[i] * r;
+    Uy[i] = Hy[i] - gy[i] * r;
+    Uz[i] = Hz[i] - gz[i] * r;
+}
+
+// explicit_relaxation! (Solve_1_api.jl:327-335)
+__global__ void k_relax_explicit(int n, double* phi, const double* __restrict__ phi0, double alpha) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    phi[i] = phi0[i] + alpha * (phi[i] - phi0[i]);
+}
+
+// _max_courant_number! (Solvers_0_functions.jl:267-276) + block max
+__global__ void k_courant(int n, const double* __restrict__ Ux, const double* __restrict__ Uy,
+                          const double* __restrict__ Uz, const double* __restrict__ dx, double dt, double* co) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double umag = sqrt(Ux[i] * Ux[i] + Uy[i] * Uy[i] + Uz[i] * Uz[i]);
+    co[i] = (umag * dt) / dx[i];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+void launch_assemble_U(cudaStream_t s, const MeshView& m, const CSRView& A, const double* mdot, const double* nueff,
+                       const double* const U[3], const double* const g[3], double* nz, double* diag0,
+                       double* const b[3], int time_scheme, int div_scheme, double dt) {
+    k_assemble_U<<<nblk(m.nC), TPB, 0, s>>>(m, A, mdot, nueff, U[0], U[1], U[2], g[0], g[1], g[2], nz, diag0, b[0],
+                                            b[1], b[2], time_scheme, div_scheme, dt);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_assemble_p(cudaStream_t s, const MeshView& m, const CSRView& A, const double* rDf, const double* divHv,
+                       double* nz, double* b) {
+    k_assemble_p<<<nblk(m.nC), TPB, 0, s>>>(m, A, rDf, divHv, nz, b);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_bc_relax_U(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, int comp,
+                       int div_scheme, double* nz, const double* diag0, double* b, const double* mdot,
+                       const double* nueff, const double* const U[3], double alpha, int flags) {
+    k_bc_relax_U<<<nblk(m.nC), TPB, 0, s>>>(m, A, bc, comp, div_scheme, nz, diag0, b, mdot, nueff, U[0], U[1], U[2],
+                                            alpha, flags);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_bc_p(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz, double* b,
+                 const double* rDf, const double* p) {
+    if (m.n_bcells == 0) return;
+    k_bc_p<<<nblk(m.n_bcells), TPB, 0, s>>>(m, A, bc, nz, b, rDf, p);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_set_reference(cudaStream_t s, const CSRView& A, double* nz, double* b, double pref) {
+    k_set_reference<<<1, 32, 0, s>>>(A, nz, b, pref);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_interp_U(cudaStream_t s, const MeshView& m, const BCView& bc, const double* const U[3], double* const Uf[3],
+                     double* mdot) {
+    k_interp_U<<<nblk(m.nF), TPB, 0, s>>>(m, bc, U[0], U[1], U[2], Uf ? Uf[0] : nullptr, Uf ? Uf[1] : nullptr,
+                                          Uf ? Uf[2] : nullptr, mdot);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_interp_scalar(cudaStream_t s, const MeshView& m, const BCView& bc, const double* phi, double* phif,
+                          double* nueff, double nu) {
+    k_interp_scalar<<<nblk(m.nF), TPB, 0, s>>>(m, bc, phi, phif, nueff, nu);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_interp_rD(cudaStream_t s, const MeshView& m, const BCView& bcU, const double* rD, double* rDf) {
+    k_interp_rD<<<nblk(m.nF), TPB, 0, s>>>(m, bcU, rD, rDf);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_fill(cudaStream_t s, double* a, double v, long n) {
+    if (n <= 0) return;
+    k_fill<<<(int)((n + TPB - 1) / TPB), TPB, 0, s>>>(a, v, n);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_green_gauss(cudaStream_t s, const MeshView& m, const double* phif, double* const g[3]) {
+    k_green_gauss<<<nblk(m.nC), TPB, 0, s>>>(m, phif, g[0], g[1], g[2]);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_green_gauss_tensor(cudaStream_t s, const MeshView& m, double* const Uf[3], double* const g[9],
+                               const double* Delta, double* nut) {
+    k_green_gauss_tensor<<<nblk(m.nC), TPB, 0, s>>>(m, Uf[0], Uf[1], Uf[2], g[0], g[1], g[2], g[3], g[4], g[5], g[6],
+                                                    g[7], g[8], Delta, nut);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_div(cudaStream_t s, const MeshView& m, const double* psif, double* out) {
+    k_div<<<nblk(m.nC), TPB, 0, s>>>(m, psif, out);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_rD_remove_H(cudaStream_t s, const MeshView& m, const CSRView& A, const double* nz,
+                        const double* const U[3], const double* const g[3], double* const b[3], double* rD,
+                        double* const H[3], int do_H) {
+    k_rD_remove_H<<<nblk(m.nC), TPB, 0, s>>>(m, A, nz, U[0], U[1], U[2], g[0], g[1], g[2], b[0], b[1], b[2], rD,
+                                             H[0], H[1], H[2], do_H);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_H(cudaStream_t s, const MeshView& m, const CSRView& A, const double* nz, const double* const U[3],
+              const double* const b[3], double* const H[3]) {
+    k_H<<<nblk(m.nC), TPB, 0, s>>>(m, A, nz, U[0], U[1], U[2], b[0], b[1], b[2], H[0], H[1], H[2]);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_correct_mdot(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bcp, const double* nz,
+                         const double* p, const double* rDf, double* mdot) {
+    k_correct_mdot<<<nblk(m.nF), TPB, 0, s>>>(m, A, bcp, nz, p, rDf, mdot);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_correct_U(cudaStream_t s, int n, double* const H[3], const double* const g[3], const double* rD,
+                      double* const U[3]) {
+    k_correct_U<<<nblk(n), TPB, 0, s>>>(n, H[0], H[1], H[2], g[0], g[1], g[2], rD, U[0], U[1], U[2]);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_relax_explicit(cudaStream_t s, int n, double* phi, const double* phi0, double alpha) {
+    k_relax_explicit<<<nblk(n), TPB, 0, s>>>(n, phi, phi0, alpha);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_courant(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* co) {
+    k_courant<<<nblk(n), TPB, 0, s>>>(n, U[0], U[1], U[2], dx, dt, co);
+    XCAL_CHECK_LAUNCH();
+}
+
+}  // namespace xcal

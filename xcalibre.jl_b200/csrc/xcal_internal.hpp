@@ -1,0 +1,150 @@
+// xcal_internal.hpp -- internal structures of libxcal_b200 (host + device).
+//
+// Data layout in HBM (structure of arrays, int32 indices, FP64 values):
+//   faces   : owner/neigh, area, delta, weight, Sf = area*normal (3), normal (3),
+//             |E_f| (Laplacian non-orthogonal magnitude, internal faces)
+//   cells   : volume, cell->internal-face CSR (face id, sign, CSR slot of the
+//             neighbour entry), cell->boundary-face CSR (ascending face id)
+//   CSR     : rowptr/colval per equation, diagonal slot per row, transpose
+//             slot per entry (DILU), owner->neighbour slot per internal face
+//   fields  : one array per component (vector fields component-major)
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/xcal_b200.h"
+
+namespace xcal {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define XCAL_CUDA(call)                                                                   \
+    do {                                                                                  \
+        cudaError_t _e = (call);                                                          \
+        if (_e != cudaSuccess)                                                            \
+            throw ::xcal::Error{_e == cudaErrorMemoryAllocation ? XCAL_ERR_OOM : XCAL_ERR_CUDA, \
+                                std::string(#call) + ": " + cudaGetErrorString(_e)};     \
+    } while (0)
+
+// number of kernels this library has launched (reported by xcal_get_launch_count)
+extern std::atomic<long long> g_launch_count;
+
+#define XCAL_CHECK_LAUNCH()                                              \
+    do {                                                                 \
+        ::xcal::g_launch_count.fetch_add(1, std::memory_order_relaxed); \
+        XCAL_CUDA(cudaGetLastError());                                   \
+    } while (0)
+
+inline void fail(int code, const std::string& m) { throw Error{code, m}; }
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count) XCAL_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    }
+    void zero(cudaStream_t s) {
+        if (n) XCAL_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    }
+    void upload(const T* host, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) XCAL_CUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
+};
+
+// ---------------------------------------------------------------------------
+// device views passed to kernels by value
+// ---------------------------------------------------------------------------
+struct MeshView {
+    int nC, nF, nB;
+    const int* owner;
+    const int* neigh;
+    const double* area;
+    const double* delta;
+    const double* weight;
+    const double* Sx;
+    const double* Sy;
+    const double* Sz;
+    const double* nx;
+    const double* ny;
+    const double* nz;
+    const double* Efmag;
+    const double* vol;
+    const int* cf_off;
+    const int* cf_face;
+    const int* cf_nb;
+    const signed char* cf_sign;
+    const int* bf_off;   // cell -> boundary faces (ascending)
+    const int* bf_face;
+    const int* bcell;    // boundary_cellsID
+    const int* bcells;   // list of cells that own boundary faces
+    int n_bcells;
+};
+
+struct CSRView {
+    int n;
+    const int* rowptr;
+    const int* colval;
+    const int* diag;   // diagonal slot per row
+    const int* trans;  // slot of (col,row) per entry
+    const int* cf_slot;   // slot of (cell, neighbour) per cell-face entry
+    const int* fslot;     // slot of (owner, neigh) per internal face (index f - nB)
+};
+
+// per boundary face BC table of one field (U, p or nut)
+struct BCView {
+    const signed char* type;   // [nB] XCAL_BC_* (0 = none)
+    const double* val;         // [nB*3] constant value (or DirichletFunction face values)
+    // periodic (parent faces and their shadows)
+    const int* peer_face;      // parent: partner face; shadow: parent face; else -1
+    const int* peer_cell;      // owner of the partner face
+    const double* pw;          // parent: w  (interpolation weight of own cell)
+    const double* pwn;         // parent: wn (weight of the partner cell)
+    const double* pEf;         // parent: |E_f| of the boundary face
+    const double* pDelta;      // parent: |C2 - C1| across the periodic pair
+    const double* pwdelta;     // parent: delta_p/(delta + delta_p) (rDf correction)
+    const int* pNN;            // parent: CSR slot (partner cell, partner cell)
+    const int* pNP;            // parent: CSR slot (partner cell, own cell)
+    const int* pPN;            // parent: CSR slot (own cell, partner cell)
+};
+
+// per-solve device scalars (Krylov state), one 128-byte aligned block
+struct alignas(128) KScalars {
+    double gamma, rNorm, eps, pNorm2, alpha, beta;   // CG
+    double rho, next_rho, omega, cv, resid, normb;   // BiCGSTAB / residual
+    double atol, rtol;
+    int iter, itmax, done, status;
+    unsigned int counter;                             // last-block ticket
+    unsigned int counter2;
+    int pad[6];
+};
+enum { KS_RUNNING = 0, KS_SOLVED = 1, KS_TIRED = 2, KS_ZERO_CURV = 3, KS_BREAKDOWN = 4, KS_ZERO_RHS = 5 };
+
+}  // namespace xcal
