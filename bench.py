@@ -1,0 +1,300 @@
+#!/usr/bin/env python
+"""Headline benchmark: SIMPLE outer iterations of the 128^3 (2,097,152-cell)
+steady laminar channel with randomly permuted cell/face numbering, FP64,
+through libxcal_b200 on one B200 per process.
+
+A "step" is one SIMPLE outer iteration of the whole case (momentum
+assembly + 3 BiCGSTAB/DILU solves, pressure assembly + CG/Jacobi solve,
+gradients, flux and velocity corrections).  Metric: Mcell-iters/s =
+cells x iterations / device seconds.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--size 128] [--precision fp64]
+
+--impl reference times the CPU restatement of the reference's path (the
+oracle; the Julia reference cannot run in this image) on the host cores.
+Multi-GPU: replicas only (independent cases, no collective in the path);
+rank 0 prints the line, `value` is the sum over ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-iters/s (FP64 vs mixed, resid 1e-6) at 2M cells; serve p50/p99 ms"
+UNIT = "Mcell-iters/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-iters", type=int, default=1, help="SIMPLE iterations in the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(n):
+    return f"channel {4}x1x1 box, {n}^3 hex = {n ** 3} cells, permuted numbering (seed 0), FP64 SIMPLE"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for ln in open(self.path):
+            p = [s.strip() for s in ln.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    """CPU restatement of the reference's path (the oracle), all host threads."""
+    world, rank, local = dist_setup(args)
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    import __graft_entry__ as ge
+    x = ge.load_package()
+    n = args.size
+    pm = x.channel_polymesh(n, n, n, seed=0)
+    om = orc.OracleMesh.from_polymesh(pm)
+    e = om.export()
+    mesh = x.Mesh3(patch_names=list(pm.patch_names), **e)
+    model, config = x.cases.channel_case(mesh, iterations=args.steps + args.warmup)
+    cfg, keep = x.build_config(model, config)
+    oc = orc.OracleCase(om, cfg)
+    cores = orc.threads()
+    # one untimed warm-up iteration (the CPU path has no JIT/caches to warm;
+    # more would only lengthen the run), then K timed iterations
+    oc.simple_iterate(min(args.warmup, 1))
+    t0 = time.perf_counter()
+    res, _ = oc.simple_iterate(args.steps)
+    dt = time.perf_counter() - t0
+    value = mesh.n_cells * args.steps / dt / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(n), "cells": mesh.n_cells, "precision": "fp64",
+                       "implementation": "CPU restatement of XCALibre.jl's path (C++/OpenMP oracle)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"SIMPLE iterations 2..{args.steps + 1} of the full case"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample(x, pm, mesh, iters):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    om = orc.OracleMesh.from_mesh3(mesh)
+    model, config = x.cases.channel_case(mesh, iterations=iters)
+    cfg, keep = x.build_config(model, config)
+    oc = orc.OracleCase(om, cfg)
+    t0 = time.perf_counter()
+    oc.simple_iterate(iters)
+    dt = time.perf_counter() - t0
+    return {"value": mesh.n_cells * iters / dt / 1e6, "unit": UNIT, "cores": orc.threads(), "kind": "port",
+            "sample": f"SIMPLE iterations 1..{iters} of the same {mesh.n_cells}-cell case from U=0, p=0 "
+                      f"({dt:.1f} s wall, C++ oracle with OpenMP over all host threads)"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    import __graft_entry__ as ge
+    x = ge.load_package()
+    A = x._abi
+    n = args.size
+    t_mesh = time.perf_counter()
+    pm = x.channel_polymesh(n, n, n, seed=0)
+    mesh = x.build_mesh3(pm)
+    t_mesh = time.perf_counter() - t_mesh
+    model, config = x.cases.channel_case(mesh, iterations=args.steps + args.warmup, precision=args.precision,
+                                         device=local)
+    cfg, keep = x.build_config(model, config)
+    ctx = x.Context(local)
+    t_setup = time.perf_counter()
+    dm = x.DeviceMesh(ctx, mesh)
+    case = x.Case(dm, cfg)
+    case.set_field(A.FIELD_U, model.momentum.U)
+    case.set_field(A.FIELD_P, model.momentum.p)
+    t_setup = time.perf_counter() - t_setup
+    nnz_p = case.nnz(A.EQN_P)
+    stream = torch.cuda.ExternalStream(case.stream(), device=torch.device("cuda", local))
+
+    # warm-up
+    case.simple_iterate(args.warmup)
+    torch.cuda.synchronize()
+    case.set_profiling(True)
+    prof0 = [case.profile(k) for k in range(3)]
+    l0 = x.launch_count()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res, _ = case.simple_iterate(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    launches = x.launch_count() - l0
+    prof1 = [case.profile(k) for k in range(3)]
+    case.set_profiling(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+    else:
+        ms_max = ms
+    cells_total = mesh.n_cells * world
+    value = cells_total * args.steps / (ms_max / 1e3) / 1e6
+
+    # roofline of the dominant kernel: CG SpMV + <p,Ap> (pressure solve)
+    spmv_ms = prof1[0][0] - prof0[0][0]
+    spmv_n = prof1[0][1] - prof0[0][1]
+    bytes_spmv = nnz_p * 12 + mesh.n_cells * 20  # nnz*(8+4) + n*(4 rowptr + 8 x + 8 y)
+    peak, peak_kind = measured_peak_hbm()
+    avg_s = spmv_ms / max(spmv_n, 1) / 1e3
+    achieved = bytes_spmv / avg_s / 1e9 if spmv_n else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    if os.path.exists(tp):
+        try:
+            tr = json.load(open(tp))
+            traffic = tr.get("bytes_per_launch_128") if n == 128 else None
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "kernel": "k_cg_spmv (CSR SpMV FP64 + p.Ap)", "achieved": achieved, "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+            "traffic": traffic, "bytes_per_launch": bytes_spmv, "launches": spmv_n,
+            "avg_launch_us": avg_s * 1e6, "share_of_step": spmv_ms / ms if ms else None}
+
+    # end-to-end through the C ABI with host buffers (copies in the timed region)
+    nC = mesh.n_cells
+    hU = torch.empty((3, nC), dtype=torch.float64, pin_memory=True).numpy()
+    hp = torch.empty(nC, dtype=torch.float64, pin_memory=True).numpy()
+    hU[:] = case.get_field(A.FIELD_U)
+    hp[:] = case.get_field(A.FIELD_P)
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        case.set_field(A.FIELD_U, hU)
+        case.set_field(A.FIELD_P, hp)
+        r, _ = case.simple_iterate(1)
+        hU[:] = case.get_field(A.FIELD_U)
+        hp[:] = case.get_field(A.FIELD_P)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": cells_total * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": 4 * nC * 8, "d2h_bytes_per_step": 4 * nC * 8 + 4 * 8,
+           "steps": args.e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(x, pm, mesh, args.cpu_iters)
+    tm = case.timings()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload_name(n), "cells": nC, "nnz_p": nnz_p, "precision": args.precision,
+                           "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                           "l2": "working set (matrices + face arrays, >1 GB) larger than L2; no flush",
+                           "mesh_build_s": round(t_mesh, 2), "setup_s": round(t_setup, 2)},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                "residuals_last": [float(v) for v in res[-1]] if len(res) else None,
+                "phases_ms_total": {"U_solve": tm[1], "p_solve": tm[2], "other": tm[3], "total": tm[5]}}
+        print(json.dumps(line), flush=True)
+    case.close()
+    dm.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

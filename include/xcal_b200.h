@@ -278,8 +278,17 @@ int32_t xcal_max_courant(xcal_case* cs, double* courant);
  * [0] assembly+BCs, [1] U Krylov, [2] p Krylov, [3] gradients/interp/flux,
  * [4] residuals, [5] total iterate; returns the number of entries written */
 int32_t xcal_get_timings(const xcal_case* cs, double* ms, int32_t n);
-/* number of kernel launches issued by this case since creation */
+/* number of kernel launches issued by this library since it was loaded
+ * (library-wide; cs may be NULL) */
 int32_t xcal_get_launch_count(const xcal_case* cs, int64_t* count);
+/* the cudaStream_t the case launches on (as void*), so a caller can record
+ * its own CUDA events around library calls */
+int32_t xcal_case_stream(const xcal_case* cs, void** stream);
+/* per-kernel CUDA-event timing of the dominant kernels (off by default).
+ * which: 0 = CG SpMV (+ p.Ap), 1 = BiCGSTAB SpMV, 2 = DILU sweep levels.
+ * ms = summed device time, launches = launches that did work. */
+int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable);
+int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,9 @@ SIGNATURES = {
     "xcal_max_courant": (_i32, [_vp, _pd]),
     "xcal_get_timings": (_i32, [_vp, _pd, _i32]),
     "xcal_get_launch_count": (_i32, [_vp, _pi64]),
+    "xcal_case_stream": (_i32, [_vp, C.POINTER(_vp)]),
+    "xcal_case_set_profiling": (_i32, [_vp, _i32]),
+    "xcal_case_get_profile": (_i32, [_vp, _i32, _pd, _pi64]),
 }
 
 _LIB = None

@@ -591,6 +591,21 @@ class Case:
         lib().xcal_get_timings(self.h, _abi.ptr(ms, C.c_double), 6)
         return ms
 
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._chk(lib().xcal_case_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def set_profiling(self, on: bool = True):
+        self._chk(lib().xcal_case_set_profiling(self.h, 1 if on else 0))
+
+    def profile(self, which: int):
+        """(summed device ms, launches) of a timed kernel class:
+        0 = CG SpMV, 1 = BiCGSTAB SpMV, 2 = DILU applications."""
+        ms, n = C.c_double(), C.c_int64()
+        self._chk(lib().xcal_case_get_profile(self.h, which, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
 
 def launch_count() -> int:
     n = C.c_int64()

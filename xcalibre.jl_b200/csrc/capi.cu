@@ -29,8 +29,6 @@ static int set_error(xcal_ctx* ctx, int code, const std::string& msg) {
         return set_error(ctx, XCAL_ERR_INVALID, e.what());                    \
     }
 
-static xcal_ctx* case_ctx(const xcal_case* cs) { return cs && cs->c ? cs->c->ctx : nullptr; }
-
 static int select_device(xcal_ctx* ctx) {
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return set_error(ctx, XCAL_ERR_CUDA, cudaGetErrorString(e));
@@ -278,8 +276,28 @@ int32_t xcal_get_timings(const xcal_case* cs, double* ms, int32_t n) {
 }
 
 int32_t xcal_get_launch_count(const xcal_case* cs, int64_t* count) {
-    if (!cs || !count) return XCAL_ERR_INVALID;
+    (void)cs;  // the count is library-wide; cs may be NULL
+    if (!count) return XCAL_ERR_INVALID;
     *count = g_launch_count.load();
+    return XCAL_OK;
+}
+
+int32_t xcal_case_stream(const xcal_case* cs, void** stream) {
+    if (!cs || !stream) return XCAL_ERR_INVALID;
+    *stream = (void*)cs->c->stream;
+    return XCAL_OK;
+}
+
+int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable) {
+    if (!cs) return XCAL_ERR_INVALID;
+    cs->c->profiling = enable != 0;
+    return XCAL_OK;
+}
+
+int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches) {
+    if (!cs || which < 0 || which > 2) return XCAL_ERR_INVALID;
+    if (ms) *ms = cs->c->prof_ms[which];
+    if (launches) *launches = cs->c->prof_n[which];
     return XCAL_OK;
 }
 

@@ -484,12 +484,21 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
 Case::~Case() {
     if (stream) cudaStreamSynchronize(stream);
     for (auto& e : ev) cudaEventDestroy(e);
+    for (auto& e : pev) cudaEventDestroy(e);
     if (h_S) cudaFreeHost(h_S);
     if (h_res) cudaFreeHost(h_res);
     if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
 void Case::sync() { XCAL_CUDA(cudaStreamSynchronize(stream)); }
+
+void Case::prof_reserve(int pairs) {
+    while ((int)pev.size() < 2 * pairs) {
+        cudaEvent_t e;
+        XCAL_CUDA(cudaEventCreate(&e));
+        pev.push_back(e);
+    }
+}
 
 double* Case::field_comp(int field, int comp, long& count) {
     count = mesh->nC;
@@ -628,8 +637,12 @@ double Case::solve_system(int eqn, int comp, int* iters) {
         for (;;) {
             if ((launched += chunk) > (long)hS->itmax + 64 + 32)
                 fail(XCAL_ERR_TIMEOUT, "CG did not report completion within itmax iterations");
+            int it0 = hS->iter;
+            if (profiling) prof_reserve(chunk);
             for (int c = 0; c < chunk; ++c) {
+                if (profiling) XCAL_CUDA(cudaEventRecord(pev[2 * c], stream));
                 kr_cg_spmv(stream, A, nz, pp, q, S, ws.part0.p);
+                if (profiling) XCAL_CUDA(cudaEventRecord(pev[2 * c + 1], stream));
                 if (pt == XCAL_PRECOND_JACOBI) {
                     kr_cg_update(stream, n, x, pp, r, q, zz, E.P.p, 1, S, ws.part0.p);
                 } else {
@@ -641,6 +654,17 @@ double Case::solve_system(int eqn, int comp, int* iters) {
             }
             XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
             sync();
+            if (profiling) {
+                // launches that did work: one per completed iteration, plus a
+                // final one that detected zero curvature
+                int real = hS->iter - it0 + (hS->status == KS_ZERO_CURV ? 1 : 0);
+                for (int c = 0; c < real && c < chunk; ++c) {
+                    float t = 0;
+                    XCAL_CUDA(cudaEventElapsedTime(&t, pev[2 * c], pev[2 * c + 1]));
+                    prof_ms[0] += t;
+                    prof_n[0] += 1;
+                }
+            }
             if (hS->done) break;
             if (chunk < 32) chunk *= 2;
         }
@@ -653,19 +677,44 @@ double Case::solve_system(int eqn, int comp, int* iters) {
         for (;;) {
             if ((launched += chunk) > (long)hS->itmax + 16 + 8)
                 fail(XCAL_ERR_TIMEOUT, "BiCGSTAB did not report completion within itmax iterations");
+            int it0 = hS->iter;
+            if (profiling) prof_reserve(3 * chunk);
             for (int c = 0; c < chunk; ++c) {
+                cudaEvent_t* e = profiling ? &pev[6 * c] : nullptr;
+                if (e) XCAL_CUDA(cudaEventRecord(e[0], stream));
                 kr_spmv(stream, A, nz, pp, q, S);
+                if (e) XCAL_CUDA(cudaEventRecord(e[1], stream));
                 apply_M(E, pt, q, v, S);
+                if (e) XCAL_CUDA(cudaEventRecord(e[2], stream));
                 kr_bicg_alpha(stream, n, b, v, S, ws.part0.p);
                 kr_bicg_s(stream, n, r, v, pp, s, x, S);
+                if (e) XCAL_CUDA(cudaEventRecord(e[3], stream));
                 kr_spmv(stream, A, nz, s, q, S);
+                if (e) XCAL_CUDA(cudaEventRecord(e[4], stream));
                 apply_M(E, pt, q, t, S);
+                if (e) XCAL_CUDA(cudaEventRecord(e[5], stream));
                 kr_bicg_omega(stream, n, t, s, S, ws.part0.p, ws.part1.p);
                 kr_bicg_xr(stream, n, x, s, t, r, b, S, ws.part0.p, ws.part1.p);
                 kr_bicg_p(stream, n, r, v, pp, S);
             }
             XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
             sync();
+            if (profiling) {
+                int real = hS->iter - it0;
+                for (int c = 0; c < real && c < chunk; ++c) {
+                    float t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+                    XCAL_CUDA(cudaEventElapsedTime(&t0, pev[6 * c], pev[6 * c + 1]));
+                    XCAL_CUDA(cudaEventElapsedTime(&t1, pev[6 * c + 3], pev[6 * c + 4]));
+                    XCAL_CUDA(cudaEventElapsedTime(&t2, pev[6 * c + 1], pev[6 * c + 2]));
+                    XCAL_CUDA(cudaEventElapsedTime(&t3, pev[6 * c + 4], pev[6 * c + 5]));
+                    prof_ms[1] += t0 + t1;
+                    prof_n[1] += 2;
+                    if (pt == XCAL_PRECOND_DILU) {
+                        prof_ms[2] += t2 + t3;
+                        prof_n[2] += 2;
+                    }
+                }
+            }
             if (hS->done) break;
             if (chunk < 8) chunk *= 2;
         }

@@ -78,6 +78,12 @@ struct Case {
     cudaEvent_t ev[8];
     KScalars* h_S = nullptr;  // pinned host mirror (2 entries)
     double* h_res = nullptr;  // pinned
+    // optional per-kernel event timing (xcal_case_set_profiling)
+    bool profiling = false;
+    std::vector<cudaEvent_t> pev;  // pairs, reused per polling chunk
+    double prof_ms[3] = {0, 0, 0};
+    long long prof_n[3] = {0, 0, 0};
+    void prof_reserve(int pairs);
 
     Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cfg);
     ~Case();

@@ -135,24 +135,46 @@ def build_mesh3(pm: PolyMesh) -> Mesh3:
     fo = pm.face_offsets.astype(np.int64)
     fsz = np.diff(fo)
     fn = pm.face_nodes.astype(np.int64)
-    face_of_node = np.repeat(np.arange(n_faces), fsz)
-    # raw entries: for each face, owner copies then neighbour copies
-    raw_cell = np.concatenate([owner[face_of_node], neigh_foam[face_of_node]])
-    raw_node = np.concatenate([fn, fn])
-    # global sequence: face-major, within a face owner block before neighbour block
-    pos_in_face = np.arange(fn.shape[0]) - fo[face_of_node]
-    seq_owner = 2 * fo[face_of_node] + pos_in_face
-    seq_neigh = 2 * fo[face_of_node] + fsz[face_of_node] + pos_in_face
-    raw_seq = np.concatenate([seq_owner, seq_neigh])
-    o = np.lexsort((raw_seq, raw_cell))
-    raw_cell, raw_node = raw_cell[o], raw_node[o]
-    key = raw_cell * (pm.points.shape[0] + 1) + raw_node
-    _, first = np.unique(key, return_index=True)
-    first = np.sort(first)
-    cn_cell = raw_cell[first]
-    cn_node = raw_node[first]
+    # Per cell, the raw node list is the node lists of its faces in foam face
+    # order (a boundary face's second, neighbour-role copy repeats nodes just
+    # added and is dropped by the dedup, so it is skipped here).  Dedup keeps
+    # first occurrences.  Done densely: one row per cell.
+    fcell = np.concatenate([owner, neigh_foam[:n_if]])
+    fidx = np.concatenate([np.arange(n_faces), np.arange(n_if)])
+    o = np.argsort(fcell * (n_faces + 1) + fidx, kind="stable")
+    fcell, fidx = fcell[o], fidx[o]
+    cf_cnt = np.bincount(fcell, minlength=n_cells)
+    cf_start = np.zeros(n_cells + 1, dtype=np.int64)
+    np.cumsum(cf_cnt, out=cf_start[1:])
+    pos = np.arange(fcell.shape[0]) - cf_start[fcell]      # face slot within its cell
+    node_cnt = np.zeros(n_cells, dtype=np.int64)
+    np.add.at(node_cnt, fcell, fsz[fidx])
+    maxraw = int(node_cnt.max())
+    # column offset of each (cell, face) entry inside the cell's row
+    col0 = np.zeros(fcell.shape[0], dtype=np.int64)
+    maxf = int(cf_cnt.max())
+    run = np.zeros(n_cells, dtype=np.int64)
+    for k in range(maxf):
+        sel = np.nonzero(pos == k)[0]
+        col0[sel] = run[fcell[sel]]
+        run[fcell[sel]] += fsz[fidx[sel]]
+    R = np.full((n_cells, maxraw), -1, dtype=np.int64)
+    maxn = int(fsz.max())
+    for j in range(maxn):
+        sel = np.nonzero(fsz[fidx] > j)[0]
+        R[fcell[sel], col0[sel] + j] = fn[fo[fidx[sel]] + j]
+    keep = R >= 0
+    for j in range(1, maxraw):
+        col = R[:, j]
+        dup = np.zeros(n_cells, dtype=bool)
+        for i in range(j):
+            dup |= (R[:, i] == col)
+        keep[:, j] &= ~dup
+    cn_node = R[keep]                                      # row-major: cell order, first-seen order
+    cn_cell = np.nonzero(keep)[0]
     cn_off = np.zeros(n_cells + 1, dtype=np.int64)
     np.cumsum(np.bincount(cn_cell, minlength=n_cells), out=cn_off[1:])
+    del R, keep
 
     # connect_face_nodes: boundary faces first, then internal faces
     src = np.concatenate([np.arange(n_if, n_faces), np.arange(n_if)])
