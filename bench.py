@@ -269,9 +269,11 @@ def main():
         t = torch.tensor([e2e_s], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {"value": cells_total * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
-           "h2d_bytes_per_step": 4 * nC * 8, "d2h_bytes_per_step": 4 * nC * 8 + 4 * 8,
-           "steps": args.e2e_steps}
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e = {"value": cells_total * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * nC * 8, "d2h_bytes_per_step": 4 * nC * 8 + 4 * 8,
+               "steps": args.e2e_steps}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

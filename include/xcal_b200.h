@@ -174,6 +174,45 @@ typedef struct {
     const xcal_bc* bc_nut;
 } xcal_config;
 
+/* ---- polyMesh input of the mesh importer --------------------------------
+ * The arrays an OpenFOAM constant/polyMesh directory holds (0-based), as read
+ * by read_FOAM3D (src/FoamMesh/FoamMesh_1_read.jl:1-23): internal faces
+ * first, then each patch's faces in patch order. */
+typedef struct {
+    int32_t n_points;
+    const double* points;         /* [3*n_points]                          */
+    int32_t n_faces;
+    const int32_t* face_offsets;  /* [n_faces+1] into face_nodes           */
+    const int32_t* face_nodes;    /* [face_offsets[n_faces]]               */
+    const int32_t* owner;         /* [n_faces]                             */
+    int32_t n_internal_faces;
+    const int32_t* neighbour;     /* [n_internal_faces]                    */
+    int32_t n_patches;
+    const int32_t* patch_sizes;   /* [n_patches] nFaces per patch          */
+} xcal_polymesh_desc;
+
+/* caller-owned output buffers of the importer (same layout as
+ * xcal_mesh_desc; sizes from xcal_foam_mesh_sizes) */
+typedef struct {
+    int32_t* face_owner;
+    int32_t* face_neigh;
+    double* face_centre;
+    double* face_normal;
+    double* face_e;
+    double* face_area;
+    double* face_delta;
+    double* face_weight;
+    double* cell_centre;
+    double* cell_volume;
+    int32_t* cell_faces_offset;
+    int32_t* cell_faces;
+    int32_t* cell_nsign;
+    int32_t* cell_neighbours;
+    int32_t* boundary_cellsID;
+    int32_t* patch_start;
+    int32_t* patch_count;
+} xcal_mesh_buffers;
+
 typedef struct xcal_ctx xcal_ctx;
 typedef struct xcal_mesh xcal_mesh;
 typedef struct xcal_case xcal_case;
@@ -186,6 +225,17 @@ int32_t xcal_ctx_destroy(xcal_ctx* ctx);
 const char* xcal_last_error(const xcal_ctx* ctx);
 /* library version string */
 const char* xcal_version(void);
+
+/* ---- mesh import (host) --------------------------------------------------*/
+/* FOAM3D_mesh (src/FoamMesh/FoamMesh_5_build.jl:21-27) without the file
+ * parsing: sizes[0..2] = n_cells, n_faces, n_bfaces of the Mesh3 built from
+ * the polyMesh.  Needs no GPU. */
+int32_t xcal_foam_mesh_sizes(const xcal_polymesh_desc* pm, int32_t* sizes);
+/* builds the Mesh3 contract (connectivity, boundary-first face order, fan
+ * geometry, weights, deltas, volumes; FoamMesh_2_connect.jl,
+ * FoamMesh_3_generate.jl, FoamMesh_4_geometry.jl, Mesh_1_functions.jl:20-51)
+ * into caller buffers.  Needs no GPU. */
+int32_t xcal_foam_mesh_build(const xcal_polymesh_desc* pm, const xcal_mesh_buffers* out);
 
 /* ---- mesh ----------------------------------------------------------------*/
 /* adapt(backend, mesh) (docs/src/user_guide/1_preprocessing.md:88): copies

@@ -65,6 +65,24 @@ class MeshDesc(C.Structure):
     ]
 
 
+class PolyMeshDesc(C.Structure):
+    _fields_ = [
+        ("n_points", C.c_int32), ("points", _pf64), ("n_faces", C.c_int32), ("face_offsets", _pi32),
+        ("face_nodes", _pi32), ("owner", _pi32), ("n_internal_faces", C.c_int32), ("neighbour", _pi32),
+        ("n_patches", C.c_int32), ("patch_sizes", _pi32),
+    ]
+
+
+class MeshBuffers(C.Structure):
+    _fields_ = [
+        ("face_owner", _pi32), ("face_neigh", _pi32), ("face_centre", _pf64), ("face_normal", _pf64),
+        ("face_e", _pf64), ("face_area", _pf64), ("face_delta", _pf64), ("face_weight", _pf64),
+        ("cell_centre", _pf64), ("cell_volume", _pf64), ("cell_faces_offset", _pi32), ("cell_faces", _pi32),
+        ("cell_nsign", _pi32), ("cell_neighbours", _pi32), ("boundary_cellsID", _pi32), ("patch_start", _pi32),
+        ("patch_count", _pi32),
+    ]
+
+
 class BCDesc(C.Structure):
     _fields_ = [
         ("type", C.c_int32), ("patch", C.c_int32), ("value", C.c_double * 3),

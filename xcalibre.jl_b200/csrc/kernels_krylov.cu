@@ -23,6 +23,79 @@ __device__ __forceinline__ double row_dot(const CSRView& A, const double* __rest
     return acc;
 }
 
+// Tile SpMV: out[k] = (A x)[row_k] for the thread's canonical rows
+// row_k = tile*RED_TILE + k*RED_THREADS + t.  The CSR segment of each
+// 256-row chunk is staged through shared memory with coalesced loads; each
+// thread then sums its row sequentially in CSR order (the reference's row
+// order), gathering x from L2.  Rows beyond n give 0.
+// Rows are computed by groups of 8 lanes: lane j of a group forms the
+// products of entries j, j+8, ... of the row (one rounding each, like the
+// scalar loop), and the group's first lane adds them in CSR order starting
+// from 0.0, so the sum is bit-identical to the sequential row walk.  A warp
+// covers 4 consecutive rows per round; each warp owns 256 consecutive rows of
+// the tile and unrolls 4 rounds for memory-level parallelism.
+constexpr int SPMV_G = 8;       // lanes per row
+constexpr int SPMV_UNROLL = 2;  // rounds in flight per warp
+struct SpmvSmem {
+    double q[RED_TILE];
+};
+
+__device__ __forceinline__ void tile_spmv(const CSRView& A, const double* __restrict__ nz,
+                                          const double* __restrict__ x, SpmvSmem& sm) {
+    const int row0 = blockIdx.x * RED_TILE;
+    const int nrows = min(RED_TILE, A.n - row0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / SPMV_G, j = lane % SPMV_G;
+    // warp w: rows [w*256, w*256+256) of the tile, 16 rows per unrolled step
+    for (int step = 0; step < RED_THREADS / (4 * SPMV_UNROLL); ++step) {
+        int rr[SPMV_UNROLL], b[SPMV_UNROLL], e[SPMV_UNROLL];
+        double prod[SPMV_UNROLL];
+#pragma unroll
+        for (int u = 0; u < SPMV_UNROLL; ++u) {
+            rr[u] = warp * RED_THREADS + step * (4 * SPMV_UNROLL) + u * 4 + g;
+            if (rr[u] < nrows) {
+                b[u] = __ldg(A.rowptr + row0 + rr[u]);
+                e[u] = __ldg(A.rowptr + row0 + rr[u] + 1);
+            } else {
+                b[u] = 0;
+                e[u] = 0;
+            }
+        }
+        double acc[SPMV_UNROLL];
+#pragma unroll
+        for (int u = 0; u < SPMV_UNROLL; ++u) acc[u] = 0.0;
+        // chunks of 8 entries (one chunk for rows of <= 8 entries)
+        int maxlen = 0;
+#pragma unroll
+        for (int u = 0; u < SPMV_UNROLL; ++u) maxlen = max(maxlen, e[u] - b[u]);
+        for (int off = 0; __any_sync(0xffffffffu, off < maxlen); off += SPMV_G) {
+#pragma unroll
+            for (int u = 0; u < SPMV_UNROLL; ++u) {
+                int idx = b[u] + off + j;
+                prod[u] = 0.0;
+                if (idx < e[u]) prod[u] = __ldcs(nz + idx) * __ldg(x + __ldcs(A.colval + idx));
+            }
+#pragma unroll
+            for (int u = 0; u < SPMV_UNROLL; ++u) {
+                int len = min(SPMV_G, e[u] - b[u] - off);
+#pragma unroll
+                for (int t = 0; t < SPMV_G; ++t) {
+                    double v = __shfl_sync(0xffffffffu, prod[u], g * SPMV_G + t);
+                    if (t < len) acc[u] = acc[u] + v;
+                }
+            }
+        }
+        if (j == 0) {
+#pragma unroll
+            for (int u = 0; u < SPMV_UNROLL; ++u)
+                if (rr[u] < nrows) sm.q[rr[u]] = acc[u];
+        }
+    }
+    __syncthreads();
+}
+// (A x) of the thread's canonical row k (valid after tile_spmv)
+__device__ __forceinline__ double tile_q(const SpmvSmem& sm, int k) { return sm.q[k * RED_THREADS + threadIdx.x]; }
+
 // CG stopping decisions after gamma_next = <r,z> (Krylov.jl cg!)
 __device__ void cg_finalize(KScalars* S, double gamma_next) {
     double rNorm = sqrt(gamma_next);
@@ -50,13 +123,16 @@ __device__ void cg_finalize(KScalars* S, double gamma_next) {
 // kernels (grid = one canonical tile per block, RED_THREADS threads)
 // ---------------------------------------------------------------------------
 // r = b - A*x0, x = 0, dx = x0 (warm start: Krylov.jl kaxpby!(n,1,b,-1,r))
-__global__ void k_init_resid(CSRView A, const double* __restrict__ nz, const double* __restrict__ b,
-                             const double* __restrict__ field, double* dx, double* x, double* r) {
+__global__ void __launch_bounds__(RED_THREADS, 8) k_init_resid(CSRView A, const double* __restrict__ nz,
+                                                            const double* __restrict__ b,
+                                                            const double* __restrict__ field, double* dx, double* x,
+                                                            double* r) {
+    __shared__ SpmvSmem sm;
+    tile_spmv(A, nz, field, sm);
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < A.n) {
-            double acc = row_dot(A, nz, field, i);
-            r[i] = b[i] - acc;
+            r[i] = b[i] - tile_q(sm, k);
             x[i] = 0.0;
             dx[i] = field[i];
         }
@@ -64,12 +140,14 @@ __global__ void k_init_resid(CSRView A, const double* __restrict__ nz, const dou
 }
 
 // y = A*x (plain SpMV, early exit when the solve is done)
-__global__ void k_spmv(CSRView A, const double* __restrict__ nz, const double* __restrict__ x, double* y,
-                       const KScalars* S) {
+__global__ void __launch_bounds__(RED_THREADS, 8) k_spmv(CSRView A, const double* __restrict__ nz,
+                                                      const double* __restrict__ x, double* y, const KScalars* S) {
     if (S && S->done) return;
+    __shared__ SpmvSmem sm;
+    tile_spmv(A, nz, x, sm);
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
-        if (i < A.n) y[i] = row_dot(A, nz, x, i);
+        if (i < A.n) y[i] = tile_q(sm, k);
     }
 }
 
@@ -134,15 +212,18 @@ __global__ void k_cg_start(int n, const double* __restrict__ r, const double* __
 }
 
 // q = A p; pAp = <p,q>; zero-curvature test; alpha = gamma / pAp
-__global__ void k_cg_spmv(CSRView A, const double* __restrict__ nz, const double* __restrict__ p, double* q,
-                          KScalars* S, double* part) {
+__global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const double* __restrict__ nz,
+                                                         const double* __restrict__ p, double* q, KScalars* S,
+                                                         double* part) {
     if (S->done) return;
     __shared__ double sm[8];
+    __shared__ SpmvSmem ssm;
+    tile_spmv(A, nz, p, ssm);
     double acc = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < A.n) {
-            double qi = row_dot(A, nz, p, i);
+            double qi = tile_q(ssm, k);
             q[i] = qi;
             acc = acc + p[i] * qi;
         }
@@ -460,14 +541,17 @@ __global__ void k_dilu_bwd(const int* __restrict__ rows, int nrows, CSRView A, c
 }
 
 // residual (src/Solve/Solve_1_api.jl:441-464): ||b - A x|| / max(||b||, 1 if tiny)
-__global__ void k_residual(CSRView A, const double* __restrict__ nz, const double* __restrict__ x,
-                           const double* __restrict__ b, KScalars* S, double* part0, double* part1, double* out) {
+__global__ void __launch_bounds__(RED_THREADS, 8) k_residual(CSRView A, const double* __restrict__ nz,
+                                                          const double* __restrict__ x, const double* __restrict__ b,
+                                                          KScalars* S, double* part0, double* part1, double* out) {
     __shared__ double sm[8];
+    __shared__ SpmvSmem ssm;
+    tile_spmv(A, nz, x, ssm);
     double a0 = 0.0, a1 = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < A.n) {
-            double fx = row_dot(A, nz, x, i);
+            double fx = tile_q(ssm, k);
             double bi = b[i];
             double d = bi - fx;
             a0 = a0 + d * d;
