@@ -23,19 +23,12 @@ __device__ __forceinline__ double row_dot(const CSRView& A, const double* __rest
     return acc;
 }
 
-// Tile SpMV: out[k] = (A x)[row_k] for the thread's canonical rows
-// row_k = tile*RED_TILE + k*RED_THREADS + t.  The CSR segment of each
-// 256-row chunk is staged through shared memory with coalesced loads; each
-// thread then sums its row sequentially in CSR order (the reference's row
-// order), gathering x from L2.  Rows beyond n give 0.
-// Rows are computed by groups of 8 lanes: lane j of a group forms the
-// products of entries j, j+8, ... of the row (one rounding each, like the
-// scalar loop), and the group's first lane adds them in CSR order starting
-// from 0.0, so the sum is bit-identical to the sequential row walk.  A warp
-// covers 4 consecutive rows per round; each warp owns 256 consecutive rows of
-// the tile and unrolls 4 rounds for memory-level parallelism.
-constexpr int SPMV_G = 8;       // lanes per row
-constexpr int SPMV_UNROLL = 2;  // rounds in flight per warp
+// Tile SpMV: the thread owning canonical row k (row = tile*RED_TILE +
+// k*RED_THREADS + t) sums that row sequentially in CSR order (the reference's
+// row order).  Each thread only reads back its own rows, so the staging array
+// needs no barrier.  (Measured on the 128^3 7-point pattern: one thread per
+// row beats lane-grouped rows and smem-staged segments; with random numbering
+// the x gathers, not the matrix stream, bound it.)
 struct SpmvSmem {
     double q[RED_TILE];
 };
@@ -44,54 +37,11 @@ __device__ __forceinline__ void tile_spmv(const CSRView& A, const double* __rest
                                           const double* __restrict__ x, SpmvSmem& sm) {
     const int row0 = blockIdx.x * RED_TILE;
     const int nrows = min(RED_TILE, A.n - row0);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int g = lane / SPMV_G, j = lane % SPMV_G;
-    // warp w: rows [w*256, w*256+256) of the tile, 16 rows per unrolled step
-    for (int step = 0; step < RED_THREADS / (4 * SPMV_UNROLL); ++step) {
-        int rr[SPMV_UNROLL], b[SPMV_UNROLL], e[SPMV_UNROLL];
-        double prod[SPMV_UNROLL];
 #pragma unroll
-        for (int u = 0; u < SPMV_UNROLL; ++u) {
-            rr[u] = warp * RED_THREADS + step * (4 * SPMV_UNROLL) + u * 4 + g;
-            if (rr[u] < nrows) {
-                b[u] = __ldg(A.rowptr + row0 + rr[u]);
-                e[u] = __ldg(A.rowptr + row0 + rr[u] + 1);
-            } else {
-                b[u] = 0;
-                e[u] = 0;
-            }
-        }
-        double acc[SPMV_UNROLL];
-#pragma unroll
-        for (int u = 0; u < SPMV_UNROLL; ++u) acc[u] = 0.0;
-        // chunks of 8 entries (one chunk for rows of <= 8 entries)
-        int maxlen = 0;
-#pragma unroll
-        for (int u = 0; u < SPMV_UNROLL; ++u) maxlen = max(maxlen, e[u] - b[u]);
-        for (int off = 0; __any_sync(0xffffffffu, off < maxlen); off += SPMV_G) {
-#pragma unroll
-            for (int u = 0; u < SPMV_UNROLL; ++u) {
-                int idx = b[u] + off + j;
-                prod[u] = 0.0;
-                if (idx < e[u]) prod[u] = __ldcs(nz + idx) * __ldg(x + __ldcs(A.colval + idx));
-            }
-#pragma unroll
-            for (int u = 0; u < SPMV_UNROLL; ++u) {
-                int len = min(SPMV_G, e[u] - b[u] - off);
-#pragma unroll
-                for (int t = 0; t < SPMV_G; ++t) {
-                    double v = __shfl_sync(0xffffffffu, prod[u], g * SPMV_G + t);
-                    if (t < len) acc[u] = acc[u] + v;
-                }
-            }
-        }
-        if (j == 0) {
-#pragma unroll
-            for (int u = 0; u < SPMV_UNROLL; ++u)
-                if (rr[u] < nrows) sm.q[rr[u]] = acc[u];
-        }
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int r = k * RED_THREADS + threadIdx.x;
+        if (r < nrows) sm.q[r] = row_dot(A, nz, x, row0 + r);
     }
-    __syncthreads();
 }
 // (A x) of the thread's canonical row k (valid after tile_spmv)
 __device__ __forceinline__ double tile_q(const SpmvSmem& sm, int k) { return sm.q[k * RED_THREADS + threadIdx.x]; }
