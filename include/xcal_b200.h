@@ -323,6 +323,26 @@ int32_t xcal_turbulence(xcal_case* cs);
 /* max_courant_number! (Solvers_0_functions.jl:253-276) */
 int32_t xcal_max_courant(xcal_case* cs, double* courant);
 
+/* ---- allocation-free residual ---------------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory (inside CUDA graph capture, under a fixed
+ * memory budget or a caller-managed pool).  Computes the scaled residual
+ * ||b - A x|| / ||b|| (||b|| replaced by 1 when it is at most eps(||b||)) of
+ * a CSR system -- the same arithmetic and reduction tree as the residual
+ * xcal_solve_system reports -- with every array (rowptr[n+1], colval, nzval,
+ * x[n], b[n]) and the result (one double) in device memory.  Runs on the
+ * calling thread's current device, on `stream` (NULL = legacy stream),
+ * without synchronising.  n is limited to 33,554,432 rows (larger n returns
+ * XCAL_ERR_INVALID).  It allocates nothing: its scratch is a fixed ~256 KiB
+ * device array inside the library, present on every GPU that loads it.  The
+ * first call on a device resolves that array's address, so make it before
+ * any stream capture.  Calls share the array: calls whose work overlaps on
+ * the GPU race and must be serialised by the caller.  err/errlen (may be
+ * NULL/0) receive a message on failure. */
+int32_t xcal_residual_noalloc(int32_t n, const int32_t* rowptr, const int32_t* colval, const double* nzval,
+                              const double* x, const double* b, double* result, void* stream, char* err,
+                              int32_t errlen);
+
 /* ---- timers --------------------------------------------------------------*/
 /* cumulative device time (ms) per phase since case creation:
  * [0] assembly+BCs, [1] U Krylov, [2] p Krylov, [3] gradients/interp/flux,
