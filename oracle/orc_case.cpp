@@ -62,10 +62,14 @@ static void spmv(const CSR& A, const std::vector<double>& x, std::vector<double>
     }
 }
 
-static double cdot(const std::vector<double>& a, const std::vector<double>& b) {
+// dot product summed in the canonical tree over the rows in order `ord`
+static double cdot(const int* ord, const std::vector<double>& a, const std::vector<double>& b) {
     const double* pa = a.data();
     const double* pb = b.data();
-    return creduce((int64_t)a.size(), [&](int64_t i) { return pa[i] * pb[i]; });
+    return creduce((int64_t)a.size(), [&](int64_t s) {
+        int64_t i = ord ? ord[s] : s;
+        return pa[i] * pb[i];
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -129,8 +133,11 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     C->cellsCourant.assign(nC, 0.0);
     C->bp.assign(nC, 0.0);
     build_pattern(*m, C->bcU, C->AU);
-    C->AU0 = C->AU;
     build_pattern(*m, C->bcP, C->Ap);
+    C->rorder = morton_order(m->ccentre);
+    C->AU.ord = C->rorder.data();
+    C->Ap.ord = C->rorder.data();
+    C->AU0 = C->AU;
     C->PU.assign(nC, 0.0);
     C->Pp.assign(nC, 0.0);
     // LES{Smagorinsky} initialise (LES_Smagorinsky.jl:84-101, LES_functions.jl:1-55)
@@ -618,7 +625,7 @@ static int krylov_cg(const CSR& A, const std::vector<double>& b, std::vector<dou
     std::vector<double>& z = MisI ? K.r : K.z;
     if (!MisI) apply_M(A, ptype, P, z, K.r);
     K.p = z;
-    double gamma = cdot(K.r, z);
+    double gamma = cdot(A.ord, K.r, z);
     double rNorm = std::sqrt(gamma);
     int iter = 0;
     if (gamma == 0.0) {
@@ -634,7 +641,7 @@ static int krylov_cg(const CSR& A, const std::vector<double>& b, std::vector<dou
     bool solved = rNorm <= eps_, tired = iter >= itmax, zero_curv = false;
     while (!(solved || tired || zero_curv)) {
         spmv(A, K.p, K.q);
-        double pAp = cdot(K.p, K.q);
+        double pAp = cdot(A.ord, K.p, K.q);
         if (pAp <= epsT * pNorm2) {
             if (std::fabs(pAp) <= epsT * pNorm2) zero_curv = true;
         }
@@ -643,7 +650,7 @@ static int krylov_cg(const CSR& A, const std::vector<double>& b, std::vector<dou
         for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + alpha * K.p[i];
         for (int i = 0; i < n; ++i) K.r[i] = K.r[i] + (-alpha) * K.q[i];
         if (!MisI) apply_M(A, ptype, P, z, K.r);
-        double gamma_next = cdot(K.r, z);
+        double gamma_next = cdot(A.ord, K.r, z);
         rNorm = std::sqrt(gamma_next);
         bool mach = (rNorm + 1.0 <= 1.0);
         solved = (rNorm <= eps_) || mach;
@@ -684,7 +691,7 @@ static int krylov_bicgstab(const CSR& A, const std::vector<double>& b, std::vect
         K.r = r0;
     K.p = K.r;
     const std::vector<double>& c = b;
-    double rNorm = std::sqrt(cdot(K.r, K.r));
+    double rNorm = std::sqrt(cdot(A.ord, K.r, K.r));
     int iter = 0;
     if (rNorm == 0.0) {
         for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + K.dx[i];
@@ -694,7 +701,7 @@ static int krylov_bicgstab(const CSR& A, const std::vector<double>& b, std::vect
     }
     int itmax = S.itmax == 0 ? 2 * n : S.itmax;
     double eps_ = S.atol + S.rtol * rNorm;
-    double next_rho = cdot(c, K.r);
+    double next_rho = cdot(A.ord, c,K.r);
     if (next_rho == 0.0) {
         for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + K.dx[i];
         field = K.x;
@@ -711,7 +718,7 @@ static int krylov_bicgstab(const CSR& A, const std::vector<double>& b, std::vect
             apply_M(A, ptype, P, K.v, K.q);
         else
             K.v = K.q;
-        double alpha = rho / cdot(c, K.v);
+        double alpha = rho / cdot(A.ord, c,K.v);
         for (int i = 0; i < n; ++i) K.s[i] = K.r[i] + (-alpha) * K.v[i];
         for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + alpha * K.p[i];
         spmv(A, K.s, d);  // d = A z, z = s
@@ -720,13 +727,13 @@ static int krylov_bicgstab(const CSR& A, const std::vector<double>& b, std::vect
         else
             K.t = d;
         std::vector<double>& tt = K.t;
-        double omega = cdot(tt, K.s) / cdot(tt, tt);
+        double omega = cdot(A.ord, tt,K.s) / cdot(A.ord, tt,tt);
         for (int i = 0; i < n; ++i) K.x[i] = K.x[i] + omega * K.s[i];
         for (int i = 0; i < n; ++i) K.r[i] = K.s[i] + (-omega) * tt[i];
-        next_rho = cdot(c, K.r);
+        next_rho = cdot(A.ord, c,K.r);
         double beta = (next_rho / rho) * (alpha / omega);
         for (int i = 0; i < n; ++i) K.p[i] = K.r[i] + beta * (K.p[i] + (-omega) * K.v[i]);
-        rNorm = std::sqrt(cdot(K.r, K.r));
+        rNorm = std::sqrt(cdot(A.ord, K.r, K.r));
         bool mach = (rNorm + 1.0 <= 1.0);
         solved = (rNorm <= eps_) || mach;
         tired = iter >= itmax;
@@ -744,11 +751,16 @@ static double residual(const CSR& A, const std::vector<double>& b, const std::ve
     spmv(A, x, Fx);
     const double* pb = b.data();
     const double* pf = Fx.data();
-    double sR = creduce(A.n, [&](int64_t i) {
+    const int* ord = A.ord;
+    double sR = creduce(A.n, [&](int64_t s) {
+        int64_t i = ord ? ord[s] : s;
         double d = pb[i] - pf[i];
         return d * d;
     });
-    double normb = std::sqrt(creduce(A.n, [&](int64_t i) { return pb[i] * pb[i]; }));
+    double normb = std::sqrt(creduce(A.n, [&](int64_t s) {
+        int64_t i = ord ? ord[s] : s;
+        return pb[i] * pb[i];
+    }));
     double denom = normb > jl_eps(normb) ? normb : 1.0;
     return std::sqrt(sR) / denom;
 }

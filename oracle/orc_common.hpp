@@ -114,6 +114,45 @@ inline double reduce_partials(const std::vector<double>& part) {
     return block_tree(acc);
 }
 
+// Row order of the canonical reductions over cells: ascending 63-bit Morton
+// key of the cell centre quantised to 21 bits per axis over the centres'
+// bounding box, ties by index (order[s] = cell at position s).  This is a
+// fixed summation order for the reference's `dot`/`sum`, whose own order is
+// left to BLAS; the device stores cells in this order.
+inline std::vector<int> morton_order(const std::vector<V3>& c) {
+    int n = (int)c.size();
+    double lo[3] = {c[0].x, c[0].y, c[0].z}, hi[3] = {c[0].x, c[0].y, c[0].z};
+    for (int i = 1; i < n; ++i) {
+        double v[3] = {c[i].x, c[i].y, c[i].z};
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], v[d]);
+            hi[d] = std::max(hi[d], v[d]);
+        }
+    }
+    auto bits = [](uint64_t q) {
+        uint64_t r = 0;
+        for (int b = 0; b < 21; ++b) r |= ((q >> b) & 1ULL) << (3 * b);
+        return r;
+    };
+    std::vector<uint64_t> key(n);
+    for (int i = 0; i < n; ++i) {
+        double v[3] = {c[i].x, c[i].y, c[i].z};
+        uint64_t q[3];
+        for (int d = 0; d < 3; ++d) {
+            double span = hi[d] - lo[d];
+            double u = span > 0.0 ? (v[d] - lo[d]) / span : 0.0;
+            double t = u * 2097151.0;
+            uint64_t qq = t > 0.0 ? (uint64_t)t : 0;
+            q[d] = qq > 2097151ULL ? 2097151ULL : qq;
+        }
+        key[i] = bits(q[0]) | (bits(q[1]) << 1) | (bits(q[2]) << 2);
+    }
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return key[a] != key[b] ? key[a] < key[b] : a < b; });
+    return order;
+}
+
 template <class F>
 inline double creduce(int64_t n, F f) {
     int64_t T = (n + RED_TILE - 1) / RED_TILE;

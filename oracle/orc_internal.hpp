@@ -38,6 +38,7 @@ struct CSR {
     std::vector<int> rowptr, colval;
     std::vector<double> nzval;
     std::vector<int> diag;  // diagonal_indices!
+    const int* ord = nullptr;  // row order of the canonical reductions (null: 0..n-1)
     int find(int i, int j) const;  // spindex (0-based, -1 when absent)
 };
 
@@ -73,6 +74,7 @@ struct Case {
     // preconditioners
     std::vector<double> PU, Pp;  // Jacobi storage (1/|A_ii|) or DILU D
     Krylov kU, kp;
+    std::vector<int> rorder;  // morton_order of the cell centres
     double time = 0.0;
     bool initialised = false;
     int iteration = 0;

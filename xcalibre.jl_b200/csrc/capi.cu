@@ -104,8 +104,15 @@ int32_t xcal_case_nnz(const xcal_case* cs, int32_t eqn, int64_t* nnz) {
 int32_t xcal_case_csr_pattern(const xcal_case* cs, int32_t eqn, int32_t* rowptr, int32_t* colval) {
     if (!cs || !rowptr || !colval || (eqn != XCAL_EQN_U && eqn != XCAL_EQN_P)) return XCAL_ERR_INVALID;
     const Equation& E = eqn == XCAL_EQN_U ? cs->c->U : cs->c->P;
-    std::memcpy(rowptr, E.rowptr.data(), E.rowptr.size() * sizeof(int32_t));
-    std::memcpy(colval, E.colval.data(), E.colval.size() * sizeof(int32_t));
+    const DevMesh& m = *cs->c->mesh;
+    // export in the original numbering (rows are stored in storage order)
+    rowptr[0] = 0;
+    long k = 0;
+    for (int i = 0; i < E.n; ++i) {
+        int st = m.inv[i];
+        for (int e = E.rowptr[st]; e < E.rowptr[st + 1]; ++e) colval[k++] = m.perm[E.colval[e]];
+        rowptr[i + 1] = (int32_t)k;
+    }
     return XCAL_OK;
 }
 
@@ -116,17 +123,26 @@ int32_t xcal_case_get_system(const xcal_case* cs, int32_t eqn, int32_t component
         const Equation& E = eqn == XCAL_EQN_U ? c->U : c->P;
         if (eqn == XCAL_EQN_U && (component < -1 || component > 2)) fail(XCAL_ERR_INVALID, "component");
         c->sync();
+        const DevMesh& m = *c->mesh;
         if (nzval) {
-            XCAL_CUDA(cudaMemcpy(nzval, E.nz.p, E.nnz * sizeof(double), cudaMemcpyDeviceToHost));
+            std::vector<double> nz(E.nnz);
+            XCAL_CUDA(cudaMemcpy(nz.data(), E.nz.p, E.nnz * sizeof(double), cudaMemcpyDeviceToHost));
             if (eqn == XCAL_EQN_U && component < 0) {
                 std::vector<double> d0(E.n);
                 XCAL_CUDA(cudaMemcpy(d0.data(), E.diag0.p, E.n * sizeof(double), cudaMemcpyDeviceToHost));
-                for (int i = 0; i < E.n; ++i) nzval[E.diag[i]] = d0[i];
+                for (int st = 0; st < E.n; ++st) nz[E.diag[st]] = d0[st];
+            }
+            long k = 0;
+            for (int i = 0; i < E.n; ++i) {
+                int st = m.inv[i];
+                for (int e = E.rowptr[st]; e < E.rowptr[st + 1]; ++e) nzval[k++] = nz[e];
             }
         }
         if (b) {
             int bc = eqn == XCAL_EQN_U ? (component < 0 ? 0 : component) : 0;
-            XCAL_CUDA(cudaMemcpy(b, E.b[bc].p, E.n * sizeof(double), cudaMemcpyDeviceToHost));
+            std::vector<double> tmp(E.n);
+            XCAL_CUDA(cudaMemcpy(tmp.data(), E.b[bc].p, E.n * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int i = 0; i < E.n; ++i) b[i] = tmp[m.inv[i]];
         }
     })
 }
@@ -143,13 +159,22 @@ static int field_io(xcal_case* cs, int32_t field, double* host, int64_t count, b
         c->field_comp(field, 0, per);
         if (count != (int64_t)ncomp * per) fail(XCAL_ERR_INVALID, "field size mismatch");
         c->sync();
+        // device arrays are in storage order; the ABI uses the original order
+        bool face = field == XCAL_FIELD_MDOTF || field == XCAL_FIELD_NUEFF || field == XCAL_FIELD_NUTF ||
+                    field == XCAL_FIELD_UF || field == XCAL_FIELD_PF || field == XCAL_FIELD_RDF;
+        const std::vector<int>& perm = face ? c->mesh->fperm : c->mesh->perm;
+        std::vector<double> tmp(per);
         for (int d = 0; d < ncomp; ++d) {
             long n = 0;
             double* p = c->field_comp(field, d, n);
-            if (set)
-                XCAL_CUDA(cudaMemcpy(p, host + (size_t)d * per, per * sizeof(double), cudaMemcpyHostToDevice));
-            else
-                XCAL_CUDA(cudaMemcpy(host + (size_t)d * per, p, per * sizeof(double), cudaMemcpyDeviceToHost));
+            double* h = host + (size_t)d * per;
+            if (set) {
+                for (long st = 0; st < per; ++st) tmp[st] = h[perm[st]];
+                XCAL_CUDA(cudaMemcpy(p, tmp.data(), per * sizeof(double), cudaMemcpyHostToDevice));
+            } else {
+                XCAL_CUDA(cudaMemcpy(tmp.data(), p, per * sizeof(double), cudaMemcpyDeviceToHost));
+                for (long st = 0; st < per; ++st) h[perm[st]] = tmp[st];
+            }
         }
     })
 }

@@ -57,9 +57,10 @@ CSRView Equation::view() const {
 }
 
 int Equation::find(int i, int j) const {
-    auto b = colval.begin() + rowptr[i], e = colval.begin() + rowptr[i + 1];
-    auto it = std::lower_bound(b, e, j);
-    return (it != e && *it == j) ? (int)(it - colval.begin()) : -1;
+    // rows are ordered by original column, not by storage column: linear scan
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e)
+        if (colval[e] == j) return e;
+    return -1;
 }
 
 BCView BCTable::view() const {
@@ -82,14 +83,136 @@ BCView BCTable::view() const {
 // ---------------------------------------------------------------------------
 // mesh upload
 // ---------------------------------------------------------------------------
-DevMesh* upload_mesh(const xcal_mesh_desc* d, cudaStream_t s) {
-    if (!d || d->n_cells <= 0 || d->n_faces <= 0 || d->n_bfaces < 0 || d->n_bfaces > d->n_faces)
+// Storage (locality) order of cells: ascending 63-bit Morton key of the cell
+// centre quantised to 21 bits per axis over the centres' bounding box, ties by
+// index.  perm[s] = original cell stored at position s.  The canonical
+// reduction tree runs over this order (the oracle uses the same definition).
+void locality_order(int n, const double* c, std::vector<int>& perm) {
+    double lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
+    for (int i = 1; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], c[3 * i + d]);
+            hi[d] = std::max(hi[d], c[3 * i + d]);
+        }
+    auto spread = [](uint64_t v) {  // 21 bits -> every third bit
+        v &= 0x1fffffULL;
+        v = (v | (v << 32)) & 0x1f00000000ffffULL;
+        v = (v | (v << 16)) & 0x1f0000ff0000ffULL;
+        v = (v | (v << 8)) & 0x100f00f00f00f00fULL;
+        v = (v | (v << 4)) & 0x10c30c30c30c30c3ULL;
+        v = (v | (v << 2)) & 0x1249249249249249ULL;
+        return v;
+    };
+    std::vector<uint64_t> key(n);
+    for (int i = 0; i < n; ++i) {
+        uint64_t q[3];
+        for (int d = 0; d < 3; ++d) {
+            double span = hi[d] - lo[d];
+            double u = span > 0.0 ? (c[3 * i + d] - lo[d]) / span : 0.0;
+            double t = u * 2097151.0;
+            uint64_t qq = t > 0.0 ? (uint64_t)t : 0;
+            q[d] = qq > 2097151ULL ? 2097151ULL : qq;
+        }
+        key[i] = spread(q[0]) | (spread(q[1]) << 1) | (spread(q[2]) << 2);
+    }
+    perm.resize(n);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] != key[b] ? key[a] < key[b] : a < b; });
+}
+
+static DevMesh* upload_mesh_ordered(const xcal_mesh_desc* d, cudaStream_t s, std::unique_ptr<DevMesh> m);
+
+DevMesh* upload_mesh(const xcal_mesh_desc* d0, cudaStream_t s) {
+    if (!d0 || d0->n_cells <= 0 || d0->n_faces <= 0 || d0->n_bfaces < 0 || d0->n_bfaces > d0->n_faces)
         fail(XCAL_ERR_INVALID, "mesh: invalid sizes");
-    if (!d->face_owner || !d->face_neigh || !d->face_normal || !d->face_area || !d->face_delta ||
-        !d->face_weight || !d->face_e || !d->cell_volume || !d->cell_faces_offset || !d->cell_faces ||
-        !d->cell_nsign || !d->cell_neighbours || !d->boundary_cellsID || !d->cell_centre || !d->face_centre)
+    if (!d0->face_owner || !d0->face_neigh || !d0->face_normal || !d0->face_area || !d0->face_delta ||
+        !d0->face_weight || !d0->face_e || !d0->cell_volume || !d0->cell_faces_offset || !d0->cell_faces ||
+        !d0->cell_nsign || !d0->cell_neighbours || !d0->boundary_cellsID || !d0->cell_centre || !d0->face_centre)
         fail(XCAL_ERR_INVALID, "mesh: missing array");
+    const int nC = d0->n_cells, nF = d0->n_faces, nB = d0->n_bfaces;
+    for (int f = 0; f < nF; ++f)
+        if (d0->face_owner[f] < 0 || d0->face_owner[f] >= nC || d0->face_neigh[f] < 0 || d0->face_neigh[f] >= nC)
+            fail(XCAL_ERR_INVALID, "mesh: face cell index out of range");
+    for (int f = 0; f < nB; ++f)
+        if (d0->boundary_cellsID[f] < 0 || d0->boundary_cellsID[f] >= nC)
+            fail(XCAL_ERR_INVALID, "mesh: boundary_cellsID out of range");
+    if (d0->cell_faces_offset[0] != 0 || d0->cell_faces_offset[nC] != 2 * (nF - nB))
+        fail(XCAL_ERR_INVALID, "mesh: cell_faces_offset mismatch");
+    for (int c = 0; c < nC; ++c)
+        if (d0->cell_faces_offset[c + 1] < d0->cell_faces_offset[c])
+            fail(XCAL_ERR_INVALID, "mesh: decreasing cell_faces_offset");
+    for (int k = 0; k < 2 * (nF - nB); ++k)
+        if (d0->cell_faces[k] < nB || d0->cell_faces[k] >= nF || d0->cell_neighbours[k] < 0 ||
+            d0->cell_neighbours[k] >= nC)
+            fail(XCAL_ERR_INVALID, "mesh: invalid cell_faces entry");
     auto m = std::make_unique<DevMesh>();
+    // cell order and face order (boundary faces keep their ids; internal faces
+    // follow their storage owner/neighbour)
+    locality_order(nC, d0->cell_centre, m->perm);
+    m->inv.resize(nC);
+    for (int st = 0; st < nC; ++st) m->inv[m->perm[st]] = st;
+    m->fperm.resize(nF);
+    std::iota(m->fperm.begin(), m->fperm.end(), 0);
+    std::sort(m->fperm.begin() + nB, m->fperm.end(), [&](int a, int b) {
+        int oa = m->inv[d0->face_owner[a]], ob = m->inv[d0->face_owner[b]];
+        if (oa != ob) return oa < ob;
+        int na = m->inv[d0->face_neigh[a]], nb = m->inv[d0->face_neigh[b]];
+        return na != nb ? na < nb : a < b;
+    });
+    m->finv.resize(nF);
+    for (int fs = 0; fs < nF; ++fs) m->finv[m->fperm[fs]] = fs;
+    // permuted copies of the Mesh3 arrays
+    std::vector<int> owner(nF), neigh(nF), cf_off(nC + 1, 0), cf(2 * (nF - nB)), nsign(2 * (nF - nB)),
+        nbr(2 * (nF - nB)), bcell(nB);
+    std::vector<double> fc(3 * (size_t)nF), fnrm(3 * (size_t)nF), fe(3 * (size_t)nF), area(nF), delta(nF), weight(nF),
+        cc(3 * (size_t)nC), vol(nC);
+    for (int fs = 0; fs < nF; ++fs) {
+        int f = m->fperm[fs];
+        owner[fs] = m->inv[d0->face_owner[f]];
+        neigh[fs] = m->inv[d0->face_neigh[f]];
+        for (int k = 0; k < 3; ++k) {
+            fc[3 * fs + k] = d0->face_centre[3 * f + k];
+            fnrm[3 * fs + k] = d0->face_normal[3 * f + k];
+            fe[3 * fs + k] = d0->face_e[3 * f + k];
+        }
+        area[fs] = d0->face_area[f];
+        delta[fs] = d0->face_delta[f];
+        weight[fs] = d0->face_weight[f];
+    }
+    for (int st = 0; st < nC; ++st) {
+        int c = m->perm[st];
+        for (int k = 0; k < 3; ++k) cc[3 * st + k] = d0->cell_centre[3 * c + k];
+        vol[st] = d0->cell_volume[c];
+        cf_off[st + 1] = cf_off[st] + (d0->cell_faces_offset[c + 1] - d0->cell_faces_offset[c]);
+        int k2 = cf_off[st];
+        for (int k = d0->cell_faces_offset[c]; k < d0->cell_faces_offset[c + 1]; ++k, ++k2) {
+            cf[k2] = m->finv[d0->cell_faces[k]];
+            nsign[k2] = d0->cell_nsign[k];
+            nbr[k2] = m->inv[d0->cell_neighbours[k]];
+        }
+    }
+    for (int f = 0; f < nB; ++f) bcell[f] = m->inv[d0->boundary_cellsID[f]];
+    xcal_mesh_desc d = *d0;
+    d.face_owner = owner.data();
+    d.face_neigh = neigh.data();
+    d.face_centre = fc.data();
+    d.face_normal = fnrm.data();
+    d.face_e = fe.data();
+    d.face_area = area.data();
+    d.face_delta = delta.data();
+    d.face_weight = weight.data();
+    d.cell_centre = cc.data();
+    d.cell_volume = vol.data();
+    d.cell_faces_offset = cf_off.data();
+    d.cell_faces = cf.data();
+    d.cell_nsign = nsign.data();
+    d.cell_neighbours = nbr.data();
+    d.boundary_cellsID = bcell.data();
+    return upload_mesh_ordered(&d, s, std::move(m));
+}
+
+// the Mesh3 arrays already in storage order
+static DevMesh* upload_mesh_ordered(const xcal_mesh_desc* d, cudaStream_t s, std::unique_ptr<DevMesh> m) {
     int nC = m->nC = d->n_cells, nF = m->nF = d->n_faces, nB = m->nB = d->n_bfaces;
     int nI = m->nI = nF - nB;
     m->owner.assign(d->face_owner, d->face_owner + nF);
@@ -222,18 +345,20 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
             extra[c2].push_back(c1);
         }
     }
+    // rows are stored in storage order; the entries of a row keep the
+    // reference's order (ascending ORIGINAL column), so row sums are unchanged
     E.rowptr.assign(n + 1, 0);
     E.colval.clear();
     E.colval.reserve((size_t)n + m.cf_face.size());
     std::vector<int> row;
     for (int c = 0; c < n; ++c) {
         row.clear();
-        row.push_back(c);
-        for (int k = m.cf_off[c]; k < m.cf_off[c + 1]; ++k) row.push_back(m.cf_nb[k]);
-        for (int j : extra[c]) row.push_back(j);
+        row.push_back(m.perm[c]);
+        for (int k = m.cf_off[c]; k < m.cf_off[c + 1]; ++k) row.push_back(m.perm[m.cf_nb[k]]);
+        for (int j : extra[c]) row.push_back(m.perm[j]);
         std::sort(row.begin(), row.end());
         row.erase(std::unique(row.begin(), row.end()), row.end());
-        E.colval.insert(E.colval.end(), row.begin(), row.end());
+        for (int j : row) E.colval.push_back(m.inv[j]);
         E.rowptr[c + 1] = (int)E.colval.size();
     }
     E.nnz = (long)E.colval.size();
@@ -268,9 +393,11 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
     if (need_dilu) {
         // dependency levels of the lower (ascending) and upper (descending)
         // triangular sweeps in the ORIGINAL numbering
+        // (rows visited in ascending original index; lvl indexed by storage row)
         std::vector<int> lvl(n, 0);
         int maxl = 0;
-        for (int i = 0; i < n; ++i) {
+        for (int io = 0; io < n; ++io) {
+            int i = m.inv[io];
             int l = 0;
             for (int e = E.rowptr[i]; e < E.diag[i]; ++e) l = std::max(l, lvl[E.colval[e]] + 1);
             lvl[i] = l;
@@ -287,7 +414,8 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
         E.d_lower_rows.upload(rows, s);
         std::fill(lvl.begin(), lvl.end(), 0);
         maxl = 0;
-        for (int i = n - 1; i >= 0; --i) {
+        for (int io = n - 1; io >= 0; --io) {
+            int i = m.inv[io];
             int l = 0;
             for (int e = E.diag[i] + 1; e < E.rowptr[i + 1]; ++e) l = std::max(l, lvl[E.colval[e]] + 1);
             lvl[i] = l;
@@ -573,7 +701,7 @@ void Case::bc_relax_U(int comp) {
 }
 
 void Case::set_reference() {
-    if (cfg.has_pref) launch_set_reference(stream, P.view(), P.nz.p, P.b[0].p, cfg.pref);
+    if (cfg.has_pref) launch_set_reference(stream, P.view(), P.nz.p, P.b[0].p, cfg.pref, mesh->inv[0]);
 }
 
 void Case::update_precond(int eqn) {

@@ -14,6 +14,9 @@ namespace xcal {
 // Mesh3 in HBM plus host copies needed to derive per-equation structures
 struct DevMesh {
     int nC = 0, nF = 0, nB = 0, nI = 0;
+    // storage order: perm[s] = original index stored at s, inv = its inverse
+    // (cells); fperm/finv likewise for faces (boundary faces are not moved)
+    std::vector<int> perm, inv, fperm, finv;
     // host copies (0-based)
     std::vector<int> owner, neigh, cf_off, cf_face, cf_nb, bcell, bf_off, bf_face, bcells, patch_start, patch_count;
     std::vector<signed char> cf_sign;

@@ -19,7 +19,7 @@ void launch_bc_relax_U(cudaStream_t s, const MeshView& m, const CSRView& A, cons
                        const double* nueff, const double* const U[3], double alpha, int flags);
 void launch_bc_p(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz, double* b,
                  const double* rDf, const double* p);
-void launch_set_reference(cudaStream_t s, const CSRView& A, double* nz, double* b, double pref);
+void launch_set_reference(cudaStream_t s, const CSRView& A, double* nz, double* b, double pref, int row);
 void launch_interp_U(cudaStream_t s, const MeshView& m, const BCView& bc, const double* const U[3],
                      double* const Uf[3], double* mdot);
 void launch_interp_scalar(cudaStream_t s, const MeshView& m, const BCView& bc, const double* phi, double* phif,

@@ -288,11 +288,11 @@ __global__ void k_bc_p(MeshView m, CSRView A, BCView bc, double* nz, double* b, 
     b[i] = bi;
 }
 
-// setReference! (Solve_1_api.jl:431-439)
-__global__ void k_set_reference(CSRView A, double* nz, double* b, double pref) {
+// setReference! (Solve_1_api.jl:431-439) on the row of the mesh's first cell
+__global__ void k_set_reference(CSRView A, double* nz, double* b, double pref, int row) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int c = A.diag[0];
-        b[0] = nz[c] * pref;
+        int c = A.diag[row];
+        b[row] = nz[c] * pref;
         nz[c] = nz[c] + nz[c];
     }
 }
@@ -703,8 +703,8 @@ void launch_bc_p(cudaStream_t s, const MeshView& m, const CSRView& A, const BCVi
     k_bc_p<<<nblk(m.n_bcells), TPB, 0, s>>>(m, A, bc, nz, b, rDf, p);
     XCAL_CHECK_LAUNCH();
 }
-void launch_set_reference(cudaStream_t s, const CSRView& A, double* nz, double* b, double pref) {
-    k_set_reference<<<1, 32, 0, s>>>(A, nz, b, pref);
+void launch_set_reference(cudaStream_t s, const CSRView& A, double* nz, double* b, double pref, int row) {
+    k_set_reference<<<1, 32, 0, s>>>(A, nz, b, pref, row);
     XCAL_CHECK_LAUNCH();
 }
 void launch_interp_U(cudaStream_t s, const MeshView& m, const BCView& bc, const double* const U[3], double* const Uf[3],
