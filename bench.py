@@ -229,10 +229,12 @@ def main():
     cells_total = mesh.n_cells * world
     value = cells_total * args.steps / (ms_max / 1e3) / 1e6
 
-    # roofline of the dominant kernel: CG SpMV + <p,Ap> (pressure solve)
+    # roofline of the dominant kernel: CG SpMV + <p,Ap> (pressure solve).  Per
+    # launch (k >= 1): values+columns nnz*(8+4), rowptr 4n, z and p_{k-1}
+    # 8n each, p_k and q written 8n each.
     spmv_ms = prof1[0][0] - prof0[0][0]
     spmv_n = prof1[0][1] - prof0[0][1]
-    bytes_spmv = nnz_p * 12 + mesh.n_cells * 20  # nnz*(8+4) + n*(4 rowptr + 8 x + 8 y)
+    bytes_spmv = nnz_p * 12 + mesh.n_cells * 36
     peak, peak_kind = measured_peak_hbm()
     avg_s = spmv_ms / max(spmv_n, 1) / 1e3
     achieved = bytes_spmv / avg_s / 1e9 if spmv_n else None
@@ -244,7 +246,7 @@ def main():
             traffic = tr.get("bytes_per_launch_128") if n == 128 else None
         except Exception:
             traffic = None
-    roof = {"bound": "hbm", "kernel": "k_cg_spmv (CSR SpMV FP64 + p.Ap)", "achieved": achieved, "peak": peak,
+    roof = {"bound": "hbm", "kernel": "k_cg_spmv (CSR SpMV FP64 fused with p = z + beta p and p.Ap)", "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
             "traffic": traffic, "bytes_per_launch": bytes_spmv, "launches": spmv_n,
             "avg_launch_us": avg_s * 1e6, "share_of_step": spmv_ms / ms if ms else None}

@@ -769,16 +769,16 @@ double Case::solve_system(int eqn, int comp, int* iters) {
             if (profiling) prof_reserve(chunk);
             for (int c = 0; c < chunk; ++c) {
                 if (profiling) XCAL_CUDA(cudaEventRecord(pev[2 * c], stream));
-                kr_cg_spmv(stream, A, nz, pp, q, S, ws.part0.p);
+                // p_k alternates between pp (even k) and v (odd k)
+                kr_cg_spmv(stream, A, nz, zz, pp, v, q, S, ws.part0.p);
                 if (profiling) XCAL_CUDA(cudaEventRecord(pev[2 * c + 1], stream));
                 if (pt == XCAL_PRECOND_JACOBI) {
-                    kr_cg_update(stream, n, x, pp, r, q, zz, E.P.p, 1, S, ws.part0.p);
+                    kr_cg_update(stream, n, x, pp, v, r, q, zz, E.P.p, 1, S, ws.part0.p);
                 } else {
-                    kr_cg_update(stream, n, x, pp, r, q, zz, E.P.p, 0, S, ws.part0.p);
+                    kr_cg_update(stream, n, x, pp, v, r, q, zz, E.P.p, 0, S, ws.part0.p);
                     if (pt == XCAL_PRECOND_DILU) dilu_ldiv(E, r, zz, S);
                     kr_cg_rz(stream, n, r, zz, S, ws.part0.p);
                 }
-                kr_cg_p(stream, n, zz, pp, S);
             }
             XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
             sync();

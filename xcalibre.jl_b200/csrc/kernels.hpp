@@ -49,12 +49,12 @@ void kr_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* x
 void kr_jacobi_apply(cudaStream_t s, int n, const double* P, const double* r, double* z, const KScalars* S);
 void kr_copy(cudaStream_t s, int n, const double* a, double* b, const KScalars* S);
 void kr_cg_start(cudaStream_t s, int n, const double* r, const double* z, double* p, KScalars* S, double* part);
-void kr_cg_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* p, double* q, KScalars* S,
-                double* part);
-void kr_cg_update(cudaStream_t s, int n, double* x, const double* p, double* r, const double* q, double* z,
-                  const double* P, int jacobi_fused, KScalars* S, double* part);
+// CG direction p_k lives in P0 (k even) / P1 (k odd); p_0 = z is stored in P0
+void kr_cg_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* z, double* P0, double* P1,
+                double* q, KScalars* S, double* part);
+void kr_cg_update(cudaStream_t s, int n, double* x, const double* P0, const double* P1, double* r, const double* q,
+                  double* z, const double* P, int jacobi_fused, KScalars* S, double* part);
 void kr_cg_rz(cudaStream_t s, int n, const double* r, const double* z, KScalars* S, double* part);
-void kr_cg_p(cudaStream_t s, int n, const double* z, double* p, const KScalars* S);
 void kr_finish(cudaStream_t s, int n, const double* x, const double* dx, double* field);
 void kr_bicg_start(cudaStream_t s, int n, const double* c, const double* r, double* p, KScalars* S, double* part0,
                    double* part1);

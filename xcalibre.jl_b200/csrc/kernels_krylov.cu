@@ -161,21 +161,42 @@ __global__ void k_cg_start(int n, const double* __restrict__ r, const double* __
     }
 }
 
-// q = A p; pAp = <p,q>; zero-curvature test; alpha = gamma / pAp
+// CG direction buffers alternate: iteration k uses p_k = P[k & 1].  cg_start
+// stores p_0 = z in P[0]; for k >= 1 the SpMV forms p_k = z + beta*p_{k-1}
+// on the fly (Krylov.jl kaxpby!(n, 1, z, beta, p) -- the same expression for
+// every reader, so gathered neighbours see bit-identical values) and the
+// thread owning a row stores it.  The separate p-update pass disappears.
+__device__ __forceinline__ double cg_dir(const double* __restrict__ z, const double* __restrict__ pold, double beta,
+                                         int j) {
+    return z[j] + beta * pold[j];
+}
+
+// q = A p_k; pAp = <p_k,q>; zero-curvature test; alpha = gamma / pAp
 __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const double* __restrict__ nz,
-                                                         const double* __restrict__ p, double* q, KScalars* S,
-                                                         double* part) {
+                                                         const double* __restrict__ z, double* P0, double* P1,
+                                                         double* q, KScalars* S, double* part) {
     if (S->done) return;
     __shared__ double sm[8];
-    __shared__ SpmvSmem ssm;
-    tile_spmv(A, nz, p, ssm);
+    const int it = S->iter;
+    const double beta = S->beta;
+    double* pk = (it & 1) ? P1 : P0;
+    const double* pold = (it & 1) ? P0 : P1;
     double acc = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < A.n) {
-            double qi = tile_q(ssm, k);
+            double qi = 0.0, pi;
+            int e1 = A.rowptr[i + 1];
+            if (it == 0) {
+                for (int e = A.rowptr[i]; e < e1; ++e) qi = qi + nz[e] * pk[A.colval[e]];
+                pi = pk[i];
+            } else {
+                for (int e = A.rowptr[i]; e < e1; ++e) qi = qi + nz[e] * cg_dir(z, pold, beta, A.colval[e]);
+                pi = cg_dir(z, pold, beta, i);
+                pk[i] = pi;
+            }
             q[i] = qi;
-            acc = acc + p[i] * qi;
+            acc = acc + pi * qi;
         }
     }
     double tot = block_tree(acc, sm);
@@ -194,11 +215,13 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const dou
     }
 }
 
-// x += alpha p; r -= alpha q; [Jacobi: z = P r; <r,z>; finalize]
-__global__ void k_cg_update(int n, double* x, const double* __restrict__ p, double* r, const double* __restrict__ q,
-                            double* z, const double* __restrict__ P, int jacobi_fused, KScalars* S, double* part) {
+// x += alpha p_k; r -= alpha q; [Jacobi: z = P r; <r,z>; finalize]
+__global__ void k_cg_update(int n, double* x, const double* __restrict__ P0, const double* __restrict__ P1,
+                            double* r, const double* __restrict__ q, double* z, const double* __restrict__ P,
+                            int jacobi_fused, KScalars* S, double* part) {
     if (S->done) return;
     __shared__ double sm[8];
+    const double* p = (S->iter & 1) ? P1 : P0;
     double alpha = S->alpha;
     double acc = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
@@ -237,16 +260,6 @@ __global__ void k_cg_rz(int n, const double* __restrict__ r, const double* __res
     if (!last_block(&S->counter)) return;
     double g = reduce_partials(part, gridDim.x, sm);
     if (threadIdx.x == 0) cg_finalize(S, g);
-}
-
-// p = z + beta p
-__global__ void k_cg_p(int n, const double* __restrict__ z, double* p, const KScalars* S) {
-    if (S->done) return;
-    double beta = S->beta;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) p[i] = z[i] + beta * p[i];
-    }
 }
 
 // field = x + dx (warm start shift)
@@ -554,22 +567,18 @@ void kr_cg_start(cudaStream_t s, int n, const double* r, const double* z, double
     k_cg_start<<<TILE_LAUNCH(n), s>>>(n, r, z, p, S, part);
     XCAL_CHECK_LAUNCH();
 }
-void kr_cg_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* p, double* q, KScalars* S,
-                double* part) {
-    k_cg_spmv<<<TILE_LAUNCH(A.n), s>>>(A, nz, p, q, S, part);
+void kr_cg_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* z, double* P0, double* P1,
+                double* q, KScalars* S, double* part) {
+    k_cg_spmv<<<TILE_LAUNCH(A.n), s>>>(A, nz, z, P0, P1, q, S, part);
     XCAL_CHECK_LAUNCH();
 }
-void kr_cg_update(cudaStream_t s, int n, double* x, const double* p, double* r, const double* q, double* z,
-                  const double* P, int jacobi_fused, KScalars* S, double* part) {
-    k_cg_update<<<TILE_LAUNCH(n), s>>>(n, x, p, r, q, z, P, jacobi_fused, S, part);
+void kr_cg_update(cudaStream_t s, int n, double* x, const double* P0, const double* P1, double* r, const double* q,
+                  double* z, const double* P, int jacobi_fused, KScalars* S, double* part) {
+    k_cg_update<<<TILE_LAUNCH(n), s>>>(n, x, P0, P1, r, q, z, P, jacobi_fused, S, part);
     XCAL_CHECK_LAUNCH();
 }
 void kr_cg_rz(cudaStream_t s, int n, const double* r, const double* z, KScalars* S, double* part) {
     k_cg_rz<<<TILE_LAUNCH(n), s>>>(n, r, z, S, part);
-    XCAL_CHECK_LAUNCH();
-}
-void kr_cg_p(cudaStream_t s, int n, const double* z, double* p, const KScalars* S) {
-    k_cg_p<<<TILE_LAUNCH(n), s>>>(n, z, p, S);
     XCAL_CHECK_LAUNCH();
 }
 void kr_finish(cudaStream_t s, int n, const double* x, const double* dx, double* field) {
