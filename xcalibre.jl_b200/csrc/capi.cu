@@ -97,7 +97,7 @@ int32_t xcal_case_destroy(xcal_case* cs) {
 
 int32_t xcal_case_nnz(const xcal_case* cs, int32_t eqn, int64_t* nnz) {
     if (!cs || !nnz || (eqn != XCAL_EQN_U && eqn != XCAL_EQN_P)) return XCAL_ERR_INVALID;
-    *nnz = eqn == XCAL_EQN_U ? cs->c->U.nnz : cs->c->P.nnz;
+    *nnz = eqn == XCAL_EQN_U ? cs->c->U.nnz_csr : cs->c->P.nnz_csr;
     return XCAL_OK;
 }
 
@@ -110,7 +110,7 @@ int32_t xcal_case_csr_pattern(const xcal_case* cs, int32_t eqn, int32_t* rowptr,
     long k = 0;
     for (int i = 0; i < E.n; ++i) {
         int st = m.inv[i];
-        for (int e = E.rowptr[st]; e < E.rowptr[st + 1]; ++e) colval[k++] = m.perm[E.colval[e]];
+        for (int q = 0; q < E.len[st]; ++q) colval[k++] = m.perm[E.colval[E.base(st) + SELL_C * q]];
         rowptr[i + 1] = (int32_t)k;
     }
     return XCAL_OK;
@@ -135,7 +135,7 @@ int32_t xcal_case_get_system(const xcal_case* cs, int32_t eqn, int32_t component
             long k = 0;
             for (int i = 0; i < E.n; ++i) {
                 int st = m.inv[i];
-                for (int e = E.rowptr[st]; e < E.rowptr[st + 1]; ++e) nzval[k++] = nz[e];
+                for (int q = 0; q < E.len[st]; ++q) nzval[k++] = nz[E.base(st) + SELL_C * q];
             }
         }
         if (b) {

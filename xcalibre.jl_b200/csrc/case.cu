@@ -47,7 +47,8 @@ MeshView DevMesh::view() const {
 CSRView Equation::view() const {
     CSRView v;
     v.n = n;
-    v.rowptr = d_rowptr.p;
+    v.slice = d_slice.p;
+    v.len = d_len.p;
     v.colval = d_colval.p;
     v.diag = d_diag.p;
     v.trans = d_trans.p;
@@ -58,8 +59,9 @@ CSRView Equation::view() const {
 
 int Equation::find(int i, int j) const {
     // rows are ordered by original column, not by storage column: linear scan
-    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e)
-        if (colval[e] == j) return e;
+    int b = base(i);
+    for (int k = 0; k < len[i]; ++k)
+        if (colval[b + SELL_C * k] == j) return b + SELL_C * k;
     return -1;
 }
 
@@ -347,10 +349,9 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
     }
     // rows are stored in storage order; the entries of a row keep the
     // reference's order (ascending ORIGINAL column), so row sums are unchanged
-    E.rowptr.assign(n + 1, 0);
-    E.colval.clear();
-    E.colval.reserve((size_t)n + m.cf_face.size());
+    std::vector<std::vector<int>> rows_s(n);
     std::vector<int> row;
+    E.nnz_csr = 0;
     for (int c = 0; c < n; ++c) {
         row.clear();
         row.push_back(m.perm[c]);
@@ -358,19 +359,40 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
         for (int j : extra[c]) row.push_back(m.perm[j]);
         std::sort(row.begin(), row.end());
         row.erase(std::unique(row.begin(), row.end()), row.end());
-        for (int j : row) E.colval.push_back(m.inv[j]);
-        E.rowptr[c + 1] = (int)E.colval.size();
+        if (row.size() > 255) fail(XCAL_ERR_UNSUPPORTED, "a matrix row has more than 255 entries");
+        for (int j : row) rows_s[c].push_back(m.inv[j]);
+        E.nnz_csr += (long)row.size();
     }
-    E.nnz = (long)E.colval.size();
+    // SELL-32 layout: slice width = longest row of the slice
+    int nsl = (n + SELL_C - 1) / SELL_C;
+    E.slice.assign(nsl + 1, 0);
+    E.len.resize(n);
+    for (int sl = 0; sl < nsl; ++sl) {
+        size_t w = 0;
+        for (int r = sl * SELL_C; r < std::min(n, (sl + 1) * SELL_C); ++r) w = std::max(w, rows_s[r].size());
+        if ((long)E.slice[sl] + (long)SELL_C * (long)w > 2147483647L) fail(XCAL_ERR_UNSUPPORTED, "matrix too large");
+        E.slice[sl + 1] = E.slice[sl] + SELL_C * (int)w;
+    }
+    E.nnz = E.slice[nsl];
+    E.colval.assign(E.nnz, 0);
+    for (int r = 0; r < n; ++r) {
+        E.len[r] = (unsigned char)rows_s[r].size();
+        int b = E.base(r);
+        for (int k = 0; k < E.len[r]; ++k) E.colval[b + SELL_C * k] = rows_s[r][k];
+        for (int k = E.len[r]; b + SELL_C * k < E.slice[r / SELL_C + 1]; ++k) E.colval[b + SELL_C * k] = r;
+    }
+    rows_s.clear();
+    rows_s.shrink_to_fit();
     E.diag.resize(n);
     for (int c = 0; c < n; ++c) E.diag[c] = E.find(c, c);
-    std::vector<int> trans(E.nnz), cf_slot(m.cf_face.size()), fslot(m.nI);
+    std::vector<int> trans(E.nnz, 0), cf_slot(m.cf_face.size()), fslot(m.nI);
     for (int i = 0; i < n; ++i)
-        for (int e = E.rowptr[i]; e < E.rowptr[i + 1]; ++e) trans[e] = E.find(E.colval[e], i);
+        for (int k = 0, b = E.base(i); k < E.len[i]; ++k) trans[b + SELL_C * k] = E.find(E.colval[b + SELL_C * k], i);
     for (int c = 0; c < n; ++c)
         for (int k = m.cf_off[c]; k < m.cf_off[c + 1]; ++k) cf_slot[k] = E.find(c, m.cf_nb[k]);
     for (int f = m.nB; f < m.nF; ++f) fslot[f - m.nB] = E.find(m.owner[f], m.neigh[f]);
-    E.d_rowptr.upload(E.rowptr, s);
+    E.d_slice.upload(E.slice, s);
+    E.d_len.upload(E.len, s);
     E.d_colval.upload(E.colval, s);
     E.d_diag.upload(E.diag, s);
     E.d_trans.upload(trans, s);
@@ -399,7 +421,7 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
         for (int io = 0; io < n; ++io) {
             int i = m.inv[io];
             int l = 0;
-            for (int e = E.rowptr[i]; e < E.diag[i]; ++e) l = std::max(l, lvl[E.colval[e]] + 1);
+            for (int e = E.base(i); e < E.diag[i]; e += SELL_C) l = std::max(l, lvl[E.colval[e]] + 1);
             lvl[i] = l;
             maxl = std::max(maxl, l);
         }
@@ -417,7 +439,8 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
         for (int io = n - 1; io >= 0; --io) {
             int i = m.inv[io];
             int l = 0;
-            for (int e = E.diag[i] + 1; e < E.rowptr[i + 1]; ++e) l = std::max(l, lvl[E.colval[e]] + 1);
+            for (int e = E.diag[i] + SELL_C; e < E.base(i) + SELL_C * E.len[i]; e += SELL_C)
+                l = std::max(l, lvl[E.colval[e]] + 1);
             lvl[i] = l;
             maxl = std::max(maxl, l);
         }

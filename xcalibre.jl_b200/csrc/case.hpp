@@ -31,8 +31,12 @@ struct DevMesh {
 struct Equation {
     int n = 0;
     long nnz = 0;
-    std::vector<int> rowptr, colval, diag;  // host pattern
-    DBuf<int> d_rowptr, d_colval, d_diag, d_trans, d_cf_slot, d_fslot;
+    long nnz_csr = 0;                       // entries without SELL padding
+    std::vector<int> slice, colval, diag;   // host pattern (SELL-32, storage rows)
+    std::vector<unsigned char> len;
+    DBuf<int> d_slice, d_colval, d_diag, d_trans, d_cf_slot, d_fslot;
+    DBuf<unsigned char> d_len;
+    int base(int r) const { return slice[r / SELL_C] + r % SELL_C; }
     DBuf<double> nz, nz0, diag0, P;
     DBuf<double> b[3];
     // DILU level schedules (rows grouped by dependency level)

@@ -259,7 +259,11 @@ __global__ void k_bc_relax_U(MeshView m, CSRView A, BCView bc, int comp, int div
         return;
     }
     double sumv = 0.0;
-    for (int e = A.rowptr[i]; e < A.rowptr[i + 1]; ++e) sumv = sumv + fabs(e == ds ? d : nz[e]);
+    const int rb = row_base(A, i), rl = A.len[i];
+    for (int k = 0; k < rl; ++k) {
+        int e = rb + SELL_C * k;
+        sumv = sumv + fabs(e == ds ? d : nz[e]);
+    }
     sumv = sumv - fabs(d);
     double D0 = d;
     double Dmax = jl_max(fabs(D0), sumv) / alpha;
@@ -566,7 +570,9 @@ __global__ void k_rD_remove_H(MeshView m, CSRView A, const double* __restrict__ 
     bz[i] = bzi;
     if (!do_H) return;
     double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int e = A.rowptr[i]; e < A.rowptr[i + 1]; ++e) {
+    const int rb = row_base(A, i), rl = A.len[i];
+    for (int k = 0; k < rl; ++k) {
+        int e = rb + SELL_C * k;
         int j = A.colval[e];
         double val = nz[e];
         sx = sx + val * Ux[j];
@@ -590,7 +596,9 @@ __global__ void k_H(MeshView m, CSRView A, const double* __restrict__ nz, const 
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.nC) return;
     double sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int e = A.rowptr[i]; e < A.rowptr[i + 1]; ++e) {
+    const int rb = row_base(A, i), rl = A.len[i];
+    for (int k = 0; k < rl; ++k) {
+        int e = rb + SELL_C * k;
         int j = A.colval[e];
         double val = nz[e];
         sx = sx + val * Ux[j];

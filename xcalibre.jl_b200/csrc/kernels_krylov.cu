@@ -18,8 +18,11 @@ __device__ __forceinline__ double row_dot(const CSRView& A, const double* __rest
                                           const double* __restrict__ x, int i) {
     // xmul! row (src/Multithread/spmvm.jl:47-53): sequential from 0.0
     double acc = 0.0;
-    int e1 = A.rowptr[i + 1];
-    for (int e = A.rowptr[i]; e < e1; ++e) acc = acc + nz[e] * x[A.colval[e]];
+    const int rb = row_base(A, i), rl = A.len[i];
+    for (int k = 0; k < rl; ++k) {
+        int e = rb + SELL_C * k;
+        acc = acc + nz[e] * x[A.colval[e]];
+    }
     return acc;
 }
 
@@ -186,12 +189,12 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const dou
         int i = tile_row(k);
         if (i < A.n) {
             double qi = 0.0, pi;
-            int e1 = A.rowptr[i + 1];
+            const int rb = row_base(A, i), e1 = rb + SELL_C * A.len[i];
             if (it == 0) {
-                for (int e = A.rowptr[i]; e < e1; ++e) qi = qi + nz[e] * pk[A.colval[e]];
+                for (int e = rb; e < e1; e += SELL_C) qi = qi + nz[e] * pk[A.colval[e]];
                 pi = pk[i];
             } else {
-                for (int e = A.rowptr[i]; e < e1; ++e) qi = qi + nz[e] * cg_dir(z, pold, beta, A.colval[e]);
+                for (int e = rb; e < e1; e += SELL_C) qi = qi + nz[e] * cg_dir(z, pold, beta, A.colval[e]);
                 pi = cg_dir(z, pold, beta, i);
                 pk[i] = pi;
             }
@@ -465,7 +468,7 @@ __global__ void k_dilu_D(const int* __restrict__ rows, int nrows, CSRView A, con
     int i = rows[t];
     int ds = A.diag[i];
     double d = nz[ds];
-    for (int e = A.rowptr[i]; e < ds; ++e) {
+    for (int e = row_base(A, i); e < ds; e += SELL_C) {
         int j = A.colval[e];
         d = d - (nz[A.trans[e]] * nz[e]) / D[j];
     }
@@ -482,7 +485,7 @@ __global__ void k_dilu_fwd(const int* __restrict__ rows, int nrows, CSRView A, c
     int i = rows[t];
     int ds = A.diag[i];
     double sum = 0.0;
-    for (int e = A.rowptr[i]; e < ds; ++e) {
+    for (int e = row_base(A, i); e < ds; e += SELL_C) {
         int j = A.colval[e];
         sum = sum + (nz[e] * y[j]) * (1.0 / D[j]);
     }
@@ -498,8 +501,8 @@ __global__ void k_dilu_bwd(const int* __restrict__ rows, int nrows, CSRView A, c
     int i = rows[t];
     int ds = A.diag[i];
     double sum = 0.0;
-    int e1 = A.rowptr[i + 1];
-    for (int e = ds + 1; e < e1; ++e) sum = sum + nz[e] * x[A.colval[e]];
+    int e1 = row_base(A, i) + SELL_C * A.len[i];
+    for (int e = ds + SELL_C; e < e1; e += SELL_C) sum = sum + nz[e] * x[A.colval[e]];
     x[i] = (x[i] - sum) / D[i];
 }
 

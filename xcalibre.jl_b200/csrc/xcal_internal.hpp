@@ -108,15 +108,27 @@ struct MeshView {
     int n_bcells;
 };
 
+// Sparse matrices are stored SELL-32: rows in slices of 32 consecutive
+// (storage) rows, each slice entry-major -- entry k of row r lives at
+// slice[r/32] + (r%32) + 32*k -- so a warp reading entry k of its 32 rows
+// issues one fully coalesced access.  Entries of a row stay in the
+// reference's CSR order (ascending original column); padding entries (up to
+// the slice's longest row) are never read.
+constexpr int SELL_C = 32;
 struct CSRView {
     int n;
-    const int* rowptr;
+    const int* slice;          // [ceil(n/32)+1] first slot of each slice
+    const unsigned char* len;  // [n] entries per row
     const int* colval;
     const int* diag;   // diagonal slot per row
     const int* trans;  // slot of (col,row) per entry
     const int* cf_slot;   // slot of (cell, neighbour) per cell-face entry
     const int* fslot;     // slot of (owner, neigh) per internal face (index f - nB)
 };
+// slot of entry 0 of row r (entry k is at row_base + SELL_C*k)
+__host__ __device__ __forceinline__ int row_base(const CSRView& A, int r) {
+    return A.slice[r / SELL_C] + (r % SELL_C);
+}
 
 // per boundary face BC table of one field (U, p or nut)
 struct BCView {
