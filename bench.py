@@ -200,7 +200,7 @@ def main():
     case.simple_iterate(args.warmup)
     torch.cuda.synchronize()
     case.set_profiling(True)
-    prof0 = [case.profile(k) for k in range(3)]
+    prof0 = [case.profile(k) for k in range(5)]
     l0 = x.launch_count()
     clocks = ClockSampler(local)
     clocks.start()
@@ -218,7 +218,7 @@ def main():
         torch.distributed.barrier()
     clk = clocks.stop()
     launches = x.launch_count() - l0
-    prof1 = [case.profile(k) for k in range(3)]
+    prof1 = [case.profile(k) for k in range(5)]
     case.set_profiling(False)
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -234,6 +234,7 @@ def main():
     # 8n each, p_k and q written 8n each.
     spmv_ms = prof1[0][0] - prof0[0][0]
     spmv_n = prof1[0][1] - prof0[0][1]
+    spmv_all = prof1[4][1] - prof0[4][1]  # every CG SpMV launch that did work
     bytes_spmv = nnz_p * 12 + mesh.n_cells * 36
     peak, peak_kind = measured_peak_hbm()
     avg_s = spmv_ms / max(spmv_n, 1) / 1e3
@@ -248,8 +249,18 @@ def main():
             traffic = None
     roof = {"bound": "hbm", "kernel": "k_cg_spmv (CSR SpMV FP64 fused with p = z + beta p and p.Ap)", "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-            "traffic": traffic, "bytes_per_launch": bytes_spmv, "launches": spmv_n,
-            "avg_launch_us": avg_s * 1e6, "share_of_step": spmv_ms / ms if ms else None}
+            "traffic": traffic, "bytes_per_launch": bytes_spmv, "launches_timed": spmv_n,
+            "launches_total": spmv_all, "avg_launch_us": avg_s * 1e6,
+            "share_of_step": avg_s * 1e3 * spmv_all / ms if ms else None}
+    # second kernel of each CG iteration: x += alpha p; r -= alpha q; z = P r;
+    # <r,z> -- reads x, p, r, q, P and writes x, r, z: 64 bytes per row
+    upd_ms = prof1[3][0] - prof0[3][0]
+    upd_n = prof1[3][1] - prof0[3][1]
+    if upd_n:
+        upd_s = upd_ms / upd_n / 1e3
+        roof["cg_update"] = {"avg_launch_us": upd_s * 1e6, "bytes_per_launch": 64 * mesh.n_cells,
+                             "achieved": 64 * mesh.n_cells / upd_s / 1e9, "launches_timed": upd_n,
+                             "share_of_step": upd_s * 1e3 * spmv_all / ms if ms else None}
 
     # end-to-end through the C ABI with host buffers (copies in the timed region)
     nC = mesh.n_cells

@@ -355,8 +355,11 @@ int32_t xcal_get_launch_count(const xcal_case* cs, int64_t* count);
  * its own CUDA events around library calls */
 int32_t xcal_case_stream(const xcal_case* cs, void** stream);
 /* per-kernel CUDA-event timing of the dominant kernels (off by default).
- * which: 0 = CG SpMV (+ p.Ap), 1 = BiCGSTAB SpMV, 2 = DILU sweep levels.
- * ms = summed device time, launches = launches that did work. */
+ * which: 0 = CG SpMV (+ p.Ap), 1 = BiCGSTAB SpMV, 2 = DILU sweep levels,
+ *        3 = CG vector update (+ Jacobi apply and r.z when fused),
+ *        4 = count only: every CG SpMV launch that did work (ms = 0).
+ * ms = summed device time, launches = timed launches that did work.  Inside
+ * the steady-state CUDA-graph chunks only sampled iterations are timed. */
 int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable);
 int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches);
 

@@ -600,8 +600,10 @@ class Case:
         self._chk(lib().xcal_case_set_profiling(self.h, 1 if on else 0))
 
     def profile(self, which: int):
-        """(summed device ms, launches) of a timed kernel class:
-        0 = CG SpMV, 1 = BiCGSTAB SpMV, 2 = DILU applications."""
+        """(summed device ms, timed launches) of a kernel class:
+        0 = CG SpMV, 1 = BiCGSTAB SpMV, 2 = DILU applications, 3 = CG update;
+        4 = (0, every CG SpMV launch that did work).  Steady-state chunks run
+        as CUDA graphs in which only sampled iterations are timed."""
         ms, n = C.c_double(), C.c_int64()
         self._chk(lib().xcal_case_get_profile(self.h, which, C.byref(ms), C.byref(n)))
         return ms.value, n.value

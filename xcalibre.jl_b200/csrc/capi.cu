@@ -9,6 +9,7 @@
 namespace xcal {
 DevMesh* upload_mesh(const xcal_mesh_desc* d, cudaStream_t s);
 std::atomic<long long> g_launch_count{0};
+thread_local long long t_launch_count = 0;
 }
 using namespace xcal;
 
@@ -320,7 +321,7 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable) {
 }
 
 int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches) {
-    if (!cs || which < 0 || which > 2) return XCAL_ERR_INVALID;
+    if (!cs || which < 0 || which > 4) return XCAL_ERR_INVALID;
     if (ms) *ms = cs->c->prof_ms[which];
     if (launches) *launches = cs->c->prof_n[which];
     return XCAL_OK;

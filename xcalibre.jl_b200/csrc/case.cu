@@ -634,6 +634,12 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
 
 Case::~Case() {
     if (stream) cudaStreamSynchronize(stream);
+    for (auto& row : chunk_graph)
+        for (auto& g : row)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (auto& row : gev)
+        for (auto& e : row)
+            if (e) cudaEventDestroy(e);
     for (auto& e : ev) cudaEventDestroy(e);
     for (auto& e : pev) cudaEventDestroy(e);
     if (h_S) cudaFreeHost(h_S);
@@ -642,6 +648,35 @@ Case::~Case() {
 }
 
 void Case::sync() { XCAL_CUDA(cudaStreamSynchronize(stream)); }
+
+// Capture `body` (a fixed sequence of launches on the case stream) once,
+// then replay it.  Launch counts follow the replays, not the capture.
+template <class F>
+void Case::replay_chunk(ChunkGraph& g, F&& body) {
+    if (!g.exec) {
+        const long long t0 = t_launch_count;
+        cudaGraph_t graph = nullptr;
+        XCAL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            body();
+        } catch (...) {
+            cudaStreamEndCapture(stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        XCAL_CUDA(cudaStreamEndCapture(stream, &graph));
+        const long long captured = t_launch_count - t0;
+        g_launch_count.fetch_sub(captured, std::memory_order_relaxed);
+        t_launch_count = t0;
+        cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        XCAL_CUDA(e);
+        g.launches = captured;
+    }
+    XCAL_CUDA(cudaGraphLaunch(g.exec, stream));
+    g_launch_count.fetch_add(g.launches, std::memory_order_relaxed);
+    t_launch_count += g.launches;
+}
 
 void Case::prof_reserve(int pairs) {
     while ((int)pev.size() < 2 * pairs) {
@@ -778,96 +813,149 @@ double Case::solve_system(int eqn, int comp, int* iters) {
     int pt = SS.precond;
     double *x = ws.x.p, *dx = ws.dx.p, *r = ws.r.p, *z = ws.z.p, *pp = ws.p.p, *q = ws.q.p, *v = ws.v.p,
            *s = ws.s.p, *t = ws.t.p;
+    // event record usable both inside a stream capture (becomes an event node)
+    // and on a live stream
+    auto rec = [&](cudaEvent_t e, bool capture) {
+        if (capture)
+            XCAL_CUDA(cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal));
+        else
+            XCAL_CUDA(cudaEventRecord(e, stream));
+    };
+    const int geq = isU ? comp : 3;
+    if (profiling)
+        for (auto& e : gev[geq])
+            if (!e) XCAL_CUDA(cudaEventCreate(&e));
     if (SS.solver == XCAL_SOLVER_CG) {
         kr_init_resid(stream, A, nz, b, field, dx, x, r);
         double* zz = pt == XCAL_PRECOND_NONE ? r : z;
         if (pt != XCAL_PRECOND_NONE) apply_M(E, pt, r, zz, nullptr);
         kr_cg_start(stream, n, r, zz, pp, S, ws.part0.p);
+        // one CG iteration; e3 (optional) = events before the SpMV, between
+        // SpMV and update, after the update
+        auto iteration = [&](cudaEvent_t* e3, bool capture) {
+            if (e3) rec(e3[0], capture);
+            // p_k alternates between pp (even k) and v (odd k)
+            kr_cg_spmv(stream, A, nz, zz, pp, v, q, S, ws.part0.p);
+            if (e3) rec(e3[1], capture);
+            if (pt == XCAL_PRECOND_JACOBI) {
+                kr_cg_update(stream, n, x, pp, v, r, q, zz, E.P.p, 1, S, ws.part0.p);
+            } else {
+                kr_cg_update(stream, n, x, pp, v, r, q, zz, E.P.p, 0, S, ws.part0.p);
+                if (pt == XCAL_PRECOND_DILU) dilu_ldiv(E, r, zz, S);
+                kr_cg_rz(stream, n, r, zz, S, ws.part0.p);
+            }
+            if (e3) rec(e3[2], capture);
+        };
+        const int CHUNK = 32;
         int chunk = 4;
         long launched = 0;
         for (;;) {
             if ((launched += chunk) > (long)hS->itmax + 64 + 32)
                 fail(XCAL_ERR_TIMEOUT, "CG did not report completion within itmax iterations");
             int it0 = hS->iter;
-            if (profiling) prof_reserve(chunk);
-            for (int c = 0; c < chunk; ++c) {
-                if (profiling) XCAL_CUDA(cudaEventRecord(pev[2 * c], stream));
-                // p_k alternates between pp (even k) and v (odd k)
-                kr_cg_spmv(stream, A, nz, zz, pp, v, q, S, ws.part0.p);
-                if (profiling) XCAL_CUDA(cudaEventRecord(pev[2 * c + 1], stream));
-                if (pt == XCAL_PRECOND_JACOBI) {
-                    kr_cg_update(stream, n, x, pp, v, r, q, zz, E.P.p, 1, S, ws.part0.p);
-                } else {
-                    kr_cg_update(stream, n, x, pp, v, r, q, zz, E.P.p, 0, S, ws.part0.p);
-                    if (pt == XCAL_PRECOND_DILU) dilu_ldiv(E, r, zz, S);
-                    kr_cg_rz(stream, n, r, zz, S, ws.part0.p);
+            const bool graphed = chunk == CHUNK;
+            // (iteration index within the chunk, its three events)
+            std::vector<std::pair<int, cudaEvent_t*>> samples;
+            if (graphed) {
+                if (profiling)
+                    for (int c = 4; c < CHUNK; c += 8) samples.push_back({c, &gev[geq][3 * (c / 8)]});
+                replay_chunk(chunk_graph[geq][profiling ? 1 : 0], [&] {
+                    for (int c = 0; c < CHUNK; ++c)
+                        iteration(profiling && c % 8 == 4 ? &gev[geq][3 * (c / 8)] : nullptr, true);
+                });
+            } else {
+                if (profiling) prof_reserve(3 * chunk / 2 + 1);
+                for (int c = 0; c < chunk; ++c) {
+                    iteration(profiling ? &pev[3 * c] : nullptr, false);
+                    if (profiling) samples.push_back({c, &pev[3 * c]});
                 }
             }
             XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
             sync();
-            if (profiling) {
-                // launches that did work: one per completed iteration, plus a
-                // final one that detected zero curvature
-                int real = hS->iter - it0 + (hS->status == KS_ZERO_CURV ? 1 : 0);
-                for (int c = 0; c < real && c < chunk; ++c) {
-                    float t = 0;
-                    XCAL_CUDA(cudaEventElapsedTime(&t, pev[2 * c], pev[2 * c + 1]));
-                    prof_ms[0] += t;
-                    prof_n[0] += 1;
+            // launches that did work: one per completed iteration, plus a
+            // final SpMV that detected zero curvature
+            const int done_it = hS->iter - it0;
+            const int real = done_it + (hS->status == KS_ZERO_CURV ? 1 : 0);
+            if (profiling) prof_n[4] += real;
+            for (auto& sm : samples) {
+                if (sm.first >= real) continue;
+                float t = 0, tu = 0;
+                XCAL_CUDA(cudaEventElapsedTime(&t, sm.second[0], sm.second[1]));
+                prof_ms[0] += t;
+                prof_n[0] += 1;
+                if (sm.first < done_it) {
+                    XCAL_CUDA(cudaEventElapsedTime(&tu, sm.second[1], sm.second[2]));
+                    prof_ms[3] += tu;
+                    prof_n[3] += 1;
                 }
             }
             if (hS->done) break;
-            if (chunk < 32) chunk *= 2;
+            if (chunk < CHUNK) chunk *= 2;
         }
     } else {
         kr_init_resid(stream, A, nz, b, field, dx, x, q);  // r0 in q
         apply_M(E, pt, q, r, nullptr);
         kr_bicg_start(stream, n, b, r, pp, S, ws.part0.p, ws.part1.p);
+        // one BiCGSTAB iteration; e6 (optional) = events around both SpMVs
+        // and both preconditioner applications
+        auto iteration = [&](cudaEvent_t* e, bool capture) {
+            if (e) rec(e[0], capture);
+            kr_spmv(stream, A, nz, pp, q, S);
+            if (e) rec(e[1], capture);
+            apply_M(E, pt, q, v, S);
+            if (e) rec(e[2], capture);
+            kr_bicg_alpha(stream, n, b, v, S, ws.part0.p);
+            kr_bicg_s(stream, n, r, v, pp, s, x, S);
+            if (e) rec(e[3], capture);
+            kr_spmv(stream, A, nz, s, q, S);
+            if (e) rec(e[4], capture);
+            apply_M(E, pt, q, t, S);
+            if (e) rec(e[5], capture);
+            kr_bicg_omega(stream, n, t, s, S, ws.part0.p, ws.part1.p);
+            kr_bicg_xr(stream, n, x, s, t, r, b, S, ws.part0.p, ws.part1.p);
+            kr_bicg_p(stream, n, r, v, pp, S);
+        };
+        const int CHUNK = 8;
         int chunk = 1;
         long launched = 0;
         for (;;) {
             if ((launched += chunk) > (long)hS->itmax + 16 + 8)
                 fail(XCAL_ERR_TIMEOUT, "BiCGSTAB did not report completion within itmax iterations");
             int it0 = hS->iter;
-            if (profiling) prof_reserve(3 * chunk);
-            for (int c = 0; c < chunk; ++c) {
-                cudaEvent_t* e = profiling ? &pev[6 * c] : nullptr;
-                if (e) XCAL_CUDA(cudaEventRecord(e[0], stream));
-                kr_spmv(stream, A, nz, pp, q, S);
-                if (e) XCAL_CUDA(cudaEventRecord(e[1], stream));
-                apply_M(E, pt, q, v, S);
-                if (e) XCAL_CUDA(cudaEventRecord(e[2], stream));
-                kr_bicg_alpha(stream, n, b, v, S, ws.part0.p);
-                kr_bicg_s(stream, n, r, v, pp, s, x, S);
-                if (e) XCAL_CUDA(cudaEventRecord(e[3], stream));
-                kr_spmv(stream, A, nz, s, q, S);
-                if (e) XCAL_CUDA(cudaEventRecord(e[4], stream));
-                apply_M(E, pt, q, t, S);
-                if (e) XCAL_CUDA(cudaEventRecord(e[5], stream));
-                kr_bicg_omega(stream, n, t, s, S, ws.part0.p, ws.part1.p);
-                kr_bicg_xr(stream, n, x, s, t, r, b, S, ws.part0.p, ws.part1.p);
-                kr_bicg_p(stream, n, r, v, pp, S);
+            const bool graphed = chunk == CHUNK;
+            std::vector<std::pair<int, cudaEvent_t*>> samples;
+            if (graphed) {
+                if (profiling) samples.push_back({4, &gev[geq][0]});
+                replay_chunk(chunk_graph[geq][profiling ? 1 : 0], [&] {
+                    for (int c = 0; c < CHUNK; ++c) iteration(profiling && c == 4 ? &gev[geq][0] : nullptr, true);
+                });
+            } else {
+                if (profiling) prof_reserve(3 * chunk);
+                for (int c = 0; c < chunk; ++c) {
+                    iteration(profiling ? &pev[6 * c] : nullptr, false);
+                    if (profiling) samples.push_back({c, &pev[6 * c]});
+                }
             }
             XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
             sync();
-            if (profiling) {
-                int real = hS->iter - it0;
-                for (int c = 0; c < real && c < chunk; ++c) {
-                    float t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-                    XCAL_CUDA(cudaEventElapsedTime(&t0, pev[6 * c], pev[6 * c + 1]));
-                    XCAL_CUDA(cudaEventElapsedTime(&t1, pev[6 * c + 3], pev[6 * c + 4]));
-                    XCAL_CUDA(cudaEventElapsedTime(&t2, pev[6 * c + 1], pev[6 * c + 2]));
-                    XCAL_CUDA(cudaEventElapsedTime(&t3, pev[6 * c + 4], pev[6 * c + 5]));
-                    prof_ms[1] += t0 + t1;
-                    prof_n[1] += 2;
-                    if (pt == XCAL_PRECOND_DILU) {
-                        prof_ms[2] += t2 + t3;
-                        prof_n[2] += 2;
-                    }
+            const int real = hS->iter - it0;
+            for (auto& sm : samples) {
+                if (sm.first >= real) continue;
+                cudaEvent_t* e = sm.second;
+                float t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+                XCAL_CUDA(cudaEventElapsedTime(&t0, e[0], e[1]));
+                XCAL_CUDA(cudaEventElapsedTime(&t1, e[3], e[4]));
+                XCAL_CUDA(cudaEventElapsedTime(&t2, e[1], e[2]));
+                XCAL_CUDA(cudaEventElapsedTime(&t3, e[4], e[5]));
+                prof_ms[1] += t0 + t1;
+                prof_n[1] += 2;
+                if (pt == XCAL_PRECOND_DILU) {
+                    prof_ms[2] += t2 + t3;
+                    prof_n[2] += 2;
                 }
             }
             if (hS->done) break;
-            if (chunk < 8) chunk *= 2;
+            if (chunk < CHUNK) chunk *= 2;
         }
     }
     kr_finish(stream, n, x, dx, field);

@@ -88,9 +88,23 @@ struct Case {
     // optional per-kernel event timing (xcal_case_set_profiling)
     bool profiling = false;
     std::vector<cudaEvent_t> pev;  // pairs, reused per polling chunk
-    double prof_ms[3] = {0, 0, 0};
-    long long prof_n[3] = {0, 0, 0};
+    double prof_ms[5] = {0, 0, 0, 0, 0};
+    long long prof_n[5] = {0, 0, 0, 0, 0};
     void prof_reserve(int pairs);
+    // Steady-state polling chunks of a Krylov solve (32 CG / 8 BiCGSTAB
+    // iterations) replay as CUDA graphs: every pointer they use is fixed for
+    // the life of the case, so each graph is captured once per equation
+    // component (BiCGSTAB reads the component's right-hand side).  The
+    // profiled variant carries event-record nodes around sampled iterations
+    // (those with c % 8 == 4).
+    struct ChunkGraph {
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;  // kernels per replay
+    };
+    ChunkGraph chunk_graph[4][2];  // [Ux, Uy, Uz, p][plain, profiled]
+    cudaEvent_t gev[4][12] = {};   // event nodes of the profiled graphs
+    template <class F>
+    void replay_chunk(ChunkGraph& g, F&& body);
 
     Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cfg);
     ~Case();

@@ -21,7 +21,7 @@ __device__ __forceinline__ double row_dot(const CSRView& A, const double* __rest
     const int rb = row_base(A, i), rl = A.len[i];
     for (int k = 0; k < rl; ++k) {
         int e = rb + SELL_C * k;
-        acc = acc + nz[e] * x[A.colval[e]];
+        acc = acc + ld_stream(nz + e) * x[ld_stream(A.colval + e)];
     }
     return acc;
 }
@@ -191,10 +191,11 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const dou
             double qi = 0.0, pi;
             const int rb = row_base(A, i), e1 = rb + SELL_C * A.len[i];
             if (it == 0) {
-                for (int e = rb; e < e1; e += SELL_C) qi = qi + nz[e] * pk[A.colval[e]];
+                for (int e = rb; e < e1; e += SELL_C) qi = qi + ld_stream(nz + e) * pk[ld_stream(A.colval + e)];
                 pi = pk[i];
             } else {
-                for (int e = rb; e < e1; e += SELL_C) qi = qi + nz[e] * cg_dir(z, pold, beta, A.colval[e]);
+                for (int e = rb; e < e1; e += SELL_C)
+                    qi = qi + ld_stream(nz + e) * cg_dir(z, pold, beta, ld_stream(A.colval + e));
                 pi = cg_dir(z, pold, beta, i);
                 pk[i] = pi;
             }
@@ -230,11 +231,13 @@ __global__ void k_cg_update(int n, double* x, const double* __restrict__ P0, con
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < n) {
-            x[i] = x[i] + alpha * p[i];
-            double ri = r[i] + (-alpha) * q[i];
+            // x, q and P are not read again before the next update: evict-first
+            // keeps L2 for z and p, which the next SpMV gathers
+            __stcs(x + i, ld_stream(x + i) + alpha * p[i]);
+            double ri = r[i] + (-alpha) * ld_stream(q + i);
             r[i] = ri;
             if (jacobi_fused) {
-                double zi = P[i] * ri;
+                double zi = ld_stream(P + i) * ri;
                 z[i] = zi;
                 acc = acc + ri * zi;
             }
@@ -486,8 +489,8 @@ __global__ void k_dilu_fwd(const int* __restrict__ rows, int nrows, CSRView A, c
     int ds = A.diag[i];
     double sum = 0.0;
     for (int e = row_base(A, i); e < ds; e += SELL_C) {
-        int j = A.colval[e];
-        sum = sum + (nz[e] * y[j]) * (1.0 / D[j]);
+        int j = ld_stream(A.colval + e);
+        sum = sum + (ld_stream(nz + e) * y[j]) * (1.0 / D[j]);
     }
     y[i] = b[i] - sum;
 }
@@ -502,7 +505,7 @@ __global__ void k_dilu_bwd(const int* __restrict__ rows, int nrows, CSRView A, c
     int ds = A.diag[i];
     double sum = 0.0;
     int e1 = row_base(A, i) + SELL_C * A.len[i];
-    for (int e = ds + SELL_C; e < e1; e += SELL_C) sum = sum + nz[e] * x[A.colval[e]];
+    for (int e = ds + SELL_C; e < e1; e += SELL_C) sum = sum + ld_stream(nz + e) * x[ld_stream(A.colval + e)];
     x[i] = (x[i] - sum) / D[i];
 }
 

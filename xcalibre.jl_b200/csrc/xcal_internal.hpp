@@ -37,12 +37,15 @@ struct Error {
                                 std::string(#call) + ": " + cudaGetErrorString(_e)};     \
     } while (0)
 
-// number of kernels this library has launched (reported by xcal_get_launch_count)
+// number of kernels this library has launched (reported by xcal_get_launch_count);
+// the per-thread count lets a stream capture find how many kernels a graph holds
 extern std::atomic<long long> g_launch_count;
+extern thread_local long long t_launch_count;
 
 #define XCAL_CHECK_LAUNCH()                                              \
     do {                                                                 \
         ::xcal::g_launch_count.fetch_add(1, std::memory_order_relaxed); \
+        ++::xcal::t_launch_count;                                        \
         XCAL_CUDA(cudaGetLastError());                                   \
     } while (0)
 
