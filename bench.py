@@ -9,7 +9,11 @@ gradients, flux and velocity corrections).  Metric: Mcell-iters/s =
 cells x iterations / device seconds.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--size 128] [--precision fp64]
+                  [--size 128] [--precision fp64|mixed] [--no-second-precision]
+
+The line's `value` is the FP64 plain path (or --precision's mode);
+`second_precision` carries the same measurement in the other mode (mixed:
+FP32 Krylov inner solves inside FP64 defect correction).
 
 --impl reference times the CPU restatement of the reference's path (the
 oracle; the Julia reference cannot run in this image) on the host cores.
@@ -45,6 +49,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-iters", type=int, default=1, help="SIMPLE iterations in the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-second-precision", action="store_true",
+                    help="skip the second timed run in the other precision mode")
     return ap.parse_args()
 
 
@@ -164,26 +170,19 @@ def cpu_baseline_sample(x, pm, mesh, iters):
                       f"({dt:.1f} s wall, C++ oracle with OpenMP over all host threads)"}
 
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        return run_reference(args)
+def spmv_bytes(nnz, n, fp32):
+    """Algorithmic bytes of one CG SpMV launch (k >= 1): matrix slots (value +
+    column index) once, row length (1 byte) and slice offsets (4 bytes per 32
+    rows), z and p_{k-1} read once, p_k and q written once."""
+    s = 4 if fp32 else 8
+    return nnz * (s + 4) + n * (1 + 4 * s) + 4 * ((n + 31) // 32)
+
+
+def measure(x, A, mesh, precision, args, local, world, stream_cls):
+    """Warm up, then time args.steps SIMPLE iterations of a fresh case on the
+    device (CUDA events on the case stream, barrier + synchronize around)."""
     import torch
-    world, rank, local = dist_setup(args)
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                             device_id=torch.device("cuda", local))
-    import __graft_entry__ as ge
-    x = ge.load_package()
-    A = x._abi
-    n = args.size
-    t_mesh = time.perf_counter()
-    pm = x.channel_polymesh(n, n, n, seed=0)
-    mesh = x.build_mesh3(pm)
-    t_mesh = time.perf_counter() - t_mesh
-    model, config = x.cases.channel_case(mesh, iterations=args.steps + args.warmup, precision=args.precision,
+    model, config = x.cases.channel_case(mesh, iterations=args.steps + args.warmup, precision=precision,
                                          device=local)
     cfg, keep = x.build_config(model, config)
     ctx = x.Context(local)
@@ -194,9 +193,7 @@ def main():
     case.set_field(A.FIELD_P, model.momentum.p)
     t_setup = time.perf_counter() - t_setup
     nnz_p = case.nnz(A.EQN_P)
-    stream = torch.cuda.ExternalStream(case.stream(), device=torch.device("cuda", local))
-
-    # warm-up
+    stream = stream_cls(case.stream(), device=torch.device("cuda", local))
     case.simple_iterate(args.warmup)
     torch.cuda.synchronize()
     case.set_profiling(True)
@@ -223,46 +220,53 @@ def main():
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_max = float(t.item())
-    else:
-        ms_max = ms
-    cells_total = mesh.n_cells * world
-    value = cells_total * args.steps / (ms_max / 1e3) / 1e6
-
-    # roofline of the dominant kernel: CG SpMV + <p,Ap> (pressure solve).  Per
-    # launch (k >= 1): values+columns nnz*(8+4), rowptr 4n, z and p_{k-1}
-    # 8n each, p_k and q written 8n each.
+        ms = float(t.item())
+    fp32 = precision == "mixed"
+    n = mesh.n_cells
+    # roofline of the dominant kernel: the CG SpMV fused with p = z + beta p
+    # and <p, Ap> (pressure solve), timed by CUDA events on sampled launches
     spmv_ms = prof1[0][0] - prof0[0][0]
     spmv_n = prof1[0][1] - prof0[0][1]
     spmv_all = prof1[4][1] - prof0[4][1]  # every CG SpMV launch that did work
-    bytes_spmv = nnz_p * 12 + mesh.n_cells * 36
+    bytes_spmv = spmv_bytes(nnz_p, n, fp32)
     peak, peak_kind = measured_peak_hbm()
     avg_s = spmv_ms / max(spmv_n, 1) / 1e3
     achieved = bytes_spmv / avg_s / 1e9 if spmv_n else None
     traffic = None
     tp = os.path.join(ROOT, "profiles", "spmv_traffic.json")
-    if os.path.exists(tp):
+    if os.path.exists(tp) and not fp32:
         try:
             tr = json.load(open(tp))
-            traffic = tr.get("bytes_per_launch_128") if n == 128 else None
+            traffic = tr.get("bytes_per_launch_128") if args.size == 128 else None
         except Exception:
             traffic = None
-    roof = {"bound": "hbm", "kernel": "k_cg_spmv (CSR SpMV FP64 fused with p = z + beta p and p.Ap)", "achieved": achieved, "peak": peak,
-            "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-            "traffic": traffic, "bytes_per_launch": bytes_spmv, "launches_timed": spmv_n,
-            "launches_total": spmv_all, "avg_launch_us": avg_s * 1e6,
+    prec_name = "FP32" if fp32 else "FP64"
+    roof = {"bound": "hbm", "kernel": f"k_cg_spmv<{prec_name}> (SELL-32 SpMV fused with p = z + beta p and <p,Ap>)",
+            "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic, "bytes_per_launch": bytes_spmv,
+            "launches_timed": spmv_n, "launches_total": spmv_all, "avg_launch_us": avg_s * 1e6,
             "share_of_step": avg_s * 1e3 * spmv_all / ms if ms else None}
     # second kernel of each CG iteration: x += alpha p; r -= alpha q; z = P r;
-    # <r,z> -- reads x, p, r, q, P and writes x, r, z: 64 bytes per row
+    # <r,z> -- reads x, p, r, q, P and writes x, r, z (8 vectors)
     upd_ms = prof1[3][0] - prof0[3][0]
     upd_n = prof1[3][1] - prof0[3][1]
     if upd_n:
         upd_s = upd_ms / upd_n / 1e3
-        roof["cg_update"] = {"avg_launch_us": upd_s * 1e6, "bytes_per_launch": 64 * mesh.n_cells,
-                             "achieved": 64 * mesh.n_cells / upd_s / 1e9, "launches_timed": upd_n,
-                             "share_of_step": upd_s * 1e3 * spmv_all / ms if ms else None}
+        ub = 8 * (4 if fp32 else 8) * n
+        roof["cg_update"] = {"avg_launch_us": upd_s * 1e6, "bytes_per_launch": ub, "achieved": ub / upd_s / 1e9,
+                             "launches_timed": upd_n, "share_of_step": upd_s * 1e3 * spmv_all / ms if ms else None}
+    tm = case.timings()
+    out = {"value": n * world * args.steps / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps, "roofline": roof,
+           "gpu_launches": launches, "clocks": clk, "setup_s": round(t_setup, 2), "nnz_p": nnz_p,
+           "residuals_last": [float(v) for v in res[-1]] if len(res) else None,
+           "phases_ms_total": {"U_solve": tm[1], "p_solve": tm[2], "other": tm[3], "total": tm[5]}}
+    return out, case, dm, model
 
-    # end-to-end through the C ABI with host buffers (copies in the timed region)
+
+def e2e_measure(x, A, case, mesh, args, world):
+    """Same metric through the public API with host buffers: every step copies
+    U and p host->device, runs one SIMPLE iteration and reads them back."""
+    import torch
     nC = mesh.n_cells
     hU = torch.empty((3, nC), dtype=torch.float64, pin_memory=True).numpy()
     hp = torch.empty(nC, dtype=torch.float64, pin_memory=True).numpy()
@@ -282,30 +286,61 @@ def main():
         t = torch.tensor([e2e_s], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = None
-    if args.e2e_steps > 0:
-        e2e = {"value": cells_total * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
-               "h2d_bytes_per_step": 4 * nC * 8, "d2h_bytes_per_step": 4 * nC * 8 + 4 * 8,
-               "steps": args.e2e_steps}
+    return {"value": nC * world * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
+            "h2d_bytes_per_step": 4 * nC * 8, "d2h_bytes_per_step": 4 * nC * 8 + 4 * 8, "steps": args.e2e_steps}
 
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    import __graft_entry__ as ge
+    x = ge.load_package()
+    A = x._abi
+    n = args.size
+    t_mesh = time.perf_counter()
+    pm = x.channel_polymesh(n, n, n, seed=0)
+    mesh = x.build_mesh3(pm)
+    t_mesh = time.perf_counter() - t_mesh
+    primary = args.precision
+    r, case, dm, model = measure(x, A, mesh, primary, args, local, world, torch.cuda.ExternalStream)
+    e2e = e2e_measure(x, A, case, mesh, args, world) if args.e2e_steps > 0 else None
+    case.close()
+    dm.close()
+    other = None
+    if not args.no_second_precision:
+        sec = "mixed" if primary == "fp64" else "fp64"
+        r2, case2, dm2, _ = measure(x, A, mesh, sec, args, local, world, torch.cuda.ExternalStream)
+        case2.close()
+        dm2.close()
+        other = {"precision": sec, "value": r2["value"], "ms_per_step": r2["ms_per_step"],
+                 "ratio_mixed_over_fp64": (r2["value"] / r["value"]) if sec == "mixed" else (r["value"] / r2["value"]),
+                 "roofline": r2["roofline"], "residuals_last": r2["residuals_last"],
+                 "phases_ms_total": r2["phases_ms_total"], "gpu_launches": r2["gpu_launches"]}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(x, pm, mesh, args.cpu_iters)
-    tm = case.timings()
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload_name(n), "cells": nC, "nnz_p": nnz_p, "precision": args.precision,
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if primary == "fp64" else "f32/f64",
+                "data": "synthetic",
+                "config": {"workload": workload_name(n), "cells": mesh.n_cells, "nnz_p": r["nnz_p"],
+                           "precision": primary,
                            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                            "l2": "working set (matrices + face arrays, >1 GB) larger than L2; no flush",
-                           "mesh_build_s": round(t_mesh, 2), "setup_s": round(t_setup, 2)},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-                "residuals_last": [float(v) for v in res[-1]] if len(res) else None,
-                "phases_ms_total": {"U_solve": tm[1], "p_solve": tm[2], "other": tm[3], "total": tm[5]}}
+                           "mesh_build_s": round(t_mesh, 2), "setup_s": r["setup_s"]},
+                "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": r["gpu_launches"],
+                "clocks": r["clocks"], "residuals_last": r["residuals_last"],
+                "phases_ms_total": r["phases_ms_total"], "second_precision": other}
         print(json.dumps(line), flush=True)
-    case.close()
-    dm.close()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0

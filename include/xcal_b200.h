@@ -168,6 +168,8 @@ typedef struct {
     double pref;
     int32_t inner_loops;        /* PISO correctors (run!(...; inner_loops))  */
     int32_t precision;          /* XCAL_PREC_*                               */
+    double inner_rtol;          /* mixed: relative tolerance of each FP32
+                                   inner solve (0 = default 1e-3)            */
     int32_t n_bc_U, n_bc_p, n_bc_nut;
     const xcal_bc* bc_U;
     const xcal_bc* bc_p;

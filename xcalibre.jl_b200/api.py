@@ -127,9 +127,12 @@ class Runtime:
 @dataclass
 class B200Backend:
     """Backend selecting libxcal_b200 (one GPU).  ``precision`` is "fp64"
-    (plain path) or "mixed" (FP32 Krylov inner iterations)."""
+    (plain path) or "mixed" (FP32 Krylov inner solves inside an FP64 defect
+    correction; each inner solve reduces its residual by ``inner_rtol`` at
+    most, never past the FP64 path's own stopping target)."""
     device: int = 0
     precision: str = "fp64"
+    inner_rtol: float = 1e-3
 
 
 @dataclass
@@ -455,6 +458,7 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
         iterations=int(config.runtime.iterations), dt=float(config.runtime.time_step),
         has_pref=0 if pref is None else 1, pref=0.0 if pref is None else float(pref),
         inner_loops=int(inner_loops), precision=prec,
+        inner_rtol=float(getattr(backend, "inner_rtol", 1e-3)),
         n_bc_U=len(bnd["U"]), n_bc_p=len(bnd["p"]), n_bc_nut=len(nut_bcs),
         bc_U=C.cast(bU, C.POINTER(_abi.BCDesc)), bc_p=C.cast(bP, C.POINTER(_abi.BCDesc)),
         bc_nut=C.cast(bN, C.POINTER(_abi.BCDesc)))

@@ -7,7 +7,8 @@
                         (peak 1 m/s), zeroGradient outlet, no-slip walls,
                         nu = 1e-3, LUST, SIMPLE
 * periodic_les_case  -- periodic cube, PISO + Smagorinsky (Cs = 0.17),
-                        Euler, Linear divergence, nu = 1e-4
+                        Euler, Linear divergence, nu = 1e-4; initial field
+                        from fourier_field (seeded, k^4 exp(-2 (k/4)^2))
 """
 from __future__ import annotations
 
@@ -77,6 +78,40 @@ def taylor_green(mesh: Mesh3, rms: float = 1.0) -> np.ndarray:
     return U * (rms / cur)
 
 
+def fourier_field(mesh: Mesh3, seed: int = 0, k0: float = 4.0, rms: float = 1.0,
+                  L: float = 2.0 * np.pi) -> np.ndarray:
+    """Seeded random divergence-free velocity on the periodic cube [0, L]^3.
+
+    Spectral method: random complex Fourier coefficients on the n^3 integer
+    wavenumber grid with amplitude sqrt(E(k) / (4 pi k^2)), E(k) = k^4
+    exp(-2 (k/k0)^2), projected onto k . u = 0 (u - k (k.u)/|k|^2); the real
+    part of the inverse FFT is sampled at the cell centres (the box mesh is a
+    uniform lattice, cells may be numbered in any order) and scaled to the
+    requested rms of |U|.  Shape (3, n_cells)."""
+    nc = mesh.n_cells
+    n = int(round(nc ** (1.0 / 3.0)))
+    if n ** 3 != nc:
+        raise ValueError("fourier_field needs an n^3 box mesh")
+    rng = np.random.default_rng(seed)
+    k1 = np.fft.fftfreq(n, d=1.0 / n) * (2.0 * np.pi / L)
+    kx, ky, kz = np.meshgrid(k1, k1, k1, indexing="ij")
+    kk = kx * kx + ky * ky + kz * kz
+    kmag = np.sqrt(kk)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        E = kmag ** 4 * np.exp(-2.0 * (kmag / k0) ** 2)
+        amp = np.where(kmag > 0, np.sqrt(E / (4.0 * np.pi * np.where(kk > 0, kk, 1.0))), 0.0)
+    u = [amp * (rng.standard_normal(kk.shape) + 1j * rng.standard_normal(kk.shape)) for _ in range(3)]
+    kdu = kx * u[0] + ky * u[1] + kz * u[2]
+    inv = np.where(kk > 0, 1.0 / np.where(kk > 0, kk, 1.0), 0.0)
+    u = [u[0] - kx * kdu * inv, u[1] - ky * kdu * inv, u[2] - kz * kdu * inv]
+    grid = np.stack([np.real(np.fft.ifftn(c)) for c in u])
+    h = L / n
+    idx = np.clip(np.floor(mesh.cell_centre / h).astype(np.int64), 0, n - 1)
+    U = grid[:, idx[:, 0], idx[:, 1], idx[:, 2]]
+    cur = np.sqrt(np.mean(np.sum(U * U, axis=0)))
+    return U * (rms / cur)
+
+
 def periodic_les_case(mesh: Mesh3, steps: int = 200, dt: float | None = None, precision: str = "fp64",
                       device: int = 0, U0: np.ndarray | None = None):
     pairs = [A.construct_periodic(mesh, None, a, b) for a, b in (("xmin", "xmax"), ("ymin", "ymax"), ("zmin", "zmax"))]
@@ -86,7 +121,7 @@ def periodic_les_case(mesh: Mesh3, steps: int = 200, dt: float | None = None, pr
     BCs = A.assign(region=mesh, U=per, p=per, nut=per)
     schemes = {"U": A.Schemes(time=A.Euler, divergence=A.Linear), "p": A.Schemes(time=A.Euler)}
     if U0 is None:
-        U0 = taylor_green(mesh)
+        U0 = fourier_field(mesh, seed=0)
     if dt is None:
         # dt from CFL = 0.5 with the Courant definition of max_courant_number!
         umag = np.sqrt(np.sum(U0 * U0, axis=0))

@@ -132,6 +132,10 @@ int32_t xcal_case_get_system(const xcal_case* cs, int32_t eqn, int32_t component
                 std::vector<double> d0(E.n);
                 XCAL_CUDA(cudaMemcpy(d0.data(), E.diag0.p, E.n * sizeof(double), cudaMemcpyDeviceToHost));
                 for (int st = 0; st < E.n; ++st) nz[E.diag[st]] = d0[st];
+                // periodic pair slots are 0 in A0 (only the BCs write them)
+                for (const std::vector<int>* v : {&c->bcU.h_pNP, &c->bcU.h_pPN})
+                    for (int s : *v)
+                        if (s >= 0) nz[s] = 0.0;
             }
             long k = 0;
             for (int i = 0; i < E.n; ++i) {

@@ -79,6 +79,8 @@ BCView BCTable::view() const {
     v.pNN = d_pNN.p;
     v.pNP = d_pNP.p;
     v.pPN = d_pPN.p;
+    v.pe_off = d_pe_off.p;
+    v.pe_face = d_pe_face.p;
     return v;
 }
 
@@ -516,9 +518,18 @@ static void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int
                     pEf[f] = std::sqrt(efx * efx + efy * efy + efz * efz);
                     pwdelta[f] = m.delta[pf] / (m.delta[f] + m.delta[pf]);  // Solvers_1_SIMPLE.jl:463
                     if (E) {
+                        // the periodic slots start from 0 at every assembly:
+                        // a pair that is also an internal neighbour (or the
+                        // cell itself) would share a slot with the face loop
+                        if (c1 == c2) fail(XCAL_ERR_UNSUPPORTED, "periodic pair maps a cell onto itself");
+                        for (int k = m.cf_off[c1]; k < m.cf_off[c1 + 1]; ++k)
+                            if (m.cf_nb[k] == c2)
+                                fail(XCAL_ERR_UNSUPPORTED, "periodic partners are also internal neighbours");
                         pNN[f] = E->find(c2, c2);
                         pNP[f] = E->find(c2, c1);
                         pPN[f] = E->find(c1, c2);
+                        if (pNN[f] < 0 || pNP[f] < 0 || pPN[f] < 0)
+                            fail(XCAL_ERR_INVALID, "periodic pair missing from the matrix pattern");
                     }
                 }
             }
@@ -536,6 +547,22 @@ static void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int
     T.d_pNN.upload(pNN, s);
     T.d_pNP.upload(pNP, s);
     T.d_pPN.upload(pPN, s);
+    T.h_pNP = pNP;
+    T.h_pPN = pPN;
+    // partner events: cell owner[face_map[f]] of every parent face f
+    if (T.has_periodic) {
+        const int nC = m.nC;
+        std::vector<int> off(nC + 1, 0), face;
+        for (int f = 0; f < nB; ++f)
+            if (T.type[f] == XCAL_BC_PERIODIC_PARENT) ++off[peer_cell[f] + 1];
+        for (int c = 0; c < nC; ++c) off[c + 1] += off[c];
+        face.assign(off[nC], 0);
+        std::vector<int> pos(off.begin(), off.end() - 1);
+        for (int f = 0; f < nB; ++f)  // ascending f: each cell's list is ascending
+            if (T.type[f] == XCAL_BC_PERIODIC_PARENT) face[pos[peer_cell[f]]++] = f;
+        T.d_pe_off.upload(off, s);
+        T.d_pe_face.upload(face, s);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -560,7 +587,6 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     std::vector<xcal_bc> bU(cfg.bc_U, cfg.bc_U + cfg.n_bc_U), bP(cfg.bc_p, cfg.bc_p + cfg.n_bc_p);
     build_equation(U, *m, bU, 3, cfg.U_solver.precond == XCAL_PRECOND_DILU, stream);
     build_equation(P, *m, bP, 1, cfg.p_solver.precond == XCAL_PRECOND_DILU, stream);
-    if (U.has_periodic) fail(XCAL_ERR_UNSUPPORTED, "periodic boundaries on U are not enabled in this build");
     build_bc_table(bcU, *m, cfg.bc_U, cfg.n_bc_U, 3, &U, stream);
     build_bc_table(bcP, *m, cfg.bc_p, cfg.n_bc_p, 1, &P, stream);
     build_bc_table(bcNut, *m, cfg.bc_nut, cfg.n_bc_nut, 1, nullptr, stream);
@@ -589,6 +615,18 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     for (DBuf<double>* b : {&ws.x, &ws.dx, &ws.r, &ws.z, &ws.p, &ws.q, &ws.v, &ws.s, &ws.t}) {
         b->alloc(nC);
         b->zero(stream);
+    }
+    if (cfg.precision == XCAL_PREC_MIXED) {
+        for (DBuf<float>* b : {&ws.fx, &ws.fr, &ws.fz, &ws.fp, &ws.fq, &ws.fv, &ws.fs, &ws.ft, &ws.fd}) {
+            b->alloc(nC);
+            b->zero(stream);
+        }
+        for (Equation* E : {&U, &P}) {
+            E->nz32.alloc(E->nnz);
+            E->nz32.zero(stream);
+            E->P32.alloc(E->n);
+            E->P32.zero(stream);
+        }
     }
     ws.part0.alloc(T);
     ws.part1.alloc(T);
@@ -774,45 +812,36 @@ void Case::update_precond(int eqn) {
     }
 }
 
-void Case::dilu_ldiv(Equation& E, const double* b, double* out, const KScalars* S) {
+template <class T>
+void Case::dilu_ldiv(Equation& E, const T* nz, const T* D, const T* b, T* out, const KScalars* S) {
     CSRView A = E.view();
     for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
-        kr_dilu_fwd(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], A, E.nz.p,
-                    E.P.p, b, out, S);
+        kr_dilu_fwd(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], A, nz, D, b, out,
+                    S);
     for (size_t l = 0; l + 1 < E.upper_off.size(); ++l)
-        kr_dilu_bwd(stream, E.d_upper_rows.p + E.upper_off[l], E.upper_off[l + 1] - E.upper_off[l], A, E.nz.p,
-                    E.P.p, out, S);
+        kr_dilu_bwd(stream, E.d_upper_rows.p + E.upper_off[l], E.upper_off[l + 1] - E.upper_off[l], A, nz, D, out, S);
 }
 
-void Case::apply_M(Equation& E, int ptype, const double* in, double* out, const KScalars* S) {
+template <class T>
+void Case::apply_M(Equation& E, int ptype, const T* nz, const T* P, const T* in, T* out, const KScalars* S) {
     if (ptype == XCAL_PRECOND_JACOBI)
-        kr_jacobi_apply(stream, E.n, E.P.p, in, out, S);
+        kr_jacobi_apply(stream, E.n, P, in, out, S);
     else if (ptype == XCAL_PRECOND_DILU)
-        dilu_ldiv(E, in, out, S);
+        dilu_ldiv(E, nz, P, in, out, S);
     else
         kr_copy(stream, E.n, in, out, S);
 }
 
-// solve_system! (Solve_1_api.jl:268-307)
-double Case::solve_system(int eqn, int comp, int* iters) {
-    bool isU = eqn == XCAL_EQN_U;
-    Equation& E = isU ? U : P;
-    const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
-    double* field = isU ? Uc[comp].p : p.p;
-    const double* b = isU ? U.b[comp].p : P.b[0].p;
-    KScalars* S = ws.S.p + (isU ? 0 : 1);
-    KScalars* hS = h_S + (isU ? 0 : 1);
-    int n = E.n;
+// Krylov iterations of one solve, from its initial residual on.  CG: V.r
+// holds r0.  BiCGSTAB: r0 holds the unpreconditioned r0 and c is Krylov.jl's
+// shadow vector (the right-hand side).  gk selects the cached chunk graphs.
+template <class T>
+void Case::krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c,
+                          const T* r0, const KrylovVecs<T>& V, KScalars* S, KScalars* hS, int gk) {
+    const int n = E.n;
+    const int pt = SS.precond;
     CSRView A = E.view();
-    const double* nz = E.nz.p;
-    std::memset(hS, 0, sizeof(KScalars));
-    hS->atol = SS.atol;
-    hS->rtol = SS.rtol;
-    hS->itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
-    XCAL_CUDA(cudaMemcpyAsync(S, hS, sizeof(KScalars), cudaMemcpyHostToDevice, stream));
-    int pt = SS.precond;
-    double *x = ws.x.p, *dx = ws.dx.p, *r = ws.r.p, *z = ws.z.p, *pp = ws.p.p, *q = ws.q.p, *v = ws.v.p,
-           *s = ws.s.p, *t = ws.t.p;
+    T *x = V.x, *r = V.r, *z = V.z, *pp = V.p, *q = V.q, *v = V.v, *s = V.s, *t = V.t;
     // event record usable both inside a stream capture (becomes an event node)
     // and on a live stream
     auto rec = [&](cudaEvent_t e, bool capture) {
@@ -821,28 +850,26 @@ double Case::solve_system(int eqn, int comp, int* iters) {
         else
             XCAL_CUDA(cudaEventRecord(e, stream));
     };
-    const int geq = isU ? comp : 3;
     if (profiling)
-        for (auto& e : gev[geq])
+        for (auto& e : gev[gk])
             if (!e) XCAL_CUDA(cudaEventCreate(&e));
     if (SS.solver == XCAL_SOLVER_CG) {
-        kr_init_resid(stream, A, nz, b, field, dx, x, r);
-        double* zz = pt == XCAL_PRECOND_NONE ? r : z;
-        if (pt != XCAL_PRECOND_NONE) apply_M(E, pt, r, zz, nullptr);
-        kr_cg_start(stream, n, r, zz, pp, S, ws.part0.p);
+        T* zz = pt == XCAL_PRECOND_NONE ? r : z;
+        if (pt != XCAL_PRECOND_NONE) apply_M(E, pt, nz, P, (const T*)r, zz, (const KScalars*)nullptr);
+        kr_cg_start(stream, n, (const T*)r, (const T*)zz, pp, S, ws.part0.p);
         // one CG iteration; e3 (optional) = events before the SpMV, between
         // SpMV and update, after the update
         auto iteration = [&](cudaEvent_t* e3, bool capture) {
             if (e3) rec(e3[0], capture);
             // p_k alternates between pp (even k) and v (odd k)
-            kr_cg_spmv(stream, A, nz, zz, pp, v, q, S, ws.part0.p);
+            kr_cg_spmv(stream, A, nz, (const T*)zz, pp, v, q, S, ws.part0.p);
             if (e3) rec(e3[1], capture);
             if (pt == XCAL_PRECOND_JACOBI) {
-                kr_cg_update(stream, n, x, pp, v, r, q, zz, E.P.p, 1, S, ws.part0.p);
+                kr_cg_update(stream, n, x, (const T*)pp, (const T*)v, r, (const T*)q, zz, P, 1, S, ws.part0.p);
             } else {
-                kr_cg_update(stream, n, x, pp, v, r, q, zz, E.P.p, 0, S, ws.part0.p);
-                if (pt == XCAL_PRECOND_DILU) dilu_ldiv(E, r, zz, S);
-                kr_cg_rz(stream, n, r, zz, S, ws.part0.p);
+                kr_cg_update(stream, n, x, (const T*)pp, (const T*)v, r, (const T*)q, zz, P, 0, S, ws.part0.p);
+                if (pt == XCAL_PRECOND_DILU) dilu_ldiv(E, nz, P, (const T*)r, zz, (const KScalars*)S);
+                kr_cg_rz(stream, n, (const T*)r, (const T*)zz, S, ws.part0.p);
             }
             if (e3) rec(e3[2], capture);
         };
@@ -858,16 +885,16 @@ double Case::solve_system(int eqn, int comp, int* iters) {
             std::vector<std::pair<int, cudaEvent_t*>> samples;
             if (graphed) {
                 if (profiling)
-                    for (int c = 4; c < CHUNK; c += 8) samples.push_back({c, &gev[geq][3 * (c / 8)]});
-                replay_chunk(chunk_graph[geq][profiling ? 1 : 0], [&] {
-                    for (int c = 0; c < CHUNK; ++c)
-                        iteration(profiling && c % 8 == 4 ? &gev[geq][3 * (c / 8)] : nullptr, true);
+                    for (int c8 = 4; c8 < CHUNK; c8 += 8) samples.push_back({c8, &gev[gk][3 * (c8 / 8)]});
+                replay_chunk(chunk_graph[gk][profiling ? 1 : 0], [&] {
+                    for (int ci = 0; ci < CHUNK; ++ci)
+                        iteration(profiling && ci % 8 == 4 ? &gev[gk][3 * (ci / 8)] : nullptr, true);
                 });
             } else {
                 if (profiling) prof_reserve(3 * chunk / 2 + 1);
-                for (int c = 0; c < chunk; ++c) {
-                    iteration(profiling ? &pev[3 * c] : nullptr, false);
-                    if (profiling) samples.push_back({c, &pev[3 * c]});
+                for (int ci = 0; ci < chunk; ++ci) {
+                    iteration(profiling ? &pev[3 * ci] : nullptr, false);
+                    if (profiling) samples.push_back({ci, &pev[3 * ci]});
                 }
             }
             XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
@@ -879,9 +906,9 @@ double Case::solve_system(int eqn, int comp, int* iters) {
             if (profiling) prof_n[4] += real;
             for (auto& sm : samples) {
                 if (sm.first >= real) continue;
-                float t = 0, tu = 0;
-                XCAL_CUDA(cudaEventElapsedTime(&t, sm.second[0], sm.second[1]));
-                prof_ms[0] += t;
+                float tm = 0, tu = 0;
+                XCAL_CUDA(cudaEventElapsedTime(&tm, sm.second[0], sm.second[1]));
+                prof_ms[0] += tm;
                 prof_n[0] += 1;
                 if (sm.first < done_it) {
                     XCAL_CUDA(cudaEventElapsedTime(&tu, sm.second[1], sm.second[2]));
@@ -893,27 +920,26 @@ double Case::solve_system(int eqn, int comp, int* iters) {
             if (chunk < CHUNK) chunk *= 2;
         }
     } else {
-        kr_init_resid(stream, A, nz, b, field, dx, x, q);  // r0 in q
-        apply_M(E, pt, q, r, nullptr);
-        kr_bicg_start(stream, n, b, r, pp, S, ws.part0.p, ws.part1.p);
-        // one BiCGSTAB iteration; e6 (optional) = events around both SpMVs
-        // and both preconditioner applications
+        apply_M(E, pt, nz, P, r0, r, (const KScalars*)nullptr);
+        kr_bicg_start(stream, n, c, (const T*)r, pp, S, ws.part0.p, ws.part1.p);
+        // one BiCGSTAB iteration; e (optional) = events around both SpMVs and
+        // both preconditioner applications
         auto iteration = [&](cudaEvent_t* e, bool capture) {
             if (e) rec(e[0], capture);
-            kr_spmv(stream, A, nz, pp, q, S);
+            kr_spmv(stream, A, nz, (const T*)pp, q, (const KScalars*)S);
             if (e) rec(e[1], capture);
-            apply_M(E, pt, q, v, S);
+            apply_M(E, pt, nz, P, (const T*)q, v, (const KScalars*)S);
             if (e) rec(e[2], capture);
-            kr_bicg_alpha(stream, n, b, v, S, ws.part0.p);
-            kr_bicg_s(stream, n, r, v, pp, s, x, S);
+            kr_bicg_alpha(stream, n, c, (const T*)v, S, ws.part0.p);
+            kr_bicg_s(stream, n, (const T*)r, (const T*)v, (const T*)pp, s, x, (const KScalars*)S);
             if (e) rec(e[3], capture);
-            kr_spmv(stream, A, nz, s, q, S);
+            kr_spmv(stream, A, nz, (const T*)s, q, (const KScalars*)S);
             if (e) rec(e[4], capture);
-            apply_M(E, pt, q, t, S);
+            apply_M(E, pt, nz, P, (const T*)q, t, (const KScalars*)S);
             if (e) rec(e[5], capture);
-            kr_bicg_omega(stream, n, t, s, S, ws.part0.p, ws.part1.p);
-            kr_bicg_xr(stream, n, x, s, t, r, b, S, ws.part0.p, ws.part1.p);
-            kr_bicg_p(stream, n, r, v, pp, S);
+            kr_bicg_omega(stream, n, (const T*)t, (const T*)s, S, ws.part0.p, ws.part1.p);
+            kr_bicg_xr(stream, n, x, (const T*)s, (const T*)t, r, c, S, ws.part0.p, ws.part1.p);
+            kr_bicg_p(stream, n, (const T*)r, (const T*)v, pp, (const KScalars*)S);
         };
         const int CHUNK = 8;
         int chunk = 1;
@@ -925,15 +951,15 @@ double Case::solve_system(int eqn, int comp, int* iters) {
             const bool graphed = chunk == CHUNK;
             std::vector<std::pair<int, cudaEvent_t*>> samples;
             if (graphed) {
-                if (profiling) samples.push_back({4, &gev[geq][0]});
-                replay_chunk(chunk_graph[geq][profiling ? 1 : 0], [&] {
-                    for (int c = 0; c < CHUNK; ++c) iteration(profiling && c == 4 ? &gev[geq][0] : nullptr, true);
+                if (profiling) samples.push_back({4, &gev[gk][0]});
+                replay_chunk(chunk_graph[gk][profiling ? 1 : 0], [&] {
+                    for (int ci = 0; ci < CHUNK; ++ci) iteration(profiling && ci == 4 ? &gev[gk][0] : nullptr, true);
                 });
             } else {
                 if (profiling) prof_reserve(3 * chunk);
-                for (int c = 0; c < chunk; ++c) {
-                    iteration(profiling ? &pev[6 * c] : nullptr, false);
-                    if (profiling) samples.push_back({c, &pev[6 * c]});
+                for (int ci = 0; ci < chunk; ++ci) {
+                    iteration(profiling ? &pev[6 * ci] : nullptr, false);
+                    if (profiling) samples.push_back({ci, &pev[6 * ci]});
                 }
             }
             XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
@@ -958,13 +984,89 @@ double Case::solve_system(int eqn, int comp, int* iters) {
             if (chunk < CHUNK) chunk *= 2;
         }
     }
-    kr_finish(stream, n, x, dx, field);
-    if (iters) *iters = hS->iter;
-    // residual (Solve_1_api.jl:441-464)
+}
+
+// solve_system! (Solve_1_api.jl:268-307)
+double Case::solve_system(int eqn, int comp, int* iters) {
+    bool isU = eqn == XCAL_EQN_U;
+    Equation& E = isU ? U : P;
+    const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
+    double* field = isU ? Uc[comp].p : p.p;
+    const double* b = isU ? U.b[comp].p : P.b[0].p;
+    KScalars* S = ws.S.p + (isU ? 0 : 1);
+    KScalars* hS = h_S + (isU ? 0 : 1);
+    int n = E.n;
+    CSRView A = E.view();
+    const double* nz = E.nz.p;
+    std::memset(hS, 0, sizeof(KScalars));
+    hS->atol = SS.atol;
+    hS->rtol = SS.rtol;
+    hS->itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
+    const int gk = isU ? comp : 3;
+    if (cfg.precision == XCAL_PREC_MIXED) {
+        solve_mixed(E, SS, field, b, S, hS, gk, iters);
+    } else {
+        XCAL_CUDA(cudaMemcpyAsync(S, hS, sizeof(KScalars), cudaMemcpyHostToDevice, stream));
+        KrylovVecs<double> V{ws.x.p, ws.r.p, ws.z.p, ws.p.p, ws.q.p, ws.v.p, ws.s.p, ws.t.p};
+        if (SS.solver == XCAL_SOLVER_CG) {
+            kr_init_resid(stream, A, nz, b, field, ws.dx.p, V.x, V.r);
+            krylov_iterate<double>(E, SS, nz, E.P.p, b, V.r, V, S, hS, gk);
+        } else {
+            kr_init_resid(stream, A, nz, b, field, ws.dx.p, V.x, V.q);  // r0 in q
+            krylov_iterate<double>(E, SS, nz, E.P.p, b, V.q, V, S, hS, gk);
+        }
+        kr_finish(stream, n, V.x, ws.dx.p, field);
+        if (iters) *iters = hS->iter;
+    }
+    // residual (Solve_1_api.jl:441-464), FP64 in both modes
     kr_residual(stream, A, nz, field, b, S, ws.part0.p, ws.part1.p, resbuf.p);
     XCAL_CUDA(cudaMemcpyAsync(h_res, resbuf.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();
     return h_res[0];
+}
+
+// Mixed precision: FP64 defect correction around FP32 Krylov solves.  Each
+// step forms d = b - A x in FP64 (A, b, x all FP64), solves A32 e = d32 in
+// FP32 from e = 0 with the FP32 copy of the preconditioner, and adds e to x
+// in FP64.  The loop ends when the inner solver's initial monitored norm of a
+// fresh defect is below the FP64 path's own target atol + rtol*||r0|| (r0 =
+// the first defect), so both modes stop on the same criterion; each inner
+// solve stops at max(target, inner_rtol * its initial norm).
+void Case::solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, const double* b, KScalars* S,
+                       KScalars* hS, int gk, int* iters) {
+    const int n = E.n;
+    CSRView A = E.view();
+    kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
+    if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, n, E.P.p, E.P32.p);
+    KrylovVecs<float> V{ws.fx.p, ws.fr.p, ws.fz.p, ws.fp.p, ws.fq.p, ws.fv.p, ws.fs.p, ws.ft.p};
+    hS->mixed = 1;
+    hS->inner_rtol = cfg.inner_rtol > 0 ? cfg.inner_rtol : 1e-3;
+    int total = 0;
+    const int max_outer = 64;
+    for (int outer = 0; outer < max_outer; ++outer) {
+        hS->outer = outer;
+        hS->iter = 0;
+        hS->done = 0;
+        hS->status = KS_RUNNING;
+        XCAL_CUDA(cudaMemcpyAsync(S, hS, sizeof(KScalars), cudaMemcpyHostToDevice, stream));
+        if (SS.solver == XCAL_SOLVER_CG) {
+            kr_defect(stream, A, E.nz.p, b, field, V.r, V.x);
+            krylov_iterate<float>(E, SS, E.nz32.p, E.P32.p, (const float*)V.r, V.r, V, S, hS, gk);
+        } else {
+            kr_defect(stream, A, E.nz.p, b, field, ws.fd.p, V.x);
+            krylov_iterate<float>(E, SS, E.nz32.p, E.P32.p, (const float*)ws.fd.p, ws.fd.p, V, S, hS, gk);
+        }
+        if (hS->outer_conv) break;  // this defect already met the target
+        total += hS->iter;
+        kr_correct(stream, n, field, V.x);
+        if (hS->status == KS_ZERO_CURV || hS->status == KS_BREAKDOWN || hS->status == KS_TIRED) break;
+        // An inner solve whose own target was the outer target and that met
+        // it leaves a defect at that target up to FP32 rounding of d (about
+        // 1e-7 relative): no further FP64 check is needed.
+        if (hS->status == KS_SOLVED && hS->eps <= hS->eps_outer) break;
+    }
+    last_outer[gk] = hS->outer + 1;
+    if (iters) *iters = total;
 }
 
 void Case::solve_equation_U(double res[3]) {  // Solve_1_api.jl:233-266

@@ -38,6 +38,7 @@ struct Equation {
     DBuf<unsigned char> d_len;
     int base(int r) const { return slice[r / SELL_C] + r % SELL_C; }
     DBuf<double> nz, nz0, diag0, P;
+    DBuf<float> nz32, P32;  // mixed precision: FP32 copies for the inner solves
     DBuf<double> b[3];
     // DILU level schedules (rows grouped by dependency level)
     DBuf<int> d_lower_rows, d_upper_rows;
@@ -53,14 +54,22 @@ struct BCTable {
     std::vector<double> val;
     DBuf<signed char> d_type;
     DBuf<double> d_val, d_pw, d_pwn, d_pEf, d_pDelta, d_pwdelta;
-    DBuf<int> d_peer_face, d_peer_cell, d_pNN, d_pNP, d_pPN;
+    DBuf<int> d_peer_face, d_peer_cell, d_pNN, d_pNP, d_pPN, d_pe_off, d_pe_face;
+    std::vector<int> h_pNP, h_pPN;  // periodic off-diagonal slots (parent faces; -1 elsewhere)
     bool has_periodic = false;
     BCView view() const;
 };
 
 struct KrylovWS {
     DBuf<double> x, dx, r, z, p, q, v, s, t, part0, part1;
+    DBuf<float> fx, fr, fz, fp, fq, fv, fs, ft, fd;  // mixed precision inner vectors
     DBuf<KScalars> S;  // [2]: U, p
+};
+
+// work vectors of one Krylov solve
+template <class T>
+struct KrylovVecs {
+    T *x, *r, *z, *p, *q, *v, *s, *t;
 };
 
 struct Case {
@@ -135,8 +144,16 @@ struct Case {
     MeshView mv() const { return mesh->view(); }
     double* field_comp(int field, int comp, long& count);
     void sync();
-    void dilu_ldiv(Equation& E, const double* b, double* out, const KScalars* S);
-    void apply_M(Equation& E, int ptype, const double* in, double* out, const KScalars* S);
+    template <class T>
+    void dilu_ldiv(Equation& E, const T* nz, const T* D, const T* b, T* out, const KScalars* S);
+    template <class T>
+    void apply_M(Equation& E, int ptype, const T* nz, const T* P, const T* in, T* out, const KScalars* S);
+    template <class T>
+    void krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c, const T* r0,
+                        const KrylovVecs<T>& V, KScalars* S, KScalars* hS, int gk);
+    void solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, const double* b, KScalars* S,
+                     KScalars* hS, int gk, int* iters);
+    int last_outer[4] = {0, 0, 0, 0};  // mixed: defect-correction steps of the last solve per system
 };
 
 }  // namespace xcal

@@ -42,36 +42,54 @@ void launch_correct_U(cudaStream_t s, int n, double* const H[3], const double* c
 void launch_relax_explicit(cudaStream_t s, int n, double* phi, const double* phi0, double alpha);
 void launch_courant(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* co);
 
-// Krylov kernels (kernels_krylov.cu)
+// Krylov kernels (kernels_krylov.cu).  Templates are instantiated for
+// T = double (plain FP64 path) and T = float (mixed-precision inner solves).
 void kr_init_resid(cudaStream_t s, const CSRView& A, const double* nz, const double* b, const double* field,
                    double* dx, double* x, double* r);
-void kr_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* x, double* y, const KScalars* S);
-void kr_jacobi_apply(cudaStream_t s, int n, const double* P, const double* r, double* z, const KScalars* S);
-void kr_copy(cudaStream_t s, int n, const double* a, double* b, const KScalars* S);
-void kr_cg_start(cudaStream_t s, int n, const double* r, const double* z, double* p, KScalars* S, double* part);
+// mixed precision: d = (float)(b - A*field), x = 0; field += x; dst = (float)src
+void kr_defect(cudaStream_t s, const CSRView& A, const double* nz, const double* b, const double* field, float* d,
+               float* x);
+void kr_correct(cudaStream_t s, int n, double* field, const float* x);
+void kr_to_float(cudaStream_t s, long n, const double* src, float* dst);
+template <class T>
+void kr_spmv(cudaStream_t s, const CSRView& A, const T* nz, const T* x, T* y, const KScalars* S);
+template <class T>
+void kr_jacobi_apply(cudaStream_t s, int n, const T* P, const T* r, T* z, const KScalars* S);
+template <class T>
+void kr_copy(cudaStream_t s, int n, const T* a, T* b, const KScalars* S);
+template <class T>
+void kr_cg_start(cudaStream_t s, int n, const T* r, const T* z, T* p, KScalars* S, double* part);
 // CG direction p_k lives in P0 (k even) / P1 (k odd); p_0 = z is stored in P0
-void kr_cg_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* z, double* P0, double* P1,
-                double* q, KScalars* S, double* part);
-void kr_cg_update(cudaStream_t s, int n, double* x, const double* P0, const double* P1, double* r, const double* q,
-                  double* z, const double* P, int jacobi_fused, KScalars* S, double* part);
-void kr_cg_rz(cudaStream_t s, int n, const double* r, const double* z, KScalars* S, double* part);
+template <class T>
+void kr_cg_spmv(cudaStream_t s, const CSRView& A, const T* nz, const T* z, T* P0, T* P1, T* q, KScalars* S,
+                double* part);
+template <class T>
+void kr_cg_update(cudaStream_t s, int n, T* x, const T* P0, const T* P1, T* r, const T* q, T* z, const T* P,
+                  int jacobi_fused, KScalars* S, double* part);
+template <class T>
+void kr_cg_rz(cudaStream_t s, int n, const T* r, const T* z, KScalars* S, double* part);
 void kr_finish(cudaStream_t s, int n, const double* x, const double* dx, double* field);
-void kr_bicg_start(cudaStream_t s, int n, const double* c, const double* r, double* p, KScalars* S, double* part0,
-                   double* part1);
-void kr_bicg_alpha(cudaStream_t s, int n, const double* c, const double* v, KScalars* S, double* part);
-void kr_bicg_s(cudaStream_t s, int n, const double* r, const double* v, const double* p, double* sv, double* x,
-               const KScalars* S);
-void kr_bicg_omega(cudaStream_t s, int n, const double* t, const double* sv, KScalars* S, double* part0,
-                   double* part1);
-void kr_bicg_xr(cudaStream_t s, int n, double* x, const double* sv, const double* t, double* r, const double* c,
-                KScalars* S, double* part0, double* part1);
-void kr_bicg_p(cudaStream_t s, int n, const double* r, const double* v, double* p, const KScalars* S);
+template <class T>
+void kr_bicg_start(cudaStream_t s, int n, const T* c, const T* r, T* p, KScalars* S, double* part0, double* part1);
+template <class T>
+void kr_bicg_alpha(cudaStream_t s, int n, const T* c, const T* v, KScalars* S, double* part);
+template <class T>
+void kr_bicg_s(cudaStream_t s, int n, const T* r, const T* v, const T* p, T* sv, T* x, const KScalars* S);
+template <class T>
+void kr_bicg_omega(cudaStream_t s, int n, const T* t, const T* sv, KScalars* S, double* part0, double* part1);
+template <class T>
+void kr_bicg_xr(cudaStream_t s, int n, T* x, const T* sv, const T* t, T* r, const T* c, KScalars* S, double* part0,
+                double* part1);
+template <class T>
+void kr_bicg_p(cudaStream_t s, int n, const T* r, const T* v, T* p, const KScalars* S);
 void kr_jacobi_update(cudaStream_t s, const CSRView& A, const double* nz, double* P);
 void kr_dilu_D(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, double* D);
-void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, const double* D,
-                 const double* b, double* y, const KScalars* S);
-void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, const double* D,
-                 double* x, const KScalars* S);
+template <class T>
+void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const T* nz, const T* D, const T* b,
+                 T* y, const KScalars* S);
+template <class T>
+void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const T* nz, const T* D, T* x,
+                 const KScalars* S);
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
                  double* part0, double* part1, double* out);
 

@@ -18,6 +18,39 @@ static inline int nblk(long n) { return (int)((n + TPB - 1) / TPB); }
 // value of a Dirichlet-like BC at boundary face f, component c
 __device__ __forceinline__ double bc_val(const BCView& bc, int f, int c) { return bc.val[3 * f + c]; }
 
+// Periodic parent face f (periodic.jl:261-443), one term at a time: the term
+// adds ac to the own diagonal and an to the (own, partner) slot, and -an to
+// the partner diagonal and -ac to the (partner, own) slot.
+// Divergence (sign +1, flux mdot_f):
+__device__ __forceinline__ void periodic_div(const BCView& bc, int f, double mdotf, int div_scheme, double& ac,
+                                             double& an) {
+    if (div_scheme == XCAL_DIV_UPWIND) {
+        double md = 1.0 * mdotf;
+        ac = jl_max(md, 0.0);
+        an = -jl_max(-md, 0.0);
+        return;
+    }
+    double w = bc.pw[f], wn = bc.pwn[f];
+    if (div_scheme == XCAL_DIV_LINEAR) {
+        double a = 1.0 * mdotf;
+        ac = a * w;
+        an = a * wn;
+    } else {  // LUST
+        double md = 1.0 * mdotf;
+        double acL = md * w, anL = md * wn;
+        double acU = jl_max(md, 0.0), anU = -jl_max(-md, 0.0);
+        ac = 0.75 * acL + 0.25 * acU;
+        an = 0.75 * anL + 0.25 * anU;
+    }
+}
+// Laplacian (sign -1, flux Gamma_f): gamma = (1 * (Gamma |E_f|)) / Delta;
+// ac = gamma, an = -gamma
+__device__ __forceinline__ void periodic_lap(const BCView& bc, int f, double flux, double& ac, double& an) {
+    double gamma = (1.0 * (flux * bc.pEf[f])) / bc.pDelta[f];
+    ac = gamma;
+    an = -gamma;
+}
+
 // U equation: terms Time + Divergence(mdotf,U) - Laplacian(nueff,U); returns
 // (AP, BP) summed over the terms in order (apply!, Discretise_5_apply_bcs.jl:158-183)
 __device__ void bc_U(const MeshView& m, const BCView& bc, int f, int cell, int comp, int div_scheme,
@@ -82,6 +115,12 @@ __device__ void bc_U(const MeshView& m, const BCView& bc, int f, int cell, int c
             bp_l = al * (vc - vn);
             break;
         }
+        case XCAL_BC_PERIODIC_PARENT: {  // own-row share; slots in k_bc_relax_U
+            double an;
+            periodic_div(bc, f, mdot[f], div_scheme, ap_d, an);
+            periodic_lap(bc, f, nueff[f], ap_l, an);
+            break;
+        }
         default:  // Empty, Periodic (shadow), none
             break;
     }
@@ -121,7 +160,12 @@ __device__ void bc_p(const MeshView& m, const BCView& bc, int f, int cell, const
             b = fl * bc_val(bc, f, 0);
             break;
         }
-        default:  // Wall, Zerogradient, Empty, Symmetry, Periodic: (0, 0)
+        case XCAL_BC_PERIODIC_PARENT: {  // own-row share; slots in k_bc_p
+            double an;
+            periodic_lap(bc, f, rDf[f], a, an);
+            break;
+        }
+        default:  // Wall, Zerogradient, Empty, Symmetry, Periodic shadow: (0, 0)
             break;
     }
     AP = 0.0 + a;
@@ -245,12 +289,40 @@ __global__ void k_bc_relax_U(MeshView m, CSRView A, BCView bc, int comp, int div
     double d = (flags & BCR_DIAG0) ? diag0[i] : nz[ds];
     double bi = b[i];
     if (flags & BCR_BC) {
-        for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
-            int f = m.bf_face[k];
-            double AP, BP;
-            bc_U(m, bc, f, i, comp, div_scheme, mdot, nueff, Ux, Uy, Uz, AP, BP);
-            d = d + AP;
-            bi = bi + BP;
+        // own boundary faces and the periodic parent faces this cell partners,
+        // merged in ascending face order (the reference's face loop order)
+        int k = m.bf_off[i], ke = m.bf_off[i + 1];
+        int q = bc.pe_off ? bc.pe_off[i] : 0, qe = bc.pe_off ? bc.pe_off[i + 1] : 0;
+        while (k < ke || q < qe) {
+            int fo = k < ke ? m.bf_face[k] : 0x7fffffff;
+            int fp = q < qe ? bc.pe_face[q] : 0x7fffffff;
+            if (fo < fp) {
+                double AP, BP;
+                bc_U(m, bc, fo, i, comp, div_scheme, mdot, nueff, Ux, Uy, Uz, AP, BP);
+                d = d + AP;
+                bi = bi + BP;
+                if (bc.type[fo] == XCAL_BC_PERIODIC_PARENT) {  // (own, partner) slot from A0 = 0
+                    double acd, and_, acl, anl;
+                    periodic_div(bc, fo, mdot[fo], div_scheme, acd, and_);
+                    periodic_lap(bc, fo, nueff[fo], acl, anl);
+                    double v = 0.0;
+                    v = v + and_;
+                    v = v + anl;
+                    nz[bc.pPN[fo]] = v;
+                }
+                ++k;
+            } else {  // this cell is the partner of parent face fp
+                double acd, and_, acl, anl;
+                periodic_div(bc, fp, mdot[fp], div_scheme, acd, and_);
+                periodic_lap(bc, fp, nueff[fp], acl, anl);
+                d = d + (-and_);
+                d = d + (-anl);
+                double v = 0.0;
+                v = v + (-acd);
+                v = v + (-acl);
+                nz[bc.pNP[fp]] = v;
+                ++q;
+            }
         }
     }
     if (!(flags & BCR_RELAX)) {
@@ -281,12 +353,31 @@ __global__ void k_bc_p(MeshView m, CSRView A, BCView bc, double* nz, double* b, 
     int ds = A.diag[i];
     double d = nz[ds];
     double bi = b[i];
-    for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
-        int f = m.bf_face[k];
-        double AP, BP;
-        bc_p(m, bc, f, i, rDf, p, AP, BP);
-        d = d + AP;
-        bi = bi + BP;
+    // own boundary faces merged with the periodic parent faces this cell
+    // partners, in ascending face order (see k_bc_relax_U)
+    int k = m.bf_off[i], ke = m.bf_off[i + 1];
+    int q = bc.pe_off ? bc.pe_off[i] : 0, qe = bc.pe_off ? bc.pe_off[i + 1] : 0;
+    while (k < ke || q < qe) {
+        int fo = k < ke ? m.bf_face[k] : 0x7fffffff;
+        int fp = q < qe ? bc.pe_face[q] : 0x7fffffff;
+        if (fo < fp) {
+            double AP, BP;
+            bc_p(m, bc, fo, i, rDf, p, AP, BP);
+            d = d + AP;
+            bi = bi + BP;
+            if (bc.type[fo] == XCAL_BC_PERIODIC_PARENT) {
+                double ac, an;
+                periodic_lap(bc, fo, rDf[fo], ac, an);
+                nz[bc.pPN[fo]] = 0.0 + an;
+            }
+            ++k;
+        } else {
+            double ac, an;
+            periodic_lap(bc, fp, rDf[fp], ac, an);
+            d = d + (-an);
+            nz[bc.pNP[fp]] = 0.0 + (-ac);
+            ++q;
+        }
     }
     nz[ds] = d;
     b[i] = bi;

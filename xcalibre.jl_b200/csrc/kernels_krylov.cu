@@ -1,4 +1,4 @@
-// kernels_krylov.cu -- Krylov solves of the hot path (FP64).
+// kernels_krylov.cu -- Krylov solves of the hot path.
 //
 // CG and BiCGSTAB follow Krylov.jl 0.10 (cg!, bicgstab!; called from
 // src/Solve/Solve_1_api.jl:286-289 with warm start, M = preconditioner,
@@ -6,6 +6,13 @@
 // canonical tile tree finished by the last block of the kernel, which also
 // takes the algorithm's scalar decisions (step sizes, stopping tests), so the
 // host only polls a `done` flag between chunks of iterations.
+//
+// Every Krylov kernel is a template over the value type T of the matrix and
+// the work vectors.  T = double is the plain FP64 path (its arithmetic is the
+// oracle's, operation for operation).  T = float is the inner solver of the
+// mixed-precision mode: FP32 matrix values, vectors and row sums, with dot
+// products accumulated in FP64 and the step scalars kept in FP64 on the
+// device and rounded to FP32 where they scale a vector.
 #include "dev_common.cuh"
 #include "kernels.hpp"
 
@@ -14,10 +21,10 @@ namespace xcal {
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double row_dot(const CSRView& A, const double* __restrict__ nz,
-                                          const double* __restrict__ x, int i) {
+template <class T>
+__device__ __forceinline__ T row_dot(const CSRView& A, const T* __restrict__ nz, const T* __restrict__ x, int i) {
     // xmul! row (src/Multithread/spmvm.jl:47-53): sequential from 0.0
-    double acc = 0.0;
+    T acc = T(0);
     const int rb = row_base(A, i), rl = A.len[i];
     for (int k = 0; k < rl; ++k) {
         int e = rb + SELL_C * k;
@@ -25,29 +32,6 @@ __device__ __forceinline__ double row_dot(const CSRView& A, const double* __rest
     }
     return acc;
 }
-
-// Tile SpMV: the thread owning canonical row k (row = tile*RED_TILE +
-// k*RED_THREADS + t) sums that row sequentially in CSR order (the reference's
-// row order).  Each thread only reads back its own rows, so the staging array
-// needs no barrier.  (Measured on the 128^3 7-point pattern: one thread per
-// row beats lane-grouped rows and smem-staged segments; with random numbering
-// the x gathers, not the matrix stream, bound it.)
-struct SpmvSmem {
-    double q[RED_TILE];
-};
-
-__device__ __forceinline__ void tile_spmv(const CSRView& A, const double* __restrict__ nz,
-                                          const double* __restrict__ x, SpmvSmem& sm) {
-    const int row0 = blockIdx.x * RED_TILE;
-    const int nrows = min(RED_TILE, A.n - row0);
-#pragma unroll
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int r = k * RED_THREADS + threadIdx.x;
-        if (r < nrows) sm.q[r] = row_dot(A, nz, x, row0 + r);
-    }
-}
-// (A x) of the thread's canonical row k (valid after tile_spmv)
-__device__ __forceinline__ double tile_q(const SpmvSmem& sm, int k) { return sm.q[k * RED_THREADS + threadIdx.x]; }
 
 // CG stopping decisions after gamma_next = <r,z> (Krylov.jl cg!)
 __device__ void cg_finalize(KScalars* S, double gamma_next) {
@@ -72,6 +56,22 @@ __device__ void cg_finalize(KScalars* S, double gamma_next) {
     }
 }
 
+// Stopping tolerance at the start of a solve.  Plain mode: Krylov.jl's
+// atol + rtol*||r0||.  Mixed mode (inner solve of a defect-correction
+// step): the outer target atol + rtol*||r0|| is fixed by the first defect of
+// the solve; an inner solve stops at the looser of that target and
+// inner_rtol times its own initial norm, and a defect already below the
+// target ends the outer loop.
+__device__ __forceinline__ void start_eps(KScalars* S, double rNorm) {
+    if (!S->mixed) {
+        S->eps = S->atol + S->rtol * rNorm;
+        return;
+    }
+    if (S->outer == 0) S->eps_outer = S->atol + S->rtol * rNorm;
+    S->eps = fmax(S->eps_outer, S->inner_rtol * rNorm);
+    S->outer_conv = rNorm <= S->eps_outer ? 1 : 0;
+}
+
 // ---------------------------------------------------------------------------
 // kernels (grid = one canonical tile per block, RED_THREADS threads)
 // ---------------------------------------------------------------------------
@@ -80,33 +80,58 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_init_resid(CSRView A, const 
                                                             const double* __restrict__ b,
                                                             const double* __restrict__ field, double* dx, double* x,
                                                             double* r) {
-    __shared__ SpmvSmem sm;
-    tile_spmv(A, nz, field, sm);
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < A.n) {
-            r[i] = b[i] - tile_q(sm, k);
+            r[i] = b[i] - row_dot(A, nz, field, i);
             x[i] = 0.0;
             dx[i] = field[i];
         }
     }
 }
 
-// y = A*x (plain SpMV, early exit when the solve is done)
-__global__ void __launch_bounds__(RED_THREADS, 8) k_spmv(CSRView A, const double* __restrict__ nz,
-                                                      const double* __restrict__ x, double* y, const KScalars* S) {
-    if (S && S->done) return;
-    __shared__ SpmvSmem sm;
-    tile_spmv(A, nz, x, sm);
+// Defect of a mixed-precision correction step: d = b - A*x in FP64, stored
+// rounded to FP32 as the inner right-hand side; the inner iterate starts at 0.
+__global__ void __launch_bounds__(RED_THREADS, 8) k_defect(CSRView A, const double* __restrict__ nz,
+                                                        const double* __restrict__ b,
+                                                        const double* __restrict__ field, float* d, float* x) {
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
-        if (i < A.n) y[i] = tile_q(sm, k);
+        if (i < A.n) {
+            d[i] = (float)(b[i] - row_dot(A, nz, field, i));
+            x[i] = 0.0f;
+        }
+    }
+}
+
+// field += correction (FP64 accumulation of the FP32 inner solution)
+__global__ void k_correct(int n, double* field, const float* __restrict__ x) {
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(k);
+        if (i < n) field[i] = field[i] + (double)x[i];
+    }
+}
+
+// dst = (float) src, any length
+__global__ void k_to_float(long n, const double* __restrict__ src, float* dst) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        dst[i] = (float)ld_stream(src + i);
+}
+
+// y = A*x (plain SpMV, early exit when the solve is done)
+template <class T>
+__global__ void __launch_bounds__(RED_THREADS, 8) k_spmv(CSRView A, const T* __restrict__ nz,
+                                                      const T* __restrict__ x, T* y, const KScalars* S) {
+    if (S && S->done) return;
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(k);
+        if (i < A.n) y[i] = row_dot(A, nz, x, i);
     }
 }
 
 // z = P .* r (Jacobi: opDiagonal multiply, ldiv = false)
-__global__ void k_jacobi_apply(int n, const double* __restrict__ P, const double* __restrict__ r, double* z,
-                               const KScalars* S) {
+template <class T>
+__global__ void k_jacobi_apply(int n, const T* __restrict__ P, const T* __restrict__ r, T* z, const KScalars* S) {
     if (S && S->done) return;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
@@ -114,7 +139,8 @@ __global__ void k_jacobi_apply(int n, const double* __restrict__ P, const double
     }
 }
 
-__global__ void k_copy(int n, const double* __restrict__ a, double* b, const KScalars* S) {
+template <class T>
+__global__ void k_copy(int n, const T* __restrict__ a, T* b, const KScalars* S) {
     if (S && S->done) return;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
@@ -124,16 +150,17 @@ __global__ void k_copy(int n, const double* __restrict__ a, double* b, const KSc
 
 // ---- CG ----
 // p = z; gamma = <r,z>; initial stopping tests
-__global__ void k_cg_start(int n, const double* __restrict__ r, const double* __restrict__ z, double* p,
-                           KScalars* S, double* part) {
+template <class T>
+__global__ void k_cg_start(int n, const T* __restrict__ r, const T* __restrict__ z, T* p, KScalars* S,
+                           double* part) {
     __shared__ double sm[8];
     double acc = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < n) {
-            double zi = z[i];
+            T zi = z[i];
             p[i] = zi;
-            acc = acc + r[i] * zi;
+            acc = acc + (double)r[i] * (double)zi;
         }
     }
     double tot = block_tree(acc, sm);
@@ -144,16 +171,19 @@ __global__ void k_cg_start(int n, const double* __restrict__ r, const double* __
         S->gamma = gamma;
         double rNorm = sqrt(gamma);
         S->rNorm = rNorm;
+        S->rNorm0 = rNorm;
         S->iter = 0;
         S->done = 0;
         S->status = KS_RUNNING;
+        S->outer_conv = 0;
         if (gamma == 0.0) {
             S->done = 1;
             S->status = KS_ZERO_RHS;
+            S->outer_conv = 1;
             return;
         }
         S->pNorm2 = gamma;
-        S->eps = S->atol + S->rtol * rNorm;
+        start_eps(S, rNorm);
         if (rNorm <= S->eps) {
             S->done = 1;
             S->status = KS_SOLVED;
@@ -169,26 +199,27 @@ __global__ void k_cg_start(int n, const double* __restrict__ r, const double* __
 // on the fly (Krylov.jl kaxpby!(n, 1, z, beta, p) -- the same expression for
 // every reader, so gathered neighbours see bit-identical values) and the
 // thread owning a row stores it.  The separate p-update pass disappears.
-__device__ __forceinline__ double cg_dir(const double* __restrict__ z, const double* __restrict__ pold, double beta,
-                                         int j) {
+template <class T>
+__device__ __forceinline__ T cg_dir(const T* __restrict__ z, const T* __restrict__ pold, T beta, int j) {
     return z[j] + beta * pold[j];
 }
 
 // q = A p_k; pAp = <p_k,q>; zero-curvature test; alpha = gamma / pAp
-__global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const double* __restrict__ nz,
-                                                         const double* __restrict__ z, double* P0, double* P1,
-                                                         double* q, KScalars* S, double* part) {
+template <class T>
+__global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const T* __restrict__ nz,
+                                                         const T* __restrict__ z, T* P0, T* P1, T* q, KScalars* S,
+                                                         double* part) {
     if (S->done) return;
     __shared__ double sm[8];
     const int it = S->iter;
-    const double beta = S->beta;
-    double* pk = (it & 1) ? P1 : P0;
-    const double* pold = (it & 1) ? P0 : P1;
+    const T beta = (T)S->beta;
+    T* pk = (it & 1) ? P1 : P0;
+    const T* pold = (it & 1) ? P0 : P1;
     double acc = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < A.n) {
-            double qi = 0.0, pi;
+            T qi = T(0), pi;
             const int rb = row_base(A, i), e1 = rb + SELL_C * A.len[i];
             if (it == 0) {
                 for (int e = rb; e < e1; e += SELL_C) qi = qi + ld_stream(nz + e) * pk[ld_stream(A.colval + e)];
@@ -200,7 +231,7 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const dou
                 pk[i] = pi;
             }
             q[i] = qi;
-            acc = acc + pi * qi;
+            acc = acc + (double)pi * (double)qi;
         }
     }
     double tot = block_tree(acc, sm);
@@ -208,7 +239,7 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const dou
     if (!last_block(&S->counter)) return;
     double pAp = reduce_partials(part, gridDim.x, sm);
     if (threadIdx.x == 0) {
-        const double epsT = 2.220446049250313e-16;  // eps(Float64)
+        const double epsT = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;  // eps(T)
         double lim = epsT * S->pNorm2;
         if (pAp <= lim && fabs(pAp) <= lim) {
             S->done = 1;
@@ -220,13 +251,14 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const dou
 }
 
 // x += alpha p_k; r -= alpha q; [Jacobi: z = P r; <r,z>; finalize]
-__global__ void k_cg_update(int n, double* x, const double* __restrict__ P0, const double* __restrict__ P1,
-                            double* r, const double* __restrict__ q, double* z, const double* __restrict__ P,
-                            int jacobi_fused, KScalars* S, double* part) {
+template <class T>
+__global__ void k_cg_update(int n, T* x, const T* __restrict__ P0, const T* __restrict__ P1, T* r,
+                            const T* __restrict__ q, T* z, const T* __restrict__ P, int jacobi_fused, KScalars* S,
+                            double* part) {
     if (S->done) return;
     __shared__ double sm[8];
-    const double* p = (S->iter & 1) ? P1 : P0;
-    double alpha = S->alpha;
+    const T* p = (S->iter & 1) ? P1 : P0;
+    const T alpha = (T)S->alpha;
     double acc = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
@@ -234,12 +266,12 @@ __global__ void k_cg_update(int n, double* x, const double* __restrict__ P0, con
             // x, q and P are not read again before the next update: evict-first
             // keeps L2 for z and p, which the next SpMV gathers
             __stcs(x + i, ld_stream(x + i) + alpha * p[i]);
-            double ri = r[i] + (-alpha) * ld_stream(q + i);
+            T ri = r[i] + (-alpha) * ld_stream(q + i);
             r[i] = ri;
             if (jacobi_fused) {
-                double zi = ld_stream(P + i) * ri;
+                T zi = ld_stream(P + i) * ri;
                 z[i] = zi;
-                acc = acc + ri * zi;
+                acc = acc + (double)ri * (double)zi;
             }
         }
     }
@@ -252,14 +284,14 @@ __global__ void k_cg_update(int n, double* x, const double* __restrict__ P0, con
 }
 
 // <r,z> + finalize when z came from a separate preconditioner apply
-__global__ void k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z, KScalars* S,
-                        double* part) {
+template <class T>
+__global__ void k_cg_rz(int n, const T* __restrict__ r, const T* __restrict__ z, KScalars* S, double* part) {
     if (S->done) return;
     __shared__ double sm[8];
     double acc = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
-        if (i < n) acc = acc + r[i] * z[i];
+        if (i < n) acc = acc + (double)r[i] * (double)z[i];
     }
     double tot = block_tree(acc, sm);
     if (threadIdx.x == 0) part[blockIdx.x] = tot;
@@ -278,17 +310,18 @@ __global__ void k_finish(int n, const double* __restrict__ x, const double* __re
 
 // ---- BiCGSTAB ----
 // p = r; rNorm = ||r||; next_rho = <c,r>; initial tests
-__global__ void k_bicg_start(int n, const double* __restrict__ c, const double* __restrict__ r, double* p,
-                             KScalars* S, double* part0, double* part1) {
+template <class T>
+__global__ void k_bicg_start(int n, const T* __restrict__ c, const T* __restrict__ r, T* p, KScalars* S,
+                             double* part0, double* part1) {
     __shared__ double sm[8];
     double a0 = 0.0, a1 = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < n) {
-            double ri = r[i];
+            T ri = r[i];
             p[i] = ri;
-            a0 = a0 + ri * ri;
-            a1 = a1 + c[i] * ri;
+            a0 = a0 + (double)ri * (double)ri;
+            a1 = a1 + (double)c[i] * (double)ri;
         }
     }
     double t0 = block_tree(a0, sm);
@@ -303,15 +336,18 @@ __global__ void k_bicg_start(int n, const double* __restrict__ c, const double* 
     if (threadIdx.x == 0) {
         double rNorm = sqrt(rr);
         S->rNorm = rNorm;
+        S->rNorm0 = rNorm;
         S->iter = 0;
         S->done = 0;
         S->status = KS_RUNNING;
+        S->outer_conv = 0;
         if (rNorm == 0.0) {
             S->done = 1;
             S->status = KS_ZERO_RHS;
+            S->outer_conv = 1;
             return;
         }
-        S->eps = S->atol + S->rtol * rNorm;
+        start_eps(S, rNorm);
         S->next_rho = cr;
         if (cr == 0.0) {
             S->done = 1;
@@ -329,14 +365,14 @@ __global__ void k_bicg_start(int n, const double* __restrict__ c, const double* 
 }
 
 // alpha = rho / <c,v> (rho = next_rho; iteration counter advances)
-__global__ void k_bicg_alpha(int n, const double* __restrict__ c, const double* __restrict__ v, KScalars* S,
-                             double* part) {
+template <class T>
+__global__ void k_bicg_alpha(int n, const T* __restrict__ c, const T* __restrict__ v, KScalars* S, double* part) {
     if (S->done) return;
     __shared__ double sm[8];
     double acc = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
-        if (i < n) acc = acc + c[i] * v[i];
+        if (i < n) acc = acc + (double)c[i] * (double)v[i];
     }
     double tot = block_tree(acc, sm);
     if (threadIdx.x == 0) part[blockIdx.x] = tot;
@@ -351,10 +387,11 @@ __global__ void k_bicg_alpha(int n, const double* __restrict__ c, const double* 
 }
 
 // s = r - alpha v; x = x + alpha p
-__global__ void k_bicg_s(int n, const double* __restrict__ r, const double* __restrict__ v,
-                         const double* __restrict__ p, double* s, double* x, const KScalars* S) {
+template <class T>
+__global__ void k_bicg_s(int n, const T* __restrict__ r, const T* __restrict__ v, const T* __restrict__ p, T* s,
+                         T* x, const KScalars* S) {
     if (S->done) return;
-    double alpha = S->alpha;
+    const T alpha = (T)S->alpha;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < n) {
@@ -365,16 +402,17 @@ __global__ void k_bicg_s(int n, const double* __restrict__ r, const double* __re
 }
 
 // omega = <t,s> / <t,t>
-__global__ void k_bicg_omega(int n, const double* __restrict__ t, const double* __restrict__ s, KScalars* S,
-                             double* part0, double* part1) {
+template <class T>
+__global__ void k_bicg_omega(int n, const T* __restrict__ t, const T* __restrict__ s, KScalars* S, double* part0,
+                             double* part1) {
     if (S->done) return;
     __shared__ double sm[8];
     double a0 = 0.0, a1 = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < n) {
-            double ti = t[i];
-            a0 = a0 + ti * s[i];
+            double ti = (double)t[i];
+            a0 = a0 + ti * (double)s[i];
             a1 = a1 + ti * ti;
         }
     }
@@ -391,21 +429,23 @@ __global__ void k_bicg_omega(int n, const double* __restrict__ t, const double* 
 }
 
 // x = x + omega s; r = s - omega t; next_rho = <c,r>; ||r||; stopping tests
-__global__ void k_bicg_xr(int n, double* x, const double* __restrict__ s, const double* __restrict__ t, double* r,
-                          const double* __restrict__ c, KScalars* S, double* part0, double* part1) {
+template <class T>
+__global__ void k_bicg_xr(int n, T* x, const T* __restrict__ s, const T* __restrict__ t, T* r,
+                          const T* __restrict__ c, KScalars* S, double* part0, double* part1) {
     if (S->done) return;
     __shared__ double sm[8];
-    double omega = S->omega;
+    const double omega = S->omega;
+    const T om = (T)omega;
     double a0 = 0.0, a1 = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < n) {
-            double si = s[i];
-            x[i] = x[i] + omega * si;
-            double ri = si + (-omega) * t[i];
+            T si = s[i];
+            x[i] = x[i] + om * si;
+            T ri = si + (-om) * t[i];
             r[i] = ri;
-            a0 = a0 + c[i] * ri;
-            a1 = a1 + ri * ri;
+            a0 = a0 + (double)c[i] * (double)ri;
+            a1 = a1 + (double)ri * (double)ri;
         }
     }
     double t0 = block_tree(a0, sm);
@@ -440,10 +480,10 @@ __global__ void k_bicg_xr(int n, double* x, const double* __restrict__ s, const 
 }
 
 // p = r + beta (p - omega v)
-__global__ void k_bicg_p(int n, const double* __restrict__ r, const double* __restrict__ v, double* p,
-                         const KScalars* S) {
+template <class T>
+__global__ void k_bicg_p(int n, const T* __restrict__ r, const T* __restrict__ v, T* p, const KScalars* S) {
     if (S->done) return;
-    double beta = S->beta, omega = S->omega;
+    const T beta = (T)S->beta, omega = (T)S->omega;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < n) p[i] = r[i] + beta * (p[i] + (-omega) * v[i]);
@@ -479,31 +519,32 @@ __global__ void k_dilu_D(const int* __restrict__ rows, int nrows, CSRView A, con
 }
 
 // forward_substitution! (preconditioners_1_DILU.jl:84-98), one level
-__global__ void k_dilu_fwd(const int* __restrict__ rows, int nrows, CSRView A, const double* __restrict__ nz,
-                           const double* __restrict__ D, const double* __restrict__ b, double* y,
-                           const KScalars* S) {
+template <class T>
+__global__ void k_dilu_fwd(const int* __restrict__ rows, int nrows, CSRView A, const T* __restrict__ nz,
+                           const T* __restrict__ D, const T* __restrict__ b, T* y, const KScalars* S) {
     if (S && S->done) return;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nrows) return;
     int i = rows[t];
     int ds = A.diag[i];
-    double sum = 0.0;
+    T sum = T(0);
     for (int e = row_base(A, i); e < ds; e += SELL_C) {
         int j = ld_stream(A.colval + e);
-        sum = sum + (ld_stream(nz + e) * y[j]) * (1.0 / D[j]);
+        sum = sum + (ld_stream(nz + e) * y[j]) * (T(1) / D[j]);
     }
     y[i] = b[i] - sum;
 }
 
 // backward_substitution! (preconditioners_1_DILU.jl:100-114), one level, in place
-__global__ void k_dilu_bwd(const int* __restrict__ rows, int nrows, CSRView A, const double* __restrict__ nz,
-                           const double* __restrict__ D, double* x, const KScalars* S) {
+template <class T>
+__global__ void k_dilu_bwd(const int* __restrict__ rows, int nrows, CSRView A, const T* __restrict__ nz,
+                           const T* __restrict__ D, T* x, const KScalars* S) {
     if (S && S->done) return;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nrows) return;
     int i = rows[t];
     int ds = A.diag[i];
-    double sum = 0.0;
+    T sum = T(0);
     int e1 = row_base(A, i) + SELL_C * A.len[i];
     for (int e = ds + SELL_C; e < e1; e += SELL_C) sum = sum + ld_stream(nz + e) * x[ld_stream(A.colval + e)];
     x[i] = (x[i] - sum) / D[i];
@@ -514,13 +555,11 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_residual(CSRView A, const do
                                                           const double* __restrict__ x, const double* __restrict__ b,
                                                           KScalars* S, double* part0, double* part1, double* out) {
     __shared__ double sm[8];
-    __shared__ SpmvSmem ssm;
-    tile_spmv(A, nz, x, ssm);
     double a0 = 0.0, a1 = 0.0;
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(k);
         if (i < A.n) {
-            double fx = tile_q(ssm, k);
+            double fx = row_dot(A, nz, x, i);
             double bi = b[i];
             double d = bi - fx;
             a0 = a0 + d * d;
@@ -557,66 +596,92 @@ void kr_init_resid(cudaStream_t s, const CSRView& A, const double* nz, const dou
     k_init_resid<<<TILE_LAUNCH(A.n), s>>>(A, nz, b, field, dx, x, r);
     XCAL_CHECK_LAUNCH();
 }
-void kr_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* x, double* y, const KScalars* S) {
-    k_spmv<<<TILE_LAUNCH(A.n), s>>>(A, nz, x, y, S);
+void kr_defect(cudaStream_t s, const CSRView& A, const double* nz, const double* b, const double* field, float* d,
+               float* x) {
+    k_defect<<<TILE_LAUNCH(A.n), s>>>(A, nz, b, field, d, x);
     XCAL_CHECK_LAUNCH();
 }
-void kr_jacobi_apply(cudaStream_t s, int n, const double* P, const double* r, double* z, const KScalars* S) {
-    k_jacobi_apply<<<TILE_LAUNCH(n), s>>>(n, P, r, z, S);
+void kr_correct(cudaStream_t s, int n, double* field, const float* x) {
+    k_correct<<<TILE_LAUNCH(n), s>>>(n, field, x);
     XCAL_CHECK_LAUNCH();
 }
-void kr_copy(cudaStream_t s, int n, const double* a, double* b, const KScalars* S) {
-    k_copy<<<TILE_LAUNCH(n), s>>>(n, a, b, S);
+void kr_to_float(cudaStream_t s, long n, const double* src, float* dst) {
+    if (n <= 0) return;
+    long blocks = (n + 255) / 256;
+    k_to_float<<<(int)(blocks < 148L * 16 ? blocks : 148L * 16), 256, 0, s>>>(n, src, dst);
     XCAL_CHECK_LAUNCH();
 }
-void kr_cg_start(cudaStream_t s, int n, const double* r, const double* z, double* p, KScalars* S, double* part) {
-    k_cg_start<<<TILE_LAUNCH(n), s>>>(n, r, z, p, S, part);
+template <class T>
+void kr_spmv(cudaStream_t s, const CSRView& A, const T* nz, const T* x, T* y, const KScalars* S) {
+    k_spmv<T><<<TILE_LAUNCH(A.n), s>>>(A, nz, x, y, S);
     XCAL_CHECK_LAUNCH();
 }
-void kr_cg_spmv(cudaStream_t s, const CSRView& A, const double* nz, const double* z, double* P0, double* P1,
-                double* q, KScalars* S, double* part) {
-    k_cg_spmv<<<TILE_LAUNCH(A.n), s>>>(A, nz, z, P0, P1, q, S, part);
+template <class T>
+void kr_jacobi_apply(cudaStream_t s, int n, const T* P, const T* r, T* z, const KScalars* S) {
+    k_jacobi_apply<T><<<TILE_LAUNCH(n), s>>>(n, P, r, z, S);
     XCAL_CHECK_LAUNCH();
 }
-void kr_cg_update(cudaStream_t s, int n, double* x, const double* P0, const double* P1, double* r, const double* q,
-                  double* z, const double* P, int jacobi_fused, KScalars* S, double* part) {
-    k_cg_update<<<TILE_LAUNCH(n), s>>>(n, x, P0, P1, r, q, z, P, jacobi_fused, S, part);
+template <class T>
+void kr_copy(cudaStream_t s, int n, const T* a, T* b, const KScalars* S) {
+    k_copy<T><<<TILE_LAUNCH(n), s>>>(n, a, b, S);
     XCAL_CHECK_LAUNCH();
 }
-void kr_cg_rz(cudaStream_t s, int n, const double* r, const double* z, KScalars* S, double* part) {
-    k_cg_rz<<<TILE_LAUNCH(n), s>>>(n, r, z, S, part);
+template <class T>
+void kr_cg_start(cudaStream_t s, int n, const T* r, const T* z, T* p, KScalars* S, double* part) {
+    k_cg_start<T><<<TILE_LAUNCH(n), s>>>(n, r, z, p, S, part);
+    XCAL_CHECK_LAUNCH();
+}
+template <class T>
+void kr_cg_spmv(cudaStream_t s, const CSRView& A, const T* nz, const T* z, T* P0, T* P1, T* q, KScalars* S,
+                double* part) {
+    k_cg_spmv<T><<<TILE_LAUNCH(A.n), s>>>(A, nz, z, P0, P1, q, S, part);
+    XCAL_CHECK_LAUNCH();
+}
+template <class T>
+void kr_cg_update(cudaStream_t s, int n, T* x, const T* P0, const T* P1, T* r, const T* q, T* z, const T* P,
+                  int jacobi_fused, KScalars* S, double* part) {
+    k_cg_update<T><<<TILE_LAUNCH(n), s>>>(n, x, P0, P1, r, q, z, P, jacobi_fused, S, part);
+    XCAL_CHECK_LAUNCH();
+}
+template <class T>
+void kr_cg_rz(cudaStream_t s, int n, const T* r, const T* z, KScalars* S, double* part) {
+    k_cg_rz<T><<<TILE_LAUNCH(n), s>>>(n, r, z, S, part);
     XCAL_CHECK_LAUNCH();
 }
 void kr_finish(cudaStream_t s, int n, const double* x, const double* dx, double* field) {
     k_finish<<<TILE_LAUNCH(n), s>>>(n, x, dx, field);
     XCAL_CHECK_LAUNCH();
 }
-void kr_bicg_start(cudaStream_t s, int n, const double* c, const double* r, double* p, KScalars* S, double* part0,
+template <class T>
+void kr_bicg_start(cudaStream_t s, int n, const T* c, const T* r, T* p, KScalars* S, double* part0,
                    double* part1) {
-    k_bicg_start<<<TILE_LAUNCH(n), s>>>(n, c, r, p, S, part0, part1);
+    k_bicg_start<T><<<TILE_LAUNCH(n), s>>>(n, c, r, p, S, part0, part1);
     XCAL_CHECK_LAUNCH();
 }
-void kr_bicg_alpha(cudaStream_t s, int n, const double* c, const double* v, KScalars* S, double* part) {
-    k_bicg_alpha<<<TILE_LAUNCH(n), s>>>(n, c, v, S, part);
+template <class T>
+void kr_bicg_alpha(cudaStream_t s, int n, const T* c, const T* v, KScalars* S, double* part) {
+    k_bicg_alpha<T><<<TILE_LAUNCH(n), s>>>(n, c, v, S, part);
     XCAL_CHECK_LAUNCH();
 }
-void kr_bicg_s(cudaStream_t s_, int n, const double* r, const double* v, const double* p, double* s, double* x,
-               const KScalars* S) {
-    k_bicg_s<<<TILE_LAUNCH(n), s_>>>(n, r, v, p, s, x, S);
+template <class T>
+void kr_bicg_s(cudaStream_t s_, int n, const T* r, const T* v, const T* p, T* s, T* x, const KScalars* S) {
+    k_bicg_s<T><<<TILE_LAUNCH(n), s_>>>(n, r, v, p, s, x, S);
     XCAL_CHECK_LAUNCH();
 }
-void kr_bicg_omega(cudaStream_t s_, int n, const double* t, const double* s, KScalars* S, double* part0,
-                   double* part1) {
-    k_bicg_omega<<<TILE_LAUNCH(n), s_>>>(n, t, s, S, part0, part1);
+template <class T>
+void kr_bicg_omega(cudaStream_t s_, int n, const T* t, const T* s, KScalars* S, double* part0, double* part1) {
+    k_bicg_omega<T><<<TILE_LAUNCH(n), s_>>>(n, t, s, S, part0, part1);
     XCAL_CHECK_LAUNCH();
 }
-void kr_bicg_xr(cudaStream_t s_, int n, double* x, const double* s, const double* t, double* r, const double* c,
-                KScalars* S, double* part0, double* part1) {
-    k_bicg_xr<<<TILE_LAUNCH(n), s_>>>(n, x, s, t, r, c, S, part0, part1);
+template <class T>
+void kr_bicg_xr(cudaStream_t s_, int n, T* x, const T* s, const T* t, T* r, const T* c, KScalars* S,
+                double* part0, double* part1) {
+    k_bicg_xr<T><<<TILE_LAUNCH(n), s_>>>(n, x, s, t, r, c, S, part0, part1);
     XCAL_CHECK_LAUNCH();
 }
-void kr_bicg_p(cudaStream_t s, int n, const double* r, const double* v, double* p, const KScalars* S) {
-    k_bicg_p<<<TILE_LAUNCH(n), s>>>(n, r, v, p, S);
+template <class T>
+void kr_bicg_p(cudaStream_t s, int n, const T* r, const T* v, T* p, const KScalars* S) {
+    k_bicg_p<T><<<TILE_LAUNCH(n), s>>>(n, r, v, p, S);
     XCAL_CHECK_LAUNCH();
 }
 void kr_jacobi_update(cudaStream_t s, const CSRView& A, const double* nz, double* P) {
@@ -628,16 +693,18 @@ void kr_dilu_D(cudaStream_t s, const int* rows, int nrows, const CSRView& A, con
     k_dilu_D<<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, A, nz, D);
     XCAL_CHECK_LAUNCH();
 }
-void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, const double* D,
-                 const double* b, double* y, const KScalars* S) {
+template <class T>
+void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const T* nz, const T* D, const T* b,
+                 T* y, const KScalars* S) {
     if (nrows <= 0) return;
-    k_dilu_fwd<<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, A, nz, D, b, y, S);
+    k_dilu_fwd<T><<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, A, nz, D, b, y, S);
     XCAL_CHECK_LAUNCH();
 }
-void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, const double* D,
-                 double* x, const KScalars* S) {
+template <class T>
+void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const T* nz, const T* D, T* x,
+                 const KScalars* S) {
     if (nrows <= 0) return;
-    k_dilu_bwd<<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, A, nz, D, x, S);
+    k_dilu_bwd<T><<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, A, nz, D, x, S);
     XCAL_CHECK_LAUNCH();
 }
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
@@ -645,5 +712,30 @@ void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const doubl
     k_residual<<<TILE_LAUNCH(A.n), s>>>(A, nz, x, b, S, part0, part1, out);
     XCAL_CHECK_LAUNCH();
 }
+
+// the two value types of the Krylov launchers
+#define XCAL_KRYLOV_INSTANTIATE(T)                                                                              \
+    template void kr_spmv<T>(cudaStream_t, const CSRView&, const T*, const T*, T*, const KScalars*);             \
+    template void kr_jacobi_apply<T>(cudaStream_t, int, const T*, const T*, T*, const KScalars*);                \
+    template void kr_copy<T>(cudaStream_t, int, const T*, T*, const KScalars*);                                  \
+    template void kr_cg_start<T>(cudaStream_t, int, const T*, const T*, T*, KScalars*, double*);                 \
+    template void kr_cg_spmv<T>(cudaStream_t, const CSRView&, const T*, const T*, T*, T*, T*, KScalars*,         \
+                                double*);                                                                       \
+    template void kr_cg_update<T>(cudaStream_t, int, T*, const T*, const T*, T*, const T*, T*, const T*, int,    \
+                                  KScalars*, double*);                                                          \
+    template void kr_cg_rz<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*);                        \
+    template void kr_bicg_start<T>(cudaStream_t, int, const T*, const T*, T*, KScalars*, double*, double*);      \
+    template void kr_bicg_alpha<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*);                   \
+    template void kr_bicg_s<T>(cudaStream_t, int, const T*, const T*, const T*, T*, T*, const KScalars*);        \
+    template void kr_bicg_omega<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*, double*);          \
+    template void kr_bicg_xr<T>(cudaStream_t, int, T*, const T*, const T*, T*, const T*, KScalars*, double*,     \
+                                double*);                                                                       \
+    template void kr_bicg_p<T>(cudaStream_t, int, const T*, const T*, T*, const KScalars*);                      \
+    template void kr_dilu_fwd<T>(cudaStream_t, const int*, int, const CSRView&, const T*, const T*, const T*, T*, \
+                                 const KScalars*);                                                              \
+    template void kr_dilu_bwd<T>(cudaStream_t, const int*, int, const CSRView&, const T*, const T*, T*,          \
+                                 const KScalars*);
+XCAL_KRYLOV_INSTANTIATE(double)
+XCAL_KRYLOV_INSTANTIATE(float)
 
 }  // namespace xcal

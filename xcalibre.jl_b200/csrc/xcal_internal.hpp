@@ -148,6 +148,10 @@ struct BCView {
     const int* pNN;            // parent: CSR slot (partner cell, partner cell)
     const int* pNP;            // parent: CSR slot (partner cell, own cell)
     const int* pPN;            // parent: CSR slot (own cell, partner cell)
+    // per cell: the periodic parent faces whose partner cell it is, ascending
+    // ([nC+1] offsets, or null when the field has no periodic pair)
+    const int* pe_off;
+    const int* pe_face;
 };
 
 // per-solve device scalars (Krylov state), one 128-byte aligned block
@@ -155,10 +159,14 @@ struct alignas(128) KScalars {
     double gamma, rNorm, eps, pNorm2, alpha, beta;   // CG
     double rho, next_rho, omega, cv, resid, normb;   // BiCGSTAB / residual
     double atol, rtol;
+    double rNorm0;                                    // monitored norm at the start of the solve
+    // mixed precision (defect correction): outer target, inner relative
+    // tolerance, outer step index, "defect already below target"
+    double eps_outer, inner_rtol;
+    int mixed, outer, outer_conv;
     int iter, itmax, done, status;
     unsigned int counter;                             // last-block ticket
     unsigned int counter2;
-    int pad[6];
 };
 enum { KS_RUNNING = 0, KS_SOLVED = 1, KS_TIRED = 2, KS_ZERO_CURV = 3, KS_BREAKDOWN = 4, KS_ZERO_RHS = 5 };
 
