@@ -603,6 +603,11 @@ class Case:
     def set_profiling(self, on: bool = True):
         self._chk(lib().xcal_case_set_profiling(self.h, 1 if on else 0))
 
+    def set_graph_mode(self, on: bool = True):
+        """Replay each SIMPLE iteration / PISO step as one captured CUDA graph
+        (device-driven Krylov loops; same results as the default mode)."""
+        self._chk(lib().xcal_case_set_graph_mode(self.h, 1 if on else 0))
+
     def profile(self, which: int):
         """(summed device ms, timed launches) of a kernel class:
         0 = CG SpMV, 1 = BiCGSTAB SpMV, 2 = DILU applications, 3 = CG update;

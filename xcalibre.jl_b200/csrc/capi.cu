@@ -324,6 +324,12 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable) {
     return XCAL_OK;
 }
 
+int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable) {
+    if (!cs) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    XCAL_GUARD(c->ctx, { c->set_graph_mode(enable != 0); })
+}
+
 int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches) {
     if (!cs || which < 0 || which > 4) return XCAL_ERR_INVALID;
     if (ms) *ms = cs->c->prof_ms[which];

@@ -582,7 +582,7 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     XCAL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     for (auto& e : ev) XCAL_CUDA(cudaEventCreate(&e));
     XCAL_CUDA(cudaMallocHost(&h_S, 2 * sizeof(KScalars)));
-    XCAL_CUDA(cudaMallocHost(&h_res, 8 * sizeof(double)));
+    XCAL_CUDA(cudaMallocHost(&h_res, 16 * sizeof(double)));
     int nC = m->nC, nF = m->nF;
     std::vector<xcal_bc> bU(cfg.bc_U, cfg.bc_U + cfg.n_bc_U), bP(cfg.bc_p, cfg.bc_p + cfg.n_bc_p);
     build_equation(U, *m, bU, 3, cfg.U_solver.precond == XCAL_PRECOND_DILU, stream);
@@ -635,6 +635,16 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     resbuf.alloc(8);
     resbuf.zero(stream);
     cmax.alloc(T);
+    cmax_ctr.alloc(1);
+    cmax_ctr.zero(stream);
+    gres.alloc(GRES_N);
+    gres.zero(stream);
+    giters.alloc(2 * 4);
+    giters.zero(stream);
+    dlaunch.alloc(1);
+    dlaunch.zero(stream);
+    XCAL_CUDA(cudaMallocHost(&h_iters, 8 * sizeof(int)));
+    XCAL_CUDA(cudaMallocHost(&h_launch, sizeof(unsigned long long)));
     // host-side per-cell constants: V^(1/3) (Courant) and the LES filter
     std::vector<double> h(nC);
     for (int i = 0; i < nC; ++i) h[i] = std::pow(m->vol[i], 1.0 / 3.0);
@@ -682,6 +692,11 @@ Case::~Case() {
     for (auto& e : pev) cudaEventDestroy(e);
     if (h_S) cudaFreeHost(h_S);
     if (h_res) cudaFreeHost(h_res);
+    if (h_iters) cudaFreeHost(h_iters);
+    if (h_launch) cudaFreeHost(h_launch);
+    if (step_graph) cudaGraphExecDestroy(step_graph);
+    for (cudaStream_t& sd : side)
+        if (sd) cudaStreamDestroy(sd);
     if (stream && own_stream) cudaStreamDestroy(stream);
 }
 
@@ -832,76 +847,121 @@ void Case::apply_M(Equation& E, int ptype, const T* nz, const T* P, const T* in,
         kr_copy(stream, E.n, in, out, S);
 }
 
-// Krylov iterations of one solve, from its initial residual on.  CG: V.r
-// holds r0.  BiCGSTAB: r0 holds the unpreconditioned r0 and c is Krylov.jl's
-// shadow vector (the right-hand side).  gk selects the cached chunk graphs.
+// Start of a Krylov solve from its initial residual.  CG: V.r holds r0.
+// BiCGSTAB: r0 holds the unpreconditioned r0 and c is Krylov.jl's shadow
+// vector (the right-hand side).
 template <class T>
-void Case::krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c,
-                          const T* r0, const KrylovVecs<T>& V, KScalars* S, KScalars* hS, int gk) {
+void Case::krylov_start(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c, const T* r0,
+                        const KrylovVecs<T>& V, KScalars* S) {
+    const int n = E.n;
+    const int pt = SS.precond;
+    if (SS.solver == XCAL_SOLVER_CG) {
+        T* zz = pt == XCAL_PRECOND_NONE ? V.r : V.z;
+        if (pt != XCAL_PRECOND_NONE) apply_M(E, pt, nz, P, (const T*)V.r, zz, (const KScalars*)nullptr);
+        kr_cg_start(stream, n, (const T*)V.r, (const T*)zz, V.p, S, ws.part0.p);
+    } else {
+        apply_M(E, pt, nz, P, r0, V.r, (const KScalars*)nullptr);
+        kr_bicg_start(stream, n, c, (const T*)V.r, V.p, S, ws.part0.p, ws.part1.p);
+    }
+}
+
+// One Krylov iteration (every kernel returns at once when the solve is done).
+// ev (optional): CG -- events before the SpMV, between SpMV and update, after
+// the update; BiCGSTAB -- around both SpMVs and both preconditioner
+// applications.  in_capture: record the events as graph event nodes.
+template <class T>
+void Case::krylov_step(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c,
+                       const KrylovVecs<T>& V, KScalars* S, cudaEvent_t* ev, bool in_capture) {
     const int n = E.n;
     const int pt = SS.precond;
     CSRView A = E.view();
-    T *x = V.x, *r = V.r, *z = V.z, *pp = V.p, *q = V.q, *v = V.v, *s = V.s, *t = V.t;
-    // event record usable both inside a stream capture (becomes an event node)
-    // and on a live stream
-    auto rec = [&](cudaEvent_t e, bool capture) {
-        if (capture)
+    auto rec = [&](cudaEvent_t e) {
+        if (in_capture)
             XCAL_CUDA(cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal));
         else
             XCAL_CUDA(cudaEventRecord(e, stream));
     };
+    T *x = V.x, *r = V.r, *pp = V.p, *q = V.q, *v = V.v, *s = V.s, *t = V.t;
+    if (SS.solver == XCAL_SOLVER_CG) {
+        T* zz = pt == XCAL_PRECOND_NONE ? r : V.z;
+        if (ev) rec(ev[0]);
+        // p_k alternates between pp (even k) and v (odd k)
+        kr_cg_spmv(stream, A, nz, (const T*)zz, pp, v, q, S, ws.part0.p);
+        if (ev) rec(ev[1]);
+        if (pt == XCAL_PRECOND_JACOBI) {
+            kr_cg_update(stream, n, x, (const T*)pp, (const T*)v, r, (const T*)q, zz, P, 1, S, ws.part0.p);
+        } else {
+            kr_cg_update(stream, n, x, (const T*)pp, (const T*)v, r, (const T*)q, zz, P, 0, S, ws.part0.p);
+            if (pt == XCAL_PRECOND_DILU) dilu_ldiv(E, nz, P, (const T*)r, zz, (const KScalars*)S);
+            kr_cg_rz(stream, n, (const T*)r, (const T*)zz, S, ws.part0.p);
+        }
+        if (ev) rec(ev[2]);
+    } else {
+        if (ev) rec(ev[0]);
+        kr_spmv(stream, A, nz, (const T*)pp, q, (const KScalars*)S);
+        if (ev) rec(ev[1]);
+        apply_M(E, pt, nz, P, (const T*)q, v, (const KScalars*)S);
+        if (ev) rec(ev[2]);
+        kr_bicg_alpha(stream, n, c, (const T*)v, S, ws.part0.p);
+        kr_bicg_s(stream, n, (const T*)r, (const T*)v, (const T*)pp, s, x, (const KScalars*)S);
+        if (ev) rec(ev[3]);
+        kr_spmv(stream, A, nz, (const T*)s, q, (const KScalars*)S);
+        if (ev) rec(ev[4]);
+        apply_M(E, pt, nz, P, (const T*)q, t, (const KScalars*)S);
+        if (ev) rec(ev[5]);
+        kr_bicg_omega(stream, n, (const T*)t, (const T*)s, S, ws.part0.p, ws.part1.p);
+        kr_bicg_xr(stream, n, x, (const T*)s, (const T*)t, r, c, S, ws.part0.p, ws.part1.p);
+        kr_bicg_p(stream, n, (const T*)r, (const T*)v, pp, (const KScalars*)S);
+    }
+}
+
+// Host-polled Krylov loop: chunks of iterations (4 -> 32 CG, 1 -> 8
+// BiCGSTAB), the steady-state chunk replayed as a cached CUDA graph, the
+// host reading the device's `done` flag after each chunk.  gk selects the
+// cached chunk graphs.
+template <class T>
+void Case::krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c,
+                          const T* r0, const KrylovVecs<T>& V, KScalars* S, KScalars* hS, int gk) {
+    const bool cg = SS.solver == XCAL_SOLVER_CG;
+    const int pt = SS.precond;
     if (profiling)
         for (auto& e : gev[gk])
             if (!e) XCAL_CUDA(cudaEventCreate(&e));
-    if (SS.solver == XCAL_SOLVER_CG) {
-        T* zz = pt == XCAL_PRECOND_NONE ? r : z;
-        if (pt != XCAL_PRECOND_NONE) apply_M(E, pt, nz, P, (const T*)r, zz, (const KScalars*)nullptr);
-        kr_cg_start(stream, n, (const T*)r, (const T*)zz, pp, S, ws.part0.p);
-        // one CG iteration; e3 (optional) = events before the SpMV, between
-        // SpMV and update, after the update
-        auto iteration = [&](cudaEvent_t* e3, bool capture) {
-            if (e3) rec(e3[0], capture);
-            // p_k alternates between pp (even k) and v (odd k)
-            kr_cg_spmv(stream, A, nz, (const T*)zz, pp, v, q, S, ws.part0.p);
-            if (e3) rec(e3[1], capture);
-            if (pt == XCAL_PRECOND_JACOBI) {
-                kr_cg_update(stream, n, x, (const T*)pp, (const T*)v, r, (const T*)q, zz, P, 1, S, ws.part0.p);
-            } else {
-                kr_cg_update(stream, n, x, (const T*)pp, (const T*)v, r, (const T*)q, zz, P, 0, S, ws.part0.p);
-                if (pt == XCAL_PRECOND_DILU) dilu_ldiv(E, nz, P, (const T*)r, zz, (const KScalars*)S);
-                kr_cg_rz(stream, n, (const T*)r, (const T*)zz, S, ws.part0.p);
+    krylov_start(E, SS, nz, P, c, r0, V, S);
+    const int CHUNK = cg ? 32 : 8;
+    const int nev = cg ? 3 : 6;  // events per timed iteration
+    int chunk = cg ? 4 : 1;
+    long launched = 0;
+    for (;;) {
+        if ((launched += chunk) > (long)hS->itmax + 2 * CHUNK + 32)
+            fail(XCAL_ERR_TIMEOUT, cg ? "CG did not report completion within itmax iterations"
+                                      : "BiCGSTAB did not report completion within itmax iterations");
+        int it0 = hS->iter;
+        const bool graphed = chunk == CHUNK;
+        // (iteration index within the chunk, its events); graphed chunks time
+        // the iterations with c % 8 == 4
+        std::vector<std::pair<int, cudaEvent_t*>> samples;
+        if (graphed) {
+            if (profiling)
+                for (int c8 = 4; c8 < CHUNK; c8 += 8) samples.push_back({c8, &gev[gk][nev * (c8 / 8)]});
+            replay_chunk(chunk_graph[gk][profiling ? 1 : 0], [&] {
+                for (int ci = 0; ci < CHUNK; ++ci)
+                    krylov_step(E, SS, nz, P, c, V, S, profiling && ci % 8 == 4 ? &gev[gk][nev * (ci / 8)] : nullptr,
+                                true);
+            });
+        } else {
+            if (profiling) prof_reserve((nev * chunk + 1) / 2 + 1);
+            for (int ci = 0; ci < chunk; ++ci) {
+                krylov_step(E, SS, nz, P, c, V, S, profiling ? &pev[nev * ci] : nullptr, false);
+                if (profiling) samples.push_back({ci, &pev[nev * ci]});
             }
-            if (e3) rec(e3[2], capture);
-        };
-        const int CHUNK = 32;
-        int chunk = 4;
-        long launched = 0;
-        for (;;) {
-            if ((launched += chunk) > (long)hS->itmax + 64 + 32)
-                fail(XCAL_ERR_TIMEOUT, "CG did not report completion within itmax iterations");
-            int it0 = hS->iter;
-            const bool graphed = chunk == CHUNK;
-            // (iteration index within the chunk, its three events)
-            std::vector<std::pair<int, cudaEvent_t*>> samples;
-            if (graphed) {
-                if (profiling)
-                    for (int c8 = 4; c8 < CHUNK; c8 += 8) samples.push_back({c8, &gev[gk][3 * (c8 / 8)]});
-                replay_chunk(chunk_graph[gk][profiling ? 1 : 0], [&] {
-                    for (int ci = 0; ci < CHUNK; ++ci)
-                        iteration(profiling && ci % 8 == 4 ? &gev[gk][3 * (ci / 8)] : nullptr, true);
-                });
-            } else {
-                if (profiling) prof_reserve(3 * chunk / 2 + 1);
-                for (int ci = 0; ci < chunk; ++ci) {
-                    iteration(profiling ? &pev[3 * ci] : nullptr, false);
-                    if (profiling) samples.push_back({ci, &pev[3 * ci]});
-                }
-            }
-            XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
-            sync();
+        }
+        XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
+        sync();
+        const int done_it = hS->iter - it0;
+        if (cg) {
             // launches that did work: one per completed iteration, plus a
             // final SpMV that detected zero curvature
-            const int done_it = hS->iter - it0;
             const int real = done_it + (hS->status == KS_ZERO_CURV ? 1 : 0);
             if (profiling) prof_n[4] += real;
             for (auto& sm : samples) {
@@ -916,57 +976,9 @@ void Case::krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz,
                     prof_n[3] += 1;
                 }
             }
-            if (hS->done) break;
-            if (chunk < CHUNK) chunk *= 2;
-        }
-    } else {
-        apply_M(E, pt, nz, P, r0, r, (const KScalars*)nullptr);
-        kr_bicg_start(stream, n, c, (const T*)r, pp, S, ws.part0.p, ws.part1.p);
-        // one BiCGSTAB iteration; e (optional) = events around both SpMVs and
-        // both preconditioner applications
-        auto iteration = [&](cudaEvent_t* e, bool capture) {
-            if (e) rec(e[0], capture);
-            kr_spmv(stream, A, nz, (const T*)pp, q, (const KScalars*)S);
-            if (e) rec(e[1], capture);
-            apply_M(E, pt, nz, P, (const T*)q, v, (const KScalars*)S);
-            if (e) rec(e[2], capture);
-            kr_bicg_alpha(stream, n, c, (const T*)v, S, ws.part0.p);
-            kr_bicg_s(stream, n, (const T*)r, (const T*)v, (const T*)pp, s, x, (const KScalars*)S);
-            if (e) rec(e[3], capture);
-            kr_spmv(stream, A, nz, (const T*)s, q, (const KScalars*)S);
-            if (e) rec(e[4], capture);
-            apply_M(E, pt, nz, P, (const T*)q, t, (const KScalars*)S);
-            if (e) rec(e[5], capture);
-            kr_bicg_omega(stream, n, (const T*)t, (const T*)s, S, ws.part0.p, ws.part1.p);
-            kr_bicg_xr(stream, n, x, (const T*)s, (const T*)t, r, c, S, ws.part0.p, ws.part1.p);
-            kr_bicg_p(stream, n, (const T*)r, (const T*)v, pp, (const KScalars*)S);
-        };
-        const int CHUNK = 8;
-        int chunk = 1;
-        long launched = 0;
-        for (;;) {
-            if ((launched += chunk) > (long)hS->itmax + 16 + 8)
-                fail(XCAL_ERR_TIMEOUT, "BiCGSTAB did not report completion within itmax iterations");
-            int it0 = hS->iter;
-            const bool graphed = chunk == CHUNK;
-            std::vector<std::pair<int, cudaEvent_t*>> samples;
-            if (graphed) {
-                if (profiling) samples.push_back({4, &gev[gk][0]});
-                replay_chunk(chunk_graph[gk][profiling ? 1 : 0], [&] {
-                    for (int ci = 0; ci < CHUNK; ++ci) iteration(profiling && ci == 4 ? &gev[gk][0] : nullptr, true);
-                });
-            } else {
-                if (profiling) prof_reserve(3 * chunk);
-                for (int ci = 0; ci < chunk; ++ci) {
-                    iteration(profiling ? &pev[6 * ci] : nullptr, false);
-                    if (profiling) samples.push_back({ci, &pev[6 * ci]});
-                }
-            }
-            XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
-            sync();
-            const int real = hS->iter - it0;
+        } else {
             for (auto& sm : samples) {
-                if (sm.first >= real) continue;
+                if (sm.first >= done_it) continue;
                 cudaEvent_t* e = sm.second;
                 float t0 = 0, t1 = 0, t2 = 0, t3 = 0;
                 XCAL_CUDA(cudaEventElapsedTime(&t0, e[0], e[1]));
@@ -980,14 +992,129 @@ void Case::krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz,
                     prof_n[2] += 2;
                 }
             }
-            if (hS->done) break;
-            if (chunk < CHUNK) chunk *= 2;
         }
+        if (hS->done) break;
+        if (chunk < CHUNK) chunk *= 2;
     }
+}
+
+// ---------------------------------------------------------------------------
+// graph mode
+// ---------------------------------------------------------------------------
+// Add a conditional WHILE node at the current point of the capture running on
+// `stream`; body(h) launches the loop body (captured into the node's body
+// graph on a side stream) and must end with a kernel that sets h.
+template <class F>
+void Case::capture_while(F&& body) {
+    if (side_depth >= 2) fail(XCAL_ERR_INVALID, "graph mode: WHILE loops nest at most two deep");
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    XCAL_CUDA(cudaStreamGetCaptureInfo(stream, &st, nullptr, &g, &deps, &nd));
+    if (st != cudaStreamCaptureStatusActive) fail(XCAL_ERR_CUDA, "graph mode: no active capture");
+    cudaGraphConditionalHandle h;
+    XCAL_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    // enter the loop with the condition set explicitly (also when the
+    // enclosing body runs again)
+    kr_set_cond(stream, h, 1u);
+    XCAL_CUDA(cudaStreamGetCaptureInfo(stream, &st, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams prm = {};
+    prm.type = cudaGraphNodeTypeConditional;
+    prm.conditional.handle = h;
+    prm.conditional.type = cudaGraphCondTypeWhile;
+    prm.conditional.size = 1;
+    cudaGraphNode_t node;
+    XCAL_CUDA(cudaGraphAddNode(&node, g, deps, nd, &prm));
+    cudaGraph_t bodyg = prm.conditional.phGraph_out[0];
+    if (!side[side_depth]) XCAL_CUDA(cudaStreamCreateWithFlags(&side[side_depth], cudaStreamNonBlocking));
+    cudaStream_t outer = stream;
+    stream = side[side_depth++];
+    const long long kb = t_launch_count;
+    XCAL_CUDA(cudaStreamBeginCaptureToGraph(stream, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+        body(h);
+    } catch (...) {
+        cudaGraph_t tmp;
+        cudaStreamEndCapture(stream, &tmp);
+        stream = outer;
+        --side_depth;
+        throw;
+    }
+    cudaGraph_t tmp;
+    XCAL_CUDA(cudaStreamEndCapture(stream, &tmp));
+    stream = outer;
+    --side_depth;
+    last_body_kernels = t_launch_count - kb;
+    if (side_depth == 0) body_kernels_captured += last_body_kernels;
+    XCAL_CUDA(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+}
+
+// solve_system! captured: per-solve setup, the Krylov loop as a WHILE node
+// (bodies of 8 iterations, at most itmax/8 + 2 bodies), the FP64 residual
+// into gres and (iterations, status) into giters.  Mixed precision nests the
+// inner loop in a WHILE node over defect-correction steps.
+void Case::solve_captured(int eqn, int comp) {
+    const bool isU = eqn == XCAL_EQN_U;
+    Equation& E = isU ? U : P;
+    const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
+    double* field = isU ? Uc[comp].p : p.p;
+    const double* b = isU ? U.b[comp].p : P.b[0].p;
+    KScalars* S = ws.S.p + (isU ? 0 : 1);
+    const int n = E.n;
+    const int slot = isU ? comp : 3;
+    CSRView A = E.view();
+    const int itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
+    const int BODY = 8;
+    const int cap = itmax / BODY + 2;
+    const bool mixed = cfg.precision == XCAL_PREC_MIXED;
+    const double inner_rtol = cfg.inner_rtol > 0 ? cfg.inner_rtol : 1e-3;
+    kr_ks_init(stream, S, SS.atol, SS.rtol, itmax, mixed ? 1 : 0, inner_rtol);
+    if (!mixed) {
+        KrylovVecs<double> V{ws.x.p, ws.r.p, ws.z.p, ws.p.p, ws.q.p, ws.v.p, ws.s.p, ws.t.p};
+        const double* r0 = SS.solver == XCAL_SOLVER_CG ? V.r : V.q;
+        kr_init_resid(stream, A, E.nz.p, b, field, ws.dx.p, V.x, SS.solver == XCAL_SOLVER_CG ? V.r : V.q);
+        krylov_start<double>(E, SS, E.nz.p, E.P.p, b, r0, V, S);
+        capture_while([&](cudaGraphConditionalHandle h) {
+            const long long k0 = t_launch_count;
+            for (int i = 0; i < BODY; ++i) krylov_step<double>(E, SS, E.nz.p, E.P.p, b, V, S, nullptr, true);
+            kr_loop_cond(stream, h, S, cap, (int)(t_launch_count - k0) + 1, dlaunch.p);
+        });
+        kr_finish(stream, n, V.x, ws.dx.p, field);
+    } else {
+        kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
+        if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, n, E.P.p, E.P32.p);
+        KrylovVecs<float> V{ws.fx.p, ws.fr.p, ws.fz.p, ws.fp.p, ws.fq.p, ws.fv.p, ws.fs.p, ws.ft.p};
+        const bool cg = SS.solver == XCAL_SOLVER_CG;
+        float* rhs = cg ? V.r : ws.fd.p;
+        capture_while([&](cudaGraphConditionalHandle ho) {
+            const long long k0 = t_launch_count;
+            kr_outer_prep(stream, S);
+            kr_defect(stream, A, E.nz.p, b, field, rhs, V.x);
+            krylov_start<float>(E, SS, E.nz32.p, E.P32.p, (const float*)rhs, (const float*)rhs, V, S);
+            capture_while([&](cudaGraphConditionalHandle hi) {
+                const long long k1 = t_launch_count;
+                for (int i = 0; i < BODY; ++i)
+                    krylov_step<float>(E, SS, E.nz32.p, E.P32.p, (const float*)rhs, V, S, nullptr, true);
+                kr_loop_cond(stream, hi, S, cap, (int)(t_launch_count - k1) + 1, dlaunch.p);
+            });
+            const long long inner_body = last_body_kernels;
+            kr_correct_masked(stream, n, field, V.x, S);
+            // this body's own kernels (the inner loop's bodies count themselves)
+            const long long outer_kernels = t_launch_count - k0 - inner_body + 1;
+            kr_outer_cond(stream, ho, S, 64, (int)outer_kernels, dlaunch.p);
+        });
+    }
+    kr_residual(stream, A, E.nz.p, field, b, S, ws.part0.p, ws.part1.p, gres.p + slot);
+    kr_record(stream, S, giters.p + 2 * slot);
 }
 
 // solve_system! (Solve_1_api.jl:268-307)
 double Case::solve_system(int eqn, int comp, int* iters) {
+    if (capturing) {  // graph mode: residual goes to gres
+        solve_captured(eqn, comp);
+        return 0.0;
+    }
     bool isU = eqn == XCAL_EQN_U;
     Equation& E = isU ? U : P;
     const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
@@ -1139,49 +1266,144 @@ void Case::turbulence() {
         launch_fill(stream, nueff.p, cfg.nu, mesh->nF);
 }
 
-double Case::max_courant() {
+// max Courant number into gres[GRES_CO] (device); the stream-mode caller reads it
+void Case::courant_to_slot() {
     const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
-    launch_courant(stream, mesh->nC, Ucp, dx13.p, cfg.dt, courant.p);
-    std::vector<double> h(mesh->nC);
-    XCAL_CUDA(cudaMemcpyAsync(h.data(), courant.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    launch_courant_max(stream, mesh->nC, Ucp, dx13.p, cfg.dt, cmax.p, cmax_ctr.p, gres.p + GRES_CO);
+}
+
+double Case::max_courant() {
+    courant_to_slot();
+    XCAL_CUDA(cudaMemcpyAsync(h_res, gres.p + GRES_CO, sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();
-    double mx = h[0];
-    for (int i = 1; i < mesh->nC; ++i) {
-        double y = h[i];
-        bool take_y = (y > mx) || (std::signbit(y) < std::signbit(mx));
-        mx = take_y ? (std::isnan(mx) ? mx : y) : (std::isnan(y) ? y : mx);
+    return h_res[0];
+}
+
+// One SIMPLE iteration's launches (Solvers_1_SIMPLE.jl:164-240).  Eager:
+// residuals returned, phases timed with events.  Under capture: residuals
+// land in gres, no events.
+void Case::simple_body(double r3[3], double& rp, bool timed) {
+    if (timed) XCAL_CUDA(cudaEventRecord(ev[0], stream));
+    solve_equation_U(r3);
+    if (timed) XCAL_CUDA(cudaEventRecord(ev[1], stream));
+    pressure_predictor(true);
+    flux_divergence();
+    XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    if (timed) XCAL_CUDA(cudaEventRecord(ev[2], stream));
+    rp = solve_equation_p();
+    if (timed) XCAL_CUDA(cudaEventRecord(ev[3], stream));
+    explicit_relaxation_p(cfg.p_solver.relax);
+    grad_p();
+    correct();
+    turbulence();
+    if (timed) XCAL_CUDA(cudaEventRecord(ev[4], stream));
+}
+
+// One PISO time step's launches (Solvers_2_PISO.jl:108-187); the Courant
+// number is left in gres[GRES_CO].
+void Case::piso_body(double r3[3], double& rp) {
+    solve_equation_U(r3);
+    pressure_predictor(false);
+    rp = 0.0;
+    for (int it = 1; it <= cfg.inner_loops; ++it) {
+        H();
+        flux_divergence();
+        XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        rp = solve_equation_p();
+        explicit_relaxation_p(it == cfg.inner_loops ? 1.0 : cfg.p_solver.relax);
+        grad_p();
+        correct();
     }
-    return mx;
+    turbulence();
+    courant_to_slot();
+}
+
+// Capture one step (SIMPLE iteration or PISO step, by the configured
+// algorithm) into step_graph.  Everything a step reads is either device state
+// or fixed for the case (coefficients, relaxation, dt), so the graph is
+// captured once and replayed for every later step.
+void Case::capture_step() {
+    if (step_graph) return;
+    sync();
+    const long long t0 = t_launch_count;
+    body_kernels_captured = 0;
+    capturing = true;
+    cudaGraph_t g = nullptr;
+    XCAL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        double r3[3], rp;
+        if (cfg.algorithm == XCAL_ALGO_PISO)
+            piso_body(r3, rp);
+        else
+            simple_body(r3, rp, false);
+    } catch (...) {
+        capturing = false;
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    capturing = false;
+    XCAL_CUDA(cudaStreamEndCapture(stream, &g));
+    const long long captured = t_launch_count - t0;
+    g_launch_count.fetch_sub(captured, std::memory_order_relaxed);
+    t_launch_count = t0;
+    step_top_kernels = captured - body_kernels_captured;
+    cudaError_t e = cudaGraphInstantiate(&step_graph, g, 0);
+    cudaGraphDestroy(g);
+    XCAL_CUDA(e);
+}
+
+// Replay the step graph; one host synchronisation reads the residuals, the
+// Courant number, the solves' iteration counts and the body-kernel count.
+void Case::run_step_graph(double res[4], double* courant) {
+    capture_step();
+    XCAL_CUDA(cudaEventRecord(ev[0], stream));
+    XCAL_CUDA(cudaGraphLaunch(step_graph, stream));
+    XCAL_CUDA(cudaEventRecord(ev[1], stream));
+    XCAL_CUDA(cudaMemcpyAsync(h_res, gres.p, GRES_N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    XCAL_CUDA(cudaMemcpyAsync(h_iters, giters.p, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    XCAL_CUDA(cudaMemcpyAsync(h_launch, dlaunch.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+    XCAL_CUDA(cudaMemsetAsync(dlaunch.p, 0, sizeof(unsigned long long), stream));
+    sync();
+    long long nk = step_top_kernels + (long long)h_launch[0];
+    g_launch_count.fetch_add(nk, std::memory_order_relaxed);
+    t_launch_count += nk;
+    float t = 0;
+    cudaEventElapsedTime(&t, ev[0], ev[1]);
+    ms[5] += t;
+    for (int k = 0; k < 4; ++k) {
+        res[k] = h_res[k];
+        last_iters[k] = h_iters[2 * k];
+        if (h_iters[2 * k + 1] == KS_LOOP_CAP)
+            fail(XCAL_ERR_TIMEOUT, "a Krylov solve did not finish within its loop-body cap");
+    }
+    if (courant) *courant = h_res[GRES_CO];
 }
 
 bool Case::simple_iteration(double res[4]) {  // Solvers_1_SIMPLE.jl:164-240
     if (!initialised) initial_calculations();
     iteration += 1;
-    XCAL_CUDA(cudaEventRecord(ev[0], stream));
-    double r3[3];
-    solve_equation_U(r3);
-    XCAL_CUDA(cudaEventRecord(ev[1], stream));
-    pressure_predictor(true);
-    flux_divergence();
-    XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    XCAL_CUDA(cudaEventRecord(ev[2], stream));
-    double rp = solve_equation_p();
-    XCAL_CUDA(cudaEventRecord(ev[3], stream));
-    explicit_relaxation_p(cfg.p_solver.relax);
-    grad_p();
-    correct();
-    turbulence();
-    XCAL_CUDA(cudaEventRecord(ev[4], stream));
-    sync();
-    float a = 0, b = 0, c = 0, d = 0;
-    cudaEventElapsedTime(&a, ev[0], ev[1]);
-    cudaEventElapsedTime(&b, ev[1], ev[2]);
-    cudaEventElapsedTime(&c, ev[2], ev[3]);
-    cudaEventElapsedTime(&d, ev[3], ev[4]);
-    ms[1] += a;
-    ms[3] += b + d;
-    ms[2] += c;
-    ms[5] += a + b + c + d;
+    double r3[3], rp;
+    if (graph_mode) {
+        double r[4];
+        run_step_graph(r, nullptr);
+        r3[0] = r[0];
+        r3[1] = r[1];
+        r3[2] = r[2];
+        rp = r[3];
+    } else {
+        simple_body(r3, rp, true);
+        sync();
+        float a = 0, b = 0, c = 0, d = 0;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        cudaEventElapsedTime(&c, ev[2], ev[3]);
+        cudaEventElapsedTime(&d, ev[3], ev[4]);
+        ms[1] += a;
+        ms[3] += b + d;
+        ms[2] += c;
+        ms[5] += a + b + c + d;
+    }
     res[0] = r3[0];
     res[1] = r3[1];
     res[2] = r3[2];
@@ -1197,26 +1419,40 @@ double Case::piso_step(double res[4]) {  // Solvers_2_PISO.jl:108-187
     if (!initialised) initial_calculations();
     iteration += 1;
     time = time + cfg.dt;
-    double r3[3];
-    solve_equation_U(r3);
-    pressure_predictor(false);
-    double rp = 0.0;
-    for (int it = 1; it <= cfg.inner_loops; ++it) {
-        H();
-        flux_divergence();
-        XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-        rp = solve_equation_p();
-        explicit_relaxation_p(it == cfg.inner_loops ? 1.0 : cfg.p_solver.relax);
-        grad_p();
-        correct();
+    double r3[3], rp, co;
+    if (graph_mode) {
+        double r[4];
+        run_step_graph(r, &co);
+        r3[0] = r[0];
+        r3[1] = r[1];
+        r3[2] = r[2];
+        rp = r[3];
+    } else {
+        XCAL_CUDA(cudaEventRecord(ev[0], stream));
+        piso_body(r3, rp);
+        XCAL_CUDA(cudaEventRecord(ev[1], stream));
+        XCAL_CUDA(cudaMemcpyAsync(h_res + GRES_CO, gres.p + GRES_CO, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        sync();
+        co = h_res[GRES_CO];
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[0], ev[1]);
+        ms[5] += t;
     }
-    turbulence();
-    double co = max_courant();
     res[0] = r3[0];
     res[1] = r3[1];
     res[2] = r3[2];
     res[3] = rp;
     return co;
+}
+
+void Case::set_graph_mode(bool on) {
+    if (on == graph_mode) return;
+    sync();
+    if (step_graph) {
+        cudaGraphExecDestroy(step_graph);
+        step_graph = nullptr;
+    }
+    graph_mode = on;
 }
 
 }  // namespace xcal

@@ -154,6 +154,42 @@ struct Case {
     void solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, const double* b, KScalars* S,
                      KScalars* hS, int gk, int* iters);
     int last_outer[4] = {0, 0, 0, 0};  // mixed: defect-correction steps of the last solve per system
+
+    // ---- graph mode: one SIMPLE iteration / PISO step captured as a CUDA
+    // graph; the Krylov (and defect-correction) loops are conditional WHILE
+    // nodes driven by device-side stopping tests, so a step needs no host
+    // round trip until its residuals are read.
+    enum { GRES_U = 0, GRES_P = 3, GRES_CO = 4, GRES_N = 8 };
+    DBuf<double> gres;          // per-step results: U x,y,z and p residuals, max Courant
+    DBuf<int> giters;           // (iterations, status) of the step's 4 solves
+    DBuf<unsigned int> cmax_ctr;
+    DBuf<unsigned long long> dlaunch;  // kernels run inside WHILE bodies (graph mode)
+    long long step_top_kernels = 0;    // kernels of a step graph outside WHILE bodies
+    bool graph_mode = false;    // xcal_case_set_graph_mode
+    bool capturing = false;     // the step functions are being captured
+    cudaStream_t side[2] = {nullptr, nullptr};  // capture streams of WHILE bodies
+    int side_depth = 0;
+    cudaGraphExec_t step_graph = nullptr;
+    long long step_graph_launches = 0;
+    int* h_iters = nullptr;     // pinned mirror of giters
+    unsigned long long* h_launch = nullptr;
+    long long body_kernels_captured = 0;
+    long long last_body_kernels = 0;  // kernels captured into the last WHILE body
+    void simple_body(double r3[3], double& rp, bool timed);
+    void piso_body(double r3[3], double& rp);
+    void set_graph_mode(bool on);
+    void courant_to_slot();
+    template <class F>
+    void capture_while(F&& body);
+    void solve_captured(int eqn, int comp);
+    template <class T>
+    void krylov_start(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c, const T* r0,
+                      const KrylovVecs<T>& V, KScalars* S);
+    template <class T>
+    void krylov_step(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c,
+                     const KrylovVecs<T>& V, KScalars* S, cudaEvent_t* ev6, bool in_capture);
+    void capture_step();
+    void run_step_graph(double res[4], double* courant);
 };
 
 }  // namespace xcal

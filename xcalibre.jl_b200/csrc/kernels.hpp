@@ -40,7 +40,8 @@ void launch_correct_mdot(cudaStream_t s, const MeshView& m, const CSRView& A, co
 void launch_correct_U(cudaStream_t s, int n, double* const H[3], const double* const g[3], const double* rD,
                       double* const U[3]);
 void launch_relax_explicit(cudaStream_t s, int n, double* phi, const double* phi0, double alpha);
-void launch_courant(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* co);
+void launch_courant_max(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* part,
+                        unsigned int* counter, double* out);
 
 // Krylov kernels (kernels_krylov.cu).  Templates are instantiated for
 // T = double (plain FP64 path) and T = float (mixed-precision inner solves).
@@ -92,5 +93,17 @@ void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, c
                  const KScalars* S);
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
                  double* part0, double* part1, double* out);
+// device-driven solve control of graph mode (conditional WHILE nodes)
+void kr_ks_init(cudaStream_t s, KScalars* S, double atol, double rtol, int itmax, int mixed, double inner_rtol);
+// body_kernels: kernels of one loop body (excluding WHILE bodies nested in
+// it), added to *launches each time the body runs
+void kr_loop_cond(cudaStream_t s, cudaGraphConditionalHandle h, KScalars* S, int cap, int body_kernels,
+                  unsigned long long* launches);
+void kr_set_cond(cudaStream_t s, cudaGraphConditionalHandle h, unsigned int v);
+void kr_outer_prep(cudaStream_t s, KScalars* S);
+void kr_correct_masked(cudaStream_t s, int n, double* field, const float* x, const KScalars* S);
+void kr_outer_cond(cudaStream_t s, cudaGraphConditionalHandle h, KScalars* S, int max_outer, int body_kernels,
+                   unsigned long long* launches);
+void kr_record(cudaStream_t s, const KScalars* S, int* out);
 
 }  // namespace xcal

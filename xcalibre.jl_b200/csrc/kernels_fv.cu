@@ -765,13 +765,38 @@ __global__ void k_relax_explicit(int n, double* phi, const double* __restrict__ 
     phi[i] = phi0[i] + alpha * (phi[i] - phi0[i]);
 }
 
-// _max_courant_number! (Solvers_0_functions.jl:267-276) + block max
-__global__ void k_courant(int n, const double* __restrict__ Ux, const double* __restrict__ Uy,
-                          const double* __restrict__ Uz, const double* __restrict__ dx, double dt, double* co) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double umag = sqrt(Ux[i] * Ux[i] + Uy[i] * Uy[i] + Uz[i] * Uz[i]);
-    co[i] = (umag * dt) / dx[i];
+// _max_courant_number! (Solvers_0_functions.jl:267-276): per-cell Courant
+// number and its maximum (Julia max; exact, so the tree order is free), the
+// last block writing the result
+__global__ void k_courant_max(int n, const double* __restrict__ Ux, const double* __restrict__ Uy,
+                              const double* __restrict__ Uz, const double* __restrict__ dx, double dt, double* part,
+                              unsigned int* counter, double* out) {
+    __shared__ double sm[8];
+    double mx = -INFINITY;
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(k);
+        if (i < n) {
+            double umag = sqrt(Ux[i] * Ux[i] + Uy[i] * Uy[i] + Uz[i] * Uz[i]);
+            mx = jl_max(mx, (umag * dt) / dx[i]);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) mx = jl_max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sm[warp] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = sm[0];
+        for (int w = 1; w < RED_THREADS / 32; ++w) b = jl_max(b, sm[w]);
+        part[blockIdx.x] = b;
+    }
+    if (!last_block(counter)) return;
+    if (threadIdx.x == 0) {
+        int T = gridDim.x;
+        double r = __ldcg(part);
+        for (int t = 1; t < T; ++t) r = jl_max(r, __ldcg(part + t));
+        *out = r;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -866,8 +891,10 @@ void launch_relax_explicit(cudaStream_t s, int n, double* phi, const double* phi
     k_relax_explicit<<<nblk(n), TPB, 0, s>>>(n, phi, phi0, alpha);
     XCAL_CHECK_LAUNCH();
 }
-void launch_courant(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* co) {
-    k_courant<<<nblk(n), TPB, 0, s>>>(n, U[0], U[1], U[2], dx, dt, co);
+void launch_courant_max(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* part,
+                        unsigned int* counter, double* out) {
+    k_courant_max<<<(n + RED_TILE - 1) / RED_TILE, RED_THREADS, 0, s>>>(n, U[0], U[1], U[2], dx, dt, part, counter,
+                                                                        out);
     XCAL_CHECK_LAUNCH();
 }
 

@@ -176,6 +176,7 @@ __global__ void k_cg_start(int n, const T* __restrict__ r, const T* __restrict__
         S->done = 0;
         S->status = KS_RUNNING;
         S->outer_conv = 0;
+        S->loops = 0;
         if (gamma == 0.0) {
             S->done = 1;
             S->status = KS_ZERO_RHS;
@@ -341,6 +342,7 @@ __global__ void k_bicg_start(int n, const T* __restrict__ c, const T* __restrict
         S->done = 0;
         S->status = KS_RUNNING;
         S->outer_conv = 0;
+        S->loops = 0;
         if (rNorm == 0.0) {
             S->done = 1;
             S->status = KS_ZERO_RHS;
@@ -586,6 +588,85 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_residual(CSRView A, const do
 }
 
 // ---------------------------------------------------------------------------
+// device-driven solve control (graph mode: the loops are conditional WHILE
+// nodes whose condition these single-thread kernels set)
+// ---------------------------------------------------------------------------
+// the host's per-solve setup of the scalar block, as a kernel
+__global__ void k_ks_init(KScalars* S, double atol, double rtol, int itmax, int mixed, double inner_rtol) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    KScalars z = {};
+    z.atol = atol;
+    z.rtol = rtol;
+    z.itmax = itmax;
+    z.mixed = mixed;
+    z.inner_rtol = inner_rtol;
+    *S = z;
+}
+
+// end of a Krylov loop body: continue while the solve runs, at most `cap`
+// bodies (a solve that has not finished by then is stopped as KS_LOOP_CAP);
+// adds the body's kernel count to the launch counter
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, KScalars* S, int cap, int body_kernels,
+                            unsigned long long* launches) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    atomicAdd(launches, (unsigned long long)body_kernels);
+    S->loops = S->loops + 1;
+    bool go = !S->done && S->loops < cap;
+    if (!go && !S->done) {
+        S->done = 1;
+        S->status = KS_LOOP_CAP;
+    }
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// a WHILE loop is entered with its condition set to 1 by this kernel, placed
+// right before the node (every execution of the enclosing graph or body)
+__global__ void k_set_cond(cudaGraphConditionalHandle h, unsigned int v) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, v);
+}
+
+// start of a defect-correction step: the inner solve state is reset
+__global__ void k_outer_prep(KScalars* S) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    S->iter = 0;
+    S->done = 0;
+    S->status = KS_RUNNING;
+}
+
+// field += inner solution unless the defect already met the target
+__global__ void k_correct_masked(int n, double* field, const float* __restrict__ x, const KScalars* S) {
+    if (S->outer_conv) return;
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(k);
+        if (i < n) field[i] = field[i] + (double)x[i];
+    }
+}
+
+// end of a defect-correction step (the host loop's exit tests, on the device)
+__global__ void k_outer_cond(cudaGraphConditionalHandle h, KScalars* S, int max_outer, int body_kernels,
+                             unsigned long long* launches) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    atomicAdd(launches, (unsigned long long)body_kernels);
+    bool stop = S->outer_conv != 0;
+    if (!stop) {
+        S->total = S->total + S->iter;
+        int st = S->status;
+        stop = st == KS_ZERO_CURV || st == KS_BREAKDOWN || st == KS_TIRED || st == KS_LOOP_CAP ||
+               (st == KS_SOLVED && S->eps <= S->eps_outer);
+    }
+    S->outer = S->outer + 1;
+    if (!stop && S->outer >= max_outer) stop = true;
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
+// iterations and status of the finished solve into out[0..1]
+__global__ void k_record(const KScalars* S, int* out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    out[0] = S->mixed ? S->total : S->iter;
+    out[1] = S->status;
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 static inline int tiles(int n) { return n <= 0 ? 1 : (n + RED_TILE - 1) / RED_TILE; }
@@ -710,6 +791,37 @@ void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, c
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
                  double* part0, double* part1, double* out) {
     k_residual<<<TILE_LAUNCH(A.n), s>>>(A, nz, x, b, S, part0, part1, out);
+    XCAL_CHECK_LAUNCH();
+}
+
+void kr_ks_init(cudaStream_t s, KScalars* S, double atol, double rtol, int itmax, int mixed, double inner_rtol) {
+    k_ks_init<<<1, 32, 0, s>>>(S, atol, rtol, itmax, mixed, inner_rtol);
+    XCAL_CHECK_LAUNCH();
+}
+void kr_loop_cond(cudaStream_t s, cudaGraphConditionalHandle h, KScalars* S, int cap, int body_kernels,
+                  unsigned long long* launches) {
+    k_loop_cond<<<1, 32, 0, s>>>(h, S, cap, body_kernels, launches);
+    XCAL_CHECK_LAUNCH();
+}
+void kr_set_cond(cudaStream_t s, cudaGraphConditionalHandle h, unsigned int v) {
+    k_set_cond<<<1, 32, 0, s>>>(h, v);
+    XCAL_CHECK_LAUNCH();
+}
+void kr_outer_prep(cudaStream_t s, KScalars* S) {
+    k_outer_prep<<<1, 32, 0, s>>>(S);
+    XCAL_CHECK_LAUNCH();
+}
+void kr_correct_masked(cudaStream_t s, int n, double* field, const float* x, const KScalars* S) {
+    k_correct_masked<<<TILE_LAUNCH(n), s>>>(n, field, x, S);
+    XCAL_CHECK_LAUNCH();
+}
+void kr_outer_cond(cudaStream_t s, cudaGraphConditionalHandle h, KScalars* S, int max_outer, int body_kernels,
+                   unsigned long long* launches) {
+    k_outer_cond<<<1, 32, 0, s>>>(h, S, max_outer, body_kernels, launches);
+    XCAL_CHECK_LAUNCH();
+}
+void kr_record(cudaStream_t s, const KScalars* S, int* out) {
+    k_record<<<1, 32, 0, s>>>(S, out);
     XCAL_CHECK_LAUNCH();
 }
 

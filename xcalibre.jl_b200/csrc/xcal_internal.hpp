@@ -164,10 +164,20 @@ struct alignas(128) KScalars {
     // tolerance, outer step index, "defect already below target"
     double eps_outer, inner_rtol;
     int mixed, outer, outer_conv;
+    int total;                                        // mixed: inner iterations over all outer steps
+    int loops;                                        // graph mode: bodies run by the current WHILE loop
     int iter, itmax, done, status;
     unsigned int counter;                             // last-block ticket
     unsigned int counter2;
 };
-enum { KS_RUNNING = 0, KS_SOLVED = 1, KS_TIRED = 2, KS_ZERO_CURV = 3, KS_BREAKDOWN = 4, KS_ZERO_RHS = 5 };
+enum {
+    KS_RUNNING = 0,
+    KS_SOLVED = 1,
+    KS_TIRED = 2,
+    KS_ZERO_CURV = 3,
+    KS_BREAKDOWN = 4,
+    KS_ZERO_RHS = 5,
+    KS_LOOP_CAP = 6  // graph mode: a device-driven loop hit its body-count cap
+};
 
 }  // namespace xcal
