@@ -28,7 +28,8 @@ enum {
     XCAL_ERR_NOT_CONVERGED = -4,  /* outer loop ended without convergence   */
     XCAL_ERR_DIVERGED = -5,       /* NaN/Inf seen in a residual             */
     XCAL_ERR_TIMEOUT = -6,        /* a bounded device wait gave up          */
-    XCAL_ERR_UNSUPPORTED = -7     /* option outside the implemented path    */
+    XCAL_ERR_UNSUPPORTED = -7,    /* option outside the implemented path    */
+    XCAL_ERR_BUSY = -8            /* batch full or device-memory budget hit */
 };
 
 /* ---- enumerations mirroring the reference's dispatch types ------------- */
@@ -218,6 +219,7 @@ typedef struct {
 typedef struct xcal_ctx xcal_ctx;
 typedef struct xcal_mesh xcal_mesh;
 typedef struct xcal_case xcal_case;
+typedef struct xcal_batch xcal_batch;
 
 /* ---- context ------------------------------------------------------------ */
 /* Hardware(backend=B200Backend()) (src/Simulate/Simulate_0_types.jl:70-74) */
@@ -371,6 +373,36 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable);
  * profiling does not apply inside the graph. */
 int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable);
 int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches);
+
+/* ---- batching / serving --------------------------------------------------
+ * A batch keeps many independent steady cases resident and advances them one
+ * SIMPLE iteration per call in lockstep.  Each Krylov solve (U x, y, z, then
+ * p) is one batched solve over all cases: a single launch per Krylov kernel
+ * covers every case's tiles (block-diagonal system, per-case offsets), with
+ * per-case Krylov scalars -- a case's results are the same alone, in any
+ * batch, and through xcal_simple_iterate.  Cases must share the precision
+ * mode, solvers and preconditioners.  Cases enter and leave between
+ * iterations; admission is bounded by max_cases and a device-memory budget.
+ * (The reference has no counterpart: it solves one case per process.) */
+/* device bytes a case will hold (mesh + fields + matrices + workspaces),
+ * from its sizes, before it is created; an upper bound */
+int32_t xcal_footprint_estimate(int64_t n_cells, int64_t n_faces, int64_t n_bfaces, int32_t precision,
+                                int32_t dilu_U, int32_t dilu_p, int64_t* bytes);
+/* device bytes held by a created case and by its mesh */
+int32_t xcal_case_footprint(const xcal_case* cs, int64_t* case_bytes, int64_t* mesh_bytes);
+int32_t xcal_batch_create(xcal_ctx* ctx, int32_t max_cases, int64_t budget_bytes, xcal_batch** out);
+int32_t xcal_batch_destroy(xcal_batch* b);
+/* admit a case (it then runs on the batch's stream); charge_bytes <= 0
+ * charges its measured footprint.  XCAL_ERR_BUSY when full or over budget. */
+int32_t xcal_batch_add(xcal_batch* b, xcal_case* cs, int64_t charge_bytes);
+int32_t xcal_batch_remove(xcal_batch* b, xcal_case* cs);
+int32_t xcal_batch_info(const xcal_batch* b, int32_t* n_cases, int64_t* used_bytes, int64_t* budget_bytes);
+/* position of a case in the batch's order (the row of its results) */
+int32_t xcal_batch_case_index(const xcal_batch* b, const xcal_case* cs, int32_t* index);
+/* one SIMPLE iteration of every admitted case; res [n_cases*4] receives the
+ * scaled residuals (Ux, Uy, Uz, p) and converged [n_cases] the per-case
+ * convergence test of Solvers_1_SIMPLE.jl:222-240 (either may be NULL) */
+int32_t xcal_batch_simple_iterate(xcal_batch* b, double* res, int32_t* converged);
 
 #ifdef __cplusplus
 }

@@ -10,7 +10,8 @@ from .api import (B200Backend, Bicgstab, Case, Cg, Configuration, Context, Devic
                   DirichletFunction, Empty, Energy, Euler, Extrapolated, Fluid, Gauss, Hardware, Incompressible,
                   Isothermal, Jacobi, LES, LUST, Laminar, Linear, Neumann, Physics, RANS, Runtime, Schemes,
                   Smagorinsky, SolverSetup, Steady, SteadyState, Symmetry, Transient, Upwind, Wall, Zerogradient,
-                  assign, build_config, construct_periodic, initialise_, launch_count, run_)
+                  assign, build_config, construct_periodic, initialise_, launch_count, run_, Batch,
+                  footprint_estimate)
 from .foam import Mesh3, build_mesh3
 from .meshgen import PolyMesh, box_polymesh, cavity_polymesh, channel_polymesh, periodic_box_polymesh
 

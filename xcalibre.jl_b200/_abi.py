@@ -14,6 +14,7 @@ XCAL_ERR_NOT_CONVERGED = -4
 XCAL_ERR_DIVERGED = -5
 XCAL_ERR_TIMEOUT = -6
 XCAL_ERR_UNSUPPORTED = -7
+XCAL_ERR_BUSY = -8
 
 # boundary conditions
 BC_DIRICHLET = 1

@@ -62,6 +62,15 @@ SIGNATURES = {
     "xcal_case_set_graph_mode": (_i32, [_vp, _i32]),
     "xcal_case_get_profile": (_i32, [_vp, _i32, _pd, _pi64]),
     "xcal_residual_noalloc": (_i32, [_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, _i32]),
+    "xcal_footprint_estimate": (_i32, [_i64, _i64, _i64, _i32, _i32, _i32, _pi64]),
+    "xcal_case_footprint": (_i32, [_vp, _pi64, _pi64]),
+    "xcal_batch_create": (_i32, [_vp, _i32, _i64, C.POINTER(_vp)]),
+    "xcal_batch_destroy": (_i32, [_vp]),
+    "xcal_batch_add": (_i32, [_vp, _vp, _i64]),
+    "xcal_batch_remove": (_i32, [_vp, _vp]),
+    "xcal_batch_info": (_i32, [_vp, _pi, _pi64, _pi64]),
+    "xcal_batch_case_index": (_i32, [_vp, _vp, _pi]),
+    "xcal_batch_simple_iterate": (_i32, [_vp, _pd, _pi]),
 }
 
 _LIB = None

@@ -618,6 +618,76 @@ class Case:
         return ms.value, n.value
 
 
+    def footprint(self) -> tuple[int, int]:
+        """(device bytes of the case, device bytes of its mesh)."""
+        cb, mb = C.c_int64(), C.c_int64()
+        self._chk(lib().xcal_case_footprint(self.h, C.byref(cb), C.byref(mb)))
+        return cb.value, mb.value
+
+
+def footprint_estimate(mesh: Mesh3, precision: str = "fp64", dilu_U: bool = True, dilu_p: bool = False) -> int:
+    """Device bytes a case on ``mesh`` will hold (mesh + case), before it is
+    created: the admission test of the serving loop."""
+    b = C.c_int64()
+    check(lib().xcal_footprint_estimate(mesh.n_cells, mesh.n_faces, mesh.n_bfaces,
+                                        _abi.PREC_MIXED if precision == "mixed" else _abi.PREC_FP64,
+                                        1 if dilu_U else 0, 1 if dilu_p else 0, C.byref(b)), None)
+    return b.value
+
+
+class Batch:
+    """Resident batch of steady cases advanced together (xcal_batch_*): each
+    Krylov solve is one batched launch sequence over all cases, with
+    per-case scalars, so results do not depend on the batch composition."""
+
+    def __init__(self, ctx: Context, max_cases: int, budget_bytes: int):
+        self.ctx = ctx
+        h = C.c_void_p()
+        check(lib().xcal_batch_create(ctx.h, int(max_cases), int(budget_bytes), C.byref(h)), ctx.h)
+        self.h = h
+        self.cases: list[Case] = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().xcal_batch_destroy(self.h)
+            self.h = None
+            self.cases = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, case: Case, charge_bytes: int = 0) -> bool:
+        """Admit a case; False when the batch is full or over its budget."""
+        code = lib().xcal_batch_add(self.h, case.h, int(charge_bytes))
+        if code == _abi.XCAL_ERR_BUSY:
+            return False
+        check(code, self.ctx.h)
+        self.cases.append(case)
+        return True
+
+    def remove(self, case: Case) -> None:
+        check(lib().xcal_batch_remove(self.h, case.h), self.ctx.h)
+        self.cases.remove(case)
+
+    def info(self) -> tuple[int, int, int]:
+        n, used, budget = C.c_int32(), C.c_int64(), C.c_int64()
+        check(lib().xcal_batch_info(self.h, C.byref(n), C.byref(used), C.byref(budget)), self.ctx.h)
+        return n.value, used.value, budget.value
+
+    def simple_iterate(self):
+        """One SIMPLE iteration of every case: (residuals [n, 4], converged [n])
+        in the order of ``self.cases``."""
+        n = len(self.cases)
+        res = np.zeros((max(n, 1), 4))
+        conv = np.zeros(max(n, 1), dtype=np.int32)
+        check(lib().xcal_batch_simple_iterate(self.h, _abi.ptr(res, C.c_double), _abi.ptr(conv, C.c_int32)),
+              self.ctx.h)
+        return res[:n], conv[:n].astype(bool)
+
+
 def launch_count() -> int:
     n = C.c_int64()
     lib().xcal_get_launch_count(None, C.byref(n))

@@ -26,8 +26,8 @@ def _solvers(U_pre=A.DILU, p_pre=A.Jacobi, relax_U=0.7, relax_p=0.3, conv=1e-7, 
     }
 
 
-def cavity_case(mesh: Mesh3, iterations: int = 1000, precision: str = "fp64", device: int = 0):
-    nu = 0.01  # Re = 100 on the unit square with lid speed 1
+def cavity_case(mesh: Mesh3, iterations: int = 1000, precision: str = "fp64", device: int = 0, nu: float = 0.01):
+    # nu = 0.01: Re = 100 on the unit square with lid speed 1
     model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=nu), turbulence=A.RANS(A.Laminar),
                       energy=A.Energy(A.Isothermal), domain=mesh)
     BCs = A.assign(
@@ -52,8 +52,8 @@ def parabolic_inlet(coords, time, index):
 
 
 def channel_case(mesh: Mesh3, iterations: int = 500, precision: str = "fp64", device: int = 0,
-                 convergence: float = 1e-6):
-    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=1e-3), turbulence=A.RANS(A.Laminar),
+                 convergence: float = 1e-6, nu: float = 1e-3):
+    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=nu), turbulence=A.RANS(A.Laminar),
                       energy=A.Energy(A.Isothermal), domain=mesh)
     BCs = A.assign(
         region=mesh,

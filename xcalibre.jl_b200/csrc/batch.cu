@@ -1,0 +1,531 @@
+// batch.cu -- continuous batching of independent steady cases (SIMPLE).
+//
+// The cases of a batch stay resident (fields, matrices, Krylov workspaces)
+// and advance one SIMPLE iteration per call in lockstep.  The face-loop and
+// correction kernels run per case on the batch stream; every Krylov solve
+// (three momentum components, then pressure) is one batched solve over all
+// cases: the same kernels' tile bodies driven through a per-system
+// descriptor table and tile map (block-diagonal system, per-case offsets),
+// with per-case Krylov scalars, so each case stops on its own test and its
+// result is the one it gets when solved alone.  Cases enter (xcal_batch_add)
+// and leave (xcal_batch_remove) between iterations; admission is bounded by a
+// device-memory budget.
+#include <algorithm>
+#include <cstring>
+
+#include "batch.hpp"
+#include "case.hpp"
+#include "dev_common.cuh"
+#include "kernels.hpp"
+
+namespace xcal {
+
+struct Batch {
+    xcal_ctx* ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    int cap = 0;
+    size_t budget = 0, used = 0;
+    std::vector<Case*> cases;
+    std::vector<size_t> footprint;   // bytes charged per case (case + mesh share)
+    std::vector<cudaStream_t> own;   // each case's own stream (restored on removal)
+    DBuf<KScalars> S;                // [cap] Krylov scalars, one block per case
+    KScalars* hS = nullptr;          // pinned
+    DBuf<double> res;                // [cap*4] scaled residuals of the iteration
+    double* hres = nullptr;          // pinned
+    // composition-dependent tables (rebuilt when cases enter or leave)
+    bool dirty = true;
+    int ntiles = 0;
+    DBuf<int2> tmap;                 // all cases
+    DBuf<int2> tmap_act;             // subset (mixed-precision outer steps)
+    DBuf<unsigned char> sys[2][4];   // [fp64, fp32][Ux, Uy, Uz, p] descriptor tables
+    DBuf<int2> dlo[2], dup[2];       // merged DILU levels per equation
+    std::vector<int> dlo_off[2], dup_off[2];
+    std::vector<int2> h_tmap;
+    long long iterations = 0;
+
+    Batch(xcal_ctx* c, int capacity, size_t bytes) : ctx(c), cap(capacity), budget(bytes) {
+        XCAL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        S.alloc(cap);
+        S.zero(stream);
+        res.alloc(4 * (size_t)cap);
+        res.zero(stream);
+        XCAL_CUDA(cudaMallocHost(&hS, cap * sizeof(KScalars)));
+        XCAL_CUDA(cudaMallocHost(&hres, 4 * cap * sizeof(double)));
+    }
+    ~Batch() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (size_t i = 0; i < cases.size(); ++i) cases[i]->stream = own[i];
+        if (hS) cudaFreeHost(hS);
+        if (hres) cudaFreeHost(hres);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void sync() { XCAL_CUDA(cudaStreamSynchronize(stream)); }
+
+    int index_of(const Case* c) const {
+        for (size_t i = 0; i < cases.size(); ++i)
+            if (cases[i] == c) return (int)i;
+        return -1;
+    }
+
+    void check_compatible(const Case* c) const {
+        if (c->cfg.algorithm != XCAL_ALGO_SIMPLE) fail(XCAL_ERR_UNSUPPORTED, "batch: steady SIMPLE cases only");
+        if (cases.empty()) return;
+        const xcal_config& a = cases[0]->cfg;
+        const xcal_config& b = c->cfg;
+        if (a.precision != b.precision || a.U_solver.solver != b.U_solver.solver ||
+            a.U_solver.precond != b.U_solver.precond || a.p_solver.solver != b.p_solver.solver ||
+            a.p_solver.precond != b.p_solver.precond)
+            fail(XCAL_ERR_UNSUPPORTED, "batch: cases must share precision, solvers and preconditioners");
+    }
+
+    void add(Case* c, size_t charge) {
+        if ((int)cases.size() >= cap) fail(XCAL_ERR_BUSY, "batch: no free slot");
+        if (used + charge > budget) fail(XCAL_ERR_BUSY, "batch: device-memory budget exceeded");
+        if (index_of(c) >= 0) fail(XCAL_ERR_INVALID, "batch: case already admitted");
+        check_compatible(c);
+        c->sync();
+        if (c->graph_mode) c->set_graph_mode(false);
+        own.push_back(c->stream);
+        c->stream = stream;
+        cases.push_back(c);
+        footprint.push_back(charge);
+        used += charge;
+        dirty = true;
+    }
+
+    void remove(Case* c) {
+        int i = index_of(c);
+        if (i < 0) fail(XCAL_ERR_INVALID, "batch: case not admitted");
+        sync();
+        c->stream = own[i];
+        used -= footprint[i];
+        cases.erase(cases.begin() + i);
+        own.erase(own.begin() + i);
+        footprint.erase(footprint.begin() + i);
+        dirty = true;
+    }
+
+    // ---- composition tables ----------------------------------------------
+    template <class T>
+    void fill_sys(int prec, int slot) {
+        const int nc = (int)cases.size();
+        std::vector<BSys<T>> h(std::max(nc, 1));
+        for (int i = 0; i < nc; ++i) {
+            Case* c = cases[i];
+            const bool isU = slot < 3;
+            Equation& E = isU ? c->U : c->P;
+            const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
+            BSys<T>& B = h[i];
+            std::memset(&B, 0, sizeof(B));
+            B.A = E.view();
+            B.n = E.n;
+            B.ntiles = (E.n + RED_TILE - 1) / RED_TILE;
+            B.S = S.p + i;
+            B.part0 = c->ws.part0.p;
+            B.part1 = c->ws.part1.p;
+            if constexpr (sizeof(T) == 8) {
+                B.nz = (const T*)E.nz.p;
+                B.P = (const T*)E.P.p;
+                T* v[KV_COUNT] = {(T*)c->ws.x.p, (T*)c->ws.r.p, (T*)c->ws.z.p, (T*)c->ws.p.p, (T*)c->ws.q.p,
+                                  (T*)c->ws.v.p, (T*)c->ws.s.p, (T*)c->ws.t.p, nullptr, (T*)c->ws.q.p};
+                for (int k = 0; k < KV_COUNT; ++k) B.vec[k] = v[k];
+                B.vec[KV_C] = (T*)(isU ? c->U.b[slot].p : c->P.b[0].p);
+            } else {
+                B.nz = (const T*)E.nz32.p;
+                B.P = (const T*)E.P32.p;
+                T* v[KV_COUNT] = {(T*)c->ws.fx.p, (T*)c->ws.fr.p, (T*)c->ws.fz.p, (T*)c->ws.fp.p, (T*)c->ws.fq.p,
+                                  (T*)c->ws.fv.p, (T*)c->ws.fs.p, (T*)c->ws.ft.p, (T*)c->ws.fd.p, (T*)c->ws.fd.p};
+                for (int k = 0; k < KV_COUNT; ++k) B.vec[k] = v[k];
+            }
+            if (SS.solver == XCAL_SOLVER_CG && SS.precond == XCAL_PRECOND_NONE) B.vec[KV_Z] = B.vec[KV_R];
+        }
+        sys[prec][slot].upload((const unsigned char*)h.data(), h.size() * sizeof(BSys<T>), stream);
+    }
+
+    void rebuild() {
+        if (!dirty) return;
+        const int nc = (int)cases.size();
+        h_tmap.clear();
+        for (int i = 0; i < nc; ++i) {
+            int nt = (cases[i]->U.n + RED_TILE - 1) / RED_TILE;
+            for (int t = 0; t < nt; ++t) h_tmap.push_back(make_int2(i, t));
+        }
+        ntiles = (int)h_tmap.size();
+        tmap.upload(h_tmap.empty() ? std::vector<int2>(1, make_int2(0, 0)) : h_tmap, stream);
+        tmap_act.alloc(std::max(ntiles, 1));
+        if (nc > 0) {
+            const bool fp32 = cases[0]->cfg.precision == XCAL_PREC_MIXED;
+            for (int slot = 0; slot < 4; ++slot) {
+                if (fp32)
+                    fill_sys<float>(1, slot);
+                else
+                    fill_sys<double>(0, slot);
+            }
+            // DILU levels merged across cases: level l holds every case's
+            // level-l rows
+            for (int e = 0; e < 2; ++e) {
+                for (int dir = 0; dir < 2; ++dir) {
+                    size_t L = 0;
+                    for (Case* c : cases) {
+                        Equation& E = e == 0 ? c->U : c->P;
+                        const std::vector<int>& off = dir == 0 ? E.lower_off : E.upper_off;
+                        if (off.size() > 1) L = std::max(L, off.size() - 1);
+                    }
+                    std::vector<int> moff(L + 1, 0);
+                    std::vector<int2> rows;
+                    for (size_t l = 0; l < L; ++l) {
+                        for (int i = 0; i < nc; ++i) {
+                            Equation& E = e == 0 ? cases[i]->U : cases[i]->P;
+                            const std::vector<int>& off = dir == 0 ? E.lower_off : E.upper_off;
+                            const std::vector<int>& hr = dir == 0 ? E.h_lower_rows : E.h_upper_rows;
+                            if (l + 1 >= off.size()) continue;
+                            for (int k = off[l]; k < off[l + 1]; ++k) rows.push_back(make_int2(i, hr[k]));
+                        }
+                        moff[l + 1] = (int)rows.size();
+                    }
+                    if (rows.empty()) rows.push_back(make_int2(0, 0));
+                    (dir == 0 ? dlo[e] : dup[e]).upload(rows, stream);
+                    (dir == 0 ? dlo_off[e] : dup_off[e]) = moff;
+                }
+            }
+        }
+        sync();
+        dirty = false;
+    }
+
+    // ---- batched Krylov solve --------------------------------------------
+    template <class T>
+    void apply_M(int prec, int slot, int e, int pt, const int2* tm, int nt, int in, int out, int use_S) {
+        const BSys<T>* sy = (const BSys<T>*)sys[prec][slot].p;
+        if (pt == XCAL_PRECOND_JACOBI)
+            kb_jacobi_apply<T>(stream, sy, tm, nt, in, out, use_S);
+        else if (pt == XCAL_PRECOND_DILU)
+            kb_dilu<T>(stream, sy, dlo[e].p, dlo_off[e], dup[e].p, dup_off[e], in, out, use_S);
+        else
+            kb_copy<T>(stream, sy, tm, nt, in, out, use_S);
+    }
+
+    // start + host-polled iterations over the systems of tile map tm (the
+    // single-case loop's chunking: 4 -> 32 CG, 1 -> 8 BiCGSTAB)
+    template <class T>
+    void krylov(int prec, int slot, const xcal_solver_setup& SS, const int2* tm, int nt,
+                const std::vector<int>& members) {
+        const int e = slot < 3 ? 0 : 1;
+        const BSys<T>* sy = (const BSys<T>*)sys[prec][slot].p;
+        const int pt = SS.precond;
+        const bool cg = SS.solver == XCAL_SOLVER_CG;
+        if (cg) {
+            if (pt != XCAL_PRECOND_NONE) apply_M<T>(prec, slot, e, pt, tm, nt, KV_R, KV_Z, 0);
+            kb_cg_start<T>(stream, sy, tm, nt);
+        } else {
+            apply_M<T>(prec, slot, e, pt, tm, nt, KV_R0, KV_R, 0);
+            kb_bicg_start<T>(stream, sy, tm, nt);
+        }
+        int itmax = 0;
+        for (int i : members) itmax = std::max(itmax, hS[i].itmax);
+        const int CHUNK = cg ? 32 : 8;
+        int chunk = cg ? 4 : 1;
+        long launched = 0;
+        for (;;) {
+            if ((launched += chunk) > (long)itmax + 2 * CHUNK + 32)
+                fail(XCAL_ERR_TIMEOUT, "batch: a Krylov solve did not report completion within itmax iterations");
+            for (int c = 0; c < chunk; ++c) {
+                if (cg) {
+                    kb_cg_spmv<T>(stream, sy, tm, nt);
+                    if (pt == XCAL_PRECOND_JACOBI) {
+                        kb_cg_update<T>(stream, sy, tm, nt, 1);
+                    } else {
+                        kb_cg_update<T>(stream, sy, tm, nt, 0);
+                        if (pt == XCAL_PRECOND_DILU) apply_M<T>(prec, slot, e, pt, tm, nt, KV_R, KV_Z, 1);
+                        kb_cg_rz<T>(stream, sy, tm, nt);
+                    }
+                } else {
+                    kb_spmv<T>(stream, sy, tm, nt, KV_P, KV_Q);
+                    apply_M<T>(prec, slot, e, pt, tm, nt, KV_Q, KV_V, 1);
+                    kb_bicg_alpha<T>(stream, sy, tm, nt);
+                    kb_bicg_s<T>(stream, sy, tm, nt);
+                    kb_spmv<T>(stream, sy, tm, nt, KV_S, KV_Q);
+                    apply_M<T>(prec, slot, e, pt, tm, nt, KV_Q, KV_T, 1);
+                    kb_bicg_omega<T>(stream, sy, tm, nt);
+                    kb_bicg_xr<T>(stream, sy, tm, nt);
+                    kb_bicg_p<T>(stream, sy, tm, nt);
+                }
+            }
+            XCAL_CUDA(cudaMemcpyAsync(hS, S.p, cases.size() * sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
+            sync();
+            bool all = true;
+            for (int i : members) all = all && hS[i].done;
+            if (all) break;
+            if (chunk < CHUNK) chunk *= 2;
+        }
+    }
+
+    // solve_system! for slot (0..2: U component, 3: p) of every case
+    void solve(int slot) {
+        const int nc = (int)cases.size();
+        const bool isU = slot < 3;
+        const int comp = isU ? slot : 0;
+        const bool mixed = cases[0]->cfg.precision == XCAL_PREC_MIXED;
+        const xcal_solver_setup& SS0 = isU ? cases[0]->cfg.U_solver : cases[0]->cfg.p_solver;
+        std::vector<int> all(nc);
+        for (int i = 0; i < nc; ++i) {
+            all[i] = i;
+            Case* c = cases[i];
+            const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
+            std::memset(&hS[i], 0, sizeof(KScalars));
+            hS[i].atol = SS.atol;
+            hS[i].rtol = SS.rtol;
+            hS[i].itmax = SS.itmax == 0 ? 2 * (isU ? c->U.n : c->P.n) : SS.itmax;
+            if (mixed) {
+                hS[i].mixed = 1;
+                hS[i].inner_rtol = c->cfg.inner_rtol > 0 ? c->cfg.inner_rtol : 1e-3;
+            }
+        }
+        if (!mixed) {
+            XCAL_CUDA(cudaMemcpyAsync(S.p, hS, nc * sizeof(KScalars), cudaMemcpyHostToDevice, stream));
+            for (Case* c : cases) {
+                Equation& E = isU ? c->U : c->P;
+                const double* b = isU ? c->U.b[comp].p : c->P.b[0].p;
+                double* field = isU ? c->Uc[comp].p : c->p.p;
+                kr_init_resid(stream, E.view(), E.nz.p, b, field, c->ws.dx.p, c->ws.x.p,
+                              SS0.solver == XCAL_SOLVER_CG ? c->ws.r.p : c->ws.q.p);
+            }
+            krylov<double>(0, slot, SS0, tmap.p, ntiles, all);
+            for (Case* c : cases) {
+                Equation& E = isU ? c->U : c->P;
+                double* field = isU ? c->Uc[comp].p : c->p.p;
+                kr_finish(stream, E.n, c->ws.x.p, c->ws.dx.p, field);
+            }
+            for (int i = 0; i < nc; ++i) cases[i]->last_iters[slot] = hS[i].iter;
+        } else {
+            for (Case* c : cases) {
+                Equation& E = isU ? c->U : c->P;
+                const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
+                kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
+                if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, E.n, E.P.p, E.P32.p);
+            }
+            std::vector<char> active(nc, 1);
+            std::vector<int> total(nc, 0);
+            for (int outer = 0; outer < 64; ++outer) {
+                std::vector<int> mem;
+                for (int i = 0; i < nc; ++i)
+                    if (active[i]) mem.push_back(i);
+                if (mem.empty()) break;
+                for (int i : mem) {
+                    hS[i].outer = outer;
+                    hS[i].iter = 0;
+                    hS[i].done = 0;
+                    hS[i].status = KS_RUNNING;
+                }
+                XCAL_CUDA(cudaMemcpyAsync(S.p, hS, nc * sizeof(KScalars), cudaMemcpyHostToDevice, stream));
+                std::vector<int2> ta;
+                for (const int2& t : h_tmap)
+                    if (active[t.x]) ta.push_back(t);
+                XCAL_CUDA(cudaMemcpyAsync(tmap_act.p, ta.data(), ta.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                                          stream));
+                for (int i : mem) {
+                    Case* c = cases[i];
+                    Equation& E = isU ? c->U : c->P;
+                    const double* b = isU ? c->U.b[comp].p : c->P.b[0].p;
+                    double* field = isU ? c->Uc[comp].p : c->p.p;
+                    float* rhs = SS0.solver == XCAL_SOLVER_CG ? c->ws.fr.p : c->ws.fd.p;
+                    kr_defect(stream, E.view(), E.nz.p, b, field, rhs, c->ws.fx.p);
+                }
+                krylov<float>(1, slot, SS0, tmap_act.p, (int)ta.size(), mem);
+                for (int i : mem) {
+                    if (hS[i].outer_conv) {
+                        active[i] = 0;
+                        continue;
+                    }
+                    total[i] += hS[i].iter;
+                    Case* c = cases[i];
+                    Equation& E = isU ? c->U : c->P;
+                    double* field = isU ? c->Uc[comp].p : c->p.p;
+                    kr_correct(stream, E.n, field, c->ws.fx.p);
+                    int st = hS[i].status;
+                    if (st == KS_ZERO_CURV || st == KS_BREAKDOWN || st == KS_TIRED ||
+                        (st == KS_SOLVED && hS[i].eps <= hS[i].eps_outer))
+                        active[i] = 0;
+                }
+            }
+            for (int i = 0; i < nc; ++i) cases[i]->last_iters[slot] = total[i];
+        }
+        // residual (Solve_1_api.jl:441-464), FP64
+        for (int i = 0; i < nc; ++i) {
+            Case* c = cases[i];
+            Equation& E = isU ? c->U : c->P;
+            const double* b = isU ? c->U.b[comp].p : c->P.b[0].p;
+            double* field = isU ? c->Uc[comp].p : c->p.p;
+            kr_residual(stream, E.view(), E.nz.p, field, b, S.p + i, c->ws.part0.p, c->ws.part1.p,
+                        res.p + 4 * i + slot);
+        }
+    }
+
+    // one SIMPLE iteration of every case (Solvers_1_SIMPLE.jl:164-240)
+    void simple_iteration(double* res_out, int* conv_out) {
+        if (cases.empty()) return;
+        rebuild();
+        for (Case* c : cases) {
+            if (!c->initialised) c->initial_calculations();
+            c->iteration += 1;
+            c->discretise(XCAL_EQN_U);
+        }
+        for (int d = 0; d < 3; ++d) {
+            for (Case* c : cases) {
+                c->bc_relax_U(d);
+                if (d == 0) c->update_precond(XCAL_EQN_U);
+            }
+            solve(d);
+        }
+        for (Case* c : cases) {
+            c->pressure_predictor(true);
+            c->flux_divergence();
+            XCAL_CUDA(cudaMemcpyAsync(c->prev.p, c->p.p, c->mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice,
+                                      stream));
+            c->discretise(XCAL_EQN_P);
+            c->apply_bcs(XCAL_EQN_P, 0);
+            c->set_reference();
+            c->update_precond(XCAL_EQN_P);
+        }
+        solve(3);
+        for (Case* c : cases) {
+            c->explicit_relaxation_p(c->cfg.p_solver.relax);
+            c->grad_p();
+            c->correct();
+            c->turbulence();
+        }
+        XCAL_CUDA(cudaMemcpyAsync(hres, res.p, 4 * cases.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        sync();
+        ++iterations;
+        for (size_t i = 0; i < cases.size(); ++i) {
+            const Case* c = cases[i];
+            const double* r = hres + 4 * i;
+            for (int k = 0; k < 4; ++k) {
+                if (res_out) res_out[4 * i + k] = r[k];
+                if (std::isnan(r[k]) || std::isinf(r[k])) fail(XCAL_ERR_DIVERGED, "batch: residual is NaN/Inf");
+            }
+            bool conv = r[0] <= c->cfg.U_solver.convergence && r[1] <= c->cfg.U_solver.convergence &&
+                        r[2] <= c->cfg.U_solver.convergence && r[3] <= c->cfg.p_solver.convergence &&
+                        c->cfg.turbulence == XCAL_TURB_LAMINAR;
+            if (conv_out) conv_out[i] = conv ? 1 : 0;
+        }
+    }
+};
+
+// Device bytes a case will hold, from the mesh sizes (upper bound of the
+// allocations of upload_mesh and Case::Case; SELL padding bounded by 2%).
+size_t estimate_case_bytes(long nC, long nF, long nB, int mixed, int dilu_U, int dilu_p) {
+    const long nI = nF - nB;
+    const double nnz = (double)(nC + 2 * nI) * 1.02 + 64.0;
+    double b = 0;
+    // mesh
+    b += 88.0 * nF + 9.0 * 2 * nI + 16.0 * (nC + 1) + 8.0 * nC + 12.0 * nB;
+    // equations U and p: slots (col 4, value 8, transpose 4 [+ fp32 value 4]),
+    // rows (len 1, diag 4, diag0 8, P 8 [+ P32 4], b 8 per component, slices),
+    // slot maps (cf_slot 2 nI, fslot nI), DILU level lists (8 per row)
+    for (int e = 0; e < 2; ++e) {
+        int nvec = e == 0 ? 3 : 1;
+        b += nnz * (16.0 + (mixed ? 4.0 : 0.0));
+        b += nC * (21.0 + 8.0 * nvec + (mixed ? 4.0 : 0.0)) + 4.0 * (nC / 32 + 2);
+        b += 4.0 * 3 * nI;
+        if ((e == 0 && dilu_U) || (e == 1 && dilu_p)) b += 8.0 * nC;
+    }
+    // three boundary-condition tables (85 bytes per boundary face) + partner lists
+    b += 3.0 * (85.0 * nB + 4.0 * (nC + 1));
+    // fields: 26 doubles per cell, 8 per face; Krylov: 9 doubles per cell
+    // [+ 9 floats]; tile partials and small buffers
+    b += nC * (26.0 + 9.0) * 8.0 + nF * 8.0 * 8.0 + (mixed ? 36.0 * nC : 0.0);
+    b += 3.0 * 8.0 * (nC / 2048 + 1) + 4096.0;
+    return (size_t)b;
+}
+
+}  // namespace xcal
+
+struct xcal_batch {
+    std::unique_ptr<xcal::Batch> b;
+};
+
+using namespace xcal;
+
+#define XCAL_BGUARD(ctx, ...)                                                 \
+    try {                                                                     \
+        __VA_ARGS__;                                                          \
+        return XCAL_OK;                                                       \
+    } catch (const ::xcal::Error& e) {                                        \
+        if (ctx) ctx->last_error = e.msg;                                     \
+        return e.code;                                                        \
+    } catch (const std::exception& e) {                                       \
+        if (ctx) ctx->last_error = e.what();                                  \
+        return XCAL_ERR_INVALID;                                              \
+    }
+
+extern "C" {
+
+int32_t xcal_footprint_estimate(int64_t n_cells, int64_t n_faces, int64_t n_bfaces, int32_t precision,
+                                int32_t dilu_U, int32_t dilu_p, int64_t* bytes) {
+    if (!bytes || n_cells <= 0 || n_faces < n_bfaces || n_bfaces < 0) return XCAL_ERR_INVALID;
+    *bytes = (int64_t)estimate_case_bytes(n_cells, n_faces, n_bfaces, precision == XCAL_PREC_MIXED ? 1 : 0,
+                                          dilu_U, dilu_p);
+    return XCAL_OK;
+}
+
+int32_t xcal_case_footprint(const xcal_case* cs, int64_t* case_bytes, int64_t* mesh_bytes) {
+    if (!cs) return XCAL_ERR_INVALID;
+    if (case_bytes) *case_bytes = (int64_t)cs->c->bytes;
+    if (mesh_bytes) *mesh_bytes = (int64_t)cs->c->mesh->bytes;
+    return XCAL_OK;
+}
+
+int32_t xcal_batch_create(xcal_ctx* ctx, int32_t max_cases, int64_t budget_bytes, xcal_batch** out) {
+    if (!ctx || !out || max_cases <= 0 || budget_bytes <= 0) return XCAL_ERR_INVALID;
+    *out = nullptr;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return XCAL_ERR_CUDA;
+    XCAL_BGUARD(ctx, {
+        std::unique_ptr<Batch> b(new Batch(ctx, max_cases, (size_t)budget_bytes));
+        xcal_batch* h = new xcal_batch();
+        h->b = std::move(b);
+        *out = h;
+    })
+}
+
+int32_t xcal_batch_destroy(xcal_batch* b) {
+    delete b;
+    return XCAL_OK;
+}
+
+int32_t xcal_batch_add(xcal_batch* bt, xcal_case* cs, int64_t charge_bytes) {
+    if (!bt || !cs) return XCAL_ERR_INVALID;
+    Batch* b = bt->b.get();
+    XCAL_BGUARD(b->ctx, {
+        size_t charge = charge_bytes > 0 ? (size_t)charge_bytes : cs->c->bytes + cs->c->mesh->bytes;
+        b->add(cs->c.get(), charge);
+    })
+}
+
+int32_t xcal_batch_remove(xcal_batch* bt, xcal_case* cs) {
+    if (!bt || !cs) return XCAL_ERR_INVALID;
+    Batch* b = bt->b.get();
+    XCAL_BGUARD(b->ctx, { b->remove(cs->c.get()); })
+}
+
+int32_t xcal_batch_info(const xcal_batch* bt, int32_t* n_cases, int64_t* used_bytes, int64_t* budget_bytes) {
+    if (!bt) return XCAL_ERR_INVALID;
+    if (n_cases) *n_cases = (int32_t)bt->b->cases.size();
+    if (used_bytes) *used_bytes = (int64_t)bt->b->used;
+    if (budget_bytes) *budget_bytes = (int64_t)bt->b->budget;
+    return XCAL_OK;
+}
+
+int32_t xcal_batch_case_index(const xcal_batch* bt, const xcal_case* cs, int32_t* index) {
+    if (!bt || !cs || !index) return XCAL_ERR_INVALID;
+    *index = bt->b->index_of(cs->c.get());
+    return *index >= 0 ? XCAL_OK : XCAL_ERR_INVALID;
+}
+
+int32_t xcal_batch_simple_iterate(xcal_batch* bt, double* res, int32_t* converged) {
+    if (!bt) return XCAL_ERR_INVALID;
+    Batch* b = bt->b.get();
+    XCAL_BGUARD(b->ctx, { b->simple_iteration(res, converged); })
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+// batch.hpp -- batched Krylov solves over many independent cases.
+//
+// A batch holds the resident cases of a request stream.  Their pressure and
+// momentum systems form one block-diagonal system: each case keeps its own
+// SELL matrix, vectors and Krylov scalars, and a launch covers every case at
+// once through a per-system descriptor table and a tile map (block b works on
+// local tile tmap[b].y of system tmap[b].x).  Row sums and reduction trees are
+// the single-case ones, so a case's result does not depend on the batch it
+// ran in.
+#pragma once
+#include "xcal_internal.hpp"
+
+namespace xcal {
+
+// roles of the work vectors in a batched system descriptor
+enum {
+    KV_X = 0,  // iterate
+    KV_R,      // residual
+    KV_Z,      // preconditioned residual (CG; = KV_R without preconditioner)
+    KV_P,      // direction (CG p_k of even k)
+    KV_Q,      // A * direction
+    KV_V,      // CG p_k of odd k; BiCGSTAB v
+    KV_S,      // BiCGSTAB s
+    KV_T,      // BiCGSTAB t
+    KV_C,      // BiCGSTAB shadow vector (right-hand side)
+    KV_R0,     // BiCGSTAB unpreconditioned initial residual
+    KV_COUNT
+};
+
+template <class T>
+struct BSys {
+    CSRView A;
+    const T* nz;
+    const T* P;  // Jacobi inverse diagonal or DILU D
+    T* vec[KV_COUNT];
+    KScalars* S;
+    double* part0;
+    double* part1;
+    int n;
+    int ntiles;
+};
+
+// batched launchers (kernels_batch.cu); tmap has ntiles_total entries
+template <class T>
+void kb_spmv(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int in, int out);
+template <class T>
+void kb_jacobi_apply(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int in, int out,
+                     int use_S);
+template <class T>
+void kb_copy(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int in, int out, int use_S);
+template <class T>
+void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int2* lo_rows, const std::vector<int>& lo_off,
+             const int2* up_rows, const std::vector<int>& up_off, int in, int out, int use_S);
+template <class T>
+void kb_cg_start(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+template <class T>
+void kb_cg_spmv(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+template <class T>
+void kb_cg_update(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int jacobi_fused);
+template <class T>
+void kb_cg_rz(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+template <class T>
+void kb_bicg_start(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+template <class T>
+void kb_bicg_alpha(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+template <class T>
+void kb_bicg_s(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+template <class T>
+void kb_bicg_omega(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+template <class T>
+void kb_bicg_xr(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+template <class T>
+void kb_bicg_p(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+
+}  // namespace xcal

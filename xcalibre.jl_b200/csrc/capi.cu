@@ -10,6 +10,7 @@ namespace xcal {
 DevMesh* upload_mesh(const xcal_mesh_desc* d, cudaStream_t s);
 std::atomic<long long> g_launch_count{0};
 thread_local long long t_launch_count = 0;
+thread_local size_t* t_alloc_acc = nullptr;
 }
 using namespace xcal;
 

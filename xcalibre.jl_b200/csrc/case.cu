@@ -150,6 +150,7 @@ DevMesh* upload_mesh(const xcal_mesh_desc* d0, cudaStream_t s) {
             d0->cell_neighbours[k] >= nC)
             fail(XCAL_ERR_INVALID, "mesh: invalid cell_faces entry");
     auto m = std::make_unique<DevMesh>();
+    AllocScope acc(&m->bytes);
     // cell order and face order (boundary faces keep their ids; internal faces
     // follow their storage owner/neighbour)
     locality_order(nC, d0->cell_centre, m->perm);
@@ -436,6 +437,7 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
             for (int i = 0; i < n; ++i) rows[cur[lvl[i]]++] = i;
         }
         E.d_lower_rows.upload(rows, s);
+        E.h_lower_rows = rows;
         std::fill(lvl.begin(), lvl.end(), 0);
         maxl = 0;
         for (int io = n - 1; io >= 0; --io) {
@@ -454,6 +456,7 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
             for (int i = 0; i < n; ++i) rows[cur[lvl[i]]++] = i;
         }
         E.d_upper_rows.upload(rows, s);
+        E.h_upper_rows = rows;
     }
 }
 
@@ -569,6 +572,7 @@ static void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int
 // case
 // ---------------------------------------------------------------------------
 Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(m), cfg(*cf) {
+    AllocScope acc(&bytes);
     if (cfg.U_solver.relax <= 0.0 || cfg.p_solver.relax <= 0.0) fail(XCAL_ERR_INVALID, "relax must be > 0");
     if (cfg.algorithm == XCAL_ALGO_PISO && cfg.dt <= 0.0) fail(XCAL_ERR_INVALID, "PISO needs dt > 0");
     if (cfg.precision != XCAL_PREC_FP64 && cfg.precision != XCAL_PREC_MIXED)

@@ -25,6 +25,7 @@ struct DevMesh {
     DBuf<int> d_owner, d_neigh, d_cf_off, d_cf_face, d_cf_nb, d_bf_off, d_bf_face, d_bcell, d_bcells;
     DBuf<signed char> d_cf_sign;
     DBuf<double> d_area, d_delta, d_weight, d_Sx, d_Sy, d_Sz, d_nx, d_ny, d_nz, d_Ef, d_vol;
+    size_t bytes = 0;  // device bytes held
     MeshView view() const;
 };
 
@@ -43,6 +44,7 @@ struct Equation {
     // DILU level schedules (rows grouped by dependency level)
     DBuf<int> d_lower_rows, d_upper_rows;
     std::vector<int> lower_off, upper_off;
+    std::vector<int> h_lower_rows, h_upper_rows;  // host copies (batched level lists)
     bool has_periodic = false;
     CSRView view() const;
     int find(int i, int j) const;  // slot or -1
@@ -76,6 +78,7 @@ struct Case {
     xcal_ctx* ctx = nullptr;
     const DevMesh* mesh = nullptr;
     xcal_config cfg{};
+    size_t bytes = 0;  // device bytes held (excluding the mesh)
     cudaStream_t stream = nullptr;
     bool own_stream = true;
     BCTable bcU, bcP, bcNut;

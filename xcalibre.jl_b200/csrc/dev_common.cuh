@@ -20,6 +20,18 @@ constexpr int RED_TILE = RED_THREADS * RED_ITEMS;
 
 __device__ __forceinline__ int tile_row(int k) { return blockIdx.x * RED_TILE + k * RED_THREADS + threadIdx.x; }
 
+// The tile a block works on and the number of tiles of its system: the grid
+// itself for a single system; a (system, local tile) map entry for a batched
+// launch over many independent systems (block-diagonal, per-system offsets).
+struct TileCtx {
+    int tile;
+    int ntiles;
+};
+__device__ __forceinline__ TileCtx grid_tiles() { return TileCtx{(int)blockIdx.x, (int)gridDim.x}; }
+__device__ __forceinline__ int tile_row(const TileCtx& tc, int k) {
+    return tc.tile * RED_TILE + k * RED_THREADS + threadIdx.x;
+}
+
 // Load of data read once per launch (matrix slots, vectors consumed by their
 // last reader): evict-first in L1 and L2, so the streams do not push the
 // gathered vectors out of L2.  Measured on the 2M-cell pressure matrix: the
@@ -66,21 +78,23 @@ __device__ __forceinline__ double reduce_partials(const double* part, int T, dou
     return block_tree(s, smem8);
 }
 
-// Last-block election: every block publishes its partial(s) before calling;
-// returns true in all threads of the block that arrives last (the counter is
-// reset by it).  No block waits, so there is no spin.
-__device__ __forceinline__ bool last_block(unsigned int* counter) {
+// Last-block election among the ntiles blocks of one system: every block
+// publishes its partial(s) before calling; returns true in all threads of the
+// block that arrives last (the counter is reset by it).  No block waits, so
+// there is no spin.
+__device__ __forceinline__ bool last_block(unsigned int* counter, int ntiles) {
     __shared__ bool is_last;
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned int ticket = atomicAdd(counter, 1u);
-        is_last = (ticket == gridDim.x - 1);
+        is_last = (ticket == (unsigned int)ntiles - 1u);
         if (is_last) *counter = 0u;
     }
     __syncthreads();
     if (is_last) __threadfence();
     return is_last;
 }
+__device__ __forceinline__ bool last_block(unsigned int* counter) { return last_block(counter, (int)gridDim.x); }
 
 }  // namespace xcal

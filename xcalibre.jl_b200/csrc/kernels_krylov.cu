@@ -13,65 +13,14 @@
 // mixed-precision mode: FP32 matrix values, vectors and row sums, with dot
 // products accumulated in FP64 and the step scalars kept in FP64 on the
 // device and rounded to FP32 where they scale a vector.
-#include "dev_common.cuh"
 #include "kernels.hpp"
+#include "krylov_bodies.cuh"
 
 namespace xcal {
 
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
-template <class T>
-__device__ __forceinline__ T row_dot(const CSRView& A, const T* __restrict__ nz, const T* __restrict__ x, int i) {
-    // xmul! row (src/Multithread/spmvm.jl:47-53): sequential from 0.0
-    T acc = T(0);
-    const int rb = row_base(A, i), rl = A.len[i];
-    for (int k = 0; k < rl; ++k) {
-        int e = rb + SELL_C * k;
-        acc = acc + ld_stream(nz + e) * x[ld_stream(A.colval + e)];
-    }
-    return acc;
-}
-
-// CG stopping decisions after gamma_next = <r,z> (Krylov.jl cg!)
-__device__ void cg_finalize(KScalars* S, double gamma_next) {
-    double rNorm = sqrt(gamma_next);
-    S->rNorm = rNorm;
-    bool mach = (rNorm + 1.0 <= 1.0);
-    bool solved = (rNorm <= S->eps) || mach;
-    if (!solved) {
-        double beta = gamma_next / S->gamma;
-        S->pNorm2 = gamma_next + (beta * beta) * S->pNorm2;
-        S->gamma = gamma_next;
-        S->beta = beta;
-    }
-    S->iter = S->iter + 1;
-    bool tired = S->iter >= S->itmax;
-    if (solved) {
-        S->done = 1;
-        S->status = KS_SOLVED;
-    } else if (tired) {
-        S->done = 1;
-        S->status = KS_TIRED;
-    }
-}
-
-// Stopping tolerance at the start of a solve.  Plain mode: Krylov.jl's
-// atol + rtol*||r0||.  Mixed mode (inner solve of a defect-correction
-// step): the outer target atol + rtol*||r0|| is fixed by the first defect of
-// the solve; an inner solve stops at the looser of that target and
-// inner_rtol times its own initial norm, and a defect already below the
-// target ends the outer loop.
-__device__ __forceinline__ void start_eps(KScalars* S, double rNorm) {
-    if (!S->mixed) {
-        S->eps = S->atol + S->rtol * rNorm;
-        return;
-    }
-    if (S->outer == 0) S->eps_outer = S->atol + S->rtol * rNorm;
-    S->eps = fmax(S->eps_outer, S->inner_rtol * rNorm);
-    S->outer_conv = rNorm <= S->eps_outer ? 1 : 0;
-}
-
 // ---------------------------------------------------------------------------
 // kernels (grid = one canonical tile per block, RED_THREADS threads)
 // ---------------------------------------------------------------------------
@@ -122,30 +71,18 @@ __global__ void k_to_float(long n, const double* __restrict__ src, float* dst) {
 template <class T>
 __global__ void __launch_bounds__(RED_THREADS, 8) k_spmv(CSRView A, const T* __restrict__ nz,
                                                       const T* __restrict__ x, T* y, const KScalars* S) {
-    if (S && S->done) return;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < A.n) y[i] = row_dot(A, nz, x, i);
-    }
+    spmv_body<T>(grid_tiles(), A, nz, x, y, S);
 }
 
 // z = P .* r (Jacobi: opDiagonal multiply, ldiv = false)
 template <class T>
 __global__ void k_jacobi_apply(int n, const T* __restrict__ P, const T* __restrict__ r, T* z, const KScalars* S) {
-    if (S && S->done) return;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) z[i] = P[i] * r[i];
-    }
+    jacobi_apply_body<T>(grid_tiles(), n, P, r, z, S);
 }
 
 template <class T>
 __global__ void k_copy(int n, const T* __restrict__ a, T* b, const KScalars* S) {
-    if (S && S->done) return;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) b[i] = a[i];
-    }
+    copy_body<T>(grid_tiles(), n, a, b, S);
 }
 
 // ---- CG ----
@@ -153,56 +90,7 @@ __global__ void k_copy(int n, const T* __restrict__ a, T* b, const KScalars* S) 
 template <class T>
 __global__ void k_cg_start(int n, const T* __restrict__ r, const T* __restrict__ z, T* p, KScalars* S,
                            double* part) {
-    __shared__ double sm[8];
-    double acc = 0.0;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) {
-            T zi = z[i];
-            p[i] = zi;
-            acc = acc + (double)r[i] * (double)zi;
-        }
-    }
-    double tot = block_tree(acc, sm);
-    if (threadIdx.x == 0) part[blockIdx.x] = tot;
-    if (!last_block(&S->counter)) return;
-    double gamma = reduce_partials(part, gridDim.x, sm);
-    if (threadIdx.x == 0) {
-        S->gamma = gamma;
-        double rNorm = sqrt(gamma);
-        S->rNorm = rNorm;
-        S->rNorm0 = rNorm;
-        S->iter = 0;
-        S->done = 0;
-        S->status = KS_RUNNING;
-        S->outer_conv = 0;
-        S->loops = 0;
-        if (gamma == 0.0) {
-            S->done = 1;
-            S->status = KS_ZERO_RHS;
-            S->outer_conv = 1;
-            return;
-        }
-        S->pNorm2 = gamma;
-        start_eps(S, rNorm);
-        if (rNorm <= S->eps) {
-            S->done = 1;
-            S->status = KS_SOLVED;
-        } else if (S->iter >= S->itmax) {
-            S->done = 1;
-            S->status = KS_TIRED;
-        }
-    }
-}
-
-// CG direction buffers alternate: iteration k uses p_k = P[k & 1].  cg_start
-// stores p_0 = z in P[0]; for k >= 1 the SpMV forms p_k = z + beta*p_{k-1}
-// on the fly (Krylov.jl kaxpby!(n, 1, z, beta, p) -- the same expression for
-// every reader, so gathered neighbours see bit-identical values) and the
-// thread owning a row stores it.  The separate p-update pass disappears.
-template <class T>
-__device__ __forceinline__ T cg_dir(const T* __restrict__ z, const T* __restrict__ pold, T beta, int j) {
-    return z[j] + beta * pold[j];
+    cg_start_body<T>(grid_tiles(), n, r, z, p, S, part);
 }
 
 // q = A p_k; pAp = <p_k,q>; zero-curvature test; alpha = gamma / pAp
@@ -210,45 +98,7 @@ template <class T>
 __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const T* __restrict__ nz,
                                                          const T* __restrict__ z, T* P0, T* P1, T* q, KScalars* S,
                                                          double* part) {
-    if (S->done) return;
-    __shared__ double sm[8];
-    const int it = S->iter;
-    const T beta = (T)S->beta;
-    T* pk = (it & 1) ? P1 : P0;
-    const T* pold = (it & 1) ? P0 : P1;
-    double acc = 0.0;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < A.n) {
-            T qi = T(0), pi;
-            const int rb = row_base(A, i), e1 = rb + SELL_C * A.len[i];
-            if (it == 0) {
-                for (int e = rb; e < e1; e += SELL_C) qi = qi + ld_stream(nz + e) * pk[ld_stream(A.colval + e)];
-                pi = pk[i];
-            } else {
-                for (int e = rb; e < e1; e += SELL_C)
-                    qi = qi + ld_stream(nz + e) * cg_dir(z, pold, beta, ld_stream(A.colval + e));
-                pi = cg_dir(z, pold, beta, i);
-                pk[i] = pi;
-            }
-            q[i] = qi;
-            acc = acc + (double)pi * (double)qi;
-        }
-    }
-    double tot = block_tree(acc, sm);
-    if (threadIdx.x == 0) part[blockIdx.x] = tot;
-    if (!last_block(&S->counter)) return;
-    double pAp = reduce_partials(part, gridDim.x, sm);
-    if (threadIdx.x == 0) {
-        const double epsT = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;  // eps(T)
-        double lim = epsT * S->pNorm2;
-        if (pAp <= lim && fabs(pAp) <= lim) {
-            S->done = 1;
-            S->status = KS_ZERO_CURV;
-            return;
-        }
-        S->alpha = S->gamma / pAp;
-    }
+    cg_spmv_body<T>(grid_tiles(), A, nz, z, P0, P1, q, S, part);
 }
 
 // x += alpha p_k; r -= alpha q; [Jacobi: z = P r; <r,z>; finalize]
@@ -256,49 +106,13 @@ template <class T>
 __global__ void k_cg_update(int n, T* x, const T* __restrict__ P0, const T* __restrict__ P1, T* r,
                             const T* __restrict__ q, T* z, const T* __restrict__ P, int jacobi_fused, KScalars* S,
                             double* part) {
-    if (S->done) return;
-    __shared__ double sm[8];
-    const T* p = (S->iter & 1) ? P1 : P0;
-    const T alpha = (T)S->alpha;
-    double acc = 0.0;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) {
-            // x, q and P are not read again before the next update: evict-first
-            // keeps L2 for z and p, which the next SpMV gathers
-            __stcs(x + i, ld_stream(x + i) + alpha * p[i]);
-            T ri = r[i] + (-alpha) * ld_stream(q + i);
-            r[i] = ri;
-            if (jacobi_fused) {
-                T zi = ld_stream(P + i) * ri;
-                z[i] = zi;
-                acc = acc + (double)ri * (double)zi;
-            }
-        }
-    }
-    if (!jacobi_fused) return;
-    double tot = block_tree(acc, sm);
-    if (threadIdx.x == 0) part[blockIdx.x] = tot;
-    if (!last_block(&S->counter)) return;
-    double g = reduce_partials(part, gridDim.x, sm);
-    if (threadIdx.x == 0) cg_finalize(S, g);
+    cg_update_body<T>(grid_tiles(), n, x, P0, P1, r, q, z, P, jacobi_fused, S, part);
 }
 
 // <r,z> + finalize when z came from a separate preconditioner apply
 template <class T>
 __global__ void k_cg_rz(int n, const T* __restrict__ r, const T* __restrict__ z, KScalars* S, double* part) {
-    if (S->done) return;
-    __shared__ double sm[8];
-    double acc = 0.0;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) acc = acc + (double)r[i] * (double)z[i];
-    }
-    double tot = block_tree(acc, sm);
-    if (threadIdx.x == 0) part[blockIdx.x] = tot;
-    if (!last_block(&S->counter)) return;
-    double g = reduce_partials(part, gridDim.x, sm);
-    if (threadIdx.x == 0) cg_finalize(S, g);
+    cg_rz_body<T>(grid_tiles(), n, r, z, S, part);
 }
 
 // field = x + dx (warm start shift)
@@ -314,182 +128,40 @@ __global__ void k_finish(int n, const double* __restrict__ x, const double* __re
 template <class T>
 __global__ void k_bicg_start(int n, const T* __restrict__ c, const T* __restrict__ r, T* p, KScalars* S,
                              double* part0, double* part1) {
-    __shared__ double sm[8];
-    double a0 = 0.0, a1 = 0.0;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) {
-            T ri = r[i];
-            p[i] = ri;
-            a0 = a0 + (double)ri * (double)ri;
-            a1 = a1 + (double)c[i] * (double)ri;
-        }
-    }
-    double t0 = block_tree(a0, sm);
-    double t1 = block_tree(a1, sm);
-    if (threadIdx.x == 0) {
-        part0[blockIdx.x] = t0;
-        part1[blockIdx.x] = t1;
-    }
-    if (!last_block(&S->counter)) return;
-    double rr = reduce_partials(part0, gridDim.x, sm);
-    double cr = reduce_partials(part1, gridDim.x, sm);
-    if (threadIdx.x == 0) {
-        double rNorm = sqrt(rr);
-        S->rNorm = rNorm;
-        S->rNorm0 = rNorm;
-        S->iter = 0;
-        S->done = 0;
-        S->status = KS_RUNNING;
-        S->outer_conv = 0;
-        S->loops = 0;
-        if (rNorm == 0.0) {
-            S->done = 1;
-            S->status = KS_ZERO_RHS;
-            S->outer_conv = 1;
-            return;
-        }
-        start_eps(S, rNorm);
-        S->next_rho = cr;
-        if (cr == 0.0) {
-            S->done = 1;
-            S->status = KS_BREAKDOWN;
-            return;
-        }
-        if (rNorm <= S->eps) {
-            S->done = 1;
-            S->status = KS_SOLVED;
-        } else if (S->iter >= S->itmax) {
-            S->done = 1;
-            S->status = KS_TIRED;
-        }
-    }
+    bicg_start_body<T>(grid_tiles(), n, c, r, p, S, part0, part1);
 }
 
 // alpha = rho / <c,v> (rho = next_rho; iteration counter advances)
 template <class T>
 __global__ void k_bicg_alpha(int n, const T* __restrict__ c, const T* __restrict__ v, KScalars* S, double* part) {
-    if (S->done) return;
-    __shared__ double sm[8];
-    double acc = 0.0;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) acc = acc + (double)c[i] * (double)v[i];
-    }
-    double tot = block_tree(acc, sm);
-    if (threadIdx.x == 0) part[blockIdx.x] = tot;
-    if (!last_block(&S->counter)) return;
-    double cv = reduce_partials(part, gridDim.x, sm);
-    if (threadIdx.x == 0) {
-        S->iter = S->iter + 1;
-        S->rho = S->next_rho;
-        S->cv = cv;
-        S->alpha = S->rho / cv;
-    }
+    bicg_alpha_body<T>(grid_tiles(), n, c, v, S, part);
 }
 
 // s = r - alpha v; x = x + alpha p
 template <class T>
 __global__ void k_bicg_s(int n, const T* __restrict__ r, const T* __restrict__ v, const T* __restrict__ p, T* s,
                          T* x, const KScalars* S) {
-    if (S->done) return;
-    const T alpha = (T)S->alpha;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) {
-            s[i] = r[i] + (-alpha) * v[i];
-            x[i] = x[i] + alpha * p[i];
-        }
-    }
+    bicg_s_body<T>(grid_tiles(), n, r, v, p, s, x, S);
 }
 
 // omega = <t,s> / <t,t>
 template <class T>
 __global__ void k_bicg_omega(int n, const T* __restrict__ t, const T* __restrict__ s, KScalars* S, double* part0,
                              double* part1) {
-    if (S->done) return;
-    __shared__ double sm[8];
-    double a0 = 0.0, a1 = 0.0;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) {
-            double ti = (double)t[i];
-            a0 = a0 + ti * (double)s[i];
-            a1 = a1 + ti * ti;
-        }
-    }
-    double t0 = block_tree(a0, sm);
-    double t1 = block_tree(a1, sm);
-    if (threadIdx.x == 0) {
-        part0[blockIdx.x] = t0;
-        part1[blockIdx.x] = t1;
-    }
-    if (!last_block(&S->counter)) return;
-    double ts = reduce_partials(part0, gridDim.x, sm);
-    double tt = reduce_partials(part1, gridDim.x, sm);
-    if (threadIdx.x == 0) S->omega = ts / tt;
+    bicg_omega_body<T>(grid_tiles(), n, t, s, S, part0, part1);
 }
 
 // x = x + omega s; r = s - omega t; next_rho = <c,r>; ||r||; stopping tests
 template <class T>
 __global__ void k_bicg_xr(int n, T* x, const T* __restrict__ s, const T* __restrict__ t, T* r,
                           const T* __restrict__ c, KScalars* S, double* part0, double* part1) {
-    if (S->done) return;
-    __shared__ double sm[8];
-    const double omega = S->omega;
-    const T om = (T)omega;
-    double a0 = 0.0, a1 = 0.0;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) {
-            T si = s[i];
-            x[i] = x[i] + om * si;
-            T ri = si + (-om) * t[i];
-            r[i] = ri;
-            a0 = a0 + (double)c[i] * (double)ri;
-            a1 = a1 + (double)ri * (double)ri;
-        }
-    }
-    double t0 = block_tree(a0, sm);
-    double t1 = block_tree(a1, sm);
-    if (threadIdx.x == 0) {
-        part0[blockIdx.x] = t0;
-        part1[blockIdx.x] = t1;
-    }
-    if (!last_block(&S->counter)) return;
-    double cr = reduce_partials(part0, gridDim.x, sm);
-    double rr = reduce_partials(part1, gridDim.x, sm);
-    if (threadIdx.x == 0) {
-        S->next_rho = cr;
-        S->beta = (cr / S->rho) * (S->alpha / omega);
-        double rNorm = sqrt(rr);
-        S->rNorm = rNorm;
-        bool mach = (rNorm + 1.0 <= 1.0);
-        bool solved = (rNorm <= S->eps) || mach;
-        bool tired = S->iter >= S->itmax;
-        bool breakdown = (S->alpha == 0.0) || isnan(S->alpha);
-        if (solved) {
-            S->done = 1;
-            S->status = KS_SOLVED;
-        } else if (tired) {
-            S->done = 1;
-            S->status = KS_TIRED;
-        } else if (breakdown) {
-            S->done = 1;
-            S->status = KS_BREAKDOWN;
-        }
-    }
+    bicg_xr_body<T>(grid_tiles(), n, x, s, t, r, c, S, part0, part1);
 }
 
 // p = r + beta (p - omega v)
 template <class T>
 __global__ void k_bicg_p(int n, const T* __restrict__ r, const T* __restrict__ v, T* p, const KScalars* S) {
-    if (S->done) return;
-    const T beta = (T)S->beta, omega = (T)S->omega;
-    for (int k = 0; k < RED_ITEMS; ++k) {
-        int i = tile_row(k);
-        if (i < n) p[i] = r[i] + beta * (p[i] + (-omega) * v[i]);
-    }
+    bicg_p_body<T>(grid_tiles(), n, r, v, p, S);
 }
 
 // ---- preconditioners ----
@@ -527,14 +199,7 @@ __global__ void k_dilu_fwd(const int* __restrict__ rows, int nrows, CSRView A, c
     if (S && S->done) return;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nrows) return;
-    int i = rows[t];
-    int ds = A.diag[i];
-    T sum = T(0);
-    for (int e = row_base(A, i); e < ds; e += SELL_C) {
-        int j = ld_stream(A.colval + e);
-        sum = sum + (ld_stream(nz + e) * y[j]) * (T(1) / D[j]);
-    }
-    y[i] = b[i] - sum;
+    dilu_fwd_row(A, nz, D, b, y, rows[t]);
 }
 
 // backward_substitution! (preconditioners_1_DILU.jl:100-114), one level, in place
@@ -544,12 +209,7 @@ __global__ void k_dilu_bwd(const int* __restrict__ rows, int nrows, CSRView A, c
     if (S && S->done) return;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nrows) return;
-    int i = rows[t];
-    int ds = A.diag[i];
-    T sum = T(0);
-    int e1 = row_base(A, i) + SELL_C * A.len[i];
-    for (int e = ds + SELL_C; e < e1; e += SELL_C) sum = sum + ld_stream(nz + e) * x[ld_stream(A.colval + e)];
-    x[i] = (x[i] - sum) / D[i];
+    dilu_bwd_row(A, nz, D, x, rows[t]);
 }
 
 // residual (src/Solve/Solve_1_api.jl:441-464): ||b - A x|| / max(||b||, 1 if tiny)

@@ -51,6 +51,15 @@ extern thread_local long long t_launch_count;
 
 inline void fail(int code, const std::string& m) { throw Error{code, m}; }
 
+// device bytes allocated by this thread are added here while an owner (mesh
+// or case under construction) has it set
+extern thread_local size_t* t_alloc_acc;
+struct AllocScope {  // RAII: account DBuf allocations to *acc
+    size_t* prev;
+    explicit AllocScope(size_t* acc) : prev(t_alloc_acc) { t_alloc_acc = acc; }
+    ~AllocScope() { t_alloc_acc = prev; }
+};
+
 // ---------------------------------------------------------------------------
 // device buffers
 // ---------------------------------------------------------------------------
@@ -71,6 +80,7 @@ struct DBuf {
         release();
         n = count;
         if (count) XCAL_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        if (t_alloc_acc) *t_alloc_acc += count * sizeof(T);
     }
     void zero(cudaStream_t s) {
         if (n) XCAL_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));

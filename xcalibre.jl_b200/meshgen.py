@@ -153,20 +153,24 @@ def box_polymesh(nx: int, ny: int, nz: int, lengths=(1.0, 1.0, 1.0), origin=(0.0
                     neighbour=nei_i.astype(np.int32), patch_names=names, patch_sizes=sizes)
 
 
-def cavity_polymesh(n: int = 80, seed: int | None = None) -> PolyMesh:
-    """Lid-driven cavity: unit square, n x n x 1 hex slab of thickness 1/n.
+def cavity_polymesh(n: int = 80, seed: int | None = None, nx: int | None = None, lx: float = 1.0) -> PolyMesh:
+    """Lid-driven cavity: [0, lx] x [0, 1] (unit square by default), an
+    nx x n x 1 hex slab (nx = n by default) of thickness 1/n.
 
-    Patches (in order): lid (y = 1), walls (x = 0, x = 1, y = 0),
+    Patches (in order): lid (y = 1), walls (x = 0, x = lx, y = 0),
     frontAndBack (z faces, Empty)."""
-    return box_polymesh(n, n, 1, lengths=(1.0, 1.0, 1.0 / n),
+    nx = n if nx is None else nx
+    return box_polymesh(nx, n, 1, lengths=(lx, 1.0, 1.0 / n),
                         patches=[("lid", ["ymax"]), ("walls", ["xmin", "xmax", "ymin"]),
                                  ("frontAndBack", ["zmin", "zmax"])], seed=seed)
 
 
-def channel_polymesh(nx: int = 128, ny: int = 128, nz: int = 128, seed: int | None = 0) -> PolyMesh:
-    """Steady channel: box [0,4]x[0,1]x[0,1]; patches inlet (x = 0),
-    outlet (x = 4), walls (y and z sides); numbering permuted from ``seed``."""
-    return box_polymesh(nx, ny, nz, lengths=(4.0, 1.0, 1.0),
+def channel_polymesh(nx: int = 128, ny: int = 128, nz: int = 128, seed: int | None = 0,
+                     length: float = 4.0) -> PolyMesh:
+    """Steady channel: box [0,length]x[0,1]x[0,1] (length 4 by default);
+    patches inlet (x = 0), outlet (x = length), walls (y and z sides);
+    numbering permuted from ``seed``."""
+    return box_polymesh(nx, ny, nz, lengths=(length, 1.0, 1.0),
                         patches=[("inlet", ["xmin"]), ("outlet", ["xmax"]),
                                  ("walls", ["ymin", "ymax", "zmin", "zmax"])], seed=seed)
 
