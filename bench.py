@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-second-precision", action="store_true",
                     help="skip the second timed run in the other precision mode")
+    ap.add_argument("--les-size", type=int, default=96, help="periodic LES box: cells per side (0 = skip)")
+    ap.add_argument("--les-steps", type=int, default=200)
+    ap.add_argument("--serve-cases", type=int, default=16, help="serving stream: requests (0 = skip)")
+    ap.add_argument("--serve-nmax", type=float, default=3e4)
+    ap.add_argument("--serve-rate", type=float, default=8.0)
     return ap.parse_args()
 
 
@@ -263,6 +268,72 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
     return out, case, dm, model
 
 
+def les_measure(x, A, args, local):
+    """Transient LES (PISO + Smagorinsky Cs = 0.17) on the periodic 2*pi cube:
+    seeded divergence-free Fourier initial field (k^4 exp(-2 (k/4)^2), rms 1),
+    nu = 1e-4, dt from CFL 0.5, 2 correctors; mixed precision; every time step
+    one CUDA graph (device-driven Krylov loops).  Steps timed with CUDA
+    events on the case stream after 3 warm-up steps."""
+    import torch
+    n = args.les_size
+    mesh = x.build_mesh3(x.periodic_box_polymesh(n, seed=0))
+    U0 = x.cases.fourier_field(mesh, seed=0)
+    out = {"workload": f"periodic LES box 2pi^3, {n}^3 hex = {mesh.n_cells} cells, PISO x2 correctors, "
+                       f"Smagorinsky 0.17, nu 1e-4, CFL 0.5, mixed precision, graph per step"}
+    model, config = x.cases.periodic_les_case(mesh, steps=args.les_steps, U0=U0, precision="mixed", device=local)
+    cfg, keep = x.build_config(model, config, pref=0.0)
+    ctx = x.Context(local)
+    dm = x.DeviceMesh(ctx, mesh)
+    case = x.Case(dm, cfg)
+    case.set_field(A.FIELD_U, model.momentum.U)
+    case.set_field(A.FIELD_P, model.momentum.p)
+    case.set_graph_mode(True)
+    stream = torch.cuda.ExternalStream(case.stream(), device=torch.device("cuda", local))
+    case.piso_step(3)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = x.launch_count()
+    e0.record(stream)
+    res, co = case.piso_step(args.les_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out.update({"value": mesh.n_cells * args.les_steps / (ms / 1e3) / 1e6, "unit": UNIT,
+                "ms_per_step": ms / args.les_steps, "steps": args.les_steps, "dt": config.runtime.time_step,
+                "courant_last": float(co[-1]), "residuals_last": [float(v) for v in res[-1]],
+                "gpu_launches": x.launch_count() - l0})
+    case.close()
+    dm.close()
+    return out
+
+
+def serve_measure(x, args, local):
+    """Serving stream: steady cavity/channel requests (50/50), N log-uniform
+    in [1e3, serve_nmax], aspect U[1,4], Re U[100,2000], Poisson arrivals at
+    serve_rate per second, mixed precision, each to a 1e-6 scaled residual
+    (cap 1500 SIMPLE iterations); continuous batching with admission by
+    device-memory footprint.  Meshes are built before the stream starts
+    (they are the requests' payload)."""
+    from importlib import import_module
+    serve = import_module(x.__name__ + ".serve")
+    reqs = serve.make_requests(args.serve_cases, seed=0, n_min=1e3, n_max=args.serve_nmax, rate=args.serve_rate)
+    for r in reqs:
+        r.build()
+    ctx = x.Context(local)
+    srv = serve.Server(ctx, budget_bytes=40 << 30, max_cases=64, precision="mixed", max_iters=1500,
+                       convergence=1e-6)
+    l0 = x.launch_count()
+    res = srv.run(reqs, realtime=True)
+    s = serve.summarize(res, srv.wall)
+    s.update({"workload": f"{len(reqs)} steady cavity/channel requests, N log-uniform [1e3, {args.serve_nmax:g}], "
+                          f"Re U[100,2000], aspect U[1,4], Poisson {args.serve_rate:g}/s, mixed, resid 1e-6",
+              "rate_per_s": args.serve_rate, "budget_bytes": 40 << 30, "max_cases": 64,
+              "max_active": max((t[1] for t in srv.timeline), default=0),
+              "gpu_launches": x.launch_count() - l0})
+    return s
+
+
 def e2e_measure(x, A, case, mesh, args, world):
     """Same metric through the public API with host buffers: every step copies
     U and p host->device, runs one SIMPLE iteration and reads them back."""
@@ -324,6 +395,8 @@ def main():
                  "ratio_mixed_over_fp64": (r2["value"] / r["value"]) if sec == "mixed" else (r["value"] / r2["value"]),
                  "roofline": r2["roofline"], "residuals_last": r2["residuals_last"],
                  "phases_ms_total": r2["phases_ms_total"], "gpu_launches": r2["gpu_launches"]}
+    les = les_measure(x, A, args, local) if args.les_size > 0 else None
+    serving = serve_measure(x, args, local) if args.serve_cases > 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(x, pm, mesh, args.cpu_iters)
@@ -339,7 +412,8 @@ def main():
                            "mesh_build_s": round(t_mesh, 2), "setup_s": r["setup_s"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": r["gpu_launches"],
                 "clocks": r["clocks"], "residuals_last": r["residuals_last"],
-                "phases_ms_total": r["phases_ms_total"], "second_precision": other}
+                "phases_ms_total": r["phases_ms_total"], "second_precision": other, "les": les,
+                "serving": serving}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

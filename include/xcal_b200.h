@@ -368,7 +368,7 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable);
 /* graph mode (off by default): each xcal_simple_iterate iteration /
  * xcal_piso_step step replays one CUDA graph captured on first use.  The
  * Krylov loops run as conditional WHILE nodes whose stopping tests are taken
- * on the device (at most itmax/8 + 2 loop bodies), so a step needs one host
+ * on the device (at most itmax/4 + 2 loop bodies), so a step needs one host
  * synchronisation.  Results are identical to the default mode.  Per-kernel
  * profiling does not apply inside the graph. */
 int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable);

@@ -1055,7 +1055,7 @@ void Case::capture_while(F&& body) {
 }
 
 // solve_system! captured: per-solve setup, the Krylov loop as a WHILE node
-// (bodies of 8 iterations, at most itmax/8 + 2 bodies), the FP64 residual
+// (bodies of 4 CG / 1 BiCGSTAB iterations, at most itmax/BODY + 2 bodies), the FP64 residual
 // into gres and (iterations, status) into giters.  Mixed precision nests the
 // inner loop in a WHILE node over defect-correction steps.
 void Case::solve_captured(int eqn, int comp) {
@@ -1069,7 +1069,10 @@ void Case::solve_captured(int eqn, int comp) {
     const int slot = isU ? comp : 3;
     CSRView A = E.view();
     const int itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
-    const int BODY = 8;
+    // iterations per loop body: a finished solve wastes at most BODY-1
+    // early-exit iterations; a BiCGSTAB iteration is already tens of
+    // launches (two SpMVs, two preconditioner sweeps), a CG iteration two
+    const int BODY = SS.solver == XCAL_SOLVER_CG ? 4 : 1;
     const int cap = itmax / BODY + 2;
     const bool mixed = cfg.precision == XCAL_PREC_MIXED;
     const double inner_rtol = cfg.inner_rtol > 0 ? cfg.inner_rtol : 1e-3;
