@@ -397,6 +397,9 @@ int32_t xcal_batch_destroy(xcal_batch* b);
 int32_t xcal_batch_add(xcal_batch* b, xcal_case* cs, int64_t charge_bytes);
 int32_t xcal_batch_remove(xcal_batch* b, xcal_case* cs);
 int32_t xcal_batch_info(const xcal_batch* b, int32_t* n_cases, int64_t* used_bytes, int64_t* budget_bytes);
+/* host wall time (ms) spent by xcal_batch_simple_iterate so far:
+ * [face loops + corrections, U solves, p solve, total] */
+int32_t xcal_batch_timings(const xcal_batch* b, double* ms4);
 /* position of a case in the batch's order (the row of its results) */
 int32_t xcal_batch_case_index(const xcal_batch* b, const xcal_case* cs, int32_t* index);
 /* one SIMPLE iteration of every admitted case; res [n_cases*4] receives the

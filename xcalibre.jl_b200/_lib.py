@@ -70,6 +70,7 @@ SIGNATURES = {
     "xcal_batch_remove": (_i32, [_vp, _vp]),
     "xcal_batch_info": (_i32, [_vp, _pi, _pi64, _pi64]),
     "xcal_batch_case_index": (_i32, [_vp, _vp, _pi]),
+    "xcal_batch_timings": (_i32, [_vp, _pd]),
     "xcal_batch_simple_iterate": (_i32, [_vp, _pd, _pi]),
 }
 

@@ -672,6 +672,12 @@ class Batch:
         check(lib().xcal_batch_remove(self.h, case.h), self.ctx.h)
         self.cases.remove(case)
 
+    def timings(self) -> dict:
+        """Host wall time (ms) of the batch iterations so far, by phase."""
+        a = np.zeros(4)
+        check(lib().xcal_batch_timings(self.h, _abi.ptr(a, C.c_double)), self.ctx.h)
+        return {"face_loops": a[0], "U_solves": a[1], "p_solve": a[2], "total": a[3]}
+
     def info(self) -> tuple[int, int, int]:
         n, used, budget = C.c_int32(), C.c_int64(), C.c_int64()
         check(lib().xcal_batch_info(self.h, C.byref(n), C.byref(used), C.byref(budget)), self.ctx.h)

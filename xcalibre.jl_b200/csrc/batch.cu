@@ -11,6 +11,7 @@
 // and leave (xcal_batch_remove) between iterations; admission is bounded by a
 // device-memory budget.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 
 #include "batch.hpp"
@@ -38,10 +39,56 @@ struct Batch {
     DBuf<int2> tmap;                 // all cases
     DBuf<int2> tmap_act;             // subset (mixed-precision outer steps)
     DBuf<unsigned char> sys[2][4];   // [fp64, fp32][Ux, Uy, Uz, p] descriptor tables
-    DBuf<int2> dlo[2], dup[2];       // merged DILU levels per equation
+    DBuf<int2> dlo[2], dup[2];       // merged DILU levels per equation (large systems)
     std::vector<int> dlo_off[2], dup_off[2];
+    DBuf<int> small_ids;             // systems that run DILU as one block
+    int n_small = 0;
     std::vector<int2> h_tmap;
     long long iterations = 0;
+    double phase_ms[4] = {0, 0, 0, 0};  // host wall time: face loops, U solves, p solve, total
+    // steady-state Krylov chunks replayed as CUDA graphs, per [precision][slot];
+    // every pointer they use is fixed until the composition changes
+    struct ChunkGraph {
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0;
+    };
+    ChunkGraph chunk_graph[2][4];
+
+    void drop_graphs() {
+        for (auto& row : chunk_graph)
+            for (auto& g : row)
+                if (g.exec) {
+                    cudaGraphExecDestroy(g.exec);
+                    g.exec = nullptr;
+                }
+    }
+
+    template <class F>
+    void replay(ChunkGraph& g, F&& body) {
+        if (!g.exec) {
+            const long long t0 = t_launch_count;
+            cudaGraph_t graph = nullptr;
+            XCAL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                body();
+            } catch (...) {
+                cudaStreamEndCapture(stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            XCAL_CUDA(cudaStreamEndCapture(stream, &graph));
+            const long long captured = t_launch_count - t0;
+            g_launch_count.fetch_sub(captured, std::memory_order_relaxed);
+            t_launch_count = t0;
+            cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            XCAL_CUDA(e);
+            g.launches = captured;
+        }
+        XCAL_CUDA(cudaGraphLaunch(g.exec, stream));
+        g_launch_count.fetch_add(g.launches, std::memory_order_relaxed);
+        t_launch_count += g.launches;
+    }
 
     Batch(xcal_ctx* c, int capacity, size_t bytes) : ctx(c), cap(capacity), budget(bytes) {
         XCAL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -54,6 +101,7 @@ struct Batch {
     }
     ~Batch() {
         if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
         for (size_t i = 0; i < cases.size(); ++i) cases[i]->stream = own[i];
         if (hS) cudaFreeHost(hS);
         if (hres) cudaFreeHost(hres);
@@ -138,12 +186,19 @@ struct Batch {
                 for (int k = 0; k < KV_COUNT; ++k) B.vec[k] = v[k];
             }
             if (SS.solver == XCAL_SOLVER_CG && SS.precond == XCAL_PRECOND_NONE) B.vec[KV_Z] = B.vec[KV_R];
+            B.lo_rows = E.d_lower_rows.p;
+            B.lo_off = E.d_lower_off.p;
+            B.up_rows = E.d_upper_rows.p;
+            B.up_off = E.d_upper_off.p;
+            B.n_lo = E.lower_off.empty() ? 0 : (int)E.lower_off.size() - 1;
+            B.n_up = E.upper_off.empty() ? 0 : (int)E.upper_off.size() - 1;
         }
         sys[prec][slot].upload((const unsigned char*)h.data(), h.size() * sizeof(BSys<T>), stream);
     }
 
     void rebuild() {
         if (!dirty) return;
+        drop_graphs();
         const int nc = (int)cases.size();
         h_tmap.clear();
         for (int i = 0; i < nc; ++i) {
@@ -161,13 +216,21 @@ struct Batch {
                 else
                     fill_sys<double>(0, slot);
             }
-            // DILU levels merged across cases: level l holds every case's
-            // level-l rows
+            // small systems: one block per DILU application
+            std::vector<int> ids;
+            for (int i = 0; i < nc; ++i)
+                if (cases[i]->U.dilu_block()) ids.push_back(i);
+            n_small = (int)ids.size();
+            if (ids.empty()) ids.push_back(0);
+            small_ids.upload(ids, stream);
+            // DILU levels of the other systems merged across cases: level l
+            // holds every such case's level-l rows
             for (int e = 0; e < 2; ++e) {
                 for (int dir = 0; dir < 2; ++dir) {
                     size_t L = 0;
                     for (Case* c : cases) {
                         Equation& E = e == 0 ? c->U : c->P;
+                        if (E.dilu_block()) continue;
                         const std::vector<int>& off = dir == 0 ? E.lower_off : E.upper_off;
                         if (off.size() > 1) L = std::max(L, off.size() - 1);
                     }
@@ -176,6 +239,7 @@ struct Batch {
                     for (size_t l = 0; l < L; ++l) {
                         for (int i = 0; i < nc; ++i) {
                             Equation& E = e == 0 ? cases[i]->U : cases[i]->P;
+                            if (E.dilu_block()) continue;
                             const std::vector<int>& off = dir == 0 ? E.lower_off : E.upper_off;
                             const std::vector<int>& hr = dir == 0 ? E.h_lower_rows : E.h_upper_rows;
                             if (l + 1 >= off.size()) continue;
@@ -200,7 +264,7 @@ struct Batch {
         if (pt == XCAL_PRECOND_JACOBI)
             kb_jacobi_apply<T>(stream, sy, tm, nt, in, out, use_S);
         else if (pt == XCAL_PRECOND_DILU)
-            kb_dilu<T>(stream, sy, dlo[e].p, dlo_off[e], dup[e].p, dup_off[e], in, out, use_S);
+            kb_dilu<T>(stream, sy, small_ids.p, n_small, dlo[e].p, dlo_off[e], dup[e].p, dup_off[e], in, out, use_S);
         else
             kb_copy<T>(stream, sy, tm, nt, in, out, use_S);
     }
@@ -226,10 +290,40 @@ struct Batch {
         const int CHUNK = cg ? 32 : 8;
         int chunk = cg ? 4 : 1;
         long launched = 0;
+        // iterations run over every system of the batch: systems outside
+        // `members` are done and their blocks return at once, so a full chunk
+        // is the same launch sequence for every solve of this slot (a cached
+        // graph); the start kernels above used the members' tile map
+        tm = tmap.p;
+        nt = ntiles;
         for (;;) {
             if ((launched += chunk) > (long)itmax + 2 * CHUNK + 32)
                 fail(XCAL_ERR_TIMEOUT, "batch: a Krylov solve did not report completion within itmax iterations");
-            for (int c = 0; c < chunk; ++c) {
+            if (chunk == CHUNK) {
+                replay(chunk_graph[prec][slot], [&] {
+                    for (int c = 0; c < CHUNK; ++c) iterate<T>(prec, slot, SS, tm, nt);
+                });
+            } else {
+                for (int c = 0; c < chunk; ++c) iterate<T>(prec, slot, SS, tm, nt);
+            }
+            XCAL_CUDA(cudaMemcpyAsync(hS, S.p, cases.size() * sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
+            sync();
+            bool all = true;
+            for (int i : members) all = all && hS[i].done;
+            if (all) break;
+            if (chunk < CHUNK) chunk *= 2;
+        }
+    }
+
+    // one Krylov iteration of every system (early exit where done)
+    template <class T>
+    void iterate(int prec, int slot, const xcal_solver_setup& SS, const int2* tm, int nt) {
+        const int e = slot < 3 ? 0 : 1;
+        const BSys<T>* sy = (const BSys<T>*)sys[prec][slot].p;
+        const int pt = SS.precond;
+        const bool cg = SS.solver == XCAL_SOLVER_CG;
+        {
+            {
                 if (cg) {
                     kb_cg_spmv<T>(stream, sy, tm, nt);
                     if (pt == XCAL_PRECOND_JACOBI) {
@@ -251,12 +345,6 @@ struct Batch {
                     kb_bicg_p<T>(stream, sy, tm, nt);
                 }
             }
-            XCAL_CUDA(cudaMemcpyAsync(hS, S.p, cases.size() * sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
-            sync();
-            bool all = true;
-            for (int i : members) all = all && hS[i].done;
-            if (all) break;
-            if (chunk < CHUNK) chunk *= 2;
         }
     }
 
@@ -364,19 +452,30 @@ struct Batch {
     // one SIMPLE iteration of every case (Solvers_1_SIMPLE.jl:164-240)
     void simple_iteration(double* res_out, int* conv_out) {
         if (cases.empty()) return;
+        using clk = std::chrono::steady_clock;
+        auto ms = [](clk::time_point a, clk::time_point b) {
+            return std::chrono::duration<double, std::milli>(b - a).count();
+        };
+        const clk::time_point t0 = clk::now();
         rebuild();
         for (Case* c : cases) {
             if (!c->initialised) c->initial_calculations();
             c->iteration += 1;
             c->discretise(XCAL_EQN_U);
         }
+        double fv = 0, us = 0;
         for (int d = 0; d < 3; ++d) {
+            clk::time_point a = clk::now();
             for (Case* c : cases) {
                 c->bc_relax_U(d);
                 if (d == 0) c->update_precond(XCAL_EQN_U);
             }
+            clk::time_point b = clk::now();
             solve(d);
+            fv += ms(a, b);
+            us += ms(b, clk::now());
         }
+        const clk::time_point t1 = clk::now();
         for (Case* c : cases) {
             c->pressure_predictor(true);
             c->flux_divergence();
@@ -387,7 +486,9 @@ struct Batch {
             c->set_reference();
             c->update_precond(XCAL_EQN_P);
         }
+        const clk::time_point t2 = clk::now();
         solve(3);
+        const clk::time_point t3 = clk::now();
         for (Case* c : cases) {
             c->explicit_relaxation_p(c->cfg.p_solver.relax);
             c->grad_p();
@@ -396,7 +497,14 @@ struct Batch {
         }
         XCAL_CUDA(cudaMemcpyAsync(hres, res.p, 4 * cases.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
         sync();
+        const clk::time_point t4 = clk::now();
         ++iterations;
+        phase_ms[1] += us;
+        phase_ms[2] += ms(t2, t3);
+        phase_ms[3] += ms(t0, t4);
+        phase_ms[0] = phase_ms[3] - phase_ms[1] - phase_ms[2];
+        (void)fv;
+        (void)t1;
         for (size_t i = 0; i < cases.size(); ++i) {
             const Case* c = cases[i];
             const double* r = hres + 4 * i;
@@ -436,6 +544,8 @@ size_t estimate_case_bytes(long nC, long nF, long nB, int mixed, int dilu_U, int
     // [+ 9 floats]; tile partials and small buffers
     b += nC * (26.0 + 9.0) * 8.0 + nF * 8.0 * 8.0 + (mixed ? 36.0 * nC : 0.0);
     b += 3.0 * 8.0 * (nC / 2048 + 1) + 4096.0;
+    // permutations (mesh) and the field staging buffer (case)
+    b += 8.0 * nC + 8.0 * nF + 8.0 * std::max(nC, nF);
     return (size_t)b;
 }
 
@@ -513,6 +623,12 @@ int32_t xcal_batch_info(const xcal_batch* bt, int32_t* n_cases, int64_t* used_by
     if (n_cases) *n_cases = (int32_t)bt->b->cases.size();
     if (used_bytes) *used_bytes = (int64_t)bt->b->used;
     if (budget_bytes) *budget_bytes = (int64_t)bt->b->budget;
+    return XCAL_OK;
+}
+
+int32_t xcal_batch_timings(const xcal_batch* bt, double* ms4) {
+    if (!bt || !ms4) return XCAL_ERR_INVALID;
+    for (int k = 0; k < 4; ++k) ms4[k] = bt->b->phase_ms[k];
     return XCAL_OK;
 }
 

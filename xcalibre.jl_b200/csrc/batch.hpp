@@ -38,6 +38,12 @@ struct BSys {
     double* part1;
     int n;
     int ntiles;
+    // DILU level schedule (one-block sweeps of small systems)
+    const int* lo_rows;
+    const int* lo_off;
+    const int* up_rows;
+    const int* up_off;
+    int n_lo, n_up;
 };
 
 // batched launchers (kernels_batch.cu); tmap has ntiles_total entries
@@ -48,9 +54,12 @@ void kb_jacobi_apply(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int n
                      int use_S);
 template <class T>
 void kb_copy(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int in, int out, int use_S);
+// DILU application: systems listed in small_ids (n <= DILU_BLOCK_MAX_ROWS)
+// one block each, the others level by level over merged (system, row) lists
 template <class T>
-void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int2* lo_rows, const std::vector<int>& lo_off,
-             const int2* up_rows, const std::vector<int>& up_off, int in, int out, int use_S);
+void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int* small_ids, int n_small, const int2* lo_rows,
+             const std::vector<int>& lo_off, const int2* up_rows, const std::vector<int>& up_off, int in, int out,
+             int use_S);
 template <class T>
 void kb_cg_start(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
 template <class T>

@@ -5,6 +5,7 @@
 #include <new>
 
 #include "case.hpp"
+#include "kernels.hpp"
 
 namespace xcal {
 DevMesh* upload_mesh(const xcal_mesh_desc* d, cudaStream_t s);
@@ -164,24 +165,27 @@ static int field_io(xcal_case* cs, int32_t field, double* host, int64_t count, b
         long per = 0;
         c->field_comp(field, 0, per);
         if (count != (int64_t)ncomp * per) fail(XCAL_ERR_INVALID, "field size mismatch");
-        c->sync();
-        // device arrays are in storage order; the ABI uses the original order
+        // device arrays are in storage order, the ABI uses the original order:
+        // each component is staged in original order and permuted on the
+        // device (set: field[st] = io[perm[st]]; get: io[i] = field[inv[i]])
         bool face = field == XCAL_FIELD_MDOTF || field == XCAL_FIELD_NUEFF || field == XCAL_FIELD_NUTF ||
                     field == XCAL_FIELD_UF || field == XCAL_FIELD_PF || field == XCAL_FIELD_RDF;
-        const std::vector<int>& perm = face ? c->mesh->fperm : c->mesh->perm;
-        std::vector<double> tmp(per);
+        const DevMesh& m = *c->mesh;
+        const int* to_storage = face ? m.d_fperm.p : m.d_perm.p;
+        const int* to_original = face ? m.d_finv.p : m.d_inv.p;
         for (int d = 0; d < ncomp; ++d) {
             long n = 0;
             double* p = c->field_comp(field, d, n);
             double* h = host + (size_t)d * per;
             if (set) {
-                for (long st = 0; st < per; ++st) tmp[st] = h[perm[st]];
-                XCAL_CUDA(cudaMemcpy(p, tmp.data(), per * sizeof(double), cudaMemcpyHostToDevice));
+                XCAL_CUDA(cudaMemcpyAsync(c->io.p, h, per * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+                launch_gather(c->stream, per, c->io.p, to_storage, p);
             } else {
-                XCAL_CUDA(cudaMemcpy(tmp.data(), p, per * sizeof(double), cudaMemcpyDeviceToHost));
-                for (long st = 0; st < per; ++st) h[perm[st]] = tmp[st];
+                launch_gather(c->stream, per, p, to_original, c->io.p);
+                XCAL_CUDA(cudaMemcpyAsync(h, c->io.p, per * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
             }
         }
+        c->sync();
     })
 }
 

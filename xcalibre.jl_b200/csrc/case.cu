@@ -328,6 +328,10 @@ static DevMesh* upload_mesh_ordered(const xcal_mesh_desc* d, cudaStream_t s, std
     m->d_nz.upload(m->nzh, s);
     m->d_Ef.upload(Ef, s);
     m->d_vol.upload(m->vol, s);
+    m->d_perm.upload(m->perm, s);
+    m->d_inv.upload(m->inv, s);
+    m->d_fperm.upload(m->fperm, s);
+    m->d_finv.upload(m->finv, s);
     XCAL_CUDA(cudaStreamSynchronize(s));
     return m.release();
 }
@@ -438,6 +442,7 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
         }
         E.d_lower_rows.upload(rows, s);
         E.h_lower_rows = rows;
+        E.d_lower_off.upload(E.lower_off, s);
         std::fill(lvl.begin(), lvl.end(), 0);
         maxl = 0;
         for (int io = n - 1; io >= 0; --io) {
@@ -457,6 +462,7 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
         }
         E.d_upper_rows.upload(rows, s);
         E.h_upper_rows = rows;
+        E.d_upper_off.upload(E.upper_off, s);
     }
 }
 
@@ -638,6 +644,7 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     ws.S.zero(stream);
     resbuf.alloc(8);
     resbuf.zero(stream);
+    io.alloc(std::max(nC, nF));
     cmax.alloc(T);
     cmax_ctr.alloc(1);
     cmax_ctr.zero(stream);
@@ -825,6 +832,11 @@ void Case::update_precond(int eqn) {
     if (pt == XCAL_PRECOND_JACOBI) {
         kr_jacobi_update(stream, E.view(), E.nz.p, E.P.p);
     } else if (pt == XCAL_PRECOND_DILU) {
+        if (E.dilu_block()) {
+            kr_dilu_D_block(stream, E.d_lower_rows.p, E.d_lower_off.p, (int)E.lower_off.size() - 1, E.view(), E.nz.p,
+                            E.P.p);
+            return;
+        }
         for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
             kr_dilu_D(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], E.view(),
                       E.nz.p, E.P.p);
@@ -834,6 +846,11 @@ void Case::update_precond(int eqn) {
 template <class T>
 void Case::dilu_ldiv(Equation& E, const T* nz, const T* D, const T* b, T* out, const KScalars* S) {
     CSRView A = E.view();
+    if (E.dilu_block()) {
+        kr_dilu_block(stream, A, nz, D, b, out, E.d_lower_rows.p, E.d_lower_off.p, (int)E.lower_off.size() - 1,
+                      E.d_upper_rows.p, E.d_upper_off.p, (int)E.upper_off.size() - 1, S);
+        return;
+    }
     for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
         kr_dilu_fwd(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], A, nz, D, b, out,
                     S);

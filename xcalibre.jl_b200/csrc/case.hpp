@@ -25,6 +25,7 @@ struct DevMesh {
     DBuf<int> d_owner, d_neigh, d_cf_off, d_cf_face, d_cf_nb, d_bf_off, d_bf_face, d_bcell, d_bcells;
     DBuf<signed char> d_cf_sign;
     DBuf<double> d_area, d_delta, d_weight, d_Sx, d_Sy, d_Sz, d_nx, d_ny, d_nz, d_Ef, d_vol;
+    DBuf<int> d_perm, d_inv, d_fperm, d_finv;  // storage <-> original order (field transfer)
     size_t bytes = 0;  // device bytes held
     MeshView view() const;
 };
@@ -45,6 +46,8 @@ struct Equation {
     DBuf<int> d_lower_rows, d_upper_rows;
     std::vector<int> lower_off, upper_off;
     std::vector<int> h_lower_rows, h_upper_rows;  // host copies (batched level lists)
+    DBuf<int> d_lower_off, d_upper_off;           // level offsets (one-block sweeps)
+    bool dilu_block() const { return n <= DILU_BLOCK_MAX_ROWS; }
     bool has_periodic = false;
     CSRView view() const;
     int find(int i, int j) const;  // slot or -1
@@ -86,7 +89,7 @@ struct Case {
     KrylovWS ws;
     // fields
     DBuf<double> Uc[3], p, mdot, nueff, gradp[3], gradU[9], rD, Hv[3], divHv, nut, nutf, Uf[3], pf, rDf, Delta, prev,
-        courant, dx13, resbuf, cmax;
+        courant, dx13, resbuf, cmax, io;  // io: staging of one field component in the original order
     bool initialised = false;
     int iteration = 0;
     double time = 0.0;

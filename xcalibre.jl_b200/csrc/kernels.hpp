@@ -40,6 +40,7 @@ void launch_correct_mdot(cudaStream_t s, const MeshView& m, const CSRView& A, co
 void launch_correct_U(cudaStream_t s, int n, double* const H[3], const double* const g[3], const double* rD,
                       double* const U[3]);
 void launch_relax_explicit(cudaStream_t s, int n, double* phi, const double* phi0, double alpha);
+void launch_gather(cudaStream_t s, long n, const double* src, const int* idx, double* dst);
 void launch_courant_max(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* part,
                         unsigned int* counter, double* out);
 
@@ -91,6 +92,12 @@ void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, c
 template <class T>
 void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const T* nz, const T* D, T* x,
                  const KScalars* S);
+// small systems (n <= DILU_BLOCK_MAX_ROWS): whole sweeps in one block
+void kr_dilu_D_block(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
+                     double* D);
+template <class T>
+void kr_dilu_block(cudaStream_t s, const CSRView& A, const T* nz, const T* D, const T* b, T* y, const int* lo_rows,
+                   const int* lo_off, int n_lo, const int* up_rows, const int* up_off, int n_up, const KScalars* S);
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
                  double* part0, double* part1, double* out);
 // device-driven solve control of graph mode (conditional WHILE nodes)

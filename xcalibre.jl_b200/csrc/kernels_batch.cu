@@ -57,6 +57,17 @@ __global__ void kbk_dilu_bwd(const BSys<T>* __restrict__ sys, const int2* __rest
     dilu_bwd_row<T>(B.A, B.nz, B.P, B.vec[out], r.y);
 }
 
+// one block per small system: a whole DILU application
+template <class T>
+__global__ void __launch_bounds__(DILU_BLOCK_THREADS) kbk_dilu_block(const BSys<T>* __restrict__ sys,
+                                                                     const int* __restrict__ ids, int in, int out,
+                                                                     int use_S) {
+    const BSys<T>& B = sys[ids[blockIdx.x]];
+    if (use_S && B.S->done) return;
+    dilu_block_sweep<T>(B.A, B.nz, B.P, B.vec[in], B.vec[out], B.lo_rows, B.lo_off, B.n_lo, B.up_rows, B.up_off,
+                        B.n_up);
+}
+
 template <class T>
 __global__ void kbk_cg_start(const BSys<T>* __restrict__ sys, const int2* tmap) {
     XCAL_BSYS
@@ -70,7 +81,7 @@ __global__ void __launch_bounds__(RED_THREADS, 8) kbk_cg_spmv(const BSys<T>* __r
 }
 
 template <class T>
-__global__ void kbk_cg_update(const BSys<T>* __restrict__ sys, const int2* tmap, int jacobi_fused) {
+__global__ void __launch_bounds__(RED_THREADS, sizeof(T) == 4 ? 4 : 8) kbk_cg_update(const BSys<T>* __restrict__ sys, const int2* tmap, int jacobi_fused) {
     XCAL_BSYS
     cg_update_body<T>(tc, B.n, B.vec[KV_X], B.vec[KV_P], B.vec[KV_V], B.vec[KV_R], B.vec[KV_Q], B.vec[KV_Z], B.P,
                       jacobi_fused, B.S, B.part0);
@@ -143,8 +154,13 @@ void kb_copy(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_to
     XCAL_BLAUNCH(kbk_copy, sys, tmap, in, out, use_S);
 }
 template <class T>
-void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int2* lo_rows, const std::vector<int>& lo_off,
-             const int2* up_rows, const std::vector<int>& up_off, int in, int out, int use_S) {
+void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int* small_ids, int n_small, const int2* lo_rows,
+             const std::vector<int>& lo_off, const int2* up_rows, const std::vector<int>& up_off, int in, int out,
+             int use_S) {
+    if (n_small > 0) {
+        kbk_dilu_block<T><<<n_small, DILU_BLOCK_THREADS, 0, s>>>(sys, small_ids, in, out, use_S);
+        XCAL_CHECK_LAUNCH();
+    }
     for (size_t l = 0; l + 1 < lo_off.size(); ++l) {
         int nr = lo_off[l + 1] - lo_off[l];
         if (nr <= 0) continue;
@@ -203,8 +219,8 @@ void kb_bicg_p(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_
     template void kb_spmv<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, int);                            \
     template void kb_jacobi_apply<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, int, int);               \
     template void kb_copy<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, int, int);                       \
-    template void kb_dilu<T>(cudaStream_t, const BSys<T>*, const int2*, const std::vector<int>&, const int2*,     \
-                             const std::vector<int>&, int, int, int);                                             \
+    template void kb_dilu<T>(cudaStream_t, const BSys<T>*, const int*, int, const int2*, const std::vector<int>&, \
+                             const int2*, const std::vector<int>&, int, int, int);                                \
     template void kb_cg_start<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                  \
     template void kb_cg_spmv<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                   \
     template void kb_cg_update<T>(cudaStream_t, const BSys<T>*, const int2*, int, int);                            \

@@ -891,6 +891,17 @@ void launch_relax_explicit(cudaStream_t s, int n, double* phi, const double* phi
     k_relax_explicit<<<nblk(n), TPB, 0, s>>>(n, phi, phi0, alpha);
     XCAL_CHECK_LAUNCH();
 }
+// dst[i] = src[idx[i]]: the storage <-> original permutation of a field
+__global__ void k_gather(long n, const double* __restrict__ src, const int* __restrict__ idx, double* dst) {
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[idx[i]];
+}
+void launch_gather(cudaStream_t s, long n, const double* src, const int* idx, double* dst) {
+    if (n <= 0) return;
+    k_gather<<<nblk(n), TPB, 0, s>>>(n, src, idx, dst);
+    XCAL_CHECK_LAUNCH();
+}
+
 void launch_courant_max(cudaStream_t s, int n, const double* const U[3], const double* dx, double dt, double* part,
                         unsigned int* counter, double* out) {
     k_courant_max<<<(n + RED_TILE - 1) / RED_TILE, RED_THREADS, 0, s>>>(n, U[0], U[1], U[2], dx, dt, part, counter,

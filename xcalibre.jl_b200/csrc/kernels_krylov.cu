@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_cg_spmv(CSRView A, const T* 
 
 // x += alpha p_k; r -= alpha q; [Jacobi: z = P r; <r,z>; finalize]
 template <class T>
-__global__ void k_cg_update(int n, T* x, const T* __restrict__ P0, const T* __restrict__ P1, T* r,
+__global__ void __launch_bounds__(RED_THREADS, sizeof(T) == 4 ? 4 : 8) k_cg_update(int n, T* x, const T* __restrict__ P0, const T* __restrict__ P1, T* r,
                             const T* __restrict__ q, T* z, const T* __restrict__ P, int jacobi_fused, KScalars* S,
                             double* part) {
     cg_update_body<T>(grid_tiles(), n, x, P0, P1, r, q, z, P, jacobi_fused, S, part);
@@ -182,14 +182,31 @@ __global__ void k_dilu_D(const int* __restrict__ rows, int nrows, CSRView A, con
                          double* D) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nrows) return;
-    int i = rows[t];
-    int ds = A.diag[i];
-    double d = nz[ds];
-    for (int e = row_base(A, i); e < ds; e += SELL_C) {
-        int j = A.colval[e];
-        d = d - (nz[A.trans[e]] * nz[e]) / D[j];
+    dilu_D_row(A, nz, D, rows[t]);
+}
+
+// the D factor of a small system in one block, level by level
+__global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_D_block(const int* __restrict__ rows,
+                                                                     const int* __restrict__ off, int nlev,
+                                                                     CSRView A, const double* __restrict__ nz,
+                                                                     double* D) {
+    for (int l = 0; l < nlev; ++l) {
+        for (int k = off[l] + threadIdx.x; k < off[l + 1]; k += blockDim.x) dilu_D_row(A, nz, D, rows[k]);
+        __syncthreads();
     }
-    D[i] = d;
+}
+
+// a whole DILU application (forward + backward sweeps) of a small system in one block
+template <class T>
+__global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_block(CSRView A, const T* __restrict__ nz,
+                                                                   const T* __restrict__ D, const T* __restrict__ b,
+                                                                   T* y, const int* __restrict__ lo_rows,
+                                                                   const int* __restrict__ lo_off, int n_lo,
+                                                                   const int* __restrict__ up_rows,
+                                                                   const int* __restrict__ up_off, int n_up,
+                                                                   const KScalars* S) {
+    if (S && S->done) return;
+    dilu_block_sweep<T>(A, nz, D, b, y, lo_rows, lo_off, n_lo, up_rows, up_off, n_up);
 }
 
 // forward_substitution! (preconditioners_1_DILU.jl:84-98), one level
@@ -448,6 +465,18 @@ void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, c
     k_dilu_bwd<T><<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, A, nz, D, x, S);
     XCAL_CHECK_LAUNCH();
 }
+void kr_dilu_D_block(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
+                     double* D) {
+    if (nlev <= 0) return;
+    k_dilu_D_block<<<1, DILU_BLOCK_THREADS, 0, s>>>(rows, off, nlev, A, nz, D);
+    XCAL_CHECK_LAUNCH();
+}
+template <class T>
+void kr_dilu_block(cudaStream_t s, const CSRView& A, const T* nz, const T* D, const T* b, T* y, const int* lo_rows,
+                   const int* lo_off, int n_lo, const int* up_rows, const int* up_off, int n_up, const KScalars* S) {
+    k_dilu_block<T><<<1, DILU_BLOCK_THREADS, 0, s>>>(A, nz, D, b, y, lo_rows, lo_off, n_lo, up_rows, up_off, n_up, S);
+    XCAL_CHECK_LAUNCH();
+}
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
                  double* part0, double* part1, double* out) {
     k_residual<<<TILE_LAUNCH(A.n), s>>>(A, nz, x, b, S, part0, part1, out);
@@ -506,7 +535,9 @@ void kr_record(cudaStream_t s, const KScalars* S, int* out) {
     template void kr_dilu_fwd<T>(cudaStream_t, const int*, int, const CSRView&, const T*, const T*, const T*, T*, \
                                  const KScalars*);                                                              \
     template void kr_dilu_bwd<T>(cudaStream_t, const int*, int, const CSRView&, const T*, const T*, T*,          \
-                                 const KScalars*);
+                                 const KScalars*);                                                              \
+    template void kr_dilu_block<T>(cudaStream_t, const CSRView&, const T*, const T*, const T*, T*, const int*,   \
+                                   const int*, int, const int*, const int*, int, const KScalars*);
 XCAL_KRYLOV_INSTANTIATE(double)
 XCAL_KRYLOV_INSTANTIATE(float)
 

@@ -199,6 +199,44 @@ __device__ __forceinline__ void cg_update_body(const TileCtx& tc, int n, T* x, c
     const T* p = (S->iter & 1) ? P1 : P0;
     const T alpha = (T)S->alpha;
     double acc = 0.0;
+    if constexpr (sizeof(T) == 4) {
+        // FP32: 4-byte elements leave too few bytes in flight per thread when
+        // each row waits for its loads; issue all rows' loads first (same
+        // arithmetic, same order of the sums).  Measured 18.4 -> 14.4 us on
+        // 2M rows.
+        if (jacobi_fused) {
+            T xv[RED_ITEMS], pv[RED_ITEMS], rv[RED_ITEMS], qv[RED_ITEMS], Pv[RED_ITEMS];
+#pragma unroll
+            for (int k = 0; k < RED_ITEMS; ++k) {
+                int i = tile_row(tc, k);
+                if (i < n) {
+                    xv[k] = ld_stream(x + i);
+                    pv[k] = p[i];
+                    rv[k] = r[i];
+                    qv[k] = ld_stream(q + i);
+                    Pv[k] = ld_stream(P + i);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < RED_ITEMS; ++k) {
+                int i = tile_row(tc, k);
+                if (i < n) {
+                    __stcs(x + i, xv[k] + alpha * pv[k]);
+                    T ri = rv[k] + (-alpha) * qv[k];
+                    r[i] = ri;
+                    T zi = Pv[k] * ri;
+                    z[i] = zi;
+                    acc = acc + (double)ri * (double)zi;
+                }
+            }
+            double tot = block_tree(acc, sm);
+            if (threadIdx.x == 0) part[tc.tile] = tot;
+            if (!last_block(&S->counter, tc.ntiles)) return;
+            double g = reduce_partials(part, tc.ntiles, sm);
+            if (threadIdx.x == 0) cg_finalize(S, g);
+            return;
+        }
+    }
     for (int k = 0; k < RED_ITEMS; ++k) {
         int i = tile_row(tc, k);
         if (i < n) {
@@ -436,6 +474,41 @@ __device__ __forceinline__ void dilu_bwd_row(const CSRView& A, const T* __restri
     int e1 = row_base(A, i) + SELL_C * A.len[i];
     for (int e = ds + SELL_C; e < e1; e += SELL_C) sum = sum + ld_stream(nz + e) * x[ld_stream(A.colval + e)];
     x[i] = (x[i] - sum) / D[i];
+}
+
+// A DILU application of a small system (n <= DILU_BLOCK_MAX_ROWS) as one
+// block: every level of the forward sweep, then of the backward sweep, with a
+// block barrier between levels (rows of a level are independent).  The
+// per-row arithmetic is the level kernels'.
+constexpr int DILU_BLOCK_THREADS = 1024;
+
+template <class T>
+__device__ __forceinline__ void dilu_block_sweep(const CSRView& A, const T* __restrict__ nz, const T* __restrict__ D,
+                                                 const T* __restrict__ in, T* out, const int* __restrict__ lo_rows,
+                                                 const int* __restrict__ lo_off, int n_lo,
+                                                 const int* __restrict__ up_rows, const int* __restrict__ up_off,
+                                                 int n_up) {
+    for (int l = 0; l < n_lo; ++l) {
+        for (int k = lo_off[l] + threadIdx.x; k < lo_off[l + 1]; k += blockDim.x)
+            dilu_fwd_row(A, nz, D, in, out, lo_rows[k]);
+        __syncthreads();
+    }
+    for (int l = 0; l < n_up; ++l) {
+        for (int k = up_off[l] + threadIdx.x; k < up_off[l + 1]; k += blockDim.x)
+            dilu_bwd_row(A, nz, D, out, up_rows[k]);
+        __syncthreads();
+    }
+}
+
+// update_dilu_diagonal! row i (preconditioners_1_DILU.jl:43-82)
+__device__ __forceinline__ void dilu_D_row(const CSRView& A, const double* __restrict__ nz, double* D, int i) {
+    int ds = A.diag[i];
+    double d = nz[ds];
+    for (int e = row_base(A, i); e < ds; e += SELL_C) {
+        int j = A.colval[e];
+        d = d - (nz[A.trans[e]] * nz[e]) / D[j];
+    }
+    D[i] = d;
 }
 
 }  // namespace xcal

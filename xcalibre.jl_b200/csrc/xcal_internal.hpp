@@ -128,6 +128,9 @@ struct MeshView {
 // reference's CSR order (ascending original column); padding entries (up to
 // the slice's longest row) are never read.
 constexpr int SELL_C = 32;
+// systems up to this many rows apply DILU (and build its factor) in one
+// block, level after level, instead of one launch per level
+constexpr int DILU_BLOCK_MAX_ROWS = 65536;
 struct CSRView {
     int n;
     const int* slice;          // [ceil(n/32)+1] first slot of each slice

@@ -138,6 +138,7 @@ class Server:
     convergence: float = 1e-6
     keep_fields: bool = False
     timeline: list = field(default_factory=list)  # (t, active, queued, used bytes)
+    phase_ms: dict = field(default_factory=dict)  # batch phase times (host wall, ms)
 
     def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
@@ -180,6 +181,7 @@ class Server:
                         time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0))))
                     continue
                 res, conv = batch.simple_iterate()
+                self.phase_ms = batch.timings()
                 done_t = time.perf_counter() - t0
                 finished = []
                 for k, a in enumerate(active):
