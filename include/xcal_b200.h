@@ -372,6 +372,10 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable);
  * synchronisation.  Results are identical to the default mode.  Per-kernel
  * profiling does not apply inside the graph. */
 int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable);
+/* launch-shape autotuner (runs on first use, or now): out6 = for U then p,
+ * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU as
+ * one-block sweeps [0/1]).  The choices never change a result. */
+int32_t xcal_case_tuning(xcal_case* cs, int32_t* out6);
 int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches);
 
 /* ---- batching / serving --------------------------------------------------

@@ -75,3 +75,24 @@ def test_graph_launch_count_reported(x, ctx):
     c.simple_iterate(2)
     n = x.launch_count() - l0
     assert n > 50, n
+
+
+def test_autotuner_choices(x, ctx):
+    """The autotuner picks a valid launch shape per equation; parity with the
+    oracle under those shapes is covered by the SIMPLE parity tests (they run
+    through simple_iterate, which tunes first)."""
+    mesh = x.build_mesh3(x.channel_polymesh(24, 12, 12, seed=5))
+    model, config = x.cases.channel_case(mesh, iterations=2)
+    cfg, keep = x.build_config(model, config)
+    dm = x.DeviceMesh(ctx, mesh)
+    c = x.Case(dm, cfg)
+    t = c.tuning()
+    assert t["U"]["spmv_rows_per_thread"] in (0, 1, 2, 4)
+    assert t["U"]["spmv_block"] in (128, 256, 512)
+    assert isinstance(t["U"]["dilu_one_block"], bool)
+    c.set_field(x._abi.FIELD_U, model.momentum.U)
+    c.set_field(x._abi.FIELD_P, model.momentum.p)
+    r1, _ = c.simple_iterate(2)
+    # a second case of the same size class reuses the cached choices
+    c2 = x.Case(x.DeviceMesh(ctx, mesh), cfg)
+    assert c2.tuning() == t

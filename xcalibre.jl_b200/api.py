@@ -603,6 +603,15 @@ class Case:
     def set_profiling(self, on: bool = True):
         self._chk(lib().xcal_case_set_profiling(self.h, 1 if on else 0))
 
+    def tuning(self) -> dict:
+        """Launch shapes chosen by the autotuner (tuning runs now if it has
+        not yet): per equation the BiCGSTAB SpMV rows per thread (0 = tile
+        kernel) and block size, and whether DILU runs as one-block sweeps."""
+        a = np.zeros(6, dtype=np.int32)
+        self._chk(lib().xcal_case_tuning(self.h, _abi.ptr(a, C.c_int32)))
+        return {eq: {"spmv_rows_per_thread": int(a[3 * k]), "spmv_block": int(a[3 * k + 1]),
+                     "dilu_one_block": bool(a[3 * k + 2])} for k, eq in enumerate(("U", "p"))}
+
     def set_graph_mode(self, on: bool = True):
         """Replay each SIMPLE iteration / PISO step as one captured CUDA graph
         (device-driven Krylov loops; same results as the default mode)."""

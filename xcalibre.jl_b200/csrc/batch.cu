@@ -131,6 +131,7 @@ struct Batch {
         if (used + charge > budget) fail(XCAL_ERR_BUSY, "batch: device-memory budget exceeded");
         if (index_of(c) >= 0) fail(XCAL_ERR_INVALID, "batch: case already admitted");
         check_compatible(c);
+        c->autotune();
         c->sync();
         if (c->graph_mode) c->set_graph_mode(false);
         own.push_back(c->stream);

@@ -329,6 +329,20 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable) {
     return XCAL_OK;
 }
 
+int32_t xcal_case_tuning(xcal_case* cs, int32_t* out6) {
+    if (!cs || !out6) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    XCAL_GUARD(c->ctx, {
+        c->autotune();
+        const Equation* E[2] = {&c->U, &c->P};
+        for (int e = 0; e < 2; ++e) {
+            out6[3 * e] = E[e]->spmv_shape.rows_per_thread;
+            out6[3 * e + 1] = E[e]->spmv_shape.block;
+            out6[3 * e + 2] = E[e]->use_block ? 1 : 0;
+        }
+    })
+}
+
 int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable) {
     if (!cs) return XCAL_ERR_INVALID;
     Case* c = cs->c.get();

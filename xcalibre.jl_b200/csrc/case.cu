@@ -342,6 +342,7 @@ static DevMesh* upload_mesh_ordered(const xcal_mesh_desc* d, cudaStream_t s, std
 static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal_bc>& bcs, int nvec,
                            bool need_dilu, cudaStream_t s) {
     int n = E.n = m.nC;
+    E.use_block = n <= DILU_BLOCK_MAX_ROWS;
     std::vector<std::vector<int>> extra(n);
     for (const xcal_bc& bc : bcs) {
         if (bc.type != XCAL_BC_PERIODIC_PARENT) continue;
@@ -919,14 +920,14 @@ void Case::krylov_step(Equation& E, const xcal_solver_setup& SS, const T* nz, co
         if (ev) rec(ev[2]);
     } else {
         if (ev) rec(ev[0]);
-        kr_spmv(stream, A, nz, (const T*)pp, q, (const KScalars*)S);
+        kr_spmv_shaped(stream, E.spmv_shape, A, nz, (const T*)pp, q, (const KScalars*)S);
         if (ev) rec(ev[1]);
         apply_M(E, pt, nz, P, (const T*)q, v, (const KScalars*)S);
         if (ev) rec(ev[2]);
         kr_bicg_alpha(stream, n, c, (const T*)v, S, ws.part0.p);
         kr_bicg_s(stream, n, (const T*)r, (const T*)v, (const T*)pp, s, x, (const KScalars*)S);
         if (ev) rec(ev[3]);
-        kr_spmv(stream, A, nz, (const T*)s, q, (const KScalars*)S);
+        kr_spmv_shaped(stream, E.spmv_shape, A, nz, (const T*)s, q, (const KScalars*)S);
         if (ev) rec(ev[4]);
         apply_M(E, pt, nz, P, (const T*)q, t, (const KScalars*)S);
         if (ev) rec(ev[5]);
@@ -1348,6 +1349,7 @@ void Case::piso_body(double r3[3], double& rp) {
 // captured once and replayed for every later step.
 void Case::capture_step() {
     if (step_graph) return;
+    autotune();
     sync();
     const long long t0 = t_launch_count;
     body_kernels_captured = 0;
@@ -1406,6 +1408,7 @@ void Case::run_step_graph(double res[4], double* courant) {
 
 bool Case::simple_iteration(double res[4]) {  // Solvers_1_SIMPLE.jl:164-240
     if (!initialised) initial_calculations();
+    autotune();
     iteration += 1;
     double r3[3], rp;
     if (graph_mode) {
@@ -1441,6 +1444,7 @@ bool Case::simple_iteration(double res[4]) {  // Solvers_1_SIMPLE.jl:164-240
 
 double Case::piso_step(double res[4]) {  // Solvers_2_PISO.jl:108-187
     if (!initialised) initial_calculations();
+    autotune();
     iteration += 1;
     time = time + cfg.dt;
     double r3[3], rp, co;
@@ -1478,5 +1482,9 @@ void Case::set_graph_mode(bool on) {
     }
     graph_mode = on;
 }
+
+template void Case::dilu_ldiv<double>(Equation&, const double*, const double*, const double*, double*,
+                                      const KScalars*);
+template void Case::dilu_ldiv<float>(Equation&, const float*, const float*, const float*, float*, const KScalars*);
 
 }  // namespace xcal

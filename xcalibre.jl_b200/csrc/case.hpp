@@ -2,6 +2,7 @@
 #pragma once
 #include <memory>
 
+#include "kernels.hpp"
 #include "xcal_internal.hpp"
 
 struct xcal_ctx {
@@ -47,7 +48,10 @@ struct Equation {
     std::vector<int> lower_off, upper_off;
     std::vector<int> h_lower_rows, h_upper_rows;  // host copies (batched level lists)
     DBuf<int> d_lower_off, d_upper_off;           // level offsets (one-block sweeps)
-    bool dilu_block() const { return n <= DILU_BLOCK_MAX_ROWS; }
+    // launch choices (autotune.cu); neither changes any result
+    bool use_block = false;   // DILU as one-block sweeps (default: n <= DILU_BLOCK_MAX_ROWS)
+    SpmvShape spmv_shape;     // BiCGSTAB SpMV row mapping / block size
+    bool dilu_block() const { return use_block; }
     bool has_periodic = false;
     CSRView view() const;
     int find(int i, int j) const;  // slot or -1
@@ -160,6 +164,8 @@ struct Case {
     void solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, const double* b, KScalars* S,
                      KScalars* hS, int gk, int* iters);
     int last_outer[4] = {0, 0, 0, 0};  // mixed: defect-correction steps of the last solve per system
+    bool tuned = false;
+    void autotune();  // launch-shape autotuner (autotune.cu), once per case
 
     // ---- graph mode: one SIMPLE iteration / PISO step captured as a CUDA
     // graph; the Krylov (and defect-correction) loops are conditional WHILE

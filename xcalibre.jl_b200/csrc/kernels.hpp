@@ -55,6 +55,15 @@ void kr_correct(cudaStream_t s, int n, double* field, const float* x);
 void kr_to_float(cudaStream_t s, long n, const double* src, float* dst);
 template <class T>
 void kr_spmv(cudaStream_t s, const CSRView& A, const T* nz, const T* x, T* y, const KScalars* S);
+// launch shape of an SpMV without a reduction: rows_per_thread 0 = the
+// canonical tile kernel (kr_spmv), else 1/2/4 rows per thread, `block` threads
+struct SpmvShape {
+    int rows_per_thread = 0;
+    int block = 256;
+};
+template <class T>
+void kr_spmv_shaped(cudaStream_t s, const SpmvShape& sh, const CSRView& A, const T* nz, const T* x, T* y,
+                    const KScalars* S);
 template <class T>
 void kr_jacobi_apply(cudaStream_t s, int n, const T* P, const T* r, T* z, const KScalars* S);
 template <class T>

@@ -74,6 +74,22 @@ __global__ void __launch_bounds__(RED_THREADS, 8) k_spmv(CSRView A, const T* __r
     spmv_body<T>(grid_tiles(), A, nz, x, y, S);
 }
 
+// y = A*x with a free row mapping (no reduction rides on this SpMV): thread g
+// of the grid computes rows g, g + G, ..., R of them (G = threads in the
+// grid).  The row sums are row_dot's, so every shape gives the same y; the
+// shape (R, block size) is chosen by the autotuner.
+template <class T, int R>
+__global__ void k_spmv_rows(CSRView A, const T* __restrict__ nz, const T* __restrict__ x, T* y, const KScalars* S) {
+    if (S && S->done) return;
+    const int G = gridDim.x * blockDim.x;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        int i = g + k * G;
+        if (i < A.n) y[i] = row_dot(A, nz, x, i);
+    }
+}
+
 // z = P .* r (Jacobi: opDiagonal multiply, ldiv = false)
 template <class T>
 __global__ void k_jacobi_apply(int n, const T* __restrict__ P, const T* __restrict__ r, T* z, const KScalars* S) {
@@ -375,6 +391,23 @@ void kr_spmv(cudaStream_t s, const CSRView& A, const T* nz, const T* x, T* y, co
     XCAL_CHECK_LAUNCH();
 }
 template <class T>
+void kr_spmv_shaped(cudaStream_t s, const SpmvShape& sh, const CSRView& A, const T* nz, const T* x, T* y,
+                    const KScalars* S) {
+    if (sh.rows_per_thread <= 0) {
+        kr_spmv(s, A, nz, x, y, S);
+        return;
+    }
+    const long per_block = (long)sh.block * sh.rows_per_thread;
+    const int grid = (int)((A.n + per_block - 1) / per_block);
+    if (grid <= 0) return;
+    switch (sh.rows_per_thread) {
+        case 1: k_spmv_rows<T, 1><<<grid, sh.block, 0, s>>>(A, nz, x, y, S); break;
+        case 2: k_spmv_rows<T, 2><<<grid, sh.block, 0, s>>>(A, nz, x, y, S); break;
+        default: k_spmv_rows<T, 4><<<grid, sh.block, 0, s>>>(A, nz, x, y, S); break;
+    }
+    XCAL_CHECK_LAUNCH();
+}
+template <class T>
 void kr_jacobi_apply(cudaStream_t s, int n, const T* P, const T* r, T* z, const KScalars* S) {
     k_jacobi_apply<T><<<TILE_LAUNCH(n), s>>>(n, P, r, z, S);
     XCAL_CHECK_LAUNCH();
@@ -517,6 +550,8 @@ void kr_record(cudaStream_t s, const KScalars* S, int* out) {
 // the two value types of the Krylov launchers
 #define XCAL_KRYLOV_INSTANTIATE(T)                                                                              \
     template void kr_spmv<T>(cudaStream_t, const CSRView&, const T*, const T*, T*, const KScalars*);             \
+    template void kr_spmv_shaped<T>(cudaStream_t, const SpmvShape&, const CSRView&, const T*, const T*, T*,      \
+                                    const KScalars*);                                                           \
     template void kr_jacobi_apply<T>(cudaStream_t, int, const T*, const T*, T*, const KScalars*);                \
     template void kr_copy<T>(cudaStream_t, int, const T*, T*, const KScalars*);                                  \
     template void kr_cg_start<T>(cudaStream_t, int, const T*, const T*, T*, KScalars*, double*);                 \
