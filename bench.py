@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--serve-cases", type=int, default=16, help="serving stream: requests (0 = skip)")
     ap.add_argument("--serve-nmax", type=float, default=3e4)
     ap.add_argument("--serve-rate", type=float, default=8.0)
+    ap.add_argument("--only", choices=["les", "serving"], default=None,
+                    help="run one secondary workload alone and print its block as the line (profiling)")
     return ap.parse_args()
 
 
@@ -239,10 +241,11 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
     achieved = bytes_spmv / avg_s / 1e9 if spmv_n else None
     traffic = None
     tp = os.path.join(ROOT, "profiles", "spmv_traffic.json")
-    if os.path.exists(tp) and not fp32:
+    if os.path.exists(tp):
         try:
             tr = json.load(open(tp))
-            traffic = tr.get("bytes_per_launch_128") if args.size == 128 else None
+            key = "bytes_per_launch_128_fp32" if fp32 else "bytes_per_launch_128"
+            traffic = tr.get(key) if args.size == 128 else None
         except Exception:
             traffic = None
     prec_name = "FP32" if fp32 else "FP64"
@@ -375,6 +378,13 @@ def main():
     import __graft_entry__ as ge
     x = ge.load_package()
     A = x._abi
+    if args.only is not None:
+        blk = les_measure(x, A, args, local) if args.only == "les" else serve_measure(x, args, local)
+        if rank == 0:
+            print(json.dumps({"only": args.only, **blk}), flush=True)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
     n = args.size
     t_mesh = time.perf_counter()
     pm = x.channel_polymesh(n, n, n, seed=0)
