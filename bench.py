@@ -118,6 +118,22 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(v: float, world: int, device=None) -> float:
+    """The largest of the ranks' values (every rank takes part; 1 rank: v)."""
+    if world <= 1:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(cells_per_rank: int, world: int, steps: int, seconds: float) -> float:
+    """Whole-job Mcell-iters/s of `world` replicas, each advancing its own
+    `cells_per_rank`-cell case `steps` iterations, timed by the slowest rank."""
+    return cells_per_rank * world * steps / seconds / 1e6
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -224,10 +240,7 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
     launches = x.launch_count() - l0
     prof1 = [case.profile(k) for k in range(5)]
     case.set_profiling(False)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world, "cuda")
     fp32 = precision == "mixed"
     n = mesh.n_cells
     # roofline of the dominant kernel: the CG SpMV fused with p = z + beta p
@@ -264,7 +277,7 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
         roof["cg_update"] = {"avg_launch_us": upd_s * 1e6, "bytes_per_launch": ub, "achieved": ub / upd_s / 1e9,
                              "launches_timed": upd_n, "share_of_step": upd_s * 1e3 * spmv_all / ms if ms else None}
     tm = case.timings()
-    out = {"value": n * world * args.steps / (ms / 1e3) / 1e6, "ms_per_step": ms / args.steps, "roofline": roof,
+    out = {"value": job_throughput(n, world, args.steps, ms / 1e3), "ms_per_step": ms / args.steps, "roofline": roof,
            "gpu_launches": launches, "clocks": clk, "setup_s": round(t_setup, 2), "nnz_p": nnz_p,
            "residuals_last": [float(v) for v in res[-1]] if len(res) else None,
            "phases_ms_total": {"U_solve": tm[1], "p_solve": tm[2], "other": tm[3], "total": tm[5]}}
@@ -355,12 +368,8 @@ def e2e_measure(x, A, case, mesh, args, world):
         r, _ = case.simple_iterate(1)
         hU[:] = case.get_field(A.FIELD_U)
         hp[:] = case.get_field(A.FIELD_P)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    return {"value": nC * world * args.e2e_steps / e2e_s / 1e6, "unit": UNIT,
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+    return {"value": job_throughput(nC, world, args.e2e_steps, e2e_s), "unit": UNIT,
             "h2d_bytes_per_step": 4 * nC * 8, "d2h_bytes_per_step": 4 * nC * 8 + 4 * 8, "steps": args.e2e_steps}
 
 
