@@ -220,7 +220,7 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
     case.simple_iterate(args.warmup)
     torch.cuda.synchronize()
     case.set_profiling(True)
-    prof0 = [case.profile(k) for k in range(5)]
+    prof0 = [case.profile(k) for k in range(6)]
     l0 = x.launch_count()
     clocks = ClockSampler(local)
     clocks.start()
@@ -238,7 +238,7 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
         torch.distributed.barrier()
     clk = clocks.stop()
     launches = x.launch_count() - l0
-    prof1 = [case.profile(k) for k in range(5)]
+    prof1 = [case.profile(k) for k in range(6)]
     case.set_profiling(False)
     ms = max_over_ranks(ms, world, "cuda")
     fp32 = precision == "mixed"
@@ -267,11 +267,29 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
             "frac": (achieved / peak) if achieved else None, "traffic": traffic, "bytes_per_launch": bytes_spmv,
             "launches_timed": spmv_n, "launches_total": spmv_all, "avg_launch_us": avg_s * 1e6,
             "share_of_step": avg_s * 1e3 * spmv_all / ms if ms else None}
+    # persistent CG: one cooperative launch per solve runs every iteration
+    # (SpMV phase + update phase, q on chip); per iteration it moves the
+    # matrix slots, row lengths and slice offsets, gathers z and p_{k-1},
+    # writes p_k, then reads x, r, P, p_k and writes x, r, z
+    pers_ms = prof1[5][0] - prof0[5][0]
+    pers_it = prof1[5][1] - prof0[5][1]
+    if pers_it:
+        s_ = 4 if fp32 else 8
+        bpi = nnz_p * (s_ + 4) + n * (1 + 10 * s_) + 4 * ((n + 31) // 32)
+        t_it = pers_ms / pers_it / 1e3
+        ach = bpi / t_it / 1e9
+        roof = {"bound": "hbm", "kernel": f"k_cg_persist<{'FP32' if fp32 else 'FP64'}> (whole CG solve in one "
+                                          "cooperative launch: SELL-32 SpMV with p = z + beta p and <p,Ap>, grid "
+                                          "barrier, x/r/z update with <r,z>, grid barrier)",
+                "achieved": ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
+                "traffic": None, "bytes_per_iteration": bpi, "iterations": pers_it,
+                "us_per_iteration": t_it * 1e6,
+                "share_of_step": pers_ms / ms if ms else None}
     # second kernel of each CG iteration: x += alpha p; r -= alpha q; z = P r;
     # <r,z> -- reads x, p, r, q, P and writes x, r, z (8 vectors)
     upd_ms = prof1[3][0] - prof0[3][0]
     upd_n = prof1[3][1] - prof0[3][1]
-    if upd_n:
+    if upd_n and not pers_it:
         upd_s = upd_ms / upd_n / 1e3
         ub = 8 * (4 if fp32 else 8) * n
         roof["cg_update"] = {"avg_launch_us": upd_s * 1e6, "bytes_per_launch": ub, "achieved": ub / upd_s / 1e9,

@@ -361,7 +361,8 @@ int32_t xcal_case_stream(const xcal_case* cs, void** stream);
 /* per-kernel CUDA-event timing of the dominant kernels (off by default).
  * which: 0 = CG SpMV (+ p.Ap), 1 = BiCGSTAB SpMV, 2 = DILU sweep levels,
  *        3 = CG vector update (+ Jacobi apply and r.z when fused),
- *        4 = count only: every CG SpMV launch that did work (ms = 0).
+ *        4 = count only: every CG SpMV launch that did work (ms = 0),
+ *        5 = persistent CG launches (ms; launches = CG iterations they ran).
  * ms = summed device time, launches = timed launches that did work.  Inside
  * the steady-state CUDA-graph chunks only sampled iterations are timed. */
 int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable);
@@ -372,6 +373,11 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable);
  * synchronisation.  Results are identical to the default mode.  Per-kernel
  * profiling does not apply inside the graph. */
 int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable);
+/* persistent CG (on by default): a CG solve with Jacobi or no preconditioner
+ * runs as one cooperative launch (grid barriers between the SpMV and update
+ * phases, q kept on chip) whenever the system's tiles fit the GPU at once;
+ * otherwise, and in graph mode, the two-kernel loop runs.  Same results. */
+int32_t xcal_case_set_persistent(xcal_case* cs, int32_t enable);
 /* launch-shape autotuner (runs on first use, or now): out6 = for U then p,
  * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU as
  * one-block sweeps [0/1]).  The choices never change a result. */

@@ -96,3 +96,26 @@ def test_autotuner_choices(x, ctx):
     # a second case of the same size class reuses the cached choices
     c2 = x.Case(x.DeviceMesh(ctx, mesh), cfg)
     assert c2.tuning() == t
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_persistent_cg_identical(x, ctx, prec):
+    """The pressure CG as one cooperative launch (grid barriers, q on chip)
+    gives the two-kernel loop's results bit for bit."""
+    mesh = x.build_mesh3(x.channel_polymesh(48, 24, 24, seed=6))
+    out = []
+    for persist in (False, True):
+        model, config = x.cases.channel_case(mesh, iterations=4, precision=prec)
+        cfg, keep = x.build_config(model, config)
+        dm = x.DeviceMesh(ctx, mesh)
+        c = x.Case(dm, cfg)
+        c.set_persistent(persist)
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+        c.set_profiling(True)
+        res, _ = c.simple_iterate(4)
+        ms, its = c.profile(5)
+        out.append((res, c.get_field(x._abi.FIELD_U), c.get_field(x._abi.FIELD_P), its))
+    assert out[0][3] == 0 and out[1][3] > 0      # the persistent kernel ran only when enabled
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])

@@ -60,6 +60,7 @@ SIGNATURES = {
     "xcal_case_stream": (_i32, [_vp, C.POINTER(_vp)]),
     "xcal_case_set_profiling": (_i32, [_vp, _i32]),
     "xcal_case_set_graph_mode": (_i32, [_vp, _i32]),
+    "xcal_case_set_persistent": (_i32, [_vp, _i32]),
     "xcal_case_tuning": (_i32, [_vp, _pi]),
     "xcal_case_get_profile": (_i32, [_vp, _i32, _pd, _pi64]),
     "xcal_residual_noalloc": (_i32, [_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, _i32]),

@@ -612,6 +612,10 @@ class Case:
         return {eq: {"spmv_rows_per_thread": int(a[3 * k]), "spmv_block": int(a[3 * k + 1]),
                      "dilu_one_block": bool(a[3 * k + 2])} for k, eq in enumerate(("U", "p"))}
 
+    def set_persistent(self, on: bool = True):
+        """Persistent CG (one cooperative launch per solve) on or off."""
+        self._chk(lib().xcal_case_set_persistent(self.h, 1 if on else 0))
+
     def set_graph_mode(self, on: bool = True):
         """Replay each SIMPLE iteration / PISO step as one captured CUDA graph
         (device-driven Krylov loops; same results as the default mode)."""
@@ -620,8 +624,9 @@ class Case:
     def profile(self, which: int):
         """(summed device ms, timed launches) of a kernel class:
         0 = CG SpMV, 1 = BiCGSTAB SpMV, 2 = DILU applications, 3 = CG update;
-        4 = (0, every CG SpMV launch that did work).  Steady-state chunks run
-        as CUDA graphs in which only sampled iterations are timed."""
+        4 = (0, every CG SpMV launch that did work); 5 = persistent CG
+        launches (ms, CG iterations).  Steady-state chunks run as CUDA graphs
+        in which only sampled iterations are timed."""
         ms, n = C.c_double(), C.c_int64()
         self._chk(lib().xcal_case_get_profile(self.h, which, C.byref(ms), C.byref(n)))
         return ms.value, n.value

@@ -329,6 +329,12 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable) {
     return XCAL_OK;
 }
 
+int32_t xcal_case_set_persistent(xcal_case* cs, int32_t enable) {
+    if (!cs) return XCAL_ERR_INVALID;
+    cs->c->persistent_cg = enable != 0;
+    return XCAL_OK;
+}
+
 int32_t xcal_case_tuning(xcal_case* cs, int32_t* out6) {
     if (!cs || !out6) return XCAL_ERR_INVALID;
     Case* c = cs->c.get();
@@ -350,7 +356,7 @@ int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable) {
 }
 
 int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches) {
-    if (!cs || which < 0 || which > 4) return XCAL_ERR_INVALID;
+    if (!cs || which < 0 || which > 5) return XCAL_ERR_INVALID;
     if (ms) *ms = cs->c->prof_ms[which];
     if (launches) *launches = cs->c->prof_n[which];
     return XCAL_OK;

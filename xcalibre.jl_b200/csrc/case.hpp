@@ -72,6 +72,8 @@ struct BCTable {
 struct KrylovWS {
     DBuf<double> x, dx, r, z, p, q, v, s, t, part0, part1;
     DBuf<float> fx, fr, fz, fp, fq, fv, fs, ft, fd;  // mixed precision inner vectors
+    DBuf<unsigned int> bar;  // persistent CG: grid-barrier state (count, generation)
+    DBuf<int> err;           // persistent CG: a barrier wait gave up
     DBuf<KScalars> S;  // [2]: U, p
 };
 
@@ -107,8 +109,9 @@ struct Case {
     // optional per-kernel event timing (xcal_case_set_profiling)
     bool profiling = false;
     std::vector<cudaEvent_t> pev;  // pairs, reused per polling chunk
-    double prof_ms[5] = {0, 0, 0, 0, 0};
-    long long prof_n[5] = {0, 0, 0, 0, 0};
+    double prof_ms[6] = {0, 0, 0, 0, 0, 0};
+    long long prof_n[6] = {0, 0, 0, 0, 0, 0};
+    bool persistent_cg = true;  // CG (Jacobi / none) as one cooperative launch when the tiles fit
     void prof_reserve(int pairs);
     // Steady-state polling chunks of a Krylov solve (32 CG / 8 BiCGSTAB
     // iterations) replay as CUDA graphs: every pointer they use is fixed for

@@ -79,6 +79,13 @@ void kr_cg_update(cudaStream_t s, int n, T* x, const T* P0, const T* P1, T* r, c
                   int jacobi_fused, KScalars* S, double* part);
 template <class T>
 void kr_cg_rz(cudaStream_t s, int n, const T* r, const T* z, KScalars* S, double* part);
+// The whole CG loop in one cooperative launch (Jacobi: jacobi = 1, P = inverse
+// diagonal; no preconditioner: jacobi = 0, z aliases r).  Returns false,
+// launching nothing, when the system's tiles cannot all be co-resident.
+// bar: 2 words of barrier state, err: set when a barrier wait gave up.
+template <class T>
+bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
+                   T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters);
 void kr_finish(cudaStream_t s, int n, const double* x, const double* dx, double* field);
 template <class T>
 void kr_bicg_start(cudaStream_t s, int n, const T* c, const T* r, T* p, KScalars* S, double* part0, double* part1);

@@ -131,6 +131,8 @@ constexpr int SELL_C = 32;
 // systems up to this many rows apply DILU (and build its factor) in one
 // block, level after level, instead of one launch per level
 constexpr int DILU_BLOCK_MAX_ROWS = 65536;
+// FP32 (mixed-precision inner) CG runs as one cooperative launch up to this size
+constexpr int PERSIST_FP32_MAX_ROWS = 262144;
 struct CSRView {
     int n;
     const int* slice;          // [ceil(n/32)+1] first slot of each slice
