@@ -382,6 +382,9 @@ int32_t xcal_case_set_persistent(xcal_case* cs, int32_t enable);
  * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU as
  * one-block sweeps [0/1]).  The choices never change a result. */
 int32_t xcal_case_tuning(xcal_case* cs, int32_t* out6);
+/* DILU execution: 0 = autotuned (default), 1 = one-block sweeps,
+ * 2 = one launch per level over level-ordered triangles.  Same results. */
+int32_t xcal_case_set_dilu_mode(xcal_case* cs, int32_t mode);
 int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches);
 
 /* ---- batching / serving --------------------------------------------------

@@ -62,6 +62,7 @@ SIGNATURES = {
     "xcal_case_set_graph_mode": (_i32, [_vp, _i32]),
     "xcal_case_set_persistent": (_i32, [_vp, _i32]),
     "xcal_case_tuning": (_i32, [_vp, _pi]),
+    "xcal_case_set_dilu_mode": (_i32, [_vp, _i32]),
     "xcal_case_get_profile": (_i32, [_vp, _i32, _pd, _pi64]),
     "xcal_residual_noalloc": (_i32, [_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, _i32]),
     "xcal_footprint_estimate": (_i32, [_i64, _i64, _i64, _i32, _i32, _i32, _pi64]),

@@ -612,6 +612,10 @@ class Case:
         return {eq: {"spmv_rows_per_thread": int(a[3 * k]), "spmv_block": int(a[3 * k + 1]),
                      "dilu_one_block": bool(a[3 * k + 2])} for k, eq in enumerate(("U", "p"))}
 
+    def set_dilu_mode(self, mode: int):
+        """0 = autotuned, 1 = one-block sweeps, 2 = per-level kernels."""
+        self._chk(lib().xcal_case_set_dilu_mode(self.h, int(mode)))
+
     def set_persistent(self, on: bool = True):
         """Persistent CG (one cooperative launch per solve) on or off."""
         self._chk(lib().xcal_case_set_persistent(self.h, 1 if on else 0))

@@ -99,7 +99,9 @@ void Case::autotune() {
                 g_spmv_choice[k] = sh;
             }
         }
-        if (SS.precond == XCAL_PRECOND_DILU && E.n <= 4 * DILU_BLOCK_MAX_ROWS) {
+        if (dilu_mode != 0) {
+            E.use_block = dilu_mode == 1;
+        } else if (SS.precond == XCAL_PRECOND_DILU && E.n <= 4 * DILU_BLOCK_MAX_ROWS) {
             TuneKey k = key_of(1, tsz, E);
             std::unique_lock<std::mutex> lk(g_tune_mu);
             auto it = g_dilu_choice.find(k);

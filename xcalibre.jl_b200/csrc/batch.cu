@@ -537,7 +537,13 @@ size_t estimate_case_bytes(long nC, long nF, long nB, int mixed, int dilu_U, int
         b += nnz * (16.0 + (mixed ? 4.0 : 0.0));
         b += nC * (21.0 + 8.0 * nvec + (mixed ? 4.0 : 0.0)) + 4.0 * (nC / 32 + 2);
         b += 4.0 * 3 * nI;
-        if ((e == 0 && dilu_U) || (e == 1 && dilu_p)) b += 8.0 * nC;
+        if ((e == 0 && dilu_U) || (e == 1 && dilu_p)) {
+            // level lists and offsets, and the level-ordered triangles: per
+            // off-diagonal slot column, source slot, value [+ fp32 value]
+            b += 8.0 * nC + 16.0 * nC;
+            // (SELL padding of the level order: up to half again)
+            b += (nnz - nC) * 1.5 * (16.0 + (mixed ? 4.0 : 0.0)) + 2.0 * nC + 8.0 * (nC / 32 + 2);
+        }
     }
     // three boundary-condition tables (85 bytes per boundary face) + partner lists
     b += 3.0 * (85.0 * nB + 4.0 * (nC + 1));

@@ -335,6 +335,14 @@ int32_t xcal_case_set_persistent(xcal_case* cs, int32_t enable) {
     return XCAL_OK;
 }
 
+int32_t xcal_case_set_dilu_mode(xcal_case* cs, int32_t mode) {
+    if (!cs || mode < 0 || mode > 2) return XCAL_ERR_INVALID;
+    Case* c = cs->c.get();
+    c->dilu_mode = mode;
+    if (mode != 0) c->U.use_block = c->P.use_block = mode == 1;
+    return XCAL_OK;
+}
+
 int32_t xcal_case_tuning(xcal_case* cs, int32_t* out6) {
     if (!cs || !out6) return XCAL_ERR_INVALID;
     Case* c = cs->c.get();

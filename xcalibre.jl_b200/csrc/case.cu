@@ -464,6 +464,48 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
         E.d_upper_rows.upload(rows, s);
         E.h_upper_rows = rows;
         E.d_upper_off.upload(E.upper_off, s);
+        // level-ordered copies of the strictly lower / upper entries
+        for (int tri = 0; tri < 2; ++tri) {
+            const std::vector<int>& order = tri == 0 ? E.h_lower_rows : E.h_upper_rows;
+            LevelSell& L = tri == 0 ? E.lsell : E.usell;
+            const int nsl2 = (n + SELL_C - 1) / SELL_C;
+            std::vector<int> sl(nsl2 + 1, 0);
+            std::vector<unsigned char> cnt(n);
+            for (int k = 0; k < n; ++k) {
+                int i = order[k];
+                int c = tri == 0 ? (E.diag[i] - E.base(i)) / SELL_C : (int)E.len[i] - 1 - (E.diag[i] - E.base(i)) / SELL_C;
+                cnt[k] = (unsigned char)c;
+            }
+            for (int sidx = 0; sidx < nsl2; ++sidx) {
+                int w = 0;
+                for (int k = sidx * SELL_C; k < std::min(n, sidx * SELL_C + SELL_C); ++k) w = std::max(w, (int)cnt[k]);
+                sl[sidx + 1] = sl[sidx] + SELL_C * w;
+            }
+            L.nslots = sl[nsl2];
+            std::vector<int> col(std::max(L.nslots, 1L)), src(std::max(L.nslots, 1L));
+            for (int k = 0; k < n; ++k) {
+                int i = order[k];
+                int b0 = sl[k / SELL_C] + k % SELL_C;
+                int first = tri == 0 ? E.base(i) : E.diag[i] + SELL_C;
+                int w = (sl[k / SELL_C + 1] - sl[k / SELL_C]) / SELL_C;
+                for (int j = 0; j < w; ++j) {
+                    int e = b0 + SELL_C * j;
+                    if (j < cnt[k]) {
+                        src[e] = first + SELL_C * j;
+                        col[e] = E.colval[src[e]];
+                    } else {  // padding: never read
+                        src[e] = E.diag[i];
+                        col[e] = i;
+                    }
+                }
+            }
+            L.slice.upload(sl, s);
+            L.cnt.upload(cnt, s);
+            L.col.upload(col, s);
+            L.src.upload(src, s);
+            L.val.alloc(std::max(L.nslots, 1L));
+            L.val.zero(s);
+        }
     }
 }
 
@@ -637,6 +679,11 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
             E->nz32.zero(stream);
             E->P32.alloc(E->n);
             E->P32.zero(stream);
+            for (LevelSell* L : {&E->lsell, &E->usell})
+                if (L->nslots > 0) {
+                    L->val32.alloc(L->nslots);
+                    L->val32.zero(stream);
+                }
         }
     }
     ws.part0.alloc(T);
@@ -856,11 +903,29 @@ void Case::dilu_ldiv(Equation& E, const T* nz, const T* D, const T* b, T* out, c
                       E.d_upper_rows.p, E.d_upper_off.p, (int)E.upper_off.size() - 1, S);
         return;
     }
+    // level kernels over the level-ordered triangles (values refreshed by
+    // dilu_refresh before the solve)
+    const T* lv = sizeof(T) == 8 ? (const T*)E.lsell.val.p : (const T*)E.lsell.val32.p;
+    const T* uv = sizeof(T) == 8 ? (const T*)E.usell.val.p : (const T*)E.usell.val32.p;
     for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
-        kr_dilu_fwd(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], A, nz, D, b, out,
-                    S);
+        kr_dilu_fwd_lv(stream, E.lower_off[l], E.lower_off[l + 1], E.d_lower_rows.p, E.lsell.slice.p, E.lsell.cnt.p,
+                       E.lsell.col.p, lv, D, b, out, S);
     for (size_t l = 0; l + 1 < E.upper_off.size(); ++l)
-        kr_dilu_bwd(stream, E.d_upper_rows.p + E.upper_off[l], E.upper_off[l + 1] - E.upper_off[l], A, nz, D, out, S);
+        kr_dilu_bwd_lv(stream, E.upper_off[l], E.upper_off[l + 1], E.d_upper_rows.p, E.usell.slice.p, E.usell.cnt.p,
+                       E.usell.col.p, uv, D, out, S);
+}
+
+// copy the current off-diagonal values into the level-ordered triangles
+// (FP64 values, or the FP32 copy nz32 for the mixed inner solves)
+void Case::dilu_refresh(Equation& E, bool fp32) {
+    if (E.dilu_block() || E.lower_off.empty()) return;
+    for (LevelSell* L : {&E.lsell, &E.usell}) {
+        if (fp32) {
+            kr_gather_vals(stream, L->nslots, L->src.p, E.nz32.p, L->val32.p);
+        } else {
+            kr_gather_vals(stream, L->nslots, L->src.p, E.nz.p, L->val.p);
+        }
+    }
 }
 
 template <class T>
@@ -1130,6 +1195,7 @@ void Case::solve_captured(int eqn, int comp) {
     const double inner_rtol = cfg.inner_rtol > 0 ? cfg.inner_rtol : 1e-3;
     kr_ks_init(stream, S, SS.atol, SS.rtol, itmax, mixed ? 1 : 0, inner_rtol);
     if (!mixed) {
+        if (SS.precond == XCAL_PRECOND_DILU) dilu_refresh(E, false);
         KrylovVecs<double> V{ws.x.p, ws.r.p, ws.z.p, ws.p.p, ws.q.p, ws.v.p, ws.s.p, ws.t.p};
         const double* r0 = SS.solver == XCAL_SOLVER_CG ? V.r : V.q;
         kr_init_resid(stream, A, E.nz.p, b, field, ws.dx.p, V.x, SS.solver == XCAL_SOLVER_CG ? V.r : V.q);
@@ -1143,6 +1209,7 @@ void Case::solve_captured(int eqn, int comp) {
     } else {
         kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
         if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, n, E.P.p, E.P32.p);
+        if (SS.precond == XCAL_PRECOND_DILU) dilu_refresh(E, true);
         KrylovVecs<float> V{ws.fx.p, ws.fr.p, ws.fz.p, ws.fp.p, ws.fq.p, ws.fv.p, ws.fs.p, ws.ft.p};
         const bool cg = SS.solver == XCAL_SOLVER_CG;
         float* rhs = cg ? V.r : ws.fd.p;
@@ -1193,6 +1260,7 @@ double Case::solve_system(int eqn, int comp, int* iters) {
         solve_mixed(E, SS, field, b, S, hS, gk, iters);
     } else {
         XCAL_CUDA(cudaMemcpyAsync(S, hS, sizeof(KScalars), cudaMemcpyHostToDevice, stream));
+        if (SS.precond == XCAL_PRECOND_DILU) dilu_refresh(E, false);
         KrylovVecs<double> V{ws.x.p, ws.r.p, ws.z.p, ws.p.p, ws.q.p, ws.v.p, ws.s.p, ws.t.p};
         if (SS.solver == XCAL_SOLVER_CG) {
             kr_init_resid(stream, A, nz, b, field, ws.dx.p, V.x, V.r);
@@ -1224,6 +1292,7 @@ void Case::solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, 
     CSRView A = E.view();
     kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
     if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, n, E.P.p, E.P32.p);
+    if (SS.precond == XCAL_PRECOND_DILU) dilu_refresh(E, true);
     KrylovVecs<float> V{ws.fx.p, ws.fr.p, ws.fz.p, ws.fp.p, ws.fq.p, ws.fv.p, ws.fs.p, ws.ft.p};
     hS->mixed = 1;
     hS->inner_rtol = cfg.inner_rtol > 0 ? cfg.inner_rtol : 1e-3;

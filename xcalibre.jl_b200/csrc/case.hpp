@@ -31,6 +31,20 @@ struct DevMesh {
     MeshView view() const;
 };
 
+// Level-ordered SELL-32 copy of one triangle's off-diagonal entries (DILU
+// sweeps of large systems): position k of the level order (the row
+// rows[k]) holds that row's strictly lower (or upper) entries in the row's
+// own order, so the rows of one level read their slots coalesced.  `src` maps
+// each slot to the matrix slot whose value it mirrors (refreshed before each
+// DILU-preconditioned solve).
+struct LevelSell {
+    long nslots = 0;
+    DBuf<int> slice, col, src;
+    DBuf<unsigned char> cnt;
+    DBuf<double> val;
+    DBuf<float> val32;
+};
+
 struct Equation {
     int n = 0;
     long nnz = 0;
@@ -48,6 +62,7 @@ struct Equation {
     std::vector<int> lower_off, upper_off;
     std::vector<int> h_lower_rows, h_upper_rows;  // host copies (batched level lists)
     DBuf<int> d_lower_off, d_upper_off;           // level offsets (one-block sweeps)
+    LevelSell lsell, usell;                       // level-ordered triangles (level-kernel sweeps)
     // launch choices (autotune.cu); neither changes any result
     bool use_block = false;   // DILU as one-block sweeps (default: n <= DILU_BLOCK_MAX_ROWS)
     SpmvShape spmv_shape;     // BiCGSTAB SpMV row mapping / block size
@@ -112,6 +127,7 @@ struct Case {
     double prof_ms[6] = {0, 0, 0, 0, 0, 0};
     long long prof_n[6] = {0, 0, 0, 0, 0, 0};
     bool persistent_cg = true;  // CG (Jacobi / none) as one cooperative launch when the tiles fit
+    int dilu_mode = 0;          // 0 = autotuned / size rule, 1 = one-block sweeps, 2 = per-level kernels
     void prof_reserve(int pairs);
     // Steady-state polling chunks of a Krylov solve (32 CG / 8 BiCGSTAB
     // iterations) replay as CUDA graphs: every pointer they use is fixed for
@@ -161,6 +177,7 @@ struct Case {
     void dilu_ldiv(Equation& E, const T* nz, const T* D, const T* b, T* out, const KScalars* S);
     template <class T>
     void apply_M(Equation& E, int ptype, const T* nz, const T* P, const T* in, T* out, const KScalars* S);
+    void dilu_refresh(Equation& E, bool fp32);
     template <class T>
     void krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz, const T* P, const T* c, const T* r0,
                         const KrylovVecs<T>& V, KScalars* S, KScalars* hS, int gk);

@@ -108,6 +108,15 @@ void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, c
 template <class T>
 void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const T* nz, const T* D, T* x,
                  const KScalars* S);
+// DILU level sweeps over level-ordered triangles (positions k0..k1 of one level)
+template <class T>
+void kr_dilu_fwd_lv(cudaStream_t s, int k0, int k1, const int* rows, const int* slice, const unsigned char* cnt,
+                    const int* col, const T* val, const T* D, const T* b, T* y, const KScalars* S);
+template <class T>
+void kr_dilu_bwd_lv(cudaStream_t s, int k0, int k1, const int* rows, const int* slice, const unsigned char* cnt,
+                    const int* col, const T* val, const T* D, T* x, const KScalars* S);
+template <class T>
+void kr_gather_vals(cudaStream_t s, long n, const int* src, const T* vals, T* dst);
 // small systems (n <= DILU_BLOCK_MAX_ROWS): whole sweeps in one block
 void kr_dilu_D_block(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
                      double* D);

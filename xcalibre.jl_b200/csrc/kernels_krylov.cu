@@ -416,6 +416,52 @@ __global__ void k_dilu_bwd(const int* __restrict__ rows, int nrows, CSRView A, c
     dilu_bwd_row(A, nz, D, x, rows[t]);
 }
 
+// DILU sweeps over the level-ordered triangles: thread per position k of a
+// level (row rows[k]); the entries are the row's own, in the row's order, so
+// each row's sum is dilu_fwd_row's / dilu_bwd_row's
+template <class T>
+__global__ void k_dilu_fwd_lv(int k0, int k1, const int* __restrict__ rows, const int* __restrict__ slice,
+                              const unsigned char* __restrict__ cnt, const int* __restrict__ col,
+                              const T* __restrict__ val, const T* __restrict__ D, const T* __restrict__ b, T* y,
+                              const KScalars* S) {
+    if (S && S->done) return;
+    const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= k1) return;
+    const int i = rows[k];
+    const int base = slice[k / SELL_C] + (k % SELL_C), c = cnt[k];
+    T sum = T(0);
+    for (int j = 0; j < c; ++j) {
+        const int e = base + SELL_C * j;
+        const int jc = ld_stream(col + e);
+        sum = sum + (ld_stream(val + e) * y[jc]) * (T(1) / D[jc]);
+    }
+    y[i] = b[i] - sum;
+}
+
+template <class T>
+__global__ void k_dilu_bwd_lv(int k0, int k1, const int* __restrict__ rows, const int* __restrict__ slice,
+                              const unsigned char* __restrict__ cnt, const int* __restrict__ col,
+                              const T* __restrict__ val, const T* __restrict__ D, T* x, const KScalars* S) {
+    if (S && S->done) return;
+    const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= k1) return;
+    const int i = rows[k];
+    const int base = slice[k / SELL_C] + (k % SELL_C), c = cnt[k];
+    T sum = T(0);
+    for (int j = 0; j < c; ++j) {
+        const int e = base + SELL_C * j;
+        sum = sum + ld_stream(val + e) * x[ld_stream(col + e)];
+    }
+    x[i] = (x[i] - sum) / D[i];
+}
+
+// dst[e] = src_vals[src[e]] (refresh of a level-ordered triangle)
+template <class T>
+__global__ void k_gather_vals(long n, const int* __restrict__ src, const T* __restrict__ vals, T* dst) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        dst[e] = vals[ld_stream(src + e)];
+}
+
 // residual (src/Solve/Solve_1_api.jl:441-464): ||b - A x|| / max(||b||, 1 if tiny)
 __global__ void __launch_bounds__(RED_THREADS, 8) k_residual(CSRView A, const double* __restrict__ nz,
                                                           const double* __restrict__ x, const double* __restrict__ b,
@@ -708,6 +754,27 @@ void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, c
     k_dilu_bwd<T><<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, A, nz, D, x, S);
     XCAL_CHECK_LAUNCH();
 }
+template <class T>
+void kr_dilu_fwd_lv(cudaStream_t s, int k0, int k1, const int* rows, const int* slice, const unsigned char* cnt,
+                    const int* col, const T* val, const T* D, const T* b, T* y, const KScalars* S) {
+    if (k1 <= k0) return;
+    k_dilu_fwd_lv<T><<<(k1 - k0 + 255) / 256, 256, 0, s>>>(k0, k1, rows, slice, cnt, col, val, D, b, y, S);
+    XCAL_CHECK_LAUNCH();
+}
+template <class T>
+void kr_dilu_bwd_lv(cudaStream_t s, int k0, int k1, const int* rows, const int* slice, const unsigned char* cnt,
+                    const int* col, const T* val, const T* D, T* x, const KScalars* S) {
+    if (k1 <= k0) return;
+    k_dilu_bwd_lv<T><<<(k1 - k0 + 255) / 256, 256, 0, s>>>(k0, k1, rows, slice, cnt, col, val, D, x, S);
+    XCAL_CHECK_LAUNCH();
+}
+template <class T>
+void kr_gather_vals(cudaStream_t s, long n, const int* src, const T* vals, T* dst) {
+    if (n <= 0) return;
+    long blocks = (n + 255) / 256;
+    k_gather_vals<T><<<(int)(blocks < 148L * 16 ? blocks : 148L * 16), 256, 0, s>>>(n, src, vals, dst);
+    XCAL_CHECK_LAUNCH();
+}
 void kr_dilu_D_block(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
                      double* D) {
     if (nlev <= 0) return;
@@ -784,7 +851,12 @@ void kr_record(cudaStream_t s, const KScalars* S, int* out) {
     template void kr_dilu_bwd<T>(cudaStream_t, const int*, int, const CSRView&, const T*, const T*, T*,          \
                                  const KScalars*);                                                              \
     template void kr_dilu_block<T>(cudaStream_t, const CSRView&, const T*, const T*, const T*, T*, const int*,   \
-                                   const int*, int, const int*, const int*, int, const KScalars*);
+                                   const int*, int, const int*, const int*, int, const KScalars*);              \
+    template void kr_dilu_fwd_lv<T>(cudaStream_t, int, int, const int*, const int*, const unsigned char*,         \
+                                    const int*, const T*, const T*, const T*, T*, const KScalars*);             \
+    template void kr_dilu_bwd_lv<T>(cudaStream_t, int, int, const int*, const int*, const unsigned char*,         \
+                                    const int*, const T*, const T*, T*, const KScalars*);                       \
+    template void kr_gather_vals<T>(cudaStream_t, long, const int*, const T*, T*);
 XCAL_KRYLOV_INSTANTIATE(double)
 XCAL_KRYLOV_INSTANTIATE(float)
 
