@@ -253,7 +253,13 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
     avg_s = spmv_ms / max(spmv_n, 1) / 1e3
     achieved = bytes_spmv / avg_s / 1e9 if spmv_n else None
     traffic = None
+    tr_all = {}
     tp = os.path.join(ROOT, "profiles", "spmv_traffic.json")
+    if os.path.exists(tp):
+        try:
+            tr_all = json.load(open(tp))
+        except Exception:
+            tr_all = {}
     if os.path.exists(tp):
         try:
             tr = json.load(open(tp))
@@ -282,7 +288,10 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
                                           "cooperative launch: SELL-32 SpMV with p = z + beta p and <p,Ap>, grid "
                                           "barrier, x/r/z update with <r,z>, grid barrier)",
                 "achieved": ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
-                "traffic": None, "bytes_per_iteration": bpi, "iterations": pers_it,
+                "traffic": (tr_all.get("persist_bytes_per_iteration_128")
+                            if (not fp32 and args.size == 128) else None),
+                "traffic_unit": "bytes per CG iteration (ncu DRAM read + write of one launch / its iterations)",
+                "bytes_per_iteration": bpi, "iterations": pers_it,
                 "us_per_iteration": t_it * 1e6,
                 "share_of_step": pers_ms / ms if ms else None}
     # second kernel of each CG iteration: x += alpha p; r -= alpha q; z = P r;
