@@ -31,8 +31,13 @@ def _mk(x, ctx, kind, n, seed, prec, nu):
 SPECS = [("cavity", 18, 1, 0.01), ("channel", 10, 2, 2e-3), ("cavity", 31, 3, 1e-3), ("channel", 7, 4, 1e-2)]
 
 
+@pytest.mark.parametrize("persist", [True, False, 256])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_batch_matches_single(x, ctx, prec):
+def test_batch_matches_single(x, ctx, prec, persist):
+    """persist: the batch runs its CG solves as one cooperative launch over
+    every member (True: widest block form that fits; 256: the narrow form) or
+    as the batched two-kernel loop (False); the cases alone use the
+    persistent single-case kernel either way."""
     iters = 6
     alone = []
     for kind, n, seed, nu in SPECS:
@@ -43,6 +48,7 @@ def test_batch_matches_single(x, ctx, prec):
     members = []
     for kind, n, seed, nu in SPECS:
         c, keep = _mk(x, ctx, kind, n, seed, prec, nu)
+        c.set_persistent(persist)
         assert batch.add(c)
         members.append((c, keep))
     hist = []

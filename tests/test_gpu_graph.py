@@ -101,10 +101,12 @@ def test_autotuner_choices(x, ctx):
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_persistent_cg_identical(x, ctx, prec):
     """The pressure CG as one cooperative launch (grid barriers, q on chip)
-    gives the two-kernel loop's results bit for bit."""
+    gives the two-kernel loop's results bit for bit, in each block form: the
+    automatic choice and the 1024-, 512- and 256-thread forms forced."""
     mesh = x.build_mesh3(x.channel_polymesh(48, 24, 24, seed=6))
     out = []
-    for persist in (False, True):
+    modes = (False, True, 1024, 512, 256)
+    for persist in modes:
         model, config = x.cases.channel_case(mesh, iterations=4, precision=prec)
         cfg, keep = x.build_config(model, config)
         dm = x.DeviceMesh(ctx, mesh)
@@ -116,6 +118,8 @@ def test_persistent_cg_identical(x, ctx, prec):
         res, _ = c.simple_iterate(4)
         ms, its = c.profile(5)
         out.append((res, c.get_field(x._abi.FIELD_U), c.get_field(x._abi.FIELD_P), its))
-    assert out[0][3] == 0 and out[1][3] > 0      # the persistent kernel ran only when enabled
-    assert np.array_equal(out[0][0], out[1][0])
-    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+    assert out[0][3] == 0                        # the persistent kernel ran only when enabled
+    for m, o in zip(modes[1:], out[1:]):
+        assert o[3] > 0, m
+        assert np.array_equal(out[0][0], o[0]), m
+        assert np.array_equal(out[0][1], o[1]) and np.array_equal(out[0][2], o[2]), m

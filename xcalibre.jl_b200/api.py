@@ -616,9 +616,11 @@ class Case:
         """0 = autotuned, 1 = one-block sweeps, 2 = per-level kernels."""
         self._chk(lib().xcal_case_set_dilu_mode(self.h, int(mode)))
 
-    def set_persistent(self, on: bool = True):
-        """Persistent CG (one cooperative launch per solve) on or off."""
-        self._chk(lib().xcal_case_set_persistent(self.h, 1 if on else 0))
+    def set_persistent(self, on=True):
+        """Persistent CG (one cooperative launch per solve): False / True, or
+        256 / 512 / 1024 to allow only that block form."""
+        mode = int(on) if isinstance(on, bool) else int(on)
+        self._chk(lib().xcal_case_set_persistent(self.h, mode))
 
     def set_graph_mode(self, on: bool = True):
         """Replay each SIMPLE iteration / PISO step as one captured CUDA graph

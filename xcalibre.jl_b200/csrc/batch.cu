@@ -43,6 +43,8 @@ struct Batch {
     std::vector<int> dlo_off[2], dup_off[2];
     DBuf<int> small_ids;             // systems that run DILU as one block
     int n_small = 0;
+    DBuf<unsigned int> bars;         // persistent CG: barrier state per system
+    DBuf<int> perr;                  // persistent CG: a barrier wait gave up
     std::vector<int2> h_tmap;
     long long iterations = 0;
     double phase_ms[4] = {0, 0, 0, 0};  // host wall time: face loops, U solves, p solve, total
@@ -98,6 +100,10 @@ struct Batch {
         res.zero(stream);
         XCAL_CUDA(cudaMallocHost(&hS, cap * sizeof(KScalars)));
         XCAL_CUDA(cudaMallocHost(&hres, 4 * cap * sizeof(double)));
+        bars.alloc(2 * (size_t)cap);
+        bars.zero(stream);
+        perr.alloc(1);
+        perr.zero(stream);
     }
     ~Batch() {
         if (stream) cudaStreamSynchronize(stream);
@@ -288,6 +294,32 @@ struct Batch {
         }
         int itmax = 0;
         for (int i : members) itmax = std::max(itmax, hS[i].itmax);
+        // every member's whole CG loop in one cooperative launch (the single
+        // case path's policy: FP64 always, FP32 up to PERSIST_FP32_MAX_ROWS)
+        if (cg && (pt == XCAL_PRECOND_JACOBI || pt == XCAL_PRECOND_NONE)) {
+            bool size_ok = true;
+            if (sizeof(T) == 4)
+                for (int i : members) size_ok = size_ok && cases[i]->U.n <= PERSIST_FP32_MAX_ROWS;
+            bool all_persist = true;
+            int width = 0;  // a block form the members ask for (tests), else the widest that fits
+            for (int i : members) {
+                all_persist = all_persist && cases[i]->persistent_cg != 0;
+                if (cases[i]->persistent_cg > 1) width = cases[i]->persistent_cg;
+            }
+            if (size_ok && all_persist &&
+                kb_cg_persist<T>(stream, sy, tm, nt, pt == XCAL_PRECOND_JACOBI ? 1 : 0, bars.p, (int)cases.size(),
+                                 perr.p, itmax + 1, width)) {
+                int errflag = 0;
+                XCAL_CUDA(cudaMemcpyAsync(hS, S.p, cases.size() * sizeof(KScalars), cudaMemcpyDeviceToHost,
+                                          stream));
+                XCAL_CUDA(cudaMemcpyAsync(&errflag, perr.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+                sync();
+                if (errflag) fail(XCAL_ERR_TIMEOUT, "batch: persistent CG grid barrier wait gave up");
+                for (int i : members)
+                    if (!hS[i].done) fail(XCAL_ERR_TIMEOUT, "batch: persistent CG did not report completion");
+                return;
+            }
+        }
         const int CHUNK = cg ? 32 : 8;
         int chunk = cg ? 4 : 1;
         long launched = 0;

@@ -62,6 +62,13 @@ void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int* small_ids, int n_sma
              int use_S);
 template <class T>
 void kb_cg_start(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
+// every system's CG solve (Jacobi: jacobi = 1; none: 0) in one cooperative
+// launch; false (nothing launched) when the tiles cannot all be co-resident.
+// bars: 2 words per system of the batch (nbars systems), err as in
+// kr_cg_persist.
+template <class T>
+bool kb_cg_persist(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int jacobi,
+                   unsigned int* bars, int nbars, int* err, int max_iters, int width = 0);
 template <class T>
 void kb_cg_spmv(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
 template <class T>

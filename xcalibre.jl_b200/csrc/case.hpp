@@ -126,7 +126,7 @@ struct Case {
     std::vector<cudaEvent_t> pev;  // pairs, reused per polling chunk
     double prof_ms[6] = {0, 0, 0, 0, 0, 0};
     long long prof_n[6] = {0, 0, 0, 0, 0, 0};
-    bool persistent_cg = true;  // CG (Jacobi / none) as one cooperative launch when the tiles fit
+    int persistent_cg = 1;  // CG (Jacobi / none) as one cooperative launch: 0 off, 1 auto width, else the width
     int dilu_mode = 0;          // 0 = autotuned / size rule, 1 = one-block sweeps, 2 = per-level kernels
     void prof_reserve(int pairs);
     // Steady-state polling chunks of a Krylov solve (32 CG / 8 BiCGSTAB

@@ -53,12 +53,14 @@ __device__ __forceinline__ double jl_eps(double x) {
 
 // Block tree of the canonical reduction: xor butterfly (16..1) inside each
 // warp, then butterfly (4,2,1) over the 8 warp sums.  Result valid in thread 0.
+// In blocks wider than RED_THREADS (the persistent CG's wide form) only
+// threads 0..RED_THREADS-1 contribute; every thread must call it.
 __device__ __forceinline__ double block_tree(double v, double* smem8) {
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, off);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __syncthreads();  // smem8 may still be read by a previous tree
-    if (lane == 0) smem8[warp] = v;
+    if (lane == 0 && warp < RED_THREADS / 32) smem8[warp] = v;
     __syncthreads();
     double r = 0.0;
     if (warp == 0) {
@@ -74,7 +76,8 @@ __device__ __forceinline__ double block_tree(double v, double* smem8) {
 // partials t, t+RED_THREADS, ... sequentially, then the block tree.
 __device__ __forceinline__ double reduce_partials(const double* part, int T, double* smem8) {
     double s = 0.0;
-    for (int i = threadIdx.x; i < T; i += RED_THREADS) s = s + __ldcg(part + i);
+    if (threadIdx.x < RED_THREADS)
+        for (int i = threadIdx.x; i < T; i += RED_THREADS) s = s + __ldcg(part + i);
     return block_tree(s, smem8);
 }
 

@@ -85,7 +85,23 @@ void kr_cg_rz(cudaStream_t s, int n, const T* r, const T* z, KScalars* S, double
 // bar: 2 words of barrier state, err: set when a barrier wait gave up.
 template <class T>
 bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
-                   T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters);
+                   T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters,
+                   int width = 0);
+// Persistent CG widths: 1024 / 512 threads per block (wide form, systems of
+// at most 1 / 2 tiles per SM) or RED_THREADS (narrow form).  The launchers
+// take the widest form whose co-resident capacity covers the tiles.
+constexpr int PERSIST_WIDTHS[3] = {1024, 512, 256};
+struct PersistCaps {
+    bool init = false;
+    int cap[3] = {0, 0, 0};  // co-resident blocks per width on this device
+};
+// index into PERSIST_WIDTHS of the form to launch for ntiles tiles, or -1
+// (kernels: the three instantiations in PERSIST_WIDTHS order; width 0 = the
+// widest that fits, else only that width)
+int persist_pick(PersistCaps& c, const void* const kernels[3], int ntiles, int width = 0);
+// cooperative launch of kernel (width index w) over ntiles blocks; false
+// (capacity lowered, nothing launched) when the device refuses the size
+bool persist_launch(PersistCaps& c, int w, const void* kernel, int ntiles, cudaStream_t s, void** args);
 void kr_finish(cudaStream_t s, int n, const double* x, const double* dx, double* field);
 template <class T>
 void kr_bicg_start(cudaStream_t s, int n, const T* c, const T* r, T* p, KScalars* S, double* part0, double* part1);

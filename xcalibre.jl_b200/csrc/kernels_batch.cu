@@ -130,6 +130,18 @@ __global__ void kbk_bicg_p(const BSys<T>* __restrict__ sys, const int2* tmap) {
     bicg_p_body<T>(tc, B.n, B.vec[KV_R], B.vec[KV_V], B.vec[KV_P], B.S);
 }
 
+// every system's whole CG solve in one cooperative launch: the blocks of a
+// system synchronise only among themselves (barrier state bars[2 s .. 2 s+1]),
+// so systems finish independently
+template <class T, int NT>
+__global__ void __launch_bounds__(NT, persist_min_blocks(NT))
+    kbk_cg_persist(const BSys<T>* __restrict__ sys, const int2* tmap, int jacobi, unsigned int* bars, int* err,
+                   int max_iters) {
+    XCAL_BSYS
+    cg_persist_body<T, NT>(tc, B.A, B.nz, B.P, jacobi, B.vec[KV_X], B.vec[KV_R], B.vec[KV_Z], B.vec[KV_P],
+                           B.vec[KV_V], B.S, B.part0, B.part1, bars + 2 * tm.x, err, max_iters);
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -173,6 +185,19 @@ void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int* small_ids, int n_sma
         kbk_dilu_bwd<T><<<(nr + 255) / 256, 256, 0, s>>>(sys, up_rows + up_off[l], nr, out, use_S);
         XCAL_CHECK_LAUNCH();
     }
+}
+template <class T>
+bool kb_cg_persist(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int jacobi,
+                   unsigned int* bars, int nbars, int* err, int max_iters, int width) {
+    static PersistCaps caps;
+    static const void* const kern[3] = {(const void*)kbk_cg_persist<T, 1024>, (const void*)kbk_cg_persist<T, 512>,
+                                        (const void*)kbk_cg_persist<T, RED_THREADS>};
+    const int w = persist_pick(caps, kern, ntiles_total, width);
+    if (w < 0) return false;
+    XCAL_CUDA(cudaMemsetAsync(bars, 0, 2 * (size_t)nbars * sizeof(unsigned int), s));
+    XCAL_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    void* args[] = {(void*)&sys, (void*)&tmap, &jacobi, &bars, &err, &max_iters};
+    return persist_launch(caps, w, kern[w], ntiles_total, s, args);
 }
 template <class T>
 void kb_cg_start(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total) {
@@ -222,6 +247,8 @@ void kb_bicg_p(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_
     template void kb_dilu<T>(cudaStream_t, const BSys<T>*, const int*, int, const int2*, const std::vector<int>&, \
                              const int2*, const std::vector<int>&, int, int, int);                                \
     template void kb_cg_start<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                  \
+    template bool kb_cg_persist<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, unsigned int*, int, int*,  \
+                                   int, int);                                                                     \
     template void kb_cg_spmv<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                   \
     template void kb_cg_update<T>(cudaStream_t, const BSys<T>*, const int2*, int, int);                            \
     template void kb_cg_rz<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                     \

@@ -131,175 +131,11 @@ __global__ void k_cg_rz(int n, const T* __restrict__ r, const T* __restrict__ z,
     cg_rz_body<T>(grid_tiles(), n, r, z, S, part);
 }
 
-// ---- persistent CG (Jacobi or no preconditioner) ----
-// Grid-wide barrier among the blocks of a cooperative launch (all
-// co-resident).  Bounded: a block that polls more than BAR_SPIN_LIMIT times
-// sets *err and goes on; after every barrier all blocks read *err and leave
-// the solve, so a failure ends the kernel within one more bounded wait.
-constexpr long BAR_SPIN_LIMIT = 1L << 22;
-__device__ __forceinline__ bool grid_barrier(unsigned int* count, volatile unsigned int* gen, int nblocks,
-                                             volatile int* err, int* sh_err) {
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned int g = *gen;
-        unsigned int ticket = atomicAdd(count, 1u);
-        if (ticket == (unsigned int)nblocks - 1u) {
-            *count = 0u;
-            __threadfence();
-            atomicAdd((unsigned int*)gen, 1u);
-        } else {
-            long spins = 0;
-            while (*gen == g) {
-                if (++spins > BAR_SPIN_LIMIT) {
-                    *err = 1;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        *sh_err = *err;
-    }
-    __syncthreads();
-    return *sh_err == 0;
-}
-
-// The whole CG loop of Krylov.jl cg! (Jacobi-fused update) in one launch:
-// block b owns canonical tile b; per iteration
-//   phase 1: p_k = z + beta p_{k-1} (gathered), q = A p_k for the tile's rows,
-//            q kept in shared memory, p_k stored; tile partial of <p_k, q>;
-//   barrier; every block reduces the partials (same tree) -> alpha, zero-
-//            curvature test (identical decisions in every block);
-//   phase 2: x += alpha p_k, r -= alpha q, z = P r; tile partial of <r, z>;
-//   barrier; every block reduces -> cg! stopping tests, beta.
-// The arithmetic is that of k_cg_spmv + k_cg_update; q never goes to HBM and
-// the two kernel boundaries per iteration disappear.  Block 0 writes the
-// scalar state back.  Runs at most max_iters iterations.
-template <class T>
-__global__ void __launch_bounds__(RED_THREADS, 8)
+template <class T, int NT>
+__global__ void __launch_bounds__(NT, persist_min_blocks(NT))
     k_cg_persist(CSRView A, const T* __restrict__ nz, const T* __restrict__ Pj, int jacobi, T* x, T* r, T* z, T* P0,
                  T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters) {
-    __shared__ T q_s[RED_TILE];
-    __shared__ double sm[8];
-    __shared__ double sh_d[4];
-    __shared__ int sh_i[3];
-    __shared__ int sh_err;
-    const TileCtx tc = grid_tiles();
-    const int n = A.n;
-    volatile unsigned int* gen = bar + 1;
-    int iter = S->iter, done = S->done, status = S->status;
-    const int itmax = S->itmax;
-    double gamma = S->gamma, beta = S->beta, pNorm2 = S->pNorm2, alpha = S->alpha, rNorm = S->rNorm;
-    const double eps = S->eps;
-    const double epsT = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;  // eps(T)
-    int ran = 0;
-    bool ok = true;
-    while (!done && ran < max_iters) {
-        // phase 1: q = A p_k (k_cg_spmv)
-        T* pk = (iter & 1) ? P1 : P0;
-        const T* pold = (iter & 1) ? P0 : P1;
-        const T b = (T)beta;
-        double acc = 0.0;
-        for (int k = 0; k < RED_ITEMS; ++k) {
-            int i = tile_row(tc, k);
-            if (i < n) {
-                T qi = T(0), pi;
-                const int rb = row_base(A, i), e1 = rb + SELL_C * A.len[i];
-                if (iter == 0) {
-                    for (int e = rb; e < e1; e += SELL_C) qi = qi + ld_stream(nz + e) * pk[ld_stream(A.colval + e)];
-                    pi = pk[i];
-                } else {
-                    for (int e = rb; e < e1; e += SELL_C)
-                        qi = qi + ld_stream(nz + e) * cg_dir(z, pold, b, ld_stream(A.colval + e));
-                    pi = cg_dir(z, pold, b, i);
-                    pk[i] = pi;
-                }
-                q_s[k * RED_THREADS + threadIdx.x] = qi;
-                acc = acc + (double)pi * (double)qi;
-            }
-        }
-        double tot = block_tree(acc, sm);
-        if (threadIdx.x == 0) part[tc.tile] = tot;
-        if (!(ok = grid_barrier(bar, gen, tc.ntiles, err, &sh_err))) break;
-        double pAp = reduce_partials(part, tc.ntiles, sm);
-        if (threadIdx.x == 0) {
-            double lim = epsT * pNorm2;
-            sh_i[0] = (pAp <= lim && fabs(pAp) <= lim) ? 1 : 0;
-            sh_d[0] = gamma / pAp;
-        }
-        __syncthreads();
-        if (sh_i[0]) {
-            done = 1;
-            status = KS_ZERO_CURV;
-            break;
-        }
-        alpha = sh_d[0];
-        // phase 2: x, r, z and <r, z> (k_cg_update, Jacobi fused)
-        const T a = (T)alpha;
-        double acc2 = 0.0;
-        for (int k = 0; k < RED_ITEMS; ++k) {
-            int i = tile_row(tc, k);
-            if (i < n) {
-                __stcs(x + i, ld_stream(x + i) + a * pk[i]);
-                T ri = r[i] + (-a) * q_s[k * RED_THREADS + threadIdx.x];
-                r[i] = ri;
-                T zi = jacobi ? ld_stream(Pj + i) * ri : ri;
-                if (jacobi) z[i] = zi;
-                acc2 = acc2 + (double)ri * (double)zi;
-            }
-        }
-        double tot2 = block_tree(acc2, sm);
-        if (threadIdx.x == 0) part2[tc.tile] = tot2;
-        if (!(ok = grid_barrier(bar, gen, tc.ntiles, err, &sh_err))) break;
-        double g = reduce_partials(part2, tc.ntiles, sm);
-        if (threadIdx.x == 0) {  // cg_finalize on the block's copy of the state
-            double rn = sqrt(g);
-            bool mach = (rn + 1.0 <= 1.0);
-            bool solved = (rn <= eps) || mach;
-            double bt = beta, pn = pNorm2, gm = gamma;
-            if (!solved) {
-                bt = g / gamma;
-                pn = g + (bt * bt) * pNorm2;
-                gm = g;
-            }
-            int it1 = iter + 1;
-            int dn = 0, stt = status;
-            if (solved) {
-                dn = 1;
-                stt = KS_SOLVED;
-            } else if (it1 >= itmax) {
-                dn = 1;
-                stt = KS_TIRED;
-            }
-            sh_d[0] = rn;
-            sh_d[1] = bt;
-            sh_d[2] = pn;
-            sh_d[3] = gm;
-            sh_i[0] = it1;
-            sh_i[1] = dn;
-            sh_i[2] = stt;
-        }
-        __syncthreads();
-        rNorm = sh_d[0];
-        beta = sh_d[1];
-        pNorm2 = sh_d[2];
-        gamma = sh_d[3];
-        iter = sh_i[0];
-        done = sh_i[1];
-        status = sh_i[2];
-        ++ran;
-    }
-    if (ok && blockIdx.x == 0 && threadIdx.x == 0) {
-        S->iter = iter;
-        S->done = done;
-        S->status = status;
-        S->gamma = gamma;
-        S->beta = beta;
-        S->pNorm2 = pNorm2;
-        S->alpha = alpha;
-        S->rNorm = rNorm;
-    }
+    cg_persist_body<T, NT>(grid_tiles(), A, nz, Pj, jacobi, x, r, z, P0, P1, S, part, part2, bar, err, max_iters);
 }
 
 // field = x + dx (warm start shift)
@@ -645,44 +481,65 @@ void kr_cg_spmv(cudaStream_t s, const CSRView& A, const T* nz, const T* z, T* P0
     k_cg_spmv<T><<<TILE_LAUNCH(A.n), s>>>(A, nz, z, P0, P1, q, S, part);
     XCAL_CHECK_LAUNCH();
 }
-template <class T>
-bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
-                   T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters) {
-    static int max_blocks = -1;  // co-resident blocks of this instantiation (per process, one device type)
-    if (max_blocks < 0) {
-        int dev = 0, sms = 0, per = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg_persist<T>, RED_THREADS, 0) != cudaSuccess) {
-            cudaGetLastError();
-            max_blocks = 0;
-        } else {
-            max_blocks = per * sms;
+static_assert(PERSIST_WIDTHS[2] == RED_THREADS, "narrow persistent form is one canonical tile row set per thread");
+
+int persist_pick(PersistCaps& c, const void* const k[3], int ntiles, int width) {
+    if (!c.init) {
+        c.init = true;
+        int dev = 0, sms = 0;
+        bool okd = cudaGetDevice(&dev) == cudaSuccess &&
+                   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
+        for (int w = 0; w < 3; ++w) {
+            int per = 0;
+            if (!okd || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k[w], PERSIST_WIDTHS[w], 0) != cudaSuccess) {
+                cudaGetLastError();
+                per = 0;
+            }
+            c.cap[w] = per * sms;
         }
     }
-    const int nt = tiles(A.n);
-    if (nt > max_blocks) return false;
-    XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
-    XCAL_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    if (ntiles <= 0) return -1;
+    for (int w = 0; w < 3; ++w)
+        if ((width == 0 || width == PERSIST_WIDTHS[w]) && ntiles <= c.cap[w]) return w;
+    return -1;
+}
+
+bool persist_launch(PersistCaps& c, int w, const void* kernel, int ntiles, cudaStream_t s, void** args) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nt);
-    cfg.blockDim = dim3(RED_THREADS);
+    cfg.gridDim = dim3(ntiles);
+    cfg.blockDim = dim3(PERSIST_WIDTHS[w]);
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeCooperative;
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k_cg_persist<T>, A, nz, P, jacobi, x, r, z, P0, P1, S, part, part2, bar,
-                                       err, max_iters);
+    cudaError_t e = cudaLaunchKernelExC(&cfg, kernel, args);
     if (e == cudaErrorCooperativeLaunchTooLarge) {
         cudaGetLastError();
-        max_blocks = nt - 1;
+        c.cap[w] = ntiles - 1;
         return false;
     }
     XCAL_CUDA(e);
     XCAL_CHECK_LAUNCH();
     return true;
+}
+
+template <class T>
+bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
+                   T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters,
+                   int width) {
+    static PersistCaps caps;  // co-resident blocks per width (per process, one device type)
+    static const void* const kern[3] = {(const void*)k_cg_persist<T, 1024>, (const void*)k_cg_persist<T, 512>,
+                                        (const void*)k_cg_persist<T, RED_THREADS>};
+    const int nt = tiles(A.n);
+    const int w = persist_pick(caps, kern, nt, width);
+    if (w < 0) return false;
+    XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
+    XCAL_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    CSRView Av = A;
+    void* args[] = {&Av, (void*)&nz, (void*)&P, &jacobi, &x, &r, &z, &P0, &P1, &S, &part, &part2, &bar, &err, &max_iters};
+    return persist_launch(caps, w, kern[w], nt, s, args);
 }
 template <class T>
 void kr_cg_update(cudaStream_t s, int n, T* x, const T* P0, const T* P1, T* r, const T* q, T* z, const T* P,
@@ -838,7 +695,7 @@ void kr_record(cudaStream_t s, const KScalars* S, int* out) {
                                   KScalars*, double*);                                                          \
     template void kr_cg_rz<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*);                        \
     template bool kr_cg_persist<T>(cudaStream_t, const CSRView&, const T*, const T*, int, T*, T*, T*, T*, T*,    \
-                                   KScalars*, double*, double*, unsigned int*, int*, int);                      \
+                                   KScalars*, double*, double*, unsigned int*, int*, int, int);                 \
     template void kr_bicg_start<T>(cudaStream_t, int, const T*, const T*, T*, KScalars*, double*, double*);      \
     template void kr_bicg_alpha<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*);                   \
     template void kr_bicg_s<T>(cudaStream_t, int, const T*, const T*, const T*, T*, T*, const KScalars*);        \

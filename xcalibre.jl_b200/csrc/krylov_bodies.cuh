@@ -511,4 +511,281 @@ __device__ __forceinline__ void dilu_D_row(const CSRView& A, const double* __res
     D[i] = d;
 }
 
+// ---- persistent CG (Jacobi or no preconditioner) ----
+// Grid-wide barrier among the nblocks co-resident blocks of one system.
+// `count` only grows during a launch (zeroed before it): barrier number nb
+// completes when it reaches (nb + 1) * nblocks, so there is no reset and no
+// second atomic.  Thread 0 alone fences (release before its arrival, acquire
+// after the wait); __syncthreads orders the rest of the block around it.  A
+// single-block system needs no more than the __syncthreads.  Bounded: a
+// block that polls more than BAR_SPIN_LIMIT times, or sees *err set by
+// another block, returns false (and sets *err), so a failure ends every
+// block within one bounded wait.
+constexpr long BAR_SPIN_LIMIT = 1L << 22;
+__device__ __forceinline__ bool grid_barrier(unsigned int* count, int nblocks, unsigned int& nb, int* err,
+                                             int* sh_err) {
+    __syncthreads();
+    if (nblocks == 1) return true;
+    if (threadIdx.x == 0) {
+        const unsigned int target = (nb + 1u) * (unsigned int)nblocks;
+        __threadfence();
+        atomicAdd(count, 1u);
+        long spins = 0;
+        int e = 0;
+        while ((int)(*(volatile unsigned int*)count - target) < 0) {
+            if (++spins > BAR_SPIN_LIMIT) {
+                e = 1;
+                *(volatile int*)err = 1;
+                break;
+            }
+            if ((spins & 255) == 0 && *(volatile int*)err) {
+                e = 1;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+        *sh_err = e;
+    }
+    ++nb;
+    __syncthreads();
+    return *sh_err == 0;
+}
+
+// q_i = sum_k nz[i,k] * d[col(i,k)] in slot order, d = p (first iteration) or
+// z + beta p_old gathered on the fly: the first 8 slots' loads are issued
+// together, the products are then added in slot order (wide form only; the
+// narrow form keeps the plain loop, which needs fewer registers).
+template <class T, bool FIRST>
+__device__ __forceinline__ T cg_row_q(const CSRView& A, const T* __restrict__ nz, const T* z, const T* pold,
+                                      const T* pk, T b, int i) {
+    const int rb = row_base(A, i), ln = A.len[i];
+    T qi = T(0);
+    int c[8];
+    T v[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+        if (t < ln) {
+            c[t] = ld_stream(A.colval + rb + SELL_C * t);
+            v[t] = ld_stream(nz + rb + SELL_C * t);
+        }
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+        if (t < ln) qi = qi + v[t] * (FIRST ? pk[c[t]] : cg_dir(z, pold, b, c[t]));
+    for (int t = 8; t < ln; ++t) {
+        const int s = rb + SELL_C * t;
+        const int cc = ld_stream(A.colval + s);
+        qi = qi + ld_stream(nz + s) * (FIRST ? pk[cc] : cg_dir(z, pold, b, cc));
+    }
+    return qi;
+}
+
+// The whole CG loop of Krylov.jl cg! (Jacobi-fused update) for one system,
+// run by its ntiles blocks (block with tile t owns canonical tile t); per
+// iteration
+//   phase 1: p_k = z + beta p_{k-1} (gathered), q = A p_k for the tile's rows,
+//            q kept in shared memory, p_k stored; tile partial of <p_k, q>;
+//   barrier; every block reduces the partials (same tree) -> alpha, zero-
+//            curvature test (identical decisions in every block);
+//   phase 2: x += alpha p_k, r -= alpha q, z = P r; tile partial of <r, z>;
+//   barrier; every block reduces -> cg! stopping tests, beta.
+// The arithmetic is that of k_cg_spmv + k_cg_update; q never goes to HBM and
+// the two kernel boundaries per iteration disappear.  The block of tile 0
+// writes the scalar state back.  Runs at most max_iters iterations.  The
+// barriers count only this system's blocks, so in a batched launch every
+// system runs (and finishes) on its own.
+//
+// NT threads per block.  NT = RED_THREADS (narrow): thread t owns the tile's
+// rows t + 256 k, k < 8, and accumulates its partial as it goes -- few
+// registers, so 7-8 blocks fit an SM and a 2M-row system is co-resident.
+// NT = 512 / 1024 (wide, for systems of at most 2 / 1 tiles per SM): thread
+// t covers rows (t mod 256) + 256 k for NT/256 times fewer k, writes each
+// row's product to shared memory, and threads 0..255 then add the products
+// of "their" rows in k order -- the same partials, bit for bit, with a 4-8x
+// shorter dependent-load chain per thread.
+// __launch_bounds__ minimum blocks per SM of each form: 64 registers for the
+// wide forms, 32 for the narrow one (8 blocks of 256 threads per SM)
+constexpr int persist_min_blocks(int nt) { return nt == 1024 ? 1 : nt == 512 ? 2 : 8; }
+
+template <class T, int NT>
+__device__ __forceinline__ void cg_persist_body(const TileCtx& tc, const CSRView& A, const T* __restrict__ nz,
+                                                const T* __restrict__ Pj, int jacobi, T* x, T* r, T* z, T* P0,
+                                                T* P1, KScalars* S, double* part, double* part2, unsigned int* bar,
+                                                int* err, int max_iters) {
+    constexpr bool WIDE = NT > RED_THREADS;
+    constexpr int IPT = RED_ITEMS / (NT / RED_THREADS);  // rows per thread
+    __shared__ T q_s[RED_TILE];
+    __shared__ double pr_s[WIDE ? RED_TILE : 1];
+    __shared__ double sm[8];
+    __shared__ double sh_d[4];
+    __shared__ int sh_i[3];
+    __shared__ int sh_err;
+    const int n = A.n;
+    const int v = threadIdx.x & (RED_THREADS - 1), k0 = (threadIdx.x / RED_THREADS) * IPT;
+    int iter = S->iter, done = S->done, status = S->status;
+    const int itmax = S->itmax;
+    double gamma = S->gamma, beta = S->beta, pNorm2 = S->pNorm2, alpha = S->alpha, rNorm = S->rNorm;
+    const double eps = S->eps;
+    const double epsT = sizeof(T) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;  // eps(T)
+    int ran = 0;
+    unsigned int nb = 0;
+    bool ok = true;
+    while (!done && ran < max_iters) {
+        // phase 1: q = A p_k (k_cg_spmv)
+        T* pk = (iter & 1) ? P1 : P0;
+        const T* pold = (iter & 1) ? P0 : P1;
+        const T b = (T)beta;
+        double acc = 0.0;
+        if constexpr (!WIDE) {
+            for (int k = 0; k < RED_ITEMS; ++k) {
+                int i = tile_row(tc, k);
+                if (i < n) {
+                    T qi = T(0), pi;
+                    const int rb = row_base(A, i), e1 = rb + SELL_C * A.len[i];
+                    if (iter == 0) {
+                        for (int e = rb; e < e1; e += SELL_C)
+                            qi = qi + ld_stream(nz + e) * pk[ld_stream(A.colval + e)];
+                        pi = pk[i];
+                    } else {
+                        for (int e = rb; e < e1; e += SELL_C)
+                            qi = qi + ld_stream(nz + e) * cg_dir(z, pold, b, ld_stream(A.colval + e));
+                        pi = cg_dir(z, pold, b, i);
+                        pk[i] = pi;
+                    }
+                    q_s[k * RED_THREADS + threadIdx.x] = qi;
+                    acc = acc + (double)pi * (double)qi;
+                }
+            }
+        } else {
+            // rows past n contribute 0.0 to the k-ordered sums below: the
+            // narrow form skips them, and x + 0.0 == x for every partial
+            // sum that starts at +0.0 (it can never be -0.0)
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                const int k = k0 + j, i = tc.tile * RED_TILE + k * RED_THREADS + v;
+                double prod = 0.0;
+                if (i < n) {
+                    T qi, pi;
+                    if (iter == 0) {
+                        qi = cg_row_q<T, true>(A, nz, z, pold, pk, b, i);
+                        pi = pk[i];
+                    } else {
+                        qi = cg_row_q<T, false>(A, nz, z, pold, pk, b, i);
+                        pi = cg_dir(z, pold, b, i);
+                        pk[i] = pi;
+                    }
+                    q_s[k * RED_THREADS + v] = qi;
+                    prod = (double)pi * (double)qi;
+                }
+                pr_s[k * RED_THREADS + v] = prod;
+            }
+            __syncthreads();
+            if (threadIdx.x < RED_THREADS)
+#pragma unroll
+                for (int k = 0; k < RED_ITEMS; ++k) acc = acc + pr_s[k * RED_THREADS + v];
+        }
+        double tot = block_tree(acc, sm);
+        if (threadIdx.x == 0) part[tc.tile] = tot;
+        if (!(ok = grid_barrier(bar, tc.ntiles, nb, err, &sh_err))) break;
+        double pAp = reduce_partials(part, tc.ntiles, sm);
+        if (threadIdx.x == 0) {
+            double lim = epsT * pNorm2;
+            sh_i[0] = (pAp <= lim && fabs(pAp) <= lim) ? 1 : 0;
+            sh_d[0] = gamma / pAp;
+        }
+        __syncthreads();
+        if (sh_i[0]) {
+            done = 1;
+            status = KS_ZERO_CURV;
+            break;
+        }
+        alpha = sh_d[0];
+        // phase 2: x, r, z and <r, z> (k_cg_update, Jacobi fused)
+        const T a = (T)alpha;
+        double acc2 = 0.0;
+        if constexpr (!WIDE) {
+            for (int k = 0; k < RED_ITEMS; ++k) {
+                int i = tile_row(tc, k);
+                if (i < n) {
+                    __stcs(x + i, ld_stream(x + i) + a * pk[i]);
+                    T ri = r[i] + (-a) * q_s[k * RED_THREADS + threadIdx.x];
+                    r[i] = ri;
+                    T zi = jacobi ? ld_stream(Pj + i) * ri : ri;
+                    if (jacobi) z[i] = zi;
+                    acc2 = acc2 + (double)ri * (double)zi;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                const int k = k0 + j, i = tc.tile * RED_TILE + k * RED_THREADS + v;
+                double prod = 0.0;
+                if (i < n) {
+                    __stcs(x + i, ld_stream(x + i) + a * pk[i]);
+                    T ri = r[i] + (-a) * q_s[k * RED_THREADS + v];
+                    r[i] = ri;
+                    T zi = jacobi ? ld_stream(Pj + i) * ri : ri;
+                    if (jacobi) z[i] = zi;
+                    prod = (double)ri * (double)zi;
+                }
+                pr_s[k * RED_THREADS + v] = prod;
+            }
+            __syncthreads();
+            if (threadIdx.x < RED_THREADS)
+#pragma unroll
+                for (int k = 0; k < RED_ITEMS; ++k) acc2 = acc2 + pr_s[k * RED_THREADS + v];
+        }
+        double tot2 = block_tree(acc2, sm);
+        if (threadIdx.x == 0) part2[tc.tile] = tot2;
+        if (!(ok = grid_barrier(bar, tc.ntiles, nb, err, &sh_err))) break;
+        double g = reduce_partials(part2, tc.ntiles, sm);
+        if (threadIdx.x == 0) {  // cg_finalize on the block's copy of the state
+            double rn = sqrt(g);
+            bool mach = (rn + 1.0 <= 1.0);
+            bool solved = (rn <= eps) || mach;
+            double bt = beta, pn = pNorm2, gm = gamma;
+            if (!solved) {
+                bt = g / gamma;
+                pn = g + (bt * bt) * pNorm2;
+                gm = g;
+            }
+            int it1 = iter + 1;
+            int dn = 0, stt = status;
+            if (solved) {
+                dn = 1;
+                stt = KS_SOLVED;
+            } else if (it1 >= itmax) {
+                dn = 1;
+                stt = KS_TIRED;
+            }
+            sh_d[0] = rn;
+            sh_d[1] = bt;
+            sh_d[2] = pn;
+            sh_d[3] = gm;
+            sh_i[0] = it1;
+            sh_i[1] = dn;
+            sh_i[2] = stt;
+        }
+        __syncthreads();
+        rNorm = sh_d[0];
+        beta = sh_d[1];
+        pNorm2 = sh_d[2];
+        gamma = sh_d[3];
+        iter = sh_i[0];
+        done = sh_i[1];
+        status = sh_i[2];
+        ++ran;
+    }
+    if (ok && tc.tile == 0 && threadIdx.x == 0) {
+        S->iter = iter;
+        S->done = done;
+        S->status = status;
+        S->gamma = gamma;
+        S->beta = beta;
+        S->pNorm2 = pNorm2;
+        S->alpha = alpha;
+        S->rNorm = rNorm;
+    }
+}
+
 }  // namespace xcal
