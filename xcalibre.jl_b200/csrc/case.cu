@@ -1031,7 +1031,8 @@ void Case::krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz,
         T* zz = pt == XCAL_PRECOND_NONE ? V.r : V.z;
         if (kr_cg_persist(stream, E.view(), nz, P, pt == XCAL_PRECOND_JACOBI ? 1 : 0, V.x, V.r, zz, V.p, V.v, S,
                           ws.part0.p, ws.part1.p, ws.bar.p, ws.err.p, hS->itmax + 1,
-                          persistent_cg > 1 ? persistent_cg : 0)) {
+                          persistent_cg > 1 ? persistent_cg : 0,
+                          E.nnz * (long)(sizeof(T) + 4) <= PERSIST_PF_MAX_BYTES ? 256 : 0)) {
             if (profiling) XCAL_CUDA(cudaEventRecord(ev[6], stream));
             int errflag = 0;
             XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));

@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(NT, persist_min_blocks(NT))
                    int max_iters) {
     XCAL_BSYS
     cg_persist_body<T, NT>(tc, B.A, B.nz, B.P, jacobi, B.vec[KV_X], B.vec[KV_R], B.vec[KV_Z], B.vec[KV_P],
-                           B.vec[KV_V], B.S, B.part0, B.part1, bars + 2 * tm.x, err, max_iters);
+                           B.vec[KV_V], B.S, B.part0, B.part1, bars + 2 * tm.x, err, max_iters, 0);
 }
 
 // ---------------------------------------------------------------------------

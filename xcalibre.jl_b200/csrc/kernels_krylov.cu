@@ -134,8 +134,10 @@ __global__ void k_cg_rz(int n, const T* __restrict__ r, const T* __restrict__ z,
 template <class T, int NT>
 __global__ void __launch_bounds__(NT, persist_min_blocks(NT))
     k_cg_persist(CSRView A, const T* __restrict__ nz, const T* __restrict__ Pj, int jacobi, T* x, T* r, T* z, T* P0,
-                 T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters) {
-    cg_persist_body<T, NT>(grid_tiles(), A, nz, Pj, jacobi, x, r, z, P0, P1, S, part, part2, bar, err, max_iters);
+                 T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters,
+                 int pf_kb) {
+    cg_persist_body<T, NT>(grid_tiles(), A, nz, Pj, jacobi, x, r, z, P0, P1, S, part, part2, bar, err, max_iters,
+                           pf_kb);
 }
 
 // field = x + dx (warm start shift)
@@ -528,7 +530,7 @@ bool persist_launch(PersistCaps& c, int w, const void* kernel, int ntiles, cudaS
 template <class T>
 bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
                    T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters,
-                   int width) {
+                   int width, int pf_kb) {
     static PersistCaps caps;  // co-resident blocks per width (per process, one device type)
     static const void* const kern[3] = {(const void*)k_cg_persist<T, 1024>, (const void*)k_cg_persist<T, 512>,
                                         (const void*)k_cg_persist<T, RED_THREADS>};
@@ -538,7 +540,9 @@ bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, in
     XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
     XCAL_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     CSRView Av = A;
-    void* args[] = {&Av, (void*)&nz, (void*)&P, &jacobi, &x, &r, &z, &P0, &P1, &S, &part, &part2, &bar, &err, &max_iters};
+    void* args[] = {&Av, (void*)&nz, (void*)&P, &jacobi, &x,         &r,    &z,
+                    &P0, &P1,        &S,        &part,   &part2,     &bar,  &err,
+                    &max_iters, &pf_kb};
     return persist_launch(caps, w, kern[w], nt, s, args);
 }
 template <class T>
@@ -695,7 +699,7 @@ void kr_record(cudaStream_t s, const KScalars* S, int* out) {
                                   KScalars*, double*);                                                          \
     template void kr_cg_rz<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*);                        \
     template bool kr_cg_persist<T>(cudaStream_t, const CSRView&, const T*, const T*, int, T*, T*, T*, T*, T*,    \
-                                   KScalars*, double*, double*, unsigned int*, int*, int, int);                 \
+                                   KScalars*, double*, double*, unsigned int*, int*, int, int, int);            \
     template void kr_bicg_start<T>(cudaStream_t, int, const T*, const T*, T*, KScalars*, double*, double*);      \
     template void kr_bicg_alpha<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*);                   \
     template void kr_bicg_s<T>(cudaStream_t, int, const T*, const T*, const T*, T*, T*, const KScalars*);        \

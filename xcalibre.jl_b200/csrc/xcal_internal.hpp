@@ -133,6 +133,10 @@ constexpr int SELL_C = 32;
 constexpr int DILU_BLOCK_MAX_ROWS = 65536;
 // FP32 (mixed-precision inner) CG runs as one cooperative launch up to this size
 constexpr int PERSIST_FP32_MAX_ROWS = 262144;
+// persistent CG, narrow form: prefetch a tile's matrix slots into L2 during
+// the second barrier when all slots (values + columns) take at most this many
+// bytes (measured: faster for a 74 MB matrix, slower for 117 and 175 MB)
+constexpr long PERSIST_PF_MAX_BYTES = 80L << 20;
 struct CSRView {
     int n;
     const int* slice;          // [ceil(n/32)+1] first slot of each slice
