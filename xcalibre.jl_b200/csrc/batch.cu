@@ -294,19 +294,17 @@ struct Batch {
         }
         int itmax = 0;
         for (int i : members) itmax = std::max(itmax, hS[i].itmax);
-        // every member's whole CG loop in one cooperative launch (the single
-        // case path's policy: FP64 always, FP32 up to PERSIST_FP32_MAX_ROWS)
+        // every member's whole CG loop in one cooperative launch (falls
+        // through to the batched two-kernel loop when the tiles of all
+        // members cannot be co-resident)
         if (cg && (pt == XCAL_PRECOND_JACOBI || pt == XCAL_PRECOND_NONE)) {
-            bool size_ok = true;
-            if (sizeof(T) == 4)
-                for (int i : members) size_ok = size_ok && cases[i]->U.n <= PERSIST_FP32_MAX_ROWS;
             bool all_persist = true;
             int width = 0;  // a block form the members ask for (tests), else the widest that fits
             for (int i : members) {
                 all_persist = all_persist && cases[i]->persistent_cg != 0;
                 if (cases[i]->persistent_cg > 1) width = cases[i]->persistent_cg;
             }
-            if (size_ok && all_persist &&
+            if (all_persist &&
                 kb_cg_persist<T>(stream, sy, tm, nt, pt == XCAL_PRECOND_JACOBI ? 1 : 0, bars.p, (int)cases.size(),
                                  perr.p, itmax + 1, width)) {
                 int errflag = 0;

@@ -1020,12 +1020,10 @@ void Case::krylov_iterate(Equation& E, const xcal_solver_setup& SS, const T* nz,
             if (!e) XCAL_CUDA(cudaEventCreate(&e));
     krylov_start(E, SS, nz, P, c, r0, V, S);
     // the whole loop in one cooperative launch (falls through when the
-    // system's tiles cannot all be co-resident).  Measured on B200: FP64
-    // faster at every size tried (6.4k-2.1M cells, 2-15%); FP32 faster up to
-    // ~0.2M cells and slower from 1M (the FP32 update phase loses the
-    // loads-first form of its own kernel), hence the FP32 size limit.
-    const bool persist_size = sizeof(T) == 8 || E.n <= PERSIST_FP32_MAX_ROWS;
-    if (cg && persistent_cg && persist_size && (pt == XCAL_PRECOND_JACOBI || pt == XCAL_PRECOND_NONE)) {
+    // system's tiles cannot all be co-resident).  Measured on B200 against
+    // the two-kernel loop: faster at every size tried (1.2k-2.1M cells), in
+    // FP64 and FP32 (2.1M cells, FP32: 51.7 vs 59 us per iteration).
+    if (cg && persistent_cg && (pt == XCAL_PRECOND_JACOBI || pt == XCAL_PRECOND_NONE)) {
         const int it0 = 0;
         if (profiling) XCAL_CUDA(cudaEventRecord(ev[5], stream));
         T* zz = pt == XCAL_PRECOND_NONE ? V.r : V.z;

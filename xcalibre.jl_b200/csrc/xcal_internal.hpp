@@ -131,8 +131,6 @@ constexpr int SELL_C = 32;
 // systems up to this many rows apply DILU (and build its factor) in one
 // block, level after level, instead of one launch per level
 constexpr int DILU_BLOCK_MAX_ROWS = 65536;
-// FP32 (mixed-precision inner) CG runs as one cooperative launch up to this size
-constexpr int PERSIST_FP32_MAX_ROWS = 262144;
 // persistent CG, narrow form: prefetch a tile's matrix slots into L2 during
 // the second barrier when all slots (values + columns) take at most this many
 // bytes (measured: faster for a 74 MB matrix, slower for 117 and 175 MB)
