@@ -43,6 +43,7 @@ struct Batch {
     std::vector<int> dlo_off[2], dup_off[2];
     DBuf<int> small_ids;             // systems that run DILU as one block
     int n_small = 0;
+    int small_n = 0;                 // rows of the largest of them
     DBuf<unsigned int> bars;         // persistent CG: barrier state per system
     DBuf<int> perr;                  // persistent CG: a barrier wait gave up
     std::vector<int2> h_tmap;
@@ -193,12 +194,8 @@ struct Batch {
                 for (int k = 0; k < KV_COUNT; ++k) B.vec[k] = v[k];
             }
             if (SS.solver == XCAL_SOLVER_CG && SS.precond == XCAL_PRECOND_NONE) B.vec[KV_Z] = B.vec[KV_R];
-            B.lo_rows = E.d_lower_rows.p;
-            B.lo_off = E.d_lower_off.p;
-            B.up_rows = E.d_upper_rows.p;
-            B.up_off = E.d_upper_off.p;
-            B.n_lo = E.lower_off.empty() ? 0 : (int)E.lower_off.size() - 1;
-            B.n_up = E.upper_off.empty() ? 0 : (int)E.upper_off.size() - 1;
+            B.lo = level_view<T>(E, 0);
+            B.up = level_view<T>(E, 1);
         }
         sys[prec][slot].upload((const unsigned char*)h.data(), h.size() * sizeof(BSys<T>), stream);
     }
@@ -225,8 +222,12 @@ struct Batch {
             }
             // small systems: one block per DILU application
             std::vector<int> ids;
+            small_n = 0;
             for (int i = 0; i < nc; ++i)
-                if (cases[i]->U.dilu_block()) ids.push_back(i);
+                if (cases[i]->U.dilu_block()) {
+                    ids.push_back(i);
+                    small_n = std::max(small_n, cases[i]->U.n);
+                }
             n_small = (int)ids.size();
             if (ids.empty()) ids.push_back(0);
             small_ids.upload(ids, stream);
@@ -271,7 +272,8 @@ struct Batch {
         if (pt == XCAL_PRECOND_JACOBI)
             kb_jacobi_apply<T>(stream, sy, tm, nt, in, out, use_S);
         else if (pt == XCAL_PRECOND_DILU)
-            kb_dilu<T>(stream, sy, small_ids.p, n_small, dlo[e].p, dlo_off[e], dup[e].p, dup_off[e], in, out, use_S);
+            kb_dilu<T>(stream, sy, small_ids.p, n_small, small_n, dlo[e].p, dlo_off[e], dup[e].p, dup_off[e], in, out,
+                       use_S);
         else
             kb_copy<T>(stream, sy, tm, nt, in, out, use_S);
     }
@@ -404,8 +406,10 @@ struct Batch {
             XCAL_CUDA(cudaMemcpyAsync(S.p, hS, nc * sizeof(KScalars), cudaMemcpyHostToDevice, stream));
             for (Case* c : cases) {
                 Equation& E = isU ? c->U : c->P;
+                const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
                 const double* b = isU ? c->U.b[comp].p : c->P.b[0].p;
                 double* field = isU ? c->Uc[comp].p : c->p.p;
+                if (SS.precond == XCAL_PRECOND_DILU) c->dilu_refresh(E, false);
                 kr_init_resid(stream, E.view(), E.nz.p, b, field, c->ws.dx.p, c->ws.x.p,
                               SS0.solver == XCAL_SOLVER_CG ? c->ws.r.p : c->ws.q.p);
             }
@@ -422,6 +426,7 @@ struct Batch {
                 const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
                 kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
                 if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, E.n, E.P.p, E.P32.p);
+                if (SS.precond == XCAL_PRECOND_DILU) c->dilu_refresh(E, true);
             }
             std::vector<char> active(nc, 1);
             std::vector<int> total(nc, 0);
@@ -571,8 +576,10 @@ size_t estimate_case_bytes(long nC, long nF, long nB, int mixed, int dilu_U, int
             // level lists and offsets, and the level-ordered triangles: per
             // off-diagonal slot column, source slot, value [+ fp32 value]
             b += 8.0 * nC + 16.0 * nC;
-            // (SELL padding of the level order: up to half again)
+            // (SELL padding of the level order: up to half again), and 1/D
+            // per lower slot [+ fp32]
             b += (nnz - nC) * 1.5 * (16.0 + (mixed ? 4.0 : 0.0)) + 2.0 * nC + 8.0 * (nC / 32 + 2);
+            b += (nnz - nC) * 0.5 * 1.5 * (8.0 + (mixed ? 4.0 : 0.0));
         }
     }
     // three boundary-condition tables (85 bytes per boundary face) + partner lists

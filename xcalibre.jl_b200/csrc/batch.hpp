@@ -8,6 +8,7 @@
 // the single-case ones, so a case's result does not depend on the batch it
 // ran in.
 #pragma once
+#include "kernels.hpp"
 #include "xcal_internal.hpp"
 
 namespace xcal {
@@ -38,12 +39,8 @@ struct BSys {
     double* part1;
     int n;
     int ntiles;
-    // DILU level schedule (one-block sweeps of small systems)
-    const int* lo_rows;
-    const int* lo_off;
-    const int* up_rows;
-    const int* up_off;
-    int n_lo, n_up;
+    // level-ordered triangles (one-block DILU sweeps of small systems)
+    LevelView<T> lo, up;
 };
 
 // batched launchers (kernels_batch.cu); tmap has ntiles_total entries
@@ -55,9 +52,11 @@ void kb_jacobi_apply(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int n
 template <class T>
 void kb_copy(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int in, int out, int use_S);
 // DILU application: systems listed in small_ids (n <= DILU_BLOCK_MAX_ROWS)
-// one block each, the others level by level over merged (system, row) lists
+// one block each over their level-ordered triangles (y in shared memory when
+// the largest of them, small_n rows, fits), the others level by level over
+// merged (system, row) lists
 template <class T>
-void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int* small_ids, int n_small, const int2* lo_rows,
+void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int* small_ids, int n_small, int small_n, const int2* lo_rows,
              const std::vector<int>& lo_off, const int2* up_rows, const std::vector<int>& up_off, int in, int out,
              int use_S);
 template <class T>

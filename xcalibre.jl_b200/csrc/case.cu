@@ -505,6 +505,10 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
             L.src.upload(src, s);
             L.val.alloc(std::max(L.nslots, 1L));
             L.val.zero(s);
+            if (tri == 0) {
+                L.dinv.alloc(std::max(L.nslots, 1L));
+                L.dinv.zero(s);
+            }
         }
     }
 }
@@ -683,6 +687,10 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
                 if (L->nslots > 0) {
                     L->val32.alloc(L->nslots);
                     L->val32.zero(stream);
+                    if (L == &E->lsell) {
+                        L->dinv32.alloc(L->nslots);
+                        L->dinv32.zero(stream);
+                    }
                 }
         }
     }
@@ -897,28 +905,28 @@ void Case::update_precond(int eqn) {
 
 template <class T>
 void Case::dilu_ldiv(Equation& E, const T* nz, const T* D, const T* b, T* out, const KScalars* S) {
-    CSRView A = E.view();
+    // both paths read the level-ordered triangles (values and 1/D refreshed
+    // by dilu_refresh before the solve); nz is the matrix those mirror
+    (void)nz;
     if (E.dilu_block()) {
-        kr_dilu_block(stream, A, nz, D, b, out, E.d_lower_rows.p, E.d_lower_off.p, (int)E.lower_off.size() - 1,
-                      E.d_upper_rows.p, E.d_upper_off.p, (int)E.upper_off.size() - 1, S);
+        kr_dilu_block(stream, E.n, level_view<T>(E, 0), level_view<T>(E, 1), D, b, out, S);
         return;
     }
-    // level kernels over the level-ordered triangles (values refreshed by
-    // dilu_refresh before the solve)
-    const T* lv = sizeof(T) == 8 ? (const T*)E.lsell.val.p : (const T*)E.lsell.val32.p;
+    const LevelView<T> lo = level_view<T>(E, 0);
     const T* uv = sizeof(T) == 8 ? (const T*)E.usell.val.p : (const T*)E.usell.val32.p;
     for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
         kr_dilu_fwd_lv(stream, E.lower_off[l], E.lower_off[l + 1], E.d_lower_rows.p, E.lsell.slice.p, E.lsell.cnt.p,
-                       E.lsell.col.p, lv, D, b, out, S);
+                       E.lsell.col.p, lo.val, lo.dinv, b, out, S);
     for (size_t l = 0; l + 1 < E.upper_off.size(); ++l)
         kr_dilu_bwd_lv(stream, E.upper_off[l], E.upper_off[l + 1], E.d_upper_rows.p, E.usell.slice.p, E.usell.cnt.p,
                        E.usell.col.p, uv, D, out, S);
 }
 
-// copy the current off-diagonal values into the level-ordered triangles
-// (FP64 values, or the FP32 copy nz32 for the mixed inner solves)
+// copy the current off-diagonal values into the level-ordered triangles and
+// form the lower triangle's 1/D per slot (FP64 values and D, or the FP32
+// copies nz32 / P32 for the mixed inner solves); D must be current
 void Case::dilu_refresh(Equation& E, bool fp32) {
-    if (E.dilu_block() || E.lower_off.empty()) return;
+    if (E.lower_off.empty()) return;
     for (LevelSell* L : {&E.lsell, &E.usell}) {
         if (fp32) {
             kr_gather_vals(stream, L->nslots, L->src.p, E.nz32.p, L->val32.p);
@@ -926,7 +934,29 @@ void Case::dilu_refresh(Equation& E, bool fp32) {
             kr_gather_vals(stream, L->nslots, L->src.p, E.nz.p, L->val.p);
         }
     }
+    if (fp32)
+        kr_level_dinv(stream, E.lsell.nslots, E.lsell.col.p, E.P32.p, E.lsell.dinv32.p);
+    else
+        kr_level_dinv(stream, E.lsell.nslots, E.lsell.col.p, E.P.p, E.lsell.dinv.p);
 }
+
+template <class T>
+LevelView<T> level_view(const Equation& E, int tri) {
+    const LevelSell& L = tri == 0 ? E.lsell : E.usell;
+    LevelView<T> v;
+    v.rows = tri == 0 ? E.d_lower_rows.p : E.d_upper_rows.p;
+    v.off = tri == 0 ? E.d_lower_off.p : E.d_upper_off.p;
+    const std::vector<int>& off = tri == 0 ? E.lower_off : E.upper_off;
+    v.nlev = off.empty() ? 0 : (int)off.size() - 1;
+    v.slice = L.slice.p;
+    v.cnt = L.cnt.p;
+    v.col = L.col.p;
+    v.val = sizeof(T) == 8 ? (const T*)L.val.p : (const T*)L.val32.p;
+    v.dinv = sizeof(T) == 8 ? (const T*)L.dinv.p : (const T*)L.dinv32.p;
+    return v;
+}
+template LevelView<double> level_view<double>(const Equation&, int);
+template LevelView<float> level_view<float>(const Equation&, int);
 
 template <class T>
 void Case::apply_M(Equation& E, int ptype, const T* nz, const T* P, const T* in, T* out, const KScalars* S) {

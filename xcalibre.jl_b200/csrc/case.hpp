@@ -35,15 +35,22 @@ struct DevMesh {
 // sweeps of large systems): position k of the level order (the row
 // rows[k]) holds that row's strictly lower (or upper) entries in the row's
 // own order, so the rows of one level read their slots coalesced.  `src` maps
-// each slot to the matrix slot whose value it mirrors (refreshed before each
-// DILU-preconditioned solve).
+// each slot to the matrix slot whose value it mirrors; values (and, for the
+// lower triangle, dinv = 1/D of each slot's column) are refreshed before
+// each DILU-preconditioned solve.
 struct LevelSell {
     long nslots = 0;
     DBuf<int> slice, col, src;
     DBuf<unsigned char> cnt;
-    DBuf<double> val;
-    DBuf<float> val32;
+    DBuf<double> val, dinv;
+    DBuf<float> val32, dinv32;
 };
+
+struct Equation;
+// device view of one level-ordered triangle of E (tri 0 lower, 1 upper) in
+// value type T (refreshed by Case::dilu_refresh)
+template <class T>
+LevelView<T> level_view(const Equation& E, int tri);
 
 struct Equation {
     int n = 0;

@@ -124,10 +124,15 @@ void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, c
 template <class T>
 void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const T* nz, const T* D, T* x,
                  const KScalars* S);
-// DILU level sweeps over level-ordered triangles (positions k0..k1 of one level)
+// DILU level sweeps over level-ordered triangles (positions k0..k1 of one
+// level); the forward sweep reads dinv (T(1)/D of each slot's column,
+// kr_level_dinv) instead of dividing per entry -- the same values
 template <class T>
 void kr_dilu_fwd_lv(cudaStream_t s, int k0, int k1, const int* rows, const int* slice, const unsigned char* cnt,
-                    const int* col, const T* val, const T* D, const T* b, T* y, const KScalars* S);
+                    const int* col, const T* val, const T* dinv, const T* b, T* y, const KScalars* S);
+// dinv[e] = T(1) / D[col[e]] for every slot of a level-ordered triangle
+template <class T>
+void kr_level_dinv(cudaStream_t s, long nslots, const int* col, const T* D, T* dinv);
 template <class T>
 void kr_dilu_bwd_lv(cudaStream_t s, int k0, int k1, const int* rows, const int* slice, const unsigned char* cnt,
                     const int* col, const T* val, const T* D, T* x, const KScalars* S);
@@ -136,9 +141,25 @@ void kr_gather_vals(cudaStream_t s, long n, const int* src, const T* vals, T* ds
 // small systems (n <= DILU_BLOCK_MAX_ROWS): whole sweeps in one block
 void kr_dilu_D_block(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
                      double* D);
+// one triangle in level order, as the one-block sweep reads it: level l is
+// positions off[l] .. off[l+1] of rows[]; position k keeps cnt[k] slots at
+// slice[k/32] + k%32 + 32 j (values val, and for the lower triangle dinv)
 template <class T>
-void kr_dilu_block(cudaStream_t s, const CSRView& A, const T* nz, const T* D, const T* b, T* y, const int* lo_rows,
-                   const int* lo_off, int n_lo, const int* up_rows, const int* up_off, int n_up, const KScalars* S);
+struct LevelView {
+    const int* rows;
+    const int* off;
+    int nlev;
+    const int* slice;
+    const unsigned char* cnt;
+    const int* col;
+    const T* val;
+    const T* dinv;
+};
+// y in shared memory for systems of at most this many bytes of y
+constexpr int DILU_SMEM_MAX_BYTES = 200 * 1024;
+template <class T>
+void kr_dilu_block(cudaStream_t s, int n, const LevelView<T>& lo, const LevelView<T>& up, const T* D, const T* b,
+                   T* y, const KScalars* S);
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
                  double* part0, double* part1, double* out);
 // device-driven solve control of graph mode (conditional WHILE nodes)

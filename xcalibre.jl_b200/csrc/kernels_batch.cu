@@ -61,11 +61,12 @@ __global__ void kbk_dilu_bwd(const BSys<T>* __restrict__ sys, const int2* __rest
 template <class T>
 __global__ void __launch_bounds__(DILU_BLOCK_THREADS) kbk_dilu_block(const BSys<T>* __restrict__ sys,
                                                                      const int* __restrict__ ids, int in, int out,
-                                                                     int use_S) {
+                                                                     int use_S, int smem) {
+    extern __shared__ __align__(16) unsigned char dilu_smem[];
     const BSys<T>& B = sys[ids[blockIdx.x]];
     if (use_S && B.S->done) return;
-    dilu_block_sweep<T>(B.A, B.nz, B.P, B.vec[in], B.vec[out], B.lo_rows, B.lo_off, B.n_lo, B.up_rows, B.up_off,
-                        B.n_up);
+    T* y = B.vec[out];
+    dilu_level_sweep<T>(B.n, B.lo, B.up, B.P, B.vec[in], y, smem ? reinterpret_cast<T*>(dilu_smem) : y);
 }
 
 template <class T>
@@ -166,11 +167,19 @@ void kb_copy(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_to
     XCAL_BLAUNCH(kbk_copy, sys, tmap, in, out, use_S);
 }
 template <class T>
-void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int* small_ids, int n_small, const int2* lo_rows,
+void kb_dilu(cudaStream_t s, const BSys<T>* sys, const int* small_ids, int n_small, int small_n, const int2* lo_rows,
              const std::vector<int>& lo_off, const int2* up_rows, const std::vector<int>& up_off, int in, int out,
              int use_S) {
     if (n_small > 0) {
-        kbk_dilu_block<T><<<n_small, DILU_BLOCK_THREADS, 0, s>>>(sys, small_ids, in, out, use_S);
+        static bool attr_set = false;
+        if (!attr_set) {
+            XCAL_CUDA(cudaFuncSetAttribute(kbk_dilu_block<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           DILU_SMEM_MAX_BYTES));
+            attr_set = true;
+        }
+        const size_t bytes = (size_t)small_n * sizeof(T);
+        const int smem = bytes <= (size_t)DILU_SMEM_MAX_BYTES ? 1 : 0;
+        kbk_dilu_block<T><<<n_small, DILU_BLOCK_THREADS, smem ? bytes : 0, s>>>(sys, small_ids, in, out, use_S, smem);
         XCAL_CHECK_LAUNCH();
     }
     for (size_t l = 0; l + 1 < lo_off.size(); ++l) {
@@ -244,7 +253,8 @@ void kb_bicg_p(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_
     template void kb_spmv<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, int);                            \
     template void kb_jacobi_apply<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, int, int);               \
     template void kb_copy<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, int, int);                       \
-    template void kb_dilu<T>(cudaStream_t, const BSys<T>*, const int*, int, const int2*, const std::vector<int>&, \
+    template void kb_dilu<T>(cudaStream_t, const BSys<T>*, const int*, int, int, const int2*,                    \
+                             const std::vector<int>&,                                                             \
                              const int2*, const std::vector<int>&, int, int, int);                                \
     template void kb_cg_start<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                  \
     template bool kb_cg_persist<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, unsigned int*, int, int*,  \

@@ -13,6 +13,8 @@
 // mixed-precision mode: FP32 matrix values, vectors and row sums, with dot
 // products accumulated in FP64 and the step scalars kept in FP64 on the
 // device and rounded to FP32 where they scale a vector.
+#include <algorithm>
+
 #include "kernels.hpp"
 #include "krylov_bodies.cuh"
 
@@ -223,15 +225,19 @@ __global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_D_block(const int* 
 
 // a whole DILU application (forward + backward sweeps) of a small system in one block
 template <class T>
-__global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_block(CSRView A, const T* __restrict__ nz,
+__global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_block(int n, LevelView<T> lo, LevelView<T> up,
                                                                    const T* __restrict__ D, const T* __restrict__ b,
-                                                                   T* y, const int* __restrict__ lo_rows,
-                                                                   const int* __restrict__ lo_off, int n_lo,
-                                                                   const int* __restrict__ up_rows,
-                                                                   const int* __restrict__ up_off, int n_up,
-                                                                   const KScalars* S) {
+                                                                   T* y, int smem, const KScalars* S) {
+    extern __shared__ __align__(16) unsigned char dilu_smem[];
     if (S && S->done) return;
-    dilu_block_sweep<T>(A, nz, D, b, y, lo_rows, lo_off, n_lo, up_rows, up_off, n_up);
+    dilu_level_sweep<T>(n, lo, up, D, b, y, smem ? reinterpret_cast<T*>(dilu_smem) : y);
+}
+
+// dinv[e] = T(1) / D[col[e]] (the forward sweep's per-entry reciprocal)
+template <class T>
+__global__ void k_level_dinv(long n, const int* __restrict__ col, const T* __restrict__ D, T* dinv) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        dinv[e] = T(1) / D[ld_stream(col + e)];
 }
 
 // forward_substitution! (preconditioners_1_DILU.jl:84-98), one level
@@ -260,8 +266,8 @@ __global__ void k_dilu_bwd(const int* __restrict__ rows, int nrows, CSRView A, c
 template <class T>
 __global__ void k_dilu_fwd_lv(int k0, int k1, const int* __restrict__ rows, const int* __restrict__ slice,
                               const unsigned char* __restrict__ cnt, const int* __restrict__ col,
-                              const T* __restrict__ val, const T* __restrict__ D, const T* __restrict__ b, T* y,
-                              const KScalars* S) {
+                              const T* __restrict__ val, const T* __restrict__ dinv, const T* __restrict__ b,
+                              T* y, const KScalars* S) {
     if (S && S->done) return;
     const int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= k1) return;
@@ -270,8 +276,7 @@ __global__ void k_dilu_fwd_lv(int k0, int k1, const int* __restrict__ rows, cons
     T sum = T(0);
     for (int j = 0; j < c; ++j) {
         const int e = base + SELL_C * j;
-        const int jc = ld_stream(col + e);
-        sum = sum + (ld_stream(val + e) * y[jc]) * (T(1) / D[jc]);
+        sum = sum + (ld_stream(val + e) * y[ld_stream(col + e)]) * ld_stream(dinv + e);
     }
     y[i] = b[i] - sum;
 }
@@ -617,9 +622,16 @@ void kr_dilu_bwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, c
 }
 template <class T>
 void kr_dilu_fwd_lv(cudaStream_t s, int k0, int k1, const int* rows, const int* slice, const unsigned char* cnt,
-                    const int* col, const T* val, const T* D, const T* b, T* y, const KScalars* S) {
+                    const int* col, const T* val, const T* dinv, const T* b, T* y, const KScalars* S) {
     if (k1 <= k0) return;
-    k_dilu_fwd_lv<T><<<(k1 - k0 + 255) / 256, 256, 0, s>>>(k0, k1, rows, slice, cnt, col, val, D, b, y, S);
+    k_dilu_fwd_lv<T><<<(k1 - k0 + 255) / 256, 256, 0, s>>>(k0, k1, rows, slice, cnt, col, val, dinv, b, y, S);
+    XCAL_CHECK_LAUNCH();
+}
+template <class T>
+void kr_level_dinv(cudaStream_t s, long nslots, const int* col, const T* D, T* dinv) {
+    if (nslots <= 0) return;
+    const long blocks = std::min((nslots + 255) / 256, 148L * 16);
+    k_level_dinv<T><<<(int)blocks, 256, 0, s>>>(nslots, col, D, dinv);
     XCAL_CHECK_LAUNCH();
 }
 template <class T>
@@ -643,9 +655,17 @@ void kr_dilu_D_block(cudaStream_t s, const int* rows, const int* off, int nlev, 
     XCAL_CHECK_LAUNCH();
 }
 template <class T>
-void kr_dilu_block(cudaStream_t s, const CSRView& A, const T* nz, const T* D, const T* b, T* y, const int* lo_rows,
-                   const int* lo_off, int n_lo, const int* up_rows, const int* up_off, int n_up, const KScalars* S) {
-    k_dilu_block<T><<<1, DILU_BLOCK_THREADS, 0, s>>>(A, nz, D, b, y, lo_rows, lo_off, n_lo, up_rows, up_off, n_up, S);
+void kr_dilu_block(cudaStream_t s, int n, const LevelView<T>& lo, const LevelView<T>& up, const T* D, const T* b,
+                   T* y, const KScalars* S) {
+    static bool attr_set = false;  // shared-memory limit of the kernel (per process, one device type)
+    if (!attr_set) {
+        XCAL_CUDA(cudaFuncSetAttribute(k_dilu_block<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       DILU_SMEM_MAX_BYTES));
+        attr_set = true;
+    }
+    const size_t bytes = (size_t)n * sizeof(T);
+    const int smem = bytes <= (size_t)DILU_SMEM_MAX_BYTES ? 1 : 0;
+    k_dilu_block<T><<<1, DILU_BLOCK_THREADS, smem ? bytes : 0, s>>>(n, lo, up, D, b, y, smem, S);
     XCAL_CHECK_LAUNCH();
 }
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
@@ -711,8 +731,9 @@ void kr_record(cudaStream_t s, const KScalars* S, int* out) {
                                  const KScalars*);                                                              \
     template void kr_dilu_bwd<T>(cudaStream_t, const int*, int, const CSRView&, const T*, const T*, T*,          \
                                  const KScalars*);                                                              \
-    template void kr_dilu_block<T>(cudaStream_t, const CSRView&, const T*, const T*, const T*, T*, const int*,   \
-                                   const int*, int, const int*, const int*, int, const KScalars*);              \
+    template void kr_dilu_block<T>(cudaStream_t, int, const LevelView<T>&, const LevelView<T>&, const T*,       \
+                                   const T*, T*, const KScalars*);                                              \
+    template void kr_level_dinv<T>(cudaStream_t, long, const int*, const T*, T*);                                \
     template void kr_dilu_fwd_lv<T>(cudaStream_t, int, int, const int*, const int*, const unsigned char*,         \
                                     const int*, const T*, const T*, const T*, T*, const KScalars*);             \
     template void kr_dilu_bwd_lv<T>(cudaStream_t, int, int, const int*, const int*, const unsigned char*,         \

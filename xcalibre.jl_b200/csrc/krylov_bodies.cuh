@@ -8,6 +8,7 @@
 // same whether it is solved alone or inside a batch.
 #pragma once
 #include "dev_common.cuh"
+#include "kernels.hpp"
 
 namespace xcal {
 
@@ -478,26 +479,81 @@ __device__ __forceinline__ void dilu_bwd_row(const CSRView& A, const T* __restri
 
 // A DILU application of a small system (n <= DILU_BLOCK_MAX_ROWS) as one
 // block: every level of the forward sweep, then of the backward sweep, with a
-// block barrier between levels (rows of a level are independent).  The
-// per-row arithmetic is the level kernels'.
+// block barrier between levels (rows of a level are independent).  It reads
+// the level-ordered triangles (position k of level order: cnt[k] slots at
+// slice[k/32] + k%32 + 32 j, coalesced across a warp) and, in the forward
+// sweep, dinv = T(1)/D[col] per slot, so a row's loads do not wait on one
+// another and no division sits on the sweep's critical path; ys is y
+// itself or, when y fits, a shared-memory copy written back at the end.
+// Per row the arithmetic is forward_substitution! / backward_substitution!
+// (preconditioners_1_DILU.jl:84-114) in the row's own entry order:
+//   forward  y_i = b_i - sum_j (a_ij y_j) (1/D_j)      (j < i)
+//   backward x_i = (x_i - sum_j a_ij x_j) / D_i        (j > i)
+// -- the values of the CSR-row sweeps (dilu_fwd_row / dilu_bwd_row), bit
+// for bit.
 constexpr int DILU_BLOCK_THREADS = 1024;
+constexpr int DILU_UNROLL = 8;  // slots per row loaded together (more: a loop)
 
 template <class T>
-__device__ __forceinline__ void dilu_block_sweep(const CSRView& A, const T* __restrict__ nz, const T* __restrict__ D,
-                                                 const T* __restrict__ in, T* out, const int* __restrict__ lo_rows,
-                                                 const int* __restrict__ lo_off, int n_lo,
-                                                 const int* __restrict__ up_rows, const int* __restrict__ up_off,
-                                                 int n_up) {
-    for (int l = 0; l < n_lo; ++l) {
-        for (int k = lo_off[l] + threadIdx.x; k < lo_off[l + 1]; k += blockDim.x)
-            dilu_fwd_row(A, nz, D, in, out, lo_rows[k]);
+__device__ __forceinline__ void dilu_level_sweep(int n, const LevelView<T>& lo, const LevelView<T>& up,
+                                                 const T* __restrict__ D, const T* __restrict__ b, T* y, T* ys) {
+    for (int l = 0; l < lo.nlev; ++l) {
+        const int k1 = lo.off[l + 1];
+        for (int k = lo.off[l] + threadIdx.x; k < k1; k += blockDim.x) {
+            const int i = lo.rows[k], c = lo.cnt[k];
+            const int base = lo.slice[k / SELL_C] + (k % SELL_C);
+            const T bi = b[i];
+            int cj[DILU_UNROLL];
+            T vj[DILU_UNROLL], dj[DILU_UNROLL];
+#pragma unroll
+            for (int j = 0; j < DILU_UNROLL; ++j)
+                if (j < c) {
+                    const int e = base + SELL_C * j;
+                    cj[j] = ld_stream(lo.col + e);
+                    vj[j] = ld_stream(lo.val + e);
+                    dj[j] = ld_stream(lo.dinv + e);
+                }
+            T sum = T(0);
+#pragma unroll
+            for (int j = 0; j < DILU_UNROLL; ++j)
+                if (j < c) sum = sum + (vj[j] * ys[cj[j]]) * dj[j];
+            for (int j = DILU_UNROLL; j < c; ++j) {
+                const int e = base + SELL_C * j;
+                sum = sum + (ld_stream(lo.val + e) * ys[ld_stream(lo.col + e)]) * ld_stream(lo.dinv + e);
+            }
+            ys[i] = bi - sum;
+        }
         __syncthreads();
     }
-    for (int l = 0; l < n_up; ++l) {
-        for (int k = up_off[l] + threadIdx.x; k < up_off[l + 1]; k += blockDim.x)
-            dilu_bwd_row(A, nz, D, out, up_rows[k]);
+    for (int l = 0; l < up.nlev; ++l) {
+        const int k1 = up.off[l + 1];
+        for (int k = up.off[l] + threadIdx.x; k < k1; k += blockDim.x) {
+            const int i = up.rows[k], c = up.cnt[k];
+            const int base = up.slice[k / SELL_C] + (k % SELL_C);
+            const T di = D[i];
+            int cj[DILU_UNROLL];
+            T vj[DILU_UNROLL];
+#pragma unroll
+            for (int j = 0; j < DILU_UNROLL; ++j)
+                if (j < c) {
+                    const int e = base + SELL_C * j;
+                    cj[j] = ld_stream(up.col + e);
+                    vj[j] = ld_stream(up.val + e);
+                }
+            T sum = T(0);
+#pragma unroll
+            for (int j = 0; j < DILU_UNROLL; ++j)
+                if (j < c) sum = sum + vj[j] * ys[cj[j]];
+            for (int j = DILU_UNROLL; j < c; ++j) {
+                const int e = base + SELL_C * j;
+                sum = sum + ld_stream(up.val + e) * ys[ld_stream(up.col + e)];
+            }
+            ys[i] = (ys[i] - sum) / di;
+        }
         __syncthreads();
     }
+    if (ys != y)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = ys[i];
 }
 
 // update_dilu_diagonal! row i (preconditioners_1_DILU.jl:43-82)
