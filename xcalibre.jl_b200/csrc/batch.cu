@@ -2,7 +2,9 @@
 //
 // The cases of a batch stay resident (fields, matrices, Krylov workspaces)
 // and advance one SIMPLE iteration per call in lockstep.  The face-loop and
-// correction kernels run per case on the batch stream; every Krylov solve
+// correction kernels run per case, each case on its own stream (forked from
+// and joined back into the batch stream with events, so the cases' small
+// kernels overlap on the GPU); every Krylov solve
 // (three momentum components, then pressure) is one batched solve over all
 // cases: the same kernels' tile bodies driven through a per-system
 // descriptor table and tile map (block-diagonal system, per-case offsets),
@@ -29,6 +31,8 @@ struct Batch {
     std::vector<Case*> cases;
     std::vector<size_t> footprint;   // bytes charged per case (case + mesh share)
     std::vector<cudaStream_t> own;   // each case's own stream (restored on removal)
+    std::vector<cudaEvent_t> joined; // per case: its per-case phase is done
+    cudaEvent_t forked = nullptr;    // the batch stream reached a per-case phase
     DBuf<KScalars> S;                // [cap] Krylov scalars, one block per case
     KScalars* hS = nullptr;          // pinned
     DBuf<double> res;                // [cap*4] scaled residuals of the iteration
@@ -39,6 +43,7 @@ struct Batch {
     DBuf<int2> tmap;                 // all cases
     DBuf<int2> tmap_act;             // subset (mixed-precision outer steps)
     DBuf<unsigned char> sys[2][4];   // [fp64, fp32][Ux, Uy, Uz, p] descriptor tables
+    DBuf<BAux> aux[4];               // [Ux, Uy, Uz, p] FP64-side tables
     DBuf<int2> dlo[2], dup[2];       // merged DILU levels per equation (large systems)
     std::vector<int> dlo_off[2], dup_off[2];
     DBuf<int> small_ids;             // systems that run DILU as one block
@@ -95,6 +100,7 @@ struct Batch {
 
     Batch(xcal_ctx* c, int capacity, size_t bytes) : ctx(c), cap(capacity), budget(bytes) {
         XCAL_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        XCAL_CUDA(cudaEventCreateWithFlags(&forked, cudaEventDisableTiming));
         S.alloc(cap);
         S.zero(stream);
         res.alloc(4 * (size_t)cap);
@@ -110,11 +116,35 @@ struct Batch {
         if (stream) cudaStreamSynchronize(stream);
         drop_graphs();
         for (size_t i = 0; i < cases.size(); ++i) cases[i]->stream = own[i];
+        for (cudaEvent_t e : joined) cudaEventDestroy(e);
+        if (forked) cudaEventDestroy(forked);
         if (hS) cudaFreeHost(hS);
         if (hres) cudaFreeHost(hres);
         if (stream) cudaStreamDestroy(stream);
     }
     void sync() { XCAL_CUDA(cudaStreamSynchronize(stream)); }
+
+    // f(case) for every case, each on its own stream after the work queued on
+    // the batch stream so far; the batch stream then waits for all of them.
+    // The cases share no memory, so their kernels may run concurrently.
+    template <class F>
+    void per_case(F&& f) {
+        XCAL_CUDA(cudaEventRecord(forked, stream));
+        for (size_t i = 0; i < cases.size(); ++i) {
+            Case* c = cases[i];
+            XCAL_CUDA(cudaStreamWaitEvent(own[i], forked, 0));
+            c->stream = own[i];
+            try {
+                f(c);
+            } catch (...) {
+                c->stream = stream;
+                throw;
+            }
+            c->stream = stream;
+            XCAL_CUDA(cudaEventRecord(joined[i], own[i]));
+        }
+        for (size_t i = 0; i < cases.size(); ++i) XCAL_CUDA(cudaStreamWaitEvent(stream, joined[i], 0));
+    }
 
     int index_of(const Case* c) const {
         for (size_t i = 0; i < cases.size(); ++i)
@@ -141,6 +171,9 @@ struct Batch {
         c->autotune();
         c->sync();
         if (c->graph_mode) c->set_graph_mode(false);
+        cudaEvent_t ev = nullptr;
+        XCAL_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        joined.push_back(ev);
         own.push_back(c->stream);
         c->stream = stream;
         cases.push_back(c);
@@ -155,6 +188,8 @@ struct Batch {
         sync();
         c->stream = own[i];
         used -= footprint[i];
+        cudaEventDestroy(joined[i]);
+        joined.erase(joined.begin() + i);
         cases.erase(cases.begin() + i);
         own.erase(own.begin() + i);
         footprint.erase(footprint.begin() + i);
@@ -200,6 +235,53 @@ struct Batch {
         sys[prec][slot].upload((const unsigned char*)h.data(), h.size() * sizeof(BSys<T>), stream);
     }
 
+    void fill_aux(int slot) {
+        const bool isU = slot < 3;
+        const int comp = isU ? slot : 0;
+        std::vector<BAux> h(cases.size());
+        for (size_t i = 0; i < cases.size(); ++i) {
+            Case* c = cases[i];
+            Equation& E = isU ? c->U : c->P;
+            const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
+            const bool cg = SS.solver == XCAL_SOLVER_CG;
+            BAux& B = h[i];
+            std::memset(&B, 0, sizeof(BAux));
+            B.A = E.view();
+            B.nz = E.nz.p;
+            B.nz32 = E.nz32.p;
+            B.P = E.P.p;
+            B.P32 = SS.precond != XCAL_PRECOND_NONE ? E.P32.p : nullptr;
+            B.b = isU ? c->U.b[comp].p : c->P.b[0].p;
+            B.field = isU ? c->Uc[comp].p : c->p.p;
+            B.dx = c->ws.dx.p;
+            B.x = c->ws.x.p;
+            B.r0 = cg ? c->ws.r.p : c->ws.q.p;
+            B.d32 = cg ? c->ws.fr.p : c->ws.fd.p;
+            B.x32 = c->ws.fx.p;
+            B.S = S.p + i;
+            B.part0 = c->ws.part0.p;
+            B.part1 = c->ws.part1.p;
+            B.res_out = res.p + 4 * i + slot;
+            if (SS.precond == XCAL_PRECOND_DILU && !E.lower_off.empty()) {
+                B.lsrc = E.lsell.src.p;
+                B.lcol = E.lsell.col.p;
+                B.lslice = E.lsell.slice.p;
+                B.lval = E.lsell.val.p;
+                B.lval32 = E.lsell.val32.p;
+                B.ldinv = E.lsell.dinv.p;
+                B.ldinv32 = E.lsell.dinv32.p;
+                B.usrc = E.usell.src.p;
+                B.uslice = E.usell.slice.p;
+                B.uval = E.usell.val.p;
+                B.uval32 = E.usell.val32.p;
+            }
+            B.n = E.n;
+            B.ntiles = (E.n + RED_TILE - 1) / RED_TILE;
+        }
+        if (h.empty()) h.resize(1);
+        aux[slot].upload(h, stream);
+    }
+
     void rebuild() {
         if (!dirty) return;
         drop_graphs();
@@ -219,6 +301,7 @@ struct Batch {
                     fill_sys<float>(1, slot);
                 else
                     fill_sys<double>(0, slot);
+                fill_aux(slot);
             }
             // small systems: one block per DILU application
             std::vector<int> ids;
@@ -404,30 +487,14 @@ struct Batch {
         }
         if (!mixed) {
             XCAL_CUDA(cudaMemcpyAsync(S.p, hS, nc * sizeof(KScalars), cudaMemcpyHostToDevice, stream));
-            for (Case* c : cases) {
-                Equation& E = isU ? c->U : c->P;
-                const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
-                const double* b = isU ? c->U.b[comp].p : c->P.b[0].p;
-                double* field = isU ? c->Uc[comp].p : c->p.p;
-                if (SS.precond == XCAL_PRECOND_DILU) c->dilu_refresh(E, false);
-                kr_init_resid(stream, E.view(), E.nz.p, b, field, c->ws.dx.p, c->ws.x.p,
-                              SS0.solver == XCAL_SOLVER_CG ? c->ws.r.p : c->ws.q.p);
-            }
+            if (SS0.precond == XCAL_PRECOND_DILU) kb_level_refresh(stream, aux[slot].p, tmap.p, ntiles, 0);
+            kb_init_resid(stream, aux[slot].p, tmap.p, ntiles);
             krylov<double>(0, slot, SS0, tmap.p, ntiles, all);
-            for (Case* c : cases) {
-                Equation& E = isU ? c->U : c->P;
-                double* field = isU ? c->Uc[comp].p : c->p.p;
-                kr_finish(stream, E.n, c->ws.x.p, c->ws.dx.p, field);
-            }
+            kb_finish(stream, aux[slot].p, tmap.p, ntiles);
             for (int i = 0; i < nc; ++i) cases[i]->last_iters[slot] = hS[i].iter;
         } else {
-            for (Case* c : cases) {
-                Equation& E = isU ? c->U : c->P;
-                const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
-                kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
-                if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, E.n, E.P.p, E.P32.p);
-                if (SS.precond == XCAL_PRECOND_DILU) c->dilu_refresh(E, true);
-            }
+            kb_to_float(stream, aux[slot].p, tmap.p, ntiles);
+            if (SS0.precond == XCAL_PRECOND_DILU) kb_level_refresh(stream, aux[slot].p, tmap.p, ntiles, 1);
             std::vector<char> active(nc, 1);
             std::vector<int> total(nc, 0);
             for (int outer = 0; outer < 64; ++outer) {
@@ -447,25 +514,17 @@ struct Batch {
                     if (active[t.x]) ta.push_back(t);
                 XCAL_CUDA(cudaMemcpyAsync(tmap_act.p, ta.data(), ta.size() * sizeof(int2), cudaMemcpyHostToDevice,
                                           stream));
-                for (int i : mem) {
-                    Case* c = cases[i];
-                    Equation& E = isU ? c->U : c->P;
-                    const double* b = isU ? c->U.b[comp].p : c->P.b[0].p;
-                    double* field = isU ? c->Uc[comp].p : c->p.p;
-                    float* rhs = SS0.solver == XCAL_SOLVER_CG ? c->ws.fr.p : c->ws.fd.p;
-                    kr_defect(stream, E.view(), E.nz.p, b, field, rhs, c->ws.fx.p);
-                }
+                kb_defect(stream, aux[slot].p, tmap_act.p, (int)ta.size());
                 krylov<float>(1, slot, SS0, tmap_act.p, (int)ta.size(), mem);
+                // field += e for every member whose defect was not already at
+                // its target (the device reads the same outer_conv flag)
+                kb_correct(stream, aux[slot].p, tmap_act.p, (int)ta.size());
                 for (int i : mem) {
                     if (hS[i].outer_conv) {
                         active[i] = 0;
                         continue;
                     }
                     total[i] += hS[i].iter;
-                    Case* c = cases[i];
-                    Equation& E = isU ? c->U : c->P;
-                    double* field = isU ? c->Uc[comp].p : c->p.p;
-                    kr_correct(stream, E.n, field, c->ws.fx.p);
                     int st = hS[i].status;
                     if (st == KS_ZERO_CURV || st == KS_BREAKDOWN || st == KS_TIRED ||
                         (st == KS_SOLVED && hS[i].eps <= hS[i].eps_outer))
@@ -475,14 +534,7 @@ struct Batch {
             for (int i = 0; i < nc; ++i) cases[i]->last_iters[slot] = total[i];
         }
         // residual (Solve_1_api.jl:441-464), FP64
-        for (int i = 0; i < nc; ++i) {
-            Case* c = cases[i];
-            Equation& E = isU ? c->U : c->P;
-            const double* b = isU ? c->U.b[comp].p : c->P.b[0].p;
-            double* field = isU ? c->Uc[comp].p : c->p.p;
-            kr_residual(stream, E.view(), E.nz.p, field, b, S.p + i, c->ws.part0.p, c->ws.part1.p,
-                        res.p + 4 * i + slot);
-        }
+        kb_residual(stream, aux[slot].p, tmap.p, ntiles);
     }
 
     // one SIMPLE iteration of every case (Solvers_1_SIMPLE.jl:164-240)
@@ -494,43 +546,43 @@ struct Batch {
         };
         const clk::time_point t0 = clk::now();
         rebuild();
-        for (Case* c : cases) {
-            if (!c->initialised) c->initial_calculations();
-            c->iteration += 1;
-            c->discretise(XCAL_EQN_U);
-        }
         double fv = 0, us = 0;
         for (int d = 0; d < 3; ++d) {
             clk::time_point a = clk::now();
-            for (Case* c : cases) {
+            per_case([&](Case* c) {
+                if (d == 0) {
+                    if (!c->initialised) c->initial_calculations();
+                    c->iteration += 1;
+                    c->discretise(XCAL_EQN_U);
+                }
                 c->bc_relax_U(d);
                 if (d == 0) c->update_precond(XCAL_EQN_U);
-            }
+            });
             clk::time_point b = clk::now();
             solve(d);
             fv += ms(a, b);
             us += ms(b, clk::now());
         }
         const clk::time_point t1 = clk::now();
-        for (Case* c : cases) {
+        per_case([&](Case* c) {
             c->pressure_predictor(true);
             c->flux_divergence();
             XCAL_CUDA(cudaMemcpyAsync(c->prev.p, c->p.p, c->mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice,
-                                      stream));
+                                      c->stream));
             c->discretise(XCAL_EQN_P);
             c->apply_bcs(XCAL_EQN_P, 0);
             c->set_reference();
             c->update_precond(XCAL_EQN_P);
-        }
+        });
         const clk::time_point t2 = clk::now();
         solve(3);
         const clk::time_point t3 = clk::now();
-        for (Case* c : cases) {
+        per_case([&](Case* c) {
             c->explicit_relaxation_p(c->cfg.p_solver.relax);
             c->grad_p();
             c->correct();
             c->turbulence();
-        }
+        });
         XCAL_CUDA(cudaMemcpyAsync(hres, res.p, 4 * cases.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
         sync();
         const clk::time_point t4 = clk::now();

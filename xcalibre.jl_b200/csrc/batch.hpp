@@ -43,6 +43,55 @@ struct BSys {
     LevelView<T> lo, up;
 };
 
+// FP64 side of one equation slot of a case inside a batched solve: the
+// matrix and vectors the solve's start, finish, mixed-precision defect
+// correction and residual touch, and the DILU level copies to refresh
+struct BAux {
+    CSRView A;
+    const double* nz;
+    float* nz32;        // FP32 copy (mixed)
+    const double* P;    // Jacobi inverse diagonal or DILU D
+    float* P32;         // its FP32 copy (mixed; null: no preconditioner)
+    const double* b;
+    double* field;
+    double* dx;         // FP64 path: warm-start shift
+    double* x;          // FP64 path: Krylov iterate
+    double* r0;         // FP64 path: initial residual (r for CG, q for BiCGSTAB)
+    float* d32;         // mixed: defect = inner right-hand side
+    float* x32;         // mixed: inner iterate
+    KScalars* S;        // the case's scalars in the batch (residual counter, outer flags)
+    double* part0;
+    double* part1;
+    double* res_out;    // scaled residual of this slot
+    // DILU: level-ordered triangles (lsrc null: no DILU)
+    const int* lsrc;
+    const int* lcol;
+    const int* lslice;
+    double* lval;
+    float* lval32;
+    double* ldinv;
+    float* ldinv32;
+    const int* usrc;
+    const int* uslice;
+    double* uval;
+    float* uval32;
+    int n, ntiles;
+};
+
+// batched per-case steps of a solve (one launch over the tile map instead of
+// one launch per case); the arithmetic of k_init_resid, k_finish, k_defect,
+// k_correct (masked by outer_conv), k_residual, k_to_float, k_gather_vals and
+// k_level_dinv
+void kb_init_resid(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total);
+void kb_finish(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total);
+void kb_defect(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total);
+void kb_correct(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total);
+void kb_residual(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total);
+void kb_to_float(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total);
+// level copies of the DILU triangles: values from nz (fp32: nz32) and the
+// lower triangle's 1/D per slot from P (fp32: P32)
+void kb_level_refresh(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total, int fp32);
+
 // batched launchers (kernels_batch.cu); tmap has ntiles_total entries
 template <class T>
 void kb_spmv(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int in, int out);

@@ -143,9 +143,162 @@ __global__ void __launch_bounds__(NT, persist_min_blocks(NT))
                            B.vec[KV_V], B.S, B.part0, B.part1, bars + 2 * tm.x, err, max_iters, 0);
 }
 
+// ---- per-case steps of a solve, batched (BAux tables) ----
+#define XCAL_BAUX                                   \
+    const int2 tm = tmap[blockIdx.x];               \
+    const BAux& B = aux[tm.x];                      \
+    const TileCtx tc{tm.y, B.ntiles};
+
+// r0 = b - A field, x = 0, dx = field (k_init_resid)
+__global__ void __launch_bounds__(RED_THREADS, 8) kbx_init_resid(const BAux* __restrict__ aux, const int2* tmap) {
+    XCAL_BAUX
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(tc, k);
+        if (i < B.n) {
+            B.r0[i] = B.b[i] - row_dot(B.A, B.nz, (const double*)B.field, i);
+            B.x[i] = 0.0;
+            B.dx[i] = B.field[i];
+        }
+    }
+}
+
+// field = x + dx (k_finish)
+__global__ void kbx_finish(const BAux* __restrict__ aux, const int2* tmap) {
+    XCAL_BAUX
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(tc, k);
+        if (i < B.n) B.field[i] = B.x[i] + B.dx[i];
+    }
+}
+
+// d32 = (float)(b - A field), x32 = 0 (k_defect)
+__global__ void __launch_bounds__(RED_THREADS, 8) kbx_defect(const BAux* __restrict__ aux, const int2* tmap) {
+    XCAL_BAUX
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(tc, k);
+        if (i < B.n) {
+            B.d32[i] = (float)(B.b[i] - row_dot(B.A, B.nz, (const double*)B.field, i));
+            B.x32[i] = 0.0f;
+        }
+    }
+}
+
+// field += x32 unless the outer loop found the defect already at its target
+// (k_correct; the case then leaves the outer loop uncorrected)
+__global__ void kbx_correct(const BAux* __restrict__ aux, const int2* tmap) {
+    XCAL_BAUX
+    if (B.S->outer_conv) return;
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(tc, k);
+        if (i < B.n) B.field[i] = B.field[i] + (double)B.x32[i];
+    }
+}
+
+// ||b - A field|| / max(||b||, 1 if tiny) per system (k_residual: the same
+// tile trees, the last of the system's blocks finishes)
+__global__ void __launch_bounds__(RED_THREADS, 8) kbx_residual(const BAux* __restrict__ aux, const int2* tmap) {
+    XCAL_BAUX
+    __shared__ double sm[8];
+    double a0 = 0.0, a1 = 0.0;
+    for (int k = 0; k < RED_ITEMS; ++k) {
+        int i = tile_row(tc, k);
+        if (i < B.n) {
+            double fx = row_dot(B.A, B.nz, (const double*)B.field, i);
+            double bi = B.b[i];
+            double d = bi - fx;
+            a0 = a0 + d * d;
+            a1 = a1 + bi * bi;
+        }
+    }
+    double t0 = block_tree(a0, sm);
+    double t1 = block_tree(a1, sm);
+    if (threadIdx.x == 0) {
+        B.part0[tc.tile] = t0;
+        B.part1[tc.tile] = t1;
+    }
+    if (!last_block(&B.S->counter2, tc.ntiles)) return;
+    double sR = reduce_partials(B.part0, tc.ntiles, sm);
+    double sb = reduce_partials(B.part1, tc.ntiles, sm);
+    if (threadIdx.x == 0) {
+        double normb = sqrt(sb);
+        double denom = normb > jl_eps(normb) ? normb : 1.0;
+        double res = sqrt(sR) / denom;
+        B.S->resid = res;
+        B.S->normb = normb;
+        *B.res_out = res;
+    }
+}
+
+// nz32 = (float) nz over the tile's slots (its rows' slices are contiguous),
+// P32 = (float) P over its rows
+__global__ void kbx_to_float(const BAux* __restrict__ aux, const int2* tmap) {
+    XCAL_BAUX
+    const int s0 = tc.tile * (RED_TILE / SELL_C);
+    const int s1 = min(s0 + RED_TILE / SELL_C, (B.n + SELL_C - 1) / SELL_C);
+    const int e1 = B.A.slice[s1];
+    for (int e = B.A.slice[s0] + threadIdx.x; e < e1; e += blockDim.x) B.nz32[e] = (float)ld_stream(B.nz + e);
+    if (B.P32)
+        for (int k = 0; k < RED_ITEMS; ++k) {
+            int i = tile_row(tc, k);
+            if (i < B.n) B.P32[i] = (float)B.P[i];
+        }
+}
+
+// level copies: slots of level positions in the tile (contiguous slices)
+template <class T>
+__device__ __forceinline__ void level_refresh_tile(const TileCtx& tc, int n, const int* slice, const int* src,
+                                                   const T* nz, T* val, const int* col, const T* D, T* dinv) {
+    const int s0 = tc.tile * (RED_TILE / SELL_C);
+    const int s1 = min(s0 + RED_TILE / SELL_C, (n + SELL_C - 1) / SELL_C);
+    const int e1 = slice[s1];
+    for (int e = slice[s0] + threadIdx.x; e < e1; e += blockDim.x) {
+        val[e] = nz[ld_stream(src + e)];
+        if (dinv) dinv[e] = T(1) / D[ld_stream(col + e)];
+    }
+}
+
+__global__ void kbx_level_refresh(const BAux* __restrict__ aux, const int2* tmap, int fp32) {
+    XCAL_BAUX
+    if (!B.lsrc) return;
+    if (fp32) {
+        level_refresh_tile<float>(tc, B.n, B.lslice, B.lsrc, B.nz32, B.lval32, B.lcol, B.P32, B.ldinv32);
+        level_refresh_tile<float>(tc, B.n, B.uslice, B.usrc, B.nz32, B.uval32, nullptr, nullptr, nullptr);
+    } else {
+        level_refresh_tile<double>(tc, B.n, B.lslice, B.lsrc, B.nz, B.lval, B.lcol, B.P, B.ldinv);
+        level_refresh_tile<double>(tc, B.n, B.uslice, B.usrc, B.nz, B.uval, nullptr, nullptr, nullptr);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+#define XCAL_XLAUNCH(K, ...)                                     \
+    do {                                                         \
+        if (ntiles_total <= 0) return;                           \
+        K<<<ntiles_total, RED_THREADS, 0, s>>>(__VA_ARGS__);     \
+        XCAL_CHECK_LAUNCH();                                     \
+    } while (0)
+void kb_init_resid(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total) {
+    XCAL_XLAUNCH(kbx_init_resid, aux, tmap);
+}
+void kb_finish(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total) {
+    XCAL_XLAUNCH(kbx_finish, aux, tmap);
+}
+void kb_defect(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total) {
+    XCAL_XLAUNCH(kbx_defect, aux, tmap);
+}
+void kb_correct(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total) {
+    XCAL_XLAUNCH(kbx_correct, aux, tmap);
+}
+void kb_residual(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total) {
+    XCAL_XLAUNCH(kbx_residual, aux, tmap);
+}
+void kb_to_float(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total) {
+    XCAL_XLAUNCH(kbx_to_float, aux, tmap);
+}
+void kb_level_refresh(cudaStream_t s, const BAux* aux, const int2* tmap, int ntiles_total, int fp32) {
+    XCAL_XLAUNCH(kbx_level_refresh, aux, tmap, fp32);
+}
 #define XCAL_BLAUNCH(K, ...)                                     \
     do {                                                         \
         if (ntiles_total <= 0) return;                           \
