@@ -716,6 +716,7 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     dlaunch.zero(stream);
     XCAL_CUDA(cudaMallocHost(&h_iters, 8 * sizeof(int)));
     XCAL_CUDA(cudaMallocHost(&h_launch, sizeof(unsigned long long)));
+    XCAL_CUDA(cudaMallocHost(&h_perr, sizeof(int)));
     // host-side per-cell constants: V^(1/3) (Courant) and the LES filter
     std::vector<double> h(nC);
     for (int i = 0; i < nC; ++i) h[i] = std::pow(m->vol[i], 1.0 / 3.0);
@@ -764,6 +765,7 @@ Case::~Case() {
     if (h_S) cudaFreeHost(h_S);
     if (h_res) cudaFreeHost(h_res);
     if (h_iters) cudaFreeHost(h_iters);
+    if (h_perr) cudaFreeHost(h_perr);
     if (h_launch) cudaFreeHost(h_launch);
     if (step_graph) cudaGraphExecDestroy(step_graph);
     for (cudaStream_t& sd : side)
@@ -1224,17 +1226,29 @@ void Case::solve_captured(int eqn, int comp) {
     const bool mixed = cfg.precision == XCAL_PREC_MIXED;
     const double inner_rtol = cfg.inner_rtol > 0 ? cfg.inner_rtol : 1e-3;
     kr_ks_init(stream, S, SS.atol, SS.rtol, itmax, mixed ? 1 : 0, inner_rtol);
+    // the CG loop as one cooperative kernel node where the driver runs those
+    // in graphs (top level; inside the mixed outer WHILE body), its barrier
+    // error flag cleared once per step and read after each replay
+    const bool persist = SS.solver == XCAL_SOLVER_CG && persistent_cg &&
+                         (SS.precond == XCAL_PRECOND_JACOBI || SS.precond == XCAL_PRECOND_NONE) &&
+                         kr_coop_capture_ok(mixed);
+    const int jac = SS.precond == XCAL_PRECOND_JACOBI ? 1 : 0;
+    const int pwidth = persistent_cg > 1 ? persistent_cg : 0;
     if (!mixed) {
         if (SS.precond == XCAL_PRECOND_DILU) dilu_refresh(E, false);
         KrylovVecs<double> V{ws.x.p, ws.r.p, ws.z.p, ws.p.p, ws.q.p, ws.v.p, ws.s.p, ws.t.p};
         const double* r0 = SS.solver == XCAL_SOLVER_CG ? V.r : V.q;
         kr_init_resid(stream, A, E.nz.p, b, field, ws.dx.p, V.x, SS.solver == XCAL_SOLVER_CG ? V.r : V.q);
         krylov_start<double>(E, SS, E.nz.p, E.P.p, b, r0, V, S);
-        capture_while([&](cudaGraphConditionalHandle h) {
-            const long long k0 = t_launch_count;
-            for (int i = 0; i < BODY; ++i) krylov_step<double>(E, SS, E.nz.p, E.P.p, b, V, S, nullptr, true);
-            kr_loop_cond(stream, h, S, cap, (int)(t_launch_count - k0) + 1, dlaunch.p);
-        });
+        const bool ran = persist && kr_cg_persist(stream, A, E.nz.p, E.P.p, jac, V.x, V.r, jac ? V.z : V.r, V.p, V.v,
+                                                  S, ws.part0.p, ws.part1.p, ws.bar.p, ws.err.p, itmax + 1, pwidth,
+                                                  E.nnz * 12L <= PERSIST_PF_MAX_BYTES ? 256 : 0, false);
+        if (!ran)
+            capture_while([&](cudaGraphConditionalHandle h) {
+                const long long k0 = t_launch_count;
+                for (int i = 0; i < BODY; ++i) krylov_step<double>(E, SS, E.nz.p, E.P.p, b, V, S, nullptr, true);
+                kr_loop_cond(stream, h, S, cap, (int)(t_launch_count - k0) + 1, dlaunch.p);
+            });
         kr_finish(stream, n, V.x, ws.dx.p, field);
     } else {
         kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
@@ -1248,13 +1262,18 @@ void Case::solve_captured(int eqn, int comp) {
             kr_outer_prep(stream, S);
             kr_defect(stream, A, E.nz.p, b, field, rhs, V.x);
             krylov_start<float>(E, SS, E.nz32.p, E.P32.p, (const float*)rhs, (const float*)rhs, V, S);
-            capture_while([&](cudaGraphConditionalHandle hi) {
-                const long long k1 = t_launch_count;
-                for (int i = 0; i < BODY; ++i)
-                    krylov_step<float>(E, SS, E.nz32.p, E.P32.p, (const float*)rhs, V, S, nullptr, true);
-                kr_loop_cond(stream, hi, S, cap, (int)(t_launch_count - k1) + 1, dlaunch.p);
-            });
-            const long long inner_body = last_body_kernels;
+            const bool ran =
+                persist && kr_cg_persist(stream, A, E.nz32.p, E.P32.p, jac, V.x, V.r, jac ? V.z : V.r, V.p, V.v, S,
+                                         ws.part0.p, ws.part1.p, ws.bar.p, ws.err.p, itmax + 1, pwidth,
+                                         E.nnz * 8L <= PERSIST_PF_MAX_BYTES ? 256 : 0, false);
+            if (!ran)
+                capture_while([&](cudaGraphConditionalHandle hi) {
+                    const long long k1 = t_launch_count;
+                    for (int i = 0; i < BODY; ++i)
+                        krylov_step<float>(E, SS, E.nz32.p, E.P32.p, (const float*)rhs, V, S, nullptr, true);
+                    kr_loop_cond(stream, hi, S, cap, (int)(t_launch_count - k1) + 1, dlaunch.p);
+                });
+            const long long inner_body = ran ? 0 : last_body_kernels;
             kr_correct_masked(stream, n, field, V.x, S);
             // this body's own kernels (the inner loop's bodies count themselves)
             const long long outer_kernels = t_launch_count - k0 - inner_body + 1;
@@ -1488,8 +1507,12 @@ void Case::capture_step() {
     body_kernels_captured = 0;
     capturing = true;
     cudaGraph_t g = nullptr;
+    // decided before the capture (the check runs graphs of its own)
+    kr_coop_capture_ok(false);
+    if (cfg.precision == XCAL_PREC_MIXED) kr_coop_capture_ok(true);
     XCAL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {
+        XCAL_CUDA(cudaMemsetAsync(ws.err.p, 0, sizeof(int), stream));
         double r3[3], rp;
         if (cfg.algorithm == XCAL_ALGO_PISO)
             piso_body(r3, rp);
@@ -1523,7 +1546,9 @@ void Case::run_step_graph(double res[4], double* courant) {
     XCAL_CUDA(cudaMemcpyAsync(h_iters, giters.p, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
     XCAL_CUDA(cudaMemcpyAsync(h_launch, dlaunch.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
     XCAL_CUDA(cudaMemsetAsync(dlaunch.p, 0, sizeof(unsigned long long), stream));
+    XCAL_CUDA(cudaMemcpyAsync(h_perr, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
     sync();
+    if (*h_perr) fail(XCAL_ERR_TIMEOUT, "persistent CG: a grid barrier wait gave up (graph mode)");
     long long nk = step_top_kernels + (long long)h_launch[0];
     g_launch_count.fetch_add(nk, std::memory_order_relaxed);
     t_launch_count += nk;

@@ -212,6 +212,7 @@ struct Case {
     long long step_graph_launches = 0;
     int* h_iters = nullptr;     // pinned mirror of giters
     unsigned long long* h_launch = nullptr;
+    int* h_perr = nullptr;      // pinned: persistent CG error flag after a graph replay
     long long body_kernels_captured = 0;
     long long last_body_kernels = 0;  // kernels captured into the last WHILE body
     void simple_body(double r3[3], double& rp, bool timed);

@@ -86,7 +86,11 @@ void kr_cg_rz(cudaStream_t s, int n, const T* r, const T* z, KScalars* S, double
 template <class T>
 bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
                    T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters,
-                   int width = 0, int pf_kb = 0);
+                   int width = 0, int pf_kb = 0, bool reset_err = true);
+// whether this device and driver run a cooperative kernel captured into a
+// CUDA graph (in_while: inside the body of a conditional WHILE node); found
+// out once per process by capturing and running a one-block no-op that way
+bool kr_coop_capture_ok(bool in_while);
 // Persistent CG widths: 1024 / 512 threads per block (wide form, systems of
 // at most 1 / 2 tiles per SM) or RED_THREADS (narrow form).  The launchers
 // take the widest form whose co-resident capacity covers the tiles.

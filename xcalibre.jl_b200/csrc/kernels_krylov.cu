@@ -419,9 +419,81 @@ __global__ void k_record(const KScalars* S, int* out) {
     out[1] = S->status;
 }
 
+__global__ void k_coop_noop() {}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+bool kr_coop_capture_ok(bool in_while) {
+    static int state[2] = {-1, -1};
+    int& st = state[in_while ? 1 : 0];
+    if (st >= 0) return st == 1;
+    cudaStream_t s = nullptr, s2 = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(32);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    void* noargs[1] = {nullptr};
+    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        if (!in_while) {
+            cfg.stream = s;
+            ok = cudaLaunchKernelExC(&cfg, (const void*)k_coop_noop, noargs) == cudaSuccess;
+        } else {
+            // WHILE node entered with its condition at 1; the body runs the
+            // no-op and sets the condition to 0, so it runs exactly once
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t cg = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            cudaGraphConditionalHandle h;
+            ok = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd) == cudaSuccess &&
+                 cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+            cudaGraphNodeParams prm = {};
+            cudaGraphNode_t node;
+            if (ok) {
+                prm.type = cudaGraphNodeTypeConditional;
+                prm.conditional.handle = h;
+                prm.conditional.type = cudaGraphCondTypeWhile;
+                prm.conditional.size = 1;
+                ok = cudaGraphAddNode(&node, cg, deps, nd, &prm) == cudaSuccess;
+            }
+            if (ok) ok = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) == cudaSuccess;
+            if (ok)
+                ok = cudaStreamBeginCaptureToGraph(s2, prm.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                cfg.stream = s2;
+                bool l1 = cudaLaunchKernelExC(&cfg, (const void*)k_coop_noop, noargs) == cudaSuccess;
+                k_set_cond<<<1, 32, 0, s2>>>(h, 0u);
+                bool l2 = cudaGetLastError() == cudaSuccess;
+                cudaGraph_t tmp = nullptr;
+                bool l3 = cudaStreamEndCapture(s2, &tmp) == cudaSuccess;
+                ok = l1 && l2 && l3;
+            }
+        }
+        cudaError_t ee = cudaStreamEndCapture(s, &g);
+        ok = ok && ee == cudaSuccess;
+    }
+    ok = ok && cudaGraphInstantiate(&ge, g, 0) == cudaSuccess;
+    ok = ok && cudaGraphLaunch(ge, s) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    if (ge) cudaGraphExecDestroy(ge);
+    if (g) cudaGraphDestroy(g);
+    if (s2) cudaStreamDestroy(s2);
+    if (s) cudaStreamDestroy(s);
+    cudaGetLastError();
+    st = ok ? 1 : 0;
+    return ok;
+}
+
 static inline int tiles(int n) { return n <= 0 ? 1 : (n + RED_TILE - 1) / RED_TILE; }
 #define TILE_LAUNCH(n) tiles(n), RED_THREADS, 0
 
@@ -535,7 +607,7 @@ bool persist_launch(PersistCaps& c, int w, const void* kernel, int ntiles, cudaS
 template <class T>
 bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
                    T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters,
-                   int width, int pf_kb) {
+                   int width, int pf_kb, bool reset_err) {
     static PersistCaps caps;  // co-resident blocks per width (per process, one device type)
     static const void* const kern[3] = {(const void*)k_cg_persist<T, 1024>, (const void*)k_cg_persist<T, 512>,
                                         (const void*)k_cg_persist<T, RED_THREADS>};
@@ -543,7 +615,7 @@ bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, in
     const int w = persist_pick(caps, kern, nt, width);
     if (w < 0) return false;
     XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
-    XCAL_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    if (reset_err) XCAL_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     CSRView Av = A;
     void* args[] = {&Av, (void*)&nz, (void*)&P, &jacobi, &x,         &r,    &z,
                     &P0, &P1,        &S,        &part,   &part2,     &bar,  &err,
@@ -719,7 +791,7 @@ void kr_record(cudaStream_t s, const KScalars* S, int* out) {
                                   KScalars*, double*);                                                          \
     template void kr_cg_rz<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*);                        \
     template bool kr_cg_persist<T>(cudaStream_t, const CSRView&, const T*, const T*, int, T*, T*, T*, T*, T*,    \
-                                   KScalars*, double*, double*, unsigned int*, int*, int, int, int);            \
+                                   KScalars*, double*, double*, unsigned int*, int*, int, int, int, bool);      \
     template void kr_bicg_start<T>(cudaStream_t, int, const T*, const T*, T*, KScalars*, double*, double*);      \
     template void kr_bicg_alpha<T>(cudaStream_t, int, const T*, const T*, KScalars*, double*);                   \
     template void kr_bicg_s<T>(cudaStream_t, int, const T*, const T*, const T*, T*, T*, const KScalars*);        \
