@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--serve-cases", type=int, default=16, help="serving stream: requests (0 = skip)")
     ap.add_argument("--serve-nmax", type=float, default=3e4)
     ap.add_argument("--serve-rate", type=float, default=8.0)
-    ap.add_argument("--only", choices=["les", "serving"], default=None,
+    ap.add_argument("--only", choices=["les", "serving", "batch"], default=None,
                     help="run one secondary workload alone and print its block as the line (profiling)")
     return ap.parse_args()
 
@@ -377,6 +377,52 @@ def serve_measure(x, args, local):
     return s
 
 
+def batch_measure(x, args, local):
+    """Batching: the serving sample's requests (same seed and sizes) resident
+    as one fixed batch, mixed precision; W warm-up batch iterations, then K
+    timed ones (each one SIMPLE iteration of every case: batched Krylov
+    solves over all cases, per-case face loops on the cases' own streams).
+    Host wall time around xcal_batch_simple_iterate, which ends in a device
+    synchronisation (it returns the residuals)."""
+    from importlib import import_module
+    serve = import_module(x.__name__ + ".serve")
+    reqs = serve.make_requests(args.serve_cases, seed=0, n_min=1e3, n_max=args.serve_nmax, rate=args.serve_rate)
+    ctx = x.Context(local)
+    batch = x.api.Batch(ctx, max(64, len(reqs)), 40 << 30)
+    keep = []
+    for r in reqs:
+        model, config, pref = r.config("mixed", 1500, 1e-6)
+        cfg, k = x.build_config(model, config, pref=pref)
+        dm = x.DeviceMesh(ctx, r.build())
+        c = x.Case(dm, cfg)
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+        if not batch.add(c):
+            raise RuntimeError("batch admission refused")
+        keep.append((c, dm, k))
+    for _ in range(args.warmup):
+        batch.simple_iterate()
+    p0 = batch.timings()
+    l0 = x.launch_count()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch.simple_iterate()
+    dt = time.perf_counter() - t0
+    p1 = batch.timings()
+    launches = x.launch_count() - l0
+    cells = sum(r.n_cells for r in reqs)
+    out = {"workload": f"{len(reqs)} steady cavity/channel cases (the serving sample's requests) as one batch, "
+                       f"mixed", "cases": len(reqs), "cells": cells, "steps": args.steps, "warmup": args.warmup,
+           "value": cells * args.steps / dt / 1e6, "unit": UNIT, "ms_per_iter": dt / args.steps * 1e3,
+           "phase_ms_per_iter": {k: (p1[k] - p0[k]) / args.steps for k in p1},
+           "gpu_launches_per_iter": launches / args.steps}
+    batch.close()
+    for c, dm, _ in keep:
+        c.close()
+        dm.close()
+    return out
+
+
 def e2e_measure(x, A, case, mesh, args, world):
     """Same metric through the public API with host buffers: every step copies
     U and p host->device, runs one SIMPLE iteration and reads them back."""
@@ -415,7 +461,8 @@ def main():
     x = ge.load_package()
     A = x._abi
     if args.only is not None:
-        blk = les_measure(x, A, args, local) if args.only == "les" else serve_measure(x, args, local)
+        blk = {"les": lambda: les_measure(x, A, args, local), "serving": lambda: serve_measure(x, args, local),
+               "batch": lambda: batch_measure(x, args, local)}[args.only]()
         if rank == 0:
             print(json.dumps({"only": args.only, **blk}), flush=True)
         if world > 1:
@@ -443,6 +490,7 @@ def main():
                  "phases_ms_total": r2["phases_ms_total"], "gpu_launches": r2["gpu_launches"]}
     les = les_measure(x, A, args, local) if args.les_size > 0 else None
     serving = serve_measure(x, args, local) if args.serve_cases > 0 else None
+    batched = batch_measure(x, args, local) if args.serve_cases > 0 else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(x, pm, mesh, args.cpu_iters)
@@ -459,7 +507,7 @@ def main():
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": r["gpu_launches"],
                 "clocks": r["clocks"], "residuals_last": r["residuals_last"],
                 "phases_ms_total": r["phases_ms_total"], "second_precision": other, "les": les,
-                "serving": serving}
+                "serving": serving, "batch": batched}
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
