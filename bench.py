@@ -439,8 +439,8 @@ def e2e_measure(x, A, case, mesh, args, world):
         case.set_field(A.FIELD_U, hU)
         case.set_field(A.FIELD_P, hp)
         r, _ = case.simple_iterate(1)
-        hU[:] = case.get_field(A.FIELD_U)
-        hp[:] = case.get_field(A.FIELD_P)
+        case.get_field(A.FIELD_U, out=hU)
+        case.get_field(A.FIELD_P, out=hp)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, "cuda")
     return {"value": job_throughput(nC, world, args.e2e_steps, e2e_s), "unit": UNIT,
             "h2d_bytes_per_step": 4 * nC * 8, "d2h_bytes_per_step": 4 * nC * 8 + 4 * 8, "steps": args.e2e_steps}

@@ -153,6 +153,13 @@ def test_determinism_two_runs(x, ctx):
         out.append((res, g.get_field(x._abi.FIELD_U), g.get_field(x._abi.FIELD_P)))
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+    # reading into a caller's buffer (get_field(out=)) gives the same values
+    U = np.empty((3, mesh.n_cells))
+    p = np.empty(mesh.n_cells)
+    assert g.get_field(x._abi.FIELD_U, out=U) is U and g.get_field(x._abi.FIELD_P, out=p) is p
+    assert np.array_equal(U, out[1][1]) and np.array_equal(p, out[1][2])
+    with pytest.raises(ValueError):
+        g.get_field(x._abi.FIELD_P, out=np.empty(mesh.n_cells, dtype=np.float32))
 
 
 @pytest.mark.parametrize("mode", [1, 2])

@@ -499,10 +499,20 @@ class Case:
         a = np.ascontiguousarray(np.asarray(values, dtype=np.float64).reshape(nc * per))
         self._chk(lib().xcal_case_set_field(self.h, field, _abi.ptr(a, C.c_double), a.size))
 
-    def get_field(self, field: int) -> np.ndarray:
+    def get_field(self, field: int, out: np.ndarray | None = None) -> np.ndarray:
+        """The field in original cell/face order ([components, n] for vectors).
+        out: a C-contiguous float64 array of that size to write into (e.g. a
+        pinned host buffer, which the device copies into directly)."""
         nc, per = self._size(field)
-        a = np.empty(nc * per)
+        if out is not None:
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != nc * per:
+                raise ValueError("get_field: out must be C-contiguous float64 with %d values" % (nc * per))
+            a = out.reshape(nc * per)
+        else:
+            a = np.empty(nc * per)
         self._chk(lib().xcal_case_get_field(self.h, field, _abi.ptr(a, C.c_double), a.size))
+        if out is not None:
+            return out
         return a.reshape(nc, per) if nc > 1 else a
 
     def nnz(self, eqn: int) -> int:
