@@ -13,6 +13,7 @@
 // and leave (xcal_batch_remove) between iterations; admission is bounded by a
 // device-memory budget.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstring>
 
@@ -61,6 +62,12 @@ struct Batch {
         long long launches = 0;
     };
     ChunkGraph chunk_graph[2][4];
+    // each case's face-loop phases (U assembly + first component, second and
+    // third components, pressure assembly, correction), captured at first
+    // use and replayed on the case's own stream: everything they read is
+    // device state or fixed for the case, as in graph mode
+    static constexpr int N_PHASES = 5;
+    std::vector<std::array<ChunkGraph, N_PHASES>> case_graph;
 
     void drop_graphs() {
         for (auto& row : chunk_graph)
@@ -71,20 +78,34 @@ struct Batch {
                 }
     }
 
+    static void drop_case_graphs(std::array<ChunkGraph, N_PHASES>& gs) {
+        for (auto& g : gs)
+            if (g.exec) {
+                cudaGraphExecDestroy(g.exec);
+                g.exec = nullptr;
+            }
+    }
+
     template <class F>
     void replay(ChunkGraph& g, F&& body) {
+        replay_on(g, stream, body);
+    }
+
+    // launch the graph captured from body() on stream s (capturing it first)
+    template <class F>
+    void replay_on(ChunkGraph& g, cudaStream_t s, F&& body) {
         if (!g.exec) {
             const long long t0 = t_launch_count;
             cudaGraph_t graph = nullptr;
-            XCAL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            XCAL_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             try {
                 body();
             } catch (...) {
-                cudaStreamEndCapture(stream, &graph);
+                cudaStreamEndCapture(s, &graph);
                 if (graph) cudaGraphDestroy(graph);
                 throw;
             }
-            XCAL_CUDA(cudaStreamEndCapture(stream, &graph));
+            XCAL_CUDA(cudaStreamEndCapture(s, &graph));
             const long long captured = t_launch_count - t0;
             g_launch_count.fetch_sub(captured, std::memory_order_relaxed);
             t_launch_count = t0;
@@ -93,7 +114,7 @@ struct Batch {
             XCAL_CUDA(e);
             g.launches = captured;
         }
-        XCAL_CUDA(cudaGraphLaunch(g.exec, stream));
+        XCAL_CUDA(cudaGraphLaunch(g.exec, s));
         g_launch_count.fetch_add(g.launches, std::memory_order_relaxed);
         t_launch_count += g.launches;
     }
@@ -115,6 +136,7 @@ struct Batch {
     ~Batch() {
         if (stream) cudaStreamSynchronize(stream);
         drop_graphs();
+        for (auto& gs : case_graph) drop_case_graphs(gs);
         for (size_t i = 0; i < cases.size(); ++i) cases[i]->stream = own[i];
         for (cudaEvent_t e : joined) cudaEventDestroy(e);
         if (forked) cudaEventDestroy(forked);
@@ -127,15 +149,19 @@ struct Batch {
     // f(case) for every case, each on its own stream after the work queued on
     // the batch stream so far; the batch stream then waits for all of them.
     // The cases share no memory, so their kernels may run concurrently.
+    // phase >= 0: f's launches are captured once per case and replayed.
     template <class F>
-    void per_case(F&& f) {
+    void per_case(F&& f, int phase = -1) {
         XCAL_CUDA(cudaEventRecord(forked, stream));
         for (size_t i = 0; i < cases.size(); ++i) {
             Case* c = cases[i];
             XCAL_CUDA(cudaStreamWaitEvent(own[i], forked, 0));
             c->stream = own[i];
             try {
-                f(c);
+                if (phase < 0)
+                    f(c);
+                else
+                    replay_on(case_graph[i][phase], own[i], [&] { f(c); });
             } catch (...) {
                 c->stream = stream;
                 throw;
@@ -174,6 +200,7 @@ struct Batch {
         cudaEvent_t ev = nullptr;
         XCAL_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         joined.push_back(ev);
+        case_graph.emplace_back();
         own.push_back(c->stream);
         c->stream = stream;
         cases.push_back(c);
@@ -190,6 +217,8 @@ struct Batch {
         used -= footprint[i];
         cudaEventDestroy(joined[i]);
         joined.erase(joined.begin() + i);
+        drop_case_graphs(case_graph[i]);
+        case_graph.erase(case_graph.begin() + i);
         cases.erase(cases.begin() + i);
         own.erase(own.begin() + i);
         footprint.erase(footprint.begin() + i);
@@ -546,43 +575,54 @@ struct Batch {
         };
         const clk::time_point t0 = clk::now();
         rebuild();
+        bool fresh = false;
+        for (Case* c : cases) {
+            fresh = fresh || !c->initialised;
+            c->iteration += 1;
+        }
+        if (fresh)
+            per_case([&](Case* c) {
+                if (!c->initialised) c->initial_calculations();
+            });
         double fv = 0, us = 0;
         for (int d = 0; d < 3; ++d) {
             clk::time_point a = clk::now();
-            per_case([&](Case* c) {
-                if (d == 0) {
-                    if (!c->initialised) c->initial_calculations();
-                    c->iteration += 1;
-                    c->discretise(XCAL_EQN_U);
-                }
-                c->bc_relax_U(d);
-                if (d == 0) c->update_precond(XCAL_EQN_U);
-            });
+            per_case(
+                [&](Case* c) {
+                    if (d == 0) c->discretise(XCAL_EQN_U);
+                    c->bc_relax_U(d);
+                    if (d == 0) c->update_precond(XCAL_EQN_U);
+                },
+                d);
             clk::time_point b = clk::now();
             solve(d);
             fv += ms(a, b);
             us += ms(b, clk::now());
         }
         const clk::time_point t1 = clk::now();
-        per_case([&](Case* c) {
-            c->pressure_predictor(true);
-            c->flux_divergence();
-            XCAL_CUDA(cudaMemcpyAsync(c->prev.p, c->p.p, c->mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice,
-                                      c->stream));
-            c->discretise(XCAL_EQN_P);
-            c->apply_bcs(XCAL_EQN_P, 0);
-            c->set_reference();
-            c->update_precond(XCAL_EQN_P);
-        });
+        per_case(
+            [&](Case* c) {
+                c->pressure_predictor(true);
+                c->flux_divergence();
+                XCAL_CUDA(cudaMemcpyAsync(c->prev.p, c->p.p, c->mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice,
+                                          c->stream));
+                c->discretise(XCAL_EQN_P);
+                c->apply_bcs(XCAL_EQN_P, 0);
+                c->set_reference();
+                c->update_precond(XCAL_EQN_P);
+            },
+            3);
         const clk::time_point t2 = clk::now();
         solve(3);
         const clk::time_point t3 = clk::now();
-        per_case([&](Case* c) {
-            c->explicit_relaxation_p(c->cfg.p_solver.relax);
-            c->grad_p();
-            c->correct();
-            c->turbulence();
-        });
+        per_case(
+            [&](Case* c) {
+                c->explicit_relaxation_p(c->cfg.p_solver.relax);
+                c->grad_p();
+                c->correct();
+                c->turbulence();
+            },
+            4);
         XCAL_CUDA(cudaMemcpyAsync(hres, res.p, 4 * cases.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
         sync();
         const clk::time_point t4 = clk::now();
