@@ -377,9 +377,12 @@ int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable);
  * runs as one cooperative launch (grid barriers between the SpMV and update
  * phases, q kept on chip) whenever the system's tiles fit the GPU at once;
  * otherwise, and in graph mode, the two-kernel loop runs.  Same results.
- * mode: 0 off, 1 on (the widest block form whose blocks are co-resident:
- * 1024, 512 or 256 threads), or 256 / 512 / 1024 = that form only (falls
- * back to the two-kernel loop when it does not fit). */
+ * mode: 0 off; 1 on: a system of at most 16 tiles of 2048 rows runs as one
+ * thread-block cluster (hardware cluster barriers), a larger one in the
+ * widest cooperative block form whose blocks are co-resident (1024, 512 or
+ * 256 threads); 2 = the cluster form only, 256 / 512 / 1024 = that
+ * cooperative form only (each falls back to the two-kernel loop when it
+ * does not fit). */
 int32_t xcal_case_set_persistent(xcal_case* cs, int32_t mode);
 /* launch-shape autotuner (runs on first use, or now): out6 = for U then p,
  * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU as

@@ -63,6 +63,35 @@ def test_batch_matches_single(x, ctx, prec, persist):
     batch.close()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_batch_cluster_form_matches_single(x, ctx, prec):
+    """Cases of 2, 5 and 10 tiles: the batch runs every pressure CG as one
+    thread-block cluster per case (16 blocks each, padding blocks without
+    rows); alone, each case runs the 1024-thread cooperative form.  Same
+    results, bit for bit."""
+    specs = [("cavity", 60, 7, 1e-3), ("channel", 20, 8, 2e-3), ("channel", 26, 9, 5e-3)]
+    iters = 3
+    alone = []
+    for kind, n, seed, nu in specs:
+        c, keep = _mk(x, ctx, kind, n, seed, prec, nu)
+        c.set_persistent(1024)
+        res, _ = c.simple_iterate(iters)
+        alone.append((res, c.get_field(x._abi.FIELD_U), c.get_field(x._abi.FIELD_P)))
+    batch = x.api.Batch(ctx, 4, 1 << 34)
+    members = []
+    for kind, n, seed, nu in specs:
+        c, keep = _mk(x, ctx, kind, n, seed, prec, nu)
+        c.set_persistent(2)
+        assert batch.add(c)
+        members.append((c, keep))
+    hist = np.stack([batch.simple_iterate()[0] for _ in range(iters)], axis=1)
+    for k, (c, keep) in enumerate(members):
+        assert np.array_equal(hist[k], alone[k][0]), (k, hist[k], alone[k][0])
+        assert np.array_equal(c.get_field(x._abi.FIELD_U), alone[k][1])
+        assert np.array_equal(c.get_field(x._abi.FIELD_P), alone[k][2])
+    batch.close()
+
+
 def test_batch_enter_leave_keeps_results(x, ctx):
     """A case that joins a running batch later and one that leaves early give
     the results they give alone."""

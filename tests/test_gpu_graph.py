@@ -100,12 +100,13 @@ def test_autotuner_choices(x, ctx):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_persistent_cg_identical(x, ctx, prec):
-    """The pressure CG as one cooperative launch (grid barriers, q on chip)
-    gives the two-kernel loop's results bit for bit, in each block form: the
-    automatic choice and the 1024-, 512- and 256-thread forms forced."""
+    """The pressure CG as one launch (q on chip) gives the two-kernel loop's
+    results bit for bit, in each form: the automatic choice, the cluster form
+    (14 tiles: one 16-block cluster, hardware barriers) and the 1024-, 512-
+    and 256-thread cooperative forms forced."""
     mesh = x.build_mesh3(x.channel_polymesh(48, 24, 24, seed=6))
     out = []
-    modes = (False, True, 1024, 512, 256)
+    modes = (False, True, 2, 1024, 512, 256)
     for persist in modes:
         model, config = x.cases.channel_case(mesh, iterations=4, precision=prec)
         cfg, keep = x.build_config(model, config)

@@ -627,8 +627,9 @@ class Case:
         self._chk(lib().xcal_case_set_dilu_mode(self.h, int(mode)))
 
     def set_persistent(self, on=True):
-        """Persistent CG (one cooperative launch per solve): False / True, or
-        256 / 512 / 1024 to allow only that block form."""
+        """Persistent CG (one launch per solve): False / True, or 2 (the
+        cluster form only) or 256 / 512 / 1024 (that cooperative block form
+        only)."""
         mode = int(on) if isinstance(on, bool) else int(on)
         self._chk(lib().xcal_case_set_persistent(self.h, mode))
 

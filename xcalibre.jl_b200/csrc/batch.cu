@@ -51,6 +51,12 @@ struct Batch {
     int n_small = 0;
     int small_n = 0;                 // rows of the largest of them
     DBuf<unsigned int> bars;         // persistent CG: barrier state per system
+    DBuf<int> mem_ids;               // persistent CG, cluster form: member systems grouped by cluster size
+    int* hmem = nullptr;             // pinned staging of mem_ids
+    // one stream per cluster-size group (1, 2, 4, 8, 16 blocks), so the
+    // groups' launches run side by side
+    cudaStream_t gstream[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t gjoined[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     DBuf<int> perr;                  // persistent CG: a barrier wait gave up
     std::vector<int2> h_tmap;
     long long iterations = 0;
@@ -129,6 +135,12 @@ struct Batch {
         XCAL_CUDA(cudaMallocHost(&hS, cap * sizeof(KScalars)));
         XCAL_CUDA(cudaMallocHost(&hres, 4 * cap * sizeof(double)));
         bars.alloc(2 * (size_t)cap);
+        mem_ids.alloc(cap);
+        XCAL_CUDA(cudaMallocHost(&hmem, cap * sizeof(int)));
+        for (int g = 0; g < 5; ++g) {
+            XCAL_CUDA(cudaStreamCreateWithFlags(&gstream[g], cudaStreamNonBlocking));
+            XCAL_CUDA(cudaEventCreateWithFlags(&gjoined[g], cudaEventDisableTiming));
+        }
         bars.zero(stream);
         perr.alloc(1);
         perr.zero(stream);
@@ -141,6 +153,14 @@ struct Batch {
         for (cudaEvent_t e : joined) cudaEventDestroy(e);
         if (forked) cudaEventDestroy(forked);
         if (hS) cudaFreeHost(hS);
+        if (hmem) cudaFreeHost(hmem);
+        for (int g = 0; g < 5; ++g) {
+            if (gstream[g]) {
+                cudaStreamSynchronize(gstream[g]);
+                cudaStreamDestroy(gstream[g]);
+            }
+            if (gjoined[g]) cudaEventDestroy(gjoined[g]);
+        }
         if (hres) cudaFreeHost(hres);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -418,9 +438,22 @@ struct Batch {
                 all_persist = all_persist && cases[i]->persistent_cg != 0;
                 if (cases[i]->persistent_cg > 1) width = cases[i]->persistent_cg;
             }
-            if (all_persist &&
-                kb_cg_persist<T>(stream, sy, tm, nt, pt == XCAL_PRECOND_JACOBI ? 1 : 0, bars.p, (int)cases.size(),
-                                 perr.p, itmax + 1, width)) {
+            const int jac = pt == XCAL_PRECOND_JACOBI ? 1 : 0;
+            int max_tiles = 0;
+            for (int i : members) max_tiles = std::max(max_tiles, (cases[i]->U.n + RED_TILE - 1) / RED_TILE);
+            bool cluster = false;
+            if (all_persist && (width == 0 || width == PERSIST_CLUSTER_ONLY) && max_tiles <= PERSIST_CLUSTER_MAX)
+                cluster = cluster_cg<T>(sy, members, jac, itmax + 1);
+            if (cluster) {
+                XCAL_CUDA(cudaMemcpyAsync(hS, S.p, cases.size() * sizeof(KScalars), cudaMemcpyDeviceToHost,
+                                          stream));
+                sync();
+                for (int i : members)
+                    if (!hS[i].done) fail(XCAL_ERR_TIMEOUT, "batch: persistent CG did not report completion");
+                return;
+            }
+            if (all_persist && width != PERSIST_CLUSTER_ONLY &&
+                kb_cg_persist<T>(stream, sy, tm, nt, jac, bars.p, (int)cases.size(), perr.p, itmax + 1, width)) {
                 int errflag = 0;
                 XCAL_CUDA(cudaMemcpyAsync(hS, S.p, cases.size() * sizeof(KScalars), cudaMemcpyDeviceToHost,
                                           stream));
@@ -458,6 +491,40 @@ struct Batch {
             if (all) break;
             if (chunk < CHUNK) chunk *= 2;
         }
+    }
+
+    // every member's CG in the cluster form, members grouped by the cluster
+    // size they need (1, 2, 4, 8 or 16 blocks: a cluster per member), one
+    // launch per group, the groups on their own streams; false (nothing
+    // launched) when the device cannot run some group's cluster size
+    template <class T>
+    bool cluster_cg(const BSys<T>* sy, const std::vector<int>& members, int jac, int max_iters) {
+        std::vector<int> grp[5];
+        for (int i : members) {
+            const int t = (cases[i]->U.n + RED_TILE - 1) / RED_TILE;
+            int g = 0;
+            while ((1 << g) < t) ++g;
+            grp[g].push_back(i);
+        }
+        for (int g = 0; g < 5; ++g)
+            if (!grp[g].empty() && persist_cluster_size(kb_cg_persist_cluster_kernel<T>(), 1 << g) != (1 << g))
+                return false;
+        int off = 0;
+        for (int g = 0; g < 5; ++g) {
+            for (int i : grp[g]) hmem[off++] = i;
+        }
+        XCAL_CUDA(cudaMemcpyAsync(mem_ids.p, hmem, off * sizeof(int), cudaMemcpyHostToDevice, stream));
+        XCAL_CUDA(cudaEventRecord(forked, stream));
+        off = 0;
+        for (int g = 0; g < 5; ++g) {
+            if (grp[g].empty()) continue;
+            XCAL_CUDA(cudaStreamWaitEvent(gstream[g], forked, 0));
+            kb_cg_persist_cluster<T>(gstream[g], sy, mem_ids.p + off, (int)grp[g].size(), 1 << g, jac, max_iters);
+            XCAL_CUDA(cudaEventRecord(gjoined[g], gstream[g]));
+            XCAL_CUDA(cudaStreamWaitEvent(stream, gjoined[g], 0));
+            off += (int)grp[g].size();
+        }
+        return true;
     }
 
     // one Krylov iteration of every system (early exit where done)

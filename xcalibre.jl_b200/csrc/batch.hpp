@@ -117,6 +117,15 @@ void kb_cg_start(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntile
 template <class T>
 bool kb_cg_persist(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total, int jacobi,
                    unsigned int* bars, int nbars, int* err, int max_iters, int width = 0);
+// the cluster form: every listed system (ids[0..nsys)) as one thread-block
+// cluster of the size its largest member needs; false (nothing launched)
+// when max_tiles exceeds PERSIST_CLUSTER_MAX or the device cannot run it
+template <class T>
+bool kb_cg_persist_cluster(cudaStream_t s, const BSys<T>* sys, const int* ids, int nsys, int max_tiles, int jacobi,
+                           int max_iters);
+// the cluster-form kernel (for persist_cluster_size queries)
+template <class T>
+const void* kb_cg_persist_cluster_kernel();
 template <class T>
 void kb_cg_spmv(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total);
 template <class T>

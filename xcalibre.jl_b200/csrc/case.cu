@@ -1229,11 +1229,17 @@ void Case::solve_captured(int eqn, int comp) {
     // the CG loop as one cooperative kernel node where the driver runs those
     // in graphs (top level; inside the mixed outer WHILE body), its barrier
     // error flag cleared once per step and read after each replay
-    const bool persist = SS.solver == XCAL_SOLVER_CG && persistent_cg &&
-                         (SS.precond == XCAL_PRECOND_JACOBI || SS.precond == XCAL_PRECOND_NONE) &&
-                         kr_coop_capture_ok(mixed);
+    // (only the launch forms the driver runs inside graphs; -1: none)
+    int pwidth = persistent_cg > 1 ? persistent_cg : 0;
+    if (!kr_cluster_capture_ok(mixed)) {
+        if (pwidth == PERSIST_CLUSTER_ONLY) pwidth = -1;
+        if (pwidth == 0) pwidth = PERSIST_COOP_ONLY;
+    }
+    if (!kr_coop_capture_ok(mixed) && pwidth != PERSIST_CLUSTER_ONLY && pwidth != -1)
+        pwidth = pwidth == 0 ? PERSIST_CLUSTER_ONLY : -1;
+    const bool persist = SS.solver == XCAL_SOLVER_CG && persistent_cg && pwidth != -1 &&
+                         (SS.precond == XCAL_PRECOND_JACOBI || SS.precond == XCAL_PRECOND_NONE);
     const int jac = SS.precond == XCAL_PRECOND_JACOBI ? 1 : 0;
-    const int pwidth = persistent_cg > 1 ? persistent_cg : 0;
     if (!mixed) {
         if (SS.precond == XCAL_PRECOND_DILU) dilu_refresh(E, false);
         KrylovVecs<double> V{ws.x.p, ws.r.p, ws.z.p, ws.p.p, ws.q.p, ws.v.p, ws.s.p, ws.t.p};
@@ -1509,7 +1515,11 @@ void Case::capture_step() {
     cudaGraph_t g = nullptr;
     // decided before the capture (the check runs graphs of its own)
     kr_coop_capture_ok(false);
-    if (cfg.precision == XCAL_PREC_MIXED) kr_coop_capture_ok(true);
+    kr_cluster_capture_ok(false);
+    if (cfg.precision == XCAL_PREC_MIXED) {
+        kr_coop_capture_ok(true);
+        kr_cluster_capture_ok(true);
+    }
     XCAL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {
         XCAL_CUDA(cudaMemsetAsync(ws.err.p, 0, sizeof(int), stream));

@@ -87,10 +87,18 @@ template <class T>
 bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
                    T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters,
                    int width = 0, int pf_kb = 0, bool reset_err = true);
+// width: 0 = the cluster form where the system has at most
+// PERSIST_CLUSTER_MAX tiles, else the widest cooperative form that fits;
+// PERSIST_CLUSTER_ONLY = the cluster form only; 256 / 512 / 1024 = that
+// cooperative form only.  false: nothing launched (does not fit).
+constexpr int PERSIST_CLUSTER_ONLY = 2;
+constexpr int PERSIST_COOP_ONLY = 3;  // the widest cooperative form that fits, never the cluster form
 // whether this device and driver run a cooperative kernel captured into a
 // CUDA graph (in_while: inside the body of a conditional WHILE node); found
 // out once per process by capturing and running a one-block no-op that way
 bool kr_coop_capture_ok(bool in_while);
+// the same for a kernel launched as thread-block clusters
+bool kr_cluster_capture_ok(bool in_while);
 // Persistent CG widths: 1024 / 512 threads per block (wide form, systems of
 // at most 1 / 2 tiles per SM) or RED_THREADS (narrow form).  The launchers
 // take the widest form whose co-resident capacity covers the tiles.
@@ -106,6 +114,14 @@ int persist_pick(PersistCaps& c, const void* const kernels[3], int ntiles, int w
 // cooperative launch of kernel (width index w) over ntiles blocks; false
 // (capacity lowered, nothing launched) when the device refuses the size
 bool persist_launch(PersistCaps& c, int w, const void* kernel, int ntiles, cudaStream_t s, void** args);
+// Cluster form of the persistent CG (1024-thread blocks): a system of at
+// most PERSIST_CLUSTER_MAX tiles runs as one thread-block cluster.  The
+// cluster size for `tiles`: the smallest power of two >= tiles that the
+// device schedules for this kernel, or 0 (too many tiles / not schedulable).
+constexpr int PERSIST_CLUSTER_MAX = 16;
+int persist_cluster_size(const void* kernel, int tiles);
+// launch nclusters clusters of C blocks (one system each)
+void persist_cluster_launch(const void* kernel, int C, int nclusters, cudaStream_t s, void** args);
 void kr_finish(cudaStream_t s, int n, const double* x, const double* dx, double* field);
 template <class T>
 void kr_bicg_start(cudaStream_t s, int n, const T* c, const T* r, T* p, KScalars* S, double* part0, double* part1);

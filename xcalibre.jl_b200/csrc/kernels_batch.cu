@@ -143,6 +143,17 @@ __global__ void __launch_bounds__(NT, persist_min_blocks(NT))
                            B.vec[KV_V], B.S, B.part0, B.part1, bars + 2 * tm.x, err, max_iters, 0);
 }
 
+// cluster form: system ids[b / C] is the cluster of blocks b (rank b % C)
+template <class T>
+__global__ void __launch_bounds__(1024, 1) kbk_cg_persist_cl(const BSys<T>* __restrict__ sys,
+                                                            const int* __restrict__ ids, int C, int jacobi,
+                                                            int max_iters) {
+    const BSys<T>& B = sys[ids[blockIdx.x / C]];
+    const TileCtx tc{(int)(blockIdx.x % C), B.ntiles};
+    cg_persist_body<T, 1024, true>(tc, B.A, B.nz, B.P, jacobi, B.vec[KV_X], B.vec[KV_R], B.vec[KV_Z], B.vec[KV_P],
+                                   B.vec[KV_V], B.S, nullptr, nullptr, nullptr, nullptr, max_iters, 0);
+}
+
 // ---- per-case steps of a solve, batched (BAux tables) ----
 #define XCAL_BAUX                                   \
     const int2 tm = tmap[blockIdx.x];               \
@@ -362,6 +373,21 @@ bool kb_cg_persist(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int nti
     return persist_launch(caps, w, kern[w], ntiles_total, s, args);
 }
 template <class T>
+const void* kb_cg_persist_cluster_kernel() {
+    return (const void*)kbk_cg_persist_cl<T>;
+}
+template <class T>
+bool kb_cg_persist_cluster(cudaStream_t s, const BSys<T>* sys, const int* ids, int nsys, int max_tiles, int jacobi,
+                           int max_iters) {
+    const void* k = (const void*)kbk_cg_persist_cl<T>;
+    const int C = persist_cluster_size(k, max_tiles);
+    if (C == 0 || nsys <= 0) return false;
+    int Cv = C;
+    void* args[] = {(void*)&sys, (void*)&ids, &Cv, &jacobi, &max_iters};
+    persist_cluster_launch(k, C, nsys, s, args);
+    return true;
+}
+template <class T>
 void kb_cg_start(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_total) {
     XCAL_BLAUNCH(kbk_cg_start, sys, tmap);
 }
@@ -412,6 +438,8 @@ void kb_bicg_p(cudaStream_t s, const BSys<T>* sys, const int2* tmap, int ntiles_
     template void kb_cg_start<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                  \
     template bool kb_cg_persist<T>(cudaStream_t, const BSys<T>*, const int2*, int, int, unsigned int*, int, int*,  \
                                    int, int);                                                                     \
+    template bool kb_cg_persist_cluster<T>(cudaStream_t, const BSys<T>*, const int*, int, int, int, int);          \
+    template const void* kb_cg_persist_cluster_kernel<T>();                                                         \
     template void kb_cg_spmv<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                   \
     template void kb_cg_update<T>(cudaStream_t, const BSys<T>*, const int2*, int, int);                            \
     template void kb_cg_rz<T>(cudaStream_t, const BSys<T>*, const int2*, int);                                     \

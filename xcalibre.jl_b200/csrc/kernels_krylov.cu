@@ -14,6 +14,8 @@
 // products accumulated in FP64 and the step scalars kept in FP64 on the
 // device and rounded to FP32 where they scale a vector.
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "kernels.hpp"
 #include "krylov_bodies.cuh"
@@ -140,6 +142,16 @@ __global__ void __launch_bounds__(NT, persist_min_blocks(NT))
                  int pf_kb) {
     cg_persist_body<T, NT>(grid_tiles(), A, nz, Pj, jacobi, x, r, z, P0, P1, S, part, part2, bar, err, max_iters,
                            pf_kb);
+}
+
+// the cluster form: the grid is one cluster, block b owns tile b
+template <class T>
+__global__ void __launch_bounds__(1024, 1)
+    k_cg_persist_cl(CSRView A, const T* __restrict__ nz, const T* __restrict__ Pj, int jacobi, T* x, T* r, T* z,
+                    T* P0, T* P1, KScalars* S, int max_iters) {
+    const TileCtx tc{(int)blockIdx.x, (A.n + RED_TILE - 1) / RED_TILE};
+    cg_persist_body<T, 1024, true>(tc, A, nz, Pj, jacobi, x, r, z, P0, P1, S, nullptr, nullptr, nullptr, nullptr,
+                                   max_iters, 0);
 }
 
 // field = x + dx (warm start shift)
@@ -424,19 +436,25 @@ __global__ void k_coop_noop() {}
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-bool kr_coop_capture_ok(bool in_while) {
-    static int state[2] = {-1, -1};
-    int& st = state[in_while ? 1 : 0];
-    if (st >= 0) return st == 1;
+// capture (top level or inside a WHILE body) and run a no-op launched
+// cooperatively (one block) or as one cluster of two blocks
+static bool capture_probe(bool in_while, bool cluster) {
     cudaStream_t s = nullptr, s2 = nullptr;
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(1);
+    cfg.gridDim = dim3(cluster ? 2 : 1);
     cfg.blockDim = dim3(32);
     cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeCooperative;
-    at[0].val.cooperative = 1;
+    if (cluster) {
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 2;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+    } else {
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+    }
     cfg.attrs = at;
     cfg.numAttrs = 1;
     void* noargs[1] = {nullptr};
@@ -490,8 +508,21 @@ bool kr_coop_capture_ok(bool in_while) {
     if (s2) cudaStreamDestroy(s2);
     if (s) cudaStreamDestroy(s);
     cudaGetLastError();
-    st = ok ? 1 : 0;
     return ok;
+}
+
+bool kr_coop_capture_ok(bool in_while) {
+    static int state[2] = {-1, -1};
+    int& st = state[in_while ? 1 : 0];
+    if (st < 0) st = capture_probe(in_while, false) ? 1 : 0;
+    return st == 1;
+}
+
+bool kr_cluster_capture_ok(bool in_while) {
+    static int state[2] = {-1, -1};
+    int& st = state[in_while ? 1 : 0];
+    if (st < 0) st = capture_probe(in_while, true) ? 1 : 0;
+    return st == 1;
 }
 
 static inline int tiles(int n) { return n <= 0 ? 1 : (n + RED_TILE - 1) / RED_TILE; }
@@ -604,6 +635,56 @@ bool persist_launch(PersistCaps& c, int w, const void* kernel, int ntiles, cudaS
     return true;
 }
 
+int persist_cluster_size(const void* kernel, int tiles) {
+    if (tiles <= 0 || tiles > PERSIST_CLUSTER_MAX) return 0;
+    int C = 1;
+    while (C < tiles) C *= 2;
+    // schedulability per (kernel, C), found once
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, bool> ok;
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair(kernel, C);
+    auto it = ok.find(key);
+    if (it == ok.end()) {
+        bool good = true;
+        if (C > 8)
+            good = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+        int num = 0;
+        if (good) {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(C);
+            cfg.blockDim = dim3(1024);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = C;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            good = cudaOccupancyMaxActiveClusters(&num, kernel, &cfg) == cudaSuccess && num >= 1;
+        }
+        cudaGetLastError();
+        it = ok.emplace(key, good).first;
+    }
+    return it->second ? C : 0;
+}
+
+void persist_cluster_launch(const void* kernel, int C, int nclusters, cudaStream_t s, void** args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C * nclusters);
+    cfg.blockDim = dim3(1024);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    XCAL_CUDA(cudaLaunchKernelExC(&cfg, kernel, args));
+    XCAL_CHECK_LAUNCH();
+}
+
 template <class T>
 bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, int jacobi, T* x, T* r, T* z, T* P0,
                    T* P1, KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters,
@@ -612,7 +693,18 @@ bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, in
     static const void* const kern[3] = {(const void*)k_cg_persist<T, 1024>, (const void*)k_cg_persist<T, 512>,
                                         (const void*)k_cg_persist<T, RED_THREADS>};
     const int nt = tiles(A.n);
-    const int w = persist_pick(caps, kern, nt, width);
+    if (width == 0 || width == PERSIST_CLUSTER_ONLY) {
+        const void* kc = (const void*)k_cg_persist_cl<T>;
+        const int C = persist_cluster_size(kc, nt);
+        if (C > 0) {
+            CSRView Av = A;
+            void* args[] = {&Av, (void*)&nz, (void*)&P, &jacobi, &x, &r, &z, &P0, &P1, &S, &max_iters};
+            persist_cluster_launch(kc, C, 1, s, args);
+            return true;
+        }
+        if (width == PERSIST_CLUSTER_ONLY) return false;
+    }
+    const int w = persist_pick(caps, kern, nt, width == PERSIST_COOP_ONLY ? 0 : width);
     if (w < 0) return false;
     XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
     if (reset_err) XCAL_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));

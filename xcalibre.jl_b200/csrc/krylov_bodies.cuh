@@ -7,6 +7,8 @@
 // system's arithmetic -- row sums, reduction trees, scalar decisions -- is the
 // same whether it is solved alone or inside a batch.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "dev_common.cuh"
 #include "kernels.hpp"
 
@@ -677,12 +679,33 @@ constexpr int persist_min_blocks(int nt) { return nt == 1024 ? 1 : nt == 512 ? 2
 // / 128^3 (FP64): the vectors 5% / 1.7% faster; the matrix another 5% at
 // 96^3 but 15% slower at 128^3 (it evicts the gathered vectors), hence the
 // size condition.
-template <class T, int NT>
+// The canonical final tree over the tile partials of a system whose blocks
+// form one thread-block cluster: thread t < T reads block t's partial from
+// its shared memory (the values reduce_partials reads from global memory).
+__device__ __forceinline__ double reduce_cluster(double* mine, int T, double* smem8) {
+    double s = 0.0;
+    if (threadIdx.x < RED_THREADS)
+        for (int i = threadIdx.x; i < T; i += RED_THREADS)
+            s = s + *cooperative_groups::this_cluster().map_shared_rank(mine, i);
+    return block_tree(s, smem8);
+}
+
+// CL (cluster form, wide blocks only): the system's tiles are the blocks of
+// one thread-block cluster (blocks past its tile count have no rows); the
+// barriers are hardware cluster barriers (release / acquire at cluster
+// scope) and the partials travel through distributed shared memory -- no
+// global spin, no atomics, no cooperative launch (clusters are scheduled
+// whole), and each cluster runs on its own.  Every block takes the same
+// decisions, so all reach the same barriers; a last barrier keeps every
+// block's shared memory alive until its peers have read it.
+template <class T, int NT, bool CL = false>
 __device__ __forceinline__ void cg_persist_body(const TileCtx& tc, const CSRView& A, const T* __restrict__ nz,
                                                 const T* __restrict__ Pj, int jacobi, T* x, T* r, T* z, T* P0,
                                                 T* P1, KScalars* S, double* part, double* part2, unsigned int* bar,
                                                 int* err, int max_iters, int pf_kb) {
     constexpr bool WIDE = NT > RED_THREADS;
+    static_assert(!CL || WIDE, "the cluster form uses wide blocks");
+    __shared__ double cl_part[2];  // cluster form: this block's two tile partials
     constexpr int IPT = RED_ITEMS / (NT / RED_THREADS);  // rows per thread
     __shared__ T q_s[RED_TILE];
     __shared__ double pr_s[WIDE ? RED_TILE : 1];
@@ -755,7 +778,12 @@ __device__ __forceinline__ void cg_persist_body(const TileCtx& tc, const CSRView
                 for (int k = 0; k < RED_ITEMS; ++k) acc = acc + pr_s[k * RED_THREADS + v];
         }
         double tot = block_tree(acc, sm);
-        if (threadIdx.x == 0) part[tc.tile] = tot;
+        if (threadIdx.x == 0) {
+            if constexpr (CL)
+                cl_part[0] = tot;
+            else
+                part[tc.tile] = tot;
+        }
         if (!WIDE && threadIdx.x < 3 && (threadIdx.x < 2 || jacobi)) {
             const long r0 = (long)tc.tile * RED_TILE;
             const long nr = min((long)RED_TILE, (long)n - r0);
@@ -763,8 +791,11 @@ __device__ __forceinline__ void cg_persist_body(const TileCtx& tc, const CSRView
             const T* base = threadIdx.x == 0 ? x : threadIdx.x == 1 ? r : Pj;
             if (bytes) l2_prefetch(base + r0, bytes);
         }
-        if (!(ok = grid_barrier(bar, tc.ntiles, nb, err, &sh_err))) break;
-        double pAp = reduce_partials(part, tc.ntiles, sm);
+        if constexpr (CL)
+            cooperative_groups::this_cluster().sync();
+        else if (!(ok = grid_barrier(bar, tc.ntiles, nb, err, &sh_err)))
+            break;
+        double pAp = CL ? reduce_cluster(&cl_part[0], tc.ntiles, sm) : reduce_partials(part, tc.ntiles, sm);
         if (threadIdx.x == 0) {
             double lim = epsT * pNorm2;
             sh_i[0] = (pAp <= lim && fabs(pAp) <= lim) ? 1 : 0;
@@ -813,7 +844,12 @@ __device__ __forceinline__ void cg_persist_body(const TileCtx& tc, const CSRView
                 for (int k = 0; k < RED_ITEMS; ++k) acc2 = acc2 + pr_s[k * RED_THREADS + v];
         }
         double tot2 = block_tree(acc2, sm);
-        if (threadIdx.x == 0) part2[tc.tile] = tot2;
+        if (threadIdx.x == 0) {
+            if constexpr (CL)
+                cl_part[1] = tot2;
+            else
+                part2[tc.tile] = tot2;
+        }
         if (!WIDE && pf_kb > 0 && threadIdx.x < 32) {
             // the tile's slots are contiguous: slices s0 .. s1 (16 KB pieces;
             // lanes 0..15 the values, 16..31 the columns)
@@ -829,8 +865,11 @@ __device__ __forceinline__ void cg_persist_body(const TileCtx& tc, const CSRView
                 if (bytes) l2_prefetch(p0 + o, bytes);
             }
         }
-        if (!(ok = grid_barrier(bar, tc.ntiles, nb, err, &sh_err))) break;
-        double g = reduce_partials(part2, tc.ntiles, sm);
+        if constexpr (CL)
+            cooperative_groups::this_cluster().sync();
+        else if (!(ok = grid_barrier(bar, tc.ntiles, nb, err, &sh_err)))
+            break;
+        double g = CL ? reduce_cluster(&cl_part[1], tc.ntiles, sm) : reduce_partials(part2, tc.ntiles, sm);
         if (threadIdx.x == 0) {  // cg_finalize on the block's copy of the state
             double rn = sqrt(g);
             bool mach = (rn + 1.0 <= 1.0);
@@ -868,6 +907,7 @@ __device__ __forceinline__ void cg_persist_body(const TileCtx& tc, const CSRView
         status = sh_i[2];
         ++ran;
     }
+    if constexpr (CL) cooperative_groups::this_cluster().sync();
     if (ok && tc.tile == 0 && threadIdx.x == 0) {
         S->iter = iter;
         S->done = done;
