@@ -494,64 +494,78 @@ __device__ __forceinline__ void dilu_bwd_row(const CSRView& A, const T* __restri
 // -- the values of the CSR-row sweeps (dilu_fwd_row / dilu_bwd_row), bit
 // for bit.
 constexpr int DILU_BLOCK_THREADS = 1024;
-constexpr int DILU_UNROLL = 8;  // slots per row loaded together (more: a loop)
+
+// One level of a sweep over level positions k0..k1.  FP32: each thread
+// takes the rows k and k + blockDim.x together (all their slot loads issued
+// before either row's sum), so a level wider than the block costs one
+// dependent load chain per pair of rows, not per row; FP64 keeps one row at a
+// time (two rows' registers spill at 1024 threads).  LOWER: forward
+// substitution (y_i = b_i - sum (a_ij y_j) (1/D_j)); else backward (x_i =
+// (x_i - sum a_ij x_j) / D_i).  The first U slots of a row sit in registers,
+// the rest are read in a loop; each row's sum runs in its own entry order.
+template <class T, bool LOWER>
+__device__ __forceinline__ void dilu_level(const LevelView<T>& L, int k0, int k1, const T* __restrict__ D,
+                                           const T* __restrict__ b, T* ys) {
+    constexpr int R = sizeof(T) == 4 ? 2 : 1;  // rows per thread per step
+    constexpr int U = sizeof(T) == 4 ? 6 : 8;
+    for (int k = k0 + threadIdx.x; k < k1; k += R * blockDim.x) {
+        int kk[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) kk[r] = k + r * (int)blockDim.x;
+        int i[R], c[R], base[R];
+        T rhs[R];
+        int cj[R][U];
+        T vj[R][U], dj[R][U];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            c[r] = 0;
+            i[r] = 0;
+            base[r] = 0;
+            rhs[r] = T(0);
+            if (kk[r] < k1) {
+                i[r] = L.rows[kk[r]];
+                c[r] = L.cnt[kk[r]];
+                base[r] = L.slice[kk[r] / SELL_C] + (kk[r] % SELL_C);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (kk[r] < k1) rhs[r] = LOWER ? b[i[r]] : D[i[r]];
+#pragma unroll
+            for (int j = 0; j < U; ++j)
+                if (j < c[r]) {
+                    const int e = base[r] + SELL_C * j;
+                    cj[r][j] = ld_stream(L.col + e);
+                    vj[r][j] = ld_stream(L.val + e);
+                    if (LOWER) dj[r][j] = ld_stream(L.dinv + e);
+                }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (kk[r] >= k1) continue;
+            T sum = T(0);
+#pragma unroll
+            for (int j = 0; j < U; ++j)
+                if (j < c[r]) sum = LOWER ? sum + (vj[r][j] * ys[cj[r][j]]) * dj[r][j] : sum + vj[r][j] * ys[cj[r][j]];
+            for (int j = U; j < c[r]; ++j) {
+                const int e = base[r] + SELL_C * j;
+                sum = LOWER ? sum + (ld_stream(L.val + e) * ys[ld_stream(L.col + e)]) * ld_stream(L.dinv + e)
+                            : sum + ld_stream(L.val + e) * ys[ld_stream(L.col + e)];
+            }
+            ys[i[r]] = LOWER ? rhs[r] - sum : (ys[i[r]] - sum) / rhs[r];
+        }
+    }
+}
 
 template <class T>
 __device__ __forceinline__ void dilu_level_sweep(int n, const LevelView<T>& lo, const LevelView<T>& up,
                                                  const T* __restrict__ D, const T* __restrict__ b, T* y, T* ys) {
     for (int l = 0; l < lo.nlev; ++l) {
-        const int k1 = lo.off[l + 1];
-        for (int k = lo.off[l] + threadIdx.x; k < k1; k += blockDim.x) {
-            const int i = lo.rows[k], c = lo.cnt[k];
-            const int base = lo.slice[k / SELL_C] + (k % SELL_C);
-            const T bi = b[i];
-            int cj[DILU_UNROLL];
-            T vj[DILU_UNROLL], dj[DILU_UNROLL];
-#pragma unroll
-            for (int j = 0; j < DILU_UNROLL; ++j)
-                if (j < c) {
-                    const int e = base + SELL_C * j;
-                    cj[j] = ld_stream(lo.col + e);
-                    vj[j] = ld_stream(lo.val + e);
-                    dj[j] = ld_stream(lo.dinv + e);
-                }
-            T sum = T(0);
-#pragma unroll
-            for (int j = 0; j < DILU_UNROLL; ++j)
-                if (j < c) sum = sum + (vj[j] * ys[cj[j]]) * dj[j];
-            for (int j = DILU_UNROLL; j < c; ++j) {
-                const int e = base + SELL_C * j;
-                sum = sum + (ld_stream(lo.val + e) * ys[ld_stream(lo.col + e)]) * ld_stream(lo.dinv + e);
-            }
-            ys[i] = bi - sum;
-        }
+        dilu_level<T, true>(lo, lo.off[l], lo.off[l + 1], D, b, ys);
         __syncthreads();
     }
     for (int l = 0; l < up.nlev; ++l) {
-        const int k1 = up.off[l + 1];
-        for (int k = up.off[l] + threadIdx.x; k < k1; k += blockDim.x) {
-            const int i = up.rows[k], c = up.cnt[k];
-            const int base = up.slice[k / SELL_C] + (k % SELL_C);
-            const T di = D[i];
-            int cj[DILU_UNROLL];
-            T vj[DILU_UNROLL];
-#pragma unroll
-            for (int j = 0; j < DILU_UNROLL; ++j)
-                if (j < c) {
-                    const int e = base + SELL_C * j;
-                    cj[j] = ld_stream(up.col + e);
-                    vj[j] = ld_stream(up.val + e);
-                }
-            T sum = T(0);
-#pragma unroll
-            for (int j = 0; j < DILU_UNROLL; ++j)
-                if (j < c) sum = sum + vj[j] * ys[cj[j]];
-            for (int j = DILU_UNROLL; j < c; ++j) {
-                const int e = base + SELL_C * j;
-                sum = sum + ld_stream(up.val + e) * ys[ld_stream(up.col + e)];
-            }
-            ys[i] = (ys[i] - sum) / di;
-        }
+        dilu_level<T, false>(up, up.off[l], up.off[l + 1], D, b, ys);
         __syncthreads();
     }
     if (ys != y)
