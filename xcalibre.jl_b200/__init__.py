@@ -13,6 +13,7 @@ from .api import (B200Backend, Bicgstab, Case, Cg, Configuration, Context, Devic
                   assign, build_config, construct_periodic, initialise_, launch_count, run_, Batch,
                   footprint_estimate)
 from .foam import Mesh3, build_mesh3
+from .foamio import FOAM3D_mesh, read_polymesh, write_polymesh
 from .meshgen import PolyMesh, box_polymesh, cavity_polymesh, channel_polymesh, periodic_box_polymesh
 
 __all__ = [n for n in dir() if not n.startswith("_")] + ["_abi"]
