@@ -270,6 +270,14 @@ int32_t xcal_case_get_system(const xcal_case* cs, int32_t eqn, int32_t component
                              double* nzval, double* b);
 /* initialise! (src/Fields/Fields_0_types.jl:381-401) and field transfer */
 int32_t xcal_case_set_field(xcal_case* cs, int32_t field, const double* host, int64_t count);
+/* Checkpoint restore (no reference counterpart: run! always starts from U
+ * and p).  After the state fields of a saved case have been set (U, p,
+ * MDOTF, NUEFF, GRADP, UF, PF and the rest of the readable fields), this
+ * marks the state as complete: the next iteration does not redo the run's
+ * initial calculations (face velocities and mass flux from U, grad p,
+ * nu_eff; Solvers_1_SIMPLE.jl:150-156), so the case continues exactly as
+ * the saved one would have. */
+int32_t xcal_case_mark_initialised(xcal_case* cs);
 int32_t xcal_case_get_field(const xcal_case* cs, int32_t field, double* host, int64_t count);
 /* replace DirichletFunction face values of BC `bc_index` of field
  * (XCAL_EQN_U or XCAL_EQN_P) -- the host-evaluated f(centre, time, i) */

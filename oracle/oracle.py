@@ -47,6 +47,7 @@ def lib():
             "orc_case_get_system": (None, [vp, i32, i32, pd, pd]),
             "orc_case_set_field": (i32, [vp, i32, pd, C.c_long]),
             "orc_case_get_field": (i32, [vp, i32, pd, C.c_long]),
+            "orc_case_mark_initialised": (i32, [vp]),
             "orc_simple_iterate": (i32, [vp, i32, pd, pi, pi]),
             "orc_piso_step": (i32, [vp, i32, pd, pd]),
             "orc_initial_calculations": (None, [vp]),
@@ -203,6 +204,9 @@ class OracleCase:
         nc, per = self._size(field)
         a = _d(np.asarray(values, dtype=np.float64).reshape(nc * per))
         assert lib().orc_case_set_field(self.h, field, _p(a, C.c_double), a.size) == 0
+
+    def mark_initialised(self):
+        assert lib().orc_case_mark_initialised(self.h) == 0
 
     def get_field(self, field):
         nc, per = self._size(field)

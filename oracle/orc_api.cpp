@@ -228,6 +228,13 @@ int orc_case_set_field(void* cp, int field, const double* host, long count) {
     return 0;
 }
 
+// the state set by orc_case_set_field is complete: the next iteration does
+// not redo the run's initial calculations (checkpoint restore)
+int orc_case_mark_initialised(void* cp) {
+    ((Case*)cp)->initialised = true;
+    return 0;
+}
+
 int orc_case_get_field(void* cp, int field, double* host, long count) {
     Case* C = (Case*)cp;
     int ncomp, per;

@@ -61,6 +61,7 @@ SIGNATURES = {
     "xcal_case_set_profiling": (_i32, [_vp, _i32]),
     "xcal_case_set_graph_mode": (_i32, [_vp, _i32]),
     "xcal_case_set_persistent": (_i32, [_vp, _i32]),
+    "xcal_case_mark_initialised": (_i32, [_vp]),
     "xcal_case_tuning": (_i32, [_vp, _pi]),
     "xcal_case_set_dilu_mode": (_i32, [_vp, _i32]),
     "xcal_case_get_profile": (_i32, [_vp, _i32, _pd, _pi64]),

@@ -626,6 +626,21 @@ class Case:
         """0 = autotuned, 1 = one-block sweeps, 2 = per-level kernels."""
         self._chk(lib().xcal_case_set_dilu_mode(self.h, int(mode)))
 
+    def checkpoint(self) -> dict:
+        """The case's state as host arrays (every field the ABI reads: U, p,
+        face mass flux, face velocity and pressure, nu_eff, gradients, rD,
+        H...): with ``restore`` a new case on the same mesh and configuration
+        continues exactly as this one would."""
+        return {name: self.get_field(getattr(_abi, name)).copy() for name in CHECKPOINT_FIELDS}
+
+    def restore(self, state: dict) -> None:
+        """Set the fields of a ``checkpoint`` and mark the state complete, so
+        the next iteration does not redo the run's initial calculations."""
+        for name in CHECKPOINT_FIELDS:
+            if name in state:
+                self.set_field(getattr(_abi, name), state[name])
+        self._chk(lib().xcal_case_mark_initialised(self.h))
+
     def set_persistent(self, on=True):
         """Persistent CG (one launch per solve): False / True, or 2 (the
         cluster form only) or 256 / 512 / 1024 (that cooperative block form
@@ -737,10 +752,47 @@ def launch_count() -> int:
 _CTX_CACHE: dict = {}
 
 
-def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0, inner_loops=None):
+class VTK:
+    """Output format: .vtu files (src/IOFormats/VTK/VTK_writer_3D.jl)."""
+
+
+class OpenFOAM:
+    """Output format: an OpenFOAM case directory (src/IOFormats/OpenFOAM/OpenFOAM_writer.jl)."""
+
+
+CHECKPOINT_FIELDS = ("FIELD_U", "FIELD_P", "FIELD_MDOTF", "FIELD_NUEFF", "FIELD_GRADP", "FIELD_GRADU", "FIELD_RD",
+                     "FIELD_HV", "FIELD_DIVHV", "FIELD_NUT", "FIELD_NUTF", "FIELD_UF", "FIELD_PF", "FIELD_RDF")
+
+
+def save_checkpoint(state: dict, path: str) -> None:
+    """Write a Case.checkpoint() to ``path`` (numpy .npz, exact doubles)."""
+    np.savez(path, **state)
+
+
+def load_checkpoint(path: str) -> dict:
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
+def _output_fields(case, model, transient_les: bool):
+    fields = [("U", case.get_field(_abi.FIELD_U)), ("p", case.get_field(_abi.FIELD_P))]
+    if transient_les:
+        fields.append(("nut", case.get_field(_abi.FIELD_NUT)))
+    return fields
+
+
+def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0, inner_loops=None, output=None,
+         output_dir: str | None = None):
     """run! (Solvers_3_solver_dispatch.jl:120,225): SIMPLE for Steady, PISO
     for Transient.  Returns the residual histories (Ux, Uy, Uz, p) and writes
-    the final fields back into ``model.momentum``."""
+    the final fields back into ``model.momentum``.
+
+    Results are written as the reference writes them (Solvers_1_SIMPLE.jl:
+    235-257, Solvers_2_PISO.jl:205): every ``runtime.write_interval``
+    iterations and, for SIMPLE, at convergence; nothing when write_interval
+    is negative.  ``output``: VTK() (default) or OpenFOAM(); files go to
+    ``output_dir`` (default: the working directory), written on a
+    background thread while the solve continues."""
     if ncorrectors != 0:
         raise NotImplementedError("non-orthogonal correctors are outside the implemented path")
     backend = config.hardware.backend
@@ -753,19 +805,58 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
     cfg, keep = build_config(model, config, pref, inner_loops)
     dmesh = DeviceMesh(ctx, model.domain)
     case = Case(dmesh, cfg)
+    wi = int(config.runtime.write_interval)
+    transient = isinstance(model.time, Transient)
+    writer = aw = None
+    if wi > 0 or (wi == 0 and not transient):
+        import os
+        from .writers import AsyncWriter, FOAMWriter, VTKWriter3D
+        pm = model.domain.polymesh
+        if pm is None:
+            raise ValueError("writing results needs the mesh's polyMesh (build it with build_mesh3 / FOAM3D_mesh)")
+        out_dir = output_dir or os.getcwd()
+        writer = (FOAMWriter(pm, out_dir, config.boundaries) if isinstance(output, OpenFOAM) else VTKWriter3D(pm))
+        aw = AsyncWriter()
+
+    def write(k):
+        fields = _output_fields(case, model, transient and isinstance(model.turbulence, LES))
+        if isinstance(writer, FOAMWriter):
+            tdir = ("%.8f" % (k * config.runtime.time_step)) if transient else "%d" % k
+            aw.submit(writer.write, tdir, fields)
+        else:
+            name = ("time_%d.vtu" if transient else "iteration_%d.vtu") % k
+            aw.submit(writer.write, os.path.join(out_dir, name), fields)
+
     try:
         case.set_field(_abi.FIELD_U, model.momentum.U)
         case.set_field(_abi.FIELD_P, model.momentum.p)
         n = config.runtime.iterations
-        if isinstance(model.time, Transient):
-            res, _ = case.piso_step(n)
-        else:
-            res, _ = case.simple_iterate(n)
+        step = wi if wi > 0 else n
+        hist, done = [], 0
+        while done < n:
+            k = min(step, n - done)
+            if transient:
+                r, _ = case.piso_step(k)
+                conv = False
+            else:
+                r, conv = case.simple_iterate(k)
+            hist.append(r)
+            done += len(r)
+            if conv and writer is not None:
+                write(done)
+                break
+            if conv:
+                break
+            if wi > 0 and done % wi == 0:
+                write(done)
+        res = np.concatenate(hist, axis=0) if hist else np.zeros((0, 4))
         model.momentum.U[:] = case.get_field(_abi.FIELD_U)
         model.momentum.p[:] = case.get_field(_abi.FIELD_P)
         if isinstance(model.turbulence, LES):
             model.nut[:] = case.get_field(_abi.FIELD_NUT)
     finally:
+        if aw is not None:
+            aw.close()
         case.close()
         dmesh.close()
     return {"Ux": res[:, 0], "Uy": res[:, 1], "Uz": res[:, 2], "p": res[:, 3]}

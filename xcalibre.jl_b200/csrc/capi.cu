@@ -329,6 +329,12 @@ int32_t xcal_case_set_profiling(xcal_case* cs, int32_t enable) {
     return XCAL_OK;
 }
 
+int32_t xcal_case_mark_initialised(xcal_case* cs) {
+    if (!cs) return XCAL_ERR_INVALID;
+    cs->c->initialised = true;
+    return XCAL_OK;
+}
+
 int32_t xcal_case_set_persistent(xcal_case* cs, int32_t mode) {
     if (!cs) return XCAL_ERR_INVALID;
     if (mode != 0 && mode != 1 && mode != 2 && mode != 256 && mode != 512 && mode != 1024) return XCAL_ERR_INVALID;

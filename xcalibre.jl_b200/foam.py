@@ -40,6 +40,7 @@ class Mesh3:
     patch_start: np.ndarray      # int32 [n_patches]
     patch_count: np.ndarray      # int32 [n_patches]
     points: np.ndarray | None = None
+    polymesh: object = None      # the PolyMesh it was built from (nodes and faces, for the writers)
 
     @property
     def n_ifaces(self) -> int:
@@ -95,4 +96,5 @@ def build_mesh3(pm: PolyMesh) -> Mesh3:
                               for f, _ in _abi.MeshBuffers._fields_})
     if lib().xcal_foam_mesh_build(C.byref(desc), C.byref(out)) != 0:
         raise ValueError("invalid polyMesh (patch sizes, node or cell indices)")
+    m.polymesh = pm
     return m
