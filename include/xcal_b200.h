@@ -168,6 +168,9 @@ typedef struct {
     int32_t has_pref;           /* run!(...; pref) given                     */
     double pref;
     int32_t inner_loops;        /* PISO correctors (run!(...; inner_loops))  */
+    int32_t ncorrectors;        /* SIMPLE non-orthogonal correctors
+                                   (run!(...; ncorrectors),
+                                   Solvers_1_SIMPLE.jl:196-206); PISO: 0  */
     int32_t precision;          /* XCAL_PREC_*                               */
     double inner_rtol;          /* mixed: relative tolerance of each FP32
                                    inner solve (0 = default 1e-3)            */

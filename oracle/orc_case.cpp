@@ -1146,6 +1146,51 @@ double max_courant(Case& C) {  // Solvers_0_functions.jl:253-276
 }
 
 // one SIMPLE iteration (Solvers_1_SIMPLE.jl:164-240); returns converged
+// nonorthogonal_face_correction (Solvers_1_SIMPLE.jl:267-318) with
+// correction_weight (:320-333): over every internal face
+//   w      = |c2 - f'| / |c2 - c1|, f' = c1 - q (c1 - c2),
+//            q = ((xf - c1).(c2 - c1)) / ((c2 - c1).(c2 - c1))
+//   gradi  = w grad[c1] + (1 - w) grad[c2]
+//   gradf  = gradi + ((p2 - p1)/delta - gradi.e) e
+//   T      = Sf - Ef, Sf = area n, Ef = dPN (|n|^2 / (dPN.n)) area
+//   corr   = (rDf_f gradf) . T;  b[c1] += corr, b[c2] -= corr
+// The reference adds with atomics (any order); here each cell adds its
+// faces' corrections in its cell_faces order, which the product follows.
+static double nonorth_face(const Case& C, int f) {
+    const Mesh& m = *C.m;
+    const int c1 = m.owner[f], c2 = m.neigh[f];
+    const V3 xC = m.ccentre[c1], xN = m.ccentre[c2], xf = m.fcentre[f], n = m.fnormal[f], e = m.fe[f];
+    const V3 c1f = xf - xC, c1c2 = xN - xC;
+    const double q = dot(c1f, c1c2) / dot(c1c2, c1c2);
+    const V3 fp = xC - q * (xC - xN);
+    const double w = norm(xN - fp) / norm(xN - xC);
+    const V3 dPN = xN - xC;
+    const V3 g1 = {C.gradp[0][c1], C.gradp[1][c1], C.gradp[2][c1]};
+    const V3 g2 = {C.gradp[0][c2], C.gradp[1][c2], C.gradp[2][c2]};
+    const V3 gi = w * g1 + (1.0 - w) * g2;
+    const double s = (C.p[c2] - C.p[c1]) / m.fdelta[f] - dot(gi, e);
+    const V3 gf = gi + s * e;
+    const double a = m.farea[f];
+    const V3 Sf = a * n;
+    const double nn = norm(n) * norm(n);
+    const V3 Ef = (dPN * (nn / dot(dPN, n))) * a;
+    const V3 T = Sf - Ef;
+    return dot(C.rDf[f] * gf, T);
+}
+
+static void nonorthogonal_correction(Case& C) {
+    const Mesh& m = *C.m;
+    for (int i = 0; i < C.nC; ++i) {
+        double bi = C.bp[i];
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            const int f = m.cell_faces[k];
+            const double corr = nonorth_face(C, f);
+            bi = m.owner[f] == i ? bi + corr : bi - corr;
+        }
+        C.bp[i] = bi;
+    }
+}
+
 bool simple_iteration(Case& C, double* res4) {
     if (!C.initialised) initial_calculations(C);
     C.iteration += 1;
@@ -1157,6 +1202,18 @@ bool simple_iteration(Case& C, double* res4) {
     double rp = solve_equation_p(C, nullptr);
     explicit_relaxation_p(C, C.cfg.p_solver.relax);
     grad_p(C);
+    // non-orthogonal correctors (Solvers_1_SIMPLE.jl:196-206): re-assemble
+    // p with its BCs (no reference pressure), add the face corrections,
+    // solve with the preconditioner of the first solve, relax against the
+    // p of before the first solve, new gradient
+    for (int k = 0; k < C.cfg.ncorrectors; ++k) {
+        discretise_p(C);
+        apply_bcs(C, false, 0);
+        nonorthogonal_correction(C);
+        rp = solve_system(C, false, 0, nullptr);
+        explicit_relaxation_p(C, C.cfg.p_solver.relax);
+        grad_p(C);
+    }
     correct(C);
     turbulence(C);
     res4[0] = r3[0];

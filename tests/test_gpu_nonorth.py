@@ -1,0 +1,69 @@
+"""Non-orthogonal correctors on the GPU against the oracle (skewed channel,
+ncorrectors 1 and 2, FP64, host-polled and graph mode; tolerance the 1e-10 relative L2 of the parity
+tests, expected 0), and a batch of skewed cases with correctors giving the
+results the cases give alone (bit for bit)."""
+import numpy as np
+import pytest
+
+from test_nonorth_oracle import skewed_channel
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("ncorr", [1, 2])
+def test_correctors_parity(x, orc, ctx, ncorr, graph):
+    mesh = skewed_channel(x, n=(12, 7, 6), seed=4)
+    model, config = x.cases.channel_case(mesh, iterations=4)
+    cfg, keep = x.build_config(model, config, ncorrectors=ncorr)
+    dm = x.DeviceMesh(ctx, mesh)
+    g = x.Case(dm, cfg)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    for c in (g, o):
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+    if graph:
+        g.set_graph_mode(True)
+    rg, _ = g.simple_iterate(4)
+    ro, _ = o.simple_iterate(4)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    for f in (x._abi.FIELD_U, x._abi.FIELD_P, x._abi.FIELD_MDOTF):
+        assert rel(g.get_field(f), o.get_field(f)) <= TOL
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_correctors_batch_matches_single(x, ctx, prec):
+    specs = [((10, 6, 5), 3), ((14, 8, 7), 5), ((9, 9, 4), 6)]
+    iters = 3
+
+    def mk(n, seed):
+        mesh = skewed_channel(x, n=n, seed=seed)
+        model, config = x.cases.channel_case(mesh, iterations=iters, precision=prec)
+        cfg, keep = x.build_config(model, config, ncorrectors=2)
+        dm = x.DeviceMesh(ctx, mesh)
+        c = x.Case(dm, cfg)
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+        return c, (dm, keep)
+
+    alone = []
+    for n, seed in specs:
+        c, keep = mk(n, seed)
+        res, _ = c.simple_iterate(iters)
+        alone.append((res, c.get_field(x._abi.FIELD_P)))
+    batch = x.api.Batch(ctx, 4, 1 << 34)
+    members = [mk(n, seed) for n, seed in specs]
+    for c, _ in members:
+        assert batch.add(c)
+    hist = np.stack([batch.simple_iterate()[0] for _ in range(iters)], axis=1)
+    for k, (c, _) in enumerate(members):
+        assert np.array_equal(hist[k], alone[k][0]), (k, hist[k], alone[k][0])
+        assert np.array_equal(c.get_field(x._abi.FIELD_P), alone[k][1])
+    batch.close()

@@ -429,9 +429,10 @@ def _solver_desc(s: SolverSetup) -> _abi.SolverSetupDesc:
                                 relax=float(s.relax), atol=float(s.atol), rtol=float(s.rtol), itmax=int(s.itmax))
 
 
-def build_config(model: Physics, config: Configuration, pref=None, inner_loops=None):
+def build_config(model: Physics, config: Configuration, pref=None, inner_loops=None, ncorrectors: int = 0):
     """Translate the Python API objects into an xcal_config (keep the second
-    return value alive while the config is in use)."""
+    return value alive while the config is in use).  ncorrectors: SIMPLE
+    non-orthogonal correctors (run!(...; ncorrectors))."""
     mesh = model.domain
     keep: list = []
     transient = isinstance(model.time, Transient)
@@ -457,7 +458,7 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
         U_solver=_solver_desc(config.solvers["U"]), p_solver=_solver_desc(config.solvers["p"]),
         iterations=int(config.runtime.iterations), dt=float(config.runtime.time_step),
         has_pref=0 if pref is None else 1, pref=0.0 if pref is None else float(pref),
-        inner_loops=int(inner_loops), precision=prec,
+        inner_loops=int(inner_loops), ncorrectors=int(ncorrectors), precision=prec,
         inner_rtol=float(getattr(backend, "inner_rtol", 1e-3)),
         n_bc_U=len(bnd["U"]), n_bc_p=len(bnd["p"]), n_bc_nut=len(nut_bcs),
         bc_U=C.cast(bU, C.POINTER(_abi.BCDesc)), bc_p=C.cast(bP, C.POINTER(_abi.BCDesc)),
@@ -793,8 +794,8 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
     is negative.  ``output``: VTK() (default) or OpenFOAM(); files go to
     ``output_dir`` (default: the working directory), written on a
     background thread while the solve continues."""
-    if ncorrectors != 0:
-        raise NotImplementedError("non-orthogonal correctors are outside the implemented path")
+    if ncorrectors != 0 and isinstance(model.time, Transient):
+        raise NotImplementedError("non-orthogonal correctors are implemented for SIMPLE (steady) runs")
     backend = config.hardware.backend
     if not isinstance(backend, B200Backend):
         raise TypeError("Hardware.backend must be B200Backend() for this implementation")
@@ -802,7 +803,7 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
     if dev not in _CTX_CACHE:
         _CTX_CACHE[dev] = Context(dev)
     ctx = _CTX_CACHE[dev]
-    cfg, keep = build_config(model, config, pref, inner_loops)
+    cfg, keep = build_config(model, config, pref, inner_loops, ncorrectors)
     dmesh = DeviceMesh(ctx, model.domain)
     case = Case(dmesh, cfg)
     wi = int(config.runtime.write_interval)

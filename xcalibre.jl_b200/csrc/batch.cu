@@ -72,7 +72,7 @@ struct Batch {
     // third components, pressure assembly, correction), captured at first
     // use and replayed on the case's own stream: everything they read is
     // device state or fixed for the case, as in graph mode
-    static constexpr int N_PHASES = 5;
+    static constexpr int N_PHASES = 8;
     std::vector<std::array<ChunkGraph, N_PHASES>> case_graph;
 
     void drop_graphs() {
@@ -205,8 +205,9 @@ struct Batch {
         const xcal_config& b = c->cfg;
         if (a.precision != b.precision || a.U_solver.solver != b.U_solver.solver ||
             a.U_solver.precond != b.U_solver.precond || a.p_solver.solver != b.p_solver.solver ||
-            a.p_solver.precond != b.p_solver.precond)
-            fail(XCAL_ERR_UNSUPPORTED, "batch: cases must share precision, solvers and preconditioners");
+            a.p_solver.precond != b.p_solver.precond || a.ncorrectors != b.ncorrectors)
+            fail(XCAL_ERR_UNSUPPORTED,
+                 "batch: cases must share precision, solvers, preconditioners and non-orthogonal correctors");
     }
 
     void add(Case* c, size_t charge) {
@@ -681,15 +682,38 @@ struct Batch {
             3);
         const clk::time_point t2 = clk::now();
         solve(3);
+        const int ncorr = cases[0]->cfg.ncorrectors;
+        if (ncorr > 0) {
+            // non-orthogonal correctors (Solvers_1_SIMPLE.jl:196-206): every
+            // corrector's pressure solve is one batched solve
+            auto relax_grad = [&](Case* c) {
+                c->explicit_relaxation_p(c->cfg.p_solver.relax);
+                c->grad_p();
+            };
+            per_case(relax_grad, 5);
+            for (int k = 0; k < ncorr; ++k) {
+                per_case(
+                    [&](Case* c) {
+                        c->discretise(XCAL_EQN_P);
+                        c->apply_bcs(XCAL_EQN_P, 0);
+                        c->nonorth_correct();
+                    },
+                    6);
+                solve(3);
+                per_case(relax_grad, 5);
+            }
+        }
         const clk::time_point t3 = clk::now();
         per_case(
             [&](Case* c) {
-                c->explicit_relaxation_p(c->cfg.p_solver.relax);
-                c->grad_p();
+                if (ncorr == 0) {
+                    c->explicit_relaxation_p(c->cfg.p_solver.relax);
+                    c->grad_p();
+                }
                 c->correct();
                 c->turbulence();
             },
-            4);
+            ncorr > 0 ? 7 : 4);
         XCAL_CUDA(cudaMemcpyAsync(hres, res.p, 4 * cases.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
         sync();
         const clk::time_point t4 = clk::now();

@@ -628,6 +628,9 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     AllocScope acc(&bytes);
     if (cfg.U_solver.relax <= 0.0 || cfg.p_solver.relax <= 0.0) fail(XCAL_ERR_INVALID, "relax must be > 0");
     if (cfg.algorithm == XCAL_ALGO_PISO && cfg.dt <= 0.0) fail(XCAL_ERR_INVALID, "PISO needs dt > 0");
+    if (cfg.ncorrectors < 0) fail(XCAL_ERR_INVALID, "ncorrectors must be >= 0");
+    if (cfg.ncorrectors > 0 && cfg.algorithm != XCAL_ALGO_SIMPLE)
+        fail(XCAL_ERR_UNSUPPORTED, "non-orthogonal correctors are implemented for SIMPLE");
     if (cfg.precision != XCAL_PREC_FP64 && cfg.precision != XCAL_PREC_MIXED)
         fail(XCAL_ERR_INVALID, "unknown precision mode");
     for (auto* ss : {&cfg.U_solver, &cfg.p_solver}) {
@@ -657,6 +660,7 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     for (int d = 0; d < 9; ++d) gradU[d].alloc(nC);
     for (DBuf<double>* b : {&p, &rD, &divHv, &nut, &Delta, &prev, &courant, &dx13}) b->alloc(nC);
     for (DBuf<double>* b : {&mdot, &nueff, &nutf, &pf, &rDf}) b->alloc(nF);
+    if (cfg.ncorrectors > 0) build_nonorth(*m, stream);
     for (int d = 0; d < 3; ++d) {
         Uc[d].zero(stream);
         gradp[d].zero(stream);
@@ -1421,6 +1425,61 @@ void Case::flux_divergence() {  // Solvers_1_SIMPLE.jl:177-185
 
 void Case::explicit_relaxation_p(double a) { launch_relax_explicit(stream, mesh->nC, p.p, prev.p, a); }
 
+// The face constants of nonorthogonal_face_correction (Solvers_1_SIMPLE.jl:
+// 267-333), per internal face in storage order, on the host once: the
+// interpolation weight w of correction_weight, e, and T = Sf - Ef with
+// Ef = dPN (|n|^2 / (dPN.n)) area.  Layout: 7 arrays of nI (w, ex, ey, ez,
+// Tx, Ty, Tz).
+void Case::build_nonorth(const DevMesh& m, cudaStream_t s) {
+    const int nB = m.nB, nI = m.nI;
+    std::vector<double> t(7 * (size_t)nI);
+    for (int j = 0; j < nI; ++j) {
+        const int f = nB + j, c1 = m.owner[f], c2 = m.neigh[f];
+        const double xCx = m.ccx[c1], xCy = m.ccy[c1], xCz = m.ccz[c1];
+        const double xNx = m.ccx[c2], xNy = m.ccy[c2], xNz = m.ccz[c2];
+        // correction_weight
+        const double afx = m.fcx[f] - xCx, afy = m.fcy[f] - xCy, afz = m.fcz[f] - xCz;
+        const double acx = xNx - xCx, acy = xNy - xCy, acz = xNz - xCz;
+        const double q = (afx * acx + afy * acy + afz * acz) / (acx * acx + acy * acy + acz * acz);
+        const double fpx = xCx - q * (xCx - xNx), fpy = xCy - q * (xCy - xNy), fpz = xCz - q * (xCz - xNz);
+        const double d1x = xNx - fpx, d1y = xNy - fpy, d1z = xNz - fpz;
+        const double d2x = xNx - xCx, d2y = xNy - xCy, d2z = xNz - xCz;
+        const double w = std::sqrt(d1x * d1x + d1y * d1y + d1z * d1z) / std::sqrt(d2x * d2x + d2y * d2y + d2z * d2z);
+        // T = Sf - Ef
+        const double nx = m.nxh[f], ny = m.nyh[f], nz = m.nzh[f], a = m.area[f];
+        const double nr = std::sqrt(nx * nx + ny * ny + nz * nz);
+        const double nn = nr * nr;
+        const double dn = acx * nx + acy * ny + acz * nz;
+        const double r = nn / dn;
+        t[j] = w;
+        t[nI + (size_t)j] = m.ex[f];
+        t[2 * (size_t)nI + j] = m.ey[f];
+        t[3 * (size_t)nI + j] = m.ez[f];
+        t[4 * (size_t)nI + j] = a * nx - (acx * r) * a;
+        t[5 * (size_t)nI + j] = a * ny - (acy * r) * a;
+        t[6 * (size_t)nI + j] = a * nz - (acz * r) * a;
+    }
+    nonorth.upload(t, s);
+}
+
+void Case::nonorth_correct() {
+    const double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
+    launch_nonorth_correct(stream, mv(), nonorth.p, p.p, gp, rDf.p, P.b[0].p);
+}
+
+// the non-orthogonal correctors of a SIMPLE iteration (Solvers_1_SIMPLE.jl:
+// 196-206); rp becomes the last corrector solve's residual
+void Case::nonorth_correctors(double& rp) {
+    for (int k = 0; k < cfg.ncorrectors; ++k) {
+        discretise(XCAL_EQN_P);
+        apply_bcs(XCAL_EQN_P, 0);
+        nonorth_correct();
+        rp = solve_system(XCAL_EQN_P, 0, &last_iters[3]);
+        explicit_relaxation_p(cfg.p_solver.relax);
+        grad_p();
+    }
+}
+
 void Case::grad_p() {  // Calculate_0_gradient.jl:105-111
     launch_interp_scalar(stream, mv(), bcP.view(), p.p, pf.p, nullptr, 0.0);
     double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
@@ -1474,9 +1533,10 @@ void Case::simple_body(double r3[3], double& rp, bool timed) {
     XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     if (timed) XCAL_CUDA(cudaEventRecord(ev[2], stream));
     rp = solve_equation_p();
-    if (timed) XCAL_CUDA(cudaEventRecord(ev[3], stream));
     explicit_relaxation_p(cfg.p_solver.relax);
     grad_p();
+    nonorth_correctors(rp);
+    if (timed) XCAL_CUDA(cudaEventRecord(ev[3], stream));
     correct();
     turbulence();
     if (timed) XCAL_CUDA(cudaEventRecord(ev[4], stream));

@@ -30,6 +30,9 @@ void launch_green_gauss(cudaStream_t s, const MeshView& m, const double* phif, d
 void launch_green_gauss_tensor(cudaStream_t s, const MeshView& m, double* const Uf[3], double* const g[9],
                                const double* Delta, double* nut);
 void launch_div(cudaStream_t s, const MeshView& m, const double* psif, double* out);
+// non-orthogonal correction of the pressure right-hand side (t: Case::build_nonorth)
+void launch_nonorth_correct(cudaStream_t s, const MeshView& m, const double* t, const double* p,
+                            const double* const g[3], const double* rDf, double* b);
 void launch_rD_remove_H(cudaStream_t s, const MeshView& m, const CSRView& A, const double* nz,
                         const double* const U[3], const double* const g[3], double* const b[3], double* rD,
                         double* const H[3], int do_H);

@@ -640,6 +640,36 @@ __global__ void k_div(MeshView m, const double* __restrict__ psif, double* out) 
     out[i] = r;
 }
 
+// nonorthogonal_face_correction (Solvers_1_SIMPLE.jl:267-318), one thread
+// per cell: b_i gets each of its internal faces' correction, in its
+// cell_faces order (+ as owner, - as neighbour; the reference adds with
+// atomics in no fixed order).  t: per internal face w, ex, ey, ez, Tx, Ty,
+// Tz (Case::build_nonorth).
+__global__ void k_nonorth_correct(MeshView m, const double* __restrict__ t, const double* __restrict__ p,
+                                  const double* __restrict__ gx, const double* __restrict__ gy,
+                                  const double* __restrict__ gz, const double* __restrict__ rDf, double* b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    const int nI = m.nF - m.nB;
+    double bi = b[i];
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        const int f = m.cf_face[k], j = f - m.nB, c1 = m.owner[f], c2 = m.neigh[f];
+        const double w = t[j], ex = t[nI + j], ey = t[2 * nI + j], ez = t[3 * nI + j];
+        const double Tx = t[4 * nI + j], Ty = t[5 * nI + j], Tz = t[6 * nI + j];
+        const double w1 = 1.0 - w;
+        // gradi = w grad[c1] + (1 - w) grad[c2]
+        const double gix = w * gx[c1] + w1 * gx[c2], giy = w * gy[c1] + w1 * gy[c2], giz = w * gz[c1] + w1 * gz[c2];
+        // gradf = gradi + ((p2 - p1)/delta - gradi.e) e
+        const double s = (p[c2] - p[c1]) / m.delta[f] - (gix * ex + giy * ey + giz * ez);
+        const double gfx = gix + s * ex, gfy = giy + s * ey, gfz = giz + s * ez;
+        // (rDf gradf) . T
+        const double r = rDf[f];
+        const double corr = (r * gfx) * Tx + (r * gfy) * Ty + (r * gfz) * Tz;
+        bi = c1 == i ? bi + corr : bi - corr;
+    }
+    b[i] = bi;
+}
+
 // ---------------------------------------------------------------------------
 // pressure-velocity coupling (Solvers_0_functions.jl, Solvers_1_SIMPLE.jl)
 // ---------------------------------------------------------------------------
@@ -859,6 +889,11 @@ void launch_green_gauss_tensor(cudaStream_t s, const MeshView& m, double* const 
                                const double* Delta, double* nut) {
     k_green_gauss_tensor<<<nblk(m.nC), TPB, 0, s>>>(m, Uf[0], Uf[1], Uf[2], g[0], g[1], g[2], g[3], g[4], g[5], g[6],
                                                     g[7], g[8], Delta, nut);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_nonorth_correct(cudaStream_t s, const MeshView& m, const double* t, const double* p,
+                            const double* const g[3], const double* rDf, double* b) {
+    k_nonorth_correct<<<nblk(m.nC), TPB, 0, s>>>(m, t, p, g[0], g[1], g[2], rDf, b);
     XCAL_CHECK_LAUNCH();
 }
 void launch_div(cudaStream_t s, const MeshView& m, const double* psif, double* out) {

@@ -50,7 +50,7 @@ class PolyMesh:
 
 
 def box_polymesh(nx: int, ny: int, nz: int, lengths=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0),
-                 patches=None, seed: int | None = None) -> PolyMesh:
+                 patches=None, seed: int | None = None, skew: float = 0.0, skew_seed: int = 0) -> PolyMesh:
     """Hex box of nx*ny*nz cells on [origin, origin+lengths].
 
     ``patches`` is a list of ``(name, [sides])`` with sides from
@@ -59,6 +59,12 @@ def box_polymesh(nx: int, ny: int, nz: int, lengths=(1.0, 1.0, 1.0), origin=(0.0
     order inside each patch are permuted by ``numpy.random.default_rng(seed)``;
     owner < neighbour is kept for every internal face (faces are flipped where
     needed so their node order still points from owner to neighbour).
+
+    ``skew`` > 0 moves every interior point by a seeded random offset of up
+    to ``skew`` times the local spacing in each direction (points on the
+    box's sides stay put), which makes the internal faces non-orthogonal
+    (face normals no longer parallel to the owner-neighbour line) and the
+    quads non-planar; keep it below about 0.25 so the cells stay convex.
     """
     if patches is None:
         patches = [(s, [s]) for s in SIDES]
@@ -72,6 +78,12 @@ def box_polymesh(nx: int, ny: int, nz: int, lengths=(1.0, 1.0, 1.0), origin=(0.0
     zs = oz + lz * (np.arange(nz + 1, dtype=np.float64) / nz)
     Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
     points = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    if skew > 0.0:
+        K, J, I = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+        inner = ((I > 0) & (I < nx) & (J > 0) & (J < ny) & (K > 0) & (K < nz)).ravel()
+        rng = np.random.default_rng(skew_seed)
+        off = rng.uniform(-skew, skew, size=(points.shape[0], 3)) * np.array([lx / nx, ly / ny, lz / nz])
+        points = points + off * inner[:, None]
 
     def pid(i, j, k):
         return i + (nx + 1) * (j + (ny + 1) * k)
