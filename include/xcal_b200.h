@@ -50,6 +50,10 @@ enum {
 enum { XCAL_TIME_STEADY = 0, XCAL_TIME_EULER = 1 };
 /* Divergence{T}: src/Discretise/Discretise_1_schemes.jl:114-180 */
 enum { XCAL_DIV_LINEAR = 0, XCAL_DIV_UPWIND = 1, XCAL_DIV_LUST = 2 };
+/* gradient schemes: Gauss (Calculate_1_green_gauss.jl) and Midpoint
+ * (Calculate_0_gradient.jl:170-262: midpoint face values, Green-Gauss, then
+ * two rounds of gradient-corrected face values and Green-Gauss) */
+enum { XCAL_GRAD_GAUSS = 0, XCAL_GRAD_MIDPOINT = 1 };
 /* Krylov solver: src/Solve/Solve_1_Krylov_solvers.jl:6-15 */
 enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
 /* preconditioner: src/Solve/Preconditioners/preconditioners_0_types.jl */
@@ -144,11 +148,12 @@ typedef struct {
     int32_t itmax;
 } xcal_solver_setup;
 
-/* Schemes (src/Solve/Solve_1_api.jl:205-211); gradient is always Gauss and
- * the Laplacian always Linear on this path. */
+/* Schemes (src/Solve/Solve_1_api.jl:205-211); the Laplacian is always
+ * Linear on this path. */
 typedef struct {
     int32_t time;               /* XCAL_TIME_*                               */
     int32_t divergence;         /* XCAL_DIV_*                                */
+    int32_t gradient;           /* XCAL_GRAD_* (p: grad p; U: grad U)       */
 } xcal_schemes;
 
 /* Configuration + Physics (src/Simulate/Simulate_0_types.jl:32-74,

@@ -957,17 +957,61 @@ static void correct_interp_periodic(Case& C, std::vector<double>& phif, const st
 }
 
 // grad!(grad p) (Calculate_0_gradient.jl:105-111)
+// Midpoint gradient (Calculate_0_gradient.jl:170-262): internal faces get
+// 0.5 (phi1 + phi2) (interpolate_midpoint!, boundary faces as for Gauss),
+// Green-Gauss, then twice: phif = 0.5 (phi1 + phi2) + (0.5 (grad1 + grad2)).Ri
+// with Ri = rf - 0.5 (rP + rN) (correct_interpolation!) and Green-Gauss.
+static V3 mid_R(const Mesh& m, int f) {
+    return m.fcentre[f] - 0.5 * (m.ccentre[m.owner[f]] + m.ccentre[m.neigh[f]]);
+}
+
 static void grad_p(Case& C) {
-    interpolate(*C.m, C.p, C.pf);
+    const Mesh& m = *C.m;
+    interpolate(m, C.p, C.pf);
     correct_boundaries(C, C.bcP, &C.pf, &C.p, false);
-    green_gauss(*C.m, C.pf, C.gradp);
+    if (C.cfg.p_schemes.gradient != XCAL_GRAD_MIDPOINT) {
+        green_gauss(m, C.pf, C.gradp);
+        return;
+    }
+    for (int f = C.nB; f < C.nF; ++f) C.pf[f] = 0.5 * (C.p[m.owner[f]] + C.p[m.neigh[f]]);
+    green_gauss(m, C.pf, C.gradp);
+    for (int it = 0; it < 2; ++it) {
+        for (int f = C.nB; f < C.nF; ++f) {
+            const int c1 = m.owner[f], c2 = m.neigh[f];
+            const V3 g1 = {C.gradp[0][c1], C.gradp[1][c1], C.gradp[2][c1]};
+            const V3 g2 = {C.gradp[0][c2], C.gradp[1][c2], C.gradp[2][c2]};
+            C.pf[f] = 0.5 * (C.p[c1] + C.p[c2]) + dot(0.5 * (g1 + g2), mid_R(m, f));
+        }
+        green_gauss(m, C.pf, C.gradp);
+    }
 }
 
 // grad!(grad U) (Calculate_0_gradient.jl:113-119)
 static void grad_U(Case& C) {
-    for (int d = 0; d < 3; ++d) interpolate(*C.m, C.U[d], C.Uf[d]);
+    const Mesh& m = *C.m;
+    for (int d = 0; d < 3; ++d) interpolate(m, C.U[d], C.Uf[d]);
     correct_boundaries(C, C.bcU, C.Uf, C.U, true);
-    green_gauss_tensor(*C.m, C.Uf, C.gradU);
+    if (C.cfg.U_schemes.gradient != XCAL_GRAD_MIDPOINT) {
+        green_gauss_tensor(m, C.Uf, C.gradU);
+        return;
+    }
+    for (int f = C.nB; f < C.nF; ++f)
+        for (int d = 0; d < 3; ++d) C.Uf[d][f] = 0.5 * (C.U[d][m.owner[f]] + C.U[d][m.neigh[f]]);
+    green_gauss_tensor(m, C.Uf, C.gradU);
+    for (int it = 0; it < 2; ++it) {
+        for (int f = C.nB; f < C.nF; ++f) {
+            const int c1 = m.owner[f], c2 = m.neigh[f];
+            const V3 R = mid_R(m, f);
+            for (int a = 0; a < 3; ++a) {
+                const double M0 = 0.5 * (C.gradU[3 * a][c1] + C.gradU[3 * a][c2]);
+                const double M1 = 0.5 * (C.gradU[3 * a + 1][c1] + C.gradU[3 * a + 1][c2]);
+                const double M2 = 0.5 * (C.gradU[3 * a + 2][c1] + C.gradU[3 * a + 2][c2]);
+                // (grad*Ri)_a = (M[a,1] R1 + M[a,2] R2) + M[a,3] R3
+                C.Uf[a][f] = 0.5 * (C.U[a][c1] + C.U[a][c2]) + (M0 * R.x + M1 * R.y + M2 * R.z);
+            }
+        }
+        green_gauss_tensor(m, C.Uf, C.gradU);
+    }
 }
 
 // update_nueff! (Solvers_0_functions.jl:5-35)

@@ -67,3 +67,48 @@ def test_correctors_batch_matches_single(x, ctx, prec):
         assert np.array_equal(hist[k], alone[k][0]), (k, hist[k], alone[k][0])
         assert np.array_equal(c.get_field(x._abi.FIELD_P), alone[k][1])
     batch.close()
+
+
+@pytest.mark.parametrize("which,ncorr", [("p", 0), ("pU", 0), ("pU", 1)])
+def test_midpoint_gradient_parity(x, orc, ctx, which, ncorr):
+    """Midpoint gradients (grad p; grad p and grad U) on the skewed channel,
+    with and without a non-orthogonal corrector: GPU against the oracle."""
+    mesh = skewed_channel(x, n=(11, 7, 6), seed=8)
+    model, config = x.cases.channel_case(mesh, iterations=4)
+    config.schemes["p"].gradient = x.api.Midpoint
+    if "U" in which:
+        config.schemes["U"].gradient = x.api.Midpoint
+    cfg, keep = x.build_config(model, config, ncorrectors=ncorr)
+    dm = x.DeviceMesh(ctx, mesh)
+    g = x.Case(dm, cfg)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    for c in (g, o):
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+    rg, _ = g.simple_iterate(4)
+    ro, _ = o.simple_iterate(4)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    for f in (x._abi.FIELD_U, x._abi.FIELD_P, x._abi.FIELD_GRADP, x._abi.FIELD_GRADU):
+        assert rel(g.get_field(f), o.get_field(f)) <= TOL, f
+
+
+def test_midpoint_les_piso_parity(x, orc, ctx):
+    """PISO + Smagorinsky with Midpoint grad U (nut from the last pass) and
+    grad p on the periodic box: GPU against the oracle."""
+    mesh = x.build_mesh3(x.periodic_box_polymesh(8, seed=3))
+    U0 = x.cases.fourier_field(mesh, seed=3)
+    model, config = x.cases.periodic_les_case(mesh, steps=3, U0=U0)
+    config.schemes["p"].gradient = x.api.Midpoint
+    config.schemes["U"].gradient = x.api.Midpoint
+    cfg, keep = x.build_config(model, config, pref=0.0)
+    dm = x.DeviceMesh(ctx, mesh)
+    g = x.Case(dm, cfg)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    for c in (g, o):
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+    rg, _ = g.piso_step(3)
+    ro, _ = o.piso_step(3)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    for f in (x._abi.FIELD_U, x._abi.FIELD_P, x._abi.FIELD_NUT):
+        assert rel(g.get_field(f), o.get_field(f)) <= TOL, f

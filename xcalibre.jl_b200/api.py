@@ -53,6 +53,9 @@ class LUST: ...
 class Gauss: ...
 
 
+class Midpoint: ...
+
+
 class Cg: ...
 
 
@@ -416,6 +419,7 @@ def dirichlet_function_values(mesh: Mesh3, bc: BC, ncomp: int, time) -> np.ndarr
 
 _SCHEME_TIME = {SteadyState: _abi.TIME_STEADY, Euler: _abi.TIME_EULER}
 _SCHEME_DIV = {Linear: _abi.DIV_LINEAR, Upwind: _abi.DIV_UPWIND, LUST: _abi.DIV_LUST}
+_SCHEME_GRAD = {Gauss: _abi.GRAD_GAUSS, Midpoint: _abi.GRAD_MIDPOINT}
 
 
 def _kind(x):
@@ -453,8 +457,10 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
         algorithm=_abi.ALGO_PISO if transient else _abi.ALGO_SIMPLE,
         turbulence=_abi.TURB_SMAGORINSKY if les else _abi.TURB_LAMINAR,
         nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if les else 0.0,
-        U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)]),
-        p_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sP.time)], divergence=_SCHEME_DIV[_kind(sP.divergence)]),
+        U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)],
+                                   gradient=_SCHEME_GRAD[_kind(sU.gradient)]),
+        p_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sP.time)], divergence=_SCHEME_DIV[_kind(sP.divergence)],
+                                   gradient=_SCHEME_GRAD[_kind(sP.gradient)]),
         U_solver=_solver_desc(config.solvers["U"]), p_solver=_solver_desc(config.solvers["p"]),
         iterations=int(config.runtime.iterations), dt=float(config.runtime.time_step),
         has_pref=0 if pref is None else 1, pref=0.0 if pref is None else float(pref),

@@ -661,6 +661,10 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     for (DBuf<double>* b : {&p, &rD, &divHv, &nut, &Delta, &prev, &courant, &dx13}) b->alloc(nC);
     for (DBuf<double>* b : {&mdot, &nueff, &nutf, &pf, &rDf}) b->alloc(nF);
     if (cfg.ncorrectors > 0) build_nonorth(*m, stream);
+    for (int g : {cfg.U_schemes.gradient, cfg.p_schemes.gradient})
+        if (g != XCAL_GRAD_GAUSS && g != XCAL_GRAD_MIDPOINT) fail(XCAL_ERR_INVALID, "unknown gradient scheme");
+    if (cfg.U_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.p_schemes.gradient == XCAL_GRAD_MIDPOINT)
+        build_midpoint(*m, stream);
     for (int d = 0; d < 3; ++d) {
         Uc[d].zero(stream);
         gradp[d].zero(stream);
@@ -1480,10 +1484,34 @@ void Case::nonorth_correctors(double& rp) {
     }
 }
 
-void Case::grad_p() {  // Calculate_0_gradient.jl:105-111
+void Case::grad_p() {  // Calculate_0_gradient.jl:105-111 (Gauss), :249-258 (Midpoint)
     launch_interp_scalar(stream, mv(), bcP.view(), p.p, pf.p, nullptr, 0.0);
     double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
+    if (cfg.p_schemes.gradient == XCAL_GRAD_MIDPOINT) {
+        const double* gc[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
+        launch_mid_scalar(stream, mv(), p.p, pf.p);
+        launch_green_gauss(stream, mv(), pf.p, gp);
+        for (int it = 0; it < 2; ++it) {
+            launch_mid_correct_scalar(stream, mv(), midR.p, p.p, gc, pf.p);
+            launch_green_gauss(stream, mv(), pf.p, gp);
+        }
+        return;
+    }
     launch_green_gauss(stream, mv(), pf.p, gp);
+}
+
+// Ri = rf - 0.5 (rP + rN) per internal face (correct_interpolation!,
+// Calculate_0_gradient.jl:214-246), storage order; 3 arrays of nI
+void Case::build_midpoint(const DevMesh& m, cudaStream_t s) {
+    const int nB = m.nB, nI = m.nI;
+    std::vector<double> t(3 * (size_t)nI);
+    for (int j = 0; j < nI; ++j) {
+        const int f = nB + j, c1 = m.owner[f], c2 = m.neigh[f];
+        t[j] = m.fcx[f] - 0.5 * (m.ccx[c1] + m.ccx[c2]);
+        t[nI + (size_t)j] = m.fcy[f] - 0.5 * (m.ccy[c1] + m.ccy[c2]);
+        t[2 * (size_t)nI + j] = m.fcz[f] - 0.5 * (m.ccz[c1] + m.ccz[c2]);
+    }
+    midR.upload(t, s);
 }
 
 void Case::correct() {  // Solvers_1_SIMPLE.jl:210-211
@@ -1501,7 +1529,19 @@ void Case::turbulence() {
     double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = gradU[q].p;
     bool les = cfg.turbulence == XCAL_TURB_SMAGORINSKY;
-    launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, les ? nut.p : nullptr);
+    if (cfg.U_schemes.gradient == XCAL_GRAD_MIDPOINT) {
+        // Midpoint (Calculate_0_gradient.jl:249-258); nut from the last pass
+        const double* gc[9];
+        for (int q = 0; q < 9; ++q) gc[q] = gradU[q].p;
+        launch_mid_vector(stream, mv(), Ucp, Ufp);
+        launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, nullptr);
+        for (int it = 0; it < 2; ++it) {
+            launch_mid_correct_vector(stream, mv(), midR.p, Ucp, gc, Ufp);
+            launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, it == 1 && les ? nut.p : nullptr);
+        }
+    } else {
+        launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, les ? nut.p : nullptr);
+    }
     if (les)
         launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
     else

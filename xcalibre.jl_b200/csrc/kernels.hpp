@@ -30,6 +30,13 @@ void launch_green_gauss(cudaStream_t s, const MeshView& m, const double* phif, d
 void launch_green_gauss_tensor(cudaStream_t s, const MeshView& m, double* const Uf[3], double* const g[9],
                                const double* Delta, double* nut);
 void launch_div(cudaStream_t s, const MeshView& m, const double* psif, double* out);
+// Midpoint gradient face passes (internal faces; R: Case::build_midpoint)
+void launch_mid_scalar(cudaStream_t s, const MeshView& m, const double* phi, double* phif);
+void launch_mid_vector(cudaStream_t s, const MeshView& m, const double* const U[3], double* const Uf[3]);
+void launch_mid_correct_scalar(cudaStream_t s, const MeshView& m, const double* R, const double* phi,
+                               const double* const g[3], double* phif);
+void launch_mid_correct_vector(cudaStream_t s, const MeshView& m, const double* R, const double* const U[3],
+                               const double* const g[9], double* const Uf[3]);
 // non-orthogonal correction of the pressure right-hand side (t: Case::build_nonorth)
 void launch_nonorth_correct(cudaStream_t s, const MeshView& m, const double* t, const double* p,
                             const double* const g[3], const double* rDf, double* b);

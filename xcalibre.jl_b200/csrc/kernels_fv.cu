@@ -5,6 +5,8 @@
 // reference's Atomix scatters: boundary contributions to a cell are applied by
 // the thread owning the cell, in ascending boundary-face order.
 #include "dev_common.cuh"
+#include <algorithm>
+
 #include "kernels.hpp"
 
 namespace xcal {
@@ -640,6 +642,56 @@ __global__ void k_div(MeshView m, const double* __restrict__ psif, double* out) 
     out[i] = r;
 }
 
+// ---- Midpoint gradient (Calculate_0_gradient.jl:170-262) ----
+// interpolate_midpoint! on internal faces (boundary faces keep the values the
+// boundary interpolation gave them): phif = 0.5 (phi1 + phi2)
+__global__ void k_mid_scalar(MeshView m, const double* __restrict__ phi, double* phif) {
+    int f = m.nB + blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nF) return;
+    phif[f] = 0.5 * (phi[m.owner[f]] + phi[m.neigh[f]]);
+}
+__global__ void k_mid_vector(MeshView m, const double* __restrict__ ux, const double* __restrict__ uy,
+                             const double* __restrict__ uz, double* fx, double* fy, double* fz) {
+    int f = m.nB + blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nF) return;
+    const int o = m.owner[f], n = m.neigh[f];
+    fx[f] = 0.5 * (ux[o] + ux[n]);
+    fy[f] = 0.5 * (uy[o] + uy[n]);
+    fz[f] = 0.5 * (uz[o] + uz[n]);
+}
+// correct_interpolation!: phif = 0.5 (phi1 + phi2) + (0.5 (grad1 + grad2)).Ri
+__global__ void k_mid_correct_scalar(MeshView m, const double* __restrict__ R, const double* __restrict__ phi,
+                                     const double* __restrict__ gx, const double* __restrict__ gy,
+                                     const double* __restrict__ gz, double* phif) {
+    int f = m.nB + blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nF) return;
+    const int nI = m.nF - m.nB, j = f - m.nB, o = m.owner[f], n = m.neigh[f];
+    const double ax = 0.5 * (gx[o] + gx[n]), ay = 0.5 * (gy[o] + gy[n]), az = 0.5 * (gz[o] + gz[n]);
+    phif[f] = 0.5 * (phi[o] + phi[n]) + (ax * R[j] + ay * R[nI + j] + az * R[2 * nI + j]);
+}
+// vector field, tensor gradient g[3a+b] = d u_a / d x_b:
+// phif_a = 0.5 (u_a1 + u_a2) + ((M[a,1] R1 + M[a,2] R2) + M[a,3] R3), M = 0.5 (grad1 + grad2)
+struct Grad9 {
+    const double* g[9];
+};
+__global__ void k_mid_correct_vector(MeshView m, const double* __restrict__ R, const double* __restrict__ ux,
+                                     const double* __restrict__ uy, const double* __restrict__ uz, Grad9 G,
+                                     double* fx, double* fy, double* fz) {
+    int f = m.nB + blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nF) return;
+    const int nI = m.nF - m.nB, j = f - m.nB, o = m.owner[f], n = m.neigh[f];
+    const double Rx = R[j], Ry = R[nI + j], Rz = R[2 * nI + j];
+    const double* u[3] = {ux, uy, uz};
+    double* out[3] = {fx, fy, fz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double M0 = 0.5 * (G.g[3 * a][o] + G.g[3 * a][n]);
+        const double M1 = 0.5 * (G.g[3 * a + 1][o] + G.g[3 * a + 1][n]);
+        const double M2 = 0.5 * (G.g[3 * a + 2][o] + G.g[3 * a + 2][n]);
+        out[a][f] = 0.5 * (u[a][o] + u[a][n]) + (M0 * Rx + M1 * Ry + M2 * Rz);
+    }
+}
+
 // nonorthogonal_face_correction (Solvers_1_SIMPLE.jl:267-318), one thread
 // per cell: b_i gets each of its internal faces' correction, in its
 // cell_faces order (+ as owner, - as neighbour; the reference adds with
@@ -889,6 +941,31 @@ void launch_green_gauss_tensor(cudaStream_t s, const MeshView& m, double* const 
                                const double* Delta, double* nut) {
     k_green_gauss_tensor<<<nblk(m.nC), TPB, 0, s>>>(m, Uf[0], Uf[1], Uf[2], g[0], g[1], g[2], g[3], g[4], g[5], g[6],
                                                     g[7], g[8], Delta, nut);
+    XCAL_CHECK_LAUNCH();
+}
+static inline int nblk_i(const MeshView& m) { return std::max(1, (m.nF - m.nB + TPB - 1) / TPB); }
+void launch_mid_scalar(cudaStream_t s, const MeshView& m, const double* phi, double* phif) {
+    if (m.nF == m.nB) return;
+    k_mid_scalar<<<nblk_i(m), TPB, 0, s>>>(m, phi, phif);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_mid_vector(cudaStream_t s, const MeshView& m, const double* const U[3], double* const Uf[3]) {
+    if (m.nF == m.nB) return;
+    k_mid_vector<<<nblk_i(m), TPB, 0, s>>>(m, U[0], U[1], U[2], Uf[0], Uf[1], Uf[2]);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_mid_correct_scalar(cudaStream_t s, const MeshView& m, const double* R, const double* phi,
+                               const double* const g[3], double* phif) {
+    if (m.nF == m.nB) return;
+    k_mid_correct_scalar<<<nblk_i(m), TPB, 0, s>>>(m, R, phi, g[0], g[1], g[2], phif);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_mid_correct_vector(cudaStream_t s, const MeshView& m, const double* R, const double* const U[3],
+                               const double* const g[9], double* const Uf[3]) {
+    if (m.nF == m.nB) return;
+    Grad9 G;
+    for (int q = 0; q < 9; ++q) G.g[q] = g[q];
+    k_mid_correct_vector<<<nblk_i(m), TPB, 0, s>>>(m, R, U[0], U[1], U[2], G, Uf[0], Uf[1], Uf[2]);
     XCAL_CHECK_LAUNCH();
 }
 void launch_nonorth_correct(cudaStream_t s, const MeshView& m, const double* t, const double* p,
