@@ -54,6 +54,10 @@ enum { XCAL_DIV_LINEAR = 0, XCAL_DIV_UPWIND = 1, XCAL_DIV_LUST = 2 };
  * (Calculate_0_gradient.jl:170-262: midpoint face values, Green-Gauss, then
  * two rounds of gradient-corrected face values and Green-Gauss) */
 enum { XCAL_GRAD_GAUSS = 0, XCAL_GRAD_MIDPOINT = 1 };
+/* gradient limiters: none, or CellBased (Calculate_0_gradient_cell_limiter.jl,
+ * Barth-Jespersen, strength level); p_schemes: after every grad p, U_schemes:
+ * after grad U in the turbulence update, per component (nut after it) */
+enum { XCAL_LIMITER_NONE = 0, XCAL_LIMITER_CELL = 1 };
 /* Krylov solver: src/Solve/Solve_1_Krylov_solvers.jl:6-15 */
 enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
 /* preconditioner: src/Solve/Preconditioners/preconditioners_0_types.jl */
@@ -154,6 +158,8 @@ typedef struct {
     int32_t time;               /* XCAL_TIME_*                               */
     int32_t divergence;         /* XCAL_DIV_*                                */
     int32_t gradient;           /* XCAL_GRAD_* (p: grad p; U: grad U)       */
+    int32_t limiter;            /* XCAL_LIMITER_*                            */
+    double limiter_level;       /* CellBased(level), 0..1                    */
 } xcal_schemes;
 
 /* Configuration + Physics (src/Simulate/Simulate_0_types.jl:32-74,

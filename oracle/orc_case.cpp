@@ -965,7 +965,48 @@ static V3 mid_R(const Mesh& m, int f) {
     return m.fcentre[f] - 0.5 * (m.ccentre[m.owner[f]] + m.ccentre[m.neigh[f]]);
 }
 
+// limit_gradient!(CellBased(level), grad F, F)
+// (Calculate_0_gradient_cell_limiter.jl:68-108), F scalar (grad F = g[0..2])
+// or one component of U with its row of grad U (:47-63): per cell the
+// neighbours' max/min of F, then the smallest ratio over its internal faces
+// of the allowed change to the gradient-extrapolated change (fc - cc).grad,
+// |change| > 10 eps(F_P); grad *= 1 - level (1 - limiter)
+static void limit_cell(Case& C, const std::vector<double>& F, std::vector<double>* g, double level) {
+    const Mesh& m = *C.m;
+    for (int i = 0; i < C.nC; ++i) {
+        const double phiP = F[i];
+        double phiMax = phiP, phiMin = phiP;
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            const double phiN = F[m.cell_neigh[k]];
+            phiMax = jl_max(phiN, phiMax);
+            phiMin = jl_min(phiN, phiMin);
+        }
+        const V3 g0 = {g[0][i], g[1][i], g[2][i]};
+        double lim = 1.0;
+        const double e = 10.0 * jl_eps(phiP);
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            const int f = m.cell_faces[k];
+            const double d = dot(m.fcentre[f] - m.ccentre[i], g0);
+            if (d > e)
+                lim = jl_min(lim, (phiMax - phiP) / d);
+            else if (d < -e)
+                lim = jl_min(lim, (phiMin - phiP) / d);
+        }
+        lim = 1.0 - level * (1.0 - lim);
+        g[0][i] = g0.x * lim;
+        g[1][i] = g0.y * lim;
+        g[2][i] = g0.z * lim;
+    }
+}
+
+static void grad_p_only(Case& C);
+
 static void grad_p(Case& C) {
+    grad_p_only(C);
+    if (C.cfg.p_schemes.limiter == XCAL_LIMITER_CELL) limit_cell(C, C.p, C.gradp, C.cfg.p_schemes.limiter_level);
+}
+
+static void grad_p_only(Case& C) {
     const Mesh& m = *C.m;
     interpolate(m, C.p, C.pf);
     correct_boundaries(C, C.bcP, &C.pf, &C.p, false);
@@ -987,7 +1028,15 @@ static void grad_p(Case& C) {
 }
 
 // grad!(grad U) (Calculate_0_gradient.jl:113-119)
-static void grad_U(Case& C) {
+static void grad_U_only(Case& C);
+
+static void grad_U(Case& C) {  // grad! + limit_gradient!(schemes.U.limiter) (RANS_laminar.jl:76-77)
+    grad_U_only(C);
+    if (C.cfg.U_schemes.limiter == XCAL_LIMITER_CELL)
+        for (int a = 0; a < 3; ++a) limit_cell(C, C.U[a], C.gradU + 3 * a, C.cfg.U_schemes.limiter_level);
+}
+
+static void grad_U_only(Case& C) {
     const Mesh& m = *C.m;
     for (int d = 0; d < 3; ++d) interpolate(m, C.U[d], C.Uf[d]);
     correct_boundaries(C, C.bcU, C.Uf, C.U, true);

@@ -50,6 +50,10 @@ inline double jl_max(double x, double y) {
     bool take_y = (y > x) || (std::signbit(y) < std::signbit(x));
     return take_y ? (std::isnan(x) ? x : y) : (std::isnan(y) ? y : x);
 }
+inline double jl_min(double x, double y) {
+    bool take_y = (y < x) || (std::signbit(y) > std::signbit(x));
+    return take_y ? (std::isnan(x) ? x : y) : (std::isnan(y) ? y : x);
+}
 inline double jl_clamp(double x, double lo, double hi) {
     return x > hi ? hi : (x < lo ? lo : x);
 }

@@ -1,7 +1,8 @@
-"""Non-orthogonal correctors on the GPU against the oracle (skewed channel,
-ncorrectors 1 and 2, FP64, host-polled and graph mode; tolerance the 1e-10 relative L2 of the parity
-tests, expected 0), and a batch of skewed cases with correctors giving the
-results the cases give alone (bit for bit)."""
+"""Non-orthogonal correctors, Midpoint gradients and the CellBased gradient
+limiter on the GPU against the oracle (skewed channel, FP64, host-polled and
+graph mode; tolerance the 1e-10 relative L2 of the parity tests, expected 0),
+and a batch of skewed cases with correctors (and limiters) giving the results
+the cases give alone (bit for bit)."""
 import numpy as np
 import pytest
 
@@ -38,14 +39,18 @@ def test_correctors_parity(x, orc, ctx, ncorr, graph):
         assert rel(g.get_field(f), o.get_field(f)) <= TOL
 
 
+@pytest.mark.parametrize("limit", [False, True])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_correctors_batch_matches_single(x, ctx, prec):
+def test_correctors_batch_matches_single(x, ctx, prec, limit):
     specs = [((10, 6, 5), 3), ((14, 8, 7), 5), ((9, 9, 4), 6)]
     iters = 3
 
     def mk(n, seed):
         mesh = skewed_channel(x, n=n, seed=seed)
         model, config = x.cases.channel_case(mesh, iterations=iters, precision=prec)
+        if limit:
+            config.schemes["p"].limiter = x.api.CellBased(1.0)
+            config.schemes["U"].limiter = x.api.CellBased(0.7)
         cfg, keep = x.build_config(model, config, ncorrectors=2)
         dm = x.DeviceMesh(ctx, mesh)
         c = x.Case(dm, cfg)
@@ -111,4 +116,56 @@ def test_midpoint_les_piso_parity(x, orc, ctx):
     ro, _ = o.piso_step(3)
     assert rel(rg, ro) <= TOL, (rg, ro)
     for f in (x._abi.FIELD_U, x._abi.FIELD_P, x._abi.FIELD_NUT):
+        assert rel(g.get_field(f), o.get_field(f)) <= TOL, f
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("grad,p_level,U_level,ncorr", [("gauss", 1.0, None, 0), ("gauss", 1.0, 1.0, 1),
+                                                        ("midpoint", 0.5, 0.8, 1)])
+def test_limiter_parity(x, orc, ctx, grad, p_level, U_level, ncorr, graph):
+    """Schemes(limiter=CellBased(level)) for p (and U) on the skewed channel,
+    Gauss or Midpoint gradients, with and without a corrector."""
+    mesh = skewed_channel(x, n=(12, 7, 6), seed=9)
+    model, config = x.cases.channel_case(mesh, iterations=4)
+    config.schemes["p"].limiter = x.api.CellBased(p_level)
+    if U_level is not None:
+        config.schemes["U"].limiter = x.api.CellBased(U_level)
+    if grad == "midpoint":
+        config.schemes["p"].gradient = x.api.Midpoint
+        config.schemes["U"].gradient = x.api.Midpoint
+    cfg, keep = x.build_config(model, config, ncorrectors=ncorr)
+    dm = x.DeviceMesh(ctx, mesh)
+    g = x.Case(dm, cfg)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    for c in (g, o):
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+    if graph:
+        g.set_graph_mode(True)
+    rg, _ = g.simple_iterate(4)
+    ro, _ = o.simple_iterate(4)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    for f in (x._abi.FIELD_U, x._abi.FIELD_P, x._abi.FIELD_GRADP, x._abi.FIELD_GRADU):
+        assert rel(g.get_field(f), o.get_field(f)) <= TOL, f
+
+
+def test_limiter_les_piso_parity(x, orc, ctx):
+    """PISO + Smagorinsky with the grad U limiter (nut from the limited
+    gradient, LES_Smagorinsky.jl:119-127) and the grad p limiter."""
+    mesh = x.build_mesh3(x.periodic_box_polymesh(8, seed=4))
+    U0 = x.cases.fourier_field(mesh, seed=4)
+    model, config = x.cases.periodic_les_case(mesh, steps=3, U0=U0)
+    config.schemes["p"].limiter = x.api.CellBased(1.0)
+    config.schemes["U"].limiter = x.api.CellBased(1.0)
+    cfg, keep = x.build_config(model, config, pref=0.0)
+    dm = x.DeviceMesh(ctx, mesh)
+    g = x.Case(dm, cfg)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    for c in (g, o):
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+    rg, _ = g.piso_step(3)
+    ro, _ = o.piso_step(3)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    for f in (x._abi.FIELD_U, x._abi.FIELD_P, x._abi.FIELD_NUT, x._abi.FIELD_GRADU):
         assert rel(g.get_field(f), o.get_field(f)) <= TOL, f

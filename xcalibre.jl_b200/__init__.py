@@ -6,7 +6,7 @@ The directory name contains a dot, so load it with ``importlib`` (see
 ``__graft_entry__.load_package``); it is registered as ``xcalibre_b200``.
 """
 from . import _abi, api, cases
-from .api import (B200Backend, Bicgstab, Case, Cg, Configuration, Context, DeviceMesh, DILU, Dirichlet, Midpoint,
+from .api import (B200Backend, Bicgstab, Case, CellBased, Cg, Configuration, Context, DeviceMesh, DILU, Dirichlet, Midpoint,
                   DirichletFunction, Empty, Energy, Euler, Extrapolated, Fluid, Gauss, Hardware, Incompressible,
                   Isothermal, Jacobi, LES, LUST, Laminar, Linear, Neumann, Physics, RANS, Runtime, Schemes,
                   Smagorinsky, SolverSetup, Steady, SteadyState, Symmetry, Transient, Upwind, Wall, Zerogradient,

@@ -31,6 +31,7 @@ BC_PERIODIC_PARENT = 10
 TIME_STEADY, TIME_EULER = 0, 1
 DIV_LINEAR, DIV_UPWIND, DIV_LUST = 0, 1, 2
 GRAD_GAUSS, GRAD_MIDPOINT = 0, 1
+LIMITER_NONE, LIMITER_CELL = 0, 1
 SOLVER_CG, SOLVER_BICGSTAB = 0, 1
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_DILU = 0, 1, 2
 TURB_LAMINAR, TURB_SMAGORINSKY = 0, 1
@@ -99,7 +100,8 @@ class SolverSetupDesc(C.Structure):
 
 
 class SchemesDesc(C.Structure):
-    _fields_ = [("time", C.c_int32), ("divergence", C.c_int32), ("gradient", C.c_int32)]
+    _fields_ = [("time", C.c_int32), ("divergence", C.c_int32), ("gradient", C.c_int32), ("limiter", C.c_int32),
+                ("limiter_level", C.c_double)]
 
 
 class ConfigDesc(C.Structure):

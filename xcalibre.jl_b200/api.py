@@ -56,6 +56,29 @@ class Gauss: ...
 class Midpoint: ...
 
 
+@dataclass
+class CellBased:
+    """Cell-based gradient limiter (Calculate_0_gradient_cell_limiter.jl):
+    level 1 = full limiting, 0 = none."""
+    level: float = 1.0
+
+    def __post_init__(self):
+        if not 0.0 <= float(self.level) <= 1.0:
+            raise ValueError(f"CellBased limiter: `level` must be between 0 and 1, got {self.level}")
+
+
+class FaceBased:
+    """Face-based limiter: not implemented (the reference's is marked
+    experimental and updates shared cells from concurrent face threads)."""
+
+    def __init__(self, *a, **k):
+        pass
+
+
+class MFaceBased(FaceBased):
+    pass
+
+
 class Cg: ...
 
 
@@ -426,6 +449,14 @@ def _kind(x):
     return x if isinstance(x, type) else type(x)
 
 
+def _limiter(lim):
+    if lim is None:
+        return _abi.LIMITER_NONE, 0.0
+    if isinstance(lim, CellBased):
+        return _abi.LIMITER_CELL, float(lim.level)
+    raise NotImplementedError("only the CellBased gradient limiter is implemented")
+
+
 def _solver_desc(s: SolverSetup) -> _abi.SolverSetupDesc:
     solver = {Cg: _abi.SOLVER_CG, Bicgstab: _abi.SOLVER_BICGSTAB}[_kind(s.solver)]
     pre = {Jacobi: _abi.PRECOND_JACOBI, DILU: _abi.PRECOND_DILU, type(None): _abi.PRECOND_NONE}[_kind(s.preconditioner)]
@@ -458,9 +489,11 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
         turbulence=_abi.TURB_SMAGORINSKY if les else _abi.TURB_LAMINAR,
         nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if les else 0.0,
         U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)],
-                                   gradient=_SCHEME_GRAD[_kind(sU.gradient)]),
+                                   gradient=_SCHEME_GRAD[_kind(sU.gradient)], limiter=_limiter(sU.limiter)[0],
+                                   limiter_level=_limiter(sU.limiter)[1]),
         p_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sP.time)], divergence=_SCHEME_DIV[_kind(sP.divergence)],
-                                   gradient=_SCHEME_GRAD[_kind(sP.gradient)]),
+                                   gradient=_SCHEME_GRAD[_kind(sP.gradient)], limiter=_limiter(sP.limiter)[0],
+                                   limiter_level=_limiter(sP.limiter)[1]),
         U_solver=_solver_desc(config.solvers["U"]), p_solver=_solver_desc(config.solvers["p"]),
         iterations=int(config.runtime.iterations), dt=float(config.runtime.time_step),
         has_pref=0 if pref is None else 1, pref=0.0 if pref is None else float(pref),

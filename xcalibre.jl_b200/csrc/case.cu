@@ -665,6 +665,14 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         if (g != XCAL_GRAD_GAUSS && g != XCAL_GRAD_MIDPOINT) fail(XCAL_ERR_INVALID, "unknown gradient scheme");
     if (cfg.U_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.p_schemes.gradient == XCAL_GRAD_MIDPOINT)
         build_midpoint(*m, stream);
+    for (const xcal_schemes* sc : {&cfg.U_schemes, &cfg.p_schemes}) {
+        if (sc->limiter != XCAL_LIMITER_NONE && sc->limiter != XCAL_LIMITER_CELL)
+            fail(XCAL_ERR_UNSUPPORTED, "gradient limiter: only CellBased is implemented");
+        if (sc->limiter == XCAL_LIMITER_CELL && !(sc->limiter_level >= 0.0 && sc->limiter_level <= 1.0))
+            fail(XCAL_ERR_INVALID, "CellBased limiter level must be in [0, 1]");
+    }
+    if (cfg.U_schemes.limiter == XCAL_LIMITER_CELL || cfg.p_schemes.limiter == XCAL_LIMITER_CELL)
+        build_limiter(*m, stream);
     for (int d = 0; d < 3; ++d) {
         Uc[d].zero(stream);
         gradp[d].zero(stream);
@@ -1484,7 +1492,10 @@ void Case::nonorth_correctors(double& rp) {
     }
 }
 
-void Case::grad_p() {  // Calculate_0_gradient.jl:105-111 (Gauss), :249-258 (Midpoint)
+// grad! + limit_gradient!(schemes.p.limiter) (Solvers_1_SIMPLE.jl:153-154,
+// 192-193, 205-206): Gauss (Calculate_0_gradient.jl:105-111) or Midpoint
+// (:249-258), then the CellBased limiter when configured
+void Case::grad_p() {
     launch_interp_scalar(stream, mv(), bcP.view(), p.p, pf.p, nullptr, 0.0);
     double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
     if (cfg.p_schemes.gradient == XCAL_GRAD_MIDPOINT) {
@@ -1495,9 +1506,25 @@ void Case::grad_p() {  // Calculate_0_gradient.jl:105-111 (Gauss), :249-258 (Mid
             launch_mid_correct_scalar(stream, mv(), midR.p, p.p, gc, pf.p);
             launch_green_gauss(stream, mv(), pf.p, gp);
         }
-        return;
+    } else {
+        launch_green_gauss(stream, mv(), pf.p, gp);
     }
-    launch_green_gauss(stream, mv(), pf.p, gp);
+    if (cfg.p_schemes.limiter == XCAL_LIMITER_CELL)
+        launch_limit_cell(stream, mv(), limD.p, p.p, gp, cfg.p_schemes.limiter_level);
+}
+
+// fc - cc per cell_faces entry (storage order), 3 arrays of 2 nI
+void Case::build_limiter(const DevMesh& m, cudaStream_t s) {
+    const size_t nk = m.cf_face.size();
+    std::vector<double> t(3 * nk);
+    for (int i = 0; i < m.nC; ++i)
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            const int f = m.cf_face[k];
+            t[k] = m.fcx[f] - m.ccx[i];
+            t[nk + k] = m.fcy[f] - m.ccy[i];
+            t[2 * nk + k] = m.fcz[f] - m.ccz[i];
+        }
+    limD.upload(t, s);
 }
 
 // Ri = rf - 0.5 (rP + rN) per internal face (correct_interpolation!,
@@ -1528,7 +1555,10 @@ void Case::turbulence() {
     launch_interp_U(stream, mv(), bcU.view(), Ucp, Ufp, nullptr);
     double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = gradU[q].p;
-    bool les = cfg.turbulence == XCAL_TURB_SMAGORINSKY;
+    const bool les = cfg.turbulence == XCAL_TURB_SMAGORINSKY;
+    const bool limit = cfg.U_schemes.limiter == XCAL_LIMITER_CELL;
+    // nut fused into the last Green-Gauss pass unless the limiter comes between
+    double* nut_gg = les && !limit ? nut.p : nullptr;
     if (cfg.U_schemes.gradient == XCAL_GRAD_MIDPOINT) {
         // Midpoint (Calculate_0_gradient.jl:249-258); nut from the last pass
         const double* gc[9];
@@ -1537,10 +1567,17 @@ void Case::turbulence() {
         launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, nullptr);
         for (int it = 0; it < 2; ++it) {
             launch_mid_correct_vector(stream, mv(), midR.p, Ucp, gc, Ufp);
-            launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, it == 1 && les ? nut.p : nullptr);
+            launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, it == 1 ? nut_gg : nullptr);
         }
     } else {
-        launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, les ? nut.p : nullptr);
+        launch_green_gauss_tensor(stream, mv(), Ufp, g, Delta.p, nut_gg);
+    }
+    if (limit) {
+        // limit_gradient!(schemes.U.limiter, gradU, U) (RANS_laminar.jl:77,
+        // LES_Smagorinsky.jl:120): the CellBased kernel once per component
+        for (int a = 0; a < 3; ++a)
+            launch_limit_cell(stream, mv(), limD.p, Uc[a].p, g + 3 * a, cfg.U_schemes.limiter_level);
+        if (les) launch_smag_nut(stream, mesh->nC, g, Delta.p, nut.p);
     }
     if (les)
         launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);

@@ -118,6 +118,7 @@ struct Case {
     // fields
     DBuf<double> nonorth;  // non-orthogonal correctors: per internal face w, e, T (7 x nI)
     DBuf<double> midR;     // Midpoint gradients: per internal face rf - 0.5 (rP + rN) (3 x nI)
+    DBuf<double> limD;     // CellBased limiter: fc - cc per cell_faces entry (3 x 2 nI)
     DBuf<double> Uc[3], p, mdot, nueff, gradp[3], gradU[9], rD, Hv[3], divHv, nut, nutf, Uf[3], pf, rDf, Delta, prev,
         courant, dx13, resbuf, cmax, io;  // io: staging of one field component in the original order
     bool initialised = false;
@@ -172,6 +173,7 @@ struct Case {
     void flux_divergence();
     void build_nonorth(const DevMesh& m, cudaStream_t s);
     void build_midpoint(const DevMesh& m, cudaStream_t s);
+    void build_limiter(const DevMesh& m, cudaStream_t s);
     void nonorth_correct();
     void nonorth_correctors(double& rp);
     void explicit_relaxation_p(double a);

@@ -45,6 +45,12 @@ __device__ __forceinline__ double jl_max(double x, double y) {
     return take_y ? (isnan(x) ? x : y) : (isnan(y) ? y : x);
 }
 
+// Julia's min(x, y) for floats (NaN propagating, -0.0 < 0.0)
+__device__ __forceinline__ double jl_min(double x, double y) {
+    bool take_y = (y < x) || (signbit(y) > signbit(x));
+    return take_y ? (isnan(x) ? x : y) : (isnan(y) ? y : x);
+}
+
 // Julia's eps(x)
 __device__ __forceinline__ double jl_eps(double x) {
     x = fabs(x);

@@ -37,6 +37,12 @@ void launch_mid_correct_scalar(cudaStream_t s, const MeshView& m, const double* 
                                const double* const g[3], double* phif);
 void launch_mid_correct_vector(cudaStream_t s, const MeshView& m, const double* R, const double* const U[3],
                                const double* const g[9], double* const Uf[3]);
+// CellBased gradient limiter of grad F, F a scalar field or one component of
+// U with its row of grad U (D: Case::build_limiter)
+void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const double* F, double* const g[3],
+                       double level);
+// Smagorinsky nut = Delta |S| from a stored grad U
+void launch_smag_nut(cudaStream_t s, int nC, const double* const g[9], const double* Delta, double* nut);
 // non-orthogonal correction of the pressure right-hand side (t: Case::build_nonorth)
 void launch_nonorth_correct(cudaStream_t s, const MeshView& m, const double* t, const double* p,
                             const double* const g[3], const double* rDf, double* b);

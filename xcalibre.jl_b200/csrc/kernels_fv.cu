@@ -573,6 +573,23 @@ __global__ void k_green_gauss(MeshView m, const double* __restrict__ phif, doubl
 
 // vector -> tensor; with Smagorinsky also nut = (C Delta)^2 sqrt(2 S:S)
 // (LES_Smagorinsky.jl:122-127)
+// |S| = sqrt((2S).S), S = 0.5 (G + G') over the column-major linear index
+// (LES_Smagorinsky.jl:124-125); G row-major, G[3a+b] = dU_a/dx_b
+__device__ __forceinline__ double smag_magS(const double r[9]) {
+    double acc = 0.0;
+    bool first = true;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            double s = 0.5 * (r[3 * a + b] + r[3 * b + a]);
+            double pr = (2.0 * s) * s;
+            acc = first ? pr : acc + pr;
+            first = false;
+        }
+    return sqrt(acc);
+}
+
 __global__ void k_green_gauss_tensor(MeshView m, const double* __restrict__ fx, const double* __restrict__ fy,
                                      const double* __restrict__ fz, double* g0, double* g1, double* g2, double* g3,
                                      double* g4, double* g5, double* g6, double* g7, double* g8,
@@ -613,21 +630,19 @@ __global__ void k_green_gauss_tensor(MeshView m, const double* __restrict__ fx, 
     g6[i] = r[6];
     g7[i] = r[7];
     g8[i] = r[8];
-    if (nut) {
-        // S = 0.5 (G + G'), (2S).S over the column-major linear index
-        double acc = 0.0;
-        bool first = true;
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                double s = 0.5 * (r[3 * a + b] + r[3 * b + a]);
-                double pr = (2.0 * s) * s;
-                acc = first ? pr : acc + pr;
-                first = false;
-            }
-        nut[i] = Delta[i] * sqrt(acc);
-    }
+    if (nut) nut[i] = Delta[i] * smag_magS(r);
+}
+
+// nut = Delta |S| from a stored grad U (LES_Smagorinsky.jl:122-127), for
+// when grad U is limited between the gradient and nut
+__global__ void k_smag_nut(int nC, const double* __restrict__ g0, const double* __restrict__ g1,
+                           const double* __restrict__ g2, const double* __restrict__ g3, const double* __restrict__ g4,
+                           const double* __restrict__ g5, const double* __restrict__ g6, const double* __restrict__ g7,
+                           const double* __restrict__ g8, const double* __restrict__ Delta, double* nut) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nC) return;
+    const double r[9] = {g0[i], g1[i], g2[i], g3[i], g4[i], g5[i], g6[i], g7[i], g8[i]};
+    nut[i] = Delta[i] * smag_magS(r);
 }
 
 // div! of a face scalar (Calculate_0_divergence.jl:129-170)
@@ -690,6 +705,40 @@ __global__ void k_mid_correct_vector(MeshView m, const double* __restrict__ R, c
         const double M2 = 0.5 * (G.g[3 * a + 2][o] + G.g[3 * a + 2][n]);
         out[a][f] = 0.5 * (u[a][o] + u[a][n]) + (M0 * Rx + M1 * Ry + M2 * Rz);
     }
+}
+
+// limit_gradient!(CellBased(level)) (Calculate_0_gradient_cell_limiter.jl:
+// 68-108), one thread per cell, for a scalar field F and its gradient (one
+// row of grad U for a vector field): F's max/min over the cell's neighbours,
+// the smallest ratio over its internal faces of the allowed change to the
+// extrapolated change d.grad (d = fc - cc, D: 3 arrays over the cell_faces
+// entries), |d.grad| > 10 eps(F_P); grad *= 1 - level (1 - limiter)
+__global__ void k_limit_cell(MeshView m, const double* __restrict__ D, const double* __restrict__ F, double* gx,
+                             double* gy, double* gz, double level) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    const int nk = 2 * (m.nF - m.nB);
+    const double phiP = F[i];
+    double phiMax = phiP, phiMin = phiP;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        const double phiN = F[m.cf_nb[k]];
+        phiMax = jl_max(phiN, phiMax);
+        phiMin = jl_min(phiN, phiMin);
+    }
+    const double x = gx[i], y = gy[i], z = gz[i];
+    double lim = 1.0;
+    const double e = 10.0 * jl_eps(phiP);
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        const double d = D[k] * x + D[nk + k] * y + D[2 * nk + k] * z;
+        if (d > e)
+            lim = jl_min(lim, (phiMax - phiP) / d);
+        else if (d < -e)
+            lim = jl_min(lim, (phiMin - phiP) / d);
+    }
+    lim = 1.0 - level * (1.0 - lim);
+    gx[i] = x * lim;
+    gy[i] = y * lim;
+    gz[i] = z * lim;
 }
 
 // nonorthogonal_face_correction (Solvers_1_SIMPLE.jl:267-318), one thread
@@ -966,6 +1015,15 @@ void launch_mid_correct_vector(cudaStream_t s, const MeshView& m, const double* 
     Grad9 G;
     for (int q = 0; q < 9; ++q) G.g[q] = g[q];
     k_mid_correct_vector<<<nblk_i(m), TPB, 0, s>>>(m, R, U[0], U[1], U[2], G, Uf[0], Uf[1], Uf[2]);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const double* F, double* const g[3],
+                       double level) {
+    k_limit_cell<<<nblk(m.nC), TPB, 0, s>>>(m, D, F, g[0], g[1], g[2], level);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_smag_nut(cudaStream_t s, int nC, const double* const g[9], const double* Delta, double* nut) {
+    k_smag_nut<<<nblk(nC), TPB, 0, s>>>(nC, g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8], Delta, nut);
     XCAL_CHECK_LAUNCH();
 }
 void launch_nonorth_correct(cudaStream_t s, const MeshView& m, const double* t, const double* p,
