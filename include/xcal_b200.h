@@ -170,6 +170,15 @@ typedef struct {
     int32_t turbulence;         /* XCAL_TURB_*                               */
     double nu;                  /* Fluid{Incompressible}(nu)                 */
     double smagorinsky_C;       /* LES{Smagorinsky}(C)                       */
+    /* LES filter width Delta = C (V / les_delta_distance)^les_delta_power,
+     * from delta_scaling(mesh, BCs) (LES_functions.jl:33-56): (the distance
+     * between the Empty patches, 0.5) for a 2D slab, else (1, 1/3).  Power 0
+     * = not given: the library takes the first Empty patch of the U BCs and
+     * the box of the boundary-face centres (the reference's box spans the
+     * boundary faces' nodes; the two agree when the patch normal is
+     * axis-aligned). */
+    double les_delta_distance;
+    double les_delta_power;
     xcal_schemes U_schemes;
     xcal_schemes p_schemes;
     xcal_solver_setup U_solver;

@@ -143,16 +143,25 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     // LES{Smagorinsky} initialise (LES_Smagorinsky.jl:84-101, LES_functions.jl:1-55)
     if (cfg->turbulence == XCAL_TURB_SMAGORINSKY) {
         double distance = 1.0, power = 1.0 / 3.0;
+        if (cfg->les_delta_power > 0.0) {  // delta_scaling evaluated by the caller
+            distance = cfg->les_delta_distance;
+            power = cfg->les_delta_power;
+        } else
         for (const BC& bc : C->bcU)
             if (bc.type == XCAL_BC_EMPTY) {
-                // 2D slab: distance between the Empty patches (delta_scaling, Mesh3)
+                // 2D slab: distance between the Empty patches (delta_scaling,
+                // Mesh3): the box of the boundary faces' nodes when the mesh
+                // has them, else of the boundary-face centres
                 V3 pmin{0, 0, 0}, pmax{0, 0, 0};
-                for (int f = 0; f < C->nB; ++f)
-                    for (int k = m->fn_off[f]; k < m->fn_off[f + 1]; ++k) {
-                        V3 c = m->points[m->face_nodes[k]];
+                const bool nodes = !m->fn_off.empty();
+                for (int f = 0; f < C->nB; ++f) {
+                    const int k0 = nodes ? m->fn_off[f] : 0, k1 = nodes ? m->fn_off[f + 1] : 1;
+                    for (int k = k0; k < k1; ++k) {
+                        V3 c = nodes ? m->points[m->face_nodes[k]] : m->fcentre[f];
                         pmin = {std::min(pmin.x, c.x), std::min(pmin.y, c.y), std::min(pmin.z, c.z)};
                         pmax = {std::max(pmax.x, c.x), std::max(pmax.y, c.y), std::max(pmax.z, c.z)};
                     }
+                }
                 V3 n = m->fnormal[bc.start];
                 distance = std::fabs(dot(pmin, n)) + std::fabs(dot(pmax, n));
                 power = 0.5;

@@ -107,7 +107,8 @@ class SchemesDesc(C.Structure):
 class ConfigDesc(C.Structure):
     _fields_ = [
         ("algorithm", C.c_int32), ("turbulence", C.c_int32), ("nu", C.c_double),
-        ("smagorinsky_C", C.c_double), ("U_schemes", SchemesDesc), ("p_schemes", SchemesDesc),
+        ("smagorinsky_C", C.c_double), ("les_delta_distance", C.c_double), ("les_delta_power", C.c_double),
+        ("U_schemes", SchemesDesc), ("p_schemes", SchemesDesc),
         ("U_solver", SolverSetupDesc), ("p_solver", SolverSetupDesc), ("iterations", C.c_int32),
         ("dt", C.c_double), ("has_pref", C.c_int32), ("pref", C.c_double), ("inner_loops", C.c_int32),
         ("ncorrectors", C.c_int32), ("precision", C.c_int32), ("inner_rtol", C.c_double), ("n_bc_U", C.c_int32), ("n_bc_p", C.c_int32), ("n_bc_nut", C.c_int32),

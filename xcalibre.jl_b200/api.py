@@ -268,8 +268,10 @@ def Zerogradient(name):
     return BC(_abi.BC_ZEROGRADIENT, name)
 
 
-def Extrapolated(name):
-    return BC(_abi.BC_EXTRAPOLATED, name)
+def Extrapolated(name, value=0.0):
+    """Extrapolated(name[, value]) (extrapolated.jl:12-20): zero gradient,
+    semi-implicitly; the value is stored but not used, as in the reference."""
+    return BC(_abi.BC_EXTRAPOLATED, name, value)
 
 
 def Empty(name):
@@ -464,6 +466,32 @@ def _solver_desc(s: SolverSetup) -> _abi.SolverSetupDesc:
                                 relax=float(s.relax), atol=float(s.atol), rtol=float(s.rtol), itmax=int(s.itmax))
 
 
+def delta_scaling(mesh: Mesh3, bcs) -> tuple[float, float]:
+    """delta_scaling(mesh::Mesh3, BCs) (LES_functions.jl:33-56): for the first
+    Empty BC, (|pmin.n| + |pmax.n|, 0.5), n the normal of the patch's first
+    face and pmin/pmax the bounding box (started at the origin) of the
+    boundary faces' nodes (bounding_box, Mesh_1_functions.jl:70-100); with no
+    Empty BC (1, 1/3)."""
+    for bc in bcs:
+        if bc.kind != _abi.BC_EMPTY:
+            continue
+        pm = mesh.polymesh
+        if pm is not None:
+            off = np.asarray(pm.face_offsets)
+            nI = int(np.asarray(pm.neighbour).size)
+            nodes = np.asarray(pm.face_nodes)[off[nI]:off[-1]]
+            pts = np.asarray(pm.points, dtype=np.float64)[nodes]
+        else:  # no node data: the boundary-face centres
+            pts = np.asarray(mesh.face_centre, dtype=np.float64)[:mesh.n_bfaces]
+        pmin = np.minimum(pts.min(axis=0), 0.0)
+        pmax = np.maximum(pts.max(axis=0), 0.0)
+        n = np.asarray(mesh.face_normal, dtype=np.float64)[mesh.patch_range(bc.name).start]
+        d1 = abs(pmin[0] * n[0] + pmin[1] * n[1] + pmin[2] * n[2])
+        d2 = abs(pmax[0] * n[0] + pmax[1] * n[1] + pmax[2] * n[2])
+        return float(d1 + d2), 0.5
+    return 1.0, 1.0 / 3.0
+
+
 def build_config(model: Physics, config: Configuration, pref=None, inner_loops=None, ncorrectors: int = 0):
     """Translate the Python API objects into an xcal_config (keep the second
     return value alive while the config is in use).  ncorrectors: SIMPLE
@@ -484,10 +512,13 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     prec = _abi.PREC_MIXED if getattr(backend, "precision", "fp64") == "mixed" else _abi.PREC_FP64
     if inner_loops is None:
         inner_loops = 2 if transient else 0
+    # delta! reads config.boundaries[1] (LES_functions.jl:7): the first field's BCs
+    dist, power = delta_scaling(mesh, next(iter(bnd.values()))) if les else (1.0, 1.0 / 3.0)
     cfg = _abi.ConfigDesc(
         algorithm=_abi.ALGO_PISO if transient else _abi.ALGO_SIMPLE,
         turbulence=_abi.TURB_SMAGORINSKY if les else _abi.TURB_LAMINAR,
         nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if les else 0.0,
+        les_delta_distance=dist, les_delta_power=power,
         U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)],
                                    gradient=_SCHEME_GRAD[_kind(sU.gradient)], limiter=_limiter(sU.limiter)[0],
                                    limiter_level=_limiter(sU.limiter)[1]),
@@ -802,6 +833,45 @@ class OpenFOAM:
 
 CHECKPOINT_FIELDS = ("FIELD_U", "FIELD_P", "FIELD_MDOTF", "FIELD_NUEFF", "FIELD_GRADP", "FIELD_GRADU", "FIELD_RD",
                      "FIELD_HV", "FIELD_DIVHV", "FIELD_NUT", "FIELD_NUTF", "FIELD_UF", "FIELD_PF", "FIELD_RDF")
+
+
+def boundary_average(patch: str, field, fieldBCs, config=None, *, mesh: Mesh3, time: float = 0.0):
+    """boundary_average(patch, field, fieldBCs, config; time)
+    (Postprocess_functions.jl:157-185): the mean over the patch's faces of the
+    field's boundary face values (the boundary interpolation of its BC on
+    that patch: Dirichlet and vector Wall the value; Zerogradient,
+    Extrapolated, scalar Wall and scalar Symmetry the owner cell's value;
+    vector Symmetry the cell value less its normal part; Empty zero),
+    summed face by face in patch order and divided by the face count.
+    ``field``: [n] (scalar) or [3, n] (vector); returns a float or a [3]
+    array."""
+    rng = mesh.patch_range(patch)
+    bc = next((b for b in fieldBCs if b.name == patch), None)
+    if bc is None:
+        raise KeyError(f'no boundary condition for patch "{patch}"')
+    f = np.asarray(field, dtype=np.float64)
+    vector = f.ndim == 2
+    ids = np.arange(rng.start, rng.stop)
+    cells = np.asarray(mesh.boundary_cellsID)[ids]
+    cell_vals = f[:, cells].T if vector else f[cells]
+    k = bc.kind
+    if k == _abi.BC_DIRICHLET or (k == _abi.BC_WALL and vector):
+        vals = np.broadcast_to(np.asarray(bc.value, dtype=np.float64), cell_vals.shape)
+    elif k == _abi.BC_DIRICHLET_FUNCTION:
+        v = dirichlet_function_values(mesh, bc, 3 if vector else 1, time)
+        vals = v.reshape(-1, 3) if vector else v.reshape(-1)
+    elif k in (_abi.BC_ZEROGRADIENT, _abi.BC_EXTRAPOLATED, _abi.BC_WALL) or (k == _abi.BC_SYMMETRY and not vector):
+        vals = cell_vals
+    elif k == _abi.BC_SYMMETRY:
+        n = np.asarray(mesh.face_normal)[ids]
+        dn = np.sum(cell_vals * n, axis=1, keepdims=True)
+        vals = cell_vals - dn * n
+    elif k == _abi.BC_EMPTY:
+        vals = np.zeros_like(cell_vals)
+    else:
+        raise NotImplementedError(f"boundary_average: boundary kind {k} (Neumann, periodic) is not supported")
+    total = np.cumsum(vals, axis=0)[-1]  # sequential, as `sum += faceField[fID]`
+    return total / len(rng) if vector else float(total / len(rng))
 
 
 def save_checkpoint(state: dict, path: str) -> None:

@@ -740,6 +740,10 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     if (cfg.turbulence == XCAL_TURB_SMAGORINSKY) {
         // LES_Smagorinsky.jl:84-101 + LES_functions.jl:1-55 (delta! with delta_scaling)
         double distance = 1.0, power = 1.0 / 3.0;
+        if (cfg.les_delta_power > 0.0) {
+            distance = cfg.les_delta_distance;
+            power = cfg.les_delta_power;
+        } else
         for (const xcal_bc& bc : bcU.src)
             if (bc.type == XCAL_BC_EMPTY) {
                 double pmin[3] = {0, 0, 0}, pmax[3] = {0, 0, 0};
