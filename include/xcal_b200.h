@@ -123,6 +123,9 @@ typedef struct {
     int32_t n_patches;
     const int32_t* patch_start;       /* [n_patches] first face id           */
     const int32_t* patch_count;       /* [n_patches]                         */
+    int32_t dim;                      /* 2: a Mesh2 (UNV2D_mesh; Courant cell
+                                         size sqrt(V), Solvers_0_functions.jl:
+                                         277-285); 0 or 3: a Mesh3           */
 } xcal_mesh_desc;
 
 /* ---- boundary condition (one per patch per field) ----------------------
@@ -150,6 +153,11 @@ typedef struct {
     double atol;
     double rtol;
     int32_t itmax;
+    int32_t smoother_loops;     /* JacobiSmoother(loops, omega): weighted
+                                   Jacobi sweeps on the field before each
+                                   Krylov solve (Smoothers_jacobi.jl:56-132,
+                                   Solve_1_api.jl:284); 0 = no smoother      */
+    double smoother_omega;
 } xcal_solver_setup;
 
 /* Schemes (src/Solve/Solve_1_api.jl:205-211); the Laplacian is always

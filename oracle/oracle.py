@@ -69,6 +69,7 @@ def lib():
             "orc_canonical_sum": (C.c_double, [pd, C.c_long]),
             "orc_dilu": (None, [i32, pi, pi, pd, pd]),
             "orc_dilu_ldiv": (None, [i32, pi, pi, pd, pd, pd, pd]),
+            "orc_jacobi_smooth": (None, [i32, pi, pi, pd, pd, pd, i32, C.c_double]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -305,4 +306,14 @@ def dilu_ldiv(rowptr, colval, nzval, D, b):
     rp, cv, nz, Dd, bb = _i(rowptr), _i(colval), _d(nzval), _d(D), _d(b)
     lib().orc_dilu_ldiv(n, _p(rp, C.c_int), _p(cv, C.c_int), _p(nz, C.c_double), _p(Dd, C.c_double),
                         _p(x, C.c_double), _p(bb, C.c_double))
+    return x
+
+
+def jacobi_smooth(rowptr, colval, nzval, b, x0, loops, omega):
+    """apply_smoother!(JacobiSmoother(loops, omega)) on a CSR system from x0."""
+    n = len(rowptr) - 1
+    x = _d(x0).copy()
+    rp, cv, nz, bb = _i(rowptr), _i(colval), _d(nzval), _d(b)
+    lib().orc_jacobi_smooth(n, _p(rp, C.c_int), _p(cv, C.c_int), _p(nz, C.c_double), _p(bb, C.c_double),
+                            _p(x, C.c_double), int(loops), float(omega))
     return x

@@ -30,6 +30,7 @@ double o_solve_system(Case& C, int eqn, int comp, int* iters);
 void o_grad_p(Case& C);
 void o_dilu(const CSR& A, std::vector<double>& D);
 void o_dilu_ldiv(const CSR& A, const std::vector<double>& D, std::vector<double>& x, const std::vector<double>& b);
+void jacobi_smooth(const CSR& A, const double* b, double* x, int loops, double omega);
 
 Mesh* mesh_from_desc(const xcal_mesh_desc* d) {
     Mesh* m = new Mesh();
@@ -60,6 +61,7 @@ Mesh* mesh_from_desc(const xcal_mesh_desc* d) {
     m->bcell.assign(d->boundary_cellsID, d->boundary_cellsID + d->n_bfaces);
     m->patch_start.assign(d->patch_start, d->patch_start + d->n_patches);
     m->patch_count.assign(d->patch_count, d->patch_count + d->n_patches);
+    m->dim = d->dim == 2 ? 2 : 3;
     return m;
 }
 }  // namespace orc
@@ -327,6 +329,19 @@ void orc_dilu_ldiv(int n, const int* rowptr, const int* colval, const double* nz
     std::vector<double> dv(D, D + n), xv(n), bv(b, b + n);
     o_dilu_ldiv(A, dv, xv, bv);
     std::memcpy(x, xv.data(), n * sizeof(double));
+}
+
+// the Jacobi smoother on an arbitrary CSR (sorted columns, diagonal present)
+void orc_jacobi_smooth(int n, const int* rowptr, const int* colval, const double* nzval, const double* b, double* x,
+                       int loops, double omega) {
+    CSR A;
+    A.n = n;
+    A.rowptr.assign(rowptr, rowptr + n + 1);
+    A.colval.assign(colval, colval + rowptr[n]);
+    A.nzval.assign(nzval, nzval + rowptr[n]);
+    A.diag.resize(n);
+    for (int i = 0; i < n; ++i) A.diag[i] = A.find(i, i);
+    jacobi_smooth(A, b, x, loops, omega);
 }
 
 }  // extern "C"

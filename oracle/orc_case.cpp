@@ -774,12 +774,34 @@ static double residual(const CSR& A, const std::vector<double>& b, const std::ve
     return std::sqrt(sR) / denom;
 }
 
+// apply_smoother!(JacobiSmoother) (Smoothers_jacobi.jl:73-86, multiply_row
+// :112-131): `loops` sweeps; per row the sum over the row from 0, less
+// a_ii x_i, then omega (1/a_ii) (b_i - sum) + (1 - omega) x_i into a scratch
+// vector, copied back after each sweep
+void jacobi_smooth(const CSR& A, const double* b, double* x, int loops, double omega) {
+    std::vector<double> xt(A.n);
+    for (int l = 0; l < loops; ++l) {
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < A.n; ++i) {
+            double sum = 0.0;
+            for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) sum = sum + A.nzval[k] * x[A.colval[k]];
+            const double a_ii = A.nzval[A.diag[i]];
+            const double xi = x[i];
+            sum = sum - a_ii * xi;
+            const double rD = 1.0 / a_ii;
+            xt[i] = omega * rD * (b[i] - sum) + (1.0 - omega) * xi;
+        }
+        std::copy(xt.begin(), xt.end(), x);
+    }
+}
+
 // solve_system! (Solve_1_api.jl:268-307)
 static double solve_system(Case& C, bool vector, int comp, int* iters) {
     const xcal_solver_setup& S = vector ? C.cfg.U_solver : C.cfg.p_solver;
     CSR& A = vector ? C.AU : C.Ap;
     std::vector<double>& b = vector ? C.bU[comp] : C.bp;
     std::vector<double>& field = vector ? C.U[comp] : C.p;
+    if (S.smoother_loops > 0) jacobi_smooth(A, b.data(), field.data(), S.smoother_loops, S.smoother_omega);
     std::vector<double>& P = vector ? C.PU : C.Pp;
     Krylov& K = vector ? C.kU : C.kp;
     int it = S.solver == XCAL_SOLVER_CG ? krylov_cg(A, b, field, S.precond, P, S, K)
@@ -1233,13 +1255,13 @@ void turbulence(Case& C) {
     update_nueff(C);
 }
 
-double max_courant(Case& C) {  // Solvers_0_functions.jl:253-276
+double max_courant(Case& C) {  // Solvers_0_functions.jl:253-285 (Mesh3 / Mesh2 kernels)
     double mx = -std::numeric_limits<double>::infinity();
     for (int i = 0; i < C.nC; ++i) {
         V3 u{C.U[0][i], C.U[1][i], C.U[2][i]};
         double umag = norm(u);
         double V = C.m->cvol[i];
-        double dx = std::pow(V, 1.0 / 3.0);
+        double dx = C.m->dim == 2 ? std::sqrt(V) : std::pow(V, 1.0 / 3.0);
         double co = (umag * C.cfg.dt) / dx;
         C.cellsCourant[i] = co;
         mx = (i == 0) ? co : jl_max(mx, co);

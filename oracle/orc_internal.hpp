@@ -11,6 +11,7 @@ namespace orc {
 // Mesh3 contract (src/Mesh/Mesh_0_types.jl), SoA, 0-based.
 struct Mesh {
     int n_cells = 0, n_faces = 0, n_bfaces = 0, n_ifaces = 0;
+    int dim = 3;  // 2 for a Mesh2
     std::vector<V3> points;
     std::vector<int> owner, neigh;  // ownerCells[1], ownerCells[2]
     std::vector<V3> fcentre, fnormal, fe;

@@ -11,6 +11,11 @@ Fixtures:
                              centroids of the 3x3 unit-square mesh they refer to.
   pitzdaily_polymesh.npz  -- examples/0_GRIDS/OF_pitzDaily/polyMesh (counts pinned by
                              test/0_TEST_CASES/2d_incompressible_pitzdaily_Smagorinsky.jl:14-16).
+  smoother_5x5.json       -- the 5x5 system of test/test_smoothers.jl:31-46 (i, j, v, b;
+                             50 Jacobi sweeps with omega 1 from zero must reach A\\b to 0.1).
+  bfs_10mm_unv.npz        -- examples/0_GRIDS/backwardFacingStep_10mm.unv (the mesh of
+                             test/0_TEST_CASES/2d_incompressible_laminar_BFS.jl), parsed by
+                             the small reader below into points, elements and groups.
 
 Usage: python tests/golden/make_fixtures.py [/path/to/XCALibre.jl]
 """
@@ -91,6 +96,62 @@ def laplace_expected(path: str) -> dict:
                 source="test/unit_test_laplace.jl:112-130")
 
 
+def smoother_system(path: str) -> dict:
+    txt = open(path).read()
+
+    def vec(name):
+        return re.search(name + r"\s*=\s*\[(.*?)\]", txt).group(1).split(",")
+
+    # entries such as 200*500: products of integers
+    b = [float(np.prod([int(f) for f in t.split("*")])) for t in vec(r"\bb")]
+    return dict(i=[int(v) for v in vec(r"\bi")], j=[int(v) for v in vec(r"\bj")], v=[float(v) for v in vec(r"\bv")],
+                b=b, loops=50, omega=1.0, atol=0.1, source="test/test_smoothers.jl:31-46")
+
+
+def read_unv_raw(path: str) -> dict:
+    """Datasets 2411 (points), 2412 (elements: 6-field header ending in the
+    vertex count, then the vertex line; beam orientation lines skipped) and
+    2467 (groups) of a .unv file, with 1-based labels as in the file."""
+    pts, ecount, eidx, everts, gnames, gelems = [], [], [], [], [], []
+    ds, inblock = None, False
+    hdr = None
+    for line in open(path):
+        s = line.split()
+        if not s:
+            continue
+        if s[0] == "-1":
+            inblock, ds = not inblock, None
+            continue
+        if inblock and ds is None:
+            ds = s[0]
+            continue
+        if ds == "2411" and "." in s[0]:
+            pts.append([float(v) for v in s[:3]])
+        elif ds == "2412":
+            if len(s) == 6:
+                hdr = (int(s[0]), int(s[-1]))
+            elif s[0] != "0" and hdr is not None and len(s) == hdr[1]:
+                eidx.append(hdr[0])
+                ecount.append(hdr[1])
+                everts.extend(int(v) for v in s)
+                hdr = None
+        elif ds == "2467":
+            if len(s) == 8 and s[1] == "0":
+                gelems.append([])
+            elif not s[0].lstrip("-").isdigit():
+                gnames.append(s[0])
+            else:
+                gelems[-1].append(int(s[1]))
+                if len(s) >= 6:
+                    gelems[-1].append(int(s[5]))
+    goff = np.zeros(len(gelems) + 1, dtype=np.int64)
+    goff[1:] = np.cumsum([len(g) for g in gelems])
+    return dict(points=np.array(pts), elem_index=np.array(eidx, dtype=np.int32),
+                elem_count=np.array(ecount, dtype=np.int32), elem_vertices=np.array(everts, dtype=np.int32),
+                group_names=np.array(gnames), group_offsets=goff,
+                group_elements=np.array([e for g in gelems for e in g], dtype=np.int32))
+
+
 def main(ref: str) -> None:
     pm = read_polymesh(os.path.join(ref, "test/grids/OF_cavity_hex/polyMesh"))
     np.savez_compressed(os.path.join(HERE, "cavity_hex_polymesh.npz"), **pm)
@@ -98,6 +159,10 @@ def main(ref: str) -> None:
     np.savez_compressed(os.path.join(HERE, "pitzdaily_polymesh.npz"), **pz)
     with open(os.path.join(HERE, "laplace_3by3.json"), "w") as f:
         json.dump(laplace_expected(os.path.join(ref, "test/unit_test_laplace.jl")), f, indent=1)
+    with open(os.path.join(HERE, "smoother_5x5.json"), "w") as f:
+        json.dump(smoother_system(os.path.join(ref, "test/test_smoothers.jl")), f, indent=1)
+    np.savez_compressed(os.path.join(HERE, "bfs_10mm_unv.npz"),
+                        **read_unv_raw(os.path.join(ref, "examples/0_GRIDS/backwardFacingStep_10mm.unv")))
     print("fixtures written to", HERE)
 
 

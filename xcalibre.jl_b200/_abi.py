@@ -64,7 +64,7 @@ class MeshDesc(C.Structure):
         ("cell_centre", _pf64), ("cell_volume", _pf64),
         ("cell_faces_offset", _pi32), ("cell_faces", _pi32), ("cell_nsign", _pi32),
         ("cell_neighbours", _pi32), ("boundary_cellsID", _pi32),
-        ("n_patches", C.c_int32), ("patch_start", _pi32), ("patch_count", _pi32),
+        ("n_patches", C.c_int32), ("patch_start", _pi32), ("patch_count", _pi32), ("dim", C.c_int32),
     ]
 
 
@@ -96,7 +96,8 @@ class BCDesc(C.Structure):
 
 class SolverSetupDesc(C.Structure):
     _fields_ = [("solver", C.c_int32), ("precond", C.c_int32), ("convergence", C.c_double),
-                ("relax", C.c_double), ("atol", C.c_double), ("rtol", C.c_double), ("itmax", C.c_int32)]
+                ("relax", C.c_double), ("atol", C.c_double), ("rtol", C.c_double), ("itmax", C.c_int32),
+                ("smoother_loops", C.c_int32), ("smoother_omega", C.c_double)]
 
 
 class SchemesDesc(C.Structure):
@@ -143,5 +144,5 @@ def mesh_desc(mesh) -> tuple[MeshDesc, list]:
         cell_faces_offset=i32(mesh.cell_faces_offset), cell_faces=i32(mesh.cell_faces),
         cell_nsign=i32(mesh.cell_nsign), cell_neighbours=i32(mesh.cell_neighbours),
         boundary_cellsID=i32(mesh.boundary_cellsID), n_patches=len(mesh.patch_start),
-        patch_start=i32(mesh.patch_start), patch_count=i32(mesh.patch_count))
+        patch_start=i32(mesh.patch_start), patch_count=i32(mesh.patch_count), dim=int(getattr(mesh, "dim", 3)))
     return d, keep

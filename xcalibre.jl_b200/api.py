@@ -122,6 +122,30 @@ class Schemes:
     limiter: object = None
 
 
+class JacobiSmoother:
+    """JacobiSmoother (Smoothers_jacobi.jl:26-51): ``loops`` weighted Jacobi
+    sweeps, weight ``omega``, applied to the field before each Krylov solve
+    (solve_system!, Solve_1_api.jl:284).  Constructors as the reference's:
+    ``JacobiSmoother(mesh)`` (5 loops, omega 1),
+    ``JacobiSmoother(domain=mesh, loops=n, omega=2/3)`` and
+    ``JacobiSmoother(loops, omega, x_temp)``."""
+
+    def __init__(self, *args, domain=None, loops=None, omega=None):
+        if len(args) == 1:
+            domain, loops, omega = args[0], 5, 1.0
+        elif len(args) >= 2:
+            loops, omega = args[0], args[1]
+        elif domain is None or loops is None:
+            raise TypeError("JacobiSmoother(mesh), JacobiSmoother(domain=, loops=[, omega=]) or "
+                            "JacobiSmoother(loops, omega, x_temp)")
+        elif omega is None:
+            omega = 2.0 / 3.0
+        self.loops = int(loops)
+        self.omega = float(omega)
+        if self.loops < 0:
+            raise ValueError("JacobiSmoother: loops must be >= 0")
+
+
 @dataclass
 class SolverSetup:
     solver: object
@@ -138,8 +162,8 @@ class SolverSetup:
     def __post_init__(self):
         if self.atol is None:
             self.atol = EPS64 ** 0.9  # (eps(float_type))^0.9 (Solve_1_api.jl:70)
-        if self.smoother is not None:
-            raise NotImplementedError("smoothers are outside the implemented path")
+        if self.smoother is not None and not isinstance(self.smoother, JacobiSmoother):
+            raise NotImplementedError("JacobiSmoother is the only smoother")
 
 
 @dataclass
@@ -462,8 +486,11 @@ def _limiter(lim):
 def _solver_desc(s: SolverSetup) -> _abi.SolverSetupDesc:
     solver = {Cg: _abi.SOLVER_CG, Bicgstab: _abi.SOLVER_BICGSTAB}[_kind(s.solver)]
     pre = {Jacobi: _abi.PRECOND_JACOBI, DILU: _abi.PRECOND_DILU, type(None): _abi.PRECOND_NONE}[_kind(s.preconditioner)]
+    sm = s.smoother
     return _abi.SolverSetupDesc(solver=solver, precond=pre, convergence=float(s.convergence),
-                                relax=float(s.relax), atol=float(s.atol), rtol=float(s.rtol), itmax=int(s.itmax))
+                                relax=float(s.relax), atol=float(s.atol), rtol=float(s.rtol), itmax=int(s.itmax),
+                                smoother_loops=sm.loops if sm is not None else 0,
+                                smoother_omega=sm.omega if sm is not None else 0.0)
 
 
 def delta_scaling(mesh: Mesh3, bcs) -> tuple[float, float]:
@@ -471,7 +498,9 @@ def delta_scaling(mesh: Mesh3, bcs) -> tuple[float, float]:
     Empty BC, (|pmin.n| + |pmax.n|, 0.5), n the normal of the patch's first
     face and pmin/pmax the bounding box (started at the origin) of the
     boundary faces' nodes (bounding_box, Mesh_1_functions.jl:70-100); with no
-    Empty BC (1, 1/3)."""
+    Empty BC (1, 1/3).  A 2D mesh (Mesh2): (1, 0.5) (:28-31)."""
+    if getattr(mesh, "dim", 3) == 2:
+        return 1.0, 0.5
     for bc in bcs:
         if bc.kind != _abi.BC_EMPTY:
             continue

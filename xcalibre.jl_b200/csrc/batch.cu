@@ -572,6 +572,7 @@ struct Batch {
         for (int i = 0; i < nc; ++i) {
             all[i] = i;
             Case* c = cases[i];
+            c->smooth(isU ? XCAL_EQN_U : XCAL_EQN_P, comp);
             const xcal_solver_setup& SS = isU ? c->cfg.U_solver : c->cfg.p_solver;
             std::memset(&hS[i], 0, sizeof(KScalars));
             hS[i].atol = SS.atol;

@@ -243,6 +243,8 @@ static DevMesh* upload_mesh_ordered(const xcal_mesh_desc* d, cudaStream_t s, std
     m->bcell.assign(d->boundary_cellsID, d->boundary_cellsID + nB);
     m->patch_start.assign(d->patch_start, d->patch_start + d->n_patches);
     m->patch_count.assign(d->patch_count, d->patch_count + d->n_patches);
+    if (d->dim != 0 && d->dim != 2 && d->dim != 3) fail(XCAL_ERR_INVALID, "mesh: dim must be 0, 2 or 3");
+    m->dim = d->dim == 2 ? 2 : 3;
     // cell -> boundary faces (ascending face id)
     std::vector<int> cnt(nC, 0);
     for (int f = 0; f < nB; ++f) {
@@ -735,7 +737,8 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     XCAL_CUDA(cudaMallocHost(&h_perr, sizeof(int)));
     // host-side per-cell constants: V^(1/3) (Courant) and the LES filter
     std::vector<double> h(nC);
-    for (int i = 0; i < nC; ++i) h[i] = std::pow(m->vol[i], 1.0 / 3.0);
+    // Courant cell size: V^(1/3) (Mesh3), sqrt(V) (Mesh2, Solvers_0_functions.jl:277-285)
+    for (int i = 0; i < nC; ++i) h[i] = m->dim == 2 ? std::sqrt(m->vol[i]) : std::pow(m->vol[i], 1.0 / 3.0);
     XCAL_CUDA(cudaMemcpyAsync(dx13.p, h.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream));
     if (cfg.turbulence == XCAL_TURB_SMAGORINSKY) {
         // LES_Smagorinsky.jl:84-101 + LES_functions.jl:1-55 (delta! with delta_scaling)
@@ -1310,8 +1313,20 @@ void Case::solve_captured(int eqn, int comp) {
     kr_record(stream, S, giters.p + 2 * slot);
 }
 
+// apply_smoother!(setup.smoother, values, A, b) (Solve_1_api.jl:284): the
+// Jacobi smoother on the field, before the Krylov solve of (eqn, comp)
+void Case::smooth(int eqn, int comp) {
+    const bool isU = eqn == XCAL_EQN_U;
+    const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
+    if (SS.smoother_loops <= 0) return;
+    Equation& E = isU ? U : P;
+    kr_jacobi_smooth(stream, E.view(), E.nz.p, isU ? U.b[comp].p : P.b[0].p, isU ? Uc[comp].p : p.p, ws.t.p,
+                     SS.smoother_loops, SS.smoother_omega);
+}
+
 // solve_system! (Solve_1_api.jl:268-307)
 double Case::solve_system(int eqn, int comp, int* iters) {
+    smooth(eqn, comp);
     if (capturing) {  // graph mode: residual goes to gres
         solve_captured(eqn, comp);
         return 0.0;

@@ -15,6 +15,7 @@ namespace xcal {
 // Mesh3 in HBM plus host copies needed to derive per-equation structures
 struct DevMesh {
     int nC = 0, nF = 0, nB = 0, nI = 0;
+    int dim = 3;  // 2 for a Mesh2
     // storage order: perm[s] = original index stored at s, inv = its inverse
     // (cells); fperm/finv likewise for faces (boundary faces are not moved)
     std::vector<int> perm, inv, fperm, finv;
@@ -174,6 +175,7 @@ struct Case {
     void build_nonorth(const DevMesh& m, cudaStream_t s);
     void build_midpoint(const DevMesh& m, cudaStream_t s);
     void build_limiter(const DevMesh& m, cudaStream_t s);
+    void smooth(int eqn, int comp);
     void nonorth_correct();
     void nonorth_correctors(double& rp);
     void explicit_relaxation_p(double a);

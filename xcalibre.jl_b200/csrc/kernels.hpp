@@ -153,6 +153,10 @@ void kr_bicg_xr(cudaStream_t s, int n, T* x, const T* sv, const T* t, T* r, cons
 template <class T>
 void kr_bicg_p(cudaStream_t s, int n, const T* r, const T* v, T* p, const KScalars* S);
 void kr_jacobi_update(cudaStream_t s, const CSRView& A, const double* nz, double* P);
+// apply_smoother!(JacobiSmoother) (Smoothers_jacobi.jl:88-110): `loops`
+// sweeps x -> xt, each copied back into x
+void kr_jacobi_smooth(cudaStream_t s, const CSRView& A, const double* nz, const double* b, double* x, double* xt,
+                      int loops, double omega);
 void kr_dilu_D(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const double* nz, double* D);
 template <class T>
 void kr_dilu_fwd(cudaStream_t s, const int* rows, int nrows, const CSRView& A, const T* nz, const T* D, const T* b,

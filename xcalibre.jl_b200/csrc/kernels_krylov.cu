@@ -203,6 +203,21 @@ __global__ void k_bicg_p(int n, const T* __restrict__ r, const T* __restrict__ v
     bicg_p_body<T>(grid_tiles(), n, r, v, p, S);
 }
 
+// multiply_row of the weighted Jacobi smoother (Smoothers_jacobi.jl:112-131):
+// the row sum in storage order, less the diagonal term, then
+// omega (1/a_ii) (b_i - sum) + (1 - omega) x_i into xt
+__global__ void k_jacobi_smooth(CSRView A, const double* __restrict__ nz, const double* __restrict__ b,
+                                const double* __restrict__ x, double* xt, double omega) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    double sum = row_dot(A, nz, x, i);
+    const double a_ii = nz[A.diag[i]];
+    const double xi = x[i];
+    sum = sum - a_ii * xi;
+    const double rD = 1.0 / a_ii;
+    xt[i] = omega * rD * (b[i] - sum) + (1.0 - omega) * xi;
+}
+
 // ---- preconditioners ----
 // update_Jacobi! (preconditioners_2_functions.jl:86-98)
 __global__ void k_jacobi_update(CSRView A, const double* __restrict__ nz, double* P) {
@@ -760,6 +775,14 @@ template <class T>
 void kr_bicg_p(cudaStream_t s, int n, const T* r, const T* v, T* p, const KScalars* S) {
     k_bicg_p<T><<<TILE_LAUNCH(n), s>>>(n, r, v, p, S);
     XCAL_CHECK_LAUNCH();
+}
+void kr_jacobi_smooth(cudaStream_t s, const CSRView& A, const double* nz, const double* b, double* x, double* xt,
+                      int loops, double omega) {
+    for (int l = 0; l < loops; ++l) {
+        k_jacobi_smooth<<<(A.n + 255) / 256, 256, 0, s>>>(A, nz, b, x, xt, omega);
+        XCAL_CHECK_LAUNCH();
+        XCAL_CUDA(cudaMemcpyAsync(x, xt, (size_t)A.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
 }
 void kr_jacobi_update(cudaStream_t s, const CSRView& A, const double* nz, double* P) {
     k_jacobi_update<<<TILE_LAUNCH(A.n), s>>>(A, nz, P);

@@ -41,6 +41,7 @@ class Mesh3:
     patch_count: np.ndarray      # int32 [n_patches]
     points: np.ndarray | None = None
     polymesh: object = None      # the PolyMesh it was built from (nodes and faces, for the writers)
+    dim: int = 3                 # 2: a Mesh2 (UNV2D_mesh), 3: a Mesh3
 
     @property
     def n_ifaces(self) -> int:
@@ -59,7 +60,7 @@ class Mesh3:
 
     def __repr__(self) -> str:  # Base.show(io, mesh) (Mesh_0_types.jl:185-198)
         n_nodes = 0 if self.points is None else len(self.points)
-        return f"3D Mesh with:\n-> {self.n_cells} cells\n-> {self.n_faces} faces\n-> {n_nodes} nodes"
+        return f"{self.dim}D Mesh with:\n-> {self.n_cells} cells\n-> {self.n_faces} faces\n-> {n_nodes} nodes"
 
 
 def build_mesh3(pm: PolyMesh) -> Mesh3:
