@@ -44,7 +44,10 @@ enum {
     XCAL_BC_SYMMETRY = 7,           /* symmetry.jl                           */
     XCAL_BC_NEUMANN = 8,            /* neumann.jl (scalar fields)            */
     XCAL_BC_PERIODIC = 9,           /* periodic.jl `Periodic` (shadow side)  */
-    XCAL_BC_PERIODIC_PARENT = 10    /* periodic.jl `PeriodicParent`          */
+    XCAL_BC_PERIODIC_PARENT = 10,   /* periodic.jl `PeriodicParent`          */
+    XCAL_BC_OMEGA_WALL = 11         /* OmegaWallFunction (Discretise_0_types.jl:
+                                       83-113; constraint RANS_functions.jl:
+                                       376-429): constants in xcal_bc.wall  */
 };
 /* Time{T}: src/Discretise/Discretise_1_schemes.jl:12-45 */
 enum { XCAL_TIME_STEADY = 0, XCAL_TIME_EULER = 1 };
@@ -62,14 +65,14 @@ enum { XCAL_LIMITER_NONE = 0, XCAL_LIMITER_CELL = 1 };
 enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
 /* preconditioner: src/Solve/Preconditioners/preconditioners_0_types.jl */
 enum { XCAL_PRECOND_NONE = 0, XCAL_PRECOND_JACOBI = 1, XCAL_PRECOND_DILU = 2 };
-/* turbulence: RANS{Laminar} / LES{Smagorinsky} */
-enum { XCAL_TURB_LAMINAR = 0, XCAL_TURB_SMAGORINSKY = 1 };
+/* turbulence: RANS{Laminar} / LES{Smagorinsky} / RANS{KOmega} */
+enum { XCAL_TURB_LAMINAR = 0, XCAL_TURB_SMAGORINSKY = 1, XCAL_TURB_KOMEGA = 2 };
 /* arithmetic of the Krylov inner iterations */
 enum { XCAL_PREC_FP64 = 0, XCAL_PREC_MIXED = 1 };
 /* pressure-velocity algorithm: run! dispatch, src/Solvers/Solvers_3_solver_dispatch.jl:120,225 */
 enum { XCAL_ALGO_SIMPLE = 0, XCAL_ALGO_PISO = 1 };
-/* equations */
-enum { XCAL_EQN_U = 0, XCAL_EQN_P = 1 };
+/* equations (k, omega: RANS{KOmega} transport equations) */
+enum { XCAL_EQN_U = 0, XCAL_EQN_P = 1, XCAL_EQN_K = 2, XCAL_EQN_OMEGA = 3 };
 
 /* field identifiers for xcal_case_get_field / xcal_case_set_field.
  * Cell fields hold n_cells values per component, face fields n_faces; vector
@@ -91,7 +94,9 @@ enum {
     XCAL_FIELD_PF = 12,    /* pf (n_faces)                                  */
     XCAL_FIELD_RDF = 13,   /* rDf (n_faces)                                 */
     XCAL_FIELD_DELTA = 14, /* LES filter (C*Delta)^2 (n_cells)              */
-    XCAL_FIELD_COUNT = 15
+    XCAL_FIELD_K = 15,     /* RANS{KOmega} k (n_cells)                      */
+    XCAL_FIELD_OMEGA = 16, /* RANS{KOmega} omega (n_cells)                  */
+    XCAL_FIELD_COUNT = 17
 };
 
 /* ---- mesh: the Mesh3 contract (src/Mesh/Mesh_0_types.jl:28-205) ---------
@@ -142,6 +147,10 @@ typedef struct {
     const int32_t* face_map;    /* [patch_count] partner face ids           */
     double distance[3];         /* LinearTransform.distance                 */
     int32_t partner_patch;
+    /* OmegaWallFunction: kappa, beta1, cmu^0.25 and yPlusLam =
+     * y_plus_laminar(E, kappa) (RANS_functions.jl:42-49), evaluated by the
+     * caller */
+    double wall[4];
 } xcal_bc;
 
 /* SolverSetup (src/Solve/Solve_1_api.jl:8-83) */
@@ -206,6 +215,18 @@ typedef struct {
     const xcal_bc* bc_U;
     const xcal_bc* bc_p;
     const xcal_bc* bc_nut;
+    /* RANS{KOmega} (RANS_kOmega.jl:29-52): coefficients beta_star (beta+),
+     * alpha1, beta1, sigma_k, sigma_omega; the k and omega equations' schemes
+     * (time, divergence) and solver setups (omega is solved with k's
+     * preconditioner type, :84-85); their boundary conditions */
+    double kw_beta_star, kw_alpha1, kw_beta1, kw_sigma_k, kw_sigma_omega;
+    xcal_schemes k_schemes;
+    xcal_schemes omega_schemes;
+    xcal_solver_setup k_solver;
+    xcal_solver_setup omega_solver;
+    int32_t n_bc_k, n_bc_omega;
+    const xcal_bc* bc_k;
+    const xcal_bc* bc_omega;
 } xcal_config;
 
 /* ---- polyMesh input of the mesh importer --------------------------------

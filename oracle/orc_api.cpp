@@ -94,6 +94,8 @@ static std::vector<double>* field_ptr(Case* C, int field, int& ncomp, int& per) 
         case XCAL_FIELD_PF: per = C->nF; return &C->pf;
         case XCAL_FIELD_RDF: per = C->nF; return &C->rDf;
         case XCAL_FIELD_DELTA: return &C->Delta;
+        case XCAL_FIELD_K: return &C->k;
+        case XCAL_FIELD_OMEGA: return &C->omega;
         default: return nullptr;
     }
 }

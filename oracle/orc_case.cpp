@@ -85,6 +85,7 @@ static void copy_bcs(const Mesh& m, const xcal_bc* src, int n, std::vector<BC>& 
         for (int c = 0; c < 3; ++c) bc.value[c] = src[b].value[c];
         bc.start = m.patch_start[bc.patch];
         bc.count = m.patch_count[bc.patch];
+        for (int c = 0; c < 4; ++c) bc.wall[c] = src[b].wall[c];
         if (bc.type == XCAL_BC_DIRICHLET_FUNCTION) {
             if (!src[b].face_values) throw std::runtime_error("DirichletFunction without values");
             bc.face_values.assign(src[b].face_values, src[b].face_values + (size_t)ncomp * bc.count);
@@ -110,6 +111,11 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     copy_bcs(*m, cfg->bc_p, cfg->n_bc_p, C->bcP, 1);
     copy_bcs(*m, cfg->bc_nut, cfg->n_bc_nut, C->bcNut, 1);
     C->cfg.bc_U = C->cfg.bc_p = C->cfg.bc_nut = nullptr;
+    if (cfg->turbulence == XCAL_TURB_KOMEGA) {
+        copy_bcs(*m, cfg->bc_k, cfg->n_bc_k, C->bcK, 1);
+        copy_bcs(*m, cfg->bc_omega, cfg->n_bc_omega, C->bcOmega, 1);
+    }
+    C->cfg.bc_k = C->cfg.bc_omega = nullptr;
     int nC = C->nC, nF = C->nF;
     for (int d = 0; d < 3; ++d) {
         C->U[d].assign(nC, 0.0);
@@ -129,6 +135,9 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     C->pf.assign(nF, 0.0);
     C->rDf.assign(nF, 1.0);  // initialise!(rDf, 1.0) (Solvers_1_SIMPLE.jl:61)
     C->Delta.assign(nC, 0.0);
+    for (std::vector<double>* v : {&C->k, &C->omega, &C->Pk, &C->Pw, &C->Dk, &C->Dw, &C->Pkw}) v->assign(nC, 0.0);
+    C->mueffk.assign(nF, 0.0);
+    C->mueffw.assign(nF, 0.0);
     C->prev.assign(nC, 0.0);
     C->cellsCourant.assign(nC, 0.0);
     C->bp.assign(nC, 0.0);
@@ -179,11 +188,11 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
 // ---------------------------------------------------------------------------
 // discretisation
 // ---------------------------------------------------------------------------
-enum TermKind { T_TIME, T_DIV, T_LAP };
+enum TermKind { T_TIME, T_DIV, T_LAP, T_SI };
 struct Term {
     TermKind kind;
     double sign;
-    const std::vector<double>* flux;  // face flux (Div: mdotf, Lap: nueff/rDf)
+    const std::vector<double>* flux;  // face flux (Div: mdotf, Lap: nueff/rDf); Si: cell coefficient
     int scheme;                       // time or divergence scheme
 };
 
@@ -199,7 +208,7 @@ static std::vector<Term> p_terms(Case& C) { return {{T_LAP, -1.0, &C.rDf, 0}}; }
 
 // scheme! (src/Discretise/Discretise_1_schemes.jl)
 static void scheme(const Mesh& m, const Term& t, int fID, int ns, double& ac, double& an) {
-    if (t.kind == T_TIME) {  // :12-23, :26-34
+    if (t.kind == T_TIME || t.kind == T_SI) {  // :12-23, :26-34, Si :204-210
         ac = 0.0;
         an = 0.0;
         return;
@@ -241,6 +250,9 @@ static void scheme_source(const Case& C, const Term& t, int c, double prev, doub
         double vol_rdt = (1.0 * C.m->cvol[c]) / C.cfg.dt;
         ac = vol_rdt;
         b = prev * vol_rdt;
+    } else if (t.kind == T_SI) {  // Si (:211-218): sign * flux[c] * volume
+        ac = (t.sign * (*t.flux)[c]) * C.m->cvol[c];
+        b = 0.0;
     } else {
         ac = 0.0;
         b = 0.0;
@@ -357,7 +369,7 @@ static void bc_functor(BCCtx& X, const BC& bc, const Term& t, int f, double& ap,
     int cell = m.bcell[f];
     ap = 0.0;
     bp = 0.0;
-    if (t.kind == T_TIME) return;  // Discretise_3_boundary_conditions.jl:2-9
+    if (t.kind == T_TIME || t.kind == T_SI) return;  // Discretise_3_boundary_conditions.jl:2-9; Si: (0, 0)
     double flux = (*t.flux)[f];
     switch (bc.type) {
         case XCAL_BC_DIRICHLET:
@@ -398,6 +410,7 @@ static void bc_functor(BCCtx& X, const BC& bc, const Term& t, int f, double& ap,
         case XCAL_BC_ZEROGRADIENT:  // zerogradient.jl
             if (t.kind == T_DIV) ap = t.sign * flux;
             return;
+        case XCAL_BC_OMEGA_WALL:    // Discretise_3_boundary_conditions.jl:28-61 (as Extrapolated)
         case XCAL_BC_EXTRAPOLATED:  // extrapolated.jl
             if (t.kind == T_LAP) {
                 double fl = ((-flux) * m.farea[f]) / m.fdelta[f];
@@ -846,6 +859,7 @@ static void correct_boundaries(Case& C, const std::vector<BC>& bcs, std::vector<
                     phif[0][f] = phi[0][c];
                 break;
             case XCAL_BC_ZEROGRADIENT:
+            case XCAL_BC_OMEGA_WALL:
             case XCAL_BC_EXTRAPOLATED:
                 for (int d = 0; d < ncomp; ++d) phif[d][f] = phi[d][c];
                 break;
@@ -1226,8 +1240,190 @@ void correct(Case& C) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// RANS{KOmega} (src/ModelPhysics/Turbulence/RANS_kOmega.jl)
+// ---------------------------------------------------------------------------
+// _discretise_scalar_model! (Discretise_2_generated_distretisation.jl:125-167)
+// with a field `phi` (Time terms) and +Source(src)
+static void discretise_scalar(Case& C, const std::vector<Term>& terms, CSR& A, std::vector<double>& b,
+                              const std::vector<double>& phi, const std::vector<double>& src) {
+    const Mesh& m = *C.m;
+    std::fill(A.nzval.begin(), A.nzval.end(), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < C.nC; ++i) {
+        double ac_sum = 0.0;
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            int fID = m.cell_faces[k], ns = m.cell_nsign[k], nID = m.cell_neigh[k];
+            double AC = 0.0, AN = 0.0;
+            for (const Term& t : terms) {
+                double ac, an;
+                scheme(m, t, fID, ns, ac, an);
+                AC = AC + ac;
+                AN = AN + an;
+            }
+            ac_sum = ac_sum + AC;
+            A.nzval[A.find(i, nID)] = AN;
+        }
+        double AC = 0.0, B = 0.0;
+        for (const Term& t : terms) {
+            double ac, bb;
+            scheme_source(C, t, i, phi[i], ac, bb);
+            AC = AC + ac;
+            B = B + bb;
+        }
+        A.nzval[A.diag[i]] = ac_sum + AC;
+        double b2 = 0.0 + (1.0 * src[i]) * m.cvol[i];  // _sources!: +Source(src)
+        b[i] = b2 + B;
+    }
+}
+
+// apply_boundary_conditions! of a scalar equation, ascending boundary face id
+static void apply_bcs_scalar(Case& C, const std::vector<Term>& terms, CSR& A, std::vector<double>& b,
+                             const std::vector<BC>& bcs, const std::vector<double>& phi) {
+    const Mesh& m = *C.m;
+    BCCtx X{&C, &A, false, 0, &phi};
+    for (int f = 0; f < C.nB; ++f) {
+        const BC* bc = find_bc(bcs, f);
+        if (!bc) continue;
+        int cell = m.bcell[f];
+        double AP = 0.0, BP = 0.0;
+        for (const Term& t : terms) {
+            double ap, bp;
+            bc_functor(X, *bc, t, f, ap, bp);
+            AP = AP + ap;
+            BP = BP + bp;
+        }
+        A.nzval[A.diag[cell]] = A.nzval[A.diag[cell]] + AP;
+        b[cell] = b[cell] + BP;
+    }
+}
+
+// implicit_relaxation_diagdom! (Solve_1_api.jl:388-411) of a scalar equation
+static void relax_scalar(CSR& A, std::vector<double>& b, const std::vector<double>& field, double alpha) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < A.n; ++i) {
+        int c = A.diag[i];
+        double sumv = 0.0;
+        for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) sumv = sumv + std::fabs(A.nzval[k]);
+        sumv = sumv - std::fabs(A.nzval[c]);
+        double D0 = A.nzval[c];
+        double D_max = jl_max(std::fabs(D0), sumv) / alpha;
+        A.nzval[c] = D_max;
+        b[i] = b[i] + (D_max - D0) * field[i];
+    }
+}
+
+// constrain_equation!(omega_eqn, OmegaWallFunction) (RANS_functions.jl:376-429):
+// per wall face, in BC order then face order, the wall cell's row becomes
+// omega = omega_log (y+ > yPlusLam) or omega_vis, from the current k
+static void constrain_omega(Case& C, CSR& A, std::vector<double>& b) {
+    const Mesh& m = *C.m;
+    const double nu = C.cfg.nu;
+    for (const BC& bc : C.bcOmega) {
+        if (bc.type != XCAL_BC_OMEGA_WALL) continue;
+        const double kappa = bc.wall[0], beta1 = bc.wall[1], c25 = bc.wall[2], yPlusLam = bc.wall[3];
+        for (int f = bc.start; f < bc.start + bc.count; ++f) {
+            const int c = m.bcell[f];
+            const double y = m.fdelta[f];
+            const double w_vis = (6.0 * nu) / (beta1 * (y * y));          // omega_vis (:50)
+            const double w_log = std::sqrt(C.k[c]) / ((c25 * kappa) * y);  // omega_log (:51)
+            const double yplus = ((c25 * y) * std::sqrt(C.k[c])) / nu;    // y_plus (:52)
+            const double wc = yplus > yPlusLam ? w_log : w_vis;
+            for (int e = A.rowptr[c]; e < A.rowptr[c + 1]; ++e) A.nzval[e] = 0.0;
+            A.nzval[A.diag[c]] = 1.0;
+            b[c] = wc;
+        }
+    }
+}
+
+// bound! (RANS_functions.jl:2-41): each cell from the values before the
+// call (the reference updates in place while neighbours read, so its result
+// can depend on thread order where adjacent cells are both clipped)
+static void bound_field(const Mesh& m, std::vector<double>& v) {
+    const double mzero = jl_eps(1.0);
+    const std::vector<double> old(v);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < (int)v.size(); ++i) {
+        double sum_flux = 0.0;
+        int sum_area = 0;
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            sum_flux = sum_flux + jl_max(old[m.cell_neigh[k]], mzero);
+            sum_area += 1;
+        }
+        const double average = sum_flux / (double)sum_area;
+        // average * signbit(v): average, or a zero with average's sign
+        const double s = std::signbit(old[i]) ? average : std::copysign(0.0, average);
+        v[i] = jl_max(jl_max(old[i], s), mzero);
+    }
+}
+
+// solve_system! of k or omega on the shared scalar system
+static double solve_scalar(Case& C, const xcal_solver_setup& SS0, int ptype, std::vector<double>& field) {
+    xcal_solver_setup SS = SS0;
+    SS.precond = ptype;
+    CSR& A = C.Ap;
+    if (SS.smoother_loops > 0) jacobi_smooth(A, C.bp.data(), field.data(), SS.smoother_loops, SS.smoother_omega);
+    if (SS.solver == XCAL_SOLVER_CG)
+        krylov_cg(A, C.bp, field, SS.precond, C.Pkw, SS, C.kp);
+    else
+        krylov_bicgstab(A, C.bp, field, SS.precond, C.Pkw, SS, C.kp);
+    return residual(A, C.bp, field);
+}
+
+// turbulence!(::KOmegaModel) after grad!(gradU) (RANS_kOmega.jl:146-210)
+static void komega(Case& C) {
+    const Mesh& m = *C.m;
+    const xcal_config& cf = C.cfg;
+    for (int i = 0; i < C.nC; ++i) {
+        // magnitude2!(Pk, S, scale_factor = 2) (RANS_tensor_algebra.jl:81-99), S = 0.5 (G + G')
+        double sum = 0.0;
+        for (int j = 0; j < 3; ++j)
+            for (int q = 0; q < 3; ++q) {
+                const double s = 0.5 * (C.gradU[3 * j + q][i] + C.gradU[3 * q + j][i]);
+                sum = sum + s * s;
+            }
+        const double mag = sum * 2.0;
+        C.Pw[i] = cf.kw_alpha1 * mag;           // rho alpha1 Pk (rho = 1)
+        C.Pk[i] = C.nut[i] * mag;               // rho nut Pk
+        C.Dw[i] = cf.kw_beta1 * C.omega[i];     // rho beta1 omega
+        C.Dk[i] = cf.kw_beta_star * C.omega[i];  // rho beta+ omega
+    }
+    for (int f = 0; f < C.nF; ++f) {  // rhof (nuf + sigma nutf), rhof = 1
+        C.mueffw[f] = cf.nu + cf.kw_sigma_omega * C.nutf[f];
+        C.mueffk[f] = cf.nu + cf.kw_sigma_k * C.nutf[f];
+    }
+    const int ptype = cf.k_solver.precond;
+    // omega: Time + Div(mdotf) - Lap(mueffw) + Si(Dw) == Source(Pw)
+    std::vector<Term> tw = {{T_TIME, 1.0, nullptr, cf.omega_schemes.time},
+                            {T_DIV, 1.0, &C.mdotf, cf.omega_schemes.divergence},
+                            {T_LAP, -1.0, &C.mueffw, 0},
+                            {T_SI, 1.0, &C.Dw, 0}};
+    discretise_scalar(C, tw, C.Ap, C.bp, C.omega, C.Pw);
+    apply_bcs_scalar(C, tw, C.Ap, C.bp, C.bcOmega, C.omega);
+    relax_scalar(C.Ap, C.bp, C.omega, cf.omega_solver.relax);
+    constrain_omega(C, C.Ap, C.bp);
+    update_precond(C.Ap, ptype, C.Pkw);
+    C.res_omega = solve_scalar(C, cf.omega_solver, ptype, C.omega);
+    bound_field(m, C.omega);
+    // k: Time + Div(mdotf) - Lap(mueffk) + Si(Dk) == Source(Pk)
+    std::vector<Term> tk = {{T_TIME, 1.0, nullptr, cf.k_schemes.time},
+                            {T_DIV, 1.0, &C.mdotf, cf.k_schemes.divergence},
+                            {T_LAP, -1.0, &C.mueffk, 0},
+                            {T_SI, 1.0, &C.Dk, 0}};
+    discretise_scalar(C, tk, C.Ap, C.bp, C.k, C.Pk);
+    apply_bcs_scalar(C, tk, C.Ap, C.bp, C.bcK, C.k);
+    relax_scalar(C.Ap, C.bp, C.k, cf.k_solver.relax);
+    update_precond(C.Ap, ptype, C.Pkw);
+    C.res_k = solve_scalar(C, cf.k_solver, ptype, C.k);
+    bound_field(m, C.k);
+    for (int i = 0; i < C.nC; ++i) C.nut[i] = C.k[i] / C.omega[i];
+    interpolate(m, C.nut, C.nutf);
+    correct_boundaries(C, C.bcNut, &C.nutf, &C.nut, false);
+}
+
 void turbulence(Case& C) {
-    grad_U(C);  // RANS_laminar.jl:73-79, LES_Smagorinsky.jl:117
+    grad_U(C);  // RANS_laminar.jl:73-79, LES_Smagorinsky.jl:117, RANS_kOmega.jl:167-168
+    if (C.cfg.turbulence == XCAL_TURB_KOMEGA) komega(C);
     if (C.cfg.turbulence == XCAL_TURB_SMAGORINSKY) {
         // LES_Smagorinsky.jl:122-131
         for (int i = 0; i < C.nC; ++i) {

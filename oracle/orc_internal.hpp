@@ -52,6 +52,7 @@ struct BC {
     V3 distance{0, 0, 0};
     int partner_patch = -1;
     int start = 0, count = 0;  // IDs_range
+    double wall[4] = {0, 0, 0, 0};  // OmegaWallFunction: kappa, beta1, cmu^0.25, yPlusLam
 };
 
 struct Krylov {
@@ -63,7 +64,7 @@ struct Krylov {
 struct Case {
     const Mesh* m = nullptr;
     xcal_config cfg{};
-    std::vector<BC> bcU, bcP, bcNut;
+    std::vector<BC> bcU, bcP, bcNut, bcK, bcOmega;
     int nC = 0, nF = 0, nB = 0;
 
     // fields
@@ -75,6 +76,10 @@ struct Case {
     // preconditioners
     std::vector<double> PU, Pp;  // Jacobi storage (1/|A_ii|) or DILU D
     Krylov kU, kp;
+    // RANS{KOmega}: fields, production / dissipation, face diffusivities,
+    // the k/omega preconditioner (shared, RANS_kOmega.jl:84-85), residuals
+    std::vector<double> k, omega, Pk, Pw, Dk, Dw, mueffk, mueffw, Pkw;
+    double res_k = 0.0, res_omega = 0.0;
     std::vector<int> rorder;  // morton_order of the cell centres
     double time = 0.0;
     bool initialised = false;

@@ -16,6 +16,9 @@ Fixtures:
   bfs_10mm_unv.npz        -- examples/0_GRIDS/backwardFacingStep_10mm.unv (the mesh of
                              test/0_TEST_CASES/2d_incompressible_laminar_BFS.jl), parsed by
                              the small reader below into points, elements and groups.
+  bfs_5mm_unv.npz         -- examples/0_GRIDS/backwardFacingStep_5mm.unv (the mesh of
+                             test/0_TEST_CASES/2d_incompressible_transient_KOmega_BFS_lowRe.jl),
+                             parsed the same way.
 
 Usage: python tests/golden/make_fixtures.py [/path/to/XCALibre.jl]
 """
@@ -161,8 +164,9 @@ def main(ref: str) -> None:
         json.dump(laplace_expected(os.path.join(ref, "test/unit_test_laplace.jl")), f, indent=1)
     with open(os.path.join(HERE, "smoother_5x5.json"), "w") as f:
         json.dump(smoother_system(os.path.join(ref, "test/test_smoothers.jl")), f, indent=1)
-    np.savez_compressed(os.path.join(HERE, "bfs_10mm_unv.npz"),
-                        **read_unv_raw(os.path.join(ref, "examples/0_GRIDS/backwardFacingStep_10mm.unv")))
+    for mm in (10, 5):
+        np.savez_compressed(os.path.join(HERE, "bfs_%dmm_unv.npz" % mm),
+                            **read_unv_raw(os.path.join(ref, "examples/0_GRIDS/backwardFacingStep_%dmm.unv" % mm)))
     print("fixtures written to", HERE)
 
 

@@ -1,0 +1,147 @@
+"""RANS{KOmega} on the GPU against the oracle (1e-10 relative L2, expected
+0): the reference's transient k-omega backward-facing step (its own grid,
+committed raw parse) host-polled and in graph mode, over 500 steps to its
+known answer (outlet Ux = 0.5 inlet Ux within 0.1 Umag); a steady SIMPLE
+k-omega channel with omega wall functions; k-omega cases refused by the
+batch."""
+import numpy as np
+import pytest
+
+from test_komega import KW_FIELDS, komega_bfs_case, set_komega_fields
+from test_nonorth_oracle import skewed_channel
+from test_unv import bfs_mesh
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0)
+
+
+def _pair(x, orc, ctx, mesh, model, cfg, graph):
+    dm = x.DeviceMesh(ctx, mesh)
+    g = x.Case(dm, cfg)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    for c in (g, o):
+        set_komega_fields(x, c, model)
+    if graph:
+        g.set_graph_mode(True)
+    return g, o, dm
+
+
+def _check(x, g, o, fields=KW_FIELDS + ("FIELD_NUTF", "FIELD_NUEFF", "FIELD_GRADU")):
+    for f in fields:
+        assert rel(g.get_field(getattr(x._abi, f)), o.get_field(getattr(x._abi, f))) <= TOL, f
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_komega_bfs_parity(x, orc, ctx, graph):
+    mesh = bfs_mesh(x, 5)
+    model, config = komega_bfs_case(x, mesh, steps=10)
+    cfg, keep = x.build_config(model, config)
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, graph)
+    rg, _ = g.piso_step(10)
+    ro, _ = o.piso_step(10)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    _check(x, g, o)
+
+
+def test_komega_bfs_known_answer_gpu(x, orc, ctx):
+    mesh = bfs_mesh(x, 5)
+    model, config = komega_bfs_case(x, mesh)
+    cfg, keep = x.build_config(model, config)
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, True)
+    rg, _ = g.piso_step(500)
+    ro, _ = o.piso_step(500)
+    assert rel(rg, ro) <= TOL
+    _check(x, g, o, KW_FIELDS)
+    U = g.get_field(x._abi.FIELD_U)
+    inlet = x.api.boundary_average("inlet", U, config.boundaries["U"], mesh=mesh)
+    outlet = x.api.boundary_average("outlet", U, config.boundaries["U"], mesh=mesh)
+    assert np.linalg.norm(outlet - 0.5 * inlet) <= 0.1 * 1.5, (inlet, outlet)
+
+
+def komega_channel_case(x, mesh, iterations, precond="Jacobi"):
+    """Steady SIMPLE with RANS{KOmega} on a 3D channel: k and omega Dirichlet
+    at the inlet, Extrapolated at the outlet, omega wall functions and
+    k = nut = 0 on the walls."""
+    A = x.api
+    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=1e-3), turbulence=A.RANS(A.KOmega),
+                      energy=A.Energy(A.Isothermal), domain=mesh)
+    BCs = A.assign(region=mesh,
+                   U=[A.Dirichlet("inlet", [1.0, 0.0, 0.0]), A.Zerogradient("outlet"), A.Wall("walls", [0.0, 0.0, 0.0])],
+                   p=[A.Zerogradient("inlet"), A.Dirichlet("outlet", 0.0), A.Wall("walls")],
+                   k=[A.Dirichlet("inlet", 0.01), A.Extrapolated("outlet"), A.Dirichlet("walls", 0.0)],
+                   omega=[A.Dirichlet("inlet", 10.0), A.Extrapolated("outlet"), A.OmegaWallFunction("walls")],
+                   nut=[A.Dirichlet("inlet", 1e-3), A.Extrapolated("outlet"), A.Dirichlet("walls", 0.0)])
+    pre = getattr(A, precond)
+
+    def ss(s, relax):
+        return A.SolverSetup(solver=s(), preconditioner=pre(), convergence=1e-7, relax=relax, rtol=1e-2)
+
+    config = A.Configuration(solvers={"U": ss(A.Bicgstab, 0.7), "p": ss(A.Cg, 0.3), "k": ss(A.Bicgstab, 0.7),
+                                      "omega": ss(A.Bicgstab, 0.7)},
+                             schemes={"U": A.Schemes(divergence=A.Upwind), "p": A.Schemes(),
+                                      "k": A.Schemes(divergence=A.Upwind), "omega": A.Schemes(divergence=A.Upwind)},
+                             runtime=A.Runtime(iterations=iterations, write_interval=-1, time_step=1.0),
+                             hardware=A.Hardware(backend=A.B200Backend()), boundaries=BCs)
+    A.initialise_(model.momentum.U, [1.0, 0.0, 0.0])
+    A.initialise_(model.momentum.p, 0.0)
+    A.initialise_(model.turbulence.k, 0.01)
+    A.initialise_(model.turbulence.omega, 10.0)
+    A.initialise_(model.turbulence.nut, 1e-3)
+    return model, config
+
+
+@pytest.mark.parametrize("precond", ["Jacobi", "DILU"])
+def test_komega_simple_channel_parity(x, orc, ctx, precond):
+    mesh = skewed_channel(x, n=(12, 7, 6), seed=11)
+    model, config = komega_channel_case(x, mesh, 6, precond)
+    cfg, keep = x.build_config(model, config)
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, False)
+    rg, _ = g.simple_iterate(6)
+    ro, _ = o.simple_iterate(6)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    _check(x, g, o)
+
+
+def test_komega_not_batched(x, ctx):
+    mesh = skewed_channel(x, n=(6, 4, 4), seed=2)
+    model, config = komega_channel_case(x, mesh, 2)
+    cfg, keep = x.build_config(model, config)
+    dm = x.DeviceMesh(ctx, mesh)
+    c = x.Case(dm, cfg)
+    batch = x.api.Batch(ctx, 2, 1 << 30)
+    with pytest.raises(Exception):
+        batch.add(c)
+    batch.close()
+
+
+def test_komega_restart_bit_identical(x, ctx):
+    """checkpoint() / restore() carry k and omega: 4 + 4 steps from a
+    restored case equal 8 steps in one go."""
+    mesh = bfs_mesh(x, 5)
+
+    def new_case():
+        model, config = komega_bfs_case(x, mesh, steps=8)
+        cfg, keep = x.build_config(model, config)
+        dm = x.DeviceMesh(ctx, mesh)
+        c = x.Case(dm, cfg)
+        set_komega_fields(x, c, model)
+        return c, (dm, keep)
+
+    a, ka = new_case()
+    ra = a.piso_step(8)[0]
+    b, kb = new_case()
+    rb = b.piso_step(4)[0]
+    state = b.checkpoint()
+    assert "FIELD_K" in state and "FIELD_OMEGA" in state
+    c, kc = new_case()
+    c.restore(state)
+    rc = c.piso_step(4)[0]
+    assert np.array_equal(np.concatenate([rb, rc]), ra)
+    for f in KW_FIELDS:
+        assert np.array_equal(c.get_field(getattr(x._abi, f)), a.get_field(getattr(x._abi, f))), f

@@ -1,0 +1,137 @@
+"""RANS{KOmega} (RANS_kOmega.jl) on the CPU oracle.
+
+* the reference's known answer of
+  test/0_TEST_CASES/2d_incompressible_transient_KOmega_BFS_lowRe.jl on its own
+  grid (backwardFacingStep_5mm.unv, committed raw parse): 500 PISO steps of
+  0.01 s with k and omega transported (OmegaWallFunction on the wall and top,
+  Midpoint gradients), outlet Ux = 0.5 inlet Ux within 0.1 Umag;
+* the wall-function constants (y_plus_laminar, RANS_functions.jl:42-45), the
+  omega wall rows (constrain!, :376-429) and bound! (:2-41) on a few steps;
+* the wall functions that are not implemented are refused."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from test_unv import bfs_mesh
+
+REF = "/root/reference/examples/0_GRIDS/backwardFacingStep_5mm.unv"
+
+
+def komega_bfs_case(x, mesh, steps=500, precision="fp64"):
+    """2d_incompressible_transient_KOmega_BFS_lowRe.jl:11-121."""
+    A = x.api
+    nu, Umag, k_in, w_in = 1e-3, 1.5, 1.0, 1000.0
+    model = A.Physics(time=A.Transient(), fluid=A.Fluid(A.Incompressible, nu=nu), turbulence=A.RANS(A.KOmega),
+                      energy=A.Energy(A.Isothermal), domain=mesh)
+    BCs = A.assign(region=mesh,
+                   U=[A.Dirichlet("inlet", [Umag, 0.0, 0.0]), A.Extrapolated("outlet"),
+                      A.Wall("wall", [0.0, 0.0, 0.0]), A.Dirichlet("top", [0.0, 0.0, 0.0])],
+                   p=[A.Extrapolated("inlet"), A.Dirichlet("outlet", 0.0), A.Extrapolated("wall"),
+                      A.Extrapolated("top")],
+                   k=[A.Dirichlet("inlet", k_in), A.Extrapolated("outlet"), A.Dirichlet("wall", 0.0),
+                      A.Dirichlet("top", 0.0)],
+                   omega=[A.Dirichlet("inlet", w_in), A.Extrapolated("outlet"), A.OmegaWallFunction("wall"),
+                          A.OmegaWallFunction("top")],
+                   nut=[A.Dirichlet("inlet", k_in / w_in), A.Extrapolated("outlet"), A.Dirichlet("wall", 0.0),
+                        A.Dirichlet("top", 0.0)])
+
+    def sch():
+        return A.Schemes(gradient=A.Midpoint, time=A.Euler)
+
+    def ss(s):
+        return A.SolverSetup(solver=s(), preconditioner=A.Jacobi(), convergence=1e-7, relax=1.0, rtol=1e-3)
+
+    config = A.Configuration(solvers={"U": ss(A.Bicgstab), "p": ss(A.Cg), "k": ss(A.Bicgstab),
+                                      "omega": ss(A.Bicgstab)},
+                             schemes={"U": sch(), "p": A.Schemes(gradient=A.Midpoint), "k": sch(), "omega": sch()},
+                             runtime=A.Runtime(iterations=steps, write_interval=steps, time_step=0.01),
+                             hardware=A.Hardware(backend=A.B200Backend(precision=precision)), boundaries=BCs)
+    A.initialise_(model.momentum.U, [Umag, 0.0, 0.0])
+    A.initialise_(model.momentum.p, 0.0)
+    A.initialise_(model.turbulence.k, k_in)
+    A.initialise_(model.turbulence.omega, w_in)
+    A.initialise_(model.turbulence.nut, k_in / w_in)
+    return model, config
+
+
+KW_FIELDS = ("FIELD_U", "FIELD_P", "FIELD_K", "FIELD_OMEGA", "FIELD_NUT")
+
+
+def set_komega_fields(x, c, model):
+    for f, v in (("FIELD_U", model.momentum.U), ("FIELD_P", model.momentum.p), ("FIELD_K", model.turbulence.k),
+                 ("FIELD_OMEGA", model.turbulence.omega), ("FIELD_NUT", model.turbulence.nut)):
+        c.set_field(getattr(x._abi, f), v)
+
+
+@pytest.mark.skipif(not os.path.isfile(REF), reason="reference checkout not present")
+def test_bfs_5mm_fixture_matches_file(x):
+    a = x.UNV2D_mesh(REF, scale=0.001)
+    b = bfs_mesh(x, 5)
+    assert (a.n_cells, a.n_faces) == (7200, 14640)
+    for k in ("face_owner", "face_neigh", "face_centre", "face_normal", "face_area", "face_delta", "face_weight",
+              "cell_centre", "cell_volume", "cell_faces", "cell_nsign", "boundary_cellsID", "patch_start"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_komega_bfs_known_answer(x, orc):
+    mesh = bfs_mesh(x, 5)
+    model, config = komega_bfs_case(x, mesh)
+    cfg, keep = x.build_config(model, config)
+    assert cfg.turbulence == x._abi.TURB_KOMEGA and cfg.n_bc_omega == 4
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    set_komega_fields(x, o, model)
+    res, _ = o.piso_step(500)
+    assert np.all(np.isfinite(res))
+    U = o.get_field(x._abi.FIELD_U)
+    inlet = x.api.boundary_average("inlet", U, config.boundaries["U"], mesh=mesh)
+    outlet = x.api.boundary_average("outlet", U, config.boundaries["U"], mesh=mesh)
+    assert inlet[0] == pytest.approx(1.5)
+    assert np.linalg.norm(outlet - 0.5 * inlet) <= 0.1 * 1.5, (inlet, outlet)
+    k, w, nut = (o.get_field(getattr(x._abi, f)) for f in ("FIELD_K", "FIELD_OMEGA", "FIELD_NUT"))
+    eps = np.spacing(1.0)
+    assert k.min() >= eps and w.min() >= eps  # bound!
+    assert np.array_equal(nut, k / w)
+
+
+def test_komega_wall_rows(x, orc):
+    """After a few steps every wall cell holds omega_vis or omega_log of the
+    k it saw, and the constants are the reference's."""
+    A = x.api
+    bc = A.OmegaWallFunction("wall")
+    yl = 11.0
+    for _ in range(10):
+        yl = math.log(max(yl * 9.8, 1.0)) / 0.41
+    assert bc.wall == (0.41, 0.075, 0.09 ** 0.25, yl)
+    assert 11.0 < yl < 12.0
+    mesh = bfs_mesh(x, 5)
+    model, config = komega_bfs_case(x, mesh, steps=3)
+    cfg, keep = x.build_config(model, config)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    set_komega_fields(x, o, model)
+    o.piso_step(2)
+    k_before = o.get_field(x._abi.FIELD_K)
+    o.piso_step(1)
+    w = o.get_field(x._abi.FIELD_OMEGA)
+    # the last wall face of each cell (BC order wall, top; face order) sets its row
+    last = {}
+    for name in ("wall", "top"):
+        for f in mesh.patch_range(name):
+            last[int(mesh.boundary_cellsID[f])] = f
+    nu = 1e-3
+    for c, f in last.items():
+        y = mesh.face_delta[f]
+        sk = math.sqrt(k_before[c])
+        w_vis = (6.0 * nu) / (0.075 * (y * y))
+        w_log = sk / ((0.09 ** 0.25 * 0.41) * y)
+        yplus = ((0.09 ** 0.25 * y) * sk) / nu
+        expect = w_log if yplus > yl else w_vis
+        assert w[c] == max(expect, np.spacing(1.0)), (c, w[c], expect)
+
+
+def test_unsupported_wall_functions(x):
+    with pytest.raises(NotImplementedError):
+        x.KWallFunction("wall")
+    with pytest.raises(NotImplementedError):
+        x.NutWallFunction("wall")

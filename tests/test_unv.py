@@ -24,9 +24,9 @@ GRIDS = os.path.join(REF, "test", "grids")
 EX = os.path.join(REF, "examples", "0_GRIDS")
 
 
-def bfs_mesh(x):
-    """backwardFacingStep_10mm.unv (scale 0.001) from tests/golden/bfs_10mm_unv.npz."""
-    d = np.load(os.path.join(GOLD, "bfs_10mm_unv.npz"))
+def bfs_mesh(x, mm=10):
+    """backwardFacingStep_<mm>mm.unv (scale 0.001) from tests/golden/bfs_<mm>mm_unv.npz."""
+    d = np.load(os.path.join(GOLD, "bfs_%dmm_unv.npz" % mm))
     verts = d["elem_vertices"] - 1
     off = np.concatenate([[0], np.cumsum(d["elem_count"])])
     elements = [(int(i), int(c), verts[off[k]:off[k + 1]].tolist())

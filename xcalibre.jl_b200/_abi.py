@@ -27,6 +27,7 @@ BC_SYMMETRY = 7
 BC_NEUMANN = 8
 BC_PERIODIC = 9
 BC_PERIODIC_PARENT = 10
+BC_OMEGA_WALL = 11
 
 TIME_STEADY, TIME_EULER = 0, 1
 DIV_LINEAR, DIV_UPWIND, DIV_LUST = 0, 1, 2
@@ -34,21 +35,22 @@ GRAD_GAUSS, GRAD_MIDPOINT = 0, 1
 LIMITER_NONE, LIMITER_CELL = 0, 1
 SOLVER_CG, SOLVER_BICGSTAB = 0, 1
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_DILU = 0, 1, 2
-TURB_LAMINAR, TURB_SMAGORINSKY = 0, 1
+TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 ALGO_SIMPLE, ALGO_PISO = 0, 1
-EQN_U, EQN_P = 0, 1
+EQN_U, EQN_P, EQN_K, EQN_OMEGA = 0, 1, 2, 3
 
 FIELD_U, FIELD_P, FIELD_MDOTF, FIELD_NUEFF, FIELD_GRADP, FIELD_GRADU = 0, 1, 2, 3, 4, 5
 FIELD_RD, FIELD_HV, FIELD_DIVHV, FIELD_NUT, FIELD_NUTF, FIELD_UF = 6, 7, 8, 9, 10, 11
-FIELD_PF, FIELD_RDF, FIELD_DELTA = 12, 13, 14
+FIELD_PF, FIELD_RDF, FIELD_DELTA, FIELD_K, FIELD_OMEGA = 12, 13, 14, 15, 16
 
 # (components, "cell"|"face") per field id
 FIELD_SHAPE = {
     FIELD_U: (3, "cell"), FIELD_P: (1, "cell"), FIELD_MDOTF: (1, "face"), FIELD_NUEFF: (1, "face"),
     FIELD_GRADP: (3, "cell"), FIELD_GRADU: (9, "cell"), FIELD_RD: (1, "cell"), FIELD_HV: (3, "cell"),
     FIELD_DIVHV: (1, "cell"), FIELD_NUT: (1, "cell"), FIELD_NUTF: (1, "face"), FIELD_UF: (3, "face"),
-    FIELD_PF: (1, "face"), FIELD_RDF: (1, "face"), FIELD_DELTA: (1, "cell"),
+    FIELD_PF: (1, "face"), FIELD_RDF: (1, "face"), FIELD_DELTA: (1, "cell"), FIELD_K: (1, "cell"),
+    FIELD_OMEGA: (1, "cell"),
 }
 
 _pi32 = C.POINTER(C.c_int32)
@@ -90,7 +92,7 @@ class BCDesc(C.Structure):
     _fields_ = [
         ("type", C.c_int32), ("patch", C.c_int32), ("value", C.c_double * 3),
         ("face_values", _pf64), ("face_map", _pi32), ("distance", C.c_double * 3),
-        ("partner_patch", C.c_int32),
+        ("partner_patch", C.c_int32), ("wall", C.c_double * 4),
     ]
 
 
@@ -114,6 +116,12 @@ class ConfigDesc(C.Structure):
         ("dt", C.c_double), ("has_pref", C.c_int32), ("pref", C.c_double), ("inner_loops", C.c_int32),
         ("ncorrectors", C.c_int32), ("precision", C.c_int32), ("inner_rtol", C.c_double), ("n_bc_U", C.c_int32), ("n_bc_p", C.c_int32), ("n_bc_nut", C.c_int32),
         ("bc_U", C.POINTER(BCDesc)), ("bc_p", C.POINTER(BCDesc)), ("bc_nut", C.POINTER(BCDesc)),
+        ("kw_beta_star", C.c_double), ("kw_alpha1", C.c_double), ("kw_beta1", C.c_double),
+        ("kw_sigma_k", C.c_double), ("kw_sigma_omega", C.c_double),
+        ("k_schemes", SchemesDesc), ("omega_schemes", SchemesDesc),
+        ("k_solver", SolverSetupDesc), ("omega_solver", SolverSetupDesc),
+        ("n_bc_k", C.c_int32), ("n_bc_omega", C.c_int32),
+        ("bc_k", C.POINTER(BCDesc)), ("bc_omega", C.POINTER(BCDesc)),
     ]
 
 

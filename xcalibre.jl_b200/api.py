@@ -19,6 +19,7 @@ selects this implementation (the reference's ``CUDABackend()`` slot).
 from __future__ import annotations
 
 import ctypes as C
+import math
 from dataclasses import dataclass, field
 from typing import Callable
 
@@ -101,6 +102,11 @@ class Laminar: ...
 
 
 class Smagorinsky: ...
+
+
+class KOmega:
+    """RANS{KOmega} (RANS_kOmega.jl): k and omega transport equations,
+    nut = k / omega."""
 
 
 class Incompressible: ...
@@ -215,7 +221,14 @@ class Fluid:
 
 @dataclass
 class RANS:
+    """RANS{Laminar} or RANS{KOmega}(; beta+, alpha1, beta1, sigma_k,
+    sigma_omega) (RANS_kOmega.jl:29-33)."""
     model: type = Laminar
+    beta_star: float = 0.09
+    alpha1: float = 0.52
+    beta1: float = 0.072
+    sigma_k: float = 0.5
+    sigma_omega: float = 0.5
 
 
 @dataclass
@@ -245,6 +258,12 @@ class Physics:
         n = domain.n_cells
         self.momentum = Momentum(U=np.zeros((3, n)), p=np.zeros(n))
         self.nut = np.zeros(n)
+        # model.turbulence.k / .omega / .nut, as the reference's fields
+        if isinstance(turbulence, (RANS, LES)):
+            turbulence.nut = self.nut
+            if isinstance(turbulence, RANS) and turbulence.model is KOmega:
+                turbulence.k = np.zeros(n)
+                turbulence.omega = np.zeros(n)
 
 
 def initialise_(field: np.ndarray, value) -> None:
@@ -272,6 +291,7 @@ class BC:
     face_map: np.ndarray | None = None
     distance: np.ndarray | None = None
     partner: str | None = None
+    wall: tuple | None = None  # OmegaWallFunction: (kappa, beta1, cmu^0.25, yPlusLam)
 
 
 def Dirichlet(name, value):
@@ -296,6 +316,29 @@ def Extrapolated(name, value=0.0):
     """Extrapolated(name[, value]) (extrapolated.jl:12-20): zero gradient,
     semi-implicitly; the value is stored but not used, as in the reference."""
     return BC(_abi.BC_EXTRAPOLATED, name, value)
+
+
+def y_plus_laminar(E: float, kappa: float) -> float:
+    """y_plus_laminar (RANS_functions.jl:42-45)."""
+    yL = 11.0
+    for _ in range(10):
+        yL = math.log(max(yL * E, 1.0)) / kappa
+    return yL
+
+
+def OmegaWallFunction(name, kappa=0.41, beta1=0.075, cmu=0.09, B=5.2, E=9.8):
+    """OmegaWallFunction (Discretise_0_types.jl:83-113): the wall cell's
+    omega fixed to omega_log or omega_vis by y+ (constrain!)."""
+    return BC(_abi.BC_OMEGA_WALL, name, 0.0,
+              wall=(float(kappa), float(beta1), float(cmu) ** 0.25, y_plus_laminar(float(E), float(kappa))))
+
+
+def KWallFunction(name, **kw):
+    raise NotImplementedError("KWallFunction (wall-function production, RANS_functions.jl:66-117) is not implemented")
+
+
+def NutWallFunction(name, **kw):
+    raise NotImplementedError("NutWallFunction (wall eddy viscosity, RANS_functions.jl:119-172) is not implemented")
 
 
 def Empty(name):
@@ -452,6 +495,9 @@ def _bc_array(mesh: Mesh3, bcs, ncomp: int, keep: list):
             for c in range(3):
                 d.distance[c] = float(bc.distance[c])
             d.partner_patch = mesh.patch_index(bc.partner)
+        if bc.wall is not None:
+            for c in range(4):
+                d.wall[c] = float(bc.wall[c])
     return arr
 
 
@@ -530,12 +576,21 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     transient = isinstance(model.time, Transient)
     turb = model.turbulence
     les = isinstance(turb, LES)
+    kw = isinstance(turb, RANS) and turb.model is KOmega
     bnd = config.boundaries
     bU = _bc_array(mesh, bnd["U"], 3, keep)
     bP = _bc_array(mesh, bnd["p"], 1, keep)
-    nut_bcs = bnd.get("nut", []) if les else []
+    nut_bcs = bnd.get("nut", []) if (les or kw) else []
     bN = _bc_array(mesh, nut_bcs, 1, keep)
-    keep += [bU, bP, bN]
+    k_bcs = bnd.get("k", []) if kw else []
+    w_bcs = bnd.get("omega", []) if kw else []
+    bK = _bc_array(mesh, k_bcs, 1, keep)
+    bW = _bc_array(mesh, w_bcs, 1, keep)
+    keep += [bU, bP, bN, bK, bW]
+    sK = config.schemes.get("k", Schemes()) if kw else Schemes()
+    sW = config.schemes.get("omega", Schemes()) if kw else Schemes()
+    slv_k = _solver_desc(config.solvers["k"]) if kw else _abi.SolverSetupDesc()
+    slv_w = _solver_desc(config.solvers["omega"]) if kw else _abi.SolverSetupDesc()
     sU, sP = config.schemes["U"], config.schemes["p"]
     backend = config.hardware.backend
     prec = _abi.PREC_MIXED if getattr(backend, "precision", "fp64") == "mixed" else _abi.PREC_FP64
@@ -545,7 +600,7 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     dist, power = delta_scaling(mesh, next(iter(bnd.values()))) if les else (1.0, 1.0 / 3.0)
     cfg = _abi.ConfigDesc(
         algorithm=_abi.ALGO_PISO if transient else _abi.ALGO_SIMPLE,
-        turbulence=_abi.TURB_SMAGORINSKY if les else _abi.TURB_LAMINAR,
+        turbulence=_abi.TURB_SMAGORINSKY if les else (_abi.TURB_KOMEGA if kw else _abi.TURB_LAMINAR),
         nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if les else 0.0,
         les_delta_distance=dist, les_delta_power=power,
         U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)],
@@ -561,7 +616,15 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
         inner_rtol=float(getattr(backend, "inner_rtol", 1e-3)),
         n_bc_U=len(bnd["U"]), n_bc_p=len(bnd["p"]), n_bc_nut=len(nut_bcs),
         bc_U=C.cast(bU, C.POINTER(_abi.BCDesc)), bc_p=C.cast(bP, C.POINTER(_abi.BCDesc)),
-        bc_nut=C.cast(bN, C.POINTER(_abi.BCDesc)))
+        bc_nut=C.cast(bN, C.POINTER(_abi.BCDesc)),
+        kw_beta_star=float(getattr(turb, "beta_star", 0.09)), kw_alpha1=float(getattr(turb, "alpha1", 0.52)),
+        kw_beta1=float(getattr(turb, "beta1", 0.072)), kw_sigma_k=float(getattr(turb, "sigma_k", 0.5)),
+        kw_sigma_omega=float(getattr(turb, "sigma_omega", 0.5)),
+        k_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sK.time)], divergence=_SCHEME_DIV[_kind(sK.divergence)]),
+        omega_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sW.time)],
+                                       divergence=_SCHEME_DIV[_kind(sW.divergence)]),
+        k_solver=slv_k, omega_solver=slv_w, n_bc_k=len(k_bcs), n_bc_omega=len(w_bcs),
+        bc_k=C.cast(bK, C.POINTER(_abi.BCDesc)), bc_omega=C.cast(bW, C.POINTER(_abi.BCDesc)))
     return cfg, keep
 
 
@@ -571,6 +634,7 @@ class Case:
     def __init__(self, dmesh: DeviceMesh, cfg: _abi.ConfigDesc):
         self.dmesh, self.ctx = dmesh, dmesh.ctx
         self.mesh = dmesh.mesh
+        self.komega = cfg.turbulence == _abi.TURB_KOMEGA
         h = C.c_void_p()
         check(lib().xcal_case_create(self.ctx.h, dmesh.h, C.byref(cfg), C.byref(h)), self.ctx.h)
         self.h = h
@@ -731,12 +795,13 @@ class Case:
         face mass flux, face velocity and pressure, nu_eff, gradients, rD,
         H...): with ``restore`` a new case on the same mesh and configuration
         continues exactly as this one would."""
-        return {name: self.get_field(getattr(_abi, name)).copy() for name in CHECKPOINT_FIELDS}
+        names = CHECKPOINT_FIELDS + (KOMEGA_FIELDS if self.komega else ())
+        return {name: self.get_field(getattr(_abi, name)).copy() for name in names}
 
     def restore(self, state: dict) -> None:
         """Set the fields of a ``checkpoint`` and mark the state complete, so
         the next iteration does not redo the run's initial calculations."""
-        for name in CHECKPOINT_FIELDS:
+        for name in CHECKPOINT_FIELDS + (KOMEGA_FIELDS if self.komega else ()):
             if name in state:
                 self.set_field(getattr(_abi, name), state[name])
         self._chk(lib().xcal_case_mark_initialised(self.h))
@@ -862,6 +927,7 @@ class OpenFOAM:
 
 CHECKPOINT_FIELDS = ("FIELD_U", "FIELD_P", "FIELD_MDOTF", "FIELD_NUEFF", "FIELD_GRADP", "FIELD_GRADU", "FIELD_RD",
                      "FIELD_HV", "FIELD_DIVHV", "FIELD_NUT", "FIELD_NUTF", "FIELD_UF", "FIELD_PF", "FIELD_RDF")
+KOMEGA_FIELDS = ("FIELD_K", "FIELD_OMEGA")  # checkpointed for RANS{KOmega} cases
 
 
 def boundary_average(patch: str, field, fieldBCs, config=None, *, mesh: Mesh3, time: float = 0.0):
@@ -969,6 +1035,10 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
     try:
         case.set_field(_abi.FIELD_U, model.momentum.U)
         case.set_field(_abi.FIELD_P, model.momentum.p)
+        if hasattr(model.turbulence, "k"):
+            case.set_field(_abi.FIELD_K, model.turbulence.k)
+            case.set_field(_abi.FIELD_OMEGA, model.turbulence.omega)
+            case.set_field(_abi.FIELD_NUT, model.turbulence.nut)
         n = config.runtime.iterations
         step = wi if wi > 0 else n
         hist, done = [], 0
@@ -991,8 +1061,11 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
         res = np.concatenate(hist, axis=0) if hist else np.zeros((0, 4))
         model.momentum.U[:] = case.get_field(_abi.FIELD_U)
         model.momentum.p[:] = case.get_field(_abi.FIELD_P)
-        if isinstance(model.turbulence, LES):
+        if isinstance(model.turbulence, LES) or hasattr(model.turbulence, "k"):
             model.nut[:] = case.get_field(_abi.FIELD_NUT)
+        if hasattr(model.turbulence, "k"):
+            model.turbulence.k[:] = case.get_field(_abi.FIELD_K)
+            model.turbulence.omega[:] = case.get_field(_abi.FIELD_OMEGA)
     finally:
         if aw is not None:
             aw.close()

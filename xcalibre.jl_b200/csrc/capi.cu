@@ -198,7 +198,7 @@ int32_t xcal_case_get_field(const xcal_case* cs, int32_t field, double* host, in
 }
 
 int32_t xcal_case_set_bc_values(xcal_case* cs, int32_t eqn, int32_t bc_index, const double* values, int64_t count) {
-    if (!cs || !values) return XCAL_ERR_INVALID;
+    if (!cs || !values || (eqn != XCAL_EQN_U && eqn != XCAL_EQN_P)) return XCAL_ERR_INVALID;
     Case* c = cs->c.get();
     XCAL_GUARD(c->ctx, {
         BCTable& T = eqn == XCAL_EQN_U ? c->bcU : c->bcP;

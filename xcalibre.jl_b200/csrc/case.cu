@@ -530,7 +530,7 @@ static void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int
     for (int b = 0; b < nbc; ++b) {
         const xcal_bc& bc = bcs[b];
         if (bc.patch < 0 || bc.patch >= np) fail(XCAL_ERR_INVALID, "bc: patch index out of range");
-        if (bc.type < XCAL_BC_DIRICHLET || bc.type > XCAL_BC_PERIODIC_PARENT)
+        if (bc.type < XCAL_BC_DIRICHLET || bc.type > XCAL_BC_OMEGA_WALL)
             fail(XCAL_ERR_INVALID, "bc: unknown type");
         if (ncomp == 3 && bc.type == XCAL_BC_NEUMANN)
             fail(XCAL_ERR_UNSUPPORTED, "Neumann boundary condition for vector fields is not implemented");
@@ -652,6 +652,23 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     build_bc_table(bcU, *m, cfg.bc_U, cfg.n_bc_U, 3, &U, stream);
     build_bc_table(bcP, *m, cfg.bc_p, cfg.n_bc_p, 1, &P, stream);
     build_bc_table(bcNut, *m, cfg.bc_nut, cfg.n_bc_nut, 1, nullptr, stream);
+    for (const BCTable* T : {&bcU, &bcP, &bcNut})
+        for (const xcal_bc& bc : T->src)
+            if (bc.type == XCAL_BC_OMEGA_WALL) fail(XCAL_ERR_INVALID, "OmegaWallFunction applies to omega only");
+    if (cfg.turbulence == XCAL_TURB_KOMEGA) {
+        // RANS{KOmega} (RANS_kOmega.jl): k / omega share the p system
+        build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, nullptr, stream);
+        build_bc_table(bcOmega, *m, cfg.bc_omega, cfg.n_bc_omega, 1, nullptr, stream);
+        if (bcK.has_periodic || bcOmega.has_periodic || bcP.has_periodic || bcNut.has_periodic || bcU.has_periodic)
+            fail(XCAL_ERR_UNSUPPORTED, "k-omega: periodic boundaries are not implemented");
+        for (DBuf<double>* b : {&kfld, &omega, &Pk, &Pw, &Dk, &Dw, &kwtmp}) {
+            b->alloc(m->nC);
+            b->zero(stream);
+        }
+        build_wall_table(*m);
+    } else if (cfg.turbulence != XCAL_TURB_LAMINAR && cfg.turbulence != XCAL_TURB_SMAGORINSKY) {
+        fail(XCAL_ERR_INVALID, "unknown turbulence model");
+    }
     cfg.bc_U = cfg.bc_p = cfg.bc_nut = nullptr;  // not retained
     for (int d = 0; d < 3; ++d) {
         Uc[d].alloc(nC);
@@ -728,11 +745,11 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     cmax_ctr.zero(stream);
     gres.alloc(GRES_N);
     gres.zero(stream);
-    giters.alloc(2 * 4);
+    giters.alloc(2 * GRES_N);
     giters.zero(stream);
     dlaunch.alloc(1);
     dlaunch.zero(stream);
-    XCAL_CUDA(cudaMallocHost(&h_iters, 8 * sizeof(int)));
+    XCAL_CUDA(cudaMallocHost(&h_iters, 2 * GRES_N * sizeof(int)));
     XCAL_CUDA(cudaMallocHost(&h_launch, sizeof(unsigned long long)));
     XCAL_CUDA(cudaMallocHost(&h_perr, sizeof(int)));
     // host-side per-cell constants: V^(1/3) (Courant) and the LES filter
@@ -853,6 +870,10 @@ double* Case::field_comp(int field, int comp, long& count) {
         case XCAL_FIELD_PF: count = mesh->nF; return pf.p;
         case XCAL_FIELD_RDF: count = mesh->nF; return rDf.p;
         case XCAL_FIELD_DELTA: return Delta.p;
+        case XCAL_FIELD_K:
+        case XCAL_FIELD_OMEGA:
+            if (cfg.turbulence != XCAL_TURB_KOMEGA) fail(XCAL_ERR_INVALID, "k / omega fields need RANS{KOmega}");
+            return field == XCAL_FIELD_K ? kfld.p : omega.p;
         default: return nullptr;
     }
 }
@@ -865,14 +886,78 @@ void Case::initial_calculations() {  // Solvers_1_SIMPLE.jl:150-156
     double* Ufp[3] = {Uf[0].p, Uf[1].p, Uf[2].p};
     launch_interp_U(stream, mv(), bcU.view(), Ucp, Ufp, mdot.p);
     grad_p();
+    // update_nueff! (Solvers_0_functions.jl:5-35) from the nutf as it stands
     if (cfg.turbulence == XCAL_TURB_LAMINAR)
         launch_fill(stream, nueff.p, cfg.nu, mesh->nF);
     else
-        launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
+        launch_nueff(stream, mesh->nF, nutf.p, nueff.p, cfg.nu);
     initialised = true;
 }
 
+// The omega wall constraint's rows (constrain_equation!, RANS_functions.jl:
+// 376-429): BCs in order, each BC's faces in order, so a cell's row ends as
+// its last such face sets it; per wall cell that face's y = delta and the
+// BC's constants
+void Case::build_wall_table(const DevMesh& m) {
+    std::vector<int> win(m.nC, -1), wf, wb;
+    for (int b = 0; b < (int)bcOmega.src.size(); ++b) {
+        const xcal_bc& bc = bcOmega.src[b];
+        if (bc.type != XCAL_BC_OMEGA_WALL) continue;
+        const int start = m.patch_start[bc.patch], count = m.patch_count[bc.patch];
+        for (int f = start; f < start + count; ++f) {
+            win[m.bcell[f]] = (int)wf.size();
+            wf.push_back(f);
+            wb.push_back(b);
+        }
+    }
+    std::vector<int> cells;
+    std::vector<double> par;
+    for (int c = 0; c < m.nC; ++c) {
+        if (win[c] < 0) continue;
+        const int f = wf[win[c]];
+        const xcal_bc& bc = bcOmega.src[wb[win[c]]];
+        cells.push_back(c);
+        for (double v : {m.delta[f], bc.wall[0], bc.wall[1], bc.wall[2], bc.wall[3]}) par.push_back(v);
+    }
+    nwall = (int)cells.size();
+    if (nwall) {
+        wcell.upload(cells, stream);
+        wpar.upload(par, stream);
+    }
+}
+
+// turbulence!(::KOmegaModel) after grad!(gradU) (RANS_kOmega.jl:146-210):
+// production and dissipation coefficients, then the omega and k equations
+// (Time + Div - Lap(nu + sigma nutf) + Si == Source) on the p system, each
+// relaxed, solved and bounded (omega's wall rows constrained first), then
+// nut = k / omega, nutf with its BCs and nueff
+void Case::komega() {
+    const double* g[9];
+    for (int q = 0; q < 9; ++q) g[q] = gradU[q].p;
+    launch_kw_sources(stream, mesh->nC, g, nut.p, omega.p, Pk.p, Pw.p, Dk.p, Dw.p, cfg.kw_alpha1, cfg.kw_beta1,
+                      cfg.kw_beta_star);
+    for (int e : {(int)XCAL_EQN_OMEGA, (int)XCAL_EQN_K}) {
+        const bool w = e == XCAL_EQN_OMEGA;
+        double* phi = w ? omega.p : kfld.p;
+        const xcal_schemes& sc = w ? cfg.omega_schemes : cfg.k_schemes;
+        const double sigma = w ? cfg.kw_sigma_omega : cfg.kw_sigma_k;
+        launch_assemble_scalar(stream, mv(), P.view(), mdot.p, nutf.p, cfg.nu, sigma, phi, w ? Dw.p : Dk.p,
+                               w ? Pw.p : Pk.p, P.nz.p, P.b[0].p, sc.time, sc.divergence, cfg.dt);
+        launch_bc_relax_scalar(stream, mv(), P.view(), (w ? bcOmega : bcK).view(), P.nz.p, P.b[0].p, mdot.p, nutf.p,
+                               cfg.nu, sigma, phi, (w ? cfg.omega_solver : cfg.k_solver).relax);
+        if (w && nwall) launch_omega_constrain(stream, nwall, P.view(), wcell.p, wpar.p, kfld.p, cfg.nu, P.nz.p, P.b[0].p);
+        update_precond(e);
+        const double r = solve_system(e, 0, &last_iters[w ? 5 : 4]);
+        (w ? res_omega : res_k) = r;
+        XCAL_CUDA(cudaMemcpyAsync(kwtmp.p, phi, (size_t)mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        launch_bound(stream, mv(), kwtmp.p, phi);
+    }
+    launch_kw_nut(stream, mesh->nC, kfld.p, omega.p, nut.p);
+    launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
+}
+
 void Case::discretise(int eqn) {
+    if (eqn != XCAL_EQN_U && eqn != XCAL_EQN_P) fail(XCAL_ERR_INVALID, "discretise: equation must be U or p");
     if (eqn == XCAL_EQN_U) {
         const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
         const double* gp[3] = {gradp[0].p, gradp[1].p, gradp[2].p};
@@ -886,6 +971,7 @@ void Case::discretise(int eqn) {
 
 // update_equation! + apply_boundary_conditions! (+ relaxation for U, fused)
 void Case::apply_bcs(int eqn, int comp) {
+    if (eqn != XCAL_EQN_U && eqn != XCAL_EQN_P) fail(XCAL_ERR_INVALID, "apply_bcs: equation must be U or p");
     if (eqn == XCAL_EQN_U) {
         const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
         launch_bc_relax_U(stream, mv(), U.view(), bcU.view(), comp, cfg.U_schemes.divergence, U.nz.p, U.diag0.p,
@@ -912,8 +998,9 @@ void Case::set_reference() {
 }
 
 void Case::update_precond(int eqn) {
-    Equation& E = eqn == XCAL_EQN_U ? U : P;
-    int pt = eqn == XCAL_EQN_U ? cfg.U_solver.precond : cfg.p_solver.precond;
+    const SolveRef R = solve_ref(eqn, 0);
+    Equation& E = *R.E;
+    const int pt = R.SS.precond;
     if (pt == XCAL_PRECOND_JACOBI) {
         kr_jacobi_update(stream, E.view(), E.nz.p, E.P.p);
     } else if (pt == XCAL_PRECOND_DILU) {
@@ -1231,14 +1318,14 @@ void Case::capture_while(F&& body) {
 // into gres and (iterations, status) into giters.  Mixed precision nests the
 // inner loop in a WHILE node over defect-correction steps.
 void Case::solve_captured(int eqn, int comp) {
-    const bool isU = eqn == XCAL_EQN_U;
-    Equation& E = isU ? U : P;
-    const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
-    double* field = isU ? Uc[comp].p : p.p;
-    const double* b = isU ? U.b[comp].p : P.b[0].p;
-    KScalars* S = ws.S.p + (isU ? 0 : 1);
+    const SolveRef R = solve_ref(eqn, comp);
+    Equation& E = *R.E;
+    const xcal_solver_setup& SS = R.SS;
+    double* field = R.field;
+    const double* b = R.b;
+    KScalars* S = ws.S.p + R.kslot;
     const int n = E.n;
-    const int slot = isU ? comp : 3;
+    const int slot = R.slot;
     CSRView A = E.view();
     const int itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
     // iterations per loop body: a finished solve wastes at most BODY-1
@@ -1316,12 +1403,30 @@ void Case::solve_captured(int eqn, int comp) {
 // apply_smoother!(setup.smoother, values, A, b) (Solve_1_api.jl:284): the
 // Jacobi smoother on the field, before the Krylov solve of (eqn, comp)
 void Case::smooth(int eqn, int comp) {
-    const bool isU = eqn == XCAL_EQN_U;
-    const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
-    if (SS.smoother_loops <= 0) return;
-    Equation& E = isU ? U : P;
-    kr_jacobi_smooth(stream, E.view(), E.nz.p, isU ? U.b[comp].p : P.b[0].p, isU ? Uc[comp].p : p.p, ws.t.p,
-                     SS.smoother_loops, SS.smoother_omega);
+    const SolveRef R = solve_ref(eqn, comp);
+    if (R.SS.smoother_loops <= 0) return;
+    kr_jacobi_smooth(stream, R.E->view(), R.E->nz.p, R.b, R.field, ws.t.p, R.SS.smoother_loops, R.SS.smoother_omega);
+}
+
+Case::SolveRef Case::solve_ref(int eqn, int comp) {
+    switch (eqn) {
+        case XCAL_EQN_U:
+            return {&U, cfg.U_solver, Uc[comp].p, U.b[comp].p, GRES_U + comp, 0, comp};
+        case XCAL_EQN_P:
+            return {&P, cfg.p_solver, p.p, P.b[0].p, GRES_P, 1, 3};
+        case XCAL_EQN_K:
+        case XCAL_EQN_OMEGA: {
+            if (cfg.turbulence != XCAL_TURB_KOMEGA) fail(XCAL_ERR_INVALID, "k / omega equations need RANS{KOmega}");
+            const bool w = eqn == XCAL_EQN_OMEGA;
+            SolveRef r{&P, w ? cfg.omega_solver : cfg.k_solver, w ? omega.p : kfld.p, P.b[0].p,
+                       w ? (int)GRES_OMEGA : (int)GRES_K, 1, w ? 5 : 4};
+            r.SS.precond = cfg.k_solver.precond;
+            return r;
+        }
+        default:
+            fail(XCAL_ERR_INVALID, "unknown equation");
+    }
+    return {};
 }
 
 // solve_system! (Solve_1_api.jl:268-307)
@@ -1331,13 +1436,13 @@ double Case::solve_system(int eqn, int comp, int* iters) {
         solve_captured(eqn, comp);
         return 0.0;
     }
-    bool isU = eqn == XCAL_EQN_U;
-    Equation& E = isU ? U : P;
-    const xcal_solver_setup& SS = isU ? cfg.U_solver : cfg.p_solver;
-    double* field = isU ? Uc[comp].p : p.p;
-    const double* b = isU ? U.b[comp].p : P.b[0].p;
-    KScalars* S = ws.S.p + (isU ? 0 : 1);
-    KScalars* hS = h_S + (isU ? 0 : 1);
+    const SolveRef R = solve_ref(eqn, comp);
+    Equation& E = *R.E;
+    const xcal_solver_setup& SS = R.SS;
+    double* field = R.field;
+    const double* b = R.b;
+    KScalars* S = ws.S.p + R.kslot;
+    KScalars* hS = h_S + R.kslot;
     int n = E.n;
     CSRView A = E.view();
     const double* nz = E.nz.p;
@@ -1345,7 +1450,7 @@ double Case::solve_system(int eqn, int comp, int* iters) {
     hS->atol = SS.atol;
     hS->rtol = SS.rtol;
     hS->itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
-    const int gk = isU ? comp : 3;
+    const int gk = R.gk;
     if (cfg.precision == XCAL_PREC_MIXED) {
         solve_mixed(E, SS, field, b, S, hS, gk, iters);
     } else {
@@ -1598,7 +1703,9 @@ void Case::turbulence() {
             launch_limit_cell(stream, mv(), limD.p, Uc[a].p, g + 3 * a, cfg.U_schemes.limiter_level);
         if (les) launch_smag_nut(stream, mesh->nC, g, Delta.p, nut.p);
     }
-    if (les)
+    if (cfg.turbulence == XCAL_TURB_KOMEGA)
+        komega();
+    else if (les)
         launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
     else
         launch_fill(stream, nueff.p, cfg.nu, mesh->nF);
@@ -1709,7 +1816,7 @@ void Case::run_step_graph(double res[4], double* courant) {
     XCAL_CUDA(cudaGraphLaunch(step_graph, stream));
     XCAL_CUDA(cudaEventRecord(ev[1], stream));
     XCAL_CUDA(cudaMemcpyAsync(h_res, gres.p, GRES_N * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    XCAL_CUDA(cudaMemcpyAsync(h_iters, giters.p, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    XCAL_CUDA(cudaMemcpyAsync(h_iters, giters.p, 2 * GRES_N * sizeof(int), cudaMemcpyDeviceToHost, stream));
     XCAL_CUDA(cudaMemcpyAsync(h_launch, dlaunch.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
     XCAL_CUDA(cudaMemsetAsync(dlaunch.p, 0, sizeof(unsigned long long), stream));
     XCAL_CUDA(cudaMemcpyAsync(h_perr, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));

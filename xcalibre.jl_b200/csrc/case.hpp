@@ -113,7 +113,7 @@ struct Case {
     size_t bytes = 0;  // device bytes held (excluding the mesh)
     cudaStream_t stream = nullptr;
     bool own_stream = true;
-    BCTable bcU, bcP, bcNut;
+    BCTable bcU, bcP, bcNut, bcK, bcOmega;
     Equation U, P;
     KrylovWS ws;
     // fields
@@ -122,10 +122,17 @@ struct Case {
     DBuf<double> limD;     // CellBased limiter: fc - cc per cell_faces entry (3 x 2 nI)
     DBuf<double> Uc[3], p, mdot, nueff, gradp[3], gradU[9], rD, Hv[3], divHv, nut, nutf, Uf[3], pf, rDf, Delta, prev,
         courant, dx13, resbuf, cmax, io;  // io: staging of one field component in the original order
+    // RANS{KOmega}: k, omega, production / dissipation per cell, a scratch
+    // copy for bound!, and the omega wall cells (storage ids) with, per cell,
+    // y = delta of its constraining face, kappa, beta1, cmu^0.25, yPlusLam
+    DBuf<double> kfld, omega, Pk, Pw, Dk, Dw, kwtmp, wpar;
+    DBuf<int> wcell;
+    int nwall = 0;
+    double res_k = 0.0, res_omega = 0.0;
     bool initialised = false;
     int iteration = 0;
     double time = 0.0;
-    int last_iters[4] = {0, 0, 0, 0};
+    int last_iters[6] = {0, 0, 0, 0, 0, 0};  // Ux, Uy, Uz, p, k, omega
     // timing
     double ms[6] = {0, 0, 0, 0, 0, 0};
     long long launches = 0;
@@ -150,8 +157,8 @@ struct Case {
         cudaGraphExec_t exec = nullptr;
         long long launches = 0;  // kernels per replay
     };
-    ChunkGraph chunk_graph[4][2];  // [Ux, Uy, Uz, p][plain, profiled]
-    cudaEvent_t gev[4][12] = {};   // event nodes of the profiled graphs
+    ChunkGraph chunk_graph[6][2];  // [Ux, Uy, Uz, p, k, omega][plain, profiled]
+    cudaEvent_t gev[6][12] = {};   // event nodes of the profiled graphs
     template <class F>
     void replay_chunk(ChunkGraph& g, F&& body);
 
@@ -176,6 +183,20 @@ struct Case {
     void build_midpoint(const DevMesh& m, cudaStream_t s);
     void build_limiter(const DevMesh& m, cudaStream_t s);
     void smooth(int eqn, int comp);
+    // one linear solve: its system, setup, field, right-hand side, graph-mode
+    // result slot, device-scalars slot and per-system index (k and omega use
+    // the p system's storage, as the reference's equations share it, and
+    // k's preconditioner type, RANS_kOmega.jl:77-85)
+    struct SolveRef {
+        Equation* E;
+        xcal_solver_setup SS;
+        double* field;
+        const double* b;
+        int slot, kslot, gk;
+    };
+    SolveRef solve_ref(int eqn, int comp);
+    void build_wall_table(const DevMesh& m);
+    void komega();
     void nonorth_correct();
     void nonorth_correctors(double& rp);
     void explicit_relaxation_p(double a);
@@ -200,7 +221,7 @@ struct Case {
                         const KrylovVecs<T>& V, KScalars* S, KScalars* hS, int gk);
     void solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, const double* b, KScalars* S,
                      KScalars* hS, int gk, int* iters);
-    int last_outer[4] = {0, 0, 0, 0};  // mixed: defect-correction steps of the last solve per system
+    int last_outer[6] = {0, 0, 0, 0, 0, 0};  // mixed: defect-correction steps of the last solve per system
     bool tuned = false;
     void autotune();  // launch-shape autotuner (autotune.cu), once per case
 
@@ -208,7 +229,7 @@ struct Case {
     // graph; the Krylov (and defect-correction) loops are conditional WHILE
     // nodes driven by device-side stopping tests, so a step needs no host
     // round trip until its residuals are read.
-    enum { GRES_U = 0, GRES_P = 3, GRES_CO = 4, GRES_N = 8 };
+    enum { GRES_U = 0, GRES_P = 3, GRES_CO = 4, GRES_K = 5, GRES_OMEGA = 6, GRES_N = 8 };
     DBuf<double> gres;          // per-step results: U x,y,z and p residuals, max Courant
     DBuf<int> giters;           // (iterations, status) of the step's 4 solves
     DBuf<unsigned int> cmax_ctr;

@@ -41,6 +41,21 @@ void launch_mid_correct_vector(cudaStream_t s, const MeshView& m, const double* 
 // U with its row of grad U (D: Case::build_limiter)
 void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const double* F, double* const g[3],
                        double level);
+// RANS{KOmega}: sources, k / omega assembly, BCs + relaxation, the omega
+// wall rows, bound!, nut = k / omega; nueff = nu + nutf
+void launch_kw_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* omega,
+                       double* Pk, double* Pw, double* Dk, double* Dw, double alpha1, double beta1, double beta_star);
+void launch_assemble_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const double* mdot,
+                            const double* nutf, double nu, double sigma, const double* phi, const double* D,
+                            const double* P, double* nz, double* b, int time_scheme, int div_scheme, double dt);
+void launch_bc_relax_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz,
+                            double* b, const double* mdot, const double* nutf, double nu, double sigma,
+                            const double* phi, double alpha);
+void launch_omega_constrain(cudaStream_t s, int nw, const CSRView& A, const int* wcell, const double* par,
+                            const double* k, double nu, double* nz, double* b);
+void launch_bound(cudaStream_t s, const MeshView& m, const double* old, double* v);
+void launch_kw_nut(cudaStream_t s, int nC, const double* k, const double* omega, double* nut);
+void launch_nueff(cudaStream_t s, int nF, const double* nutf, double* nueff, double nu);
 // Smagorinsky nut = Delta |S| from a stored grad U
 void launch_smag_nut(cudaStream_t s, int nC, const double* const g[9], const double* Delta, double* nut);
 // non-orthogonal correction of the pressure right-hand side (t: Case::build_nonorth)

@@ -346,6 +346,244 @@ __global__ void k_bc_relax_U(MeshView m, CSRView A, BCView bc, int comp, int div
     b[i] = bi + (Dmax - D0) * U[i];
 }
 
+// ---------------------------------------------------------------------------
+// RANS{KOmega} (RANS_kOmega.jl): the k and omega equations
+//   Time + Divergence(mdot, phi) - Laplacian(mueff, phi) + Si(D, phi) == Source(P)
+// with mueff = nu + sigma nutf (rho = 1), on the p system's storage
+// ---------------------------------------------------------------------------
+// production / dissipation (RANS_kOmega.jl:170-178): magnitude2!(S, 2)
+// (RANS_tensor_algebra.jl:81-99, S = 0.5 (G + G'), rows outer) into
+// Pw = alpha1 |S|^2, Pk = nut |S|^2; Dw = beta1 omega, Dk = beta+ omega
+__global__ void k_kw_sources(int nC, const double* __restrict__ g0, const double* __restrict__ g1,
+                             const double* __restrict__ g2, const double* __restrict__ g3,
+                             const double* __restrict__ g4, const double* __restrict__ g5,
+                             const double* __restrict__ g6, const double* __restrict__ g7,
+                             const double* __restrict__ g8, const double* __restrict__ nut,
+                             const double* __restrict__ omega, double* Pk, double* Pw, double* Dk, double* Dw,
+                             double alpha1, double beta1, double beta_star) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nC) return;
+    const double G[9] = {g0[i], g1[i], g2[i], g3[i], g4[i], g5[i], g6[i], g7[i], g8[i]};
+    double sum = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double s = 0.5 * (G[3 * j + q] + G[3 * q + j]);
+            sum = sum + s * s;
+        }
+    const double mag = sum * 2.0;
+    Pw[i] = alpha1 * mag;
+    Pk[i] = nut[i] * mag;
+    const double w = omega[i];
+    Dw[i] = beta1 * w;
+    Dk[i] = beta_star * w;
+}
+
+// _discretise_scalar_model! (Discretise_2_generated_distretisation.jl:125-167)
+// of the k / omega equation: terms Time, Divergence, Laplacian, Si in order
+__global__ void k_assemble_scalar(MeshView m, CSRView A, const double* __restrict__ mdot,
+                                  const double* __restrict__ nutf, double nu, double sigma,
+                                  const double* __restrict__ phi, const double* __restrict__ D,
+                                  const double* __restrict__ P, double* nz, double* b, int time_scheme,
+                                  int div_scheme, double dt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    double ac_sum = 0.0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        int f = m.cf_face[k];
+        int ns = m.cf_sign[k];
+        double dns = (double)ns;
+        double AC = 0.0, AN = 0.0;
+        AC = AC + 0.0;  // Time
+        AN = AN + 0.0;
+        double ap = 1.0 * (mdot[f] * dns);  // Divergence (Discretise_1_schemes.jl:114-180)
+        double ac, an;
+        if (div_scheme == XCAL_DIV_LINEAR) {
+            double w = m.weight[f];
+            w = 0.5 + dns * (w - 0.5);
+            ac = ap * w;
+            an = ap * (1.0 - w);
+        } else if (div_scheme == XCAL_DIV_UPWIND) {
+            ac = jl_max(ap, 0.0);
+            an = -jl_max(-ap, 0.0);
+        } else {
+            double w = m.weight[f];
+            if (ns < 0) w = 1.0 - w;
+            double acL = ap * w, anL = ap * (1.0 - w);
+            double acU = jl_max(ap, 0.0), anU = -jl_max(-ap, 0.0);
+            ac = 0.75 * acL + 0.25 * acU;
+            an = 0.75 * anL + 0.25 * anU;
+        }
+        AC = AC + ac;
+        AN = AN + an;
+        const double muf = nu + sigma * nutf[f];
+        double apl = (-1.0 * (muf * m.Efmag[f])) / m.delta[f];  // Laplacian, sign -1
+        AC = AC + (-apl);
+        AN = AN + apl;
+        AC = AC + 0.0;  // Si (:204-210)
+        AN = AN + 0.0;
+        ac_sum = ac_sum + AC;
+        nz[A.cf_slot[k]] = AN;
+    }
+    const double V = m.vol[i];
+    double acs = 0.0, bs = 0.0;
+    if (time_scheme == XCAL_TIME_EULER) {
+        double vol_rdt = (1.0 * V) / dt;  // Discretise_1_schemes.jl:36-45
+        acs = acs + vol_rdt;
+        bs = bs + phi[i] * vol_rdt;
+    } else {
+        acs = acs + 0.0;
+        bs = bs + 0.0;
+    }
+    acs = acs + 0.0;  // Divergence, Laplacian
+    bs = bs + 0.0;
+    acs = acs + 0.0;
+    bs = bs + 0.0;
+    acs = acs + (1.0 * D[i]) * V;  // Si (:211-218)
+    bs = bs + 0.0;
+    nz[A.diag[i]] = ac_sum + acs;
+    const double b2 = 0.0 + (1.0 * P[i]) * V;  // +Source(P)
+    b[i] = b2 + bs;
+}
+
+// one boundary face of the k / omega equation (Time, Divergence, Laplacian,
+// Si; Discretise_3_boundary_conditions.jl, boundary_conditions/*.jl):
+// OmegaWallFunction contributes as Extrapolated (its wall rows are then
+// constrained)
+__device__ void bc_scalar_transport(const MeshView& m, const BCView& bc, int f, int cell, const double* mdot,
+                                    double muf, const double* phi, double& AP, double& BP) {
+    double ap_d = 0.0, bp_d = 0.0, ap_l = 0.0, bp_l = 0.0;
+    switch (bc.type[f]) {
+        case XCAL_BC_DIRICHLET:
+        case XCAL_BC_DIRICHLET_FUNCTION: {  // dirichlet.jl:19-31
+            const double val = bc_val(bc, f, 0);
+            bp_d = (1.0 * (-mdot[f])) * val;
+            double fl = (muf * m.area[f]) / m.delta[f];
+            double al = -1.0 * (-fl);
+            ap_l = al;
+            bp_l = al * val;
+            break;
+        }
+        case XCAL_BC_WALL:  // wall.jl:43-102 (scalar)
+        case XCAL_BC_ZEROGRADIENT:
+        case XCAL_BC_SYMMETRY:
+            ap_d = 1.0 * mdot[f];
+            break;
+        case XCAL_BC_EXTRAPOLATED:  // extrapolated.jl:21-45
+        case XCAL_BC_OMEGA_WALL: {
+            ap_d = 1.0 * mdot[f];
+            double fl = ((-muf) * m.area[f]) / m.delta[f];
+            double al = -1.0 * fl;
+            ap_l = al;
+            bp_l = al * phi[cell];
+            break;
+        }
+        case XCAL_BC_NEUMANN: {  // neumann.jl (scalar)
+            const double val = bc_val(bc, f, 0);
+            double a = 1.0 * mdot[f];
+            ap_d = a;
+            bp_d = ((-val) * a) * m.delta[f];
+            bp_l = (muf * m.area[f]) * val;
+            break;
+        }
+        default:  // Empty
+            break;
+    }
+    double ap = 0.0, bp = 0.0;
+    ap = ap + 0.0;  // Time
+    bp = bp + 0.0;
+    ap = ap + ap_d;
+    bp = bp + bp_d;
+    ap = ap + ap_l;
+    bp = bp + bp_l;
+    ap = ap + 0.0;  // Si
+    bp = bp + 0.0;
+    AP = ap;
+    BP = bp;
+}
+
+// apply_boundary_conditions! (ascending face id per cell) then
+// implicit_relaxation_diagdom! (Solve_1_api.jl:388-411) of the k / omega
+// equation, one thread per row
+__global__ void k_bc_relax_scalar(MeshView m, CSRView A, BCView bc, double* nz, double* b,
+                                  const double* __restrict__ mdot, const double* __restrict__ nutf, double nu,
+                                  double sigma, const double* __restrict__ phi, double alpha) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    const int ds = A.diag[i];
+    double d = nz[ds];
+    double bi = b[i];
+    for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
+        const int f = m.bf_face[k];
+        double AP, BP;
+        bc_scalar_transport(m, bc, f, i, mdot, nu + sigma * nutf[f], phi, AP, BP);
+        d = d + AP;
+        bi = bi + BP;
+    }
+    double sumv = 0.0;
+    const int rb = row_base(A, i), rl = A.len[i];
+    for (int k = 0; k < rl; ++k) {
+        int e = rb + SELL_C * k;
+        sumv = sumv + fabs(e == ds ? d : nz[e]);
+    }
+    sumv = sumv - fabs(d);
+    const double D0 = d;
+    const double Dmax = jl_max(fabs(D0), sumv) / alpha;
+    nz[ds] = Dmax;
+    b[i] = bi + (Dmax - D0) * phi[i];
+}
+
+// constrain!(omega_eqn, OmegaWallFunction) (RANS_functions.jl:380-429) per
+// wall cell: the row becomes omega = omega_log (y+ > yPlusLam) or omega_vis
+// (:46-52) from the current k; par: y, kappa, beta1, cmu^0.25, yPlusLam
+__global__ void k_omega_constrain(int nw, CSRView A, const int* __restrict__ wcell, const double* __restrict__ par,
+                                  const double* __restrict__ k, double nu, double* nz, double* b) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nw) return;
+    const int c = wcell[t];
+    const double y = par[5 * t], kappa = par[5 * t + 1], beta1 = par[5 * t + 2], c25 = par[5 * t + 3],
+                 yPlusLam = par[5 * t + 4];
+    const double sk = sqrt(k[c]);
+    const double w_vis = (6.0 * nu) / (beta1 * (y * y));
+    const double w_log = sk / ((c25 * kappa) * y);
+    const double yplus = ((c25 * y) * sk) / nu;
+    const double wc = yplus > yPlusLam ? w_log : w_vis;
+    const int rb = row_base(A, c), rl = A.len[c];
+    for (int q = 0; q < rl; ++q) nz[rb + SELL_C * q] = 0.0;
+    nz[A.diag[c]] = 1.0;
+    b[c] = wc;
+}
+
+// bound! (RANS_functions.jl:2-41) from a copy of the values before the call
+__global__ void k_bound(MeshView m, const double* __restrict__ old, double* v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    const double mzero = jl_eps(1.0);
+    double sum_flux = 0.0;
+    int sum_area = 0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        sum_flux = sum_flux + jl_max(old[m.cf_nb[k]], mzero);
+        sum_area += 1;
+    }
+    const double average = sum_flux / (double)sum_area;
+    const double vi = old[i];
+    const double s = signbit(vi) ? average : copysign(0.0, average);
+    v[i] = jl_max(jl_max(vi, s), mzero);
+}
+
+// nut = k / omega (RANS_kOmega.jl:201)
+__global__ void k_kw_nut(int nC, const double* __restrict__ k, const double* __restrict__ omega, double* nut) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nC) nut[i] = k[i] / omega[i];
+}
+
+// update_nueff_turbulent! (Solvers_0_functions.jl:30-35)
+__global__ void k_nueff(int nF, const double* __restrict__ nutf, double* nueff, double nu) {
+    int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < nF) nueff[f] = nu + nutf[f];
+}
+
 // boundary conditions of the p equation (cells owning boundary faces)
 __global__ void k_bc_p(MeshView m, CSRView A, BCView bc, double* nz, double* b, const double* __restrict__ rDf,
                        const double* __restrict__ p) {
@@ -486,6 +724,7 @@ __global__ void k_interp_scalar(MeshView m, BCView bc, const double* __restrict_
             case XCAL_BC_WALL:
             case XCAL_BC_ZEROGRADIENT:
             case XCAL_BC_EXTRAPOLATED:
+            case XCAL_BC_OMEGA_WALL:
             case XCAL_BC_SYMMETRY:
                 v = phi[o];
                 break;
@@ -1020,6 +1259,43 @@ void launch_mid_correct_vector(cudaStream_t s, const MeshView& m, const double* 
 void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const double* F, double* const g[3],
                        double level) {
     k_limit_cell<<<nblk(m.nC), TPB, 0, s>>>(m, D, F, g[0], g[1], g[2], level);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_kw_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* omega,
+                       double* Pk, double* Pw, double* Dk, double* Dw, double alpha1, double beta1, double beta_star) {
+    k_kw_sources<<<nblk(nC), TPB, 0, s>>>(nC, g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8], nut, omega, Pk, Pw,
+                                          Dk, Dw, alpha1, beta1, beta_star);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_assemble_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const double* mdot,
+                            const double* nutf, double nu, double sigma, const double* phi, const double* D,
+                            const double* P, double* nz, double* b, int time_scheme, int div_scheme, double dt) {
+    k_assemble_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, mdot, nutf, nu, sigma, phi, D, P, nz, b, time_scheme,
+                                                 div_scheme, dt);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_bc_relax_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz,
+                            double* b, const double* mdot, const double* nutf, double nu, double sigma,
+                            const double* phi, double alpha) {
+    k_bc_relax_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, bc, nz, b, mdot, nutf, nu, sigma, phi, alpha);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_omega_constrain(cudaStream_t s, int nw, const CSRView& A, const int* wcell, const double* par,
+                            const double* k, double nu, double* nz, double* b) {
+    if (nw <= 0) return;
+    k_omega_constrain<<<nblk(nw), TPB, 0, s>>>(nw, A, wcell, par, k, nu, nz, b);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_bound(cudaStream_t s, const MeshView& m, const double* old, double* v) {
+    k_bound<<<nblk(m.nC), TPB, 0, s>>>(m, old, v);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_kw_nut(cudaStream_t s, int nC, const double* k, const double* omega, double* nut) {
+    k_kw_nut<<<nblk(nC), TPB, 0, s>>>(nC, k, omega, nut);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_nueff(cudaStream_t s, int nF, const double* nutf, double* nueff, double nu) {
+    k_nueff<<<nblk(nF), TPB, 0, s>>>(nF, nutf, nueff, nu);
     XCAL_CHECK_LAUNCH();
 }
 void launch_smag_nut(cudaStream_t s, int nC, const double* const g[9], const double* Delta, double* nut) {
