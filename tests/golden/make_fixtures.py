@@ -19,6 +19,9 @@ Fixtures:
   bfs_5mm_unv.npz         -- examples/0_GRIDS/backwardFacingStep_5mm.unv (the mesh of
                              test/0_TEST_CASES/2d_incompressible_transient_KOmega_BFS_lowRe.jl),
                              parsed the same way.
+  cavity_hex_unv3.npz     -- test/grids/OF_cavity_hex/cavity_hex.unv (hex cells; counts pinned by
+                             test/test_mesh_conversion.jl:43-61), 3D parse below.
+  streamtube_unv3.npz     -- examples/0_GRIDS/3d_streamtube_1.0x0.1x0.1_0.08mm.unv (tetrahedra).
 
 Usage: python tests/golden/make_fixtures.py [/path/to/XCALibre.jl]
 """
@@ -155,6 +158,64 @@ def read_unv_raw(path: str) -> dict:
                 group_elements=np.array([e for g in gelems for e in g], dtype=np.int32))
 
 
+def read_unv3_raw(path: str) -> dict:
+    """Datasets 2411 (3-field point lines), 2412 (edges skipped; faces 41/44
+    and cells 111/112/115 with their node lines) and 2467 (group name lines,
+    then entity lines whose element labels, less the edge count, are face
+    positions) of a 3D .unv file; labels stay 1-based."""
+    pts, fcount, fverts, ccount, cverts, gnames, gelems = [], [], [], [], [], [], []
+    n_edge = 0
+    lines = [ln.strip() for ln in open(path)]
+    i, ds = 0, ""
+    while i < len(lines):
+        ln = lines[i]
+        i += 1
+        if not ln:
+            continue
+        if ln == "-1":
+            if ds == "":
+                ds = lines[i]
+                i += 1
+                ds = "" if ds == "-1" else ds
+            else:
+                ds = ""
+            continue
+        t = ln.split()
+        if ds == "2411" and len(t) == 3:
+            pts.append([float(v.replace("D", "e")) for v in t])
+        elif ds == "2412" and len(t) == 6:
+            etype, nn = int(t[1]), int(t[5])
+            if nn == 2 or etype == 11:
+                n_edge += 1
+                i += 1
+            elif etype in (41, 44):
+                fv = [int(v) for v in lines[i].split()]
+                i += 1
+                fcount.append(len(fv))
+                fverts.extend(fv)
+            elif etype in (111, 112, 115):
+                cv = []
+                while len(cv) < nn:
+                    cv.extend(int(v) for v in lines[i].split())
+                    i += 1
+                ccount.append(len(cv))
+                cverts.extend(cv)
+        elif ds == "2467":
+            if len(t) == 1 and not t[0].lstrip("-").isdigit():
+                gnames.append(t[0])
+                gelems.append([])
+            elif gelems and len(t) in (4, 8) and t[1] != "0":
+                gelems[-1].append(int(t[1]) - n_edge)
+                if len(t) == 8:
+                    gelems[-1].append(int(t[5]) - n_edge)
+    goff = np.zeros(len(gelems) + 1, dtype=np.int64)
+    goff[1:] = np.cumsum([len(g) for g in gelems])
+    return dict(points=np.array(pts), face_count=np.array(fcount, dtype=np.int32),
+                face_vertices=np.array(fverts, dtype=np.int32), cell_count=np.array(ccount, dtype=np.int32),
+                cell_vertices=np.array(cverts, dtype=np.int32), group_names=np.array(gnames),
+                group_offsets=goff, group_faces=np.array([e for g in gelems for e in g], dtype=np.int32))
+
+
 def main(ref: str) -> None:
     pm = read_polymesh(os.path.join(ref, "test/grids/OF_cavity_hex/polyMesh"))
     np.savez_compressed(os.path.join(HERE, "cavity_hex_polymesh.npz"), **pm)
@@ -164,6 +225,10 @@ def main(ref: str) -> None:
         json.dump(laplace_expected(os.path.join(ref, "test/unit_test_laplace.jl")), f, indent=1)
     with open(os.path.join(HERE, "smoother_5x5.json"), "w") as f:
         json.dump(smoother_system(os.path.join(ref, "test/test_smoothers.jl")), f, indent=1)
+    np.savez_compressed(os.path.join(HERE, "cavity_hex_unv3.npz"),
+                        **read_unv3_raw(os.path.join(ref, "test/grids/OF_cavity_hex/cavity_hex.unv")))
+    np.savez_compressed(os.path.join(HERE, "streamtube_unv3.npz"),
+                        **read_unv3_raw(os.path.join(ref, "examples/0_GRIDS/3d_streamtube_1.0x0.1x0.1_0.08mm.unv")))
     for mm in (10, 5):
         np.savez_compressed(os.path.join(HERE, "bfs_%dmm_unv.npz" % mm),
                             **read_unv_raw(os.path.join(ref, "examples/0_GRIDS/backwardFacingStep_%dmm.unv" % mm)))

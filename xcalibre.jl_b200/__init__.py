@@ -15,7 +15,7 @@ from .api import (B200Backend, Bicgstab, Case, CellBased, Cg, Configuration, Con
                   KOmega, OmegaWallFunction, KWallFunction, NutWallFunction)
 from .foam import Mesh3, build_mesh3
 from .foamio import FOAM3D_mesh, read_polymesh, write_polymesh
-from .unv import UNV2D_mesh
+from .unv import UNV2D_mesh, UNV3D_mesh
 from .meshgen import PolyMesh, box_polymesh, cavity_polymesh, channel_polymesh, periodic_box_polymesh
 
 __all__ = [n for n in dir() if not n.startswith("_")] + ["_abi"]

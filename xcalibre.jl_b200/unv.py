@@ -302,3 +302,240 @@ def unv2_mesh(points, elements, groups, scale: float = 1.0, source: str = "mesh"
                  cell_faces_offset=off, cell_faces=cat(c_faces), cell_nsign=cat(nsign), cell_neighbours=cat(c_neigh),
                  boundary_cellsID=bcell, patch_names=[g[0] for g in groups], patch_start=patch_start,
                  patch_count=patch_count, points=points, dim=2)
+
+
+# ---------------------------------------------------------------------------
+# 3D meshes: UNV3D_mesh (src/UNV3)
+# ---------------------------------------------------------------------------
+def _unv_float(s: str) -> float:
+    """_parse_unv_float (UNV3_1_reader.jl:150-156): Fortran 'D' exponents."""
+    return float(s.replace("D", "e").replace("d", "e"))
+
+
+def read_unv3(path: str, scale: float = 1.0):
+    """read_UNV3 (UNV3_1_reader.jl:12-148): (points [n, 3] scaled, faces
+    [vertex lists, 0-based], cells [vertex lists, 0-based], groups [(name,
+    [face positions, 1-based])]).  After each "-1" the next line names the
+    dataset; 2411 points are its 3-field lines; 2412 elements are 6-field
+    headers (edges: type 11 or 2 nodes, one line skipped; faces: 41 with 3
+    or 44 with 4 nodes; cells: 111, 112, 115, nodes over as many lines as
+    needed), numbered edges, then faces, then cells; 2467 groups are a name
+    line then 8- or 4-field entity lines whose element labels (fields 2 and
+    6) less the edge count are face positions."""
+    points, faces, cells, groups = [], [], [], []
+    n_edge = 0
+    with open(path, "r") as f:
+        lines = iter(f)
+        ds = ""
+        for line in lines:
+            line = line.strip()
+            if not line:
+                continue
+            if line == "-1":
+                if ds == "":
+                    ds = next(lines).strip()
+                    if ds == "-1":
+                        ds = ""
+                else:
+                    ds = ""
+                continue
+            t = line.split()
+            if ds == "2411":
+                if len(t) == 3:
+                    points.append((_unv_float(t[0]) * scale, _unv_float(t[1]) * scale, _unv_float(t[2]) * scale))
+            elif ds == "2412":
+                if len(t) != 6:
+                    continue
+                eid, etype, nn = int(t[0]), int(t[1]), int(t[5])
+                if nn == 2 or etype == 11:
+                    n_edge += 1
+                    next(lines)
+                elif (etype == 41 and nn == 3) or (etype == 44 and nn == 4):
+                    if eid - n_edge != len(faces) + 1:
+                        raise ValueError(f"{path}: face index in UNV file are not in order at UNV index {eid}")
+                    faces.append([int(v) - 1 for v in next(lines).split()])
+                elif etype in (111, 115, 112):
+                    if eid - len(faces) - n_edge != len(cells) + 1:
+                        raise ValueError(f"{path}: cell index in UNV file are not in order at UNV index {eid}")
+                    nodes = []
+                    while len(nodes) < nn:
+                        nodes.extend(int(v) - 1 for v in next(lines).split())
+                    cells.append(nodes)
+            elif ds == "2467":
+                if len(t) == 1 and _try_int(t[0]) is None:
+                    groups.append((t[0], []))
+                elif groups:
+                    if len(t) == 8 and int(t[1]) != 0:
+                        groups[-1][1].extend((int(t[1]) - n_edge, int(t[5]) - n_edge))
+                    elif len(t) == 4 and int(t[1]) != 0:
+                        groups[-1][1].append(int(t[1]) - n_edge)
+    return np.array(points, dtype=np.float64).reshape(-1, 3), faces, cells, groups
+
+
+_TET = ((0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3))
+_HEX = ((0, 1, 2, 3), (4, 5, 6, 7), (0, 1, 5, 4), (1, 2, 6, 5), (2, 3, 7, 6), (3, 0, 4, 7))
+_PRI3 = ((0, 1, 2), (3, 4, 5))
+_PRI4 = ((0, 1, 4, 3), (1, 2, 5, 4), (2, 0, 3, 5))
+
+
+def _cross(a, b):
+    return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+
+def UNV3D_mesh(path: str, scale: float = 1.0) -> Mesh3:
+    """UNV3D_mesh(meshFile; scale) (UNV3_2_builder.jl:14-30)."""
+    return unv3_mesh(*read_unv3(path, scale), source=path)
+
+
+def unv3_mesh(points, faces, cells, groups, source: str = "mesh") -> Mesh3:
+    """_build_UNV3D_mesh_core (UNV3_2_builder.jl:32-64): boundary faces in
+    group order, each owned by the first cell (of its first node's cells)
+    holding all its nodes; internal faces from each cell's element faces
+    (tet, hex, prism maps; a face keyed by its sorted nodes, boundary keys
+    skipped), owner the first cell to list it and neighbour the second;
+    then calculate_centres! (node means), calculate_face_properties! (a
+    triangle fan about the face's node mean: area vector, fan-weighted
+    centroid, normal = area vector / (area + 1e-16), oriented out of the
+    owner, weight/delta/e from the node-mean cell centres) and
+    calculate_area_and_volume! (pyramids on each face from the node-mean
+    centre: volume sum and volume-weighted centroid)."""
+    pts = [tuple(p) for p in np.asarray(points, dtype=np.float64).tolist()]
+    nC = len(cells)
+    node_cells = [[] for _ in pts]
+    for c, vs in enumerate(cells):
+        for v in vs:
+            node_cells[v].append(c)
+    b_nodes, b_cell, bkeys = [], [], {}
+    for name, fl in groups:
+        for fi in fl:
+            nodes = faces[fi - 1]
+            owner = -1
+            for c in node_cells[nodes[0]]:
+                if all(n in cells[c] for n in nodes):
+                    owner = c
+                    break
+            if owner < 0:
+                raise ValueError(f"{source}: boundary face {fi} has no cell")
+            bkeys[tuple(sorted(nodes))] = len(b_nodes)
+            b_nodes.append(list(nodes))
+            b_cell.append(owner)
+    nB = len(b_nodes)
+    i_nodes, i_own, ikeys = [], [], {}
+    for c, vs in enumerate(cells):
+        nc = len(vs)
+        maps = _TET if nc == 4 else (_PRI3 + _PRI4 if nc == 6 else (_HEX if nc == 8 else ()))
+        for mp in maps:
+            fn = [vs[q] for q in mp]
+            key = tuple(sorted(fn))
+            if key in bkeys:
+                continue
+            k = ikeys.get(key)
+            if k is not None:
+                i_own[k][1] = c
+            else:
+                ikeys[key] = len(i_nodes)
+                i_nodes.append(fn)
+                i_own.append([c, -1])
+    if any(o[1] < 0 for o in i_own):
+        raise ValueError(f"{source}: an internal face has one cell")
+    fnodes = b_nodes + i_nodes
+    owner = b_cell + [o[0] for o in i_own]
+    neigh = b_cell + [o[1] for o in i_own]
+    nF = len(fnodes)
+    c_faces = [[] for _ in range(nC)]
+    c_sign = [[] for _ in range(nC)]
+    c_nb = [[] for _ in range(nC)]
+    for f in range(nB, nF):
+        o, n = owner[f], neigh[f]
+        c_faces[o].append(f)
+        c_sign[o].append(1)
+        c_nb[o].append(n)
+        c_faces[n].append(f)
+        c_sign[n].append(-1)
+        c_nb[n].append(o)
+    cc = [_mean(pts, vs) for vs in cells]  # calculate_centres!
+    fc0 = [_mean(pts, fn) for fn in fnodes]
+    fc = [None] * nF
+    normal = [None] * nF
+    area = [0.0] * nF
+    e_vec = [None] * nF
+    delta = [0.0] * nF
+    weight = [0.0] * nF
+    for f in range(nF):  # calculate_face_properties!
+        fn = fnodes[f]
+        L = len(fn)
+        C1 = cc[owner[f]]
+        E = fc0[f]
+        ax = ay = az = 0.0
+        tx = ty = tz = 0.0
+        sa = 0.0
+        for j in range(L):
+            p1, p2 = pts[fn[j]], pts[fn[(j + 1) % L]]
+            cr = _cross(_sub(p1, E), _sub(p2, E))
+            a = (0.5 * cr[0], 0.5 * cr[1], 0.5 * cr[2])
+            am = _norm(a)
+            ax, ay, az = ax + a[0], ay + a[1], az + a[2]
+            sa = sa + am
+            m3 = ((E[0] + p1[0]) + p2[0], (E[1] + p1[1]) + p2[1], (E[2] + p1[2]) + p2[2])
+            tx, ty, tz = tx + am * (m3[0] / 3.0), ty + am * (m3[1] / 3.0), tz + am * (m3[2] / 3.0)
+        av = (ax, ay, az)
+        A = _norm(av)
+        n = _div(av, A + 1e-16)
+        F = _div((tx, ty, tz), sa + 1e-16)
+        check = _sub(F, C1) if f < nB else _sub(cc[neigh[f]], C1)
+        if _dot(check, n) < 0.0:
+            n = _neg(n)
+            fnodes[f] = fn[::-1] if L > 1 else fn
+        if f < nB:
+            weight[f], delta[f], e_vec[f] = _wde_boundary(_sub(F, C1), n)
+        else:
+            C2 = cc[neigh[f]]
+            weight[f], delta[f], e_vec[f] = _wde_internal(_sub(F, C1), _sub(F, C2), _sub(C2, C1), n)
+        fc[f], normal[f], area[f] = F, n, A
+    # calculate_area_and_volume!: per cell its boundary faces, then its
+    # internal faces, each in face order
+    per = [[] for _ in range(nC)]
+    for f in range(nB):
+        per[b_cell[f]].append(f)
+    for f in range(nB, nF):
+        per[owner[f]].append(f)
+        per[neigh[f]].append(f)
+    centre = [None] * nC
+    volume = [0.0] * nC
+    third = 1.0 / 3.0
+    for c in range(nC):
+        apex = cc[c]
+        vt = 0.0
+        qx = qy = qz = 0.0
+        for f in per[c]:
+            h = _sub(fc[f], apex)
+            S = (normal[f][0] * area[f], normal[f][1] * area[f], normal[f][2] * area[f])
+            if _dot(h, S) < 0.0:
+                S = _neg(S)
+            vp = third * _dot(h, S)
+            Cp = (0.75 * fc[f][0] + 0.25 * apex[0], 0.75 * fc[f][1] + 0.25 * apex[1], 0.75 * fc[f][2] + 0.25 * apex[2])
+            vt = vt + vp
+            qx, qy, qz = qx + vp * Cp[0], qy + vp * Cp[1], qz + vp * Cp[2]
+        volume[c] = abs(vt)
+        centre[c] = _div((qx, qy, qz), vt) if vt > 1e-16 else apex
+    patch_count, patch_start, s = [], [], 0
+    for _, fl in groups:
+        patch_start.append(s)
+        patch_count.append(len(fl))
+        s += len(fl)
+    off = np.zeros(nC + 1, dtype=np.int32)
+    off[1:] = np.cumsum([len(v) for v in c_faces])
+
+    def cat(lists):
+        return np.array([v for lst in lists for v in lst], dtype=np.int32)
+
+    return Mesh3(n_cells=nC, n_faces=nF, n_bfaces=nB,
+                 face_owner=np.array(owner, dtype=np.int32), face_neigh=np.array(neigh, dtype=np.int32),
+                 face_centre=np.array(fc, dtype=np.float64), face_normal=np.array(normal, dtype=np.float64),
+                 face_e=np.array(e_vec, dtype=np.float64), face_area=np.array(area, dtype=np.float64),
+                 face_delta=np.array(delta, dtype=np.float64), face_weight=np.array(weight, dtype=np.float64),
+                 cell_centre=np.array(centre, dtype=np.float64), cell_volume=np.array(volume, dtype=np.float64),
+                 cell_faces_offset=off, cell_faces=cat(c_faces), cell_nsign=cat(c_sign), cell_neighbours=cat(c_nb),
+                 boundary_cellsID=np.array(b_cell, dtype=np.int32), patch_names=[g[0] for g in groups],
+                 patch_start=np.array(patch_start, dtype=np.int32), patch_count=np.array(patch_count, dtype=np.int32),
+                 points=np.asarray(points, dtype=np.float64), dim=3)
