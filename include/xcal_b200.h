@@ -66,13 +66,13 @@ enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
 /* preconditioner: src/Solve/Preconditioners/preconditioners_0_types.jl */
 enum { XCAL_PRECOND_NONE = 0, XCAL_PRECOND_JACOBI = 1, XCAL_PRECOND_DILU = 2 };
 /* turbulence: RANS{Laminar} / LES{Smagorinsky} / RANS{KOmega} */
-enum { XCAL_TURB_LAMINAR = 0, XCAL_TURB_SMAGORINSKY = 1, XCAL_TURB_KOMEGA = 2 };
+enum { XCAL_TURB_LAMINAR = 0, XCAL_TURB_SMAGORINSKY = 1, XCAL_TURB_KOMEGA = 2, XCAL_TURB_KOMEGA_SST = 3 };
 /* arithmetic of the Krylov inner iterations */
 enum { XCAL_PREC_FP64 = 0, XCAL_PREC_MIXED = 1 };
 /* pressure-velocity algorithm: run! dispatch, src/Solvers/Solvers_3_solver_dispatch.jl:120,225 */
 enum { XCAL_ALGO_SIMPLE = 0, XCAL_ALGO_PISO = 1 };
 /* equations (k, omega: RANS{KOmega} transport equations) */
-enum { XCAL_EQN_U = 0, XCAL_EQN_P = 1, XCAL_EQN_K = 2, XCAL_EQN_OMEGA = 3 };
+enum { XCAL_EQN_U = 0, XCAL_EQN_P = 1, XCAL_EQN_K = 2, XCAL_EQN_OMEGA = 3, XCAL_EQN_WALLDIST = 4 };
 
 /* field identifiers for xcal_case_get_field / xcal_case_set_field.
  * Cell fields hold n_cells values per component, face fields n_faces; vector
@@ -96,7 +96,8 @@ enum {
     XCAL_FIELD_DELTA = 14, /* LES filter (C*Delta)^2 (n_cells)              */
     XCAL_FIELD_K = 15,     /* RANS{KOmega} k (n_cells)                      */
     XCAL_FIELD_OMEGA = 16, /* RANS{KOmega} omega (n_cells)                  */
-    XCAL_FIELD_COUNT = 17
+    XCAL_FIELD_WALLDIST = 17, /* RANS{KOmegaSST} wall distance y (n_cells)  */
+    XCAL_FIELD_COUNT = 18
 };
 
 /* ---- mesh: the Mesh3 contract (src/Mesh/Mesh_0_types.jl:28-205) ---------
@@ -227,6 +228,17 @@ typedef struct {
     int32_t n_bc_k, n_bc_omega;
     const xcal_bc* bc_k;
     const xcal_bc* bc_omega;
+    /* RANS{KOmegaSST} (RANS_kOmegaSST.jl:57-79): beta+, alpha1, beta1,
+     * sigma_k1, sigma_omega1 in kw_*, and beta2, sigma_k2, sigma_omega2
+     * here; grad k uses k_schemes.gradient, grad omega p_schemes.gradient
+     * (:146-147); the wall distance (wall_distance!,
+     * Calculate_4_wall_distance.jl:4-78): its solver, gradient scheme and
+     * BCs (Dirichlet 0 on the walls, Empty, Extrapolated elsewhere) */
+    double sst_beta2, sst_sigma_k2, sst_sigma_omega2;
+    xcal_schemes y_schemes;
+    xcal_solver_setup y_solver;
+    int32_t n_bc_y;
+    const xcal_bc* bc_y;
 } xcal_config;
 
 /* ---- polyMesh input of the mesh importer --------------------------------

@@ -96,6 +96,7 @@ static std::vector<double>* field_ptr(Case* C, int field, int& ncomp, int& per) 
         case XCAL_FIELD_DELTA: return &C->Delta;
         case XCAL_FIELD_K: return &C->k;
         case XCAL_FIELD_OMEGA: return &C->omega;
+        case XCAL_FIELD_WALLDIST: return &C->yw;
         default: return nullptr;
     }
 }

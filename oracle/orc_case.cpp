@@ -100,6 +100,8 @@ static void copy_bcs(const Mesh& m, const xcal_bc* src, int n, std::vector<BC>& 
     }
 }
 
+static void wall_distance(Case& C);
+
 Case* case_create(const Mesh* m, const xcal_config* cfg) {
     Case* C = new Case();
     C->m = m;
@@ -111,11 +113,12 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     copy_bcs(*m, cfg->bc_p, cfg->n_bc_p, C->bcP, 1);
     copy_bcs(*m, cfg->bc_nut, cfg->n_bc_nut, C->bcNut, 1);
     C->cfg.bc_U = C->cfg.bc_p = C->cfg.bc_nut = nullptr;
-    if (cfg->turbulence == XCAL_TURB_KOMEGA) {
+    if (cfg->turbulence == XCAL_TURB_KOMEGA || cfg->turbulence == XCAL_TURB_KOMEGA_SST) {
         copy_bcs(*m, cfg->bc_k, cfg->n_bc_k, C->bcK, 1);
         copy_bcs(*m, cfg->bc_omega, cfg->n_bc_omega, C->bcOmega, 1);
     }
-    C->cfg.bc_k = C->cfg.bc_omega = nullptr;
+    if (cfg->turbulence == XCAL_TURB_KOMEGA_SST) copy_bcs(*m, cfg->bc_y, cfg->n_bc_y, C->bcY, 1);
+    C->cfg.bc_k = C->cfg.bc_omega = C->cfg.bc_y = nullptr;
     int nC = C->nC, nF = C->nF;
     for (int d = 0; d < 3; ++d) {
         C->U[d].assign(nC, 0.0);
@@ -138,6 +141,15 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     for (std::vector<double>* v : {&C->k, &C->omega, &C->Pk, &C->Pw, &C->Dk, &C->Dw, &C->Pkw}) v->assign(nC, 0.0);
     C->mueffk.assign(nF, 0.0);
     C->mueffw.assign(nF, 0.0);
+    if (cfg->turbulence == XCAL_TURB_KOMEGA_SST) {
+        for (std::vector<double>* v : {&C->yw, &C->F1, &C->F2, &C->Om, &C->D2, &C->Pww}) v->assign(nC, 0.0);
+        for (int d = 0; d < 3; ++d) {
+            C->gk[d].assign(nC, 0.0);
+            C->gw[d].assign(nC, 0.0);
+        }
+        C->kfs.assign(nF, 0.0);
+        C->wfs.assign(nF, 0.0);
+    }
     C->prev.assign(nC, 0.0);
     C->cellsCourant.assign(nC, 0.0);
     C->bp.assign(nC, 0.0);
@@ -182,6 +194,7 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
             C->Delta[i] = dc * dc;
         }
     }
+    if (cfg->turbulence == XCAL_TURB_KOMEGA_SST) wall_distance(*C);
     return C;
 }
 
@@ -1358,15 +1371,16 @@ static void bound_field(const Mesh& m, std::vector<double>& v) {
 }
 
 // solve_system! of k or omega on the shared scalar system
-static double solve_scalar(Case& C, const xcal_solver_setup& SS0, int ptype, std::vector<double>& field) {
+static double solve_scalar(Case& C, const xcal_solver_setup& SS0, int ptype, std::vector<double>& field,
+                           std::vector<double>& P) {
     xcal_solver_setup SS = SS0;
     SS.precond = ptype;
     CSR& A = C.Ap;
     if (SS.smoother_loops > 0) jacobi_smooth(A, C.bp.data(), field.data(), SS.smoother_loops, SS.smoother_omega);
     if (SS.solver == XCAL_SOLVER_CG)
-        krylov_cg(A, C.bp, field, SS.precond, C.Pkw, SS, C.kp);
+        krylov_cg(A, C.bp, field, SS.precond, P, SS, C.kp);
     else
-        krylov_bicgstab(A, C.bp, field, SS.precond, C.Pkw, SS, C.kp);
+        krylov_bicgstab(A, C.bp, field, SS.precond, P, SS, C.kp);
     return residual(A, C.bp, field);
 }
 
@@ -1403,7 +1417,7 @@ static void komega(Case& C) {
     relax_scalar(C.Ap, C.bp, C.omega, cf.omega_solver.relax);
     constrain_omega(C, C.Ap, C.bp);
     update_precond(C.Ap, ptype, C.Pkw);
-    C.res_omega = solve_scalar(C, cf.omega_solver, ptype, C.omega);
+    C.res_omega = solve_scalar(C, cf.omega_solver, ptype, C.omega, C.Pkw);
     bound_field(m, C.omega);
     // k: Time + Div(mdotf) - Lap(mueffk) + Si(Dk) == Source(Pk)
     std::vector<Term> tk = {{T_TIME, 1.0, nullptr, cf.k_schemes.time},
@@ -1414,15 +1428,138 @@ static void komega(Case& C) {
     apply_bcs_scalar(C, tk, C.Ap, C.bp, C.bcK, C.k);
     relax_scalar(C.Ap, C.bp, C.k, cf.k_solver.relax);
     update_precond(C.Ap, ptype, C.Pkw);
-    C.res_k = solve_scalar(C, cf.k_solver, ptype, C.k);
+    C.res_k = solve_scalar(C, cf.k_solver, ptype, C.k, C.Pkw);
     bound_field(m, C.k);
     for (int i = 0; i < C.nC; ++i) C.nut[i] = C.k[i] / C.omega[i];
     interpolate(m, C.nut, C.nutf);
     correct_boundaries(C, C.bcNut, &C.nutf, &C.nut, false);
 }
 
+// grad! of a scalar with its BCs, Gauss or Midpoint (Calculate_0_gradient.jl)
+static void scalar_grad(Case& C, const std::vector<double>& phi, std::vector<double>& phif, const std::vector<BC>& bcs,
+                        int scheme, std::vector<double>* g) {
+    const Mesh& m = *C.m;
+    interpolate(m, phi, phif);
+    correct_boundaries(C, bcs, &phif, &phi, false);
+    green_gauss(m, phif, g);
+    if (scheme != XCAL_GRAD_MIDPOINT) return;
+    for (int f = C.nB; f < C.nF; ++f) phif[f] = 0.5 * (phi[m.owner[f]] + phi[m.neigh[f]]);
+    green_gauss(m, phif, g);
+    for (int it = 0; it < 2; ++it) {
+        for (int f = C.nB; f < C.nF; ++f) {
+            const int c1 = m.owner[f], c2 = m.neigh[f];
+            const V3 g1 = {g[0][c1], g[1][c1], g[2][c1]};
+            const V3 g2 = {g[0][c2], g[1][c2], g[2][c2]};
+            phif[f] = 0.5 * (phi[c1] + phi[c2]) + dot(0.5 * (g1 + g2), mid_R(m, f));
+        }
+        green_gauss(m, phif, g);
+    }
+}
+
+// wall_distance! (Calculate_4_wall_distance.jl:4-78): -Laplacian(1, phi) ==
+// Source(1) with the wall BCs, solved (y_solver) and explicitly relaxed up to
+// 1000 times until its residual is below the convergence, then
+// y = -|grad phi| + sqrt(|grad phi|^2 + 2 phi) (:80-92)
+static void wall_distance(Case& C) {
+    const Mesh& m = *C.m;
+    const xcal_solver_setup& SS = C.cfg.y_solver;
+    std::vector<double> phi(C.nC, 0.0), prev(C.nC), ones_f(C.nF, 1.0), ones_c(C.nC, 1.0), phif(C.nF), g[3];
+    for (int d = 0; d < 3; ++d) g[d].assign(C.nC, 0.0);
+    std::vector<Term> terms = {{T_LAP, -1.0, &ones_f, 0}};
+    scalar_grad(C, phi, phif, C.bcY, C.cfg.y_schemes.gradient, g);
+    for (int it = 0; it < 1000; ++it) {
+        prev = phi;
+        discretise_scalar(C, terms, C.Ap, C.bp, phi, ones_c);
+        apply_bcs_scalar(C, terms, C.Ap, C.bp, C.bcY, phi);
+        update_precond(C.Ap, SS.precond, C.Pkw);
+        const double res = solve_scalar(C, SS, SS.precond, phi, C.Pkw);
+        for (int i = 0; i < C.nC; ++i) phi[i] = prev[i] + SS.relax * (phi[i] - prev[i]);
+        if (res < SS.convergence) break;
+    }
+    scalar_grad(C, phi, phif, C.bcY, C.cfg.y_schemes.gradient, g);
+    for (int i = 0; i < C.nC; ++i) {
+        const double gm = std::sqrt(g[0][i] * g[0][i] + g[1][i] * g[1][i] + g[2][i] * g[2][i]);
+        C.yw[i] = (-gm) + std::sqrt(gm * gm + 2.0 * phi[i]);
+    }
+}
+
+// turbulence!(::KOmegaSSTModel) after grad!(gradU) (RANS_kOmegaSST.jl:190-315)
+static void komega_sst(Case& C) {
+    const Mesh& m = *C.m;
+    const xcal_config& cf = C.cfg;
+    const double bs = cf.kw_beta_star, al1 = cf.kw_alpha1, b1 = cf.kw_beta1, b2 = cf.sst_beta2;
+    const double sk1 = cf.kw_sigma_k, sk2 = cf.sst_sigma_k2, sw1 = cf.kw_sigma_omega, sw2 = cf.sst_sigma_omega2;
+    const double nu = cf.nu, eps = jl_eps(1.0);
+    scalar_grad(C, C.omega, C.wfs, C.bcOmega, cf.p_schemes.gradient, C.gw);  // Grad{schemes.p.gradient}(omega)
+    scalar_grad(C, C.k, C.kfs, C.bcK, cf.k_schemes.gradient, C.gk);
+    for (int i = 0; i < C.nC; ++i) {
+        double sum = 0.0;  // magnitude2!(Pk, S, 2)
+        for (int j = 0; j < 3; ++j)
+            for (int q = 0; q < 3; ++q) {
+                const double s = 0.5 * (C.gradU[3 * j + q][i] + C.gradU[3 * q + j][i]);
+                sum = sum + s * s;
+            }
+        const double mag = sum * 2.0;
+        C.Om[i] = std::sqrt(mag);  // Omega = sqrt(Pk)
+        const double w = C.omega[i], kk = C.k[i], y = C.yw[i];
+        const double dkdw = (C.gk[0][i] * C.gw[0][i] + C.gk[1][i] * C.gw[1][i]) + C.gk[2][i] * C.gw[2][i];
+        const double CD = jl_max(((2.0 * sw2) * dkdw) / w, 1e-10);
+        const double sq = std::sqrt(jl_max(kk, eps));
+        const double a1 = jl_min(jl_min(jl_max(sq / ((bs * w) * y), (500.0 * nu) / (w * (y * y))),
+                                        ((4.0 * sw2) * kk) / (CD * (y * y))),
+                                 10.0);
+        const double a2 = jl_min(jl_max((2.0 * sq) / ((bs * w) * y), (500.0 * nu) / ((y * y) * w)), 100.0);
+        const double f2 = det_tanh_pos(a2 * a2);
+        const double f1 = det_tanh_pos((a1 * a1) * (a1 * a1));
+        C.F1[i] = f1;
+        C.F2[i] = f2;
+        const double beta = b1 * f1 + (1.0 - f1) * b2;
+        const double gamma = (5.0 / 9.0) * f1 + (1.0 - f1) * 0.44;
+        C.Dw[i] = beta * w;
+        C.Dk[i] = bs * w;
+        C.Pw[i] = gamma * jl_min(mag, (((10.0 / al1) * bs) * w) * jl_max(al1 * w, f2 * C.Om[i]));
+        C.Pk[i] = jl_min(mag * C.nut[i], ((10.0 * bs) * kk) * w);
+        C.D2[i] = ((((2.0 * (f1 - 1.0)) * sw2) * dkdw) / w) / w;
+    }
+    for (int f = 0; f < C.nF; ++f) {  // interpolate!(F1f, F1); sigma blending; mueff
+        const double wt = m.fweight[f];
+        const double F1f = wt * C.F1[m.owner[f]] + (1.0 - wt) * C.F1[m.neigh[f]];
+        const double sk = sk1 * F1f + (1.0 - F1f) * sk2;
+        const double sw = sw1 * F1f + (1.0 - F1f) * sw2;
+        C.mueffw[f] = nu + sw * C.nutf[f];
+        C.mueffk[f] = nu + sk * C.nutf[f];
+    }
+    // omega: Time + Div - Lap(mueffw) + Si(Dw) + Si(D2) == Source(Pw), its own preconditioner
+    std::vector<Term> tw = {{T_TIME, 1.0, nullptr, cf.omega_schemes.time},
+                            {T_DIV, 1.0, &C.mdotf, cf.omega_schemes.divergence},
+                            {T_LAP, -1.0, &C.mueffw, 0},
+                            {T_SI, 1.0, &C.Dw, 0},
+                            {T_SI, 1.0, &C.D2, 0}};
+    discretise_scalar(C, tw, C.Ap, C.bp, C.omega, C.Pw);
+    apply_bcs_scalar(C, tw, C.Ap, C.bp, C.bcOmega, C.omega);
+    relax_scalar(C.Ap, C.bp, C.omega, cf.omega_solver.relax);
+    constrain_omega(C, C.Ap, C.bp);
+    update_precond(C.Ap, cf.omega_solver.precond, C.Pww);
+    C.res_omega = solve_scalar(C, cf.omega_solver, cf.omega_solver.precond, C.omega, C.Pww);
+    bound_field(m, C.omega);
+    std::vector<Term> tk = {{T_TIME, 1.0, nullptr, cf.k_schemes.time},
+                            {T_DIV, 1.0, &C.mdotf, cf.k_schemes.divergence},
+                            {T_LAP, -1.0, &C.mueffk, 0},
+                            {T_SI, 1.0, &C.Dk, 0}};
+    discretise_scalar(C, tk, C.Ap, C.bp, C.k, C.Pk);
+    apply_bcs_scalar(C, tk, C.Ap, C.bp, C.bcK, C.k);
+    relax_scalar(C.Ap, C.bp, C.k, cf.k_solver.relax);
+    update_precond(C.Ap, cf.k_solver.precond, C.Pkw);
+    C.res_k = solve_scalar(C, cf.k_solver, cf.k_solver.precond, C.k, C.Pkw);
+    bound_field(m, C.k);
+    for (int i = 0; i < C.nC; ++i) C.nut[i] = (al1 * C.k[i]) / jl_max(al1 * C.omega[i], C.F2[i] * C.Om[i]);
+    interpolate(m, C.nut, C.nutf);
+    correct_boundaries(C, C.bcNut, &C.nutf, &C.nut, false);
+}
+
 void turbulence(Case& C) {
     grad_U(C);  // RANS_laminar.jl:73-79, LES_Smagorinsky.jl:117, RANS_kOmega.jl:167-168
+    if (C.cfg.turbulence == XCAL_TURB_KOMEGA_SST) komega_sst(C);
     if (C.cfg.turbulence == XCAL_TURB_KOMEGA) komega(C);
     if (C.cfg.turbulence == XCAL_TURB_SMAGORINSKY) {
         // LES_Smagorinsky.jl:122-131

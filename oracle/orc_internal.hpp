@@ -64,7 +64,7 @@ struct Krylov {
 struct Case {
     const Mesh* m = nullptr;
     xcal_config cfg{};
-    std::vector<BC> bcU, bcP, bcNut, bcK, bcOmega;
+    std::vector<BC> bcU, bcP, bcNut, bcK, bcOmega, bcY;
     int nC = 0, nF = 0, nB = 0;
 
     // fields
@@ -80,6 +80,10 @@ struct Case {
     // the k/omega preconditioner (shared, RANS_kOmega.jl:84-85), residuals
     std::vector<double> k, omega, Pk, Pw, Dk, Dw, mueffk, mueffw, Pkw;
     double res_k = 0.0, res_omega = 0.0;
+    // RANS{KOmegaSST}: wall distance, blending, |S|, the second omega Si
+    // coefficient, grad k / grad omega, their face values, omega's own
+    // preconditioner
+    std::vector<double> yw, F1, F2, Om, D2, gk[3], gw[3], kfs, wfs, Pww;
     std::vector<int> rorder;  // morton_order of the cell centres
     double time = 0.0;
     bool initialised = false;

@@ -145,3 +145,33 @@ def test_komega_restart_bit_identical(x, ctx):
     assert np.array_equal(np.concatenate([rb, rc]), ra)
     for f in KW_FIELDS:
         assert np.array_equal(c.get_field(getattr(x._abi, f)), a.get_field(getattr(x._abi, f))), f
+
+
+@pytest.mark.parametrize("precond", ["Jacobi", "DILU"])
+def test_sst_channel_parity(x, orc, ctx, precond):
+    from test_komega import sst_channel_case
+    mesh = skewed_channel(x, n=(12, 8, 7), seed=13)
+    model, config = sst_channel_case(x, mesh, 6, precond)
+    cfg, keep = x.build_config(model, config)
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, False)
+    assert rel(g.get_field(x._abi.FIELD_WALLDIST), o.get_field(x._abi.FIELD_WALLDIST)) <= TOL
+    rg, _ = g.simple_iterate(6)
+    ro, _ = o.simple_iterate(6)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    _check(x, g, o)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_sst_bfs_transient_parity(x, orc, ctx, graph):
+    """PISO with k-omega SST on the 2D backward-facing step (walls: wall, top)."""
+    from test_komega import sst_channel_case
+    mesh = bfs_mesh(x, 10)
+    model, config = sst_channel_case(x, mesh, 5, transient=True, walls=("wall", "top"))
+    config.schemes["p"].gradient = x.api.Midpoint
+    config.schemes["k"].gradient = x.api.Midpoint
+    cfg, keep = x.build_config(model, config)
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, graph)
+    rg, _ = g.piso_step(5)
+    ro, _ = o.piso_step(5)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    _check(x, g, o, KW_FIELDS + ("FIELD_WALLDIST", "FIELD_NUTF"))

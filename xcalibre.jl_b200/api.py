@@ -109,6 +109,11 @@ class KOmega:
     nut = k / omega."""
 
 
+class KOmegaSST:
+    """RANS{KOmegaSST} (RANS_kOmegaSST.jl): k-omega with F1/F2 blending from
+    the wall distance, cross-diffusion and a limited nut."""
+
+
 class Incompressible: ...
 
 
@@ -221,14 +226,36 @@ class Fluid:
 
 @dataclass
 class RANS:
-    """RANS{Laminar} or RANS{KOmega}(; beta+, alpha1, beta1, sigma_k,
-    sigma_omega) (RANS_kOmega.jl:29-33)."""
+    """RANS{Laminar}, RANS{KOmega}(; beta+, alpha1, beta1, sigma_k,
+    sigma_omega) (RANS_kOmega.jl:29-33) or RANS{KOmegaSST}(; beta+, alpha1,
+    sigma_k1, sigma_k2, sigma_omega1, sigma_omega2, beta1, beta2, kappa,
+    walls) (RANS_kOmegaSST.jl:57-61); unset coefficients take the model's
+    defaults."""
     model: type = Laminar
-    beta_star: float = 0.09
-    alpha1: float = 0.52
-    beta1: float = 0.072
-    sigma_k: float = 0.5
-    sigma_omega: float = 0.5
+    beta_star: float | None = None
+    alpha1: float | None = None
+    beta1: float | None = None
+    sigma_k: float | None = None
+    sigma_omega: float | None = None
+    beta2: float | None = None
+    sigma_k1: float | None = None
+    sigma_k2: float | None = None
+    sigma_omega1: float | None = None
+    sigma_omega2: float | None = None
+    kappa: float | None = None
+    walls: list | None = None
+
+    def coeffs(self) -> dict:
+        if self.model is KOmegaSST:
+            d = dict(beta_star=0.09, alpha1=0.31, sigma_k1=0.85, sigma_k2=1.0, sigma_omega1=0.5, sigma_omega2=0.856,
+                     beta1=0.075, beta2=0.0828, kappa=0.41)
+        else:
+            d = dict(beta_star=0.09, alpha1=0.52, beta1=0.072, sigma_k=0.5, sigma_omega=0.5)
+        for k in list(d):
+            v = getattr(self, k, None)
+            if v is not None:
+                d[k] = float(v)
+        return d
 
 
 @dataclass
@@ -261,9 +288,11 @@ class Physics:
         # model.turbulence.k / .omega / .nut, as the reference's fields
         if isinstance(turbulence, (RANS, LES)):
             turbulence.nut = self.nut
-            if isinstance(turbulence, RANS) and turbulence.model is KOmega:
+            if isinstance(turbulence, RANS) and turbulence.model in (KOmega, KOmegaSST):
                 turbulence.k = np.zeros(n)
                 turbulence.omega = np.zeros(n)
+            if isinstance(turbulence, RANS) and turbulence.model is KOmegaSST:
+                turbulence.y = np.zeros(n)
 
 
 def initialise_(field: np.ndarray, value) -> None:
@@ -576,7 +605,8 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     transient = isinstance(model.time, Transient)
     turb = model.turbulence
     les = isinstance(turb, LES)
-    kw = isinstance(turb, RANS) and turb.model is KOmega
+    sst = isinstance(turb, RANS) and turb.model is KOmegaSST
+    kw = isinstance(turb, RANS) and turb.model in (KOmega, KOmegaSST)
     bnd = config.boundaries
     bU = _bc_array(mesh, bnd["U"], 3, keep)
     bP = _bc_array(mesh, bnd["p"], 1, keep)
@@ -586,7 +616,23 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     w_bcs = bnd.get("omega", []) if kw else []
     bK = _bc_array(mesh, k_bcs, 1, keep)
     bW = _bc_array(mesh, w_bcs, 1, keep)
-    keep += [bU, bP, bN, bK, bW]
+    # wall_distance! (Calculate_4_wall_distance.jl:12-27): per BC of the
+    # first field, Dirichlet 0 on the walls, Empty, else Extrapolated
+    y_bcs = []
+    if sst:
+        walls = list(turb.walls or [])
+        for bc in next(iter(bnd.values())):
+            if bc.name in walls:
+                y_bcs.append(Dirichlet(bc.name, 0.0))
+            elif bc.kind == _abi.BC_EMPTY:
+                y_bcs.append(Empty(bc.name))
+            else:
+                y_bcs.append(Extrapolated(bc.name))
+    bY = _bc_array(mesh, y_bcs, 1, keep)
+    keep += [bU, bP, bN, bK, bW, bY]
+    sY = config.schemes.get("y", Schemes()) if sst else Schemes()
+    slv_y = _solver_desc(config.solvers["y"]) if sst else _abi.SolverSetupDesc()
+    co = turb.coeffs() if kw else {}
     sK = config.schemes.get("k", Schemes()) if kw else Schemes()
     sW = config.schemes.get("omega", Schemes()) if kw else Schemes()
     slv_k = _solver_desc(config.solvers["k"]) if kw else _abi.SolverSetupDesc()
@@ -600,7 +646,8 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     dist, power = delta_scaling(mesh, next(iter(bnd.values()))) if les else (1.0, 1.0 / 3.0)
     cfg = _abi.ConfigDesc(
         algorithm=_abi.ALGO_PISO if transient else _abi.ALGO_SIMPLE,
-        turbulence=_abi.TURB_SMAGORINSKY if les else (_abi.TURB_KOMEGA if kw else _abi.TURB_LAMINAR),
+        turbulence=(_abi.TURB_SMAGORINSKY if les else _abi.TURB_KOMEGA_SST if sst else _abi.TURB_KOMEGA if kw
+                    else _abi.TURB_LAMINAR),
         nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if les else 0.0,
         les_delta_distance=dist, les_delta_power=power,
         U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)],
@@ -617,10 +664,15 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
         n_bc_U=len(bnd["U"]), n_bc_p=len(bnd["p"]), n_bc_nut=len(nut_bcs),
         bc_U=C.cast(bU, C.POINTER(_abi.BCDesc)), bc_p=C.cast(bP, C.POINTER(_abi.BCDesc)),
         bc_nut=C.cast(bN, C.POINTER(_abi.BCDesc)),
-        kw_beta_star=float(getattr(turb, "beta_star", 0.09)), kw_alpha1=float(getattr(turb, "alpha1", 0.52)),
-        kw_beta1=float(getattr(turb, "beta1", 0.072)), kw_sigma_k=float(getattr(turb, "sigma_k", 0.5)),
-        kw_sigma_omega=float(getattr(turb, "sigma_omega", 0.5)),
-        k_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sK.time)], divergence=_SCHEME_DIV[_kind(sK.divergence)]),
+        kw_beta_star=co.get("beta_star", 0.0), kw_alpha1=co.get("alpha1", 0.0), kw_beta1=co.get("beta1", 0.0),
+        kw_sigma_k=co.get("sigma_k1" if sst else "sigma_k", 0.0),
+        kw_sigma_omega=co.get("sigma_omega1" if sst else "sigma_omega", 0.0),
+        sst_beta2=co.get("beta2", 0.0), sst_sigma_k2=co.get("sigma_k2", 0.0),
+        sst_sigma_omega2=co.get("sigma_omega2", 0.0),
+        y_schemes=_abi.SchemesDesc(gradient=_SCHEME_GRAD[_kind(sY.gradient)]), y_solver=slv_y, n_bc_y=len(y_bcs),
+        bc_y=C.cast(bY, C.POINTER(_abi.BCDesc)),
+        k_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sK.time)], divergence=_SCHEME_DIV[_kind(sK.divergence)],
+                                   gradient=_SCHEME_GRAD[_kind(sK.gradient)]),
         omega_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sW.time)],
                                        divergence=_SCHEME_DIV[_kind(sW.divergence)]),
         k_solver=slv_k, omega_solver=slv_w, n_bc_k=len(k_bcs), n_bc_omega=len(w_bcs),
@@ -634,7 +686,7 @@ class Case:
     def __init__(self, dmesh: DeviceMesh, cfg: _abi.ConfigDesc):
         self.dmesh, self.ctx = dmesh, dmesh.ctx
         self.mesh = dmesh.mesh
-        self.komega = cfg.turbulence == _abi.TURB_KOMEGA
+        self.komega = cfg.turbulence in (_abi.TURB_KOMEGA, _abi.TURB_KOMEGA_SST)
         h = C.c_void_p()
         check(lib().xcal_case_create(self.ctx.h, dmesh.h, C.byref(cfg), C.byref(h)), self.ctx.h)
         self.h = h

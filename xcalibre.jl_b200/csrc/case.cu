@@ -655,15 +655,25 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     for (const BCTable* T : {&bcU, &bcP, &bcNut})
         for (const xcal_bc& bc : T->src)
             if (bc.type == XCAL_BC_OMEGA_WALL) fail(XCAL_ERR_INVALID, "OmegaWallFunction applies to omega only");
-    if (cfg.turbulence == XCAL_TURB_KOMEGA) {
-        // RANS{KOmega} (RANS_kOmega.jl): k / omega share the p system
+    if (rans_kw()) {
+        // RANS{KOmega} / RANS{KOmegaSST}: k / omega share the p system
         build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, nullptr, stream);
         build_bc_table(bcOmega, *m, cfg.bc_omega, cfg.n_bc_omega, 1, nullptr, stream);
-        if (bcK.has_periodic || bcOmega.has_periodic || bcP.has_periodic || bcNut.has_periodic || bcU.has_periodic)
+        if (sst()) build_bc_table(bcY, *m, cfg.bc_y, cfg.n_bc_y, 1, nullptr, stream);
+        if (bcK.has_periodic || bcOmega.has_periodic || bcP.has_periodic || bcNut.has_periodic || bcU.has_periodic ||
+            bcY.has_periodic)
             fail(XCAL_ERR_UNSUPPORTED, "k-omega: periodic boundaries are not implemented");
         for (DBuf<double>* b : {&kfld, &omega, &Pk, &Pw, &Dk, &Dw, &kwtmp}) {
             b->alloc(m->nC);
             b->zero(stream);
+        }
+        if (sst()) {
+            for (DBuf<double>* b : {&yw, &yphi, &F1b, &F2b, &Omb, &D2b, &gkv[0], &gkv[1], &gkv[2], &gwv[0], &gwv[1],
+                                    &gwv[2]}) {
+                b->alloc(m->nC);
+                b->zero(stream);
+            }
+            fscr.alloc(m->nF);
         }
         build_wall_table(*m);
     } else if (cfg.turbulence != XCAL_TURB_LAMINAR && cfg.turbulence != XCAL_TURB_SMAGORINSKY) {
@@ -682,7 +692,12 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     if (cfg.ncorrectors > 0) build_nonorth(*m, stream);
     for (int g : {cfg.U_schemes.gradient, cfg.p_schemes.gradient})
         if (g != XCAL_GRAD_GAUSS && g != XCAL_GRAD_MIDPOINT) fail(XCAL_ERR_INVALID, "unknown gradient scheme");
-    if (cfg.U_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.p_schemes.gradient == XCAL_GRAD_MIDPOINT)
+    if (cfg.turbulence == XCAL_TURB_KOMEGA_SST)
+        for (int g : {cfg.k_schemes.gradient, cfg.y_schemes.gradient})
+            if (g != XCAL_GRAD_GAUSS && g != XCAL_GRAD_MIDPOINT) fail(XCAL_ERR_INVALID, "unknown gradient scheme");
+    if (cfg.U_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.p_schemes.gradient == XCAL_GRAD_MIDPOINT ||
+        (cfg.turbulence == XCAL_TURB_KOMEGA_SST &&
+         (cfg.k_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.y_schemes.gradient == XCAL_GRAD_MIDPOINT)))
         build_midpoint(*m, stream);
     for (const xcal_schemes* sc : {&cfg.U_schemes, &cfg.p_schemes}) {
         if (sc->limiter != XCAL_LIMITER_NONE && sc->limiter != XCAL_LIMITER_CELL)
@@ -790,6 +805,7 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         XCAL_CUDA(cudaMemcpyAsync(Delta.p, h.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream));
     }
     XCAL_CUDA(cudaStreamSynchronize(stream));
+    if (sst()) wall_distance();  // initialise(::KOmegaSST) (RANS_kOmegaSST.jl:167)
 }
 
 Case::~Case() {
@@ -872,8 +888,11 @@ double* Case::field_comp(int field, int comp, long& count) {
         case XCAL_FIELD_DELTA: return Delta.p;
         case XCAL_FIELD_K:
         case XCAL_FIELD_OMEGA:
-            if (cfg.turbulence != XCAL_TURB_KOMEGA) fail(XCAL_ERR_INVALID, "k / omega fields need RANS{KOmega}");
+            if (!rans_kw()) fail(XCAL_ERR_INVALID, "k / omega fields need RANS{KOmega} or RANS{KOmegaSST}");
             return field == XCAL_FIELD_K ? kfld.p : omega.p;
+        case XCAL_FIELD_WALLDIST:
+            if (!sst()) fail(XCAL_ERR_INVALID, "the wall distance needs RANS{KOmegaSST}");
+            return yw.p;
         default: return nullptr;
     }
 }
@@ -934,17 +953,34 @@ void Case::build_wall_table(const DevMesh& m) {
 void Case::komega() {
     const double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = gradU[q].p;
-    launch_kw_sources(stream, mesh->nC, g, nut.p, omega.p, Pk.p, Pw.p, Dk.p, Dw.p, cfg.kw_alpha1, cfg.kw_beta1,
-                      cfg.kw_beta_star);
+    const bool S = sst();
+    if (S) {
+        // RANS_kOmegaSST.jl:214-266: grad omega (p's gradient scheme), grad k, then the cell fields
+        double* gw[3] = {gwv[0].p, gwv[1].p, gwv[2].p};
+        double* gk[3] = {gkv[0].p, gkv[1].p, gkv[2].p};
+        scalar_grad(omega.p, bcOmega, cfg.p_schemes.gradient, gw);
+        scalar_grad(kfld.p, bcK, cfg.k_schemes.gradient, gk);
+        const double* gwc[3] = {gw[0], gw[1], gw[2]};
+        const double* gkc[3] = {gk[0], gk[1], gk[2]};
+        launch_sst_fields(stream, mesh->nC, g, gkc, gwc, kfld.p, omega.p, nut.p, yw.p, F1b.p, F2b.p, Omb.p, Pk.p, Pw.p,
+                          Dk.p, Dw.p, D2b.p, cfg.kw_beta_star, cfg.kw_alpha1, cfg.kw_beta1, cfg.sst_beta2,
+                          cfg.sst_sigma_omega2, cfg.nu);
+    } else {
+        launch_kw_sources(stream, mesh->nC, g, nut.p, omega.p, Pk.p, Pw.p, Dk.p, Dw.p, cfg.kw_alpha1, cfg.kw_beta1,
+                          cfg.kw_beta_star);
+    }
     for (int e : {(int)XCAL_EQN_OMEGA, (int)XCAL_EQN_K}) {
         const bool w = e == XCAL_EQN_OMEGA;
         double* phi = w ? omega.p : kfld.p;
         const xcal_schemes& sc = w ? cfg.omega_schemes : cfg.k_schemes;
         const double sigma = w ? cfg.kw_sigma_omega : cfg.kw_sigma_k;
-        launch_assemble_scalar(stream, mv(), P.view(), mdot.p, nutf.p, cfg.nu, sigma, phi, w ? Dw.p : Dk.p,
-                               w ? Pw.p : Pk.p, P.nz.p, P.b[0].p, sc.time, sc.divergence, cfg.dt);
+        const double sigma2 = w ? cfg.sst_sigma_omega2 : cfg.sst_sigma_k2;
+        const double* F1 = S ? F1b.p : nullptr;
+        const double* D2 = (S && w) ? D2b.p : nullptr;
+        launch_assemble_scalar(stream, mv(), P.view(), mdot.p, nutf.p, cfg.nu, sigma, F1, sigma2, phi,
+                               w ? Dw.p : Dk.p, D2, w ? Pw.p : Pk.p, P.nz.p, P.b[0].p, sc.time, sc.divergence, cfg.dt);
         launch_bc_relax_scalar(stream, mv(), P.view(), (w ? bcOmega : bcK).view(), P.nz.p, P.b[0].p, mdot.p, nutf.p,
-                               cfg.nu, sigma, phi, (w ? cfg.omega_solver : cfg.k_solver).relax);
+                               cfg.nu, sigma, F1, sigma2, D2 ? 1 : 0, phi, (w ? cfg.omega_solver : cfg.k_solver).relax);
         if (w && nwall) launch_omega_constrain(stream, nwall, P.view(), wcell.p, wpar.p, kfld.p, cfg.nu, P.nz.p, P.b[0].p);
         update_precond(e);
         const double r = solve_system(e, 0, &last_iters[w ? 5 : 4]);
@@ -952,8 +988,55 @@ void Case::komega() {
         XCAL_CUDA(cudaMemcpyAsync(kwtmp.p, phi, (size_t)mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
         launch_bound(stream, mv(), kwtmp.p, phi);
     }
-    launch_kw_nut(stream, mesh->nC, kfld.p, omega.p, nut.p);
+    if (S)
+        launch_sst_nut(stream, mesh->nC, kfld.p, omega.p, F2b.p, Omb.p, cfg.kw_alpha1, nut.p);
+    else
+        launch_kw_nut(stream, mesh->nC, kfld.p, omega.p, nut.p);
     launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
+}
+
+// grad! of a scalar with its BCs (Calculate_0_gradient.jl): Gauss, or the
+// Midpoint passes (as grad p)
+void Case::scalar_grad(const double* phi, const BCTable& T, int scheme, double* const g[3]) {
+    launch_interp_scalar(stream, mv(), T.view(), phi, fscr.p, nullptr, 0.0);
+    launch_green_gauss(stream, mv(), fscr.p, g);
+    if (scheme != XCAL_GRAD_MIDPOINT) return;
+    const double* gc[3] = {g[0], g[1], g[2]};
+    launch_mid_scalar(stream, mv(), phi, fscr.p);
+    launch_green_gauss(stream, mv(), fscr.p, g);
+    for (int it = 0; it < 2; ++it) {
+        launch_mid_correct_scalar(stream, mv(), midR.p, phi, gc, fscr.p);
+        launch_green_gauss(stream, mv(), fscr.p, g);
+    }
+}
+
+// wall_distance! (Calculate_4_wall_distance.jl:4-92), once at case creation:
+// -Laplacian(1, phi) == Source(1) with the wall BCs on the p system (the p
+// assembly with rDf = 1 and divHv = -1 gives the same coefficients), solved
+// and explicitly relaxed until the residual is below y_solver.convergence
+// (1000 at most); y = -|grad phi| + sqrt(|grad phi|^2 + 2 phi)
+void Case::wall_distance() {
+    const int nC = mesh->nC, nF = mesh->nF;
+    DBuf<double> ones_f, mone_c;
+    ones_f.alloc(nF);
+    mone_c.alloc(nC);
+    launch_fill(stream, ones_f.p, 1.0, nF);
+    launch_fill(stream, mone_c.p, -1.0, nC);
+    const xcal_solver_setup& SS = cfg.y_solver;
+    for (int it = 0; it < 1000; ++it) {
+        XCAL_CUDA(cudaMemcpyAsync(kwtmp.p, yphi.p, (size_t)nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        launch_assemble_p(stream, mv(), P.view(), ones_f.p, mone_c.p, P.nz.p, P.b[0].p);
+        launch_bc_p(stream, mv(), P.view(), bcY.view(), P.nz.p, P.b[0].p, ones_f.p, yphi.p);
+        update_precond(XCAL_EQN_WALLDIST);
+        const double res = solve_system(XCAL_EQN_WALLDIST, 0, &last_iters[6]);
+        launch_relax_explicit(stream, nC, yphi.p, kwtmp.p, SS.relax);
+        if (res < SS.convergence) break;
+    }
+    double* g[3] = {gkv[0].p, gkv[1].p, gkv[2].p};
+    scalar_grad(yphi.p, bcY, cfg.y_schemes.gradient, g);
+    const double* gc[3] = {g[0], g[1], g[2]};
+    launch_walldist(stream, nC, yphi.p, gc, yw.p);
+    sync();
 }
 
 void Case::discretise(int eqn) {
@@ -1416,13 +1499,17 @@ Case::SolveRef Case::solve_ref(int eqn, int comp) {
             return {&P, cfg.p_solver, p.p, P.b[0].p, GRES_P, 1, 3};
         case XCAL_EQN_K:
         case XCAL_EQN_OMEGA: {
-            if (cfg.turbulence != XCAL_TURB_KOMEGA) fail(XCAL_ERR_INVALID, "k / omega equations need RANS{KOmega}");
+            if (!rans_kw()) fail(XCAL_ERR_INVALID, "k / omega equations need RANS{KOmega} or RANS{KOmegaSST}");
             const bool w = eqn == XCAL_EQN_OMEGA;
             SolveRef r{&P, w ? cfg.omega_solver : cfg.k_solver, w ? omega.p : kfld.p, P.b[0].p,
                        w ? (int)GRES_OMEGA : (int)GRES_K, 1, w ? 5 : 4};
-            r.SS.precond = cfg.k_solver.precond;
+            // k-omega: omega with k's preconditioner; SST: each its own (RANS_kOmegaSST.jl:163-164)
+            r.SS.precond = (w && sst()) ? cfg.omega_solver.precond : cfg.k_solver.precond;
             return r;
         }
+        case XCAL_EQN_WALLDIST:
+            if (!sst()) fail(XCAL_ERR_INVALID, "the wall distance needs RANS{KOmegaSST}");
+            return {&P, cfg.y_solver, yphi.p, P.b[0].p, GRES_K, 1, 6};
         default:
             fail(XCAL_ERR_INVALID, "unknown equation");
     }
@@ -1703,7 +1790,7 @@ void Case::turbulence() {
             launch_limit_cell(stream, mv(), limD.p, Uc[a].p, g + 3 * a, cfg.U_schemes.limiter_level);
         if (les) launch_smag_nut(stream, mesh->nC, g, Delta.p, nut.p);
     }
-    if (cfg.turbulence == XCAL_TURB_KOMEGA)
+    if (rans_kw())
         komega();
     else if (les)
         launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);

@@ -113,7 +113,7 @@ struct Case {
     size_t bytes = 0;  // device bytes held (excluding the mesh)
     cudaStream_t stream = nullptr;
     bool own_stream = true;
-    BCTable bcU, bcP, bcNut, bcK, bcOmega;
+    BCTable bcU, bcP, bcNut, bcK, bcOmega, bcY;
     Equation U, P;
     KrylovWS ws;
     // fields
@@ -126,13 +126,16 @@ struct Case {
     // copy for bound!, and the omega wall cells (storage ids) with, per cell,
     // y = delta of its constraining face, kappa, beta1, cmu^0.25, yPlusLam
     DBuf<double> kfld, omega, Pk, Pw, Dk, Dw, kwtmp, wpar;
+    // RANS{KOmegaSST}: wall distance (and its potential), F1, F2, Omega, the
+    // second omega Si coefficient, grad k, grad omega, a face scratch
+    DBuf<double> yw, yphi, F1b, F2b, Omb, D2b, gkv[3], gwv[3], fscr;
     DBuf<int> wcell;
     int nwall = 0;
     double res_k = 0.0, res_omega = 0.0;
     bool initialised = false;
     int iteration = 0;
     double time = 0.0;
-    int last_iters[6] = {0, 0, 0, 0, 0, 0};  // Ux, Uy, Uz, p, k, omega
+    int last_iters[7] = {0, 0, 0, 0, 0, 0, 0};  // Ux, Uy, Uz, p, k, omega, wall distance
     // timing
     double ms[6] = {0, 0, 0, 0, 0, 0};
     long long launches = 0;
@@ -157,8 +160,8 @@ struct Case {
         cudaGraphExec_t exec = nullptr;
         long long launches = 0;  // kernels per replay
     };
-    ChunkGraph chunk_graph[6][2];  // [Ux, Uy, Uz, p, k, omega][plain, profiled]
-    cudaEvent_t gev[6][12] = {};   // event nodes of the profiled graphs
+    ChunkGraph chunk_graph[7][2];  // [Ux, Uy, Uz, p, k, omega, wall distance][plain, profiled]
+    cudaEvent_t gev[7][12] = {};   // event nodes of the profiled graphs
     template <class F>
     void replay_chunk(ChunkGraph& g, F&& body);
 
@@ -197,6 +200,10 @@ struct Case {
     SolveRef solve_ref(int eqn, int comp);
     void build_wall_table(const DevMesh& m);
     void komega();
+    bool sst() const { return cfg.turbulence == XCAL_TURB_KOMEGA_SST; }
+    bool rans_kw() const { return cfg.turbulence == XCAL_TURB_KOMEGA || sst(); }
+    void scalar_grad(const double* phi, const BCTable& T, int scheme, double* const g[3]);
+    void wall_distance();
     void nonorth_correct();
     void nonorth_correctors(double& rp);
     void explicit_relaxation_p(double a);
@@ -221,7 +228,7 @@ struct Case {
                         const KrylovVecs<T>& V, KScalars* S, KScalars* hS, int gk);
     void solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, const double* b, KScalars* S,
                      KScalars* hS, int gk, int* iters);
-    int last_outer[6] = {0, 0, 0, 0, 0, 0};  // mixed: defect-correction steps of the last solve per system
+    int last_outer[7] = {0, 0, 0, 0, 0, 0, 0};  // mixed: defect-correction steps of the last solve per system
     bool tuned = false;
     void autotune();  // launch-shape autotuner (autotune.cu), once per case
 

@@ -51,6 +51,25 @@ __device__ __forceinline__ double jl_min(double x, double y) {
     return take_y ? (isnan(x) ? x : y) : (isnan(y) ? y : x);
 }
 
+// exp(y) for y <= 0 and tanh(x) for x >= 0 from +, *, / and ldexp only, the
+// same operations on the host and the device: Cody-Waite reduction
+// y = k ln2 + r (ln2 split in a 12-bit head and its remainder), exp(r) by its
+// Taylor series to r^14 / 14!; tanh(x) = (1 - e^-2x) / (1 + e^-2x), 1 past 20
+__host__ __device__ __forceinline__ double det_exp_neg(double y) {
+    if (y < -745.0) return 0.0;
+    const double LN2_HEAD = 0.693145751953125, LN2_TAIL = 1.4286068203094172321e-06;
+    const double k = rint(y * 1.4426950408889634);
+    const double r = (y - k * LN2_HEAD) - k * LN2_TAIL;
+    double p = 1.0;
+    for (int n = 14; n >= 1; --n) p = 1.0 + (r / (double)n) * p;
+    return ldexp(p, (int)k);
+}
+__host__ __device__ __forceinline__ double det_tanh_pos(double x) {
+    if (x > 20.0) return 1.0;
+    const double e = det_exp_neg(-2.0 * x);
+    return (1.0 - e) / (1.0 + e);
+}
+
 // Julia's eps(x)
 __device__ __forceinline__ double jl_eps(double x) {
     x = fabs(x);

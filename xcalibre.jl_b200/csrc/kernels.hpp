@@ -45,12 +45,23 @@ void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const
 // wall rows, bound!, nut = k / omega; nueff = nu + nutf
 void launch_kw_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* omega,
                        double* Pk, double* Pw, double* Dk, double* Dw, double alpha1, double beta1, double beta_star);
+// (F1 null: constant sigma; F1 set: sigma blended with sigma2 (k-omega SST);
+// D2 / si2: the omega equation's second Si term of k-omega SST)
 void launch_assemble_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const double* mdot,
-                            const double* nutf, double nu, double sigma, const double* phi, const double* D,
-                            const double* P, double* nz, double* b, int time_scheme, int div_scheme, double dt);
+                            const double* nutf, double nu, double sigma, const double* F1, double sigma2,
+                            const double* phi, const double* D, const double* D2, const double* P, double* nz,
+                            double* b, int time_scheme, int div_scheme, double dt);
 void launch_bc_relax_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz,
                             double* b, const double* mdot, const double* nutf, double nu, double sigma,
-                            const double* phi, double alpha);
+                            const double* F1, double sigma2, int si2, const double* phi, double alpha);
+// k-omega SST: cell fields, nut, and the wall distance from phi and grad phi
+void launch_sst_fields(cudaStream_t s, int nC, const double* const g[9], const double* const gk[3],
+                       const double* const gw[3], const double* k, const double* omega, const double* nut,
+                       const double* yw, double* F1, double* F2, double* Om, double* Pk, double* Pw, double* Dk,
+                       double* Dw, double* D2, double bs, double al1, double b1, double b2, double sw2, double nu);
+void launch_sst_nut(cudaStream_t s, int nC, const double* k, const double* omega, const double* F2, const double* Om,
+                    double al1, double* nut);
+void launch_walldist(cudaStream_t s, int nC, const double* phi, const double* const g[3], double* y);
 void launch_omega_constrain(cudaStream_t s, int nw, const CSRView& A, const int* wcell, const double* par,
                             const double* k, double nu, double* nz, double* b);
 void launch_bound(cudaStream_t s, const MeshView& m, const double* old, double* v);

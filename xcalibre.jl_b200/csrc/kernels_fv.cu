@@ -382,9 +382,21 @@ __global__ void k_kw_sources(int nC, const double* __restrict__ g0, const double
 
 // _discretise_scalar_model! (Discretise_2_generated_distretisation.jl:125-167)
 // of the k / omega equation: terms Time, Divergence, Laplacian, Si in order
+// face diffusivity nu + sigma nutf; with F1 (k-omega SST) sigma blends as
+// s1 F1f + (1 - F1f) s2, F1f the plain interpolation of F1
+__device__ __forceinline__ double kw_mueff(const MeshView& m, int f, const double* nutf, double nu, double s1,
+                                           const double* F1, double s2) {
+    if (!F1) return nu + s1 * nutf[f];
+    const double w = m.weight[f];
+    const double F1f = w * F1[m.owner[f]] + (1.0 - w) * F1[m.neigh[f]];
+    const double sg = s1 * F1f + (1.0 - F1f) * s2;
+    return nu + sg * nutf[f];
+}
+
 __global__ void k_assemble_scalar(MeshView m, CSRView A, const double* __restrict__ mdot,
                                   const double* __restrict__ nutf, double nu, double sigma,
-                                  const double* __restrict__ phi, const double* __restrict__ D,
+                                  const double* __restrict__ F1, double sigma2, const double* __restrict__ phi,
+                                  const double* __restrict__ D, const double* __restrict__ D2,
                                   const double* __restrict__ P, double* nz, double* b, int time_scheme,
                                   int div_scheme, double dt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -417,12 +429,16 @@ __global__ void k_assemble_scalar(MeshView m, CSRView A, const double* __restric
         }
         AC = AC + ac;
         AN = AN + an;
-        const double muf = nu + sigma * nutf[f];
+        const double muf = kw_mueff(m, f, nutf, nu, sigma, F1, sigma2);
         double apl = (-1.0 * (muf * m.Efmag[f])) / m.delta[f];  // Laplacian, sign -1
         AC = AC + (-apl);
         AN = AN + apl;
         AC = AC + 0.0;  // Si (:204-210)
         AN = AN + 0.0;
+        if (D2) {  // a second Si (omega of k-omega SST)
+            AC = AC + 0.0;
+            AN = AN + 0.0;
+        }
         ac_sum = ac_sum + AC;
         nz[A.cf_slot[k]] = AN;
     }
@@ -442,6 +458,10 @@ __global__ void k_assemble_scalar(MeshView m, CSRView A, const double* __restric
     bs = bs + 0.0;
     acs = acs + (1.0 * D[i]) * V;  // Si (:211-218)
     bs = bs + 0.0;
+    if (D2) {
+        acs = acs + (1.0 * D2[i]) * V;
+        bs = bs + 0.0;
+    }
     nz[A.diag[i]] = ac_sum + acs;
     const double b2 = 0.0 + (1.0 * P[i]) * V;  // +Source(P)
     b[i] = b2 + bs;
@@ -452,7 +472,7 @@ __global__ void k_assemble_scalar(MeshView m, CSRView A, const double* __restric
 // OmegaWallFunction contributes as Extrapolated (its wall rows are then
 // constrained)
 __device__ void bc_scalar_transport(const MeshView& m, const BCView& bc, int f, int cell, const double* mdot,
-                                    double muf, const double* phi, double& AP, double& BP) {
+                                    double muf, const double* phi, bool si2, double& AP, double& BP) {
     double ap_d = 0.0, bp_d = 0.0, ap_l = 0.0, bp_l = 0.0;
     switch (bc.type[f]) {
         case XCAL_BC_DIRICHLET:
@@ -499,6 +519,10 @@ __device__ void bc_scalar_transport(const MeshView& m, const BCView& bc, int f, 
     bp = bp + bp_l;
     ap = ap + 0.0;  // Si
     bp = bp + 0.0;
+    if (si2) {
+        ap = ap + 0.0;
+        bp = bp + 0.0;
+    }
     AP = ap;
     BP = bp;
 }
@@ -508,7 +532,8 @@ __device__ void bc_scalar_transport(const MeshView& m, const BCView& bc, int f, 
 // equation, one thread per row
 __global__ void k_bc_relax_scalar(MeshView m, CSRView A, BCView bc, double* nz, double* b,
                                   const double* __restrict__ mdot, const double* __restrict__ nutf, double nu,
-                                  double sigma, const double* __restrict__ phi, double alpha) {
+                                  double sigma, const double* __restrict__ F1, double sigma2, int si2,
+                                  const double* __restrict__ phi, double alpha) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.nC) return;
     const int ds = A.diag[i];
@@ -517,7 +542,7 @@ __global__ void k_bc_relax_scalar(MeshView m, CSRView A, BCView bc, double* nz, 
     for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
         const int f = m.bf_face[k];
         double AP, BP;
-        bc_scalar_transport(m, bc, f, i, mdot, nu + sigma * nutf[f], phi, AP, BP);
+        bc_scalar_transport(m, bc, f, i, mdot, kw_mueff(m, f, nutf, nu, sigma, F1, sigma2), phi, si2 != 0, AP, BP);
         d = d + AP;
         bi = bi + BP;
     }
@@ -570,6 +595,74 @@ __global__ void k_bound(MeshView m, const double* __restrict__ old, double* v) {
     const double vi = old[i];
     const double s = signbit(vi) ? average : copysign(0.0, average);
     v[i] = jl_max(jl_max(vi, s), mzero);
+}
+
+// k-omega SST cell fields (RANS_kOmegaSST.jl:214-266): |S|^2 (as k-omega),
+// Omega = sqrt(2|S|^2), CDkw, arg1/arg2, F1 = tanh(arg1^4), F2 = tanh(arg2^2),
+// beta and gamma blends, Dw = beta w, Dk = beta+ w, the limited productions
+// and the cross-diffusion Si coefficient D2; g: grad U, gk / gw: grad k /
+// grad omega
+__global__ void k_sst_fields(int nC, const double* __restrict__ g0, const double* __restrict__ g1,
+                             const double* __restrict__ g2, const double* __restrict__ g3,
+                             const double* __restrict__ g4, const double* __restrict__ g5,
+                             const double* __restrict__ g6, const double* __restrict__ g7,
+                             const double* __restrict__ g8, const double* __restrict__ gkx,
+                             const double* __restrict__ gky, const double* __restrict__ gkz,
+                             const double* __restrict__ gwx, const double* __restrict__ gwy,
+                             const double* __restrict__ gwz, const double* __restrict__ kf,
+                             const double* __restrict__ omega, const double* __restrict__ nut,
+                             const double* __restrict__ yw, double* F1o, double* F2o, double* Omo, double* Pk,
+                             double* Pw, double* Dk, double* Dw, double* D2, double bs, double al1, double b1,
+                             double b2, double sw2, double nu) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nC) return;
+    const double G[9] = {g0[i], g1[i], g2[i], g3[i], g4[i], g5[i], g6[i], g7[i], g8[i]};
+    double sum = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double s = 0.5 * (G[3 * j + q] + G[3 * q + j]);
+            sum = sum + s * s;
+        }
+    const double mag = sum * 2.0;
+    const double Om = sqrt(mag);
+    const double w = omega[i], kk = kf[i], y = yw[i];
+    const double dkdw = (gkx[i] * gwx[i] + gky[i] * gwy[i]) + gkz[i] * gwz[i];
+    const double CD = jl_max(((2.0 * sw2) * dkdw) / w, 1e-10);
+    const double sq = sqrt(jl_max(kk, jl_eps(1.0)));
+    const double a1 = jl_min(jl_min(jl_max(sq / ((bs * w) * y), (500.0 * nu) / (w * (y * y))),
+                                    ((4.0 * sw2) * kk) / (CD * (y * y))),
+                             10.0);
+    const double a2 = jl_min(jl_max((2.0 * sq) / ((bs * w) * y), (500.0 * nu) / ((y * y) * w)), 100.0);
+    const double f2 = det_tanh_pos(a2 * a2);
+    const double f1 = det_tanh_pos((a1 * a1) * (a1 * a1));
+    const double beta = b1 * f1 + (1.0 - f1) * b2;
+    const double gamma = (5.0 / 9.0) * f1 + (1.0 - f1) * 0.44;
+    F1o[i] = f1;
+    F2o[i] = f2;
+    Omo[i] = Om;
+    Dw[i] = beta * w;
+    Dk[i] = bs * w;
+    Pw[i] = gamma * jl_min(mag, (((10.0 / al1) * bs) * w) * jl_max(al1 * w, f2 * Om));
+    Pk[i] = jl_min(mag * nut[i], ((10.0 * bs) * kk) * w);
+    D2[i] = ((((2.0 * (f1 - 1.0)) * sw2) * dkdw) / w) / w;
+}
+
+// nut = alpha1 k / max(alpha1 omega, F2 Omega) (RANS_kOmegaSST.jl:303-306)
+__global__ void k_sst_nut(int nC, const double* __restrict__ k, const double* __restrict__ omega,
+                          const double* __restrict__ F2, const double* __restrict__ Om, double al1, double* nut) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nC) nut[i] = (al1 * k[i]) / jl_max(al1 * omega[i], F2[i] * Om[i]);
+}
+
+// normal_distance! (Calculate_4_wall_distance.jl:80-92)
+__global__ void k_walldist(int nC, const double* __restrict__ phi, const double* __restrict__ gx,
+                           const double* __restrict__ gy, const double* __restrict__ gz, double* y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nC) return;
+    const double gm = sqrt(gx[i] * gx[i] + gy[i] * gy[i] + gz[i] * gz[i]);
+    y[i] = (-gm) + sqrt(gm * gm + 2.0 * phi[i]);
 }
 
 // nut = k / omega (RANS_kOmega.jl:201)
@@ -1268,16 +1361,35 @@ void launch_kw_sources(cudaStream_t s, int nC, const double* const g[9], const d
     XCAL_CHECK_LAUNCH();
 }
 void launch_assemble_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const double* mdot,
-                            const double* nutf, double nu, double sigma, const double* phi, const double* D,
-                            const double* P, double* nz, double* b, int time_scheme, int div_scheme, double dt) {
-    k_assemble_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, mdot, nutf, nu, sigma, phi, D, P, nz, b, time_scheme,
-                                                 div_scheme, dt);
+                            const double* nutf, double nu, double sigma, const double* F1, double sigma2,
+                            const double* phi, const double* D, const double* D2, const double* P, double* nz,
+                            double* b, int time_scheme, int div_scheme, double dt) {
+    k_assemble_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, mdot, nutf, nu, sigma, F1, sigma2, phi, D, D2, P, nz, b,
+                                                 time_scheme, div_scheme, dt);
     XCAL_CHECK_LAUNCH();
 }
 void launch_bc_relax_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz,
                             double* b, const double* mdot, const double* nutf, double nu, double sigma,
-                            const double* phi, double alpha) {
-    k_bc_relax_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, bc, nz, b, mdot, nutf, nu, sigma, phi, alpha);
+                            const double* F1, double sigma2, int si2, const double* phi, double alpha) {
+    k_bc_relax_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, bc, nz, b, mdot, nutf, nu, sigma, F1, sigma2, si2, phi, alpha);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_sst_fields(cudaStream_t s, int nC, const double* const g[9], const double* const gk[3],
+                       const double* const gw[3], const double* k, const double* omega, const double* nut,
+                       const double* yw, double* F1, double* F2, double* Om, double* Pk, double* Pw, double* Dk,
+                       double* Dw, double* D2, double bs, double al1, double b1, double b2, double sw2, double nu) {
+    k_sst_fields<<<nblk(nC), TPB, 0, s>>>(nC, g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8], gk[0], gk[1],
+                                          gk[2], gw[0], gw[1], gw[2], k, omega, nut, yw, F1, F2, Om, Pk, Pw, Dk, Dw,
+                                          D2, bs, al1, b1, b2, sw2, nu);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_sst_nut(cudaStream_t s, int nC, const double* k, const double* omega, const double* F2, const double* Om,
+                    double al1, double* nut) {
+    k_sst_nut<<<nblk(nC), TPB, 0, s>>>(nC, k, omega, F2, Om, al1, nut);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_walldist(cudaStream_t s, int nC, const double* phi, const double* const g[3], double* y) {
+    k_walldist<<<nblk(nC), TPB, 0, s>>>(nC, phi, g[0], g[1], g[2], y);
     XCAL_CHECK_LAUNCH();
 }
 void launch_omega_constrain(cudaStream_t s, int nw, const CSRView& A, const int* wcell, const double* par,
