@@ -45,9 +45,12 @@ enum {
     XCAL_BC_NEUMANN = 8,            /* neumann.jl (scalar fields)            */
     XCAL_BC_PERIODIC = 9,           /* periodic.jl `Periodic` (shadow side)  */
     XCAL_BC_PERIODIC_PARENT = 10,   /* periodic.jl `PeriodicParent`          */
-    XCAL_BC_OMEGA_WALL = 11         /* OmegaWallFunction (Discretise_0_types.jl:
+    XCAL_BC_OMEGA_WALL = 11,        /* OmegaWallFunction (Discretise_0_types.jl:
                                        83-113; constraint RANS_functions.jl:
                                        376-429): constants in xcal_bc.wall  */
+    XCAL_BC_K_WALL = 12,            /* KWallFunction (production, RANS_functions.jl:
+                                       66-117)                               */
+    XCAL_BC_NUT_WALL = 13           /* NutWallFunction (nutf, :119-172)      */
 };
 /* Time{T}: src/Discretise/Discretise_1_schemes.jl:12-45 */
 enum { XCAL_TIME_STEADY = 0, XCAL_TIME_EULER = 1 };
@@ -148,10 +151,10 @@ typedef struct {
     const int32_t* face_map;    /* [patch_count] partner face ids           */
     double distance[3];         /* LinearTransform.distance                 */
     int32_t partner_patch;
-    /* OmegaWallFunction: kappa, beta1, cmu^0.25 and yPlusLam =
-     * y_plus_laminar(E, kappa) (RANS_functions.jl:42-49), evaluated by the
-     * caller */
-    double wall[4];
+    /* wall functions: kappa, beta1, cmu^0.25, yPlusLam =
+     * y_plus_laminar(E, kappa) (RANS_functions.jl:42-49) and E, evaluated by
+     * the caller */
+    double wall[5];
 } xcal_bc;
 
 /* SolverSetup (src/Solve/Solve_1_api.jl:8-83) */

@@ -85,7 +85,7 @@ static void copy_bcs(const Mesh& m, const xcal_bc* src, int n, std::vector<BC>& 
         for (int c = 0; c < 3; ++c) bc.value[c] = src[b].value[c];
         bc.start = m.patch_start[bc.patch];
         bc.count = m.patch_count[bc.patch];
-        for (int c = 0; c < 4; ++c) bc.wall[c] = src[b].wall[c];
+        for (int c = 0; c < 5; ++c) bc.wall[c] = src[b].wall[c];
         if (bc.type == XCAL_BC_DIRICHLET_FUNCTION) {
             if (!src[b].face_values) throw std::runtime_error("DirichletFunction without values");
             bc.face_values.assign(src[b].face_values, src[b].face_values + (size_t)ncomp * bc.count);
@@ -421,6 +421,8 @@ static void bc_functor(BCCtx& X, const BC& bc, const Term& t, int f, double& ap,
             return;
         }
         case XCAL_BC_ZEROGRADIENT:  // zerogradient.jl
+        case XCAL_BC_K_WALL:        // Discretise_3_boundary_conditions.jl:12-51 (Laplacian (0, 0))
+        case XCAL_BC_NUT_WALL:
             if (t.kind == T_DIV) ap = t.sign * flux;
             return;
         case XCAL_BC_OMEGA_WALL:    // Discretise_3_boundary_conditions.jl:28-61 (as Extrapolated)
@@ -873,6 +875,8 @@ static void correct_boundaries(Case& C, const std::vector<BC>& bcs, std::vector<
                 break;
             case XCAL_BC_ZEROGRADIENT:
             case XCAL_BC_OMEGA_WALL:
+            case XCAL_BC_K_WALL:
+            case XCAL_BC_NUT_WALL:
             case XCAL_BC_EXTRAPOLATED:
                 for (int d = 0; d < ncomp; ++d) phif[d][f] = phi[d][c];
                 break;
@@ -1370,6 +1374,52 @@ static void bound_field(const Mesh& m, std::vector<double>& v) {
     }
 }
 
+// nut_wall (RANS_functions.jl:61-63)
+static double nut_wall(double nu, double yplus, double kappa, double E) {
+    return jl_max(nu * (((yplus * kappa) / det_log(jl_max(E * yplus, 1.0 + 1e-4))) - 1.0), 0.0);
+}
+
+// correct_production!(Pk, KWallFunction) (RANS_functions.jl:66-117): per
+// wall face (BC order, face order), the cell's production from the log law
+static void kwall_production(Case& C) {
+    const Mesh& m = *C.m;
+    const double nu = C.cfg.nu;
+    for (const BC& bc : C.bcK) {
+        if (bc.type != XCAL_BC_K_WALL) continue;
+        const double kappa = bc.wall[0], c25 = bc.wall[2], yPlusLam = bc.wall[3], E = bc.wall[4];
+        for (int f = bc.start; f < bc.start + bc.count; ++f) {
+            const int c = m.bcell[f];
+            const double delta = m.fdelta[f];
+            const V3 n = m.fnormal[f];
+            const double sk = std::sqrt(C.k[c]);
+            const double uStar = c25 * sk;
+            const double dUdy = uStar / (kappa * delta);
+            const double yplus = ((c25 * delta) * sk) / nu;
+            const double nutw = nut_wall(nu, yplus, kappa, E);
+            const V3 Ud = {C.U[0][c] - 0.0, C.U[1][c] - 0.0, C.U[2][c] - 0.0};  // Ui - Uw, Uw = 0
+            const V3 Up = Ud - dot(Ud, n) * n;
+            const V3 g = Up / delta;
+            const double mag = std::sqrt(g.x * g.x + g.y * g.y + g.z * g.z);
+            C.Pk[c] = yplus > yPlusLam ? ((nu + nutw) * mag) * dUdy : 0.0;
+        }
+    }
+}
+
+// correct_eddy_viscosity!(nutf, NutWallFunction) (RANS_functions.jl:119-172)
+static void nutwall_correct(Case& C) {
+    const Mesh& m = *C.m;
+    const double nu = C.cfg.nu;
+    for (const BC& bc : C.bcNut) {
+        if (bc.type != XCAL_BC_NUT_WALL) continue;
+        const double kappa = bc.wall[0], c25 = bc.wall[2], yPlusLam = bc.wall[3], E = bc.wall[4];
+        for (int f = bc.start; f < bc.start + bc.count; ++f) {
+            const int c = m.bcell[f];
+            const double yplus = ((c25 * m.fdelta[f]) * std::sqrt(C.k[c])) / nu;
+            C.nutf[f] = yplus > yPlusLam ? nut_wall(nu, yplus, kappa, E) : 0.0;
+        }
+    }
+}
+
 // solve_system! of k or omega on the shared scalar system
 static double solve_scalar(Case& C, const xcal_solver_setup& SS0, int ptype, std::vector<double>& field,
                            std::vector<double>& P) {
@@ -1402,6 +1452,7 @@ static void komega(Case& C) {
         C.Dw[i] = cf.kw_beta1 * C.omega[i];     // rho beta1 omega
         C.Dk[i] = cf.kw_beta_star * C.omega[i];  // rho beta+ omega
     }
+    kwall_production(C);
     for (int f = 0; f < C.nF; ++f) {  // rhof (nuf + sigma nutf), rhof = 1
         C.mueffw[f] = cf.nu + cf.kw_sigma_omega * C.nutf[f];
         C.mueffk[f] = cf.nu + cf.kw_sigma_k * C.nutf[f];
@@ -1433,6 +1484,7 @@ static void komega(Case& C) {
     for (int i = 0; i < C.nC; ++i) C.nut[i] = C.k[i] / C.omega[i];
     interpolate(m, C.nut, C.nutf);
     correct_boundaries(C, C.bcNut, &C.nutf, &C.nut, false);
+    nutwall_correct(C);
 }
 
 // grad! of a scalar with its BCs, Gauss or Midpoint (Calculate_0_gradient.jl)
@@ -1521,6 +1573,7 @@ static void komega_sst(Case& C) {
         C.Pk[i] = jl_min(mag * C.nut[i], ((10.0 * bs) * kk) * w);
         C.D2[i] = ((((2.0 * (f1 - 1.0)) * sw2) * dkdw) / w) / w;
     }
+    kwall_production(C);
     for (int f = 0; f < C.nF; ++f) {  // interpolate!(F1f, F1); sigma blending; mueff
         const double wt = m.fweight[f];
         const double F1f = wt * C.F1[m.owner[f]] + (1.0 - wt) * C.F1[m.neigh[f]];
@@ -1555,6 +1608,7 @@ static void komega_sst(Case& C) {
     for (int i = 0; i < C.nC; ++i) C.nut[i] = (al1 * C.k[i]) / jl_max(al1 * C.omega[i], C.F2[i] * C.Om[i]);
     interpolate(m, C.nut, C.nutf);
     correct_boundaries(C, C.bcNut, &C.nutf, &C.nut, false);
+    nutwall_correct(C);
 }
 
 void turbulence(Case& C) {

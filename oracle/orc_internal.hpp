@@ -52,7 +52,7 @@ struct BC {
     V3 distance{0, 0, 0};
     int partner_patch = -1;
     int start = 0, count = 0;  // IDs_range
-    double wall[4] = {0, 0, 0, 0};  // OmegaWallFunction: kappa, beta1, cmu^0.25, yPlusLam
+    double wall[5] = {0, 0, 0, 0, 0};  // wall functions: kappa, beta1, cmu^0.25, yPlusLam, E
 };
 
 struct Krylov {

@@ -64,28 +64,35 @@ def test_komega_bfs_known_answer_gpu(x, orc, ctx):
     assert np.linalg.norm(outlet - 0.5 * inlet) <= 0.1 * 1.5, (inlet, outlet)
 
 
-def komega_channel_case(x, mesh, iterations, precond="Jacobi"):
-    """Steady SIMPLE with RANS{KOmega} on a 3D channel: k and omega Dirichlet
-    at the inlet, Extrapolated at the outlet, omega wall functions and
-    k = nut = 0 on the walls."""
+def komega_channel_case(x, mesh, iterations, precond="Jacobi", wallfn=False, sst=False):
+    """Steady SIMPLE with RANS{KOmega} (or SST) on a 3D channel: k and omega
+    Dirichlet at the inlet, Extrapolated at the outlet, omega wall functions
+    on the walls, and k = nut = 0 there or (wallfn, nu 1e-5 so the wall
+    cells sit in the log layer) k and nut wall functions."""
     A = x.api
-    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=1e-3), turbulence=A.RANS(A.KOmega),
+    turb = A.RANS(A.KOmegaSST, walls=["walls"]) if sst else A.RANS(A.KOmega)
+    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=1e-5 if wallfn else 1e-3), turbulence=turb,
                       energy=A.Energy(A.Isothermal), domain=mesh)
+    kw = A.KWallFunction("walls") if wallfn else A.Dirichlet("walls", 0.0)
+    nw = A.NutWallFunction("walls") if wallfn else A.Dirichlet("walls", 0.0)
     BCs = A.assign(region=mesh,
                    U=[A.Dirichlet("inlet", [1.0, 0.0, 0.0]), A.Zerogradient("outlet"), A.Wall("walls", [0.0, 0.0, 0.0])],
                    p=[A.Zerogradient("inlet"), A.Dirichlet("outlet", 0.0), A.Wall("walls")],
-                   k=[A.Dirichlet("inlet", 0.01), A.Extrapolated("outlet"), A.Dirichlet("walls", 0.0)],
+                   k=[A.Dirichlet("inlet", 0.01), A.Extrapolated("outlet"), kw],
                    omega=[A.Dirichlet("inlet", 10.0), A.Extrapolated("outlet"), A.OmegaWallFunction("walls")],
-                   nut=[A.Dirichlet("inlet", 1e-3), A.Extrapolated("outlet"), A.Dirichlet("walls", 0.0)])
+                   nut=[A.Dirichlet("inlet", 1e-3), A.Extrapolated("outlet"), nw])
     pre = getattr(A, precond)
 
     def ss(s, relax):
         return A.SolverSetup(solver=s(), preconditioner=pre(), convergence=1e-7, relax=relax, rtol=1e-2)
 
     config = A.Configuration(solvers={"U": ss(A.Bicgstab, 0.7), "p": ss(A.Cg, 0.3), "k": ss(A.Bicgstab, 0.7),
-                                      "omega": ss(A.Bicgstab, 0.7)},
+                                      "omega": ss(A.Bicgstab, 0.7),
+                                      "y": A.SolverSetup(solver=A.Cg(), preconditioner=A.Jacobi(), convergence=1e-8,
+                                                         relax=0.9, rtol=1e-3)},
                              schemes={"U": A.Schemes(divergence=A.Upwind), "p": A.Schemes(),
-                                      "k": A.Schemes(divergence=A.Upwind), "omega": A.Schemes(divergence=A.Upwind)},
+                                      "k": A.Schemes(divergence=A.Upwind), "omega": A.Schemes(divergence=A.Upwind),
+                                      "y": A.Schemes()},
                              runtime=A.Runtime(iterations=iterations, write_interval=-1, time_step=1.0),
                              hardware=A.Hardware(backend=A.B200Backend()), boundaries=BCs)
     A.initialise_(model.momentum.U, [1.0, 0.0, 0.0])
@@ -175,3 +182,19 @@ def test_sst_bfs_transient_parity(x, orc, ctx, graph):
     ro, _ = o.piso_step(5)
     assert rel(rg, ro) <= TOL, (rg, ro)
     _check(x, g, o, KW_FIELDS + ("FIELD_WALLDIST", "FIELD_NUTF"))
+
+
+@pytest.mark.parametrize("sst", [False, True])
+def test_wall_functions_parity(x, orc, ctx, sst):
+    """KWallFunction and NutWallFunction (log-law wall cells) with k-omega
+    and k-omega SST."""
+    mesh = skewed_channel(x, n=(12, 7, 6), seed=17)
+    model, config = komega_channel_case(x, mesh, 6, wallfn=True, sst=sst)
+    cfg, keep = x.build_config(model, config)
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, False)
+    rg, _ = g.simple_iterate(6)
+    ro, _ = o.simple_iterate(6)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    _check(x, g, o)
+    walls = list(mesh.patch_range("walls"))
+    assert np.all(g.get_field(x._abi.FIELD_NUTF)[walls] > 0)  # the log-law branch ran

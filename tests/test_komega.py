@@ -7,7 +7,8 @@
   Midpoint gradients), outlet Ux = 0.5 inlet Ux within 0.1 Umag;
 * the wall-function constants (y_plus_laminar, RANS_functions.jl:42-45), the
   omega wall rows (constrain!, :376-429) and bound! (:2-41) on a few steps;
-* the wall functions that are not implemented are refused."""
+* the k and nut wall functions in the log layer (nutf = nut_wall(nu, y+));
+* k-omega SST on a channel: the wall distance and a few SIMPLE iterations."""
 import math
 import os
 
@@ -103,7 +104,7 @@ def test_komega_wall_rows(x, orc):
     yl = 11.0
     for _ in range(10):
         yl = math.log(max(yl * 9.8, 1.0)) / 0.41
-    assert bc.wall == (0.41, 0.075, 0.09 ** 0.25, yl)
+    assert bc.wall == (0.41, 0.075, 0.09 ** 0.25, yl, 9.8)
     assert 11.0 < yl < 12.0
     mesh = bfs_mesh(x, 5)
     model, config = komega_bfs_case(x, mesh, steps=3)
@@ -130,11 +131,28 @@ def test_komega_wall_rows(x, orc):
         assert w[c] == max(expect, np.spacing(1.0)), (c, w[c], expect)
 
 
-def test_unsupported_wall_functions(x):
-    with pytest.raises(NotImplementedError):
-        x.KWallFunction("wall")
-    with pytest.raises(NotImplementedError):
-        x.NutWallFunction("wall")
+def test_wall_function_values(x, orc):
+    """NutWallFunction faces hold nut_wall(nu, y+) of their cell's k
+    (RANS_functions.jl:61-63, 135-172) and KWallFunction keeps k finite:
+    a k-omega channel at nu = 1e-5 (wall cells in the log layer), oracle."""
+    from test_gpu_komega import komega_channel_case
+    from test_nonorth_oracle import skewed_channel
+    mesh = skewed_channel(x, n=(10, 6, 5), seed=5)
+    model, config = komega_channel_case(x, mesh, 4, wallfn=True)
+    cfg, keep = x.build_config(model, config)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    set_komega_fields(x, o, model)
+    res, _ = o.simple_iterate(4)
+    assert np.all(np.isfinite(res))
+    k = o.get_field(x._abi.FIELD_K)
+    nutf = o.get_field(x._abi.FIELD_NUTF)
+    kappa, E, c25 = 0.41, 9.8, 0.09 ** 0.25
+    yl = x.api.y_plus_laminar(E, kappa)
+    for f in mesh.patch_range("walls"):
+        c = mesh.boundary_cellsID[f]
+        yp = c25 * mesh.face_delta[f] * math.sqrt(k[c]) / 1e-5
+        expect = max(1e-5 * (yp * kappa / math.log(max(E * yp, 1.0001)) - 1.0), 0.0) if yp > yl else 0.0
+        assert nutf[f] == pytest.approx(expect, rel=1e-13, abs=1e-300)
 
 
 def sst_channel_case(x, mesh, iterations, precond="Jacobi", transient=False, walls=("walls",)):

@@ -28,6 +28,8 @@ BC_NEUMANN = 8
 BC_PERIODIC = 9
 BC_PERIODIC_PARENT = 10
 BC_OMEGA_WALL = 11
+BC_K_WALL = 12
+BC_NUT_WALL = 13
 
 TIME_STEADY, TIME_EULER = 0, 1
 DIV_LINEAR, DIV_UPWIND, DIV_LUST = 0, 1, 2
@@ -92,7 +94,7 @@ class BCDesc(C.Structure):
     _fields_ = [
         ("type", C.c_int32), ("patch", C.c_int32), ("value", C.c_double * 3),
         ("face_values", _pf64), ("face_map", _pi32), ("distance", C.c_double * 3),
-        ("partner_patch", C.c_int32), ("wall", C.c_double * 4),
+        ("partner_patch", C.c_int32), ("wall", C.c_double * 5),
     ]
 
 

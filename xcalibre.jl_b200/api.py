@@ -320,7 +320,7 @@ class BC:
     face_map: np.ndarray | None = None
     distance: np.ndarray | None = None
     partner: str | None = None
-    wall: tuple | None = None  # OmegaWallFunction: (kappa, beta1, cmu^0.25, yPlusLam)
+    wall: tuple | None = None  # wall functions: (kappa, beta1, cmu^0.25, yPlusLam, E)
 
 
 def Dirichlet(name, value):
@@ -355,19 +355,27 @@ def y_plus_laminar(E: float, kappa: float) -> float:
     return yL
 
 
+def _wall_consts(kappa, beta1, cmu, E):
+    return (float(kappa), float(beta1), float(cmu) ** 0.25, y_plus_laminar(float(E), float(kappa)), float(E))
+
+
 def OmegaWallFunction(name, kappa=0.41, beta1=0.075, cmu=0.09, B=5.2, E=9.8):
     """OmegaWallFunction (Discretise_0_types.jl:83-113): the wall cell's
     omega fixed to omega_log or omega_vis by y+ (constrain!)."""
-    return BC(_abi.BC_OMEGA_WALL, name, 0.0,
-              wall=(float(kappa), float(beta1), float(cmu) ** 0.25, y_plus_laminar(float(E), float(kappa))))
+    return BC(_abi.BC_OMEGA_WALL, name, 0.0, wall=_wall_consts(kappa, beta1, cmu, E))
 
 
-def KWallFunction(name, **kw):
-    raise NotImplementedError("KWallFunction (wall-function production, RANS_functions.jl:66-117) is not implemented")
+def KWallFunction(name, kappa=0.41, beta1=0.075, cmu=0.09, B=5.2, E=9.8):
+    """KWallFunction (Discretise_0_types.jl:39-66): zero gradient for k, and
+    the wall cell's production from the log law (set_production!,
+    RANS_functions.jl:66-117)."""
+    return BC(_abi.BC_K_WALL, name, 0.0, wall=_wall_consts(kappa, beta1, cmu, E))
 
 
-def NutWallFunction(name, **kw):
-    raise NotImplementedError("NutWallFunction (wall eddy viscosity, RANS_functions.jl:119-172) is not implemented")
+def NutWallFunction(name, kappa=0.41, beta1=0.075, cmu=0.09, B=5.2, E=9.8):
+    """NutWallFunction: zero gradient for nut, and the wall face's nutf from
+    the log law (correct_nut_wall!, RANS_functions.jl:119-172)."""
+    return BC(_abi.BC_NUT_WALL, name, 0.0, wall=_wall_consts(kappa, beta1, cmu, E))
 
 
 def Empty(name):
@@ -525,7 +533,7 @@ def _bc_array(mesh: Mesh3, bcs, ncomp: int, keep: list):
                 d.distance[c] = float(bc.distance[c])
             d.partner_patch = mesh.patch_index(bc.partner)
         if bc.wall is not None:
-            for c in range(4):
+            for c in range(5):
                 d.wall[c] = float(bc.wall[c])
     return arr
 

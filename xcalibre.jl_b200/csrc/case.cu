@@ -530,7 +530,7 @@ static void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int
     for (int b = 0; b < nbc; ++b) {
         const xcal_bc& bc = bcs[b];
         if (bc.patch < 0 || bc.patch >= np) fail(XCAL_ERR_INVALID, "bc: patch index out of range");
-        if (bc.type < XCAL_BC_DIRICHLET || bc.type > XCAL_BC_OMEGA_WALL)
+        if (bc.type < XCAL_BC_DIRICHLET || bc.type > XCAL_BC_NUT_WALL)
             fail(XCAL_ERR_INVALID, "bc: unknown type");
         if (ncomp == 3 && bc.type == XCAL_BC_NEUMANN)
             fail(XCAL_ERR_UNSUPPORTED, "Neumann boundary condition for vector fields is not implemented");
@@ -652,9 +652,13 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     build_bc_table(bcU, *m, cfg.bc_U, cfg.n_bc_U, 3, &U, stream);
     build_bc_table(bcP, *m, cfg.bc_p, cfg.n_bc_p, 1, &P, stream);
     build_bc_table(bcNut, *m, cfg.bc_nut, cfg.n_bc_nut, 1, nullptr, stream);
-    for (const BCTable* T : {&bcU, &bcP, &bcNut})
+    for (const BCTable* T : {&bcU, &bcP})
         for (const xcal_bc& bc : T->src)
-            if (bc.type == XCAL_BC_OMEGA_WALL) fail(XCAL_ERR_INVALID, "OmegaWallFunction applies to omega only");
+            if (bc.type == XCAL_BC_OMEGA_WALL || bc.type == XCAL_BC_K_WALL || bc.type == XCAL_BC_NUT_WALL)
+                fail(XCAL_ERR_INVALID, "wall functions apply to k, omega and nut only");
+    for (const xcal_bc& bc : bcNut.src)
+        if (bc.type == XCAL_BC_OMEGA_WALL || bc.type == XCAL_BC_K_WALL)
+            fail(XCAL_ERR_INVALID, "OmegaWallFunction / KWallFunction do not apply to nut");
     if (rans_kw()) {
         // RANS{KOmega} / RANS{KOmegaSST}: k / omega share the p system
         build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, nullptr, stream);
@@ -943,6 +947,45 @@ void Case::build_wall_table(const DevMesh& m) {
         wcell.upload(cells, stream);
         wpar.upload(par, stream);
     }
+    // KWallFunction (set_production!, RANS_functions.jl:66-117): the last
+    // face per cell in BC then face order; NutWallFunction faces
+    std::vector<int> kwin(m.nC, -1), kf, kc, nf;
+    std::vector<double> kp, np_;
+    for (const xcal_bc& bc : bcK.src) {
+        if (bc.type != XCAL_BC_K_WALL) continue;
+        const int start = m.patch_start[bc.patch], count = m.patch_count[bc.patch];
+        for (int f = start; f < start + count; ++f) {
+            const int c = m.bcell[f];
+            if (kwin[c] < 0) {
+                kwin[c] = (int)kc.size();
+                kc.push_back(c);
+                kf.push_back(f);
+                kp.insert(kp.end(), {0, 0, 0, 0});
+            }
+            const int t = kwin[c];
+            kf[t] = f;
+            for (int q = 0; q < 4; ++q) kp[4 * t + q] = q == 0 ? bc.wall[0] : bc.wall[q + 1];
+        }
+    }
+    for (const xcal_bc& bc : bcNut.src) {
+        if (bc.type != XCAL_BC_NUT_WALL) continue;
+        const int start = m.patch_start[bc.patch], count = m.patch_count[bc.patch];
+        for (int f = start; f < start + count; ++f) {
+            nf.push_back(f);
+            for (double v : {bc.wall[0], bc.wall[2], bc.wall[3], bc.wall[4]}) np_.push_back(v);
+        }
+    }
+    nkwall = (int)kc.size();
+    nnutwall = (int)nf.size();
+    if (nkwall) {
+        kwcell.upload(kc, stream);
+        kwface.upload(kf, stream);
+        kwpar.upload(kp, stream);
+    }
+    if (nnutwall) {
+        nwface.upload(nf, stream);
+        nwpar.upload(np_, stream);
+    }
 }
 
 // turbulence!(::KOmegaModel) after grad!(gradU) (RANS_kOmega.jl:146-210):
@@ -969,6 +1012,8 @@ void Case::komega() {
         launch_kw_sources(stream, mesh->nC, g, nut.p, omega.p, Pk.p, Pw.p, Dk.p, Dw.p, cfg.kw_alpha1, cfg.kw_beta1,
                           cfg.kw_beta_star);
     }
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    launch_kwall_production(stream, nkwall, mv(), kwcell.p, kwface.p, kwpar.p, kfld.p, Ucp, cfg.nu, Pk.p);
     for (int e : {(int)XCAL_EQN_OMEGA, (int)XCAL_EQN_K}) {
         const bool w = e == XCAL_EQN_OMEGA;
         double* phi = w ? omega.p : kfld.p;
@@ -993,6 +1038,7 @@ void Case::komega() {
     else
         launch_kw_nut(stream, mesh->nC, kfld.p, omega.p, nut.p);
     launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
+    launch_nutwall(stream, nnutwall, mv(), nwface.p, nwpar.p, kfld.p, cfg.nu, nutf.p, nueff.p);
 }
 
 // grad! of a scalar with its BCs (Calculate_0_gradient.jl): Gauss, or the

@@ -131,6 +131,11 @@ struct Case {
     DBuf<double> yw, yphi, F1b, F2b, Omb, D2b, gkv[3], gwv[3], fscr;
     DBuf<int> wcell;
     int nwall = 0;
+    // KWallFunction cells (last face in BC / face order) and NutWallFunction
+    // faces, with kappa, cmu^0.25, yPlusLam, E per entry
+    DBuf<int> kwcell, kwface, nwface;
+    DBuf<double> kwpar, nwpar;
+    int nkwall = 0, nnutwall = 0;
     double res_k = 0.0, res_omega = 0.0;
     bool initialised = false;
     int iteration = 0;

@@ -64,6 +64,21 @@ __host__ __device__ __forceinline__ double det_exp_neg(double y) {
     for (int n = 14; n >= 1; --n) p = 1.0 + (r / (double)n) * p;
     return ldexp(p, (int)k);
 }
+// log(x) for x > 0 from frexp (exact) and +, *, /: x = 2^e m with
+// m in [sqrt(1/2), sqrt(2)), log m = 2 atanh(s), s = (m - 1) / (m + 1), by
+// its series to s^29
+__host__ __device__ __forceinline__ double det_log(double x) {
+    int e = 0;
+    double m = frexp(x, &e);
+    if (m < 0.70710678118654752) {
+        m = 2.0 * m;
+        e -= 1;
+    }
+    const double s = (m - 1.0) / (m + 1.0), s2 = s * s;
+    double t = 0.0;
+    for (int n = 29; n >= 3; n -= 2) t = (t + 1.0 / (double)n) * s2;
+    return (double)e * 0.6931471805599453 + 2.0 * (s + s * t);
+}
 __host__ __device__ __forceinline__ double det_tanh_pos(double x) {
     if (x > 20.0) return 1.0;
     const double e = det_exp_neg(-2.0 * x);

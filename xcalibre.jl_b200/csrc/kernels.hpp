@@ -62,6 +62,12 @@ void launch_sst_fields(cudaStream_t s, int nC, const double* const g[9], const d
 void launch_sst_nut(cudaStream_t s, int nC, const double* k, const double* omega, const double* F2, const double* Om,
                     double al1, double* nut);
 void launch_walldist(cudaStream_t s, int nC, const double* phi, const double* const g[3], double* y);
+// wall functions: KWallFunction production per wall cell, NutWallFunction
+// nutf (and nueff) per wall face; par: kappa, cmu^0.25, yPlusLam, E
+void launch_kwall_production(cudaStream_t s, int nw, const MeshView& m, const int* cell, const int* face,
+                             const double* par, const double* k, const double* const U[3], double nu, double* Pk);
+void launch_nutwall(cudaStream_t s, int nw, const MeshView& m, const int* face, const double* par, const double* k,
+                    double nu, double* nutf, double* nueff);
 void launch_omega_constrain(cudaStream_t s, int nw, const CSRView& A, const int* wcell, const double* par,
                             const double* k, double nu, double* nz, double* b);
 void launch_bound(cudaStream_t s, const MeshView& m, const double* old, double* v);

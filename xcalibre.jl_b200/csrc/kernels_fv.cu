@@ -488,6 +488,8 @@ __device__ void bc_scalar_transport(const MeshView& m, const BCView& bc, int f, 
         case XCAL_BC_WALL:  // wall.jl:43-102 (scalar)
         case XCAL_BC_ZEROGRADIENT:
         case XCAL_BC_SYMMETRY:
+        case XCAL_BC_K_WALL:  // Discretise_3_boundary_conditions.jl:12-51 (Laplacian (0, 0))
+        case XCAL_BC_NUT_WALL:
             ap_d = 1.0 * mdot[f];
             break;
         case XCAL_BC_EXTRAPOLATED:  // extrapolated.jl:21-45
@@ -665,6 +667,50 @@ __global__ void k_walldist(int nC, const double* __restrict__ phi, const double*
     y[i] = (-gm) + sqrt(gm * gm + 2.0 * phi[i]);
 }
 
+// nut_wall (RANS_functions.jl:61-63)
+__device__ __forceinline__ double nut_wall(double nu, double yplus, double kappa, double E) {
+    return jl_max(nu * (((yplus * kappa) / det_log(jl_max(E * yplus, 1.0 + 1e-4))) - 1.0), 0.0);
+}
+
+// set_production!(Pk, KWallFunction) (RANS_functions.jl:84-117) per wall
+// cell (its constraining face f): log-law production or 0 below yPlusLam;
+// par per entry: kappa, cmu^0.25, yPlusLam, E
+__global__ void k_kwall_production(int nw, MeshView m, const int* __restrict__ cell, const int* __restrict__ face,
+                                   const double* __restrict__ par, const double* __restrict__ k,
+                                   const double* __restrict__ Ux, const double* __restrict__ Uy,
+                                   const double* __restrict__ Uz, double nu, double* Pk) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nw) return;
+    const int c = cell[t], f = face[t];
+    const double kappa = par[4 * t], c25 = par[4 * t + 1], yPlusLam = par[4 * t + 2], E = par[4 * t + 3];
+    const double delta = m.delta[f];
+    const double nx = m.nx[f], ny = m.ny[f], nz = m.nz[f];
+    const double sk = sqrt(k[c]);
+    const double uStar = c25 * sk;
+    const double dUdy = uStar / (kappa * delta);
+    const double yplus = ((c25 * delta) * sk) / nu;
+    const double nutw = nut_wall(nu, yplus, kappa, E);
+    const double ux = Ux[c] - 0.0, uy = Uy[c] - 0.0, uz = Uz[c] - 0.0;
+    const double dn = ux * nx + uy * ny + uz * nz;
+    const double gx = (ux - dn * nx) / delta, gy = (uy - dn * ny) / delta, gz = (uz - dn * nz) / delta;
+    const double mag = sqrt(gx * gx + gy * gy + gz * gz);
+    Pk[c] = yplus > yPlusLam ? ((nu + nutw) * mag) * dUdy : 0.0;
+}
+
+// correct_nut_wall!(nutf, NutWallFunction) (RANS_functions.jl:135-172) per
+// wall face, then nueff = nu + nutf there
+__global__ void k_nutwall(int nw, MeshView m, const int* __restrict__ face, const double* __restrict__ par,
+                          const double* __restrict__ k, double nu, double* nutf, double* nueff) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nw) return;
+    const int f = face[t], c = m.owner[f];
+    const double kappa = par[4 * t], c25 = par[4 * t + 1], yPlusLam = par[4 * t + 2], E = par[4 * t + 3];
+    const double yplus = ((c25 * m.delta[f]) * sqrt(k[c])) / nu;
+    const double v = yplus > yPlusLam ? nut_wall(nu, yplus, kappa, E) : 0.0;
+    nutf[f] = v;
+    nueff[f] = nu + v;
+}
+
 // nut = k / omega (RANS_kOmega.jl:201)
 __global__ void k_kw_nut(int nC, const double* __restrict__ k, const double* __restrict__ omega, double* nut) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -818,6 +864,8 @@ __global__ void k_interp_scalar(MeshView m, BCView bc, const double* __restrict_
             case XCAL_BC_ZEROGRADIENT:
             case XCAL_BC_EXTRAPOLATED:
             case XCAL_BC_OMEGA_WALL:
+            case XCAL_BC_K_WALL:
+            case XCAL_BC_NUT_WALL:
             case XCAL_BC_SYMMETRY:
                 v = phi[o];
                 break;
@@ -1386,6 +1434,18 @@ void launch_sst_fields(cudaStream_t s, int nC, const double* const g[9], const d
 void launch_sst_nut(cudaStream_t s, int nC, const double* k, const double* omega, const double* F2, const double* Om,
                     double al1, double* nut) {
     k_sst_nut<<<nblk(nC), TPB, 0, s>>>(nC, k, omega, F2, Om, al1, nut);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_kwall_production(cudaStream_t s, int nw, const MeshView& m, const int* cell, const int* face,
+                             const double* par, const double* k, const double* const U[3], double nu, double* Pk) {
+    if (nw <= 0) return;
+    k_kwall_production<<<nblk(nw), TPB, 0, s>>>(nw, m, cell, face, par, k, U[0], U[1], U[2], nu, Pk);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_nutwall(cudaStream_t s, int nw, const MeshView& m, const int* face, const double* par, const double* k,
+                    double nu, double* nutf, double* nueff) {
+    if (nw <= 0) return;
+    k_nutwall<<<nblk(nw), TPB, 0, s>>>(nw, m, face, par, k, nu, nutf, nueff);
     XCAL_CHECK_LAUNCH();
 }
 void launch_walldist(cudaStream_t s, int nC, const double* phi, const double* const g[3], double* y) {
