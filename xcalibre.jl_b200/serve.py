@@ -139,6 +139,8 @@ class Server:
     keep_fields: bool = False
     timeline: list = field(default_factory=list)  # (t, active, queued, used bytes)
     phase_ms: dict = field(default_factory=dict)  # batch phase times (host wall, ms)
+    admit_s: float = 0.0    # wall time spent admitting (mesh build, case set-up, batch.add)
+    iterate_s: float = 0.0  # wall time spent in batch iterations
 
     def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
@@ -154,6 +156,7 @@ class Server:
                 while pending and (pending[0].arrival <= now or not realtime):
                     queue.append(pending.popleft())
                 # admission, in arrival order, by device-memory footprint
+                ta = time.perf_counter()
                 while queue and len(active) < self.max_cases:
                     req = queue[0]
                     mesh = req.build()
@@ -175,12 +178,15 @@ class Server:
                     used += est
                     queue.popleft()
                     active.append(_Active(req, case, dm, (cfg, keep), est, time.perf_counter() - t0))
+                self.admit_s += time.perf_counter() - ta
                 self.timeline.append((time.perf_counter() - t0, len(active), len(queue), used))
                 if not active:
                     if pending and realtime:
                         time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0))))
                     continue
+                ti = time.perf_counter()
                 res, conv = batch.simple_iterate()
+                self.iterate_s += time.perf_counter() - ti
                 self.phase_ms = batch.timings()
                 done_t = time.perf_counter() - t0
                 finished = []
