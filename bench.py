@@ -319,7 +319,7 @@ def les_measure(x, A, args, local):
     events on the case stream after 3 warm-up steps."""
     import torch
     n = args.les_size
-    mesh = x.build_mesh3(x.periodic_box_polymesh(n, seed=0))
+    mesh = x.build_mesh3(x.periodic_box_polymesh(n, seed=0), device=local)
     U0 = x.cases.fourier_field(mesh, seed=0)
     out = {"workload": f"periodic LES box 2pi^3, {n}^3 hex = {mesh.n_cells} cells, PISO x2 correctors, "
                        f"Smagorinsky 0.17, nu 1e-4, CFL 0.5, mixed precision, graph per step"}
@@ -472,7 +472,7 @@ def main():
     n = args.size
     t_mesh = time.perf_counter()
     pm = x.channel_polymesh(n, n, n, seed=0)
-    mesh = x.build_mesh3(pm)
+    mesh = x.build_mesh3(pm, device=local)  # geometry on the GPU (identical to the host build)
     t_mesh = time.perf_counter() - t_mesh
     primary = args.precision
     r, case, dm, model = measure(x, A, mesh, primary, args, local, world, torch.cuda.ExternalStream)

@@ -307,6 +307,11 @@ int32_t xcal_foam_mesh_sizes(const xcal_polymesh_desc* pm, int32_t* sizes);
  * FoamMesh_3_generate.jl, FoamMesh_4_geometry.jl, Mesh_1_functions.jl:20-51)
  * into caller buffers.  Needs no GPU. */
 int32_t xcal_foam_mesh_build(const xcal_polymesh_desc* pm, const xcal_mesh_buffers* out);
+/* the same Mesh3 for large meshes, with its geometry (cell centres, face fan
+ * geometry, weights, deltas, volumes) computed on GPU `device` by the same
+ * operations in the same order: outputs identical to xcal_foam_mesh_build.
+ * The connectivity stays on the host; inputs and outputs are host arrays. */
+int32_t xcal_foam_mesh_build_device(int32_t device, const xcal_polymesh_desc* pm, const xcal_mesh_buffers* out);
 
 /* ---- mesh ----------------------------------------------------------------*/
 /* adapt(backend, mesh) (docs/src/user_guide/1_preprocessing.md:88): copies

@@ -28,6 +28,7 @@ SIGNATURES = {
     "xcal_version": (C.c_char_p, []),
     "xcal_foam_mesh_sizes": (_i32, [C.POINTER(_abi.PolyMeshDesc), _pi]),
     "xcal_foam_mesh_build": (_i32, [C.POINTER(_abi.PolyMeshDesc), C.POINTER(_abi.MeshBuffers)]),
+    "xcal_foam_mesh_build_device": (_i32, [_i32, C.POINTER(_abi.PolyMeshDesc), C.POINTER(_abi.MeshBuffers)]),
     "xcal_mesh_upload": (_i32, [_vp, C.POINTER(_abi.MeshDesc), C.POINTER(_vp)]),
     "xcal_mesh_destroy": (_i32, [_vp]),
     "xcal_case_create": (_i32, [_vp, _vp, C.POINTER(_abi.ConfigDesc), C.POINTER(_vp)]),

@@ -63,8 +63,10 @@ class Mesh3:
         return f"{self.dim}D Mesh with:\n-> {self.n_cells} cells\n-> {self.n_faces} faces\n-> {n_nodes} nodes"
 
 
-def build_mesh3(pm: PolyMesh) -> Mesh3:
-    """FOAM3D_mesh: polyMesh -> Mesh3 (Float64, 0-based) via the native importer."""
+def build_mesh3(pm: PolyMesh, device: int | None = None) -> Mesh3:
+    """FOAM3D_mesh: polyMesh -> Mesh3 (Float64, 0-based) via the native
+    importer; with ``device`` the geometry is computed on that GPU (the same
+    result, for large meshes)."""
     from ._lib import lib
     keep = []
 
@@ -95,7 +97,9 @@ def build_mesh3(pm: PolyMesh) -> Mesh3:
               patch_count=np.empty(len(pm.patch_sizes), np.int32), points=pts)
     out = _abi.MeshBuffers(**{f: _abi.ptr(getattr(m, f), C.c_int32 if getattr(m, f).dtype == np.int32 else C.c_double)
                               for f, _ in _abi.MeshBuffers._fields_})
-    if lib().xcal_foam_mesh_build(C.byref(desc), C.byref(out)) != 0:
-        raise ValueError("invalid polyMesh (patch sizes, node or cell indices)")
+    code = (lib().xcal_foam_mesh_build(C.byref(desc), C.byref(out)) if device is None else
+            lib().xcal_foam_mesh_build_device(int(device), C.byref(desc), C.byref(out)))
+    if code != 0:
+        raise ValueError(f"invalid polyMesh (patch sizes, node or cell indices), or the device build failed ({code})")
     m.polymesh = pm
     return m

@@ -148,10 +148,11 @@ def read_polymesh(path: str, scale: float = 1.0) -> PolyMesh:
                     patch_names=[p[0] for p in patches], patch_sizes=[p[1] for p in patches])
 
 
-def FOAM3D_mesh(path: str, scale: float = 1.0) -> Mesh3:
+def FOAM3D_mesh(path: str, scale: float = 1.0, device: int | None = None) -> Mesh3:
     """FOAM3D_mesh(meshFile; scale) (src/FoamMesh/FoamMesh_5_build.jl:21-27):
-    read a polyMesh directory and build the Mesh3 (Float64, 0-based)."""
-    return build_mesh3(read_polymesh(path, scale))
+    read a polyMesh directory and build the Mesh3 (Float64, 0-based); with
+    ``device`` the geometry is computed on that GPU."""
+    return build_mesh3(read_polymesh(path, scale), device=device)
 
 
 _HEADER = """/*--------------------------------*- C++ -*----------------------------------*\\
