@@ -373,7 +373,7 @@ def serve_measure(x, args, local):
                           f"Re U[100,2000], aspect U[1,4], Poisson {args.serve_rate:g}/s, mixed, resid 1e-6",
               "rate_per_s": args.serve_rate, "budget_bytes": 40 << 30, "max_cases": 64,
               "max_active": max((t[1] for t in srv.timeline), default=0),
-              "admission_s": srv.admit_s, "iterate_s": srv.iterate_s,
+              "admission_s": srv.admit_s, "iterate_s": srv.iterate_s, "retire_s": srv.retire_s,
               "gpu_launches": x.launch_count() - l0})
     return s
 

@@ -141,12 +141,18 @@ class Server:
     phase_ms: dict = field(default_factory=dict)  # batch phase times (host wall, ms)
     admit_s: float = 0.0    # wall time spent admitting (mesh build, case set-up, batch.add)
     iterate_s: float = 0.0  # wall time spent in batch iterations
+    retire_s: float = 0.0   # wall time spent retiring finished cases (batch.remove, freeing)
+    # finished cases leave the batch at once; freeing their device memory
+    # (which waits for the device) is deferred until this many are pending,
+    # or the run ends, so it does not stall the running batch every time
+    free_every: int = 16
 
     def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         queue: deque = deque()
         active: list[_Active] = []
         results: list[Result] = []
+        retired: list = []  # (case, device mesh) out of the batch, not yet freed
         batch = A.Batch(self.ctx, self.max_cases, self.budget_bytes)
         used = 0
         t0 = time.perf_counter()
@@ -194,17 +200,26 @@ class Server:
                     a.iters += 1
                     if conv[k] or a.iters >= self.max_iters:
                         finished.append((a, bool(conv[k]), res[k].copy()))
+                tr = time.perf_counter()
                 for a, ok, r in finished:
                     U = a.case.get_field(A._abi.FIELD_U) if self.keep_fields else None
                     p = a.case.get_field(A._abi.FIELD_P) if self.keep_fields else None
                     results.append(Result(a.req.rid, a.req.n_cells, a.req.arrival, a.admitted, done_t, a.iters, ok,
                                           r, U, p))
                     batch.remove(a.case)
-                    a.case.close()
-                    a.dmesh.close()
+                    retired.append((a.case, a.dmesh))
                     used -= a.charge
                     active.remove(a)
+                if len(retired) >= self.free_every or (not active and not queue and not pending):
+                    for case, dm in retired:
+                        case.close()
+                        dm.close()
+                    retired.clear()
+                self.retire_s += time.perf_counter() - tr
         finally:
+            for case, dm in retired:
+                case.close()
+                dm.close()
             for a in active:
                 try:
                     batch.remove(a.case)
