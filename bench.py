@@ -374,6 +374,7 @@ def serve_measure(x, args, local):
               "rate_per_s": args.serve_rate, "budget_bytes": 40 << 30, "max_cases": 64,
               "max_active": max((t[1] for t in srv.timeline), default=0),
               "admission_s": srv.admit_s, "iterate_s": srv.iterate_s, "retire_s": srv.retire_s,
+              "idle_s": srv.idle_s, "cleanup_s": srv.cleanup_s,
               "gpu_launches": x.launch_count() - l0})
     return s
 

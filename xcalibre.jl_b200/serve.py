@@ -23,6 +23,7 @@ is the same alone and in the mix.
 from __future__ import annotations
 
 import time
+from concurrent.futures import ThreadPoolExecutor
 from collections import deque
 from dataclasses import dataclass, field
 
@@ -142,10 +143,19 @@ class Server:
     admit_s: float = 0.0    # wall time spent admitting (mesh build, case set-up, batch.add)
     iterate_s: float = 0.0  # wall time spent in batch iterations
     retire_s: float = 0.0   # wall time spent retiring finished cases (batch.remove, freeing)
+    idle_s: float = 0.0     # wall time waiting for arrivals with nothing to run
+    cleanup_s: float = 0.0  # wall time freeing what is left at the end
     # finished cases leave the batch at once; freeing their device memory
     # (which waits for the device) is deferred until this many are pending,
     # or the run ends, so it does not stall the running batch every time
     free_every: int = 16
+    # the last case of a drained stream leaves the batch and finishes alone
+    # in graph mode (device-driven Krylov loops, no host round trip per
+    # chunk; its iterates are the same bit for bit)
+    solo_tail: bool = True
+    # meshes are built on this many host threads from the moment a request
+    # arrives, overlapping the batch iterations (0: at admission)
+    build_threads: int = 2
 
     def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
@@ -153,6 +163,8 @@ class Server:
         active: list[_Active] = []
         results: list[Result] = []
         retired: list = []  # (case, device mesh) out of the batch, not yet freed
+        pool = ThreadPoolExecutor(self.build_threads) if self.build_threads > 0 else None
+        builds: dict = {}
         batch = A.Batch(self.ctx, self.max_cases, self.budget_bytes)
         used = 0
         t0 = time.perf_counter()
@@ -160,12 +172,16 @@ class Server:
             while pending or queue or active:
                 now = time.perf_counter() - t0
                 while pending and (pending[0].arrival <= now or not realtime):
-                    queue.append(pending.popleft())
+                    req = pending.popleft()
+                    if pool is not None:
+                        builds[req.rid] = pool.submit(req.build)
+                    queue.append(req)
                 # admission, in arrival order, by device-memory footprint
                 ta = time.perf_counter()
                 while queue and len(active) < self.max_cases:
                     req = queue[0]
-                    mesh = req.build()
+                    fut = builds.pop(req.rid, None)
+                    mesh = fut.result() if fut is not None else req.build()
                     est = A.footprint_estimate(mesh, self.precision, dilu_U=True, dilu_p=False)
                     if est > self.budget_bytes:
                         raise ValueError(f"request {req.rid} needs {est} bytes, more than the budget")
@@ -188,7 +204,27 @@ class Server:
                 self.timeline.append((time.perf_counter() - t0, len(active), len(queue), used))
                 if not active:
                     if pending and realtime:
+                        tw = time.perf_counter()
                         time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0))))
+                        self.idle_s += time.perf_counter() - tw
+                    continue
+                if self.solo_tail and len(active) == 1 and not queue and not pending:
+                    a = active[0]
+                    ti = time.perf_counter()
+                    batch.remove(a.case)
+                    a.case.set_graph_mode(True)
+                    r, ok = a.case.simple_iterate(max(0, self.max_iters - a.iters))
+                    self.iterate_s += time.perf_counter() - ti
+                    a.iters += len(r)
+                    done_t = time.perf_counter() - t0
+                    U = a.case.get_field(A._abi.FIELD_U) if self.keep_fields else None
+                    p = a.case.get_field(A._abi.FIELD_P) if self.keep_fields else None
+                    last = r[-1].copy() if len(r) else np.zeros(4)
+                    results.append(Result(a.req.rid, a.req.n_cells, a.req.arrival, a.admitted, done_t, a.iters, ok,
+                                          last, U, p))
+                    retired.append((a.case, a.dmesh))
+                    used -= a.charge
+                    active.remove(a)
                     continue
                 ti = time.perf_counter()
                 res, conv = batch.simple_iterate()
@@ -217,6 +253,9 @@ class Server:
                     retired.clear()
                 self.retire_s += time.perf_counter() - tr
         finally:
+            tc = time.perf_counter()
+            if pool is not None:
+                pool.shutdown(wait=True)
             for case, dm in retired:
                 case.close()
                 dm.close()
@@ -228,6 +267,7 @@ class Server:
                 a.case.close()
                 a.dmesh.close()
             batch.close()
+            self.cleanup_s += time.perf_counter() - tc
         self.wall = time.perf_counter() - t0
         return sorted(results, key=lambda r: r.rid)
 
