@@ -118,6 +118,16 @@ class Result:
         return self.finished - self.arrival
 
 
+class _Done:
+    """A finished result with the interface of a future."""
+
+    def __init__(self, value):
+        self.value = value
+
+    def result(self):
+        return self.value
+
+
 @dataclass
 class _Active:
     req: Request
@@ -153,9 +163,27 @@ class Server:
     # in graph mode (device-driven Krylov loops, no host round trip per
     # chunk; its iterates are the same bit for bit)
     solo_tail: bool = True
-    # meshes are built on this many host threads from the moment a request
-    # arrives, overlapping the batch iterations (0: at admission)
+    # cases (mesh, configuration, device mesh, case, initial fields) are set
+    # up on this many host threads for the first `prepare_ahead` queued
+    # requests, overlapping the batch iterations (0 threads: at admission);
+    # the budget check and batch.add stay on this thread
     build_threads: int = 2
+    prepare_ahead: int = 4
+
+    def _prepare(self, req: Request):
+        """A request's case ready for batch.add: (footprint, case, device
+        mesh, configuration kept alive); case None when it exceeds the budget."""
+        mesh = req.build()
+        est = A.footprint_estimate(mesh, self.precision, dilu_U=True, dilu_p=False)
+        if est > self.budget_bytes:
+            return est, None, None, None
+        model, config, pref = req.config(self.precision, self.max_iters, self.convergence)
+        cfg, keep = A.build_config(model, config, pref=pref)
+        dm = A.DeviceMesh(self.ctx, mesh)
+        case = A.Case(dm, cfg)
+        case.set_field(A._abi.FIELD_U, model.momentum.U)
+        case.set_field(A._abi.FIELD_P, model.momentum.p)
+        return est, case, dm, (cfg, keep)
 
     def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
@@ -172,34 +200,27 @@ class Server:
             while pending or queue or active:
                 now = time.perf_counter() - t0
                 while pending and (pending[0].arrival <= now or not realtime):
-                    req = pending.popleft()
-                    if pool is not None:
-                        builds[req.rid] = pool.submit(req.build)
-                    queue.append(req)
+                    queue.append(pending.popleft())
+                if pool is not None:
+                    for req in list(queue)[: self.prepare_ahead]:
+                        if req.rid not in builds:
+                            builds[req.rid] = pool.submit(self._prepare, req)
                 # admission, in arrival order, by device-memory footprint
                 ta = time.perf_counter()
                 while queue and len(active) < self.max_cases:
                     req = queue[0]
-                    fut = builds.pop(req.rid, None)
-                    mesh = fut.result() if fut is not None else req.build()
-                    est = A.footprint_estimate(mesh, self.precision, dilu_U=True, dilu_p=False)
-                    if est > self.budget_bytes:
+                    fut = builds.get(req.rid)
+                    if fut is None:
+                        fut = builds[req.rid] = _Done(self._prepare(req))
+                    est, case, dm, keep = fut.result()
+                    if case is None:
                         raise ValueError(f"request {req.rid} needs {est} bytes, more than the budget")
-                    if used + est > self.budget_bytes:
-                        break
-                    model, config, pref = req.config(self.precision, self.max_iters, self.convergence)
-                    cfg, keep = A.build_config(model, config, pref=pref)
-                    dm = A.DeviceMesh(self.ctx, mesh)
-                    case = A.Case(dm, cfg)
-                    case.set_field(A._abi.FIELD_U, model.momentum.U)
-                    case.set_field(A._abi.FIELD_P, model.momentum.p)
-                    if not batch.add(case, est):
-                        case.close()
-                        dm.close()
-                        break
+                    if used + est > self.budget_bytes or not batch.add(case, est):
+                        break  # stays prepared until it fits
+                    builds.pop(req.rid)
                     used += est
                     queue.popleft()
-                    active.append(_Active(req, case, dm, (cfg, keep), est, time.perf_counter() - t0))
+                    active.append(_Active(req, case, dm, keep, est, time.perf_counter() - t0))
                 self.admit_s += time.perf_counter() - ta
                 self.timeline.append((time.perf_counter() - t0, len(active), len(queue), used))
                 if not active:
@@ -256,6 +277,11 @@ class Server:
             tc = time.perf_counter()
             if pool is not None:
                 pool.shutdown(wait=True)
+            for fut in builds.values():  # set up but never admitted
+                est, case, dm, keep = fut.result()
+                if case is not None:
+                    case.close()
+                    dm.close()
             for case, dm in retired:
                 case.close()
                 dm.close()
