@@ -56,7 +56,9 @@ def parse():
     ap.add_argument("--serve-cases", type=int, default=16, help="serving stream: requests (0 = skip)")
     ap.add_argument("--serve-nmax", type=float, default=3e4)
     ap.add_argument("--serve-rate", type=float, default=8.0)
-    ap.add_argument("--only", choices=["les", "serving", "batch"], default=None,
+    ap.add_argument("--converge-cap", type=int, default=1200,
+                    help="time-to-convergence block: SIMPLE iteration cap per precision (0 = skip)")
+    ap.add_argument("--only", choices=["les", "serving", "batch", "converge"], default=None,
                     help="run one secondary workload alone and print its block as the line (profiling)")
     return ap.parse_args()
 
@@ -74,12 +76,13 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+        self.path = None
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
+            import tempfile
+            fd, self.path = tempfile.mkstemp(prefix=f"xcal_clocks_gpu{self.gpu}_", suffix=".csv")
+            self.f = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-i", str(self.gpu), "-lms", "200"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
@@ -96,10 +99,15 @@ class ClockSampler:
             self.proc.kill()
         self.f.close()
         rows = []
-        for ln in open(self.path):
-            p = [s.strip() for s in ln.split(",")]
-            if len(p) >= 9:
-                rows.append(p)
+        with open(self.path) as f:
+            for ln in f:
+                p = [s.strip() for s in ln.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -279,7 +287,24 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
     # writes p_k, then reads x, r, P, p_k and writes x, r, z
     pers_ms = prof1[5][0] - prof0[5][0]
     pers_it = prof1[5][1] - prof0[5][1]
-    if pers_it:
+    if pers_it and fp32:
+        # folded FP32 CG (Jacobi-scaled system, implicit unit diagonal): per
+        # iteration the off-diagonal slots (value + column) and row lengths
+        # stream once, r and p_{k-1} are gathered, p_k is written, and phase 2
+        # reads and writes r (x, p_k and q stay in shared memory)
+        nnz_off = nnz_p - n
+        bpi = nnz_off * 8 + n * (1 + 4 + 4 + 4 + 4 + 4) + 4 * ((n + 31) // 32)
+        t_it = pers_ms / pers_it / 1e3
+        ach = bpi / t_it / 1e9
+        roof = {"bound": "hbm", "kernel": "k_cgf_persist (FP32 CG on the Jacobi-scaled system, whole solve in one "
+                                          "cooperative launch, one block per SM: gathered SpMV of the off-diagonal "
+                                          "slots with p = r + beta p, grid barrier, x/r update, grid barrier)",
+                "achieved": ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
+                "traffic": (tr_all.get("fold_bytes_per_iteration_128") if args.size == 128 else None),
+                "traffic_unit": "bytes per CG iteration (ncu DRAM read + write of one launch / its iterations)",
+                "bytes_per_iteration": bpi, "iterations": pers_it, "us_per_iteration": t_it * 1e6,
+                "share_of_step": pers_ms / ms if ms else None}
+    elif pers_it:
         s_ = 4 if fp32 else 8
         bpi = nnz_p * (s_ + 4) + n * (1 + 10 * s_) + 4 * ((n + 31) // 32)
         t_it = pers_ms / pers_it / 1e3
@@ -425,6 +450,45 @@ def batch_measure(x, args, local):
     return out
 
 
+def converge_measure(x, A, mesh, args, local):
+    """Time to the 1e-6 scaled residual: the same case from rest in FP64 and
+    in mixed precision, each run until the SIMPLE convergence test passes
+    (Solvers_1_SIMPLE.jl:222-240) or the cap; CUDA events on the case
+    stream; then U and p of the two end states compared (relative L2)."""
+    import torch
+    out = {"workload": workload_name(args.size).replace(", FP64 SIMPLE", "") + ", SIMPLE from rest to 1e-6",
+           "cap": args.converge_cap}
+    ends = {}
+    for prec in ("fp64", "mixed"):
+        model, config = x.cases.channel_case(mesh, iterations=args.converge_cap, precision=prec, device=local)
+        cfg, keep = x.build_config(model, config)
+        ctx = x.Context(local)
+        dm = x.DeviceMesh(ctx, mesh)
+        case = x.Case(dm, cfg)
+        case.set_field(A.FIELD_U, model.momentum.U)
+        case.set_field(A.FIELD_P, model.momentum.p)
+        stream = torch.cuda.ExternalStream(case.stream(), device=torch.device("cuda", local))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res, conv = case.simple_iterate(args.converge_cap)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        ends[prec] = (case.get_field(A.FIELD_U), case.get_field(A.FIELD_P))
+        out[prec] = {"iterations": len(res), "converged": bool(conv), "seconds": sec,
+                     "value": mesh.n_cells * len(res) / sec / 1e6, "unit": UNIT,
+                     "residuals_last": [float(v) for v in res[-1]]}
+        case.close()
+        dm.close()
+    out["time_ratio_fp64_over_mixed"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+    (U64, p64), (U32, p32) = ends["fp64"], ends["mixed"]
+    out["mixed_vs_fp64_rel_l2"] = {"U": float(np.linalg.norm(U32 - U64) / np.linalg.norm(U64)),
+                                   "p": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))}
+    return out
+
+
 def e2e_measure(x, A, case, mesh, args, world):
     """Same metric through the public API with host buffers: every step copies
     U and p host->device, runs one SIMPLE iteration and reads them back."""
@@ -463,8 +527,11 @@ def main():
     x = ge.load_package()
     A = x._abi
     if args.only is not None:
+        def conv_only():
+            m = x.build_mesh3(x.channel_polymesh(args.size, args.size, args.size, seed=0), device=local)
+            return converge_measure(x, A, m, args, local)
         blk = {"les": lambda: les_measure(x, A, args, local), "serving": lambda: serve_measure(x, args, local),
-               "batch": lambda: batch_measure(x, args, local)}[args.only]()
+               "batch": lambda: batch_measure(x, args, local), "converge": conv_only}[args.only]()
         if rank == 0:
             print(json.dumps({"only": args.only, **blk}), flush=True)
         if world > 1:
@@ -490,6 +557,7 @@ def main():
                  "ratio_mixed_over_fp64": (r2["value"] / r["value"]) if sec == "mixed" else (r["value"] / r2["value"]),
                  "roofline": r2["roofline"], "residuals_last": r2["residuals_last"],
                  "phases_ms_total": r2["phases_ms_total"], "gpu_launches": r2["gpu_launches"]}
+    converge = converge_measure(x, A, mesh, args, local) if args.converge_cap > 0 else None
     les = les_measure(x, A, args, local) if args.les_size > 0 else None
     serving = serve_measure(x, args, local) if args.serve_cases > 0 else None
     batched = batch_measure(x, args, local) if args.serve_cases > 0 else None
@@ -508,7 +576,8 @@ def main():
                            "mesh_build_s": round(t_mesh, 2), "setup_s": r["setup_s"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": r["gpu_launches"],
                 "clocks": r["clocks"], "residuals_last": r["residuals_last"],
-                "phases_ms_total": r["phases_ms_total"], "second_precision": other, "les": les,
+                "phases_ms_total": r["phases_ms_total"], "second_precision": other, "to_convergence": converge,
+                "les": les,
                 "serving": serving, "batch": batched}
         print(json.dumps(line), flush=True)
     if world > 1:

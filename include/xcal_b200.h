@@ -292,10 +292,31 @@ typedef struct xcal_batch xcal_batch;
 /* Hardware(backend=B200Backend()) (src/Simulate/Simulate_0_types.jl:70-74) */
 int32_t xcal_ctx_create(int32_t device, xcal_ctx** out);
 int32_t xcal_ctx_destroy(xcal_ctx* ctx);
-/* message of the last error on this context (never NULL) */
+/* message of the calling thread's last failed call on this context (never
+ * NULL; "" when it has none).  Messages are kept per host thread, so threads
+ * sharing a context never read each other's errors. */
 const char* xcal_last_error(const xcal_ctx* ctx);
 /* library version string */
 const char* xcal_version(void);
+
+/* ---- struct layouts, for bindings -----------------------------------------
+ * No counterpart in the reference (it has no C boundary).  sizeof and the
+ * field offsets of the structs above as this library was compiled, so a
+ * binding's mirror (Julia structs, ctypes) can be checked against them:
+ * out[0] = sizeof, out[1 + k] = offset of field k in declaration order (array
+ * fields: their first element).  Returns the number of values written, or
+ * XCAL_ERR_INVALID for an unknown `which` or too small a `cap`.  Needs no
+ * device. */
+enum {
+    XCAL_LAYOUT_MESH_DESC = 0,
+    XCAL_LAYOUT_BC = 1,
+    XCAL_LAYOUT_SOLVER_SETUP = 2,
+    XCAL_LAYOUT_SCHEMES = 3,
+    XCAL_LAYOUT_CONFIG = 4,
+    XCAL_LAYOUT_POLYMESH_DESC = 5,
+    XCAL_LAYOUT_MESH_BUFFERS = 6
+};
+int32_t xcal_abi_layout(int32_t which, int64_t* out, int32_t cap);
 
 /* ---- mesh import (host) --------------------------------------------------*/
 /* FOAM3D_mesh (src/FoamMesh/FoamMesh_5_build.jl:21-27) without the file
@@ -412,9 +433,12 @@ int32_t xcal_max_courant(xcal_case* cs, double* courant);
  * cannot allocate device memory (inside CUDA graph capture, under a fixed
  * memory budget or a caller-managed pool).  Computes the scaled residual
  * ||b - A x|| / ||b|| (||b|| replaced by 1 when it is at most eps(||b||)) of
- * a CSR system -- the same arithmetic and reduction tree as the residual
- * xcal_solve_system reports -- with every array (rowptr[n+1], colval, nzval,
- * x[n], b[n]) and the result (one double) in device memory.  Runs on the
+ * a CSR system with every array (rowptr[n+1], colval, nzval, x[n], b[n]) and
+ * the result (one double) in device memory.  Each row's sum follows its CSR
+ * order and the two norms use the library's fixed reduction tree over the
+ * rows in the order given, so for rows given in any order the result equals
+ * the residual xcal_solve_system reports up to rounding; it is the same value
+ * bit for bit only when the rows come in the library's storage order.  Runs on the
  * calling thread's current device, on `stream` (NULL = legacy stream),
  * without synchronising.  n is limited to 33,554,432 rows (larger n returns
  * XCAL_ERR_INVALID).  It allocates nothing: its scratch is a fixed ~256 KiB
@@ -426,6 +450,18 @@ int32_t xcal_max_courant(xcal_case* cs, double* courant);
 int32_t xcal_residual_noalloc(int32_t n, const int32_t* rowptr, const int32_t* colval, const double* nzval,
                               const double* x, const double* b, double* result, void* stream, char* err,
                               int32_t errlen);
+
+/* ---- bounded waits ----------------------------------------------------------
+ * No counterpart in the reference.  The persistent kernels' grid barriers
+ * poll a bounded number of times, then set an error flag and return, so a
+ * block that never arrives becomes XCAL_ERR_TIMEOUT on the host, not a hung
+ * GPU.  This check runs that path on purpose and without any fault: one
+ * block waits at a barrier for a second block that is never launched, giving
+ * up after spin_limit polls (1 .. 4,194,304; about 0.1 us each).  gave_up = 1
+ * and flag_set = 1 when the wait ended by its limit; ran_after = 1 when a
+ * kernel launched after it still ran (the context stayed usable). */
+int32_t xcal_check_bounded_wait(xcal_ctx* ctx, int64_t spin_limit, int32_t* gave_up, int32_t* flag_set,
+                                int32_t* ran_after);
 
 /* ---- timers --------------------------------------------------------------*/
 /* cumulative device time (ms) per phase since case creation:
@@ -464,6 +500,27 @@ int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable);
  * cooperative form only (each falls back to the two-kernel loop when it
  * does not fit). */
 int32_t xcal_case_set_persistent(xcal_case* cs, int32_t mode);
+/* Krylov report of the last solve of each system (Ux, Uy, Uz, p, k, omega,
+ * wall distance): iterations (mixed precision: inner iterations over all
+ * defect-correction steps) and status -- 0 running, 1 solved, 2 stopped at
+ * itmax, 3 zero curvature, 4 breakdown, 5 zero right-hand side -- and the
+ * number of solves since the case was created that stopped at itmax.
+ * solve_system! warns "Maximum number of iterations reached!" for those
+ * (src/Solve/Solve_1_api.jl:302); the library keeps going as the reference
+ * does and reports them here.  Any pointer may be NULL. */
+int32_t xcal_case_solve_report(const xcal_case* cs, int32_t* iters7, int32_t* status7, int64_t* itmax_hits);
+/* Mixed precision, CG with the Jacobi preconditioner: form of the FP32 inner
+ * solves.  No counterpart in the reference (its Krylov.jl solves have no
+ * inner precision).  0 (default) = CG on the Jacobi-scaled system
+ * M^1/2 A M^1/2 (the same iteration in exact arithmetic, deterministic, its
+ * own reduction order) where the system fits one block per SM, else as 1;
+ * 1 = the FP32 form of the FP64 path's kernels; 2..5 = the scaled-system
+ * kernel in launch shape 0..3 (threads per block, rows in flight per
+ * thread); 6..9 = the same shapes with the iterate and the direction kept in
+ * global memory instead of shared memory (bit-identical to 2..5).  All meet
+ * the same stopping tests; results agree within the mixed-precision
+ * tolerance. */
+int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode);
 /* launch-shape autotuner (runs on first use, or now): out6 = for U then p,
  * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU as
  * one-block sweeps [0/1]).  The choices never change a result. */
@@ -492,7 +549,9 @@ int32_t xcal_case_footprint(const xcal_case* cs, int64_t* case_bytes, int64_t* m
 int32_t xcal_batch_create(xcal_ctx* ctx, int32_t max_cases, int64_t budget_bytes, xcal_batch** out);
 int32_t xcal_batch_destroy(xcal_batch* b);
 /* admit a case (it then runs on the batch's stream); charge_bytes <= 0
- * charges its measured footprint.  XCAL_ERR_BUSY when full or over budget. */
+ * charges its measured footprint.  XCAL_ERR_BUSY when full or over budget.
+ * An admitted case's mixed-precision inner CG takes the canonical form
+ * (xcal_case_set_inner_cg mode 1), the batch's own, for good. */
 int32_t xcal_batch_add(xcal_batch* b, xcal_case* cs, int64_t charge_bytes);
 int32_t xcal_batch_remove(xcal_batch* b, xcal_case* cs);
 int32_t xcal_batch_info(const xcal_batch* b, int32_t* n_cases, int64_t* used_bytes, int64_t* budget_bytes);
@@ -503,7 +562,12 @@ int32_t xcal_batch_timings(const xcal_batch* b, double* ms4);
 int32_t xcal_batch_case_index(const xcal_batch* b, const xcal_case* cs, int32_t* index);
 /* one SIMPLE iteration of every admitted case; res [n_cases*4] receives the
  * scaled residuals (Ux, Uy, Uz, p) and converged [n_cases] the per-case
- * convergence test of Solvers_1_SIMPLE.jl:222-240 (either may be NULL) */
+ * convergence test of Solvers_1_SIMPLE.jl:222-240: 1 converged, 0 not yet,
+ * or XCAL_ERR_DIVERGED for a case whose residual was NaN/Inf.  Such a case
+ * has left the batch when the call returns (its budget charge is released;
+ * the caller destroys or inspects it); the other cases are unaffected and
+ * the call returns XCAL_OK.  Rows follow the order before the call (either
+ * array may be NULL). */
 int32_t xcal_batch_simple_iterate(xcal_batch* b, double* res, int32_t* converged);
 
 #ifdef __cplusplus

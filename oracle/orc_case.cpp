@@ -1732,8 +1732,10 @@ bool simple_iteration(Case& C, double* res4) {
     res4[2] = r3[2];
     res4[3] = rp;
     bool turb_conv = C.cfg.turbulence == XCAL_TURB_LAMINAR;
-    return r3[0] <= C.cfg.U_solver.convergence && r3[1] <= C.cfg.U_solver.convergence &&
-           r3[2] <= C.cfg.U_solver.convergence && rp <= C.cfg.p_solver.convergence && turb_conv;
+    // Uz enters the test on 3D meshes only (Solvers_1_SIMPLE.jl:220-223)
+    const bool uz_conv = C.m->dim == 2 || r3[2] <= C.cfg.U_solver.convergence;
+    return r3[0] <= C.cfg.U_solver.convergence && r3[1] <= C.cfg.U_solver.convergence && uz_conv &&
+           rp <= C.cfg.p_solver.convergence && turb_conv;
 }
 
 // one PISO time step (Solvers_2_PISO.jl:108-187); returns the Courant number

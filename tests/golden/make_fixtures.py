@@ -23,7 +23,8 @@ Fixtures:
                              test/test_mesh_conversion.jl:43-61), 3D parse below.
   streamtube_unv3.npz     -- examples/0_GRIDS/3d_streamtube_1.0x0.1x0.1_0.08mm.unv (tetrahedra).
 
-Usage: python tests/golden/make_fixtures.py [/path/to/XCALibre.jl]
+Usage: python tests/golden/make_fixtures.py /path/to/XCALibre.jl
+       (or XCAL_REFERENCE_DIR=/path/to/XCALibre.jl python tests/golden/make_fixtures.py)
 """
 from __future__ import annotations
 
@@ -236,4 +237,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("XCAL_REFERENCE_DIR", "")
+    if not ref:
+        sys.exit("usage: make_fixtures.py /path/to/XCALibre.jl (or set XCAL_REFERENCE_DIR)")
+    main(ref)

@@ -8,8 +8,9 @@ import os
 
 import numpy as np
 import pytest
+from refpath import ref_path
 
-REF_CAVITY = "/root/reference/test/grids/OF_cavity_hex/polyMesh"
+REF_CAVITY = ref_path("test/grids/OF_cavity_hex/polyMesh")
 
 MESH3_FIELDS = ["face_owner", "face_neigh", "face_centre", "face_normal", "face_e", "face_area", "face_delta",
                 "face_weight", "cell_centre", "cell_volume", "cell_faces_offset", "cell_faces", "cell_nsign",
@@ -51,7 +52,7 @@ def test_scale_and_errors(x, tmp_path):
         x.read_polymesh(d)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_CAVITY), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isdir(REF_CAVITY), reason="XCAL_REFERENCE_DIR (an XCALibre.jl checkout) not set")
 def test_reference_cavity_grid(x, orc):
     pm = x.read_polymesh(REF_CAVITY, scale=0.001)
     mesh = x.FOAM3D_mesh(REF_CAVITY, scale=0.001)

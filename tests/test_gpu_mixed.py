@@ -63,3 +63,62 @@ def test_mixed_converged_cavity_matches_fp64(x, ctx):
         out[prec] = (c.get_field(x._abi.FIELD_U), c.get_field(x._abi.FIELD_P), len(res))
     assert rel(out["mixed"][0], out["fp64"][0]) <= 1e-5, rel(out["mixed"][0], out["fp64"][0])
     assert rel(out["mixed"][1], out["fp64"][1]) <= 1e-5, rel(out["mixed"][1], out["fp64"][1])
+
+
+def _tight_pressure(x, ctx, mesh, prec, inner_cg=None):
+    """One pressure solve to rtol 1e-9 after a momentum predictor from a
+    seeded velocity; returns p."""
+    model, config = x.cases.channel_case(mesh, iterations=3, precision=prec)
+    config.solvers["p"].rtol = 1e-9
+    rng = np.random.default_rng(1)
+    model.momentum.U[:] = rng.standard_normal(model.momentum.U.shape) * 0.1
+    c, keep = _case(x, ctx, mesh, model, config)
+    if inner_cg is not None:
+        c.set_inner_cg(inner_cg)
+    c.initial_calculations()
+    c.solve_equation(0)
+    c.pressure_predictor()
+    c.flux_divergence()
+    c.solve_equation(1)
+    p = c.get_field(x._abi.FIELD_P)
+    c.close()
+    keep[2].close()
+    return p
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
+def test_inner_cg_forms_tight(x, ctx, mode):
+    """Every form of the FP32 inner CG (Jacobi-scaled system in each launch
+    shape; the canonical kernels) meets the tight-solve bound against FP64."""
+    mesh = x.build_mesh3(x.channel_polymesh(24, 12, 12, seed=3))
+    p64 = _tight_pressure(x, ctx, mesh, "fp64")
+    p = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=mode)
+    assert rel(p, p64) <= 1e-6, rel(p, p64)
+
+
+@pytest.mark.parametrize("form", [0, 1, 2, 3])
+def test_inner_cg_vectors_in_global_memory_identical(x, ctx, form):
+    """The scaled-system kernel with x and p in global memory (the layout
+    of systems too large for shared memory) gives the shared-memory layout's
+    result bit for bit: only where the vectors live differs."""
+    mesh = x.build_mesh3(x.channel_polymesh(40, 24, 20, seed=4))
+    a = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=2 + form)
+    b = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=6 + form)
+    assert np.array_equal(a, b)
+
+
+def test_inner_cg_graph_mode_identical(x, ctx):
+    """The scaled-system inner CG captured in a step graph gives the
+    host-polled run's results bit for bit (deterministic reductions)."""
+    mesh = x.build_mesh3(x.channel_polymesh(20, 10, 10, seed=6))
+    out = []
+    for graph in (False, True):
+        model, config = x.cases.channel_case(mesh, iterations=4, precision="mixed")
+        c, keep = _case(x, ctx, mesh, model, config)
+        c.set_graph_mode(graph)
+        res, _ = c.simple_iterate(4)
+        out.append((res, c.get_field(x._abi.FIELD_U), c.get_field(x._abi.FIELD_P)))
+        c.close()
+        keep[2].close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)

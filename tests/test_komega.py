@@ -16,8 +16,9 @@ import numpy as np
 import pytest
 
 from test_unv import bfs_mesh
+from refpath import ref_path
 
-REF = "/root/reference/examples/0_GRIDS/backwardFacingStep_5mm.unv"
+REF = ref_path("examples/0_GRIDS/backwardFacingStep_5mm.unv")
 
 
 def komega_bfs_case(x, mesh, steps=500, precision="fp64"):
@@ -66,7 +67,7 @@ def set_komega_fields(x, c, model):
         c.set_field(getattr(x._abi, f), v)
 
 
-@pytest.mark.skipif(not os.path.isfile(REF), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isfile(REF), reason="XCAL_REFERENCE_DIR (an XCALibre.jl checkout) not set")
 def test_bfs_5mm_fixture_matches_file(x):
     a = x.UNV2D_mesh(REF, scale=0.001)
     b = bfs_mesh(x, 5)

@@ -10,8 +10,9 @@ import os
 
 import numpy as np
 import pytest
+from refpath import ref_path
 
-PITZ = "/root/reference/examples/0_GRIDS/OF_pitzDaily/polyMesh"
+PITZ = ref_path("examples/0_GRIDS/OF_pitzDaily/polyMesh")
 
 
 def slab_les_case(x, mesh, steps, dt, U_inlet=10.0, nu=1e-5, walls=("upperWall", "lowerWall")):
@@ -67,7 +68,7 @@ def test_delta_scaling_and_boundary_average(x):
     assert A.boundary_average("outlet", U[0], config.boundaries["p"], mesh=mesh) == 0.0
 
 
-@pytest.mark.skipif(not os.path.isdir(PITZ), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isdir(PITZ), reason="XCAL_REFERENCE_DIR (an XCALibre.jl checkout) not set")
 def test_pitzdaily_smagorinsky_known_answer(x, orc):
     mesh = x.FOAM3D_mesh(PITZ)
     assert (mesh.n_cells, mesh.n_faces, mesh.points.shape[0]) == (12225, 49180, 25012)

@@ -17,11 +17,11 @@ import os
 import numpy as np
 import pytest
 
+from refpath import ref_path
 from test_oracle_golden import GOLD
 
-REF = "/root/reference"
-GRIDS = os.path.join(REF, "test", "grids")
-EX = os.path.join(REF, "examples", "0_GRIDS")
+GRIDS = ref_path("test", "grids")
+EX = ref_path("examples", "0_GRIDS")
 
 
 def bfs_mesh(x, mm=10):
@@ -80,7 +80,7 @@ def _closure(m):
     return np.abs(acc).max() / np.abs(S).max()
 
 
-@pytest.mark.skipif(not os.path.isdir(GRIDS), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isdir(GRIDS), reason="XCAL_REFERENCE_DIR (an XCALibre.jl checkout) not set")
 @pytest.mark.parametrize("grid,counts", [("trig40.unv", (3484, 5306, 1823)), ("quad40.unv", (1600, 3280, 1681))])
 def test_reference_grid_counts(x, grid, counts):
     m = x.UNV2D_mesh(os.path.join(GRIDS, grid), scale=0.001)
@@ -91,7 +91,7 @@ def test_reference_grid_counts(x, grid, counts):
     assert np.all(np.abs(m.face_normal[:, 2]) == 0.0) and np.all(m.face_weight[: m.n_bfaces] == 1.0)
 
 
-@pytest.mark.skipif(not os.path.isdir(EX), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isdir(EX), reason="XCAL_REFERENCE_DIR (an XCALibre.jl checkout) not set")
 def test_laplace_unit_3by3_unv(x, orc):
     """unit_test_laplace.jl on its own mesh: -Laplacian(k=1, T) == 0 as the p
     equation (rDf = 1), A and b compared in the reference's cell order."""
@@ -122,7 +122,7 @@ def test_laplace_unit_3by3_unv(x, orc):
     assert np.allclose(b, np.array(g["b"]), rtol=1.5e-8, atol=0)
 
 
-@pytest.mark.skipif(not os.path.isdir(EX), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isdir(EX), reason="XCAL_REFERENCE_DIR (an XCALibre.jl checkout) not set")
 def test_bfs_fixture_matches_file(x):
     a = x.UNV2D_mesh(os.path.join(EX, "backwardFacingStep_10mm.unv"), scale=0.001)
     b = bfs_mesh(x)

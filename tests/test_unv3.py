@@ -12,12 +12,12 @@ import os
 import numpy as np
 import pytest
 
+from refpath import ref_path
 from test_oracle_golden import GOLD
 
-REF = "/root/reference"
-CAV_UNV = os.path.join(REF, "test/grids/OF_cavity_hex/cavity_hex.unv")
-CAV_FOAM = os.path.join(REF, "test/grids/OF_cavity_hex/polyMesh")
-TUBE = os.path.join(REF, "examples/0_GRIDS/3d_streamtube_1.0x0.1x0.1_0.08mm.unv")
+CAV_UNV = ref_path("test/grids/OF_cavity_hex/cavity_hex.unv")
+CAV_FOAM = ref_path("test/grids/OF_cavity_hex/polyMesh")
+TUBE = ref_path("examples/0_GRIDS/3d_streamtube_1.0x0.1x0.1_0.08mm.unv")
 
 
 def unv3_fixture_mesh(x, name, scale=0.001):
@@ -48,7 +48,7 @@ ARRAYS = ("face_owner", "face_neigh", "face_centre", "face_normal", "face_e", "f
           "cell_neighbours", "boundary_cellsID", "patch_start", "patch_count")
 
 
-@pytest.mark.skipif(not os.path.isfile(CAV_UNV), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isfile(CAV_UNV), reason="XCAL_REFERENCE_DIR (an XCALibre.jl checkout) not set")
 def test_cavity_hex_unv_matches_foam_counts(x):
     u = x.UNV3D_mesh(CAV_UNV, scale=0.001)
     f = x.FOAM3D_mesh(CAV_FOAM, scale=0.001)
@@ -58,7 +58,7 @@ def test_cavity_hex_unv_matches_foam_counts(x):
         assert np.array_equal(getattr(u, k), getattr(b, k)), k
 
 
-@pytest.mark.skipif(not os.path.isfile(TUBE), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isfile(TUBE), reason="XCAL_REFERENCE_DIR (an XCALibre.jl checkout) not set")
 def test_streamtube_fixture_matches_file(x):
     u = x.UNV3D_mesh(TUBE, scale=0.001)
     b = unv3_fixture_mesh(x, "streamtube_unv3.npz")

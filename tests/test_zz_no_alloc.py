@@ -1,10 +1,12 @@
 """GPU test of xcal_residual_noalloc, the entry point for callers that cannot
 allocate device memory (graph capture, fixed budgets, caller-managed pools).
 
-It must give the same scaled residual as the one xcal_solve_system reports
-for the same system (same arithmetic, same reduction tree), on two calls in a
-row (the shared scratch array keeps the previous call's contents).  This file
-is collected last so a failure here never hides other tests.
+It must give the scaled residual xcal_solve_system reports for the same
+system, on two calls in a row (the shared scratch array keeps the previous
+call's contents).  The system is passed in the caller's original row order,
+while the library sums rows in its own storage order, so the two agree to
+rounding (the stated 1e-10), not bit for bit.  This file is collected last so
+a failure here never hides other tests.
 """
 import ctypes
 

@@ -65,6 +65,10 @@ SIGNATURES = {
     "xcal_case_mark_initialised": (_i32, [_vp]),
     "xcal_case_tuning": (_i32, [_vp, _pi]),
     "xcal_case_set_dilu_mode": (_i32, [_vp, _i32]),
+    "xcal_case_set_inner_cg": (_i32, [_vp, _i32]),
+    "xcal_abi_layout": (_i32, [_i32, C.POINTER(C.c_int64), _i32]),
+    "xcal_case_solve_report": (_i32, [_vp, _pi, _pi, _pi64]),
+    "xcal_check_bounded_wait": (_i32, [_vp, _i64, _pi, _pi, _pi]),
     "xcal_case_get_profile": (_i32, [_vp, _i32, _pd, _pi64]),
     "xcal_residual_noalloc": (_i32, [_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, _i32]),
     "xcal_footprint_estimate": (_i32, [_i64, _i64, _i64, _i32, _i32, _i32, _pi64]),

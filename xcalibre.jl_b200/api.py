@@ -850,6 +850,25 @@ class Case:
         """0 = autotuned, 1 = one-block sweeps, 2 = per-level kernels."""
         self._chk(lib().xcal_case_set_dilu_mode(self.h, int(mode)))
 
+    def solve_report(self) -> dict:
+        """Last Krylov solve of each system (Ux, Uy, Uz, p, k, omega, wall
+        distance): iterations and status (0 running, 1 solved, 2 stopped at
+        itmax, 3 zero curvature, 4 breakdown, 5 zero right-hand side), and
+        how many solves since creation stopped at itmax."""
+        it = np.zeros(7, dtype=np.int32)
+        st = np.zeros(7, dtype=np.int32)
+        hits = C.c_int64()
+        self._chk(lib().xcal_case_solve_report(self.h, _abi.ptr(it, C.c_int32), _abi.ptr(st, C.c_int32),
+                                               C.byref(hits)))
+        return {"iterations": it, "status": st, "itmax_hits": int(hits.value)}
+
+    def set_inner_cg(self, mode: int):
+        """Mixed precision, CG + Jacobi inner solves: 0 = on the Jacobi-scaled
+        system (default), 1 = the FP32 form of the FP64 path's kernels,
+        2..5 = the scaled-system kernel in launch shape 0..3, 6..9 = those
+        shapes with x and p in global memory (same results as 2..5)."""
+        self._chk(lib().xcal_case_set_inner_cg(self.h, int(mode)))
+
     def checkpoint(self) -> dict:
         """The case's state as host arrays (every field the ABI reads: U, p,
         face mass flux, face velocity and pressure, nu_eff, gradients, rD,
@@ -917,6 +936,7 @@ class Batch:
         check(lib().xcal_batch_create(ctx.h, int(max_cases), int(budget_bytes), C.byref(h)), ctx.h)
         self.h = h
         self.cases: list[Case] = []
+        self.last_diverged: list[Case] = []
 
     def close(self):
         if getattr(self, "h", None):
@@ -956,13 +976,20 @@ class Batch:
 
     def simple_iterate(self):
         """One SIMPLE iteration of every case: (residuals [n, 4], converged [n])
-        in the order of ``self.cases``."""
+        in the order of ``self.cases`` before the call.  A case whose residual
+        became NaN/Inf has left the batch (the others are unaffected): it is
+        listed in ``self.last_diverged`` and its ``converged`` entry is
+        False."""
         n = len(self.cases)
         res = np.zeros((max(n, 1), 4))
         conv = np.zeros(max(n, 1), dtype=np.int32)
         check(lib().xcal_batch_simple_iterate(self.h, _abi.ptr(res, C.c_double), _abi.ptr(conv, C.c_int32)),
               self.ctx.h)
-        return res[:n], conv[:n].astype(bool)
+        conv = conv[:n]
+        self.last_diverged = [c for c, s in zip(self.cases, conv) if s == _abi.XCAL_ERR_DIVERGED]
+        for c in self.last_diverged:
+            self.cases.remove(c)
+        return res[:n], conv == 1
 
 
 def launch_count() -> int:
@@ -1119,6 +1146,13 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
             if wi > 0 and done % wi == 0:
                 write(done)
         res = np.concatenate(hist, axis=0) if hist else np.zeros((0, 4))
+        hits = case.solve_report()["itmax_hits"]
+        if hits:
+            # solve_system! warns for every solve that stopped at itmax
+            # (Solve_1_api.jl:302); the run carries on, as there
+            import warnings
+            warnings.warn(f"Maximum number of iterations reached! ({hits} Krylov solves stopped at itmax)",
+                          RuntimeWarning, stacklevel=2)
         model.momentum.U[:] = case.get_field(_abi.FIELD_U)
         model.momentum.p[:] = case.get_field(_abi.FIELD_P)
         if isinstance(model.turbulence, LES) or hasattr(model.turbulence, "k"):

@@ -60,6 +60,7 @@ struct Batch {
     DBuf<int> perr;                  // persistent CG: a barrier wait gave up
     std::vector<int2> h_tmap;
     long long iterations = 0;
+    long diverged_total = 0;  // cases retired for a NaN/Inf residual
     double phase_ms[4] = {0, 0, 0, 0};  // host wall time: face loops, U solves, p solve, total
     // steady-state Krylov chunks replayed as CUDA graphs, per [precision][slot];
     // every pointer they use is fixed until the composition changes
@@ -726,18 +727,28 @@ struct Batch {
         phase_ms[0] = phase_ms[3] - phase_ms[1] - phase_ms[2];
         (void)fv;
         (void)t1;
+        // A case whose residual is NaN/Inf leaves the batch now, reported as
+        // XCAL_ERR_DIVERGED in its row; the others are not touched (every
+        // batched kernel keeps each case's data and scalars apart), so they
+        // carry on exactly as they would have without it.
+        std::vector<Case*> diverged;
         for (size_t i = 0; i < cases.size(); ++i) {
-            const Case* c = cases[i];
+            Case* c = cases[i];
             const double* r = hres + 4 * i;
+            bool bad = false;
             for (int k = 0; k < 4; ++k) {
                 if (res_out) res_out[4 * i + k] = r[k];
-                if (std::isnan(r[k]) || std::isinf(r[k])) fail(XCAL_ERR_DIVERGED, "batch: residual is NaN/Inf");
+                bad |= std::isnan(r[k]) || std::isinf(r[k]);
             }
-            bool conv = r[0] <= c->cfg.U_solver.convergence && r[1] <= c->cfg.U_solver.convergence &&
-                        r[2] <= c->cfg.U_solver.convergence && r[3] <= c->cfg.p_solver.convergence &&
-                        c->cfg.turbulence == XCAL_TURB_LAMINAR;
-            if (conv_out) conv_out[i] = conv ? 1 : 0;
+            // Uz enters the test on 3D meshes only (Solvers_1_SIMPLE.jl:220-223)
+            const bool uz = c->mesh->dim == 2 || r[2] <= c->cfg.U_solver.convergence;
+            bool conv = r[0] <= c->cfg.U_solver.convergence && r[1] <= c->cfg.U_solver.convergence && uz &&
+                        r[3] <= c->cfg.p_solver.convergence && c->cfg.turbulence == XCAL_TURB_LAMINAR;
+            if (conv_out) conv_out[i] = bad ? XCAL_ERR_DIVERGED : (conv ? 1 : 0);
+            if (bad) diverged.push_back(c);
         }
+        for (Case* c : diverged) remove(c);
+        diverged_total += (long)diverged.size();
     }
 };
 
@@ -791,10 +802,10 @@ using namespace xcal;
         __VA_ARGS__;                                                          \
         return XCAL_OK;                                                       \
     } catch (const ::xcal::Error& e) {                                        \
-        if (ctx) ctx->last_error = e.msg;                                     \
+        if (ctx) ctx->set_error(e.msg);                                       \
         return e.code;                                                        \
     } catch (const std::exception& e) {                                       \
-        if (ctx) ctx->last_error = e.what();                                  \
+        if (ctx) ctx->set_error(e.what());                                    \
         return XCAL_ERR_INVALID;                                              \
     }
 
@@ -838,6 +849,10 @@ int32_t xcal_batch_add(xcal_batch* bt, xcal_case* cs, int64_t charge_bytes) {
     XCAL_BGUARD(b->ctx, {
         size_t charge = charge_bytes > 0 ? (size_t)charge_bytes : cs->c->bytes + cs->c->mesh->bytes;
         b->add(cs->c.get(), charge);
+        // the batch's FP32 inner solves use the canonical kernels; the case
+        // keeps that form if it later runs alone, so its arithmetic never
+        // depends on whether it was batched
+        cs->c->set_inner_cg(1);
     })
 }
 

@@ -1,7 +1,9 @@
 // capi.cu -- extern "C" entry points of libxcal_b200.so (include/xcal_b200.h).
 // Every call catches library errors and turns them into a status code plus a
 // message retrievable with xcal_last_error; nothing aborts the process.
+#include <cstddef>
 #include <exception>
+#include <vector>
 #include <new>
 
 #include "case.hpp"
@@ -16,7 +18,7 @@ thread_local size_t* t_alloc_acc = nullptr;
 using namespace xcal;
 
 static int set_error(xcal_ctx* ctx, int code, const std::string& msg) {
-    if (ctx) ctx->last_error = msg;
+    if (ctx) ctx->set_error(msg);
     return code;
 }
 
@@ -42,6 +44,84 @@ extern "C" {
 
 const char* xcal_version(void) { return "xcal_b200 0.1 (sm_100a, FP64 hot path)"; }
 
+#define XCAL_OFF(T, f) (int64_t) offsetof(T, f)
+int32_t xcal_abi_layout(int32_t which, int64_t* out, int32_t cap) {
+    std::vector<int64_t> v;
+    switch (which) {
+        case XCAL_LAYOUT_MESH_DESC: {
+            using T = xcal_mesh_desc;
+            v = {sizeof(T), XCAL_OFF(T, n_cells), XCAL_OFF(T, n_faces), XCAL_OFF(T, n_bfaces),
+                 XCAL_OFF(T, face_owner), XCAL_OFF(T, face_neigh), XCAL_OFF(T, face_centre),
+                 XCAL_OFF(T, face_normal), XCAL_OFF(T, face_e), XCAL_OFF(T, face_area), XCAL_OFF(T, face_delta),
+                 XCAL_OFF(T, face_weight), XCAL_OFF(T, cell_centre), XCAL_OFF(T, cell_volume),
+                 XCAL_OFF(T, cell_faces_offset), XCAL_OFF(T, cell_faces), XCAL_OFF(T, cell_nsign),
+                 XCAL_OFF(T, cell_neighbours), XCAL_OFF(T, boundary_cellsID), XCAL_OFF(T, n_patches),
+                 XCAL_OFF(T, patch_start), XCAL_OFF(T, patch_count), XCAL_OFF(T, dim)};
+            break;
+        }
+        case XCAL_LAYOUT_BC: {
+            using T = xcal_bc;
+            v = {sizeof(T), XCAL_OFF(T, type), XCAL_OFF(T, patch), XCAL_OFF(T, value), XCAL_OFF(T, face_values),
+                 XCAL_OFF(T, face_map), XCAL_OFF(T, distance), XCAL_OFF(T, partner_patch), XCAL_OFF(T, wall)};
+            break;
+        }
+        case XCAL_LAYOUT_SOLVER_SETUP: {
+            using T = xcal_solver_setup;
+            v = {sizeof(T), XCAL_OFF(T, solver), XCAL_OFF(T, precond), XCAL_OFF(T, convergence), XCAL_OFF(T, relax),
+                 XCAL_OFF(T, atol), XCAL_OFF(T, rtol), XCAL_OFF(T, itmax), XCAL_OFF(T, smoother_loops),
+                 XCAL_OFF(T, smoother_omega)};
+            break;
+        }
+        case XCAL_LAYOUT_SCHEMES: {
+            using T = xcal_schemes;
+            v = {sizeof(T), XCAL_OFF(T, time), XCAL_OFF(T, divergence), XCAL_OFF(T, gradient), XCAL_OFF(T, limiter),
+                 XCAL_OFF(T, limiter_level)};
+            break;
+        }
+        case XCAL_LAYOUT_CONFIG: {
+            using T = xcal_config;
+            v = {sizeof(T),
+                 XCAL_OFF(T, algorithm), XCAL_OFF(T, turbulence), XCAL_OFF(T, nu), XCAL_OFF(T, smagorinsky_C),
+                 XCAL_OFF(T, les_delta_distance), XCAL_OFF(T, les_delta_power), XCAL_OFF(T, U_schemes),
+                 XCAL_OFF(T, p_schemes), XCAL_OFF(T, U_solver), XCAL_OFF(T, p_solver), XCAL_OFF(T, iterations),
+                 XCAL_OFF(T, dt), XCAL_OFF(T, has_pref), XCAL_OFF(T, pref), XCAL_OFF(T, inner_loops),
+                 XCAL_OFF(T, ncorrectors), XCAL_OFF(T, precision), XCAL_OFF(T, inner_rtol), XCAL_OFF(T, n_bc_U),
+                 XCAL_OFF(T, n_bc_p), XCAL_OFF(T, n_bc_nut), XCAL_OFF(T, bc_U), XCAL_OFF(T, bc_p),
+                 XCAL_OFF(T, bc_nut), XCAL_OFF(T, kw_beta_star), XCAL_OFF(T, kw_alpha1), XCAL_OFF(T, kw_beta1),
+                 XCAL_OFF(T, kw_sigma_k), XCAL_OFF(T, kw_sigma_omega), XCAL_OFF(T, k_schemes),
+                 XCAL_OFF(T, omega_schemes), XCAL_OFF(T, k_solver), XCAL_OFF(T, omega_solver), XCAL_OFF(T, n_bc_k),
+                 XCAL_OFF(T, n_bc_omega), XCAL_OFF(T, bc_k), XCAL_OFF(T, bc_omega), XCAL_OFF(T, sst_beta2),
+                 XCAL_OFF(T, sst_sigma_k2), XCAL_OFF(T, sst_sigma_omega2), XCAL_OFF(T, y_schemes),
+                 XCAL_OFF(T, y_solver), XCAL_OFF(T, n_bc_y), XCAL_OFF(T, bc_y)};
+            break;
+        }
+        case XCAL_LAYOUT_POLYMESH_DESC: {
+            using T = xcal_polymesh_desc;
+            v = {sizeof(T), XCAL_OFF(T, n_points), XCAL_OFF(T, points), XCAL_OFF(T, n_faces),
+                 XCAL_OFF(T, face_offsets), XCAL_OFF(T, face_nodes), XCAL_OFF(T, owner),
+                 XCAL_OFF(T, n_internal_faces), XCAL_OFF(T, neighbour), XCAL_OFF(T, n_patches),
+                 XCAL_OFF(T, patch_sizes)};
+            break;
+        }
+        case XCAL_LAYOUT_MESH_BUFFERS: {
+            using T = xcal_mesh_buffers;
+            v = {sizeof(T), XCAL_OFF(T, face_owner), XCAL_OFF(T, face_neigh), XCAL_OFF(T, face_centre),
+                 XCAL_OFF(T, face_normal), XCAL_OFF(T, face_e), XCAL_OFF(T, face_area), XCAL_OFF(T, face_delta),
+                 XCAL_OFF(T, face_weight), XCAL_OFF(T, cell_centre), XCAL_OFF(T, cell_volume),
+                 XCAL_OFF(T, cell_faces_offset), XCAL_OFF(T, cell_faces), XCAL_OFF(T, cell_nsign),
+                 XCAL_OFF(T, cell_neighbours), XCAL_OFF(T, boundary_cellsID), XCAL_OFF(T, patch_start),
+                 XCAL_OFF(T, patch_count)};
+            break;
+        }
+        default:
+            return XCAL_ERR_INVALID;
+    }
+    if (!out || cap < (int32_t)v.size()) return XCAL_ERR_INVALID;
+    for (size_t k = 0; k < v.size(); ++k) out[k] = v[k];
+    return (int32_t)v.size();
+}
+#undef XCAL_OFF
+
 int32_t xcal_ctx_create(int32_t device, xcal_ctx** out) {
     if (!out) return XCAL_ERR_INVALID;
     *out = nullptr;
@@ -61,7 +141,9 @@ int32_t xcal_ctx_destroy(xcal_ctx* ctx) {
     return XCAL_OK;
 }
 
-const char* xcal_last_error(const xcal_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+const char* xcal_last_error(const xcal_ctx* ctx) {
+    return ctx ? const_cast<xcal_ctx*>(ctx)->last_error() : "no context";
+}
 
 int32_t xcal_mesh_upload(xcal_ctx* ctx, const xcal_mesh_desc* desc, xcal_mesh** out) {
     if (!ctx || !out) return XCAL_ERR_INVALID;
@@ -340,6 +422,22 @@ int32_t xcal_case_set_persistent(xcal_case* cs, int32_t mode) {
     if (mode != 0 && mode != 1 && mode != 2 && mode != 256 && mode != 512 && mode != 1024) return XCAL_ERR_INVALID;
     cs->c->persistent_cg = mode;
     return XCAL_OK;
+}
+
+int32_t xcal_case_solve_report(const xcal_case* cs, int32_t* iters7, int32_t* status7, int64_t* itmax_hits) {
+    if (!cs) return XCAL_ERR_INVALID;
+    const Case* c = cs->c.get();
+    for (int k = 0; k < 7; ++k) {
+        if (iters7) iters7[k] = c->last_iters[k];
+        if (status7) status7[k] = c->last_status[k];
+    }
+    if (itmax_hits) *itmax_hits = c->itmax_hits;
+    return XCAL_OK;
+}
+
+int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode) {
+    if (!cs || mode < 0 || mode >= 2 + 2 * FOLD_NFORMS) return XCAL_ERR_INVALID;
+    XCAL_GUARD(cs->c->ctx, cs->c->set_inner_cg(mode));
 }
 
 int32_t xcal_case_set_dilu_mode(xcal_case* cs, int32_t mode) {

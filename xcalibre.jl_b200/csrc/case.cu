@@ -338,6 +338,48 @@ static DevMesh* upload_mesh_ordered(const xcal_mesh_desc* d, cudaStream_t s, std
     return m.release();
 }
 
+// Off-diagonal SELL-32 storage of an equation for the folded FP32 CG
+// (cg_folded.cu): per 32-row slice, width = the longest row's off-diagonal
+// count; each row keeps its entries' order with the diagonal left out; map =
+// the entry's slot in E's own storage.  Built once, on first use.
+static void build_fold(Equation& E, cudaStream_t s) {
+    if (E.fold_built) return;
+    const int n = E.n, nsl = (n + SELL_C - 1) / SELL_C;
+    std::vector<int> fsl(nsl + 1, 0);
+    std::vector<unsigned char> flen(n);
+    for (int r = 0; r < n; ++r) {
+        if (E.diag[r] < 0) fail(XCAL_ERR_INVALID, "folded CG: a row has no diagonal entry");
+        if (E.len[r] - 1 > 127) fail(XCAL_ERR_UNSUPPORTED, "folded CG: a row has more than 127 off-diagonals");
+        flen[r] = (unsigned char)(E.len[r] - 1);
+    }
+    for (int sl = 0; sl < nsl; ++sl) {
+        int w = 0;
+        for (int r = sl * SELL_C; r < std::min(n, (sl + 1) * SELL_C); ++r) w = std::max(w, (int)flen[r]);
+        fsl[sl + 1] = fsl[sl] + SELL_C * w;
+    }
+    const long nslots = fsl[nsl];
+    std::vector<int> fcol(nslots, 0), fmap(nslots, 0);
+    for (int r = 0; r < n; ++r) {
+        const int b = E.base(r), fb = fsl[r / SELL_C] + r % SELL_C;
+        int m = 0;
+        for (int k = 0; k < E.len[r]; ++k) {
+            const int slot = b + SELL_C * k;
+            if (slot == E.diag[r]) continue;
+            fcol[fb + SELL_C * m] = E.colval[slot];
+            fmap[fb + SELL_C * m] = slot;
+            ++m;
+        }
+    }
+    E.f_slice.upload(fsl, s);
+    E.f_len.upload(flen, s);
+    E.f_col.upload(fcol, s);
+    E.f_map.upload(fmap, s);
+    E.f_val.alloc(nslots);
+    E.f_val.zero(s);
+    XCAL_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    E.fold_built = true;
+}
+
 // ---------------------------------------------------------------------------
 // equation pattern (sparse_matrix_connectivity + extend_matrix + sparsecsr)
 // ---------------------------------------------------------------------------
@@ -732,6 +774,8 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
             b->alloc(nC);
             b->zero(stream);
         }
+        ws.fpart.alloc(2 * FOLD_MAX_BLOCKS);
+        ws.fpart.zero(stream);
         for (Equation* E : {&U, &P}) {
             E->nz32.alloc(E->nnz);
             E->nz32.zero(stream);
@@ -1495,6 +1539,23 @@ void Case::solve_captured(int eqn, int comp) {
                 kr_loop_cond(stream, h, S, cap, (int)(t_launch_count - k0) + 1, dlaunch.p);
             });
         kr_finish(stream, n, V.x, ws.dx.p, field);
+    } else if (use_fold(E, SS, true) && E.fold_built) {
+        // folded FP32 CG (cg_folded.cu): each defect step is the scaled
+        // defect, the start, and one cooperative node that also applies the
+        // correction
+        kr_fold_scale(stream, E.fold_mut(), E.nz.p, E.d_diag.p, E.P.p);
+        KrylovVecs<float> V{ws.fx.p, ws.fr.p, ws.fz.p, ws.fp.p, ws.fq.p, ws.fv.p, ws.fs.p, ws.ft.p};
+        capture_while([&](cudaGraphConditionalHandle ho) {
+            const long long k0 = t_launch_count;
+            kr_outer_prep(stream, S);
+            kr_fold_defect(stream, A, E.nz.p, b, field, E.P.p, V.r);
+            kr_cg_start<float>(stream, n, V.r, V.r, V.p, S, ws.part0.p);
+            if (!kr_cgf_persist(stream, E.fold_view(), V.r, V.p, V.v, V.x, field, E.P.p, S, ws.fpart.p,
+                                ws.fpart.p + FOLD_MAX_BLOCKS, ws.bar.p, ws.err.p, itmax + 1, false, fold_form(),
+                                fold_smem()))
+                fail(XCAL_ERR_UNSUPPORTED, "folded CG: the system does not fit one block per SM");
+            kr_outer_cond(stream, ho, S, 64, (int)(t_launch_count - k0) + 1, dlaunch.p);
+        });
     } else {
         kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
         if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, n, E.P.p, E.P32.p);
@@ -1600,11 +1661,43 @@ double Case::solve_system(int eqn, int comp, int* iters) {
         kr_finish(stream, n, V.x, ws.dx.p, field);
         if (iters) *iters = hS->iter;
     }
+    note_status(gk, hS->status);
     // residual (Solve_1_api.jl:441-464), FP64 in both modes
     kr_residual(stream, A, nz, field, b, S, ws.part0.p, ws.part1.p, resbuf.p);
     XCAL_CUDA(cudaMemcpyAsync(h_res, resbuf.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();
     return h_res[0];
+}
+
+bool Case::use_fold(const Equation& E, const xcal_solver_setup& SS, bool captured) const {
+    if (cfg.precision != XCAL_PREC_MIXED || inner_cg == 1 || !persistent_cg) return false;
+    if (SS.solver != XCAL_SOLVER_CG || SS.precond != XCAL_PRECOND_JACOBI) return false;
+    if (captured && !kr_coop_capture_ok(true)) return false;
+    return fold_shape(E.n, fold_form(), fold_smem()).blocks > 0;
+}
+
+void Case::fold_iterate(Equation& E, double* field, const KrylovVecs<float>& V, KScalars* S, KScalars* hS, int gk) {
+    (void)gk;
+    kr_cg_start<float>(stream, E.n, V.r, V.r, V.p, S, ws.part0.p);
+    if (profiling) XCAL_CUDA(cudaEventRecord(ev[5], stream));
+    if (!kr_cgf_persist(stream, E.fold_view(), V.r, V.p, V.v, V.x, field, E.P.p, S, ws.fpart.p,
+                        ws.fpart.p + FOLD_MAX_BLOCKS, ws.bar.p, ws.err.p, hS->itmax + 1, true, fold_form(),
+                        fold_smem()))
+        fail(XCAL_ERR_UNSUPPORTED, "folded CG: the system does not fit one block per SM");
+    if (profiling) XCAL_CUDA(cudaEventRecord(ev[6], stream));
+    int errflag = 0;
+    XCAL_CUDA(cudaMemcpyAsync(hS, S, sizeof(KScalars), cudaMemcpyDeviceToHost, stream));
+    XCAL_CUDA(cudaMemcpyAsync(&errflag, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    sync();
+    if (errflag) fail(XCAL_ERR_TIMEOUT, "folded CG: a grid barrier wait gave up");
+    if (!hS->done) fail(XCAL_ERR_TIMEOUT, "folded CG did not report completion");
+    if (profiling) {
+        float t = 0;
+        XCAL_CUDA(cudaEventElapsedTime(&t, ev[5], ev[6]));
+        prof_ms[5] += t;
+        prof_n[5] += hS->iter;
+        prof_n[4] += hS->iter + (hS->status == KS_ZERO_CURV ? 1 : 0);
+    }
 }
 
 // Mixed precision: FP64 defect correction around FP32 Krylov solves.  Each
@@ -1618,9 +1711,15 @@ void Case::solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, 
                        KScalars* hS, int gk, int* iters) {
     const int n = E.n;
     CSRView A = E.view();
-    kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
-    if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, n, E.P.p, E.P32.p);
-    if (SS.precond == XCAL_PRECOND_DILU) dilu_refresh(E, true);
+    const bool fold = use_fold(E, SS, false);
+    if (fold) {
+        build_fold(E, stream);
+        kr_fold_scale(stream, E.fold_mut(), E.nz.p, E.d_diag.p, E.P.p);
+    } else {
+        kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
+        if (SS.precond != XCAL_PRECOND_NONE) kr_to_float(stream, n, E.P.p, E.P32.p);
+        if (SS.precond == XCAL_PRECOND_DILU) dilu_refresh(E, true);
+    }
     KrylovVecs<float> V{ws.fx.p, ws.fr.p, ws.fz.p, ws.fp.p, ws.fq.p, ws.fv.p, ws.fs.p, ws.ft.p};
     hS->mixed = 1;
     hS->inner_rtol = cfg.inner_rtol > 0 ? cfg.inner_rtol : 1e-3;
@@ -1632,6 +1731,17 @@ void Case::solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, 
         hS->done = 0;
         hS->status = KS_RUNNING;
         XCAL_CUDA(cudaMemcpyAsync(S, hS, sizeof(KScalars), cudaMemcpyHostToDevice, stream));
+        if (fold) {
+            // scaled defect, inner solve, and the correction applied by the
+            // solve's own kernel (unless this defect met the target)
+            kr_fold_defect(stream, A, E.nz.p, b, field, E.P.p, V.r);
+            fold_iterate(E, field, V, S, hS, gk);
+            if (hS->outer_conv) break;
+            total += hS->iter;
+            if (hS->status == KS_ZERO_CURV || hS->status == KS_BREAKDOWN || hS->status == KS_TIRED) break;
+            if (hS->status == KS_SOLVED && hS->eps <= hS->eps_outer) break;
+            continue;
+        }
         if (SS.solver == XCAL_SOLVER_CG) {
             kr_defect(stream, A, E.nz.p, b, field, V.r, V.x);
             krylov_iterate<float>(E, SS, E.nz32.p, E.P32.p, (const float*)V.r, V.r, V, S, hS, gk);
@@ -1915,6 +2025,8 @@ void Case::capture_step() {
     if (cfg.precision == XCAL_PREC_MIXED) {
         kr_coop_capture_ok(true);
         kr_cluster_capture_ok(true);
+        // the folded inner CG's storage (uploads) cannot be made under capture
+        if (use_fold(P, cfg.p_solver, true)) build_fold(P, stream);
     }
     XCAL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {
@@ -1966,6 +2078,7 @@ void Case::run_step_graph(double res[4], double* courant) {
         last_iters[k] = h_iters[2 * k];
         if (h_iters[2 * k + 1] == KS_LOOP_CAP)
             fail(XCAL_ERR_TIMEOUT, "a Krylov solve did not finish within its loop-body cap");
+        note_status(k, h_iters[2 * k + 1]);
     }
     if (courant) *courant = h_res[GRES_CO];
 }
@@ -2002,8 +2115,10 @@ bool Case::simple_iteration(double res[4]) {  // Solvers_1_SIMPLE.jl:164-240
     for (int k = 0; k < 4; ++k)
         if (std::isnan(res[k]) || std::isinf(res[k])) fail(XCAL_ERR_DIVERGED, "residual is NaN/Inf");
     bool turb_conv = cfg.turbulence == XCAL_TURB_LAMINAR;
-    return r3[0] <= cfg.U_solver.convergence && r3[1] <= cfg.U_solver.convergence &&
-           r3[2] <= cfg.U_solver.convergence && rp <= cfg.p_solver.convergence && turb_conv;
+    // Uz enters the test on 3D meshes only (Solvers_1_SIMPLE.jl:220-223)
+    const bool uz_conv = mesh->dim == 2 || r3[2] <= cfg.U_solver.convergence;
+    return r3[0] <= cfg.U_solver.convergence && r3[1] <= cfg.U_solver.convergence && uz_conv &&
+           rp <= cfg.p_solver.convergence && turb_conv;
 }
 
 double Case::piso_step(double res[4]) {  // Solvers_2_PISO.jl:108-187
@@ -2035,6 +2150,16 @@ double Case::piso_step(double res[4]) {  // Solvers_2_PISO.jl:108-187
     res[2] = r3[2];
     res[3] = rp;
     return co;
+}
+
+void Case::set_inner_cg(int mode) {
+    if (mode == inner_cg) return;
+    sync();
+    inner_cg = mode;
+    if (step_graph) {
+        cudaGraphExecDestroy(step_graph);
+        step_graph = nullptr;
+    }
 }
 
 void Case::set_graph_mode(bool on) {

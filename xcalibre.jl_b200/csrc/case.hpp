@@ -1,13 +1,35 @@
 // case.hpp -- host objects behind the C ABI handles.
 #pragma once
 #include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
 
 #include "kernels.hpp"
 #include "xcal_internal.hpp"
 
+// A context may be used from several host threads at once (serving sets up
+// cases on worker threads while another thread iterates), so each thread
+// keeps its own last error message: a failure on one thread never shows up
+// as another thread's error.  Elements of an unordered_map keep their address
+// across insertions, so the pointer xcal_last_error returns stays valid until
+// the same thread's next failing call on this context.
 struct xcal_ctx {
     int device = 0;
-    std::string last_error;
+    void set_error(const std::string& msg) {
+        std::lock_guard<std::mutex> g(mu);
+        errors[std::this_thread::get_id()] = msg;
+    }
+    const char* last_error() {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = errors.find(std::this_thread::get_id());
+        return it == errors.end() ? "" : it->second.c_str();
+    }
+
+   private:
+    std::mutex mu;
+    std::unordered_map<std::thread::id, std::string> errors;
 };
 
 namespace xcal {
@@ -64,6 +86,14 @@ struct Equation {
     int base(int r) const { return slice[r / SELL_C] + r % SELL_C; }
     DBuf<double> nz, nz0, diag0, P;
     DBuf<float> nz32, P32;  // mixed precision: FP32 copies for the inner solves
+    // mixed precision, CG + Jacobi: off-diagonal slots of the Jacobi-scaled
+    // system (built at first use; values refreshed per solve)
+    DBuf<int> f_slice, f_col, f_map;
+    DBuf<unsigned char> f_len;
+    DBuf<float> f_val;
+    bool fold_built = false;
+    FoldView fold_view() const { return FoldView{n, f_slice.p, f_len.p, f_col.p, f_val.p}; }
+    FoldMut fold_mut() { return FoldMut{n, f_slice.p, f_len.p, f_col.p, f_map.p, f_val.p}; }
     DBuf<double> b[3];
     // DILU level schedules (rows grouped by dependency level)
     DBuf<int> d_lower_rows, d_upper_rows;
@@ -95,6 +125,7 @@ struct BCTable {
 struct KrylovWS {
     DBuf<double> x, dx, r, z, p, q, v, s, t, part0, part1;
     DBuf<float> fx, fr, fz, fp, fq, fv, fs, ft, fd;  // mixed precision inner vectors
+    DBuf<double> fpart;  // folded inner CG: block partials (2 x FOLD_MAX_BLOCKS)
     DBuf<unsigned int> bar;  // persistent CG: grid-barrier state (count, generation)
     DBuf<int> err;           // persistent CG: a barrier wait gave up
     DBuf<KScalars> S;  // [2]: U, p
@@ -141,6 +172,14 @@ struct Case {
     int iteration = 0;
     double time = 0.0;
     int last_iters[7] = {0, 0, 0, 0, 0, 0, 0};  // Ux, Uy, Uz, p, k, omega, wall distance
+    // Krylov status (KS_*) of each system's last solve, and how many solves
+    // since creation stopped at itmax (Solve_1_api.jl:302 warns on those)
+    int last_status[7] = {0, 0, 0, 0, 0, 0, 0};
+    long long itmax_hits = 0;
+    void note_status(int gk, int status) {
+        last_status[gk] = status;
+        if (status == KS_TIRED) ++itmax_hits;
+    }
     // timing
     double ms[6] = {0, 0, 0, 0, 0, 0};
     long long launches = 0;
@@ -153,6 +192,14 @@ struct Case {
     double prof_ms[6] = {0, 0, 0, 0, 0, 0};
     long long prof_n[6] = {0, 0, 0, 0, 0, 0};
     int persistent_cg = 1;  // CG (Jacobi / none) as one cooperative launch: 0 off, 1 auto width, else the width
+    // mixed-precision inner CG with Jacobi: 0 = on the Jacobi-scaled system
+    // (cg_folded.cu) where it fits, 1 = the canonical FP32 kernels, 2 + f =
+    // the scaled-system kernel in form f (launch shape), 2 + FOLD_NFORMS + f =
+    // form f with x and p kept in global memory
+    int inner_cg = 0;
+    int fold_form() const { return inner_cg >= 2 ? (inner_cg - 2) % FOLD_NFORMS : FOLD_DEFAULT_FORM; }
+    bool fold_smem() const { return inner_cg < 2 + FOLD_NFORMS; }
+    void set_inner_cg(int mode);  // drops a captured step graph of the other form
     int dilu_mode = 0;          // 0 = autotuned / size rule, 1 = one-block sweeps, 2 = per-level kernels
     void prof_reserve(int pairs);
     // Steady-state polling chunks of a Krylov solve (32 CG / 8 BiCGSTAB
@@ -233,6 +280,11 @@ struct Case {
                         const KrylovVecs<T>& V, KScalars* S, KScalars* hS, int gk);
     void solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, const double* b, KScalars* S,
                      KScalars* hS, int gk, int* iters);
+    // mixed precision, CG + Jacobi: whether the inner solves of E run on the
+    // Jacobi-scaled system (cg_folded.cu), and one such inner solve of the
+    // scaled defect in V.r (host-polled; field corrected by the kernel)
+    bool use_fold(const Equation& E, const xcal_solver_setup& SS, bool captured) const;
+    void fold_iterate(Equation& E, double* field, const KrylovVecs<float>& V, KScalars* S, KScalars* hS, int gk);
     int last_outer[7] = {0, 0, 0, 0, 0, 0, 0};  // mixed: defect-correction steps of the last solve per system
     bool tuned = false;
     void autotune();  // launch-shape autotuner (autotune.cu), once per case

@@ -247,4 +247,53 @@ void kr_outer_cond(cudaStream_t s, cudaGraphConditionalHandle h, KScalars* S, in
                    unsigned long long* launches);
 void kr_record(cudaStream_t s, const KScalars* S, int* out);
 
+// ---- mixed precision: FP32 inner CG on the Jacobi-scaled system (cg_folded.cu)
+// Off-diagonal entries of Ahat = M^1/2 A M^1/2 (M = diag(1/|a_ii|)) in
+// SELL-32 slices over the storage rows: entry m of row i at slice[i/32] +
+// i%32 + 32 m; len[i] = the row's off-diagonal count, bit 7 set when its
+// diagonal is negative (ahat_ii = -1); map = the slot of the same entry in
+// the equation's own SELL storage.
+struct FoldView {
+    int n;
+    const int* slice;
+    const unsigned char* len;
+    const int* col;
+    const float* val;
+};
+struct FoldMut {
+    int n;
+    const int* slice;
+    unsigned char* len;
+    const int* col;
+    const int* map;
+    float* val;
+};
+// kernel forms of the folded CG (block size / row pairing; cg_folded.cu)
+constexpr int FOLD_NFORMS = 4;
+// most blocks of a folded-CG launch (one per SM); its two partial buffers
+// hold this many doubles each
+constexpr int FOLD_MAX_BLOCKS = 1024;
+constexpr int FOLD_DEFAULT_FORM = 3;  // 1024 threads (measured fastest at 2.1M rows)
+struct FoldShape {
+    int form = 0, nt = 0, blocks = 0, rows = 0, smem = 0;
+    bool smem_p = false, smem_x = false;
+};
+// blocks = 0: the system is too large for the folded CG.  vectors_in_smem:
+// keep x and p in shared memory where they fit (else both in global memory;
+// the same arithmetic either way)
+FoldShape fold_shape(int n, int form = FOLD_DEFAULT_FORM, bool vectors_in_smem = true);
+// r = (float)(sqrt(P) (b - A field)) in FP64 (P: FP64 Jacobi inverse diagonal)
+void kr_fold_defect(cudaStream_t s, const CSRView& A, const double* nz, const double* b, const double* field,
+                    const double* P, float* r);
+// scaled off-diagonal values and diagonal signs from the FP64 matrix and P
+void kr_fold_scale(cudaStream_t s, const FoldMut& F, const double* nz, const int* diag, const double* P);
+// the whole inner solve after kr_cg_start(rhat, rhat, P0), with field +=
+// sqrt(P) xhat applied at its end unless S->outer_conv; false: too large
+// (nothing launched).  xg: an n-float buffer used when x does not fit
+// shared memory; part, part2: FOLD_MAX_BLOCKS doubles each.
+bool kr_cgf_persist(cudaStream_t s, const FoldView& F, float* r, float* P0, float* P1, float* xg, double* field,
+                    const double* Pj, KScalars* S, double* part, double* part2, unsigned int* bar, int* err,
+                    int max_iters, bool reset_err = true, int form = FOLD_DEFAULT_FORM,
+                    bool vectors_in_smem = true);
+
 }  // namespace xcal

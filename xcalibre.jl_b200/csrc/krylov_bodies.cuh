@@ -595,7 +595,7 @@ __device__ __forceinline__ void dilu_D_row(const CSRView& A, const double* __res
 // block within one bounded wait.
 constexpr long BAR_SPIN_LIMIT = 1L << 22;
 __device__ __forceinline__ bool grid_barrier(unsigned int* count, int nblocks, unsigned int& nb, int* err,
-                                             int* sh_err) {
+                                             int* sh_err, long spin_limit = BAR_SPIN_LIMIT) {
     __syncthreads();
     if (nblocks == 1) return true;
     if (threadIdx.x == 0) {
@@ -605,7 +605,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* count, int nblocks, u
         long spins = 0;
         int e = 0;
         while ((int)(*(volatile unsigned int*)count - target) < 0) {
-            if (++spins > BAR_SPIN_LIMIT) {
+            if (++spins > spin_limit) {
                 e = 1;
                 *(volatile int*)err = 1;
                 break;

@@ -19,6 +19,15 @@ Reported: per-request time-to-converged (finish - arrival, queueing
 included), p50/p99, throughput in cases/s and Mcell-iterations/s.  A case's
 arithmetic does not depend on what it shares the batch with, so each result
 is the same alone and in the mix.
+
+Failures stay with their request: a request larger than the budget is
+rejected, one whose set-up raises is failed, and one whose residual becomes
+NaN/Inf leaves the batch as diverged (the library retires it without
+touching the other cases); each gets a Result with that status and the
+stream goes on.  Device memory stays within the budget: a case set up ahead
+of admission holds a reservation of its footprint from the moment its set-up
+is submitted, and a finished case keeps its charge until its memory is
+actually freed.
 """
 from __future__ import annotations
 
@@ -30,6 +39,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import api as A
+from ._lib import XcalError
 from . import cases as K
 from .foam import Mesh3, build_mesh3
 from .meshgen import cavity_polymesh, channel_polymesh
@@ -112,6 +122,11 @@ class Result:
     residuals: np.ndarray
     U: np.ndarray | None = None
     p: np.ndarray | None = None
+    # "converged", "max_iters" (cap reached first), "diverged" (NaN/Inf
+    # residual), "rejected" (footprint above the budget), "failed" (set-up
+    # raised); error: the message of the last two
+    status: str = "converged"
+    error: str | None = None
 
     @property
     def latency(self) -> float:
@@ -126,6 +141,16 @@ class _Done:
 
     def result(self):
         return self.value
+
+
+class _Failed:
+    """A failed set-up with the interface of a future."""
+
+    def __init__(self, exc):
+        self.exc = exc
+
+    def result(self):
+        raise self.exc
 
 
 @dataclass
@@ -170,144 +195,227 @@ class Server:
     build_threads: int = 2
     prepare_ahead: int = 4
 
+    def footprint(self, req: Request) -> int:
+        """Device bytes the request's case will hold (an upper bound, from
+        the mesh sizes, before anything is allocated)."""
+        return A.footprint_estimate(req.build(), self.precision, dilu_U=True, dilu_p=False)
+
     def _prepare(self, req: Request):
-        """A request's case ready for batch.add: (footprint, case, device
-        mesh, configuration kept alive); case None when it exceeds the budget."""
-        mesh = req.build()
-        est = A.footprint_estimate(mesh, self.precision, dilu_U=True, dilu_p=False)
-        if est > self.budget_bytes:
-            return est, None, None, None
+        """A request's case ready for batch.add: (case, device mesh,
+        configuration kept alive).  Frees what it made if a step fails."""
         model, config, pref = req.config(self.precision, self.max_iters, self.convergence)
         cfg, keep = A.build_config(model, config, pref=pref)
-        dm = A.DeviceMesh(self.ctx, mesh)
-        case = A.Case(dm, cfg)
-        case.set_field(A._abi.FIELD_U, model.momentum.U)
-        case.set_field(A._abi.FIELD_P, model.momentum.p)
-        return est, case, dm, (cfg, keep)
+        dm = A.DeviceMesh(self.ctx, req.build())
+        try:
+            case = A.Case(dm, cfg)
+        except Exception:
+            dm.close()
+            raise
+        try:
+            case.set_field(A._abi.FIELD_U, model.momentum.U)
+            case.set_field(A._abi.FIELD_P, model.momentum.p)
+        except Exception:
+            case.close()
+            dm.close()
+            raise
+        return case, dm, (cfg, keep)
+
+    @staticmethod
+    def _free(case, dm):
+        """Close a case and its device mesh; a failure to close one is not
+        allowed to leak the other or to end the stream."""
+        for h in (case, dm):
+            try:
+                if h is not None:
+                    h.close()
+            except Exception:
+                pass
 
     def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         queue: deque = deque()
         active: list[_Active] = []
         results: list[Result] = []
-        retired: list = []  # (case, device mesh) out of the batch, not yet freed
+        retired: list = []  # (case, device mesh, charge) out of the batch, not yet freed
         pool = ThreadPoolExecutor(self.build_threads) if self.build_threads > 0 else None
-        builds: dict = {}
+        builds: dict = {}   # rid -> (future of _prepare, reserved bytes)
         batch = A.Batch(self.ctx, self.max_cases, self.budget_bytes)
+        # device bytes: `used` = admitted cases plus finished ones not yet
+        # freed; `reserved` = cases being set up or set up ahead of admission
         used = 0
+        reserved = 0
         t0 = time.perf_counter()
+
+        def now():
+            return time.perf_counter() - t0
+
+        def fail_request(req, status, msg):
+            t = now()
+            results.append(Result(req.rid, req.n_cells, req.arrival, t, t, 0, False, np.full(4, np.nan),
+                                  status=status, error=msg))
+
+        def free_retired():
+            nonlocal used
+            for case, dm, charge in retired:
+                self._free(case, dm)
+                used -= charge
+            retired.clear()
+
+        def finish(a, status, r, U=None, p=None):
+            nonlocal used
+            results.append(Result(a.req.rid, a.req.n_cells, a.req.arrival, a.admitted, now(), a.iters,
+                                  status == "converged", r, U, p, status=status))
+            retired.append((a.case, a.dmesh, a.charge))
+            active.remove(a)
+
         try:
             while pending or queue or active:
-                now = time.perf_counter() - t0
-                while pending and (pending[0].arrival <= now or not realtime):
+                while pending and (pending[0].arrival <= now() or not realtime):
                     queue.append(pending.popleft())
+                # set-up ahead of admission, each under a reservation of its
+                # footprint, never past the budget
                 if pool is not None:
                     for req in list(queue)[: self.prepare_ahead]:
-                        if req.rid not in builds:
-                            builds[req.rid] = pool.submit(self._prepare, req)
-                # admission, in arrival order, by device-memory footprint
+                        if req.rid in builds:
+                            continue
+                        est = self.footprint(req)
+                        if est > self.budget_bytes:
+                            continue  # rejected at admission
+                        if used + reserved + est > self.budget_bytes:
+                            break
+                        reserved += est
+                        builds[req.rid] = (pool.submit(self._prepare, req), est)
+                # admission, in arrival order, by device-memory footprint;
+                # a request not set up ahead is reserved and set up here
                 ta = time.perf_counter()
                 while queue and len(active) < self.max_cases:
                     req = queue[0]
-                    fut = builds.get(req.rid)
-                    if fut is None:
-                        fut = builds[req.rid] = _Done(self._prepare(req))
-                    est, case, dm, keep = fut.result()
-                    if case is None:
-                        raise ValueError(f"request {req.rid} needs {est} bytes, more than the budget")
-                    if used + est > self.budget_bytes or not batch.add(case, est):
-                        break  # stays prepared until it fits
+                    if req.rid not in builds:
+                        est = self.footprint(req)
+                        if est > self.budget_bytes:
+                            queue.popleft()
+                            fail_request(req, "rejected",
+                                         f"needs {est} bytes, more than the budget {self.budget_bytes}")
+                            continue
+                        if used + reserved + est > self.budget_bytes:
+                            if retired:
+                                free_retired()
+                                continue
+                            break
+                        reserved += est
+                        try:
+                            builds[req.rid] = (_Done(self._prepare(req)), est)
+                        except Exception as e:
+                            builds[req.rid] = (_Failed(e), est)
+                    fut, est = builds[req.rid]
+                    try:
+                        case, dm, keep = fut.result()
+                    except Exception as e:  # this request's set-up failed; the stream goes on
+                        builds.pop(req.rid)
+                        reserved -= est
+                        queue.popleft()
+                        fail_request(req, "failed", f"{type(e).__name__}: {e}")
+                        continue
+                    if not batch.add(case, est):
+                        break  # stays set up, under its reservation, until it fits
                     builds.pop(req.rid)
+                    reserved -= est
                     used += est
                     queue.popleft()
-                    active.append(_Active(req, case, dm, keep, est, time.perf_counter() - t0))
+                    active.append(_Active(req, case, dm, keep, est, now()))
                 self.admit_s += time.perf_counter() - ta
-                self.timeline.append((time.perf_counter() - t0, len(active), len(queue), used))
+                self.timeline.append((now(), len(active), len(queue), used))
                 if not active:
                     if pending and realtime:
                         tw = time.perf_counter()
-                        time.sleep(max(0.0, min(0.05, pending[0].arrival - (time.perf_counter() - t0))))
+                        time.sleep(max(0.0, min(0.05, pending[0].arrival - now())))
                         self.idle_s += time.perf_counter() - tw
+                    elif queue and retired:
+                        free_retired()
                     continue
                 if self.solo_tail and len(active) == 1 and not queue and not pending:
                     a = active[0]
                     ti = time.perf_counter()
                     batch.remove(a.case)
                     a.case.set_graph_mode(True)
-                    r, ok = a.case.simple_iterate(max(0, self.max_iters - a.iters))
+                    try:
+                        r, ok = a.case.simple_iterate(max(0, self.max_iters - a.iters))
+                    except XcalError as e:
+                        if e.code != A._abi.XCAL_ERR_DIVERGED:
+                            raise
+                        self.iterate_s += time.perf_counter() - ti
+                        finish(a, "diverged", np.full(4, np.nan))
+                        results[-1].error = str(e)
+                        continue
                     self.iterate_s += time.perf_counter() - ti
                     a.iters += len(r)
-                    done_t = time.perf_counter() - t0
                     U = a.case.get_field(A._abi.FIELD_U) if self.keep_fields else None
                     p = a.case.get_field(A._abi.FIELD_P) if self.keep_fields else None
                     last = r[-1].copy() if len(r) else np.zeros(4)
-                    results.append(Result(a.req.rid, a.req.n_cells, a.req.arrival, a.admitted, done_t, a.iters, ok,
-                                          last, U, p))
-                    retired.append((a.case, a.dmesh))
-                    used -= a.charge
-                    active.remove(a)
+                    finish(a, "converged" if ok else "max_iters", last, U, p)
                     continue
                 ti = time.perf_counter()
+                members = list(batch.cases)
                 res, conv = batch.simple_iterate()
                 self.iterate_s += time.perf_counter() - ti
                 self.phase_ms = batch.timings()
-                done_t = time.perf_counter() - t0
-                finished = []
-                for k, a in enumerate(active):
-                    a.iters += 1
-                    if conv[k] or a.iters >= self.max_iters:
-                        finished.append((a, bool(conv[k]), res[k].copy()))
                 tr = time.perf_counter()
-                for a, ok, r in finished:
-                    U = a.case.get_field(A._abi.FIELD_U) if self.keep_fields else None
-                    p = a.case.get_field(A._abi.FIELD_P) if self.keep_fields else None
-                    results.append(Result(a.req.rid, a.req.n_cells, a.req.arrival, a.admitted, done_t, a.iters, ok,
-                                          r, U, p))
-                    batch.remove(a.case)
-                    retired.append((a.case, a.dmesh))
-                    used -= a.charge
-                    active.remove(a)
+                by_case = {id(a.case): a for a in active}
+                for k, c in enumerate(members):
+                    a = by_case[id(c)]
+                    a.iters += 1
+                    if c in batch.last_diverged:  # already out of the batch
+                        finish(a, "diverged", res[k].copy())
+                        results[-1].error = "residual became NaN/Inf"
+                    elif conv[k] or a.iters >= self.max_iters:
+                        U = a.case.get_field(A._abi.FIELD_U) if self.keep_fields else None
+                        p = a.case.get_field(A._abi.FIELD_P) if self.keep_fields else None
+                        batch.remove(a.case)
+                        finish(a, "converged" if conv[k] else "max_iters", res[k].copy(), U, p)
                 if len(retired) >= self.free_every or (not active and not queue and not pending):
-                    for case, dm in retired:
-                        case.close()
-                        dm.close()
-                    retired.clear()
+                    free_retired()
                 self.retire_s += time.perf_counter() - tr
         finally:
             tc = time.perf_counter()
             if pool is not None:
                 pool.shutdown(wait=True)
-            for fut in builds.values():  # set up but never admitted
-                est, case, dm, keep = fut.result()
-                if case is not None:
-                    case.close()
-                    dm.close()
-            for case, dm in retired:
-                case.close()
-                dm.close()
+            for fut, _ in builds.values():  # set up but never admitted
+                try:
+                    case, dm, keep = fut.result()
+                except Exception:
+                    continue
+                self._free(case, dm)
+            free_retired()
             for a in active:
                 try:
                     batch.remove(a.case)
                 except Exception:
                     pass
-                a.case.close()
-                a.dmesh.close()
-            batch.close()
+                self._free(a.case, a.dmesh)
+            try:
+                batch.close()
+            except Exception:
+                pass
             self.cleanup_s += time.perf_counter() - tc
         self.wall = time.perf_counter() - t0
         return sorted(results, key=lambda r: r.rid)
 
 
 def summarize(results: list[Result], wall: float) -> dict:
-    lat = np.array([r.latency for r in results]) * 1e3
-    cell_iters = sum(r.n_cells * r.iterations for r in results)
+    """Throughput and time-to-result over the solved requests (rejected and
+    failed ones are counted, not timed)."""
+    solved = [r for r in results if r.status in ("converged", "max_iters", "diverged")]
+    lat = np.array([r.latency for r in solved]) * 1e3
+    cell_iters = sum(r.n_cells * r.iterations for r in solved)
     return {
         "cases": len(results),
         "converged": int(sum(r.converged for r in results)),
+        "status_counts": {st: sum(r.status == st for r in results)
+                          for st in ("converged", "max_iters", "diverged", "rejected", "failed")},
         "wall_s": wall,
         "cases_per_s": len(results) / wall if wall > 0 else None,
         "mcell_iters_per_s": cell_iters / wall / 1e6 if wall > 0 else None,
         "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
         "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
-        "mean_iterations": float(np.mean([r.iterations for r in results])) if results else None,
+        "mean_iterations": float(np.mean([r.iterations for r in solved])) if solved else None,
     }
