@@ -299,6 +299,17 @@ const char* xcal_last_error(const xcal_ctx* ctx);
 /* library version string */
 const char* xcal_version(void);
 
+/* ---- the library's exp / log / tanh -----------------------------------------
+ * No counterpart in the reference.  The k-omega SST blending (tanh) and the
+ * wall functions (log) call the library's own restatements of these
+ * functions, written from +, *, / and ldexp/frexp so the device and the host
+ * compute them alike (Cody-Waite reduction with a Taylor series for exp of
+ * y <= 0; the atanh series for log of x > 0; tanh(x) = (1 - e^-2x) /
+ * (1 + e^-2x) for x >= 0).  This evaluates those same functions, compiled
+ * for the host, on n inputs: which 0 = exp, 1 = log, 2 = tanh; for testing
+ * their error against the C library.  Needs no device. */
+int32_t xcal_det_math(int32_t which, const double* in, double* out, int64_t n);
+
 /* ---- struct layouts, for bindings -----------------------------------------
  * No counterpart in the reference (it has no C boundary).  sizeof and the
  * field offsets of the structs above as this library was compiled, so a
@@ -428,6 +439,61 @@ int32_t xcal_turbulence(xcal_case* cs);
 /* max_courant_number! (Solvers_0_functions.jl:253-276) */
 int32_t xcal_max_courant(xcal_case* cs, double* courant);
 
+/* ---- equations from the operator DSL ----------------------------------------
+ * (Time + Divergence - Laplacian + Si == Source) -> ScalarEquation
+ * (ModelFramework_0_types.jl:18-100, 135-165; ModelFramework_1_operations.jl:
+ * 3-63): the terms in the order written, each with the sign the DSL gave it
+ * (`-` sets -1 on the operator after it), the sources likewise.  The drivers
+ * (xcal_simple_iterate, xcal_piso_step) assemble their own equations; these
+ * entry points take any scalar equation of these operators on a case's mesh,
+ * with its own boundary conditions, and assemble, constrain and solve it
+ * with the same kernels' arithmetic. */
+enum { XCAL_OP_TIME = 0, XCAL_OP_DIVERGENCE = 1, XCAL_OP_LAPLACIAN = 2, XCAL_OP_SI = 3 };
+typedef struct {
+    int32_t op;          /* XCAL_OP_*                                        */
+    int32_t scheme;      /* Time: XCAL_TIME_*; Divergence: XCAL_DIV_*;
+                            Laplacian (Linear) and Si: 0                     */
+    double sign;         /* +1, or -1 where the DSL put a minus before it    */
+    const double* flux;  /* Divergence, Laplacian: per face [n_faces];
+                            Time, Si: per cell [n_cells]; original numbering;
+                            NULL: the constant `value` (a ConstantScalar)    */
+    double value;
+} xcal_term;
+typedef struct {         /* Source(field), Src{F,S} (ModelFramework_0_types.jl:81-93) */
+    double sign;
+    const double* field; /* per cell [n_cells]; NULL: the constant `value`   */
+    double value;
+} xcal_source;
+typedef struct xcal_equation xcal_equation;
+/* `terms -> ScalarEquation(phi, bcs)` on cs's mesh: the CSR pattern of
+ * sparse_matrix_connectivity (ModelFramework_0_types.jl:223-243), at most 8
+ * terms and 8 sources (copied; host arrays are read during the call), the
+ * field's boundary conditions (no periodic pairs).  Runs on cs's stream. */
+int32_t xcal_equation_create(xcal_case* cs, int32_t n_terms, const xcal_term* terms, int32_t n_sources,
+                             const xcal_source* sources, int32_t n_bcs, const xcal_bc* bcs, xcal_equation** out);
+int32_t xcal_equation_destroy(xcal_equation* eq);
+/* discretise!(eqn, prev, config) (Discretise_2_generated_distretisation.jl:
+ * 90-168): prev [n_cells] = the previous values Time{Euler} reads (NULL
+ * without a Time{Euler} term), dt its time step */
+int32_t xcal_equation_discretise(xcal_equation* eq, const double* prev, double dt);
+/* apply_boundary_conditions!(eqn, BCs) (Discretise_5_apply_bcs.jl) for a
+ * scalar field: every term's boundary functor per boundary face
+ * (boundary_conditions/*.jl); phi [n_cells] = the field's current values
+ * (Extrapolated reads them; NULL when no boundary needs them) */
+int32_t xcal_equation_apply_bcs(xcal_equation* eq, const double* phi);
+int32_t xcal_equation_nnz(const xcal_equation* eq, int64_t* nnz);
+/* the assembled system in the original numbering, rows in the reference's
+ * CSR order: rowptr [n_cells+1], colval [nnz], nzval [nnz], b [n_cells]
+ * (any may be NULL) */
+int32_t xcal_equation_get_system(const xcal_equation* eq, int32_t* rowptr, int32_t* colval, double* nzval,
+                                 double* b);
+/* update_preconditioner! + solve_system! (Solve_1_api.jl:268-307) in FP64:
+ * phi [n_cells] is the initial guess and receives the solution; residual =
+ * the scaled residual (:441-464), iterations = Krylov iterations (either may
+ * be NULL) */
+int32_t xcal_equation_solve(xcal_equation* eq, const xcal_solver_setup* setup, double* phi, double* residual,
+                            int32_t* iterations);
+
 /* ---- allocation-free residual ---------------------------------------------
  * No counterpart in the reference: an extra entry point for callers that
  * cannot allocate device memory (inside CUDA graph capture, under a fixed
@@ -514,12 +580,14 @@ int32_t xcal_case_solve_report(const xcal_case* cs, int32_t* iters7, int32_t* st
  * inner precision).  0 (default) = CG on the Jacobi-scaled system
  * M^1/2 A M^1/2 (the same iteration in exact arithmetic, deterministic, its
  * own reduction order) where the system fits one block per SM, else as 1;
- * 1 = the FP32 form of the FP64 path's kernels; 2..5 = the scaled-system
- * kernel in launch shape 0..3 (threads per block, rows in flight per
- * thread); 6..9 = the same shapes with the iterate and the direction kept in
- * global memory instead of shared memory (bit-identical to 2..5).  All meet
- * the same stopping tests; results agree within the mixed-precision
- * tolerance. */
+ * 1 = the FP32 form of the FP64 path's kernels; 2 + v = the scaled-system
+ * kernel with v = s + 4 g + 8 w: s (0..3) its launch shape (768 or 1024
+ * threads per block, with or without the next row's loads issued early),
+ * g = 1 the iterate and the direction kept in global memory instead of
+ * shared memory, w = 1 per-slice slot widths even where one uniform width
+ * would do; g and w change where data lives, not the results (2 + v gives
+ * the results of 2 + s bit for bit).  All meet the same stopping tests;
+ * results agree within the mixed-precision tolerance. */
 int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode);
 /* launch-shape autotuner (runs on first use, or now): out6 = for U then p,
  * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU as

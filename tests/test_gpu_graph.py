@@ -113,6 +113,7 @@ def test_persistent_cg_identical(x, ctx, prec):
         dm = x.DeviceMesh(ctx, mesh)
         c = x.Case(dm, cfg)
         c.set_persistent(persist)
+        c.set_inner_cg(1)  # mixed: the canonical FP32 kernels in every form
         c.set_field(x._abi.FIELD_U, model.momentum.U)
         c.set_field(x._abi.FIELD_P, model.momentum.p)
         c.set_profiling(True)

@@ -86,7 +86,7 @@ def _tight_pressure(x, ctx, mesh, prec, inner_cg=None):
     return p
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5, 13])
 def test_inner_cg_forms_tight(x, ctx, mode):
     """Every form of the FP32 inner CG (Jacobi-scaled system in each launch
     shape; the canonical kernels) meets the tight-solve bound against FP64."""
@@ -97,14 +97,17 @@ def test_inner_cg_forms_tight(x, ctx, mode):
 
 
 @pytest.mark.parametrize("form", [0, 1, 2, 3])
-def test_inner_cg_vectors_in_global_memory_identical(x, ctx, form):
+def test_inner_cg_layouts_identical(x, ctx, form):
     """The scaled-system kernel with x and p in global memory (the layout
-    of systems too large for shared memory) gives the shared-memory layout's
-    result bit for bit: only where the vectors live differs."""
+    of systems too large for shared memory), with per-slice slot widths (the
+    layout of meshes whose rows differ widely in length), and with both,
+    gives the default layout's result bit for bit: only where data lives
+    differs."""
     mesh = x.build_mesh3(x.channel_polymesh(40, 24, 20, seed=4))
     a = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=2 + form)
-    b = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=6 + form)
-    assert np.array_equal(a, b)
+    for extra in (4, 8, 12):
+        b = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=2 + form + extra)
+        assert np.array_equal(a, b), extra
 
 
 def test_inner_cg_graph_mode_identical(x, ctx):

@@ -54,6 +54,7 @@ def test_correctors_batch_matches_single(x, ctx, prec, limit):
         cfg, keep = x.build_config(model, config, ncorrectors=2)
         dm = x.DeviceMesh(ctx, mesh)
         c = x.Case(dm, cfg)
+        c.set_inner_cg(1)  # the batch's FP32 inner CG form (a case takes it when admitted)
         c.set_field(x._abi.FIELD_U, model.momentum.U)
         c.set_field(x._abi.FIELD_P, model.momentum.p)
         return c, (dm, keep)

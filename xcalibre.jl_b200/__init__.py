@@ -13,6 +13,8 @@ from .api import (B200Backend, Bicgstab, Case, CellBased, Cg, Configuration, Con
                   assign, build_config, construct_periodic, initialise_, launch_count, run_, Batch,
                   footprint_estimate, VTK, OpenFOAM, save_checkpoint, load_checkpoint, boundary_average, JacobiSmoother,
                   KOmega, KOmegaSST, OmegaWallFunction, KWallFunction, NutWallFunction)
+from . import dsl
+from .dsl import Divergence, Equation, Laplacian, ScalarEquation, Si, Source, Time
 from .foam import Mesh3, build_mesh3
 from .foamio import FOAM3D_mesh, read_polymesh, write_polymesh
 from .unv import UNV2D_mesh, UNV3D_mesh

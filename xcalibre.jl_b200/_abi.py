@@ -130,6 +130,18 @@ class ConfigDesc(C.Structure):
     ]
 
 
+OP_TIME, OP_DIVERGENCE, OP_LAPLACIAN, OP_SI = 0, 1, 2, 3
+
+
+class TermDesc(C.Structure):
+    _fields_ = [("op", C.c_int32), ("scheme", C.c_int32), ("sign", C.c_double), ("flux", _pf64),
+                ("value", C.c_double)]
+
+
+class SourceDesc(C.Structure):
+    _fields_ = [("sign", C.c_double), ("field", _pf64), ("value", C.c_double)]
+
+
 def ptr(a: np.ndarray, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 

@@ -69,6 +69,15 @@ SIGNATURES = {
     "xcal_abi_layout": (_i32, [_i32, C.POINTER(C.c_int64), _i32]),
     "xcal_case_solve_report": (_i32, [_vp, _pi, _pi, _pi64]),
     "xcal_check_bounded_wait": (_i32, [_vp, _i64, _pi, _pi, _pi]),
+    "xcal_det_math": (_i32, [_i32, _pd, _pd, _i64]),
+    "xcal_equation_create": (_i32, [_vp, _i32, C.POINTER(_abi.TermDesc), _i32, C.POINTER(_abi.SourceDesc), _i32,
+                                    C.POINTER(_abi.BCDesc), C.POINTER(_vp)]),
+    "xcal_equation_destroy": (_i32, [_vp]),
+    "xcal_equation_discretise": (_i32, [_vp, _pd, C.c_double]),
+    "xcal_equation_apply_bcs": (_i32, [_vp, _pd]),
+    "xcal_equation_nnz": (_i32, [_vp, _pi64]),
+    "xcal_equation_get_system": (_i32, [_vp, _pi, _pi, _pd, _pd]),
+    "xcal_equation_solve": (_i32, [_vp, C.POINTER(_abi.SolverSetupDesc), _pd, _pd, _pi]),
     "xcal_case_get_profile": (_i32, [_vp, _i32, _pd, _pi64]),
     "xcal_residual_noalloc": (_i32, [_i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, _i32]),
     "xcal_footprint_estimate": (_i32, [_i64, _i64, _i64, _i32, _i32, _i32, _pi64]),

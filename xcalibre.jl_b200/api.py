@@ -865,8 +865,9 @@ class Case:
     def set_inner_cg(self, mode: int):
         """Mixed precision, CG + Jacobi inner solves: 0 = on the Jacobi-scaled
         system (default), 1 = the FP32 form of the FP64 path's kernels,
-        2..5 = the scaled-system kernel in launch shape 0..3, 6..9 = those
-        shapes with x and p in global memory (same results as 2..5)."""
+        2 + s + 4 g + 8 w = the scaled-system kernel in launch shape s (0..3),
+        with x and p in global memory (g = 1) and per-slice slot widths
+        (w = 1); g and w give the same results as 2 + s."""
         self._chk(lib().xcal_case_set_inner_cg(self.h, int(mode)))
 
     def checkpoint(self) -> dict:

@@ -7,6 +7,7 @@
 #include <new>
 
 #include "case.hpp"
+#include "dev_common.cuh"
 #include "kernels.hpp"
 
 namespace xcal {
@@ -43,6 +44,13 @@ static int select_device(xcal_ctx* ctx) {
 extern "C" {
 
 const char* xcal_version(void) { return "xcal_b200 0.1 (sm_100a, FP64 hot path)"; }
+
+int32_t xcal_det_math(int32_t which, const double* in, double* out, int64_t n) {
+    if (!in || !out || n < 0 || which < 0 || which > 2) return XCAL_ERR_INVALID;
+    for (int64_t i = 0; i < n; ++i)
+        out[i] = which == 0 ? det_exp_neg(in[i]) : which == 1 ? det_log(in[i]) : det_tanh_pos(in[i]);
+    return XCAL_OK;
+}
 
 #define XCAL_OFF(T, f) (int64_t) offsetof(T, f)
 int32_t xcal_abi_layout(int32_t which, int64_t* out, int32_t cap) {
@@ -436,7 +444,7 @@ int32_t xcal_case_solve_report(const xcal_case* cs, int32_t* iters7, int32_t* st
 }
 
 int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode) {
-    if (!cs || mode < 0 || mode >= 2 + 2 * FOLD_NFORMS) return XCAL_ERR_INVALID;
+    if (!cs || mode < 0 || mode >= 2 + 16) return XCAL_ERR_INVALID;
     XCAL_GUARD(cs->c->ctx, cs->c->set_inner_cg(mode));
 }
 

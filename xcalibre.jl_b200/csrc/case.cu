@@ -341,9 +341,14 @@ static DevMesh* upload_mesh_ordered(const xcal_mesh_desc* d, cudaStream_t s, std
 // Off-diagonal SELL-32 storage of an equation for the folded FP32 CG
 // (cg_folded.cu): per 32-row slice, width = the longest row's off-diagonal
 // count; each row keeps its entries' order with the diagonal left out; map =
-// the entry's slot in E's own storage.  Built once, on first use.
-static void build_fold(Equation& E, cudaStream_t s) {
-    if (E.fold_built) return;
+// the entry's slot in E's own storage.  When padding every slice to the
+// longest row of all costs at most a quarter more slots (hexahedral meshes:
+// 6 per row), every slice takes that width and padding slots hold the row's
+// own column (value 0), so the kernel reads a fixed number of slots per row
+// at computed addresses.  Built once, on first use.
+static void build_fold(Equation& E, cudaStream_t s, bool uniform_ok) {
+    if (E.fold_built && E.fold_uniform_ok == uniform_ok) return;
+    E.fold_uniform_ok = uniform_ok;
     const int n = E.n, nsl = (n + SELL_C - 1) / SELL_C;
     std::vector<int> fsl(nsl + 1, 0);
     std::vector<unsigned char> flen(n);
@@ -352,15 +357,25 @@ static void build_fold(Equation& E, cudaStream_t s) {
         if (E.len[r] - 1 > 127) fail(XCAL_ERR_UNSUPPORTED, "folded CG: a row has more than 127 off-diagonals");
         flen[r] = (unsigned char)(E.len[r] - 1);
     }
+    long narrow = 0;
+    int W = 0;
     for (int sl = 0; sl < nsl; ++sl) {
         int w = 0;
         for (int r = sl * SELL_C; r < std::min(n, (sl + 1) * SELL_C); ++r) w = std::max(w, (int)flen[r]);
         fsl[sl + 1] = fsl[sl] + SELL_C * w;
+        narrow += (long)SELL_C * w;
+        W = std::max(W, w);
     }
+    const bool uniform = uniform_ok && W > 0 && (long)nsl * SELL_C * W <= narrow + narrow / 4 &&
+                         (long)nsl * SELL_C * W <= 2147483647L;
+    if (uniform)
+        for (int sl = 0; sl <= nsl; ++sl) fsl[sl] = SELL_C * W * sl;
     const long nslots = fsl[nsl];
     std::vector<int> fcol(nslots, 0), fmap(nslots, 0);
     for (int r = 0; r < n; ++r) {
         const int b = E.base(r), fb = fsl[r / SELL_C] + r % SELL_C;
+        if (uniform)
+            for (int m = flen[r]; m < W; ++m) fcol[fb + SELL_C * m] = r;  // padding: own column, value 0
         int m = 0;
         for (int k = 0; k < E.len[r]; ++k) {
             const int slot = b + SELL_C * k;
@@ -377,13 +392,14 @@ static void build_fold(Equation& E, cudaStream_t s) {
     E.f_val.alloc(nslots);
     E.f_val.zero(s);
     XCAL_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    E.f_W = uniform ? W : 0;
     E.fold_built = true;
 }
 
 // ---------------------------------------------------------------------------
 // equation pattern (sparse_matrix_connectivity + extend_matrix + sparsecsr)
 // ---------------------------------------------------------------------------
-static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal_bc>& bcs, int nvec,
+void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal_bc>& bcs, int nvec,
                            bool need_dilu, cudaStream_t s) {
     int n = E.n = m.nC;
     E.use_block = n <= DILU_BLOCK_MAX_ROWS;
@@ -560,7 +576,7 @@ static void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal
 // ---------------------------------------------------------------------------
 // BC tables
 // ---------------------------------------------------------------------------
-static void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int nbc, int ncomp, const Equation* E,
+void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int nbc, int ncomp, const Equation* E,
                            cudaStream_t s) {
     int nB = m.nB;
     T.src.assign(bcs, bcs + nbc);
@@ -1172,8 +1188,10 @@ void Case::set_reference() {
 
 void Case::update_precond(int eqn) {
     const SolveRef R = solve_ref(eqn, 0);
-    Equation& E = *R.E;
-    const int pt = R.SS.precond;
+    update_precond_E(*R.E, R.SS.precond);
+}
+
+void Case::update_precond_E(Equation& E, int pt) {
     if (pt == XCAL_PRECOND_JACOBI) {
         kr_jacobi_update(stream, E.view(), E.nz.p, E.P.p);
     } else if (pt == XCAL_PRECOND_DILU) {
@@ -1539,7 +1557,7 @@ void Case::solve_captured(int eqn, int comp) {
                 kr_loop_cond(stream, h, S, cap, (int)(t_launch_count - k0) + 1, dlaunch.p);
             });
         kr_finish(stream, n, V.x, ws.dx.p, field);
-    } else if (use_fold(E, SS, true) && E.fold_built) {
+    } else if (use_fold(E, SS, true) && E.fold_built && E.fold_uniform_ok == fold_uniform_ok()) {
         // folded FP32 CG (cg_folded.cu): each defect step is the scaled
         // defect, the start, and one cooperative node that also applies the
         // correction
@@ -1630,7 +1648,12 @@ double Case::solve_system(int eqn, int comp, int* iters) {
         solve_captured(eqn, comp);
         return 0.0;
     }
-    const SolveRef R = solve_ref(eqn, comp);
+    return solve_system_ref(solve_ref(eqn, comp), iters, false);
+}
+
+// the host-polled solve of one system R (fp64: the plain FP64 path whatever
+// the case's precision)
+double Case::solve_system_ref(const SolveRef& R, int* iters, bool fp64) {
     Equation& E = *R.E;
     const xcal_solver_setup& SS = R.SS;
     double* field = R.field;
@@ -1645,7 +1668,7 @@ double Case::solve_system(int eqn, int comp, int* iters) {
     hS->rtol = SS.rtol;
     hS->itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
     const int gk = R.gk;
-    if (cfg.precision == XCAL_PREC_MIXED) {
+    if (cfg.precision == XCAL_PREC_MIXED && !fp64) {
         solve_mixed(E, SS, field, b, S, hS, gk, iters);
     } else {
         XCAL_CUDA(cudaMemcpyAsync(S, hS, sizeof(KScalars), cudaMemcpyHostToDevice, stream));
@@ -1713,7 +1736,7 @@ void Case::solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, 
     CSRView A = E.view();
     const bool fold = use_fold(E, SS, false);
     if (fold) {
-        build_fold(E, stream);
+        build_fold(E, stream, fold_uniform_ok());
         kr_fold_scale(stream, E.fold_mut(), E.nz.p, E.d_diag.p, E.P.p);
     } else {
         kr_to_float(stream, E.nnz, E.nz.p, E.nz32.p);
@@ -2026,7 +2049,7 @@ void Case::capture_step() {
         kr_coop_capture_ok(true);
         kr_cluster_capture_ok(true);
         // the folded inner CG's storage (uploads) cannot be made under capture
-        if (use_fold(P, cfg.p_solver, true)) build_fold(P, stream);
+        if (use_fold(P, cfg.p_solver, true)) build_fold(P, stream, fold_uniform_ok());
     }
     XCAL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     try {

@@ -92,7 +92,9 @@ struct Equation {
     DBuf<unsigned char> f_len;
     DBuf<float> f_val;
     bool fold_built = false;
-    FoldView fold_view() const { return FoldView{n, f_slice.p, f_len.p, f_col.p, f_val.p}; }
+    bool fold_uniform_ok = true;  // the layout rule the storage was built with
+    int f_W = 0;  // uniform slice width of the folded storage (0: per-slice widths)
+    FoldView fold_view() const { return FoldView{n, f_slice.p, f_len.p, f_col.p, f_val.p, f_W}; }
     FoldMut fold_mut() { return FoldMut{n, f_slice.p, f_len.p, f_col.p, f_map.p, f_val.p}; }
     DBuf<double> b[3];
     // DILU level schedules (rows grouped by dependency level)
@@ -109,6 +111,15 @@ struct Equation {
     CSRView view() const;
     int find(int i, int j) const;  // slot or -1
 };
+
+// the CSR pattern, slot maps and (need_dilu) DILU level structures of an
+// equation on mesh m (periodic BCs add their partner entries); the BC table
+// of a field (E: the equation whose periodic slots it resolves, or null)
+void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal_bc>& bcs, int nvec, bool need_dilu,
+                    cudaStream_t s);
+struct BCTable;
+void build_bc_table(BCTable& T, const DevMesh& m, const xcal_bc* bcs, int nbc, int ncomp, const Equation* E,
+                    cudaStream_t s);
 
 struct BCTable {
     std::vector<xcal_bc> src;  // as given (pointers not retained)
@@ -193,12 +204,14 @@ struct Case {
     long long prof_n[6] = {0, 0, 0, 0, 0, 0};
     int persistent_cg = 1;  // CG (Jacobi / none) as one cooperative launch: 0 off, 1 auto width, else the width
     // mixed-precision inner CG with Jacobi: 0 = on the Jacobi-scaled system
-    // (cg_folded.cu) where it fits, 1 = the canonical FP32 kernels, 2 + f =
-    // the scaled-system kernel in form f (launch shape), 2 + FOLD_NFORMS + f =
-    // form f with x and p kept in global memory
+    // (cg_folded.cu) where it fits, 1 = the canonical FP32 kernels, 2 + v =
+    // the scaled-system kernel with v = form (bits 0-1, launch shape) + 4 (x
+    // and p kept in global memory) + 8 (per-slice slot widths even where the
+    // uniform width would do); every v gives the same results as v & 3
     int inner_cg = 0;
-    int fold_form() const { return inner_cg >= 2 ? (inner_cg - 2) % FOLD_NFORMS : FOLD_DEFAULT_FORM; }
-    bool fold_smem() const { return inner_cg < 2 + FOLD_NFORMS; }
+    int fold_form() const { return inner_cg >= 2 ? (inner_cg - 2) & 3 : FOLD_DEFAULT_FORM; }
+    bool fold_smem() const { return inner_cg < 2 || !((inner_cg - 2) & 4); }
+    bool fold_uniform_ok() const { return inner_cg < 2 || !((inner_cg - 2) & 8); }
     void set_inner_cg(int mode);  // drops a captured step graph of the other form
     int dilu_mode = 0;          // 0 = autotuned / size rule, 1 = one-block sweeps, 2 = per-level kernels
     void prof_reserve(int pairs);
@@ -250,6 +263,8 @@ struct Case {
         int slot, kslot, gk;
     };
     SolveRef solve_ref(int eqn, int comp);
+    double solve_system_ref(const SolveRef& R, int* iters, bool fp64);
+    void update_precond_E(Equation& E, int precond);
     void build_wall_table(const DevMesh& m);
     void komega();
     bool sst() const { return cfg.turbulence == XCAL_TURB_KOMEGA_SST; }

@@ -91,32 +91,60 @@ __device__ __forceinline__ double fold_grid_sum(const double* part, int nblocks,
     return fold_block_sum(v, sm);
 }
 
-// q_i = s_i d_i + sum_j ahat_ij d_j over row i's off-diagonal slots, with
-// d = r (first iteration: p_0 = z = r) or r + beta p_old, formed for every
-// gathered column the same way; the row's slot loads are issued together
-template <bool FIRST, int U>
-__device__ __forceinline__ float fold_row(const FoldView& F, const float* r, const float* pold, float beta, int i,
-                                          float& pi) {
-    const unsigned lb = F.len[i];
-    const int ln = lb & 0x7f;
-    const int base = F.slice[i >> 5] + (i & 31);
+// The first U off-diagonal slots of a row (columns and values), loaded
+// together.  UNI (every slice padded to the same width W, padding slots
+// holding the row's own column and a zero value): the row's first slot sits
+// at 32 W (i / 32) + i % 32, so no slice offset and no row length stand in
+// front of these loads; else the slice offset and the row length are read
+// first and only the row's own slots are loaded.
+template <int U>
+struct FoldSlots {
     int c[U];
     float v[U];
+};
+template <bool UNI, int U>
+__device__ __forceinline__ void fold_load(const FoldView& F, int i, FoldSlots<U>& s) {
+    if constexpr (UNI) {
+        const int base = SELL_C * F.W * (i >> 5) + (i & 31);
 #pragma unroll
-    for (int m = 0; m < U; ++m)
-        if (m < ln) {
-            c[m] = ld_stream(F.col + base + SELL_C * m);
-            v[m] = ld_stream(F.val + base + SELL_C * m);
-        }
+        for (int m = 0; m < U; ++m)
+            if (m < F.W) {
+                s.c[m] = ld_stream(F.col + base + SELL_C * m);
+                s.v[m] = ld_stream(F.val + base + SELL_C * m);
+            }
+    } else {
+        const int ln = F.len[i] & 0x7f;
+        const int base = F.slice[i >> 5] + (i & 31);
+#pragma unroll
+        for (int m = 0; m < U; ++m)
+            if (m < ln) {
+                s.c[m] = ld_stream(F.col + base + SELL_C * m);
+                s.v[m] = ld_stream(F.val + base + SELL_C * m);
+            }
+    }
+}
+
+// q_i = s_i d_i + sum_j ahat_ij d_j over row i's off-diagonal slots (s_i the
+// sign of its diagonal), with d = r (first iteration: p_0 = z = r) or
+// r + beta p_old, formed for every gathered column the same way; slots past
+// the first U are read here
+template <bool FIRST, bool UNI, int U>
+__device__ __forceinline__ float fold_q(const FoldView& F, const float* r, const float* pold, float beta, int i,
+                                        const FoldSlots<U>& s, float& pi) {
+    const unsigned lb = F.len[i];
+    const int n_slots = UNI ? F.W : (int)(lb & 0x7f);
     pi = FIRST ? r[i] : __fmaf_rn(beta, pold[i], r[i]);
     float q = (lb & 0x80) ? -pi : pi;
 #pragma unroll
     for (int m = 0; m < U; ++m)
-        if (m < ln) q = __fmaf_rn(v[m], FIRST ? r[c[m]] : __fmaf_rn(beta, pold[c[m]], r[c[m]]), q);
-    for (int m = U; m < ln; ++m) {
-        const int s = base + SELL_C * m;
-        const int cc = ld_stream(F.col + s);
-        q = __fmaf_rn(ld_stream(F.val + s), FIRST ? r[cc] : __fmaf_rn(beta, pold[cc], r[cc]), q);
+        if (m < n_slots) q = __fmaf_rn(s.v[m], FIRST ? r[s.c[m]] : __fmaf_rn(beta, pold[s.c[m]], r[s.c[m]]), q);
+    if (n_slots > U) {
+        const int base = UNI ? SELL_C * F.W * (i >> 5) + (i & 31) : F.slice[i >> 5] + (i & 31);
+        for (int m = U; m < n_slots; ++m) {
+            const int sl = base + SELL_C * m;
+            const int cc = ld_stream(F.col + sl);
+            q = __fmaf_rn(ld_stream(F.val + sl), FIRST ? r[cc] : __fmaf_rn(beta, pold[cc], r[cc]), q);
+        }
     }
     return q;
 }
@@ -136,10 +164,11 @@ __device__ __forceinline__ float fold_row(const FoldView& F, const float* r, con
 // shared memory (else in xg / re-read from the direction buffer).
 //
 // NT threads per block; U slots per row issued together (the rest in a
-// loop); PAIR: each thread takes rows k and k + NT together, so two rows'
-// loads are in flight at once.  Each row's arithmetic is the same in every
-// shape; only the grouping of the block partials follows NT.
-template <int NT, int U, bool PAIR>
+// loop); PIPE: a thread issues the slot loads of its next row before it
+// gathers for the current one, so the two rows' loads overlap.  UNI: the
+// uniform-width slot layout (fold_load).  Each row's arithmetic is the same
+// in every shape; only the grouping of the block partials follows NT.
+template <int NT, int U, bool PIPE, bool UNI>
 __global__ void __launch_bounds__(NT, 1)
     k_cgf_persist(FoldView F, float* r, float* P0, float* P1, float* xg, double* field, const double* __restrict__ Pj,
                   KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters, int R,
@@ -173,44 +202,27 @@ __global__ void __launch_bounds__(NT, 1)
         const float* pold = (iter & 1) ? P0 : P1;
         const float bt = (float)beta;
         double acc = 0.0;
-        if constexpr (PAIR) {
-            for (int k = threadIdx.x; k < nr; k += 2 * NT) {
-                const int k2 = k + NT;
-                const bool two = k2 < nr;
-                const int i = row0 + k, i2 = row0 + (two ? k2 : k);
-                float pi, qi, pi2, qi2;
-                if (iter == 0) {
-                    qi = fold_row<true, U>(F, r, pold, bt, i, pi);
-                    qi2 = fold_row<true, U>(F, r, pold, bt, i2, pi2);
-                } else {
-                    qi = fold_row<false, U>(F, r, pold, bt, i, pi);
-                    qi2 = fold_row<false, U>(F, r, pold, bt, i2, pi2);
-                    pk[i] = pi;
-                    if (two) pk[i2] = pi2;
-                }
-                q_s[k] = qi;
-                if (smem_p) p_s[k] = pi;
-                acc = acc + (double)pi * (double)qi;
-                if (two) {
-                    q_s[k2] = qi2;
-                    if (smem_p) p_s[k2] = pi2;
-                    acc = acc + (double)pi2 * (double)qi2;
-                }
+        FoldSlots<U> cur, nxt;
+        int k = threadIdx.x;
+        if (PIPE && k < nr) fold_load<UNI, U>(F, row0 + k, cur);
+        for (; k < nr; k += NT) {
+            const int i = row0 + k;
+            if constexpr (PIPE) {
+                if (k + NT < nr) fold_load<UNI, U>(F, i + NT, nxt);
+            } else {
+                fold_load<UNI, U>(F, i, cur);
             }
-        } else {
-            for (int k = threadIdx.x; k < nr; k += NT) {
-                const int i = row0 + k;
-                float pi, qi;
-                if (iter == 0) {
-                    qi = fold_row<true, U>(F, r, pold, bt, i, pi);
-                } else {
-                    qi = fold_row<false, U>(F, r, pold, bt, i, pi);
-                    pk[i] = pi;
-                }
-                q_s[k] = qi;
-                if (smem_p) p_s[k] = pi;
-                acc = acc + (double)pi * (double)qi;
+            float pi, qi;
+            if (iter == 0) {
+                qi = fold_q<true, UNI, U>(F, r, pold, bt, i, cur, pi);
+            } else {
+                qi = fold_q<false, UNI, U>(F, r, pold, bt, i, cur, pi);
+                pk[i] = pi;
             }
+            q_s[k] = qi;
+            if (smem_p) p_s[k] = pi;
+            acc = acc + (double)pi * (double)qi;
+            if constexpr (PIPE) cur = nxt;
         }
         double tot = fold_block_sum(acc, sm);
         if (threadIdx.x == 0) part[blockIdx.x] = tot;
@@ -295,11 +307,19 @@ struct FoldKernel {
     const void* fn;
     int nt;
 };
-static const FoldKernel FOLD_FORMS[FOLD_NFORMS] = {
-    {(const void*)k_cgf_persist<512, 8, false>, 512},
-    {(const void*)k_cgf_persist<512, 8, true>, 512},
-    {(const void*)k_cgf_persist<768, 6, false>, 768},
-    {(const void*)k_cgf_persist<1024, 6, false>, 1024},
+static const FoldKernel FOLD_FORMS[2][FOLD_NFORMS] = {
+    {
+        {(const void*)k_cgf_persist<768, 6, false, false>, 768},
+        {(const void*)k_cgf_persist<1024, 6, false, false>, 1024},
+        {(const void*)k_cgf_persist<768, 6, true, false>, 768},
+        {(const void*)k_cgf_persist<1024, 6, true, false>, 1024},
+    },
+    {
+        {(const void*)k_cgf_persist<768, 6, false, true>, 768},
+        {(const void*)k_cgf_persist<1024, 6, false, true>, 1024},
+        {(const void*)k_cgf_persist<768, 6, true, true>, 768},
+        {(const void*)k_cgf_persist<1024, 6, true, true>, 1024},
+    },
 };
 
 // launch geometry of the folded CG (form `form`) for n rows: blocks (one per
@@ -319,15 +339,16 @@ FoldShape fold_shape(int n, int form, bool vectors_in_smem) {
         cudaGetLastError();
     }
     if (attr_ok[form] < 0) {
-        int per = 0;
-        const FoldKernel& K = FOLD_FORMS[form];
-        attr_ok[form] = cudaFuncSetAttribute(K.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FOLD_SMEM_MAX) ==
-                                    cudaSuccess &&
-                                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, K.fn, K.nt, FOLD_SMEM_MAX) ==
-                                    cudaSuccess &&
-                                per >= 1
-                            ? 1
-                            : 0;
+        attr_ok[form] = 1;
+        for (int uni = 0; uni < 2; ++uni) {  // both slot layouts of the form
+            int per = 0;
+            const FoldKernel& K = FOLD_FORMS[uni][form];
+            if (cudaFuncSetAttribute(K.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FOLD_SMEM_MAX) !=
+                    cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, K.fn, K.nt, FOLD_SMEM_MAX) != cudaSuccess ||
+                per < 1)
+                attr_ok[form] = 0;
+        }
         cudaGetLastError();
     }
     FoldShape sh;
@@ -338,7 +359,7 @@ FoldShape fold_shape(int n, int form, bool vectors_in_smem) {
     if (q > FOLD_SMEM_MAX) return sh;
     if ((n + R - 1) / R > FOLD_MAX_BLOCKS) return sh;
     sh.form = form;
-    sh.nt = FOLD_FORMS[form].nt;
+    sh.nt = FOLD_FORMS[0][form].nt;
     sh.blocks = (n + R - 1) / R;
     sh.rows = R;
     sh.smem_p = vectors_in_smem && 2 * q <= FOLD_SMEM_MAX;
@@ -368,7 +389,7 @@ bool kr_cgf_persist(cudaStream_t s, const FoldView& F, float* r, float* P0, floa
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    XCAL_CUDA(cudaLaunchKernelExC(&cfg, FOLD_FORMS[sh.form].fn, args));
+    XCAL_CUDA(cudaLaunchKernelExC(&cfg, FOLD_FORMS[F.W > 0 ? 1 : 0][sh.form].fn, args));
     XCAL_CHECK_LAUNCH();
     return true;
 }

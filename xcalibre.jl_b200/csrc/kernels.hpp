@@ -252,13 +252,16 @@ void kr_record(cudaStream_t s, const KScalars* S, int* out);
 // SELL-32 slices over the storage rows: entry m of row i at slice[i/32] +
 // i%32 + 32 m; len[i] = the row's off-diagonal count, bit 7 set when its
 // diagonal is negative (ahat_ii = -1); map = the slot of the same entry in
-// the equation's own SELL storage.
+// the equation's own SELL storage.  W > 0: every slice has the same width
+// W (slice[s] = 32 W s) and a row's slots past its count hold its own column
+// and a zero value, so a kernel may read all W without the row's count.
 struct FoldView {
     int n;
     const int* slice;
     const unsigned char* len;
     const int* col;
     const float* val;
+    int W;
 };
 struct FoldMut {
     int n;
@@ -268,12 +271,13 @@ struct FoldMut {
     const int* map;
     float* val;
 };
-// kernel forms of the folded CG (block size / row pairing; cg_folded.cu)
+// kernel forms of the folded CG (block size / software pipelining over rows;
+// cg_folded.cu)
 constexpr int FOLD_NFORMS = 4;
 // most blocks of a folded-CG launch (one per SM); its two partial buffers
 // hold this many doubles each
 constexpr int FOLD_MAX_BLOCKS = 1024;
-constexpr int FOLD_DEFAULT_FORM = 3;  // 1024 threads (measured fastest at 2.1M rows)
+constexpr int FOLD_DEFAULT_FORM = 2;  // 768 threads, next row's loads early (fastest at 2.1M rows, no spills)
 struct FoldShape {
     int form = 0, nt = 0, blocks = 0, rows = 0, smem = 0;
     bool smem_p = false, smem_x = false;
