@@ -471,6 +471,8 @@ typedef struct xcal_equation xcal_equation;
  * field's boundary conditions (no periodic pairs).  Runs on cs's stream. */
 int32_t xcal_equation_create(xcal_case* cs, int32_t n_terms, const xcal_term* terms, int32_t n_sources,
                              const xcal_source* sources, int32_t n_bcs, const xcal_bc* bcs, xcal_equation** out);
+/* frees the equation; it may be called after its case was destroyed (every
+ * other xcal_equation_* call needs the case alive) */
 int32_t xcal_equation_destroy(xcal_equation* eq);
 /* discretise!(eqn, prev, config) (Discretise_2_generated_distretisation.jl:
  * 90-168): prev [n_cells] = the previous values Time{Euler} reads (NULL
@@ -590,11 +592,14 @@ int32_t xcal_case_solve_report(const xcal_case* cs, int32_t* iters7, int32_t* st
  * results agree within the mixed-precision tolerance. */
 int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode);
 /* launch-shape autotuner (runs on first use, or now): out6 = for U then p,
- * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU as
- * one-block sweeps [0/1]).  The choices never change a result. */
+ * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU
+ * form [0 one launch per level, 1 one-block sweeps, 2 one cooperative launch
+ * over every level]).  The choices never change a result. */
 int32_t xcal_case_tuning(xcal_case* cs, int32_t* out6);
 /* DILU execution: 0 = autotuned (default), 1 = one-block sweeps,
- * 2 = one launch per level over level-ordered triangles.  Same results. */
+ * 2 = one launch per level over level-ordered triangles, 3 = every level of
+ * an application in one cooperative launch (a grid barrier between levels).
+ * Same results, bit for bit. */
 int32_t xcal_case_set_dilu_mode(xcal_case* cs, int32_t mode);
 int32_t xcal_case_get_profile(const xcal_case* cs, int32_t which, double* ms, int64_t* launches);
 

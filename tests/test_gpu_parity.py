@@ -162,10 +162,11 @@ def test_determinism_two_runs(x, ctx):
         g.get_field(x._abi.FIELD_P, out=np.empty(mesh.n_cells, dtype=np.float32))
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3])
 def test_dilu_modes_parity(x, orc, ctx, mode):
-    """Momentum DILU as one-block sweeps and as per-level kernels over the
-    level-ordered triangles: both equal the oracle bit for bit."""
+    """Momentum DILU as one-block sweeps, as per-level kernels over the
+    level-ordered triangles, and as one cooperative launch over every level:
+    each equals the oracle bit for bit."""
     mesh = x.build_mesh3(x.channel_polymesh(34, 44, 46, seed=12))   # 68,816 cells
     model, config = x.cases.channel_case(mesh, iterations=2)
     g, o, keep = make_pair(x, orc, ctx, mesh, model, config)
@@ -174,3 +175,24 @@ def test_dilu_modes_parity(x, orc, ctx, mode):
     ro, co = o.simple_iterate(2)
     assert rel(rg, ro) <= TOL, (rg, ro)
     compare_fields(x, g, o, ["FIELD_U", "FIELD_P"], tol=0.0)
+
+
+def test_dilu_grid_mixed_identical(x, ctx):
+    """Mixed precision: the FP32 momentum DILU as per-level kernels and as
+    one cooperative launch over every level give the same run bit for bit."""
+    mesh = x.build_mesh3(x.channel_polymesh(40, 30, 30, seed=8))
+    out = []
+    for mode in (2, 3):
+        model, config = x.cases.channel_case(mesh, iterations=3, precision="mixed")
+        cfg, keep = x.build_config(model, config)
+        dm = x.DeviceMesh(ctx, mesh)
+        g = x.Case(dm, cfg)
+        g.set_field(x._abi.FIELD_U, model.momentum.U)
+        g.set_field(x._abi.FIELD_P, model.momentum.p)
+        g.set_dilu_mode(mode)
+        res, _ = g.simple_iterate(3)
+        out.append((res, g.get_field(x._abi.FIELD_U), g.get_field(x._abi.FIELD_P)))
+        g.close()
+        dm.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)

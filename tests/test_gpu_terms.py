@@ -121,7 +121,7 @@ def _restate(mesh, terms, sources, bcs_by_patch, prev, dt, phi):
             f, ns, j = mesh.cell_faces[k], float(mesh.cell_nsign[k]), mesh.cell_neighbours[k]
             AC = AN = 0.0
             for t in terms:
-                fl = t["flux"][f] if np.ndim(t["flux"]) else t["flux"]
+                fl = (t["flux"][f] if np.ndim(t["flux"]) else t["flux"]) if t["op"] in ("lap", "div") else 0.0
                 if t["op"] == "lap":
                     Sf = [ns * mesh.face_area[f] * nrm[f, c] for c in range(3)]
                     e = [ns * ee[f, c] for c in range(3)]
@@ -151,7 +151,7 @@ def _restate(mesh, terms, sources, bcs_by_patch, prev, dt, phi):
         V = mesh.cell_volume[i]
         acs = bs = 0.0
         for t in terms:
-            fl = t["flux"][i] if np.ndim(t["flux"]) else t["flux"]
+            fl = (t["flux"][i] if np.ndim(t["flux"]) else t["flux"]) if t["op"] in ("time", "si") else 0.0
             if t["op"] == "time":
                 vr = (fl * V) / dt
                 acs += vr
@@ -168,7 +168,7 @@ def _restate(mesh, terms, sources, bcs_by_patch, prev, dt, phi):
         kind, val = bcs_by_patch[f]
         ap = bp = 0.0
         for t in terms:
-            fl = t["flux"][f] if np.ndim(t["flux"]) else t["flux"]
+            fl = (t["flux"][f] if np.ndim(t["flux"]) else t["flux"]) if t["op"] in ("lap", "div") else 0.0
             a = q = 0.0
             if t["op"] == "lap":
                 if kind == "dirichlet":

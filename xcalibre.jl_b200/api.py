@@ -844,10 +844,12 @@ class Case:
         a = np.zeros(6, dtype=np.int32)
         self._chk(lib().xcal_case_tuning(self.h, _abi.ptr(a, C.c_int32)))
         return {eq: {"spmv_rows_per_thread": int(a[3 * k]), "spmv_block": int(a[3 * k + 1]),
-                     "dilu_one_block": bool(a[3 * k + 2])} for k, eq in enumerate(("U", "p"))}
+                     "dilu_one_block": bool(a[3 * k + 2] == 1), "dilu_grid": bool(a[3 * k + 2] == 2)}
+                for k, eq in enumerate(("U", "p"))}
 
     def set_dilu_mode(self, mode: int):
-        """0 = autotuned, 1 = one-block sweeps, 2 = per-level kernels."""
+        """0 = autotuned, 1 = one-block sweeps, 2 = per-level kernels,
+        3 = every level in one cooperative launch (same results)."""
         self._chk(lib().xcal_case_set_dilu_mode(self.h, int(mode)))
 
     def solve_report(self) -> dict:

@@ -4,8 +4,10 @@
 //  * the row mapping and block size of the SpMVs that carry no reduction
 //    (the BiCGSTAB SpMV): the canonical tile kernel or 1/2/4 rows per thread
 //    in blocks of 128/256/512 threads;
-//  * how a DILU application runs for systems of up to 262,144 rows: one block
-//    sweeping every level, or one launch per level.
+//  * how a DILU application runs: one block sweeping every level (systems of
+//    up to 262,144 rows), one launch per level, or every level in one
+//    cooperative launch with a grid barrier between levels (systems of more
+//    than 32,768 rows).
 // Each candidate is timed with CUDA events on the case's own matrix at first
 // use; choices are cached per size class (value size, log2 rows, entries per
 // row), so later cases of the same class reuse them without timing.
@@ -64,21 +66,37 @@ static SpmvShape tune_spmv(Case& C, Equation& E, const T* nz, const T* x, T* y) 
     return best;
 }
 
+// the fastest DILU form on this system: 1 one-block sweeps, 2 one launch per
+// level, 3 one cooperative launch over every level
 template <class T>
-static bool tune_dilu(Case& C, Equation& E, const T* nz, const T* D, const T* b, T* out) {
+static int tune_dilu(Case& C, Equation& E, const T* nz, const T* D, const T* b, T* out) {
     const int reps = (int)std::max(3L, std::min(20L, 20000000L / std::max(E.nnz_csr, 1L)));
-    const bool saved = E.use_block;
-    E.use_block = true;
-    float tb = time_ms(C.stream, C.ev[6], C.ev[7], reps, [&] { C.dilu_ldiv(E, nz, D, b, out, nullptr); });
-    E.use_block = false;
-    float tl = time_ms(C.stream, C.ev[6], C.ev[7], reps, [&] { C.dilu_ldiv(E, nz, D, b, out, nullptr); });
-    E.use_block = saved;
-    return tb <= tl;
+    const bool sb = E.use_block, sg = E.use_grid;
+    int best = 2;
+    float best_ms = 1e30f;
+    for (int form = 1; form <= 3; ++form) {
+        if (form == 1 && E.n > 4 * DILU_BLOCK_MAX_ROWS) continue;
+        if (form == 3 && E.n <= DILU_BLOCK_MAX_ROWS / 2) continue;
+        E.use_block = form == 1;
+        E.use_grid = form == 3;
+        float ms = time_ms(C.stream, C.ev[6], C.ev[7], reps, [&] { C.dilu_ldiv(E, nz, D, b, out, nullptr); });
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = form;
+        }
+    }
+    E.use_block = sb;
+    E.use_grid = sg;
+    return best;
 }
 
 void Case::autotune() {
     if (tuned || capturing) return;
     tuned = true;
+    // whether cooperative kernels run inside captured graphs: found here,
+    // before any capture (the checks run graphs of their own)
+    kr_coop_capture_ok(false);
+    kr_coop_capture_ok(true);
     const bool mixed = cfg.precision == XCAL_PREC_MIXED;
     const int tsz = mixed ? 4 : 8;
     for (int e = 0; e < 2; ++e) {
@@ -101,20 +119,23 @@ void Case::autotune() {
         }
         if (dilu_mode != 0) {
             E.use_block = dilu_mode == 1;
-        } else if (SS.precond == XCAL_PRECOND_DILU && E.n <= 4 * DILU_BLOCK_MAX_ROWS) {
+            E.use_grid = dilu_mode == 3;
+        } else if (SS.precond == XCAL_PRECOND_DILU) {
             TuneKey k = key_of(1, tsz, E);
             std::unique_lock<std::mutex> lk(g_tune_mu);
             auto it = g_dilu_choice.find(k);
+            int form;
             if (it != g_dilu_choice.end()) {
-                E.use_block = it->second != 0;
+                form = it->second;
             } else {
                 lk.unlock();
-                bool blk = mixed ? tune_dilu<float>(*this, E, E.nz32.p, E.P32.p, ws.fr.p, ws.fz.p)
-                                 : tune_dilu<double>(*this, E, E.nz.p, E.P.p, ws.r.p, ws.z.p);
-                E.use_block = blk;
+                form = mixed ? tune_dilu<float>(*this, E, E.nz32.p, E.P32.p, ws.fr.p, ws.fz.p)
+                             : tune_dilu<double>(*this, E, E.nz.p, E.P.p, ws.r.p, ws.z.p);
                 lk.lock();
-                g_dilu_choice[k] = blk ? 1 : 0;
+                g_dilu_choice[k] = form;
             }
+            E.use_block = form == 1;
+            E.use_grid = form == 3;
         }
     }
     sync();

@@ -449,10 +449,18 @@ int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode) {
 }
 
 int32_t xcal_case_set_dilu_mode(xcal_case* cs, int32_t mode) {
-    if (!cs || mode < 0 || mode > 2) return XCAL_ERR_INVALID;
+    if (!cs || mode < 0 || mode > 3) return XCAL_ERR_INVALID;
     Case* c = cs->c.get();
     c->dilu_mode = mode;
-    if (mode != 0) c->U.use_block = c->P.use_block = mode == 1;
+    if (mode != 0) {
+        c->U.use_block = c->P.use_block = mode == 1;
+        c->U.use_grid = c->P.use_grid = mode == 3;
+    }
+    if (c->step_graph) {  // a captured step holds the previous form
+        c->sync();
+        cudaGraphExecDestroy(c->step_graph);
+        c->step_graph = nullptr;
+    }
     return XCAL_OK;
 }
 
@@ -465,7 +473,7 @@ int32_t xcal_case_tuning(xcal_case* cs, int32_t* out6) {
         for (int e = 0; e < 2; ++e) {
             out6[3 * e] = E[e]->spmv_shape.rows_per_thread;
             out6[3 * e + 1] = E[e]->spmv_shape.block;
-            out6[3 * e + 2] = E[e]->use_block ? 1 : 0;
+            out6[3 * e + 2] = E[e]->use_block ? 1 : (E[e]->use_grid ? 2 : 0);
         }
     })
 }

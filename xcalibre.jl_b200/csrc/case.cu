@@ -1186,6 +1186,15 @@ void Case::set_reference() {
     if (cfg.has_pref) launch_set_reference(stream, P.view(), P.nz.p, P.b[0].p, cfg.pref, mesh->inv[0]);
 }
 
+bool Case::coop_ok_here() {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return st == cudaStreamCaptureStatusNone || kr_coop_capture_ok(side_depth > 0);
+}
+
 void Case::update_precond(int eqn) {
     const SolveRef R = solve_ref(eqn, 0);
     update_precond_E(*R.E, R.SS.precond);
@@ -1200,6 +1209,10 @@ void Case::update_precond_E(Equation& E, int pt) {
                             E.P.p);
             return;
         }
+        if (E.use_grid && coop_ok_here() &&
+            kr_dilu_D_grid(stream, E.d_lower_rows.p, E.d_lower_off.p, (int)E.lower_off.size() - 1, E.view(), E.nz.p,
+                           E.P.p, ws.bar.p, ws.err.p))
+            return;
         for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
             kr_dilu_D(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], E.view(),
                       E.nz.p, E.P.p);
@@ -1215,6 +1228,9 @@ void Case::dilu_ldiv(Equation& E, const T* nz, const T* D, const T* b, T* out, c
         kr_dilu_block(stream, E.n, level_view<T>(E, 0), level_view<T>(E, 1), D, b, out, S);
         return;
     }
+    if (E.use_grid && coop_ok_here() &&
+        kr_dilu_grid(stream, level_view<T>(E, 0), level_view<T>(E, 1), D, b, out, ws.bar.p, ws.err.p, S))
+        return;
     const LevelView<T> lo = level_view<T>(E, 0);
     const T* uv = sizeof(T) == 8 ? (const T*)E.usell.val.p : (const T*)E.usell.val32.p;
     for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
@@ -1668,6 +1684,10 @@ double Case::solve_system_ref(const SolveRef& R, int* iters, bool fp64) {
     hS->rtol = SS.rtol;
     hS->itmax = SS.itmax == 0 ? 2 * n : SS.itmax;
     const int gk = R.gk;
+    // the DILU factor and applications as cooperative launches report a
+    // barrier wait that gave up through ws.err, read back with the residual
+    // below (it stays 0 otherwise)
+    const bool grid_dilu = SS.precond == XCAL_PRECOND_DILU && E.use_grid && !E.dilu_block();
     if (cfg.precision == XCAL_PREC_MIXED && !fp64) {
         solve_mixed(E, SS, field, b, S, hS, gk, iters);
     } else {
@@ -1688,7 +1708,9 @@ double Case::solve_system_ref(const SolveRef& R, int* iters, bool fp64) {
     // residual (Solve_1_api.jl:441-464), FP64 in both modes
     kr_residual(stream, A, nz, field, b, S, ws.part0.p, ws.part1.p, resbuf.p);
     XCAL_CUDA(cudaMemcpyAsync(h_res, resbuf.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    if (grid_dilu) XCAL_CUDA(cudaMemcpyAsync(h_perr, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
     sync();
+    if (grid_dilu && *h_perr) fail(XCAL_ERR_TIMEOUT, "DILU sweep: a grid barrier wait gave up");
     return h_res[0];
 }
 

@@ -105,6 +105,7 @@ struct Equation {
     LevelSell lsell, usell;                       // level-ordered triangles (level-kernel sweeps)
     // launch choices (autotune.cu); neither changes any result
     bool use_block = false;   // DILU as one-block sweeps (default: n <= DILU_BLOCK_MAX_ROWS)
+    bool use_grid = false;    // else as one cooperative launch over every level (k_dilu_grid)
     SpmvShape spmv_shape;     // BiCGSTAB SpMV row mapping / block size
     bool dilu_block() const { return use_block; }
     bool has_periodic = false;
@@ -213,7 +214,11 @@ struct Case {
     bool fold_smem() const { return inner_cg < 2 || !((inner_cg - 2) & 4); }
     bool fold_uniform_ok() const { return inner_cg < 2 || !((inner_cg - 2) & 8); }
     void set_inner_cg(int mode);  // drops a captured step graph of the other form
-    int dilu_mode = 0;          // 0 = autotuned / size rule, 1 = one-block sweeps, 2 = per-level kernels
+    int dilu_mode = 0;          // 0 = autotuned / size rule, 1 = one-block sweeps, 2 = per-level kernels,
+                                // 3 = one cooperative launch over every level
+    // whether a cooperative kernel may be launched on the case stream now
+    // (not capturing, or capturing where the driver runs such nodes)
+    bool coop_ok_here();
     void prof_reserve(int pairs);
     // Steady-state polling chunks of a Krylov solve (32 CG / 8 BiCGSTAB
     // iterations) replay as CUDA graphs: every pointer they use is fixed for

@@ -232,6 +232,17 @@ constexpr int DILU_SMEM_MAX_BYTES = 200 * 1024;
 template <class T>
 void kr_dilu_block(cudaStream_t s, int n, const LevelView<T>& lo, const LevelView<T>& up, const T* D, const T* b,
                    T* y, const KScalars* S);
+// a whole DILU application (every level of both sweeps) as one cooperative
+// launch with a grid barrier between levels; false (nothing launched) when
+// the device cannot run it.  bar: 2 words zeroed here; err: set when a
+// barrier wait gave up (the result is then incomplete)
+template <class T>
+bool kr_dilu_grid(cudaStream_t s, const LevelView<T>& lo, const LevelView<T>& up, const T* D, const T* b, T* y,
+                  unsigned int* bar, int* err, const KScalars* S);
+// the DILU factor D (every level of the lower triangle) as one cooperative
+// launch; rows/off: the lower triangle's level lists on the device
+bool kr_dilu_D_grid(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
+                    double* D, unsigned int* bar, int* err);
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
                  double* part0, double* part1, double* out);
 // device-driven solve control of graph mode (conditional WHILE nodes)

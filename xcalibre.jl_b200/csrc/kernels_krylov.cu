@@ -260,6 +260,50 @@ __global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_block(int n, LevelV
     dilu_level_sweep<T>(n, lo, up, D, b, y, smem ? reinterpret_cast<T*>(dilu_smem) : y);
 }
 
+// Every level of one DILU application in one cooperative launch: the
+// forward sweep's levels, then the backward sweep's, each spread over the
+// whole grid (rows of a level are independent), with the bounded grid
+// barrier between consecutive levels.  Each row's arithmetic is that of the
+// level kernels (dilu_level_s), bit for bit; only the launches go.  A barrier
+// that gives up sets *err and ends every block.
+constexpr int DILU_GRID_THREADS = 512;
+template <class T>
+__global__ void __launch_bounds__(DILU_GRID_THREADS) k_dilu_grid(LevelView<T> lo, LevelView<T> up,
+                                                                 const T* __restrict__ D, const T* __restrict__ b,
+                                                                 T* y, unsigned int* bar, int* err,
+                                                                 const KScalars* S) {
+    __shared__ int sh_err;
+    if (S && S->done) return;
+    const int start = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    const int total = lo.nlev + up.nlev;
+    unsigned int nb = 0;
+    for (int l = 0; l < total; ++l) {
+        if (l < lo.nlev) {
+            dilu_level_s<T, true>(lo, lo.off[l], lo.off[l + 1], D, b, y, start, stride);
+        } else {
+            const int u = l - lo.nlev;
+            dilu_level_s<T, false>(up, up.off[u], up.off[u + 1], D, b, y, start, stride);
+        }
+        if (l + 1 < total && !grid_barrier(bar, gridDim.x, nb, err, &sh_err)) return;
+    }
+}
+
+// The DILU factor D of a large system in one cooperative launch: the lower
+// triangle's levels spread over the grid, a grid barrier between levels,
+// each row's arithmetic that of k_dilu_D (dilu_D_row).
+__global__ void __launch_bounds__(DILU_GRID_THREADS) k_dilu_D_grid(const int* __restrict__ rows,
+                                                                   const int* __restrict__ off, int nlev, CSRView A,
+                                                                   const double* __restrict__ nz, double* D,
+                                                                   unsigned int* bar, int* err) {
+    __shared__ int sh_err;
+    const int start = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    unsigned int nb = 0;
+    for (int l = 0; l < nlev; ++l) {
+        for (int k = off[l] + start; k < off[l + 1]; k += stride) dilu_D_row(A, nz, D, rows[k]);
+        if (l + 1 < nlev && !grid_barrier(bar, gridDim.x, nb, err, &sh_err)) return;
+    }
+}
+
 // dinv[e] = T(1) / D[col[e]] (the forward sweep's per-entry reciprocal)
 template <class T>
 __global__ void k_level_dinv(long n, const int* __restrict__ col, const T* __restrict__ D, T* dinv) {
@@ -855,6 +899,76 @@ void kr_dilu_block(cudaStream_t s, int n, const LevelView<T>& lo, const LevelVie
     k_dilu_block<T><<<1, DILU_BLOCK_THREADS, smem ? bytes : 0, s>>>(n, lo, up, D, b, y, smem, S);
     XCAL_CHECK_LAUNCH();
 }
+template <class T>
+bool kr_dilu_grid(cudaStream_t s, const LevelView<T>& lo, const LevelView<T>& up, const T* D, const T* b, T* y,
+                  unsigned int* bar, int* err, const KScalars* S) {
+    // blocks: up to two per SM that are co-resident (found once per process
+    // and value type); 0 = the device cannot run it cooperatively
+    static int blocks = -1;
+    if (blocks < 0) {
+        int dev = 0, sms = 0, per = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k_dilu_grid<T>, DILU_GRID_THREADS, 0) ==
+                cudaSuccess)
+            blocks = sms * std::min(per, 2);
+        else
+            blocks = 0;
+        cudaGetLastError();
+    }
+    if (blocks <= 0) return false;
+    XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
+    LevelView<T> l = lo, u = up;
+    void* args[] = {&l, &u, (void*)&D, (void*)&b, &y, &bar, &err, (void*)&S};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(DILU_GRID_THREADS);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    XCAL_CUDA(cudaLaunchKernelExC(&cfg, (const void*)k_dilu_grid<T>, args));
+    XCAL_CHECK_LAUNCH();
+    return true;
+}
+bool kr_dilu_D_grid(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
+                    double* D, unsigned int* bar, int* err) {
+    static int blocks = -1;
+    if (blocks < 0) {
+        int dev = 0, sms = 0, per = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k_dilu_D_grid, DILU_GRID_THREADS, 0) ==
+                cudaSuccess)
+            blocks = sms * std::min(per, 2);
+        else
+            blocks = 0;
+        cudaGetLastError();
+    }
+    if (blocks <= 0 || nlev <= 0) return false;
+    XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
+    CSRView Av = A;
+    void* args[] = {(void*)&rows, (void*)&off, &nlev, &Av, (void*)&nz, &D, &bar, &err};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(DILU_GRID_THREADS);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    XCAL_CUDA(cudaLaunchKernelExC(&cfg, (const void*)k_dilu_D_grid, args));
+    XCAL_CHECK_LAUNCH();
+    return true;
+}
+template bool kr_dilu_grid<double>(cudaStream_t, const LevelView<double>&, const LevelView<double>&, const double*,
+                                   const double*, double*, unsigned int*, int*, const KScalars*);
+template bool kr_dilu_grid<float>(cudaStream_t, const LevelView<float>&, const LevelView<float>&, const float*,
+                                  const float*, float*, unsigned int*, int*, const KScalars*);
+
 void kr_residual(cudaStream_t s, const CSRView& A, const double* nz, const double* x, const double* b, KScalars* S,
                  double* part0, double* part1, double* out) {
     k_residual<<<TILE_LAUNCH(A.n), s>>>(A, nz, x, b, S, part0, part1, out);

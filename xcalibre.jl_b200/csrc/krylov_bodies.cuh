@@ -503,15 +503,18 @@ constexpr int DILU_BLOCK_THREADS = 1024;
 // substitution (y_i = b_i - sum (a_ij y_j) (1/D_j)); else backward (x_i =
 // (x_i - sum a_ij x_j) / D_i).  The first U slots of a row sit in registers,
 // the rest are read in a loop; each row's sum runs in its own entry order.
+// (start, stride): the thread's first position and the stride between its
+// positions -- the block (threadIdx.x, blockDim.x) for one-block sweeps, the
+// grid for sweeps spread over every block (k_dilu_grid).
 template <class T, bool LOWER>
-__device__ __forceinline__ void dilu_level(const LevelView<T>& L, int k0, int k1, const T* __restrict__ D,
-                                           const T* __restrict__ b, T* ys) {
+__device__ __forceinline__ void dilu_level_s(const LevelView<T>& L, int k0, int k1, const T* __restrict__ D,
+                                             const T* __restrict__ b, T* ys, int start, int stride) {
     constexpr int R = sizeof(T) == 4 ? 2 : 1;  // rows per thread per step
     constexpr int U = sizeof(T) == 4 ? 6 : 8;
-    for (int k = k0 + threadIdx.x; k < k1; k += R * blockDim.x) {
+    for (int k = k0 + start; k < k1; k += R * stride) {
         int kk[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) kk[r] = k + r * (int)blockDim.x;
+        for (int r = 0; r < R; ++r) kk[r] = k + r * stride;
         int i[R], c[R], base[R];
         T rhs[R];
         int cj[R][U];
@@ -555,6 +558,12 @@ __device__ __forceinline__ void dilu_level(const LevelView<T>& L, int k0, int k1
             ys[i[r]] = LOWER ? rhs[r] - sum : (ys[i[r]] - sum) / rhs[r];
         }
     }
+}
+
+template <class T, bool LOWER>
+__device__ __forceinline__ void dilu_level(const LevelView<T>& L, int k0, int k1, const T* __restrict__ D,
+                                           const T* __restrict__ b, T* ys) {
+    dilu_level_s<T, LOWER>(L, k0, k1, D, b, ys, (int)threadIdx.x, (int)blockDim.x);
 }
 
 template <class T>

@@ -323,11 +323,10 @@ int32_t xcal_equation_create(xcal_case* cs, int32_t n_terms, const xcal_term* te
     return XCAL_OK;
 }
 
+// frees the equation's device memory (cudaFree waits for work using it);
+// touches nothing of its case, which may already be gone
 int32_t xcal_equation_destroy(xcal_equation* q) {
-    if (q) {
-        if (q->c) cudaStreamSynchronize(q->c->stream);
-        delete q;
-    }
+    delete q;
     return XCAL_OK;
 }
 

@@ -197,6 +197,10 @@ class Equation:
     def _chk(self, code):
         check(code, self.case.dmesh.ctx.h)
 
+    def _live(self):
+        if not getattr(self, "h", None) or not getattr(self.case, "h", None):
+            raise RuntimeError("the equation or its case has been closed")
+
     def close(self):
         if getattr(self, "h", None):
             lib().xcal_equation_destroy(self.h)
@@ -211,6 +215,7 @@ class Equation:
     def discretise(self, prev=None, dt: float = 0.0):
         """discretise!(eqn, prev, config): prev = the previous values read
         by Time{Euler} (None without one), dt its time step."""
+        self._live()
         p = None
         if prev is not None:
             p = np.ascontiguousarray(prev, dtype=np.float64)
@@ -221,11 +226,13 @@ class Equation:
     def apply_boundary_conditions(self, phi=None):
         """apply_boundary_conditions!(eqn, BCs) with the field's current
         values (read by Extrapolated boundaries)."""
+        self._live()
         p = None if phi is None else np.ascontiguousarray(phi, dtype=np.float64)
         self._chk(lib().xcal_equation_apply_bcs(self.h, _abi.ptr(p, C.c_double) if p is not None else None))
 
     def system(self):
         """(rowptr, colval, nzval, b) in the original numbering."""
+        self._live()
         nnz = C.c_int64()
         self._chk(lib().xcal_equation_nnz(self.h, C.byref(nnz)))
         rp = np.empty(self.n + 1, dtype=np.int32)
@@ -239,6 +246,7 @@ class Equation:
     def solve(self, setup: A.SolverSetup, phi):
         """solve_system! in FP64 from the initial guess phi: (solution,
         scaled residual, Krylov iterations)."""
+        self._live()
         x = np.array(phi, dtype=np.float64, copy=True)
         res, its = C.c_double(), C.c_int32()
         desc = A._solver_desc(setup)
