@@ -56,11 +56,53 @@ def parse():
     ap.add_argument("--serve-cases", type=int, default=16, help="serving stream: requests (0 = skip)")
     ap.add_argument("--serve-nmax", type=float, default=3e4)
     ap.add_argument("--serve-rate", type=float, default=8.0)
+    ap.add_argument("--serve-iters", type=int, default=1500, help="serving: SIMPLE iteration cap per request")
+    ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="serving: device-memory budget (GB)")
     ap.add_argument("--converge-cap", type=int, default=1200,
                     help="time-to-convergence block: SIMPLE iteration cap per precision (0 = skip)")
-    ap.add_argument("--only", choices=["les", "serving", "batch", "converge"], default=None,
-                    help="run one secondary workload alone and print its block as the line (profiling)")
+    ap.add_argument("--only", choices=["les", "serving", "batch", "converge", "step-window"], default=None,
+                    help="run one secondary workload alone and print its block as the line (profiling); "
+                         "step-window: --steps SIMPLE iterations of the channel case after --warmup, between "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--inner-cg", type=int, default=None,
+                    help="mixed precision: form of the FP32 inner CG (xcal_case_set_inner_cg; default: the "
+                         "library's)")
+    ap.add_argument("--ncu-table", default=None, metavar="CSV",
+                    help="print the per-kernel table (launches, time, share, DRAM bytes) of an ncu --csv "
+                         "per-launch metrics file and exit (no GPU)")
     return ap.parse_args()
+
+
+def ncu_table(path):
+    """Per-kernel sums of an ncu --csv log of gpu__time_duration.sum and
+    dram__bytes_read/write.sum, one line per kernel, by total time."""
+    import collections
+    import csv
+    import re
+    rows = list(csv.reader(ln for ln in open(path) if not ln.startswith("==")))
+    ix = {h: i for i, h in enumerate(rows[0])}
+    scale = {"ns": 1e-9, "nsecond": 1e-9, "us": 1e-6, "usecond": 1e-6, "ms": 1e-3, "msecond": 1e-3,
+             "second": 1.0, "byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    agg = collections.OrderedDict()
+    for r in rows[1:]:
+        if len(r) < len(ix):
+            continue
+        name = re.sub(r"\(.*", "", r[ix["Kernel Name"]]).replace("void ", "").replace("xcal::", "")
+        a = agg.setdefault(name, {"ids": set(), "t": 0.0, "rd": 0.0, "wr": 0.0})
+        a["ids"].add(r[ix["ID"]])
+        v = float(r[ix["Metric Value"]].replace(",", "")) * scale.get(r[ix["Metric Unit"]], 1.0)
+        key = {"gpu__time_duration.sum": "t", "dram__bytes_read.sum": "rd", "dram__bytes_write.sum": "wr"}
+        if r[ix["Metric Name"]] in key:
+            a[key[r[ix["Metric Name"]]]] += v
+    tot = sum(a["t"] for a in agg.values())
+    print(f"{'kernel':44s} {'launches':>8s} {'time ms':>9s} {'share':>6s} {'DRAM MB/launch':>14s} {'DRAM GB/s':>9s}")
+    for name, a in sorted(agg.items(), key=lambda kv: -kv[1]["t"]):
+        k = len(a["ids"])
+        gbs = (a["rd"] + a["wr"]) / a["t"] / 1e9 if a["t"] else 0.0
+        print(f"{name[:44]:44s} {k:8d} {a['t'] * 1e3:9.3f} {a['t'] / tot:6.1%} {(a['rd'] + a['wr']) / k / 1e6:14.2f} "
+              f"{gbs:9.0f}")
+    print(f"total device time {tot * 1e3:.3f} ms over {sum(len(a['ids']) for a in agg.values())} launches")
+    return 0
 
 
 def workload_name(n):
@@ -220,6 +262,8 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
     t_setup = time.perf_counter()
     dm = x.DeviceMesh(ctx, mesh)
     case = x.Case(dm, cfg)
+    if args.inner_cg is not None and precision == "mixed":
+        case.set_inner_cg(args.inner_cg)
     case.set_field(A.FIELD_U, model.momentum.U)
     case.set_field(A.FIELD_P, model.momentum.p)
     t_setup = time.perf_counter() - t_setup
@@ -290,15 +334,17 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
     if pers_it and fp32:
         # folded FP32 CG (Jacobi-scaled system, implicit unit diagonal): per
         # iteration the off-diagonal slots (value + column) and row lengths
-        # stream once, r and p_{k-1} are gathered, p_k is written, and phase 2
-        # reads and writes r (x, p_k and q stay in shared memory)
+        # stream once, the (r, p_{k-1}) pairs are gathered (8 B per row), and
+        # phase 2 reads the row's pair and writes the next (r, p_k) pair (x
+        # and q stay in shared memory)
         nnz_off = nnz_p - n
-        bpi = nnz_off * 8 + n * (1 + 4 + 4 + 4 + 4 + 4) + 4 * ((n + 31) // 32)
+        bpi = nnz_off * 8 + n * (1 + 8 + 8 + 8)
         t_it = pers_ms / pers_it / 1e3
         ach = bpi / t_it / 1e9
-        roof = {"bound": "hbm", "kernel": "k_cgf_persist (FP32 CG on the Jacobi-scaled system, whole solve in one "
-                                          "cooperative launch, one block per SM: gathered SpMV of the off-diagonal "
-                                          "slots with p = r + beta p, grid barrier, x/r update, grid barrier)",
+        roof = {"bound": "hbm", "kernel": "k_cgf_staged / k_cgf_persist (FP32 CG on the Jacobi-scaled system, "
+                                          "whole solve in one cooperative launch, one block per SM: gathered SpMV "
+                                          "of the off-diagonal slots with p = r + beta p, grid barrier, x/r "
+                                          "update, grid barrier)",
                 "achieved": ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
                 "traffic": (tr_all.get("fold_bytes_per_iteration_128") if args.size == 128 else None),
                 "traffic_unit": "bytes per CG iteration (ncu DRAM read + write of one launch / its iterations)",
@@ -381,22 +427,27 @@ def serve_measure(x, args, local):
     in [1e3, serve_nmax], aspect U[1,4], Re U[100,2000], Poisson arrivals at
     serve_rate per second, mixed precision, each to a 1e-6 scaled residual
     (cap 1500 SIMPLE iterations); continuous batching with admission by
-    device-memory footprint.  Meshes are built before the stream starts
-    (they are the requests' payload)."""
+    device-memory footprint (serve_budget_gb).  Meshes are built before the
+    stream starts (they are the requests' payload).  serve_iters caps each
+    request's SIMPLE iterations."""
     from importlib import import_module
     serve = import_module(x.__name__ + ".serve")
     reqs = serve.make_requests(args.serve_cases, seed=0, n_min=1e3, n_max=args.serve_nmax, rate=args.serve_rate)
     for r in reqs:
         r.build()
     ctx = x.Context(local)
-    srv = serve.Server(ctx, budget_bytes=40 << 30, max_cases=64, precision="mixed", max_iters=1500,
+    budget = int(args.serve_budget_gb * (1 << 30))
+    srv = serve.Server(ctx, budget_bytes=budget, max_cases=64, precision="mixed", max_iters=args.serve_iters,
                        convergence=1e-6)
     l0 = x.launch_count()
     res = srv.run(reqs, realtime=True)
     s = serve.summarize(res, srv.wall)
     s.update({"workload": f"{len(reqs)} steady cavity/channel requests, N log-uniform [1e3, {args.serve_nmax:g}], "
-                          f"Re U[100,2000], aspect U[1,4], Poisson {args.serve_rate:g}/s, mixed, resid 1e-6",
-              "rate_per_s": args.serve_rate, "budget_bytes": 40 << 30, "max_cases": 64,
+                          f"Re U[100,2000], aspect U[1,4], Poisson {args.serve_rate:g}/s, mixed, resid 1e-6, "
+                          f"cap {args.serve_iters} iterations",
+              "rate_per_s": args.serve_rate, "budget_bytes": budget, "max_cases": 64,
+              "converged_ge_1e5_cells": "%d/%d" % (sum(r.converged for r in res if r.n_cells >= 1e5),
+                                                    sum(1 for r in res if r.n_cells >= 1e5)),
               "max_active": max((t[1] for t in srv.timeline), default=0),
               "admission_s": srv.admit_s, "iterate_s": srv.iterate_s, "retire_s": srv.retire_s,
               "idle_s": srv.idle_s, "cleanup_s": srv.cleanup_s,
@@ -465,6 +516,8 @@ def converge_measure(x, A, mesh, args, local):
         ctx = x.Context(local)
         dm = x.DeviceMesh(ctx, mesh)
         case = x.Case(dm, cfg)
+        if args.inner_cg is not None and prec == "mixed":
+            case.set_inner_cg(args.inner_cg)
         case.set_field(A.FIELD_U, model.momentum.U)
         case.set_field(A.FIELD_P, model.momentum.p)
         stream = torch.cuda.ExternalStream(case.stream(), device=torch.device("cuda", local))
@@ -486,6 +539,38 @@ def converge_measure(x, A, mesh, args, local):
     (U64, p64), (U32, p32) = ends["fp64"], ends["mixed"]
     out["mixed_vs_fp64_rel_l2"] = {"U": float(np.linalg.norm(U32 - U64) / np.linalg.norm(U64)),
                                    "p": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))}
+    return out
+
+
+def step_window(x, A, args, local):
+    """--warmup SIMPLE iterations of the --size channel case in --precision,
+    then --steps more between cudaProfilerStart/Stop, so that an ncu capture
+    with --profile-from-start off sees exactly those steps' launches."""
+    import torch
+    n = args.size
+    mesh = x.build_mesh3(x.channel_polymesh(n, n, n, seed=0), device=local)
+    model, config = x.cases.channel_case(mesh, iterations=100, precision=args.precision)
+    cfg, keep = x.build_config(model, config)
+    ctx = x.Context(local)
+    dm = x.DeviceMesh(ctx, mesh)
+    case = x.Case(dm, cfg)
+    if args.inner_cg is not None and args.precision == "mixed":
+        case.set_inner_cg(args.inner_cg)
+    case.set_field(A.FIELD_U, model.momentum.U)
+    case.set_field(A.FIELD_P, model.momentum.p)
+    case.simple_iterate(args.warmup)
+    torch.cuda.synchronize()
+    l0 = x.launch_count()
+    torch.cuda.profiler.start()
+    res, _ = case.simple_iterate(args.steps)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    rep = case.solve_report()
+    out = {"workload": workload_name(n), "precision": args.precision, "warmup": args.warmup, "steps": args.steps,
+           "launches": x.launch_count() - l0, "residuals_last": [float(v) for v in res[-1]],
+           "krylov_iterations_last": [int(v) for v in rep["iterations"]]}
+    case.close()
+    dm.close()
     return out
 
 
@@ -514,6 +599,8 @@ def e2e_measure(x, A, case, mesh, args, world):
 
 def main():
     args = parse()
+    if args.ncu_table:
+        return ncu_table(args.ncu_table)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -531,7 +618,8 @@ def main():
             m = x.build_mesh3(x.channel_polymesh(args.size, args.size, args.size, seed=0), device=local)
             return converge_measure(x, A, m, args, local)
         blk = {"les": lambda: les_measure(x, A, args, local), "serving": lambda: serve_measure(x, args, local),
-               "batch": lambda: batch_measure(x, args, local), "converge": conv_only}[args.only]()
+               "batch": lambda: batch_measure(x, args, local), "converge": conv_only,
+               "step-window": lambda: step_window(x, A, args, local)}[args.only]()
         if rank == 0:
             print(json.dumps({"only": args.only, **blk}), flush=True)
         if world > 1:

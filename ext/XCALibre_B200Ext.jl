@@ -188,8 +188,27 @@ struct ConfigDesc
     bc_y::Ptr{BCDesc}
 end
 
+# xcal_term / xcal_source: one operator / source of an equation built with
+# the DSL (ModelFramework_0_types.jl:18-100), for xcal_equation_create
+struct TermDesc
+    op::Int32
+    scheme::Int32
+    sign::Float64
+    flux::Ptr{Float64}
+    value::Float64
+end
+
+struct SourceDesc
+    sign::Float64
+    field::Ptr{Float64}
+    value::Float64
+end
+
+const LAYOUT_TERM, LAYOUT_SOURCE = Int32(7), Int32(8)
+
 const MIRRORS = ((LAYOUT_MESH_DESC, MeshDesc), (LAYOUT_BC, BCDesc), (LAYOUT_SOLVER_SETUP, SolverSetupDesc),
-                 (LAYOUT_SCHEMES, SchemesDesc), (LAYOUT_CONFIG, ConfigDesc))
+                 (LAYOUT_SCHEMES, SchemesDesc), (LAYOUT_CONFIG, ConfigDesc), (LAYOUT_TERM, TermDesc),
+                 (LAYOUT_SOURCE, SourceDesc))
 
 # the library's sizeof and field offsets against the mirrors
 function check_layouts()
@@ -495,6 +514,12 @@ function b200_run(model, config, algorithm; pref=nothing, ncorrectors=0, inner_l
         if hasproperty(model.turbulence, :nut)
             model.turbulence.nut.values .= get_field!(ctx[], case[], FIELD_NUT, Vector{Float64}(undef, nC))
         end
+        # solve_system! warns for every solve that stopped at itmax
+        # (Solve_1_api.jl:302); the library counts them
+        hits = Ref{Int64}(0)
+        check(ctx[], ccall((:xcal_case_solve_report, libxcal), Int32, (Ptr{Cvoid}, Ptr{Int32}, Ptr{Int32}, Ref{Int64}),
+                           case[], C_NULL, C_NULL, hits))
+        hits[] > 0 && @warn "Maximum number of iterations reached! ($(hits[]) Krylov solves stopped at itmax)"
         R = reshape(res, 4, :)[:, 1:done[]]
         return (Ux=R[1, :], Uy=R[2, :], Uz=R[3, :], p=R[4, :])
     finally

@@ -30,6 +30,8 @@ STRUCTS = [
     (4, "xcal_config", "ConfigDesc", "ConfigDesc"),
     (5, "xcal_polymesh_desc", "PolyMeshDesc", None),
     (6, "xcal_mesh_buffers", "MeshBuffers", None),
+    (7, "xcal_term", "TermDesc", "TermDesc"),
+    (8, "xcal_source", "SourceDesc", "SourceDesc"),
 ]
 
 

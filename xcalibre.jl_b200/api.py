@@ -840,7 +840,8 @@ class Case:
     def tuning(self) -> dict:
         """Launch shapes chosen by the autotuner (tuning runs now if it has
         not yet): per equation the BiCGSTAB SpMV rows per thread (0 = tile
-        kernel) and block size, and whether DILU runs as one-block sweeps."""
+        kernel) and block size, and the DILU form (one-block sweeps, or one
+        cooperative launch over every level)."""
         a = np.zeros(6, dtype=np.int32)
         self._chk(lib().xcal_case_tuning(self.h, _abi.ptr(a, C.c_int32)))
         return {eq: {"spmv_rows_per_thread": int(a[3 * k]), "spmv_block": int(a[3 * k + 1]),
@@ -867,9 +868,12 @@ class Case:
     def set_inner_cg(self, mode: int):
         """Mixed precision, CG + Jacobi inner solves: 0 = on the Jacobi-scaled
         system (default), 1 = the FP32 form of the FP64 path's kernels,
-        2 + s + 4 g + 8 w = the scaled-system kernel in launch shape s (0..3),
-        with x and p in global memory (g = 1) and per-slice slot widths
-        (w = 1); g and w give the same results as 2 + s."""
+        2 + s + 8 g + 16 w = the scaled-system kernel in launch shape s
+        (0..3 register-loaded slots, 768/1024 threads with or without early
+        loads of the next row; 4, 5 slots staged in shared memory by bulk
+        copies, 768/1024 threads), with x and p in global memory (g = 1) and
+        per-slice slot widths (w = 1).  Shapes with the same thread count, g
+        and w give the same results bit for bit."""
         self._chk(lib().xcal_case_set_inner_cg(self.h, int(mode)))
 
     def checkpoint(self) -> dict:

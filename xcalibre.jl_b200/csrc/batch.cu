@@ -781,8 +781,9 @@ size_t estimate_case_bytes(long nC, long nF, long nB, int mixed, int dilu_U, int
     // three boundary-condition tables (85 bytes per boundary face) + partner lists
     b += 3.0 * (85.0 * nB + 4.0 * (nC + 1));
     // fields: 26 doubles per cell, 8 per face; Krylov: 9 doubles per cell
-    // [+ 9 floats]; tile partials and small buffers
-    b += nC * (26.0 + 9.0) * 8.0 + nF * 8.0 * 8.0 + (mixed ? 36.0 * nC : 0.0);
+    // [+ 9 floats and two (r, p) float pairs, folded-CG partials]; tile
+    // partials and small buffers
+    b += nC * (26.0 + 9.0) * 8.0 + nF * 8.0 * 8.0 + (mixed ? 52.0 * nC + 16384.0 : 0.0);
     b += 3.0 * 8.0 * (nC / 2048 + 1) + 4096.0;
     // permutations (mesh) and the field staging buffer (case)
     b += 8.0 * nC + 8.0 * nF + 8.0 * std::max(nC, nF);

@@ -121,6 +121,17 @@ int32_t xcal_abi_layout(int32_t which, int64_t* out, int32_t cap) {
                  XCAL_OFF(T, patch_count)};
             break;
         }
+        case XCAL_LAYOUT_TERM: {
+            using T = xcal_term;
+            v = {sizeof(T), XCAL_OFF(T, op), XCAL_OFF(T, scheme), XCAL_OFF(T, sign), XCAL_OFF(T, flux),
+                 XCAL_OFF(T, value)};
+            break;
+        }
+        case XCAL_LAYOUT_SOURCE: {
+            using T = xcal_source;
+            v = {sizeof(T), XCAL_OFF(T, sign), XCAL_OFF(T, field), XCAL_OFF(T, value)};
+            break;
+        }
         default:
             return XCAL_ERR_INVALID;
     }
@@ -444,7 +455,8 @@ int32_t xcal_case_solve_report(const xcal_case* cs, int32_t* iters7, int32_t* st
 }
 
 int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode) {
-    if (!cs || mode < 0 || mode >= 2 + 16) return XCAL_ERR_INVALID;
+    if (!cs || mode < 0 || mode >= 2 + 32 || (mode >= 2 && ((mode - 2) & 7) >= FOLD_NFORMS + FOLD_NSTAGED))
+        return XCAL_ERR_INVALID;
     XCAL_GUARD(cs->c->ctx, cs->c->set_inner_cg(mode));
 }
 

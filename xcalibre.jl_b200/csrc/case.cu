@@ -351,7 +351,7 @@ static void build_fold(Equation& E, cudaStream_t s, bool uniform_ok) {
     E.fold_uniform_ok = uniform_ok;
     const int n = E.n, nsl = (n + SELL_C - 1) / SELL_C;
     std::vector<int> fsl(nsl + 1, 0);
-    std::vector<unsigned char> flen(n);
+    std::vector<unsigned char> flen((size_t)nsl * SELL_C, 0);  // whole slices (copied slice by slice)
     for (int r = 0; r < n; ++r) {
         if (E.diag[r] < 0) fail(XCAL_ERR_INVALID, "folded CG: a row has no diagonal entry");
         if (E.len[r] - 1 > 127) fail(XCAL_ERR_UNSUPPORTED, "folded CG: a row has more than 127 off-diagonals");
@@ -792,6 +792,8 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         }
         ws.fpart.alloc(2 * FOLD_MAX_BLOCKS);
         ws.fpart.zero(stream);
+        ws.frp.alloc(2L * nC);
+        ws.frp.zero(stream);
         for (Equation* E : {&U, &P}) {
             E->nz32.alloc(E->nnz);
             E->nz32.zero(stream);
@@ -1582,9 +1584,9 @@ void Case::solve_captured(int eqn, int comp) {
         capture_while([&](cudaGraphConditionalHandle ho) {
             const long long k0 = t_launch_count;
             kr_outer_prep(stream, S);
-            kr_fold_defect(stream, A, E.nz.p, b, field, E.P.p, V.r);
-            kr_cg_start<float>(stream, n, V.r, V.r, V.p, S, ws.part0.p);
-            if (!kr_cgf_persist(stream, E.fold_view(), V.r, V.p, V.v, V.x, field, E.P.p, S, ws.fpart.p,
+            kr_fold_defect(stream, A, E.nz.p, b, field, E.P.p, ws.frp.p);
+            kr_fold_start(stream, n, ws.frp.p, S, ws.part0.p);
+            if (!kr_cgf_persist(stream, E.fold_view(), ws.frp.p, ws.frp.p + n, V.x, field, E.P.p, S, ws.fpart.p,
                                 ws.fpart.p + FOLD_MAX_BLOCKS, ws.bar.p, ws.err.p, itmax + 1, false, fold_form(),
                                 fold_smem()))
                 fail(XCAL_ERR_UNSUPPORTED, "folded CG: the system does not fit one block per SM");
@@ -1723,9 +1725,9 @@ bool Case::use_fold(const Equation& E, const xcal_solver_setup& SS, bool capture
 
 void Case::fold_iterate(Equation& E, double* field, const KrylovVecs<float>& V, KScalars* S, KScalars* hS, int gk) {
     (void)gk;
-    kr_cg_start<float>(stream, E.n, V.r, V.r, V.p, S, ws.part0.p);
+    kr_fold_start(stream, E.n, ws.frp.p, S, ws.part0.p);
     if (profiling) XCAL_CUDA(cudaEventRecord(ev[5], stream));
-    if (!kr_cgf_persist(stream, E.fold_view(), V.r, V.p, V.v, V.x, field, E.P.p, S, ws.fpart.p,
+    if (!kr_cgf_persist(stream, E.fold_view(), ws.frp.p, ws.frp.p + E.n, V.x, field, E.P.p, S, ws.fpart.p,
                         ws.fpart.p + FOLD_MAX_BLOCKS, ws.bar.p, ws.err.p, hS->itmax + 1, true, fold_form(),
                         fold_smem()))
         fail(XCAL_ERR_UNSUPPORTED, "folded CG: the system does not fit one block per SM");
@@ -1779,7 +1781,7 @@ void Case::solve_mixed(Equation& E, const xcal_solver_setup& SS, double* field, 
         if (fold) {
             // scaled defect, inner solve, and the correction applied by the
             // solve's own kernel (unless this defect met the target)
-            kr_fold_defect(stream, A, E.nz.p, b, field, E.P.p, V.r);
+            kr_fold_defect(stream, A, E.nz.p, b, field, E.P.p, ws.frp.p);
             fold_iterate(E, field, V, S, hS, gk);
             if (hS->outer_conv) break;
             total += hS->iter;

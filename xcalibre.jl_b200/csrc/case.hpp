@@ -138,6 +138,7 @@ struct KrylovWS {
     DBuf<double> x, dx, r, z, p, q, v, s, t, part0, part1;
     DBuf<float> fx, fr, fz, fp, fq, fv, fs, ft, fd;  // mixed precision inner vectors
     DBuf<double> fpart;  // folded inner CG: block partials (2 x FOLD_MAX_BLOCKS)
+    DBuf<float2> frp;    // folded inner CG: two buffers of n (r, p_old) pairs
     DBuf<unsigned int> bar;  // persistent CG: grid-barrier state (count, generation)
     DBuf<int> err;           // persistent CG: a barrier wait gave up
     DBuf<KScalars> S;  // [2]: U, p
@@ -210,9 +211,14 @@ struct Case {
     // and p kept in global memory) + 8 (per-slice slot widths even where the
     // uniform width would do); every v gives the same results as v & 3
     int inner_cg = 0;
-    int fold_form() const { return inner_cg >= 2 ? (inner_cg - 2) & 3 : FOLD_DEFAULT_FORM; }
-    bool fold_smem() const { return inner_cg < 2 || !((inner_cg - 2) & 4); }
-    bool fold_uniform_ok() const { return inner_cg < 2 || !((inner_cg - 2) & 8); }
+    // inner_cg = 2 + s + 8 g + 16 w: form s, x/p in global memory (g),
+    // per-slice slot widths (w)
+    int fold_form() const {
+        const int f = (inner_cg - 2) & 7;
+        return inner_cg >= 2 && f < FOLD_NFORMS + FOLD_NSTAGED ? f : FOLD_DEFAULT_FORM;
+    }
+    bool fold_smem() const { return inner_cg < 2 || !((inner_cg - 2) & 8); }
+    bool fold_uniform_ok() const { return inner_cg < 2 || !((inner_cg - 2) & 16); }
     void set_inner_cg(int mode);  // drops a captured step graph of the other form
     int dilu_mode = 0;          // 0 = autotuned / size rule, 1 = one-block sweeps, 2 = per-level kernels,
                                 // 3 = one cooperative launch over every level

@@ -284,7 +284,8 @@ struct FoldMut {
 };
 // kernel forms of the folded CG (block size / software pipelining over rows;
 // cg_folded.cu)
-constexpr int FOLD_NFORMS = 4;
+constexpr int FOLD_NFORMS = 4;   // register-loaded forms 0..3
+constexpr int FOLD_NSTAGED = 2;  // staged forms FOLD_NFORMS.. (slots by bulk copies; uniform layout)
 // most blocks of a folded-CG launch (one per SM); its two partial buffers
 // hold this many doubles each
 constexpr int FOLD_MAX_BLOCKS = 1024;
@@ -297,16 +298,21 @@ struct FoldShape {
 // keep x and p in shared memory where they fit (else both in global memory;
 // the same arithmetic either way)
 FoldShape fold_shape(int n, int form = FOLD_DEFAULT_FORM, bool vectors_in_smem = true);
-// r = (float)(sqrt(P) (b - A field)) in FP64 (P: FP64 Jacobi inverse diagonal)
+// rp[].x = (float)(sqrt(P) (b - A field)) in FP64 (P: FP64 Jacobi inverse
+// diagonal); rp[].y is left as it is
 void kr_fold_defect(cudaStream_t s, const CSRView& A, const double* nz, const double* b, const double* field,
-                    const double* P, float* r);
+                    const double* P, float2* rp);
+// gamma = <r, r> over rp[].x and cg!'s start tests into S (part: one double
+// per reduction tile)
+void kr_fold_start(cudaStream_t s, int n, const float2* rp, KScalars* S, double* part);
 // scaled off-diagonal values and diagonal signs from the FP64 matrix and P
 void kr_fold_scale(cudaStream_t s, const FoldMut& F, const double* nz, const int* diag, const double* P);
-// the whole inner solve after kr_cg_start(rhat, rhat, P0), with field +=
+// the whole inner solve after kr_fold_defect(RP0) and kr_fold_start, with field +=
 // sqrt(P) xhat applied at its end unless S->outer_conv; false: too large
 // (nothing launched).  xg: an n-float buffer used when x does not fit
-// shared memory; part, part2: FOLD_MAX_BLOCKS doubles each.
-bool kr_cgf_persist(cudaStream_t s, const FoldView& F, float* r, float* P0, float* P1, float* xg, double* field,
+// shared memory; part, part2: FOLD_MAX_BLOCKS doubles each.  RP0, RP1: n
+// (r, p_old) pairs each, swapped every iteration.
+bool kr_cgf_persist(cudaStream_t s, const FoldView& F, float2* RP0, float2* RP1, float* xg, double* field,
                     const double* Pj, KScalars* S, double* part, double* part2, unsigned int* bar, int* err,
                     int max_iters, bool reset_err = true, int form = FOLD_DEFAULT_FORM,
                     bool vectors_in_smem = true);

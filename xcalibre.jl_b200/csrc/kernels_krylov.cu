@@ -260,31 +260,103 @@ __global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_block(int n, LevelV
     dilu_level_sweep<T>(n, lo, up, D, b, y, smem ? reinterpret_cast<T*>(dilu_smem) : y);
 }
 
+// One row of a level-ordered triangle with its first U slots in registers
+// (column, value and, for the lower triangle, 1/D of the column): what a
+// row's sweep reads that no sweep writes, so it can be loaded early.
+template <class T, int U>
+struct LvRow {
+    int i, c, base;
+    T rhs;
+    int cj[U];
+    T vj[U], dj[U];
+};
+template <class T, int U>
+__device__ __forceinline__ void lv_load(const LevelView<T>& L, bool lower, int k, const T* __restrict__ D,
+                                        const T* __restrict__ b, LvRow<T, U>& r) {
+    r.i = L.rows[k];
+    r.c = L.cnt[k];
+    r.base = L.slice[k / SELL_C] + (k % SELL_C);
+    r.rhs = lower ? b[r.i] : D[r.i];
+#pragma unroll
+    for (int j = 0; j < U; ++j)
+        if (j < r.c) {
+            const int e = r.base + SELL_C * j;
+            r.cj[j] = ld_stream(L.col + e);
+            r.vj[j] = ld_stream(L.val + e);
+            if (lower) r.dj[j] = ld_stream(L.dinv + e);
+        }
+}
+// the row's sweep: dilu_level_s's arithmetic (the same sum in the same
+// entry order), slots past the first U read here
+template <class T, bool LOWER, int U>
+__device__ __forceinline__ void lv_apply(const LevelView<T>& L, const LvRow<T, U>& r, T* ys) {
+    T sum = T(0);
+#pragma unroll
+    for (int j = 0; j < U; ++j)
+        if (j < r.c) sum = LOWER ? sum + (r.vj[j] * ys[r.cj[j]]) * r.dj[j] : sum + r.vj[j] * ys[r.cj[j]];
+    for (int j = U; j < r.c; ++j) {
+        const int e = r.base + SELL_C * j;
+        sum = LOWER ? sum + (ld_stream(L.val + e) * ys[ld_stream(L.col + e)]) * ld_stream(L.dinv + e)
+                    : sum + ld_stream(L.val + e) * ys[ld_stream(L.col + e)];
+    }
+    ys[r.i] = LOWER ? r.rhs - sum : (ys[r.i] - sum) / r.rhs;
+}
+
 // Every level of one DILU application in one cooperative launch: the
 // forward sweep's levels, then the backward sweep's, each spread over the
 // whole grid (rows of a level are independent), with the bounded grid
-// barrier between consecutive levels.  Each row's arithmetic is that of the
-// level kernels (dilu_level_s), bit for bit; only the launches go.  A barrier
-// that gives up sets *err and ends every block.
+// barrier between consecutive levels.  A thread loads its first row of the
+// next level (indices, slots, right-hand side: nothing the sweep writes)
+// before it enters the barrier, so only the gathers of y wait behind it.
+// Each row's arithmetic is that of the level kernels (dilu_level_s), bit for
+// bit; only the launches go.  A barrier that gives up sets *err and ends
+// every block.
 constexpr int DILU_GRID_THREADS = 512;
 template <class T>
-__global__ void __launch_bounds__(DILU_GRID_THREADS) k_dilu_grid(LevelView<T> lo, LevelView<T> up,
-                                                                 const T* __restrict__ D, const T* __restrict__ b,
-                                                                 T* y, unsigned int* bar, int* err,
-                                                                 const KScalars* S) {
+__global__ void __launch_bounds__(DILU_GRID_THREADS, 2) k_dilu_grid(LevelView<T> lo, LevelView<T> up,
+                                                                    const T* __restrict__ D,
+                                                                    const T* __restrict__ b, T* y,
+                                                                    unsigned int* bar, int* err,
+                                                                    const KScalars* S) {
+    constexpr int U = sizeof(T) == 4 ? 6 : 4;
     __shared__ int sh_err;
     if (S && S->done) return;
     const int start = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     const int total = lo.nlev + up.nlev;
     unsigned int nb = 0;
+    LvRow<T, U> r;
+    bool have = false;  // r holds this thread's first row of level l
+    if (total > 0 && lo.nlev > 0 && lo.off[0] + start < lo.off[1]) {
+        lv_load<T, U>(lo, true, lo.off[0] + start, D, b, r);
+        have = true;
+    }
     for (int l = 0; l < total; ++l) {
-        if (l < lo.nlev) {
-            dilu_level_s<T, true>(lo, lo.off[l], lo.off[l + 1], D, b, y, start, stride);
-        } else {
-            const int u = l - lo.nlev;
-            dilu_level_s<T, false>(up, up.off[u], up.off[u + 1], D, b, y, start, stride);
+        const bool lower = l < lo.nlev;
+        const LevelView<T>& L = lower ? lo : up;
+        const int lv = lower ? l : l - lo.nlev;
+        const int k1 = L.off[lv + 1];
+        int k = L.off[lv] + start;
+        if (have) {
+            if (lower)
+                lv_apply<T, true, U>(L, r, y);
+            else
+                lv_apply<T, false, U>(L, r, y);
+            k += stride;
         }
-        if (l + 1 < total && !grid_barrier(bar, gridDim.x, nb, err, &sh_err)) return;
+        for (; k < k1; k += stride) {
+            lv_load<T, U>(L, lower, k, D, b, r);
+            if (lower)
+                lv_apply<T, true, U>(L, r, y);
+            else
+                lv_apply<T, false, U>(L, r, y);
+        }
+        if (l + 1 == total) break;
+        const bool nlower = l + 1 < lo.nlev;
+        const LevelView<T>& N = nlower ? lo : up;
+        const int nv = nlower ? l + 1 : l + 1 - lo.nlev;
+        have = N.off[nv] + start < N.off[nv + 1];
+        if (have) lv_load<T, U>(N, nlower, N.off[nv] + start, D, b, r);
+        if (!grid_barrier(bar, gridDim.x, nb, err, &sh_err)) return;
     }
 }
 

@@ -103,6 +103,35 @@ __device__ __forceinline__ void copy_body(const TileCtx& tc, int n, const T* __r
     }
 }
 
+// the start of a cg! solve from gamma = <r0, z0> (Krylov.jl cg!): norms,
+// the stopping tolerance (start_eps), zero right-hand side, immediate stop
+__device__ __forceinline__ void cg_start_scalars(KScalars* S, double gamma) {
+    S->gamma = gamma;
+    double rNorm = sqrt(gamma);
+    S->rNorm = rNorm;
+    S->rNorm0 = rNorm;
+    S->iter = 0;
+    S->done = 0;
+    S->status = KS_RUNNING;
+    S->outer_conv = 0;
+    S->loops = 0;
+    if (gamma == 0.0) {
+        S->done = 1;
+        S->status = KS_ZERO_RHS;
+        S->outer_conv = 1;
+        return;
+    }
+    S->pNorm2 = gamma;
+    start_eps(S, rNorm);
+    if (rNorm <= S->eps) {
+        S->done = 1;
+        S->status = KS_SOLVED;
+    } else if (S->iter >= S->itmax) {
+        S->done = 1;
+        S->status = KS_TIRED;
+    }
+}
+
 template <class T>
 __device__ __forceinline__ void cg_start_body(const TileCtx& tc, int n, const T* __restrict__ r, const T* __restrict__ z, T* p, KScalars* S,
                            double* part) {
@@ -120,32 +149,7 @@ __device__ __forceinline__ void cg_start_body(const TileCtx& tc, int n, const T*
     if (threadIdx.x == 0) part[tc.tile] = tot;
     if (!last_block(&S->counter, tc.ntiles)) return;
     double gamma = reduce_partials(part, tc.ntiles, sm);
-    if (threadIdx.x == 0) {
-        S->gamma = gamma;
-        double rNorm = sqrt(gamma);
-        S->rNorm = rNorm;
-        S->rNorm0 = rNorm;
-        S->iter = 0;
-        S->done = 0;
-        S->status = KS_RUNNING;
-        S->outer_conv = 0;
-        S->loops = 0;
-        if (gamma == 0.0) {
-            S->done = 1;
-            S->status = KS_ZERO_RHS;
-            S->outer_conv = 1;
-            return;
-        }
-        S->pNorm2 = gamma;
-        start_eps(S, rNorm);
-        if (rNorm <= S->eps) {
-            S->done = 1;
-            S->status = KS_SOLVED;
-        } else if (S->iter >= S->itmax) {
-            S->done = 1;
-            S->status = KS_TIRED;
-        }
-    }
+    if (threadIdx.x == 0) cg_start_scalars(S, gamma);
 }
 
 template <class T>
