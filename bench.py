@@ -341,10 +341,10 @@ def measure(x, A, mesh, precision, args, local, world, stream_cls):
         bpi = nnz_off * 8 + n * (1 + 8 + 8 + 8)
         t_it = pers_ms / pers_it / 1e3
         ach = bpi / t_it / 1e9
-        roof = {"bound": "hbm", "kernel": "k_cgf_staged / k_cgf_persist (FP32 CG on the Jacobi-scaled system, "
-                                          "whole solve in one cooperative launch, one block per SM: gathered SpMV "
-                                          "of the off-diagonal slots with p = r + beta p, grid barrier, x/r "
-                                          "update, grid barrier)",
+        roof = {"bound": "hbm", "kernel": "k_cgf_persist (FP32 CG on the Jacobi-scaled system, whole solve in one "
+                                          "cooperative launch, one block per SM: gathered SpMV of the off-diagonal "
+                                          "slots with p = r + beta p from (r, p) pairs, grid barrier, x/r update, "
+                                          "grid barrier)",
                 "achieved": ach, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak,
                 "traffic": (tr_all.get("fold_bytes_per_iteration_128") if args.size == 128 else None),
                 "traffic_unit": "bytes per CG iteration (ncu DRAM read + write of one launch / its iterations)",

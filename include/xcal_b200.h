@@ -585,16 +585,14 @@ int32_t xcal_case_solve_report(const xcal_case* cs, int32_t* iters7, int32_t* st
  * M^1/2 A M^1/2 (the same iteration in exact arithmetic, deterministic, its
  * own reduction order) where the system fits one block per SM, else as 1;
  * 1 = the FP32 form of the FP64 path's kernels; 2 + v = the scaled-system
- * kernel with v = s + 8 g + 16 w: s its launch shape -- 0..3: 768 or 1024
+ * kernel with v = s + 4 g + 8 w: s (0..3) its launch shape (768 or 1024
  * threads per block, with or without the next row's slot loads issued
- * early; 4, 5: 768 or 1024 threads with the slots streamed into shared
- * memory by bulk asynchronous copies (uniform slot widths up to 8; else
- * shape 2 or 3) --, g = 1 the iterate and the direction kept in global
- * memory instead of shared memory, w = 1 per-slice slot widths even where
- * one uniform width would do.  Shapes with the same thread count, g and w
- * change where data lives, not the results (768-thread shapes agree bit for
- * bit, as do 1024-thread ones).  All meet the same stopping tests; results
- * agree within the mixed-precision tolerance. */
+ * early), g = 1 the iterate and the direction kept in global memory instead
+ * of shared memory, w = 1 per-slice slot widths even where one uniform width
+ * would do.  Shapes with the same thread count, g and w change where data
+ * lives, not the results (768-thread shapes agree bit for bit, as do
+ * 1024-thread ones).  All meet the same stopping tests; results agree within
+ * the mixed-precision tolerance. */
 int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode);
 /* launch-shape autotuner (runs on first use, or now): out6 = for U then p,
  * (SpMV rows per thread [0 = canonical tile kernel], SpMV block size, DILU

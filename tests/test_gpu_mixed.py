@@ -86,7 +86,7 @@ def _tight_pressure(x, ctx, mesh, prec, inner_cg=None):
     return p
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5, 6, 7, 21])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4, 5, 13])
 def test_inner_cg_forms_tight(x, ctx, mode):
     """Every form of the FP32 inner CG (Jacobi-scaled system in each launch
     shape; the canonical kernels) meets the tight-solve bound against FP64."""
@@ -96,20 +96,20 @@ def test_inner_cg_forms_tight(x, ctx, mode):
     assert rel(p, p64) <= 1e-6, rel(p, p64)
 
 
-@pytest.mark.parametrize("form", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("form", [0, 1, 2, 3])
 def test_inner_cg_layouts_identical(x, ctx, form):
     """The scaled-system kernel with x and p in global memory (the layout
     of systems too large for shared memory), with per-slice slot widths (the
     layout of meshes whose rows differ widely in length), and with both,
     gives the default layout's result bit for bit: only where data lives
-    differs.  The staged shapes (4, 5) equal the register-loaded shapes of
-    the same thread count (0, 2 and 1, 3)."""
+    differs.  Shapes of the same thread count (0 and 2, 1 and 3) agree bit
+    for bit as well."""
     mesh = x.build_mesh3(x.channel_polymesh(40, 24, 20, seed=4))
     a = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=2 + form)
-    for extra in (8, 16, 24):
+    for extra in (4, 8, 12):
         b = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=2 + form + extra)
         assert np.array_equal(a, b), extra
-    same_nt = {0: 2, 1: 3, 2: 0, 3: 1, 4: 0, 5: 1}[form]
+    same_nt = {0: 2, 1: 3, 2: 0, 3: 1}[form]
     b = _tight_pressure(x, ctx, mesh, "mixed", inner_cg=2 + same_nt)
     assert np.array_equal(a, b), same_nt
 

@@ -868,12 +868,11 @@ class Case:
     def set_inner_cg(self, mode: int):
         """Mixed precision, CG + Jacobi inner solves: 0 = on the Jacobi-scaled
         system (default), 1 = the FP32 form of the FP64 path's kernels,
-        2 + s + 8 g + 16 w = the scaled-system kernel in launch shape s
-        (0..3 register-loaded slots, 768/1024 threads with or without early
-        loads of the next row; 4, 5 slots staged in shared memory by bulk
-        copies, 768/1024 threads), with x and p in global memory (g = 1) and
-        per-slice slot widths (w = 1).  Shapes with the same thread count, g
-        and w give the same results bit for bit."""
+        2 + s + 4 g + 8 w = the scaled-system kernel in launch shape s (0..3:
+        768/1024 threads, with or without early loads of the next row's
+        slots), with x and p in global memory (g = 1) and per-slice slot
+        widths (w = 1).  Shapes with the same thread count, g and w give the
+        same results bit for bit."""
         self._chk(lib().xcal_case_set_inner_cg(self.h, int(mode)))
 
     def checkpoint(self) -> dict:

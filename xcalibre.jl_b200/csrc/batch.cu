@@ -776,6 +776,9 @@ size_t estimate_case_bytes(long nC, long nF, long nB, int mixed, int dilu_U, int
             // per lower slot [+ fp32]
             b += (nnz - nC) * 1.5 * (16.0 + (mixed ? 4.0 : 0.0)) + 2.0 * nC + 8.0 * (nC / 32 + 2);
             b += (nnz - nC) * 0.5 * 1.5 * (8.0 + (mixed ? 4.0 : 0.0));
+            // the factor's transposed-entry slots (lower triangle) and
+            // diagonal slots per position
+            b += (nnz - nC) * 0.5 * 1.5 * 4.0 + 4.0 * nC;
         }
     }
     // three boundary-condition tables (85 bytes per boundary face) + partner lists

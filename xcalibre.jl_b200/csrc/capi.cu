@@ -455,8 +455,7 @@ int32_t xcal_case_solve_report(const xcal_case* cs, int32_t* iters7, int32_t* st
 }
 
 int32_t xcal_case_set_inner_cg(xcal_case* cs, int32_t mode) {
-    if (!cs || mode < 0 || mode >= 2 + 32 || (mode >= 2 && ((mode - 2) & 7) >= FOLD_NFORMS + FOLD_NSTAGED))
-        return XCAL_ERR_INVALID;
+    if (!cs || mode < 0 || mode >= 2 + 16) return XCAL_ERR_INVALID;
     XCAL_GUARD(cs->c->ctx, cs->c->set_inner_cg(mode));
 }
 

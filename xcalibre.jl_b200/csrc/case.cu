@@ -351,7 +351,7 @@ static void build_fold(Equation& E, cudaStream_t s, bool uniform_ok) {
     E.fold_uniform_ok = uniform_ok;
     const int n = E.n, nsl = (n + SELL_C - 1) / SELL_C;
     std::vector<int> fsl(nsl + 1, 0);
-    std::vector<unsigned char> flen((size_t)nsl * SELL_C, 0);  // whole slices (copied slice by slice)
+    std::vector<unsigned char> flen((size_t)nsl * SELL_C, 0);  // whole slices
     for (int r = 0; r < n; ++r) {
         if (E.diag[r] < 0) fail(XCAL_ERR_INVALID, "folded CG: a row has no diagonal entry");
         if (E.len[r] - 1 > 127) fail(XCAL_ERR_UNSUPPORTED, "folded CG: a row has more than 127 off-diagonals");
@@ -563,6 +563,13 @@ void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal_bc>& b
             L.cnt.upload(cnt, s);
             L.col.upload(col, s);
             L.src.upload(src, s);
+            if (tri == 0) {  // what the DILU factor reads besides: a_ji's slot, each row's diagonal slot
+                std::vector<int> tsrc(src.size()), dslot(n);
+                for (size_t e = 0; e < src.size(); ++e) tsrc[e] = trans[src[e]];
+                for (int k = 0; k < n; ++k) dslot[k] = E.diag[order[k]];
+                L.tsrc.upload(tsrc, s);
+                L.dslot.upload(dslot, s);
+            }
             L.val.alloc(std::max(L.nslots, 1L));
             L.val.zero(s);
             if (tri == 0) {
@@ -1207,13 +1214,10 @@ void Case::update_precond_E(Equation& E, int pt) {
         kr_jacobi_update(stream, E.view(), E.nz.p, E.P.p);
     } else if (pt == XCAL_PRECOND_DILU) {
         if (E.dilu_block()) {
-            kr_dilu_D_block(stream, E.d_lower_rows.p, E.d_lower_off.p, (int)E.lower_off.size() - 1, E.view(), E.nz.p,
-                            E.P.p);
+            kr_dilu_D_lv_block(stream, E.n, level_d_view(E), E.nz.p, E.P.p);
             return;
         }
-        if (E.use_grid && coop_ok_here() &&
-            kr_dilu_D_grid(stream, E.d_lower_rows.p, E.d_lower_off.p, (int)E.lower_off.size() - 1, E.view(), E.nz.p,
-                           E.P.p, ws.bar.p, ws.err.p))
+        if (E.use_grid && coop_ok_here() && kr_dilu_D_lv_grid(stream, level_d_view(E), E.nz.p, E.P.p, ws.bar.p, ws.err.p))
             return;
         for (size_t l = 0; l + 1 < E.lower_off.size(); ++l)
             kr_dilu_D(stream, E.d_lower_rows.p + E.lower_off[l], E.lower_off[l + 1] - E.lower_off[l], E.view(),
@@ -1259,6 +1263,12 @@ void Case::dilu_refresh(Equation& E, bool fp32) {
         kr_level_dinv(stream, E.lsell.nslots, E.lsell.col.p, E.P32.p, E.lsell.dinv32.p);
     else
         kr_level_dinv(stream, E.lsell.nslots, E.lsell.col.p, E.P.p, E.lsell.dinv.p);
+}
+
+LevelDView level_d_view(const Equation& E) {
+    const LevelSell& L = E.lsell;
+    return LevelDView{E.d_lower_rows.p, E.d_lower_off.p, (int)E.lower_off.size() - 1, L.slice.p, L.cnt.p,
+                      L.col.p, L.src.p, L.tsrc.p, L.dslot.p};
 }
 
 template <class T>

@@ -64,6 +64,8 @@ struct DevMesh {
 struct LevelSell {
     long nslots = 0;
     DBuf<int> slice, col, src;
+    DBuf<int> tsrc;   // lower triangle: slot of the transposed entry a_ji (DILU factor)
+    DBuf<int> dslot;  // lower triangle: diagonal slot of each position's row (DILU factor)
     DBuf<unsigned char> cnt;
     DBuf<double> val, dinv;
     DBuf<float> val32, dinv32;
@@ -74,6 +76,8 @@ struct Equation;
 // value type T (refreshed by Case::dilu_refresh)
 template <class T>
 LevelView<T> level_view(const Equation& E, int tri);
+// the level-ordered lower triangle as the DILU factor reads it
+LevelDView level_d_view(const Equation& E);
 
 struct Equation {
     int n = 0;
@@ -211,14 +215,11 @@ struct Case {
     // and p kept in global memory) + 8 (per-slice slot widths even where the
     // uniform width would do); every v gives the same results as v & 3
     int inner_cg = 0;
-    // inner_cg = 2 + s + 8 g + 16 w: form s, x/p in global memory (g),
+    // inner_cg = 2 + s + 4 g + 8 w: form s, x/p in global memory (g),
     // per-slice slot widths (w)
-    int fold_form() const {
-        const int f = (inner_cg - 2) & 7;
-        return inner_cg >= 2 && f < FOLD_NFORMS + FOLD_NSTAGED ? f : FOLD_DEFAULT_FORM;
-    }
-    bool fold_smem() const { return inner_cg < 2 || !((inner_cg - 2) & 8); }
-    bool fold_uniform_ok() const { return inner_cg < 2 || !((inner_cg - 2) & 16); }
+    int fold_form() const { return inner_cg >= 2 ? (inner_cg - 2) & 3 : FOLD_DEFAULT_FORM; }
+    bool fold_smem() const { return inner_cg < 2 || !((inner_cg - 2) & 4); }
+    bool fold_uniform_ok() const { return inner_cg < 2 || !((inner_cg - 2) & 8); }
     void set_inner_cg(int mode);  // drops a captured step graph of the other form
     int dilu_mode = 0;          // 0 = autotuned / size rule, 1 = one-block sweeps, 2 = per-level kernels,
                                 // 3 = one cooperative launch over every level

@@ -27,9 +27,6 @@
 // order, so every block takes the same decisions.
 #include <cooperative_groups.h>
 
-#include <algorithm>
-#include <vector>
-
 #include "dev_common.cuh"
 #include "kernels.hpp"
 #include "krylov_bodies.cuh"
@@ -328,269 +325,6 @@ __global__ void __launch_bounds__(NT, 1)
     }
 }
 
-// ---------------------------------------------------------------------------
-// Staged form: the matrix slots reach shared memory by bulk asynchronous
-// copies (cp.async.bulk, completion counted on an mbarrier), so no slot load
-// stands in front of a row's gathers and the copy engine, not the warps'
-// registers, keeps the matrix stream in flight.  Uniform slot layout only.
-//
-// Each warp owns a ring of `nstage` stages; a stage holds one slice (32
-// rows): W columns, W values and the 32 length bytes, 256 W + 32 bytes.  A
-// warp's slices are the ones its rows fall in (rows 32 (w + j NW) + lane of
-// the block, exactly the rows the other forms give that thread), taken in
-// order, then again from the first: the matrix does not change during the
-// solve, so the copies of the next iteration's first slices run during the
-// grid barriers.  A stage is refilled as soon as the warp has used it.
-//
-// Per row the arithmetic is fold_q's, and the rows each thread adds are the
-// same as in k_cgf_persist with the same NT: the two give the same results
-// bit for bit.  p_k is not stored: phase 2 re-forms it from the same pair
-// (r, p_old) with the same operation.  Every wait is bounded; a stage wait
-// that gives up sets the error flag and the block leaves before the next
-// grid barrier (the others then leave theirs); copies still in flight are
-// waited for, with the same bound, before any block exits.
-
-constexpr int STAGE_WMAX = 8;             // widest uniform row (slots) the staged form takes
-constexpr int STAGE_MAX = 6;              // stages per warp at most
-constexpr int STAGE_SMEM_MAX = 224 * 1024;  // dynamic shared memory (q, x, stages)
-constexpr long STAGE_SPIN_LIMIT = 1L << 24;  // polls before a stage wait gives up
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect(unsigned long long* b, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_done(unsigned long long* b, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// bounded wait for the completion of phase `parity`; false: gave up
-__device__ __forceinline__ bool mbar_wait(unsigned long long* b, unsigned parity) {
-    for (long k = 0; k < STAGE_SPIN_LIMIT; ++k)
-        if (mbar_done(b, parity)) return true;
-    return false;
-}
-// global -> this block's shared memory, `bytes` (a multiple of 16, both
-// addresses 16-byte aligned), counted on b
-__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, unsigned bytes, unsigned long long* b) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(b))
-                 : "memory");
-}
-
-// q_i and p_i of row i from its slots, already read out of the stage (c,
-// v: columns and values; lb: the row's length byte)
-template <bool FIRST>
-__device__ __forceinline__ float stage_q(const float2* rp, float beta, int i, int W, const int (&c)[STAGE_WMAX],
-                                         const float (&v)[STAGE_WMAX], unsigned lb, float& pi) {
-    pi = fold_dir<FIRST>(rp, beta, i);
-    float q = (lb & 0x80) ? -pi : pi;
-#pragma unroll
-    for (int m = 0; m < STAGE_WMAX; ++m)
-        if (m < W) q = __fmaf_rn(v[m], fold_dir<FIRST>(rp, beta, c[m]), q);
-    return q;
-}
-
-template <int NT>
-__global__ void __launch_bounds__(NT, 1)
-    k_cgf_staged(FoldView F, float2* RP0, float2* RP1, float* xg, double* field, const double* __restrict__ Pj,
-                 KScalars* S, double* part, double* part2, unsigned int* bar, int* err, int max_iters, int R,
-                 int smem_x, int nstage) {
-    constexpr int NW = NT / 32;
-    extern __shared__ __align__(128) unsigned char stage_raw[];
-    __shared__ double sm[33];
-    __shared__ int sh_err, sh_stage;
-    __shared__ unsigned long long mbar[NW * STAGE_MAX];
-    const int W = F.W;
-    const int SB = 256 * W + 32;  // bytes of one stage
-    float* q_s = (float*)stage_raw;
-    float* x_s = q_s + R;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* ring = stage_raw + 4L * R * (1 + smem_x) + (long)warp * nstage * SB;
-    unsigned long long* wb = mbar + warp * STAGE_MAX;
-    const int n = F.n;
-    const int row0 = blockIdx.x * R;
-    const int nr = max(0, min(R, n - row0));
-    const int G = gridDim.x;
-    // this warp's slices per iteration (local slice j: rows 32 (warp + j NW) + lane)
-    const int nsw = nr > 32 * warp ? (nr - 32 * warp + 32 * NW - 1) / (32 * NW) : 0;
-    if (threadIdx.x == 0) sh_stage = 0;
-    if (lane == 0)
-        for (int s = 0; s < nstage; ++s) mbar_init(wb + s, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    __syncthreads();
-    // this warp's stage sequence (the same in every lane): the next stage
-    // to fill and the local slice it gets; the next stage to use and the
-    // parity of the fill it waits for; fills not yet used
-    int iss_s = 0, iss_j = 0, use_s = 0, pending = 0;
-    unsigned use_ph = 0;
-    auto issue = [&]() {
-        if (lane == 0) {
-            const long g = (long)(row0 >> 5) + warp + (long)iss_j * NW;
-            unsigned char* st = ring + (long)iss_s * SB;
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_expect(wb + iss_s, (unsigned)SB);
-            bulk_to_smem(st, F.col + (long)SELL_C * W * g, 128u * W, wb + iss_s);
-            bulk_to_smem(st + 128 * W, F.val + (long)SELL_C * W * g, 128u * W, wb + iss_s);
-            bulk_to_smem(st + 256 * W, F.len + (long)SELL_C * g, 32u, wb + iss_s);
-        }
-        iss_s = iss_s + 1 == nstage ? 0 : iss_s + 1;
-        iss_j = iss_j + 1 == nsw ? 0 : iss_j + 1;
-        ++pending;
-    };
-    auto retire = [&]() {
-        if (++use_s == nstage) {
-            use_s = 0;
-            use_ph ^= 1u;
-        }
-        --pending;
-    };
-    if (nsw > 0)
-        for (int s = 0; s < nstage; ++s) issue();
-    for (int k = threadIdx.x; k < nr; k += NT) {
-        if (smem_x)
-            x_s[k] = 0.0f;
-        else
-            xg[row0 + k] = 0.0f;
-    }
-    int iter = S->iter, done = S->done, status = S->status;
-    const int itmax = S->itmax, outer_conv = S->outer_conv;
-    double gamma = S->gamma, beta = S->beta, pNorm2 = S->pNorm2, alpha = S->alpha, rNorm = S->rNorm;
-    const double eps = S->eps;
-    const double epsT = 1.1920928955078125e-07;  // eps(Float32)
-    unsigned int nb = 0;
-    bool ok = true;
-    int ran = 0;
-    while (!done && ran < max_iters) {
-        const float2* cur = (iter & 1) ? RP1 : RP0;
-        float2* nxt = (iter & 1) ? RP0 : RP1;
-        const float bt = (float)beta;
-        double acc = 0.0;
-        for (int j = 0; j < nsw; ++j) {
-            if (!__all_sync(0xffffffffu, mbar_wait(wb + use_s, use_ph))) {
-                if (lane == 0) sh_stage = 1;
-                break;
-            }
-            // read the row's slots out of the stage, then refill the stage
-            // before the gathers, so the copy runs while they wait
-            const unsigned char* st = ring + (long)use_s * SB;
-            const int k = SELL_C * (warp + j * NW) + lane;
-            int c[STAGE_WMAX];
-            float v[STAGE_WMAX];
-            unsigned lb = 0;
-            if (k < nr) {
-                const int* cs = (const int*)st;
-                const float* vs = (const float*)(st + 128 * W);
-#pragma unroll
-                for (int m = 0; m < STAGE_WMAX; ++m)
-                    if (m < W) {
-                        c[m] = cs[SELL_C * m + lane];
-                        v[m] = vs[SELL_C * m + lane];
-                    }
-                lb = st[256 * W + lane];
-            }
-            __syncwarp();
-            retire();
-            issue();
-            if (k < nr) {
-                const int i = row0 + k;
-                float pi, qi;
-                if (iter == 0)
-                    qi = stage_q<true>(cur, bt, i, W, c, v, lb, pi);
-                else
-                    qi = stage_q<false>(cur, bt, i, W, c, v, lb, pi);
-                q_s[k] = qi;
-                acc = acc + (double)pi * (double)qi;
-            }
-        }
-        double tot = fold_block_sum(acc, sm);
-        if (sh_stage) {  // uniform: read after the block sum's barriers
-            if (threadIdx.x == 0) *(volatile int*)err = 1;
-            ok = false;
-            break;
-        }
-        if (threadIdx.x == 0) part[blockIdx.x] = tot;
-        if (!(ok = grid_barrier(bar, G, nb, err, &sh_err))) break;
-        const double pAp = fold_grid_sum(part, G, sm);
-        const double lim = epsT * pNorm2;
-        if (pAp <= lim && fabs(pAp) <= lim) {
-            done = 1;
-            status = KS_ZERO_CURV;
-            break;
-        }
-        alpha = gamma / pAp;
-        const float a = (float)alpha;
-        double acc2 = 0.0;
-        for (int k = threadIdx.x; k < nr; k += NT) {
-            const int i = row0 + k;
-            const float2 g = cur[i];
-            const float pi = iter == 0 ? g.x : __fmaf_rn(bt, g.y, g.x);
-            if (smem_x)
-                x_s[k] = __fmaf_rn(a, pi, x_s[k]);
-            else
-                xg[i] = __fmaf_rn(a, pi, xg[i]);
-            const float ri = __fmaf_rn(-a, q_s[k], g.x);
-            nxt[i] = make_float2(ri, pi);
-            acc2 = acc2 + (double)ri * (double)ri;
-        }
-        double tot2 = fold_block_sum(acc2, sm);
-        if (threadIdx.x == 0) part2[blockIdx.x] = tot2;
-        if (!(ok = grid_barrier(bar, G, nb, err, &sh_err))) break;
-        const double g2 = fold_grid_sum(part2, G, sm);
-        // cg! stopping tests (the same as cg_finalize), in every thread
-        rNorm = sqrt(g2);
-        const bool solved = (rNorm <= eps) || (rNorm + 1.0 <= 1.0);
-        if (!solved) {
-            const double b2 = g2 / gamma;
-            pNorm2 = g2 + (b2 * b2) * pNorm2;
-            gamma = g2;
-            beta = b2;
-        }
-        iter = iter + 1;
-        if (solved) {
-            done = 1;
-            status = KS_SOLVED;
-        } else if (iter >= itmax) {
-            done = 1;
-            status = KS_TIRED;
-        }
-        ++ran;
-    }
-    // the copies still in flight land before the block's shared memory goes
-    while (pending > 0) {
-        mbar_wait(wb + use_s, use_ph);
-        retire();
-    }
-    __syncwarp();
-    if (!ok) return;
-    if (!outer_conv)
-        for (int k = threadIdx.x; k < nr; k += NT) {
-            const int i = row0 + k;
-            const float xh = smem_x ? x_s[k] : xg[i];
-            field[i] = field[i] + sqrt(Pj[i]) * (double)xh;
-        }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        S->iter = iter;
-        S->done = done;
-        S->status = status;
-        S->gamma = gamma;
-        S->beta = beta;
-        S->pNorm2 = pNorm2;
-        S->alpha = alpha;
-        S->rNorm = rNorm;
-    }
-}
-
 void kr_fold_defect(cudaStream_t s, const CSRView& A, const double* nz, const double* b, const double* field,
                     const double* P, float2* rp) {
     k_fold_defect<<<(A.n + RED_TILE - 1) / RED_TILE, RED_THREADS, 0, s>>>(A, nz, b, field, P, rp);
@@ -628,12 +362,6 @@ static const FoldKernel FOLD_FORMS[2][FOLD_NFORMS] = {
     },
 };
 
-// the staged forms (index form - FOLD_NFORMS): uniform slot layout only
-static const FoldKernel STAGED[FOLD_NSTAGED] = {
-    {(const void*)k_cgf_staged<768>, 768},
-    {(const void*)k_cgf_staged<1024>, 1024},
-};
-
 // launch geometry of the folded CG (form `form`) for n rows: blocks (one per
 // SM while the rows fit), rows per block (a multiple of 32) and which vectors
 // stay in shared memory; blocks = 0 when the system does not fit
@@ -642,14 +370,7 @@ FoldShape fold_shape(int n, int form, bool vectors_in_smem) {
     // block with the largest shared-memory request is co-resident on an SM
     static int sms = -1;
     static int attr_ok[FOLD_NFORMS] = {-1, -1, -1, -1};
-    if (form < 0 || form >= FOLD_NFORMS + FOLD_NSTAGED) form = FOLD_DEFAULT_FORM;
-    if (form >= FOLD_NFORMS) {
-        // a staged form: the blocks and rows of the pipelined form with its
-        // thread count (its fallback when the staged geometry does not fit)
-        FoldShape sh = fold_shape(n, form - 2, vectors_in_smem);
-        if (sh.blocks > 0) sh.form = form;
-        return sh;
-    }
+    if (form < 0 || form >= FOLD_NFORMS) form = FOLD_DEFAULT_FORM;
     if (sms < 0) {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -687,66 +408,17 @@ FoldShape fold_shape(int n, int form, bool vectors_in_smem) {
     return sh;
 }
 
-// geometry of a staged form for rows of W slots: stages per warp and
-// whether x stays in shared memory; false when it does not fit (the caller
-// then runs the pipelined form with the same thread count)
-static bool stage_shape(const FoldShape& sh, int W, bool vectors_in_smem, int& nstage, int& smem_x, int& smem) {
-    if (W <= 0 || W > STAGE_WMAX) return false;
-    const int k = sh.form - FOLD_NFORMS;
-    static int attr_ok[FOLD_NSTAGED] = {-1, -1};
-    if (attr_ok[k] < 0) {
-        int per = 0;
-        attr_ok[k] = cudaFuncSetAttribute(STAGED[k].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          STAGE_SMEM_MAX) == cudaSuccess &&
-                     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, STAGED[k].fn, STAGED[k].nt,
-                                                                   STAGE_SMEM_MAX) == cudaSuccess &&
-                     per >= 1;
-        cudaGetLastError();
-    }
-    if (attr_ok[k] != 1) return false;
-    const long per_stage = (long)(STAGED[k].nt / 32) * (256L * W + 32);
-    for (int sx = vectors_in_smem ? 1 : 0; sx >= 0; --sx) {
-        const long vec = 4L * sh.rows * (1 + sx);
-        const long ns = std::min<long>(STAGE_MAX, (STAGE_SMEM_MAX - vec) / per_stage);
-        if (ns >= 2) {
-            nstage = (int)ns;
-            smem_x = sx;
-            smem = (int)(vec + ns * per_stage);
-            return true;
-        }
-    }
-    return false;
-}
-
 bool kr_cgf_persist(cudaStream_t s, const FoldView& F, float2* RP0, float2* RP1, float* xg, double* field,
                     const double* Pj, KScalars* S, double* part, double* part2, unsigned int* bar, int* err,
                     int max_iters, bool reset_err, int form, bool vectors_in_smem) {
-    FoldShape sh = fold_shape(F.n, form, vectors_in_smem);
+    const FoldShape sh = fold_shape(F.n, form, vectors_in_smem);
     if (sh.blocks <= 0) return false;
     XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
     if (reset_err) XCAL_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     FoldView Fv = F;
     int R = sh.rows, sp = sh.smem_p ? 1 : 0, sx = sh.smem_x ? 1 : 0;
-    int nstage = 0, ssx = 0, ssmem = 0;
-    const void* fn = nullptr;
-    std::vector<void*> args;
-    if (sh.form >= FOLD_NFORMS) {
-        if (stage_shape(sh, F.W, vectors_in_smem, nstage, ssx, ssmem)) {
-            fn = STAGED[sh.form - FOLD_NFORMS].fn;
-            args = {&Fv, &RP0, &RP1, &xg, &field, (void*)&Pj, &S, &part, &part2, &bar, &err, &max_iters,
-                    &R, &ssx, &nstage};
-            sh.smem = ssmem;
-        } else {
-            sh = fold_shape(F.n, sh.form - 2, vectors_in_smem);
-            sp = sh.smem_p ? 1 : 0;
-            sx = sh.smem_x ? 1 : 0;
-        }
-    }
-    if (!fn) {
-        fn = FOLD_FORMS[F.W > 0 ? 1 : 0][sh.form].fn;
-        args = {&Fv, &RP0, &RP1, &xg, &field, (void*)&Pj, &S, &part, &part2, &bar, &err, &max_iters,
-                &R, &sp, &sx};
-    }
+    void* args[] = {&Fv, &RP0, &RP1, &xg, &field, (void*)&Pj, &S, &part, &part2, &bar, &err, &max_iters,
+                    &R, &sp, &sx};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(sh.blocks);
     cfg.blockDim = dim3(sh.nt);
@@ -757,7 +429,7 @@ bool kr_cgf_persist(cudaStream_t s, const FoldView& F, float2* RP0, float2* RP1,
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    XCAL_CUDA(cudaLaunchKernelExC(&cfg, fn, args.data()));
+    XCAL_CUDA(cudaLaunchKernelExC(&cfg, FOLD_FORMS[F.W > 0 ? 1 : 0][sh.form].fn, args));
     XCAL_CHECK_LAUNCH();
     return true;
 }

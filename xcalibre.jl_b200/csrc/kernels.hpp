@@ -211,6 +211,28 @@ void kr_dilu_bwd_lv(cudaStream_t s, int k0, int k1, const int* rows, const int* 
 template <class T>
 void kr_gather_vals(cudaStream_t s, long n, const int* src, const T* vals, T* dst);
 // small systems (n <= DILU_BLOCK_MAX_ROWS): whole sweeps in one block
+// the lower triangle in level order, as the DILU factor reads it: per
+// position k its row, the diagonal slot of that row (dslot), and per entry
+// (in the row's own order) the column, the slot of a_ij (src) and of a_ji
+// (tsrc) in the matrix
+struct LevelDView {
+    const int* rows;
+    const int* off;
+    int nlev;
+    const int* slice;
+    const unsigned char* cnt;
+    const int* col;
+    const int* src;
+    const int* tsrc;
+    const int* dslot;
+};
+// the D factor over the level-ordered lower triangle: one block (D staged in
+// shared memory when it fits), or one cooperative launch over the grid with
+// a grid barrier between levels (false: nothing launched); each row's
+// arithmetic that of kr_dilu_D
+void kr_dilu_D_lv_block(cudaStream_t s, int n, const LevelDView& L, const double* nz, double* D);
+bool kr_dilu_D_lv_grid(cudaStream_t s, const LevelDView& L, const double* nz, double* D, unsigned int* bar,
+                       int* err);
 void kr_dilu_D_block(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
                      double* D);
 // one triangle in level order, as the one-block sweep reads it: level l is
@@ -284,8 +306,7 @@ struct FoldMut {
 };
 // kernel forms of the folded CG (block size / software pipelining over rows;
 // cg_folded.cu)
-constexpr int FOLD_NFORMS = 4;   // register-loaded forms 0..3
-constexpr int FOLD_NSTAGED = 2;  // staged forms FOLD_NFORMS.. (slots by bulk copies; uniform layout)
+constexpr int FOLD_NFORMS = 4;
 // most blocks of a folded-CG launch (one per SM); its two partial buffers
 // hold this many doubles each
 constexpr int FOLD_MAX_BLOCKS = 1024;

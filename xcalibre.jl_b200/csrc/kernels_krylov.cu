@@ -239,6 +239,46 @@ __global__ void k_dilu_D(const int* __restrict__ rows, int nrows, CSRView A, con
     dilu_D_row(A, nz, D, rows[t]);
 }
 
+// update_dilu_diagonal! for the row at level position k, reading the
+// level-ordered lower triangle (coalesced over consecutive positions): the
+// same operands, in the same order, as dilu_D_row.  Dr: where earlier
+// levels' D values are read; the row's value goes to D (and Ds when given)
+__device__ __forceinline__ void dilu_D_pos(const LevelDView& L, int k, const double* __restrict__ nz,
+                                           const double* Dr, double* D, double* Ds) {
+    const int i = L.rows[k];
+    const int c = L.cnt[k];
+    const int base = L.slice[k / SELL_C] + (k % SELL_C);
+    int e[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+        if (m < c) e[m] = base + SELL_C * m;
+    double d = nz[L.dslot[k]];
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+        if (m < c) d = d - (nz[ld_stream(L.tsrc + e[m])] * nz[ld_stream(L.src + e[m])]) / Dr[ld_stream(L.col + e[m])];
+    for (int m = 8; m < c; ++m) {
+        const int em = base + SELL_C * m;
+        d = d - (nz[ld_stream(L.tsrc + em)] * nz[ld_stream(L.src + em)]) / Dr[ld_stream(L.col + em)];
+    }
+    D[i] = d;
+    if (Ds) Ds[i] = d;
+}
+
+// the D factor of a small system in one block, level by level over the
+// level-ordered lower triangle; D in shared memory (smem) when it fits,
+// copied out at the end
+__global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_D_lv_block(int n, LevelDView L,
+                                                                        const double* __restrict__ nz, double* D,
+                                                                        int smem) {
+    extern __shared__ __align__(16) unsigned char dilu_smem[];
+    double* Ds = smem ? reinterpret_cast<double*>(dilu_smem) : nullptr;
+    for (int l = 0; l < L.nlev; ++l) {
+        for (int k = L.off[l] + threadIdx.x; k < L.off[l + 1]; k += blockDim.x)
+            dilu_D_pos(L, k, nz, smem ? (const double*)Ds : (const double*)D, D, Ds);
+        __syncthreads();
+    }
+}
+
 // the D factor of a small system in one block, level by level
 __global__ void __launch_bounds__(DILU_BLOCK_THREADS) k_dilu_D_block(const int* __restrict__ rows,
                                                                      const int* __restrict__ off, int nlev,
@@ -305,15 +345,17 @@ __device__ __forceinline__ void lv_apply(const LevelView<T>& L, const LvRow<T, U
 // Every level of one DILU application in one cooperative launch: the
 // forward sweep's levels, then the backward sweep's, each spread over the
 // whole grid (rows of a level are independent), with the bounded grid
-// barrier between consecutive levels.  A thread loads its first row of the
-// next level (indices, slots, right-hand side: nothing the sweep writes)
-// before it enters the barrier, so only the gathers of y wait behind it.
-// Each row's arithmetic is that of the level kernels (dilu_level_s), bit for
-// bit; only the launches go.  A barrier that gives up sets *err and ends
-// every block.
+// barrier between consecutive levels.  FP32: a thread loads its first row
+// of the next level (indices, slots, right-hand side: nothing the sweep
+// writes) before it enters the barrier, so only the gathers of y wait
+// behind it (FP64 rows hold twice the registers; there the level runs as
+// dilu_level_s, which measured faster).  Each row's arithmetic is that of
+// the level kernels (dilu_level_s), bit for bit; only the launches go.  A
+// barrier that gives up sets *err and ends every block.
 constexpr int DILU_GRID_THREADS = 512;
 template <class T>
-__global__ void __launch_bounds__(DILU_GRID_THREADS, 2) k_dilu_grid(LevelView<T> lo, LevelView<T> up,
+__global__ void __launch_bounds__(DILU_GRID_THREADS, sizeof(T) == 4 ? 2 : 1) k_dilu_grid(LevelView<T> lo,
+                                                                                       LevelView<T> up,
                                                                     const T* __restrict__ D,
                                                                     const T* __restrict__ b, T* y,
                                                                     unsigned int* bar, int* err,
@@ -324,6 +366,18 @@ __global__ void __launch_bounds__(DILU_GRID_THREADS, 2) k_dilu_grid(LevelView<T>
     const int start = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     const int total = lo.nlev + up.nlev;
     unsigned int nb = 0;
+    if constexpr (sizeof(T) == 8) {
+        for (int l = 0; l < total; ++l) {
+            if (l < lo.nlev) {
+                dilu_level_s<T, true>(lo, lo.off[l], lo.off[l + 1], D, b, y, start, stride);
+            } else {
+                const int u = l - lo.nlev;
+                dilu_level_s<T, false>(up, up.off[u], up.off[u + 1], D, b, y, start, stride);
+            }
+            if (l + 1 < total && !grid_barrier(bar, gridDim.x, nb, err, &sh_err)) return;
+        }
+        return;
+    }
     LvRow<T, U> r;
     bool have = false;  // r holds this thread's first row of level l
     if (total > 0 && lo.nlev > 0 && lo.off[0] + start < lo.off[1]) {
@@ -373,6 +427,18 @@ __global__ void __launch_bounds__(DILU_GRID_THREADS) k_dilu_D_grid(const int* __
     for (int l = 0; l < nlev; ++l) {
         for (int k = off[l] + start; k < off[l + 1]; k += stride) dilu_D_row(A, nz, D, rows[k]);
         if (l + 1 < nlev && !grid_barrier(bar, gridDim.x, nb, err, &sh_err)) return;
+    }
+}
+
+// the same over the level-ordered lower triangle
+__global__ void __launch_bounds__(DILU_GRID_THREADS) k_dilu_D_lv_grid(LevelDView L, const double* __restrict__ nz,
+                                                                      double* D, unsigned int* bar, int* err) {
+    __shared__ int sh_err;
+    const int start = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    unsigned int nb = 0;
+    for (int l = 0; l < L.nlev; ++l) {
+        for (int k = L.off[l] + start; k < L.off[l + 1]; k += stride) dilu_D_pos(L, k, nz, D, D, nullptr);
+        if (l + 1 < L.nlev && !grid_barrier(bar, gridDim.x, nb, err, &sh_err)) return;
     }
 }
 
@@ -950,6 +1016,50 @@ void kr_gather_vals(cudaStream_t s, long n, const int* src, const T* vals, T* ds
     long blocks = (n + 255) / 256;
     k_gather_vals<T><<<(int)(blocks < 148L * 16 ? blocks : 148L * 16), 256, 0, s>>>(n, src, vals, dst);
     XCAL_CHECK_LAUNCH();
+}
+void kr_dilu_D_lv_block(cudaStream_t s, int n, const LevelDView& L, const double* nz, double* D) {
+    if (L.nlev <= 0) return;
+    static bool attr_set = false;
+    if (!attr_set) {
+        XCAL_CUDA(cudaFuncSetAttribute((const void*)k_dilu_D_lv_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       DILU_SMEM_MAX_BYTES));
+        attr_set = true;
+    }
+    const size_t bytes = (size_t)n * sizeof(double);
+    const int smem = bytes <= (size_t)DILU_SMEM_MAX_BYTES ? 1 : 0;
+    k_dilu_D_lv_block<<<1, DILU_BLOCK_THREADS, smem ? bytes : 0, s>>>(n, L, nz, D, smem);
+    XCAL_CHECK_LAUNCH();
+}
+bool kr_dilu_D_lv_grid(cudaStream_t s, const LevelDView& L, const double* nz, double* D, unsigned int* bar,
+                       int* err) {
+    static int blocks = -1;
+    if (blocks < 0) {
+        int dev = 0, sms = 0, per = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, (const void*)k_dilu_D_lv_grid, DILU_GRID_THREADS,
+                                                          0) == cudaSuccess)
+            blocks = sms * std::min(per, 2);
+        else
+            blocks = 0;
+        cudaGetLastError();
+    }
+    if (blocks <= 0 || L.nlev <= 0) return false;
+    XCAL_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned int), s));
+    LevelDView Lv = L;
+    void* args[] = {&Lv, (void*)&nz, &D, &bar, &err};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(DILU_GRID_THREADS);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    XCAL_CUDA(cudaLaunchKernelExC(&cfg, (const void*)k_dilu_D_lv_grid, args));
+    XCAL_CHECK_LAUNCH();
+    return true;
 }
 void kr_dilu_D_block(cudaStream_t s, const int* rows, const int* off, int nlev, const CSRView& A, const double* nz,
                      double* D) {
