@@ -14,14 +14,14 @@
 // not bit-exactness with it; the FP64 path keeps the canonical kernel.
 //
 // Per iteration the off-diagonal slots (value + column) stream once; the
-// direction and residual are gathered; the block's rows of x, p and q stay
-// in shared memory for the whole solve (x reaches HBM only as the final FP64
-// correction), so HBM sees the matrix, two gathered vectors, and the writes
-// of p and r.
+// residual and the previous direction are gathered as one (r, p) pair per
+// neighbour; the block's rows of x, p and q stay in shared memory for the
+// whole solve (x reaches HBM only as the final FP64 correction), so HBM sees
+// the matrix, the gathered pairs, and the write of each row's next pair.
 //
-// Launch shape: one 1024-thread block per SM (cooperative), each owning a
-// contiguous run of rows -- 148 blocks meet at each grid barrier instead of
-// one per 2048-row tile.  Reductions are deterministic: every thread adds
+// Launch shape: one block of 768 or 1024 threads per SM (cooperative), each
+// owning a contiguous run of rows -- 148 blocks meet at each grid barrier
+// instead of one per 2048-row tile.  Reductions are deterministic: every thread adds
 // its rows in a fixed order (FP64 accumulators), the block adds its warps
 // in a fixed tree, and every block adds the block partials in the same
 // order, so every block takes the same decisions.
@@ -85,30 +85,38 @@ __global__ void k_fold_scale(int n, const int* __restrict__ slice, unsigned char
     len[i] = (unsigned char)(ln | (nz[diag[i]] < 0.0 ? 0x80 : 0));
 }
 
-// every thread's value summed over the block in a fixed order; valid in
-// every thread (sm: 33 doubles)
-__device__ __forceinline__ double fold_block_sum(double v, double* sm) {
+// every thread's value summed over the block in a fixed order, for thread
+// 0 only (one block barrier; sm: 32 doubles, free again after the next
+// block barrier)
+__device__ __forceinline__ double fold_block_partial(double v, double* sm) {
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, off);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    __syncthreads();  // sm may still be read by the previous sum
     if (lane == 0) sm[warp] = v;
     __syncthreads();
+    double w = 0.0;
     if (warp == 0) {
-        double w = lane < nw ? sm[lane] : 0.0;
+        w = lane < nw ? sm[lane] : 0.0;
 #pragma unroll
         for (int off = 16; off >= 1; off >>= 1) w = w + __shfl_xor_sync(0xffffffffu, w, off);
-        if (lane == 0) sm[32] = w;
+    }
+    return w;
+}
+
+// the block partials of one reduction, added in the same order by every
+// block: warp 0 alone (lane l adds partials l, l + 32, ... in turn, then the
+// lanes' sums in a fixed tree), the total handed to the block through sm[32]
+// with one block barrier
+__device__ __forceinline__ double fold_grid_sum(const double* part, int nblocks, double* sm) {
+    if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += 32) v = v + __ldcg(part + b);
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, off);
+        if (threadIdx.x == 0) sm[32] = v;
     }
     __syncthreads();
     return sm[32];
-}
-
-// the block partials of one reduction, added in the same order by every block
-__device__ __forceinline__ double fold_grid_sum(const double* part, int nblocks, double* sm) {
-    double v = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v = v + __ldcg(part + b);
-    return fold_block_sum(v, sm);
 }
 
 // The first U off-diagonal slots of a row (columns and values), loaded
@@ -259,7 +267,7 @@ __global__ void __launch_bounds__(NT, 1)
             acc = acc + (double)pi * (double)qi;
             if constexpr (PIPE) sl = sl_next;
         }
-        double tot = fold_block_sum(acc, sm);
+        const double tot = fold_block_partial(acc, sm);
         if (threadIdx.x == 0) part[blockIdx.x] = tot;
         if (!(ok = grid_barrier(bar, G, nb, err, &sh_err))) break;
         const double pAp = fold_grid_sum(part, G, sm);
@@ -283,7 +291,7 @@ __global__ void __launch_bounds__(NT, 1)
             nxt[i] = make_float2(ri, pi);
             acc2 = acc2 + (double)ri * (double)ri;
         }
-        double tot2 = fold_block_sum(acc2, sm);
+        const double tot2 = fold_block_partial(acc2, sm);
         if (threadIdx.x == 0) part2[blockIdx.x] = tot2;
         if (!(ok = grid_barrier(bar, G, nb, err, &sh_err))) break;
         const double g = fold_grid_sum(part2, G, sm);
