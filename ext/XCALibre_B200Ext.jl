@@ -67,7 +67,8 @@ const GRAD_GAUSS, GRAD_MIDPOINT = Int32(0), Int32(1)
 const LIMITER_NONE, LIMITER_CELL = Int32(0), Int32(1)
 const SOLVER_CG, SOLVER_BICGSTAB = Int32(0), Int32(1)
 const PRECOND_NONE, PRECOND_JACOBI, PRECOND_DILU = Int32(0), Int32(1), Int32(2)
-const TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST = Int32(0), Int32(1), Int32(2), Int32(3)
+const TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST, TURB_KEQUATION =
+    Int32(0), Int32(1), Int32(2), Int32(3), Int32(4)
 const PREC_FP64, PREC_MIXED = Int32(0), Int32(1)
 const ALGO_SIMPLE, ALGO_PISO = Int32(0), Int32(1)
 
@@ -186,6 +187,8 @@ struct ConfigDesc
     y_solver::SolverSetupDesc
     n_bc_y::Int32
     bc_y::Ptr{BCDesc}
+    keq_ck::Float64
+    keq_ce::Float64
 end
 
 # xcal_term / xcal_source: one operator / source of an equation built with
@@ -405,6 +408,7 @@ function config_desc(model, config; pref=nothing, inner_loops=0, ncorrectors=0, 
     tname = nameof(typeof(turb))
     tk = tname == :Laminar ? TURB_LAMINAR : tname == :Smagorinsky ? TURB_SMAGORINSKY :
          tname == :KOmega ? TURB_KOMEGA : tname == :KOmegaSST ? TURB_KOMEGA_SST :
+         tname == :KEquation ? TURB_KEQUATION :
          error("libxcal_b200: turbulence model $(tname) is not on the B200 path")
     time = 0.0
     keep = Any[]
@@ -438,7 +442,8 @@ function config_desc(model, config; pref=nothing, inner_loops=0, ncorrectors=0, 
         Int32(length(bk)), Int32(length(bw)), ptr(bk), ptr(bw),
         gs(:β2), gs(:σk2), gs(:σω2),
         schemes_desc(getopt(schemes, :y)), solver_desc(getopt(solvers, :y)),
-        Int32(length(by)), ptr(by))
+        Int32(length(by)), ptr(by),
+        tk == TURB_KEQUATION ? Float64(turb.coeffs.ck) : 0.0, tk == TURB_KEQUATION ? Float64(turb.coeffs.ce) : 0.0)
     return desc, keep
 end
 

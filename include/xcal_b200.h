@@ -69,7 +69,13 @@ enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
 /* preconditioner: src/Solve/Preconditioners/preconditioners_0_types.jl */
 enum { XCAL_PRECOND_NONE = 0, XCAL_PRECOND_JACOBI = 1, XCAL_PRECOND_DILU = 2 };
 /* turbulence: RANS{Laminar} / LES{Smagorinsky} / RANS{KOmega} */
-enum { XCAL_TURB_LAMINAR = 0, XCAL_TURB_SMAGORINSKY = 1, XCAL_TURB_KOMEGA = 2, XCAL_TURB_KOMEGA_SST = 3 };
+enum {
+    XCAL_TURB_LAMINAR = 0,
+    XCAL_TURB_SMAGORINSKY = 1,
+    XCAL_TURB_KOMEGA = 2,
+    XCAL_TURB_KOMEGA_SST = 3,
+    XCAL_TURB_KEQUATION = 4  /* LES{KEquation} (LES_KEquation.jl) */
+};
 /* arithmetic of the Krylov inner iterations */
 enum { XCAL_PREC_FP64 = 0, XCAL_PREC_MIXED = 1 };
 /* pressure-velocity algorithm: run! dispatch, src/Solvers/Solvers_3_solver_dispatch.jl:120,225 */
@@ -96,11 +102,16 @@ enum {
     XCAL_FIELD_UF = 11,    /* Uf (3 x n_faces)                              */
     XCAL_FIELD_PF = 12,    /* pf (n_faces)                                  */
     XCAL_FIELD_RDF = 13,   /* rDf (n_faces)                                 */
-    XCAL_FIELD_DELTA = 14, /* LES filter (C*Delta)^2 (n_cells)              */
-    XCAL_FIELD_K = 15,     /* RANS{KOmega} k (n_cells)                      */
+    XCAL_FIELD_DELTA = 14, /* LES filter: (C*Delta)^2 (Smagorinsky), Delta
+                              (KEquation) (n_cells)                     */
+    XCAL_FIELD_K = 15,     /* k: RANS{KOmega}, LES{KEquation} (n_cells)     */
     XCAL_FIELD_OMEGA = 16, /* RANS{KOmega} omega (n_cells)                  */
     XCAL_FIELD_WALLDIST = 17, /* RANS{KOmegaSST} wall distance y (n_cells)  */
-    XCAL_FIELD_COUNT = 18
+    XCAL_FIELD_PK = 18,    /* the k equation's Source (n_cells)             */
+    XCAL_FIELD_DK = 19,    /* the k equation's Si coefficient (n_cells)     */
+    XCAL_FIELD_DW = 20,    /* omega's Si coefficient (k-omega), the k
+                              equation's second Si coefficient (KEquation) */
+    XCAL_FIELD_COUNT = 21
 };
 
 /* ---- mesh: the Mesh3 contract (src/Mesh/Mesh_0_types.jl:28-205) ---------
@@ -242,6 +253,12 @@ typedef struct {
     xcal_solver_setup y_solver;
     int32_t n_bc_y;
     const xcal_bc* bc_y;
+    /* LES{KEquation}(; ck, ce) (LES_KEquation.jl:35-39): the subgrid k
+     * equation Time + Div(mdotf) - Lap(nu + nut_f) + Si(ce sqrt(k) / Delta)
+     * + Si(2/3 tr grad U) == Source(2 nut grad U : dev(S)), solved with
+     * k_schemes / k_solver / bc_k, then nut = ck Delta sqrt(k) with Delta =
+     * (V / les_delta_distance)^les_delta_power (:80-186) */
+    double keq_ck, keq_ce;
 } xcal_config;
 
 /* ---- polyMesh input of the mesh importer --------------------------------
@@ -482,7 +499,7 @@ int32_t xcal_equation_destroy(xcal_equation* eq);
 int32_t xcal_equation_discretise(xcal_equation* eq, const double* prev, double dt);
 /* apply_boundary_conditions!(eqn, BCs) (Discretise_5_apply_bcs.jl) for a
  * scalar field: every term's boundary functor per boundary face
- * (boundary_conditions/*.jl); phi [n_cells] = the field's current values
+ * (the boundary_conditions sources); phi [n_cells] = the field's current values
  * (Extrapolated reads them; NULL when no boundary needs them) */
 int32_t xcal_equation_apply_bcs(xcal_equation* eq, const double* phi);
 int32_t xcal_equation_nnz(const xcal_equation* eq, int64_t* nnz);
@@ -567,7 +584,9 @@ int32_t xcal_case_set_graph_mode(xcal_case* cs, int32_t enable);
  * thread-block cluster (hardware cluster barriers), a larger one in the
  * widest cooperative block form whose blocks are co-resident (1024, 512 or
  * 256 threads); 2 = the cluster form only, 256 / 512 / 1024 = that
- * cooperative form only (each falls back to the two-kernel loop when it
+ * cooperative form only, 4 / 5 = one block of 1024 / 512 threads per SM,
+ * each owning every 148th tile (its q in shared memory: up to 12 FP64 / 25
+ * FP32 tiles per block) (each falls back to the two-kernel loop when it
  * does not fit). */
 int32_t xcal_case_set_persistent(xcal_case* cs, int32_t mode);
 /* Krylov report of the last solve of each system (Ux, Uy, Uz, p, k, omega,

@@ -97,6 +97,9 @@ static std::vector<double>* field_ptr(Case* C, int field, int& ncomp, int& per) 
         case XCAL_FIELD_K: return &C->k;
         case XCAL_FIELD_OMEGA: return &C->omega;
         case XCAL_FIELD_WALLDIST: return &C->yw;
+        case XCAL_FIELD_PK: return &C->Pk;
+        case XCAL_FIELD_DK: return &C->Dk;
+        case XCAL_FIELD_DW: return &C->Dw;
         default: return nullptr;
     }
 }

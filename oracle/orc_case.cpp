@@ -117,6 +117,7 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
         copy_bcs(*m, cfg->bc_k, cfg->n_bc_k, C->bcK, 1);
         copy_bcs(*m, cfg->bc_omega, cfg->n_bc_omega, C->bcOmega, 1);
     }
+    if (cfg->turbulence == XCAL_TURB_KEQUATION) copy_bcs(*m, cfg->bc_k, cfg->n_bc_k, C->bcK, 1);
     if (cfg->turbulence == XCAL_TURB_KOMEGA_SST) copy_bcs(*m, cfg->bc_y, cfg->n_bc_y, C->bcY, 1);
     C->cfg.bc_k = C->cfg.bc_omega = C->cfg.bc_y = nullptr;
     int nC = C->nC, nF = C->nF;
@@ -161,8 +162,10 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     C->AU0 = C->AU;
     C->PU.assign(nC, 0.0);
     C->Pp.assign(nC, 0.0);
-    // LES{Smagorinsky} initialise (LES_Smagorinsky.jl:84-101, LES_functions.jl:1-55)
-    if (cfg->turbulence == XCAL_TURB_SMAGORINSKY) {
+    // LES{Smagorinsky} initialise (LES_Smagorinsky.jl:84-101, LES_functions.jl:1-55);
+    // LES{KEquation} initialise (LES_KEquation.jl:85-94): delta! alone
+    const bool keq = cfg->turbulence == XCAL_TURB_KEQUATION;
+    if (cfg->turbulence == XCAL_TURB_SMAGORINSKY || keq) {
         double distance = 1.0, power = 1.0 / 3.0;
         if (cfg->les_delta_power > 0.0) {  // delta_scaling evaluated by the caller
             distance = cfg->les_delta_distance;
@@ -191,7 +194,7 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
         for (int i = 0; i < nC; ++i) {
             double d = std::pow(m->cvol[i] / distance, power);
             double dc = d * cfg->smagorinsky_C;
-            C->Delta[i] = dc * dc;
+            C->Delta[i] = keq ? d : dc * dc;
         }
     }
     if (cfg->turbulence == XCAL_TURB_KOMEGA_SST) wall_distance(*C);
@@ -1487,6 +1490,55 @@ static void komega(Case& C) {
     nutwall_correct(C);
 }
 
+// turbulence!(::KEquationModel) after grad!(gradU) and its limiter
+// (LES_KEquation.jl:134-186), rho = 1: mueffk = nu + nut_f; per cell
+// Pk = 2 nut (grad U . dev(S)) (the Frobenius product over the column-major
+// entries, S = (G + G')/2, dev(S) = S - tr(S)/3 I), Dkf = ce sqrt(k) / Delta,
+// divU = 2/3 tr(grad U); the k equation Time + Div(mdotf) - Lap(mueffk) +
+// Si(Dkf) + Si(divU) == Source(Pk), its BCs, implicit relaxation, solve,
+// bound!; nut = ck Delta sqrt(k), interpolated with its BCs and the wall
+// functions (correct_eddy_viscosity!)
+static void kequation(Case& C) {
+    const Mesh& m = *C.m;
+    const xcal_config& cf = C.cfg;
+    for (int i = 0; i < C.nC; ++i) {
+        double G[3][3], S[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) G[a][b] = C.gradU[3 * a + b][i];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) S[a][b] = 0.5 * (G[a][b] + G[b][a]);
+        const double third = (1.0 / 3.0) * ((S[0][0] + S[1][1]) + S[2][2]);
+        double dot = 0.0;
+        bool first = true;
+        for (int b = 0; b < 3; ++b)
+            for (int a = 0; a < 3; ++a) {
+                const double pr = G[a][b] * (a == b ? S[a][b] - third : S[a][b]);
+                dot = first ? pr : dot + pr;
+                first = false;
+            }
+        C.Pk[i] = (2.0 * C.nut[i]) * dot;
+        C.Dk[i] = (cf.keq_ce * std::sqrt(C.k[i])) / C.Delta[i];
+        C.Dw[i] = (2.0 / 3.0) * ((G[0][0] + G[1][1]) + G[2][2]);
+    }
+    for (int f = 0; f < C.nF; ++f) C.mueffk[f] = cf.nu + C.nutf[f];
+    const int ptype = cf.k_solver.precond;
+    std::vector<Term> tk = {{T_TIME, 1.0, nullptr, cf.k_schemes.time},
+                            {T_DIV, 1.0, &C.mdotf, cf.k_schemes.divergence},
+                            {T_LAP, -1.0, &C.mueffk, 0},
+                            {T_SI, 1.0, &C.Dk, 0},
+                            {T_SI, 1.0, &C.Dw, 0}};
+    discretise_scalar(C, tk, C.Ap, C.bp, C.k, C.Pk);
+    apply_bcs_scalar(C, tk, C.Ap, C.bp, C.bcK, C.k);
+    relax_scalar(C.Ap, C.bp, C.k, cf.k_solver.relax);
+    update_precond(C.Ap, ptype, C.Pkw);
+    C.res_k = solve_scalar(C, cf.k_solver, ptype, C.k, C.Pkw);
+    bound_field(m, C.k);
+    for (int i = 0; i < C.nC; ++i) C.nut[i] = (cf.keq_ck * C.Delta[i]) * std::sqrt(C.k[i]);
+    interpolate(m, C.nut, C.nutf);
+    correct_boundaries(C, C.bcNut, &C.nutf, &C.nut, false);
+    nutwall_correct(C);
+}
+
 // grad! of a scalar with its BCs, Gauss or Midpoint (Calculate_0_gradient.jl)
 static void scalar_grad(Case& C, const std::vector<double>& phi, std::vector<double>& phif, const std::vector<BC>& bcs,
                         int scheme, std::vector<double>* g) {
@@ -1615,6 +1667,7 @@ void turbulence(Case& C) {
     grad_U(C);  // RANS_laminar.jl:73-79, LES_Smagorinsky.jl:117, RANS_kOmega.jl:167-168
     if (C.cfg.turbulence == XCAL_TURB_KOMEGA_SST) komega_sst(C);
     if (C.cfg.turbulence == XCAL_TURB_KOMEGA) komega(C);
+    if (C.cfg.turbulence == XCAL_TURB_KEQUATION) kequation(C);
     if (C.cfg.turbulence == XCAL_TURB_SMAGORINSKY) {
         // LES_Smagorinsky.jl:122-131
         for (int i = 0; i < C.nC; ++i) {

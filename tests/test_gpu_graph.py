@@ -102,11 +102,12 @@ def test_autotuner_choices(x, ctx):
 def test_persistent_cg_identical(x, ctx, prec):
     """The pressure CG as one launch (q on chip) gives the two-kernel loop's
     results bit for bit, in each form: the automatic choice, the cluster form
-    (14 tiles: one 16-block cluster, hardware barriers) and the 1024-, 512-
-    and 256-thread cooperative forms forced."""
+    (14 tiles: one 16-block cluster, hardware barriers), the 1024-, 512-
+    and 256-thread cooperative forms forced, and the one-block-per-SM forms
+    (here one tile per block)."""
     mesh = x.build_mesh3(x.channel_polymesh(48, 24, 24, seed=6))
     out = []
-    modes = (False, True, 2, 1024, 512, 256)
+    modes = (False, True, 2, 1024, 512, 256, 4, 5)
     for persist in modes:
         model, config = x.cases.channel_case(mesh, iterations=4, precision=prec)
         cfg, keep = x.build_config(model, config)
@@ -125,3 +126,33 @@ def test_persistent_cg_identical(x, ctx, prec):
         assert o[3] > 0, m
         assert np.array_equal(out[0][0], o[0]), m
         assert np.array_equal(out[0][1], o[1]) and np.array_equal(out[0][2], o[2]), m
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_persistent_multi_tile_identical(x, ctx, prec):
+    """One block per SM owning several tiles (160 tiles over at most 148
+    blocks: some blocks run two) gives the two-kernel loop's results bit for
+    bit, with 1024 and with 512 threads per block."""
+    mesh = x.build_mesh3(x.channel_polymesh(80, 64, 64, seed=9))
+    assert mesh.n_cells > 148 * 2048
+    out = []
+    for persist in (False, 4, 5):
+        model, config = x.cases.channel_case(mesh, iterations=2, precision=prec)
+        cfg, keep = x.build_config(model, config)
+        dm = x.DeviceMesh(ctx, mesh)
+        c = x.Case(dm, cfg)
+        c.set_persistent(persist)
+        c.set_inner_cg(1)
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+        c.set_profiling(True)
+        res, _ = c.simple_iterate(2)
+        ms, its = c.profile(5)
+        out.append((res, c.get_field(x._abi.FIELD_U), c.get_field(x._abi.FIELD_P), its))
+        c.close()
+        dm.close()
+    assert out[0][3] == 0
+    for o in out[1:]:
+        assert o[3] > 0
+        assert np.array_equal(out[0][0], o[0])
+        assert np.array_equal(out[0][1], o[1]) and np.array_equal(out[0][2], o[2])

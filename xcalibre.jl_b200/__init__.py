@@ -12,7 +12,7 @@ from .api import (B200Backend, Bicgstab, Case, CellBased, Cg, Configuration, Con
                   Smagorinsky, SolverSetup, Steady, SteadyState, Symmetry, Transient, Upwind, Wall, Zerogradient,
                   assign, build_config, construct_periodic, initialise_, launch_count, run_, Batch,
                   footprint_estimate, VTK, OpenFOAM, save_checkpoint, load_checkpoint, boundary_average, JacobiSmoother,
-                  KOmega, KOmegaSST, OmegaWallFunction, KWallFunction, NutWallFunction)
+                  KOmega, KOmegaSST, OmegaWallFunction, KWallFunction, NutWallFunction, KEquation)
 from . import dsl
 from .dsl import Divergence, Equation, Laplacian, ScalarEquation, Si, Source, Time
 from .foam import Mesh3, build_mesh3

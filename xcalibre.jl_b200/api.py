@@ -104,6 +104,11 @@ class Laminar: ...
 class Smagorinsky: ...
 
 
+class KEquation:
+    """LES{KEquation} (LES_KEquation.jl): a subgrid kinetic energy
+    equation; nut = ck Delta sqrt(k)."""
+
+
 class KOmega:
     """RANS{KOmega} (RANS_kOmega.jl): k and omega transport equations,
     nut = k / omega."""
@@ -260,8 +265,12 @@ class RANS:
 
 @dataclass
 class LES:
+    """LES{Smagorinsky}(; C) (LES_Smagorinsky.jl) or LES{KEquation}(; ck,
+    ce) (LES_KEquation.jl:35-39)."""
     model: type = Smagorinsky
     C: float = 0.15
+    ck: float = 0.094
+    ce: float = 1.048
 
 
 @dataclass
@@ -291,6 +300,8 @@ class Physics:
             if isinstance(turbulence, RANS) and turbulence.model in (KOmega, KOmegaSST):
                 turbulence.k = np.zeros(n)
                 turbulence.omega = np.zeros(n)
+            if isinstance(turbulence, LES) and turbulence.model is KEquation:
+                turbulence.k = np.zeros(n)
             if isinstance(turbulence, RANS) and turbulence.model is KOmegaSST:
                 turbulence.y = np.zeros(n)
 
@@ -613,6 +624,7 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     transient = isinstance(model.time, Transient)
     turb = model.turbulence
     les = isinstance(turb, LES)
+    keq = les and turb.model is KEquation
     sst = isinstance(turb, RANS) and turb.model is KOmegaSST
     kw = isinstance(turb, RANS) and turb.model in (KOmega, KOmegaSST)
     bnd = config.boundaries
@@ -620,7 +632,7 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     bP = _bc_array(mesh, bnd["p"], 1, keep)
     nut_bcs = bnd.get("nut", []) if (les or kw) else []
     bN = _bc_array(mesh, nut_bcs, 1, keep)
-    k_bcs = bnd.get("k", []) if kw else []
+    k_bcs = bnd.get("k", []) if (kw or keq) else []
     w_bcs = bnd.get("omega", []) if kw else []
     bK = _bc_array(mesh, k_bcs, 1, keep)
     bW = _bc_array(mesh, w_bcs, 1, keep)
@@ -641,9 +653,9 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     sY = config.schemes.get("y", Schemes()) if sst else Schemes()
     slv_y = _solver_desc(config.solvers["y"]) if sst else _abi.SolverSetupDesc()
     co = turb.coeffs() if kw else {}
-    sK = config.schemes.get("k", Schemes()) if kw else Schemes()
+    sK = config.schemes.get("k", Schemes()) if (kw or keq) else Schemes()
     sW = config.schemes.get("omega", Schemes()) if kw else Schemes()
-    slv_k = _solver_desc(config.solvers["k"]) if kw else _abi.SolverSetupDesc()
+    slv_k = _solver_desc(config.solvers["k"]) if (kw or keq) else _abi.SolverSetupDesc()
     slv_w = _solver_desc(config.solvers["omega"]) if kw else _abi.SolverSetupDesc()
     sU, sP = config.schemes["U"], config.schemes["p"]
     backend = config.hardware.backend
@@ -654,9 +666,9 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     dist, power = delta_scaling(mesh, next(iter(bnd.values()))) if les else (1.0, 1.0 / 3.0)
     cfg = _abi.ConfigDesc(
         algorithm=_abi.ALGO_PISO if transient else _abi.ALGO_SIMPLE,
-        turbulence=(_abi.TURB_SMAGORINSKY if les else _abi.TURB_KOMEGA_SST if sst else _abi.TURB_KOMEGA if kw
-                    else _abi.TURB_LAMINAR),
-        nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if les else 0.0,
+        turbulence=(_abi.TURB_KEQUATION if keq else _abi.TURB_SMAGORINSKY if les else _abi.TURB_KOMEGA_SST if sst
+                    else _abi.TURB_KOMEGA if kw else _abi.TURB_LAMINAR),
+        nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if (les and not keq) else 0.0,
         les_delta_distance=dist, les_delta_power=power,
         U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)],
                                    gradient=_SCHEME_GRAD[_kind(sU.gradient)], limiter=_limiter(sU.limiter)[0],
@@ -684,7 +696,8 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
         omega_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sW.time)],
                                        divergence=_SCHEME_DIV[_kind(sW.divergence)]),
         k_solver=slv_k, omega_solver=slv_w, n_bc_k=len(k_bcs), n_bc_omega=len(w_bcs),
-        bc_k=C.cast(bK, C.POINTER(_abi.BCDesc)), bc_omega=C.cast(bW, C.POINTER(_abi.BCDesc)))
+        bc_k=C.cast(bK, C.POINTER(_abi.BCDesc)), bc_omega=C.cast(bW, C.POINTER(_abi.BCDesc)),
+        keq_ck=float(turb.ck) if keq else 0.0, keq_ce=float(turb.ce) if keq else 0.0)
     return cfg, keep
 
 
@@ -695,6 +708,7 @@ class Case:
         self.dmesh, self.ctx = dmesh, dmesh.ctx
         self.mesh = dmesh.mesh
         self.komega = cfg.turbulence in (_abi.TURB_KOMEGA, _abi.TURB_KOMEGA_SST)
+        self.kequation = cfg.turbulence == _abi.TURB_KEQUATION
         h = C.c_void_p()
         check(lib().xcal_case_create(self.ctx.h, dmesh.h, C.byref(cfg), C.byref(h)), self.ctx.h)
         self.h = h
@@ -880,21 +894,22 @@ class Case:
         face mass flux, face velocity and pressure, nu_eff, gradients, rD,
         H...): with ``restore`` a new case on the same mesh and configuration
         continues exactly as this one would."""
-        names = CHECKPOINT_FIELDS + (KOMEGA_FIELDS if self.komega else ())
+        names = CHECKPOINT_FIELDS + (KOMEGA_FIELDS if self.komega else ("FIELD_K",) if self.kequation else ())
         return {name: self.get_field(getattr(_abi, name)).copy() for name in names}
 
     def restore(self, state: dict) -> None:
         """Set the fields of a ``checkpoint`` and mark the state complete, so
         the next iteration does not redo the run's initial calculations."""
-        for name in CHECKPOINT_FIELDS + (KOMEGA_FIELDS if self.komega else ()):
+        for name in CHECKPOINT_FIELDS + (KOMEGA_FIELDS if self.komega else ("FIELD_K",) if self.kequation else ()):
             if name in state:
                 self.set_field(getattr(_abi, name), state[name])
         self._chk(lib().xcal_case_mark_initialised(self.h))
 
     def set_persistent(self, on=True):
         """Persistent CG (one launch per solve): False / True, or 2 (the
-        cluster form only) or 256 / 512 / 1024 (that cooperative block form
-        only)."""
+        cluster form only), 256 / 512 / 1024 (that cooperative block form
+        only), 4 / 5 (one block of 1024 / 512 threads per SM owning every
+        G-th tile).  Same results in every form."""
         mode = int(on) if isinstance(on, bool) else int(on)
         self._chk(lib().xcal_case_set_persistent(self.h, mode))
 
@@ -1108,12 +1123,19 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
     writer = aw = None
     if wi > 0 or (wi == 0 and not transient):
         import os
-        from .writers import AsyncWriter, FOAMWriter, VTKWriter3D
+        from .writers import AsyncWriter, FOAMWriter, VTKWriter2D, VTKWriter3D
         pm = model.domain.polymesh
-        if pm is None:
-            raise ValueError("writing results needs the mesh's polyMesh (build it with build_mesh3 / FOAM3D_mesh)")
         out_dir = output_dir or os.getcwd()
-        writer = (FOAMWriter(pm, out_dir, config.boundaries) if isinstance(output, OpenFOAM) else VTKWriter3D(pm))
+        if pm is None and getattr(model.domain, "cell_nodes", None) is not None:
+            if isinstance(output, OpenFOAM):  # initialise_writer(::OpenFOAM, mesh) takes a Mesh3 only
+                raise ValueError("OpenFOAM output needs a 3D mesh; this 2D mesh writes VTK")
+            writer = VTKWriter2D(model.domain.points, model.domain.cell_nodes)
+        elif pm is None:
+            raise ValueError("writing results needs the mesh's nodes and faces (a mesh from build_mesh3, "
+                             "FOAM3D_mesh, UNV3D_mesh or UNV2D_mesh)")
+        else:
+            writer = (FOAMWriter(pm, out_dir, config.boundaries) if isinstance(output, OpenFOAM)
+                      else VTKWriter3D(pm))
         aw = AsyncWriter()
 
     def write(k):
@@ -1122,7 +1144,8 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
             tdir = ("%.8f" % (k * config.runtime.time_step)) if transient else "%d" % k
             aw.submit(writer.write, tdir, fields)
         else:
-            name = ("time_%d.vtu" if transient else "iteration_%d.vtu") % k
+            ext = "vtk" if isinstance(writer, VTKWriter2D) else "vtu"
+            name = ("time_%d." if transient else "iteration_%d.") % k + ext
             aw.submit(writer.write, os.path.join(out_dir, name), fields)
 
     try:
@@ -1130,7 +1153,8 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
         case.set_field(_abi.FIELD_P, model.momentum.p)
         if hasattr(model.turbulence, "k"):
             case.set_field(_abi.FIELD_K, model.turbulence.k)
-            case.set_field(_abi.FIELD_OMEGA, model.turbulence.omega)
+            if hasattr(model.turbulence, "omega"):
+                case.set_field(_abi.FIELD_OMEGA, model.turbulence.omega)
             case.set_field(_abi.FIELD_NUT, model.turbulence.nut)
         n = config.runtime.iterations
         step = wi if wi > 0 else n
@@ -1165,7 +1189,8 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
             model.nut[:] = case.get_field(_abi.FIELD_NUT)
         if hasattr(model.turbulence, "k"):
             model.turbulence.k[:] = case.get_field(_abi.FIELD_K)
-            model.turbulence.omega[:] = case.get_field(_abi.FIELD_OMEGA)
+            if hasattr(model.turbulence, "omega"):
+                model.turbulence.omega[:] = case.get_field(_abi.FIELD_OMEGA)
     finally:
         if aw is not None:
             aw.close()

@@ -70,6 +70,39 @@ def channel_case(mesh: Mesh3, iterations: int = 500, precision: str = "fp64", de
     return model, config
 
 
+
+def kequation_channel_case(mesh: Mesh3, steps: int = 20, precision: str = "fp64", device: int = 0,
+                           nu: float = 1e-4, dt: float = 2e-3, k_in: float = 1e-3, ck: float = 0.094,
+                           ce: float = 1.048, seed: int = 0):
+    """LES{KEquation} on the channel (PISO, Euler, Linear divergence): the
+    parabolic inlet with inflow k = k_in, walls with k = 0 and nut = 0, a
+    seeded disturbance of U (5% of the inlet peak) and k = k_in inside."""
+    model = A.Physics(time=A.Transient(), fluid=A.Fluid(A.Incompressible, nu=nu),
+                      turbulence=A.LES(A.KEquation, ck=ck, ce=ce), energy=A.Energy(A.Isothermal), domain=mesh)
+    BCs = A.assign(
+        region=mesh,
+        U=[A.DirichletFunction("inlet", parabolic_inlet), A.Zerogradient("outlet"), A.Wall("walls", [0.0, 0.0, 0.0])],
+        p=[A.Zerogradient("inlet"), A.Dirichlet("outlet", 0.0), A.Wall("walls")],
+        k=[A.Dirichlet("inlet", k_in), A.Zerogradient("outlet"), A.Dirichlet("walls", 0.0)],
+        nut=[A.Zerogradient("inlet"), A.Zerogradient("outlet"), A.Dirichlet("walls", 0.0)],
+    )
+    lin = A.Schemes(time=A.Euler, divergence=A.Linear)
+    s = _solvers(relax_U=1.0, relax_p=1.0, rtol_U=0.1, rtol_p=0.01)
+    s["k"] = A.SolverSetup(solver=A.Bicgstab(), preconditioner=A.Jacobi(), convergence=1e-7, relax=1.0, rtol=1e-3)
+    config = A.Configuration(solvers=s, schemes={"U": lin, "p": A.Schemes(), "k": lin},
+                             runtime=A.Runtime(iterations=steps, write_interval=-1, time_step=dt),
+                             hardware=A.Hardware(backend=A.B200Backend(device=device, precision=precision)),
+                             boundaries=BCs)
+    rng = np.random.default_rng(seed)
+    U = np.zeros((3, mesh.n_cells))
+    U[0] = 1.0
+    U += 0.05 * rng.standard_normal(U.shape)
+    model.momentum.U[:] = U
+    A.initialise_(model.momentum.p, 0.0)
+    A.initialise_(model.turbulence.k, k_in)
+    A.initialise_(model.turbulence.nut, 0.0)
+    return model, config
+
 def taylor_green(mesh: Mesh3, rms: float = 1.0) -> np.ndarray:
     """Divergence-free periodic field on [0, 2pi]^3 (deterministic)."""
     x, y, z = mesh.cell_centre[:, 0], mesh.cell_centre[:, 1], mesh.cell_centre[:, 2]

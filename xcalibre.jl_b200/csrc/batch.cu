@@ -201,7 +201,7 @@ struct Batch {
 
     void check_compatible(const Case* c) const {
         if (c->cfg.algorithm != XCAL_ALGO_SIMPLE) fail(XCAL_ERR_UNSUPPORTED, "batch: steady SIMPLE cases only");
-        if (c->rans_kw()) fail(XCAL_ERR_UNSUPPORTED, "batch: k-omega cases run alone");
+        if (c->has_k()) fail(XCAL_ERR_UNSUPPORTED, "batch: k-omega and k-equation LES cases run alone");
         if (cases.empty()) return;
         const xcal_config& a = cases[0]->cfg;
         const xcal_config& b = c->cfg;

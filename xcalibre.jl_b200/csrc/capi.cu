@@ -100,7 +100,8 @@ int32_t xcal_abi_layout(int32_t which, int64_t* out, int32_t cap) {
                  XCAL_OFF(T, omega_schemes), XCAL_OFF(T, k_solver), XCAL_OFF(T, omega_solver), XCAL_OFF(T, n_bc_k),
                  XCAL_OFF(T, n_bc_omega), XCAL_OFF(T, bc_k), XCAL_OFF(T, bc_omega), XCAL_OFF(T, sst_beta2),
                  XCAL_OFF(T, sst_sigma_k2), XCAL_OFF(T, sst_sigma_omega2), XCAL_OFF(T, y_schemes),
-                 XCAL_OFF(T, y_solver), XCAL_OFF(T, n_bc_y), XCAL_OFF(T, bc_y)};
+                 XCAL_OFF(T, y_solver), XCAL_OFF(T, n_bc_y), XCAL_OFF(T, bc_y),
+                 XCAL_OFF(T, keq_ck), XCAL_OFF(T, keq_ce)};
             break;
         }
         case XCAL_LAYOUT_POLYMESH_DESC: {
@@ -438,7 +439,9 @@ int32_t xcal_case_mark_initialised(xcal_case* cs) {
 
 int32_t xcal_case_set_persistent(xcal_case* cs, int32_t mode) {
     if (!cs) return XCAL_ERR_INVALID;
-    if (mode != 0 && mode != 1 && mode != 2 && mode != 256 && mode != 512 && mode != 1024) return XCAL_ERR_INVALID;
+    if (mode != 0 && mode != 1 && mode != 2 && mode != PERSIST_MT1024 && mode != PERSIST_MT512 && mode != 256 &&
+        mode != 512 && mode != 1024)
+        return XCAL_ERR_INVALID;
     cs->c->persistent_cg = mode;
     return XCAL_OK;
 }

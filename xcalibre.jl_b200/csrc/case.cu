@@ -724,7 +724,17 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     for (const xcal_bc& bc : bcNut.src)
         if (bc.type == XCAL_BC_OMEGA_WALL || bc.type == XCAL_BC_K_WALL)
             fail(XCAL_ERR_INVALID, "OmegaWallFunction / KWallFunction do not apply to nut");
-    if (rans_kw()) {
+    if (keq()) {
+        // LES{KEquation}: the subgrid k equation shares the p system
+        build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, nullptr, stream);
+        if (bcK.has_periodic || bcP.has_periodic || bcNut.has_periodic || bcU.has_periodic)
+            fail(XCAL_ERR_UNSUPPORTED, "LES{KEquation}: periodic boundaries are not implemented");
+        for (DBuf<double>* b : {&kfld, &Pk, &Dk, &Dw, &kwtmp}) {
+            b->alloc(m->nC);
+            b->zero(stream);
+        }
+        build_wall_table(*m);
+    } else if (rans_kw()) {
         // RANS{KOmega} / RANS{KOmegaSST}: k / omega share the p system
         build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, nullptr, stream);
         build_bc_table(bcOmega, *m, cfg.bc_omega, cfg.n_bc_omega, 1, nullptr, stream);
@@ -845,8 +855,9 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     // Courant cell size: V^(1/3) (Mesh3), sqrt(V) (Mesh2, Solvers_0_functions.jl:277-285)
     for (int i = 0; i < nC; ++i) h[i] = m->dim == 2 ? std::sqrt(m->vol[i]) : std::pow(m->vol[i], 1.0 / 3.0);
     XCAL_CUDA(cudaMemcpyAsync(dx13.p, h.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream));
-    if (cfg.turbulence == XCAL_TURB_SMAGORINSKY) {
-        // LES_Smagorinsky.jl:84-101 + LES_functions.jl:1-55 (delta! with delta_scaling)
+    if (cfg.turbulence == XCAL_TURB_SMAGORINSKY || keq()) {
+        // LES_Smagorinsky.jl:84-101 + LES_functions.jl:1-55 (delta! with
+        // delta_scaling); Smagorinsky keeps (C Delta)^2, KEquation Delta
         double distance = 1.0, power = 1.0 / 3.0;
         if (cfg.les_delta_power > 0.0) {
             distance = cfg.les_delta_distance;
@@ -873,7 +884,7 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         for (int i = 0; i < nC; ++i) {
             double dd = std::pow(m->vol[i] / distance, power);
             double dc = dd * cfg.smagorinsky_C;
-            h[i] = dc * dc;
+            h[i] = keq() ? dd : dc * dc;
         }
         XCAL_CUDA(cudaMemcpyAsync(Delta.p, h.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream));
     }
@@ -961,11 +972,18 @@ double* Case::field_comp(int field, int comp, long& count) {
         case XCAL_FIELD_DELTA: return Delta.p;
         case XCAL_FIELD_K:
         case XCAL_FIELD_OMEGA:
-            if (!rans_kw()) fail(XCAL_ERR_INVALID, "k / omega fields need RANS{KOmega} or RANS{KOmegaSST}");
+            if (field == XCAL_FIELD_K && keq()) return kfld.p;
+            if (!rans_kw())
+                fail(XCAL_ERR_INVALID, "k / omega fields need RANS{KOmega}, RANS{KOmegaSST} or (k) LES{KEquation}");
             return field == XCAL_FIELD_K ? kfld.p : omega.p;
         case XCAL_FIELD_WALLDIST:
             if (!sst()) fail(XCAL_ERR_INVALID, "the wall distance needs RANS{KOmegaSST}");
             return yw.p;
+        case XCAL_FIELD_PK:
+        case XCAL_FIELD_DK:
+        case XCAL_FIELD_DW:
+            if (!has_k()) fail(XCAL_ERR_INVALID, "k-equation sources need RANS{KOmega} or LES{KEquation}");
+            return field == XCAL_FIELD_PK ? Pk.p : field == XCAL_FIELD_DK ? Dk.p : Dw.p;
         default: return nullptr;
     }
 }
@@ -1106,6 +1124,30 @@ void Case::komega() {
         launch_sst_nut(stream, mesh->nC, kfld.p, omega.p, F2b.p, Omb.p, cfg.kw_alpha1, nut.p);
     else
         launch_kw_nut(stream, mesh->nC, kfld.p, omega.p, nut.p);
+    launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
+    launch_nutwall(stream, nnutwall, mv(), nwface.p, nwpar.p, kfld.p, cfg.nu, nutf.p, nueff.p);
+}
+
+// turbulence!(::KEquationModel) (LES_KEquation.jl:134-186), grad U already
+// formed (and limited): the cell sources from the previous nut and k, the k
+// equation Time + Div(mdotf) - Lap(nu + nut_f) + Si(Dk) + Si(Dw) ==
+// Source(Pk) assembled on the p system with k's BCs and implicit
+// relaxation, solved, bounded; then nut = ck Delta sqrt(k), its faces with
+// their BCs and the wall functions' nut (correct_eddy_viscosity!)
+void Case::kequation() {
+    const double* g[9];
+    for (int q = 0; q < 9; ++q) g[q] = gradU[q].p;
+    launch_keq_sources(stream, mesh->nC, g, nut.p, kfld.p, Delta.p, cfg.keq_ce, Pk.p, Dk.p, Dw.p);
+    const xcal_schemes& sc = cfg.k_schemes;
+    launch_assemble_scalar(stream, mv(), P.view(), mdot.p, nutf.p, cfg.nu, 1.0, nullptr, 0.0, kfld.p, Dk.p, Dw.p,
+                           Pk.p, P.nz.p, P.b[0].p, sc.time, sc.divergence, cfg.dt);
+    launch_bc_relax_scalar(stream, mv(), P.view(), bcK.view(), P.nz.p, P.b[0].p, mdot.p, nutf.p, cfg.nu, 1.0, nullptr,
+                           0.0, 1, kfld.p, cfg.k_solver.relax);
+    update_precond(XCAL_EQN_K);
+    res_k = solve_system(XCAL_EQN_K, 0, &last_iters[4]);
+    XCAL_CUDA(cudaMemcpyAsync(kwtmp.p, kfld.p, (size_t)mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    launch_bound(stream, mv(), kwtmp.p, kfld.p);
+    launch_keq_nut(stream, mesh->nC, kfld.p, Delta.p, cfg.keq_ck, nut.p);
     launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
     launch_nutwall(stream, nnutwall, mv(), nwface.p, nwpar.p, kfld.p, cfg.nu, nutf.p, nueff.p);
 }
@@ -1652,6 +1694,7 @@ Case::SolveRef Case::solve_ref(int eqn, int comp) {
             return {&P, cfg.p_solver, p.p, P.b[0].p, GRES_P, 1, 3};
         case XCAL_EQN_K:
         case XCAL_EQN_OMEGA: {
+            if (eqn == XCAL_EQN_K && keq()) return {&P, cfg.k_solver, kfld.p, P.b[0].p, (int)GRES_K, 1, 4};
             if (!rans_kw()) fail(XCAL_ERR_INVALID, "k / omega equations need RANS{KOmega} or RANS{KOmegaSST}");
             const bool w = eqn == XCAL_EQN_OMEGA;
             SolveRef r{&P, w ? cfg.omega_solver : cfg.k_solver, w ? omega.p : kfld.p, P.b[0].p,
@@ -1682,6 +1725,9 @@ double Case::solve_system(int eqn, int comp, int* iters) {
 // the host-polled solve of one system R (fp64: the plain FP64 path whatever
 // the case's precision)
 double Case::solve_system_ref(const SolveRef& R, int* iters, bool fp64) {
+    static const char* const names[7] = {"solve Ux", "solve Uy", "solve Uz", "solve p", "solve k", "solve omega",
+                                         "solve wall distance"};
+    NvtxRange range(names[R.gk >= 0 && R.gk < 7 ? R.gk : 3]);
     Equation& E = *R.E;
     const xcal_solver_setup& SS = R.SS;
     double* field = R.field;
@@ -1979,7 +2025,7 @@ void Case::turbulence() {
     launch_interp_U(stream, mv(), bcU.view(), Ucp, Ufp, nullptr);
     double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = gradU[q].p;
-    const bool les = cfg.turbulence == XCAL_TURB_SMAGORINSKY;
+    const bool les = cfg.turbulence == XCAL_TURB_SMAGORINSKY;  // nut from grad U alone
     const bool limit = cfg.U_schemes.limiter == XCAL_LIMITER_CELL;
     // nut fused into the last Green-Gauss pass unless the limiter comes between
     double* nut_gg = les && !limit ? nut.p : nullptr;
@@ -2005,6 +2051,8 @@ void Case::turbulence() {
     }
     if (rans_kw())
         komega();
+    else if (keq())
+        kequation();
     else if (les)
         launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
     else
@@ -2028,30 +2076,48 @@ double Case::max_courant() {
 // residuals returned, phases timed with events.  Under capture: residuals
 // land in gres, no events.
 void Case::simple_body(double r3[3], double& rp, bool timed) {
+    NvtxRange range("SIMPLE iteration");
     if (timed) XCAL_CUDA(cudaEventRecord(ev[0], stream));
-    solve_equation_U(r3);
+    {
+        NvtxRange r("momentum predictor");
+        solve_equation_U(r3);
+    }
     if (timed) XCAL_CUDA(cudaEventRecord(ev[1], stream));
-    pressure_predictor(true);
-    flux_divergence();
+    {
+        NvtxRange r("pressure predictor + flux divergence");
+        pressure_predictor(true);
+        flux_divergence();
+    }
     XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     if (timed) XCAL_CUDA(cudaEventRecord(ev[2], stream));
-    rp = solve_equation_p();
-    explicit_relaxation_p(cfg.p_solver.relax);
-    grad_p();
-    nonorth_correctors(rp);
+    {
+        NvtxRange r("pressure equation");
+        rp = solve_equation_p();
+        explicit_relaxation_p(cfg.p_solver.relax);
+        grad_p();
+        nonorth_correctors(rp);
+    }
     if (timed) XCAL_CUDA(cudaEventRecord(ev[3], stream));
-    correct();
-    turbulence();
+    {
+        NvtxRange r("correction + turbulence");
+        correct();
+        turbulence();
+    }
     if (timed) XCAL_CUDA(cudaEventRecord(ev[4], stream));
 }
 
 // One PISO time step's launches (Solvers_2_PISO.jl:108-187); the Courant
 // number is left in gres[GRES_CO].
 void Case::piso_body(double r3[3], double& rp) {
-    solve_equation_U(r3);
+    NvtxRange range("PISO step");
+    {
+        NvtxRange r("momentum predictor");
+        solve_equation_U(r3);
+    }
     pressure_predictor(false);
     rp = 0.0;
     for (int it = 1; it <= cfg.inner_loops; ++it) {
+        NvtxRange r("pressure corrector");
         H();
         flux_divergence();
         XCAL_CUDA(cudaMemcpyAsync(prev.p, p.p, mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
@@ -2060,7 +2126,10 @@ void Case::piso_body(double r3[3], double& rp) {
         grad_p();
         correct();
     }
-    turbulence();
+    {
+        NvtxRange r("turbulence");
+        turbulence();
+    }
     courant_to_slot();
 }
 

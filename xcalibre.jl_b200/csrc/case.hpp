@@ -279,8 +279,11 @@ struct Case {
     void update_precond_E(Equation& E, int precond);
     void build_wall_table(const DevMesh& m);
     void komega();
+    void kequation();  // turbulence!(::KEquationModel) after grad U (LES_KEquation.jl:134-186)
     bool sst() const { return cfg.turbulence == XCAL_TURB_KOMEGA_SST; }
     bool rans_kw() const { return cfg.turbulence == XCAL_TURB_KOMEGA || sst(); }
+    bool keq() const { return cfg.turbulence == XCAL_TURB_KEQUATION; }
+    bool has_k() const { return rans_kw() || keq(); }  // a k field and equation
     void scalar_grad(const double* phi, const BCTable& T, int scheme, double* const g[3]);
     void wall_distance();
     void nonorth_correct();

@@ -72,6 +72,10 @@ void launch_omega_constrain(cudaStream_t s, int nw, const CSRView& A, const int*
                             const double* k, double nu, double* nz, double* b);
 void launch_bound(cudaStream_t s, const MeshView& m, const double* old, double* v);
 void launch_kw_nut(cudaStream_t s, int nC, const double* k, const double* omega, double* nut);
+// LES{KEquation}: the k equation's cell sources (Pk, Si coefficients) and nut
+void launch_keq_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* k,
+                        const double* Delta, double ce, double* Pk, double* Dk, double* Dw);
+void launch_keq_nut(cudaStream_t s, int nC, const double* k, const double* Delta, double ck, double* nut);
 void launch_nueff(cudaStream_t s, int nF, const double* nutf, double* nueff, double nu);
 // Smagorinsky nut = Delta |S| from a stored grad U
 void launch_smag_nut(cudaStream_t s, int nC, const double* const g[9], const double* Delta, double* nut);
@@ -141,6 +145,11 @@ bool kr_cg_persist(cudaStream_t s, const CSRView& A, const T* nz, const T* P, in
 // cooperative form only.  false: nothing launched (does not fit).
 constexpr int PERSIST_CLUSTER_ONLY = 2;
 constexpr int PERSIST_COOP_ONLY = 3;  // the widest cooperative form that fits, never the cluster form
+// one block per SM, each owning every G-th tile (1024 or 512 threads; the
+// block's q in shared memory: at most PERSIST_MT_SMEM bytes)
+constexpr int PERSIST_MT1024 = 4;
+constexpr int PERSIST_MT512 = 5;
+constexpr int PERSIST_MT_SMEM = 200 * 1024;
 // whether this device and driver run a cooperative kernel captured into a
 // CUDA graph (in_while: inside the body of a conditional WHILE node); found
 // out once per process by capturing and running a one-block no-op that way

@@ -1462,6 +1462,58 @@ void launch_bound(cudaStream_t s, const MeshView& m, const double* old, double* 
     k_bound<<<nblk(m.nC), TPB, 0, s>>>(m, old, v);
     XCAL_CHECK_LAUNCH();
 }
+// LES{KEquation} cell sources (LES_KEquation.jl:164-168), rho = 1:
+//   Pk = 2 nut (grad U . dev(S)), the Frobenius product over the tensor's
+//        column-major entries in order, S = (G + G')/2, dev(S) = S - tr(S)/3 I
+//   Dk = ce sqrt(k) / Delta      (Si on k)
+//   Dw = 2/3 tr(grad U)          (a second Si on k)
+// G[a][b] = g[3 a + b] is entry (a, b) of the tensor the reference builds.
+__global__ void k_keq_sources(int nC, const double* __restrict__ g0, const double* __restrict__ g1,
+                              const double* __restrict__ g2, const double* __restrict__ g3,
+                              const double* __restrict__ g4, const double* __restrict__ g5,
+                              const double* __restrict__ g6, const double* __restrict__ g7,
+                              const double* __restrict__ g8, const double* __restrict__ nut,
+                              const double* __restrict__ k, const double* __restrict__ Delta, double ce, double* Pk,
+                              double* Dk, double* Dw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nC) return;
+    const double G[3][3] = {{g0[i], g1[i], g2[i]}, {g3[i], g4[i], g5[i]}, {g6[i], g7[i], g8[i]}};
+    double S[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) S[a][b] = 0.5 * (G[a][b] + G[b][a]);
+    const double trS = (S[0][0] + S[1][1]) + S[2][2];
+    const double third = (1.0 / 3.0) * trS;
+    double dot = 0.0;
+    bool first = true;
+    for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+            const double dev = a == b ? S[a][b] - third : S[a][b];
+            const double pr = G[a][b] * dev;
+            dot = first ? pr : dot + pr;
+            first = false;
+        }
+    Pk[i] = (2.0 * nut[i]) * dot;
+    Dk[i] = (ce * sqrt(k[i])) / Delta[i];
+    Dw[i] = (2.0 / 3.0) * ((G[0][0] + G[1][1]) + G[2][2]);
+}
+
+// nut = ck Delta sqrt(k) (LES_KEquation.jl:180-183)
+__global__ void k_keq_nut(int nC, const double* __restrict__ k, const double* __restrict__ Delta, double ck,
+                          double* nut) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nC) nut[i] = (ck * Delta[i]) * sqrt(k[i]);
+}
+
+void launch_keq_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* k,
+                        const double* Delta, double ce, double* Pk, double* Dk, double* Dw) {
+    k_keq_sources<<<nblk(nC), TPB, 0, s>>>(nC, g[0], g[1], g[2], g[3], g[4], g[5], g[6], g[7], g[8], nut, k, Delta, ce,
+                                           Pk, Dk, Dw);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_keq_nut(cudaStream_t s, int nC, const double* k, const double* Delta, double ck, double* nut) {
+    k_keq_nut<<<nblk(nC), TPB, 0, s>>>(nC, k, Delta, ck, nut);
+    XCAL_CHECK_LAUNCH();
+}
 void launch_kw_nut(cudaStream_t s, int nC, const double* k, const double* omega, double* nut) {
     k_kw_nut<<<nblk(nC), TPB, 0, s>>>(nC, k, omega, nut);
     XCAL_CHECK_LAUNCH();

@@ -18,8 +18,20 @@
 #include <vector>
 
 #include "../../include/xcal_b200.h"
+#include <nvtx3/nvToolsExt.h>
 
 namespace xcal {
+
+// A named NVTX range over a scope of host code (the phases of a SIMPLE
+// iteration / PISO step, each equation's solve, the batch's phases), for
+// timeline profilers; nvtxRangePush costs a pointer test when none is
+// attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ---------------------------------------------------------------------------
 // errors

@@ -42,6 +42,7 @@ class Mesh3:
     points: np.ndarray | None = None
     polymesh: object = None      # the PolyMesh it was built from (nodes and faces, for the writers)
     dim: int = 3                 # 2: a Mesh2 (UNV2D_mesh), 3: a Mesh3
+    cell_nodes: list | None = None  # 2D meshes read from UNV: each cell's nodes in element order (the 2D writer)
 
     @property
     def n_ifaces(self) -> int:

@@ -301,7 +301,7 @@ def unv2_mesh(points, elements, groups, scale: float = 1.0, source: str = "mesh"
                  cell_centre=np.array(centre, dtype=np.float64), cell_volume=np.array(volume, dtype=np.float64),
                  cell_faces_offset=off, cell_faces=cat(c_faces), cell_nsign=cat(nsign), cell_neighbours=cat(c_neigh),
                  boundary_cellsID=bcell, patch_names=[g[0] for g in groups], patch_start=patch_start,
-                 patch_count=patch_count, points=points, dim=2)
+                 patch_count=patch_count, points=points, dim=2, cell_nodes=[list(vs) for vs in cells_nodes])
 
 
 # ---------------------------------------------------------------------------
@@ -385,6 +385,31 @@ def _cross(a, b):
 def UNV3D_mesh(path: str, scale: float = 1.0) -> Mesh3:
     """UNV3D_mesh(meshFile; scale) (UNV3_2_builder.jl:14-30)."""
     return unv3_mesh(*read_unv3(path, scale), source=path)
+
+
+def _unv3_polymesh(points, fnodes, owner, neigh, nB, groups):
+    """The polyMesh view of a UNV3 mesh, for the result writers: internal
+    faces first, each with the lower-numbered cell as owner (its nodes
+    reversed when that swaps owner and neighbour, so the normal keeps
+    pointing out of the owner), in (owner, neighbour) order; then the
+    boundary faces, group by group.  fnodes are oriented out of their owner
+    (as calculate_face_properties! leaves them)."""
+    from .meshgen import PolyMesh
+    internal = []
+    for f in range(nB, len(fnodes)):
+        o, n, fn = owner[f], neigh[f], list(fnodes[f])
+        if o > n:
+            o, n, fn = n, o, fn[::-1]
+        internal.append((o, n, fn))
+    internal.sort(key=lambda t: (t[0], t[1]))
+    faces = [t[2] for t in internal] + [list(fnodes[f]) for f in range(nB)]
+    off = np.zeros(len(faces) + 1, dtype=np.int32)
+    off[1:] = np.cumsum([len(fn) for fn in faces])
+    return PolyMesh(points=np.asarray(points, dtype=np.float64), face_offsets=off,
+                    face_nodes=np.array([v for fn in faces for v in fn], dtype=np.int32),
+                    owner=np.array([t[0] for t in internal] + [owner[f] for f in range(nB)], dtype=np.int32),
+                    neighbour=np.array([t[1] for t in internal], dtype=np.int32),
+                    patch_names=[g[0] for g in groups], patch_sizes=[len(g[1]) for g in groups])
 
 
 def unv3_mesh(points, faces, cells, groups, source: str = "mesh") -> Mesh3:
@@ -538,4 +563,5 @@ def unv3_mesh(points, faces, cells, groups, source: str = "mesh") -> Mesh3:
                  cell_faces_offset=off, cell_faces=cat(c_faces), cell_nsign=cat(c_sign), cell_neighbours=cat(c_nb),
                  boundary_cellsID=np.array(b_cell, dtype=np.int32), patch_names=[g[0] for g in groups],
                  patch_start=np.array(patch_start, dtype=np.int32), patch_count=np.array(patch_count, dtype=np.int32),
-                 points=np.asarray(points, dtype=np.float64), dim=3)
+                 points=np.asarray(points, dtype=np.float64), dim=3,
+                 polymesh=_unv3_polymesh(points, fnodes, owner, neigh, nB, groups))

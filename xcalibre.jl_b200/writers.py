@@ -8,6 +8,11 @@ src/IOFormats/OpenFOAM/OpenFOAM_writer.jl):
   normal points out of the cell (the owner's node order, reversed for the
   neighbour).  File ``iteration_<k>.vtu`` for steady runs, ``time_<k>.vtu``
   for transient ones; cell data U (3 components) and p, plus nut for LES.
+  A 2D mesh read from a UNV file (a Mesh2 in the reference,
+  src/IOFormats/VTK/VTK_writer.jl) is written as a legacy ASCII .vtk file
+  (``iteration_<k>.vtk`` / ``time_<k>.vtk``): the points, each cell's nodes
+  in element order, cell type 5 (triangle), 9 (quad) or 7 (polygon), and
+  SCALARS / VECTORS cell data.
 * OpenFOAM: ``constant/polyMesh`` written once, then one time directory per
   write (``<k>`` steady, ``%.8f`` of the time transient) holding
   volVectorField U / volScalarField p with their internal values and one
@@ -35,6 +40,38 @@ def _fmt(a: np.ndarray) -> str:
     if a.ndim == 1:
         return "\n".join(map(repr, a.tolist())) + "\n"
     return "\n".join(" ".join(map(repr, row)) for row in a.tolist()) + "\n"
+
+
+class VTKWriter2D:
+    """A 2D mesh's .vtk writer: points and the cells' node lists, written
+    out in full with the fields at each write (write_results for a Mesh2)."""
+
+    def __init__(self, points, cell_nodes):
+        pts = np.asarray(points, dtype=np.float64)
+        self.n_cells = len(cell_nodes)
+        size = sum(len(c) for c in cell_nodes) + self.n_cells
+        types = ["5" if len(c) == 3 else "9" if len(c) == 4 else "7" for c in cell_nodes]
+        self.header = (
+            "# vtk DataFile Version 3.0\nXCALibre B200 simulation data\nASCII\nDATASET UNSTRUCTURED_GRID\n"
+            f"POINTS {pts.shape[0]} double\n" + _fmt(pts)
+            + f"CELLS {self.n_cells} {size}\n"
+            + "".join(f"{len(c)} " + " ".join(map(str, c)) + "\n" for c in cell_nodes)
+            + f"CELL_TYPES {self.n_cells}\n" + "\n".join(types) + "\n"
+            + f"CELL_DATA {self.n_cells}\n")
+
+    def write(self, path: str, fields) -> None:
+        """fields: [(label, values)] with values [n] (scalar) or [3, n] / [n, 3]."""
+        with open(path, "w") as f:
+            f.write(self.header)
+            for label, v in fields:
+                v = np.asarray(v, dtype=np.float64)
+                if v.ndim == 2 and v.shape[0] == 3 and v.shape[1] == self.n_cells:
+                    v = v.T
+                if v.ndim == 1:
+                    f.write(f"SCALARS {label} double 1\nLOOKUP_TABLE CellColors\n")
+                else:
+                    f.write(f"VECTORS {label} double\n")
+                f.write(_fmt(v))
 
 
 class VTKWriter3D:
