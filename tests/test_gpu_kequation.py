@@ -73,6 +73,26 @@ def test_kequation_restart_and_mixed(x, ctx):
         assert err <= 1e-4, (f, err)
 
 
+@pytest.mark.parametrize("graph", [False, True])
+def test_kequation_periodic_parity(x, orc, ctx, graph):
+    """The periodic LES box with the k equation: k's periodic pairs in the
+    shared p storage, GPU equal to the oracle bit for bit over 4 steps."""
+    mesh = x.build_mesh3(x.periodic_box_polymesh(10, seed=4))
+    U0 = x.cases.fourier_field(mesh, seed=4)
+    model, config = x.cases.periodic_les_case(mesh, steps=4, U0=U0, model_kind=x.KEquation)
+    cfg, keep = x.build_config(model, config)
+    assert cfg.turbulence == x._abi.TURB_KEQUATION
+    g, dm = _gpu(x, ctx, mesh, model, cfg, graph)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    _set(x, o, model)
+    rg, cg = g.piso_step(4)
+    ro, co = o.piso_step(4)
+    assert np.array_equal(rg, ro) and np.array_equal(cg, co)
+    for f in FIELDS:
+        a, b = g.get_field(getattr(x._abi, f)), o.get_field(getattr(x._abi, f))
+        assert np.array_equal(a, b), f
+
+
 def test_kequation_batch_refused(x, ctx):
     mesh = x.build_mesh3(x.channel_polymesh(12, 6, 6, seed=1))
     model, config = x.cases.kequation_channel_case(mesh, steps=2)

@@ -198,3 +198,46 @@ def test_wall_functions_parity(x, orc, ctx, sst):
     _check(x, g, o)
     walls = list(mesh.patch_range("walls"))
     assert np.all(g.get_field(x._abi.FIELD_NUTF)[walls] > 0)  # the log-law branch ran
+
+
+@pytest.mark.parametrize("sst", [False, True])
+def test_komega_periodic_channel_parity(x, orc, ctx, sst):
+    """k-omega (and SST) on a channel periodic in the flow direction (inlet
+    and outlet paired by construct_periodic, every field periodic there),
+    with a disturbed initial velocity and a pressure reference: the scalar
+    equations' periodic pairs in the shared p storage; GPU equal to the
+    oracle over 3 SIMPLE iterations."""
+    A = x.api
+    mesh = x.build_mesh3(x.channel_polymesh(12, 6, 6, seed=7))
+    per = list(A.construct_periodic(mesh, None, "inlet", "outlet"))
+    turb = A.RANS(A.KOmegaSST, walls=["walls"]) if sst else A.RANS(A.KOmega)
+    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=1e-3), turbulence=turb,
+                      energy=A.Energy(A.Isothermal), domain=mesh)
+    BCs = A.assign(region=mesh, U=per + [A.Wall("walls", [0.0, 0.0, 0.0])], p=per + [A.Wall("walls")],
+                   k=per + [A.Dirichlet("walls", 0.0)], omega=per + [A.OmegaWallFunction("walls")],
+                   nut=per + [A.Dirichlet("walls", 0.0)])
+
+    def ss(s, relax):
+        return A.SolverSetup(solver=s(), preconditioner=A.Jacobi(), convergence=1e-7, relax=relax, rtol=1e-2)
+
+    config = A.Configuration(solvers={"U": ss(A.Bicgstab, 0.7), "p": ss(A.Cg, 0.3), "k": ss(A.Bicgstab, 0.7),
+                                      "omega": ss(A.Bicgstab, 0.7),
+                                      "y": A.SolverSetup(solver=A.Cg(), preconditioner=A.Jacobi(), convergence=1e-8,
+                                                         relax=0.9, rtol=1e-3)},
+                             schemes={"U": A.Schemes(divergence=A.Upwind), "p": A.Schemes(),
+                                      "k": A.Schemes(divergence=A.Upwind), "omega": A.Schemes(divergence=A.Upwind),
+                                      "y": A.Schemes()},
+                             runtime=A.Runtime(iterations=3, write_interval=-1, time_step=1.0),
+                             hardware=A.Hardware(backend=A.B200Backend()), boundaries=BCs)
+    rng = np.random.default_rng(7)
+    model.momentum.U[:] = np.array([[1.0], [0.0], [0.0]]) + 0.05 * rng.standard_normal((3, mesh.n_cells))
+    A.initialise_(model.momentum.p, 0.0)
+    A.initialise_(model.turbulence.k, 0.01)
+    A.initialise_(model.turbulence.omega, 10.0)
+    A.initialise_(model.turbulence.nut, 1e-3)
+    cfg, keep = x.build_config(model, config, pref=0.0)
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, False)
+    rg, _ = g.simple_iterate(3)
+    ro, _ = o.simple_iterate(3)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    _check(x, g, o)

@@ -65,3 +65,23 @@ def test_kequation_relations(x, orc):
         assert np.array_equal(o.get_field(A.FIELD_DK), Dk)
         assert np.array_equal(o.get_field(A.FIELD_DW), Dw)
     assert k.max() > 0.0 and nut.max() > 0.0
+
+
+def test_kequation_periodic_oracle(x, orc):
+    """On the periodic box the k equation runs with every field periodic:
+    finite, k >= 0, nut = ck Delta sqrt(k)."""
+    mesh = x.build_mesh3(x.periodic_box_polymesh(8, seed=2))
+    U0 = x.cases.fourier_field(mesh, seed=2)
+    model, config = x.cases.periodic_les_case(mesh, steps=3, U0=U0, model_kind=x.KEquation)
+    cfg, keep = x.build_config(model, config)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    A = x._abi
+    for f, v in (("FIELD_U", model.momentum.U), ("FIELD_P", model.momentum.p), ("FIELD_K", model.turbulence.k),
+                 ("FIELD_NUT", model.turbulence.nut)):
+        o.set_field(getattr(A, f), v)
+    res, co = o.piso_step(3)
+    assert np.all(np.isfinite(res)) and np.all(np.isfinite(co))
+    k, nut = o.get_field(A.FIELD_K), o.get_field(A.FIELD_NUT)
+    Delta = o.get_field(A.FIELD_DELTA)
+    assert np.all(k >= 0.0) and k.max() > 0.0
+    assert np.array_equal(nut, (0.094 * Delta) * np.sqrt(k))

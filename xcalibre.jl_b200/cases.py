@@ -8,7 +8,9 @@
                         nu = 1e-3, LUST, SIMPLE
 * periodic_les_case  -- periodic cube, PISO + Smagorinsky (Cs = 0.17),
                         Euler, Linear divergence, nu = 1e-4; initial field
-                        from fourier_field (seeded, k^4 exp(-2 (k/4)^2))
+                        from fourier_field (seeded, k^4 exp(-2 (k/4)^2));
+                        or the subgrid k equation (LES{KEquation})
+* kequation_channel_case -- the channel with LES{KEquation}, PISO
 """
 from __future__ import annotations
 
@@ -70,7 +72,6 @@ def channel_case(mesh: Mesh3, iterations: int = 500, precision: str = "fp64", de
     return model, config
 
 
-
 def kequation_channel_case(mesh: Mesh3, steps: int = 20, precision: str = "fp64", device: int = 0,
                            nu: float = 1e-4, dt: float = 2e-3, k_in: float = 1e-3, ck: float = 0.094,
                            ce: float = 1.048, seed: int = 0):
@@ -102,6 +103,7 @@ def kequation_channel_case(mesh: Mesh3, steps: int = 20, precision: str = "fp64"
     A.initialise_(model.turbulence.k, k_in)
     A.initialise_(model.turbulence.nut, 0.0)
     return model, config
+
 
 def taylor_green(mesh: Mesh3, rms: float = 1.0) -> np.ndarray:
     """Divergence-free periodic field on [0, 2pi]^3 (deterministic)."""
@@ -146,13 +148,20 @@ def fourier_field(mesh: Mesh3, seed: int = 0, k0: float = 4.0, rms: float = 1.0,
 
 
 def periodic_les_case(mesh: Mesh3, steps: int = 200, dt: float | None = None, precision: str = "fp64",
-                      device: int = 0, U0: np.ndarray | None = None):
+                      device: int = 0, U0: np.ndarray | None = None, model_kind=None, k0: float = 1e-3):
+    """The periodic LES box: Smagorinsky (C = 0.17) by default, or
+    model_kind=A.KEquation (the subgrid k equation, k = k0 initially, every
+    field periodic)."""
     pairs = [A.construct_periodic(mesh, None, a, b) for a, b in (("xmin", "xmax"), ("ymin", "ymax"), ("zmin", "zmax"))]
     per = [bc for pair in pairs for bc in pair]
-    model = A.Physics(time=A.Transient(), fluid=A.Fluid(A.Incompressible, nu=1e-4), turbulence=A.LES(A.Smagorinsky, C=0.17),
+    keq = model_kind is A.KEquation
+    turb = A.LES(A.KEquation) if keq else A.LES(A.Smagorinsky, C=0.17)
+    model = A.Physics(time=A.Transient(), fluid=A.Fluid(A.Incompressible, nu=1e-4), turbulence=turb,
                       energy=A.Energy(A.Isothermal), domain=mesh)
-    BCs = A.assign(region=mesh, U=per, p=per, nut=per)
+    BCs = A.assign(region=mesh, U=per, p=per, nut=per, **({"k": per} if keq else {}))
     schemes = {"U": A.Schemes(time=A.Euler, divergence=A.Linear), "p": A.Schemes(time=A.Euler)}
+    if keq:
+        schemes["k"] = A.Schemes(time=A.Euler, divergence=A.Linear)
     if U0 is None:
         U0 = fourier_field(mesh, seed=0)
     if dt is None:
@@ -161,10 +170,15 @@ def periodic_les_case(mesh: Mesh3, steps: int = 200, dt: float | None = None, pr
         dx = np.power(mesh.cell_volume, 1.0 / 3.0)
         dt = 0.5 * float(np.min(dx / np.maximum(umag, 1e-30)))
     solvers = _solvers(relax_U=1.0, relax_p=1.0, rtol_U=0.1, rtol_p=0.01)
+    if keq:
+        solvers["k"] = A.SolverSetup(solver=A.Bicgstab(), preconditioner=A.Jacobi(), convergence=1e-7, relax=1.0,
+                                     rtol=1e-3)
     config = A.Configuration(solvers=solvers, schemes=schemes,
                              runtime=A.Runtime(iterations=steps, write_interval=-1, time_step=dt),
                              hardware=A.Hardware(backend=A.B200Backend(device=device, precision=precision)),
                              boundaries=BCs)
     model.momentum.U[:] = U0
     A.initialise_(model.momentum.p, 0.0)
+    if keq:
+        A.initialise_(model.turbulence.k, k0)
     return model, config

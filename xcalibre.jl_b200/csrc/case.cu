@@ -725,23 +725,20 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         if (bc.type == XCAL_BC_OMEGA_WALL || bc.type == XCAL_BC_K_WALL)
             fail(XCAL_ERR_INVALID, "OmegaWallFunction / KWallFunction do not apply to nut");
     if (keq()) {
-        // LES{KEquation}: the subgrid k equation shares the p system
-        build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, nullptr, stream);
-        if (bcK.has_periodic || bcP.has_periodic || bcNut.has_periodic || bcU.has_periodic)
-            fail(XCAL_ERR_UNSUPPORTED, "LES{KEquation}: periodic boundaries are not implemented");
+        // LES{KEquation}: the subgrid k equation shares the p system (its
+        // periodic pairs resolve to the p system's partner slots)
+        build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, &P, stream);
         for (DBuf<double>* b : {&kfld, &Pk, &Dk, &Dw, &kwtmp}) {
             b->alloc(m->nC);
             b->zero(stream);
         }
         build_wall_table(*m);
     } else if (rans_kw()) {
-        // RANS{KOmega} / RANS{KOmegaSST}: k / omega share the p system
-        build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, nullptr, stream);
-        build_bc_table(bcOmega, *m, cfg.bc_omega, cfg.n_bc_omega, 1, nullptr, stream);
-        if (sst()) build_bc_table(bcY, *m, cfg.bc_y, cfg.n_bc_y, 1, nullptr, stream);
-        if (bcK.has_periodic || bcOmega.has_periodic || bcP.has_periodic || bcNut.has_periodic || bcU.has_periodic ||
-            bcY.has_periodic)
-            fail(XCAL_ERR_UNSUPPORTED, "k-omega: periodic boundaries are not implemented");
+        // RANS{KOmega} / RANS{KOmegaSST}: k / omega share the p system (their
+        // periodic pairs resolve to the p system's partner slots)
+        build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, &P, stream);
+        build_bc_table(bcOmega, *m, cfg.bc_omega, cfg.n_bc_omega, 1, &P, stream);
+        if (sst()) build_bc_table(bcY, *m, cfg.bc_y, cfg.n_bc_y, 1, &P, stream);
         for (DBuf<double>* b : {&kfld, &omega, &Pk, &Pw, &Dk, &Dw, &kwtmp}) {
             b->alloc(m->nC);
             b->zero(stream);
@@ -1112,7 +1109,8 @@ void Case::komega() {
         launch_assemble_scalar(stream, mv(), P.view(), mdot.p, nutf.p, cfg.nu, sigma, F1, sigma2, phi,
                                w ? Dw.p : Dk.p, D2, w ? Pw.p : Pk.p, P.nz.p, P.b[0].p, sc.time, sc.divergence, cfg.dt);
         launch_bc_relax_scalar(stream, mv(), P.view(), (w ? bcOmega : bcK).view(), P.nz.p, P.b[0].p, mdot.p, nutf.p,
-                               cfg.nu, sigma, F1, sigma2, D2 ? 1 : 0, phi, (w ? cfg.omega_solver : cfg.k_solver).relax);
+                               cfg.nu, sigma, F1, sigma2, D2 ? 1 : 0, phi, (w ? cfg.omega_solver : cfg.k_solver).relax,
+                               sc.divergence);
         if (w && nwall) launch_omega_constrain(stream, nwall, P.view(), wcell.p, wpar.p, kfld.p, cfg.nu, P.nz.p, P.b[0].p);
         update_precond(e);
         const double r = solve_system(e, 0, &last_iters[w ? 5 : 4]);
@@ -1142,7 +1140,7 @@ void Case::kequation() {
     launch_assemble_scalar(stream, mv(), P.view(), mdot.p, nutf.p, cfg.nu, 1.0, nullptr, 0.0, kfld.p, Dk.p, Dw.p,
                            Pk.p, P.nz.p, P.b[0].p, sc.time, sc.divergence, cfg.dt);
     launch_bc_relax_scalar(stream, mv(), P.view(), bcK.view(), P.nz.p, P.b[0].p, mdot.p, nutf.p, cfg.nu, 1.0, nullptr,
-                           0.0, 1, kfld.p, cfg.k_solver.relax);
+                           0.0, 1, kfld.p, cfg.k_solver.relax, sc.divergence);
     update_precond(XCAL_EQN_K);
     res_k = solve_system(XCAL_EQN_K, 0, &last_iters[4]);
     XCAL_CUDA(cudaMemcpyAsync(kwtmp.p, kfld.p, (size_t)mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));

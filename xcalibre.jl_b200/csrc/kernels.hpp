@@ -53,7 +53,8 @@ void launch_assemble_scalar(cudaStream_t s, const MeshView& m, const CSRView& A,
                             double* b, int time_scheme, int div_scheme, double dt);
 void launch_bc_relax_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz,
                             double* b, const double* mdot, const double* nutf, double nu, double sigma,
-                            const double* F1, double sigma2, int si2, const double* phi, double alpha);
+                            const double* F1, double sigma2, int si2, const double* phi, double alpha,
+                            int div_scheme);
 // k-omega SST: cell fields, nut, and the wall distance from phi and grad phi
 void launch_sst_fields(cudaStream_t s, int nC, const double* const g[9], const double* const gk[3],
                        const double* const gw[3], const double* k, const double* omega, const double* nut,

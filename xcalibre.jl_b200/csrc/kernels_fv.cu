@@ -472,7 +472,8 @@ __global__ void k_assemble_scalar(MeshView m, CSRView A, const double* __restric
 // OmegaWallFunction contributes as Extrapolated (its wall rows are then
 // constrained)
 __device__ void bc_scalar_transport(const MeshView& m, const BCView& bc, int f, int cell, const double* mdot,
-                                    double muf, const double* phi, bool si2, double& AP, double& BP) {
+                                    double muf, const double* phi, bool si2, int div_scheme, double& AP,
+                                    double& BP) {
     double ap_d = 0.0, bp_d = 0.0, ap_l = 0.0, bp_l = 0.0;
     switch (bc.type[f]) {
         case XCAL_BC_DIRICHLET:
@@ -509,7 +510,13 @@ __device__ void bc_scalar_transport(const MeshView& m, const BCView& bc, int f, 
             bp_l = (muf * m.area[f]) * val;
             break;
         }
-        default:  // Empty
+        case XCAL_BC_PERIODIC_PARENT: {  // own-row share; slots in k_bc_relax_scalar
+            double an;
+            periodic_div(bc, f, mdot[f], div_scheme, ap_d, an);
+            periodic_lap(bc, f, muf, ap_l, an);
+            break;
+        }
+        default:  // Empty, the periodic partner faces
             break;
     }
     double ap = 0.0, bp = 0.0;
@@ -531,22 +538,56 @@ __device__ void bc_scalar_transport(const MeshView& m, const BCView& bc, int f, 
 
 // apply_boundary_conditions! (ascending face id per cell) then
 // implicit_relaxation_diagdom! (Solve_1_api.jl:388-411) of the k / omega
-// equation, one thread per row
+// equation, one thread per row.  Periodic pairs (periodic.jl:261-443): a
+// parent face adds its own-row share through the functor and writes the
+// (own, partner) slot; the partner cell adds its diagonal share and writes
+// the (partner, own) slot -- its own boundary faces and the parent faces it
+// partners merged in ascending face order, the reference's face loop order.
 __global__ void k_bc_relax_scalar(MeshView m, CSRView A, BCView bc, double* nz, double* b,
                                   const double* __restrict__ mdot, const double* __restrict__ nutf, double nu,
                                   double sigma, const double* __restrict__ F1, double sigma2, int si2,
-                                  const double* __restrict__ phi, double alpha) {
+                                  const double* __restrict__ phi, double alpha, int div_scheme) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.nC) return;
     const int ds = A.diag[i];
     double d = nz[ds];
     double bi = b[i];
-    for (int k = m.bf_off[i]; k < m.bf_off[i + 1]; ++k) {
-        const int f = m.bf_face[k];
-        double AP, BP;
-        bc_scalar_transport(m, bc, f, i, mdot, kw_mueff(m, f, nutf, nu, sigma, F1, sigma2), phi, si2 != 0, AP, BP);
-        d = d + AP;
-        bi = bi + BP;
+    int k = m.bf_off[i];
+    const int ke = m.bf_off[i + 1];
+    int q = bc.pe_off ? bc.pe_off[i] : 0;
+    const int qe = bc.pe_off ? bc.pe_off[i + 1] : 0;
+    while (k < ke || q < qe) {
+        const int fo = k < ke ? m.bf_face[k] : 0x7fffffff;
+        const int fp = q < qe ? bc.pe_face[q] : 0x7fffffff;
+        if (fo < fp) {
+            const double muf = kw_mueff(m, fo, nutf, nu, sigma, F1, sigma2);
+            double AP, BP;
+            bc_scalar_transport(m, bc, fo, i, mdot, muf, phi, si2 != 0, div_scheme, AP, BP);
+            d = d + AP;
+            bi = bi + BP;
+            if (bc.type[fo] == XCAL_BC_PERIODIC_PARENT) {  // (own, partner) slot from A0 = 0
+                double acd, and_, acl, anl;
+                periodic_div(bc, fo, mdot[fo], div_scheme, acd, and_);
+                periodic_lap(bc, fo, muf, acl, anl);
+                double v = 0.0;
+                v = v + and_;
+                v = v + anl;
+                nz[bc.pPN[fo]] = v;
+            }
+            ++k;
+        } else {  // this cell is the partner of parent face fp
+            const double muf = kw_mueff(m, fp, nutf, nu, sigma, F1, sigma2);
+            double acd, and_, acl, anl;
+            periodic_div(bc, fp, mdot[fp], div_scheme, acd, and_);
+            periodic_lap(bc, fp, muf, acl, anl);
+            d = d + (-and_);
+            d = d + (-anl);
+            double v = 0.0;
+            v = v + (-acd);
+            v = v + (-acl);
+            nz[bc.pNP[fp]] = v;
+            ++q;
+        }
     }
     double sumv = 0.0;
     const int rb = row_base(A, i), rl = A.len[i];
@@ -1418,8 +1459,10 @@ void launch_assemble_scalar(cudaStream_t s, const MeshView& m, const CSRView& A,
 }
 void launch_bc_relax_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz,
                             double* b, const double* mdot, const double* nutf, double nu, double sigma,
-                            const double* F1, double sigma2, int si2, const double* phi, double alpha) {
-    k_bc_relax_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, bc, nz, b, mdot, nutf, nu, sigma, F1, sigma2, si2, phi, alpha);
+                            const double* F1, double sigma2, int si2, const double* phi, double alpha,
+                            int div_scheme) {
+    k_bc_relax_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, bc, nz, b, mdot, nutf, nu, sigma, F1, sigma2, si2, phi, alpha,
+                                                 div_scheme);
     XCAL_CHECK_LAUNCH();
 }
 void launch_sst_fields(cudaStream_t s, int nC, const double* const g[9], const double* const gk[3],
