@@ -435,19 +435,31 @@ def serve_measure(x, args, local):
     (cap 1500 SIMPLE iterations); continuous batching with admission by
     device-memory footprint (serve_budget_gb).  Meshes are built before the
     stream starts (they are the requests' payload).  serve_iters caps each
-    request's SIMPLE iterations."""
+    request's SIMPLE iterations.  With several ranks (one process per GPU)
+    the stream is sharded: rank r serves requests r, r + N, ... with its own
+    Server, the ranks start together, and the line reports every request
+    (throughput over the slowest rank's wall time, p50/p99 over all)."""
     from importlib import import_module
     serve = import_module(x.__name__ + ".serve")
+    world, rank = (torch_world() if args.gpus > 1 else (1, 0))
     reqs = serve.make_requests(args.serve_cases, seed=0, n_min=1e3, n_max=args.serve_nmax, rate=args.serve_rate)
-    for r in reqs:
+    mine = serve.shard_requests(reqs, rank, world)
+    for r in mine:
         r.build()
     ctx = x.Context(local)
     budget = int(args.serve_budget_gb * (1 << 30))
     srv = serve.Server(ctx, budget_bytes=budget, max_cases=64, precision="mixed", max_iters=args.serve_iters,
                        convergence=1e-6)
     l0 = x.launch_count()
-    res = srv.run(reqs, realtime=True)
-    s = serve.summarize(res, srv.wall)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+    res = srv.run(mine, realtime=True)
+    wall = srv.wall
+    if world > 1:
+        res, wall = gather_served(res, wall, world, serve)
+    s = serve.summarize(res, wall)
+    s["sharding"] = f"{world} ranks, request i on rank i mod {world}" if world > 1 else "1 GPU"
     s.update({"workload": f"{len(reqs)} steady cavity/channel requests, N log-uniform [1e3, {args.serve_nmax:g}], "
                           f"Re U[100,2000], aspect U[1,4], Poisson {args.serve_rate:g}/s, mixed, resid 1e-6, "
                           f"cap {args.serve_iters} iterations",
@@ -459,6 +471,23 @@ def serve_measure(x, args, local):
               "idle_s": srv.idle_s, "cleanup_s": srv.cleanup_s,
               "gpu_launches": x.launch_count() - l0})
     return s
+
+
+def torch_world():
+    """(world size, rank) of the running process group, or (1, 0)."""
+    import torch
+    if torch.distributed.is_available() and torch.distributed.is_initialized():
+        return torch.distributed.get_world_size(), torch.distributed.get_rank()
+    return 1, 0
+
+
+def gather_served(results, wall, world, serve):
+    """Every rank's served requests (records without field arrays) and the
+    slowest rank's wall time, on every rank."""
+    import torch
+    parts = [None] * world
+    torch.distributed.all_gather_object(parts, ([serve.result_record(r) for r in results], wall))
+    return serve.merge_records([p[0] for p in parts]), max(p[1] for p in parts)
 
 
 def batch_measure(x, args, local):

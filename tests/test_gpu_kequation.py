@@ -3,7 +3,7 @@ a disturbed inflow, PISO steps with the subgrid k equation, host-polled and
 in graph mode -- U, p, k, nut, their face values, grad U and the k
 equation's sources equal bit for bit; a checkpoint/restore continues
 exactly; mixed precision stays within the mixed-precision tolerance; the
-batch refuses the model."""
+batch (steady SIMPLE only) refuses the transient model."""
 import numpy as np
 import pytest
 

@@ -115,15 +115,40 @@ def test_komega_simple_channel_parity(x, orc, ctx, precond):
     _check(x, g, o)
 
 
-def test_komega_not_batched(x, ctx):
-    mesh = skewed_channel(x, n=(6, 4, 4), seed=2)
-    model, config = komega_channel_case(x, mesh, 2)
-    cfg, keep = x.build_config(model, config)
-    dm = x.DeviceMesh(ctx, mesh)
-    c = x.Case(dm, cfg)
-    batch = x.api.Batch(ctx, 2, 1 << 30)
-    with pytest.raises(Exception):
-        batch.add(c)
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_komega_batch_matches_single(x, ctx, prec):
+    """k-omega cases in a batch: their U and p solves batched with the other
+    members', their k and omega solves each on its own stream; every case
+    equals the same case advanced alone, bit for bit."""
+    specs = [((12, 7, 6), 11, "Jacobi"), ((10, 6, 6), 3, "Jacobi")]
+
+    def mk(n, seed):
+        mesh = skewed_channel(x, n=n, seed=seed)
+        model, config = komega_channel_case(x, mesh, 4)
+        config.hardware.backend.precision = prec
+        cfg, keep = x.build_config(model, config)
+        dm = x.DeviceMesh(ctx, mesh)
+        c = x.Case(dm, cfg)
+        c.set_inner_cg(1)
+        set_komega_fields(x, c, model)
+        return c, (dm, keep, cfg)
+
+    alone = []
+    for n, seed, _ in specs:
+        c, keep = mk(n, seed)
+        res, _ = c.simple_iterate(4)
+        alone.append((res, [c.get_field(getattr(x._abi, f)) for f in KW_FIELDS]))
+    batch = x.api.Batch(ctx, 4, 1 << 32)
+    members = []
+    for n, seed, _ in specs:
+        c, keep = mk(n, seed)
+        assert batch.add(c)
+        members.append((c, keep))
+    hist = np.stack([batch.simple_iterate()[0] for _ in range(4)], axis=1)
+    for k, (c, keep) in enumerate(members):
+        assert np.array_equal(hist[k], alone[k][0]), k
+        for f, ref in zip(KW_FIELDS, alone[k][1]):
+            assert np.array_equal(c.get_field(getattr(x._abi, f)), ref), (k, f)
     batch.close()
 
 

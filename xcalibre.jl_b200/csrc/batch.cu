@@ -201,7 +201,6 @@ struct Batch {
 
     void check_compatible(const Case* c) const {
         if (c->cfg.algorithm != XCAL_ALGO_SIMPLE) fail(XCAL_ERR_UNSUPPORTED, "batch: steady SIMPLE cases only");
-        if (c->has_k()) fail(XCAL_ERR_UNSUPPORTED, "batch: k-omega and k-equation LES cases run alone");
         if (cases.empty()) return;
         const xcal_config& a = cases[0]->cfg;
         const xcal_config& b = c->cfg;
@@ -714,9 +713,19 @@ struct Batch {
                     c->grad_p();
                 }
                 c->correct();
-                c->turbulence();
+                if (!c->has_k()) c->turbulence();
             },
             ncorr > 0 ? 7 : 4);
+        // turbulence with transported k (and omega): each case's own k /
+        // omega solves (host-polled Krylov on its stream, on the p system's
+        // storage, which the next iteration's pressure assembly rewrites),
+        // so this phase runs uncaptured
+        bool any_k = false;
+        for (Case* c : cases) any_k = any_k || c->has_k();
+        if (any_k)
+            per_case([&](Case* c) {
+                if (c->has_k()) c->turbulence();
+            });
         XCAL_CUDA(cudaMemcpyAsync(hres, res.p, 4 * cases.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
         sync();
         const clk::time_point t4 = clk::now();

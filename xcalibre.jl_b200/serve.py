@@ -401,6 +401,33 @@ class Server:
         return sorted(results, key=lambda r: r.rid)
 
 
+def shard_requests(requests: list[Request], rank: int, world: int) -> list[Request]:
+    """The requests one of `world` servers takes (one process per GPU, each
+    with its own Server): request i goes to rank i mod world, arrival times
+    unchanged, so every rank sees the same stream rate divided by world."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must lie in [0, world)")
+    return [r for r in requests if r.rid % world == rank]
+
+
+def result_record(r: Result) -> tuple:
+    """A Result without its field arrays, for gathering across ranks."""
+    return (r.rid, r.n_cells, r.arrival, r.admitted, r.finished, r.iterations, bool(r.converged), r.status,
+            r.error)
+
+
+def merge_records(parts: list[list[tuple]]) -> list[Result]:
+    """Every rank's result records as Results, in request order; each request
+    must appear exactly once."""
+    out = [Result(rid=t[0], n_cells=t[1], arrival=t[2], admitted=t[3], finished=t[4], iterations=t[5],
+                  converged=t[6], residuals=np.zeros(0), status=t[7], error=t[8]) for part in parts for t in part]
+    out.sort(key=lambda r: r.rid)
+    rids = [r.rid for r in out]
+    if len(set(rids)) != len(rids):
+        raise ValueError("a request was served by more than one rank")
+    return out
+
+
 def summarize(results: list[Result], wall: float) -> dict:
     """Throughput and time-to-result over the solved requests (rejected and
     failed ones are counted, not timed)."""
