@@ -64,7 +64,7 @@ const BC_NUT_WALL = Int32(13)
 const TIME_STEADY, TIME_EULER = Int32(0), Int32(1)
 const DIV_LINEAR, DIV_UPWIND, DIV_LUST = Int32(0), Int32(1), Int32(2)
 const GRAD_GAUSS, GRAD_MIDPOINT = Int32(0), Int32(1)
-const LIMITER_NONE, LIMITER_CELL = Int32(0), Int32(1)
+const LIMITER_NONE, LIMITER_CELL, LIMITER_FACE = Int32(0), Int32(1), Int32(2)
 const SOLVER_CG, SOLVER_BICGSTAB = Int32(0), Int32(1)
 const PRECOND_NONE, PRECOND_JACOBI, PRECOND_DILU = Int32(0), Int32(1), Int32(2)
 const TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST, TURB_KEQUATION =
@@ -384,9 +384,14 @@ grad_kind(g) = g === XCALibre.Discretise.Midpoint ? GRAD_MIDPOINT : GRAD_GAUSS
 function schemes_desc(s)
     lim, level = LIMITER_NONE, 0.0
     if hasproperty(s, :limiter) && s.limiter !== nothing
-        nameof(typeof(s.limiter)) == :CellBased ||
-            error("libxcal_b200: limiter $(typeof(s.limiter)) is not on the B200 path (CellBased)")
-        lim, level = LIMITER_CELL, Float64(s.limiter.level)
+        lname = nameof(typeof(s.limiter))
+        if lname == :CellBased
+            lim, level = LIMITER_CELL, Float64(s.limiter.level)
+        elseif lname == :FaceBased
+            lim = LIMITER_FACE
+        else
+            error("libxcal_b200: limiter $(typeof(s.limiter)) is not on the B200 path (CellBased, FaceBased)")
+        end
     end
     SchemesDesc(time_kind(s.time), div_kind(s.divergence), grad_kind(s.gradient), lim, level)
 end

@@ -63,7 +63,10 @@ enum { XCAL_GRAD_GAUSS = 0, XCAL_GRAD_MIDPOINT = 1 };
 /* gradient limiters: none, or CellBased (Calculate_0_gradient_cell_limiter.jl,
  * Barth-Jespersen, strength level); p_schemes: after every grad p, U_schemes:
  * after grad U in the turbulence update, per component (nut after it) */
-enum { XCAL_LIMITER_NONE = 0, XCAL_LIMITER_CELL = 1 };
+/* CellBased(level) (Calculate_0_gradient_cell_limiter.jl); FaceBased
+ * (Calculate_0_gradient_face_limiter.jl: per cell the minimum over its
+ * internal faces, no level) */
+enum { XCAL_LIMITER_NONE = 0, XCAL_LIMITER_CELL = 1, XCAL_LIMITER_FACE = 2 };
 /* Krylov solver: src/Solve/Solve_1_Krylov_solvers.jl:6-15 */
 enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
 /* preconditioner: src/Solve/Preconditioners/preconditioners_0_types.jl */

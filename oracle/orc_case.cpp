@@ -1064,11 +1064,75 @@ static void limit_cell(Case& C, const std::vector<double>& F, std::vector<double
     }
 }
 
+// limit_gradient!(FaceBased) (Calculate_0_gradient_face_limiter.jl:31-92,
+// 152-170): each internal face lowers both cells' limiters (an atomic
+// minimum in the reference, so a cell's limiter is the smallest candidate
+// of its faces and 1 in any order; here each cell's faces in turn).  Per
+// face the bounds min/max(F_owner, F_neighbour) widened by their difference,
+// the cell's extrapolated change dF = grad . (fc - cc) and the candidate
+// (Fmax - F)/dF (dF > Fmax - F) or (Fmin - F)/dF (dF < Fmin - F); then
+// grad *= limiter.
+static void lower_limiter(double& lim, double Fmax, double Fmin, double dF, double F) {
+    const double dmax = Fmax - F, dmin = Fmin - F;
+    if (dF > dmax) {
+        const double v = dmax / dF;
+        if (v < lim) lim = v;
+    } else if (dF < dmin) {
+        const double v = dmin / dF;
+        if (v < lim) lim = v;
+    }
+}
+static void limit_face_scalar(Case& C, const std::vector<double>& F, std::vector<double>* g) {
+    const Mesh& m = *C.m;
+    for (int i = 0; i < C.nC; ++i) {
+        const V3 g0 = {g[0][i], g[1][i], g[2][i]};
+        double lim = 1.0;
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            const int f = m.cell_faces[k];
+            const double F1 = F[m.owner[f]], F2 = F[m.neigh[f]];
+            double mn = jl_min(F1, F2), mx = jl_max(F1, F2);
+            const double dl = mx - mn;
+            mn = mn - dl;
+            mx = mx + dl;
+            lower_limiter(lim, mx, mn, dot(g0, m.fcentre[f] - m.ccentre[i]), F[i]);
+        }
+        g[0][i] = g0.x * lim;
+        g[1][i] = g0.y * lim;
+        g[2][i] = g0.z * lim;
+    }
+}
+// the vector form (:94-151): gradf = grad U (fc - cc) (row a . d), both
+// cells' U projected on it, measure gradf . gradf; one limiter per cell
+// scales all nine components
+static void limit_face_vector(Case& C, std::vector<double>* g) {
+    const Mesh& m = *C.m;
+    for (int i = 0; i < C.nC; ++i) {
+        double lim = 1.0;
+        for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+            const int f = m.cell_faces[k];
+            const V3 d = m.fcentre[f] - m.ccentre[i];
+            double gf[3];
+            for (int a = 0; a < 3; ++a)
+                gf[a] = (g[3 * a][i] * d.x + g[3 * a + 1][i] * d.y) + g[3 * a + 2][i] * d.z;
+            const int o = m.owner[f], n = m.neigh[f];
+            const double vOwn = (gf[0] * C.U[0][o] + gf[1] * C.U[1][o]) + gf[2] * C.U[2][o];
+            const double vNei = (gf[0] * C.U[0][n] + gf[1] * C.U[1][n]) + gf[2] * C.U[2][n];
+            double mx = jl_max(vOwn, vNei), mn = jl_min(vOwn, vNei);
+            const double dl = mx - mn;
+            mx = mx + dl;
+            mn = mn - dl;
+            lower_limiter(lim, mx, mn, (gf[0] * gf[0] + gf[1] * gf[1]) + gf[2] * gf[2], i == o ? vOwn : vNei);
+        }
+        for (int q = 0; q < 9; ++q) g[q][i] = g[q][i] * lim;
+    }
+}
+
 static void grad_p_only(Case& C);
 
 static void grad_p(Case& C) {
     grad_p_only(C);
     if (C.cfg.p_schemes.limiter == XCAL_LIMITER_CELL) limit_cell(C, C.p, C.gradp, C.cfg.p_schemes.limiter_level);
+    if (C.cfg.p_schemes.limiter == XCAL_LIMITER_FACE) limit_face_scalar(C, C.p, C.gradp);
 }
 
 static void grad_p_only(Case& C) {
@@ -1099,6 +1163,7 @@ static void grad_U(Case& C) {  // grad! + limit_gradient!(schemes.U.limiter) (RA
     grad_U_only(C);
     if (C.cfg.U_schemes.limiter == XCAL_LIMITER_CELL)
         for (int a = 0; a < 3; ++a) limit_cell(C, C.U[a], C.gradU + 3 * a, C.cfg.U_schemes.limiter_level);
+    if (C.cfg.U_schemes.limiter == XCAL_LIMITER_FACE) limit_face_vector(C, C.gradU);
 }
 
 static void grad_U_only(Case& C) {

@@ -1,5 +1,5 @@
-"""Non-orthogonal correctors, Midpoint gradients and the CellBased gradient
-limiter on the GPU against the oracle (skewed channel, FP64, host-polled and
+"""Non-orthogonal correctors, Midpoint gradients and the CellBased and FaceBased
+gradient limiters on the GPU against the oracle (skewed channel, FP64, host-polled and
 graph mode; tolerance the 1e-10 relative L2 of the parity tests, expected 0),
 and a batch of skewed cases with correctors (and limiters) giving the results
 the cases give alone (bit for bit)."""
@@ -149,6 +149,34 @@ def test_limiter_parity(x, orc, ctx, grad, p_level, U_level, ncorr, graph):
     for f in (x._abi.FIELD_U, x._abi.FIELD_P, x._abi.FIELD_GRADP, x._abi.FIELD_GRADU):
         assert rel(g.get_field(f), o.get_field(f)) <= TOL, f
 
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("grad", ["gauss", "midpoint"])
+def test_face_limiter_parity(x, orc, ctx, grad, graph):
+    """Schemes(limiter=FaceBased) for p (scalar form) and U (tensor form) on
+    the skewed channel with a corrector: GPU equal to the oracle."""
+    mesh = skewed_channel(x, n=(12, 7, 6), seed=10)
+    model, config = x.cases.channel_case(mesh, iterations=4)
+    config.schemes["p"].limiter = x.api.FaceBased(mesh)
+    config.schemes["U"].limiter = x.api.FaceBased(mesh)
+    if grad == "midpoint":
+        config.schemes["p"].gradient = x.api.Midpoint
+        config.schemes["U"].gradient = x.api.Midpoint
+    cfg, keep = x.build_config(model, config, ncorrectors=1)
+    dm = x.DeviceMesh(ctx, mesh)
+    g = x.Case(dm, cfg)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    for c in (g, o):
+        c.set_field(x._abi.FIELD_U, model.momentum.U)
+        c.set_field(x._abi.FIELD_P, model.momentum.p)
+    if graph:
+        g.set_graph_mode(True)
+    rg, _ = g.simple_iterate(4)
+    ro, _ = o.simple_iterate(4)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    for f in (x._abi.FIELD_U, x._abi.FIELD_P, x._abi.FIELD_GRADP, x._abi.FIELD_GRADU):
+        assert rel(g.get_field(f), o.get_field(f)) <= TOL, f
 
 def test_limiter_les_piso_parity(x, orc, ctx):
     """PISO + Smagorinsky with the grad U limiter (nut from the limited

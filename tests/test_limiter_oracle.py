@@ -3,7 +3,14 @@ applied after every grad p, Solvers_1_SIMPLE.jl:154/193/206, and after grad U
 in the turbulence update, RANS_laminar.jl:77) on the CPU oracle, skewed
 channel: with level 1 every gradient-extrapolated face value stays inside the
 cell's neighbour range (Barth-Jespersen bound); level 0 gives the unlimited
-run bit for bit; the API checks level and refuses the face-based limiters."""
+run bit for bit; the API checks level and refuses MFaceBased.
+
+FaceBased (Calculate_0_gradient_face_limiter.jl): after limiting, every
+cell's gradient, extrapolated to each of its internal faces, stays inside
+the bounds min/max(F_owner, F_neighbour) widened by their difference (the
+scalar form, checked for p); the vector form leaves every cell's gradient a
+non-negative multiple (at most 1) of the unlimited one computed from the same
+fields."""
 import numpy as np
 import pytest
 
@@ -69,6 +76,51 @@ def test_limiter_api(x):
         x.api.CellBased(-0.1)
     mesh = skewed_channel(x, n=(4, 3, 3))
     model, config = x.cases.channel_case(mesh, iterations=1)
-    config.schemes["p"].limiter = x.api.FaceBased(mesh)
+    config.schemes["p"].limiter = x.api.MFaceBased(mesh)
     with pytest.raises(NotImplementedError):
         x.build_config(model, config)
+    config.schemes["p"].limiter = x.api.FaceBased(mesh)
+    cfg, keep = x.build_config(model, config)
+    assert cfg.p_schemes.limiter == x._abi.LIMITER_FACE
+
+
+def _check_face_bound(mesh, F, g):
+    """F_P + (fc - cc).g within [min - d, max + d] of the face's two cells'
+    values, d = max - min, for every internal face of every cell."""
+    off, cf, nb = mesh.cell_faces_offset, mesh.cell_faces, mesh.cell_neighbours
+    fc, cc = np.asarray(mesh.face_centre), np.asarray(mesh.cell_centre)
+    cells = np.repeat(np.arange(mesh.n_cells), np.diff(off))
+    d = fc[cf] - cc[cells]
+    ext = F[cells] + np.einsum("kd,dk->k", d, g[:, cells])
+    hi = np.maximum(F[nb], F[cells])
+    lo = np.minimum(F[nb], F[cells])
+    w = hi - lo
+    tol = 1e-9 * (np.ptp(F) + 1e-300)
+    assert np.all(ext <= hi + w + tol) and np.all(ext >= lo - w - tol)
+
+
+def test_face_limiter_bounds(x, orc):
+    mesh = skewed_channel(x, seed=7)
+    res0, f0 = _run(x, orc, mesh)
+    res1, f1 = _run(x, orc, mesh, p_lim=x.api.FaceBased(mesh), U_lim=x.api.FaceBased(mesh))
+    assert np.all(np.isfinite(res1))
+    assert not np.array_equal(f0[x._abi.FIELD_GRADP], f1[x._abi.FIELD_GRADP])
+    _check_face_bound(mesh, f1[x._abi.FIELD_P], f1[x._abi.FIELD_GRADP])
+    with pytest.raises(AssertionError):
+        _check_face_bound(mesh, f0[x._abi.FIELD_P], f0[x._abi.FIELD_GRADP])
+
+
+def test_face_limiter_vector_scales(x, orc):
+    """The vector form scales each cell's whole gradient tensor by one
+    factor in [0, 1]: one oracle iteration with and without it from the same
+    state gives gradients in that ratio, cell by cell."""
+    mesh = skewed_channel(x, seed=8)
+    res, f = _run(x, orc, mesh, iters=1)
+    _, fl = _run(x, orc, mesh, U_lim=x.api.FaceBased(mesh), iters=1)
+    G0, G1 = f[x._abi.FIELD_GRADU], fl[x._abi.FIELD_GRADU]
+    n0 = np.linalg.norm(G0, axis=0)
+    ok = n0 > 0
+    ratio = np.linalg.norm(G1, axis=0)[ok] / n0[ok]
+    assert np.all(ratio <= 1.0 + 1e-12) and np.all(ratio >= 0.0) and np.any(ratio < 1.0)
+    # parallel: G1 = ratio * G0 per cell
+    assert np.allclose(G1[:, ok], G0[:, ok] * ratio, rtol=1e-12, atol=0.0)

@@ -69,15 +69,22 @@ class CellBased:
 
 
 class FaceBased:
-    """Face-based limiter: not implemented (the reference's is marked
-    experimental and updates shared cells from concurrent face threads)."""
+    """Face-based gradient limiter (Calculate_0_gradient_face_limiter.jl):
+    per cell the smallest ratio over its internal faces, bounds widened by
+    the two cells' difference; FaceBased(mesh) as in the reference (the mesh
+    argument is not needed)."""
 
     def __init__(self, *a, **k):
         pass
 
 
-class MFaceBased(FaceBased):
-    pass
+class MFaceBased:
+    """The modified face-based limiter: not implemented (each face thread
+    rewrites both cells' gradients while other faces read them, so the
+    reference's result depends on thread order)."""
+
+    def __init__(self, *a, **k):
+        pass
 
 
 class Cg: ...
@@ -574,7 +581,9 @@ def _limiter(lim):
         return _abi.LIMITER_NONE, 0.0
     if isinstance(lim, CellBased):
         return _abi.LIMITER_CELL, float(lim.level)
-    raise NotImplementedError("only the CellBased gradient limiter is implemented")
+    if _kind(lim) is FaceBased:
+        return _abi.LIMITER_FACE, 0.0
+    raise NotImplementedError("the CellBased and FaceBased gradient limiters are implemented (not MFaceBased)")
 
 
 def _solver_desc(s: SolverSetup) -> _abi.SolverSetupDesc:

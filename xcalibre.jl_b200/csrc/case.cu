@@ -776,12 +776,12 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
          (cfg.k_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.y_schemes.gradient == XCAL_GRAD_MIDPOINT)))
         build_midpoint(*m, stream);
     for (const xcal_schemes* sc : {&cfg.U_schemes, &cfg.p_schemes}) {
-        if (sc->limiter != XCAL_LIMITER_NONE && sc->limiter != XCAL_LIMITER_CELL)
-            fail(XCAL_ERR_UNSUPPORTED, "gradient limiter: only CellBased is implemented");
+        if (sc->limiter != XCAL_LIMITER_NONE && sc->limiter != XCAL_LIMITER_CELL && sc->limiter != XCAL_LIMITER_FACE)
+            fail(XCAL_ERR_UNSUPPORTED, "gradient limiter: CellBased or FaceBased");
         if (sc->limiter == XCAL_LIMITER_CELL && !(sc->limiter_level >= 0.0 && sc->limiter_level <= 1.0))
             fail(XCAL_ERR_INVALID, "CellBased limiter level must be in [0, 1]");
     }
-    if (cfg.U_schemes.limiter == XCAL_LIMITER_CELL || cfg.p_schemes.limiter == XCAL_LIMITER_CELL)
+    if (cfg.U_schemes.limiter != XCAL_LIMITER_NONE || cfg.p_schemes.limiter != XCAL_LIMITER_NONE)
         build_limiter(*m, stream);
     for (int d = 0; d < 3; ++d) {
         Uc[d].zero(stream);
@@ -1979,6 +1979,8 @@ void Case::grad_p() {
     }
     if (cfg.p_schemes.limiter == XCAL_LIMITER_CELL)
         launch_limit_cell(stream, mv(), limD.p, p.p, gp, cfg.p_schemes.limiter_level);
+    else if (cfg.p_schemes.limiter == XCAL_LIMITER_FACE)
+        launch_limit_face_scalar(stream, mv(), limD.p, p.p, gp);
 }
 
 // fc - cc per cell_faces entry (storage order), 3 arrays of 2 nI
@@ -2024,7 +2026,7 @@ void Case::turbulence() {
     double* g[9];
     for (int q = 0; q < 9; ++q) g[q] = gradU[q].p;
     const bool les = cfg.turbulence == XCAL_TURB_SMAGORINSKY;  // nut from grad U alone
-    const bool limit = cfg.U_schemes.limiter == XCAL_LIMITER_CELL;
+    const bool limit = cfg.U_schemes.limiter != XCAL_LIMITER_NONE;
     // nut fused into the last Green-Gauss pass unless the limiter comes between
     double* nut_gg = les && !limit ? nut.p : nullptr;
     if (cfg.U_schemes.gradient == XCAL_GRAD_MIDPOINT) {
@@ -2042,9 +2044,13 @@ void Case::turbulence() {
     }
     if (limit) {
         // limit_gradient!(schemes.U.limiter, gradU, U) (RANS_laminar.jl:77,
-        // LES_Smagorinsky.jl:120): the CellBased kernel once per component
-        for (int a = 0; a < 3; ++a)
-            launch_limit_cell(stream, mv(), limD.p, Uc[a].p, g + 3 * a, cfg.U_schemes.limiter_level);
+        // LES_Smagorinsky.jl:120): CellBased once per component row,
+        // FaceBased once for the tensor
+        if (cfg.U_schemes.limiter == XCAL_LIMITER_FACE)
+            launch_limit_face_vector(stream, mv(), limD.p, Ucp, g);
+        else
+            for (int a = 0; a < 3; ++a)
+                launch_limit_cell(stream, mv(), limD.p, Uc[a].p, g + 3 * a, cfg.U_schemes.limiter_level);
         if (les) launch_smag_nut(stream, mesh->nC, g, Delta.p, nut.p);
     }
     if (rans_kw())

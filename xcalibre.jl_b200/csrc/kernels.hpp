@@ -39,6 +39,12 @@ void launch_mid_correct_vector(cudaStream_t s, const MeshView& m, const double* 
                                const double* const g[9], double* const Uf[3]);
 // CellBased gradient limiter of grad F, F a scalar field or one component of
 // U with its row of grad U (D: Case::build_limiter)
+// limit_gradient!(FaceBased) of a scalar's gradient (3 arrays) / a vector's
+// (9 arrays, one limiter per cell for all nine); D as for launch_limit_cell
+void launch_limit_face_scalar(cudaStream_t s, const MeshView& m, const double* D, const double* F,
+                              double* const g[3]);
+void launch_limit_face_vector(cudaStream_t s, const MeshView& m, const double* D, const double* const U[3],
+                              double* const g[9]);
 void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const double* F, double* const g[3],
                        double level);
 // RANS{KOmega}: sources, k / omega assembly, BCs + relaxation, the omega

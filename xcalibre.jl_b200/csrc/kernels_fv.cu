@@ -1162,6 +1162,91 @@ __global__ void k_limit_cell(MeshView m, const double* __restrict__ D, const dou
     gz[i] = z * lim;
 }
 
+// limit_gradient!(FaceBased) (Calculate_0_gradient_face_limiter.jl:31-113,
+// 152-170) as a gather, one thread per cell.  The reference runs one thread
+// per internal face, each lowering both of its cells' limiters with an
+// atomic minimum (compare-and-swap while the value is smaller); a cell's
+// limiter is thus the smallest of its faces' candidate ratios and 1, the
+// same in any order -- here its faces in cell_faces order.  Per face: the
+// bounds min/max(F_own, F_nei) widened by their difference, this cell's
+// extrapolated change dF = grad . (fc - cc) (D), and the candidate
+// (Fmax - F)/dF when dF > Fmax - F, (Fmin - F)/dF when dF < Fmin - F; then
+// grad *= limiter.
+__global__ void k_limit_face_scalar(MeshView m, const double* __restrict__ D, const double* __restrict__ F,
+                                    double* gx, double* gy, double* gz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    const int nk = 2 * (m.nF - m.nB);
+    const double x = gx[i], y = gy[i], z = gz[i];
+    const double Fi = F[i];
+    double lim = 1.0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        const double Fo = F[m.cf_nb[k]];
+        const bool own = m.cf_sign[k] > 0;
+        double mn = own ? jl_min(Fi, Fo) : jl_min(Fo, Fi);
+        double mx = own ? jl_max(Fi, Fo) : jl_max(Fo, Fi);
+        const double dl = mx - mn;
+        mn = mn - dl;
+        mx = mx + dl;
+        const double dF = (x * D[k] + y * D[nk + k]) + z * D[2 * nk + k];
+        const double dmax = mx - Fi, dmin = mn - Fi;
+        if (dF > dmax) {
+            const double v = dmax / dF;
+            if (v < lim) lim = v;
+        } else if (dF < dmin) {
+            const double v = dmin / dF;
+            if (v < lim) lim = v;
+        }
+    }
+    gx[i] = x * lim;
+    gy[i] = y * lim;
+    gz[i] = z * lim;
+}
+
+// the vector form (:94-151, OpenFOAM's faceLimitedGrad<vector>): per face
+// side the gradient tensor times (fc - cc) gives gradf; both cells' values
+// projected on it bound this cell's projected value, the extrapolation
+// measure is gradf . gradf; one limiter scales all nine components.
+// G[a][b] = g[3 a + b] is entry (a, b) of the tensor.
+struct GradW9 {
+    double* g[9];
+};
+__global__ void k_limit_face_vector(MeshView m, const double* __restrict__ D, const double* __restrict__ U0,
+                                    const double* __restrict__ U1, const double* __restrict__ U2, GradW9 Gd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    const int nk = 2 * (m.nF - m.nB);
+    double G[9];
+    for (int q = 0; q < 9; ++q) G[q] = Gd.g[q][i];
+    const double ui[3] = {U0[i], U1[i], U2[i]};
+    double lim = 1.0;
+    for (int k = m.cf_off[i]; k < m.cf_off[i + 1]; ++k) {
+        const int o = m.cf_nb[k];
+        const double uo[3] = {U0[o], U1[o], U2[o]};
+        const double d[3] = {D[k], D[nk + k], D[2 * nk + k]};
+        double gf[3];
+        for (int a = 0; a < 3; ++a) gf[a] = (G[3 * a] * d[0] + G[3 * a + 1] * d[1]) + G[3 * a + 2] * d[2];
+        const double vi = (gf[0] * ui[0] + gf[1] * ui[1]) + gf[2] * ui[2];
+        const double vo = (gf[0] * uo[0] + gf[1] * uo[1]) + gf[2] * uo[2];
+        const bool own = m.cf_sign[k] > 0;
+        const double vOwn = own ? vi : vo, vNei = own ? vo : vi;
+        double mx = jl_max(vOwn, vNei), mn = jl_min(vOwn, vNei);
+        const double dl = mx - mn;
+        mx = mx + dl;
+        mn = mn - dl;
+        const double dF = (gf[0] * gf[0] + gf[1] * gf[1]) + gf[2] * gf[2];
+        const double dmax = mx - vi, dmin = mn - vi;
+        if (dF > dmax) {
+            const double v = dmax / dF;
+            if (v < lim) lim = v;
+        } else if (dF < dmin) {
+            const double v = dmin / dF;
+            if (v < lim) lim = v;
+        }
+    }
+    for (int q = 0; q < 9; ++q) Gd.g[q][i] = G[q] * lim;
+}
+
 // nonorthogonal_face_correction (Solvers_1_SIMPLE.jl:267-318), one thread
 // per cell: b_i gets each of its internal faces' correction, in its
 // cell_faces order (+ as owner, - as neighbour; the reference adds with
@@ -1441,6 +1526,18 @@ void launch_mid_correct_vector(cudaStream_t s, const MeshView& m, const double* 
 void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const double* F, double* const g[3],
                        double level) {
     k_limit_cell<<<nblk(m.nC), TPB, 0, s>>>(m, D, F, g[0], g[1], g[2], level);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_limit_face_scalar(cudaStream_t s, const MeshView& m, const double* D, const double* F,
+                              double* const g[3]) {
+    k_limit_face_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, D, F, g[0], g[1], g[2]);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_limit_face_vector(cudaStream_t s, const MeshView& m, const double* D, const double* const U[3],
+                              double* const g[9]) {
+    GradW9 G;
+    for (int q = 0; q < 9; ++q) G.g[q] = g[q];
+    k_limit_face_vector<<<nblk(m.nC), TPB, 0, s>>>(m, D, U[0], U[1], U[2], G);
     XCAL_CHECK_LAUNCH();
 }
 void launch_kw_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* omega,
