@@ -19,8 +19,8 @@ With `Hardware(backend=B200Backend(), workgroup=32)` in the configuration,
 its user API (`Physics`, `assign`, `SolverSetup`, `Schemes`, `Runtime`,
 `Configuration`, `initialise!`): `simple!` / `piso!` below marshal the mesh,
 boundary conditions and configuration once, run every iteration in the
-library, and copy U, p (and k, omega, nut where the model has them) back into
-the model's fields.  Residual histories come back as the reference returns
+library, and copy U, p (and k, omega, kl, nut where the model has them) back
+into the model's fields.  Residual histories come back as the reference returns
 them, `(Ux=..., Uy=..., Uz=..., p=...)`.
 
 The structs below mirror the C structs field for field; `__init__` compares
@@ -67,12 +67,13 @@ const GRAD_GAUSS, GRAD_MIDPOINT = Int32(0), Int32(1)
 const LIMITER_NONE, LIMITER_CELL, LIMITER_FACE = Int32(0), Int32(1), Int32(2)
 const SOLVER_CG, SOLVER_BICGSTAB = Int32(0), Int32(1)
 const PRECOND_NONE, PRECOND_JACOBI, PRECOND_DILU = Int32(0), Int32(1), Int32(2)
-const TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST, TURB_KEQUATION =
-    Int32(0), Int32(1), Int32(2), Int32(3), Int32(4)
+const TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST, TURB_KEQUATION, TURB_KOMEGA_LKE =
+    Int32(0), Int32(1), Int32(2), Int32(3), Int32(4), Int32(5)
 const PREC_FP64, PREC_MIXED = Int32(0), Int32(1)
 const ALGO_SIMPLE, ALGO_PISO = Int32(0), Int32(1)
 
-const FIELD_U, FIELD_P, FIELD_NUT, FIELD_K, FIELD_OMEGA = Int32(0), Int32(1), Int32(9), Int32(15), Int32(16)
+const FIELD_U, FIELD_P, FIELD_NUT, FIELD_K, FIELD_OMEGA, FIELD_KL =
+    Int32(0), Int32(1), Int32(9), Int32(15), Int32(16), Int32(21)
 
 # xcal_abi_layout selectors
 const LAYOUT_MESH_DESC, LAYOUT_BC, LAYOUT_SOLVER_SETUP, LAYOUT_SCHEMES, LAYOUT_CONFIG =
@@ -189,6 +190,11 @@ struct ConfigDesc
     bc_y::Ptr{BCDesc}
     keq_ck::Float64
     keq_ce::Float64
+    lke_Tu::Float64
+    kl_schemes::SchemesDesc
+    kl_solver::SolverSetupDesc
+    n_bc_kl::Int32
+    bc_kl::Ptr{BCDesc}
 end
 
 # xcal_term / xcal_source: one operator / source of an equation built with
@@ -413,7 +419,7 @@ function config_desc(model, config; pref=nothing, inner_loops=0, ncorrectors=0, 
     tname = nameof(typeof(turb))
     tk = tname == :Laminar ? TURB_LAMINAR : tname == :Smagorinsky ? TURB_SMAGORINSKY :
          tname == :KOmega ? TURB_KOMEGA : tname == :KOmegaSST ? TURB_KOMEGA_SST :
-         tname == :KEquation ? TURB_KEQUATION :
+         tname == :KEquation ? TURB_KEQUATION : tname == :KOmegaLKE ? TURB_KOMEGA_LKE :
          error("libxcal_b200: turbulence model $(tname) is not on the B200 path")
     time = 0.0
     keep = Any[]
@@ -424,7 +430,8 @@ function config_desc(model, config; pref=nothing, inner_loops=0, ncorrectors=0, 
     bk, kk = tab(:k, 1)
     bw, kw = tab(:omega, 1)
     by, ky = tab(:y, 1)
-    append!(keep, (bU, bp, bnut, bk, bw, by, kU, kp, knut, kk, kw, ky))
+    bkl, kkl = tab(:kl, 1)
+    append!(keep, (bU, bp, bnut, bk, bw, by, bkl, kU, kp, knut, kk, kw, ky, kkl))
     ptr(v) = isempty(v) ? Ptr{BCDesc}(C_NULL) : pointer(v)
     C = tk == TURB_SMAGORINSKY ? Float64(turb.coeffs.C) : 0.0
     kwc = tk in (TURB_KOMEGA, TURB_KOMEGA_SST) ? turb.coeffs : nothing
@@ -448,7 +455,9 @@ function config_desc(model, config; pref=nothing, inner_loops=0, ncorrectors=0, 
         gs(:β2), gs(:σk2), gs(:σω2),
         schemes_desc(getopt(schemes, :y)), solver_desc(getopt(solvers, :y)),
         Int32(length(by)), ptr(by),
-        tk == TURB_KEQUATION ? Float64(turb.coeffs.ck) : 0.0, tk == TURB_KEQUATION ? Float64(turb.coeffs.ce) : 0.0)
+        tk == TURB_KEQUATION ? Float64(turb.coeffs.ck) : 0.0, tk == TURB_KEQUATION ? Float64(turb.coeffs.ce) : 0.0,
+        tk == TURB_KOMEGA_LKE ? Float64(turb.Tu) : 0.0,
+        schemes_desc(getopt(schemes, :kl)), solver_desc(getopt(solvers, :kl)), Int32(length(bkl)), ptr(bkl))
     return desc, keep
 end
 
@@ -491,10 +500,11 @@ function b200_run(model, config, algorithm; pref=nothing, ncorrectors=0, inner_l
         (; U, p) = model.momentum
         set_field!(ctx[], case[], FIELD_U, vcat(U.x.values, U.y.values, U.z.values))
         set_field!(ctx[], case[], FIELD_P, Vector{Float64}(p.values))
-        komega = hasproperty(model.turbulence, :k) && hasproperty(model.turbulence, :omega)
-        if komega
-            set_field!(ctx[], case[], FIELD_K, Vector{Float64}(model.turbulence.k.values))
-            set_field!(ctx[], case[], FIELD_OMEGA, Vector{Float64}(model.turbulence.omega.values))
+        # the turbulence fields the model has (k, omega, kl, nut)
+        tfields = [(s, id) for (s, id) in ((:k, FIELD_K), (:omega, FIELD_OMEGA), (:kl, FIELD_KL), (:nut, FIELD_NUT))
+                   if hasproperty(model.turbulence, s)]
+        for (s, id) in tfields
+            set_field!(ctx[], case[], id, Vector{Float64}(getproperty(model.turbulence, s).values))
         end
         be.graph && check(ctx[], ccall((:xcal_case_set_graph_mode, libxcal), Int32, (Ptr{Cvoid}, Int32), case[], 1))
         n = Int32(config.runtime.iterations)
@@ -517,12 +527,8 @@ function b200_run(model, config, algorithm; pref=nothing, ncorrectors=0, inner_l
         U.y.values .= @view Uh[nC+1:2nC]
         U.z.values .= @view Uh[2nC+1:3nC]
         p.values .= get_field!(ctx[], case[], FIELD_P, Vector{Float64}(undef, nC))
-        if komega
-            model.turbulence.k.values .= get_field!(ctx[], case[], FIELD_K, Vector{Float64}(undef, nC))
-            model.turbulence.omega.values .= get_field!(ctx[], case[], FIELD_OMEGA, Vector{Float64}(undef, nC))
-        end
-        if hasproperty(model.turbulence, :nut)
-            model.turbulence.nut.values .= get_field!(ctx[], case[], FIELD_NUT, Vector{Float64}(undef, nC))
+        for (s, id) in tfields
+            getproperty(model.turbulence, s).values .= get_field!(ctx[], case[], id, Vector{Float64}(undef, nC))
         end
         # solve_system! warns for every solve that stopped at itmax
         # (Solve_1_api.jl:302); the library counts them

@@ -77,14 +77,17 @@ enum {
     XCAL_TURB_SMAGORINSKY = 1,
     XCAL_TURB_KOMEGA = 2,
     XCAL_TURB_KOMEGA_SST = 3,
-    XCAL_TURB_KEQUATION = 4  /* LES{KEquation} (LES_KEquation.jl) */
+    XCAL_TURB_KEQUATION = 4,  /* LES{KEquation} (LES_KEquation.jl) */
+    XCAL_TURB_KOMEGA_LKE = 5  /* RANS{KOmegaLKE} (RANS_kOmegaLKE.jl): k, omega
+                                 and the laminar kinetic energy kl */
 };
 /* arithmetic of the Krylov inner iterations */
 enum { XCAL_PREC_FP64 = 0, XCAL_PREC_MIXED = 1 };
 /* pressure-velocity algorithm: run! dispatch, src/Solvers/Solvers_3_solver_dispatch.jl:120,225 */
 enum { XCAL_ALGO_SIMPLE = 0, XCAL_ALGO_PISO = 1 };
 /* equations (k, omega: RANS{KOmega} transport equations) */
-enum { XCAL_EQN_U = 0, XCAL_EQN_P = 1, XCAL_EQN_K = 2, XCAL_EQN_OMEGA = 3, XCAL_EQN_WALLDIST = 4 };
+enum { XCAL_EQN_U = 0, XCAL_EQN_P = 1, XCAL_EQN_K = 2, XCAL_EQN_OMEGA = 3, XCAL_EQN_WALLDIST = 4,
+       XCAL_EQN_KL = 5 /* RANS{KOmegaLKE} laminar kinetic energy */ };
 
 /* field identifiers for xcal_case_get_field / xcal_case_set_field.
  * Cell fields hold n_cells values per component, face fields n_faces; vector
@@ -107,14 +110,16 @@ enum {
     XCAL_FIELD_RDF = 13,   /* rDf (n_faces)                                 */
     XCAL_FIELD_DELTA = 14, /* LES filter: (C*Delta)^2 (Smagorinsky), Delta
                               (KEquation) (n_cells)                     */
-    XCAL_FIELD_K = 15,     /* k: RANS{KOmega}, LES{KEquation} (n_cells)     */
-    XCAL_FIELD_OMEGA = 16, /* RANS{KOmega} omega (n_cells)                  */
-    XCAL_FIELD_WALLDIST = 17, /* RANS{KOmegaSST} wall distance y (n_cells)  */
+    XCAL_FIELD_K = 15,     /* k: RANS{KOmega*}, LES{KEquation} (n_cells)    */
+    XCAL_FIELD_OMEGA = 16, /* RANS{KOmega*} omega (n_cells)                 */
+    XCAL_FIELD_WALLDIST = 17, /* RANS{KOmegaSST, KOmegaLKE} wall distance y */
     XCAL_FIELD_PK = 18,    /* the k equation's Source (n_cells)             */
     XCAL_FIELD_DK = 19,    /* the k equation's Si coefficient (n_cells)     */
     XCAL_FIELD_DW = 20,    /* omega's Si coefficient (k-omega), the k
                               equation's second Si coefficient (KEquation) */
-    XCAL_FIELD_COUNT = 21
+    XCAL_FIELD_KL = 21,    /* RANS{KOmegaLKE} laminar kinetic energy kl     */
+    XCAL_FIELD_GAMMA = 22, /* RANS{KOmegaLKE} intermittency trigger gamma   */
+    XCAL_FIELD_COUNT = 23
 };
 
 /* ---- mesh: the Mesh3 contract (src/Mesh/Mesh_0_types.jl:28-205) ---------
@@ -262,6 +267,17 @@ typedef struct {
      * k_schemes / k_solver / bc_k, then nut = ck Delta sqrt(k) with Delta =
      * (V / les_delta_distance)^les_delta_power (:80-186) */
     double keq_ck, keq_ce;
+    /* RANS{KOmegaLKE}(; Tu, walls) (RANS_kOmegaLKE.jl:60-100): the
+     * freestream turbulence intensity Tu (eta = 0.02974 tanh(59.79 Tu^1.191
+     * + 1.65e-13); the other coefficients are the model's constants); k and
+     * omega use k_* / omega_* (each equation its own preconditioner), the
+     * laminar kinetic energy kl the fields below, the wall distance the y_*
+     * fields (Dirichlet 0 on the walls) */
+    double lke_Tu;
+    xcal_schemes kl_schemes;
+    xcal_solver_setup kl_solver;
+    int32_t n_bc_kl;
+    const xcal_bc* bc_kl;
 } xcal_config;
 
 /* ---- polyMesh input of the mesh importer --------------------------------
@@ -326,8 +342,9 @@ const char* xcal_version(void);
  * compute them alike (Cody-Waite reduction with a Taylor series for exp of
  * y <= 0; the atanh series for log of x > 0; tanh(x) = (1 - e^-2x) /
  * (1 + e^-2x) for x >= 0).  This evaluates those same functions, compiled
- * for the host, on n inputs: which 0 = exp, 1 = log, 2 = tanh; for testing
- * their error against the C library.  Needs no device. */
+ * for the host, on n inputs: which 0 = exp, 1 = log, 2 = tanh, 3 = x^-1.3
+ * (k-omega LKE's Re_upsilon^-1.30, exp(-1.3 log x)); for testing their error
+ * against the C library.  Needs no device. */
 int32_t xcal_det_math(int32_t which, const double* in, double* out, int64_t n);
 
 /* ---- struct layouts, for bindings -----------------------------------------

@@ -178,7 +178,7 @@ class OracleMesh:
 _FIELD_SHAPE = {0: (3, "cell"), 1: (1, "cell"), 2: (1, "face"), 3: (1, "face"), 4: (3, "cell"), 5: (9, "cell"),
                 6: (1, "cell"), 7: (3, "cell"), 8: (1, "cell"), 9: (1, "cell"), 10: (1, "face"), 11: (3, "face"),
                 12: (1, "face"), 13: (1, "face"), 14: (1, "cell"), 15: (1, "cell"), 16: (1, "cell"), 17: (1, "cell"),
-                18: (1, "cell"), 19: (1, "cell"), 20: (1, "cell")}
+                18: (1, "cell"), 19: (1, "cell"), 20: (1, "cell"), 21: (1, "cell"), 22: (1, "cell")}
 
 
 class OracleCase:

@@ -100,6 +100,8 @@ static std::vector<double>* field_ptr(Case* C, int field, int& ncomp, int& per) 
         case XCAL_FIELD_PK: return &C->Pk;
         case XCAL_FIELD_DK: return &C->Dk;
         case XCAL_FIELD_DW: return &C->Dw;
+        case XCAL_FIELD_KL: return C->kl.empty() ? nullptr : &C->kl;
+        case XCAL_FIELD_GAMMA: return C->gam.empty() ? nullptr : &C->gam;
         default: return nullptr;
     }
 }

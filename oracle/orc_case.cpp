@@ -113,13 +113,16 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     copy_bcs(*m, cfg->bc_p, cfg->n_bc_p, C->bcP, 1);
     copy_bcs(*m, cfg->bc_nut, cfg->n_bc_nut, C->bcNut, 1);
     C->cfg.bc_U = C->cfg.bc_p = C->cfg.bc_nut = nullptr;
-    if (cfg->turbulence == XCAL_TURB_KOMEGA || cfg->turbulence == XCAL_TURB_KOMEGA_SST) {
+    const bool lke = cfg->turbulence == XCAL_TURB_KOMEGA_LKE;
+    const bool has_y = cfg->turbulence == XCAL_TURB_KOMEGA_SST || lke;
+    if (cfg->turbulence == XCAL_TURB_KOMEGA || cfg->turbulence == XCAL_TURB_KOMEGA_SST || lke) {
         copy_bcs(*m, cfg->bc_k, cfg->n_bc_k, C->bcK, 1);
         copy_bcs(*m, cfg->bc_omega, cfg->n_bc_omega, C->bcOmega, 1);
     }
     if (cfg->turbulence == XCAL_TURB_KEQUATION) copy_bcs(*m, cfg->bc_k, cfg->n_bc_k, C->bcK, 1);
-    if (cfg->turbulence == XCAL_TURB_KOMEGA_SST) copy_bcs(*m, cfg->bc_y, cfg->n_bc_y, C->bcY, 1);
-    C->cfg.bc_k = C->cfg.bc_omega = C->cfg.bc_y = nullptr;
+    if (has_y) copy_bcs(*m, cfg->bc_y, cfg->n_bc_y, C->bcY, 1);
+    if (lke) copy_bcs(*m, cfg->bc_kl, cfg->n_bc_kl, C->bcKl, 1);
+    C->cfg.bc_k = C->cfg.bc_omega = C->cfg.bc_y = C->cfg.bc_kl = nullptr;
     int nC = C->nC, nF = C->nF;
     for (int d = 0; d < 3; ++d) {
         C->U[d].assign(nC, 0.0);
@@ -142,7 +145,15 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
     for (std::vector<double>* v : {&C->k, &C->omega, &C->Pk, &C->Pw, &C->Dk, &C->Dw, &C->Pkw}) v->assign(nC, 0.0);
     C->mueffk.assign(nF, 0.0);
     C->mueffw.assign(nF, 0.0);
-    if (cfg->turbulence == XCAL_TURB_KOMEGA_SST) {
+    if (lke) {
+        for (std::vector<double>* v : {&C->kl, &C->PkL, &C->DkL, &C->S2, &C->normU, &C->divU, &C->ReL, &C->gam,
+                                       &C->nueffS, &C->Pkl})
+            v->assign(nC, 0.0);
+        C->mueffl.assign(nF, 0.0);
+        // eta = 0.02974 tanh(59.79 Tu^1.191 + 1.65e-13) (RANS_kOmegaLKE.jl:97)
+        C->lke_eta = 0.02974 * det_tanh_pos(59.79 * det_pow(cfg->lke_Tu, 1.191) + 1.65e-13);
+    }
+    if (has_y) {
         for (std::vector<double>* v : {&C->yw, &C->F1, &C->F2, &C->Om, &C->D2, &C->Pww}) v->assign(nC, 0.0);
         for (int d = 0; d < 3; ++d) {
             C->gk[d].assign(nC, 0.0);
@@ -197,7 +208,7 @@ Case* case_create(const Mesh* m, const xcal_config* cfg) {
             C->Delta[i] = keq ? d : dc * dc;
         }
     }
-    if (cfg->turbulence == XCAL_TURB_KOMEGA_SST) wall_distance(*C);
+    if (has_y) wall_distance(*C);  // initialise (RANS_kOmegaSST.jl:167, RANS_kOmegaLKE.jl:236)
     return C;
 }
 
@@ -1728,8 +1739,159 @@ static void komega_sst(Case& C) {
     nutwall_correct(C);
 }
 
+// solve one transport equation of k-omega LKE on the shared scalar system
+// (RANS_kOmegaLKE.jl:339-345, :393-399, :427-433): discretise!,
+// apply_boundary_conditions!, implicit_relaxation!, (omega: constrain),
+// update_preconditioner!, solve_system!, bound!
+static double lke_solve(Case& C, const std::vector<Term>& t, std::vector<double>& phi, const std::vector<double>& src,
+                        const std::vector<BC>& bcs, const xcal_solver_setup& SS, std::vector<double>& Pre,
+                        bool constrain) {
+    discretise_scalar(C, t, C.Ap, C.bp, phi, src);
+    apply_bcs_scalar(C, t, C.Ap, C.bp, bcs, phi);
+    relax_scalar(C.Ap, C.bp, phi, SS.relax);
+    if (constrain) constrain_omega(C, C.Ap, C.bp);
+    update_precond(C.Ap, SS.precond, Pre);
+    const double r = solve_scalar(C, SS, SS.precond, phi, Pre);
+    bound_field(*C.m, phi);
+    return r;
+}
+
+// the diffusivity of a k-omega LKE equation: the cell field interpolated,
+// boundary faces from nut's BCs (interpolate! + correct_boundaries!)
+static void lke_face(Case& C, const std::vector<double>& cell, std::vector<double>& face) {
+    interpolate(*C.m, cell, face);
+    correct_boundaries(C, C.bcNut, &face, &cell, false);
+}
+
+// Re_upsilon^-1.30, Re_upsilon = sqrt(sqrt(2 nu^2 kl / y^2)) y / nu
+static double lke_reu_pow(double nu, double kl, double y) {
+    const double ru = (std::sqrt(std::sqrt(((2.0 * (nu * nu)) * kl) / (y * y))) * y) / nu;
+    return det_pow(ru, -1.30);
+}
+
+// turbulence!(::KOmegaLKEModel) after grad!(gradU) and its limiter
+// (RANS_kOmegaLKE.jl:262-474), rho = 1, the model's constants (:83-98)
+static void komega_lke(Case& C) {
+    const xcal_config& cf = C.cfg;
+    const double nu = cf.nu, eta = C.lke_eta;
+    const double Cmu = 0.09, Cw1 = 0.52, Cw2 = 0.0708, Ccrit = 76500.0, CSS = 1.45, Cv = 0.43, sk = 0.5,
+                 sd = 0.125, skl = 0.0125, sw = 0.5;
+    for (int i = 0; i < C.nC; ++i) {
+        // :284-306.  S_dev = (g + g')/2 - tr(g)/3 I; S2 = 2 sum(S_dev.^2);
+        // Omega = sqrt(2 sum(((g - g')/2).^2)); Pk = sum(g .* 2*S_dev), which
+        // Julia reads as the matrix product (g .* 2) * S_dev (.* and * share
+        // a precedence level, left to right).  Sums run over the column-major
+        // entries from the first; a product entry is ((a1 b1 + a2 b2) + a3 b3)
+        double G[3][3], Sd[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) G[a][b] = C.gradU[3 * a + b][i];
+        const double divU = (G[0][0] + G[1][1]) + G[2][2];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                Sd[a][b] = 0.5 * (G[a][b] + G[b][a]);
+                if (a == b) Sd[a][b] = Sd[a][b] - divU / 3.0;
+            }
+        double s2 = 0.0, om = 0.0, pk = 0.0;
+        for (int b = 0; b < 3; ++b)
+            for (int a = 0; a < 3; ++a) {
+                const double sq = Sd[a][b] * Sd[a][b];
+                const double w = 0.5 * (G[a][b] - G[b][a]);
+                double mab = (G[a][0] * 2.0) * Sd[0][b];
+                mab = mab + (G[a][1] * 2.0) * Sd[1][b];
+                mab = mab + (G[a][2] * 2.0) * Sd[2][b];
+                if (a == 0 && b == 0) {
+                    s2 = sq;
+                    om = w * w;
+                    pk = mab;
+                } else {
+                    s2 = s2 + sq;
+                    om = om + w * w;
+                    pk = pk + mab;
+                }
+            }
+        C.divU[i] = divU;
+        C.S2[i] = 2.0 * s2;
+        C.Om[i] = std::sqrt(2.0 * om);
+        C.Pk[i] = pk;
+        const double u0 = C.U[0][i], u1 = C.U[1][i], u2 = C.U[2][i];
+        C.normU[i] = std::sqrt((u0 * u0 + u1 * u1) + u2 * u2);
+        C.ReL[i] = (jl_max(C.normU[i], std::sqrt(jl_eps(1.0))) * C.yw[i]) / nu;  // kMin = eps()
+    }
+    for (int i = 0; i < C.nC; ++i) {
+        // :309-335 (Re_lambda^0.5 as sqrt)
+        const double y = C.yw[i], kl = C.kl[i], S2 = C.S2[i];
+        const double pru = lke_reu_pow(nu, kl, y), prl = std::sqrt(C.ReL[i]);
+        const double uy = C.normU[i] / y;
+        const double nutL1 = ((((eta * kl) * std::sqrt(S2)) * pru) * prl) / jl_max(S2, uy * uy);
+        const double ReLt = jl_min((kl / jl_max(jl_min(nu, nutL1), 1e-15)) / jl_max(C.Om[i], 1e-15), 5000.0);
+        C.gam[i] = jl_min(ReLt * ReLt, Ccrit) / Ccrit;
+        C.PkL[i] = (((std::sqrt(S2) * eta) * kl) * pru) * prl;
+        C.DkL[i] = (2.0 * nu) / (y * y);
+        C.nueffS[i] = nu + (skl * std::sqrt(kl)) * y;
+    }
+    // kl: Time + Div(mdotf) - Lap(nueffkL) + Si(DkLf) == Source(PkL) (:165-173, :337-345)
+    lke_face(C, C.nueffS, C.mueffl);
+    const std::vector<Term> tl = {{T_TIME, 1.0, nullptr, cf.kl_schemes.time},
+                                  {T_DIV, 1.0, &C.mdotf, cf.kl_schemes.divergence},
+                                  {T_LAP, -1.0, &C.mueffl, 0},
+                                  {T_SI, 1.0, &C.DkL, 0}};
+    C.res_kl = lke_solve(C, tl, C.kl, C.PkL, C.bcKl, cf.kl_solver, C.Pkl, false);
+    // cross diffusion (:371-374): grad omega with p's gradient scheme, grad k
+    scalar_grad(C, C.omega, C.wfs, C.bcOmega, cf.p_schemes.gradient, C.gw);
+    scalar_grad(C, C.k, C.kfs, C.bcK, cf.k_schemes.gradient, C.gk);
+    for (int i = 0; i < C.nC; ++i) {  // :377-387
+        const double w = C.omega[i], sw_ = jl_max(w, 1e-15);
+        C.Pw[i] = Cw1 * C.Pk[i];
+        C.Pw[i] = C.Pw[i] - (((2.0 / 3.0) * Cw1) * C.divU[i]) * w;
+        C.Dw[i] = Cw2 * w;
+        C.nueffS[i] = nu + sw * (C.k[i] / sw_);
+        const double dkdw = (C.gk[0][i] * C.gw[0][i] + C.gk[1][i] * C.gw[1][i]) + C.gk[2][i] * C.gw[2][i];
+        C.D2[i] = jl_max((sd / (sw_ * sw_)) * dkdw, 0.0);
+    }
+    // omega: Time + Div - Lap(nueffw) + Si(Dwf) - Si(dkdomegadx) == Source(Pw) (:185-195)
+    lke_face(C, C.nueffS, C.mueffw);
+    const std::vector<Term> tw = {{T_TIME, 1.0, nullptr, cf.omega_schemes.time},
+                                  {T_DIV, 1.0, &C.mdotf, cf.omega_schemes.divergence},
+                                  {T_LAP, -1.0, &C.mueffw, 0},
+                                  {T_SI, 1.0, &C.Dw, 0},
+                                  {T_SI, -1.0, &C.D2, 0}};
+    C.res_omega = lke_solve(C, tw, C.omega, C.Pw, C.bcOmega, cf.omega_solver, C.Pww, true);
+    for (int i = 0; i < C.nC; ++i) {  // :401-420
+        const double w = C.omega[i], g = C.gam[i];
+        const double sw_ = jl_max(w, 1e-15), sk_ = jl_max(C.k[i], 1e-15), snu = jl_max(nu, 1e-15);
+        const double fv = 1.0 - det_exp_neg((-std::sqrt(sk_ / (snu * sw_))) / Cv);
+        const double pku = ((fv * (sk_ / sw_)) * C.Pk[i]) * g;
+        const double pkl = jl_min(pku, ((20.0 * Cmu) * sk_) * w);
+        C.Pk[i] = pkl - ((2.0 / 3.0) * C.divU[i]) * C.k[i];
+        C.Dk[i] = (Cmu * g) * w;
+        C.nueffS[i] = nu + sk * (sk_ / sw_);
+    }
+    lke_face(C, C.nueffS, C.mueffk);
+    kwall_production(C);  // correct_production! (:424)
+    const std::vector<Term> tk = {{T_TIME, 1.0, nullptr, cf.k_schemes.time},
+                                  {T_DIV, 1.0, &C.mdotf, cf.k_schemes.divergence},
+                                  {T_LAP, -1.0, &C.mueffk, 0},
+                                  {T_SI, 1.0, &C.Dk, 0}};
+    C.res_k = lke_solve(C, tk, C.k, C.Pk, C.bcK, cf.k_solver, C.Pkw, false);
+    for (int i = 0; i < C.nC; ++i) {  // :436-460
+        const double kl = C.kl[i], y = C.yw[i], S2 = C.S2[i];
+        const double sw_ = jl_max(C.omega[i], 1e-15), sk_ = jl_max(C.k[i], 1e-15);
+        const double PkLv = (((std::sqrt(S2) * eta) * kl) * lke_reu_pow(nu, kl, y)) * std::sqrt(C.ReL[i]);
+        const double uy = C.normU[i] / y;
+        const double nuL = PkLv / jl_max(S2, uy * uy);
+        const double x = ((CSS * nu) * C.Om[i]) / sk_;
+        const double fSS = det_exp_neg(-(x * x));
+        const double nuts = fSS * (sk_ / sw_);
+        C.nut[i] = nuts + nuL;
+    }
+    interpolate(*C.m, C.nut, C.nutf);
+    correct_boundaries(C, C.bcNut, &C.nutf, &C.nut, false);
+    nutwall_correct(C);
+}
+
 void turbulence(Case& C) {
     grad_U(C);  // RANS_laminar.jl:73-79, LES_Smagorinsky.jl:117, RANS_kOmega.jl:167-168
+    if (C.cfg.turbulence == XCAL_TURB_KOMEGA_LKE) komega_lke(C);
     if (C.cfg.turbulence == XCAL_TURB_KOMEGA_SST) komega_sst(C);
     if (C.cfg.turbulence == XCAL_TURB_KOMEGA) komega(C);
     if (C.cfg.turbulence == XCAL_TURB_KEQUATION) kequation(C);

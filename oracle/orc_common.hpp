@@ -201,5 +201,14 @@ inline double det_tanh_pos(double x) {
     const double e = det_exp_neg(-2.0 * x);
     return (1.0 - e) / (1.0 + e);
 }
+// x^a for x >= 0 as exp(a log x) (Julia's ^ for a non-integer exponent):
+// 0^a = Inf for a < 0, Inf^a = 0; the exp reduction also holds for y > 0,
+// up to the overflow at 709.7
+inline double det_pow(double x, double a) {
+    if (x == 0.0) return a < 0.0 ? HUGE_VAL : 0.0;
+    if (std::isinf(x)) return a < 0.0 ? 0.0 : HUGE_VAL;
+    const double y = a * det_log(x);
+    return y >= 709.7 ? HUGE_VAL : det_exp_neg(y);
+}
 
 }  // namespace orc

@@ -64,7 +64,7 @@ struct Krylov {
 struct Case {
     const Mesh* m = nullptr;
     xcal_config cfg{};
-    std::vector<BC> bcU, bcP, bcNut, bcK, bcOmega, bcY;
+    std::vector<BC> bcU, bcP, bcNut, bcK, bcOmega, bcY, bcKl;
     int nC = 0, nF = 0, nB = 0;
 
     // fields
@@ -84,6 +84,12 @@ struct Case {
     // coefficient, grad k / grad omega, their face values, omega's own
     // preconditioner
     std::vector<double> yw, F1, F2, Om, D2, gk[3], gw[3], kfs, wfs, Pww;
+    // RANS{KOmegaLKE}: kl, its source and Si coefficient, the flow quantities
+    // of one turbulence! call (Omega in Om, the cross diffusion in D2), the
+    // intermittency gamma, a cell diffusivity and kl's face diffusivity and
+    // preconditioner; eta from Tu
+    std::vector<double> kl, PkL, DkL, S2, normU, divU, ReL, gam, nueffS, mueffl, Pkl;
+    double res_kl = 0.0, lke_eta = 0.0;
     std::vector<int> rorder;  // morton_order of the cell centres
     double time = 0.0;
     bool initialised = false;

@@ -11,7 +11,8 @@ correctly rounded to within an ulp) is bounded here:
   log(x), x in [1e-300, 1e300] and near 1: <= 2 ulp;
   tanh(x), x >= 0.1:        <= 8 ulp;  x < 0.1: absolute error <= 2.2e-16
                              (1 - e^-2x cancels there; the SST blending uses
-                             tanh as a switch between 0 and 1).
+                             tanh as a switch between 0 and 1);
+  x^-1.30 (det_pow):         relative 4e-16 (1 + |1.3 log x|).
 """
 import ctypes as C
 
@@ -69,3 +70,19 @@ def test_tanh(ev):
     assert np.abs(got - ref)[~big].max() <= 2.2e-16
     assert np.all((got >= 0.0) & (got <= 1.0))
     assert ev(2, np.array([0.0]))[0] == 0.0
+
+
+def test_pow_m130(ev):
+    """x^-1.30 = exp(-1.3 log x) (k-omega LKE's Re_upsilon^-1.30): the log's
+    rounding is carried through the product, so the relative error grows
+    with |1.3 log x|: within 4e-16 (1 + |1.3 log x|) over [1e-100, 1e100]
+    (about 12 ulp over [1e-3, 1e3]); 0 -> Inf, Inf -> 0, 1 -> 1."""
+    rng = np.random.default_rng(3)
+    xs = np.exp(rng.uniform(np.log(1e-100), np.log(1e100), 200_000))
+    got, ref = ev(3, xs), xs ** -1.30
+    assert np.all(np.abs(got / ref - 1.0) <= 4e-16 * (1.0 + np.abs(1.3 * np.log(xs))))
+    near = np.exp(rng.uniform(np.log(1e-3), np.log(1e3), 100_000))
+    assert ulps(ev(3, near), near ** -1.30).max() <= 16.0
+    assert ev(3, np.array([1.0]))[0] == 1.0
+    z = ev(3, np.array([0.0, np.inf]))
+    assert z[0] == np.inf and z[1] == 0.0

@@ -1,0 +1,125 @@
+"""RANS{KOmegaLKE} on the GPU against the oracle (1e-10 relative L2,
+expected 0): the flat plate of examples/2D_flatplate_LKE_ERCOFTAC.jl (steady
+SIMPLE, OmegaWallFunction on the wall) host-polled with Jacobi and DILU and
+in graph mode; the wall distance; a restart from a checkpoint; LKE cases in
+a batch equal to the same cases alone; run_ writing k, omega, kl, nut and y."""
+import os
+
+import numpy as np
+import pytest
+
+from test_komega_lke import KL_FIELDS, flatplate, set_lke_fields
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+ALL = KL_FIELDS + ("FIELD_GAMMA", "FIELD_NUTF", "FIELD_NUEFF", "FIELD_GRADU", "FIELD_PK", "FIELD_DK", "FIELD_DW")
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / (nb if nb > 0 else 1.0)
+
+
+def _pair(x, orc, ctx, mesh, model, cfg, graph=False):
+    dm = x.DeviceMesh(ctx, mesh)
+    g = x.Case(dm, cfg)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    for c in (g, o):
+        set_lke_fields(x, c, model)
+    if graph:
+        g.set_graph_mode(True)
+    return g, o, dm
+
+
+@pytest.mark.parametrize("precond,graph", [("Jacobi", False), ("DILU", False), ("Jacobi", True)])
+def test_lke_flatplate_parity(x, orc, ctx, precond, graph):
+    mesh = flatplate(x, 30, 14, seed=5)
+    model, config = x.cases.lke_flatplate_case(mesh, 12, precond=getattr(x.api, precond))
+    cfg, keep = x.build_config(model, config)
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, graph)
+    assert rel(g.get_field(x._abi.FIELD_WALLDIST), o.get_field(x._abi.FIELD_WALLDIST)) <= TOL
+    rg, _ = g.simple_iterate(12)
+    ro, _ = o.simple_iterate(12)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    for f in ALL:
+        assert rel(g.get_field(getattr(x._abi, f)), o.get_field(getattr(x._abi, f))) <= TOL, f
+
+
+def test_lke_restart_bit_identical(x, ctx):
+    """checkpoint() / restore() carry kl too: 3 + 3 iterations from a
+    restored case equal 6 in one go."""
+    mesh = flatplate(x, 20, 10)
+
+    def new_case():
+        model, config = x.cases.lke_flatplate_case(mesh, 6)
+        cfg, keep = x.build_config(model, config)
+        dm = x.DeviceMesh(ctx, mesh)
+        c = x.Case(dm, cfg)
+        set_lke_fields(x, c, model)
+        return c, (dm, keep)
+
+    a, ka = new_case()
+    ra = a.simple_iterate(6)[0]
+    b, kb = new_case()
+    rb = b.simple_iterate(3)[0]
+    state = b.checkpoint()
+    assert "FIELD_KL" in state
+    c, kc = new_case()
+    c.restore(state)
+    rc = c.simple_iterate(3)[0]
+    assert np.array_equal(np.concatenate([rb, rc]), ra)
+    for f in KL_FIELDS:
+        assert np.array_equal(c.get_field(getattr(x._abi, f)), a.get_field(getattr(x._abi, f))), f
+
+
+def test_lke_batch_matches_single(x, ctx):
+    """LKE cases in a batch (their U and p solves batched, kl / omega / k on
+    each case's stream) equal the same cases advanced alone, bit for bit."""
+    specs = [(24, 12, 1), (20, 10, 2)]
+
+    def mk(nx, ny, seed):
+        mesh = flatplate(x, nx, ny, seed)
+        model, config = x.cases.lke_flatplate_case(mesh, 4)
+        cfg, keep = x.build_config(model, config)
+        dm = x.DeviceMesh(ctx, mesh)
+        c = x.Case(dm, cfg)
+        c.set_inner_cg(1)
+        set_lke_fields(x, c, model)
+        return c, (dm, keep, cfg)
+
+    alone = []
+    for s in specs:
+        c, keep = mk(*s)
+        res, _ = c.simple_iterate(4)
+        alone.append((res, [c.get_field(getattr(x._abi, f)) for f in KL_FIELDS]))
+    batch = x.api.Batch(ctx, 4, 1 << 32)
+    members = []
+    for s in specs:
+        c, keep = mk(*s)
+        assert batch.add(c)
+        members.append((c, keep))
+    hist = np.stack([batch.simple_iterate()[0] for _ in range(4)], axis=1)
+    for k, (c, keep) in enumerate(members):
+        assert np.array_equal(hist[k], alone[k][0]), k
+        for f, ref in zip(KL_FIELDS, alone[k][1]):
+            assert np.array_equal(c.get_field(getattr(x._abi, f)), ref), (k, f)
+    batch.close()
+
+
+def test_lke_run_writes_fields(x, tmp_path):
+    """run_ through the public API: the model's k, omega, kl, nut and y come
+    back from the device; the VTK file carries them (save_output,
+    RANS_kOmegaLKE.jl:478-489)."""
+    mesh = flatplate(x, 20, 10)
+    model, config = x.cases.lke_flatplate_case(mesh, 5)
+    config.runtime.write_interval = 5
+    x.api.run_(model, config, output_dir=str(tmp_path))
+    t = model.turbulence
+    for v in (t.k, t.omega, t.kl, t.nut, t.y):
+        assert np.all(np.isfinite(v)) and v.max() > 0.0
+    files = sorted(os.listdir(tmp_path))
+    assert files, files
+    text = open(os.path.join(tmp_path, files[-1])).read()
+    for name in ("\"k\"", "\"omega\"", "\"kl\"", "\"nut\"", "\"y\""):
+        assert name in text, name

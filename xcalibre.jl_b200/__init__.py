@@ -12,12 +12,13 @@ from .api import (B200Backend, Bicgstab, Case, CellBased, Cg, Configuration, Con
                   Smagorinsky, SolverSetup, Steady, SteadyState, Symmetry, Transient, Upwind, Wall, Zerogradient,
                   assign, build_config, construct_periodic, initialise_, launch_count, run_, Batch,
                   footprint_estimate, VTK, OpenFOAM, save_checkpoint, load_checkpoint, boundary_average, JacobiSmoother,
-                  KOmega, KOmegaSST, OmegaWallFunction, KWallFunction, NutWallFunction, KEquation)
+                  KOmega, KOmegaSST, KOmegaLKE, OmegaWallFunction, KWallFunction, NutWallFunction, KEquation)
 from . import dsl
 from .dsl import Divergence, Equation, Laplacian, ScalarEquation, Si, Source, Time
 from .foam import Mesh3, build_mesh3
 from .foamio import FOAM3D_mesh, read_polymesh, write_polymesh
 from .unv import UNV2D_mesh, UNV3D_mesh
-from .meshgen import PolyMesh, box_polymesh, cavity_polymesh, channel_polymesh, periodic_box_polymesh
+from .meshgen import (PolyMesh, box_polymesh, cavity_polymesh, channel_polymesh, flatplate_polymesh,
+                      periodic_box_polymesh)
 
 __all__ = [n for n in dir() if not n.startswith("_")] + ["_abi"]

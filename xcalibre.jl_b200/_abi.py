@@ -37,15 +37,15 @@ GRAD_GAUSS, GRAD_MIDPOINT = 0, 1
 LIMITER_NONE, LIMITER_CELL, LIMITER_FACE = 0, 1, 2
 SOLVER_CG, SOLVER_BICGSTAB = 0, 1
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_DILU = 0, 1, 2
-TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST, TURB_KEQUATION = 0, 1, 2, 3, 4
+TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST, TURB_KEQUATION, TURB_KOMEGA_LKE = 0, 1, 2, 3, 4, 5
 PREC_FP64, PREC_MIXED = 0, 1
 ALGO_SIMPLE, ALGO_PISO = 0, 1
-EQN_U, EQN_P, EQN_K, EQN_OMEGA, EQN_WALLDIST = 0, 1, 2, 3, 4
+EQN_U, EQN_P, EQN_K, EQN_OMEGA, EQN_WALLDIST, EQN_KL = 0, 1, 2, 3, 4, 5
 
 FIELD_U, FIELD_P, FIELD_MDOTF, FIELD_NUEFF, FIELD_GRADP, FIELD_GRADU = 0, 1, 2, 3, 4, 5
 FIELD_RD, FIELD_HV, FIELD_DIVHV, FIELD_NUT, FIELD_NUTF, FIELD_UF = 6, 7, 8, 9, 10, 11
 FIELD_PF, FIELD_RDF, FIELD_DELTA, FIELD_K, FIELD_OMEGA, FIELD_WALLDIST = 12, 13, 14, 15, 16, 17
-FIELD_PK, FIELD_DK, FIELD_DW = 18, 19, 20
+FIELD_PK, FIELD_DK, FIELD_DW, FIELD_KL, FIELD_GAMMA = 18, 19, 20, 21, 22
 
 # (components, "cell"|"face") per field id
 FIELD_SHAPE = {
@@ -54,7 +54,7 @@ FIELD_SHAPE = {
     FIELD_DIVHV: (1, "cell"), FIELD_NUT: (1, "cell"), FIELD_NUTF: (1, "face"), FIELD_UF: (3, "face"),
     FIELD_PF: (1, "face"), FIELD_RDF: (1, "face"), FIELD_DELTA: (1, "cell"), FIELD_K: (1, "cell"),
     FIELD_OMEGA: (1, "cell"), FIELD_WALLDIST: (1, "cell"), FIELD_PK: (1, "cell"), FIELD_DK: (1, "cell"),
-    FIELD_DW: (1, "cell"),
+    FIELD_DW: (1, "cell"), FIELD_KL: (1, "cell"), FIELD_GAMMA: (1, "cell"),
 }
 
 _pi32 = C.POINTER(C.c_int32)
@@ -129,6 +129,8 @@ class ConfigDesc(C.Structure):
         ("sst_beta2", C.c_double), ("sst_sigma_k2", C.c_double), ("sst_sigma_omega2", C.c_double),
         ("y_schemes", SchemesDesc), ("y_solver", SolverSetupDesc), ("n_bc_y", C.c_int32),
         ("bc_y", C.POINTER(BCDesc)), ("keq_ck", C.c_double), ("keq_ce", C.c_double),
+        ("lke_Tu", C.c_double), ("kl_schemes", SchemesDesc), ("kl_solver", SolverSetupDesc), ("n_bc_kl", C.c_int32),
+        ("bc_kl", C.POINTER(BCDesc)),
     ]
 
 

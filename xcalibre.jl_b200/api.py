@@ -126,6 +126,12 @@ class KOmegaSST:
     the wall distance, cross-diffusion and a limited nut."""
 
 
+class KOmegaLKE:
+    """RANS{KOmegaLKE} (RANS_kOmegaLKE.jl): k-omega with a laminar kinetic
+    energy kl and an intermittency trigger for transition; needs Tu (the
+    freestream turbulence intensity) and the wall patches."""
+
+
 class Incompressible: ...
 
 
@@ -241,8 +247,9 @@ class RANS:
     """RANS{Laminar}, RANS{KOmega}(; beta+, alpha1, beta1, sigma_k,
     sigma_omega) (RANS_kOmega.jl:29-33) or RANS{KOmegaSST}(; beta+, alpha1,
     sigma_k1, sigma_k2, sigma_omega1, sigma_omega2, beta1, beta2, kappa,
-    walls) (RANS_kOmegaSST.jl:57-61); unset coefficients take the model's
-    defaults."""
+    walls) (RANS_kOmegaSST.jl:57-61) or RANS{KOmegaLKE}(; Tu, walls)
+    (RANS_kOmegaLKE.jl:60-64, its other coefficients fixed); unset
+    coefficients take the model's defaults."""
     model: type = Laminar
     beta_star: float | None = None
     alpha1: float | None = None
@@ -256,6 +263,7 @@ class RANS:
     sigma_omega2: float | None = None
     kappa: float | None = None
     walls: list | None = None
+    Tu: float | None = None
 
     def coeffs(self) -> dict:
         if self.model is KOmegaSST:
@@ -304,12 +312,14 @@ class Physics:
         # model.turbulence.k / .omega / .nut, as the reference's fields
         if isinstance(turbulence, (RANS, LES)):
             turbulence.nut = self.nut
-            if isinstance(turbulence, RANS) and turbulence.model in (KOmega, KOmegaSST):
+            if isinstance(turbulence, RANS) and turbulence.model in (KOmega, KOmegaSST, KOmegaLKE):
                 turbulence.k = np.zeros(n)
                 turbulence.omega = np.zeros(n)
             if isinstance(turbulence, LES) and turbulence.model is KEquation:
                 turbulence.k = np.zeros(n)
-            if isinstance(turbulence, RANS) and turbulence.model is KOmegaSST:
+            if isinstance(turbulence, RANS) and turbulence.model is KOmegaLKE:
+                turbulence.kl = np.zeros(n)
+            if isinstance(turbulence, RANS) and turbulence.model in (KOmegaSST, KOmegaLKE):
                 turbulence.y = np.zeros(n)
 
 
@@ -635,7 +645,10 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     les = isinstance(turb, LES)
     keq = les and turb.model is KEquation
     sst = isinstance(turb, RANS) and turb.model is KOmegaSST
-    kw = isinstance(turb, RANS) and turb.model in (KOmega, KOmegaSST)
+    lke = isinstance(turb, RANS) and turb.model is KOmegaLKE
+    kw = isinstance(turb, RANS) and turb.model in (KOmega, KOmegaSST, KOmegaLKE)
+    if lke and turb.Tu is None:
+        raise ValueError("RANS{KOmegaLKE} needs Tu (RANS_kOmegaLKE.jl:60)")
     bnd = config.boundaries
     bU = _bc_array(mesh, bnd["U"], 3, keep)
     bP = _bc_array(mesh, bnd["p"], 1, keep)
@@ -643,12 +656,14 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     bN = _bc_array(mesh, nut_bcs, 1, keep)
     k_bcs = bnd.get("k", []) if (kw or keq) else []
     w_bcs = bnd.get("omega", []) if kw else []
+    kl_bcs = bnd.get("kl", []) if lke else []
     bK = _bc_array(mesh, k_bcs, 1, keep)
     bW = _bc_array(mesh, w_bcs, 1, keep)
+    bKl = _bc_array(mesh, kl_bcs, 1, keep)
     # wall_distance! (Calculate_4_wall_distance.jl:12-27): per BC of the
     # first field, Dirichlet 0 on the walls, Empty, else Extrapolated
     y_bcs = []
-    if sst:
+    if sst or lke:
         walls = list(turb.walls or [])
         for bc in next(iter(bnd.values())):
             if bc.name in walls:
@@ -658,10 +673,12 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
             else:
                 y_bcs.append(Extrapolated(bc.name))
     bY = _bc_array(mesh, y_bcs, 1, keep)
-    keep += [bU, bP, bN, bK, bW, bY]
-    sY = config.schemes.get("y", Schemes()) if sst else Schemes()
-    slv_y = _solver_desc(config.solvers["y"]) if sst else _abi.SolverSetupDesc()
-    co = turb.coeffs() if kw else {}
+    keep += [bU, bP, bN, bK, bW, bY, bKl]
+    sY = config.schemes.get("y", Schemes()) if (sst or lke) else Schemes()
+    slv_y = _solver_desc(config.solvers["y"]) if (sst or lke) else _abi.SolverSetupDesc()
+    sKl = config.schemes.get("kl", Schemes()) if lke else Schemes()
+    slv_kl = _solver_desc(config.solvers["kl"]) if lke else _abi.SolverSetupDesc()
+    co = turb.coeffs() if (kw and not lke) else {}
     sK = config.schemes.get("k", Schemes()) if (kw or keq) else Schemes()
     sW = config.schemes.get("omega", Schemes()) if kw else Schemes()
     slv_k = _solver_desc(config.solvers["k"]) if (kw or keq) else _abi.SolverSetupDesc()
@@ -676,7 +693,7 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
     cfg = _abi.ConfigDesc(
         algorithm=_abi.ALGO_PISO if transient else _abi.ALGO_SIMPLE,
         turbulence=(_abi.TURB_KEQUATION if keq else _abi.TURB_SMAGORINSKY if les else _abi.TURB_KOMEGA_SST if sst
-                    else _abi.TURB_KOMEGA if kw else _abi.TURB_LAMINAR),
+                    else _abi.TURB_KOMEGA_LKE if lke else _abi.TURB_KOMEGA if kw else _abi.TURB_LAMINAR),
         nu=float(model.fluid.nu), smagorinsky_C=float(turb.C) if (les and not keq) else 0.0,
         les_delta_distance=dist, les_delta_power=power,
         U_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sU.time)], divergence=_SCHEME_DIV[_kind(sU.divergence)],
@@ -706,7 +723,11 @@ def build_config(model: Physics, config: Configuration, pref=None, inner_loops=N
                                        divergence=_SCHEME_DIV[_kind(sW.divergence)]),
         k_solver=slv_k, omega_solver=slv_w, n_bc_k=len(k_bcs), n_bc_omega=len(w_bcs),
         bc_k=C.cast(bK, C.POINTER(_abi.BCDesc)), bc_omega=C.cast(bW, C.POINTER(_abi.BCDesc)),
-        keq_ck=float(turb.ck) if keq else 0.0, keq_ce=float(turb.ce) if keq else 0.0)
+        keq_ck=float(turb.ck) if keq else 0.0, keq_ce=float(turb.ce) if keq else 0.0,
+        lke_Tu=float(turb.Tu) if lke else 0.0,
+        kl_schemes=_abi.SchemesDesc(time=_SCHEME_TIME[_kind(sKl.time)], divergence=_SCHEME_DIV[_kind(sKl.divergence)],
+                                    gradient=_SCHEME_GRAD[_kind(sKl.gradient)]),
+        kl_solver=slv_kl, n_bc_kl=len(kl_bcs), bc_kl=C.cast(bKl, C.POINTER(_abi.BCDesc)))
     return cfg, keep
 
 
@@ -716,7 +737,8 @@ class Case:
     def __init__(self, dmesh: DeviceMesh, cfg: _abi.ConfigDesc):
         self.dmesh, self.ctx = dmesh, dmesh.ctx
         self.mesh = dmesh.mesh
-        self.komega = cfg.turbulence in (_abi.TURB_KOMEGA, _abi.TURB_KOMEGA_SST)
+        self.komega = cfg.turbulence in (_abi.TURB_KOMEGA, _abi.TURB_KOMEGA_SST, _abi.TURB_KOMEGA_LKE)
+        self.lke = cfg.turbulence == _abi.TURB_KOMEGA_LKE
         self.kequation = cfg.turbulence == _abi.TURB_KEQUATION
         h = C.c_void_p()
         check(lib().xcal_case_create(self.ctx.h, dmesh.h, C.byref(cfg), C.byref(h)), self.ctx.h)
@@ -903,13 +925,16 @@ class Case:
         face mass flux, face velocity and pressure, nu_eff, gradients, rD,
         H...): with ``restore`` a new case on the same mesh and configuration
         continues exactly as this one would."""
-        names = CHECKPOINT_FIELDS + (KOMEGA_FIELDS if self.komega else ("FIELD_K",) if self.kequation else ())
-        return {name: self.get_field(getattr(_abi, name)).copy() for name in names}
+        return {name: self.get_field(getattr(_abi, name)).copy() for name in self._state_fields()}
+
+    def _state_fields(self) -> tuple:
+        extra = KOMEGA_FIELDS if self.komega else ("FIELD_K",) if self.kequation else ()
+        return CHECKPOINT_FIELDS + extra + (("FIELD_KL",) if self.lke else ())
 
     def restore(self, state: dict) -> None:
         """Set the fields of a ``checkpoint`` and mark the state complete, so
         the next iteration does not redo the run's initial calculations."""
-        for name in CHECKPOINT_FIELDS + (KOMEGA_FIELDS if self.komega else ("FIELD_K",) if self.kequation else ()):
+        for name in self._state_fields():
             if name in state:
                 self.set_field(getattr(_abi, name), state[name])
         self._chk(lib().xcal_case_mark_initialised(self.h))
@@ -1097,9 +1122,24 @@ def load_checkpoint(path: str) -> dict:
 
 
 def _output_fields(case, model, transient_les: bool):
+    """The fields save_output writes per turbulence model (isothermal):
+    U, p; then k, omega, nut (RANS_kOmega.jl:236-246), with y (KOmegaSST,
+    RANS_kOmegaSST.jl:323-336), with kl and y (KOmegaLKE,
+    RANS_kOmegaLKE.jl:478-489); k, nut (LES_KEquation.jl:198-207); nut for
+    transient Smagorinsky."""
     fields = [("U", case.get_field(_abi.FIELD_U)), ("p", case.get_field(_abi.FIELD_P))]
-    if transient_les:
-        fields.append(("nut", case.get_field(_abi.FIELD_NUT)))
+    t = model.turbulence
+    names = []
+    if isinstance(t, RANS) and t.model in (KOmega, KOmegaSST, KOmegaLKE):
+        names = ["k", "omega"] + (["kl"] if t.model is KOmegaLKE else []) + ["nut"]
+        names += ["y"] if t.model in (KOmegaSST, KOmegaLKE) else []
+    elif isinstance(t, LES) and t.model is KEquation:
+        names = ["k", "nut"]
+    elif transient_les:
+        names = ["nut"]
+    ids = {"k": _abi.FIELD_K, "omega": _abi.FIELD_OMEGA, "kl": _abi.FIELD_KL, "nut": _abi.FIELD_NUT,
+           "y": _abi.FIELD_WALLDIST}
+    fields += [(n, case.get_field(ids[n])) for n in names]
     return fields
 
 
@@ -1164,6 +1204,8 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
             case.set_field(_abi.FIELD_K, model.turbulence.k)
             if hasattr(model.turbulence, "omega"):
                 case.set_field(_abi.FIELD_OMEGA, model.turbulence.omega)
+            if hasattr(model.turbulence, "kl"):
+                case.set_field(_abi.FIELD_KL, model.turbulence.kl)
             case.set_field(_abi.FIELD_NUT, model.turbulence.nut)
         n = config.runtime.iterations
         step = wi if wi > 0 else n
@@ -1200,6 +1242,10 @@ def run_(model: Physics, config: Configuration, pref=None, ncorrectors: int = 0,
             model.turbulence.k[:] = case.get_field(_abi.FIELD_K)
             if hasattr(model.turbulence, "omega"):
                 model.turbulence.omega[:] = case.get_field(_abi.FIELD_OMEGA)
+            if hasattr(model.turbulence, "kl"):
+                model.turbulence.kl[:] = case.get_field(_abi.FIELD_KL)
+            if hasattr(model.turbulence, "y"):
+                model.turbulence.y[:] = case.get_field(_abi.FIELD_WALLDIST)
     finally:
         if aw is not None:
             aw.close()

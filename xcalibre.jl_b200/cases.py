@@ -11,6 +11,9 @@
                         from fourier_field (seeded, k^4 exp(-2 (k/4)^2));
                         or the subgrid k equation (LES{KEquation})
 * kequation_channel_case -- the channel with LES{KEquation}, PISO
+* lke_flatplate_case -- steady RANS{KOmegaLKE} flat plate (Tu = 0.01, U =
+                        5.4 m/s, nu = 1.48e-5), after
+                        examples/2D_flatplate_LKE_ERCOFTAC.jl:16-151
 """
 from __future__ import annotations
 
@@ -102,6 +105,53 @@ def kequation_channel_case(mesh: Mesh3, steps: int = 20, precision: str = "fp64"
     A.initialise_(model.momentum.p, 0.0)
     A.initialise_(model.turbulence.k, k_in)
     A.initialise_(model.turbulence.nut, 0.0)
+    return model, config
+
+
+def lke_flatplate_case(mesh: Mesh3, iterations: int = 1000, precision: str = "fp64", device: int = 0,
+                       precond=A.Jacobi, Tu: float = 0.01):
+    """RANS{KOmegaLKE} on the flat plate (patches inlet, outlet, wall, top,
+    frontAndBack): inflow 5.4 m/s with k = 0.0575, kl = 0.0115, omega = 275;
+    OmegaWallFunction on the wall, Extrapolated on the top; LUST divergence;
+    the solvers, relaxation and initial fields of the reference example."""
+    velocity, nu = [5.4, 0.0, 0.0], 1.48e-5
+    k_in, kl_in, w_in = 0.0575, 0.0115, 275.0
+    model = A.Physics(time=A.Steady(), fluid=A.Fluid(A.Incompressible, nu=nu),
+                      turbulence=A.RANS(A.KOmegaLKE, Tu=Tu, walls=["wall"]), energy=A.Energy(A.Isothermal),
+                      domain=mesh)
+    fb = A.Empty("frontAndBack")
+    BCs = A.assign(
+        region=mesh,
+        U=[A.Dirichlet("inlet", velocity), A.Zerogradient("outlet"), A.Wall("wall", [0.0, 0.0, 0.0]),
+           A.Extrapolated("top"), fb],
+        p=[A.Zerogradient("inlet"), A.Dirichlet("outlet", 0.0), A.Wall("wall"), A.Extrapolated("top"), fb],
+        k=[A.Dirichlet("inlet", k_in), A.Zerogradient("outlet"), A.Dirichlet("wall", 0.0), A.Extrapolated("top"), fb],
+        kl=[A.Dirichlet("inlet", kl_in), A.Zerogradient("outlet"), A.Dirichlet("wall", 0.0), A.Extrapolated("top"),
+            fb],
+        omega=[A.Dirichlet("inlet", w_in), A.Zerogradient("outlet"), A.OmegaWallFunction("wall"),
+               A.Extrapolated("top"), fb],
+        nut=[A.Dirichlet("inlet", k_in / w_in), A.Extrapolated("outlet"), A.Dirichlet("wall", 0.0),
+             A.Extrapolated("top"), fb],
+    )
+    lust = A.Schemes(divergence=A.LUST)
+
+    def ss(solver, relax, conv=1e-8, rtol=1e-2):
+        return A.SolverSetup(solver=solver(), preconditioner=precond(), convergence=conv, relax=relax, rtol=rtol)
+
+    solvers = {"U": ss(A.Bicgstab, 0.7), "p": ss(A.Cg, 0.2, rtol=1e-3),
+               "y": A.SolverSetup(solver=A.Cg(), preconditioner=A.Jacobi(), convergence=1e-7, relax=0.9, rtol=1e-3),
+               "kl": ss(A.Bicgstab, 0.3), "k": ss(A.Bicgstab, 0.3), "omega": ss(A.Bicgstab, 0.3)}
+    schemes = {"U": lust, "p": A.Schemes(divergence=A.LUST), "k": lust, "y": A.Schemes(), "kl": lust, "omega": lust}
+    config = A.Configuration(solvers=solvers, schemes=schemes,
+                             runtime=A.Runtime(iterations=iterations, write_interval=-1, time_step=1.0),
+                             hardware=A.Hardware(backend=A.B200Backend(device=device, precision=precision)),
+                             boundaries=BCs)
+    A.initialise_(model.momentum.U, velocity)
+    A.initialise_(model.momentum.p, 0.0)
+    A.initialise_(model.turbulence.kl, kl_in)
+    A.initialise_(model.turbulence.k, k_in)
+    A.initialise_(model.turbulence.omega, w_in)
+    A.initialise_(model.turbulence.nut, k_in / w_in)
     return model, config
 
 

@@ -46,9 +46,12 @@ extern "C" {
 const char* xcal_version(void) { return "xcal_b200 0.1 (sm_100a, FP64 hot path)"; }
 
 int32_t xcal_det_math(int32_t which, const double* in, double* out, int64_t n) {
-    if (!in || !out || n < 0 || which < 0 || which > 2) return XCAL_ERR_INVALID;
+    if (!in || !out || n < 0 || which < 0 || which > 3) return XCAL_ERR_INVALID;
     for (int64_t i = 0; i < n; ++i)
-        out[i] = which == 0 ? det_exp_neg(in[i]) : which == 1 ? det_log(in[i]) : det_tanh_pos(in[i]);
+        out[i] = which == 0   ? det_exp_neg(in[i])
+                 : which == 1 ? det_log(in[i])
+                 : which == 2 ? det_tanh_pos(in[i])
+                              : det_pow(in[i], -1.30);
     return XCAL_OK;
 }
 
@@ -101,7 +104,8 @@ int32_t xcal_abi_layout(int32_t which, int64_t* out, int32_t cap) {
                  XCAL_OFF(T, n_bc_omega), XCAL_OFF(T, bc_k), XCAL_OFF(T, bc_omega), XCAL_OFF(T, sst_beta2),
                  XCAL_OFF(T, sst_sigma_k2), XCAL_OFF(T, sst_sigma_omega2), XCAL_OFF(T, y_schemes),
                  XCAL_OFF(T, y_solver), XCAL_OFF(T, n_bc_y), XCAL_OFF(T, bc_y),
-                 XCAL_OFF(T, keq_ck), XCAL_OFF(T, keq_ce)};
+                 XCAL_OFF(T, keq_ck), XCAL_OFF(T, keq_ce), XCAL_OFF(T, lke_Tu), XCAL_OFF(T, kl_schemes),
+                 XCAL_OFF(T, kl_solver), XCAL_OFF(T, n_bc_kl), XCAL_OFF(T, bc_kl)};
             break;
         }
         case XCAL_LAYOUT_POLYMESH_DESC: {

@@ -8,6 +8,7 @@
 
 #include "case.hpp"
 #include "kernels.hpp"
+#include "dev_common.cuh"
 
 namespace xcal {
 
@@ -738,12 +739,24 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         // periodic pairs resolve to the p system's partner slots)
         build_bc_table(bcK, *m, cfg.bc_k, cfg.n_bc_k, 1, &P, stream);
         build_bc_table(bcOmega, *m, cfg.bc_omega, cfg.n_bc_omega, 1, &P, stream);
-        if (sst()) build_bc_table(bcY, *m, cfg.bc_y, cfg.n_bc_y, 1, &P, stream);
+        if (has_y()) build_bc_table(bcY, *m, cfg.bc_y, cfg.n_bc_y, 1, &P, stream);
         for (DBuf<double>* b : {&kfld, &omega, &Pk, &Pw, &Dk, &Dw, &kwtmp}) {
             b->alloc(m->nC);
             b->zero(stream);
         }
-        if (sst()) {
+        if (lke()) {
+            // RANS{KOmegaLKE}: kl on the p system too; eta from Tu (RANS_kOmegaLKE.jl:97)
+            if (!(cfg.lke_Tu >= 0.0)) fail(XCAL_ERR_INVALID, "RANS{KOmegaLKE} needs Tu >= 0");
+            build_bc_table(bcKl, *m, cfg.bc_kl, cfg.n_bc_kl, 1, &P, stream);
+            for (DBuf<double>* b : {&kl, &PkL, &DkL, &S2b, &normUb, &divUb, &ReLb, &gam, &nueffS}) {
+                b->alloc(m->nC);
+                b->zero(stream);
+            }
+            fmu.alloc(m->nF);
+            fmu.zero(stream);
+            lke_eta = 0.02974 * det_tanh_pos(59.79 * det_pow(cfg.lke_Tu, 1.191) + 1.65e-13);
+        }
+        if (has_y()) {
             for (DBuf<double>* b : {&yw, &yphi, &F1b, &F2b, &Omb, &D2b, &gkv[0], &gkv[1], &gkv[2], &gwv[0], &gwv[1],
                                     &gwv[2]}) {
                 b->alloc(m->nC);
@@ -756,6 +769,7 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         fail(XCAL_ERR_INVALID, "unknown turbulence model");
     }
     cfg.bc_U = cfg.bc_p = cfg.bc_nut = nullptr;  // not retained
+    cfg.bc_kl = nullptr;
     for (int d = 0; d < 3; ++d) {
         Uc[d].alloc(nC);
         gradp[d].alloc(nC);
@@ -768,12 +782,11 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     if (cfg.ncorrectors > 0) build_nonorth(*m, stream);
     for (int g : {cfg.U_schemes.gradient, cfg.p_schemes.gradient})
         if (g != XCAL_GRAD_GAUSS && g != XCAL_GRAD_MIDPOINT) fail(XCAL_ERR_INVALID, "unknown gradient scheme");
-    if (cfg.turbulence == XCAL_TURB_KOMEGA_SST)
+    if (has_y())
         for (int g : {cfg.k_schemes.gradient, cfg.y_schemes.gradient})
             if (g != XCAL_GRAD_GAUSS && g != XCAL_GRAD_MIDPOINT) fail(XCAL_ERR_INVALID, "unknown gradient scheme");
     if (cfg.U_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.p_schemes.gradient == XCAL_GRAD_MIDPOINT ||
-        (cfg.turbulence == XCAL_TURB_KOMEGA_SST &&
-         (cfg.k_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.y_schemes.gradient == XCAL_GRAD_MIDPOINT)))
+        (has_y() && (cfg.k_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.y_schemes.gradient == XCAL_GRAD_MIDPOINT)))
         build_midpoint(*m, stream);
     for (const xcal_schemes* sc : {&cfg.U_schemes, &cfg.p_schemes}) {
         if (sc->limiter != XCAL_LIMITER_NONE && sc->limiter != XCAL_LIMITER_CELL && sc->limiter != XCAL_LIMITER_FACE)
@@ -886,7 +899,8 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         XCAL_CUDA(cudaMemcpyAsync(Delta.p, h.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream));
     }
     XCAL_CUDA(cudaStreamSynchronize(stream));
-    if (sst()) wall_distance();  // initialise(::KOmegaSST) (RANS_kOmegaSST.jl:167)
+    // initialise(::KOmegaSST) (RANS_kOmegaSST.jl:167), initialise(::KOmegaLKE) (RANS_kOmegaLKE.jl:236)
+    if (has_y()) wall_distance();
 }
 
 Case::~Case() {
@@ -974,8 +988,12 @@ double* Case::field_comp(int field, int comp, long& count) {
                 fail(XCAL_ERR_INVALID, "k / omega fields need RANS{KOmega}, RANS{KOmegaSST} or (k) LES{KEquation}");
             return field == XCAL_FIELD_K ? kfld.p : omega.p;
         case XCAL_FIELD_WALLDIST:
-            if (!sst()) fail(XCAL_ERR_INVALID, "the wall distance needs RANS{KOmegaSST}");
+            if (!has_y()) fail(XCAL_ERR_INVALID, "the wall distance needs RANS{KOmegaSST} or RANS{KOmegaLKE}");
             return yw.p;
+        case XCAL_FIELD_KL:
+        case XCAL_FIELD_GAMMA:
+            if (!lke()) fail(XCAL_ERR_INVALID, "kl / gamma need RANS{KOmegaLKE}");
+            return field == XCAL_FIELD_KL ? kl.p : gam.p;
         case XCAL_FIELD_PK:
         case XCAL_FIELD_DK:
         case XCAL_FIELD_DW:
@@ -1146,6 +1164,80 @@ void Case::kequation() {
     XCAL_CUDA(cudaMemcpyAsync(kwtmp.p, kfld.p, (size_t)mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     launch_bound(stream, mv(), kwtmp.p, kfld.p);
     launch_keq_nut(stream, mesh->nC, kfld.p, Delta.p, cfg.keq_ck, nut.p);
+    launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
+    launch_nutwall(stream, nnutwall, mv(), nwface.p, nwpar.p, kfld.p, cfg.nu, nutf.p, nueff.p);
+}
+
+// turbulence!(::KOmegaLKEModel) after grad!(gradU) and its limiter
+// (RANS_kOmegaLKE.jl:262-474), rho = 1.  Each equation Time + Div(mdotf) -
+// Lap(nueff_f) + Si(D) [- Si(D2)] == Source(P) goes on the p system with
+// its own BCs, implicit relaxation and preconditioner and is bounded after
+// its solve; nueff_f is the equation's cell diffusivity interpolated with
+// nut's BCs (interpolate! + correct_boundaries!).  Order: the cell fields
+// and gamma, kl; grad omega, grad k and the omega equation (its wall rows
+// constrained from the current k); the k equation (KWallFunction production
+// after its cell loop); nut = fSS k / omega + nuL, nutf with nut's BCs and
+// the wall functions
+void Case::komega_lke() {
+    LkeView V{};
+    for (int q = 0; q < 9; ++q) V.g[q] = gradU[q].p;
+    for (int d = 0; d < 3; ++d) {
+        V.U[d] = Uc[d].p;
+        V.gk[d] = gkv[d].p;
+        V.gw[d] = gwv[d].p;
+    }
+    V.y = yw.p;
+    V.kl = kl.p;
+    V.k = kfld.p;
+    V.omega = omega.p;
+    V.divU = divUb.p;
+    V.S2 = S2b.p;
+    V.Om = Omb.p;
+    V.normU = normUb.p;
+    V.ReL = ReLb.p;
+    V.gam = gam.p;
+    V.Pk = Pk.p;
+    V.Pw = Pw.p;
+    V.PkL = PkL.p;
+    V.Dk = Dk.p;
+    V.Dw = Dw.p;
+    V.DkL = DkL.p;
+    V.D2 = D2b.p;
+    V.nueffS = nueffS.p;
+    V.nut = nut.p;
+    V.nC = mesh->nC;
+    V.nu = cfg.nu;
+    V.eta = lke_eta;
+    auto transport = [&](int e, double* phi, const BCTable& T, const xcal_schemes& sc, const xcal_solver_setup& SS,
+                         const double* D, const double* D2, const double* src, bool constrain, int slot) {
+        launch_interp_scalar(stream, mv(), bcNut.view(), nueffS.p, fmu.p, nullptr, 0.0);
+        launch_assemble_scalar(stream, mv(), P.view(), mdot.p, fmu.p, 0.0, 1.0, nullptr, 0.0, phi, D, D2, src, P.nz.p,
+                               P.b[0].p, sc.time, sc.divergence, cfg.dt, -1.0);
+        launch_bc_relax_scalar(stream, mv(), P.view(), T.view(), P.nz.p, P.b[0].p, mdot.p, fmu.p, 0.0, 1.0, nullptr,
+                               0.0, D2 ? 1 : 0, phi, SS.relax, sc.divergence);
+        if (constrain && nwall)
+            launch_omega_constrain(stream, nwall, P.view(), wcell.p, wpar.p, kfld.p, cfg.nu, P.nz.p, P.b[0].p);
+        update_precond(e);
+        const double r = solve_system(e, 0, &last_iters[slot]);
+        XCAL_CUDA(cudaMemcpyAsync(kwtmp.p, phi, (size_t)mesh->nC * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        launch_bound(stream, mv(), kwtmp.p, phi);
+        return r;
+    };
+    launch_lke_fields(stream, V);
+    res_kl = transport(XCAL_EQN_KL, kl.p, bcKl, cfg.kl_schemes, cfg.kl_solver, DkL.p, nullptr, PkL.p, false, 7);
+    double* gw[3] = {gwv[0].p, gwv[1].p, gwv[2].p};
+    double* gk[3] = {gkv[0].p, gkv[1].p, gkv[2].p};
+    scalar_grad(omega.p, bcOmega, cfg.p_schemes.gradient, gw);  // Grad{schemes.p.gradient}(omega) (:177)
+    scalar_grad(kfld.p, bcK, cfg.k_schemes.gradient, gk);
+    launch_lke_omega(stream, V);
+    // omega: ... + Si(Dw) - Si(cross diffusion) == Source(Pw)
+    res_omega = transport(XCAL_EQN_OMEGA, omega.p, bcOmega, cfg.omega_schemes, cfg.omega_solver, Dw.p, D2b.p, Pw.p,
+                          true, 5);
+    launch_lke_k(stream, V);
+    const double* Ucp[3] = {Uc[0].p, Uc[1].p, Uc[2].p};
+    launch_kwall_production(stream, nkwall, mv(), kwcell.p, kwface.p, kwpar.p, kfld.p, Ucp, cfg.nu, Pk.p);
+    res_k = transport(XCAL_EQN_K, kfld.p, bcK, cfg.k_schemes, cfg.k_solver, Dk.p, nullptr, Pk.p, false, 4);
+    launch_lke_nut(stream, V);
     launch_interp_scalar(stream, mv(), bcNut.view(), nut.p, nutf.p, nueff.p, cfg.nu);
     launch_nutwall(stream, nnutwall, mv(), nwface.p, nwpar.p, kfld.p, cfg.nu, nutf.p, nueff.p);
 }
@@ -1697,12 +1789,16 @@ Case::SolveRef Case::solve_ref(int eqn, int comp) {
             const bool w = eqn == XCAL_EQN_OMEGA;
             SolveRef r{&P, w ? cfg.omega_solver : cfg.k_solver, w ? omega.p : kfld.p, P.b[0].p,
                        w ? (int)GRES_OMEGA : (int)GRES_K, 1, w ? 5 : 4};
-            // k-omega: omega with k's preconditioner; SST: each its own (RANS_kOmegaSST.jl:163-164)
-            r.SS.precond = (w && sst()) ? cfg.omega_solver.precond : cfg.k_solver.precond;
+            // k-omega: omega with k's preconditioner; SST and LKE: each its own
+            // (RANS_kOmegaSST.jl:163-164, RANS_kOmegaLKE.jl:210-212)
+            r.SS.precond = (w && (sst() || lke())) ? cfg.omega_solver.precond : cfg.k_solver.precond;
             return r;
         }
+        case XCAL_EQN_KL:
+            if (!lke()) fail(XCAL_ERR_INVALID, "the kl equation needs RANS{KOmegaLKE}");
+            return {&P, cfg.kl_solver, kl.p, P.b[0].p, GRES_KL, 1, 7};
         case XCAL_EQN_WALLDIST:
-            if (!sst()) fail(XCAL_ERR_INVALID, "the wall distance needs RANS{KOmegaSST}");
+            if (!has_y()) fail(XCAL_ERR_INVALID, "the wall distance needs RANS{KOmegaSST} or RANS{KOmegaLKE}");
             return {&P, cfg.y_solver, yphi.p, P.b[0].p, GRES_K, 1, 6};
         default:
             fail(XCAL_ERR_INVALID, "unknown equation");
@@ -2053,7 +2149,9 @@ void Case::turbulence() {
                 launch_limit_cell(stream, mv(), limD.p, Uc[a].p, g + 3 * a, cfg.U_schemes.limiter_level);
         if (les) launch_smag_nut(stream, mesh->nC, g, Delta.p, nut.p);
     }
-    if (rans_kw())
+    if (lke())
+        komega_lke();
+    else if (rans_kw())
         komega();
     else if (keq())
         kequation();

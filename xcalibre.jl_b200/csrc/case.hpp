@@ -161,7 +161,7 @@ struct Case {
     size_t bytes = 0;  // device bytes held (excluding the mesh)
     cudaStream_t stream = nullptr;
     bool own_stream = true;
-    BCTable bcU, bcP, bcNut, bcK, bcOmega, bcY;
+    BCTable bcU, bcP, bcNut, bcK, bcOmega, bcY, bcKl;
     Equation U, P;
     KrylovWS ws;
     // fields
@@ -177,6 +177,12 @@ struct Case {
     // RANS{KOmegaSST}: wall distance (and its potential), F1, F2, Omega, the
     // second omega Si coefficient, grad k, grad omega, a face scratch
     DBuf<double> yw, yphi, F1b, F2b, Omb, D2b, gkv[3], gwv[3], fscr;
+    // RANS{KOmegaLKE}: kl, its source and Si coefficient, the per-cell flow
+    // quantities of one turbulence! call (div U, S2, |U|, Re_lambda; Omega in
+    // Omb, the cross diffusion in D2b), the intermittency gamma, the cell
+    // diffusivity of the equation being set up and its face interpolation
+    DBuf<double> kl, PkL, DkL, S2b, normUb, divUb, ReLb, gam, nueffS, fmu;
+    double lke_eta = 0.0;  // 0.02974 tanh(59.79 Tu^1.191 + 1.65e-13)
     DBuf<int> wcell;
     int nwall = 0;
     // KWallFunction cells (last face in BC / face order) and NutWallFunction
@@ -184,14 +190,14 @@ struct Case {
     DBuf<int> kwcell, kwface, nwface;
     DBuf<double> kwpar, nwpar;
     int nkwall = 0, nnutwall = 0;
-    double res_k = 0.0, res_omega = 0.0;
+    double res_k = 0.0, res_omega = 0.0, res_kl = 0.0;
     bool initialised = false;
     int iteration = 0;
     double time = 0.0;
-    int last_iters[7] = {0, 0, 0, 0, 0, 0, 0};  // Ux, Uy, Uz, p, k, omega, wall distance
+    int last_iters[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // Ux, Uy, Uz, p, k, omega, wall distance, kl
     // Krylov status (KS_*) of each system's last solve, and how many solves
     // since creation stopped at itmax (Solve_1_api.jl:302 warns on those)
-    int last_status[7] = {0, 0, 0, 0, 0, 0, 0};
+    int last_status[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long itmax_hits = 0;
     void note_status(int gk, int status) {
         last_status[gk] = status;
@@ -280,8 +286,11 @@ struct Case {
     void build_wall_table(const DevMesh& m);
     void komega();
     void kequation();  // turbulence!(::KEquationModel) after grad U (LES_KEquation.jl:134-186)
+    void komega_lke();  // turbulence!(::KOmegaLKEModel) after grad U (RANS_kOmegaLKE.jl:262-474)
     bool sst() const { return cfg.turbulence == XCAL_TURB_KOMEGA_SST; }
-    bool rans_kw() const { return cfg.turbulence == XCAL_TURB_KOMEGA || sst(); }
+    bool lke() const { return cfg.turbulence == XCAL_TURB_KOMEGA_LKE; }
+    bool has_y() const { return sst() || lke(); }  // a wall distance field
+    bool rans_kw() const { return cfg.turbulence == XCAL_TURB_KOMEGA || sst() || lke(); }
     bool keq() const { return cfg.turbulence == XCAL_TURB_KEQUATION; }
     bool has_k() const { return rans_kw() || keq(); }  // a k field and equation
     void scalar_grad(const double* phi, const BCTable& T, int scheme, double* const g[3]);
@@ -323,7 +332,7 @@ struct Case {
     // graph; the Krylov (and defect-correction) loops are conditional WHILE
     // nodes driven by device-side stopping tests, so a step needs no host
     // round trip until its residuals are read.
-    enum { GRES_U = 0, GRES_P = 3, GRES_CO = 4, GRES_K = 5, GRES_OMEGA = 6, GRES_N = 8 };
+    enum { GRES_U = 0, GRES_P = 3, GRES_CO = 4, GRES_K = 5, GRES_OMEGA = 6, GRES_KL = 7, GRES_N = 8 };
     DBuf<double> gres;          // per-step results: U x,y,z and p residuals, max Courant
     DBuf<int> giters;           // (iterations, status) of the step's 4 solves
     DBuf<unsigned int> cmax_ctr;

@@ -84,6 +84,15 @@ __host__ __device__ __forceinline__ double det_tanh_pos(double x) {
     const double e = det_exp_neg(-2.0 * x);
     return (1.0 - e) / (1.0 + e);
 }
+// x^a for x >= 0 as exp(a log x) (k-omega LKE's Re_upsilon^-1.30): 0^a =
+// Inf for a < 0, Inf^a = 0; det_exp_neg's reduction also holds for y > 0,
+// up to the overflow at 709.7
+__host__ __device__ __forceinline__ double det_pow(double x, double a) {
+    if (x == 0.0) return a < 0.0 ? INFINITY : 0.0;
+    if (isinf(x)) return a < 0.0 ? 0.0 : INFINITY;
+    const double y = a * det_log(x);
+    return y >= 709.7 ? INFINITY : det_exp_neg(y);
+}
 
 // Julia's eps(x)
 __device__ __forceinline__ double jl_eps(double x) {

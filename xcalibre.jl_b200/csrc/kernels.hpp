@@ -52,11 +52,12 @@ void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const
 void launch_kw_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* omega,
                        double* Pk, double* Pw, double* Dk, double* Dw, double alpha1, double beta1, double beta_star);
 // (F1 null: constant sigma; F1 set: sigma blended with sigma2 (k-omega SST);
-// D2 / si2: the omega equation's second Si term of k-omega SST)
+// D2 / si2: a second Si term with sign d2_sign: omega's cross diffusion in
+// k-omega SST (+) and k-omega LKE (-), KEquation's 2/3 div U (+))
 void launch_assemble_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const double* mdot,
                             const double* nutf, double nu, double sigma, const double* F1, double sigma2,
                             const double* phi, const double* D, const double* D2, const double* P, double* nz,
-                            double* b, int time_scheme, int div_scheme, double dt);
+                            double* b, int time_scheme, int div_scheme, double dt, double d2_sign = 1.0);
 void launch_bc_relax_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz,
                             double* b, const double* mdot, const double* nutf, double nu, double sigma,
                             const double* F1, double sigma2, int si2, const double* phi, double alpha,
@@ -83,6 +84,28 @@ void launch_kw_nut(cudaStream_t s, int nC, const double* k, const double* omega,
 void launch_keq_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* k,
                         const double* Delta, double ce, double* Pk, double* Dk, double* Dw);
 void launch_keq_nut(cudaStream_t s, int nC, const double* k, const double* Delta, double ck, double* nut);
+// RANS{KOmegaLKE} (RANS_kOmegaLKE.jl:270-460): the cell loops of one
+// turbulence! call over these buffers (n_cells each)
+struct LkeView {
+    const double* g[9];   // grad U, row-major (d u_a / d x_b at 3a + b)
+    const double* U[3];
+    const double* gk[3];  // grad k, grad omega (cross diffusion)
+    const double* gw[3];
+    const double* y;      // wall distance
+    const double* kl;
+    const double* k;
+    const double* omega;
+    double *divU, *S2, *Om, *normU, *ReL, *gam;  // per-cell flow quantities
+    double *Pk, *Pw, *PkL, *Dk, *Dw, *DkL, *D2;   // sources and Si coefficients
+    double* nueffS;  // the equation being set up: its cell diffusivity
+    double* nut;
+    int nC;
+    double nu, eta;
+};
+void launch_lke_fields(cudaStream_t s, const LkeView& V);  // flow quantities, gamma, the kl equation
+void launch_lke_omega(cudaStream_t s, const LkeView& V);   // the omega equation
+void launch_lke_k(cudaStream_t s, const LkeView& V);       // fv and the k equation
+void launch_lke_nut(cudaStream_t s, const LkeView& V);     // nut = nuts + nuL
 void launch_nueff(cudaStream_t s, int nF, const double* nutf, double* nueff, double nu);
 // Smagorinsky nut = Delta |S| from a stored grad U
 void launch_smag_nut(cudaStream_t s, int nC, const double* const g[9], const double* Delta, double* nut);

@@ -383,7 +383,9 @@ __global__ void k_kw_sources(int nC, const double* __restrict__ g0, const double
 // _discretise_scalar_model! (Discretise_2_generated_distretisation.jl:125-167)
 // of the k / omega equation: terms Time, Divergence, Laplacian, Si in order
 // face diffusivity nu + sigma nutf; with F1 (k-omega SST) sigma blends as
-// s1 F1f + (1 - F1f) s2, F1f the plain interpolation of F1
+// s1 F1f + (1 - F1f) s2, F1f the plain interpolation of F1.  k-omega LKE
+// passes its interpolated face diffusivity as nutf with nu = 0, sigma = 1
+// (0 + 1 x = x)
 __device__ __forceinline__ double kw_mueff(const MeshView& m, int f, const double* nutf, double nu, double s1,
                                            const double* F1, double s2) {
     if (!F1) return nu + s1 * nutf[f];
@@ -398,7 +400,7 @@ __global__ void k_assemble_scalar(MeshView m, CSRView A, const double* __restric
                                   const double* __restrict__ F1, double sigma2, const double* __restrict__ phi,
                                   const double* __restrict__ D, const double* __restrict__ D2,
                                   const double* __restrict__ P, double* nz, double* b, int time_scheme,
-                                  int div_scheme, double dt) {
+                                  int div_scheme, double dt, double d2_sign) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.nC) return;
     double ac_sum = 0.0;
@@ -459,7 +461,7 @@ __global__ void k_assemble_scalar(MeshView m, CSRView A, const double* __restric
     acs = acs + (1.0 * D[i]) * V;  // Si (:211-218)
     bs = bs + 0.0;
     if (D2) {
-        acs = acs + (1.0 * D2[i]) * V;
+        acs = acs + (d2_sign * D2[i]) * V;
         bs = bs + 0.0;
     }
     nz[A.diag[i]] = ac_sum + acs;
@@ -1549,9 +1551,9 @@ void launch_kw_sources(cudaStream_t s, int nC, const double* const g[9], const d
 void launch_assemble_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const double* mdot,
                             const double* nutf, double nu, double sigma, const double* F1, double sigma2,
                             const double* phi, const double* D, const double* D2, const double* P, double* nz,
-                            double* b, int time_scheme, int div_scheme, double dt) {
+                            double* b, int time_scheme, int div_scheme, double dt, double d2_sign) {
     k_assemble_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, A, mdot, nutf, nu, sigma, F1, sigma2, phi, D, D2, P, nz, b,
-                                                 time_scheme, div_scheme, dt);
+                                                 time_scheme, div_scheme, dt, d2_sign);
     XCAL_CHECK_LAUNCH();
 }
 void launch_bc_relax_scalar(cudaStream_t s, const MeshView& m, const CSRView& A, const BCView& bc, double* nz,
@@ -1642,6 +1644,132 @@ __global__ void k_keq_nut(int nC, const double* __restrict__ k, const double* __
                           double* nut) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nC) nut[i] = (ck * Delta[i]) * sqrt(k[i]);
+}
+
+// ---- RANS{KOmegaLKE} (RANS_kOmegaLKE.jl) ---------------------------------
+// the model's constants (:83-98)
+constexpr double LKE_CMU = 0.09, LKE_CW1 = 0.52, LKE_CW2 = 0.0708, LKE_CCRIT = 76500.0, LKE_CSS = 1.45,
+                 LKE_CV = 0.43, LKE_SK = 0.5, LKE_SD = 0.125, LKE_SKL = 0.0125, LKE_SW = 0.5;
+
+// Re_upsilon = sqrt(sqrt(2 nu^2 kl / y^2)) y / nu and its power -1.30 (:321, :447)
+__device__ __forceinline__ double lke_reu_pow(double nu, double kl, double y) {
+    const double ru = (sqrt(sqrt(((2.0 * (nu * nu)) * kl) / (y * y))) * y) / nu;
+    return det_pow(ru, -1.30);
+}
+
+// the first two cell loops of turbulence! (:284-335), after grad U: div U,
+// S2 = 2 |dev(S)|^2, Omega = sqrt(2) |skew(grad U)|, Pk = sum((2 grad U)
+// dev(S)) (the code's `g .* 2*S_dev` is a matrix product: .* and * share a
+// precedence level and associate left), |U|, Re_lambda; then gamma, the kl
+// equation's source and Si coefficient and its cell diffusivity.  Sums over
+// the 3x3 entries run in column-major order from the first entry; the
+// product's entries are ((a1 b1 + a2 b2) + a3 b3)
+__global__ void k_lke_fields(LkeView V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V.nC) return;
+    double G[3][3];
+    for (int q = 0; q < 9; ++q) G[q / 3][q % 3] = V.g[q][i];
+    const double divU = (G[0][0] + G[1][1]) + G[2][2];
+    const double d3 = divU / 3.0;
+    double Sd[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            const double sy = 0.5 * (G[a][b] + G[b][a]);
+            Sd[a][b] = a == b ? sy - d3 : sy;
+        }
+    double s2 = 0.0, om = 0.0, pk = 0.0;
+    for (int b = 0; b < 3; ++b)
+        for (int a = 0; a < 3; ++a) {
+            const double sq = Sd[a][b] * Sd[a][b];
+            const double w = 0.5 * (G[a][b] - G[b][a]);
+            const double m = (((G[a][0] * 2.0) * Sd[0][b]) + ((G[a][1] * 2.0) * Sd[1][b])) + ((G[a][2] * 2.0) * Sd[2][b]);
+            const bool first = a == 0 && b == 0;
+            s2 = first ? sq : s2 + sq;
+            om = first ? w * w : om + w * w;
+            pk = first ? m : pk + m;
+        }
+    const double S2 = 2.0 * s2, Om = sqrt(2.0 * om);
+    const double u0 = V.U[0][i], u1 = V.U[1][i], u2 = V.U[2][i];
+    const double normU = sqrt((u0 * u0 + u1 * u1) + u2 * u2);
+    const double nu = V.nu, y = V.y[i], kl = V.kl[i];
+    const double ReL = (jl_max(normU, 1.4901161193847656e-08) * y) / nu;  // sqrt(eps())
+    V.divU[i] = divU;
+    V.S2[i] = S2;
+    V.Om[i] = Om;
+    V.Pk[i] = pk;
+    V.normU[i] = normU;
+    V.ReL[i] = ReL;
+    // :312-335
+    const double pru = lke_reu_pow(nu, kl, y), prl = sqrt(ReL), sS2 = sqrt(S2);
+    const double uy = normU / y;
+    const double nutL1 = ((((V.eta * kl) * sS2) * pru) * prl) / jl_max(S2, uy * uy);
+    const double ReLt = jl_min((kl / jl_max(jl_min(nu, nutL1), 1e-15)) / jl_max(Om, 1e-15), 5000.0);
+    V.gam[i] = jl_min(ReLt * ReLt, LKE_CCRIT) / LKE_CCRIT;
+    V.PkL[i] = (((sS2 * V.eta) * kl) * pru) * prl;
+    V.DkL[i] = (2.0 * nu) / (y * y);
+    V.nueffS[i] = nu + ((LKE_SKL * sqrt(kl)) * y);
+}
+
+// the omega equation's cell loop (:377-387): production from the loop's Pk,
+// Cw2 omega, the diffusivity nu + sigma_w k / omega, the cross diffusion
+// max(sigma_d / omega^2 grad k . grad omega, 0)
+__global__ void k_lke_omega(LkeView V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V.nC) return;
+    const double w = V.omega[i], sw = jl_max(w, 1e-15);
+    double pw = LKE_CW1 * V.Pk[i];
+    pw = pw - ((((2.0 / 3.0) * LKE_CW1) * V.divU[i]) * w);
+    V.Pw[i] = pw;
+    V.Dw[i] = LKE_CW2 * w;
+    V.nueffS[i] = V.nu + LKE_SW * (V.k[i] / sw);
+    const double dkdw = (V.gk[0][i] * V.gw[0][i] + V.gk[1][i] * V.gw[1][i]) + V.gk[2][i] * V.gw[2][i];
+    V.D2[i] = jl_max((LKE_SD / (sw * sw)) * dkdw, 0.0);
+}
+
+// the k equation's cell loop (:401-420), after the omega solve: fv, the
+// limited production Pk, Cmu gamma omega, the diffusivity nu + sigma_k k / omega
+__global__ void k_lke_k(LkeView V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V.nC) return;
+    const double w = V.omega[i], gam = V.gam[i], kk = V.k[i];
+    const double sw = jl_max(w, 1e-15), sk = jl_max(kk, 1e-15), snu = jl_max(V.nu, 1e-15);
+    const double fv = 1.0 - det_exp_neg((-sqrt(sk / (snu * sw))) / LKE_CV);
+    const double pku = ((fv * (sk / sw)) * V.Pk[i]) * gam;
+    const double pkl = jl_min(pku, ((20.0 * LKE_CMU) * sk) * w);
+    V.Pk[i] = pkl - (((2.0 / 3.0) * V.divU[i]) * kk);
+    V.Dk[i] = (LKE_CMU * gam) * w;
+    V.nueffS[i] = V.nu + LKE_SK * (sk / sw);
+}
+
+// nut = fSS k / omega + nuL from the solved kl, k, omega (:435-460)
+__global__ void k_lke_nut(LkeView V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V.nC) return;
+    const double kl = V.kl[i], nu = V.nu, y = V.y[i], S2 = V.S2[i], normU = V.normU[i];
+    const double sw = jl_max(V.omega[i], 1e-15), sk = jl_max(V.k[i], 1e-15);
+    const double PkL = (((sqrt(S2) * V.eta) * kl) * lke_reu_pow(nu, kl, y)) * sqrt(V.ReL[i]);
+    const double uy = normU / y;
+    const double nuL = PkL / jl_max(S2, uy * uy);
+    const double x = ((LKE_CSS * nu) * V.Om[i]) / sk;
+    const double fSS = det_exp_neg(-(x * x));
+    V.nut[i] = fSS * (sk / sw) + nuL;
+}
+
+void launch_lke_fields(cudaStream_t s, const LkeView& V) {
+    k_lke_fields<<<nblk(V.nC), TPB, 0, s>>>(V);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_lke_omega(cudaStream_t s, const LkeView& V) {
+    k_lke_omega<<<nblk(V.nC), TPB, 0, s>>>(V);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_lke_k(cudaStream_t s, const LkeView& V) {
+    k_lke_k<<<nblk(V.nC), TPB, 0, s>>>(V);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_lke_nut(cudaStream_t s, const LkeView& V) {
+    k_lke_nut<<<nblk(V.nC), TPB, 0, s>>>(V);
+    XCAL_CHECK_LAUNCH();
 }
 
 void launch_keq_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* k,

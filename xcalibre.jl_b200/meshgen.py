@@ -187,6 +187,17 @@ def channel_polymesh(nx: int = 128, ny: int = 128, nz: int = 128, seed: int | No
                                  ("walls", ["ymin", "ymax", "zmin", "zmax"])], seed=seed)
 
 
+def flatplate_polymesh(nx: int = 60, ny: int = 30, length: float = 0.5, height: float = 0.05,
+                       seed: int | None = 0) -> PolyMesh:
+    """2D flat plate (one cell deep): box [0,length]x[0,height]x[0,height/ny];
+    patches inlet (x = 0), outlet (x = length), wall (y = 0), top (y =
+    height), frontAndBack (the z sides, Empty); numbering permuted from
+    ``seed``."""
+    return box_polymesh(nx, ny, 1, lengths=(length, height, height / ny),
+                        patches=[("inlet", ["xmin"]), ("outlet", ["xmax"]), ("wall", ["ymin"]), ("top", ["ymax"]),
+                                 ("frontAndBack", ["zmin", "zmax"])], seed=seed)
+
+
 def periodic_box_polymesh(n: int = 96, seed: int | None = None) -> PolyMesh:
     """Cube of side 2*pi with six patches xmin..zmax (periodic pairs)."""
     L = 2.0 * np.pi
