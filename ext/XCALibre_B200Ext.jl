@@ -64,7 +64,7 @@ const BC_NUT_WALL = Int32(13)
 const TIME_STEADY, TIME_EULER = Int32(0), Int32(1)
 const DIV_LINEAR, DIV_UPWIND, DIV_LUST = Int32(0), Int32(1), Int32(2)
 const GRAD_GAUSS, GRAD_MIDPOINT = Int32(0), Int32(1)
-const LIMITER_NONE, LIMITER_CELL, LIMITER_FACE = Int32(0), Int32(1), Int32(2)
+const LIMITER_NONE, LIMITER_CELL, LIMITER_FACE, LIMITER_MFACE = Int32(0), Int32(1), Int32(2), Int32(3)
 const SOLVER_CG, SOLVER_BICGSTAB = Int32(0), Int32(1)
 const PRECOND_NONE, PRECOND_JACOBI, PRECOND_DILU = Int32(0), Int32(1), Int32(2)
 const TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST, TURB_KEQUATION, TURB_KOMEGA_LKE =
@@ -395,8 +395,10 @@ function schemes_desc(s)
             lim, level = LIMITER_CELL, Float64(s.limiter.level)
         elseif lname == :FaceBased
             lim = LIMITER_FACE
+        elseif lname == :MFaceBased
+            lim = LIMITER_MFACE
         else
-            error("libxcal_b200: limiter $(typeof(s.limiter)) is not on the B200 path (CellBased, FaceBased)")
+            error("libxcal_b200: limiter $(typeof(s.limiter)) is not on the B200 path")
         end
     end
     SchemesDesc(time_kind(s.time), div_kind(s.divergence), grad_kind(s.gradient), lim, level)

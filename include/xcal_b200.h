@@ -65,8 +65,11 @@ enum { XCAL_GRAD_GAUSS = 0, XCAL_GRAD_MIDPOINT = 1 };
  * after grad U in the turbulence update, per component (nut after it) */
 /* CellBased(level) (Calculate_0_gradient_cell_limiter.jl); FaceBased
  * (Calculate_0_gradient_face_limiter.jl: per cell the minimum over its
- * internal faces, no level) */
-enum { XCAL_LIMITER_NONE = 0, XCAL_LIMITER_CELL = 1, XCAL_LIMITER_FACE = 2 };
+ * internal faces, no level); MFaceBased
+ * (Calculate_0_gradient_mface_limiter.jl: each internal face corrects both
+ * cells' gradients in turn; the library applies a cell's faces in ascending
+ * face order, the reference run on one thread) */
+enum { XCAL_LIMITER_NONE = 0, XCAL_LIMITER_CELL = 1, XCAL_LIMITER_FACE = 2, XCAL_LIMITER_MFACE = 3 };
 /* Krylov solver: src/Solve/Solve_1_Krylov_solvers.jl:6-15 */
 enum { XCAL_SOLVER_CG = 0, XCAL_SOLVER_BICGSTAB = 1 };
 /* preconditioner: src/Solve/Preconditioners/preconditioners_0_types.jl */

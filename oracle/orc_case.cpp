@@ -1138,12 +1138,91 @@ static void limit_face_vector(Case& C, std::vector<double>* g) {
     }
 }
 
+// limit_gradient!(::MFaceBased) (Calculate_0_gradient_mface_limiter.jl):
+// the face kernel run on one thread, face by face in ascending id; a face's
+// two updates touch different cells, so each cell takes its own internal
+// faces' corrections in ascending face order (set_limiter, :62-74):
+// grad += d (bound - grad . d) / (d . d) where grad . d leaves
+// [min, max](F_own, F_nei) - F_cell, d = fc - cc
+static std::vector<int> sorted_internal_faces(const Mesh& m, int i) {
+    std::vector<int> fs(m.cell_faces.begin() + m.cf_off[i], m.cell_faces.begin() + m.cf_off[i + 1]);
+    std::sort(fs.begin(), fs.end());
+    return fs;
+}
+static void limit_mface_scalar(Case& C, const std::vector<double>& F, std::vector<double>* g) {
+    const Mesh& m = *C.m;
+    for (int i = 0; i < C.nC; ++i) {
+        V3 gr = {g[0][i], g[1][i], g[2][i]};
+        for (int f : sorted_internal_faces(m, i)) {
+            const double F1 = F[m.owner[f]], F2 = F[m.neigh[f]];
+            const double dmax = jl_max(F1, F2) - F[i], dmin = jl_min(F1, F2) - F[i];
+            const V3 d = m.fcentre[f] - m.ccentre[i];
+            const double fval = dot(gr, d), d2 = dot(d, d);
+            if (fval > dmax)
+                gr = {gr.x + (d.x * (dmax - fval)) / d2, gr.y + (d.y * (dmax - fval)) / d2,
+                      gr.z + (d.z * (dmax - fval)) / d2};
+            else if (fval < dmin)
+                gr = {gr.x + (d.x * (dmin - fval)) / d2, gr.y + (d.y * (dmin - fval)) / d2,
+                      gr.z + (d.z * (dmin - fval)) / d2};
+        }
+        g[0][i] = gr.x;
+        g[1][i] = gr.y;
+        g[2][i] = gr.z;
+    }
+}
+// Julia's isless on Float64 and Base's lexicographic isless of vectors
+// (cmp: the first entry not isequal decides); min / max(x, y) of two
+// vectors are whole vectors: isless(y, x) ? y : x and isless(y, x) ? x : y
+static bool jl_isless_d(double a, double b) {
+    if (std::isnan(a)) return false;
+    if (std::isnan(b)) return true;
+    return a < b || (a == b && std::signbit(a) && !std::signbit(b));
+}
+static bool lex_isless(const double* a, const double* b) {
+    for (int j = 0; j < 3; ++j) {
+        const bool eq = (std::isnan(a[j]) && std::isnan(b[j])) ||
+                        (a[j] == b[j] && std::signbit(a[j]) == std::signbit(b[j]));
+        if (!eq) return jl_isless_d(a[j], b[j]);
+    }
+    return false;
+}
+// the tensor form (:76-113): row a of grad U against component a
+static void limit_mface_vector(Case& C, std::vector<double>* g) {
+    const Mesh& m = *C.m;
+    for (int i = 0; i < C.nC; ++i) {
+        double G[9];
+        for (int q = 0; q < 9; ++q) G[q] = g[q][i];
+        const double ui[3] = {C.U[0][i], C.U[1][i], C.U[2][i]};
+        for (int f : sorted_internal_faces(m, i)) {
+            const int o = m.owner[f], n = m.neigh[f];
+            const double F1[3] = {C.U[0][o], C.U[1][o], C.U[2][o]};
+            const double F2[3] = {C.U[0][n], C.U[1][n], C.U[2][n]};
+            const bool lt = lex_isless(F2, F1);
+            const double* mx = lt ? F1 : F2;
+            const double* mn = lt ? F2 : F1;
+            const V3 d = m.fcentre[f] - m.ccentre[i];
+            const double dv[3] = {d.x, d.y, d.z};
+            const double d2 = dot(d, d);
+            for (int a = 0; a < 3; ++a) {
+                const double dmax = mx[a] - ui[a], dmin = mn[a] - ui[a];
+                const double fval = (G[3 * a] * d.x + G[3 * a + 1] * d.y) + G[3 * a + 2] * d.z;
+                if (fval > dmax)
+                    for (int b = 0; b < 3; ++b) G[3 * a + b] = G[3 * a + b] + (dv[b] * (dmax - fval)) / d2;
+                else if (fval < dmin)
+                    for (int b = 0; b < 3; ++b) G[3 * a + b] = G[3 * a + b] + (dv[b] * (dmin - fval)) / d2;
+            }
+        }
+        for (int q = 0; q < 9; ++q) g[q][i] = G[q];
+    }
+}
+
 static void grad_p_only(Case& C);
 
 static void grad_p(Case& C) {
     grad_p_only(C);
     if (C.cfg.p_schemes.limiter == XCAL_LIMITER_CELL) limit_cell(C, C.p, C.gradp, C.cfg.p_schemes.limiter_level);
     if (C.cfg.p_schemes.limiter == XCAL_LIMITER_FACE) limit_face_scalar(C, C.p, C.gradp);
+    if (C.cfg.p_schemes.limiter == XCAL_LIMITER_MFACE) limit_mface_scalar(C, C.p, C.gradp);
 }
 
 static void grad_p_only(Case& C) {
@@ -1175,6 +1254,7 @@ static void grad_U(Case& C) {  // grad! + limit_gradient!(schemes.U.limiter) (RA
     if (C.cfg.U_schemes.limiter == XCAL_LIMITER_CELL)
         for (int a = 0; a < 3; ++a) limit_cell(C, C.U[a], C.gradU + 3 * a, C.cfg.U_schemes.limiter_level);
     if (C.cfg.U_schemes.limiter == XCAL_LIMITER_FACE) limit_face_vector(C, C.gradU);
+    if (C.cfg.U_schemes.limiter == XCAL_LIMITER_MFACE) limit_mface_vector(C, C.gradU);
 }
 
 static void grad_U_only(Case& C) {

@@ -1,4 +1,4 @@
-"""Non-orthogonal correctors, Midpoint gradients and the CellBased and FaceBased
+"""Non-orthogonal correctors, Midpoint gradients and the CellBased, FaceBased and MFaceBased
 gradient limiters on the GPU against the oracle (skewed channel, FP64, host-polled and
 graph mode; tolerance the 1e-10 relative L2 of the parity tests, expected 0),
 and a batch of skewed cases with correctors (and limiters) giving the results
@@ -151,15 +151,17 @@ def test_limiter_parity(x, orc, ctx, grad, p_level, U_level, ncorr, graph):
 
 
 
+@pytest.mark.parametrize("kind", ["FaceBased", "MFaceBased"])
 @pytest.mark.parametrize("graph", [False, True])
 @pytest.mark.parametrize("grad", ["gauss", "midpoint"])
-def test_face_limiter_parity(x, orc, ctx, grad, graph):
-    """Schemes(limiter=FaceBased) for p (scalar form) and U (tensor form) on
-    the skewed channel with a corrector: GPU equal to the oracle."""
+def test_face_limiter_parity(x, orc, ctx, grad, graph, kind):
+    """Schemes(limiter=FaceBased / MFaceBased) for p (scalar form) and U
+    (tensor form) on the skewed channel with a corrector: GPU equal to the
+    oracle."""
     mesh = skewed_channel(x, n=(12, 7, 6), seed=10)
     model, config = x.cases.channel_case(mesh, iterations=4)
-    config.schemes["p"].limiter = x.api.FaceBased(mesh)
-    config.schemes["U"].limiter = x.api.FaceBased(mesh)
+    config.schemes["p"].limiter = getattr(x.api, kind)(mesh)
+    config.schemes["U"].limiter = getattr(x.api, kind)(mesh)
     if grad == "midpoint":
         config.schemes["p"].gradient = x.api.Midpoint
         config.schemes["U"].gradient = x.api.Midpoint

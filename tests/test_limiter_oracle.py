@@ -3,7 +3,7 @@ applied after every grad p, Solvers_1_SIMPLE.jl:154/193/206, and after grad U
 in the turbulence update, RANS_laminar.jl:77) on the CPU oracle, skewed
 channel: with level 1 every gradient-extrapolated face value stays inside the
 cell's neighbour range (Barth-Jespersen bound); level 0 gives the unlimited
-run bit for bit; the API checks level and refuses MFaceBased.
+run bit for bit; the API checks level and refuses unknown limiters.
 
 FaceBased (Calculate_0_gradient_face_limiter.jl): after limiting, every
 cell's gradient, extrapolated to each of its internal faces, stays inside
@@ -76,9 +76,12 @@ def test_limiter_api(x):
         x.api.CellBased(-0.1)
     mesh = skewed_channel(x, n=(4, 3, 3))
     model, config = x.cases.channel_case(mesh, iterations=1)
-    config.schemes["p"].limiter = x.api.MFaceBased(mesh)
+    config.schemes["p"].limiter = object()
     with pytest.raises(NotImplementedError):
         x.build_config(model, config)
+    config.schemes["p"].limiter = x.api.MFaceBased(mesh)
+    cfg, keep = x.build_config(model, config)
+    assert cfg.p_schemes.limiter == x._abi.LIMITER_MFACE
     config.schemes["p"].limiter = x.api.FaceBased(mesh)
     cfg, keep = x.build_config(model, config)
     assert cfg.p_schemes.limiter == x._abi.LIMITER_FACE
@@ -124,3 +127,75 @@ def test_face_limiter_vector_scales(x, orc):
     assert np.all(ratio <= 1.0 + 1e-12) and np.all(ratio >= 0.0) and np.any(ratio < 1.0)
     # parallel: G1 = ratio * G0 per cell
     assert np.allclose(G1[:, ok], G0[:, ok] * ratio, rtol=1e-12, atol=0.0)
+
+
+def _mface_loop(mesh, F, g):
+    """limit_gradient!(::MFaceBased) (Calculate_0_gradient_mface_limiter.jl)
+    as its kernel reads, run on one thread: internal faces in id order, each
+    correcting its owner's then its neighbour's gradient.  F: [n] (g [3, n])
+    or [3, n] (g [9, n], rows of grad U); vector bounds are Base's min / max
+    of two vectors, chosen whole by the lexicographic order."""
+    g = np.array(g, dtype=np.float64)
+    fc, cc = np.asarray(mesh.face_centre), np.asarray(mesh.cell_centre)
+    own, nei = np.asarray(mesh.face_owner), np.asarray(mesh.face_neigh)
+    vec = F.ndim == 2
+    for f in range(mesh.n_bfaces, mesh.n_faces):
+        o, n = own[f], nei[f]
+        if vec:
+            F1, F2 = F[:, o], F[:, n]
+            lt = tuple(F2) < tuple(F1)
+            mx, mn = (F1, F2) if lt else (F2, F1)
+        else:
+            mx, mn = max(F[o], F[n]), min(F[o], F[n])
+        for c in (o, n):
+            d = fc[f] - cc[c]
+            d2 = d @ d
+            rows = range(3) if vec else [None]
+            for a in rows:
+                sl = slice(3 * a, 3 * a + 3) if vec else slice(0, 3)
+                hi = (mx[a] - F[a, c]) if vec else (mx - F[c])
+                lo = (mn[a] - F[a, c]) if vec else (mn - F[c])
+                fval = g[sl, c] @ d
+                if fval > hi:
+                    g[sl, c] = g[sl, c] + d * (hi - fval) / d2
+                elif fval < lo:
+                    g[sl, c] = g[sl, c] + d * (lo - fval) / d2
+    return g
+
+
+def _green_gauss(mesh, pf):
+    """sum over a cell's faces of phi_f S_f / V (Calculate_0_gradient.jl)"""
+    S = np.asarray(mesh.face_normal) * np.asarray(mesh.face_area)[:, None]
+    own, nei = np.asarray(mesh.face_owner), np.asarray(mesh.face_neigh)
+    g = np.zeros((3, mesh.n_cells))
+    nB = mesh.n_bfaces
+    np.add.at(g.T, own, pf[:, None] * S)
+    np.add.at(g.T, nei[nB:], -(pf[nB:, None] * S[nB:]))
+    return g / np.asarray(mesh.cell_volume)
+
+
+def test_mface_limiter_restated(x, orc):
+    """The oracle's per-cell form equals the reference's face loop on one
+    thread: p's limited gradient against the loop applied to the Green-Gauss
+    gradient of the same face values; grad U against the loop applied to the
+    unlimited grad U of the same U (a laminar iteration's U does not depend
+    on its U limiter)."""
+    mesh = skewed_channel(x, seed=9)
+    model, config = x.cases.channel_case(mesh, iterations=1)
+    config.schemes["p"].limiter = x.api.MFaceBased(mesh)
+    cfg, keep = x.build_config(model, config)
+    o = orc.OracleCase(orc.OracleMesh.from_mesh3(mesh), cfg)
+    o.set_field(x._abi.FIELD_U, model.momentum.U)
+    o.set_field(x._abi.FIELD_P, model.momentum.p)
+    o.simple_iterate(1)
+    P, pf, gp = (o.get_field(f) for f in (x._abi.FIELD_P, x._abi.FIELD_PF, x._abi.FIELD_GRADP))
+    ref = _mface_loop(mesh, P, _green_gauss(mesh, pf))
+    assert np.max(np.abs(gp - ref)) <= 1e-9 * np.max(np.abs(ref))
+    assert not np.allclose(ref, _green_gauss(mesh, pf))  # the limiter acted
+    _, f0 = _run(x, orc, mesh, iters=1)
+    _, f1 = _run(x, orc, mesh, U_lim=x.api.MFaceBased(mesh), iters=1)
+    assert np.array_equal(f0[x._abi.FIELD_U], f1[x._abi.FIELD_U])
+    refU = _mface_loop(mesh, f0[x._abi.FIELD_U], f0[x._abi.FIELD_GRADU])
+    G1 = f1[x._abi.FIELD_GRADU]
+    assert np.max(np.abs(G1 - refU)) <= 1e-9 * np.max(np.abs(refU))
+    assert not np.array_equal(G1, f0[x._abi.FIELD_GRADU])

@@ -34,7 +34,7 @@ BC_NUT_WALL = 13
 TIME_STEADY, TIME_EULER = 0, 1
 DIV_LINEAR, DIV_UPWIND, DIV_LUST = 0, 1, 2
 GRAD_GAUSS, GRAD_MIDPOINT = 0, 1
-LIMITER_NONE, LIMITER_CELL, LIMITER_FACE = 0, 1, 2
+LIMITER_NONE, LIMITER_CELL, LIMITER_FACE, LIMITER_MFACE = 0, 1, 2, 3
 SOLVER_CG, SOLVER_BICGSTAB = 0, 1
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_DILU = 0, 1, 2
 TURB_LAMINAR, TURB_SMAGORINSKY, TURB_KOMEGA, TURB_KOMEGA_SST, TURB_KEQUATION, TURB_KOMEGA_LKE = 0, 1, 2, 3, 4, 5

@@ -79,9 +79,11 @@ class FaceBased:
 
 
 class MFaceBased:
-    """The modified face-based limiter: not implemented (each face thread
-    rewrites both cells' gradients while other faces read them, so the
-    reference's result depends on thread order)."""
+    """The modified face-based limiter (Calculate_0_gradient_mface_limiter.jl):
+    each internal face corrects both cells' gradients toward the face's value
+    bounds in turn.  Applied per cell in ascending face order, which is the
+    reference's kernel run on one thread (its parallel runs race on cells
+    that share faces); MFaceBased(mesh) as in the reference."""
 
     def __init__(self, *a, **k):
         pass
@@ -593,7 +595,9 @@ def _limiter(lim):
         return _abi.LIMITER_CELL, float(lim.level)
     if _kind(lim) is FaceBased:
         return _abi.LIMITER_FACE, 0.0
-    raise NotImplementedError("the CellBased and FaceBased gradient limiters are implemented (not MFaceBased)")
+    if _kind(lim) is MFaceBased:
+        return _abi.LIMITER_MFACE, 0.0
+    raise NotImplementedError(f"unknown gradient limiter {lim!r} (CellBased, FaceBased, MFaceBased)")
 
 
 def _solver_desc(s: SolverSetup) -> _abi.SolverSetupDesc:

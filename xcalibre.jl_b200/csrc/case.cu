@@ -789,8 +789,9 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
         (has_y() && (cfg.k_schemes.gradient == XCAL_GRAD_MIDPOINT || cfg.y_schemes.gradient == XCAL_GRAD_MIDPOINT)))
         build_midpoint(*m, stream);
     for (const xcal_schemes* sc : {&cfg.U_schemes, &cfg.p_schemes}) {
-        if (sc->limiter != XCAL_LIMITER_NONE && sc->limiter != XCAL_LIMITER_CELL && sc->limiter != XCAL_LIMITER_FACE)
-            fail(XCAL_ERR_UNSUPPORTED, "gradient limiter: CellBased or FaceBased");
+        if (sc->limiter != XCAL_LIMITER_NONE && sc->limiter != XCAL_LIMITER_CELL && sc->limiter != XCAL_LIMITER_FACE &&
+            sc->limiter != XCAL_LIMITER_MFACE)
+            fail(XCAL_ERR_UNSUPPORTED, "gradient limiter: CellBased, FaceBased or MFaceBased");
         if (sc->limiter == XCAL_LIMITER_CELL && !(sc->limiter_level >= 0.0 && sc->limiter_level <= 1.0))
             fail(XCAL_ERR_INVALID, "CellBased limiter level must be in [0, 1]");
     }
@@ -2077,6 +2078,8 @@ void Case::grad_p() {
         launch_limit_cell(stream, mv(), limD.p, p.p, gp, cfg.p_schemes.limiter_level);
     else if (cfg.p_schemes.limiter == XCAL_LIMITER_FACE)
         launch_limit_face_scalar(stream, mv(), limD.p, p.p, gp);
+    else if (cfg.p_schemes.limiter == XCAL_LIMITER_MFACE)
+        launch_limit_mface_scalar(stream, mv(), limOrd.p, limD.p, p.p, gp);
 }
 
 // fc - cc per cell_faces entry (storage order), 3 arrays of 2 nI
@@ -2091,6 +2094,15 @@ void Case::build_limiter(const DevMesh& m, cudaStream_t s) {
             t[2 * nk + k] = m.fcz[f] - m.ccz[i];
         }
     limD.upload(t, s);
+    // MFaceBased: per cell its entries by the reference's face id (fperm
+    // maps storage faces back to it)
+    std::vector<int> ord(nk);
+    for (int i = 0; i < m.nC; ++i) {
+        std::iota(ord.begin() + m.cf_off[i], ord.begin() + m.cf_off[i + 1], m.cf_off[i]);
+        std::sort(ord.begin() + m.cf_off[i], ord.begin() + m.cf_off[i + 1],
+                  [&](int a, int b) { return m.fperm[m.cf_face[a]] < m.fperm[m.cf_face[b]]; });
+    }
+    limOrd.upload(ord, s);
 }
 
 // Ri = rf - 0.5 (rP + rN) per internal face (correct_interpolation!,
@@ -2141,9 +2153,11 @@ void Case::turbulence() {
     if (limit) {
         // limit_gradient!(schemes.U.limiter, gradU, U) (RANS_laminar.jl:77,
         // LES_Smagorinsky.jl:120): CellBased once per component row,
-        // FaceBased once for the tensor
+        // FaceBased and MFaceBased once for the tensor
         if (cfg.U_schemes.limiter == XCAL_LIMITER_FACE)
             launch_limit_face_vector(stream, mv(), limD.p, Ucp, g);
+        else if (cfg.U_schemes.limiter == XCAL_LIMITER_MFACE)
+            launch_limit_mface_vector(stream, mv(), limOrd.p, limD.p, Ucp, g);
         else
             for (int a = 0; a < 3; ++a)
                 launch_limit_cell(stream, mv(), limD.p, Uc[a].p, g + 3 * a, cfg.U_schemes.limiter_level);

@@ -168,6 +168,7 @@ struct Case {
     DBuf<double> nonorth;  // non-orthogonal correctors: per internal face w, e, T (7 x nI)
     DBuf<double> midR;     // Midpoint gradients: per internal face rf - 0.5 (rP + rN) (3 x nI)
     DBuf<double> limD;     // CellBased limiter: fc - cc per cell_faces entry (3 x 2 nI)
+    DBuf<int> limOrd;      // MFaceBased: each cell's cell_faces entries in ascending reference face id
     DBuf<double> Uc[3], p, mdot, nueff, gradp[3], gradU[9], rD, Hv[3], divHv, nut, nutf, Uf[3], pf, rDf, Delta, prev,
         courant, dx13, resbuf, cmax, io;  // io: staging of one field component in the original order
     // RANS{KOmega}: k, omega, production / dissipation per cell, a scratch

@@ -47,6 +47,12 @@ void launch_limit_face_vector(cudaStream_t s, const MeshView& m, const double* D
                               double* const g[9]);
 void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const double* F, double* const g[3],
                        double level);
+// MFaceBased: a cell's internal faces in ascending face order (ord: the
+// cell_faces entries so sorted), each correcting the gradient in turn
+void launch_limit_mface_scalar(cudaStream_t s, const MeshView& m, const int* ord, const double* D, const double* F,
+                               double* const g[3]);
+void launch_limit_mface_vector(cudaStream_t s, const MeshView& m, const int* ord, const double* D,
+                               const double* const U[3], double* const g[9]);
 // RANS{KOmega}: sources, k / omega assembly, BCs + relaxation, the omega
 // wall rows, bound!, nut = k / omega; nueff = nu + nutf
 void launch_kw_sources(cudaStream_t s, int nC, const double* const g[9], const double* nut, const double* omega,

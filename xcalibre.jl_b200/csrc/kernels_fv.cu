@@ -1530,6 +1530,108 @@ void launch_limit_cell(cudaStream_t s, const MeshView& m, const double* D, const
     k_limit_cell<<<nblk(m.nC), TPB, 0, s>>>(m, D, F, g[0], g[1], g[2], level);
     XCAL_CHECK_LAUNCH();
 }
+// limit_gradient!(::MFaceBased) (Calculate_0_gradient_mface_limiter.jl):
+// each internal face moves both cells' gradients so that the extrapolation
+// grad . d (d = fc - cc) stays within [min, max](F_own, F_nei) - F_cell,
+// grad += d (bound - grad . d) / (d . d).  A face's two updates read and
+// write different cells, so a cell's result is its own faces' updates
+// applied in turn; here in ascending face order (ord: the cell's cell_faces
+// entries sorted by the reference's face id), the reference's kernel run on
+// one thread.  (Its parallel runs race on cells that share faces.)
+__global__ void k_limit_mface_scalar(MeshView m, const int* __restrict__ ord, const double* __restrict__ D,
+                                     const double* __restrict__ F, double* gx, double* gy, double* gz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    const int nk = 2 * (m.nF - m.nB);
+    double x = gx[i], y = gy[i], z = gz[i];
+    const double Fi = F[i];
+    for (int e = m.cf_off[i]; e < m.cf_off[i + 1]; ++e) {
+        const int k = ord[e];
+        const double Fo = F[m.cf_nb[k]];
+        const bool own = m.cf_sign[k] > 0;
+        const double F1 = own ? Fi : Fo, F2 = own ? Fo : Fi;
+        const double dmax = jl_max(F1, F2) - Fi, dmin = jl_min(F1, F2) - Fi;
+        const double d0 = D[k], d1 = D[nk + k], d2 = D[2 * nk + k];
+        const double fval = (x * d0 + y * d1) + z * d2;
+        const double dd = (d0 * d0 + d1 * d1) + d2 * d2;
+        if (fval > dmax || fval < dmin) {
+            const double t = (fval > dmax ? dmax : dmin) - fval;
+            x = x + (d0 * t) / dd;
+            y = y + (d1 * t) / dd;
+            z = z + (d2 * t) / dd;
+        }
+    }
+    gx[i] = x;
+    gy[i] = y;
+    gz[i] = z;
+}
+
+// Julia's isless / isequal on Float64 (NaN above everything, -0.0 < 0.0)
+__device__ __forceinline__ bool jl_isless(double a, double b) {
+    if (isnan(a)) return false;
+    if (isnan(b)) return true;
+    return a < b || (a == b && signbit(a) && !signbit(b));
+}
+__device__ __forceinline__ bool jl_isequal(double a, double b) {
+    if (isnan(a) || isnan(b)) return isnan(a) && isnan(b);
+    return a == b && signbit(a) == signbit(b);
+}
+// isless of two 3-vectors: Base's lexicographic cmp (the first entry that
+// differs by isequal decides by isless)
+__device__ __forceinline__ bool lex_isless(const double* a, const double* b) {
+    for (int j = 0; j < 3; ++j)
+        if (!jl_isequal(a[j], b[j])) return jl_isless(a[j], b[j]);
+    return false;
+}
+
+// the tensor form: min / max(U_own, U_nei) are Base's generic min / max of
+// two vectors, whole vectors chosen by the lexicographic isless; each row a
+// of grad U (d u_a / d x_b) is corrected against component a of the bounds
+__global__ void k_limit_mface_vector(MeshView m, const int* __restrict__ ord, const double* __restrict__ D,
+                                     const double* __restrict__ U0, const double* __restrict__ U1,
+                                     const double* __restrict__ U2, GradW9 Gd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nC) return;
+    const int nk = 2 * (m.nF - m.nB);
+    double G[9];
+    for (int q = 0; q < 9; ++q) G[q] = Gd.g[q][i];
+    const double ui[3] = {U0[i], U1[i], U2[i]};
+    for (int e = m.cf_off[i]; e < m.cf_off[i + 1]; ++e) {
+        const int k = ord[e];
+        const int o = m.cf_nb[k];
+        const double uo[3] = {U0[o], U1[o], U2[o]};
+        const bool own = m.cf_sign[k] > 0;
+        const double* F1 = own ? ui : uo;
+        const double* F2 = own ? uo : ui;
+        const bool lt = lex_isless(F2, F1);  // max = F1 if F2 < F1, min = F2 then
+        const double* mx = lt ? F1 : F2;
+        const double* mn = lt ? F2 : F1;
+        const double d[3] = {D[k], D[nk + k], D[2 * nk + k]};
+        const double dd = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2];
+        for (int a = 0; a < 3; ++a) {
+            const double dmax = mx[a] - ui[a], dmin = mn[a] - ui[a];
+            const double fval = (G[3 * a] * d[0] + G[3 * a + 1] * d[1]) + G[3 * a + 2] * d[2];
+            if (fval > dmax || fval < dmin) {
+                const double t = (fval > dmax ? dmax : dmin) - fval;
+                for (int b = 0; b < 3; ++b) G[3 * a + b] = G[3 * a + b] + (d[b] * t) / dd;
+            }
+        }
+    }
+    for (int q = 0; q < 9; ++q) Gd.g[q][i] = G[q];
+}
+
+void launch_limit_mface_scalar(cudaStream_t s, const MeshView& m, const int* ord, const double* D, const double* F,
+                               double* const g[3]) {
+    k_limit_mface_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, ord, D, F, g[0], g[1], g[2]);
+    XCAL_CHECK_LAUNCH();
+}
+void launch_limit_mface_vector(cudaStream_t s, const MeshView& m, const int* ord, const double* D,
+                               const double* const U[3], double* const g[9]) {
+    GradW9 G;
+    for (int q = 0; q < 9; ++q) G.g[q] = g[q];
+    k_limit_mface_vector<<<nblk(m.nC), TPB, 0, s>>>(m, ord, D, U[0], U[1], U[2], G);
+    XCAL_CHECK_LAUNCH();
+}
 void launch_limit_face_scalar(cudaStream_t s, const MeshView& m, const double* D, const double* F,
                               double* const g[3]) {
     k_limit_face_scalar<<<nblk(m.nC), TPB, 0, s>>>(m, D, F, g[0], g[1], g[2]);
