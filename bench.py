@@ -61,10 +61,12 @@ def parse():
     ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="serving: device-memory budget (GB)")
     ap.add_argument("--converge-cap", type=int, default=1200,
                     help="time-to-convergence block: SIMPLE iteration cap per precision (0 = skip)")
-    ap.add_argument("--only", choices=["les", "serving", "batch", "converge", "step-window"], default=None,
+    ap.add_argument("--only", choices=["les", "serving", "batch", "converge", "step-window", "les-window"],
+                    default=None,
                     help="run one secondary workload alone and print its block as the line (profiling); "
                          "step-window: --steps SIMPLE iterations of the channel case after --warmup, between "
-                         "cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off); les-window: the same for "
+                         "--steps host-polled PISO steps of the --les-size LES box")
     ap.add_argument("--inner-cg", type=int, default=None,
                     help="mixed precision: form of the FP32 inner CG (xcal_case_set_inner_cg; default: the "
                          "library's)")
@@ -609,6 +611,37 @@ def step_window(x, A, args, local):
     return out
 
 
+def les_window(x, A, args, local):
+    """--warmup PISO steps of the --les-size LES box (the les block's case),
+    then --steps more between cudaProfilerStart/Stop.  Host-polled, not graph
+    mode: ncu profiles no kernel node of a graph with conditional nodes (the
+    graph's device-driven Krylov loops); the kernels are the same."""
+    import torch
+    n = args.les_size
+    mesh = x.build_mesh3(x.periodic_box_polymesh(n, seed=0), device=local)
+    U0 = x.cases.fourier_field(mesh, seed=0)
+    model, config = x.cases.periodic_les_case(mesh, steps=args.steps, U0=U0, precision="mixed", device=local)
+    cfg, keep = x.build_config(model, config, pref=0.0)
+    ctx = x.Context(local)
+    dm = x.DeviceMesh(ctx, mesh)
+    case = x.Case(dm, cfg)
+    case.set_field(A.FIELD_U, model.momentum.U)
+    case.set_field(A.FIELD_P, model.momentum.p)
+    case.piso_step(args.warmup)
+    torch.cuda.synchronize()
+    l0 = x.launch_count()
+    torch.cuda.profiler.start()
+    res, _ = case.piso_step(args.steps)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    out = {"workload": f"periodic LES box {n}^3 = {mesh.n_cells} cells, mixed, host-polled",
+           "warmup": args.warmup, "steps": args.steps, "launches": x.launch_count() - l0,
+           "residuals_last": [float(v) for v in res[-1]]}
+    case.close()
+    dm.close()
+    return out
+
+
 def e2e_measure(x, A, case, mesh, args, world):
     """Same metric through the public API with host buffers: every step copies
     U and p host->device, runs one SIMPLE iteration and reads them back."""
@@ -654,7 +687,8 @@ def main():
             return converge_measure(x, A, m, args, local)
         blk = {"les": lambda: les_measure(x, A, args, local), "serving": lambda: serve_measure(x, args, local),
                "batch": lambda: batch_measure(x, args, local), "converge": conv_only,
-               "step-window": lambda: step_window(x, A, args, local)}[args.only]()
+               "step-window": lambda: step_window(x, A, args, local),
+               "les-window": lambda: les_window(x, A, args, local)}[args.only]()
         if rank == 0:
             print(json.dumps({"only": args.only, **blk}), flush=True)
         if world > 1:
