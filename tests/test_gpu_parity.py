@@ -178,11 +178,12 @@ def test_dilu_modes_parity(x, orc, ctx, mode):
 
 
 def test_dilu_grid_mixed_identical(x, ctx):
-    """Mixed precision: the FP32 momentum DILU as per-level kernels and as
-    one cooperative launch over every level give the same run bit for bit."""
+    """Mixed precision: the FP32 momentum DILU as one-block sweeps (next
+    level's rows loaded before each barrier), as per-level kernels and as one
+    cooperative launch over every level give the same run bit for bit."""
     mesh = x.build_mesh3(x.channel_polymesh(40, 30, 30, seed=8))
     out = []
-    for mode in (2, 3):
+    for mode in (1, 2, 3):
         model, config = x.cases.channel_case(mesh, iterations=3, precision="mixed")
         cfg, keep = x.build_config(model, config)
         dm = x.DeviceMesh(ctx, mesh)
