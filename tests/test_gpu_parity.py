@@ -198,3 +198,21 @@ def test_dilu_grid_mixed_identical(x, ctx):
     for o in out[1:]:
         for a, b in zip(out[0], o):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_neumann_p_parity(x, orc, ctx, graph):
+    """p with a Neumann inlet (neumann.jl, scalar: a fixed normal gradient in
+    the face value, the Laplacian's boundary source and the interpolation)
+    through SIMPLE: GPU equal to the oracle, host-polled and in graph mode."""
+    mesh = x.build_mesh3(x.channel_polymesh(12, 7, 6, seed=6))
+    model, config = x.cases.channel_case(mesh, iterations=4)
+    config.boundaries["p"] = x.api.assign(region=mesh, p=[x.api.Neumann("inlet", 0.05), x.api.Dirichlet("outlet", 0.0),
+                                                           x.api.Wall("walls")])["p"]
+    g, o, keep = make_pair(x, orc, ctx, mesh, model, config)
+    if graph:
+        g.set_graph_mode(True)
+    rg, _ = g.simple_iterate(4)
+    ro, _ = o.simple_iterate(4)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    compare_fields(x, g, o)
