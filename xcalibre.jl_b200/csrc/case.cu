@@ -1209,11 +1209,12 @@ void Case::komega_lke() {
     V.nC = mesh->nC;
     V.nu = cfg.nu;
     V.eta = lke_eta;
+    // D2 (omega's cross diffusion) enters with sign -1: - Si(dkdomegadx, omega)
     auto transport = [&](int e, double* phi, const BCTable& T, const xcal_schemes& sc, const xcal_solver_setup& SS,
                          const double* D, const double* D2, const double* src, bool constrain, int slot) {
         launch_interp_scalar(stream, mv(), bcNut.view(), nueffS.p, fmu.p, nullptr, 0.0);
         launch_assemble_scalar(stream, mv(), P.view(), mdot.p, fmu.p, 0.0, 1.0, nullptr, 0.0, phi, D, D2, src, P.nz.p,
-                               P.b[0].p, sc.time, sc.divergence, cfg.dt, -1.0);
+                               P.b[0].p, sc.time, sc.divergence, cfg.dt, /*d2_sign=*/-1.0);
         launch_bc_relax_scalar(stream, mv(), P.view(), T.view(), P.nz.p, P.b[0].p, mdot.p, fmu.p, 0.0, 1.0, nullptr,
                                0.0, D2 ? 1 : 0, phi, SS.relax, sc.divergence);
         if (constrain && nwall)
