@@ -120,9 +120,13 @@ void locality_order(int n, const double* c, std::vector<int>& perm) {
         }
         key[i] = spread(q[0]) | (spread(q[1]) << 1) | (spread(q[2]) << 2);
     }
+    // (key, index) pairs sorted in place: the order of (key, then index),
+    // without an indirect key lookup per comparison
+    std::vector<std::pair<uint64_t, int>> kv(n);
+    for (int i = 0; i < n; ++i) kv[i] = {key[i], i};
+    std::sort(kv.begin(), kv.end());
     perm.resize(n);
-    std::iota(perm.begin(), perm.end(), 0);
-    std::sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] != key[b] ? key[a] < key[b] : a < b; });
+    for (int i = 0; i < n; ++i) perm[i] = kv[i].second;
 }
 
 static DevMesh* upload_mesh_ordered(const xcal_mesh_desc* d, cudaStream_t s, std::unique_ptr<DevMesh> m);
@@ -157,14 +161,33 @@ DevMesh* upload_mesh(const xcal_mesh_desc* d0, cudaStream_t s) {
     locality_order(nC, d0->cell_centre, m->perm);
     m->inv.resize(nC);
     for (int st = 0; st < nC; ++st) m->inv[m->perm[st]] = st;
+    // internal faces by (storage owner, storage neighbour, id): a counting
+    // sort on the storage owner (ids ascending within each owner), then each
+    // owner's few faces by (storage neighbour, id)
     m->fperm.resize(nF);
-    std::iota(m->fperm.begin(), m->fperm.end(), 0);
-    std::sort(m->fperm.begin() + nB, m->fperm.end(), [&](int a, int b) {
-        int oa = m->inv[d0->face_owner[a]], ob = m->inv[d0->face_owner[b]];
-        if (oa != ob) return oa < ob;
-        int na = m->inv[d0->face_neigh[a]], nb = m->inv[d0->face_neigh[b]];
-        return na != nb ? na < nb : a < b;
-    });
+    std::iota(m->fperm.begin(), m->fperm.begin() + nB, 0);
+    {
+        std::vector<int> start(nC + 1, 0);
+        for (int f = nB; f < nF; ++f) ++start[m->inv[d0->face_owner[f]] + 1];
+        for (int c = 0; c < nC; ++c) start[c + 1] += start[c];
+        std::vector<int> next(start.begin(), start.end() - 1);
+        for (int f = nB; f < nF; ++f) m->fperm[nB + next[m->inv[d0->face_owner[f]]]++] = f;
+        for (int c = 0; c < nC; ++c) {
+            int* b = m->fperm.data() + nB + start[c];
+            const int len = start[c + 1] - start[c];
+            for (int a = 1; a < len; ++a) {  // insertion sort by (neighbour, id)
+                const int f = b[a], nf = m->inv[d0->face_neigh[f]];
+                int j = a - 1;
+                while (j >= 0) {
+                    const int g = b[j], ng = m->inv[d0->face_neigh[g]];
+                    if (ng < nf || (ng == nf && g < f)) break;
+                    b[j + 1] = g;
+                    --j;
+                }
+                b[j + 1] = f;
+            }
+        }
+    }
     m->finv.resize(nF);
     for (int fs = 0; fs < nF; ++fs) m->finv[m->fperm[fs]] = fs;
     // permuted copies of the Mesh3 arrays
