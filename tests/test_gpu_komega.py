@@ -266,3 +266,21 @@ def test_komega_periodic_channel_parity(x, orc, ctx, sst):
     ro, _ = o.simple_iterate(3)
     assert rel(rg, ro) <= TOL, (rg, ro)
     _check(x, g, o)
+
+
+def test_komega_dilu_k_jacobi_p_parity(x, orc, ctx):
+    """k and omega DILU-preconditioned while p is Jacobi: the p system's
+    storage, which k and omega share, carries the DILU levels their solves
+    need.  GPU equal to the oracle."""
+    mesh = skewed_channel(x, n=(12, 7, 6), seed=11)
+    model, config = komega_channel_case(x, mesh, 6, "DILU")
+    A = x.api
+    config.solvers["p"] = A.SolverSetup(solver=A.Cg(), preconditioner=A.Jacobi(), convergence=1e-7, relax=0.3,
+                                        rtol=1e-2)
+    cfg, keep = x.build_config(model, config)
+    assert cfg.p_solver.precond == x._abi.PRECOND_JACOBI and cfg.k_solver.precond == x._abi.PRECOND_DILU
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg, False)
+    rg, _ = g.simple_iterate(6)
+    ro, _ = o.simple_iterate(6)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    _check(x, g, o)

@@ -145,3 +145,21 @@ def test_lke_mixed_precision(x, ctx):
         dm.close()
     for f in KL_FIELDS:
         assert rel(out["mixed"][f], out["fp64"][f]) <= 1e-3, f
+
+
+def test_lke_dilu_scalars_jacobi_p_parity(x, orc, ctx):
+    """kl, omega and k DILU-preconditioned while p is Jacobi (the p system's
+    storage carries their DILU levels): GPU equal to the oracle."""
+    mesh = flatplate(x, 30, 14, seed=5)
+    model, config = x.cases.lke_flatplate_case(mesh, 8, precond=x.api.DILU)
+    A = x.api
+    config.solvers["p"] = A.SolverSetup(solver=A.Cg(), preconditioner=A.Jacobi(), convergence=1e-8, relax=0.2,
+                                        rtol=1e-3)
+    cfg, keep = x.build_config(model, config)
+    assert cfg.p_solver.precond == x._abi.PRECOND_JACOBI and cfg.kl_solver.precond == x._abi.PRECOND_DILU
+    g, o, dm = _pair(x, orc, ctx, mesh, model, cfg)
+    rg, _ = g.simple_iterate(8)
+    ro, _ = o.simple_iterate(8)
+    assert rel(rg, ro) <= TOL, (rg, ro)
+    for f in ALL:
+        assert rel(g.get_field(getattr(x._abi, f)), o.get_field(getattr(x._abi, f))) <= TOL, f

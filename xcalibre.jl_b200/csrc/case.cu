@@ -737,7 +737,13 @@ Case::Case(xcal_ctx* c, const DevMesh* m, const xcal_config* cf) : ctx(c), mesh(
     int nC = m->nC, nF = m->nF;
     std::vector<xcal_bc> bU(cfg.bc_U, cfg.bc_U + cfg.n_bc_U), bP(cfg.bc_p, cfg.bc_p + cfg.n_bc_p);
     build_equation(U, *m, bU, 3, cfg.U_solver.precond == XCAL_PRECOND_DILU, stream);
-    build_equation(P, *m, bP, 1, cfg.p_solver.precond == XCAL_PRECOND_DILU, stream);
+    // the p system's storage also carries k, omega, kl and the wall distance:
+    // its DILU levels are needed when any solve on it is DILU-preconditioned
+    auto dilu = [](const xcal_solver_setup& ss) { return ss.precond == XCAL_PRECOND_DILU; };
+    const bool p_dilu = dilu(cfg.p_solver) || (has_k() && dilu(cfg.k_solver)) ||
+                        (rans_kw() && dilu(cfg.omega_solver)) || (lke() && dilu(cfg.kl_solver)) ||
+                        (has_y() && dilu(cfg.y_solver));
+    build_equation(P, *m, bP, 1, p_dilu, stream);
     build_bc_table(bcU, *m, cfg.bc_U, cfg.n_bc_U, 3, &U, stream);
     build_bc_table(bcP, *m, cfg.bc_p, cfg.n_bc_p, 1, &P, stream);
     build_bc_table(bcNut, *m, cfg.bc_nut, cfg.n_bc_nut, 1, nullptr, stream);
