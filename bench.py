@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=8.0)
     ap.add_argument("--serve-iters", type=int, default=1500, help="serving: SIMPLE iteration cap per request")
     ap.add_argument("--serve-budget-gb", type=float, default=40.0, help="serving: device-memory budget (GB)")
+    ap.add_argument("--serve-max-cases", type=int, default=64, help="serving: most requests resident at once")
     ap.add_argument("--converge-cap", type=int, default=1200,
                     help="time-to-convergence block: SIMPLE iteration cap per precision (0 = skip)")
     ap.add_argument("--only", choices=["les", "serving", "batch", "converge", "step-window", "les-window"],
@@ -450,7 +451,8 @@ def serve_measure(x, args, local):
         r.build()
     ctx = x.Context(local)
     budget = int(args.serve_budget_gb * (1 << 30))
-    srv = serve.Server(ctx, budget_bytes=budget, max_cases=64, precision="mixed", max_iters=args.serve_iters,
+    srv = serve.Server(ctx, budget_bytes=budget, max_cases=args.serve_max_cases, precision="mixed",
+                       max_iters=args.serve_iters,
                        convergence=1e-6)
     l0 = x.launch_count()
     if world > 1:
@@ -465,7 +467,7 @@ def serve_measure(x, args, local):
     s.update({"workload": f"{len(reqs)} steady cavity/channel requests, N log-uniform [1e3, {args.serve_nmax:g}], "
                           f"Re U[100,2000], aspect U[1,4], Poisson {args.serve_rate:g}/s, mixed, resid 1e-6, "
                           f"cap {args.serve_iters} iterations",
-              "rate_per_s": args.serve_rate, "budget_bytes": budget, "max_cases": 64,
+              "rate_per_s": args.serve_rate, "budget_bytes": budget, "max_cases": args.serve_max_cases,
               "converged_ge_1e5_cells": "%d/%d" % (sum(r.converged for r in res if r.n_cells >= 1e5),
                                                     sum(1 for r in res if r.n_cells >= 1e5)),
               "max_active": max((t[1] for t in srv.timeline), default=0),
