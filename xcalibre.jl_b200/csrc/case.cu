@@ -478,11 +478,30 @@ void build_equation(Equation& E, const DevMesh& m, const std::vector<xcal_bc>& b
     E.diag.resize(n);
     for (int c = 0; c < n; ++c) E.diag[c] = E.find(c, c);
     std::vector<int> trans(E.nnz, 0), cf_slot(m.cf_face.size()), fslot(m.nI);
-    for (int i = 0; i < n; ++i)
-        for (int k = 0, b = E.base(i); k < E.len[i]; ++k) trans[b + SELL_C * k] = E.find(E.colval[b + SELL_C * k], i);
     for (int c = 0; c < n; ++c)
         for (int k = m.cf_off[c]; k < m.cf_off[c + 1]; ++k) cf_slot[k] = E.find(c, m.cf_nb[k]);
     for (int f = m.nB; f < m.nF; ++f) fslot[f - m.nB] = E.find(m.owner[f], m.neigh[f]);
+    // trans: the slot of (col, row) per entry.  The diagonal is its own; an
+    // internal face pairs (owner, neigh) with (neigh, owner); the periodic
+    // couplings (no face) are looked up row by row
+    {
+        std::vector<char> set(E.nnz, 0);
+        for (int c = 0; c < n; ++c) {
+            trans[E.diag[c]] = E.diag[c];
+            set[E.diag[c]] = 1;
+        }
+        for (int f = m.nB; f < m.nF; ++f) {
+            const int a = fslot[f - m.nB], b = E.find(m.neigh[f], m.owner[f]);
+            trans[a] = b;
+            trans[b] = a;
+            set[a] = set[b] = 1;
+        }
+        for (int i = 0; i < n; ++i)
+            for (int k = 0, b = E.base(i); k < E.len[i]; ++k) {
+                const int e = b + SELL_C * k;
+                if (!set[e]) trans[e] = E.find(E.colval[e], i);
+            }
+    }
     E.d_slice.upload(E.slice, s);
     E.d_len.upload(E.len, s);
     E.d_colval.upload(E.colval, s);
