@@ -1721,7 +1721,6 @@ static void scalar_grad(Case& C, const std::vector<double>& phi, std::vector<dou
 // 1000 times until its residual is below the convergence, then
 // y = -|grad phi| + sqrt(|grad phi|^2 + 2 phi) (:80-92)
 static void wall_distance(Case& C) {
-    const Mesh& m = *C.m;
     const xcal_solver_setup& SS = C.cfg.y_solver;
     std::vector<double> phi(C.nC, 0.0), prev(C.nC), ones_f(C.nF, 1.0), ones_c(C.nC, 1.0), phif(C.nF), g[3];
     for (int d = 0; d < 3; ++d) g[d].assign(C.nC, 0.0);
